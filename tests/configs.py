@@ -1,0 +1,99 @@
+"""Run configurations used by the parity tests and the benchmark.
+
+Each builder returns an ``amrclaw_b200.data.ClawRunData`` exactly like a
+reference ``setrun.py`` would: the regression-test setups restate
+``tests/advection_2d_square/setrun.py`` and ``tests/acoustics_2d_radial/setrun.py``
+of the reference; the benchmark workloads restate the configurations the
+benchmark is quoted on (2D advection, 2D Euler quadrants, 3D Euler blast,
+2D acoustics pulse, 3D swirl), with optional down-scaling for fast tests.
+"""
+from __future__ import annotations
+
+import math
+
+from amrclaw_b200.data import ClawRunData
+
+
+def advection_square_regression() -> ClawRunData:
+    """tests/advection_2d_square/setrun.py of the reference (gauges 1, 2 pinned)."""
+    rd = ClawRunData(num_dim=2)
+    p = rd.probdata
+    p.add_param("problem", "advection_square")
+    p.add_param("u", 0.5)
+    p.add_param("v", 1.0)
+    c = rd.clawdata
+    c.lower = [0.0, 0.0]; c.upper = [1.0, 1.0]; c.num_cells = [50, 50]
+    c.num_eqn = 1; c.num_waves = 1; c.num_aux = 0
+    c.output_style = 1; c.num_output_times = 1; c.tfinal = 0.4; c.output_t0 = True
+    c.dt_variable = True; c.dt_initial = 0.016; c.dt_max = 1e99; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.steps_max = 100000; c.order = 2; c.transverse_waves = "all"; c.limiter = ["vanleer"]
+    c.bc_lower = ["periodic", "periodic"]; c.bc_upper = ["periodic", "periodic"]
+    rd.gaugedata.gauges = [[1, 0.65, 0.4, 0.0, 10.0], [2, 0.2, 0.8, 0.0, 10.0]]
+    a = rd.amrdata
+    a.amr_levels_max = 3; a.refinement_ratios_x = [2, 2]; a.refinement_ratios_y = [2, 2]; a.refinement_ratios_t = [2, 2]
+    a.flag2refine = True; a.flag2refine_tol = 0.05; a.regrid_interval = 2; a.regrid_buffer_width = 3
+    a.clustering_cutoff = 0.7
+    rd.regiondata.regions = [[1, 1, 0, 1e10, 0., 1., 0., 1.], [1, 3, 0, 1e10, 0., 1., 0., 0.7]]
+    return rd
+
+
+def acoustics_radial_regression() -> ClawRunData:
+    """tests/acoustics_2d_radial/setrun.py of the reference (gauges 0, 1, 2 pinned)."""
+    rd = ClawRunData(num_dim=2)
+    p = rd.probdata
+    p.add_param("problem", "acoustics_cosine")
+    p.add_param("rho", 1.0)
+    p.add_param("bulk", 4.0)
+    c = rd.clawdata
+    c.lower = [-1.0, -1.0]; c.upper = [1.0, 1.0]; c.num_cells = [50, 50]
+    c.num_eqn = 3; c.num_waves = 2; c.num_aux = 0
+    c.output_style = 1; c.num_output_times = 1; c.tfinal = 0.2; c.output_t0 = True
+    c.dt_variable = True; c.dt_initial = 1e-2; c.dt_max = 1e99; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.steps_max = 50000; c.order = 2; c.transverse_waves = 2; c.limiter = ["vanleer", "vanleer"]
+    c.bc_lower = ["extrap", "extrap"]; c.bc_upper = ["extrap", "extrap"]
+    rd.gaugedata.gauges = [[0, 0.0, 0.0, 0., 10.], [1, 0.7, 0.0, 0., 10.],
+                           [2, 0.7 / math.sqrt(2.), 0.7 / math.sqrt(2.), 0., 10.]]
+    a = rd.amrdata
+    a.amr_levels_max = 3; a.refinement_ratios_x = [2, 2]; a.refinement_ratios_y = [2, 2]; a.refinement_ratios_t = [2, 2]
+    a.flag2refine = True; a.flag2refine_tol = 0.2; a.regrid_interval = 2; a.regrid_buffer_width = 2
+    a.clustering_cutoff = 0.7
+    rd.regiondata.regions = [[1, 1, 0, 1e10, -1., 1., -1., 1.], [1, 3, 0, 1e10, -1., 1., -.2, .2]]
+    return rd
+
+
+def advection_square_bench(n: int = 50, tfinal: float = 2.0, levels: int = 3) -> ClawRunData:
+    """2D constant advection, periodic, u=(0.5,1), square IC, MC limiter, buffer 2, tol 0.05."""
+    rd = advection_square_regression()
+    c = rd.clawdata
+    c.num_cells = [n, n]; c.tfinal = tfinal; c.limiter = ["mc"]
+    rd.gaugedata.gauges = []
+    rd.regiondata.regions = []
+    a = rd.amrdata
+    a.amr_levels_max = levels; a.regrid_buffer_width = 2
+    a.refinement_ratios_x = [2] * max(1, levels - 1); a.refinement_ratios_y = [2] * max(1, levels - 1)
+    a.refinement_ratios_t = [2] * max(1, levels - 1)
+    return rd
+
+
+def euler_quadrants(n: int = 100, levels: int = 4, tfinal: float = 0.8, ratio: int = 2) -> ClawRunData:
+    """2D Euler four-quadrant Riemann problem, Roe + entropy fix, density flagging at 0.1."""
+    rd = ClawRunData(num_dim=2)
+    p = rd.probdata
+    p.add_param("problem", "euler_quadrants")
+    p.add_param("gamma", 1.4)
+    p.add_param("efix", 1)
+    p.add_param("flag_component", 1)
+    c = rd.clawdata
+    c.lower = [0.0, 0.0]; c.upper = [1.0, 1.0]; c.num_cells = [n, n]
+    c.num_eqn = 4; c.num_waves = 4; c.num_aux = 0
+    c.output_style = 1; c.num_output_times = 1; c.tfinal = tfinal; c.output_t0 = False
+    c.dt_variable = True; c.dt_initial = 5e-4; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.order = 2; c.transverse_waves = 2; c.limiter = ["mc"] * 4
+    c.bc_lower = ["extrap", "extrap"]; c.bc_upper = ["extrap", "extrap"]
+    a = rd.amrdata
+    a.amr_levels_max = levels
+    a.refinement_ratios_x = [ratio] * max(1, levels - 1); a.refinement_ratios_y = [ratio] * max(1, levels - 1)
+    a.refinement_ratios_t = [ratio] * max(1, levels - 1)
+    a.flag2refine = True; a.flag2refine_tol = 0.1; a.regrid_interval = 2; a.regrid_buffer_width = 2
+    a.clustering_cutoff = 0.7
+    return rd
