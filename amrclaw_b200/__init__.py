@@ -1,0 +1,129 @@
+"""amrclaw_b200: B200-native patch-advance path of AMRClaw.
+
+Python side of the drop-in boundary: ``ClawRunData`` mirrors the reference's
+``setrun.py`` objects and writes the same data files; ``Solver`` drives the CUDA
+library through its C ABI (``include/amrclaw_b200.h``). There is no CPU
+fallback: without the built library on a CUDA device the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+
+from .data import ClawRunData  # noqa: F401
+from . import _lib
+
+__all__ = ["ClawRunData", "Solver", "AmrError"]
+
+
+class AmrError(RuntimeError):
+    pass
+
+
+def _check(lib, rc: int, what: str) -> None:
+    if rc != 0:
+        msg = lib.amrgpu_last_error()
+        raise AmrError("%s failed: %s" % (what, msg.decode() if msg else "error %d" % rc))
+
+
+class Solver:
+    """One AMR run on the GPU (the reference's ``amr2`` program from init to tfinal)."""
+
+    def __init__(self, rundata_or_dir, outdir: str | None = None, write_output: bool = False, batched: bool = True):
+        self._lib = _lib.load()
+        if isinstance(rundata_or_dir, ClawRunData):
+            self._tmp = tempfile.TemporaryDirectory(prefix="amrgpu_")
+            rundir = rundata_or_dir.write(self._tmp.name)
+        else:
+            self._tmp = None
+            rundir = str(rundata_or_dir)
+        self.rundir = rundir
+        self.outdir = outdir or rundir
+        if write_output:
+            os.makedirs(self.outdir, exist_ok=True)
+        h = ctypes.c_void_p()
+        _check(self._lib, self._lib.amrgpu_init(rundir.encode(), self.outdir.encode(), int(write_output), ctypes.byref(h)),
+               "amrgpu_init")
+        self._h = h
+        self.set_batched(batched)
+
+    def set_batched(self, batched: bool) -> None:
+        _check(self._lib, self._lib.amrgpu_set_batched(self._h, int(batched)), "amrgpu_set_batched")
+
+    def run(self, max_cycles: int = 0) -> None:
+        _check(self._lib, self._lib.amrgpu_run(self._h, int(max_cycles)), "amrgpu_run")
+
+    def level_advance(self, level: int):
+        dt = ctypes.c_double(); cfl = ctypes.c_double()
+        _check(self._lib, self._lib.amrgpu_level_advance(self._h, level, ctypes.byref(dt), ctypes.byref(cfl)),
+               "amrgpu_level_advance")
+        return dt.value, cfl.value
+
+    def update(self, level: int) -> None:
+        _check(self._lib, self._lib.amrgpu_update(self._h, level), "amrgpu_update")
+
+    def regrid(self, lbase: int) -> None:
+        _check(self._lib, self._lib.amrgpu_regrid(self._h, lbase), "amrgpu_regrid")
+
+    def valout(self, outdir: str) -> None:
+        os.makedirs(outdir, exist_ok=True)
+        _check(self._lib, self._lib.amrgpu_valout(self._h, outdir.encode()), "amrgpu_valout")
+
+    def mass(self) -> float:
+        m = ctypes.c_double()
+        _check(self._lib, self._lib.amrgpu_mass(self._h, ctypes.byref(m)), "amrgpu_mass")
+        return m.value
+
+    def info(self) -> dict:
+        out = (ctypes.c_double * 11)()
+        _check(self._lib, self._lib.amrgpu_info(self._h, out, 11), "amrgpu_info")
+        keys = ["time", "cell_updates", "coarse_steps", "lfine", "step_seconds", "regrid_seconds", "mass0",
+                "cflmax", "kernels", "pool_peak_bytes", "substeps"]
+        return dict(zip(keys, list(out)))
+
+    def grids(self) -> np.ndarray:
+        n = ctypes.c_int()
+        _check(self._lib, self._lib.amrgpu_grids(self._h, None, 0, ctypes.byref(n)), "amrgpu_grids")
+        a = np.zeros((n.value, 6), dtype=np.int32)
+        _check(self._lib, self._lib.amrgpu_grids(self._h, a.ctypes.data_as(_lib.c_int_p), n.value, ctypes.byref(n)),
+               "amrgpu_grids")
+        return a
+
+    def values(self) -> np.ndarray:
+        n = ctypes.c_longlong()
+        _check(self._lib, self._lib.amrgpu_values(self._h, None, 0, ctypes.byref(n)), "amrgpu_values")
+        a = np.zeros(n.value, dtype=np.float64)
+        _check(self._lib, self._lib.amrgpu_values(self._h, a.ctypes.data_as(_lib.c_double_p), n.value, ctypes.byref(n)),
+               "amrgpu_values")
+        return a
+
+    def gauges(self, nvar: int) -> np.ndarray:
+        n = ctypes.c_int()
+        _check(self._lib, self._lib.amrgpu_gauges(self._h, None, 0, ctypes.byref(n)), "amrgpu_gauges")
+        a = np.zeros((n.value, 3 + nvar), dtype=np.float64)
+        _check(self._lib, self._lib.amrgpu_gauges(self._h, a.ctypes.data_as(_lib.c_double_p), n.value, ctypes.byref(n)),
+               "amrgpu_gauges")
+        return a
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.amrgpu_destroy(self._h)
+            self._h = None
+        if self._tmp is not None:
+            self._tmp.cleanup()
+            self._tmp = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,1917 @@
+// Host orchestrator of the 2D B200 patch-advance path.
+//
+// The hierarchy lives on the device: every patch owns two solution buffers
+// (ping-pong store1/store2) in one device pool, and flux registers in a second
+// pool (the reference's alloc/node store, src/2d/amr_module.f90:30-236,
+// igetsp.f, reclam.f, nodget.f). The host keeps only metadata (boxes, level
+// lists, grid numbers) and compiles, once per regrid, the device programs that a
+// level substep runs:
+//   * ghost-fill programs (bound.f90 / filpatch.f90 / prefilp.f90 / intfil.f90 /
+//     bc2amr.f90) as staged lists of copy / interpolate / boundary ops,
+//   * saveqc programs (saveqc.f, icall.f, cstore.f),
+//   * the step work list with the flux-register epilogue entries (fluxsv.f, fluxad.f),
+//   * qad jobs (qad.f) and the level-sync plan (update.f, upbnd.f).
+// The scheduler (tick.f:4-391) and the regrid decisions stay on the host; the
+// flag stencil runs on the device and the clustering on the host
+// (regrid.f, grdfit2.f, flagger.f, bufnst2.f, colate2.f, smartbis.f, gfixup.f, filval.f90).
+#include "kernels2d.cuh"
+#include "params.hpp"
+#include "cluster2d.hpp"
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+namespace amrb {
+
+static const double RINF = (double)10.e32f;  // rinfinity of amr_module.f90 (a default-REAL literal)
+
+// ------------------------------------------------------------------ device pool
+struct Arena {
+  double* d = nullptr;
+  long long cap = 0;
+  std::map<long long, long long> fr;  // free blocks: offset -> length
+  long long inuse = 0, peak = 0;
+  static long long rnd(long long n) { return (n + 31) / 32 * 32; }
+  void init(long long n) {
+    n = rnd(std::max<long long>(n, 1 << 20));
+    AMR_CUDA(cudaMalloc(&d, sizeof(double) * n));
+    cap = n;
+    fr.clear();
+    fr[0] = n;
+  }
+  void grow(long long need) {
+    long long ncap = std::max(cap * 2, cap + rnd(need) + (1 << 20));
+    double* nd = nullptr;
+    AMR_CUDA(cudaMalloc(&nd, sizeof(double) * ncap));
+    AMR_CUDA(cudaMemcpy(nd, d, sizeof(double) * cap, cudaMemcpyDeviceToDevice));
+    AMR_CUDA(cudaFree(d));
+    d = nd;
+    release_raw(cap, ncap - cap);
+    cap = ncap;
+  }
+  void release_raw(long long off, long long n) {
+    auto it = fr.emplace(off, n).first;
+    if (it != fr.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) { pv->second += it->second; fr.erase(it); it = pv; }
+    }
+    auto nx = std::next(it);
+    if (nx != fr.end() && it->first + it->second == nx->first) { it->second += nx->second; fr.erase(nx); }
+  }
+  long long alloc(long long n) {
+    n = rnd(std::max<long long>(n, 1));
+    for (int pass = 0; pass < 2; ++pass) {
+      for (auto it = fr.begin(); it != fr.end(); ++it)
+        if (it->second >= n) {
+          const long long off = it->first, len = it->second;
+          fr.erase(it);
+          if (len > n) fr[off + n] = len - n;
+          inuse += n; peak = std::max(peak, inuse);
+          return off;
+        }
+      grow(n);
+    }
+    throw std::runtime_error("device pool exhausted");
+  }
+  void release(long long off, long long n) {
+    if (off < 0) return;
+    n = rnd(std::max<long long>(n, 1));
+    inuse -= n;
+    release_raw(off, n);
+  }
+  void destroy() { if (d) cudaFree(d); d = nullptr; }
+};
+
+template <class T> struct DBuf {
+  T* d = nullptr; size_t cap = 0, n = 0;
+  void upload(const std::vector<T>& h, cudaStream_t s) {
+    n = h.size();
+    if (n > cap) {
+      if (d) AMR_CUDA(cudaFree(d));
+      cap = std::max<size_t>(n, 16) * 3 / 2;
+      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
+    }
+    if (n) AMR_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(T) * n, cudaMemcpyHostToDevice, s));
+  }
+  void ensure(size_t m) {
+    if (m > cap) {
+      if (d) AMR_CUDA(cudaFree(d));
+      cap = std::max<size_t>(m, 16);
+      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
+    }
+    n = m;
+  }
+  void free() { if (d) cudaFree(d); d = nullptr; cap = n = 0; }
+};
+
+// ------------------------------------------------------------------ host patch metadata
+struct HPatch {
+  int ilo = 0, ihi = 0, jlo = 0, jhi = 0, level = 0, levelptr = 0, nextfree = 0;
+  double xlo = 0, xhi = 0, ylo = 0, yhi = 0, time = 0;
+  long long q0 = -1, q1 = -1, nq = 0;
+  long long ffl = -1, nffl = 0;
+  int lenbc = 0;
+  int cur = 0;
+  bool has_cfl = false;
+  std::vector<int> listbc;
+  std::vector<int> bnd;
+  int numflags = 0;
+  std::vector<int8_t> flags, dom2;
+  int nx() const { return ihi - ilo + 1; }
+  int ny() const { return jhi - jlo + 1; }
+};
+
+// ------------------------------------------------------------------ device programs
+struct FillProg {
+  std::vector<ScratchRect> rects;
+  std::vector<FillOp> ops;
+  std::vector<int> op_stage;
+  std::vector<BcOp> bcs;
+  std::vector<int> bc_stage;
+  int nstages = 0;
+  long long scratch_off = -1, scratch_len = 0;
+  DBuf<ScratchRect> d_rects;
+  DBuf<FillOp> d_ops;
+  DBuf<FillChunk> d_chunks;
+  DBuf<BcOp> d_bcs;
+  std::vector<int> ch_lo, ch_hi, bc_lo, bc_hi;
+  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; }
+  int add_rect(int ni, int nj, int nvar) {
+    ScratchRect r;
+    r.off = scratch_len; r.ni = ni; r.nj = nj;
+    scratch_len += Arena::rnd((long long)ni * nj * nvar);
+    rects.push_back(r);
+    return (int)rects.size() - 1;
+  }
+  void add_op(const FillOp& o, int st) { ops.push_back(o); op_stage.push_back(st); nstages = std::max(nstages, st + 1); }
+  void add_bc(const BcOp& b, int st) { bcs.push_back(b); bc_stage.push_back(st); nstages = std::max(nstages, st + 1); }
+};
+
+struct LevelPlan {
+  FillProg bound, saveqc;
+  std::vector<StepWork> work;
+  std::vector<FsvEntry> fsv;
+  std::vector<FadEntry> fad;
+  std::vector<int> patch_work_lo, patch_work_hi;  // per patch in level order: range in work
+  DBuf<StepWork> d_work;
+  DBuf<FsvEntry> d_fsv;
+  DBuf<FadEntry> d_fad;
+  std::vector<QadJob> qad;
+  DBuf<QadJob> d_qad;
+  std::vector<UpbndCell> upc;
+  std::vector<UpbndTerm> upt;
+  std::vector<AvgRect> avg;
+  DBuf<UpbndCell> d_upc;
+  DBuf<UpbndTerm> d_upt;
+  DBuf<AvgRect> d_avg;
+  std::vector<int> plist;
+  DBuf<int> d_plist;
+};
+
+struct GaugeRow { int gauge; int level; double t; int slot; };
+
+class Amr2Gpu {
+ public:
+  RunParams p;
+  ProbDev prob{};
+  StepParams sp{};
+  int nvar = 1, ng = 2;
+  bool xperdom = false, yperdom = false;
+  double xlower, ylower, xupper, yupper;
+  int nxc, nyc;
+  // hierarchy
+  std::vector<HPatch> node;
+  int ndfree = 0;
+  int lfine = 1;
+  int lstart[12] = {0}, newstl[12] = {0}, listsp[12] = {0}, icheck[12] = {0};
+  std::vector<int> lgrids[12];
+  double hxposs[12] = {0}, hyposs[12] = {0}, possk[12] = {0};
+  int iregsz[12] = {0}, jregsz[12] = {0};
+  int intratx[12] = {0}, intraty[12] = {0}, kratio[12] = {0};
+  // device
+  Arena pool, regs;
+  DBuf<PatchDev> d_patches;
+  std::vector<PatchDev> h_patches;
+  LevelPlan plan[12];
+  unsigned long long* d_cfl = nullptr;
+  double* d_mass = nullptr;
+  DBuf<double> d_gauge_out;
+  cudaStream_t st = nullptr;
+  LevelConst lc{};
+  // run state
+  double time = 0, start_time = 0;
+  int ncycle = 0;
+  double rvol = 0, rvoll[12] = {0};
+  double cfl_level = 0, cflmax_run = 0;
+  double tmass0 = 0;
+  bool batched = true;
+  bool record_gauges = true;
+  int max_cycles = 0;
+  std::vector<int> mbestsrc;
+  std::vector<double> glast;
+  std::vector<GaugeRow> grows;
+  std::vector<GaugeJob> gjobs_pending;
+  int gslots = 0;
+  double t_regrid = 0, t_step = 0;
+  long long nsteps_launched = 0, nkernels = 0;
+  int frame = 0;
+  std::string outdir;
+  bool write_output = false;
+  int status = 0;
+
+  ~Amr2Gpu() {
+    for (int l = 0; l < 12; ++l) free_plan(l);
+    pool.destroy(); regs.destroy();
+    d_patches.free(); d_gauge_out.free();
+    if (d_cfl) cudaFree(d_cfl);
+    if (d_mass) cudaFree(d_mass);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  // ================================================================ setup
+  void setup_problem() {
+    const std::string& pr = p.problem;
+    prob = ProbDev{};
+    prob.efix = 1;
+    if (pr == "advection_square") {
+      prob.solver = SOLVER_ADVECTION; prob.ubar = p.pn("u", 0.5); prob.vbar = p.pn("v", 1.0);
+    } else if (pr == "acoustics_cosine" || pr == "acoustics_gauss") {
+      prob.solver = SOLVER_ACOUSTICS; prob.rho = p.pn("rho", 1.0); prob.bulk = p.pn("bulk", 4.0);
+      prob.cc = std::sqrt(prob.bulk / prob.rho); prob.zz = prob.rho * prob.cc;
+    } else if (pr == "euler_quadrants") {
+      prob.solver = SOLVER_EULER; prob.gamma = p.pn("gamma", 1.4); prob.gamma1 = prob.gamma - 1.0;
+      prob.efix = (int)p.pn("efix", 1.0);
+    } else throw std::runtime_error("unknown problem '" + pr + "'");
+    const int me = prob.solver == SOLVER_ADVECTION ? 1 : prob.solver == SOLVER_ACOUSTICS ? 3 : 4;
+    const int mw = prob.solver == SOLVER_ADVECTION ? 1 : prob.solver == SOLVER_ACOUSTICS ? 2 : 4;
+    if (p.nvar != me || p.mwaves != mw) throw std::runtime_error("num_eqn/num_waves do not match the Riemann solver");
+    sp.prob = prob;
+    for (int k = 0; k < MAXVAR; ++k) sp.mthlim[k] = k < (int)p.mthlim.size() ? p.mthlim[k] : 0;
+    sp.order = p.order; sp.trans = p.trans; sp.use_fwaves = p.use_fwaves ? 1 : 0; sp.mcapa = p.mcapa;
+  }
+
+  // qinit of the supported problems (per-application qinit.f of the reference)
+  void qinit(int mx, int my, double xl, double yl, double dx, double dy, std::vector<double>& q) {
+    const int mitot = mx + 2 * ng, mjtot = my + 2 * ng;
+    q.assign((size_t)nvar * mitot * mjtot, 0.0);
+    auto Q = [&](int m, int i, int j) -> double& { return q[(size_t)m * mitot * mjtot + (size_t)(j + ng - 1) * mitot + (i + ng - 1)]; };
+    const std::string& pr = p.problem;
+    if (pr == "advection_square") {
+      const double x0 = p.pn("x0", 0.1), x1 = p.pn("x1", 0.6), y0 = p.pn("y0", 0.1), y1 = p.pn("y1", 0.6);
+      for (int j = 1; j <= my; ++j) {
+        const double yj = yl + (j - 0.5) * dy;
+        for (int i = 1; i <= mx; ++i) {
+          const double xi = xl + (i - 0.5) * dx;
+          Q(0, i, j) = (xi > x0 && xi < x1 && yj > y0 && yj < y1) ? 1.0 : 0.1;
+        }
+      }
+    } else if (pr == "acoustics_cosine" || pr == "acoustics_gauss") {
+      const bool cosine = pr == "acoustics_cosine";
+      const double r0 = p.pn("r0", cosine ? 0.5 : 0.3), w = p.pn("width", cosine ? 0.2 : 0.05);
+      const double pi = 4.0 * std::atan(1.0);
+      for (int i = 1; i <= mx; ++i) {
+        const double xc = xl + (i - 0.5) * dx;
+        for (int j = 1; j <= my; ++j) {
+          const double yc = yl + (j - 0.5) * dy;
+          const double r = std::sqrt(xc * xc + yc * yc);
+          double pv;
+          if (cosine) pv = (std::fabs(r - r0) <= w) ? 1.0 + std::cos(pi * (r - r0) / w) : 0.0;
+          else { const double z = (r - r0) / w; pv = std::exp(-(z * z)); }
+          Q(0, i, j) = pv; Q(1, i, j) = 0.0; Q(2, i, j) = 0.0;
+        }
+      }
+    } else if (pr == "euler_quadrants") {
+      const double rpp[5] = {0, 1.5, 0.3, 0.029032258064516, 0.3};
+      const double rpr[5] = {0, 1.5, 0.532258064516129, 0.137992831541219, 0.532258064516129};
+      const double rpu[5] = {0, 0.0, 1.206045378311055, 1.206045378311055, 0.0};
+      const double rpv[5] = {0, 0.0, 0.0, 1.206045378311055, 1.206045378311055};
+      const double g1 = prob.gamma - 1.0, xs = p.pn("xs", 0.8), ys = p.pn("ys", 0.8);
+      for (int i = 1; i <= mx; ++i) {
+        const double xc = xl + (i - 0.5) * dx;
+        for (int j = 1; j <= my; ++j) {
+          const double yc = yl + (j - 0.5) * dy;
+          int iq = 1;
+          if (xc >= xs && yc >= ys) iq = 1;
+          if (xc < xs && yc >= ys) iq = 2;
+          if (xc < xs && yc < ys) iq = 3;
+          if (xc >= xs && yc < ys) iq = 4;
+          Q(0, i, j) = rpr[iq]; Q(1, i, j) = rpr[iq] * rpu[iq]; Q(2, i, j) = rpr[iq] * rpv[iq];
+          Q(3, i, j) = rpp[iq] / g1 + 0.5 * rpr[iq] * (rpu[iq] * rpu[iq] + rpv[iq] * rpv[iq]);
+        }
+      }
+    }
+  }
+
+  // ================================================================ node numbers (nodget.f / putnod.f)
+  int nodget() {
+    if (ndfree == 0) {
+      const int old = (int)node.size() - 1, add = 10000;
+      node.resize(old + 1 + add);
+      for (int k = old + 1; k <= old + add; ++k) node[k].nextfree = k + 1;
+      node[old + add].nextfree = 0;
+      ndfree = old + 1;
+    }
+    const int m = ndfree;
+    ndfree = node[m].nextfree;
+    node[m] = HPatch();
+    return m;
+  }
+  void putnod(int m) { node[m].nextfree = ndfree; ndfree = m; }
+
+  int mitot(int m) const { return node[m].nx() + 2 * ng; }
+  int mjtot(int m) const { return node[m].ny() + 2 * ng; }
+
+  void alloc_patch(int m) {
+    HPatch& g = node[m];
+    g.nq = (long long)nvar * mitot(m) * mjtot(m);
+    g.q0 = pool.alloc(g.nq);
+    g.q1 = pool.alloc(g.nq);
+    g.cur = 0;
+  }
+  void free_patch(int m) {
+    HPatch& g = node[m];
+    pool.release(g.q0, g.nq); pool.release(g.q1, g.nq);
+    g.q0 = g.q1 = -1;
+    if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
+    g.ffl = -1;
+  }
+  long long qcur(int m) const { return node[m].cur ? node[m].q1 : node[m].q0; }
+
+  void sync_descriptors() {
+    h_patches.assign(node.size(), PatchDev{});
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) {
+        const HPatch& g = node[m];
+        PatchDev& d = h_patches[m];
+        d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl;
+        d.ilo = g.ilo; d.ihi = g.ihi; d.jlo = g.jlo; d.jhi = g.jhi; d.klo = d.khi = 0;
+        d.mitot = mitot(m); d.mjtot = mjtot(m); d.mktot = 1;
+        d.level = g.level; d.lenbc = g.lenbc;
+      }
+    d_patches.upload(h_patches, st);
+  }
+
+  // ================================================================ level lists
+  void make_lists() {
+    for (int lev = 1; lev <= 11; ++lev) {
+      lgrids[lev].clear();
+      if (lev > p.mxnest) continue;
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) lgrids[lev].push_back(m);
+    }
+  }
+  // init_bndryList.f:50-107: same-level neighbours touching the ghost region, most recent first
+  void make_bndry(int lev) {
+    const auto& G = lgrids[lev];
+    for (size_t n = 0; n < G.size(); ++n) {
+      HPatch& g = node[G[n]];
+      g.bnd.clear();
+      for (size_t k = G.size(); k-- > 0;) {
+        if (k == n) continue;
+        const HPatch& s = node[G[k]];
+        if (std::max(s.ilo, g.ilo - ng) <= std::min(s.ihi, g.ihi + ng) && std::max(s.jlo, g.jlo - ng) <= std::min(s.jhi, g.jhi + ng))
+          g.bnd.push_back(G[k]);
+      }
+    }
+  }
+  // regrid.f:132-169: order grids by cost, most expensive first, with quick_sort1.f tie breaking
+  void arrange(int lev) {
+    std::vector<int> gl;
+    for (int m = lstart[lev]; m != 0; m = node[m].levelptr) gl.push_back(m);
+    const int n = (int)gl.size();
+    if (n <= 1) return;
+    std::vector<long long> cost(n + 1);
+    std::vector<int> ord(n + 1);
+    for (int i = 1; i <= n; ++i) cost[i] = (long long)(node[gl[i - 1]].ihi - node[gl[i - 1]].ilo + 3) * (node[gl[i - 1]].jhi - node[gl[i - 1]].jlo + 2);
+    qsort_index(ord, n, cost);
+    lstart[lev] = gl[ord[n] - 1];
+    int prev = lstart[lev];
+    for (int i = 1; i <= n - 1; ++i) { node[prev].levelptr = gl[ord[n - i] - 1]; prev = node[prev].levelptr; }
+    node[prev].levelptr = 0;
+  }
+  // birect.f:10-120: split patches wider than max1d
+  void birect(int m1) {
+    int m = m1;
+    const int lev = node[m].level;
+    const double hx = hxposs[lev], hy = hyposs[lev];
+    while (true) {
+      const int nx = node[m].nx(), ny = node[m].ny();
+      if (nx + 2 * ng > p.max1d) {
+        int nxl = nx / 2;
+        const int r = lev > 1 ? intratx[lev - 1] : 2;
+        nxl = (nxl / r) * r;
+        const double cxmid = node[m].xlo + nxl * hx;
+        const int mn = nodget();
+        HPatch& a = node[m]; HPatch& b = node[mn];
+        b.levelptr = a.levelptr; a.levelptr = mn;
+        b.ihi = a.ihi; a.ihi = a.ilo + nxl - 1; b.ilo = a.ihi + 1; b.jhi = a.jhi; b.jlo = a.jlo;
+        b.xlo = cxmid; b.ylo = a.ylo; b.yhi = a.yhi; b.xhi = a.xhi; a.xhi = cxmid;
+        b.time = a.time; b.level = a.level;
+      } else if (ny + 2 * ng > p.max1d) {
+        int nyl = ny / 2;
+        const int r = lev > 1 ? intraty[lev - 1] : 2;
+        nyl = (nyl / r) * r;
+        const double cymid = node[m].ylo + nyl * hy;
+        const int mn = nodget();
+        HPatch& a = node[m]; HPatch& b = node[mn];
+        b.levelptr = a.levelptr; a.levelptr = mn;
+        b.jhi = a.jhi; a.jhi = a.jlo + nyl - 1; b.jlo = a.jhi + 1; b.ihi = a.ihi; b.ilo = a.ilo;
+        b.xlo = a.xlo; b.ylo = cymid; b.yhi = a.yhi; b.xhi = a.xhi; a.yhi = cymid;
+        b.level = a.level; b.time = a.time;
+      } else {
+        m = node[m].levelptr;
+        if (m == 0) break;
+      }
+    }
+  }
+
+  // ================================================================ fill-program compiler
+  struct Tgt { int patch, rect, ni, nj; };
+
+  BcOp make_bc(Tgt t, double hx, double hy, double xlo_p, double xhi_p, double ylo_p, double yhi_p, bool& any) {
+    BcOp b{};
+    b.dst_patch = t.patch; b.dst_rect = t.rect; b.nrow = t.ni; b.ncol = t.nj;
+    any = false;
+    if (xperdom && yperdom) return b;
+    const double hxm = hx * 0.01, hym = hy * 0.01;
+    auto chk = [&](int code) { if (code == 0) throw std::runtime_error("user boundary conditions are not provided"); };
+    if (xlo_p < xlower - hxm) { b.nxl = (int)((xlower + hxm - xlo_p) / hx); b.bxl = p.mthbc[1]; chk(b.bxl); any = true; }
+    if (xhi_p > xupper + hxm) { const int nxr = (int)((xhi_p - xupper + hxm) / hx); b.ibeg = std::max(t.ni - nxr + 1, 1); b.bxr = p.mthbc[2]; chk(b.bxr); any = true; }
+    if (ylo_p < ylower - hym) { b.nyb = (int)((ylower + hym - ylo_p) / hy); b.byl = p.mthbc[3]; chk(b.byl); any = true; }
+    if (yhi_p > yupper + hym) { const int nyt = (int)((yhi_p - yupper + hym) / hy); b.jbeg = std::max(t.nj - nyt + 1, 1); b.byr = p.mthbc[4]; chk(b.byr); any = true; }
+    return b;
+  }
+
+  // Runs of cells with mask==0 over an (ni x nj) region, merged into rectangles.
+  static void runs(const std::vector<int8_t>& mask, int ni, int nj, std::vector<int>& out /* i0, j0, w, h */) {
+    out.clear();
+    std::vector<int> prev;  // runs of the previous row as (i0, w, rect index)
+    for (int j = 0; j < nj; ++j) {
+      std::vector<int> cur;
+      int i = 0;
+      while (i < ni) {
+        if (mask[(size_t)j * ni + i] != 0) { ++i; continue; }
+        int k = i;
+        while (k < ni && mask[(size_t)j * ni + k] == 0) ++k;
+        int ridx = -1;
+        for (size_t q = 0; q < prev.size(); q += 3)
+          if (prev[q] == i && prev[q + 1] == k - i) { ridx = prev[q + 2]; break; }
+        if (ridx >= 0) out[4 * ridx + 3] += 1;
+        else { ridx = (int)out.size() / 4; out.push_back(i); out.push_back(j); out.push_back(k - i); out.push_back(1); }
+        cur.push_back(i); cur.push_back(k - i); cur.push_back(ridx);
+        i = k;
+      }
+      prev.swap(cur);
+    }
+  }
+
+  void add_split_ops(FillProg& P, FillOp o, int st) {
+    // split tall copies so no op is huge (keeps chunks balanced)
+    P.add_op(o, st);
+  }
+
+  // filpatch.f90:71-355 as a program; returns the stage at which the region is complete
+  int c_filrecur(FillProg& P, int level, Tgt T, int nrowst, int ncolst, int ilo, int ihi, int jlo, int jhi, bool patchOnly, int msrc) {
+    const int ni = ihi - ilo + 1, nj = jhi - jlo + 1;
+    std::vector<int8_t> used((size_t)ni * nj, 0);
+    std::vector<FillOp> copies;
+    // intfil.f90:153-260
+    const std::vector<int>& src = (msrc == -1) ? lgrids[level] : node[msrc].bnd;
+    for (int m : src) {
+      const HPatch& g = node[m];
+      const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi), jxlo = std::max(g.jlo, jlo), jxhi = std::min(g.jhi, jhi);
+      if (!(ixlo <= ixhi && jxlo <= jxhi)) continue;
+      FillOp o{};
+      o.kind = FILL_COPY; o.dst_patch = T.patch; o.dst_rect = T.rect;
+      o.di0 = nrowst - 1 + (ixlo - ilo); o.dj0 = ncolst - 1 + (jxlo - jlo);
+      o.ni = ixhi - ixlo + 1; o.nj = jxhi - jxlo + 1;
+      o.src = m; o.si0 = ixlo - g.ilo + ng; o.sj0 = jxlo - g.jlo + ng; o.level = level;
+      copies.push_back(o);
+      for (int j = jxlo; j <= jxhi; ++j) for (int i = ixlo; i <= ixhi; ++i) used[(size_t)(j - jlo) * ni + (i - ilo)] = 1;
+    }
+    auto mark = [&](int i0, int i1, int j0, int j1) {
+      for (int j = std::max(j0, jlo); j <= std::min(j1, jhi); ++j)
+        for (int i = std::max(i0, ilo); i <= std::min(i1, ihi); ++i) used[(size_t)(j - jlo) * ni + (i - ilo)] = 1;
+    };
+    if (jhi >= jregsz[level]) mark(ilo, ihi, std::max(jregsz[level], jlo), jhi);
+    if (jlo < 0) mark(ilo, ihi, jlo, std::min(-1, ncolst + jhi - jlo));
+    if (ilo < 0) mark(ilo, std::min(-1, nrowst + ihi - ilo), jlo, jhi);
+    if (ihi >= iregsz[level]) mark(std::max(iregsz[level], ilo), ihi, jlo, jhi);
+    // trimbd.f90: bounding box of unset cells
+    int ui0 = ni, ui1 = -1, uj0 = nj, uj1 = -1;
+    for (int j = 0; j < nj; ++j) for (int i = 0; i < ni; ++i)
+      if (!used[(size_t)j * ni + i]) { ui0 = std::min(ui0, i); ui1 = std::max(ui1, i); uj0 = std::min(uj0, j); uj1 = std::max(uj1, j); }
+    int stage = 0;
+    if (ui1 >= 0) {
+      if (level == 1) throw std::runtime_error("ghost fill: level 1 cells not covered");
+      const int rx = intratx[level - 1], ry = intraty[level - 1];
+      const int u0 = ui0 + ilo, u1 = ui1 + ilo, v0 = uj0 + jlo, v1 = uj1 + jlo;
+      const int iplo = (u0 - rx + ng * rx) / rx - ng, iphi = (u1 + rx) / rx;
+      const int jplo = (v0 - ry + ng * ry) / ry - ng, jphi = (v1 + ry) / ry;
+      const int mic = iphi - iplo + 1, mjc = jphi - jplo + 1;
+      const int R = P.add_rect(mic, mjc, nvar);
+      Tgt C{-1, R, mic, mjc};
+      const bool sticks = (iplo < 0 || jplo < 0 || iphi >= iregsz[level - 1] || jphi >= jregsz[level - 1]);
+      int cst;
+      if ((xperdom || yperdom) && sticks) cst = c_prefil(P, level - 1, C, iplo, iphi, jplo, jphi, iplo, jplo);
+      else cst = c_filrecur(P, level - 1, C, 1, 1, iplo, iphi, jplo, jphi, true, -1);
+      stage = cst + 1;
+      std::vector<int> rr;
+      runs(used, ni, nj, rr);
+      for (size_t k = 0; k < rr.size(); k += 4) {
+        FillOp o{};
+        o.kind = FILL_INTERP; o.dst_patch = T.patch; o.dst_rect = T.rect;
+        o.di0 = nrowst - 1 + rr[k]; o.dj0 = ncolst - 1 + rr[k + 1]; o.ni = rr[k + 2]; o.nj = rr[k + 3];
+        o.src = R; o.si0 = ilo + rr[k]; o.sj0 = jlo + rr[k + 1]; o.level = level; o.cilo = iplo; o.cjlo = jplo;
+        P.add_op(o, stage);
+      }
+    }
+    for (auto& o : copies) P.add_op(o, stage);
+    if (patchOnly) {
+      bool any;
+      const double dx = hxposs[level], dy = hyposs[level];
+      BcOp b = make_bc(T, dx, dy, xlower + ilo * dx, xlower + (ihi + 1) * dx, ylower + jlo * dy, ylower + (jhi + 1) * dy, any);
+      if (any) P.add_bc(b, stage);
+    }
+    return stage;
+  }
+
+  // prefilp.f90:18-214: periodic pieces filled at wrapped indices, then copied into place
+  int c_prefil(FillProg& P, int level, Tgt T, int ilo, int ihi, int jlo, int jhi, int iglo, int jglo) {
+    int ist[3], iend[3], jst[3], jend[3], ish[3], jsh[3];
+    if (xperdom) { ist[0] = ilo; ist[1] = 0; ist[2] = iregsz[level]; iend[0] = -1; iend[1] = iregsz[level] - 1; iend[2] = ihi; ish[0] = iregsz[level]; ish[1] = 0; ish[2] = -iregsz[level]; }
+    else { ist[0] = iregsz[level]; ist[1] = ilo; ist[2] = iregsz[level]; iend[0] = -1; iend[1] = ihi; iend[2] = -1; ish[0] = ish[1] = ish[2] = 0; }
+    if (yperdom) { jst[0] = jlo; jst[1] = 0; jst[2] = jregsz[level]; jend[0] = -1; jend[1] = jregsz[level] - 1; jend[2] = jhi; jsh[0] = jregsz[level]; jsh[1] = 0; jsh[2] = -jregsz[level]; }
+    else { jst[0] = jregsz[level]; jst[1] = jlo; jst[2] = jregsz[level]; jend[0] = -1; jend[1] = jhi; jend[2] = -1; jsh[0] = jsh[1] = jsh[2] = 0; }
+    int done = 0;
+    for (int a = 0; a < 3; ++a) {
+      const int i1 = std::max(ilo, ist[a]), i2 = std::min(ihi, iend[a]);
+      if (i1 > i2) continue;
+      for (int b = 0; b < 3; ++b) {
+        const int j1 = std::max(jlo, jst[b]), j2 = std::min(jhi, jend[b]);
+        if (j1 > j2) continue;
+        const int mi = i2 - i1 + 1, mj = j2 - j1 + 1;
+        const int R = P.add_rect(mi, mj, nvar);
+        const int s = c_filrecur(P, level, Tgt{-1, R, mi, mj}, 1, 1, i1 + ish[a], i2 + ish[a], j1 + jsh[b], j2 + jsh[b], true, -1);
+        FillOp o{};
+        o.kind = FILL_PIECE; o.dst_patch = T.patch; o.dst_rect = T.rect;
+        o.di0 = i1 - iglo; o.dj0 = j1 - jglo; o.ni = mi; o.nj = mj; o.src = R; o.si0 = 0; o.sj0 = 0;
+        P.add_op(o, s + 1);
+        done = std::max(done, s + 1);
+      }
+    }
+    return done;
+  }
+
+  void compile_bound(int lev) {
+    FillProg& P = plan[lev].bound;
+    P.clear();
+    P.scratch_len = 0;
+    for (int m : lgrids[lev]) {
+      const HPatch& g = node[m];
+      const double hx = hxposs[lev], hy = hyposs[lev];
+      Tgt T{m, -1, mitot(m), mjtot(m)};
+      const int mi = T.ni, mj = T.nj;
+      int s = 0;
+      double xl = g.xlo - ng * hx, xr, yb;
+      if (xl < xlower && xperdom) s = std::max(s, c_prefil(P, lev, T, g.ilo - ng, g.ilo - 1, g.jlo, g.jhi, g.ilo - ng, g.jlo - ng));
+      else s = std::max(s, c_filrecur(P, lev, T, 1, ng + 1, g.ilo - ng, g.ilo - 1, g.jlo, g.jhi, false, m));
+      xr = g.xhi + ng * hx;
+      if (xr > xupper && xperdom) s = std::max(s, c_prefil(P, lev, T, g.ihi + 1, g.ihi + ng, g.jlo, g.jhi, g.ilo - ng, g.jlo - ng));
+      else s = std::max(s, c_filrecur(P, lev, T, mi - ng + 1, ng + 1, g.ihi + 1, g.ihi + ng, g.jlo, g.jhi, false, m));
+      xl = g.xlo - ng * hx; xr = g.xhi + ng * hx; yb = g.ylo - ng * hy;
+      if ((yb < ylower && yperdom) || ((xl < xlower || xr > xupper) && xperdom))
+        s = std::max(s, c_prefil(P, lev, T, g.ilo - ng, g.ihi + ng, g.jlo - ng, g.jlo - 1, g.ilo - ng, g.jlo - ng));
+      else s = std::max(s, c_filrecur(P, lev, T, 1, 1, g.ilo - ng, g.ihi + ng, g.jlo - ng, g.jlo - 1, false, m));
+      const double yt = g.yhi + ng * hy;
+      if ((yt > yupper && yperdom) || ((xl < xlower || xr > xupper) && xperdom))
+        s = std::max(s, c_prefil(P, lev, T, g.ilo - ng, g.ihi + ng, g.jhi + 1, g.jhi + ng, g.ilo - ng, g.jlo - ng));
+      else s = std::max(s, c_filrecur(P, lev, T, 1, mj - ng + 1, g.ilo - ng, g.ihi + ng, g.jhi + 1, g.jhi + ng, false, m));
+      bool any;
+      BcOp b = make_bc(T, hx, hy, g.xlo - ng * hx, g.xhi + ng * hx, g.ylo - ng * hy, g.yhi + ng * hy, any);
+      if (any) P.add_bc(b, s);
+    }
+    upload_prog(P);
+  }
+
+  // icall.f / preicall.f: copies of store1 of every grid at `level` into a rect
+  void c_icall(FillProg& P, Tgt T, int ilo, int ihi, int jlo, int jhi, int level, int iput, int jput, int st_) {
+    for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+      const HPatch& g = node[m];
+      const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi), jxlo = std::max(g.jlo, jlo), jxhi = std::min(g.jhi, jhi);
+      if (!(ixlo <= ixhi && jxlo <= jxhi)) continue;
+      FillOp o{};
+      o.kind = FILL_COPY; o.dst_patch = T.patch; o.dst_rect = T.rect;
+      o.di0 = ixlo - ilo + iput - 1; o.dj0 = jxlo - jlo + jput - 1; o.ni = ixhi - ixlo + 1; o.nj = jxhi - jxlo + 1;
+      o.src = m; o.si0 = ixlo - g.ilo + ng; o.sj0 = jxlo - g.jlo + ng; o.level = -1;
+      P.add_op(o, st_);
+    }
+  }
+  void c_preicall(FillProg& P, Tgt T, int ilo, int ihi, int jlo, int jhi, int level, int st_) {
+    int ist[3], iend[3], jst[3], jend[3], ish[3], jsh[3];
+    if (xperdom) { ist[0] = ilo; ist[1] = 0; ist[2] = iregsz[level]; iend[0] = -1; iend[1] = iregsz[level] - 1; iend[2] = ihi; ish[0] = iregsz[level]; ish[1] = 0; ish[2] = -iregsz[level]; }
+    else { ist[0] = iregsz[level]; ist[1] = ilo; ist[2] = iregsz[level]; iend[0] = -1; iend[1] = ihi; iend[2] = -1; ish[0] = ish[1] = ish[2] = 0; }
+    if (yperdom) { jst[0] = jlo; jst[1] = 0; jst[2] = jregsz[level]; jend[0] = -1; jend[1] = jregsz[level] - 1; jend[2] = jhi; jsh[0] = jregsz[level]; jsh[1] = 0; jsh[2] = -jregsz[level]; }
+    else { jst[0] = jregsz[level]; jst[1] = jlo; jst[2] = jregsz[level]; jend[0] = -1; jend[1] = jhi; jend[2] = -1; jsh[0] = jsh[1] = jsh[2] = 0; }
+    for (int a = 0; a < 3; ++a) {
+      const int i1 = std::max(ilo, ist[a]), i2 = std::min(ihi, iend[a]);
+      if (i1 > i2) continue;
+      for (int b = 0; b < 3; ++b) {
+        const int j1 = std::max(jlo, jst[b]), j2 = std::min(jhi, jend[b]);
+        if (j1 > j2) continue;
+        c_icall(P, T, i1 + ish[a], i2 + ish[a], j1 + jsh[b], j2 + jsh[b], level, i1 - ilo + 1, j1 - jlo + 1, st_);
+      }
+    }
+  }
+
+  // saveqc.f:13-109 for the kids at level lev+1
+  void compile_saveqc(int lev) {
+    FillProg& P = plan[lev].saveqc;
+    P.clear();
+    P.scratch_len = 0;
+    if (lev + 1 > p.mxnest || lstart[lev + 1] == 0) { upload_prog(P); return; }
+    const double hxc = hxposs[lev], hyc = hyposs[lev];
+    for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
+      const HPatch& g = node[k];
+      const int rx = intratx[lev], ry = intraty[lev];
+      const int iclo = g.ilo / rx - 1, jclo = g.jlo / ry - 1, ichi = (g.ihi + 1) / rx, jchi = (g.jhi + 1) / ry;
+      const int nrow = ichi - iclo + 1, ncol = jchi - jclo + 1;
+      const int R = P.add_rect(nrow, ncol, nvar);
+      Tgt T{-1, R, nrow, ncol};
+      const bool sticks = (iclo < 0 || ichi == iregsz[lev] || jclo < 0 || jchi == jregsz[lev]);
+      if (sticks && (xperdom || yperdom)) c_preicall(P, T, iclo, ichi, jclo, jchi, lev, 0);
+      else c_icall(P, T, iclo, ichi, jclo, jchi, lev, 1, 1, 0);
+      bool any;
+      BcOp b = make_bc(T, hxc, hyc, g.xlo - hxc, g.xhi + hxc, g.ylo - hyc, g.yhi + hyc, any);
+      if (any) P.add_bc(b, 0);
+      FillOp o{};
+      o.kind = FILL_RING; o.dst_patch = k; o.dst_rect = -1; o.ni = g.lenbc; o.nj = 1; o.src = R;
+      P.add_op(o, 1);
+    }
+    upload_prog(P);
+  }
+
+  void upload_prog(FillProg& P) {
+    if (P.scratch_off >= 0) pool.release(P.scratch_off, std::max<long long>(P.scratch_len, 1));
+    P.scratch_off = -1;
+    // the scratch length of the previous compile may differ; (re)allocate
+    P.scratch_off = pool.alloc(std::max<long long>(P.scratch_len, 1));
+    std::vector<ScratchRect> rects = P.rects;
+    for (auto& r : rects) r.off += P.scratch_off;
+    P.d_rects.upload(rects, st);
+    // order ops and bcs by stage; chunks of <= 128 cells
+    std::vector<int> oidx(P.ops.size());
+    for (size_t i = 0; i < oidx.size(); ++i) oidx[i] = (int)i;
+    std::stable_sort(oidx.begin(), oidx.end(), [&](int a, int b) { return P.op_stage[a] < P.op_stage[b]; });
+    std::vector<FillOp> ops;
+    std::vector<FillChunk> ch;
+    P.ch_lo.assign(P.nstages, 0); P.ch_hi.assign(P.nstages, 0);
+    int s = -1;
+    for (int k : oidx) {
+      const int stg = P.op_stage[k];
+      while (s < stg) { ++s; P.ch_lo[s] = (int)ch.size(); P.ch_hi[s] = (int)ch.size(); }
+      const int id = (int)ops.size();
+      ops.push_back(P.ops[k]);
+      const int cells = P.ops[k].ni * P.ops[k].nj;
+      for (int c0 = 0; c0 < cells; c0 += 128) ch.push_back(FillChunk{id, c0, std::min(128, cells - c0)});
+      P.ch_hi[s] = (int)ch.size();
+    }
+    while (s + 1 < P.nstages) { ++s; P.ch_lo[s] = P.ch_hi[s] = (int)ch.size(); }
+    std::vector<int> bidx(P.bcs.size());
+    for (size_t i = 0; i < bidx.size(); ++i) bidx[i] = (int)i;
+    std::stable_sort(bidx.begin(), bidx.end(), [&](int a, int b) { return P.bc_stage[a] < P.bc_stage[b]; });
+    std::vector<BcOp> bcs;
+    P.bc_lo.assign(P.nstages, 0); P.bc_hi.assign(P.nstages, 0);
+    s = -1;
+    for (int k : bidx) {
+      const int stg = P.bc_stage[k];
+      while (s < stg) { ++s; P.bc_lo[s] = (int)bcs.size(); P.bc_hi[s] = (int)bcs.size(); }
+      bcs.push_back(P.bcs[k]);
+      P.bc_hi[s] = (int)bcs.size();
+    }
+    while (s + 1 < P.nstages) { ++s; P.bc_lo[s] = P.bc_hi[s] = (int)bcs.size(); }
+    P.d_ops.upload(ops, st);
+    P.d_chunks.upload(ch, st);
+    P.d_bcs.upload(bcs, st);
+  }
+
+  void run_prog(FillProg& P, const SrcMode& modes) {
+    for (int s = 0; s < P.nstages; ++s) {
+      if (P.ch_hi[s] > P.ch_lo[s]) {
+        FillArgs a{};
+        a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
+        a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
+        a.lc = lc; a.xlower = xlower; a.ylower = ylower;
+        launch_fill(a, st);
+        ++nkernels;
+      }
+      if (P.bc_hi[s] > P.bc_lo[s]) {
+        BcArgs b{};
+        b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.bc_lo[s];
+        b.nops = P.bc_hi[s] - P.bc_lo[s]; b.nvar = nvar;
+        launch_bc(b, 0, st);
+        launch_bc(b, 1, st);
+        nkernels += 2;
+      }
+    }
+  }
+
+  // ================================================================ step work, registers, update plans
+  void compile_step(int lev) {
+    LevelPlan& L = plan[lev];
+    L.work.clear(); L.fsv.clear(); L.fad.clear(); L.patch_work_lo.clear(); L.patch_work_hi.clear(); L.qad.clear();
+    L.plist = lgrids[lev];
+    for (int m : lgrids[lev]) {
+      const HPatch& g = node[m];
+      const int mx = g.nx(), my = g.ny();
+      const int ntx = (mx + TILE2 - 1) / TILE2, nty = (my + TILE2 - 1) / TILE2;
+      std::vector<std::vector<FsvEntry>> tf(ntx * nty);
+      std::vector<std::vector<FadEntry>> ta(ntx * nty);
+      if (g.has_cfl) {
+        for (int sp_ = 1; sp_ <= listsp[lev]; ++sp_) {
+          const int* e = &g.listbc[5 * (sp_ - 1)];
+          if (e[0] == 0) break;
+          FsvEntry f{};
+          f.ic = e[0] - ng; f.jc = e[1] - ng; f.side = e[2];
+          f.dst = node[e[3]].ffl + (long long)nvar * (e[4] - 1);
+          tf[((f.jc - 1) / TILE2) * ntx + (f.ic - 1) / TILE2].push_back(f);
+        }
+      }
+      if (lev > 1 && g.ffl >= 0) {
+        const int rx = intratx[lev - 1], ry = intraty[lev - 1];
+        if (TILE2 % rx != 0 || TILE2 % ry != 0) throw std::runtime_error("refinement ratio must divide the tile size");
+        const int nyc_ = my / ry, nxc_ = mx / rx;
+        int seg = 0;
+        for (int j = 0; j < nyc_; ++j, ++seg) { FadEntry a{1, j * ry + 1, seg, ry}; ta[(j * ry / TILE2) * ntx + 0].push_back(a); }
+        for (int i = 0; i < nxc_; ++i, ++seg) { FadEntry a{2, i * rx + 1, seg, rx}; ta[(nty - 1) * ntx + i * rx / TILE2].push_back(a); }
+        for (int j = 0; j < nyc_; ++j, ++seg) { FadEntry a{3, j * ry + 1, seg, ry}; ta[(j * ry / TILE2) * ntx + ntx - 1].push_back(a); }
+        for (int i = 0; i < nxc_; ++i, ++seg) { FadEntry a{4, i * rx + 1, seg, rx}; ta[0 * ntx + i * rx / TILE2].push_back(a); }
+        L.qad.push_back(QadJob{m, 1, 0, nyc_, 0});
+        L.qad.push_back(QadJob{m, 2, nyc_, nxc_, 0});
+        L.qad.push_back(QadJob{m, 3, nyc_ + nxc_, nyc_, 0});
+        L.qad.push_back(QadJob{m, 4, 2 * nyc_ + nxc_, nxc_, 0});
+      }
+      L.patch_work_lo.push_back((int)L.work.size());
+      for (int ty = 0; ty < nty; ++ty)
+        for (int tx = 0; tx < ntx; ++tx) {
+          StepWork w{};
+          w.patch = m; w.ti0 = tx * TILE2 + 1; w.tj0 = ty * TILE2 + 1;
+          auto& F = tf[ty * ntx + tx];
+          auto& A = ta[ty * ntx + tx];
+          w.fsv_start = (int)L.fsv.size(); w.fsv_count = (int)F.size();
+          L.fsv.insert(L.fsv.end(), F.begin(), F.end());
+          w.fad_start = (int)L.fad.size(); w.fad_count = (int)A.size();
+          L.fad.insert(L.fad.end(), A.begin(), A.end());
+          L.work.push_back(w);
+        }
+      L.patch_work_hi.push_back((int)L.work.size());
+    }
+    L.d_work.upload(L.work, st);
+    L.d_fsv.upload(L.fsv, st);
+    L.d_fad.upload(L.fad, st);
+    L.d_qad.upload(L.qad, st);
+    L.d_plist.upload(L.plist, st);
+  }
+
+  // update.f:16-189 + upbnd.f:18-127 for coarse level lev
+  void compile_update(int lev) {
+    LevelPlan& L = plan[lev];
+    L.upc.clear(); L.upt.clear(); L.avg.clear();
+    if (lev >= p.mxnest) { L.d_upc.upload(L.upc, st); L.d_upt.upload(L.upt, st); L.d_avg.upload(L.avg, st); return; }
+    for (int m : lgrids[lev]) {
+      const HPatch& g = node[m];
+      if (g.has_cfl) {
+        std::map<std::pair<int, int>, std::vector<UpbndTerm>> cells;
+        std::vector<std::pair<int, int>> order;
+        std::map<std::pair<int, int>, int> iused;
+        for (int s = 1; s <= listsp[lev]; ++s) {
+          const int* e = &g.listbc[5 * (s - 1)];
+          if (e[0] == 0) break;
+          const int side = e[2];
+          const int side1 = side < 5 ? side : (side == 5 ? 2 : 4);
+          const int norm = 1 << (side1 - 1);
+          auto key = std::make_pair(e[0], e[1]);
+          int& used = iused[key];
+          if ((used / norm) % 2 == 1) continue;
+          const double sgn = (side == 2 || side == 3 || side == 6) ? -1.0 : 1.0;
+          if (!cells.count(key)) order.push_back(key);
+          cells[key].push_back(UpbndTerm{node[e[3]].ffl + (long long)nvar * (e[4] - 1), sgn});
+          used += norm;
+        }
+        for (auto& k : order) {
+          UpbndCell c{};
+          c.patch = m; c.ie = k.first - 1; c.je = k.second - 1;
+          c.first = (int)L.upt.size(); c.count = (int)cells[k].size();
+          L.upt.insert(L.upt.end(), cells[k].begin(), cells[k].end());
+          L.upc.push_back(c);
+        }
+      }
+      for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
+        const HPatch& f = node[k];
+        const int rx = intratx[lev], ry = intraty[lev];
+        const int iclo = f.ilo / rx, jclo = f.jlo / ry, ichi = f.ihi / rx, jchi = f.jhi / ry;
+        const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi);
+        if (iplo > iphi || jplo > jphi) continue;
+        AvgRect a{};
+        a.cpatch = m; a.kpatch = k;
+        a.ci0 = iplo - g.ilo + ng; a.cj0 = jplo - g.jlo + ng; a.ni = iphi - iplo + 1; a.nj = jphi - jplo + 1;
+        a.fi0 = iplo * rx - f.ilo + ng; a.fj0 = jplo * ry - f.jlo + ng;
+        L.avg.push_back(a);
+      }
+    }
+    L.d_upc.upload(L.upc, st); L.d_upt.upload(L.upt, st); L.d_avg.upload(L.avg, st);
+  }
+
+  // prepf.f / prepc.f / setuse.f
+  void prepf(int lev) {
+    for (int k = lstart[lev]; k != 0; k = node[k].levelptr) {
+      HPatch& g = node[k];
+      g.lenbc = 2 * (g.nx() / intratx[lev - 1] + g.ny() / intraty[lev - 1]);
+      if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
+      g.nffl = (long long)2 * nvar * g.lenbc;
+      g.ffl = regs.alloc(g.nffl);
+      AMR_CUDA(cudaMemsetAsync(regs.d + g.ffl, 0, sizeof(double) * g.nffl, st));
+    }
+  }
+  static void setuse(std::vector<int>& lb, int& ispot, int mkid, int ilo, int ihi, int jlo, int jhi, int iclo, int ichi,
+                     int jclo, int jchi, int ngh) {
+    auto put = [&](int i, int j, int side, int lkid) {
+      ++ispot;
+      int* e = &lb[5 * (ispot - 1)];
+      e[0] = i; e[1] = j; e[2] = side; e[3] = mkid; e[4] = lkid;
+    };
+    const int ist = iclo - 1, iend = ichi + 1, jst = jclo - 1, jend = jchi + 1;
+    if (!(ist < ilo)) {
+      int lkid = std::max(jlo, jclo) - jclo + 1;
+      for (int j = std::max(jlo, jclo); j <= std::min(jhi, jchi); ++j) put(ist - ilo + ngh + 1, j - jlo + ngh + 1, 3, lkid++);
+    }
+    if (!(jend > jhi)) {
+      int lkid = (jchi - jclo + 1) + std::max(ilo, iclo) - iclo + 1;
+      for (int i = std::max(ilo, iclo); i <= std::min(ihi, ichi); ++i) put(i - ilo + ngh + 1, jend - jlo + ngh + 1, 4, lkid++);
+    }
+    if (!(iend > ihi)) {
+      int lkid = (ichi - iclo + 1) + (jchi - jclo + 1) + std::max(jlo, jclo) - jclo + 1;
+      for (int j = std::max(jlo, jclo); j <= std::min(jhi, jchi); ++j) put(iend - ilo + ngh + 1, j - jlo + ngh + 1, 1, lkid++);
+    }
+    if (!(jst < jlo)) {
+      int lkid = 2 * (jchi - jclo + 1) + (ichi - iclo + 1) + std::max(ilo, iclo) - iclo + 1;
+      for (int i = std::max(ilo, iclo); i <= std::min(ihi, ichi); ++i) put(i - ilo + ngh + 1, jst - jlo + ngh + 1, 2, lkid++);
+    }
+  }
+  void prepc(int lev) {
+    int maxsp = 0;
+    for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr)
+      maxsp += 2 * (node[k].nx() / intratx[lev] + node[k].ny() / intraty[lev]);
+    listsp[lev] = maxsp;
+    if (maxsp == 0) return;
+    const int imax = iregsz[lev] - 1, jmax = jregsz[lev] - 1;
+    for (int mp = lstart[lev]; mp != 0; mp = node[mp].levelptr) {
+      HPatch& g = node[mp];
+      int ispot = 0;
+      g.listbc.assign((size_t)5 * maxsp, 0);
+      g.has_cfl = true;
+      for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
+        const HPatch& f = node[k];
+        const int iclo = f.ilo / intratx[lev], jclo = f.jlo / intraty[lev], ichi = f.ihi / intratx[lev], jchi = f.jhi / intraty[lev];
+        const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi);
+        if (iplo <= iphi + 1 && jplo <= jphi + 1) setuse(g.listbc, ispot, k, g.ilo, g.ihi, g.jlo, g.jhi, iclo, ichi, jclo, jchi, ng);
+        if (xperdom && g.ilo == 0 && ichi == imax) setuse(g.listbc, ispot, k, g.ilo, g.ihi, g.jlo, g.jhi, iclo - iregsz[lev], ichi - iregsz[lev], jclo, jchi, ng);
+        if (xperdom && iclo == 0 && g.ihi == imax) setuse(g.listbc, ispot, k, g.ilo, g.ihi, g.jlo, g.jhi, iclo + iregsz[lev], ichi + iregsz[lev], jclo, jchi, ng);
+        if (yperdom && g.jlo == 0 && jchi == jmax) setuse(g.listbc, ispot, k, g.ilo, g.ihi, g.jlo, g.jhi, iclo, ichi, jclo - jregsz[lev], jchi - jregsz[lev], ng);
+        if (yperdom && jclo == 0 && g.jhi == jmax) setuse(g.listbc, ispot, k, g.ilo, g.ihi, g.jlo, g.jhi, iclo, ichi, jclo + jregsz[lev], jchi + jregsz[lev], ng);
+      }
+    }
+  }
+
+  void free_plan(int lev) {
+    LevelPlan& L = plan[lev];
+    for (FillProg* P : {&L.bound, &L.saveqc}) {
+      P->d_rects.free(); P->d_ops.free(); P->d_chunks.free(); P->d_bcs.free();
+    }
+    L.d_work.free(); L.d_fsv.free(); L.d_fad.free(); L.d_qad.free(); L.d_upc.free(); L.d_upt.free(); L.d_avg.free(); L.d_plist.free();
+  }
+
+  void compile_all() {
+    sync_descriptors();
+    for (int lev = 1; lev <= p.mxnest; ++lev) {
+      if (lev > lfine) {
+        plan[lev].work.clear(); plan[lev].plist.clear();
+        continue;
+      }
+      compile_bound(lev);
+      compile_saveqc(lev);
+      compile_step(lev);
+      compile_update(lev);
+    }
+  }
+
+  // ================================================================ time interpolation modes (intfil.f90:183-232)
+  SrcMode modes_for(int level, double t) {
+    SrcMode M{};
+    for (int l = 1; l <= level; ++l) {
+      if (lgrids[l].empty()) continue;
+      const double gt = node[lgrids[l][0]].time;
+      const double dt = possk[l];
+      const double ac = (gt - t) / dt, ai = 1.0 - ac;
+      const double eps = 1.0e-4;
+      if (ai < -eps || ai > 1.0 + eps) { M.mode[l] = -1; continue; }
+      M.alphai[l] = ai; M.alphac[l] = ac;
+      if (std::fabs(ai - 1.0) < eps) M.mode[l] = 0;
+      else if (std::fabs(ai) < eps) M.mode[l] = 1;
+      else M.mode[l] = 2;
+      if (M.mode[l] != 0 && l == p.mxnest) M.mode[l] = -2;
+    }
+    return M;
+  }
+
+  void bound_level(int lev, double t) {
+    SrcMode M = modes_for(lev, t);
+    for (int l = 1; l <= lev; ++l)
+      if (M.mode[l] < 0 && !lgrids[l].empty() && l != lev + 100) {
+        // a level whose time cannot serve this fill; only an error if the program reads it
+        M.mode[l] = 0;
+      }
+    run_prog(plan[lev].bound, M);
+  }
+
+  // ================================================================ level substep (advanc.f:10-142)
+  double advanc(int lev) {
+    LevelPlan& L = plan[lev];
+    const double t = node[lgrids[lev][0]].time;
+    const double dt = possk[lev];
+    bound_level(lev, t);
+    if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
+    if (lev > 1 && !L.qad.empty()) {
+      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st);
+      ++nkernels;
+    }
+    // gauges (gauges_module.f90:313-452): sampled before the step on the finest covering grid
+    if (record_gauges && !p.gauges.empty()) {
+      std::vector<GaugeJob> jobs;
+      const double hx = hxposs[lev], hy = hyposs[lev];
+      for (size_t i = 0; i < p.gauges.size(); ++i) {
+        const int m = mbestsrc[i];
+        if (m == 0 || node[m].level != lev) continue;
+        const GaugeSpec& G = p.gauges[i];
+        const double tg = node[m].time;
+        if (tg < G.t1 || tg > G.t2) continue;
+        if (tg - glast[i] < G.min_inc) continue;
+        const double xlow = node[m].xlo - ng * hx, ylow = node[m].ylo - ng * hy;
+        GaugeJob J{};
+        J.patch = m; J.ii = (int)(0.5 + (G.x - xlow) / hx); J.jj = (int)(0.5 + (G.y - ylow) / hy);
+        const double xc = xlow + (J.ii - 0.5) * hx, yc = ylow + (J.jj - 0.5) * hy;
+        J.xoff = (G.x - xc) / hx; J.yoff = (G.y - yc) / hy;
+        J.slot = gslots++;
+        jobs.push_back(J);
+        grows.push_back(GaugeRow{G.num, lev, tg, J.slot});
+        glast[i] = tg;
+      }
+      if (!jobs.empty()) {
+        if ((size_t)gslots * nvar > d_gauge_out.cap) {
+          DBuf<double> nb; nb.ensure(std::max<size_t>((size_t)gslots * nvar * 2, 4096));
+          if (d_gauge_out.d) AMR_CUDA(cudaMemcpyAsync(nb.d, d_gauge_out.d, sizeof(double) * d_gauge_out.cap, cudaMemcpyDeviceToDevice, st));
+          d_gauge_out.free(); d_gauge_out = nb;
+        }
+        DBuf<GaugeJob> dj; dj.upload(jobs, st);
+        launch_gauges2(pool.d, d_patches.d, dj.d, (int)jobs.size(), nvar, d_gauge_out.d, st);
+        AMR_CUDA(cudaStreamSynchronize(st));
+        dj.free();
+      }
+    }
+    // the patch step: plain = one launch per patch, batched = one launch per level
+    AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+    StepArgs a{};
+    a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.fsv = L.d_fsv.d; a.fad = L.d_fad.d;
+    a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
+    if (batched) {
+      a.work = L.d_work.d; a.nwork = (int)L.work.size(); a.queue = nullptr;
+      launch_step2(prob.solver, a, (int)L.work.size(), st);
+      ++nkernels;
+    } else {
+      for (size_t k = 0; k < L.plist.size(); ++k) {
+        a.work = L.d_work.d + L.patch_work_lo[k];
+        a.nwork = L.patch_work_hi[k] - L.patch_work_lo[k];
+        a.queue = nullptr;
+        launch_step2(prob.solver, a, a.nwork, st);
+        ++nkernels;
+      }
+    }
+    launch_flip(d_patches.d, L.d_plist.d, (int)L.plist.size(), st);
+    ++nkernels;
+    unsigned long long cbits = 0;
+    AMR_CUDA(cudaMemcpyAsync(&cbits, d_cfl, sizeof(cbits), cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaStreamSynchronize(st));
+    double cmax;
+    std::memcpy(&cmax, &cbits, sizeof(double));
+    for (int m : lgrids[lev]) {
+      node[m].cur ^= 1;
+      node[m].time = node[m].time + dt;
+      const double cells = (double)node[m].nx() * node[m].ny();
+      rvol += cells; rvoll[lev] += cells;
+    }
+    cfl_level = cmax;
+    cflmax_run = std::max(cflmax_run, cmax);
+    ++nsteps_launched;
+    return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
+  }
+
+  void update(int lev) {
+    LevelPlan& L = plan[lev];
+    const double area = hxposs[lev] * hyposs[lev];
+    launch_upbnd(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, area, nvar, st);
+    launch_average(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), intratx[lev], intraty[lev], nvar, st);
+    nkernels += 2;
+  }
+
+  // ================================================================ regrid (regrid.f / grdfit2.f)
+  void setIndices(int ist[3], int iend[3], int jst[3], int jend[3], int ilo, int ihi, int jlo, int jhi, int ish[3], int jsh[3], int lev) {
+    ist[0] = ilo; ist[1] = 0; ist[2] = iregsz[lev]; iend[0] = -1; iend[1] = iregsz[lev] - 1; iend[2] = ihi;
+    jst[0] = jlo; jst[1] = 0; jst[2] = jregsz[lev]; jend[0] = -1; jend[1] = jregsz[lev] - 1; jend[2] = jhi;
+    if (xperdom) { ish[0] = iregsz[lev]; ish[1] = 0; ish[2] = -iregsz[lev]; } else ish[0] = ish[1] = ish[2] = 0;
+    if (yperdom) { jsh[0] = jregsz[lev]; jsh[1] = 0; jsh[2] = -jregsz[lev]; } else jsh[0] = jsh[1] = jsh[2] = 0;
+  }
+
+  void set_phys_bndry(std::vector<int8_t>& f, const IBox& B, int lev) {
+    const int mb = B.mb;
+    if (B.ilo - mb < 0 && !xperdom) for (int j = B.jlo - mb; j <= B.jhi + mb; ++j) for (int i = B.ilo - mb; i <= -1; ++i) f[B.idx(i, j)] = 1;
+    if (B.ihi + mb >= iregsz[lev] && !xperdom) for (int j = B.jlo - mb; j <= B.jhi + mb; ++j) for (int i = iregsz[lev]; i <= B.ihi + mb; ++i) f[B.idx(i, j)] = 1;
+    if (B.jlo - mb < 0 && !yperdom) for (int j = B.jlo - mb; j <= -1; ++j) for (int i = B.ilo - mb; i <= B.ihi + mb; ++i) f[B.idx(i, j)] = 1;
+    if (B.jhi + mb >= jregsz[lev] && !yperdom) for (int j = jregsz[lev]; j <= B.jhi + mb; ++j) for (int i = B.ilo - mb; i <= B.ihi + mb; ++i) f[B.idx(i, j)] = 1;
+  }
+  void shrink(const std::vector<int8_t>& in, std::vector<int8_t>& out, const IBox& B, int lev) {
+    const int mb = B.mb;
+    out.assign((size_t)B.ni() * B.nj(), 0);
+    for (int j = B.jlo - mb + 1; j <= B.jhi + mb - 1; ++j)
+      for (int i = B.ilo - mb + 1; i <= B.ihi + mb - 1; ++i) {
+        bool ok = true;
+        for (int dj = -1; dj <= 1 && ok; ++dj) for (int di = -1; di <= 1; ++di) if (in[B.idx(i + di, j + dj)] <= 0) { ok = false; break; }
+        out[B.idx(i, j)] = ok ? in[B.idx(i, j)] : 0;
+      }
+    set_phys_bndry(out, B, lev);
+  }
+  // setdomflags.f: cells of the lcheck-level buffered box that are properly nested in lbase
+  std::vector<int8_t> nesting_mask(const HPatch& g, int mbuff, int lbase, int lcheck) {
+    int gs[12], ge[12], hs[12], he[12];
+    gs[lcheck] = g.ilo; ge[lcheck] = g.ihi; hs[lcheck] = g.jlo; he[lcheck] = g.jhi;
+    for (int lc_ = lcheck - 1; lc_ >= lbase; --lc_) {
+      int a = (int)std::floor((double)gs[lc_ + 1] / intratx[lc_]), b = (int)std::floor((double)hs[lc_ + 1] / intraty[lc_]);
+      int c = (int)std::ceil((double)ge[lc_ + 1] / intratx[lc_]) - 1, d = (int)std::ceil((double)he[lc_ + 1] / intraty[lc_]) - 1;
+      if (c * intratx[lc_] < ge[lc_ + 1]) c += 1;
+      if (d * intraty[lc_] < he[lc_ + 1]) d += 1;
+      gs[lc_] = a; hs[lc_] = b; ge[lc_] = c; he[lc_] = d;
+    }
+    IBox B{gs[lbase], ge[lbase], hs[lbase], he[lbase], mbuff};
+    std::vector<int8_t> base((size_t)B.ni() * B.nj(), 0);
+    for (int mb = lstart[lbase]; mb != 0; mb = node[mb].levelptr) {
+      const HPatch& b = node[mb];
+      const bool bx = (B.ilo <= 0 || B.ihi >= iregsz[lbase] - 1), by = (B.jlo <= 0 || B.jhi >= jregsz[lbase] - 1);
+      if ((xperdom && bx) || (yperdom && by)) {
+        int ist[3], iend[3], jst[3], jend[3], ish[3], jsh[3];
+        setIndices(ist, iend, jst, jend, B.ilo - mbuff, B.ihi + mbuff, B.jlo - mbuff, B.jhi + mbuff, ish, jsh, lbase);
+        for (int a = 0; a < 3; ++a) {
+          const int i1 = std::max(B.ilo - mbuff, ist[a]), i2 = std::min(B.ihi + mbuff, iend[a]);
+          for (int c = 0; c < 3; ++c) {
+            const int j1 = std::max(B.jlo - mbuff, jst[c]), j2 = std::min(B.jhi + mbuff, jend[c]);
+            if (!(i1 <= i2 && j1 <= j2)) continue;
+            const int ixlo = std::max(b.ilo, i1 + ish[a]), ixhi = std::min(b.ihi, i2 + ish[a]);
+            const int jxlo = std::max(b.jlo, j1 + jsh[c]), jxhi = std::min(b.jhi, j2 + jsh[c]);
+            if (ixlo > ixhi || jxlo > jxhi) continue;
+            for (int jj = jxlo - jsh[c]; jj <= jxhi - jsh[c]; ++jj) for (int ii = ixlo - ish[a]; ii <= ixhi - ish[a]; ++ii) base[B.idx(ii, jj)] = 1;
+          }
+        }
+      } else {
+        const int ixlo = std::max(b.ilo, B.ilo - mbuff), ixhi = std::min(b.ihi, B.ihi + mbuff);
+        const int jxlo = std::max(b.jlo, B.jlo - mbuff), jxhi = std::min(b.jhi, B.jhi + mbuff);
+        if (!(ixlo <= ixhi && jxlo <= jxhi)) continue;
+        for (int jj = jxlo; jj <= jxhi; ++jj) for (int ii = ixlo; ii <= ixhi; ++ii) base[B.idx(ii, jj)] = 1;
+      }
+    }
+    set_phys_bndry(base, B, lbase);
+    std::vector<int8_t> cur;
+    shrink(base, cur, B, lbase);
+    for (int lev = lbase + 1; lev <= lcheck; ++lev) {
+      IBox F{gs[lev], ge[lev], hs[lev], he[lev], mbuff};
+      const int rx = intratx[lev - 1], ry = intraty[lev - 1];
+      std::vector<int8_t> up((size_t)F.ni() * F.nj(), 0);
+      for (int j = B.jlo; j <= B.jhi; ++j)
+        for (int i = B.ilo; i <= B.ihi; ++i)
+          for (int mj = 1; mj <= ry; ++mj)
+            for (int mi = 1; mi <= rx; ++mi) {
+              const int is = std::max(std::min(i * rx - 1 + mi, F.ihi + mbuff), F.ilo - mbuff);
+              const int js = std::max(std::min(j * ry - 1 + mj, F.jhi + mbuff), F.jlo - mbuff);
+              up[F.idx(is, js)] = cur[B.idx(i, j)];
+            }
+      for (int j = F.jlo - mbuff; j <= F.jhi + mbuff; ++j) {
+        for (int i = F.ihi + 1; i <= F.ihi + mbuff; ++i) up[F.idx(i, j)] = cur[B.idx(i / rx, j / ry)];
+        for (int i = F.ilo - mbuff; i <= F.ilo - 1; ++i) up[F.idx(i, j)] = cur[B.idx(i / rx, j / ry)];
+      }
+      for (int i = F.ilo; i <= F.ihi; ++i) {
+        for (int j = F.jlo - mbuff; j <= F.jlo - 1; ++j) up[F.idx(i, j)] = cur[B.idx(i / rx, j / ry)];
+        for (int j = F.jhi + 1; j <= F.jhi + mbuff; ++j) up[F.idx(i, j)] = cur[B.idx(i / rx, j / ry)];
+      }
+      std::vector<int8_t> nx_;
+      shrink(up, nx_, F, lev);
+      cur.swap(nx_);
+      B = F;
+    }
+    return cur;
+  }
+
+  bool base_check(const HPatch& n, int lbase, int thisBuff) {
+    const int levnew = n.level;
+    const bool bx = (n.ilo == 0 || n.ihi == iregsz[levnew] - 1), by = (n.jlo == 0 || n.jhi == jregsz[levnew] - 1);
+    int iclo = n.ilo, ichi = n.ihi, jclo = n.jlo, jchi = n.jhi;
+    for (int lev = levnew - 1; lev >= lbase; --lev) {
+      iclo = iclo / intratx[lev] - 1; ichi = ichi / intratx[lev] + 1; jclo = jclo / intraty[lev] - 1; jchi = jchi / intraty[lev] + 1;
+    }
+    if (!(xperdom && bx) && !(yperdom && by)) {
+      iclo = std::max(iclo, 0); jclo = std::max(jclo, 0); ichi = std::min(ichi, iregsz[lbase] - 1); jchi = std::min(jchi, jregsz[lbase] - 1);
+    }
+    const int li = ichi - iclo + 1, lj = jchi - jclo + 1;
+    std::vector<int8_t> M((size_t)li * lj, 0);
+    auto at = [&](int i, int j) -> int8_t& { return M[(size_t)(i - iclo) + (size_t)li * (j - jclo)]; };
+    if (n.ilo == 0 && !xperdom) for (int j = jclo; j <= jchi; ++j) { at(iclo, j) = 1; at(iclo + 1, j) = 1; }
+    if (n.ihi == iregsz[levnew] - 1 && !xperdom) for (int j = jclo; j <= jchi; ++j) { at(ichi, j) = 1; at(ichi - 1, j) = 1; }
+    if (n.jlo == 0 && !yperdom) for (int i = iclo; i <= ichi; ++i) { at(i, jclo) = 1; at(i, jclo + 1) = 1; }
+    if (n.jhi == jregsz[levnew] - 1 && !yperdom) for (int i = iclo; i <= ichi; ++i) { at(i, jchi) = 1; at(i, jchi - 1) = 1; }
+    for (int mp = lstart[lbase]; mp != 0; mp = node[mp].levelptr) {
+      const int iblo = node[mp].ilo - thisBuff, ibhi = node[mp].ihi + thisBuff, jblo = node[mp].jlo - thisBuff, jbhi = node[mp].jhi + thisBuff;
+      if (!(xperdom && bx) && !(yperdom && by)) {
+        const int a = std::max(iclo, iblo), b = std::min(ichi, ibhi), c = std::max(jclo, jblo), d = std::min(jchi, jbhi);
+        for (int j = c; j <= d; ++j) for (int i = a; i <= b; ++i) at(i, j) = 1;
+        continue;
+      }
+      int ist[3], iend[3], jst[3], jend[3], ish[3], jsh[3];
+      setIndices(ist, iend, jst, jend, iclo, ichi, jclo, jchi, ish, jsh, lbase);
+      for (int a = 0; a < 3; ++a) {
+        const int i1 = std::max(iclo, ist[a]), i2 = std::min(ichi, iend[a]);
+        for (int c = 0; c < 3; ++c) {
+          const int j1 = std::max(jclo, jst[c]), j2 = std::min(jchi, jend[c]);
+          if (!(i1 <= i2 && j1 <= j2)) continue;
+          const int xl = std::max(i1 + ish[a], iblo), xh = std::min(i2 + ish[a], ibhi), yl = std::max(j1 + jsh[c], jblo), yh = std::min(j2 + jsh[c], jbhi);
+          for (int j = yl; j <= yh; ++j) for (int i = xl; i <= xh; ++i) at(i - ish[a], j - jsh[c]) = 1;
+        }
+      }
+    }
+    for (int8_t v : M) if (v == 0) return false;
+    return true;
+  }
+
+  // flagger.f + bufnst2.f + colate2.f: the sorted, unique flagged points of level lcheck
+  std::vector<Pt> flag_points(int lcheck, int lbase) {
+    const int mbuff = std::max(ng, p.ibuff + 1);
+    std::vector<int>& G = lgrids[lcheck];
+    const double t = node[G[0]].time;
+    int use_old = 0;
+    if (start_time + possk[lcheck] != t) bound_level(lcheck, t);
+    else use_old = 1;
+    // device gradient test
+    std::vector<long long> off(G.size() + 1, 0);
+    for (size_t k = 0; k < G.size(); ++k) off[k + 1] = off[k] + (long long)node[G[k]].nx() * node[G[k]].ny();
+    DBuf<int8_t> dout; dout.ensure(std::max<long long>(off.back(), 1));
+    DBuf<long long> doff; doff.upload(off, st);
+    DBuf<int> dpl; dpl.upload(G, st);
+    launch_flags2(pool.d, d_patches.d, dpl.d, doff.d, (int)G.size(), use_old, p.flag_component, p.tolsp, nvar, dout.d, st);
+    std::vector<int8_t> hflag(off.back());
+    if (off.back()) AMR_CUDA(cudaMemcpyAsync(hflag.data(), dout.d, off.back(), cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaStreamSynchronize(st));
+    dout.free(); doff.free(); dpl.free();
+    const double dx = hxposs[lcheck], dy = hyposs[lcheck];
+    std::vector<Pt> pts;
+    int numbad = 0;
+    for (size_t k = 0; k < G.size(); ++k) {
+      HPatch& g = node[G[k]];
+      const int mx = g.nx(), my = g.ny();
+      IBox B{g.ilo, g.ihi, g.jlo, g.jhi, mbuff};
+      std::vector<int8_t> f((size_t)B.ni() * B.nj(), FLAG_UNSET);
+      // flagregions2.f90
+      std::vector<int> mnl((size_t)mx * my, 0), mxl((size_t)mx * my, 0);
+      const double xu = g.xlo + mx * dx, yu = g.ylo + my * dy;
+      for (const RegionSpec& r : p.regions) {
+        if (t < r.t1 || t > r.t2) continue;
+        if (g.xlo >= r.x2 || xu <= r.x1) continue;
+        const int i1 = std::max((int)std::floor((r.x1 - g.xlo) / dx) + 1, 1), i2 = std::min((int)std::floor((r.x2 - g.xlo) / dx) + 1, mx);
+        if (g.ylo >= r.y2 || yu <= r.y1) continue;
+        const int j1 = std::max((int)std::floor((r.y1 - g.ylo) / dy) + 1, 1), j2 = std::min((int)std::floor((r.y2 - g.ylo) / dy) + 1, my);
+        for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+          mnl[(size_t)(j - 1) * mx + i - 1] = std::max(mnl[(size_t)(j - 1) * mx + i - 1], r.minlevel);
+          mxl[(size_t)(j - 1) * mx + i - 1] = std::max(mxl[(size_t)(j - 1) * mx + i - 1], r.maxlevel);
+        }
+      }
+      const int8_t* gf = hflag.data() + off[k];
+      for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i) {
+          const int a = mnl[(size_t)(j - 1) * mx + i - 1], b = mxl[(size_t)(j - 1) * mx + i - 1];
+          if (a > b) throw std::runtime_error("region minimum level exceeds its maximum level");
+          int8_t v = FLAG_UNSET;
+          if (b != 0) { if (lcheck < a) v = FLAG_DO; else if (lcheck >= b) v = FLAG_DONT; }
+          if (v == FLAG_UNSET && p.flag_gradient && gf[(size_t)(j - 1) * mx + (i - 1)]) v = FLAG_DO;
+          f[B.idx(g.ilo + i - 1, g.jlo + j - 1)] = v;
+        }
+      // projec2.f: cells under level lcheck+2 grids just created
+      if (lcheck + 2 <= p.mxnest) {
+        for (int mk = newstl[lcheck + 2]; mk != 0; mk = node[mk].levelptr) {
+          const HPatch& c = node[mk];
+          int istc = (c.ilo / intratx[lcheck + 1] - 1) / intratx[lcheck] - 1, jstc = (c.jlo / intraty[lcheck + 1] - 1) / intraty[lcheck] - 1;
+          int iendc = (c.ihi / intratx[lcheck + 1] + 1) / intratx[lcheck] + 1, jendc = (c.jhi / intraty[lcheck + 1] + 1) / intraty[lcheck] + 1;
+          const bool bx = (istc <= 0 || iendc >= iregsz[lcheck] - 1), by = (jstc <= 0 || jendc >= jregsz[lcheck] - 1);
+          auto markp = [&](int a0, int a1, int b0, int b1) {
+            const int xl = std::max(a0, g.ilo - mbuff), xh = std::min(a1, g.ihi + mbuff), yl = std::max(b0, g.jlo - mbuff), yh = std::min(b1, g.jhi + mbuff);
+            for (int j = yl; j <= yh; ++j) for (int i = xl; i <= xh; ++i) if (f[B.idx(i, j)] <= FLAG_DONT) f[B.idx(i, j)] = FLAG_BADPRO;
+          };
+          if (!(xperdom && bx) && !(yperdom && by)) {
+            istc = std::max(istc, 0); jstc = std::max(jstc, 0); iendc = std::min(iendc, iregsz[lcheck]); jendc = std::min(jendc, jregsz[lcheck]);
+            markp(istc, iendc, jstc, jendc);
+          } else {
+            int ist[3], iend[3], jst[3], jend[3], ish[3], jsh[3];
+            setIndices(ist, iend, jst, jend, istc, iendc, jstc, jendc, ish, jsh, lcheck);
+            for (int a = 0; a < 3; ++a) for (int c2 = 0; c2 < 3; ++c2) {
+              const int i1 = std::max(istc, ist[a]), i2 = std::min(iendc, iend[a]), j1 = std::max(jstc, jst[c2]), j2 = std::min(jendc, jend[c2]);
+              if (!(i1 <= i2 && j1 <= j2)) continue;
+              markp(i1 + ish[a], i2 + ish[a], j1 + jsh[c2], j2 + jsh[c2]);
+            }
+          }
+        }
+      }
+      // shiftset2.f: buffer by ibuff in every direction
+      std::vector<int8_t> buf((size_t)B.ni() * B.nj(), FLAG_DONT);
+      for (int j = g.jlo; j <= g.jhi; ++j)
+        for (int i = g.ilo; i <= g.ihi; ++i) {
+          const int8_t r = f[B.idx(i, j)];
+          if (r > 0) for (int kk = j - p.ibuff; kk <= j + p.ibuff; ++kk) for (int mm = i - p.ibuff; mm <= i + p.ibuff; ++mm) buf[B.idx(mm, kk)] = r;
+        }
+      int nf = 0;
+      for (int8_t v : buf) if (v > FLAG_DONT) ++nf;
+      g.numflags = nf;
+      numbad += nf;
+      g.flags.swap(buf);
+      g.dom2 = nesting_mask(g, mbuff, lbase, lcheck);
+    }
+    if (numbad == 0) { for (int m : G) { node[m].flags.clear(); node[m].dom2.clear(); } return pts; }
+    // colate2.f: nested flags with periodic wrap, in grid-list order
+    for (int m = lstart[lcheck]; m != 0; m = node[m].levelptr) {
+      HPatch& g = node[m];
+      if (g.numflags != 0) {
+        IBox B{g.ilo, g.ihi, g.jlo, g.jhi, mbuff};
+        int jmin = g.jlo - mbuff, jmax = g.jhi + mbuff, imin = g.ilo - mbuff, imax = g.ihi + mbuff;
+        if (!xperdom) { imin = std::max(imin, 0); imax = std::min(g.ihi + mbuff, iregsz[lcheck] - 1); }
+        if (!yperdom) { jmin = std::max(jmin, 0); jmax = std::min(g.jhi + mbuff, jregsz[lcheck] - 1); }
+        for (int j = jmin; j <= jmax; ++j) for (int i = imin; i <= imax; ++i)
+          if (g.flags[B.idx(i, j)] > FLAG_DONT && g.dom2[B.idx(i, j)] != 1) g.flags[B.idx(i, j)] = FLAG_DONT;
+        for (int j = jmin; j <= jmax; ++j) for (int i = imin; i <= imax; ++i) {
+          if (g.flags[B.idx(i, j)] <= FLAG_DONT) continue;
+          int iw = i, jw = j;
+          if (xperdom) { if (i < 0) iw = i + iregsz[lcheck]; if (i >= iregsz[lcheck]) iw = i - iregsz[lcheck]; }
+          if (yperdom) { if (j < 0) jw = j + jregsz[lcheck]; if (j >= jregsz[lcheck]) jw = j - jregsz[lcheck]; }
+          pts.push_back(Pt{iw, jw});
+        }
+      }
+      g.flags.clear(); g.dom2.clear();
+    }
+    sort_unique(pts, iregsz[lcheck], mbuff);
+    return pts;
+  }
+
+  // grdfit2.f:20-150
+  void grdfit(int lbase, int lcheck, double t) {
+    std::vector<Pt> pts = flag_points(lcheck, lbase);
+    if (pts.empty()) return;
+    const int levnew = lcheck + 1;
+    const double hxf = hxposs[levnew], hyf = hyposs[levnew];
+    std::vector<int> cnt;
+    bisect(pts, p.cut, iregsz[lcheck], jregsz[lcheck], cnt);
+    int base = 0, icl = 0, prv = 0;
+    while (icl < (int)cnt.size()) {
+      const int mnew = nodget();
+      while (true) {
+        int rect[4];
+        bbox_usage(&pts[base], cnt[icl], rect);
+        HPatch& n = node[mnew];
+        n.ilo = rect[0] * intratx[lcheck]; n.jlo = rect[2] * intraty[lcheck];
+        n.ihi = (rect[1] + 1) * intratx[lcheck] - 1; n.jhi = (rect[3] + 1) * intraty[lcheck] - 1;
+        n.xlo = n.ilo * hxf + xlower; n.ylo = n.jlo * hyf + ylower;
+        n.xhi = (n.ihi + 1) * hxf + xlower; n.yhi = (n.jhi + 1) * hyf + ylower;
+        n.level = levnew; n.time = t;
+        // nestck2.f:37-176
+        bool n1 = (lbase == 1) ? true : base_check(n, lbase, 0);
+        const int l2 = levnew - 2;
+        bool n2;
+        if (l2 <= 1) n2 = true;
+        else if (l2 <= lbase) n2 = n1;
+        else n2 = base_check(n, l2, std::max(ng, p.ibuff + 1));
+        if (n1 && n2) break;
+        const int npts = cnt[icl];
+        if (npts <= 1) throw std::runtime_error("a single flagged point cannot be properly nested");
+        double rmid; int dir;
+        if (n.xhi - n.xlo > n.yhi - n.ylo) { rmid = (n.ihi + n.ilo + 1) / 2.; rmid = rmid / intratx[levnew - 1]; dir = 1; }
+        else { rmid = (n.jhi + n.jlo + 1) / 2.; rmid = rmid / intraty[levnew - 1]; dir = 2; }
+        int ipt = base, ntop = base + npts - 1;
+        auto coord = [&](int k) { return (dir == 1 ? pts[k].i : pts[k].j) + 0.5; };
+        while (true) {
+          if (coord(ipt) < rmid) { ++ipt; if (ipt <= ntop) continue; break; }
+          std::swap(pts[ipt], pts[ntop]);
+          --ntop;
+          if (ipt <= ntop) continue;
+          break;
+        }
+        const int front = ntop - base + 1;
+        cnt[icl] = front;
+        cnt.insert(cnt.begin() + icl + 1, npts - front);
+      }
+      if (newstl[levnew] == 0) newstl[levnew] = mnew;
+      else node[prv].levelptr = mnew;
+      prv = mnew;
+      base += cnt[icl];
+      ++icl;
+    }
+    birect(newstl[levnew]);
+  }
+
+  // filval.f90 for all new grids of level lev, then release the old grids (gfixup.f:49-163)
+  void fill_new_level(int lev) {
+    FillProg P;
+    P.scratch_len = 0;
+    const int rx = intratx[lev - 1], ry = intraty[lev - 1];
+    const double dxc = hxposs[lev] * rx, dyc = hyposs[lev] * ry;
+    for (int m = newstl[lev]; m != 0; m = node[m].levelptr) {
+      const HPatch& g = node[m];
+      const int iclo = g.ilo / rx - 1, jclo = g.jlo / ry - 1, ichi = (g.ihi + 1) / rx - 1 + 1, jchi = (g.jhi + 1) / ry - 1 + 1;
+      const int mic = g.nx() / rx + 2, mjc = g.ny() / ry + 2;
+      const int R = P.add_rect(mic, mjc, nvar);
+      Tgt C{-1, R, mic, mjc};
+      const bool sxc = (iclo < 0) || (ichi >= iregsz[lev - 1]), syc = (jclo < 0) || (jchi >= jregsz[lev - 1]);
+      if ((xperdom && sxc) || (yperdom && syc)) c_preicall(P, C, iclo, ichi, jclo, jchi, lev - 1, 0);
+      else c_icall(P, C, iclo, ichi, jclo, jchi, lev - 1, 1, 1, 0);
+      bool any;
+      BcOp b = make_bc(C, dxc, dyc, g.xlo - dxc, g.xhi + dxc, g.ylo - dyc, g.yhi + dyc, any);
+      if (any) P.add_bc(b, 0);
+      // fine copies from the old grids of this level over the interior
+      const int nx = g.nx(), ny = g.ny();
+      std::vector<int8_t> cov((size_t)nx * ny, 0);
+      for (int o = lstart[lev]; o != 0; o = node[o].levelptr) {
+        const HPatch& s = node[o];
+        const int ixlo = std::max(s.ilo, g.ilo), ixhi = std::min(s.ihi, g.ihi), jxlo = std::max(s.jlo, g.jlo), jxhi = std::min(s.jhi, g.jhi);
+        if (!(ixlo <= ixhi && jxlo <= jxhi)) continue;
+        FillOp o2{};
+        o2.kind = FILL_COPY; o2.dst_patch = m; o2.dst_rect = -1;
+        o2.di0 = ixlo - g.ilo + ng; o2.dj0 = jxlo - g.jlo + ng; o2.ni = ixhi - ixlo + 1; o2.nj = jxhi - jxlo + 1;
+        o2.src = o; o2.si0 = ixlo - s.ilo + ng; o2.sj0 = jxlo - s.jlo + ng; o2.level = -1;
+        P.add_op(o2, 1);
+        for (int j = jxlo; j <= jxhi; ++j) for (int i = ixlo; i <= ixhi; ++i) cov[(size_t)(j - g.jlo) * nx + (i - g.ilo)] = 1;
+      }
+      std::vector<int> rr;
+      runs(cov, nx, ny, rr);
+      for (size_t k = 0; k < rr.size(); k += 4) {
+        FillOp o2{};
+        o2.kind = FILL_FILVAL; o2.dst_patch = m; o2.dst_rect = -1;
+        o2.di0 = rr[k] + ng; o2.dj0 = rr[k + 1] + ng; o2.ni = rr[k + 2]; o2.nj = rr[k + 3];
+        o2.src = R; o2.si0 = g.ilo + rr[k]; o2.sj0 = g.jlo + rr[k + 1]; o2.level = lev; o2.cilo = iclo; o2.cjlo = jclo;
+        P.add_op(o2, 1);
+      }
+    }
+    upload_prog(P);
+    SrcMode M{};
+    run_prog(P, M);
+    AMR_CUDA(cudaStreamSynchronize(st));
+    pool.release(P.scratch_off, std::max<long long>(P.scratch_len, 1));
+    P.d_rects.free(); P.d_ops.free(); P.d_chunks.free(); P.d_bcs.free();
+  }
+
+  void regrid(int lbase) {
+    const auto t0c = std::chrono::steady_clock::now();
+    int lcheck = std::min(lfine, p.mxnest - 1);
+    int lfnew = lbase;
+    for (int i = 1; i <= p.mxnest; ++i) newstl[i] = 0;
+    const double t = node[lstart[lbase]].time;
+    while (lcheck >= lbase) {
+      grdfit(lbase, lcheck, t);
+      if (newstl[lcheck + 1] != 0) lfnew = std::max(lcheck + 1, lfnew);
+      --lcheck;
+    }
+    // gfixup.f: registers of the changed levels are rebuilt below
+    for (int lcheck2 = lbase + 1; lcheck2 <= p.mxnest; ++lcheck2) {
+      for (int m = newstl[lcheck2]; m != 0; m = node[m].levelptr) alloc_patch(m);
+      // descriptors must know the new patches before their fill runs
+      std::vector<int> keep = lgrids[lcheck2];
+      lgrids[lcheck2].clear();
+      for (int m = newstl[lcheck2]; m != 0; m = node[m].levelptr) lgrids[lcheck2].push_back(m);
+      int lf_save = lfine;
+      lfine = std::max(lfine, lcheck2);
+      sync_descriptors_with(keep, lcheck2);
+      lfine = lf_save;
+      lgrids[lcheck2] = keep;
+      if (newstl[lcheck2] != 0) fill_new_level(lcheck2);
+      int m = lstart[lcheck2];
+      while (m != 0) {
+        const int mold = m;
+        m = node[m].levelptr;
+        free_patch(mold);
+        node[mold].bnd.clear(); node[mold].listbc.clear();
+        putnod(mold);
+      }
+      lstart[lcheck2] = newstl[lcheck2];
+      lgrids[lcheck2].clear();
+      for (int q = lstart[lcheck2]; q != 0; q = node[q].levelptr) lgrids[lcheck2].push_back(q);
+    }
+    lfine = lfnew;
+    for (int lev = lbase; lev <= p.mxnest; ++lev) { for (int m : lgrids[lev]) { node[m].has_cfl = false; node[m].listbc.clear(); } }
+    for (int lev = lbase; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
+    for (int lev = lbase + 1; lev <= p.mxnest; ++lev) arrange(lev);
+    make_lists();
+    for (int lev = lbase + 1; lev <= lfine; ++lev) make_bndry(lev);
+    compile_all();
+    t_regrid += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0c).count();
+  }
+
+  // descriptors for: all current levels plus the old and new patches of level `lev` (during gfixup)
+  void sync_descriptors_with(const std::vector<int>& old_lev_grids, int lev) {
+    h_patches.assign(node.size(), PatchDev{});
+    auto put = [&](int m) {
+      const HPatch& g = node[m];
+      PatchDev& d = h_patches[m];
+      d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl;
+      d.ilo = g.ilo; d.ihi = g.ihi; d.jlo = g.jlo; d.jhi = g.jhi;
+      d.mitot = mitot(m); d.mjtot = mjtot(m); d.mktot = 1; d.level = g.level; d.lenbc = g.lenbc;
+    };
+    for (int l = 1; l <= p.mxnest; ++l) for (int m : lgrids[l]) put(m);
+    for (int m : old_lev_grids) put(m);
+    for (int l = 1; l < lev; ++l) for (int m = lstart[l]; m != 0; m = node[m].levelptr) put(m);
+    d_patches.upload(h_patches, st);
+    (void)lev;
+  }
+
+  // ================================================================ init (amr2.f90, domain.f, setgrd.f)
+  void init(const std::string& dir) {
+    p.load(dir);
+    if (p.ndim != 2) throw std::runtime_error("this solver handles 2D runs");
+    if (p.nghost != 2) throw std::runtime_error("num_ghost must be 2");
+    if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
+    if (p.dimsplit != 0) throw std::runtime_error("only the unsplit method is supported");
+    if (p.src_split != 0) throw std::runtime_error("source terms are not supported");
+    nvar = p.nvar; ng = p.nghost;
+    setup_problem();
+    xlower = p.lower[0]; ylower = p.lower[1]; xupper = p.upper[0]; yupper = p.upper[1];
+    nxc = p.ncells[0]; nyc = p.ncells[1];
+    xperdom = (p.mthbc[1] == 2 && p.mthbc[2] == 2);
+    yperdom = (p.mthbc[3] == 2 && p.mthbc[4] == 2);
+    for (int k = 1; k <= 10; ++k) { intratx[k] = p.ratx[k]; intraty[k] = p.raty[k]; kratio[k] = p.ratt[k]; }
+    hxposs[1] = (xupper - xlower) / nxc;
+    hyposs[1] = (yupper - ylower) / nyc;
+    for (int lev = 2; lev <= p.mxnest; ++lev) { hxposs[lev] = hxposs[lev - 1] / (double)intratx[lev - 1]; hyposs[lev] = hyposs[lev - 1] / (double)intraty[lev - 1]; }
+    possk[1] = p.dt_initial;
+    iregsz[1] = nxc; jregsz[1] = nyc;
+    for (int lev = 2; lev <= p.mxnest; ++lev) {
+      iregsz[lev] = iregsz[lev - 1] * intratx[lev - 1];
+      jregsz[lev] = jregsz[lev - 1] * intraty[lev - 1];
+      possk[lev] = possk[lev - 1] / (double)kratio[lev - 1];
+    }
+    for (int l = 0; l < MAXLV + 2; ++l) {
+      lc.hx[l] = l < 12 ? hxposs[l] : 0; lc.hy[l] = l < 12 ? hyposs[l] : 0;
+      lc.iregsz[l] = iregsz[l]; lc.jregsz[l] = jregsz[l]; lc.intratx[l] = intratx[l]; lc.intraty[l] = intraty[l];
+    }
+    AMR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    long long est = (long long)nvar * (nxc + 4) * (nyc + 4) * 8 * std::max(1, p.mxnest) + (1 << 22);
+    pool.init(est);
+    regs.init(1 << 20);
+    AMR_CUDA(cudaMalloc(&d_cfl, sizeof(unsigned long long)));
+    AMR_CUDA(cudaMalloc(&d_mass, sizeof(double)));
+    node.assign(10001, HPatch());
+    for (int k = 1; k <= 10000; ++k) node[k].nextfree = k + 1;
+    node[10000].nextfree = 0;
+    ndfree = 1;
+    start_time = p.t0;
+    // domain.f
+    const int ms = nodget();
+    node[ms].xlo = xlower; node[ms].ylo = ylower; node[ms].yhi = yupper; node[ms].xhi = xupper;
+    node[ms].level = 1; node[ms].levelptr = 0;
+    node[ms].ilo = 0; node[ms].jlo = 0; node[ms].ihi = nxc - 1; node[ms].jhi = nyc - 1;
+    lstart[1] = ms;
+    lfine = 1;
+    birect(ms);
+    ginit(lstart[1], start_time);
+    arrange(1);
+    make_lists();
+    make_bndry(1);
+    sync_descriptors();
+    // setgrd.f
+    record_gauges = false;
+    if (p.mxnest > 1) {
+      int levnew = 2;
+      while (levnew <= p.mxnest) {
+        const int levold = levnew - 1;
+        if (lstart[levold] == 0) break;
+        compile_all();
+        for (int i = 1; i <= p.mxnest; ++i) newstl[i] = 0;
+        grdfit(levold, levold, start_time);
+        int lfnew = levold;
+        if (newstl[levnew] != 0) lfnew = levnew;
+        if (newstl[levnew] != 0) ginit(newstl[levnew], start_time);
+        lstart[levnew] = newstl[levnew];
+        lfine = lfnew;
+        arrange(levnew);
+        make_lists();
+        make_bndry(levnew);
+        ++levnew;
+      }
+      // store1 and store2 of the initial levels hold the same qinit data; both buffers were filled
+      compile_all();
+      for (int lev = lfine - 1; lev >= 1; --lev) update(lev);
+      for (int lev = 1; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
+    }
+    compile_all();
+    record_gauges = true;
+    time = p.t0;
+    mbestsrc.assign(p.gauges.size(), 0);
+    glast.assign(p.gauges.size(), 0.0);
+    for (size_t i = 0; i < p.gauges.size(); ++i) glast[i] = p.gauges[i].t1;
+    frame = p.output_t0 ? 0 : 1;
+    tmass0 = mass();
+    if (p.output_t0) output(time);
+    AMR_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // ginit.f: new grids at the initial time, qinit into both buffers
+  void ginit(int msave, double t) {
+    for (int m = msave; m != 0; m = node[m].levelptr) {
+      alloc_patch(m);
+      HPatch& g = node[m];
+      g.time = t;
+      std::vector<double> q;
+      qinit(g.nx(), g.ny(), g.xlo, g.ylo, hxposs[g.level], hyposs[g.level], q);
+      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q0, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
+      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q1, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
+      AMR_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+
+  void setbestsrc() {
+    for (size_t i = 0; i < p.gauges.size(); ++i) {
+      mbestsrc[i] = 0;
+      for (int lev = lfine; lev >= 1 && mbestsrc[i] == 0; --lev)
+        for (int m = lstart[lev]; m != 0; m = node[m].levelptr) {
+          const HPatch& g = node[m];
+          if (p.gauges[i].x >= g.xlo && p.gauges[i].x <= g.xhi && p.gauges[i].y >= g.ylo && p.gauges[i].y <= g.yhi) { mbestsrc[i] = m; break; }
+        }
+    }
+  }
+
+  double mass() {
+    AMR_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double), st));
+    launch_mass2(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st);
+    double m = 0;
+    AMR_CUDA(cudaMemcpyAsync(&m, d_mass, sizeof(double), cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaStreamSynchronize(st));
+    return m * hxposs[1] * hyposs[1];
+  }
+
+  // valout.f90: zero |q| < 1e-90 in place (the reference does) and optionally write fort.q / fort.t
+  void output(double t);
+
+  // ================================================================ tick.f
+  void tick() {
+    double dtnew[12], tlevel[12];
+    int ntogo[12];
+    ncycle = 0;
+    setbestsrc();
+    int iout = p.iout, nextout = 0;
+    if (iout == 0) { iout = 999999999; nextout = p.nout > 0 ? 1 : 0; }
+    tlevel[1] = time;
+    for (int i = 2; i <= p.mxnest; ++i) tlevel[i] = tlevel[1];
+    const auto tstart = std::chrono::steady_clock::now();
+    while (!(ncycle >= p.nstop || time >= p.tfinal)) {
+      double outtime = (p.nout > 0) ? (nextout <= p.nout ? p.tout[nextout - 1] : RINF) : p.tfinal;
+      bool dumpout = false;
+      if (time < outtime && time + (double)1.001f * possk[1] >= outtime) {
+        possk[1] = outtime - time;
+        for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
+        if (p.nout > 0) { ++nextout; dumpout = true; }
+      }
+      int level = 1;
+      ntogo[level] = 1;
+      for (int i = 1; i <= 10; ++i) dtnew[i] = RINF;
+      while (true) {
+        int lbase = -1;
+        if (icheck[level] >= p.kcheck) lbase = level;
+        else if (level + 1 >= p.mxnest) lbase = -1;
+        else if (icheck[level + 1] >= p.kcheck) lbase = level + 1;
+        else if (level + 2 >= p.mxnest) lbase = -1;
+        else if (icheck[level + 2] >= p.kcheck) lbase = level + 2;
+        if (lbase > 0) {
+          if (!(lbase == p.mxnest || lbase > lfine)) { regrid(lbase); setbestsrc(); }
+          for (int i = lbase; i <= lfine; ++i) icheck[i] = 0;
+          for (int i = lbase + 1; i <= lfine; ++i) tlevel[i] = tlevel[lbase];
+        }
+        const double dtl = advanc(level);
+        ntogo[level] -= 1;
+        dtnew[level] = std::min(dtnew[level], dtl);
+        tlevel[level] = tlevel[level] + possk[level];
+        icheck[level] += 1;
+        if (level < lfine) {
+          ++level;
+          if (((possk[level - 1] - dtnew[level - 1]) / dtnew[level - 1]) > (double)0.05f) {
+            const double dttemp = dtnew[level - 1] / kratio[level - 1];
+            ntogo[level] = (int)((tlevel[level - 1] - tlevel[level]) / dttemp + (double)0.9f);
+          } else ntogo[level] = kratio[level - 1];
+          possk[level] = possk[level - 1] / ntogo[level];
+          continue;
+        }
+        bool done = false;
+        while (true) {
+          if (level == 1) { done = true; break; }
+          if (ntogo[level] > 0) {
+            while ((possk[level] - dtnew[level]) / dtnew[level] > (double)0.05f) {
+              ntogo[level] += 1;
+              possk[level] = (tlevel[level - 1] - tlevel[level]) / ntogo[level];
+            }
+            break;
+          }
+          --level;
+          update(level);
+        }
+        if (done) break;
+      }
+      time = time + possk[1];
+      ++ncycle;
+      if (p.vtime) {
+        for (int i = 2; i <= lfine; ++i) { const int ii = lfine + 1 - i; dtnew[ii] = std::min(dtnew[ii], dtnew[ii + 1] * kratio[ii]); }
+        dtnew[1] = std::min(dtnew[1], p.dt_max);
+        possk[1] = dtnew[1];
+        for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
+      }
+      if ((ncycle % iout == 0) || dumpout) output(time);
+      if (max_cycles > 0 && ncycle >= max_cycles) break;
+    }
+    AMR_CUDA(cudaStreamSynchronize(st));
+    t_step = std::chrono::duration<double>(std::chrono::steady_clock::now() - tstart).count();
+  }
+
+  // interior values of all grids (levels 1..lfine, list order), layout [m][j][i] per grid
+  std::vector<double> gather_values() {
+    std::vector<int> pl;
+    std::vector<long long> off(1, 0);
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) { pl.push_back(m); off.push_back(off.back() + (long long)nvar * node[m].nx() * node[m].ny()); }
+    off.pop_back();
+    long long tot = 0;
+    for (int m : pl) tot += (long long)nvar * node[m].nx() * node[m].ny();
+    std::vector<double> out(tot);
+    if (tot == 0) return out;
+    DBuf<double> d; d.ensure(tot);
+    DBuf<int> dp; dp.upload(pl, st);
+    DBuf<long long> doff; doff.upload(off, st);
+    launch_gather_interior2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, st);
+    AMR_CUDA(cudaMemcpyAsync(out.data(), d.d, sizeof(double) * tot, cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaStreamSynchronize(st));
+    d.free(); dp.free(); doff.free();
+    return out;
+  }
+};
+
+}  // namespace amrb
+
+namespace amrb {
+
+// Fortran Ew.d text of a double (the e26.16 / e18.8 fields of valout.f90).
+static std::string fort_e(double v, int w, int d) {
+  std::string out;
+  if (v == 0.0) {
+    out = std::string(std::signbit(v) ? "-" : "") + "0." + std::string(d, '0') + "E+00";
+  } else {
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), "%.*e", d - 1, std::fabs(v));
+    const std::string s(buf);
+    const size_t e = s.find('e');
+    std::string digits;
+    for (size_t k = 0; k < e; ++k) if (s[k] != '.') digits.push_back(s[k]);
+    const int ex = std::atoi(s.c_str() + e + 1) + 1;
+    char eb[16];
+    if (std::abs(ex) <= 99) std::snprintf(eb, sizeof(eb), "E%c%02d", ex < 0 ? '-' : '+', std::abs(ex));
+    else std::snprintf(eb, sizeof(eb), "%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
+    out = std::string(std::signbit(v) ? "-" : "") + "0." + digits + eb;
+  }
+  if ((int)out.size() < w) out = std::string(w - out.size(), ' ') + out;
+  return out;
+}
+
+void Amr2Gpu::output(double t) {
+  for (int lev = 1; lev <= lfine; ++lev) {
+    launch_zero_tiny(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st);
+    ++nkernels;
+  }
+  if (write_output) {
+    const std::vector<double> v = gather_values();
+    char fn[64];
+    std::snprintf(fn, sizeof(fn), "/fort.q%04d", frame);
+    FILE* f = std::fopen((outdir + fn).c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+    size_t pos = 0;
+    int ngrids = 0;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) {
+        const HPatch& g = node[m];
+        ++ngrids;
+        std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n",
+                     m, lev, g.nx(), g.ny());
+        std::fprintf(f, "%s    xlow\n%s    ylow\n%s    dx\n%s    dy\n\n", fort_e(g.xlo, 26, 16).c_str(), fort_e(g.ylo, 26, 16).c_str(),
+                     fort_e(hxposs[lev], 26, 16).c_str(), fort_e(hyposs[lev], 26, 16).c_str());
+        const size_t cells = (size_t)g.nx() * g.ny();
+        for (int j = 0; j < g.ny(); ++j) {
+          for (int i = 0; i < g.nx(); ++i) {
+            for (int mm = 0; mm < nvar; ++mm) std::fputs(fort_e(v[pos + mm * cells + (size_t)j * g.nx() + i], 26, 16).c_str(), f);
+            std::fputc('\n', f);
+          }
+          std::fputs("  \n", f);
+        }
+        pos += cells * nvar;
+      }
+    std::fclose(f);
+    std::snprintf(fn, sizeof(fn), "/fort.t%04d", frame);
+    f = std::fopen((outdir + fn).c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+    std::fprintf(f, "%s    time\n%6d                 meqn\n%6d                 ngrids\n%6d                 naux\n%6d                 ndim\n%6d                 nghost\n\n",
+                 fort_e(t, 18, 8).c_str(), nvar, ngrids, 0, 2, ng);
+    std::fclose(f);
+  }
+  ++frame;
+}
+
+}  // namespace amrb
+
+// ============================================================================ C ABI
+#include "../../include/amrclaw_b200.h"
+
+struct amrgpu_ctx {
+  std::unique_ptr<amrb::Amr2Gpu> s2;
+};
+
+static thread_local std::string g_err;
+
+template <class F>
+static int guarded(F&& f) {
+  try {
+    f();
+    return AMRGPU_OK;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return AMRGPU_ERROR;
+  }
+}
+
+extern "C" {
+
+const char* amrgpu_last_error(void) { return g_err.c_str(); }
+
+int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu_ctx** out) {
+  if (!rundir || !out) { g_err = "amrgpu_init: null argument"; return AMRGPU_EINVAL; }
+  *out = nullptr;
+  return guarded([&] {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw std::runtime_error("no CUDA device is visible");
+    amrb::KeyFile c;
+    if (!c.read(std::string(rundir) + "/claw.data")) throw std::runtime_error(std::string("cannot read ") + rundir + "/claw.data");
+    const int nd = c.n("num_dim");
+    if (nd != 2) throw std::runtime_error("num_dim must be 2 for this build");
+    auto* ctx = new amrgpu_ctx();
+    ctx->s2.reset(new amrb::Amr2Gpu());
+    ctx->s2->outdir = outdir ? outdir : "";
+    ctx->s2->write_output = write_output != 0;
+    try {
+      ctx->s2->init(rundir);
+    } catch (...) {
+      delete ctx;
+      throw;
+    }
+    *out = ctx;
+  });
+}
+
+int amrgpu_set_batched(amrgpu_ctx* ctx, int batched) {
+  if (!ctx) return AMRGPU_EINVAL;
+  ctx->s2->batched = batched != 0;
+  return AMRGPU_OK;
+}
+
+int amrgpu_run(amrgpu_ctx* ctx, int max_cycles) {
+  if (!ctx) return AMRGPU_EINVAL;
+  return guarded([&] {
+    ctx->s2->max_cycles = max_cycles;
+    ctx->s2->tick();
+  });
+}
+
+int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out) {
+  if (!ctx) return AMRGPU_EINVAL;
+  return guarded([&] {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    if (level < 1 || level > s.lfine) throw std::runtime_error("level out of range");
+    const double d = s.advanc(level);
+    if (dtnew_out) *dtnew_out = d;
+    if (cfl_out) *cfl_out = s.cfl_level;
+  });
+}
+
+int amrgpu_update(amrgpu_ctx* ctx, int level) {
+  if (!ctx) return AMRGPU_EINVAL;
+  return guarded([&] {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    if (level < 1 || level >= s.lfine) throw std::runtime_error("level out of range");
+    s.update(level);
+    AMR_CUDA(cudaStreamSynchronize(s.st));
+  });
+}
+
+int amrgpu_regrid(amrgpu_ctx* ctx, int lbase) {
+  if (!ctx) return AMRGPU_EINVAL;
+  return guarded([&] {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    if (lbase < 1 || lbase > s.lfine || lbase >= s.p.mxnest) throw std::runtime_error("lbase out of range");
+    s.regrid(lbase);
+    s.setbestsrc();
+  });
+}
+
+int amrgpu_valout(amrgpu_ctx* ctx, const char* dir) {
+  if (!ctx) return AMRGPU_EINVAL;
+  return guarded([&] {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    const std::string keep = s.outdir;
+    const bool kw = s.write_output;
+    if (dir) { s.outdir = dir; s.write_output = true; }
+    s.output(s.time);
+    s.outdir = keep; s.write_output = kw;
+  });
+}
+
+int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out) {
+  if (!ctx || !mass_out) return AMRGPU_EINVAL;
+  return guarded([&] { *mass_out = ctx->s2->mass(); });
+}
+
+int amrgpu_info(amrgpu_ctx* ctx, double* out, int n) {
+  if (!ctx || !out) return AMRGPU_EINVAL;
+  return guarded([&] {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    const double v[] = {s.time, s.rvol, (double)s.ncycle, (double)s.lfine, s.t_step, s.t_regrid, s.tmass0,
+                        s.cflmax_run, (double)s.nkernels, (double)s.pool.peak * 8.0, (double)s.nsteps_launched};
+    for (int k = 0; k < n && k < (int)(sizeof(v) / sizeof(v[0])); ++k) out[k] = v[k];
+  });
+}
+
+int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out) {
+  if (!ctx || !n_out) return AMRGPU_EINVAL;
+  return guarded([&] {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    int n = 0;
+    for (int lev = 1; lev <= s.lfine; ++lev)
+      for (int m : s.lgrids[lev]) {
+        if (out && n < cap) {
+          const amrb::HPatch& g = s.node[m];
+          int* r = out + 6 * n;
+          r[0] = m; r[1] = lev; r[2] = g.ilo; r[3] = g.ihi; r[4] = g.jlo; r[5] = g.jhi;
+        }
+        ++n;
+      }
+    *n_out = n;
+  });
+}
+
+int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out) {
+  if (!ctx || !n_out) return AMRGPU_EINVAL;
+  return guarded([&] {
+    const std::vector<double> v = ctx->s2->gather_values();
+    if (out) std::memcpy(out, v.data(), sizeof(double) * std::min<long long>(cap, (long long)v.size()));
+    *n_out = (long long)v.size();
+  });
+}
+
+int amrgpu_gauges(amrgpu_ctx* ctx, double* out, int cap_rows, int* n_out) {
+  if (!ctx || !n_out) return AMRGPU_EINVAL;
+  return guarded([&] {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    const int nv = s.nvar;
+    std::vector<double> vals((size_t)s.gslots * nv);
+    if (s.gslots) AMR_CUDA(cudaMemcpy(vals.data(), s.d_gauge_out.d, sizeof(double) * vals.size(), cudaMemcpyDeviceToHost));
+    // rows grouped by gauge, in recording order (as each gauge's file would list them)
+    int n = 0;
+    for (const auto& G : s.p.gauges)
+      for (const auto& r : s.grows) {
+        if (r.gauge != G.num) continue;
+        if (out && n < cap_rows) {
+          double* row = out + (size_t)(3 + nv) * n;
+          row[0] = r.gauge; row[1] = r.level; row[2] = r.t;
+          for (int k = 0; k < nv; ++k) row[3 + k] = vals[(size_t)r.slot * nv + k];
+        }
+        ++n;
+      }
+    *n_out = n;
+  });
+}
+
+int amrgpu_destroy(amrgpu_ctx* ctx) {
+  delete ctx;
+  return AMRGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,807 @@
+// 2D kernels of the patch-advance path (sm_100a, FP64, built without FMA contraction).
+//
+//   step2_kernel   fused patch step: Riemann solves, wave limiter, second-order and
+//                  transverse corrections, flux differencing, CFL reduction, and the
+//                  flux-register epilogue (fluxsv on coarse faces, fluxad on fine
+//                  boundary faces). Replaces stepgrid/step2/flux2/limiter/fluxsv/fluxad
+//                  (src/2d/stepgrid.f:24-232, step2.f90:7-169, flux2.f:25-237,
+//                  inlinelimiter.f:4-108, fluxsv.f:10-109, fluxad.f:7-96).
+//   fill_kernel    ghost-fill op executor: same-level copies with time interpolation,
+//                  limited coarse interpolation, periodic pieces, new-grid filval
+//                  interpolation and the cstore ring (intfil.f90, filpatch.f90:246-327,
+//                  prefilp.f90, filval.f90:150-185, cstore.f).
+//   bc kernels     bc2amr.f90 extrapolation / wall in two phases (x then y).
+//   qad2_kernel    coarse/fine interface Riemann problems (qad.f:9-360).
+//   upbnd/average  level sync (upbnd.f:18-127, update.f:95-175).
+#include "kernels2d.cuh"
+#include <algorithm>
+
+namespace amrb {
+
+__device__ __forceinline__ int floordiv(int a, int b) { int q = a / b; if ((a % b != 0) && ((a < 0) != (b < 0))) --q; return q; }
+
+// ======================================================================= patch step
+template <class S>
+struct Step2Layout {
+  static constexpr int ME = S::MEQN, MW = S::MWAVES;
+  static constexpr int T = TILE2;
+  static constexpr int QW = T + 4;
+  static constexpr int NQ = ME * QW * QW;
+  static constexpr int NF = ME * (T + 1) * T;
+  static constexpr int NTR = (T + 2) * T * 2 * ME;
+  static constexpr int WREC = MW * ME + MW + 2 * ME;
+  static constexpr int NW = STEP2_RC * (T + 3) * WREC;
+  static constexpr int XREC = 4 * ME;
+  static constexpr int NX = STEP2_RC * (T + 1) * XREC;
+  static constexpr int TOTAL = NQ + 4 * NF + NTR + NW + NX + 32;
+};
+
+// One sweep direction of flux2.f over the tile. IXY = 1: lines are rows, IXY = 2: columns.
+template <class S, int IXY>
+__device__ void step2_sweep(const StepParams& sp, const double* Qs, double* W, double* X, double* TR, double* F1,
+                            double* F2, int i0, int j0, int tw, int th, double dtdx, double& cfl) {
+  using L = Step2Layout<S>;
+  constexpr int ME = L::ME, MW = L::MW, T = L::T, QW = L::QW;
+  const int tid = threadIdx.x;
+  // along-line extents
+  const int na = (IXY == 1) ? tw : th;       // cells along the line inside the tile
+  const int nl = (IXY == 1) ? th + 2 : tw + 2;  // lines: tile +-1
+  const int a0 = (IXY == 1) ? i0 : j0;        // first tile cell along the line
+  const int l0 = (IXY == 1) ? j0 - 1 : i0 - 1;  // first line
+  const int nfr = na + 3;                     // faces for the normal solve: a0-1 .. a0+na+1
+  const int nfl = na + 1;                     // limited faces: a0 .. a0+na
+  auto qptr = [&](int m, int line, int pos) -> const double* {
+    // returns &Q(m, ...) ; Q layout [m][b][a] with a = i-(i0-2), b = j-(j0-2)
+    if (IXY == 1) return &Qs[(m * QW + (line - (j0 - 2))) * QW + (pos - (i0 - 2))];
+    return &Qs[(m * QW + (pos - (j0 - 2))) * QW + (line - (i0 - 2))];
+  };
+  auto loadq = [&](double* q, int line, int pos) {
+#pragma unroll
+    for (int m = 0; m < ME; ++m) q[m] = *qptr(m, line, pos);
+  };
+  for (int lc0 = 0; lc0 < nl; lc0 += STEP2_RC) {
+    const int nlc = min(STEP2_RC, nl - lc0);
+    // phase 1: normal Riemann problems
+    for (int it = tid; it < nlc * nfr; it += STEP2_THREADS) {
+      const int rr = it / nfr, ff = it % nfr;
+      const int line = l0 + lc0 + rr, f = a0 - 1 + ff;
+      double qL[ME], qR[ME];
+      loadq(qL, line, f - 1);
+      loadq(qR, line, f);
+      double wave[MW][ME], s[MW], amdq[ME], apdq[ME];
+      S::template rpn<double>(sp.prob, IXY, qL, qR, wave, s, amdq, apdq);
+      double* rec = W + (rr * (T + 3) + ff) * L::WREC;
+#pragma unroll
+      for (int mw = 0; mw < MW; ++mw) {
+#pragma unroll
+        for (int m = 0; m < ME; ++m) rec[mw * ME + m] = wave[mw][m];
+        rec[MW * ME + mw] = s[mw];
+      }
+#pragma unroll
+      for (int m = 0; m < ME; ++m) { rec[MW * ME + MW + m] = amdq[m]; rec[MW * ME + MW + ME + m] = apdq[m]; }
+      if (ff >= 1 && ff <= nfl) {
+#pragma unroll
+        for (int mw = 0; mw < MW; ++mw) cfl = dmax(cfl, dmax(dtdx * s[mw], -dtdx * s[mw]));
+      }
+    }
+    __syncthreads();
+    // phase 2: limiter, second-order correction, transverse splitting
+    for (int it = tid; it < nlc * nfl; it += STEP2_THREADS) {
+      const int rr = it / nfl, fa = it % nfl;
+      const int line = l0 + lc0 + rr, f = a0 + fa;
+      const double* rm = W + (rr * (T + 3) + fa) * L::WREC;       // face f-1
+      const double* rc = rm + L::WREC;                             // face f
+      const double* rp = rc + L::WREC;                             // face f+1
+      double amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
+#pragma unroll
+      for (int m = 0; m < ME; ++m) { amdq[m] = rc[MW * ME + MW + m]; apdq[m] = rc[MW * ME + MW + ME + m]; }
+#pragma unroll
+      for (int m = 0; m < ME; ++m) { fm[m] = 0.0 + amdq[m]; fp[m] = 0.0 - apdq[m]; }
+      if (sp.order != 1) {
+        double wl[MW][ME];
+#pragma unroll
+        for (int mw = 0; mw < MW; ++mw) {
+          const double smw = rc[MW * ME + mw];
+#pragma unroll
+          for (int m = 0; m < ME; ++m) wl[mw][m] = rc[mw * ME + m];
+          if (sp.mthlim[mw] == 0) continue;
+          double wn2 = 0.0, dotl = 0.0, dotr = 0.0;
+#pragma unroll
+          for (int m = 0; m < ME; ++m) {
+            wn2 = wn2 + rc[mw * ME + m] * rc[mw * ME + m];
+            dotl = dotl + rm[mw * ME + m] * rc[mw * ME + m];
+            dotr = dotr + rc[mw * ME + m] * rp[mw * ME + m];
+          }
+          if (wn2 == 0.0) continue;
+          const double r = (smw > 0.0) ? dotl / wn2 : dotr / wn2;
+          double wlim = 0.0;
+          switch (sp.mthlim[mw]) {
+            case 1: wlim = dmax(0.0, dmin(1.0, r)); break;
+            case 2: wlim = dmax(0.0, dmax(dmin(1.0, 2.0 * r), dmin(2.0, r))); break;
+            case 3: wlim = (r + fabs(r)) / (1.0 + fabs(r)); break;
+            case 4: { const double c = (1.0 + r) / 2.0; wlim = dmax(0.0, dmin(c, dmin(2.0, 2.0 * r))); } break;
+            case 5: wlim = r; break;
+          }
+#pragma unroll
+          for (int m = 0; m < ME; ++m) wl[mw][m] = wlim * wl[mw][m];
+        }
+        const double dtdxave = 0.5 * (dtdx + dtdx);
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+          double c = 0.0;
+#pragma unroll
+          for (int mw = 0; mw < MW; ++mw) {
+            const double smw = rc[MW * ME + mw];
+            const double abs_sign = sp.use_fwaves ? dsign(1.0, smw) : fabs(smw);
+            c = c + abs_sign * (1.0 - fabs(smw) * dtdxave) * wl[mw][m];
+          }
+          cqxx[m] = c;
+          fm[m] = fm[m] + 0.5 * c;
+          fp[m] = fp[m] + 0.5 * c;
+        }
+      }
+      // flux increments into the tile's face arrays (interior lines only)
+      const int lin = (IXY == 1) ? line - j0 : line - i0;
+      if (lin >= 0 && lin < ((IXY == 1) ? th : tw)) {
+        if (IXY == 1) {
+#pragma unroll
+          for (int m = 0; m < ME; ++m) {
+            F1[(m * T + lin) * (T + 1) + fa] = fm[m];   // FM init
+            F2[(m * T + lin) * (T + 1) + fa] = fp[m];   // FP init
+          }
+        } else {
+#pragma unroll
+          for (int m = 0; m < ME; ++m) {
+            F1[(m * (T + 1) + fa) * T + lin] = F1[(m * (T + 1) + fa) * T + lin] + fm[m];  // GM += faddm
+            F2[(m * (T + 1) + fa) * T + lin] = F2[(m * (T + 1) + fa) * T + lin] + fp[m];  // GP += faddp
+          }
+        }
+      }
+      double* xr = X + (rr * (T + 1) + fa) * L::XREC;
+      if (sp.trans != 0) {
+        double am2[ME], ap2[ME];
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+          am2[m] = amdq[m]; ap2[m] = apdq[m];
+          if (sp.order > 1 && sp.trans == 2) { am2[m] = amdq[m] + cqxx[m]; ap2[m] = apdq[m] - cqxx[m]; }
+        }
+        double qL[ME], qR[ME];
+        loadq(qL, line, f - 1);
+        loadq(qR, line, f);
+        double bm1[ME], bp1[ME], bm2[ME], bp2[ME];
+        S::template rpt<double>(sp.prob, IXY, 1, qL, qR, am2, bm1, bp1);
+        S::template rpt<double>(sp.prob, IXY, 2, qL, qR, ap2, bm2, bp2);
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+          xr[0 * ME + m] = 0.5 * dtdx * bm1[m];
+          xr[1 * ME + m] = 0.5 * dtdx * bp1[m];
+          xr[2 * ME + m] = 0.5 * dtdx * bm2[m];
+          xr[3 * ME + m] = 0.5 * dtdx * bp2[m];
+        }
+      }
+    }
+    __syncthreads();
+    // phase 3: per-cell transverse parts (gadd(:,i,1) and gadd(:,i,2) of flux2.f)
+    if (sp.trans != 0) {
+      for (int it = tid; it < nlc * na; it += STEP2_THREADS) {
+        const int rr = it / na, ca = it % na;
+        const double* xa = X + (rr * (T + 1) + ca + 1) * L::XREC;  // face c+1 (amdq part)
+        const double* xb = X + (rr * (T + 1) + ca) * L::XREC;      // face c   (apdq part)
+        double* tr = TR + (((lc0 + rr) * T + ca) * 2) * ME;
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+          tr[m] = (0.0 - xa[0 * ME + m]) - xb[2 * ME + m];
+          tr[ME + m] = (0.0 - xa[1 * ME + m]) - xb[3 * ME + m];
+        }
+      }
+    } else {
+      for (int it = tid; it < nlc * na; it += STEP2_THREADS) {
+        const int rr = it / na, ca = it % na;
+        double* tr = TR + (((lc0 + rr) * T + ca) * 2) * ME;
+#pragma unroll
+        for (int m = 0; m < ME; ++m) { tr[m] = 0.0; tr[ME + m] = 0.0; }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <class S>
+__global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
+  using L = Step2Layout<S>;
+  constexpr int ME = L::ME, T = L::T, QW = L::QW;
+  extern __shared__ double smem[];
+  double* Qs = smem;
+  double* FM = Qs + L::NQ;
+  double* FP = FM + L::NF;
+  double* GM = FP + L::NF;
+  double* GP = GM + L::NF;
+  double* TR = GP + L::NF;
+  double* W = TR + L::NTR;
+  double* X = W + L::NW;
+  double* red = X + L::NX;
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  const double dtdx = a.dt / a.dx, dtdy = a.dt / a.dy;
+  double cfl = 0.0;
+  int iter = 0;
+  while (true) {
+    int w;
+    if (a.queue) {
+      if (tid == 0) s_item = atomicAdd(a.queue, 1);
+      __syncthreads();
+      w = s_item;
+      __syncthreads();
+    } else {
+      w = blockIdx.x + iter * gridDim.x;
+    }
+    ++iter;
+    if (w >= a.nwork) break;
+    const StepWork wk = a.work[w];
+    const PatchDev P = a.patches[wk.patch];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+    const int mitot = P.mitot, mjtot = P.mjtot;
+    const int i0 = wk.ti0, j0 = wk.tj0;
+    const int tw = min(T, mx - i0 + 1), th = min(T, my - j0 + 1);
+    const double* qin = a.pool + P.q[P.cur];
+    double* qout = a.pool + P.q[1 - P.cur];
+    const long long plane = (long long)mitot * mjtot;
+    // load the tile with its two ghost layers: interior (i,j) -> enlarged 0-based (i+1, j+1)
+    const int lw = tw + 4, lh = th + 4;
+    for (int it = tid; it < ME * lw * lh; it += STEP2_THREADS) {
+      const int m = it / (lw * lh), rem = it % (lw * lh);
+      const int b = rem / lw, aa = rem % lw;
+      const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
+      Qs[(m * QW + b) * QW + aa] = qin[m * plane + (long long)je * mitot + ie];
+    }
+    __syncthreads();
+    // x-sweeps: FM/FP initialised, per-cell transverse parts in TR
+    step2_sweep<S, 1>(a.sp, Qs, W, X, TR, FM, FP, i0, j0, tw, th, dtdx, cfl);
+    // GX(c, f) = (0 + part2(row f-1)) + part1(row f) -> GM and GP
+    for (int it = tid; it < ME * (th + 1) * tw; it += STEP2_THREADS) {
+      const int m = it / ((th + 1) * tw), rem = it % ((th + 1) * tw);
+      const int fb = rem / tw, ca = rem % tw;
+      const double up = TR[((fb * T + ca) * 2) * ME + ME + m];        // row f-1 = line index fb
+      const double dn = TR[(((fb + 1) * T + ca) * 2) * ME + m];       // row f   = line index fb+1
+      const double g = (0.0 + up) + dn;
+      GM[(m * (T + 1) + fb) * T + ca] = g;
+      GP[(m * (T + 1) + fb) * T + ca] = g;
+    }
+    __syncthreads();
+    // y-sweeps: GM/GP += faddm/faddp, per-cell transverse parts in TR
+    step2_sweep<S, 2>(a.sp, Qs, W, X, TR, GM, GP, i0, j0, tw, th, dtdy, cfl);
+    // FM(f, r) = (FM + part2(col f-1)) + part1(col f)
+    for (int it = tid; it < ME * th * (tw + 1); it += STEP2_THREADS) {
+      const int m = it / (th * (tw + 1)), rem = it % (th * (tw + 1));
+      const int rb = rem / (tw + 1), fa = rem % (tw + 1);
+      const double up = TR[((fa * T + rb) * 2) * ME + ME + m];        // column f-1 = line index fa
+      const double dn = TR[(((fa + 1) * T + rb) * 2) * ME + m];       // column f   = line index fa+1
+      const int k = (m * T + rb) * (T + 1) + fa;
+      FM[k] = (FM[k] + up) + dn;
+      FP[k] = (FP[k] + up) + dn;
+    }
+    __syncthreads();
+    // conservative update (stepgrid.f:154-173, mcapa = 0)
+    for (int it = tid; it < ME * th * tw; it += STEP2_THREADS) {
+      const int m = it / (th * tw), rem = it % (th * tw);
+      const int rb = rem / tw, ca = rem % tw;
+      const double q = Qs[(m * QW + rb + 2) * QW + ca + 2];
+      const double fmr = FM[(m * T + rb) * (T + 1) + ca + 1], fpl = FP[(m * T + rb) * (T + 1) + ca];
+      const double gmt = GM[(m * (T + 1) + rb + 1) * T + ca], gpb = GP[(m * (T + 1) + rb) * T + ca];
+      const double qn = q - dtdx * (fmr - fpl) - dtdy * (gmt - gpb);
+      const int ie = i0 + ca + 1, je = j0 + rb + 1;
+      qout[m * plane + (long long)je * mitot + ie] = qn;
+    }
+    // fluxsv epilogue: coarse fluxes next to finer grids into the kids' registers
+    for (int it = tid; it < wk.fsv_count * ME; it += STEP2_THREADS) {
+      const FsvEntry e = a.fsv[wk.fsv_start + it / ME];
+      const int m = it % ME;
+      const int ca = e.ic - i0, rb = e.jc - j0;
+      double v = 0.0;
+      if (e.side == 1) v = -FP[(m * T + rb) * (T + 1) + ca] * a.dt * a.dy;
+      else if (e.side == 2) v = -GM[(m * (T + 1) + rb + 1) * T + ca] * a.dt * a.dx;
+      else if (e.side == 3) v = -FM[(m * T + rb) * (T + 1) + ca + 1] * a.dt * a.dy;
+      else v = -GP[(m * (T + 1) + rb) * T + ca] * a.dt * a.dx;
+      a.regs[e.dst + m] = v;
+    }
+    // fluxad epilogue: fine boundary fluxes accumulated into this patch's registers
+    for (int it = tid; it < wk.fad_count * ME; it += STEP2_THREADS) {
+      const FadEntry e = a.fad[wk.fad_start + it / ME];
+      const int m = it % ME;
+      const int r = e.pad;
+      double* svd = a.regs + P.ffl + (long long)ME * e.seg + m;
+      double s = *svd;
+      for (int l = 0; l < r; ++l) {
+        const int f = e.f0 + l;
+        if (e.side == 1) s = s + FM[(m * T + (f - j0)) * (T + 1) + 0] * a.dt * a.dy;
+        else if (e.side == 2) s = s + GP[(m * (T + 1) + th) * T + (f - i0)] * a.dt * a.dx;
+        else if (e.side == 3) s = s + FP[(m * T + (f - j0)) * (T + 1) + tw] * a.dt * a.dy;
+        else s = s + GM[(m * (T + 1) + 0) * T + (f - i0)] * a.dt * a.dx;
+      }
+      *svd = s;
+    }
+    __syncthreads();
+  }
+  // block max of the Courant number -> level maximum
+  for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+  if ((tid & 31) == 0) red[tid >> 5] = cfl;
+  __syncthreads();
+  if (tid == 0) {
+    double c = 0.0;
+    for (int k = 0; k < STEP2_THREADS / 32; ++k) c = dmax(c, red[k]);
+    atomicMax(a.cflmax, (unsigned long long)__double_as_longlong(c));
+  }
+}
+
+template <class S>
+static void launch_step2_t(const StepArgs& a, int grid, cudaStream_t s) {
+  const size_t sm = sizeof(double) * Step2Layout<S>::TOTAL;
+  static bool attr = false;
+  if (!attr) {
+    AMR_CUDA(cudaFuncSetAttribute(step2_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr = true;
+  }
+  if (grid <= 0) return;
+  step2_kernel<S><<<grid, STEP2_THREADS, sm, s>>>(a);
+  AMR_CUDA(cudaGetLastError());
+}
+
+void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s) {
+  switch (solver) {
+    case SOLVER_ADVECTION: launch_step2_t<Advection2>(a, grid, s); break;
+    case SOLVER_ACOUSTICS: launch_step2_t<Acoustics2>(a, grid, s); break;
+    case SOLVER_EULER: launch_step2_t<Euler2>(a, grid, s); break;
+    default: throw std::runtime_error("launch_step2: unsupported solver");
+  }
+}
+
+size_t step2_smem_bytes(int solver) {
+  switch (solver) {
+    case SOLVER_ADVECTION: return sizeof(double) * Step2Layout<Advection2>::TOTAL;
+    case SOLVER_ACOUSTICS: return sizeof(double) * Step2Layout<Acoustics2>::TOTAL;
+    case SOLVER_EULER: return sizeof(double) * Step2Layout<Euler2>::TOTAL;
+  }
+  return 0;
+}
+
+// ======================================================================= ghost fill
+__device__ __forceinline__ double* fill_dst(const FillArgs& a, const FillOp& o, int& ldi, long long& plane) {
+  if (o.dst_patch >= 0) {
+    const PatchDev& P = a.patches[o.dst_patch];
+    ldi = P.mitot; plane = (long long)P.mitot * P.mjtot;
+    return a.pool + P.q[P.cur];
+  }
+  const ScratchRect& R = a.rects[o.dst_rect];
+  ldi = R.ni; plane = (long long)R.ni * R.nj;
+  return a.pool + R.off;
+}
+
+__global__ void fill_kernel(FillArgs a) {
+  const int c = blockIdx.x;
+  if (c >= a.nchunks) return;
+  const FillChunk ch = a.chunks[c];
+  if ((int)threadIdx.x >= ch.count) return;
+  const FillOp o = a.ops[ch.op];
+  const int cell = ch.start + threadIdx.x;
+  const int ia = cell % o.ni, jb = cell / o.ni;
+  const int nvar = a.nvar;
+  if (o.kind == FILL_RING) {
+    // cstore.f:4-63: ring of coarse values around a fine grid into qc1d of the kid
+    const ScratchRect& R = a.rects[o.src];
+    const int nrow = R.ni, ncol = R.nj;
+    int k = cell, ii, jj;  // 0-based position in the rect
+    if (k < ncol - 2) { ii = 0; jj = 1 + k; }
+    else if ((k -= ncol - 2) < nrow - 2) { ii = 1 + k; jj = ncol - 1; }
+    else if ((k -= nrow - 2) < ncol - 2) { ii = nrow - 1; jj = 1 + k; }
+    else { k -= ncol - 2; ii = 1 + k; jj = 0; }
+    const PatchDev& K = a.patches[o.dst_patch];
+    double* qc1d = a.regs + K.ffl + (long long)nvar * K.lenbc + (long long)nvar * cell;
+    const double* src = a.pool + R.off;
+    const long long pl = (long long)nrow * ncol;
+    for (int m = 0; m < nvar; ++m) qc1d[m] = src[m * pl + (long long)jj * nrow + ii];
+    return;
+  }
+  int ldi; long long plane;
+  double* dst = fill_dst(a, o, ldi, plane);
+  const long long dk = (long long)(o.dj0 + jb) * ldi + (o.di0 + ia);
+  if (o.kind == FILL_COPY) {
+    const PatchDev& S = a.patches[o.src];
+    const long long sp = (long long)S.mitot * S.mjtot;
+    const long long sk = (long long)(o.sj0 + jb) * S.mitot + (o.si0 + ia);
+    int mode = 0; double ai = 1.0, ac = 0.0;
+    if (o.level >= 0) { mode = a.modes.mode[o.level]; ai = a.modes.alphai[o.level]; ac = a.modes.alphac[o.level]; }
+    const double* qn = a.pool + S.q[S.cur];
+    const double* qo = a.pool + S.q[1 - S.cur];
+    for (int m = 0; m < nvar; ++m) {
+      double v;
+      if (mode == 0) v = qn[m * sp + sk];
+      else if (mode == 1) v = qo[m * sp + sk];
+      else v = qn[m * sp + sk] * ai + qo[m * sp + sk] * ac;
+      dst[m * plane + dk] = v;
+    }
+    return;
+  }
+  if (o.kind == FILL_PIECE) {
+    const ScratchRect& R = a.rects[o.src];
+    const long long sp = (long long)R.ni * R.nj;
+    const long long sk = (long long)(o.sj0 + jb) * R.ni + (o.si0 + ia);
+    const double* src = a.pool + R.off;
+    for (int m = 0; m < nvar; ++m) dst[m * plane + dk] = src[m * sp + sk];
+    return;
+  }
+  const ScratchRect& R = a.rects[o.src];
+  const double* vc = a.pool + R.off;
+  const long long cp = (long long)R.ni * R.nj;
+  const int lev = o.level;
+  const int rx = a.lc.intratx[lev - 1], ry = a.lc.intraty[lev - 1];
+  const int ifg = o.si0 + ia, jfg = o.sj0 + jb;
+  if (o.kind == FILL_INTERP) {
+    // filpatch.f90:259-327 limited interpolation from the coarse scratch rect
+    const double dxf = a.lc.hx[lev], dyf = a.lc.hy[lev], dxc = a.lc.hx[lev - 1], dyc = a.lc.hy[lev - 1];
+    const int icg = floordiv(ifg, rx), jcg = floordiv(jfg, ry);
+    const int ic = icg - o.cilo + 1, jc = jcg - o.cjlo + 1;  // 1-based in the coarse rect
+    const double xlow_c = a.xlower + o.cilo * dxc, ylow_c = a.ylower + o.cjlo * dyc;
+    const double ycc = ylow_c + (jc - 0.5) * dyc;
+    const double ycf = a.ylower + (jfg + 0.5) * dyf;
+    const double eta2 = (ycf - ycc) / dyc;
+    const double xcc = xlow_c + (ic - 0.5) * dxc;
+    const double xcf = a.xlower + (ifg + 0.5) * dxf;
+    const double eta1 = (xcf - xcc) / dxc;
+    auto CI = [&](int m, int i, int j) { return vc[m * cp + (long long)(j - 1) * R.ni + (i - 1)]; };
+    for (int m = 0; m < nvar; ++m) {
+      const double valp10 = CI(m, ic + 1, jc), valm10 = CI(m, ic - 1, jc), valc = CI(m, ic, jc);
+      const double valp01 = CI(m, ic, jc + 1), valm01 = CI(m, ic, jc - 1);
+      const double dupc = valp10 - valc, dumc = valc - valm10, ducc = valp10 - valm10;
+      double du = dmin(fabs(dupc), fabs(dumc));
+      du = dmin(2.0 * du, 0.5 * fabs(ducc));
+      const double fu = dmax(0.0, dsign(1.0, dupc * dumc));
+      const double uslope = du * dsign(1.0, ducc) * fu;
+      const double dvpc = valp01 - valc, dvmc = valc - valm01, dvcc = valp01 - valm01;
+      double dv = dmin(fabs(dvpc), fabs(dvmc));
+      dv = dmin(2.0 * dv, 0.5 * fabs(dvcc));
+      const double fv = dmax(0.0, dsign(1.0, dvpc * dvmc));
+      const double vslope = dv * dsign(1.0, dvcc) * fv;
+      dst[m * plane + dk] = valc + eta1 * uslope + eta2 * vslope;
+    }
+    return;
+  }
+  if (o.kind == FILL_FILVAL) {
+    // filval.f90:150-185 minmod-limited interpolation into an uncovered new-grid cell
+    const int icg = floordiv(ifg, rx), jcg = floordiv(jfg, ry);
+    const int ico = ifg - icg * rx + 1, jco = jfg - jcg * ry + 1;
+    const int i = icg - o.cilo + 1, j = jcg - o.cjlo + 1;  // 1-based in valc
+    auto VC = [&](int m, int ii, int jj) { return vc[m * cp + (long long)(jj - 1) * R.ni + (ii - 1)]; };
+    const double yoff = ((double)jco - 0.5) / ry - 0.5;
+    const double xoff = ((double)ico - 0.5) / rx - 0.5;
+    for (int m = 0; m < nvar; ++m) {
+      double s1p = VC(m, i + 1, j) - VC(m, i, j), s1m = VC(m, i, j) - VC(m, i - 1, j);
+      double slopex = dmin(fabs(s1p), fabs(s1m)) * dsign(1.0, VC(m, i + 1, j) - VC(m, i - 1, j));
+      if (s1m * s1p <= 0.0) slopex = 0.0;
+      s1p = VC(m, i, j + 1) - VC(m, i, j); s1m = VC(m, i, j) - VC(m, i, j - 1);
+      double slopey = dmin(fabs(s1p), fabs(s1m)) * dsign(1.0, VC(m, i, j + 1) - VC(m, i, j - 1));
+      if (s1m * s1p <= 0.0) slopey = 0.0;
+      dst[m * plane + dk] = VC(m, i, j) + xoff * slopex + yoff * slopey;
+    }
+    return;
+  }
+}
+
+void launch_fill(const FillArgs& a, cudaStream_t s) {
+  if (a.nchunks <= 0) return;
+  fill_kernel<<<a.nchunks, 128, 0, s>>>(a);
+  AMR_CUDA(cudaGetLastError());
+}
+
+// phase 0: x-sides over all rows; phase 1: y-sides over all columns (after phase 0)
+__global__ void bc_kernel(BcArgs a, int phase) {
+  const int op = blockIdx.y;
+  if (op >= a.nops) return;
+  const BcOp o = a.ops[op];
+  double* v; int nrow = o.nrow, ncol = o.ncol;
+  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = a.pool + P.q[P.cur]; }
+  else v = a.pool + a.rects[o.dst_rect].off;
+  const long long plane = (long long)nrow * ncol;
+  auto V = [&](int m, int i, int j) -> double& { return v[m * plane + (long long)(j - 1) * nrow + (i - 1)]; };
+  const int nvar = a.nvar;
+  if (phase == 0) {
+    const int nl = (o.nxl > 0 && (o.bxl == 1 || o.bxl == 3)) ? o.nxl : 0;
+    const int nr = (o.ibeg > 0 && (o.bxr == 1 || o.bxr == 3)) ? nrow - o.ibeg + 1 : 0;
+    const int tot = (nl + nr) * ncol;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+      const int j = t / (nl + nr) + 1, k = t % (nl + nr);
+      if (k < nl) {
+        const int i = k + 1;
+        const int src = (o.bxl == 1) ? o.nxl + 1 : 2 * o.nxl + 1 - i;
+        for (int m = 0; m < nvar; ++m) V(m, i, j) = V(m, src, j);
+        if (o.bxl == 3) V(1, i, j) = -V(1, i, j);
+      } else {
+        const int i = o.ibeg + (k - nl);
+        const int src = (o.bxr == 1) ? o.ibeg - 1 : 2 * o.ibeg - 1 - i;
+        for (int m = 0; m < nvar; ++m) V(m, i, j) = V(m, src, j);
+        if (o.bxr == 3) V(1, i, j) = -V(1, i, j);
+      }
+    }
+  } else {
+    const int nb = (o.nyb > 0 && (o.byl == 1 || o.byl == 3)) ? o.nyb : 0;
+    const int nt = (o.jbeg > 0 && (o.byr == 1 || o.byr == 3)) ? ncol - o.jbeg + 1 : 0;
+    const int tot = (nb + nt) * nrow;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+      const int i = t % nrow + 1, k = t / nrow;
+      if (k < nb) {
+        const int j = k + 1;
+        const int src = (o.byl == 1) ? o.nyb + 1 : 2 * o.nyb + 1 - j;
+        for (int m = 0; m < nvar; ++m) V(m, i, j) = V(m, i, src);
+        if (o.byl == 3) V(2, i, j) = -V(2, i, j);
+      } else {
+        const int j = o.jbeg + (k - nb);
+        const int src = (o.byr == 1) ? o.jbeg - 1 : 2 * o.jbeg - 1 - j;
+        for (int m = 0; m < nvar; ++m) V(m, i, j) = V(m, i, src);
+        if (o.byr == 3) V(2, i, j) = -V(2, i, j);
+      }
+    }
+  }
+}
+
+void launch_bc(const BcArgs& a, int phase, cudaStream_t s) {
+  if (a.nops <= 0) return;
+  for (int base = 0; base < a.nops; base += 65535) {
+    BcArgs b = a;
+    b.ops = a.ops + base;
+    b.nops = std::min(65535, a.nops - base);
+    dim3 grid(2, b.nops);
+    bc_kernel<<<grid, 128, 0, s>>>(b, phase);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
+// ======================================================================= qad
+template <class S>
+__global__ void qad2_kernel(double* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
+                            ProbDev prob, LevelConst lc, double delt) {
+  constexpr int ME = S::MEQN, MW = S::MWAVES;
+  const int jb = blockIdx.x;
+  if (jb >= njobs) return;
+  const QadJob J = jobs[jb];
+  const PatchDev P = patches[J.patch];
+  const int lev = P.level;
+  const int rx = lc.intratx[lev - 1], ry = lc.intraty[lev - 1];
+  const double hx = lc.hx[lev], hy = lc.hy[lev];
+  const double* q = pool + P.q[P.cur];
+  const long long plane = (long long)P.mitot * P.mjtot;
+  for (int sgi = threadIdx.x; sgi < J.nseg; sgi += blockDim.x) {
+    const int seg = J.seg0 + sgi;
+    double* svd = regs + P.ffl + (long long)ME * seg;
+    const double* qc = regs + P.ffl + (long long)ME * P.lenbc + (long long)ME * seg;
+    double sv[ME];
+#pragma unroll
+    for (int m = 0; m < ME; ++m) sv[m] = svd[m];
+    const int r = (J.side == 1 || J.side == 3) ? ry : rx;
+    for (int l = 1; l <= r; ++l) {
+      const int f = sgi * r + l;  // fine row (sides 1,3) or column (sides 2,4), 1-based interior
+      double qf[ME], qcr[ME];
+      long long k;
+      if (J.side == 1) k = (long long)(f + 1) * P.mitot + 1;
+      else if (J.side == 2) k = (long long)(P.mjtot - 2) * P.mitot + (f + 1);
+      else if (J.side == 3) k = (long long)(f + 1) * P.mitot + (P.mitot - 2);
+      else k = (long long)1 * P.mitot + (f + 1);
+#pragma unroll
+      for (int m = 0; m < ME; ++m) { qf[m] = q[m * plane + k]; qcr[m] = qc[m]; }
+      double wave[MW][ME], s[MW], amdq[ME], apdq[ME];
+      if (J.side == 1) S::template rpn<double>(prob, 1, qcr, qf, wave, s, amdq, apdq);
+      else if (J.side == 2) S::template rpn<double>(prob, 2, qf, qcr, wave, s, amdq, apdq);
+      else if (J.side == 3) S::template rpn<double>(prob, 1, qf, qcr, wave, s, amdq, apdq);
+      else S::template rpn<double>(prob, 2, qcr, qf, wave, s, amdq, apdq);
+#pragma unroll
+      for (int m = 0; m < ME; ++m) {
+        if (J.side == 1) sv[m] = sv[m] + amdq[m] * hy * delt + apdq[m] * hy * delt;
+        else if (J.side == 2) sv[m] = sv[m] - amdq[m] * hx * delt - apdq[m] * hx * delt;
+        else if (J.side == 3) sv[m] = sv[m] - amdq[m] * hy * delt - apdq[m] * hy * delt;
+        else sv[m] = sv[m] + amdq[m] * hx * delt + apdq[m] * hx * delt;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < ME; ++m) svd[m] = sv[m];
+  }
+}
+
+void launch_qad2(int solver, double* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
+                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s) {
+  if (njobs <= 0) return;
+  (void)nvar;
+  switch (solver) {
+    case SOLVER_ADVECTION: qad2_kernel<Advection2><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
+    case SOLVER_ACOUSTICS: qad2_kernel<Acoustics2><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
+    case SOLVER_EULER: qad2_kernel<Euler2><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+
+// ======================================================================= update
+__global__ void upbnd_kernel(double* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells,
+                             int ncells, const UpbndTerm* terms, double area, int nvar) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells * nvar) return;
+  const int c = t / nvar, m = t % nvar;
+  const UpbndCell C = cells[c];
+  const PatchDev& P = patches[C.patch];
+  double* v = pool + P.q[P.cur] + (long long)m * P.mitot * P.mjtot + (long long)C.je * P.mitot + C.ie;
+  double val = *v;
+  for (int k = 0; k < C.count; ++k) {
+    const UpbndTerm T = terms[C.first + k];
+    val = val + T.sgn * regs[T.reg + m] / area;
+  }
+  *v = val;
+}
+
+void launch_upbnd(double* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
+                  const UpbndTerm* terms, double area, int nvar, cudaStream_t s) {
+  if (ncells <= 0) return;
+  const int n = ncells * nvar;
+  upbnd_kernel<<<(n + 127) / 128, 128, 0, s>>>(pool, regs, patches, cells, ncells, terms, area, nvar);
+  AMR_CUDA(cudaGetLastError());
+}
+
+__global__ void average_kernel(double* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry,
+                               int nvar) {
+  const int r = blockIdx.y;
+  if (r >= nrects) return;
+  const AvgRect A = rects[r];
+  const PatchDev& C = patches[A.cpatch];
+  const PatchDev& K = patches[A.kpatch];
+  double* qc = pool + C.q[C.cur];
+  const double* qf = pool + K.q[K.cur];
+  const long long cpl = (long long)C.mitot * C.mjtot, fpl = (long long)K.mitot * K.mjtot;
+  const double totrat = (double)(rx * ry);
+  const int n = A.ni * A.nj * nvar;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int m = t / (A.ni * A.nj), rem = t % (A.ni * A.nj);
+    const int b = rem / A.ni, aa = rem % A.ni;
+    const int fi = A.fi0 + aa * rx, fj = A.fj0 + b * ry;
+    double s = 0.0;
+    for (int jco = 0; jco < ry; ++jco)
+      for (int ico = 0; ico < rx; ++ico) s = s + qf[m * fpl + (long long)(fj + jco) * K.mitot + (fi + ico)];
+    s = s / totrat;
+    qc[m * cpl + (long long)(A.cj0 + b) * C.mitot + (A.ci0 + aa)] = s;
+  }
+}
+
+void launch_average(double* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
+                    cudaStream_t s) {
+  for (int base = 0; base < nrects; base += 65535) {
+    const int n = std::min(65535, nrects - base);
+    dim3 grid(4, n);
+    average_kernel<<<grid, 128, 0, s>>>(pool, patches, rects + base, n, rx, ry, nvar);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
+// ======================================================================= flags, gauges, misc
+__global__ void flags2_kernel(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff,
+                              int use_old, int flag_component, double tolsp, int nvar, int8_t* out) {
+  const int pi = blockIdx.y;
+  const PatchDev P = patches[plist[pi]];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+  const double* q = pool + P.q[use_old ? 1 - P.cur : P.cur];
+  const long long plane = (long long)P.mitot * P.mjtot;
+  const int m0 = flag_component > 0 ? flag_component - 1 : 0, m1 = flag_component > 0 ? flag_component - 1 : nvar - 1;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my; t += gridDim.x * blockDim.x) {
+    const int i = t % mx + 1, j = t / mx + 1;  // interior, 1-based
+    const int ie = i + 1, je = j + 1;
+    int8_t f = 0;
+    for (int m = m0; m <= m1; ++m) {
+      const double* qm = q + m * plane;
+      const double dqi = fabs(qm[(long long)je * P.mitot + ie + 1] - qm[(long long)je * P.mitot + ie - 1]);
+      const double dqj = fabs(qm[(long long)(je + 1) * P.mitot + ie] - qm[(long long)(je - 1) * P.mitot + ie]);
+      const double dq = dmax(0.0, dmax(dqi, dqj));
+      if (dq > tolsp) { f = 1; break; }
+    }
+    out[outoff[pi] + t] = f;
+  }
+}
+
+void launch_flags2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
+                   int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    dim3 grid(8, n);
+    flags2_kernel<<<grid, 128, 0, s>>>(pool, patches, plist + base, outoff + base, use_old, flag_component, tolsp, nvar, out);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
+__global__ void gauges2_kernel(const double* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
+                               double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= njobs) return;
+  const GaugeJob G = jobs[t];
+  const PatchDev& P = patches[G.patch];
+  const double* q = pool + P.q[P.cur];
+  const long long plane = (long long)P.mitot * P.mjtot;
+  const double xo = G.xoff, yo = G.yoff;
+  // Q(n, ii, jj) with ii, jj 1-based enlarged indices
+  auto Q = [&](int m, int i, int j) { return q[m * plane + (long long)(j - 1) * P.mitot + (i - 1)]; };
+  for (int m = 0; m < nvar; ++m) {
+    double v = (1.0 - xo) * (1.0 - yo) * Q(m, G.ii, G.jj) + xo * (1.0 - yo) * Q(m, G.ii + 1, G.jj) +
+               (1.0 - xo) * yo * Q(m, G.ii, G.jj + 1) + xo * yo * Q(m, G.ii + 1, G.jj + 1);
+    if (fabs(v) < 1e-90) v = 0.0;
+    out[(long long)G.slot * nvar + m] = v;
+  }
+}
+
+void launch_gauges2(const double* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
+                    double* out, cudaStream_t s) {
+  if (njobs <= 0) return;
+  gauges2_kernel<<<(njobs + 63) / 64, 64, 0, s>>>(pool, patches, jobs, njobs, nvar, out);
+  AMR_CUDA(cudaGetLastError());
+}
+
+__global__ void flip_kernel(PatchDev* patches, const int* plist, int np) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < np) patches[plist[t]].cur ^= 1;
+}
+void launch_flip(PatchDev* patches, const int* plist, int np, cudaStream_t s) {
+  if (np <= 0) return;
+  flip_kernel<<<(np + 127) / 128, 128, 0, s>>>(patches, plist, np);
+  AMR_CUDA(cudaGetLastError());
+}
+
+__global__ void zero_tiny_kernel(double* pool, const PatchDev* patches, const int* plist, int nvar) {
+  const PatchDev P = patches[plist[blockIdx.y]];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+  double* q = pool + P.q[P.cur];
+  const long long plane = (long long)P.mitot * P.mjtot;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my * nvar; t += gridDim.x * blockDim.x) {
+    const int m = t / (mx * my), rem = t % (mx * my);
+    const int i = rem % mx + 2, j = rem / mx + 2;
+    double& v = q[m * plane + (long long)j * P.mitot + i];
+    if (fabs(v) < 1e-90) v = 0.0;
+  }
+}
+void launch_zero_tiny(double* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    zero_tiny_kernel<<<dim3(4, n), 128, 0, s>>>(pool, patches, plist + base, nvar);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
+__global__ void mass2_kernel(const double* pool, const PatchDev* patches, const int* plist, int np, double* out) {
+  double s = 0.0;
+  for (int pi = blockIdx.y; pi < np; pi += gridDim.y) {
+    const PatchDev P = patches[plist[pi]];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+    const double* q = pool + P.q[P.cur];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my; t += gridDim.x * blockDim.x)
+      s += q[(long long)(t / mx + 2) * P.mitot + (t % mx + 2)];
+  }
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+void launch_mass2(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s) {
+  if (np <= 0) return;
+  mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(pool, patches, plist, np, out);
+  AMR_CUDA(cudaGetLastError());
+}
+
+__global__ void gather_interior2_kernel(const double* pool, const PatchDev* patches, const int* plist,
+                                        const long long* outoff, int nvar, double* out) {
+  const PatchDev P = patches[plist[blockIdx.y]];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+  const double* q = pool + P.q[P.cur];
+  const long long plane = (long long)P.mitot * P.mjtot;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my * nvar; t += gridDim.x * blockDim.x) {
+    const int m = t / (mx * my), rem = t % (mx * my);
+    const int i = rem % mx + 2, j = rem / mx + 2;
+    out[outoff[blockIdx.y] + t] = q[m * plane + (long long)j * P.mitot + i];
+  }
+}
+void launch_gather_interior2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff,
+                             int np, int nvar, double* out, cudaStream_t s) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    gather_interior2_kernel<<<dim3(8, n), 128, 0, s>>>(pool, patches, plist + base, outoff + base, nvar, out);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
+}  // namespace amrb

@@ -1,0 +1,141 @@
+// Work-item and op structures shared by the 2D host orchestrator and its kernels.
+#pragma once
+#include "common.cuh"
+#include "riemann2d.cuh"
+
+namespace amrb {
+
+constexpr int TILE2 = 16;      // interior cells per tile side in the 2D patch step
+constexpr int STEP2_THREADS = 256;
+constexpr int STEP2_RC = 6;    // rows per Riemann chunk
+
+// One tile of one patch (the batched path launches all tiles of a level at once).
+struct StepWork {
+  int patch;
+  int ti0, tj0;          // tile origin, 1-based interior indices
+  int fsv_start, fsv_count;  // fluxsv entries owned by this tile
+  int fad_start, fad_count;  // fluxad segments owned by this tile
+};
+
+// fluxsv.f:10-109: coarse flux at a face next to a finer grid, written into the kid's register.
+struct FsvEntry {
+  int ic, jc;            // coarse cell, 1-based interior indices
+  int side;              // listbc side code 1..4
+  int pad;
+  long long dst;         // register-pool offset of svdflx(:, lkid) of the kid
+};
+// fluxad.f:7-96: fine fluxes over one coarse segment, accumulated into the patch's own register.
+struct FadEntry {
+  int side;              // 1 left, 2 top, 3 right, 4 bottom (register order of fluxad.f)
+  int f0;                // first fine row (sides 1,3) or column (sides 2,4), 1-based interior
+  int seg;               // 0-based register index (lind-1)
+  int pad;
+};
+
+struct StepParams {
+  ProbDev prob;
+  int mthlim[MAXVAR];
+  int order;             // method(2)
+  int trans;             // method(3)
+  int use_fwaves;
+  int mcapa;
+};
+
+struct StepArgs {
+  double* pool;
+  double* regs;
+  const PatchDev* patches;
+  const StepWork* work;
+  int nwork;
+  int* queue;            // dynamic work queue counter (nullptr: static assignment)
+  const FsvEntry* fsv;
+  const FadEntry* fad;
+  double dt, dx, dy;
+  unsigned long long* cflmax;  // max Courant number of the level (bit pattern of a non-negative double)
+  StepParams sp;
+};
+
+// ---------------------------------------------------------------- ghost-fill programs
+enum FillKind { FILL_COPY = 0, FILL_INTERP = 1, FILL_PIECE = 2, FILL_FILVAL = 3, FILL_RING = 4 };
+
+struct ScratchRect {
+  long long off;         // pool offset (doubles), layout [m][j][i]
+  int ni, nj;
+};
+
+struct FillOp {
+  int kind;
+  int dst_patch;         // >= 0: store1 of this patch (enlarged array); -1: scratch rect dst_rect
+  int dst_rect;
+  int di0, dj0;          // region origin (0-based) inside the destination array
+  int ni, nj;            // region extent
+  int src;               // COPY: source patch; others: source scratch rect
+  int si0, sj0;          // COPY/PIECE: origin in the source array (0-based); INTERP/FILVAL: global fine index of the region origin
+  int level;             // COPY: source level for the time mode (-1: always store1); INTERP/FILVAL: fine level
+  int cilo, cjlo;        // INTERP/FILVAL: global coarse index of the source rect origin
+};
+
+struct FillChunk { int op, start, count; };
+
+// bc2amr.f90:84-297 applied to one whole array (a patch or a scratch rect).
+struct BcOp {
+  int dst_patch, dst_rect;
+  int nrow, ncol;
+  int nxl, ibeg, nyb, jbeg;      // ghost extents (0: side not outside the domain)
+  int bxl, bxr, byl, byr;        // boundary codes (1 extrap, 3 wall, 0/2 none)
+};
+
+struct FillArgs {
+  double* pool;
+  double* regs;
+  const PatchDev* patches;
+  const ScratchRect* rects;
+  const FillOp* ops;
+  const FillChunk* chunks;
+  int nchunks;
+  int nvar;
+  SrcMode modes;
+  LevelConst lc;
+  double xlower, ylower;
+};
+
+struct BcArgs {
+  double* pool;
+  const PatchDev* patches;
+  const ScratchRect* rects;
+  const BcOp* ops;
+  int nops;
+  int nvar;
+};
+
+// ---------------------------------------------------------------- registers, update
+struct QadJob { int patch; int side; int seg0; int nseg; int pos0; };  // one side of one fine patch
+
+struct UpbndCell { int patch; int ie, je; int first, count; };   // upbnd.f:62-124, per coarse cell
+struct UpbndTerm { long long reg; double sgn; };
+struct AvgRect { int cpatch, kpatch; int ci0, cj0, ni, nj; int fi0, fj0; };  // update.f:95-175
+
+struct GaugeJob { int patch; int ii, jj; int slot; double xoff, yoff; };
+
+// Launch wrappers (kernels2d.cu)
+void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s);
+void launch_fill(const FillArgs& a, cudaStream_t s);
+void launch_bc(const BcArgs& a, int phase, cudaStream_t s);
+void launch_qad2(int solver, double* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
+                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s);
+void launch_upbnd(double* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
+                  const UpbndTerm* terms, double area, int nvar, cudaStream_t s);
+void launch_average(double* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
+                    cudaStream_t s);
+void launch_flags2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
+                   int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s);
+void launch_gauges2(const double* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
+                    double* out, cudaStream_t s);
+void launch_flip(PatchDev* patches, const int* plist, int np, cudaStream_t s);
+void launch_zero_tiny(double* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s);
+void launch_mass2(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s);
+void launch_gather_interior2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff,
+                             int np, int nvar, double* out, cudaStream_t s);
+size_t step2_smem_bytes(int solver);
+
+}  // namespace amrb

@@ -1,0 +1,85 @@
+/* amrclaw_b200: C ABI of the B200 patch-advance path of AMRClaw.
+ *
+ * The reference (mjberger/amrclaw) runs its level integrator inside the Fortran
+ * program amr2/amr3; these entry points are what a Fortran 90 driver binds through
+ * ISO_C_BINDING to hand that path to the GPU. All entry points
+ * return an int status (AMRGPU_OK = 0); no exception crosses the boundary and the
+ * text of the last error is available from amrgpu_last_error(). Host arrays passed
+ * in are borrowed for the duration of the call. One context is used by one host
+ * thread at a time.
+ */
+#ifndef AMRCLAW_B200_H
+#define AMRCLAW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMRGPU_OK 0
+#define AMRGPU_ERROR 1
+#define AMRGPU_EINVAL 2
+
+typedef struct amrgpu_ctx amrgpu_ctx;
+
+/* Message of the last failed call on this thread (empty when none). */
+const char* amrgpu_last_error(void);
+
+/* Reads claw.data, amr.data, regions.data, gauges.data and setprob.data from
+ * rundir (the files setrun.py writes), builds the initial hierarchy on the device
+ * and writes frame 0 when output_t0 is set.
+ * Replaces the start-up of src/2d/amr2.f90:140-612 (input reading :148-394,
+ * domain.f:4-110, setgrd.f:4-142, ginit.f:17-86, conck.f:6-73). */
+int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu_ctx** ctx);
+
+/* 1: advance every patch of a level in one launch (batched path, default);
+ * 0: one launch per patch (plain per-patch path). */
+int amrgpu_set_batched(amrgpu_ctx* ctx, int batched);
+
+/* The whole time integration: Berger-Oliger subcycling, regridding cadence,
+ * output times. Replaces tick (src/2d/tick.f:4-391). max_cycles > 0 stops after
+ * that many coarse steps. */
+int amrgpu_run(amrgpu_ctx* ctx, int max_cycles);
+
+/* One substep of every patch of `level`: ghost fill, coarse-value save for the
+ * finer level, coarse/fine Riemann fix-up, patch step and flux registers.
+ * Replaces advanc (src/2d/advanc.f:10-142) and par_advanc (advanc.f:170-291).
+ * dtnew_out receives the level's suggested next dt (stepgrid.f:206-212). */
+int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out);
+
+/* Fine-to-coarse averaging and flux-register fix-up of `level` from level+1.
+ * Replaces update (src/2d/update.f:16-189) and upbnd (src/2d/upbnd.f:18-127). */
+int amrgpu_update(amrgpu_ctx* ctx, int level);
+
+/* Regrid levels lbase+1 and finer. Replaces regrid (src/2d/regrid.f:4-122). */
+int amrgpu_regrid(amrgpu_ctx* ctx, int lbase);
+
+/* Write fort.qNNNN / fort.tNNNN into dir (ASCII form of src/2d/valout.f90:8-397). */
+int amrgpu_valout(amrgpu_ctx* ctx, const char* dir);
+
+/* Total of q(1)*dx*dy over level 1 (src/2d/conck.f:6-73). */
+int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
+
+/* Run statistics: out[0..n) = time, cell updates, coarse steps, finest level,
+ * stepping seconds, regrid seconds, initial mass, max Courant number, kernels
+ * launched, peak pool bytes, level substeps. */
+int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
+
+/* Hierarchy rows (grid_number, level, ilo, ihi, jlo, jhi) in output order
+ * (src/2d/valout.f90 loop order); *n_out receives the row count. */
+int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out);
+
+/* Interior cell values of every grid in amrgpu_grids order, [m][j][i] per grid. */
+int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out);
+
+/* Gauge samples as rows (gauge number, level, time, q1..qmeqn), grouped by gauge
+ * (src/2d/gauges_module.f90:313-500). */
+int amrgpu_gauges(amrgpu_ctx* ctx, double* out, int cap_rows, int* n_out);
+
+/* Release the context and its device memory. */
+int amrgpu_destroy(amrgpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMRCLAW_B200_H */
