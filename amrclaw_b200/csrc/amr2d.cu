@@ -132,7 +132,7 @@ struct FillProg {
   std::vector<BcOp> bcs;
   std::vector<int> bc_stage;
   int nstages = 0;
-  long long scratch_off = -1, scratch_len = 0;
+  long long scratch_off = -1, scratch_len = 0, scratch_alloc = 0;
   DBuf<ScratchRect> d_rects;
   DBuf<FillOp> d_ops;
   DBuf<FillChunk> d_chunks;
@@ -654,10 +654,9 @@ class Amr2Gpu {
   }
 
   void upload_prog(FillProg& P) {
-    if (P.scratch_off >= 0) pool.release(P.scratch_off, std::max<long long>(P.scratch_len, 1));
-    P.scratch_off = -1;
-    // the scratch length of the previous compile may differ; (re)allocate
-    P.scratch_off = pool.alloc(std::max<long long>(P.scratch_len, 1));
+    if (P.scratch_off >= 0) pool.release(P.scratch_off, P.scratch_alloc);
+    P.scratch_alloc = std::max<long long>(P.scratch_len, 1);
+    P.scratch_off = pool.alloc(P.scratch_alloc);
     std::vector<ScratchRect> rects = P.rects;
     for (auto& r : rects) r.off += P.scratch_off;
     P.d_rects.upload(rects, st);
@@ -1271,6 +1270,13 @@ class Amr2Gpu {
       g.flags.clear(); g.dom2.clear();
     }
     sort_unique(pts, iregsz[lcheck], mbuff);
+    if (std::getenv("AMRB_DEBUG")) {
+      long long gsum = 0;
+      for (int8_t v : hflag) gsum += v;
+      std::fprintf(stderr, "FLAGS lcheck=%d lbase=%d t=%.17g use_old=%d grad=%lld npts=%zu:", lcheck, lbase, t, use_old, gsum, pts.size());
+      for (size_t k = 0; k < pts.size() && k < 12; ++k) std::fprintf(stderr, " (%d,%d)", pts[k].i, pts[k].j);
+      std::fprintf(stderr, "\n");
+    }
     return pts;
   }
 
@@ -1375,7 +1381,7 @@ class Amr2Gpu {
     SrcMode M{};
     run_prog(P, M);
     AMR_CUDA(cudaStreamSynchronize(st));
-    pool.release(P.scratch_off, std::max<long long>(P.scratch_len, 1));
+    pool.release(P.scratch_off, P.scratch_alloc);
     P.d_rects.free(); P.d_ops.free(); P.d_chunks.free(); P.d_bcs.free();
   }
 

@@ -1701,6 +1701,11 @@ struct Amr2 {
     const int npts = index;
     drivesort(npts, badpts, lcheck, nunique, mbuff);
     badpts.resize(2 * (size_t)nunique);
+    if (std::getenv("AMRB_DEBUG")) {
+      std::fprintf(stderr, "FLAGS lcheck=%d npts=%d:", lcheck, nunique);
+      for (int k = 0; k < nunique && k < 12; ++k) std::fprintf(stderr, " (%d,%d)", (int)(badpts[2 * k] - 0.5), (int)(badpts[2 * k + 1] - 0.5));
+      std::fprintf(stderr, "\n");
+    }
   }
 
   // ================================================================ clustering
