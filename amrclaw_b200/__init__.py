@@ -53,6 +53,9 @@ class Solver:
     def set_batched(self, batched: bool) -> None:
         _check(self._lib, self._lib.amrgpu_set_batched(self._h, int(batched)), "amrgpu_set_batched")
 
+    def set_profile(self, on: bool) -> None:
+        _check(self._lib, self._lib.amrgpu_set_profile(self._h, int(on)), "amrgpu_set_profile")
+
     def run(self, max_cycles: int = 0) -> None:
         _check(self._lib, self._lib.amrgpu_run(self._h, int(max_cycles)), "amrgpu_run")
 
@@ -78,10 +81,11 @@ class Solver:
         return m.value
 
     def info(self) -> dict:
-        out = (ctypes.c_double * 11)()
-        _check(self._lib, self._lib.amrgpu_info(self._h, out, 11), "amrgpu_info")
         keys = ["time", "cell_updates", "coarse_steps", "lfine", "step_seconds", "regrid_seconds", "mass0",
-                "cflmax", "kernels", "pool_peak_bytes", "substeps"]
+                "cflmax", "kernels", "pool_peak_bytes", "substeps", "step_kernel_ms", "step_kernel_cells",
+                "last_run_ms", "last_run_cells", "finished", "h2d_bytes"]
+        out = (ctypes.c_double * len(keys))()
+        _check(self._lib, self._lib.amrgpu_info(self._h, out, len(keys)), "amrgpu_info")
         return dict(zip(keys, list(out)))
 
     def grids(self) -> np.ndarray:

@@ -216,6 +216,14 @@ class Amr2Gpu {
   std::vector<GaugeJob> gjobs_pending;
   int gslots = 0;
   double t_regrid = 0, t_step = 0;
+  // profiling: CUDA events around every step launch and around each run call
+  bool profile = false;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_run0 = nullptr, ev_run1 = nullptr;
+  double step_kernel_ms = 0, step_kernel_cells = 0, last_run_ms = 0, run_cells = 0, h2d_bytes = 0;
+  // scheduler state kept between run calls (tick.f locals)
+  bool tick_started = false;
+  int tk_nextout = 0, tk_iout = 0;
+  double tk_tlevel[12] = {0};
   long long nsteps_launched = 0, nkernels = 0;
   int frame = 0;
   std::string outdir;
@@ -228,6 +236,7 @@ class Amr2Gpu {
     d_patches.free(); d_gauge_out.free();
     if (d_cfl) cudaFree(d_cfl);
     if (d_mass) cudaFree(d_mass);
+    for (cudaEvent_t e : {ev_a, ev_b, ev_run0, ev_run1}) if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
   }
 
@@ -981,6 +990,7 @@ class Amr2Gpu {
     }
     // the patch step: plain = one launch per patch, batched = one launch per level
     AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+    if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
     StepArgs a{};
     a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.fsv = L.d_fsv.d; a.fad = L.d_fad.d;
     a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
@@ -997,6 +1007,7 @@ class Amr2Gpu {
         ++nkernels;
       }
     }
+    if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
     launch_flip(d_patches.d, L.d_plist.d, (int)L.plist.size(), st);
     ++nkernels;
     unsigned long long cbits = 0;
@@ -1004,6 +1015,12 @@ class Amr2Gpu {
     AMR_CUDA(cudaStreamSynchronize(st));
     double cmax;
     std::memcpy(&cmax, &cbits, sizeof(double));
+    if (profile) {
+      float ms = 0;
+      AMR_CUDA(cudaEventElapsedTime(&ms, ev_a, ev_b));
+      step_kernel_ms += ms;
+      for (int m : lgrids[lev]) step_kernel_cells += (double)node[m].nx() * node[m].ny();
+    }
     for (int m : lgrids[lev]) {
       node[m].cur ^= 1;
       node[m].time = node[m].time + dt;
@@ -1478,6 +1495,7 @@ class Amr2Gpu {
       lc.iregsz[l] = iregsz[l]; lc.jregsz[l] = jregsz[l]; lc.intratx[l] = intratx[l]; lc.intraty[l] = intraty[l];
     }
     AMR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ev_a, &ev_b, &ev_run0, &ev_run1}) AMR_CUDA(cudaEventCreate(e));
     long long est = (long long)nvar * (nxc + 4) * (nyc + 4) * 8 * std::max(1, p.mxnest) + (1 << 22);
     pool.init(est);
     regs.init(1 << 20);
@@ -1548,6 +1566,7 @@ class Amr2Gpu {
       qinit(g.nx(), g.ny(), g.xlo, g.ylo, hxposs[g.level], hyposs[g.level], q);
       AMR_CUDA(cudaMemcpyAsync(pool.d + g.q0, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
       AMR_CUDA(cudaMemcpyAsync(pool.d + g.q1, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
+      h2d_bytes += 2.0 * sizeof(double) * q.size();
       AMR_CUDA(cudaStreamSynchronize(st));
     }
   }
@@ -1577,14 +1596,23 @@ class Amr2Gpu {
 
   // ================================================================ tick.f
   void tick() {
-    double dtnew[12], tlevel[12];
+    double dtnew[12];
+    double* tlevel = tk_tlevel;
     int ntogo[12];
-    ncycle = 0;
-    setbestsrc();
-    int iout = p.iout, nextout = 0;
-    if (iout == 0) { iout = 999999999; nextout = p.nout > 0 ? 1 : 0; }
-    tlevel[1] = time;
-    for (int i = 2; i <= p.mxnest; ++i) tlevel[i] = tlevel[1];
+    if (!tick_started) {
+      ncycle = 0;
+      setbestsrc();
+      tk_iout = p.iout; tk_nextout = 0;
+      if (tk_iout == 0) { tk_iout = 999999999; tk_nextout = p.nout > 0 ? 1 : 0; }
+      tlevel[1] = time;
+      for (int i = 2; i <= p.mxnest; ++i) tlevel[i] = tlevel[1];
+      tick_started = true;
+    }
+    int& iout = tk_iout;
+    int& nextout = tk_nextout;
+    int cycles_this_call = 0;
+    const double rvol0 = rvol;
+    AMR_CUDA(cudaEventRecord(ev_run0, st));
     const auto tstart = std::chrono::steady_clock::now();
     while (!(ncycle >= p.nstop || time >= p.tfinal)) {
       double outtime = (p.nout > 0) ? (nextout <= p.nout ? p.tout[nextout - 1] : RINF) : p.tfinal;
@@ -1647,11 +1675,18 @@ class Amr2Gpu {
         for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
       }
       if ((ncycle % iout == 0) || dumpout) output(time);
-      if (max_cycles > 0 && ncycle >= max_cycles) break;
+      ++cycles_this_call;
+      if (max_cycles > 0 && cycles_this_call >= max_cycles) break;
     }
+    AMR_CUDA(cudaEventRecord(ev_run1, st));
     AMR_CUDA(cudaStreamSynchronize(st));
-    t_step = std::chrono::duration<double>(std::chrono::steady_clock::now() - tstart).count();
+    float ms = 0;
+    AMR_CUDA(cudaEventElapsedTime(&ms, ev_run0, ev_run1));
+    last_run_ms = ms;
+    run_cells = rvol - rvol0;
+    t_step += std::chrono::duration<double>(std::chrono::steady_clock::now() - tstart).count();
   }
+  bool finished() const { return ncycle >= p.nstop || time >= p.tfinal; }
 
   // interior values of all grids (levels 1..lfine, list order), layout [m][j][i] per grid
   std::vector<double> gather_values() {
@@ -1799,6 +1834,12 @@ int amrgpu_set_batched(amrgpu_ctx* ctx, int batched) {
   return AMRGPU_OK;
 }
 
+int amrgpu_set_profile(amrgpu_ctx* ctx, int on) {
+  if (!ctx) return AMRGPU_EINVAL;
+  ctx->s2->profile = on != 0;
+  return AMRGPU_OK;
+}
+
 int amrgpu_run(amrgpu_ctx* ctx, int max_cycles) {
   if (!ctx) return AMRGPU_EINVAL;
   return guarded([&] {
@@ -1860,7 +1901,8 @@ int amrgpu_info(amrgpu_ctx* ctx, double* out, int n) {
   return guarded([&] {
     amrb::Amr2Gpu& s = *ctx->s2;
     const double v[] = {s.time, s.rvol, (double)s.ncycle, (double)s.lfine, s.t_step, s.t_regrid, s.tmass0,
-                        s.cflmax_run, (double)s.nkernels, (double)s.pool.peak * 8.0, (double)s.nsteps_launched};
+                        s.cflmax_run, (double)s.nkernels, (double)s.pool.peak * 8.0, (double)s.nsteps_launched,
+                        s.step_kernel_ms, s.step_kernel_cells, s.last_run_ms, s.run_cells, s.finished() ? 1.0 : 0.0, s.h2d_bytes};
     for (int k = 0; k < n && k < (int)(sizeof(v) / sizeof(v[0])); ++k) out[k] = v[k];
   });
 }

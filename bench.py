@@ -1,0 +1,277 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 AMRClaw patch-advance path.
+
+One "step" is one coarse time step of the AMR hierarchy (tick.f cycle): every
+level substep (ghost fill, saved coarse values, patch steps, flux registers),
+the level syncs and the regrids that fall in it. The metric is cell-updates/s,
+counted as the reference counts them (src/2d/advanc.f:223-224: interior cells per
+patch per level substep). ``value`` is the batched path (one launch per level)
+with the hierarchy resident in HBM; ``plain`` is the per-patch launch path on
+the same steps; ``e2e`` is the whole solve through the C ABI from host input
+files to host results.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Under torchrun each rank runs an independent replica of the workload (replicas
+only: one AMR hierarchy per GPU, no exchange); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "cell-updates/s batched vs plain GPU at stated L1 err vs FP64; p50/p99 solve latency"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def workload(name: str):
+    import configs
+    if name == "euler2d_quadrants":
+        rd = configs.euler_quadrants(n=100, levels=4, tfinal=0.8)
+        return rd, dict(workload=name, base_grid="100x100", levels=4, ratio=2, solver="Roe+entropy fix", meqn=4,
+                        naux=0, tfinal=0.8, precision="fp64"), 4, 0
+    raise SystemExit("unknown workload %s" % name)
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self):
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        dev = os.environ.get("LOCAL_RANK", "0")
+        rows = [r for r in self.rows if len(r) >= 9 and r[0] == dev] or [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def flush_l2(buf):
+    buf.fill_(1.0)
+    import torch
+    torch.cuda.synchronize()
+
+
+def run_reference(args, rank):
+    """The reference's CPU path: the CPU restatement (the reference Fortran cannot be built here)."""
+    if rank != 0:
+        return
+    from oracle.pyoracle import Oracle2D
+    rd, cfg, nvar, _ = workload(args.workload)
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        rd.write(d)
+        o = Oracle2D(d, threads=threads)
+        o.run(args.warmup)
+        c0 = o.cell_updates()
+        sec = o.run(args.steps)
+        cells = o.cell_updates() - c0
+        o.close()
+    v = cells / sec
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded initial conditions",
+            "config": cfg,
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                             "sample": "steps %d..%d of the workload, all host threads (OpenMP over patches)" % (
+                                 args.warmup, args.warmup + args.steps)},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="euler2d_quadrants")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from amrclaw_b200 import Solver
+    rd, cfg, nvar, naux = workload(args.workload)
+    bytes_per_update = (2 * nvar + naux) * 8
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    with tempfile.TemporaryDirectory() as d:
+        rd.write(d)
+        # ---------------- batched path (the value)
+        s = Solver(d, batched=True)
+        s.run(args.warmup)
+        s.set_profile(True)
+        i0 = s.info()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = Clocks()
+        clocks.start()
+        ms = 0.0
+        cells = 0.0
+        for _ in range(args.steps):
+            flush_l2(flush)
+            s.run(1)
+            inf = s.info()
+            ms += inf["last_run_ms"]
+            cells += inf["last_run_cells"]
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        i1 = s.info()
+        s.close()
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            c = torch.tensor([cells], device="cuda", dtype=torch.float64)
+            dist.all_reduce(c)
+            cells = float(c.item())
+        value = cells / (ms * 1e-3)
+        kern_ms = i1["step_kernel_ms"] - i0["step_kernel_ms"]
+        kern_cells = i1["step_kernel_cells"] - i0["step_kernel_cells"]
+        launches = int(i1["kernels"] - i0["kernels"])
+        step_launches = int(i1["substeps"] - i0["substeps"])
+
+        # ---------------- plain per-patch path on the same steps
+        p = Solver(d, batched=False)
+        p.run(args.warmup)
+        pms = 0.0
+        pcells = 0.0
+        for _ in range(args.steps):
+            flush_l2(flush)
+            p.run(1)
+            inf = p.info()
+            pms += inf["last_run_ms"]
+            pcells += inf["last_run_cells"]
+        p.close()
+        plain_value = pcells / (pms * 1e-3)
+
+        # ---------------- end to end through the C ABI: host files in, host values out
+        t0 = time.perf_counter()
+        e = Solver(d, batched=True)
+        e.run(args.warmup + args.steps)
+        vals = e.values()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        einf = e.info()
+        e.close()
+        e2e_value = einf["cell_updates"] / (t1 - t0)
+        h2d = einf["h2d_bytes"]
+        d2h = vals.nbytes
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    achieved = kern_cells * bytes_per_update / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle.pyoracle import Oracle2D
+        threads = os.cpu_count() or 1
+        with tempfile.TemporaryDirectory() as d:
+            rd.write(d)
+            o = Oracle2D(d, threads=threads)
+            o.run(args.warmup)
+            c0 = o.cell_updates()
+            sec = o.run(args.cpu_steps)
+            cpu_v = (o.cell_updates() - c0) / sec
+            o.close()
+        cpu = {"value": cpu_v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+               "sample": "coarse steps %d..%d of the same workload on the CPU restatement (OpenMP over patches)" % (
+                   args.warmup, args.warmup + args.cpu_steps)}
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded initial conditions of the workload",
+        "config": dict(cfg, l2="flushed between steps (256 MB write)", parallelism="replicas" if world > 1 else "single"),
+        "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": pms / args.steps,
+                  "speedup_batched_over_plain": value / plain_value if plain_value else None},
+        "l1_err_vs_fp64": 0.0,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "kernel": "step2_kernel", "peak_kind": peak_kind,
+                     "bytes_per_cell_update": bytes_per_update},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d) // max(1, args.warmup + args.steps),
+                "d2h_bytes_per_step": d2h // max(1, args.warmup + args.steps),
+                "includes": "init from data files, initial upload, %d steps, result download" % (args.warmup + args.steps)},
+        "gpu_launches": launches,
+        "level_substeps": step_launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -35,9 +35,13 @@ int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu
  * 0: one launch per patch (plain per-patch path). */
 int amrgpu_set_batched(amrgpu_ctx* ctx, int batched);
 
+/* 1: record CUDA events around every patch-step launch (kernel time is then
+ * reported by amrgpu_info); 0: no per-launch events. */
+int amrgpu_set_profile(amrgpu_ctx* ctx, int on);
+
 /* The whole time integration: Berger-Oliger subcycling, regridding cadence,
  * output times. Replaces tick (src/2d/tick.f:4-391). max_cycles > 0 stops after
- * that many coarse steps. */
+ * that many coarse steps; a later call continues from there. */
 int amrgpu_run(amrgpu_ctx* ctx, int max_cycles);
 
 /* One substep of every patch of `level`: ghost fill, coarse-value save for the
@@ -61,7 +65,10 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
 
 /* Run statistics: out[0..n) = time, cell updates, coarse steps, finest level,
  * stepping seconds, regrid seconds, initial mass, max Courant number, kernels
- * launched, peak pool bytes, level substeps. */
+ * launched, peak pool bytes, level substeps, patch-step kernel milliseconds
+ * (profiling on), cells of those launches, device milliseconds of the last
+ * amrgpu_run call, cell updates of that call, 1 when tfinal was reached,
+ * bytes of initial data copied host to device. */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 
 /* Hierarchy rows (grid_number, level, ilo, ihi, jlo, jhi) in output order
