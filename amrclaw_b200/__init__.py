@@ -83,7 +83,8 @@ class Solver:
     def info(self) -> dict:
         keys = ["time", "cell_updates", "coarse_steps", "lfine", "step_seconds", "regrid_seconds", "mass0",
                 "cflmax", "kernels", "pool_peak_bytes", "substeps", "step_kernel_ms", "step_kernel_cells",
-                "last_run_ms", "last_run_cells", "finished", "h2d_bytes"]
+                "last_run_ms", "last_run_cells", "finished", "h2d_bytes",
+                "regrid_flags_s", "regrid_hostflags_s", "regrid_cluster_s", "regrid_fill_s", "regrid_prep_s", "regrid_compile_s"]
         out = (ctypes.c_double * len(keys))()
         _check(self._lib, self._lib.amrgpu_info(self._h, out, len(keys)), "amrgpu_info")
         return dict(zip(keys, list(out)))

@@ -216,6 +216,7 @@ class Amr2Gpu {
   std::vector<GaugeJob> gjobs_pending;
   int gslots = 0;
   double t_regrid = 0, t_step = 0;
+  double tr_flags = 0, tr_host = 0, tr_cluster = 0, tr_fill = 0, tr_prep = 0, tr_compile = 0;
   // profiling: CUDA events around every step launch and around each run call
   bool profile = false;
   cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_run0 = nullptr, ev_run1 = nullptr;
@@ -901,17 +902,21 @@ class Amr2Gpu {
     L.d_work.free(); L.d_fsv.free(); L.d_fad.free(); L.d_qad.free(); L.d_upc.free(); L.d_upt.free(); L.d_avg.free(); L.d_plist.free();
   }
 
-  void compile_all() {
+  // Programs of levels finer than lbase change with a regrid of lbase+1..; the
+  // saveqc, step and update plans of lbase itself change with its kids.
+  void compile_all(int lbase = 0) {
     sync_descriptors();
     for (int lev = 1; lev <= p.mxnest; ++lev) {
       if (lev > lfine) {
         plan[lev].work.clear(); plan[lev].plist.clear();
         continue;
       }
-      compile_bound(lev);
-      compile_saveqc(lev);
-      compile_step(lev);
-      compile_update(lev);
+      if (lev > lbase) compile_bound(lev);
+      if (lev >= lbase) {
+        compile_saveqc(lev);
+        compile_step(lev);
+        compile_update(lev);
+      }
     }
   }
 
@@ -1184,6 +1189,7 @@ class Amr2Gpu {
     if (start_time + possk[lcheck] != t) bound_level(lcheck, t);
     else use_old = 1;
     // device gradient test
+    const auto tf0 = std::chrono::steady_clock::now();
     std::vector<long long> off(G.size() + 1, 0);
     for (size_t k = 0; k < G.size(); ++k) off[k + 1] = off[k] + (long long)node[G[k]].nx() * node[G[k]].ny();
     DBuf<int8_t> dout; dout.ensure(std::max<long long>(off.back(), 1));
@@ -1194,6 +1200,8 @@ class Amr2Gpu {
     if (off.back()) AMR_CUDA(cudaMemcpyAsync(hflag.data(), dout.d, off.back(), cudaMemcpyDeviceToHost, st));
     AMR_CUDA(cudaStreamSynchronize(st));
     dout.free(); doff.free(); dpl.free();
+    const auto tf1 = std::chrono::steady_clock::now();
+    tr_flags += std::chrono::duration<double>(tf1 - tf0).count();
     const double dx = hxposs[lcheck], dy = hyposs[lcheck];
     std::vector<Pt> pts;
     int numbad = 0;
@@ -1287,6 +1295,7 @@ class Amr2Gpu {
       g.flags.clear(); g.dom2.clear();
     }
     sort_unique(pts, iregsz[lcheck], mbuff);
+    tr_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - tf1).count();
     if (std::getenv("AMRB_DEBUG")) {
       long long gsum = 0;
       for (int8_t v : hflag) gsum += v;
@@ -1304,6 +1313,7 @@ class Amr2Gpu {
     const int levnew = lcheck + 1;
     const double hxf = hxposs[levnew], hyf = hyposs[levnew];
     std::vector<int> cnt;
+    const auto tc0 = std::chrono::steady_clock::now();
     bisect(pts, p.cut, iregsz[lcheck], jregsz[lcheck], cnt);
     int base = 0, icl = 0, prv = 0;
     while (icl < (int)cnt.size()) {
@@ -1350,6 +1360,7 @@ class Amr2Gpu {
       ++icl;
     }
     birect(newstl[levnew]);
+    tr_cluster += std::chrono::duration<double>(std::chrono::steady_clock::now() - tc0).count();
   }
 
   // filval.f90 for all new grids of level lev, then release the old grids (gfixup.f:49-163)
@@ -1425,7 +1436,9 @@ class Amr2Gpu {
       sync_descriptors_with(keep, lcheck2);
       lfine = lf_save;
       lgrids[lcheck2] = keep;
+      const auto tq0 = std::chrono::steady_clock::now();
       if (newstl[lcheck2] != 0) fill_new_level(lcheck2);
+      tr_fill += std::chrono::duration<double>(std::chrono::steady_clock::now() - tq0).count();
       int m = lstart[lcheck2];
       while (m != 0) {
         const int mold = m;
@@ -1440,11 +1453,17 @@ class Amr2Gpu {
     }
     lfine = lfnew;
     for (int lev = lbase; lev <= p.mxnest; ++lev) { for (int m : lgrids[lev]) { node[m].has_cfl = false; node[m].listbc.clear(); } }
+    const auto tp0 = std::chrono::steady_clock::now();
     for (int lev = lbase; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
     for (int lev = lbase + 1; lev <= p.mxnest; ++lev) arrange(lev);
     make_lists();
     for (int lev = lbase + 1; lev <= lfine; ++lev) make_bndry(lev);
-    compile_all();
+    const auto tp1 = std::chrono::steady_clock::now();
+    compile_all(lbase);
+    AMR_CUDA(cudaStreamSynchronize(st));
+    const auto tp2 = std::chrono::steady_clock::now();
+    tr_prep += std::chrono::duration<double>(tp1 - tp0).count();
+    tr_compile += std::chrono::duration<double>(tp2 - tp1).count();
     t_regrid += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0c).count();
   }
 
@@ -1902,7 +1921,8 @@ int amrgpu_info(amrgpu_ctx* ctx, double* out, int n) {
     amrb::Amr2Gpu& s = *ctx->s2;
     const double v[] = {s.time, s.rvol, (double)s.ncycle, (double)s.lfine, s.t_step, s.t_regrid, s.tmass0,
                         s.cflmax_run, (double)s.nkernels, (double)s.pool.peak * 8.0, (double)s.nsteps_launched,
-                        s.step_kernel_ms, s.step_kernel_cells, s.last_run_ms, s.run_cells, s.finished() ? 1.0 : 0.0, s.h2d_bytes};
+                        s.step_kernel_ms, s.step_kernel_cells, s.last_run_ms, s.run_cells, s.finished() ? 1.0 : 0.0, s.h2d_bytes,
+                        s.tr_flags, s.tr_host, s.tr_cluster, s.tr_fill, s.tr_prep, s.tr_compile};
     for (int k = 0; k < n && k < (int)(sizeof(v) / sizeof(v[0])); ++k) out[k] = v[k];
   });
 }

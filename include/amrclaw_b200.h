@@ -68,7 +68,9 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
  * launched, peak pool bytes, level substeps, patch-step kernel milliseconds
  * (profiling on), cells of those launches, device milliseconds of the last
  * amrgpu_run call, cell updates of that call, 1 when tfinal was reached,
- * bytes of initial data copied host to device. */
+ * bytes of initial data copied host to device, then regrid seconds spent in:
+ * device flagging, host flag processing, clustering, new-grid fill, register
+ * and list set-up, device-program compilation. */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 
 /* Hierarchy rows (grid_number, level, ilo, ihi, jlo, jhi) in output order
