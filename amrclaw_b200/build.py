@@ -13,6 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libamrgpu.so")
+BUILD = os.path.join(HERE, "_build")
 SOURCES = ["kernels2d.cu", "amr2d.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -35,12 +36,27 @@ def needs_build() -> bool:
     return os.path.exists(hdr) and os.path.getmtime(hdr) > t
 
 
+FLAGS = ["-std=c++17", "-O3", *ARCH, "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off"]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object (in parallel), then link the shared library."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc(), "-std=c++17", "-O3", *ARCH, "-lineinfo", "--fmad=false",
-           "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-o", LIB]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(BUILD, exist_ok=True)
+
+    def one(src: str) -> str:
+        obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), *FLAGS, "-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True, cwd=CSRC)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(one, SOURCES))
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=CSRC)

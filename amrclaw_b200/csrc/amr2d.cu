@@ -17,8 +17,13 @@
 #include "kernels2d.cuh"
 #include "params.hpp"
 #include "cluster2d.hpp"
+#include "gridindex.hpp"
+#include "workpool.hpp"
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -26,7 +31,28 @@
 
 namespace amrb {
 
-static const double RINF = (double)10.e32f;  // rinfinity of amr_module.f90 (a default-REAL literal)
+static const double RINF = (double)10.e32f;
+
+// Host-side section timers, printed at context destruction when AMRB_PROF is set.
+struct HostProf {
+  std::map<std::string, std::pair<double, long long>> acc;
+  bool on = std::getenv("AMRB_PROF") != nullptr;
+  ~HostProf() {
+    if (!on) return;
+    for (auto& kv : acc) std::fprintf(stderr, "PROF %-22s %9.4f s %8lld calls\n", kv.first.c_str(), kv.second.first, kv.second.second);
+  }
+};
+struct ScopedTimer {
+  HostProf& P; const char* name; std::chrono::steady_clock::time_point t0;
+  ScopedTimer(HostProf& p, const char* n) : P(p), name(n), t0(std::chrono::steady_clock::now()) {}
+  ~ScopedTimer() {
+    if (!P.on) return;
+    auto& a = P.acc[name];
+    a.first += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    a.second += 1;
+  }
+};
+#define HPROF(name) ScopedTimer _hp_##__LINE__(hprof, name)  // rinfinity of amr_module.f90 (a default-REAL literal)
 
 // ------------------------------------------------------------------ device pool
 struct Arena {
@@ -85,21 +111,48 @@ struct Arena {
   void destroy() { if (d) cudaFree(d); d = nullptr; }
 };
 
+// Pinned host staging for host-to-device uploads: a copy from pinned memory is
+// queued without the driver's pageable bounce. Space is reused only after the
+// stream has been synchronized (Staging::reset is called right after each sync).
+struct Staging {
+  char* h = nullptr;
+  size_t cap = 0, used = 0;
+  const void* put(const void* src, size_t n, cudaStream_t s) {
+    const size_t n2 = (n + 255) & ~(size_t)255;
+    if (used + n2 > cap) {
+      AMR_CUDA(cudaStreamSynchronize(s));
+      used = 0;
+      if (n2 > cap) {
+        if (h) AMR_CUDA(cudaFreeHost(h));
+        cap = std::max<size_t>({n2, cap * 2, (size_t)8 << 20});
+        AMR_CUDA(cudaMallocHost((void**)&h, cap));
+      }
+    }
+    char* dst = h + used;
+    std::memcpy(dst, src, n);
+    used += n2;
+    return dst;
+  }
+  void reset() { used = 0; }
+  void destroy() { if (h) cudaFreeHost(h); h = nullptr; cap = used = 0; }
+};
+
 template <class T> struct DBuf {
   T* d = nullptr; size_t cap = 0, n = 0;
-  void upload(const std::vector<T>& h, cudaStream_t s) {
-    n = h.size();
+  void upload(const std::vector<T>& h, cudaStream_t s, Staging& stg) { upload(h.data(), h.size(), s, stg); }
+  void upload(const T* h, size_t cnt, cudaStream_t s, Staging& stg) {
+    n = cnt;
     if (n > cap) {
       if (d) AMR_CUDA(cudaFree(d));
       cap = std::max<size_t>(n, 16) * 3 / 2;
       AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
     }
-    if (n) AMR_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(T) * n, cudaMemcpyHostToDevice, s));
+    if (n) AMR_CUDA(cudaMemcpyAsync(d, stg.put(h, sizeof(T) * n, s), sizeof(T) * n, cudaMemcpyHostToDevice, s));
   }
   void ensure(size_t m) {
     if (m > cap) {
       if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(m, 16);
+      cap = std::max<size_t>(m, 16) * 3 / 2;
       AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
     }
     n = m;
@@ -188,17 +241,28 @@ class Amr2Gpu {
   int lfine = 1;
   int lstart[12] = {0}, newstl[12] = {0}, listsp[12] = {0}, icheck[12] = {0};
   std::vector<int> lgrids[12];
+  GridIndex gidx[12];
+  bool gidx_ok[12] = {false};
   double hxposs[12] = {0}, hyposs[12] = {0}, possk[12] = {0};
   int iregsz[12] = {0}, jregsz[12] = {0};
   int intratx[12] = {0}, intraty[12] = {0}, kratio[12] = {0};
   // device
   Arena pool, regs;
+  Staging stg;
+  WorkPool pool_host;
+  HostProf hprof;
+  void sync_stream() { AMR_CUDA(cudaStreamSynchronize(st)); stg.reset(); }
   DBuf<PatchDev> d_patches;
   std::vector<PatchDev> h_patches;
+  int id_hwm = 1;  // 1 + largest patch id that ever held storage (descriptor table size)
   LevelPlan plan[12];
+  FillProg newfill;  // gfixup/filval program of the level being regridded
   unsigned long long* d_cfl = nullptr;
   double* d_mass = nullptr;
   DBuf<double> d_gauge_out;
+  DBuf<int8_t> fl_out;
+  DBuf<long long> fl_off;
+  DBuf<int> fl_pl;
   cudaStream_t st = nullptr;
   LevelConst lc{};
   // run state
@@ -233,8 +297,11 @@ class Amr2Gpu {
 
   ~Amr2Gpu() {
     for (int l = 0; l < 12; ++l) free_plan(l);
+    newfill.d_rects.free(); newfill.d_ops.free(); newfill.d_chunks.free(); newfill.d_bcs.free();
     pool.destroy(); regs.destroy();
-    d_patches.free(); d_gauge_out.free();
+    if (st) cudaStreamSynchronize(st);
+    stg.destroy();
+    d_patches.free(); d_gauge_out.free(); fl_out.free(); fl_off.free(); fl_pl.free();
     if (d_cfl) cudaFree(d_cfl);
     if (d_mass) cudaFree(d_mass);
     for (cudaEvent_t e : {ev_a, ev_b, ev_run0, ev_run1}) if (e) cudaEventDestroy(e);
@@ -335,6 +402,7 @@ class Amr2Gpu {
   int mjtot(int m) const { return node[m].ny() + 2 * ng; }
 
   void alloc_patch(int m) {
+    id_hwm = std::max(id_hwm, m + 1);
     HPatch& g = node[m];
     g.nq = (long long)nvar * mitot(m) * mjtot(m);
     g.q0 = pool.alloc(g.nq);
@@ -351,7 +419,8 @@ class Amr2Gpu {
   long long qcur(int m) const { return node[m].cur ? node[m].q1 : node[m].q0; }
 
   void sync_descriptors() {
-    h_patches.assign(node.size(), PatchDev{});
+    HPROF("sync_descriptors");
+    h_patches.assign(id_hwm, PatchDev{});
     for (int lev = 1; lev <= lfine; ++lev)
       for (int m : lgrids[lev]) {
         const HPatch& g = node[m];
@@ -361,7 +430,7 @@ class Amr2Gpu {
         d.mitot = mitot(m); d.mjtot = mjtot(m); d.mktot = 1;
         d.level = g.level; d.lenbc = g.lenbc;
       }
-    d_patches.upload(h_patches, st);
+    d_patches.upload(h_patches, st, stg);
   }
 
   // ================================================================ level lists
@@ -372,18 +441,28 @@ class Amr2Gpu {
       for (int m = lstart[lev]; m != 0; m = node[m].levelptr) lgrids[lev].push_back(m);
     }
   }
+  // Index of the committed patches of a level (the list from lstart), rebuilt after touch(lev).
+  void touch(int lev) { gidx_ok[lev] = false; }
+  const GridIndex& GI(int lev) {
+    if (!gidx_ok[lev]) {
+      std::vector<int> l;
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) l.push_back(m);
+      gidx[lev].build(l, [&](int m) { const HPatch& g = node[m]; return std::array<int, 6>{g.ilo, g.ihi, g.jlo, g.jhi, 0, 0}; });
+      gidx_ok[lev] = true;
+    }
+    return gidx[lev];
+  }
   // init_bndryList.f:50-107: same-level neighbours touching the ghost region, most recent first
   void make_bndry(int lev) {
-    const auto& G = lgrids[lev];
-    for (size_t n = 0; n < G.size(); ++n) {
-      HPatch& g = node[G[n]];
+    HPROF("make_bndry");
+    const GridIndex& X = GI(lev);
+    std::vector<int> hits;
+    for (int m : lgrids[lev]) {
+      HPatch& g = node[m];
       g.bnd.clear();
-      for (size_t k = G.size(); k-- > 0;) {
-        if (k == n) continue;
-        const HPatch& s = node[G[k]];
-        if (std::max(s.ilo, g.ilo - ng) <= std::min(s.ihi, g.ihi + ng) && std::max(s.jlo, g.jlo - ng) <= std::min(s.jhi, g.jhi + ng))
-          g.bnd.push_back(G[k]);
-      }
+      X.query2(g.ilo - ng, g.ihi + ng, g.jlo - ng, g.jhi + ng, hits);
+      for (size_t k = hits.size(); k-- > 0;)
+        if (X.id(hits[k]) != m) g.bnd.push_back(X.id(hits[k]));
     }
   }
   // regrid.f:132-169: order grids by cost, most expensive first, with quick_sort1.f tie breaking
@@ -400,6 +479,7 @@ class Amr2Gpu {
     int prev = lstart[lev];
     for (int i = 1; i <= n - 1; ++i) { node[prev].levelptr = gl[ord[n - i] - 1]; prev = node[prev].levelptr; }
     node[prev].levelptr = 0;
+    touch(lev);
   }
   // birect.f:10-120: split patches wider than max1d
   void birect(int m1) {
@@ -488,7 +568,15 @@ class Amr2Gpu {
     std::vector<int8_t> used((size_t)ni * nj, 0);
     std::vector<FillOp> copies;
     // intfil.f90:153-260
-    const std::vector<int>& src = (msrc == -1) ? lgrids[level] : node[msrc].bnd;
+    std::vector<int> src;
+    if (msrc == -1) {
+      const GridIndex& X = GI(level);
+      std::vector<int> hits;
+      X.query2(ilo, ihi, jlo, jhi, hits);
+      for (int r : hits) src.push_back(X.id(r));
+    } else {
+      src = node[msrc].bnd;
+    }
     for (int m : src) {
       const HPatch& g = node[m];
       const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi), jxlo = std::max(g.jlo, jlo), jxhi = std::min(g.jhi, jhi);
@@ -575,11 +663,42 @@ class Amr2Gpu {
     return done;
   }
 
+  // Appends program S after the ops already in D (rect indices and scratch offsets shifted).
+  static void merge_prog(FillProg& D, const FillProg& S) {
+    const int r0 = (int)D.rects.size();
+    const long long s0 = D.scratch_len;
+    for (ScratchRect r : S.rects) { r.off += s0; D.rects.push_back(r); }
+    D.scratch_len += S.scratch_len;
+    for (size_t k = 0; k < S.ops.size(); ++k) {
+      FillOp o = S.ops[k];
+      if (o.dst_patch < 0) o.dst_rect += r0;
+      if (o.kind != FILL_COPY) o.src += r0;
+      D.add_op(o, S.op_stage[k]);
+    }
+    for (size_t k = 0; k < S.bcs.size(); ++k) {
+      BcOp b = S.bcs[k];
+      if (b.dst_patch < 0) b.dst_rect += r0;
+      D.add_bc(b, S.bc_stage[k]);
+    }
+  }
+
+  // bound.f90:51-158 for every patch of the level: compiled per patch on the host
+  // threads, then joined in level order.
   void compile_bound(int lev) {
+    HPROF("compile_bound");
     FillProg& P = plan[lev].bound;
     P.clear();
     P.scratch_len = 0;
-    for (int m : lgrids[lev]) {
+    for (int l = 1; l <= lev; ++l) GI(l);
+    const std::vector<int>& G = lgrids[lev];
+    std::vector<FillProg> part(G.size());
+    pool_host.run((int)G.size(), [&](int k) { compile_bound_patch(part[k], lev, G[k]); });
+    for (auto& q : part) merge_prog(P, q);
+    upload_prog(P);
+  }
+  void compile_bound_patch(FillProg& P, int lev, int m) {
+    P.scratch_len = 0;
+    {
       const HPatch& g = node[m];
       const double hx = hxposs[lev], hy = hyposs[lev];
       Tgt T{m, -1, mitot(m), mjtot(m)};
@@ -603,12 +722,15 @@ class Amr2Gpu {
       BcOp b = make_bc(T, hx, hy, g.xlo - ng * hx, g.xhi + ng * hx, g.ylo - ng * hy, g.yhi + ng * hy, any);
       if (any) P.add_bc(b, s);
     }
-    upload_prog(P);
   }
 
   // icall.f / preicall.f: copies of store1 of every grid at `level` into a rect
   void c_icall(FillProg& P, Tgt T, int ilo, int ihi, int jlo, int jhi, int level, int iput, int jput, int st_) {
-    for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+    const GridIndex& X = GI(level);
+    std::vector<int> hits;
+    X.query2(ilo, ihi, jlo, jhi, hits);
+    for (int r : hits) {
+      const int m = X.id(r);
       const HPatch& g = node[m];
       const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi), jxlo = std::max(g.jlo, jlo), jxhi = std::min(g.jhi, jhi);
       if (!(ixlo <= ixhi && jxlo <= jxhi)) continue;
@@ -638,6 +760,7 @@ class Amr2Gpu {
 
   // saveqc.f:13-109 for the kids at level lev+1
   void compile_saveqc(int lev) {
+    HPROF("compile_saveqc");
     FillProg& P = plan[lev].saveqc;
     P.clear();
     P.scratch_len = 0;
@@ -664,12 +787,13 @@ class Amr2Gpu {
   }
 
   void upload_prog(FillProg& P) {
+    HPROF("upload_prog");
     if (P.scratch_off >= 0) pool.release(P.scratch_off, P.scratch_alloc);
     P.scratch_alloc = std::max<long long>(P.scratch_len, 1);
     P.scratch_off = pool.alloc(P.scratch_alloc);
     std::vector<ScratchRect> rects = P.rects;
     for (auto& r : rects) r.off += P.scratch_off;
-    P.d_rects.upload(rects, st);
+    P.d_rects.upload(rects, st, stg);
     // order ops and bcs by stage; chunks of <= 128 cells
     std::vector<int> oidx(P.ops.size());
     for (size_t i = 0; i < oidx.size(); ++i) oidx[i] = (int)i;
@@ -701,9 +825,9 @@ class Amr2Gpu {
       P.bc_hi[s] = (int)bcs.size();
     }
     while (s + 1 < P.nstages) { ++s; P.bc_lo[s] = P.bc_hi[s] = (int)bcs.size(); }
-    P.d_ops.upload(ops, st);
-    P.d_chunks.upload(ch, st);
-    P.d_bcs.upload(bcs, st);
+    P.d_ops.upload(ops, st, stg);
+    P.d_chunks.upload(ch, st, stg);
+    P.d_bcs.upload(bcs, st, stg);
   }
 
   void run_prog(FillProg& P, const SrcMode& modes) {
@@ -729,6 +853,7 @@ class Amr2Gpu {
 
   // ================================================================ step work, registers, update plans
   void compile_step(int lev) {
+    HPROF("compile_step");
     LevelPlan& L = plan[lev];
     L.work.clear(); L.fsv.clear(); L.fad.clear(); L.patch_work_lo.clear(); L.patch_work_hi.clear(); L.qad.clear();
     L.plist = lgrids[lev];
@@ -739,7 +864,7 @@ class Amr2Gpu {
       std::vector<std::vector<FsvEntry>> tf(ntx * nty);
       std::vector<std::vector<FadEntry>> ta(ntx * nty);
       if (g.has_cfl) {
-        for (int sp_ = 1; sp_ <= listsp[lev]; ++sp_) {
+        for (int sp_ = 1; sp_ <= (int)g.listbc.size() / 5; ++sp_) {
           const int* e = &g.listbc[5 * (sp_ - 1)];
           if (e[0] == 0) break;
           FsvEntry f{};
@@ -777,79 +902,110 @@ class Amr2Gpu {
         }
       L.patch_work_hi.push_back((int)L.work.size());
     }
-    L.d_work.upload(L.work, st);
-    L.d_fsv.upload(L.fsv, st);
-    L.d_fad.upload(L.fad, st);
-    L.d_qad.upload(L.qad, st);
-    L.d_plist.upload(L.plist, st);
+    L.d_work.upload(L.work, st, stg);
+    L.d_fsv.upload(L.fsv, st, stg);
+    L.d_fad.upload(L.fad, st, stg);
+    L.d_qad.upload(L.qad, st, stg);
+    L.d_plist.upload(L.plist, st, stg);
   }
 
   // update.f:16-189 + upbnd.f:18-127 for coarse level lev
   void compile_update(int lev) {
+    HPROF("compile_update");
     LevelPlan& L = plan[lev];
     L.upc.clear(); L.upt.clear(); L.avg.clear();
-    if (lev >= p.mxnest) { L.d_upc.upload(L.upc, st); L.d_upt.upload(L.upt, st); L.d_avg.upload(L.avg, st); return; }
-    for (int m : lgrids[lev]) {
-      const HPatch& g = node[m];
-      if (g.has_cfl) {
-        std::map<std::pair<int, int>, std::vector<UpbndTerm>> cells;
-        std::vector<std::pair<int, int>> order;
-        std::map<std::pair<int, int>, int> iused;
-        for (int s = 1; s <= listsp[lev]; ++s) {
-          const int* e = &g.listbc[5 * (s - 1)];
-          if (e[0] == 0) break;
-          const int side = e[2];
-          const int side1 = side < 5 ? side : (side == 5 ? 2 : 4);
-          const int norm = 1 << (side1 - 1);
-          auto key = std::make_pair(e[0], e[1]);
-          int& used = iused[key];
-          if ((used / norm) % 2 == 1) continue;
-          const double sgn = (side == 2 || side == 3 || side == 6) ? -1.0 : 1.0;
-          if (!cells.count(key)) order.push_back(key);
-          cells[key].push_back(UpbndTerm{node[e[3]].ffl + (long long)nvar * (e[4] - 1), sgn});
-          used += norm;
-        }
-        for (auto& k : order) {
-          UpbndCell c{};
-          c.patch = m; c.ie = k.first - 1; c.je = k.second - 1;
-          c.first = (int)L.upt.size(); c.count = (int)cells[k].size();
-          L.upt.insert(L.upt.end(), cells[k].begin(), cells[k].end());
-          L.upc.push_back(c);
-        }
+    if (lev >= p.mxnest) { L.d_upc.upload(L.upc, st, stg); L.d_upt.upload(L.upt, st, stg); L.d_avg.upload(L.avg, st, stg); return; }
+    GI(lev + 1);
+    const std::vector<int>& G = lgrids[lev];
+    struct Part { std::vector<UpbndCell> upc; std::vector<UpbndTerm> upt; std::vector<AvgRect> avg; };
+    std::vector<Part> part(G.size());
+    pool_host.run((int)G.size(), [&](int k) { compile_update_patch(lev, G[k], part[k].upc, part[k].upt, part[k].avg); });
+    for (auto& q : part) {
+      const int base = (int)L.upt.size();
+      for (UpbndCell c : q.upc) { c.first += base; L.upc.push_back(c); }
+      L.upt.insert(L.upt.end(), q.upt.begin(), q.upt.end());
+      L.avg.insert(L.avg.end(), q.avg.begin(), q.avg.end());
+    }
+    L.d_upc.upload(L.upc, st, stg); L.d_upt.upload(L.upt, st, stg); L.d_avg.upload(L.avg, st, stg);
+  }
+  // upbnd.f:62-124 cells (one term per side not yet used, in listbc order) and
+  // update.f:95-175 overlap rectangles of coarse patch m
+  void compile_update_patch(int lev, int m, std::vector<UpbndCell>& upc, std::vector<UpbndTerm>& upt, std::vector<AvgRect>& avg) {
+    const GridIndex& XF = gidx[lev + 1];
+    std::vector<int> hits;
+    const HPatch& g = node[m];
+    if (g.has_cfl) {
+      const int mi = mitot(m), mj = mjtot(m);
+      std::vector<int> used((size_t)mi * mj, 0), slot((size_t)mi * mj, -1), order;
+      std::vector<std::vector<UpbndTerm>> terms;
+      for (int s = 1; s <= (int)g.listbc.size() / 5; ++s) {
+        const int* e = &g.listbc[5 * (s - 1)];
+        if (e[0] == 0) break;
+        const int side = e[2];
+        const int side1 = side < 5 ? side : (side == 5 ? 2 : 4);
+        const int norm = 1 << (side1 - 1);
+        const size_t key = (size_t)(e[1] - 1) * mi + (e[0] - 1);
+        if ((used[key] / norm) % 2 == 1) continue;
+        const double sgn = (side == 2 || side == 3 || side == 6) ? -1.0 : 1.0;
+        if (slot[key] < 0) { slot[key] = (int)terms.size(); terms.emplace_back(); order.push_back((int)key); }
+        terms[slot[key]].push_back(UpbndTerm{node[e[3]].ffl + (long long)nvar * (e[4] - 1), sgn});
+        used[key] += norm;
       }
-      for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
-        const HPatch& f = node[k];
-        const int rx = intratx[lev], ry = intraty[lev];
-        const int iclo = f.ilo / rx, jclo = f.jlo / ry, ichi = f.ihi / rx, jchi = f.jhi / ry;
-        const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi);
-        if (iplo > iphi || jplo > jphi) continue;
-        AvgRect a{};
-        a.cpatch = m; a.kpatch = k;
-        a.ci0 = iplo - g.ilo + ng; a.cj0 = jplo - g.jlo + ng; a.ni = iphi - iplo + 1; a.nj = jphi - jplo + 1;
-        a.fi0 = iplo * rx - f.ilo + ng; a.fj0 = jplo * ry - f.jlo + ng;
-        L.avg.push_back(a);
+      for (int key : order) {
+        UpbndCell c{};
+        c.patch = m; c.ie = key % mi; c.je = key / mi;
+        const auto& T = terms[slot[key]];
+        c.first = (int)upt.size(); c.count = (int)T.size();
+        upt.insert(upt.end(), T.begin(), T.end());
+        upc.push_back(c);
       }
     }
-    L.d_upc.upload(L.upc, st); L.d_upt.upload(L.upt, st); L.d_avg.upload(L.avg, st);
+    const int rx = intratx[lev], ry = intraty[lev];
+    XF.query2(g.ilo * rx, g.ihi * rx + rx - 1, g.jlo * ry, g.jhi * ry + ry - 1, hits);
+    for (int r : hits) {
+      const int k = XF.id(r);
+      const HPatch& f = node[k];
+      const int iclo = f.ilo / rx, jclo = f.jlo / ry, ichi = f.ihi / rx, jchi = f.jhi / ry;
+      const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi);
+      if (iplo > iphi || jplo > jphi) continue;
+      AvgRect a{};
+      a.cpatch = m; a.kpatch = k;
+      a.ci0 = iplo - g.ilo + ng; a.cj0 = jplo - g.jlo + ng; a.ni = iphi - iplo + 1; a.nj = jphi - jplo + 1;
+      a.fi0 = iplo * rx - f.ilo + ng; a.fj0 = jplo * ry - f.jlo + ng;
+      avg.push_back(a);
+    }
   }
 
   // prepf.f / prepc.f / setuse.f
   void prepf(int lev) {
+    HPROF("prepf");
+    std::vector<std::pair<long long, long long>> zr;
     for (int k = lstart[lev]; k != 0; k = node[k].levelptr) {
       HPatch& g = node[k];
       g.lenbc = 2 * (g.nx() / intratx[lev - 1] + g.ny() / intraty[lev - 1]);
       if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
       g.nffl = (long long)2 * nvar * g.lenbc;
       g.ffl = regs.alloc(g.nffl);
-      AMR_CUDA(cudaMemsetAsync(regs.d + g.ffl, 0, sizeof(double) * g.nffl, st));
+      zr.emplace_back(g.ffl, Arena::rnd(g.nffl));
+    }
+    zero_ranges(regs.d, zr);
+  }
+  // one cudaMemsetAsync per run of adjacent ranges
+  void zero_ranges(double* base, std::vector<std::pair<long long, long long>>& zr) {
+    std::sort(zr.begin(), zr.end());
+    for (size_t a = 0; a < zr.size();) {
+      long long lo = zr[a].first, hi = zr[a].first + zr[a].second;
+      size_t b = a + 1;
+      while (b < zr.size() && zr[b].first <= hi) { hi = std::max(hi, zr[b].first + zr[b].second); ++b; }
+      AMR_CUDA(cudaMemsetAsync(base + lo, 0, sizeof(double) * (hi - lo), st));
+      a = b;
     }
   }
   static void setuse(std::vector<int>& lb, int& ispot, int mkid, int ilo, int ihi, int jlo, int jhi, int iclo, int ichi,
                      int jclo, int jchi, int ngh) {
     auto put = [&](int i, int j, int side, int lkid) {
       ++ispot;
-      int* e = &lb[5 * (ispot - 1)];
-      e[0] = i; e[1] = j; e[2] = side; e[3] = mkid; e[4] = lkid;
+      lb.insert(lb.end(), {i, j, side, mkid, lkid});
     };
     const int ist = iclo - 1, iend = ichi + 1, jst = jclo - 1, jend = jchi + 1;
     if (!(ist < ilo)) {
@@ -870,18 +1026,27 @@ class Amr2Gpu {
     }
   }
   void prepc(int lev) {
+    HPROF("prepc");
     int maxsp = 0;
     for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr)
       maxsp += 2 * (node[k].nx() / intratx[lev] + node[k].ny() / intraty[lev]);
     listsp[lev] = maxsp;
     if (maxsp == 0) return;
     const int imax = iregsz[lev] - 1, jmax = jregsz[lev] - 1;
+    const GridIndex& XF = GI(lev + 1);
+    std::vector<int> hits;
+    const int rx = intratx[lev], ry = intraty[lev];
     for (int mp = lstart[lev]; mp != 0; mp = node[mp].levelptr) {
       HPatch& g = node[mp];
       int ispot = 0;
-      g.listbc.assign((size_t)5 * maxsp, 0);
+      g.listbc.clear();  // only the entries setuse makes (the reference reserves 5*maxsp per patch)
       g.has_cfl = true;
-      for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
+      // kids within one coarse cell of the patch; periodic images can come from anywhere
+      const bool wrap = (xperdom && (g.ilo == 0 || g.ihi == imax)) || (yperdom && (g.jlo == 0 || g.jhi == jmax));
+      if (wrap) { hits.resize(XF.size()); for (size_t r = 0; r < hits.size(); ++r) hits[r] = (int)r; }
+      else XF.query2((g.ilo - 1) * rx, (g.ihi + 2) * rx - 1, (g.jlo - 1) * ry, (g.jhi + 2) * ry - 1, hits);
+      for (int r : hits) {
+        const int k = XF.id(r);
         const HPatch& f = node[k];
         const int iclo = f.ilo / intratx[lev], jclo = f.jlo / intraty[lev], ichi = f.ihi / intratx[lev], jchi = f.jhi / intraty[lev];
         const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi);
@@ -951,6 +1116,7 @@ class Amr2Gpu {
 
   // ================================================================ level substep (advanc.f:10-142)
   double advanc(int lev) {
+    HPROF("advanc");
     LevelPlan& L = plan[lev];
     const double t = node[lgrids[lev][0]].time;
     const double dt = possk[lev];
@@ -987,9 +1153,9 @@ class Amr2Gpu {
           if (d_gauge_out.d) AMR_CUDA(cudaMemcpyAsync(nb.d, d_gauge_out.d, sizeof(double) * d_gauge_out.cap, cudaMemcpyDeviceToDevice, st));
           d_gauge_out.free(); d_gauge_out = nb;
         }
-        DBuf<GaugeJob> dj; dj.upload(jobs, st);
+        DBuf<GaugeJob> dj; dj.upload(jobs, st, stg);
         launch_gauges2(pool.d, d_patches.d, dj.d, (int)jobs.size(), nvar, d_gauge_out.d, st);
-        AMR_CUDA(cudaStreamSynchronize(st));
+        sync_stream();
         dj.free();
       }
     }
@@ -1017,7 +1183,10 @@ class Amr2Gpu {
     ++nkernels;
     unsigned long long cbits = 0;
     AMR_CUDA(cudaMemcpyAsync(&cbits, d_cfl, sizeof(cbits), cudaMemcpyDeviceToHost, st));
-    AMR_CUDA(cudaStreamSynchronize(st));
+    {
+      HPROF("advanc_sync");
+      sync_stream();
+    }
     double cmax;
     std::memcpy(&cmax, &cbits, sizeof(double));
     if (profile) {
@@ -1039,6 +1208,7 @@ class Amr2Gpu {
   }
 
   void update(int lev) {
+    HPROF("update");
     LevelPlan& L = plan[lev];
     const double area = hxposs[lev] * hyposs[lev];
     launch_upbnd(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, area, nvar, st);
@@ -1085,8 +1255,15 @@ class Amr2Gpu {
     }
     IBox B{gs[lbase], ge[lbase], hs[lbase], he[lbase], mbuff};
     std::vector<int8_t> base((size_t)B.ni() * B.nj(), 0);
-    for (int mb = lstart[lbase]; mb != 0; mb = node[mb].levelptr) {
-      const HPatch& b = node[mb];
+    const GridIndex& XB = GI(lbase);
+    std::vector<int> hits;
+    {
+      const bool bx = (B.ilo <= 0 || B.ihi >= iregsz[lbase] - 1), by = (B.jlo <= 0 || B.jhi >= jregsz[lbase] - 1);
+      if ((xperdom && bx) || (yperdom && by)) { hits.resize(XB.size()); for (size_t r = 0; r < hits.size(); ++r) hits[r] = (int)r; }
+      else XB.query2(B.ilo - mbuff, B.ihi + mbuff, B.jlo - mbuff, B.jhi + mbuff, hits);
+    }
+    for (int r : hits) {
+      const HPatch& b = node[XB.id(r)];
       const bool bx = (B.ilo <= 0 || B.ihi >= iregsz[lbase] - 1), by = (B.jlo <= 0 || B.jhi >= jregsz[lbase] - 1);
       if ((xperdom && bx) || (yperdom && by)) {
         int ist[3], iend[3], jst[3], jend[3], ish[3], jsh[3];
@@ -1141,6 +1318,7 @@ class Amr2Gpu {
   }
 
   bool base_check(const HPatch& n, int lbase, int thisBuff) {
+    HPROF("base_check");
     const int levnew = n.level;
     const bool bx = (n.ilo == 0 || n.ihi == iregsz[levnew] - 1), by = (n.jlo == 0 || n.jhi == jregsz[levnew] - 1);
     int iclo = n.ilo, ichi = n.ihi, jclo = n.jlo, jchi = n.jhi;
@@ -1157,7 +1335,12 @@ class Amr2Gpu {
     if (n.ihi == iregsz[levnew] - 1 && !xperdom) for (int j = jclo; j <= jchi; ++j) { at(ichi, j) = 1; at(ichi - 1, j) = 1; }
     if (n.jlo == 0 && !yperdom) for (int i = iclo; i <= ichi; ++i) { at(i, jclo) = 1; at(i, jclo + 1) = 1; }
     if (n.jhi == jregsz[levnew] - 1 && !yperdom) for (int i = iclo; i <= ichi; ++i) { at(i, jchi) = 1; at(i, jchi - 1) = 1; }
-    for (int mp = lstart[lbase]; mp != 0; mp = node[mp].levelptr) {
+    const GridIndex& XB = GI(lbase);
+    std::vector<int> hits;
+    if ((xperdom && bx) || (yperdom && by)) { hits.resize(XB.size()); for (size_t r = 0; r < hits.size(); ++r) hits[r] = (int)r; }
+    else XB.query2(iclo - thisBuff, ichi + thisBuff, jclo - thisBuff, jchi + thisBuff, hits);
+    for (int r : hits) {
+      const int mp = XB.id(r);
       const int iblo = node[mp].ilo - thisBuff, ibhi = node[mp].ihi + thisBuff, jblo = node[mp].jlo - thisBuff, jbhi = node[mp].jhi + thisBuff;
       if (!(xperdom && bx) && !(yperdom && by)) {
         const int a = std::max(iclo, iblo), b = std::min(ichi, ibhi), c = std::max(jclo, jblo), d = std::min(jchi, jbhi);
@@ -1186,32 +1369,56 @@ class Amr2Gpu {
     std::vector<int>& G = lgrids[lcheck];
     const double t = node[G[0]].time;
     int use_old = 0;
-    if (start_time + possk[lcheck] != t) bound_level(lcheck, t);
-    else use_old = 1;
+    {
+      HPROF("flag_bound");
+      if (start_time + possk[lcheck] != t) bound_level(lcheck, t);
+      else use_old = 1;
+    }
     // device gradient test
     const auto tf0 = std::chrono::steady_clock::now();
     std::vector<long long> off(G.size() + 1, 0);
     for (size_t k = 0; k < G.size(); ++k) off[k + 1] = off[k] + (long long)node[G[k]].nx() * node[G[k]].ny();
-    DBuf<int8_t> dout; dout.ensure(std::max<long long>(off.back(), 1));
-    DBuf<long long> doff; doff.upload(off, st);
-    DBuf<int> dpl; dpl.upload(G, st);
+    DBuf<int8_t>& dout = fl_out; dout.ensure(std::max<long long>(off.back(), 1));
+    DBuf<long long>& doff = fl_off; doff.upload(off, st, stg);
+    DBuf<int>& dpl = fl_pl; dpl.upload(G, st, stg);
     launch_flags2(pool.d, d_patches.d, dpl.d, doff.d, (int)G.size(), use_old, p.flag_component, p.tolsp, nvar, dout.d, st);
     std::vector<int8_t> hflag(off.back());
     if (off.back()) AMR_CUDA(cudaMemcpyAsync(hflag.data(), dout.d, off.back(), cudaMemcpyDeviceToHost, st));
-    AMR_CUDA(cudaStreamSynchronize(st));
-    dout.free(); doff.free(); dpl.free();
+    sync_stream();
     const auto tf1 = std::chrono::steady_clock::now();
     tr_flags += std::chrono::duration<double>(tf1 - tf0).count();
     const double dx = hxposs[lcheck], dy = hyposs[lcheck];
     std::vector<Pt> pts;
     int numbad = 0;
-    for (size_t k = 0; k < G.size(); ++k) {
+    // projec2.f boxes of the level lcheck+2 grids just created, indexed; wrapping ones are tried on every patch
+    std::vector<int> pnew, pwrap;
+    GridIndex XP;
+    if (lcheck + 2 <= p.mxnest) {
+      std::vector<std::array<int, 6>> pb;
+      for (int mk = newstl[lcheck + 2]; mk != 0; mk = node[mk].levelptr) {
+        const HPatch& c = node[mk];
+        const int istc = (c.ilo / intratx[lcheck + 1] - 1) / intratx[lcheck] - 1, jstc = (c.jlo / intraty[lcheck + 1] - 1) / intraty[lcheck] - 1;
+        const int iendc = (c.ihi / intratx[lcheck + 1] + 1) / intratx[lcheck] + 1, jendc = (c.jhi / intraty[lcheck + 1] + 1) / intraty[lcheck] + 1;
+        const bool bx = (istc <= 0 || iendc >= iregsz[lcheck] - 1), by = (jstc <= 0 || jendc >= jregsz[lcheck] - 1);
+        if ((xperdom && bx) || (yperdom && by)) pwrap.push_back(mk);
+        else { pnew.push_back(mk); pb.push_back({istc, iendc, jstc, jendc, 0, 0}); }
+      }
+      std::vector<int> ids(pb.size());
+      for (size_t r = 0; r < ids.size(); ++r) ids[r] = (int)r;
+      XP.build(ids, [&](int r) { return pb[r]; });
+    }
+    GI(lbase);  // built here: the per-patch work below only reads the index
+    std::vector<std::vector<Pt>> ptsp(G.size());
+    ScopedTimer tpp(hprof, "flag_patches");
+    pool_host.run((int)G.size(), [&](int k) {
       HPatch& g = node[G[k]];
       const int mx = g.nx(), my = g.ny();
       IBox B{g.ilo, g.ihi, g.jlo, g.jhi, mbuff};
       std::vector<int8_t> f((size_t)B.ni() * B.nj(), FLAG_UNSET);
+      std::vector<int> phits;
       // flagregions2.f90
-      std::vector<int> mnl((size_t)mx * my, 0), mxl((size_t)mx * my, 0);
+      std::vector<int> mnl, mxl;
+      if (!p.regions.empty()) { mnl.assign((size_t)mx * my, 0); mxl.assign((size_t)mx * my, 0); }
       const double xu = g.xlo + mx * dx, yu = g.ylo + my * dy;
       for (const RegionSpec& r : p.regions) {
         if (t < r.t1 || t > r.t2) continue;
@@ -1227,7 +1434,7 @@ class Amr2Gpu {
       const int8_t* gf = hflag.data() + off[k];
       for (int j = 1; j <= my; ++j)
         for (int i = 1; i <= mx; ++i) {
-          const int a = mnl[(size_t)(j - 1) * mx + i - 1], b = mxl[(size_t)(j - 1) * mx + i - 1];
+          const int a = mnl.empty() ? 0 : mnl[(size_t)(j - 1) * mx + i - 1], b = mxl.empty() ? 0 : mxl[(size_t)(j - 1) * mx + i - 1];
           if (a > b) throw std::runtime_error("region minimum level exceeds its maximum level");
           int8_t v = FLAG_UNSET;
           if (b != 0) { if (lcheck < a) v = FLAG_DO; else if (lcheck >= b) v = FLAG_DONT; }
@@ -1236,7 +1443,11 @@ class Amr2Gpu {
         }
       // projec2.f: cells under level lcheck+2 grids just created
       if (lcheck + 2 <= p.mxnest) {
-        for (int mk = newstl[lcheck + 2]; mk != 0; mk = node[mk].levelptr) {
+        std::vector<int> cand;
+        XP.query2(g.ilo - mbuff, g.ihi + mbuff, g.jlo - mbuff, g.jhi + mbuff, phits);
+        for (int r : phits) cand.push_back(pnew[r]);
+        cand.insert(cand.end(), pwrap.begin(), pwrap.end());
+        for (int mk : cand) {
           const HPatch& c = node[mk];
           int istc = (c.ilo / intratx[lcheck + 1] - 1) / intratx[lcheck] - 1, jstc = (c.jlo / intraty[lcheck + 1] - 1) / intraty[lcheck] - 1;
           int iendc = (c.ihi / intratx[lcheck + 1] + 1) / intratx[lcheck] + 1, jendc = (c.jhi / intraty[lcheck + 1] + 1) / intraty[lcheck] + 1;
@@ -1260,41 +1471,48 @@ class Amr2Gpu {
         }
       }
       // shiftset2.f: buffer by ibuff in every direction
-      std::vector<int8_t> buf((size_t)B.ni() * B.nj(), FLAG_DONT);
+      // Only "flagged or not" survives buffering (colate2 tests > DONTFLAG), so the
+      // (2*ibuff+1)^2 stamp is applied as a row pass and a column pass.
+      std::vector<int8_t> row((size_t)B.ni() * B.nj(), 0), buf((size_t)B.ni() * B.nj(), FLAG_DONT);
       for (int j = g.jlo; j <= g.jhi; ++j)
-        for (int i = g.ilo; i <= g.ihi; ++i) {
-          const int8_t r = f[B.idx(i, j)];
-          if (r > 0) for (int kk = j - p.ibuff; kk <= j + p.ibuff; ++kk) for (int mm = i - p.ibuff; mm <= i + p.ibuff; ++mm) buf[B.idx(mm, kk)] = r;
-        }
+        for (int i = g.ilo; i <= g.ihi; ++i)
+          if (f[B.idx(i, j)] > 0) for (int mm = i - p.ibuff; mm <= i + p.ibuff; ++mm) row[B.idx(mm, j)] = 1;
+      for (int j = g.jlo; j <= g.jhi; ++j)
+        for (int i = g.ilo - p.ibuff; i <= g.ihi + p.ibuff; ++i)
+          if (row[B.idx(i, j)]) for (int kk = j - p.ibuff; kk <= j + p.ibuff; ++kk) buf[B.idx(i, kk)] = FLAG_DO;
       int nf = 0;
       for (int8_t v : buf) if (v > FLAG_DONT) ++nf;
       g.numflags = nf;
-      numbad += nf;
-      g.flags.swap(buf);
-      g.dom2 = nesting_mask(g, mbuff, lbase, lcheck);
-    }
-    if (numbad == 0) { for (int m : G) { node[m].flags.clear(); node[m].dom2.clear(); } return pts; }
-    // colate2.f: nested flags with periodic wrap, in grid-list order
-    for (int m = lstart[lcheck]; m != 0; m = node[m].levelptr) {
-      HPatch& g = node[m];
-      if (g.numflags != 0) {
-        IBox B{g.ilo, g.ihi, g.jlo, g.jhi, mbuff};
+      // colate2.f: nested flags with periodic wrap (the point order is irrelevant:
+      // drivesort sorts them and drops duplicates)
+      std::vector<Pt>& out = ptsp[k];
+      out.clear();
+      if (nf != 0) {
+        const std::vector<int8_t> dom2 = nesting_mask(g, mbuff, lbase, lcheck);
         int jmin = g.jlo - mbuff, jmax = g.jhi + mbuff, imin = g.ilo - mbuff, imax = g.ihi + mbuff;
         if (!xperdom) { imin = std::max(imin, 0); imax = std::min(g.ihi + mbuff, iregsz[lcheck] - 1); }
         if (!yperdom) { jmin = std::max(jmin, 0); jmax = std::min(g.jhi + mbuff, jregsz[lcheck] - 1); }
-        for (int j = jmin; j <= jmax; ++j) for (int i = imin; i <= imax; ++i)
-          if (g.flags[B.idx(i, j)] > FLAG_DONT && g.dom2[B.idx(i, j)] != 1) g.flags[B.idx(i, j)] = FLAG_DONT;
-        for (int j = jmin; j <= jmax; ++j) for (int i = imin; i <= imax; ++i) {
-          if (g.flags[B.idx(i, j)] <= FLAG_DONT) continue;
-          int iw = i, jw = j;
-          if (xperdom) { if (i < 0) iw = i + iregsz[lcheck]; if (i >= iregsz[lcheck]) iw = i - iregsz[lcheck]; }
-          if (yperdom) { if (j < 0) jw = j + jregsz[lcheck]; if (j >= jregsz[lcheck]) jw = j - jregsz[lcheck]; }
-          pts.push_back(Pt{iw, jw});
-        }
+        for (int j = jmin; j <= jmax; ++j)
+          for (int i = imin; i <= imax; ++i) {
+            if (buf[B.idx(i, j)] <= FLAG_DONT || dom2[B.idx(i, j)] != 1) continue;
+            int iw = i, jw = j;
+            if (xperdom) { if (i < 0) iw = i + iregsz[lcheck]; if (i >= iregsz[lcheck]) iw = i - iregsz[lcheck]; }
+            if (yperdom) { if (j < 0) jw = j + jregsz[lcheck]; if (j >= jregsz[lcheck]) jw = j - jregsz[lcheck]; }
+            out.push_back(Pt{iw, jw});
+          }
       }
-      g.flags.clear(); g.dom2.clear();
+    });
+    for (int m : G) numbad += node[m].numflags;
+    ScopedTimer tcol(hprof, "colate");
+    if (numbad == 0) return pts;
+    size_t tot = 0;
+    for (size_t k = 0; k < G.size(); ++k) tot += ptsp[k].size();
+    pts.reserve(tot);
+    for (size_t k = 0; k < G.size(); ++k) pts.insert(pts.end(), ptsp[k].begin(), ptsp[k].end());
+    {
+      HPROF("sort_unique");
+      sort_unique(pts, iregsz[lcheck], mbuff);
     }
-    sort_unique(pts, iregsz[lcheck], mbuff);
     tr_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - tf1).count();
     if (std::getenv("AMRB_DEBUG")) {
       long long gsum = 0;
@@ -1314,7 +1532,10 @@ class Amr2Gpu {
     const double hxf = hxposs[levnew], hyf = hyposs[levnew];
     std::vector<int> cnt;
     const auto tc0 = std::chrono::steady_clock::now();
-    bisect(pts, p.cut, iregsz[lcheck], jregsz[lcheck], cnt);
+    {
+      HPROF("bisect");
+      bisect(pts, p.cut, iregsz[lcheck], jregsz[lcheck], cnt);
+    }
     int base = 0, icl = 0, prv = 0;
     while (icl < (int)cnt.size()) {
       const int mnew = nodget();
@@ -1365,11 +1586,30 @@ class Amr2Gpu {
 
   // filval.f90 for all new grids of level lev, then release the old grids (gfixup.f:49-163)
   void fill_new_level(int lev) {
-    FillProg P;
+    HPROF("fill_new_level");
+    FillProg& P = newfill;
+    P.clear();
+    P.rects.clear();
+    P.scratch_len = 0;
+    GI(lev - 1); GI(lev);
+    std::vector<int> nl;
+    for (int m = newstl[lev]; m != 0; m = node[m].levelptr) nl.push_back(m);
+    std::vector<FillProg> part(nl.size());
+    pool_host.run((int)nl.size(), [&](int k) { fill_new_patch(part[k], lev, nl[k]); });
+    for (auto& q : part) merge_prog(P, q);
+    upload_prog(P);
+    SrcMode M{};
+    run_prog(P, M);
+    sync_stream();
+    pool.release(P.scratch_off, P.scratch_alloc);
+    P.scratch_off = -1;
+  }
+  // filval.f90 for new patch m: coarse values around it, then copies from the old grids
+  void fill_new_patch(FillProg& P, int lev, int m) {
     P.scratch_len = 0;
     const int rx = intratx[lev - 1], ry = intraty[lev - 1];
     const double dxc = hxposs[lev] * rx, dyc = hyposs[lev] * ry;
-    for (int m = newstl[lev]; m != 0; m = node[m].levelptr) {
+    {
       const HPatch& g = node[m];
       const int iclo = g.ilo / rx - 1, jclo = g.jlo / ry - 1, ichi = (g.ihi + 1) / rx - 1 + 1, jchi = (g.jhi + 1) / ry - 1 + 1;
       const int mic = g.nx() / rx + 2, mjc = g.ny() / ry + 2;
@@ -1384,7 +1624,11 @@ class Amr2Gpu {
       // fine copies from the old grids of this level over the interior
       const int nx = g.nx(), ny = g.ny();
       std::vector<int8_t> cov((size_t)nx * ny, 0);
-      for (int o = lstart[lev]; o != 0; o = node[o].levelptr) {
+      const GridIndex& XO = GI(lev);
+      std::vector<int> hits;
+      XO.query2(g.ilo, g.ihi, g.jlo, g.jhi, hits);
+      for (int r : hits) {
+        const int o = XO.id(r);
         const HPatch& s = node[o];
         const int ixlo = std::max(s.ilo, g.ilo), ixhi = std::min(s.ihi, g.ihi), jxlo = std::max(s.jlo, g.jlo), jxhi = std::min(s.jhi, g.jhi);
         if (!(ixlo <= ixhi && jxlo <= jxhi)) continue;
@@ -1405,12 +1649,6 @@ class Amr2Gpu {
         P.add_op(o2, 1);
       }
     }
-    upload_prog(P);
-    SrcMode M{};
-    run_prog(P, M);
-    AMR_CUDA(cudaStreamSynchronize(st));
-    pool.release(P.scratch_off, P.scratch_alloc);
-    P.d_rects.free(); P.d_ops.free(); P.d_chunks.free(); P.d_bcs.free();
   }
 
   void regrid(int lbase) {
@@ -1448,6 +1686,7 @@ class Amr2Gpu {
         putnod(mold);
       }
       lstart[lcheck2] = newstl[lcheck2];
+      touch(lcheck2);
       lgrids[lcheck2].clear();
       for (int q = lstart[lcheck2]; q != 0; q = node[q].levelptr) lgrids[lcheck2].push_back(q);
     }
@@ -1460,7 +1699,10 @@ class Amr2Gpu {
     for (int lev = lbase + 1; lev <= lfine; ++lev) make_bndry(lev);
     const auto tp1 = std::chrono::steady_clock::now();
     compile_all(lbase);
-    AMR_CUDA(cudaStreamSynchronize(st));
+    {
+      HPROF("regrid_final_sync");
+      sync_stream();
+    }
     const auto tp2 = std::chrono::steady_clock::now();
     tr_prep += std::chrono::duration<double>(tp1 - tp0).count();
     tr_compile += std::chrono::duration<double>(tp2 - tp1).count();
@@ -1469,7 +1711,7 @@ class Amr2Gpu {
 
   // descriptors for: all current levels plus the old and new patches of level `lev` (during gfixup)
   void sync_descriptors_with(const std::vector<int>& old_lev_grids, int lev) {
-    h_patches.assign(node.size(), PatchDev{});
+    h_patches.assign(id_hwm, PatchDev{});
     auto put = [&](int m) {
       const HPatch& g = node[m];
       PatchDev& d = h_patches[m];
@@ -1480,7 +1722,7 @@ class Amr2Gpu {
     for (int l = 1; l <= p.mxnest; ++l) for (int m : lgrids[l]) put(m);
     for (int m : old_lev_grids) put(m);
     for (int l = 1; l < lev; ++l) for (int m = lstart[l]; m != 0; m = node[m].levelptr) put(m);
-    d_patches.upload(h_patches, st);
+    d_patches.upload(h_patches, st, stg);
     (void)lev;
   }
 
@@ -1531,6 +1773,7 @@ class Amr2Gpu {
     node[ms].level = 1; node[ms].levelptr = 0;
     node[ms].ilo = 0; node[ms].jlo = 0; node[ms].ihi = nxc - 1; node[ms].jhi = nyc - 1;
     lstart[1] = ms;
+    touch(1);
     lfine = 1;
     birect(ms);
     ginit(lstart[1], start_time);
@@ -1552,6 +1795,7 @@ class Amr2Gpu {
         if (newstl[levnew] != 0) lfnew = levnew;
         if (newstl[levnew] != 0) ginit(newstl[levnew], start_time);
         lstart[levnew] = newstl[levnew];
+        touch(levnew);
         lfine = lfnew;
         arrange(levnew);
         make_lists();
@@ -1572,7 +1816,7 @@ class Amr2Gpu {
     frame = p.output_t0 ? 0 : 1;
     tmass0 = mass();
     if (p.output_t0) output(time);
-    AMR_CUDA(cudaStreamSynchronize(st));
+    sync_stream();
   }
 
   // ginit.f: new grids at the initial time, qinit into both buffers
@@ -1586,7 +1830,7 @@ class Amr2Gpu {
       AMR_CUDA(cudaMemcpyAsync(pool.d + g.q0, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
       AMR_CUDA(cudaMemcpyAsync(pool.d + g.q1, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
       h2d_bytes += 2.0 * sizeof(double) * q.size();
-      AMR_CUDA(cudaStreamSynchronize(st));
+      sync_stream();
     }
   }
 
@@ -1606,7 +1850,7 @@ class Amr2Gpu {
     launch_mass2(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st);
     double m = 0;
     AMR_CUDA(cudaMemcpyAsync(&m, d_mass, sizeof(double), cudaMemcpyDeviceToHost, st));
-    AMR_CUDA(cudaStreamSynchronize(st));
+    sync_stream();
     return m * hxposs[1] * hyposs[1];
   }
 
@@ -1698,7 +1942,7 @@ class Amr2Gpu {
       if (max_cycles > 0 && cycles_this_call >= max_cycles) break;
     }
     AMR_CUDA(cudaEventRecord(ev_run1, st));
-    AMR_CUDA(cudaStreamSynchronize(st));
+    sync_stream();
     float ms = 0;
     AMR_CUDA(cudaEventElapsedTime(&ms, ev_run0, ev_run1));
     last_run_ms = ms;
@@ -1719,11 +1963,11 @@ class Amr2Gpu {
     std::vector<double> out(tot);
     if (tot == 0) return out;
     DBuf<double> d; d.ensure(tot);
-    DBuf<int> dp; dp.upload(pl, st);
-    DBuf<long long> doff; doff.upload(off, st);
+    DBuf<int> dp; dp.upload(pl, st, stg);
+    DBuf<long long> doff; doff.upload(off, st, stg);
     launch_gather_interior2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, st);
     AMR_CUDA(cudaMemcpyAsync(out.data(), d.d, sizeof(double) * tot, cudaMemcpyDeviceToHost, st));
-    AMR_CUDA(cudaStreamSynchronize(st));
+    sync_stream();
     d.free(); dp.free(); doff.free();
     return out;
   }

@@ -77,22 +77,32 @@ inline void qsort_index(std::vector<int>& ord, int n, const std::vector<long lon
 // i+0.5, j+0.5 in doubles; integer centres carry the same information).
 struct Pt { int i, j; };
 
+// drivesort.f: sort the flagged points by the key i + (isize+2*mbuff)*j and drop
+// duplicates. Distinct integer keys have exactly one ascending order, so a scan of
+// a byte map over the points' bounding box (j outer, i inner) gives the
+// reference's result without its quicksort.
 inline void sort_unique(std::vector<Pt>& pts, int isize, int mbuff) {
-  const int n = (int)pts.size();
+  (void)isize; (void)mbuff;
+  const size_t n = pts.size();
   if (n == 0) return;
-  std::vector<long long> key(n + 1);
-  std::vector<int> ord(n + 1);
-  const long long w = (long long)isize + 2 * mbuff;
-  for (int k = 1; k <= n; ++k) key[k] = (long long)(pts[k - 1].i + mbuff) + w * (pts[k - 1].j + mbuff);
-  qsort_index(ord, n, key);
+  int i0 = pts[0].i, i1 = i0, j0 = pts[0].j, j1 = j0;
+  for (const Pt& q : pts) { i0 = std::min(i0, q.i); i1 = std::max(i1, q.i); j0 = std::min(j0, q.j); j1 = std::max(j1, q.j); }
+  const size_t w = (size_t)(i1 - i0 + 1), h = (size_t)(j1 - j0 + 1);
   std::vector<Pt> out;
-  out.reserve(n);
-  int k = 1;
-  while (k <= n) {
-    const long long e = key[ord[k]];
-    out.push_back(Pt{(int)(e % w) - mbuff, (int)(e / w) - mbuff});
-    ++k;
-    while (k <= n && key[ord[k]] == key[ord[k - 1]]) ++k;
+  if (w * h <= 16 * n + (1u << 22)) {
+    std::vector<uint8_t> map(w * h, 0);
+    for (const Pt& q : pts) map[(size_t)(q.j - j0) * w + (q.i - i0)] = 1;
+    out.reserve(n);
+    for (size_t j = 0; j < h; ++j)
+      for (size_t i = 0; i < w; ++i)
+        if (map[j * w + i]) out.push_back(Pt{(int)i + i0, (int)j + j0});
+  } else {
+    std::vector<long long> key(n);
+    for (size_t k = 0; k < n; ++k) key[k] = (long long)(pts[k].i - i0) + (long long)w * (pts[k].j - j0);
+    std::sort(key.begin(), key.end());
+    key.erase(std::unique(key.begin(), key.end()), key.end());
+    out.reserve(key.size());
+    for (long long e : key) out.push_back(Pt{(int)(e % (long long)w) + i0, (int)(e / (long long)w) + j0});
   }
   pts.swap(out);
 }
