@@ -65,6 +65,13 @@ class Solver:
                "amrgpu_level_advance")
         return dt.value, cfl.value
 
+    def level_advance_noalloc(self, level: int):
+        """amrgpu_level_advance with the ghost-fill scratch in a fixed device array (no allocation)."""
+        dt = ctypes.c_double(); cfl = ctypes.c_double()
+        _check(self._lib, self._lib.amrgpu_level_advance_noalloc(self._h, level, ctypes.byref(dt), ctypes.byref(cfl)),
+               "amrgpu_level_advance_noalloc")
+        return dt.value, cfl.value
+
     def update(self, level: int) -> None:
         _check(self._lib, self._lib.amrgpu_update(self._h, level), "amrgpu_update")
 

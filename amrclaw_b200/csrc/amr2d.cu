@@ -19,6 +19,7 @@
 #include "cluster2d.hpp"
 #include "gridindex.hpp"
 #include "workpool.hpp"
+#include "noalloc2d.cuh"
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -1207,6 +1208,70 @@ class Amr2Gpu {
     return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
   }
 
+  // advanc without device allocation: the bound and saveqc programs run with their
+  // scratch rects in the fixed device array (noalloc2d.cu); no gauge sampling, no
+  // profiling events, no host timers. Returns dtnew like advanc.
+  void run_prog_fixed(FillProg& P, const SrcMode& modes, const double* scratch) {
+    for (int s = 0; s < P.nstages; ++s) {
+      if (P.ch_hi[s] > P.ch_lo[s]) {
+        FillArgs a{};
+        a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
+        a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
+        a.lc = lc; a.xlower = xlower; a.ylower = ylower;
+        launch_fill_fixed(a, scratch, P.scratch_off, st);
+        ++nkernels;
+      }
+      if (P.bc_hi[s] > P.bc_lo[s]) {
+        BcArgs b{};
+        b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.bc_lo[s];
+        b.nops = P.bc_hi[s] - P.bc_lo[s]; b.nvar = nvar;
+        launch_bc_fixed(b, 0, scratch, P.scratch_off, st);
+        launch_bc_fixed(b, 1, scratch, P.scratch_off, st);
+        nkernels += 2;
+      }
+    }
+  }
+  double advanc_fixed(int lev, const double* scratch) {
+    LevelPlan& L = plan[lev];
+    const bool kids = lev + 1 <= p.mxnest && lstart[lev + 1] != 0;
+    if (L.bound.scratch_len > NOALLOC_SCRATCH_DOUBLES || (kids && L.saveqc.scratch_len > NOALLOC_SCRATCH_DOUBLES))
+      throw std::invalid_argument("ghost-fill scratch of this level exceeds the fixed array (4194304 doubles)");
+    const double t = node[lgrids[lev][0]].time;
+    const double dt = possk[lev];
+    SrcMode M = modes_for(lev, t);
+    for (int l = 1; l <= lev; ++l)
+      if (M.mode[l] < 0 && !lgrids[l].empty()) M.mode[l] = 0;
+    run_prog_fixed(L.bound, M, scratch);
+    if (kids) { SrcMode Z{}; run_prog_fixed(L.saveqc, Z, scratch); }
+    if (lev > 1 && !L.qad.empty()) {
+      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st);
+      ++nkernels;
+    }
+    AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+    StepArgs a{};
+    a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.fsv = L.d_fsv.d; a.fad = L.d_fad.d;
+    a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
+    a.work = L.d_work.d; a.nwork = (int)L.work.size(); a.queue = nullptr;
+    launch_step2(prob.solver, a, (int)L.work.size(), st);
+    launch_flip(d_patches.d, L.d_plist.d, (int)L.plist.size(), st);
+    nkernels += 2;
+    unsigned long long cbits = 0;
+    AMR_CUDA(cudaMemcpyAsync(&cbits, d_cfl, sizeof(cbits), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    double cmax;
+    std::memcpy(&cmax, &cbits, sizeof(double));
+    for (int m : lgrids[lev]) {
+      node[m].cur ^= 1;
+      node[m].time = node[m].time + dt;
+      const double cells = (double)node[m].nx() * node[m].ny();
+      rvol += cells; rvoll[lev] += cells;
+    }
+    cfl_level = cmax;
+    cflmax_run = std::max(cflmax_run, cmax);
+    ++nsteps_launched;
+    return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
+  }
+
   void update(int lev) {
     HPROF("update");
     LevelPlan& L = plan[lev];
@@ -2120,6 +2185,27 @@ int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* 
     if (dtnew_out) *dtnew_out = d;
     if (cfl_out) *cfl_out = s.cfl_level;
   });
+}
+
+int amrgpu_level_advance_noalloc(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out) {
+  if (!ctx) return AMRGPU_EINVAL;
+  try {
+    amrb::Amr2Gpu& s = *ctx->s2;
+    if (level < 1 || level > s.lfine) { g_err = "level out of range"; return AMRGPU_EINVAL; }
+    double* scratch = nullptr;
+    std::string err;
+    if (amrb::fixed_scratch_address(&scratch, err) != 0) { g_err = err; return AMRGPU_ERROR; }
+    const double d = s.advanc_fixed(level, scratch);
+    if (dtnew_out) *dtnew_out = d;
+    if (cfl_out) *cfl_out = s.cfl_level;
+    return AMRGPU_OK;
+  } catch (std::invalid_argument& e) {
+    g_err = e.what();
+    return AMRGPU_EINVAL;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return AMRGPU_ERROR;
+  }
 }
 
 int amrgpu_update(amrgpu_ctx* ctx, int level) {

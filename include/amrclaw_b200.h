@@ -50,6 +50,20 @@ int amrgpu_run(amrgpu_ctx* ctx, int max_cycles);
  * dtnew_out receives the level's suggested next dt (stepgrid.f:206-212). */
 int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out);
 
+/* amrgpu_level_advance without any device allocation. No counterpart in the
+ * reference (its level advance allocates per call from the alloc heap).
+ * The ghost-fill and saved-coarse-value programs stage their coarse scratch
+ * rectangles in one file-scope device array of 4194304 doubles (32 MiB)
+ * instead of the context's device pool; a level whose programs need more
+ * returns AMRGPU_EINVAL with a message. The first call on a device looks up
+ * the array's address (cudaGetSymbolAddress) with that device current; make
+ * that first call before anything that must not see set-up work. The array is
+ * shared by every context on the device and keeps the last call's contents:
+ * nothing in it needs to start at zero (every scratch cell is written before
+ * it is read), but calls that overlap in time, from any context, race on it.
+ * Gauges are not sampled and no profiling events are recorded. */
+int amrgpu_level_advance_noalloc(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out);
+
 /* Fine-to-coarse averaging and flux-register fix-up of `level` from level+1.
  * Replaces update (src/2d/update.f:16-189) and upbnd (src/2d/upbnd.f:18-127). */
 int amrgpu_update(amrgpu_ctx* ctx, int level);
