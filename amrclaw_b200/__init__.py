@@ -91,15 +91,25 @@ class Solver:
         keys = ["time", "cell_updates", "coarse_steps", "lfine", "step_seconds", "regrid_seconds", "mass0",
                 "cflmax", "kernels", "pool_peak_bytes", "substeps", "step_kernel_ms", "step_kernel_cells",
                 "last_run_ms", "last_run_cells", "finished", "h2d_bytes",
-                "regrid_flags_s", "regrid_hostflags_s", "regrid_cluster_s", "regrid_fill_s", "regrid_prep_s", "regrid_compile_s"]
+                "regrid_flags_s", "regrid_hostflags_s", "regrid_cluster_s", "regrid_fill_s", "regrid_prep_s", "regrid_compile_s",
+                "num_dim"]
         out = (ctypes.c_double * len(keys))()
         _check(self._lib, self._lib.amrgpu_info(self._h, out, len(keys)), "amrgpu_info")
         return dict(zip(keys, list(out)))
 
+    @property
+    def num_dim(self) -> int:
+        """2 or 3: the dimension of the run's data files."""
+        d = self._lib.amrgpu_num_dim(self._h)
+        if d < 0:
+            _check(self._lib, d, "amrgpu_num_dim")
+        return d
+
     def grids(self) -> np.ndarray:
+        """Rows (grid_number, level, ilo, ihi, jlo, jhi[, klo, khi]) in output order."""
         n = ctypes.c_int()
         _check(self._lib, self._lib.amrgpu_grids(self._h, None, 0, ctypes.byref(n)), "amrgpu_grids")
-        a = np.zeros((n.value, 6), dtype=np.int32)
+        a = np.zeros((n.value, 2 + 2 * self.num_dim), dtype=np.int32)
         _check(self._lib, self._lib.amrgpu_grids(self._h, a.ctypes.data_as(_lib.c_int_p), n.value, ctypes.byref(n)),
                "amrgpu_grids")
         return a

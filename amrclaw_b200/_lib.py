@@ -28,6 +28,7 @@ SIGNATURES = {
     "amrgpu_grids": (ctypes.c_int, [ctypes.c_void_p, c_int_p, ctypes.c_int, c_int_p]),
     "amrgpu_values": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_longlong, c_ll_p]),
     "amrgpu_gauges": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_int, c_int_p]),
+    "amrgpu_num_dim": (ctypes.c_int, [ctypes.c_void_p]),
     "amrgpu_destroy": (ctypes.c_int, [ctypes.c_void_p]),
 }
 

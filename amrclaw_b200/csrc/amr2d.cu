@@ -20,6 +20,8 @@
 #include "gridindex.hpp"
 #include "workpool.hpp"
 #include "noalloc2d.cuh"
+#include "hostutil.hpp"
+#include "solver.hpp"
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -31,135 +33,6 @@
 #include <vector>
 
 namespace amrb {
-
-static const double RINF = (double)10.e32f;
-
-// Host-side section timers, printed at context destruction when AMRB_PROF is set.
-struct HostProf {
-  std::map<std::string, std::pair<double, long long>> acc;
-  bool on = std::getenv("AMRB_PROF") != nullptr;
-  ~HostProf() {
-    if (!on) return;
-    for (auto& kv : acc) std::fprintf(stderr, "PROF %-22s %9.4f s %8lld calls\n", kv.first.c_str(), kv.second.first, kv.second.second);
-  }
-};
-struct ScopedTimer {
-  HostProf& P; const char* name; std::chrono::steady_clock::time_point t0;
-  ScopedTimer(HostProf& p, const char* n) : P(p), name(n), t0(std::chrono::steady_clock::now()) {}
-  ~ScopedTimer() {
-    if (!P.on) return;
-    auto& a = P.acc[name];
-    a.first += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    a.second += 1;
-  }
-};
-#define HPROF(name) ScopedTimer _hp_##__LINE__(hprof, name)  // rinfinity of amr_module.f90 (a default-REAL literal)
-
-// ------------------------------------------------------------------ device pool
-struct Arena {
-  double* d = nullptr;
-  long long cap = 0;
-  std::map<long long, long long> fr;  // free blocks: offset -> length
-  long long inuse = 0, peak = 0;
-  static long long rnd(long long n) { return (n + 31) / 32 * 32; }
-  void init(long long n) {
-    n = rnd(std::max<long long>(n, 1 << 20));
-    AMR_CUDA(cudaMalloc(&d, sizeof(double) * n));
-    cap = n;
-    fr.clear();
-    fr[0] = n;
-  }
-  void grow(long long need) {
-    long long ncap = std::max(cap * 2, cap + rnd(need) + (1 << 20));
-    double* nd = nullptr;
-    AMR_CUDA(cudaMalloc(&nd, sizeof(double) * ncap));
-    AMR_CUDA(cudaMemcpy(nd, d, sizeof(double) * cap, cudaMemcpyDeviceToDevice));
-    AMR_CUDA(cudaFree(d));
-    d = nd;
-    release_raw(cap, ncap - cap);
-    cap = ncap;
-  }
-  void release_raw(long long off, long long n) {
-    auto it = fr.emplace(off, n).first;
-    if (it != fr.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) { pv->second += it->second; fr.erase(it); it = pv; }
-    }
-    auto nx = std::next(it);
-    if (nx != fr.end() && it->first + it->second == nx->first) { it->second += nx->second; fr.erase(nx); }
-  }
-  long long alloc(long long n) {
-    n = rnd(std::max<long long>(n, 1));
-    for (int pass = 0; pass < 2; ++pass) {
-      for (auto it = fr.begin(); it != fr.end(); ++it)
-        if (it->second >= n) {
-          const long long off = it->first, len = it->second;
-          fr.erase(it);
-          if (len > n) fr[off + n] = len - n;
-          inuse += n; peak = std::max(peak, inuse);
-          return off;
-        }
-      grow(n);
-    }
-    throw std::runtime_error("device pool exhausted");
-  }
-  void release(long long off, long long n) {
-    if (off < 0) return;
-    n = rnd(std::max<long long>(n, 1));
-    inuse -= n;
-    release_raw(off, n);
-  }
-  void destroy() { if (d) cudaFree(d); d = nullptr; }
-};
-
-// Pinned host staging for host-to-device uploads: a copy from pinned memory is
-// queued without the driver's pageable bounce. Space is reused only after the
-// stream has been synchronized (Staging::reset is called right after each sync).
-struct Staging {
-  char* h = nullptr;
-  size_t cap = 0, used = 0;
-  const void* put(const void* src, size_t n, cudaStream_t s) {
-    const size_t n2 = (n + 255) & ~(size_t)255;
-    if (used + n2 > cap) {
-      AMR_CUDA(cudaStreamSynchronize(s));
-      used = 0;
-      if (n2 > cap) {
-        if (h) AMR_CUDA(cudaFreeHost(h));
-        cap = std::max<size_t>({n2, cap * 2, (size_t)8 << 20});
-        AMR_CUDA(cudaMallocHost((void**)&h, cap));
-      }
-    }
-    char* dst = h + used;
-    std::memcpy(dst, src, n);
-    used += n2;
-    return dst;
-  }
-  void reset() { used = 0; }
-  void destroy() { if (h) cudaFreeHost(h); h = nullptr; cap = used = 0; }
-};
-
-template <class T> struct DBuf {
-  T* d = nullptr; size_t cap = 0, n = 0;
-  void upload(const std::vector<T>& h, cudaStream_t s, Staging& stg) { upload(h.data(), h.size(), s, stg); }
-  void upload(const T* h, size_t cnt, cudaStream_t s, Staging& stg) {
-    n = cnt;
-    if (n > cap) {
-      if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(n, 16) * 3 / 2;
-      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
-    }
-    if (n) AMR_CUDA(cudaMemcpyAsync(d, stg.put(h, sizeof(T) * n, s), sizeof(T) * n, cudaMemcpyHostToDevice, s));
-  }
-  void ensure(size_t m) {
-    if (m > cap) {
-      if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(m, 16) * 3 / 2;
-      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
-    }
-    n = m;
-  }
-  void free() { if (d) cudaFree(d); d = nullptr; cap = n = 0; }
-};
 
 // ------------------------------------------------------------------ host patch metadata
 struct HPatch {
@@ -2111,8 +1984,77 @@ void Amr2Gpu::output(double t) {
 // ============================================================================ C ABI
 #include "../../include/amrclaw_b200.h"
 
+namespace amrb {
+
+// The 2D solver behind the C ABI's solver interface.
+class Solver2 : public AmrSolver {
+ public:
+  Amr2Gpu g;
+  int num_dim() const override { return 2; }
+  void set_batched(bool on) override { g.batched = on; }
+  void set_profile(bool on) override { g.profile = on; }
+  void run(int max_cycles) override { g.max_cycles = max_cycles; g.tick(); }
+  double level_advance(int level, double* cfl) override {
+    if (level < 1 || level > g.lfine) throw std::runtime_error("level out of range");
+    const double d = g.advanc(level);
+    if (cfl) *cfl = g.cfl_level;
+    return d;
+  }
+  void update_level(int level) override {
+    if (level < 1 || level >= g.lfine) throw std::runtime_error("level out of range");
+    g.update(level);
+    AMR_CUDA(cudaStreamSynchronize(g.st));
+  }
+  void regrid_from(int lbase) override {
+    if (lbase < 1 || lbase > g.lfine || lbase >= g.p.mxnest) throw std::runtime_error("lbase out of range");
+    g.regrid(lbase);
+    g.setbestsrc();
+  }
+  void valout(const char* dir) override {
+    const std::string keep = g.outdir;
+    const bool kw = g.write_output;
+    if (dir) { g.outdir = dir; g.write_output = true; }
+    g.output(g.time);
+    g.outdir = keep; g.write_output = kw;
+  }
+  double mass() override { return g.mass(); }
+  std::vector<double> info() override {
+    return {g.time, g.rvol, (double)g.ncycle, (double)g.lfine, g.t_step, g.t_regrid, g.tmass0,
+            g.cflmax_run, (double)g.nkernels, (double)g.pool.peak * 8.0, (double)g.nsteps_launched,
+            g.step_kernel_ms, g.step_kernel_cells, g.last_run_ms, g.run_cells, g.finished() ? 1.0 : 0.0, g.h2d_bytes,
+            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0};
+  }
+  std::vector<int> grid_rows() override {
+    std::vector<int> r;
+    for (int lev = 1; lev <= g.lfine; ++lev)
+      for (int m : g.lgrids[lev]) {
+        const HPatch& h = g.node[m];
+        r.insert(r.end(), {m, lev, h.ilo, h.ihi, h.jlo, h.jhi});
+      }
+    return r;
+  }
+  std::vector<double> values() override { return g.gather_values(); }
+  std::vector<double> gauge_rows() override {
+    const int nv = g.nvar;
+    std::vector<double> vals((size_t)g.gslots * nv), out;
+    if (g.gslots) AMR_CUDA(cudaMemcpy(vals.data(), g.d_gauge_out.d, sizeof(double) * vals.size(), cudaMemcpyDeviceToHost));
+    // rows grouped by gauge, in recording order (as each gauge's file would list them)
+    for (const auto& G : g.p.gauges)
+      for (const auto& r : g.grows) {
+        if (r.gauge != G.num) continue;
+        out.push_back(r.gauge); out.push_back(r.level); out.push_back(r.t);
+        for (int k = 0; k < nv; ++k) out.push_back(vals[(size_t)r.slot * nv + k]);
+      }
+    return out;
+  }
+};
+
+}  // namespace amrb
+
 struct amrgpu_ctx {
-  std::unique_ptr<amrb::Amr2Gpu> s2;
+  std::unique_ptr<amrb::AmrSolver> s;
+  amrb::Amr2Gpu* s2 = nullptr;  // the 2D solver, for the 2D-only entry points
+  int nvar = 0;
 };
 
 static thread_local std::string g_err;
@@ -2141,54 +2083,54 @@ int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu
     amrb::KeyFile c;
     if (!c.read(std::string(rundir) + "/claw.data")) throw std::runtime_error(std::string("cannot read ") + rundir + "/claw.data");
     const int nd = c.n("num_dim");
-    if (nd != 2) throw std::runtime_error("num_dim must be 2 for this build");
-    auto* ctx = new amrgpu_ctx();
-    ctx->s2.reset(new amrb::Amr2Gpu());
-    ctx->s2->outdir = outdir ? outdir : "";
-    ctx->s2->write_output = write_output != 0;
-    try {
-      ctx->s2->init(rundir);
-    } catch (...) {
-      delete ctx;
-      throw;
+    std::unique_ptr<amrgpu_ctx> ctx(new amrgpu_ctx());
+    ctx->nvar = c.n("num_eqn");
+    if (nd == 2) {
+      auto* s2 = new amrb::Solver2();
+      ctx->s.reset(s2);
+      ctx->s2 = &s2->g;
+      s2->g.outdir = outdir ? outdir : "";
+      s2->g.write_output = write_output != 0;
+      s2->g.init(rundir);
+    } else if (nd == 3) {
+      ctx->s.reset(amrb::make_solver3(rundir, outdir ? outdir : "", write_output != 0));
+    } else {
+      throw std::runtime_error("num_dim must be 2 or 3");
     }
-    *out = ctx;
+    *out = ctx.release();
   });
 }
 
 int amrgpu_set_batched(amrgpu_ctx* ctx, int batched) {
   if (!ctx) return AMRGPU_EINVAL;
-  ctx->s2->batched = batched != 0;
+  ctx->s->set_batched(batched != 0);
   return AMRGPU_OK;
 }
 
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on) {
   if (!ctx) return AMRGPU_EINVAL;
-  ctx->s2->profile = on != 0;
+  ctx->s->set_profile(on != 0);
   return AMRGPU_OK;
 }
 
 int amrgpu_run(amrgpu_ctx* ctx, int max_cycles) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] {
-    ctx->s2->max_cycles = max_cycles;
-    ctx->s2->tick();
-  });
+  return guarded([&] { ctx->s->run(max_cycles); });
 }
 
 int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out) {
   if (!ctx) return AMRGPU_EINVAL;
   return guarded([&] {
-    amrb::Amr2Gpu& s = *ctx->s2;
-    if (level < 1 || level > s.lfine) throw std::runtime_error("level out of range");
-    const double d = s.advanc(level);
+    double cfl = 0;
+    const double d = ctx->s->level_advance(level, &cfl);
     if (dtnew_out) *dtnew_out = d;
-    if (cfl_out) *cfl_out = s.cfl_level;
+    if (cfl_out) *cfl_out = cfl;
   });
 }
 
 int amrgpu_level_advance_noalloc(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out) {
   if (!ctx) return AMRGPU_EINVAL;
+  if (!ctx->s2) { g_err = "amrgpu_level_advance_noalloc: 2D runs only"; return AMRGPU_EINVAL; }
   try {
     amrb::Amr2Gpu& s = *ctx->s2;
     if (level < 1 || level > s.lfine) { g_err = "level out of range"; return AMRGPU_EINVAL; }
@@ -2210,67 +2152,39 @@ int amrgpu_level_advance_noalloc(amrgpu_ctx* ctx, int level, double* dtnew_out, 
 
 int amrgpu_update(amrgpu_ctx* ctx, int level) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] {
-    amrb::Amr2Gpu& s = *ctx->s2;
-    if (level < 1 || level >= s.lfine) throw std::runtime_error("level out of range");
-    s.update(level);
-    AMR_CUDA(cudaStreamSynchronize(s.st));
-  });
+  return guarded([&] { ctx->s->update_level(level); });
 }
 
 int amrgpu_regrid(amrgpu_ctx* ctx, int lbase) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] {
-    amrb::Amr2Gpu& s = *ctx->s2;
-    if (lbase < 1 || lbase > s.lfine || lbase >= s.p.mxnest) throw std::runtime_error("lbase out of range");
-    s.regrid(lbase);
-    s.setbestsrc();
-  });
+  return guarded([&] { ctx->s->regrid_from(lbase); });
 }
 
 int amrgpu_valout(amrgpu_ctx* ctx, const char* dir) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] {
-    amrb::Amr2Gpu& s = *ctx->s2;
-    const std::string keep = s.outdir;
-    const bool kw = s.write_output;
-    if (dir) { s.outdir = dir; s.write_output = true; }
-    s.output(s.time);
-    s.outdir = keep; s.write_output = kw;
-  });
+  return guarded([&] { ctx->s->valout(dir); });
 }
 
 int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out) {
   if (!ctx || !mass_out) return AMRGPU_EINVAL;
-  return guarded([&] { *mass_out = ctx->s2->mass(); });
+  return guarded([&] { *mass_out = ctx->s->mass(); });
 }
 
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n) {
   if (!ctx || !out) return AMRGPU_EINVAL;
   return guarded([&] {
-    amrb::Amr2Gpu& s = *ctx->s2;
-    const double v[] = {s.time, s.rvol, (double)s.ncycle, (double)s.lfine, s.t_step, s.t_regrid, s.tmass0,
-                        s.cflmax_run, (double)s.nkernels, (double)s.pool.peak * 8.0, (double)s.nsteps_launched,
-                        s.step_kernel_ms, s.step_kernel_cells, s.last_run_ms, s.run_cells, s.finished() ? 1.0 : 0.0, s.h2d_bytes,
-                        s.tr_flags, s.tr_host, s.tr_cluster, s.tr_fill, s.tr_prep, s.tr_compile};
-    for (int k = 0; k < n && k < (int)(sizeof(v) / sizeof(v[0])); ++k) out[k] = v[k];
+    const std::vector<double> v = ctx->s->info();
+    for (int k = 0; k < n && k < (int)v.size(); ++k) out[k] = v[k];
   });
 }
 
 int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out) {
   if (!ctx || !n_out) return AMRGPU_EINVAL;
   return guarded([&] {
-    amrb::Amr2Gpu& s = *ctx->s2;
-    int n = 0;
-    for (int lev = 1; lev <= s.lfine; ++lev)
-      for (int m : s.lgrids[lev]) {
-        if (out && n < cap) {
-          const amrb::HPatch& g = s.node[m];
-          int* r = out + 6 * n;
-          r[0] = m; r[1] = lev; r[2] = g.ilo; r[3] = g.ihi; r[4] = g.jlo; r[5] = g.jhi;
-        }
-        ++n;
-      }
+    const std::vector<int> r = ctx->s->grid_rows();
+    const int w = 2 + 2 * ctx->s->num_dim();
+    const int n = (int)(r.size() / w);
+    if (out) std::memcpy(out, r.data(), sizeof(int) * (size_t)w * std::min(cap, n));
     *n_out = n;
   });
 }
@@ -2278,7 +2192,7 @@ int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out) {
 int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out) {
   if (!ctx || !n_out) return AMRGPU_EINVAL;
   return guarded([&] {
-    const std::vector<double> v = ctx->s2->gather_values();
+    const std::vector<double> v = ctx->s->values();
     if (out) std::memcpy(out, v.data(), sizeof(double) * std::min<long long>(cap, (long long)v.size()));
     *n_out = (long long)v.size();
   });
@@ -2287,22 +2201,10 @@ int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out)
 int amrgpu_gauges(amrgpu_ctx* ctx, double* out, int cap_rows, int* n_out) {
   if (!ctx || !n_out) return AMRGPU_EINVAL;
   return guarded([&] {
-    amrb::Amr2Gpu& s = *ctx->s2;
-    const int nv = s.nvar;
-    std::vector<double> vals((size_t)s.gslots * nv);
-    if (s.gslots) AMR_CUDA(cudaMemcpy(vals.data(), s.d_gauge_out.d, sizeof(double) * vals.size(), cudaMemcpyDeviceToHost));
-    // rows grouped by gauge, in recording order (as each gauge's file would list them)
-    int n = 0;
-    for (const auto& G : s.p.gauges)
-      for (const auto& r : s.grows) {
-        if (r.gauge != G.num) continue;
-        if (out && n < cap_rows) {
-          double* row = out + (size_t)(3 + nv) * n;
-          row[0] = r.gauge; row[1] = r.level; row[2] = r.t;
-          for (int k = 0; k < nv; ++k) row[3 + k] = vals[(size_t)r.slot * nv + k];
-        }
-        ++n;
-      }
+    const std::vector<double> v = ctx->s->gauge_rows();
+    const int w = 3 + ctx->nvar;
+    const int n = (int)(v.size() / w);
+    if (out) std::memcpy(out, v.data(), sizeof(double) * (size_t)w * std::min(cap_rows, n));
     *n_out = n;
   });
 }
@@ -2311,5 +2213,7 @@ int amrgpu_destroy(amrgpu_ctx* ctx) {
   delete ctx;
   return AMRGPU_OK;
 }
+
+int amrgpu_num_dim(amrgpu_ctx* ctx) { return ctx ? ctx->s->num_dim() : 0; }
 
 }  // extern "C"

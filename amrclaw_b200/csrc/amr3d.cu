@@ -1,0 +1,1892 @@
+// Host orchestrator of the 3D B200 patch-advance path (3D Euler).
+//
+// Same organisation as the 2D orchestrator: patches live in a device pool with two
+// solution buffers each (store1 / store2 as a ping-pong pair), flux registers in a
+// second pool, and the host compiles per regrid the device programs of a level
+// substep: ghost fill (src/3d/bound.f, filpatch.f, intfil.f, bc3amr.f90), saved
+// coarse values (saveqc.f, cstore.f), the step work (step3.f, flux3.f) with its
+// register epilogue (fluxsv.f, fluxad.f), qad jobs (qad.f) and the level sync
+// (update.f, upbnd.f). The scheduler (tick.f) and the regrid decisions stay on the
+// host; 3D regridding flags whole levels in int8 arrays as the reference does
+// (flglvl.f, domprep.f, domshrink.f, domup.f, domcopy.f, spest.f, bufnst.f,
+// projec.f, shiftset.f, colate.f, smartbis.f, findcut.f, moment.f, nestck.f,
+// grdfit.f, birect.f, gfixup.f, filval.f) with the gradient test on the device.
+#include "kernels3d.cuh"
+#include "params.hpp"
+#include "gridindex.hpp"
+#include "workpool.hpp"
+#include "hostutil.hpp"
+#include "solver.hpp"
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+namespace amrb {
+
+namespace {
+
+constexpr int G3 = 2;  // num_ghost
+
+struct HPatch3 {
+  int ilo = 0, ihi = 0, jlo = 0, jhi = 0, klo = 0, khi = 0, level = 0, levelptr = 0, nextfree = 0;
+  double xlo = 0, xhi = 0, ylo = 0, yhi = 0, zlo = 0, zhi = 0, time = 0;
+  long long q0 = -1, q1 = -1, nq = 0;
+  long long ffl = -1, nffl = 0;
+  int lenbc = 0;
+  int cur = 0;
+  bool has_cfl = false;
+  std::vector<int> listbc;  // 6 ints per entry (setuse.f): i, j, k (enlarged, 1-based), side, kid, register
+  std::vector<int> bnd;
+  int nx() const { return ihi - ilo + 1; }
+  int ny() const { return jhi - jlo + 1; }
+  int nz() const { return khi - klo + 1; }
+};
+
+struct Prog3 {
+  std::vector<Rect3> rects;
+  std::vector<Fill3Op> ops;
+  std::vector<int> op_stage;
+  std::vector<Bc3Op> bcs;
+  std::vector<int> bc_stage;
+  int nstages = 0;
+  long long scratch_off = -1, scratch_len = 0, scratch_alloc = 0;
+  DBuf<Rect3> d_rects;
+  DBuf<Fill3Op> d_ops;
+  DBuf<Fill3Chunk> d_chunks;
+  DBuf<Bc3Op> d_bcs;
+  std::vector<int> ch_lo, ch_hi, bc_lo, bc_hi;
+  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; scratch_len = 0; }
+  int add_rect(int ni, int nj, int nk, int nvar) {
+    Rect3 r; r.off = scratch_len; r.ni = ni; r.nj = nj; r.nk = nk;
+    scratch_len += Arena::rnd((long long)ni * nj * nk * nvar);
+    rects.push_back(r);
+    return (int)rects.size() - 1;
+  }
+  void add_op(const Fill3Op& o, int st) { ops.push_back(o); op_stage.push_back(st); nstages = std::max(nstages, st + 1); }
+  void add_bc(const Bc3Op& b, int st) { bcs.push_back(b); bc_stage.push_back(st); nstages = std::max(nstages, st + 1); }
+  void free_dev() { d_rects.free(); d_ops.free(); d_chunks.free(); d_bcs.free(); }
+};
+
+// Appends program S after the ops already in D (rect indices and scratch offsets shifted).
+void merge_prog(Prog3& D, const Prog3& S) {
+  const int r0 = (int)D.rects.size();
+  const long long s0 = D.scratch_len;
+  for (Rect3 r : S.rects) { r.off += s0; D.rects.push_back(r); }
+  D.scratch_len += S.scratch_len;
+  for (size_t k = 0; k < S.ops.size(); ++k) {
+    Fill3Op o = S.ops[k];
+    if (o.dst_patch < 0) o.dst_rect += r0;
+    if (o.kind != F3_COPY) o.src += r0;
+    D.add_op(o, S.op_stage[k]);
+  }
+  for (size_t k = 0; k < S.bcs.size(); ++k) {
+    Bc3Op b = S.bcs[k];
+    if (b.dst_patch < 0) b.dst_rect += r0;
+    D.add_bc(b, S.bc_stage[k]);
+  }
+}
+
+struct Plan3 {
+  Prog3 bound, saveqc;
+  std::vector<int> plist;
+  std::vector<long long> sweep0, face0, cell0;
+  long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;
+  std::vector<Fsv3> fsv;
+  std::vector<Fad3> fad;
+  std::vector<Qad3Job> qad;
+  std::vector<Upbnd3Cell> upc;
+  std::vector<Upbnd3Term> upt;
+  std::vector<Avg3> avg;
+  DBuf<int> d_plist;
+  DBuf<long long> d_sweep0, d_face0, d_cell0;
+  DBuf<Fsv3> d_fsv;
+  DBuf<Fad3> d_fad;
+  DBuf<Qad3Job> d_qad;
+  DBuf<Upbnd3Cell> d_upc;
+  DBuf<Upbnd3Term> d_upt;
+  DBuf<Avg3> d_avg;
+  void free_dev() {
+    bound.free_dev(); saveqc.free_dev();
+    d_plist.free(); d_sweep0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_fad.free(); d_qad.free();
+    d_upc.free(); d_upt.free(); d_avg.free();
+  }
+};
+
+// integer*1 level array with indices (0:is+1, 0:js+1, 0:ks+1)
+struct I1 {
+  std::vector<int8_t> v; int is = 0, js = 0, ks = 0;
+  void init(int a, int b, int c) { is = a; js = b; ks = c; v.assign((size_t)(a + 2) * (b + 2) * (c + 2), 0); }
+  int8_t& operator()(int i, int j, int k) { return v[(size_t)i + (size_t)(is + 2) * ((size_t)j + (size_t)(js + 2) * k)]; }
+};
+
+struct Tgt3 { int patch, rect, ni, nj, nk; };
+
+}  // namespace
+
+class Amr3Gpu : public AmrSolver {
+ public:
+  RunParams p;
+  Step3Params sp{};
+  int nvar = 5;
+  double xlower, ylower, zlower, xupper, yupper, zupper;
+  int nxc, nyc, nzc;
+  std::vector<HPatch3> node;
+  int ndfree = 0, lfine = 1, id_hwm = 1;
+  int lstart[12] = {0}, newstl[12] = {0}, listsp[12] = {0}, icheck[12] = {0};
+  std::vector<int> lgrids[12];
+  GridIndex gidx[12];
+  bool gidx_ok[12] = {false};
+  double hxposs[12] = {0}, hyposs[12] = {0}, hzposs[12] = {0}, possk[12] = {0};
+  int iregsz[12] = {0}, jregsz[12] = {0}, kregsz[12] = {0};
+  int intratx[12] = {0}, intraty[12] = {0}, intratz[12] = {0}, kratio[12] = {0};
+  Arena pool, regs;
+  Staging stg;
+  WorkPool pool_host;
+  HostProf hprof;
+  DBuf<PatchDev> d_patches;
+  std::vector<PatchDev> h_patches;
+  Plan3 plan[12];
+  Prog3 newfill;
+  DBuf<double> d_stash, d_flux;
+  DBuf<int8_t> fl_out;
+  DBuf<double> d_gauge_out;
+  unsigned long long* d_cfl = nullptr;
+  double* d_mass = nullptr;
+  cudaStream_t st = nullptr;
+  LevelConst lc{};
+  double time = 0, start_time = 0;
+  int ncycle = 0;
+  double rvol = 0, rvoll[12] = {0};
+  double cfl_level = 0, cflmax_run = 0, tmass0 = 0;
+  bool batched = true, profile = false, record_gauges = true;
+  int max_cycles = 0;
+  double t_regrid = 0, t_step = 0, step_kernel_ms = 0, step_kernel_cells = 0, last_run_ms = 0, run_cells = 0, h2d_bytes = 0;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_run0 = nullptr, ev_run1 = nullptr;
+  bool tick_started = false;
+  int tk_nextout = 0;
+  double tk_tlevel[12] = {0};
+  long long nkernels = 0, nsteps_launched = 0;
+  int frame = 0;
+  std::string outdir;
+  bool write_output = false;
+  // gauges
+  std::vector<int> mbestsrc;
+  std::vector<double> glast;
+  struct GRow { int gauge, level; double t; int slot; };
+  std::vector<GRow> grows;
+  int gslots = 0;
+
+  ~Amr3Gpu() override {
+    if (st) cudaStreamSynchronize(st);
+    for (auto& L : plan) L.free_dev();
+    newfill.free_dev();
+    pool.destroy(); regs.destroy();
+    stg.destroy();
+    d_patches.free(); d_stash.free(); d_flux.free(); fl_out.free(); d_gauge_out.free();
+    if (d_cfl) cudaFree(d_cfl);
+    if (d_mass) cudaFree(d_mass);
+    for (cudaEvent_t e : {ev_a, ev_b, ev_run0, ev_run1}) if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+  void sync_stream() { AMR_CUDA(cudaStreamSynchronize(st)); stg.reset(); }
+
+  int mitot(int m) const { return node[m].nx() + 2 * G3; }
+  int mjtot(int m) const { return node[m].ny() + 2 * G3; }
+  int mktot(int m) const { return node[m].nz() + 2 * G3; }
+
+  // ================================================================ setup
+  void setup_problem() {
+    if (p.problem != "euler_blast") throw std::runtime_error("3D device path: unknown problem '" + p.problem + "' (the 3D device path solves the Euler equations)");
+    if (p.nvar != 5 || p.mwaves != 3) throw std::runtime_error("3D Euler needs num_eqn = 5 and num_waves = 3");
+    if (p.naux != 0) throw std::runtime_error("3D device path: aux arrays are not supported");
+    if (p.nghost != G3) throw std::runtime_error("num_ghost must be 2");
+    if (p.mcapa != 0 || p.dimsplit != 0) throw std::runtime_error("capacity functions and dimensional splitting are not supported");
+    if (p.use_fwaves) throw std::runtime_error("f-waves are not supported in 3D");
+    if (p.flag_richardson || p.tol > 0) throw std::runtime_error("Richardson estimation (flag_richardson_tol > 0) is not supported");
+    for (int d = 1; d <= 6; ++d)
+      if (p.mthbc[d] != 1 && p.mthbc[d] != 3) throw std::runtime_error("3D device path: boundaries must be extrapolation or wall");
+    sp.gamma = p.pn("gamma", 1.4); sp.gamma1 = sp.gamma - 1.0;
+    sp.efix = (int)p.pn("efix", 1.0);
+    for (int k = 0; k < 3; ++k) sp.mthlim[k] = k < (int)p.mthlim.size() ? p.mthlim[k] : 0;
+    sp.order = p.order;
+    if (p.trans < 0) throw std::runtime_error("transverse_waves < 0 is not supported");
+    sp.m3 = p.trans / 10; sp.m4 = p.trans - 10 * sp.m3;
+    if (sp.m3 > 2 || sp.m4 > 2 || (sp.m3 < 2 && sp.m4 == 2) || (sp.m3 >= 1 && sp.order == 1 && sp.m3 == 2))
+      throw std::runtime_error("unsupported transverse_waves / order combination");
+  }
+  double blast_x = 0, blast_y = 0, blast_z = 0, blast_r = 0.2, blast_pin = 5, blast_pout = 1;
+  int flag_pressure = 1;
+
+  // qinit (Euler blast): rho = 1, u = 0, p = pin within r0 of the centre, pout outside; layout [m][k][j][i]
+  void qinit(const HPatch3& g, double dx, double dy, double dz, std::vector<double>& q) {
+    const int mi = g.nx() + 2 * G3, mj = g.ny() + 2 * G3, mk = g.nz() + 2 * G3;
+    const long long pl = (long long)mi * mj * mk;
+    q.assign((size_t)pl * nvar, 0.0);
+    const double g1 = sp.gamma - 1.0;
+    for (int k = 1; k <= g.nz(); ++k) {
+      const double zc = g.zlo + (k - 0.5) * dz;
+      for (int j = 1; j <= g.ny(); ++j) {
+        const double yc = g.ylo + (j - 0.5) * dy;
+        for (int i = 1; i <= g.nx(); ++i) {
+          const double xc = g.xlo + (i - 0.5) * dx;
+          const double ddx = xc - blast_x, ddy = yc - blast_y, ddz = zc - blast_z;
+          const double r = std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+          const double pr = (r <= blast_r) ? blast_pin : blast_pout;
+          const long long at = ((long long)(k - 1 + G3) * mj + (j - 1 + G3)) * mi + (i - 1 + G3);
+          q[0 * pl + at] = 1.0; q[1 * pl + at] = 0.0; q[2 * pl + at] = 0.0; q[3 * pl + at] = 0.0;
+          q[4 * pl + at] = pr / g1;
+        }
+      }
+    }
+  }
+
+  // ================================================================ node store
+  int nodget() {
+    if (ndfree == 0) {
+      const int old = (int)node.size() - 1, add = 10000;
+      node.resize(old + 1 + add);
+      for (int k = old + 1; k <= old + add; ++k) node[k].nextfree = k + 1;
+      node[old + add].nextfree = 0;
+      ndfree = old + 1;
+    }
+    const int m = ndfree;
+    ndfree = node[m].nextfree;
+    node[m] = HPatch3();
+    return m;
+  }
+  void putnod(int m) { node[m].nextfree = ndfree; ndfree = m; }
+  void alloc_patch(int m) {
+    id_hwm = std::max(id_hwm, m + 1);
+    HPatch3& g = node[m];
+    g.nq = (long long)nvar * mitot(m) * mjtot(m) * mktot(m);
+    g.q0 = pool.alloc(g.nq);
+    g.q1 = pool.alloc(g.nq);
+    g.cur = 0;
+  }
+  void free_patch(int m) {
+    HPatch3& g = node[m];
+    pool.release(g.q0, g.nq); pool.release(g.q1, g.nq);
+    g.q0 = g.q1 = -1;
+    if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
+    g.ffl = -1; g.nffl = 0;
+  }
+  void put_desc(int m) {
+    const HPatch3& g = node[m];
+    PatchDev& d = h_patches[m];
+    d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl;
+    d.ilo = g.ilo; d.ihi = g.ihi; d.jlo = g.jlo; d.jhi = g.jhi; d.klo = g.klo; d.khi = g.khi;
+    d.mitot = mitot(m); d.mjtot = mjtot(m); d.mktot = mktot(m); d.level = g.level; d.lenbc = g.lenbc;
+  }
+  void sync_descriptors(const std::vector<int>* extra = nullptr, int extra_levels_below = 0) {
+    h_patches.assign(id_hwm, PatchDev{});
+    for (int l = 1; l <= p.mxnest; ++l) for (int m : lgrids[l]) put_desc(m);
+    if (extra) for (int m : *extra) put_desc(m);
+    for (int l = 1; l < extra_levels_below; ++l) for (int m = lstart[l]; m != 0; m = node[m].levelptr) put_desc(m);
+    d_patches.upload(h_patches, st, stg);
+  }
+
+  // ================================================================ lists
+  void touch(int lev) { gidx_ok[lev] = false; }
+  const GridIndex& GI(int lev) {
+    if (!gidx_ok[lev]) {
+      std::vector<int> l;
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) l.push_back(m);
+      gidx[lev].build(l, [&](int m) { const HPatch3& g = node[m]; return std::array<int, 6>{g.ilo, g.ihi, g.jlo, g.jhi, g.klo, g.khi}; });
+      gidx_ok[lev] = true;
+    }
+    return gidx[lev];
+  }
+  void make_lists() {
+    for (int lev = 1; lev <= 11; ++lev) {
+      lgrids[lev].clear();
+      if (lev > p.mxnest) continue;
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) lgrids[lev].push_back(m);
+    }
+  }
+  // init_bndryList.f:50-107 (neighbours by their i,j extents, most recent first)
+  void make_bndry(int lev) {
+    const GridIndex& X = GI(lev);
+    std::vector<int> hits;
+    for (int m : lgrids[lev]) {
+      HPatch3& g = node[m];
+      g.bnd.clear();
+      X.query(g.ilo - G3, g.ihi + G3, g.jlo - G3, g.jhi + G3, -(1 << 29), 1 << 29, hits);
+      for (size_t k = hits.size(); k-- > 0;)
+        if (X.id(hits[k]) != m) g.bnd.push_back(X.id(hits[k]));
+    }
+  }
+  // regrid.f:122-159: cost nx*ny, most expensive first, quick_sort1.f tie breaking
+  static void qsorti(std::vector<int>& ord, int n, const std::vector<long long>& a);
+  void arrange(int lev) {
+    std::vector<int> gl;
+    for (int m = lstart[lev]; m != 0; m = node[m].levelptr) gl.push_back(m);
+    const int n = (int)gl.size();
+    if (n <= 1) return;
+    std::vector<long long> cost(n + 1);
+    std::vector<int> ord(n + 1);
+    for (int i = 1; i <= n; ++i) cost[i] = (long long)node[gl[i - 1]].nx() * node[gl[i - 1]].ny();
+    qsorti(ord, n, cost);
+    lstart[lev] = gl[ord[n] - 1];
+    int prev = lstart[lev];
+    for (int i = 1; i <= n - 1; ++i) { node[prev].levelptr = gl[ord[n - i] - 1]; prev = node[prev].levelptr; }
+    node[prev].levelptr = 0;
+    touch(lev);
+  }
+  // birect.f:4-172
+  void birect(int m1) {
+    int m = m1;
+    const int lev = node[m].level;
+    const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
+    while (true) {
+      const int nx = node[m].nx(), ny = node[m].ny(), nz = node[m].nz();
+      if (nx + 2 * G3 > p.max1d || ny + 2 * G3 > p.max1d || nz + 2 * G3 > p.max1d) {
+        const int dir = (nx + 2 * G3 > p.max1d) ? 0 : (ny + 2 * G3 > p.max1d) ? 1 : 2;
+        const int n = dir == 0 ? nx : dir == 1 ? ny : nz;
+        int nl = n / 2;
+        const int r = lev > 1 ? (dir == 0 ? intratx[lev - 1] : dir == 1 ? intraty[lev - 1] : intratz[lev - 1]) : 2;
+        nl = (nl / r) * r;
+        const double mid = (dir == 0 ? node[m].xlo + nl * hx : dir == 1 ? node[m].ylo + nl * hy : node[m].zlo + nl * hz);
+        const int mn = nodget();
+        HPatch3& a = node[m]; HPatch3& b = node[mn];
+        b = a;
+        b.bnd.clear(); b.listbc.clear(); b.q0 = b.q1 = -1; b.ffl = -1;
+        b.levelptr = a.levelptr; a.levelptr = mn;
+        if (dir == 0) { b.ihi = a.ihi; a.ihi = a.ilo + nl - 1; b.ilo = a.ihi + 1; b.xlo = mid; a.xhi = mid; }
+        else if (dir == 1) { b.jhi = a.jhi; a.jhi = a.jlo + nl - 1; b.jlo = a.jhi + 1; b.ylo = mid; a.yhi = mid; }
+        else { b.khi = a.khi; a.khi = a.klo + nl - 1; b.klo = a.khi + 1; b.zlo = mid; a.zhi = mid; }
+      } else {
+        m = node[m].levelptr;
+        if (m == 0) break;
+      }
+    }
+  }
+
+  // ================================================================ fill-program compiler
+  Bc3Op make_bc(Tgt3 t, double hx, double hy, double hz, double xl, double xr, double yl, double yr, double zl, double zr, bool& any) {
+    Bc3Op b{};
+    b.dst_patch = t.patch; b.dst_rect = t.rect; b.nrow = t.ni; b.ncol = t.nj; b.nfil = t.nk;
+    any = false;
+    const double hxm = hx * .01, hym = hy * .01, hzm = hz * .01;
+    if (xl < xlower - hxm) { b.nxl = (int)((xlower + hxm - xl) / hx); b.bxl = p.mthbc[1]; any = true; }
+    if (xr > xupper + hxm) { const int n = (int)((xr - xupper + hxm) / hx); b.ibeg = std::max(t.ni - n + 1, 1); b.bxr = p.mthbc[2]; any = true; }
+    if (yl < ylower - hym) { b.nyl = (int)((ylower + hym - yl) / hy); b.byl = p.mthbc[3]; any = true; }
+    if (yr > yupper + hym) { const int n = (int)((yr - yupper + hym) / hy); b.jbeg = std::max(t.nj - n + 1, 1); b.byr = p.mthbc[4]; any = true; }
+    if (zl < zlower - hzm) { b.nzl = (int)((zlower + hzm - zl) / hz); b.bzl = p.mthbc[5]; any = true; }
+    if (zr > zupper + hzm) { const int n = (int)((zr - zupper + hzm) / hz); b.kbeg = std::max(t.nk - n + 1, 1); b.bzr = p.mthbc[6]; any = true; }
+    return b;
+  }
+
+  // boxes of cells with mask == 0 (merged row runs per plane, then along k)
+  static void runs3(const std::vector<int8_t>& mask, int ni, int nj, int nk, std::vector<std::array<int, 6>>& out) {
+    out.clear();
+    std::vector<std::array<int, 6>> prevk;
+    for (int k = 0; k < nk; ++k) {
+      std::vector<std::array<int, 6>> cur;  // i0, j0, k0, w, h, d
+      std::vector<int> prevrow;             // runs of the previous row: i0, w, index into cur
+      for (int j = 0; j < nj; ++j) {
+        std::vector<int> row;
+        int i = 0;
+        while (i < ni) {
+          if (mask[((size_t)k * nj + j) * ni + i] != 0) { ++i; continue; }
+          int e = i;
+          while (e < ni && mask[((size_t)k * nj + j) * ni + e] == 0) ++e;
+          int idx = -1;
+          for (size_t q = 0; q < prevrow.size(); q += 3)
+            if (prevrow[q] == i && prevrow[q + 1] == e - i) { idx = prevrow[q + 2]; break; }
+          if (idx >= 0) cur[idx][4] += 1;
+          else { idx = (int)cur.size(); cur.push_back({i, j, k, e - i, 1, 1}); }
+          row.push_back(i); row.push_back(e - i); row.push_back(idx);
+          i = e;
+        }
+        prevrow.swap(row);
+      }
+      // extend boxes of the previous plane that match exactly
+      std::vector<std::array<int, 6>> next;
+      for (auto& b : cur) {
+        bool merged = false;
+        for (auto& pb : prevk)
+          if (pb[0] == b[0] && pb[1] == b[1] && pb[3] == b[3] && pb[4] == b[4] && pb[2] + pb[5] == k) {
+            pb[5] += 1; merged = true; next.push_back(pb); break;
+          }
+        if (!merged) next.push_back(b);
+      }
+      for (auto& pb : prevk) {
+        bool kept = false;
+        for (auto& n2 : next) if (n2[0] == pb[0] && n2[1] == pb[1] && n2[2] == pb[2] && n2[3] == pb[3] && n2[4] == pb[4]) kept = true;
+        if (!kept) out.push_back(pb);
+      }
+      prevk.swap(next);
+    }
+    for (auto& b : prevk) out.push_back(b);
+  }
+
+  // filpatch.f:4-282 (with intfil.f, trimbd.f) as a program; returns the stage completing the region
+  int c_filrecur(Prog3& P, int level, Tgt3 T, int nrowst, int ncolst, int nfilst, int ilo, int ihi, int jlo, int jhi, int klo,
+                 int khi, bool patchOnly, int msrc) {
+    const int ni = ihi - ilo + 1, nj = jhi - jlo + 1, nk = khi - klo + 1;
+    std::vector<int8_t> used((size_t)ni * nj * nk, 0);
+    auto U = [&](int i, int j, int k) -> int8_t& { return used[((size_t)(k - klo) * nj + (j - jlo)) * ni + (i - ilo)]; };
+    std::vector<Fill3Op> copies;
+    std::vector<int> src;
+    if (msrc == -1) {
+      const GridIndex& X = GI(level);
+      std::vector<int> hits;
+      X.query(ilo, ihi, jlo, jhi, klo, khi, hits);
+      for (int r : hits) src.push_back(X.id(r));
+    } else src = node[msrc].bnd;
+    for (int m : src) {
+      const HPatch3& g = node[m];
+      const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi);
+      const int jxlo = std::max(g.jlo, jlo), jxhi = std::min(g.jhi, jhi);
+      const int kxlo = std::max(g.klo, klo), kxhi = std::min(g.khi, khi);
+      if (!((ixlo <= ixhi && jxlo <= jxhi) && kxlo <= kxhi)) continue;
+      Fill3Op o{};
+      o.kind = F3_COPY; o.dst_patch = T.patch; o.dst_rect = T.rect;
+      o.di0 = nrowst - 1 + (ixlo - ilo); o.dj0 = ncolst - 1 + (jxlo - jlo); o.dk0 = nfilst - 1 + (kxlo - klo);
+      o.ni = ixhi - ixlo + 1; o.nj = jxhi - jxlo + 1; o.nk = kxhi - kxlo + 1;
+      o.src = m; o.si0 = ixlo - g.ilo + G3; o.sj0 = jxlo - g.jlo + G3; o.sk0 = kxlo - g.klo + G3; o.level = level;
+      copies.push_back(o);
+      for (int k = kxlo; k <= kxhi; ++k) for (int j = jxlo; j <= jxhi; ++j) for (int i = ixlo; i <= ixhi; ++i) U(i, j, k) = 1;
+    }
+    // intfil.f:211-260: cells outside the domain count as set (bounds use the destination offsets as the reference does)
+    auto mark = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
+      for (int k = std::max(k0, klo); k <= std::min(k1, khi); ++k)
+        for (int j = std::max(j0, jlo); j <= std::min(j1, jhi); ++j)
+          for (int i = std::max(i0, ilo); i <= std::min(i1, ihi); ++i) U(i, j, k) = 1;
+    };
+    if (khi >= kregsz[level]) mark(ilo, ihi, jlo, jhi, std::max(kregsz[level], klo), khi);
+    if (klo < 0) mark(ilo, ihi, jlo, jhi, klo, std::min(-1, nfilst + nk - 1));
+    if (jhi >= jregsz[level]) mark(ilo, ihi, std::max(jregsz[level], jlo), jhi, klo, khi);
+    if (jlo < 0) mark(ilo, ihi, jlo, std::min(-1, ncolst + nj - 1), klo, khi);
+    if (ilo < 0) mark(ilo, std::min(-1, nrowst + ni - 1), jlo, jhi, klo, khi);
+    if (ihi >= iregsz[level]) mark(std::max(iregsz[level], ilo), ihi, jlo, jhi, klo, khi);
+    // trimbd.f: bounding box of the unset cells
+    int il = 1 << 30, ir = -(1 << 30), jl = 1 << 30, jr = -(1 << 30), kl = 1 << 30, kr = -(1 << 30);
+    for (int k = klo; k <= khi; ++k) for (int j = jlo; j <= jhi; ++j) for (int i = ilo; i <= ihi; ++i)
+      if (!U(i, j, k)) { il = std::min(il, i); ir = std::max(ir, i); jl = std::min(jl, j); jr = std::max(jr, j); kl = std::min(kl, k); kr = std::max(kr, k); }
+    int stage = 0;
+    if (ir >= il) {
+      if (level == 1) throw std::runtime_error("ghost fill: level 1 cells not covered");
+      const int rx = intratx[level - 1], ry = intraty[level - 1], rz = intratz[level - 1];
+      const int iplo = (il - rx + G3 * rx) / rx - G3, jplo = (jl - ry + G3 * ry) / ry - G3, kplo = (kl - rz + G3 * rz) / rz - G3;
+      const int iphi = (ir + rx) / rx, jphi = (jr + ry) / ry, kphi = (kr + rz) / rz;
+      const int nrowc = iphi - iplo + 1, ncolc = jphi - jplo + 1, nfilc = kphi - kplo + 1;
+      if (nrowc > ni + 2 || ncolc > nj + 2 || nfilc > nk + 2) throw std::runtime_error("ghost fill: coarse box too large");
+      const int R = P.add_rect(nrowc, ncolc, nfilc, nvar);
+      const int cst = c_filrecur(P, level - 1, Tgt3{-1, R, nrowc, ncolc, nfilc}, 1, 1, 1, iplo, iphi, jplo, jphi, kplo, kphi, true, -1);
+      stage = cst + 1;
+      std::vector<std::array<int, 6>> boxes;
+      runs3(used, ni, nj, nk, boxes);
+      for (auto& b : boxes) {
+        Fill3Op o{};
+        o.kind = F3_INTERP; o.dst_patch = T.patch; o.dst_rect = T.rect;
+        o.di0 = nrowst - 1 + b[0]; o.dj0 = ncolst - 1 + b[1]; o.dk0 = nfilst - 1 + b[2];
+        o.ni = b[3]; o.nj = b[4]; o.nk = b[5];
+        o.src = R; o.si0 = ilo + b[0]; o.sj0 = jlo + b[1]; o.sk0 = klo + b[2]; o.level = level;
+        o.cilo = iplo; o.cjlo = jplo; o.cklo = kplo;
+        P.add_op(o, stage);
+      }
+    }
+    for (auto& o : copies) P.add_op(o, stage);
+    if (patchOnly) {
+      bool any;
+      const double hx = hxposs[level], hy = hyposs[level], hz = hzposs[level];
+      Bc3Op b = make_bc(T, hx, hy, hz, xlower + (double)ilo * hx, xlower + (double)(ihi + 1) * hx, ylower + (double)jlo * hy,
+                        ylower + (double)(jhi + 1) * hy, zlower + (double)klo * hz, zlower + (double)(khi + 1) * hz, any);
+      if (any) P.add_bc(b, stage);
+    }
+    return stage;
+  }
+
+  // bound.f:4-211 for one patch
+  void compile_bound_patch(Prog3& P, int lev, int m) {
+    const HPatch3& g = node[m];
+    const int mi = mitot(m), mj = mjtot(m), mk = mktot(m);
+    Tgt3 T{m, -1, mi, mj, mk};
+    int s = 0;
+    s = std::max(s, c_filrecur(P, lev, T, 1, 1, G3 + 1, g.ilo - G3, g.ilo - 1, g.jlo - G3, g.jhi + G3, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, mi - G3 + 1, 1, G3 + 1, g.ihi + 1, g.ihi + G3, g.jlo - G3, g.jhi + G3, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, G3 + 1, 1, G3 + 1, g.ilo, g.ihi, g.jlo - G3, g.jlo - 1, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, G3 + 1, mj - G3 + 1, G3 + 1, g.ilo, g.ihi, g.jhi + 1, g.jhi + G3, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, 1, 1, 1, g.ilo - G3, g.ihi + G3, g.jlo - G3, g.jhi + G3, g.klo - G3, g.klo - 1, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, 1, 1, mk - G3 + 1, g.ilo - G3, g.ihi + G3, g.jlo - G3, g.jhi + G3, g.khi + 1, g.khi + G3, false, m));
+    const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
+    bool any;
+    Bc3Op b = make_bc(T, hx, hy, hz, g.xlo - G3 * hx, g.xhi + G3 * hx, g.ylo - G3 * hy, g.yhi + G3 * hy, g.zlo - G3 * hz, g.zhi + G3 * hz, any);
+    if (any) P.add_bc(b, s);
+  }
+  void compile_bound(int lev) {
+    HPROF("compile_bound3");
+    Prog3& P = plan[lev].bound;
+    P.clear();
+    for (int l = 1; l <= lev; ++l) GI(l);
+    const std::vector<int>& G = lgrids[lev];
+    std::vector<Prog3> part(G.size());
+    pool_host.run((int)G.size(), [&](int k) { compile_bound_patch(part[k], lev, G[k]); });
+    for (auto& q : part) merge_prog(P, q);
+    upload_prog(P);
+  }
+
+  // icall.f / intcopy.f: copies of store1 of the grids of `level` into a target
+  void c_icall(Prog3& P, Tgt3 T, int ilo, int ihi, int jlo, int jhi, int klo, int khi, int level, int iput, int jput, int kput, int st_) {
+    const GridIndex& X = GI(level);
+    std::vector<int> hits;
+    X.query(ilo, ihi, jlo, jhi, klo, khi, hits);
+    for (int r : hits) {
+      const int m = X.id(r);
+      const HPatch3& g = node[m];
+      const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi), jxlo = std::max(g.jlo, jlo), jxhi = std::min(g.jhi, jhi);
+      const int kxlo = std::max(g.klo, klo), kxhi = std::min(g.khi, khi);
+      if (!((ixlo <= ixhi && jxlo <= jxhi) && kxlo <= kxhi)) continue;
+      Fill3Op o{};
+      o.kind = F3_COPY; o.dst_patch = T.patch; o.dst_rect = T.rect;
+      o.di0 = ixlo - ilo + iput - 1; o.dj0 = jxlo - jlo + jput - 1; o.dk0 = kxlo - klo + kput - 1;
+      o.ni = ixhi - ixlo + 1; o.nj = jxhi - jxlo + 1; o.nk = kxhi - kxlo + 1;
+      o.src = m; o.si0 = ixlo - g.ilo + G3; o.sj0 = jxlo - g.jlo + G3; o.sk0 = kxlo - g.klo + G3; o.level = -1;
+      P.add_op(o, st_);
+    }
+  }
+
+  // saveqc.f:3-111 for the kids at level lev+1
+  void compile_saveqc(int lev) {
+    Prog3& P = plan[lev].saveqc;
+    P.clear();
+    if (lev + 1 > p.mxnest || lstart[lev + 1] == 0) { upload_prog(P); return; }
+    GI(lev);
+    const double hxc = hxposs[lev], hyc = hyposs[lev], hzc = hzposs[lev];
+    const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
+    for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
+      const HPatch3& g = node[k];
+      const int iclo = g.ilo / rx - 1, jclo = g.jlo / ry - 1, kclo = g.klo / rz - 1;
+      const int ichi = (g.ihi + 1) / rx, jchi = (g.jhi + 1) / ry, kchi = (g.khi + 1) / rz;
+      const int nrow = ichi - iclo + 1, ncol = jchi - jclo + 1, nfil = kchi - kclo + 1;
+      const int R = P.add_rect(nrow, ncol, nfil, nvar);
+      Tgt3 T{-1, R, nrow, ncol, nfil};
+      c_icall(P, T, iclo, ichi, jclo, jchi, kclo, kchi, lev, 1, 1, 1, 0);
+      bool any;
+      Bc3Op b = make_bc(T, hxc, hyc, hzc, g.xlo - hxc, g.xhi + hxc, g.ylo - hyc, g.yhi + hyc, g.zlo - hzc, g.zhi + hzc, any);
+      if (any) P.add_bc(b, 0);
+      Fill3Op o{};
+      o.kind = F3_RING; o.dst_patch = k; o.dst_rect = -1; o.ni = g.lenbc; o.nj = 1; o.nk = 1; o.src = R;
+      P.add_op(o, 1);
+    }
+    upload_prog(P);
+  }
+
+  void upload_prog(Prog3& P) {
+    if (P.scratch_off >= 0) pool.release(P.scratch_off, P.scratch_alloc);
+    P.scratch_alloc = std::max<long long>(P.scratch_len, 1);
+    P.scratch_off = pool.alloc(P.scratch_alloc);
+    std::vector<Rect3> rects = P.rects;
+    for (auto& r : rects) r.off += P.scratch_off;
+    P.d_rects.upload(rects, st, stg);
+    std::vector<int> oidx(P.ops.size());
+    for (size_t i = 0; i < oidx.size(); ++i) oidx[i] = (int)i;
+    std::stable_sort(oidx.begin(), oidx.end(), [&](int a, int b) { return P.op_stage[a] < P.op_stage[b]; });
+    std::vector<Fill3Op> ops;
+    std::vector<Fill3Chunk> ch;
+    P.ch_lo.assign(P.nstages, 0); P.ch_hi.assign(P.nstages, 0);
+    int s = -1;
+    for (int k : oidx) {
+      const int stg_ = P.op_stage[k];
+      while (s < stg_) { ++s; P.ch_lo[s] = (int)ch.size(); P.ch_hi[s] = (int)ch.size(); }
+      const int id = (int)ops.size();
+      ops.push_back(P.ops[k]);
+      const long long cells = (long long)P.ops[k].ni * P.ops[k].nj * P.ops[k].nk;
+      for (long long c0 = 0; c0 < cells; c0 += 128) ch.push_back(Fill3Chunk{id, c0, (int)std::min<long long>(128, cells - c0)});
+      P.ch_hi[s] = (int)ch.size();
+    }
+    while (s + 1 < P.nstages) { ++s; P.ch_lo[s] = P.ch_hi[s] = (int)ch.size(); }
+    std::vector<int> bidx(P.bcs.size());
+    for (size_t i = 0; i < bidx.size(); ++i) bidx[i] = (int)i;
+    std::stable_sort(bidx.begin(), bidx.end(), [&](int a, int b) { return P.bc_stage[a] < P.bc_stage[b]; });
+    std::vector<Bc3Op> bcs;
+    P.bc_lo.assign(P.nstages, 0); P.bc_hi.assign(P.nstages, 0);
+    s = -1;
+    for (int k : bidx) {
+      const int stg_ = P.bc_stage[k];
+      while (s < stg_) { ++s; P.bc_lo[s] = (int)bcs.size(); P.bc_hi[s] = (int)bcs.size(); }
+      bcs.push_back(P.bcs[k]);
+      P.bc_hi[s] = (int)bcs.size();
+    }
+    while (s + 1 < P.nstages) { ++s; P.bc_lo[s] = P.bc_hi[s] = (int)bcs.size(); }
+    P.d_ops.upload(ops, st, stg);
+    P.d_chunks.upload(ch, st, stg);
+    P.d_bcs.upload(bcs, st, stg);
+  }
+
+  void run_prog(Prog3& P, const SrcMode& modes) {
+    for (int s = 0; s < P.nstages; ++s) {
+      if (P.ch_hi[s] > P.ch_lo[s]) {
+        Fill3Args a{};
+        a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
+        a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
+        a.lc = lc; a.xlower = xlower; a.ylower = ylower; a.zlower = zlower;
+        launch_fill3(a, st);
+        ++nkernels;
+      }
+      if (P.bc_hi[s] > P.bc_lo[s]) {
+        Bc3Args b{};
+        b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.bc_lo[s];
+        b.nops = P.bc_hi[s] - P.bc_lo[s]; b.nvar = nvar;
+        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st);
+        nkernels += 3;
+      }
+    }
+  }
+
+  // ================================================================ step plan, registers, update plan
+  void compile_step(int lev) {
+    HPROF("compile_step3");
+    Plan3& L = plan[lev];
+    L.plist = lgrids[lev];
+    const int np = (int)L.plist.size();
+    L.sweep0.assign((size_t)3 * (np + 1), 0);
+    L.face0.assign(np + 1, 0); L.cell0.assign(np + 1, 0);
+    long long slot = 0;
+    for (int d = 0; d < 3; ++d) {
+      for (int k = 0; k < np; ++k) {
+        const HPatch3& g = node[L.plist[k]];
+        const long long mx = g.nx(), my = g.ny(), mz = g.nz();
+        L.sweep0[(size_t)d * (np + 1) + k] = slot;
+        slot += d == 0 ? (my + 2) * (mz + 2) * (mx + 1) : d == 1 ? (mx + 2) * (mz + 2) * (my + 1) : (mx + 2) * (my + 2) * (mz + 1);
+      }
+      L.sweep0[(size_t)d * (np + 1) + np] = slot;
+      L.items[d] = L.sweep0[(size_t)d * (np + 1) + np] - L.sweep0[(size_t)d * (np + 1)];
+    }
+    L.slots = slot;
+    for (int k = 0; k < np; ++k) {
+      const HPatch3& g = node[L.plist[k]];
+      L.face0[k + 1] = L.face0[k] + (long long)(g.nx() + 1) * (g.ny() + 1) * (g.nz() + 1);
+      L.cell0[k + 1] = L.cell0[k] + (long long)g.nx() * g.ny() * g.nz();
+    }
+    L.faces = L.face0[np]; L.cells = L.cell0[np];
+    L.fsv.clear(); L.fad.clear(); L.qad.clear();
+    for (int k = 0; k < np; ++k) {
+      const int m = L.plist[k];
+      const HPatch3& g = node[m];
+      if (g.has_cfl)
+        for (size_t e = 0; e + 5 < g.listbc.size(); e += 6) {
+          const int* b = &g.listbc[e];
+          Fsv3 f{};
+          f.patch = m; f.pidx = k; f.i = b[0] - G3; f.j = b[1] - G3; f.k = b[2] - G3; f.side = b[3];
+          f.dst = node[b[4]].ffl + (long long)nvar * (b[5] - 1);
+          L.fsv.push_back(f);
+        }
+      if (lev > 1 && g.ffl >= 0) {
+        const int rx = intratx[lev - 1], ry = intraty[lev - 1], rz = intratz[lev - 1];
+        const int nxc_ = g.nx() / rx, nyc_ = g.ny() / ry, nzc_ = g.nz() / rz;
+        int seg = 0;
+        auto add = [&](int side, int na, int nb, int ra, int rb) {
+          for (int bc = 0; bc < nb; ++bc)
+            for (int ac = 0; ac < na; ++ac) {
+              L.fad.push_back(Fad3{m, k, side, ac * ra, bc * rb, ra, rb, seg});
+              Qad3Job q{};
+              q.patch = m; q.side = side; q.slab = bc; q.row0 = ac * ra; q.nreg = 1; q.reg0 = seg; q.ratio_a = ra; q.ratio_b = rb;
+              L.qad.push_back(q);
+              ++seg;
+            }
+        };
+        add(1, nyc_, nzc_, ry, rz);
+        add(2, nxc_, nzc_, rx, rz);
+        add(3, nyc_, nzc_, ry, rz);
+        add(4, nxc_, nzc_, rx, rz);
+        add(5, nxc_, nyc_, rx, ry);
+        add(6, nxc_, nyc_, rx, ry);
+      }
+    }
+    L.d_plist.upload(L.plist, st, stg);
+    L.d_sweep0.upload(L.sweep0, st, stg);
+    L.d_face0.upload(L.face0, st, stg);
+    L.d_cell0.upload(L.cell0, st, stg);
+    L.d_fsv.upload(L.fsv, st, stg);
+    L.d_fad.upload(L.fad, st, stg);
+    L.d_qad.upload(L.qad, st, stg);
+    // staging and face-flux buffers sized for the largest level
+    d_stash.ensure(std::max<size_t>(d_stash.n, (size_t)(L.slots * STASH3)));
+    d_flux.ensure(std::max<size_t>(d_flux.n, (size_t)(L.faces * 30)));
+  }
+
+  // update.f:4-192 + upbnd.f:4-94 for coarse level lev
+  void compile_update(int lev) {
+    HPROF("compile_update3");
+    Plan3& L = plan[lev];
+    L.upc.clear(); L.upt.clear(); L.avg.clear();
+    if (lev < p.mxnest && lstart[lev + 1] != 0) {
+      const GridIndex& XF = GI(lev + 1);
+      std::vector<int> hits;
+      const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
+      const double chsign[7] = {0, 1., -1., -1., 1., 1., -1.};
+      for (int m : lgrids[lev]) {
+        const HPatch3& g = node[m];
+        if (g.has_cfl) {
+          const int mi = mitot(m), mj = mjtot(m), mk = mktot(m);
+          std::vector<int> used((size_t)mi * mj * mk, 0), slot((size_t)mi * mj * mk, -1), order;
+          std::vector<std::vector<Upbnd3Term>> terms;
+          for (size_t e = 0; e + 5 < g.listbc.size(); e += 6) {
+            const int* b = &g.listbc[e];
+            const int side = b[3], norm = 1 << (side - 1);
+            const size_t key = ((size_t)(b[2] - 1) * mj + (b[1] - 1)) * mi + (b[0] - 1);
+            if ((used[key] / norm) % 2 == 1) continue;
+            if (slot[key] < 0) { slot[key] = (int)terms.size(); terms.emplace_back(); order.push_back((int)key); }
+            terms[slot[key]].push_back(Upbnd3Term{node[b[4]].ffl + (long long)nvar * (b[5] - 1), chsign[side]});
+            used[key] += norm;
+          }
+          for (int key : order) {
+            Upbnd3Cell c{};
+            c.patch = m; c.ie = key % mi; c.je = (key / mi) % mj; c.ke = key / (mi * mj);
+            const auto& T = terms[slot[key]];
+            c.first = (int)L.upt.size(); c.count = (int)T.size();
+            L.upt.insert(L.upt.end(), T.begin(), T.end());
+            L.upc.push_back(c);
+          }
+        }
+        XF.query(g.ilo * rx, g.ihi * rx + rx - 1, g.jlo * ry, g.jhi * ry + ry - 1, g.klo * rz, g.khi * rz + rz - 1, hits);
+        for (int r : hits) {
+          const int kk = XF.id(r);
+          const HPatch3& f = node[kk];
+          const int iclo = f.ilo / rx, jclo = f.jlo / ry, kclo = f.klo / rz, ichi = f.ihi / rx, jchi = f.jhi / ry, kchi = f.khi / rz;
+          const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), kplo = std::max(g.klo, kclo);
+          const int iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi), kphi = std::min(g.khi, kchi);
+          if (iplo > iphi || jplo > jphi || kplo > kphi) continue;
+          Avg3 a{};
+          a.cpatch = m; a.kpatch = kk;
+          a.ci0 = iplo - g.ilo + G3; a.cj0 = jplo - g.jlo + G3; a.ck0 = kplo - g.klo + G3;
+          a.ni = iphi - iplo + 1; a.nj = jphi - jplo + 1; a.nk = kphi - kplo + 1;
+          a.fi0 = iplo * rx - f.ilo + G3; a.fj0 = jplo * ry - f.jlo + G3; a.fk0 = kplo * rz - f.klo + G3;
+          L.avg.push_back(a);
+        }
+      }
+    }
+    L.d_upc.upload(L.upc, st, stg); L.d_upt.upload(L.upt, st, stg); L.d_avg.upload(L.avg, st, stg);
+  }
+
+  // prepf.f:4-41
+  void prepf(int lev) {
+    std::vector<std::pair<long long, long long>> zr;
+    for (int k = lstart[lev]; k != 0; k = node[k].levelptr) {
+      HPatch3& g = node[k];
+      const int ik = g.nx() / intratx[lev - 1], jk = g.ny() / intraty[lev - 1], kk = g.nz() / intratz[lev - 1];
+      g.lenbc = 2 * (ik * jk + jk * kk + kk * ik);
+      if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
+      g.nffl = (long long)2 * nvar * g.lenbc;
+      g.ffl = regs.alloc(g.nffl);
+      zr.emplace_back(g.ffl, Arena::rnd(g.nffl));
+    }
+    std::sort(zr.begin(), zr.end());
+    for (size_t a = 0; a < zr.size();) {
+      long long lo = zr[a].first, hi = zr[a].first + zr[a].second;
+      size_t b = a + 1;
+      while (b < zr.size() && zr[b].first <= hi) { hi = std::max(hi, zr[b].first + zr[b].second); ++b; }
+      AMR_CUDA(cudaMemsetAsync(regs.d + lo, 0, sizeof(double) * (hi - lo), st));
+      a = b;
+    }
+  }
+  // setuse.f:4-173
+  void setuse(std::vector<int>& lb, int mkid, const HPatch3& p_, int iclo, int ichi, int jclo, int jchi, int kclo, int kchi) {
+    auto put = [&](int i, int j, int k, int side, int lkid) { lb.insert(lb.end(), {i, j, k, side, mkid, lkid}); };
+    const int ilo = p_.ilo, ihi = p_.ihi, jlo = p_.jlo, jhi = p_.jhi, klo = p_.klo, khi = p_.khi;
+    const int ist = iclo - 1, iend = ichi + 1, jst = jclo - 1, jend = jchi + 1, kst = kclo - 1, kend = kchi + 1;
+    const int ni = ichi - iclo + 1, nj = jchi - jclo + 1, nk = kchi - kclo + 1;
+    if (!(ist < ilo))
+      for (int k = std::max(klo, kclo); k <= std::min(khi, kchi); ++k) {
+        int lkid = (k - kclo) * nj + std::max(jlo, jclo) - jclo + 1;
+        for (int j = std::max(jlo, jclo); j <= std::min(jhi, jchi); ++j) put(ist - ilo + G3 + 1, j - jlo + G3 + 1, k - klo + G3 + 1, 3, lkid++);
+      }
+    if (!(jend > jhi))
+      for (int k = std::max(klo, kclo); k <= std::min(khi, kchi); ++k) {
+        int lkid = nk * nj + (k - kclo) * ni + std::max(ilo, iclo) - iclo + 1;
+        for (int i = std::max(ilo, iclo); i <= std::min(ihi, ichi); ++i) put(i - ilo + G3 + 1, jend - jlo + G3 + 1, k - klo + G3 + 1, 4, lkid++);
+      }
+    if (!(iend > ihi))
+      for (int k = std::max(klo, kclo); k <= std::min(khi, kchi); ++k) {
+        int lkid = nk * nj + nk * ni + (k - kclo) * nj + std::max(jlo, jclo) - jclo + 1;
+        for (int j = std::max(jlo, jclo); j <= std::min(jhi, jchi); ++j) put(iend - ilo + G3 + 1, j - jlo + G3 + 1, k - klo + G3 + 1, 1, lkid++);
+      }
+    if (!(jst < jlo))
+      for (int k = std::max(klo, kclo); k <= std::min(khi, kchi); ++k) {
+        int lkid = 2 * nk * nj + nk * ni + (k - kclo) * ni + std::max(ilo, iclo) - iclo + 1;
+        for (int i = std::max(ilo, iclo); i <= std::min(ihi, ichi); ++i) put(i - ilo + G3 + 1, jst - jlo + G3 + 1, k - klo + G3 + 1, 2, lkid++);
+      }
+    if (!(kst < klo))
+      for (int j = std::max(jlo, jclo); j <= std::min(jhi, jchi); ++j) {
+        int lkid = 2 * nk * nj + 2 * nk * ni + (j - jclo) * ni + std::max(ilo, iclo) - iclo + 1;
+        for (int i = std::max(ilo, iclo); i <= std::min(ihi, ichi); ++i) put(i - ilo + G3 + 1, j - jlo + G3 + 1, kst - klo + G3 + 1, 6, lkid++);
+      }
+    if (!(kend > khi))
+      for (int j = std::max(jlo, jclo); j <= std::min(jhi, jchi); ++j) {
+        int lkid = 2 * nk * nj + 2 * nk * ni + nj * ni + (j - jclo) * ni + std::max(ilo, iclo) - iclo + 1;
+        for (int i = std::max(ilo, iclo); i <= std::min(ihi, ichi); ++i) put(i - ilo + G3 + 1, j - jlo + G3 + 1, kend - klo + G3 + 1, 5, lkid++);
+      }
+  }
+  // prepc.f:4-138
+  void prepc(int lev) {
+    int maxsp = 0;
+    for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
+      const HPatch3& f = node[k];
+      const int ik = f.nx() / intratx[lev], jk = f.ny() / intraty[lev], kk = f.nz() / intratz[lev];
+      maxsp += 2 * (ik * jk + jk * kk + kk * ik);
+    }
+    listsp[lev] = maxsp;
+    if (maxsp == 0) return;
+    const GridIndex& XF = GI(lev + 1);
+    std::vector<int> hits;
+    const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
+    for (int mp = lstart[lev]; mp != 0; mp = node[mp].levelptr) {
+      HPatch3& g = node[mp];
+      g.listbc.clear();
+      g.has_cfl = true;
+      XF.query((g.ilo - 1) * rx, (g.ihi + 2) * rx - 1, (g.jlo - 1) * ry, (g.jhi + 2) * ry - 1, (g.klo - 1) * rz, (g.khi + 2) * rz - 1, hits);
+      for (int r : hits) {
+        const int k = XF.id(r);
+        const HPatch3& f = node[k];
+        const int iclo = f.ilo / rx, jclo = f.jlo / ry, kclo = f.klo / rz, ichi = f.ihi / rx, jchi = f.jhi / ry, kchi = f.khi / rz;
+        const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), kplo = std::max(g.klo, kclo);
+        const int iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi), kphi = std::min(g.khi, kchi);
+        if ((iplo <= iphi + 1 && jplo <= jphi + 1) && kplo <= kphi + 1) setuse(g.listbc, k, g, iclo, ichi, jclo, jchi, kclo, kchi);
+      }
+    }
+  }
+
+  void compile_all(int lbase = 0) {
+    sync_descriptors();
+    for (int lev = 1; lev <= p.mxnest; ++lev) {
+      if (lev > lfine) { plan[lev].plist.clear(); continue; }
+      if (lev > lbase) compile_bound(lev);
+      if (lev >= lbase) {
+        compile_saveqc(lev);
+        compile_step(lev);
+        compile_update(lev);
+      }
+    }
+  }
+
+  // ================================================================ level substep
+  // intfil.f:115-154: which buffer of a source level serves time t (teps = possk/10)
+  SrcMode modes_for(int level, double t) {
+    SrcMode M{};
+    for (int l = 1; l <= level; ++l) {
+      if (lgrids[l].empty()) continue;
+      const double gt = node[lgrids[l][0]].time;
+      const double dt = possk[l];
+      const double teps = dt / 10.0;
+      const double ac = (gt - t) / dt, ai = 1.0 - ac;
+      M.alphai[l] = ai; M.alphac[l] = ac;
+      if (ai < -teps || ai > 1.0 + teps) { M.mode[l] = 0; continue; }
+      if (std::fabs(ai - 1.0) < teps) M.mode[l] = 0;
+      else if (std::fabs(ai) < teps) M.mode[l] = 1;
+      else M.mode[l] = 2;
+    }
+    return M;
+  }
+  void bound_level(int lev, double t) { run_prog(plan[lev].bound, modes_for(lev, t)); }
+
+  // advanc.f:4-139 with par_advanc (:166-303) for all patches of the level at once
+  double advanc(int lev) {
+    HPROF("advanc3");
+    Plan3& L = plan[lev];
+    const double t = node[lgrids[lev][0]].time;
+    const double dt = possk[lev];
+    bound_level(lev, t);
+    if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
+    if (lev > 1 && !L.qad.empty()) {
+      launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st);
+      ++nkernels;
+    }
+    sample_gauges(lev);
+    AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+    if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
+    Step3Args a{};
+    a.pool = pool.d; a.patches = d_patches.d; a.sp = sp;
+    a.stash = d_stash.d; a.stash_stride = L.slots; a.flux = d_flux.d; a.flux_stride = L.faces;
+    a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.dz = hzposs[lev]; a.cflmax = d_cfl;
+    if (batched) {
+      a.plist = L.d_plist.d; a.np = (int)L.plist.size();
+      a.sweep0 = L.d_sweep0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
+      launch_step3(a, L.items, L.faces, L.cells, st);
+      nkernels += 5;
+    } else {
+      // one patch per launch sequence: per-patch prefix arrays are views of the level's
+      const int np = (int)L.plist.size();
+      if ((int)pp_sweep.size() != np) build_plain_views(L);
+      for (int k = 0; k < np; ++k) {
+        Step3Args b = a;
+        b.plist = L.d_plist.d + k; b.np = 1;
+        b.sweep0 = d_pp_sweep.d + (size_t)6 * k; b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
+        long long it[3];
+        for (int d = 0; d < 3; ++d) it[d] = L.sweep0[(size_t)d * (np + 1) + k + 1] - L.sweep0[(size_t)d * (np + 1) + k];
+        launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st);
+        nkernels += 5;
+      }
+    }
+    if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
+    if (!L.fsv.empty()) {
+      launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
+      ++nkernels;
+    }
+    if (!L.fad.empty()) {
+      launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.fad.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
+      ++nkernels;
+    }
+    flip_level(lev);
+    unsigned long long cbits = 0;
+    AMR_CUDA(cudaMemcpyAsync(&cbits, d_cfl, sizeof(cbits), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    double cmax;
+    std::memcpy(&cmax, &cbits, sizeof(double));
+    if (profile) {
+      float ms = 0;
+      AMR_CUDA(cudaEventElapsedTime(&ms, ev_a, ev_b));
+      step_kernel_ms += ms;
+      step_kernel_cells += (double)L.cells;
+    }
+    for (int m : lgrids[lev]) {
+      node[m].time = node[m].time + dt;
+      const double cells = (double)node[m].nx() * node[m].ny() * node[m].nz();
+      rvol += cells; rvoll[lev] += cells;
+    }
+    cfl_level = cmax;
+    cflmax_run = std::max(cflmax_run, cmax);
+    ++nsteps_launched;
+    return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
+  }
+  // per-patch sweep prefix views for the plain path: [x0, x1, y0, y1, z0, z1] per patch
+  std::vector<long long> pp_sweep;
+  DBuf<long long> d_pp_sweep;
+  void build_plain_views(Plan3& L) {
+    const int np = (int)L.plist.size();
+    pp_sweep.assign((size_t)6 * np, 0);
+    for (int k = 0; k < np; ++k)
+      for (int d = 0; d < 3; ++d) {
+        pp_sweep[(size_t)6 * k + 2 * d] = L.sweep0[(size_t)d * (np + 1) + k];
+        pp_sweep[(size_t)6 * k + 2 * d + 1] = L.sweep0[(size_t)d * (np + 1) + k + 1];
+      }
+    d_pp_sweep.upload(pp_sweep, st, stg);
+  }
+  // the new values were written to the other buffer: swap store1 / store2 of every patch of the level
+  void flip_level(int lev) {
+    for (int m : lgrids[lev]) { node[m].cur ^= 1; h_patches[m].cur = node[m].cur; }
+    // descriptors of this level only: a small upload
+    for (int m : lgrids[lev])
+      AMR_CUDA(cudaMemcpyAsync(d_patches.d + m, stg.put(&h_patches[m], sizeof(PatchDev), st), sizeof(PatchDev), cudaMemcpyHostToDevice, st));
+  }
+
+  // update.f:4-192 (upbnd then averaging)
+  void update(int lev) {
+    Plan3& L = plan[lev];
+    const double vol = hxposs[lev] * hyposs[lev] * hzposs[lev];
+    launch_upbnd3(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, vol, nvar, st);
+    launch_average3(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), intratx[lev], intraty[lev], intratz[lev], nvar, st);
+    nkernels += 2;
+  }
+
+  // ================================================================ gauges (gauges_module.f90:302-460)
+  void setbestsrc() {
+    mbestsrc.assign(p.gauges.size(), 0);
+    for (size_t i = 0; i < p.gauges.size(); ++i)
+      for (int lev = lfine; lev >= 1 && mbestsrc[i] == 0; --lev)
+        for (int m = lstart[lev]; m != 0; m = node[m].levelptr) {
+          const HPatch3& g = node[m];
+          const GaugeSpec& G = p.gauges[i];
+          if (G.x >= g.xlo && G.x <= g.xhi && G.y >= g.ylo && G.y <= g.yhi && G.z >= g.zlo && G.z <= g.zhi) { mbestsrc[i] = m; break; }
+        }
+  }
+  void sample_gauges(int lev) {
+    if (!record_gauges || p.gauges.empty()) return;
+    std::vector<Gauge3Job> jobs;
+    const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
+    for (size_t i = 0; i < p.gauges.size(); ++i) {
+      const int m = mbestsrc[i];
+      if (m == 0 || node[m].level != lev) continue;
+      const GaugeSpec& G = p.gauges[i];
+      const double tg = node[m].time;
+      if (tg < G.t1 || tg > G.t2) continue;
+      if (tg - glast[i] < G.min_inc) continue;
+      const double xlow = node[m].xlo - G3 * hx, ylow = node[m].ylo - G3 * hy, zlow = node[m].zlo - G3 * hz;
+      Gauge3Job J{};
+      J.patch = m;
+      J.ii = (int)(0.5 + (G.x - xlow) / hx); J.jj = (int)(0.5 + (G.y - ylow) / hy); J.kk = (int)(0.5 + (G.z - zlow) / hz);
+      J.xoff = (G.x - (xlow + (J.ii - 0.5) * hx)) / hx; J.yoff = (G.y - (ylow + (J.jj - 0.5) * hy)) / hy;
+      J.zoff = (G.z - (zlow + (J.kk - 0.5) * hz)) / hz;
+      J.slot = gslots++;
+      jobs.push_back(J);
+      grows.push_back(GRow{G.num, lev, tg, J.slot});
+      glast[i] = tg;
+    }
+    if (jobs.empty()) return;
+    if ((size_t)gslots * nvar > d_gauge_out.cap) {
+      DBuf<double> nb; nb.ensure(std::max<size_t>((size_t)gslots * nvar * 2, 4096));
+      if (d_gauge_out.d) AMR_CUDA(cudaMemcpyAsync(nb.d, d_gauge_out.d, sizeof(double) * d_gauge_out.cap, cudaMemcpyDeviceToDevice, st));
+      sync_stream();
+      d_gauge_out.free(); d_gauge_out = nb;
+    }
+    DBuf<Gauge3Job> dj; dj.upload(jobs, st, stg);
+    launch_gauges3(pool.d, d_patches.d, dj.d, (int)jobs.size(), nvar, d_gauge_out.d, st);
+    sync_stream();
+    dj.free();
+  }
+
+  // ================================================================ regrid (host flag arrays)
+  void extend_borders(I1& f, int is, int js, int ks) {
+    for (int k = 1; k <= ks; ++k) for (int j = 1; j <= js; ++j) { if (f(1, j, k) == 1) f(0, j, k) = 1; if (f(is, j, k) == 1) f(is + 1, j, k) = 1; }
+    for (int k = 1; k <= ks; ++k) for (int i = 1; i <= is; ++i) { if (f(i, 1, k) == 1) f(i, 0, k) = 1; if (f(i, js, k) == 1) f(i, js + 1, k) = 1; }
+    for (int j = 1; j <= js; ++j) for (int i = 1; i <= is; ++i) { if (f(i, j, 1) == 1) f(i, j, 0) = 1; if (f(i, j, ks) == 1) f(i, j, ks + 1) = 1; }
+  }
+  void fill_edges_corners(I1& f, int is, int js, int ks) {
+    for (int k = 1; k <= ks; ++k) {
+      if (f(0, 1, k) + f(1, 0, k) == 2) f(0, 0, k) = 1;
+      if (f(0, js, k) + f(1, js + 1, k) == 2) f(0, js + 1, k) = 1;
+      if (f(is, 0, k) + f(is + 1, 1, k) == 2) f(is + 1, 0, k) = 1;
+      if (f(is, js + 1, k) + f(is + 1, js, k) == 2) f(is + 1, js + 1, k) = 1;
+    }
+    for (int i = 1; i <= is; ++i) {
+      if (f(i, 0, 1) + f(i, 1, 0) == 2) f(i, 0, 0) = 1;
+      if (f(i, js, 0) + f(i, js + 1, 1) == 2) f(i, js + 1, 0) = 1;
+      if (f(i, 0, ks) + f(i, 1, ks + 1) == 2) f(i, 0, ks + 1) = 1;
+      if (f(i, js + 1, ks) + f(i, js, ks + 1) == 2) f(i, js + 1, ks + 1) = 1;
+    }
+    for (int j = 1; j <= js; ++j) {
+      if (f(0, j, 1) + f(1, j, 0) == 2) f(0, j, 0) = 1;
+      if (f(is, j, 0) + f(is + 1, j, 1) == 2) f(is + 1, j, 0) = 1;
+      if (f(0, j, ks) + f(1, j, ks + 1) == 2) f(0, j, ks + 1) = 1;
+      if (f(is + 1, j, ks) + f(is, j, ks + 1) == 2) f(is + 1, j, ks + 1) = 1;
+    }
+    if (f(0, 0, 1) + f(0, 1, 0) + f(1, 0, 0) == 3) f(0, 0, 0) = 1;
+    if (f(is + 1, 0, 1) + f(is + 1, 1, 0) + f(is, 0, 0) == 3) f(is + 1, 0, 0) = 1;
+    if (f(0, js + 1, 1) + f(0, js, 0) + f(1, js + 1, 0) == 3) f(0, js + 1, 0) = 1;
+    if (f(is + 1, js + 1, 1) + f(is + 1, js, 0) + f(is, js + 1, 0) == 3) f(is + 1, js + 1, 0) = 1;
+    if (f(0, 0, ks) + f(0, 1, ks + 1) + f(1, 0, ks + 1) == 3) f(0, 0, ks + 1) = 1;
+    if (f(is + 1, 0, ks) + f(is + 1, 1, ks + 1) + f(is, 0, ks + 1) == 3) f(is + 1, 0, ks + 1) = 1;
+    if (f(0, js + 1, ks) + f(0, js, ks + 1) + f(1, js + 1, ks + 1) == 3) f(0, js + 1, ks + 1) = 1;
+    if (f(is + 1, js + 1, ks) + f(is + 1, js, ks + 1) + f(is, js + 1, ks + 1) == 3) f(is + 1, js + 1, ks + 1) = 1;
+  }
+  // domprep.f
+  void domprep(I1& f, int lbase, int ib, int jb, int kb) {
+    f.init(ib, jb, kb);
+    for (int m = lstart[lbase]; m != 0; m = node[m].levelptr) {
+      const HPatch3& g = node[m];
+      for (int k = g.klo + 1; k <= g.khi + 1; ++k) for (int j = g.jlo + 1; j <= g.jhi + 1; ++j)
+        std::memset(&f(g.ilo + 1, j, k), 1, (size_t)g.nx());
+    }
+    extend_borders(f, ib, jb, kb);
+    fill_edges_corners(f, ib, jb, kb);
+  }
+  // domshrink.f (27-cell erosion; planes processed on the host threads)
+  void domshrink(I1& in, I1& out, int id, int jd, int kd) {
+    if (out.is != id || out.js != jd || out.ks != kd) out.init(id, jd, kd);
+    pool_host.run(kd, [&](int kk) {
+      const int k = kk + 1;
+      for (int j = 1; j <= jd; ++j)
+        for (int i = 1; i <= id; ++i) {
+          bool ok = true;
+          for (int c = -1; c <= 1 && ok; ++c)
+            for (int b = -1; b <= 1 && ok; ++b) {
+              const int8_t* row = &in(i - 1, j + b, k + c);
+              if (row[0] <= 0 || row[1] <= 0 || row[2] <= 0) ok = false;
+            }
+          out(i, j, k) = ok ? in(i, j, k) : 0;
+        }
+    });
+    extend_borders(out, id, jd, kd);
+  }
+  // domup.f
+  void domup(I1& fine, I1& crse, int ib, int jb, int kb, int is, int js, int ks, int lev) {
+    fine.init(is, js, ks);
+    const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
+    for (int k = 1; k <= kb; ++k) for (int j = 1; j <= jb; ++j) for (int i = 1; i <= ib; ++i) {
+      const int8_t v = crse(i, j, k);
+      if (v == 0) continue;
+      for (int mk = 1; mk <= rz; ++mk) for (int mj = 1; mj <= ry; ++mj) for (int mi = 1; mi <= rx; ++mi)
+        fine((i - 1) * rx + mi, (j - 1) * ry + mj, (k - 1) * rz + mk) = v;
+    }
+    extend_borders(fine, is, js, ks);
+    fill_edges_corners(fine, is, js, ks);
+  }
+
+  // spest.f + flag2refine.f (device) + setflags.f (host add)
+  void spest(int lcheck, I1& flags) {
+    const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
+    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) std::memset(&flags(1, j, k), 0, (size_t)isize);
+    if (!p.flag_gradient) return;
+    const std::vector<int>& G = lgrids[lcheck];
+    const double t = node[G[0]].time;
+    bound_level(lcheck, t);
+    std::vector<long long> c0(G.size() + 1, 0);
+    for (size_t k = 0; k < G.size(); ++k) c0[k + 1] = c0[k] + (long long)node[G[k]].nx() * node[G[k]].ny() * node[G[k]].nz();
+    fl_out.ensure(std::max<long long>(c0.back(), 1));
+    DBuf<long long> dc; dc.upload(c0, st, stg);
+    DBuf<int> dp; dp.upload(G, st, stg);
+    launch_flags3(pool.d, d_patches.d, dp.d, dc.d, (int)G.size(), flag_pressure, sp.gamma1, p.tolsp, nvar, fl_out.d, c0.back(), st);
+    std::vector<int8_t> hf(c0.back());
+    if (c0.back()) AMR_CUDA(cudaMemcpyAsync(hf.data(), fl_out.d, c0.back(), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    dc.free(); dp.free();
+    for (size_t n = 0; n < G.size(); ++n) {
+      const HPatch3& g = node[G[n]];
+      const int8_t* src = hf.data() + c0[n];
+      for (int k = 0; k < g.nz(); ++k)
+        for (int j = 0; j < g.ny(); ++j) {
+          int8_t* row = &flags(g.ilo + 1, g.jlo + 1 + j, g.klo + 1 + k);
+          const int8_t* s = src + ((size_t)k * g.ny() + j) * g.nx();
+          for (int i = 0; i < g.nx(); ++i) row[i] = (int8_t)(row[i] + s[i]);
+        }
+    }
+  }
+
+  // bufnst.f + projec.f + shiftset.f; returns the number of flagged cells
+  int bufnst(int lcheck, I1& f) {
+    const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
+    if (lcheck + 2 <= p.mxnest) {
+      const int lrx = intratx[lcheck] * intratx[lcheck + 1], lry = intraty[lcheck] * intraty[lcheck + 1], lrz = intratz[lcheck] * intratz[lcheck + 1];
+      for (int mk = newstl[lcheck + 2]; mk != 0; mk = node[mk].levelptr) {
+        const HPatch3& c = node[mk];
+        int ist = c.ilo / lrx, jst = c.jlo / lry, kst = c.klo / lrz;
+        int iend = (c.ihi + lrx - 1) / lrx, jend = (c.jhi + lry - 1) / lry, kend = (c.khi + lrz - 1) / lrz;
+        if (p.ibuff == 0) {
+          if (ist * lrx == c.ilo) ist = ist - 1;
+          if (jst * lry == c.jlo) jst = jst - 1;
+          if (kst * lrz == c.klo) kst = kst - 1;
+          if (iend * lrx == c.ihi + 1) iend = iend + 1;
+          if (jend * lry == c.jhi + 1) jend = jend + 1;
+          if (kend * lrz == c.khi + 1) kend = kend + 1;
+        }
+        for (int k = kst + 1; k <= kend + 1; ++k) for (int j = jst + 1; j <= jend + 1; ++j) for (int i = ist + 1; i <= iend + 1; ++i)
+          if (f(i, j, k) == 0) f(i, j, k) = 3;
+      }
+    }
+    for (int k = 0; k <= ksize + 1; ++k) for (int j = 0; j <= jsize + 1; ++j) { f(0, j, k) = 0; f(isize + 1, j, k) = 0; }
+    for (int k = 0; k <= ksize + 1; ++k) for (int i = 0; i <= isize + 1; ++i) { f(i, 0, k) = 0; f(i, jsize + 1, k) = 0; }
+    for (int j = 0; j <= jsize + 1; ++j) for (int i = 0; i <= isize + 1; ++i) { f(i, j, 0) = 0; f(i, j, ksize + 1) = 0; }
+    // shiftset.f: every positive flag, visited in (k, j, i) order, stamps its value on the
+    // (2*ibuff+1)^3 box around it, so a cell ends with the value of the lexicographically last
+    // (k, j, i) source within ibuff of it in every direction. Three separable passes find it:
+    // the last source along i, then the last j-row holding one, then the last k-plane.
+    const int b = p.ibuff;
+    I1 f2, t1, t2;
+    f2.init(isize, jsize, ksize); t1.init(isize, jsize, ksize); t2.init(isize, jsize, ksize);
+    pool_host.run(ksize, [&](int kk0) {
+      const int k = kk0 + 1;
+      for (int j = 1; j <= jsize; ++j)
+        for (int i = 0; i <= isize + 1; ++i) {
+          int8_t v = 0;
+          for (int s = std::min(i + b, isize); s >= std::max(i - b, 1); --s)
+            if (f(s, j, k) > 0) { v = f(s, j, k); break; }
+          t1(i, j, k) = v;
+        }
+      for (int jj = 0; jj <= jsize + 1; ++jj)
+        for (int i = 0; i <= isize + 1; ++i) {
+          int8_t v = 0;
+          for (int j = std::min(jj + b, jsize); j >= std::max(jj - b, 1); --j)
+            if (t1(i, j, k) > 0) { v = t1(i, j, k); break; }
+          t2(i, jj, k) = v;
+        }
+    });
+    pool_host.run(ksize + 2, [&](int kk) {
+      for (int jj = 0; jj <= jsize + 1; ++jj)
+        for (int ii = 0; ii <= isize + 1; ++ii) {
+          int8_t v = 0;
+          for (int k = std::min(kk + b, ksize); k >= std::max(kk - b, 1); --k)
+            if (t2(ii, jj, k) > 0) { v = t2(ii, jj, k); break; }
+          f2(ii, jj, kk) = v;
+        }
+    });
+    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) for (int i = 1; i <= isize; ++i) f(i, j, k) = (int8_t)(f(i, j, k) + f2(i, j, k));
+    int numbad = 0;
+    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) for (int i = 1; i <= isize; ++i) if (f(i, j, k) != 0) ++numbad;
+    return numbad;
+  }
+
+  // flglvl.f + colate.f: flagged points (i-.5, j-.5, k-.5) and the nesting domain of level lcheck
+  void flglvl(int lcheck, int lbase, std::vector<double>& badpts, I1& i1flags) {
+    int idim = iregsz[lbase], jdim = jregsz[lbase], kdim = kregsz[lbase];
+    I1 dom1;
+    domprep(i1flags, lbase, idim, jdim, kdim);
+    domshrink(i1flags, dom1, idim, jdim, kdim);
+    for (int lev = lbase + 1; lev <= lcheck; ++lev) {
+      domup(i1flags, dom1, idim, jdim, kdim, intratx[lev - 1] * idim, intraty[lev - 1] * jdim, intratz[lev - 1] * kdim, lev - 1);
+      idim *= intratx[lev - 1]; jdim *= intraty[lev - 1]; kdim *= intratz[lev - 1];
+      domshrink(i1flags, dom1, idim, jdim, kdim);
+    }
+    i1flags = dom1;
+    extend_borders(i1flags, iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]);
+    spest(lcheck, dom1);
+    const int numbad = bufnst(lcheck, dom1);
+    badpts.clear();
+    if (numbad == 0) return;
+    const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
+    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) for (int i = 1; i <= isize; ++i) {
+      const int8_t v = std::min(dom1(i, j, k), i1flags(i, j, k));
+      dom1(i, j, k) = v;
+      if (v != 0) { badpts.push_back((double)i - .5); badpts.push_back((double)j - .5); badpts.push_back((double)k - .5); }
+    }
+  }
+
+  // moment.f
+  static void moment(int rect[6], const double* bp, int npt, double& usage) {
+    double emx1 = bp[0], emn1 = emx1, emx2 = bp[1], emn2 = emx2, emx3 = bp[2], emn3 = emx3;
+    for (int q = 0; q < npt; ++q) {
+      const double* b = bp + 3 * q;
+      if (b[0] > emx1) emx1 = b[0];
+      if (b[0] < emn1) emn1 = b[0];
+      if (b[1] > emx2) emx2 = b[1];
+      if (b[1] < emn2) emn2 = b[1];
+      if (b[2] > emx3) emx3 = b[2];
+      if (b[2] < emn3) emn3 = b[2];
+    }
+    rect[0] = (int)std::lround(emn1 - .5); rect[1] = (int)std::lround(emx1 - .5);
+    rect[2] = (int)std::lround(emn2 - .5); rect[3] = (int)std::lround(emx2 - .5);
+    rect[4] = (int)std::lround(emn3 - .5); rect[5] = (int)std::lround(emx3 - .5);
+    const int gpall = (rect[1] - rect[0] + 1) * (rect[3] - rect[2] + 1) * (rect[5] - rect[4] + 1);
+    usage = (double)npt / gpall;
+  }
+  // signs.f + findcut.f
+  static void findcut(const double* bp, int ist, int iend, int idim, int jdim, int kdim, int& index, int& iside) {
+    std::vector<int> iscr(idim + 2, 0), jscr(jdim + 2, 0), kscr(kdim + 2, 0);
+    int ilo = 1, ihi = idim, jlo = 1, jhi = jdim, klo = 1, khi = kdim;
+    for (int q = ist; q <= iend; ++q) {
+      const double* b = bp + 3 * (q - 1);
+      iscr[(int)(b[0] + 1.1)] += 1; jscr[(int)(b[1] + 1.1)] += 1; kscr[(int)(b[2] + 1.1)] += 1;
+    }
+    for (int t = 1; t <= idim; ++t) if (iscr[t] != 0) { ilo = t; break; }
+    for (int t = 1; t <= idim; ++t) if (iscr[idim + 1 - t] != 0) { ihi = idim + 1 - t; break; }
+    for (int t = 1; t <= jdim; ++t) if (jscr[t] != 0) { jlo = t; break; }
+    for (int t = 1; t <= jdim; ++t) if (jscr[jdim + 1 - t] != 0) { jhi = jdim + 1 - t; break; }
+    for (int t = 1; t <= kdim; ++t) if (kscr[t] != 0) { klo = t; break; }
+    for (int t = 1; t <= kdim; ++t) if (kscr[kdim + 1 - t] != 0) { khi = kdim + 1 - t; break; }
+    for (int i = ilo; i <= ihi; ++i) if (iscr[i] == 0) { index = i; iside = 1; return; }
+    for (int j = jlo; j <= jhi; ++j) if (jscr[j] == 0) { index = j; iside = 2; return; }
+    for (int k = klo; k <= khi; ++k) if (kscr[k] == 0) { index = k; iside = 3; return; }
+    auto lap = [&](std::vector<int>& s, int lo, int hi, int& locmax, int& idx, int& mid) {
+      int pre = s[lo];
+      for (int i = lo + 1; i <= hi - 1; ++i) { const int cur = s[i]; s[i] = s[i + 1] - 2 * cur + pre; pre = cur; }
+      locmax = 0; idx = 0; mid = (lo + hi) / 2;
+      for (int i = lo + 2; i <= hi - 2 + 1; ++i) {
+        const int t1 = s[i - 1], t2 = s[i], d = std::abs(t1 - t2);
+        if (t1 * t2 < 0) {
+          if (d > locmax) { locmax = d; idx = i; }
+          else if (d == locmax && std::abs(i - mid) < std::abs(idx - mid)) idx = i;
+        }
+      }
+    };
+    int lv[3][4];
+    lap(iscr, ilo, ihi, lv[0][0], lv[0][2], lv[0][3]); lv[0][1] = 1;
+    lap(jscr, jlo, jhi, lv[1][0], lv[1][2], lv[1][3]); lv[1][1] = 2;
+    lap(kscr, klo, khi, lv[2][0], lv[2][2], lv[2][3]); lv[2][1] = 3;
+    for (int a = 0; a < 2; ++a)
+      for (int b = a + 1; b < 3; ++b)
+        if (lv[a][0] < lv[b][0]) for (int t = 0; t < 4; ++t) std::swap(lv[a][t], lv[b][t]);
+    int icount = (lv[0][0] > lv[1][0]) ? 1 : (lv[1][0] > lv[2][0]) ? 2 : 3;
+    if (icount != 1)
+      for (int a = 0; a < icount - 1; ++a)
+        for (int b = a + 1; b < icount; ++b)
+          if (std::abs(lv[a][2] - lv[a][3]) > std::abs(lv[b][2] - lv[b][3])) for (int t = 0; t < 4; ++t) std::swap(lv[a][t], lv[b][t]);
+    index = lv[0][2];
+    iside = lv[0][1];
+    if (lv[0][0] < 2) index = 0;
+  }
+  // smartbis.f (numptc 1-based)
+  static void smartbis(std::vector<double>& bp, int npts, double cutoff, std::vector<int>& numptc, int& nclust, int idim, int jdim, int kdim) {
+    nclust = 1;
+    numptc.assign(2, 0);
+    numptc[1] = npts;
+    int icl = 1, ist = 1, iend = numptc[icl];
+    while (true) {
+      int rect[6]; double usenew;
+      moment(rect, bp.data() + 3 * (ist - 1), numptc[icl], usenew);
+      bool advance = (usenew >= cutoff);
+      int index = 0, iside = 0;
+      if (!advance) { findcut(bp.data(), ist, iend, idim, jdim, kdim, index, iside); if (index == 0) advance = true; }
+      if (advance) {
+        icl = icl + 1;
+        if (icl > nclust) break;
+        ist = iend + 1;
+        iend = ist + numptc[icl] - 1;
+        continue;
+      }
+      const double fmid = index - .5;
+      const int idir = iside;
+      auto c = [&](int q) { return bp[3 * (q - 1) + idir - 1]; };
+      auto swp = [&](int a, int b) { for (int d = 0; d < 3; ++d) std::swap(bp[3 * (a - 1) + d], bp[3 * (b - 1) + d]); };
+      int itop = ist - 1, ibot = iend + 1, i = ist;
+      while (true) {
+        if (c(i) < fmid) {
+          bool done = false;
+          while (true) {
+            ibot = ibot - 1;
+            if (c(ibot) < fmid) { if (ibot == i) { done = true; break; } continue; }
+            swp(ibot, i);
+            break;
+          }
+          if (done) break;
+          if (itop + 1 < ibot) continue;
+          break;
+        } else {
+          itop = itop + 1;
+          if (itop + 1 >= ibot) break;
+          i = i + 1;
+        }
+      }
+      numptc[icl] = itop - ist + 1;
+      numptc.insert(numptc.begin() + icl + 1, iend - ibot + 1);
+      nclust = nclust + 1;
+      iend = itop;
+    }
+  }
+  // nestck.f
+  bool nestck(int mnew, int lbase, std::vector<double>& bp, int ibase, int npts, std::vector<int>& numptc, int icl, int& nclust, I1& dom) {
+    if (lbase == 1) return true;
+    const HPatch3& n = node[mnew];
+    const int lev = n.level;
+    const int rx = intratx[lev - 1], ry = intraty[lev - 1], rz = intratz[lev - 1];
+    bool nested = true;
+    for (int k = n.klo / rz + 1; k <= n.khi / rz + 1 && nested; ++k)
+      for (int j = n.jlo / ry + 1; j <= n.jhi / ry + 1 && nested; ++j)
+        for (int i = n.ilo / rx + 1; i <= n.ihi / rx + 1; ++i)
+          if (dom(i, j, k) == 0) { nested = false; break; }
+    if (nested) return true;
+    if (npts <= 1) throw std::runtime_error("nestck: a single point cannot be properly nested");
+    double sidemx = std::max(n.xhi - n.xlo, n.yhi - n.ylo);
+    sidemx = std::max(sidemx, n.zhi - n.zlo);
+    double rmid; int idir;
+    if (n.xhi - n.xlo >= sidemx) { rmid = (double)(float)((n.ihi + n.ilo + 1) / 2.f); rmid = rmid / rx; idir = 1; }
+    else if (n.yhi - n.ylo >= sidemx) { rmid = (double)(float)((n.jhi + n.jlo + 1) / 2.f); rmid = rmid / ry; idir = 2; }
+    else { rmid = (double)(float)((n.khi + n.klo + 1) / 2.f); rmid = rmid / rz; idir = 3; }
+    auto c = [&](int q) { return bp[3 * (ibase + q - 1) + idir - 1]; };
+    int ipt = 1, ntop = npts;
+    while (true) {
+      if (c(ipt) < rmid) { ipt = ipt + 1; if (ipt <= ntop) continue; break; }
+      for (int d = 0; d < 3; ++d) std::swap(bp[3 * (ibase + ipt - 1) + d], bp[3 * (ibase + ntop - 1) + d]);
+      ntop = ntop - 1;
+      if (ipt <= ntop) continue;
+      break;
+    }
+    numptc[icl] = ntop;
+    numptc.insert(numptc.begin() + icl + 1, npts - ntop);
+    nclust = nclust + 1;
+    return false;
+  }
+  // grdfit.f
+  void grdfit(int lbase, int lcheck, double t) {
+    std::vector<double> bp;
+    I1 i1flags;
+    {
+      HPROF("flglvl3");
+      flglvl(lcheck, lbase, bp, i1flags);
+    }
+    const int npts = (int)bp.size() / 3;
+    if (npts == 0) return;
+    HPROF("cluster3");
+    const int levnew = lcheck + 1;
+    const double hxf = hxposs[levnew], hyf = hyposs[levnew], hzf = hzposs[levnew];
+    std::vector<int> numptc;
+    int nclust = 0;
+    smartbis(bp, npts, p.cut, numptc, nclust, iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]);
+    int ibase = 0, icl = 1, prv = 0;
+    while (icl <= nclust) {
+      const int mnew = nodget();
+      while (true) {
+        int rect[6]; double usage;
+        moment(rect, bp.data() + 3 * ibase, numptc[icl], usage);
+        HPatch3& n = node[mnew];
+        n.ilo = rect[0] * intratx[lcheck]; n.jlo = rect[2] * intraty[lcheck]; n.klo = rect[4] * intratz[lcheck];
+        n.ihi = (rect[1] + 1) * intratx[lcheck] - 1; n.jhi = (rect[3] + 1) * intraty[lcheck] - 1; n.khi = (rect[5] + 1) * intratz[lcheck] - 1;
+        n.xlo = n.ilo * hxf + xlower; n.ylo = n.jlo * hyf + ylower; n.zlo = n.klo * hzf + zlower;
+        n.xhi = (n.ihi + 1) * hxf + xlower; n.yhi = (n.jhi + 1) * hyf + ylower; n.zhi = (n.khi + 1) * hzf + zlower;
+        n.level = levnew; n.time = t;
+        if (nestck(mnew, lbase, bp, ibase, numptc[icl], numptc, icl, nclust, i1flags)) break;
+      }
+      if (newstl[levnew] == 0) newstl[levnew] = mnew;
+      else node[prv].levelptr = mnew;
+      prv = mnew;
+      ibase += numptc[icl];
+      ++icl;
+    }
+    birect(newstl[levnew]);
+  }
+
+  // filval.f for the new grids of level lev: coarse box (icall + bc3amr), limited interpolation, copies from the old grids
+  void fill_new_patch(Prog3& P, int lev, int m) {
+    const HPatch3& g = node[m];
+    const int rx = intratx[lev - 1], ry = intraty[lev - 1], rz = intratz[lev - 1];
+    const double hxc = hxposs[lev] * rx, hyc = hyposs[lev] * ry, hzc = hzposs[lev] * rz;
+    const int iclo = g.ilo / rx - 1, jclo = g.jlo / ry - 1, kclo = g.klo / rz - 1;
+    const int ichi = (g.ihi + 1) / rx - 1 + 1, jchi = (g.jhi + 1) / ry - 1 + 1, kchi = (g.khi + 1) / rz - 1 + 1;
+    const int mic = g.nx() / rx + 2, mjc = g.ny() / ry + 2, mkc = g.nz() / rz + 2;
+    const int R = P.add_rect(mic, mjc, mkc, nvar);
+    Tgt3 C{-1, R, mic, mjc, mkc};
+    c_icall(P, C, iclo, ichi, jclo, jchi, kclo, kchi, lev - 1, 1, 1, 1, 0);
+    bool any;
+    Bc3Op b = make_bc(C, hxc, hyc, hzc, g.xlo - hxc, g.xhi + hxc, g.ylo - hyc, g.yhi + hyc, g.zlo - hzc, g.zhi + hzc, any);
+    if (any) P.add_bc(b, 0);
+    Fill3Op o{};
+    o.kind = F3_FILVAL; o.dst_patch = m; o.dst_rect = -1;
+    o.di0 = G3; o.dj0 = G3; o.dk0 = G3; o.ni = g.nx(); o.nj = g.ny(); o.nk = g.nz();
+    o.src = R; o.si0 = g.ilo; o.sj0 = g.jlo; o.sk0 = g.klo; o.level = lev; o.cilo = iclo; o.cjlo = jclo; o.cklo = kclo;
+    P.add_op(o, 1);
+    c_icall(P, Tgt3{m, -1, mitot(m), mjtot(m), mktot(m)}, g.ilo - G3, g.ihi + G3, g.jlo - G3, g.jhi + G3, g.klo - G3, g.khi + G3, lev, 1, 1, 1, 2);
+  }
+  void fill_new_level(int lev) {
+    HPROF("fill_new_level3");
+    Prog3& P = newfill;
+    P.clear();
+    GI(lev - 1); GI(lev);
+    std::vector<int> nl;
+    for (int m = newstl[lev]; m != 0; m = node[m].levelptr) nl.push_back(m);
+    std::vector<Prog3> part(nl.size());
+    pool_host.run((int)nl.size(), [&](int k) { fill_new_patch(part[k], lev, nl[k]); });
+    for (auto& q : part) merge_prog(P, q);
+    upload_prog(P);
+    run_prog(P, SrcMode{});
+    sync_stream();
+    pool.release(P.scratch_off, P.scratch_alloc);
+    P.scratch_off = -1;
+  }
+
+  // regrid.f:4-118 with gfixup.f
+  void regrid(int lbase) {
+    HPROF("regrid3");
+    const auto t0c = std::chrono::steady_clock::now();
+    int lcheck = std::min(lfine, p.mxnest - 1);
+    int lfnew = lbase;
+    for (int i = 1; i <= p.mxnest; ++i) newstl[i] = 0;
+    const double t = node[lstart[lbase]].time;
+    while (lcheck >= lbase) {
+      grdfit(lbase, lcheck, t);
+      if (newstl[lcheck + 1] != 0) lfnew = std::max(lcheck + 1, lfnew);
+      --lcheck;
+    }
+    for (int lev = lbase; lev <= p.mxnest; ++lev) for (int m : lgrids[lev]) { node[m].has_cfl = false; node[m].listbc.clear(); }
+    for (int l2 = lbase + 1; l2 <= p.mxnest; ++l2) {
+      std::vector<int> nl;
+      for (int m = newstl[l2]; m != 0; m = node[m].levelptr) { alloc_patch(m); nl.push_back(m); }
+      // descriptors: current levels (levels below l2 already replaced), the old grids of l2 and the new ones
+      sync_descriptors(&nl, 0);
+      if (newstl[l2] != 0) fill_new_level(l2);
+      int m = lstart[l2];
+      while (m != 0) {
+        const int mold = m;
+        m = node[m].levelptr;
+        free_patch(mold);
+        node[mold].bnd.clear(); node[mold].listbc.clear();
+        putnod(mold);
+      }
+      lstart[l2] = newstl[l2];
+      touch(l2);
+      lgrids[l2].clear();
+      for (int q = lstart[l2]; q != 0; q = node[q].levelptr) lgrids[l2].push_back(q);
+    }
+    lfine = lfnew;
+    for (int lev = lbase; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
+    for (int lev = lbase + 1; lev <= p.mxnest; ++lev) arrange(lev);
+    make_lists();
+    for (int lev = lbase + 1; lev <= lfine; ++lev) make_bndry(lev);
+    compile_all(lbase);
+    sync_stream();
+    t_regrid += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0c).count();
+  }
+
+  // ================================================================ init (amr3.f90, domain.f, setgrd.f, ginit.f)
+  void ginit(int msave, double t) {
+    for (int m = msave; m != 0; m = node[m].levelptr) {
+      alloc_patch(m);
+      HPatch3& g = node[m];
+      g.time = t;
+      std::vector<double> q;
+      qinit(g, hxposs[g.level], hyposs[g.level], hzposs[g.level], q);
+      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q0, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
+      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q1, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
+      h2d_bytes += 2.0 * sizeof(double) * q.size();
+      sync_stream();
+    }
+  }
+  void init(const std::string& dir) {
+    p.load(dir);
+    if (p.ndim != 3) throw std::runtime_error("num_dim must be 3");
+    nvar = p.nvar;
+    blast_x = p.pn("x0", 0.0); blast_y = p.pn("y0", 0.0); blast_z = p.pn("z0", 0.0);
+    blast_r = p.pn("r0", 0.2); blast_pin = p.pn("pin", 5.0); blast_pout = p.pn("pout", 1.0);
+    flag_pressure = (int)p.pn("flag_pressure", 1.0);
+    setup_problem();
+    xlower = p.lower[0]; ylower = p.lower[1]; zlower = p.lower[2];
+    xupper = p.upper[0]; yupper = p.upper[1]; zupper = p.upper[2];
+    nxc = p.ncells[0]; nyc = p.ncells[1]; nzc = p.ncells[2];
+    if ((nxc / 2) * 2 != nxc || (nyc / 2) * 2 != nyc || (nzc / 2) * 2 != nzc) throw std::runtime_error("cell counts must be even");
+    for (int k = 1; k <= 10; ++k) { intratx[k] = p.ratx[k]; intraty[k] = p.raty[k]; intratz[k] = p.ratz[k]; kratio[k] = p.ratt[k]; }
+    hxposs[1] = (xupper - xlower) / nxc; hyposs[1] = (yupper - ylower) / nyc; hzposs[1] = (zupper - zlower) / nzc;
+    for (int lev = 2; lev <= p.mxnest; ++lev) {
+      hxposs[lev] = hxposs[lev - 1] / (double)intratx[lev - 1];
+      hyposs[lev] = hyposs[lev - 1] / (double)intraty[lev - 1];
+      hzposs[lev] = hzposs[lev - 1] / (double)intratz[lev - 1];
+    }
+    possk[1] = p.dt_initial;
+    iregsz[1] = nxc; jregsz[1] = nyc; kregsz[1] = nzc;
+    for (int lev = 2; lev <= p.mxnest; ++lev) {
+      iregsz[lev] = iregsz[lev - 1] * intratx[lev - 1];
+      jregsz[lev] = jregsz[lev - 1] * intraty[lev - 1];
+      kregsz[lev] = kregsz[lev - 1] * intratz[lev - 1];
+      possk[lev] = possk[lev - 1] / (double)kratio[lev - 1];
+    }
+    for (int l = 0; l < MAXLV + 2; ++l) {
+      lc.hx[l] = l < 12 ? hxposs[l] : 0; lc.hy[l] = l < 12 ? hyposs[l] : 0; lc.hz[l] = l < 12 ? hzposs[l] : 0;
+      lc.iregsz[l] = iregsz[l]; lc.jregsz[l] = jregsz[l]; lc.kregsz[l] = kregsz[l];
+      lc.intratx[l] = intratx[l]; lc.intraty[l] = intraty[l]; lc.intratz[l] = intratz[l];
+    }
+    AMR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ev_a, &ev_b, &ev_run0, &ev_run1}) AMR_CUDA(cudaEventCreate(e));
+    pool.init((long long)nvar * (nxc + 4) * (nyc + 4) * (nzc + 4) * 4 + (1 << 22));
+    regs.init(1 << 20);
+    AMR_CUDA(cudaMalloc(&d_cfl, sizeof(unsigned long long)));
+    AMR_CUDA(cudaMalloc(&d_mass, sizeof(double)));
+    node.assign(10001, HPatch3());
+    for (int k = 1; k <= 10000; ++k) node[k].nextfree = k + 1;
+    node[10000].nextfree = 0;
+    ndfree = 1;
+    start_time = p.t0;
+    glast.assign(p.gauges.size(), 0.0);
+    for (size_t i = 0; i < p.gauges.size(); ++i) glast[i] = p.gauges[i].t1;
+    // domain.f
+    const int ms = nodget();
+    HPatch3& g = node[ms];
+    g.xlo = xlower; g.ylo = ylower; g.zlo = zlower; g.xhi = xupper; g.yhi = yupper; g.zhi = zupper;
+    g.level = 1; g.levelptr = 0;
+    g.ilo = 0; g.jlo = 0; g.klo = 0; g.ihi = nxc - 1; g.jhi = nyc - 1; g.khi = nzc - 1;
+    lstart[1] = ms;
+    touch(1);
+    lfine = 1;
+    birect(ms);
+    ginit(lstart[1], start_time);
+    arrange(1);
+    make_lists();
+    make_bndry(1);
+    compile_all(0);
+    // setgrd.f
+    record_gauges = false;
+    int levnew = 2;
+    while (levnew <= p.mxnest) {
+      const int levold = levnew - 1;
+      if (lstart[levold] == 0) break;
+      for (int i = 1; i <= p.mxnest; ++i) newstl[i] = 0;
+      grdfit(levold, levold, start_time);
+      if (newstl[levnew] == 0) break;
+      ginit(newstl[levnew], start_time);
+      lstart[levnew] = newstl[levnew];
+      touch(levnew);
+      lfine = levnew;
+      arrange(levnew);
+      make_lists();
+      make_bndry(levnew);
+      compile_all(levold);
+      ++levnew;
+    }
+    // setgrd.f:110-121 swaps store1/store2 after re-initialising store2: both hold qinit, nothing to do.
+    // update.f runs before prepf/prepc, so no coarse patch has a register list yet (averaging only).
+    make_lists();
+    compile_all(0);
+    for (int level = 1; level <= lfine - 1; ++level) update(lfine - level);
+    for (int level = 1; level <= lfine - 1; ++level) { prepf(level + 1); prepc(level); }
+    compile_all(0);
+    sync_stream();
+    record_gauges = true;
+    time = start_time;
+    tmass0 = mass();
+    if (p.output_t0 && write_output) output(time);
+  }
+
+  // ================================================================ tick.f
+  bool finished() const { return ncycle >= p.nstop || time >= p.tfinal; }
+  void tick() {
+    double dtnew[12];
+    int ntogo[12];
+    int cycles = 0;
+    run_cells = 0;
+    const double rvol0 = rvol;
+    const auto tw0 = std::chrono::steady_clock::now();
+    AMR_CUDA(cudaEventRecord(ev_run0, st));
+    setbestsrc();
+    int nextout = 0, iout = p.iout;
+    if (iout == 0) { iout = 999999999; nextout = (p.nout > 0) ? 1 : 0; }
+    if (tick_started) nextout = tk_nextout;
+    double* tlevel = tk_tlevel;
+    if (!tick_started) { tlevel[1] = time; for (int i = 2; i <= p.mxnest; ++i) tlevel[i] = tlevel[1]; }
+    tick_started = true;
+    while (!finished()) {
+      double outtime;
+      if (p.nout > 0) outtime = (nextout <= p.nout) ? p.tout[nextout - 1] : RINF;
+      else outtime = p.tfinal;
+      bool dumpout = false;
+      if (time < outtime && time + (double)1.001f * possk[1] >= outtime) {
+        possk[1] = outtime - time;
+        for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
+        if (p.nout > 0) { ++nextout; dumpout = true; }
+      }
+      int level = 1;
+      ntogo[level] = 1;
+      for (int i = 1; i <= 10; ++i) dtnew[i] = RINF;
+      while (true) {
+        int lbase = -1;
+        if (icheck[level] >= p.kcheck) lbase = level;
+        else if (level + 1 >= p.mxnest) lbase = -1;
+        else if (icheck[level + 1] >= p.kcheck) lbase = level + 1;
+        else if (level + 2 >= p.mxnest) lbase = -1;
+        else if (icheck[level + 2] >= p.kcheck) lbase = level + 2;
+        if (lbase > 0) {
+          if (!(lbase == p.mxnest || lbase > lfine)) { regrid(lbase); setbestsrc(); }
+          for (int i = lbase; i <= lfine; ++i) icheck[i] = 0;
+          for (int i = lbase + 1; i <= lfine; ++i) tlevel[i] = tlevel[lbase];
+        }
+        const double dtl = advanc(level);
+        ntogo[level] -= 1;
+        dtnew[level] = std::min(dtnew[level], dtl);
+        tlevel[level] = tlevel[level] + possk[level];
+        icheck[level] += 1;
+        if (level < lfine) {
+          ++level;
+          if (((possk[level - 1] - dtnew[level - 1]) / dtnew[level - 1]) > (double)0.05f) {
+            const double dttemp = dtnew[level - 1] / kratio[level - 1];
+            ntogo[level] = (int)((tlevel[level - 1] - tlevel[level]) / dttemp + (double)0.9f);
+          } else ntogo[level] = kratio[level - 1];
+          possk[level] = possk[level - 1] / ntogo[level];
+          continue;
+        }
+        bool done = false;
+        while (true) {
+          if (level == 1) { done = true; break; }
+          if (ntogo[level] > 0) {
+            while ((possk[level] - dtnew[level]) / dtnew[level] > (double)0.05f) {
+              ntogo[level] += 1;
+              possk[level] = (tlevel[level - 1] - tlevel[level]) / ntogo[level];
+            }
+            break;
+          }
+          --level;
+          update(level);
+        }
+        if (done) break;
+      }
+      time = time + possk[1];
+      ++ncycle;
+      if (p.vtime) {
+        for (int i = 2; i <= lfine; ++i) { const int ii = lfine + 1 - i; dtnew[ii] = std::min(dtnew[ii], dtnew[ii + 1] * kratio[ii]); }
+        dtnew[1] = std::min(dtnew[1], p.dt_max);
+        possk[1] = dtnew[1];
+        for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
+      }
+      if ((ncycle % iout == 0) || dumpout) output(time);
+      ++cycles;
+      if (max_cycles > 0 && cycles >= max_cycles) break;
+    }
+    tk_nextout = nextout;
+    AMR_CUDA(cudaEventRecord(ev_run1, st));
+    sync_stream();
+    float ms = 0;
+    AMR_CUDA(cudaEventElapsedTime(&ms, ev_run0, ev_run1));
+    last_run_ms = ms;
+    run_cells = rvol - rvol0;
+    t_step += std::chrono::duration<double>(std::chrono::steady_clock::now() - tw0).count();
+  }
+
+  // ================================================================ results
+  double mass() {
+    AMR_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double), st));
+    DBuf<int> dp; dp.upload(lgrids[1], st, stg);
+    launch_mass3(pool.d, d_patches.d, dp.d, (int)lgrids[1].size(), d_mass, st);
+    double m = 0;
+    AMR_CUDA(cudaMemcpyAsync(&m, d_mass, sizeof(double), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    dp.free();
+    return m * hxposs[1] * hyposs[1] * hzposs[1];
+  }
+  std::vector<double> gather_values() {
+    std::vector<int> pl;
+    std::vector<long long> c0(1, 0);
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) { pl.push_back(m); c0.push_back(c0.back() + (long long)node[m].nx() * node[m].ny() * node[m].nz()); }
+    std::vector<double> out((size_t)c0.back() * nvar);
+    if (out.empty()) return out;
+    DBuf<int> dp; dp.upload(pl, st, stg);
+    DBuf<long long> dc; dc.upload(c0, st, stg);
+    DBuf<double> dout; dout.ensure(out.size());
+    launch_gather3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nvar, c0.back(), dout.d, st);
+    AMR_CUDA(cudaMemcpyAsync(out.data(), dout.d, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    dp.free(); dc.free(); dout.free();
+    return out;
+  }
+  void output(double t) {
+    if (!write_output) { ++frame; return; }
+    const std::vector<double> v = gather_values();
+    char fn[64];
+    std::snprintf(fn, sizeof(fn), "/fort.q%04d", frame);
+    FILE* f = std::fopen((outdir + fn).c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+    size_t off = 0;
+    int ngrids = 0;
+    auto E = [](double x, int w, int d) {
+      char b[64];
+      std::snprintf(b, sizeof(b), "%*.*E", w, d - 1, x);  // e.g. 1.0000000000000000E+00 (width w)
+      return std::string(b);
+    };
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) {
+        ++ngrids;
+        const HPatch3& g = node[m];
+        std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n%6d                 mz\n",
+                     m, lev, g.nx(), g.ny(), g.nz());
+        std::fprintf(f, "%s    xlow\n%s    ylow\n%s    zlow\n%s    dx\n%s    dy\n%s    dz\n\n", E(g.xlo, 26, 17).c_str(), E(g.ylo, 26, 17).c_str(),
+                     E(g.zlo, 26, 17).c_str(), E(hxposs[lev], 26, 17).c_str(), E(hyposs[lev], 26, 17).c_str(), E(hzposs[lev], 26, 17).c_str());
+        const size_t n = (size_t)g.nx() * g.ny() * g.nz();
+        for (int k = 0; k < g.nz(); ++k) {
+          for (int j = 0; j < g.ny(); ++j) {
+            for (int i = 0; i < g.nx(); ++i) {
+              for (int iv = 0; iv < nvar; ++iv) {
+                double x = v[off + iv * n + ((size_t)k * g.ny() + j) * g.nx() + i];
+                if (std::fabs(x) < 1e-90) x = 0.0;
+                std::fputs(E(x, 26, 17).c_str(), f);
+              }
+              std::fputc('\n', f);
+            }
+            std::fputs("  \n", f);
+          }
+          std::fputs("  \n", f);
+        }
+        off += n * nvar;
+      }
+    std::fclose(f);
+    std::snprintf(fn, sizeof(fn), "/fort.t%04d", frame);
+    f = std::fopen((outdir + fn).c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+    std::fprintf(f, "%s    time\n%6d                 meqn\n%6d                 ngrids\n%6d                 naux\n%6d                 ndim\n%6d                 nghost\n\n",
+                 E(t, 18, 9).c_str(), nvar, ngrids, 0, 3, G3);
+    std::fclose(f);
+    ++frame;
+  }
+
+  // ================================================================ AmrSolver
+  int num_dim() const override { return 3; }
+  void set_batched(bool on) override { batched = on; }
+  void set_profile(bool on) override { profile = on; }
+  void run(int mc) override { max_cycles = mc; tick(); }
+  double level_advance(int level, double* cfl) override {
+    if (level < 1 || level > lfine) throw std::runtime_error("level out of range");
+    const double d = advanc(level);
+    if (cfl) *cfl = cfl_level;
+    return d;
+  }
+  void update_level(int level) override {
+    if (level < 1 || level >= lfine) throw std::runtime_error("level out of range");
+    update(level);
+    sync_stream();
+  }
+  void regrid_from(int lbase) override {
+    if (lbase < 1 || lbase > lfine || lbase >= p.mxnest) throw std::runtime_error("lbase out of range");
+    regrid(lbase);
+    setbestsrc();
+  }
+  void valout(const char* dir) override {
+    const std::string keep = outdir;
+    const bool kw = write_output;
+    if (dir) { outdir = dir; write_output = true; }
+    output(time);
+    outdir = keep; write_output = kw;
+  }
+  double mass_() { return mass(); }
+  std::vector<double> info() override {
+    return {time, rvol, (double)ncycle, (double)lfine, t_step, t_regrid, tmass0, cflmax_run, (double)nkernels, (double)pool.peak * 8.0,
+            (double)nsteps_launched, step_kernel_ms, step_kernel_cells, last_run_ms, run_cells, finished() ? 1.0 : 0.0, h2d_bytes,
+            0, 0, 0, 0, 0, 0, 3.0};
+  }
+  std::vector<int> grid_rows() override {
+    std::vector<int> r;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) {
+        const HPatch3& g = node[m];
+        r.insert(r.end(), {m, lev, g.ilo, g.ihi, g.jlo, g.jhi, g.klo, g.khi});
+      }
+    return r;
+  }
+  std::vector<double> values() override { return gather_values(); }
+  std::vector<double> gauge_rows() override {
+    std::vector<double> vals((size_t)gslots * nvar), out;
+    if (gslots) AMR_CUDA(cudaMemcpy(vals.data(), d_gauge_out.d, sizeof(double) * vals.size(), cudaMemcpyDeviceToHost));
+    for (const auto& G : p.gauges)
+      for (const auto& r : grows) {
+        if (r.gauge != G.num) continue;
+        out.push_back(r.gauge); out.push_back(r.level); out.push_back(r.t);
+        for (int k = 0; k < nvar; ++k) out.push_back(vals[(size_t)r.slot * nvar + k]);
+      }
+    return out;
+  }
+};
+
+// quick_sort1.f (qsorti): non-stable index sort with the reference's comparison sequence (1-based views)
+void Amr3Gpu::qsorti(std::vector<int>& ord, int n, const std::vector<long long>& a) {
+  int poplst[2][64];
+  int ndeep = 0, u1 = n, l1 = 1;
+  for (int i = 1; i <= n; ++i) ord[i] = i;
+  int l, u, p, q, ix, iz, yp, ip, iq;
+  long long x, z, xx, zz, y;
+L2:
+  if (u1 <= l1) return;
+L3:
+  l = l1; u = u1;
+L4:
+  p = l; q = u;
+  x = a[ord[p]]; z = a[ord[q]];
+  if (!(x <= z)) { y = x; x = z; z = y; yp = ord[p]; ord[p] = ord[q]; ord[q] = yp; }
+  if (u - l <= 1) goto L15;
+  xx = x; ix = p; zz = z; iz = q;
+L6:
+  p = p + 1;
+  if (p >= q) goto L7;
+  x = a[ord[p]];
+  if (x >= xx) goto L8;
+  goto L6;
+L7:
+  p = q - 1;
+  goto L13;
+L8:
+  q = q - 1;
+  if (q <= p) goto L9;
+  z = a[ord[q]];
+  if (z <= zz) goto L10;
+  goto L8;
+L9:
+  q = p; p = p - 1; z = x; x = a[ord[p]];
+L10:
+  if (!(x <= z)) { y = x; x = z; z = y; ip = ord[p]; ord[p] = ord[q]; ord[q] = ip; }
+  if (!(x <= xx)) { xx = x; ix = p; }
+  if (!(z >= zz)) { zz = z; iz = q; }
+  goto L6;
+L13:
+  if (p != ix && x != xx) { ip = ord[p]; ord[p] = ord[ix]; ord[ix] = ip; }
+  if (q != iz && z != zz) { iq = ord[q]; ord[q] = ord[iz]; ord[iz] = iq; }
+L15:
+  if (u - q <= p - l) goto L16;
+  l1 = l; u1 = p - 1; l = q + 1;
+  goto L17;
+L16:
+  u1 = u; l1 = q + 1; u = p - 1;
+L17:
+  if (u1 <= l1) goto L18;
+  ndeep = ndeep + 1;
+  poplst[0][ndeep] = u; poplst[1][ndeep] = l;
+  goto L3;
+L18:
+  if (u > l) goto L4;
+  if (ndeep == 0) goto L2;
+  u = poplst[0][ndeep]; l = poplst[1][ndeep]; ndeep = ndeep - 1;
+  goto L18;
+}
+
+AmrSolver* make_solver3(const std::string& rundir, const std::string& outdir, bool write_output) {
+  std::unique_ptr<Amr3Gpu> s(new Amr3Gpu());
+  s->outdir = outdir;
+  s->write_output = write_output;
+  s->init(rundir);
+  return s.release();
+}
+
+}  // namespace amrb

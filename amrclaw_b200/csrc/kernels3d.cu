@@ -1,0 +1,1000 @@
+// 3D kernels of the patch-advance path (sm_100a, FP64, built without FMA contraction).
+//
+//   sweep3_kernel<DIR>  one thread per cell of every pencil of a sweep direction of
+//                       every patch of a level (flux3.f:4-633 over step3.f's pencils):
+//                       Roe solves of the cell's own interface and of the next one,
+//                       wave limiter, second-order correction, and the transverse and
+//                       doubly transverse splits. The cell's transverse increments
+//                       (gadd, hadd) are accumulated in the reference's statement
+//                       order (terms of interface c, then of interface c+1) and left
+//                       in a per-level staging buffer together with faddm/faddp.
+//   face3_kernel        every face flux of the level, summing the staged increments
+//                       in the order step3.f adds them (x-, y-, then z-sweeps; pencils
+//                       in loop order).
+//   update3_kernel      conservative update (stepgrid.f:142-153) into the other buffer.
+//   fsv3 / fad3         flux registers from the face fluxes (fluxsv.f, fluxad.f).
+//   qad3_kernel         coarse/fine Riemann problems into the registers (qad.f:4-534).
+//   fill3 / bc3         ghost-fill programs (intfil.f, filpatch.f, filval.f, cstore.f)
+//                       and bc3amr.f90 extrapolation / wall boundaries.
+//   upbnd3 / average3   level sync (upbnd.f, update.f).
+//   flags3, gauges3, mass3, gather3: flagging (spest.f + flag2refine.f), gauge
+//                       sampling (gauges_module.f90:302-460), conck.f, output gather.
+#include "kernels3d.cuh"
+#include <algorithm>
+
+namespace amrb {
+
+namespace {
+
+constexpr int NG3 = 2;  // num_ghost (the host rejects other values)
+
+__device__ __forceinline__ int floordiv3(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
+
+__device__ __forceinline__ int find_patch(const long long* pre, int np, long long t) {
+  int lo = 0, hi = np - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
+  atomicMax(p, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double philim3(int meth, double r) {
+  switch (meth) {
+    case 1: return dmax(0.0, dmin(1.0, r));
+    case 2: return dmax(dmax(0.0, dmin(1.0, 2.0 * r)), dmin(2.0, r));
+    case 3: return (r + fabs(r)) / (1.0 + fabs(r));
+    case 4: { const double c = (1.0 + r) / 2.0; return dmax(0.0, dmin(dmin(c, 2.0), 2.0 * r)); }
+    case 5: return r;
+  }
+  return 0.0;
+}
+
+// ------------------------------------------------------------------- sweeps
+template <int DIR>
+__global__ void __launch_bounds__(128) sweep3_kernel(Step3Args A) {
+  const long long* s0 = A.sweep0 + (long long)(DIR - 1) * (A.np + 1);
+  const long long first = s0[0], last = s0[A.np];
+  const Step3Params sp = A.sp;
+  double cfl = 0.0;
+  for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < last; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(s0, A.np, t);
+    const PatchDev& P = A.patches[A.plist[pi]];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+    const int n1 = DIR == 1 ? mx : DIR == 2 ? my : mz;
+    const int n2 = DIR == 1 ? my : mx;
+    const long long loc = t - s0[pi];
+    const int c = (int)(loc % (n1 + 1)) + 1;
+    const long long pen = loc / (n1 + 1);
+    const int a = (int)(pen % (n2 + 2)), b = (int)(pen / (n2 + 2));
+    const long long mi = P.mitot, mj = P.mjtot;
+    long long base, step;  // enlarged-array index of pencil cell e is base + e*step
+    if (DIR == 1) { base = ((long long)(b - 1 + NG3) * mj + (a - 1 + NG3)) * mi + (NG3 - 1); step = 1; }
+    else if (DIR == 2) { base = ((long long)(b - 1 + NG3) * mj + (NG3 - 1)) * mi + (a - 1 + NG3); step = mi; }
+    else { base = ((long long)(NG3 - 1) * mj + (b - 1 + NG3)) * mi + (a - 1 + NG3); step = mi * mj; }
+    const long long plane = mi * mj * P.mktot;
+    const double* q = A.pool + P.q[P.cur];
+    const double dn = DIR == 1 ? A.dx : DIR == 2 ? A.dy : A.dz;
+    const double dtdx = A.dt / dn;
+    // transverse steps of flux3's dtdy / dtdz arguments for this sweep (step3.f:192, 300, 416)
+    const double dtdy = DIR == 1 ? A.dt / A.dy : DIR == 2 ? A.dt / A.dz : A.dt / A.dx;
+    const double dtdz = DIR == 1 ? A.dt / A.dz : DIR == 2 ? A.dt / A.dx : A.dt / A.dy;
+    const bool hasB = (c + 1 <= n1 + 1);
+    // cells c-2 .. c+2 (index 0..4), 1-based components
+    double Q[5][6];
+#pragma unroll
+    for (int x = 0; x < 5; ++x) {
+      const int e = c - 2 + x;
+      if (e > n1 + 2) { for (int m = 0; m < 6; ++m) Q[x][m] = 1.0; continue; }
+      const long long at = base + (long long)e * step;
+#pragma unroll
+      for (int m = 1; m <= 5; ++m) Q[x][m] = q[(m - 1) * plane + at];
+      Q[x][0] = 0.0;
+    }
+    // Riemann solves at interfaces c-1 .. c+2 (interface e sits between cells e-1 and e)
+    double Wc[3][5], Sc[3], AMc[5], APc[5];
+    double Wn[3][5], Sn[3], AMn[5], APn[5];
+    double dl_c[3], dr_c[3], dr_n[3];  // dot(W_{c-1},W_c), dot(W_c,W_{c+1}), dot(W_{c+1},W_{c+2})
+    {
+      double Wp[3][5], Sp[3], t1[5], t2[5];
+      euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[0], Q[1], Wp, Sp, t1, t2);
+      euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[1], Q[2], Wc, Sc, AMc, APc);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double d = 0.0;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) d = d + Wp[k][m] * Wc[k][m];
+        dl_c[k] = d;
+      }
+    }
+    euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[2], Q[3], Wn, Sn, AMn, APn);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double d = 0.0;
+#pragma unroll
+      for (int m = 0; m < 5; ++m) d = d + Wc[k][m] * Wn[k][m];
+      dr_c[k] = d;
+    }
+    if (hasB) {
+      double Wq[3][5], Sq[3], t1[5], t2[5];
+      euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[3], Q[4], Wq, Sq, t1, t2);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double d = 0.0;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) d = d + Wn[k][m] * Wq[k][m];
+        dr_n[k] = d;
+      }
+    }
+    // Courant number of interface c (flux3.f:237-246)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cfl = dmax(cfl, dmax(dtdx * Sc[k], -dtdx * Sc[k]));
+    // limiter (limiter.f) and second-order corrections of interfaces c and c+1
+    double CQc[5], CQn[5];
+    const double dtdxave = 0.5 * (dtdx + dtdx);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) { CQc[m] = 0.0; CQn[m] = 0.0; }
+    if (sp.order != 1) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (sp.mthlim[k] == 0) continue;
+        double wn = 0.0;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) wn = wn + Wc[k][m] * Wc[k][m];
+        if (wn != 0.0) {
+          const double r = (Sc[k] > 0.0) ? dl_c[k] / wn : dr_c[k] / wn;
+          const double phi = philim3(sp.mthlim[k], r);
+#pragma unroll
+          for (int m = 0; m < 5; ++m) Wc[k][m] = phi * Wc[k][m];
+        }
+        if (hasB) {
+          double wn2 = 0.0;
+#pragma unroll
+          for (int m = 0; m < 5; ++m) wn2 = wn2 + Wn[k][m] * Wn[k][m];
+          if (wn2 != 0.0) {
+            const double r = (Sn[k] > 0.0) ? dr_c[k] / wn2 : dr_n[k] / wn2;
+            const double phi = philim3(sp.mthlim[k], r);
+#pragma unroll
+            for (int m = 0; m < 5; ++m) Wn[k][m] = phi * Wn[k][m];
+          }
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        double x = 0.0, y = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          x = x + 0.5 * fabs(Sc[k]) * (1.0 - fabs(Sc[k]) * dtdxave) * Wc[k][m];
+          y = y + 0.5 * fabs(Sn[k]) * (1.0 - fabs(Sn[k]) * dtdxave) * Wn[k][m];
+        }
+        CQc[m] = x; CQn[m] = y;
+      }
+    }
+    double* st = A.stash + t;
+    const long long ss = A.stash_stride;
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      double fm = 0.0 + AMc[m], fp = 0.0 - APc[m];
+      if (sp.order != 1) { fm = fm + CQc[m]; fp = fp + CQc[m]; }
+      st[(long long)m * ss] = fm;
+      st[(long long)(5 + m) * ss] = fp;
+    }
+    if (sp.m3 <= 0) {
+      for (int e = 10; e < STASH3; ++e) st[(long long)e * ss] = 0.0;
+      continue;
+    }
+    const double c6 = 1.0 / 6.0;
+    const int m3 = sp.m3, m4 = sp.m4;
+    double G[2][3][5], H[2][3][5];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int m = 0; m < 5; ++m) { G[s][d][m] = 0.0; H[s][d][m] = 0.0; }
+    // ---- terms of interface c (the apdq side; flux3.f:429-505 and 552-628 for cell i = c)
+    {
+      const Roe3D R = roe3d(sp.gamma1, Q[1], Q[2]);
+      double bma[5], bpa[5], cma[5], cpa[5], bmq[5], bpq[5], cmq[5], cpq[5];
+      euler3d_trans(R, DIR, 2, APc, bma, bpa);
+      euler3d_trans(R, DIR, 3, APc, cma, cpa);
+      if (m3 == 2) { euler3d_trans(R, DIR, 2, CQc, bmq, bpq); euler3d_trans(R, DIR, 3, CQc, cmq, cpq); }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { G[0][1][m] = G[0][1][m] - 0.5 * dtdx * bma[m]; G[1][1][m] = G[1][1][m] - 0.5 * dtdx * bpa[m]; }
+      if (m4 > 0) {
+        double c2p[5], c2m[5], P1[5], P2[5], M1[5], M2[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          c2p[m] = (m4 == 2) ? cpa[m] - 3.0 * cpq[m] : cpa[m];
+          c2m[m] = (m4 == 2) ? cma[m] - 3.0 * cmq[m] : cma[m];
+        }
+        euler3d_trans(R, DIR, 2, c2p, P1, P2);
+        euler3d_trans(R, DIR, 2, c2m, M1, M2);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          G[1][1][m] = G[1][1][m] + c6 * dtdx * dtdz * (P2[m] - M2[m]);
+          G[0][1][m] = G[0][1][m] + c6 * dtdx * dtdz * (P1[m] - M1[m]);
+          G[1][2][m] = G[1][2][m] - c6 * dtdx * dtdz * P2[m];
+          G[0][2][m] = G[0][2][m] - c6 * dtdx * dtdz * P1[m];
+          G[1][0][m] = G[1][0][m] + c6 * dtdx * dtdz * M2[m];
+          G[0][0][m] = G[0][0][m] + c6 * dtdx * dtdz * M1[m];
+        }
+      }
+      if (m3 == 2) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) { G[1][1][m] = G[1][1][m] + dtdx * bpq[m]; G[0][1][m] = G[0][1][m] + dtdx * bmq[m]; }
+      }
+      // hadd
+      double X1[5], X2[5], Y1[5], Y2[5];
+      if (m4 > 0) {
+        double bp2[5], bm2[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          bp2[m] = (m4 == 2) ? bpa[m] - 3.0 * bpq[m] : bpa[m];
+          bm2[m] = (m4 == 2) ? bma[m] - 3.0 * bmq[m] : bma[m];
+        }
+        euler3d_trans(R, DIR, 3, bp2, X1, X2);
+        euler3d_trans(R, DIR, 3, bm2, Y1, Y2);
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        H[0][1][m] = H[0][1][m] - 0.5 * dtdx * cma[m];
+        H[1][1][m] = H[1][1][m] - 0.5 * dtdx * cpa[m];
+        if (m4 > 0) {
+          H[1][1][m] = H[1][1][m] + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
+          H[0][1][m] = H[0][1][m] + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
+          H[1][2][m] = H[1][2][m] - c6 * dtdx * dtdy * X2[m];
+          H[0][2][m] = H[0][2][m] - c6 * dtdx * dtdy * X1[m];
+          H[1][0][m] = H[1][0][m] + c6 * dtdx * dtdy * Y2[m];
+          H[0][0][m] = H[0][0][m] + c6 * dtdx * dtdy * Y1[m];
+        }
+        if (m3 == 2) {
+          H[1][1][m] = H[1][1][m] + dtdx * cpq[m];
+          H[0][1][m] = H[0][1][m] + dtdx * cmq[m];
+        }
+      }
+    }
+    // ---- terms of interface c+1 (the amdq side, added to cell i-1 = c)
+    if (hasB) {
+      const Roe3D R = roe3d(sp.gamma1, Q[2], Q[3]);
+      double bmm[5], bpm[5], cmm[5], cpm[5], bmq[5], bpq[5], cmq[5], cpq[5];
+      euler3d_trans(R, DIR, 2, AMn, bmm, bpm);
+      euler3d_trans(R, DIR, 3, AMn, cmm, cpm);
+      if (m3 == 2) { euler3d_trans(R, DIR, 2, CQn, bmq, bpq); euler3d_trans(R, DIR, 3, CQn, cmq, cpq); }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { G[0][1][m] = G[0][1][m] - 0.5 * dtdx * bmm[m]; G[1][1][m] = G[1][1][m] - 0.5 * dtdx * bpm[m]; }
+      if (m4 > 0) {
+        double c2p[5], c2m[5], P1[5], P2[5], M1[5], M2[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          c2p[m] = (m4 == 2) ? cpm[m] + 3.0 * cpq[m] : cpm[m];
+          c2m[m] = (m4 == 2) ? cmm[m] + 3.0 * cmq[m] : cmm[m];
+        }
+        euler3d_trans(R, DIR, 2, c2p, P1, P2);
+        euler3d_trans(R, DIR, 2, c2m, M1, M2);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          G[1][1][m] = G[1][1][m] + c6 * dtdx * dtdz * (P2[m] - M2[m]);
+          G[0][1][m] = G[0][1][m] + c6 * dtdx * dtdz * (P1[m] - M1[m]);
+          G[1][2][m] = G[1][2][m] - c6 * dtdx * dtdz * P2[m];
+          G[0][2][m] = G[0][2][m] - c6 * dtdx * dtdz * P1[m];
+          G[1][0][m] = G[1][0][m] + c6 * dtdx * dtdz * M2[m];
+          G[0][0][m] = G[0][0][m] + c6 * dtdx * dtdz * M1[m];
+        }
+      }
+      if (m3 == 2) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) { G[1][1][m] = G[1][1][m] - dtdx * bpq[m]; G[0][1][m] = G[0][1][m] - dtdx * bmq[m]; }
+      }
+      double X1[5], X2[5], Y1[5], Y2[5];
+      if (m4 > 0) {
+        double bp2[5], bm2[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          bp2[m] = (m4 == 2) ? bpm[m] + 3.0 * bpq[m] : bpm[m];
+          bm2[m] = (m4 == 2) ? bmm[m] + 3.0 * bmq[m] : bmm[m];
+        }
+        euler3d_trans(R, DIR, 3, bp2, X1, X2);
+        euler3d_trans(R, DIR, 3, bm2, Y1, Y2);
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        H[0][1][m] = H[0][1][m] - 0.5 * dtdx * cmm[m];
+        H[1][1][m] = H[1][1][m] - 0.5 * dtdx * cpm[m];
+        if (m4 > 0) {
+          H[1][1][m] = H[1][1][m] + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
+          H[0][1][m] = H[0][1][m] + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
+          H[1][2][m] = H[1][2][m] - c6 * dtdx * dtdy * X2[m];
+          H[0][2][m] = H[0][2][m] - c6 * dtdx * dtdy * X1[m];
+          H[1][0][m] = H[1][0][m] + c6 * dtdx * dtdy * Y2[m];
+          H[0][0][m] = H[0][0][m] + c6 * dtdx * dtdy * Y1[m];
+        }
+        if (m3 == 2) {
+          H[1][1][m] = H[1][1][m] - dtdx * cpq[m];
+          H[0][1][m] = H[0][1][m] - dtdx * cmq[m];
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          st[(long long)(10 + (s * 3 + d) * 5 + m) * ss] = G[s][d][m];
+          st[(long long)(40 + (s * 3 + d) * 5 + m) * ss] = H[s][d][m];
+        }
+  }
+  // block-wide max of the Courant number, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
+  if ((threadIdx.x & 31) == 0 && cfl > 0.0) atomic_max_nonneg(A.cflmax, cfl);
+}
+
+// stash element of gadd (kind 10) / hadd (kind 40) for side s (1,2), offset d (-1..1), component m (0..4)
+__device__ __forceinline__ int sidx(int kind, int s, int d, int m) { return kind + ((s - 1) * 3 + (d + 1)) * 5 + m; }
+
+// ------------------------------------------------------------------- faces
+__global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
+  // face cells [face0[0], face0[np]): the level's, or one patch's through a one-patch view
+  const long long first = A.face0[0], total = A.face0[A.np];
+  const long long ss = A.stash_stride;
+  const double* S = A.stash;
+  for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(A.face0, A.np, t);
+    const PatchDev& P = A.patches[A.plist[pi]];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+    const long long loc = t - A.face0[pi];
+    const int i = (int)(loc % (mx + 1)) + 1;
+    const int j = (int)((loc / (mx + 1)) % (my + 1)) + 1;
+    const int k = (int)(loc / ((long long)(mx + 1) * (my + 1))) + 1;
+    const long long bx = A.sweep0[pi], by = A.sweep0[(A.np + 1) + pi], bz = A.sweep0[2 * (A.np + 1) + pi];
+    auto xs = [&](int jj, int kk, int ii) { return bx + ((long long)(kk * (my + 2) + jj) * (mx + 1) + (ii - 1)); };
+    auto ys = [&](int ii, int kk, int jj) { return by + ((long long)(kk * (mx + 2) + ii) * (my + 1) + (jj - 1)); };
+    auto zs = [&](int ii, int jj, int kk) { return bz + ((long long)(jj * (mx + 2) + ii) * (mz + 1) + (kk - 1)); };
+    double* F = A.flux + t;
+    const long long fs = A.flux_stride;
+    if (j <= my && k <= mz) {  // x-face i
+      double fm[5], fp[5];
+      const long long sx = xs(j, k, i);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { fm[m] = 0.0 + S[m * ss + sx]; fp[m] = 0.0 + S[(5 + m) * ss + sx]; }
+      // y-sweeps: k' = k-1, k, k+1 (d = +1, 0, -1); pencil i-1 (side 2) then i (side 1)
+#pragma unroll
+      for (int d = 1; d >= -1; --d) {
+        const long long s2 = ys(i - 1, k - d, j), s1 = ys(i, k - d, j);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          const double t2 = S[sidx(40, 2, d, m) * ss + s2];
+          fm[m] = fm[m] + t2; fp[m] = fp[m] + t2;
+          const double t1 = S[sidx(40, 1, d, m) * ss + s1];
+          fm[m] = fm[m] + t1; fp[m] = fp[m] + t1;
+        }
+      }
+      // z-sweeps: j' = j-1, j, j+1 (d = +1, 0, -1); pencil i-1 (side 2) then i (side 1)
+#pragma unroll
+      for (int d = 1; d >= -1; --d) {
+        const long long s2 = zs(i - 1, j - d, k), s1 = zs(i, j - d, k);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          const double t2 = S[sidx(10, 2, d, m) * ss + s2];
+          fm[m] = fm[m] + t2; fp[m] = fp[m] + t2;
+          const double t1 = S[sidx(10, 1, d, m) * ss + s1];
+          fm[m] = fm[m] + t1; fp[m] = fp[m] + t1;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { F[(0 * 5 + m) * fs] = fm[m]; F[(1 * 5 + m) * fs] = fp[m]; }
+    }
+    if (i <= mx && k <= mz) {  // y-face j
+      double gm[5], gp[5];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) gm[m] = 0.0;
+      // x-sweeps: k' = k-1, k, k+1 (d = +1, 0, -1); pencil j-1 (side 2) then j (side 1)
+#pragma unroll
+      for (int d = 1; d >= -1; --d) {
+        const long long s2 = xs(j - 1, k - d, i), s1 = xs(j, k - d, i);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          gm[m] = gm[m] + S[sidx(10, 2, d, m) * ss + s2];
+          gm[m] = gm[m] + S[sidx(10, 1, d, m) * ss + s1];
+        }
+      }
+      const long long sy = ys(i, k, j);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { gp[m] = gm[m] + S[(5 + m) * ss + sy]; gm[m] = gm[m] + S[m * ss + sy]; }
+      // z-sweeps: j' = j-1 (side 2) for i' = i-1, i, i+1 (d = +1, 0, -1), then j' = j (side 1)
+#pragma unroll
+      for (int side = 2; side >= 1; --side) {
+        const int jp = (side == 2) ? j - 1 : j;
+#pragma unroll
+        for (int d = 1; d >= -1; --d) {
+          const long long sz = zs(i - d, jp, k);
+#pragma unroll
+          for (int m = 0; m < 5; ++m) {
+            const double tv = S[sidx(40, side, d, m) * ss + sz];
+            gm[m] = gm[m] + tv; gp[m] = gp[m] + tv;
+          }
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { F[(2 * 5 + m) * fs] = gm[m]; F[(3 * 5 + m) * fs] = gp[m]; }
+    }
+    if (i <= mx && j <= my) {  // z-face k
+      double hm[5], hp[5];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) hm[m] = 0.0;
+      // x-sweeps: k' = k-1 (side 2) for j' = j-1, j, j+1 (d = +1, 0, -1), then k' = k (side 1)
+#pragma unroll
+      for (int side = 2; side >= 1; --side) {
+        const int kp = (side == 2) ? k - 1 : k;
+#pragma unroll
+        for (int d = 1; d >= -1; --d) {
+          const long long sx = xs(j - d, kp, i);
+#pragma unroll
+          for (int m = 0; m < 5; ++m) hm[m] = hm[m] + S[sidx(40, side, d, m) * ss + sx];
+        }
+      }
+      // y-sweeps: k' = k-1 (side 2) for i' = i-1, i, i+1, then k' = k (side 1)
+#pragma unroll
+      for (int side = 2; side >= 1; --side) {
+        const int kp = (side == 2) ? k - 1 : k;
+#pragma unroll
+        for (int d = 1; d >= -1; --d) {
+          const long long sy = ys(i - d, kp, j);
+#pragma unroll
+          for (int m = 0; m < 5; ++m) hm[m] = hm[m] + S[sidx(10, side, d, m) * ss + sy];
+        }
+      }
+      const long long sz = zs(i, j, k);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { hp[m] = hm[m] + S[(5 + m) * ss + sz]; hm[m] = hm[m] + S[m * ss + sz]; }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { F[(4 * 5 + m) * fs] = hm[m]; F[(5 * 5 + m) * fs] = hp[m]; }
+    }
+  }
+}
+
+// ------------------------------------------------------------------- update
+__global__ void __launch_bounds__(256) update3_kernel(Step3Args A) {
+  const long long first = A.cell0[0], total = A.cell0[A.np];
+  const long long fs = A.flux_stride;
+  const double dtdx = A.dt / A.dx, dtdy = A.dt / A.dy, dtdz = A.dt / A.dz;
+  for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(A.cell0, A.np, t);
+    const PatchDev& P = A.patches[A.plist[pi]];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+    const long long loc = t - A.cell0[pi];
+    const int i = (int)(loc % mx) + 1, j = (int)((loc / mx) % my) + 1, k = (int)(loc / ((long long)mx * my)) + 1;
+    const long long f0 = A.face0[pi];
+    auto fidx = [&](int ii, int jj, int kk) { return f0 + ((long long)(kk - 1) * (my + 1) + (jj - 1)) * (mx + 1) + (ii - 1); };
+    const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
+    const long long at = ((long long)(k - 1 + NG3) * P.mjtot + (j - 1 + NG3)) * P.mitot + (i - 1 + NG3);
+    const double* q = A.pool + P.q[P.cur];
+    double* qn = const_cast<double*>(A.pool) + P.q[1 - P.cur];
+    const long long c = fidx(i, j, k), cx = fidx(i + 1, j, k), cy = fidx(i, j + 1, k), cz = fidx(i, j, k + 1);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      const double* F = A.flux + (long long)m * fs;
+      const double fmv = F[0 * 5 * fs + cx], fpv = F[1 * 5 * fs + c];
+      const double gmv = F[2 * 5 * fs + cy], gpv = F[3 * 5 * fs + c];
+      const double hmv = F[4 * 5 * fs + cz], hpv = F[5 * 5 * fs + c];
+      qn[m * plane + at] = q[m * plane + at] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv) - dtdz * (hmv - hpv);
+    }
+  }
+}
+
+// fluxsv.f:4-94: one register entry per thread
+__global__ void fsv3_kernel(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
+                            const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const Fsv3 E = e[t];
+  const PatchDev& P = patches[E.patch];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+  auto fidx = [&](int ii, int jj, int kk) { return face0[E.pidx] + ((long long)(kk - 1) * (my + 1) + (jj - 1)) * (mx + 1) + (ii - 1); };
+  int comp; long long c; double h1, h2;
+  switch (E.side) {
+    case 1: comp = 1; c = fidx(E.i, E.j, E.k); h1 = hy; h2 = hz; break;
+    case 2: comp = 2; c = fidx(E.i, E.j + 1, E.k); h1 = hx; h2 = hz; break;
+    case 3: comp = 0; c = fidx(E.i + 1, E.j, E.k); h1 = hy; h2 = hz; break;
+    case 4: comp = 3; c = fidx(E.i, E.j, E.k); h1 = hx; h2 = hz; break;
+    case 5: comp = 5; c = fidx(E.i, E.j, E.k); h1 = hx; h2 = hy; break;
+    default: comp = 4; c = fidx(E.i, E.j, E.k + 1); h1 = hx; h2 = hy; break;
+  }
+  for (int m = 0; m < nvar; ++m) regs[E.dst + m] = -flux[((long long)comp * 5 + m) * fs + c] * dtc * h1 * h2;
+}
+
+// fluxad.f:4-155: one coarse face (register) of a fine patch per thread
+__global__ void fad3_kernel(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
+                            const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const Fad3 E = e[t];
+  const PatchDev& P = patches[E.patch];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+  auto fidx = [&](int ii, int jj, int kk) { return face0[E.pidx] + ((long long)(kk - 1) * (my + 1) + (jj - 1)) * (mx + 1) + (ii - 1); };
+  double* sv = regs + P.ffl + (long long)nvar * E.seg;
+  int comp; double h1, h2;
+  switch (E.side) {
+    case 1: comp = 0; h1 = hy; h2 = hz; break;
+    case 2: comp = 3; h1 = hx; h2 = hz; break;
+    case 3: comp = 1; h1 = hy; h2 = hz; break;
+    case 4: comp = 2; h1 = hx; h2 = hz; break;
+    case 5: comp = 4; h1 = hx; h2 = hy; break;
+    default: comp = 5; h1 = hx; h2 = hy; break;
+  }
+  for (int m = 0; m < nvar; ++m) {
+    double acc = sv[m];
+    const double* F = flux + ((long long)comp * 5 + m) * fs;
+    for (int ob = 1; ob <= E.nb; ++ob)
+      for (int oa = 1; oa <= E.na; ++oa) {
+        long long c;
+        switch (E.side) {
+          case 1: c = fidx(1, E.a0 + oa, E.b0 + ob); break;
+          case 2: c = fidx(E.a0 + oa, my + 1, E.b0 + ob); break;
+          case 3: c = fidx(mx + 1, E.a0 + oa, E.b0 + ob); break;
+          case 4: c = fidx(E.a0 + oa, 1, E.b0 + ob); break;
+          case 5: c = fidx(E.a0 + oa, E.b0 + ob, 1); break;
+          default: c = fidx(E.a0 + oa, E.b0 + ob, mz + 1); break;
+        }
+        acc = acc + F[c] * dtf * h1 * h2;
+      }
+    sv[m] = acc;
+  }
+}
+
+// qad.f:4-534: one register of one side of a fine patch per thread
+__global__ void qad3_kernel(double* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
+                            int nvar, double hx, double hy, double hz, double delt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= njobs) return;
+  const Qad3Job J = jobs[t];
+  const PatchDev& P = patches[J.patch];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+  const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
+  const double* q = pool + P.q[P.cur];
+  auto at = [&](int i, int j, int k) { return ((long long)(k - 1 + NG3) * P.mjtot + (j - 1 + NG3)) * P.mitot + (i - 1 + NG3); };
+  double* sv = regs + P.ffl + (long long)nvar * J.reg0;
+  const double* qc = regs + P.ffl + (long long)nvar * P.lenbc + (long long)nvar * J.reg0;
+  double C[6], Fv[6];
+  C[0] = 0.0; Fv[0] = 0.0;
+  for (int m = 1; m <= 5; ++m) C[m] = qc[m - 1];
+  int dir; double sgn, h1, h2;
+  switch (J.side) {
+    case 1: dir = 1; sgn = 1.0; h1 = hy; h2 = hz; break;
+    case 2: dir = 2; sgn = -1.0; h1 = hx; h2 = hz; break;
+    case 3: dir = 1; sgn = -1.0; h1 = hy; h2 = hz; break;
+    case 4: dir = 2; sgn = 1.0; h1 = hx; h2 = hz; break;
+    case 5: dir = 3; sgn = 1.0; h1 = hx; h2 = hy; break;
+    default: dir = 3; sgn = -1.0; h1 = hx; h2 = hy; break;
+  }
+  double acc[5];
+  for (int m = 0; m < 5; ++m) acc[m] = sv[m];
+  for (int ks = 1; ks <= J.ratio_b; ++ks) {       // fine rows of the slab (outer loop of qad.f)
+    for (int l = 1; l <= J.ratio_a; ++l) {         // fine cells of the coarse face
+      const int r = J.row0 + l;                    // fine index along the row, 1-based interior
+      const int s = J.slab * J.ratio_b + ks;       // fine index across the rows
+      int i, j, k;
+      switch (J.side) {
+        case 1: i = 0; j = r; k = s; break;
+        case 2: i = r; j = my + 1; k = s; break;
+        case 3: i = mx + 1; j = r; k = s; break;
+        case 4: i = r; j = 0; k = s; break;
+        case 5: i = r; j = s; k = 0; break;
+        default: i = r; j = s; k = mz + 1; break;
+      }
+      const long long a = at(i, j, k);
+      for (int m = 1; m <= 5; ++m) Fv[m] = q[(m - 1) * plane + a];
+      double W[3][5], S[3], am[5], ap[5];
+      const bool low = (J.side == 1 || J.side == 4 || J.side == 5);
+      if (low) euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, dir, C, Fv, W, S, am, ap);
+      else euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, dir, Fv, C, W, S, am, ap);
+      for (int m = 0; m < 5; ++m) {
+        if (sgn > 0.0) acc[m] = acc[m] + am[m] * h1 * h2 * delt + ap[m] * h1 * h2 * delt;
+        else acc[m] = acc[m] - am[m] * h1 * h2 * delt - ap[m] * h1 * h2 * delt;
+      }
+    }
+  }
+  for (int m = 0; m < 5; ++m) sv[m] = acc[m];
+  (void)nvar; (void)mz;
+}
+
+// ------------------------------------------------------------------- ghost fill
+__device__ __forceinline__ double* fill3_dst(const Fill3Args& a, const Fill3Op& o, int& ni, int& nj, long long& plane) {
+  if (o.dst_patch >= 0) {
+    const PatchDev& P = a.patches[o.dst_patch];
+    ni = P.mitot; nj = P.mjtot; plane = (long long)P.mitot * P.mjtot * P.mktot;
+    return a.pool + P.q[P.cur];
+  }
+  const Rect3& R = a.rects[o.dst_rect];
+  ni = R.ni; nj = R.nj; plane = (long long)R.ni * R.nj * R.nk;
+  return a.pool + R.off;
+}
+
+__global__ void fill3_kernel(Fill3Args a) {
+  const int c = blockIdx.x;
+  if (c >= a.nchunks) return;
+  const Fill3Chunk ch = a.chunks[c];
+  if ((int)threadIdx.x >= ch.count) return;
+  const Fill3Op o = a.ops[ch.op];
+  const long long cell = ch.start + threadIdx.x;
+  const int nvar = a.nvar;
+  if (o.kind == F3_RING) {
+    // cstore.f:4-96: faces x-left, y-top, x-right, y-bottom, z-bottom, z-top
+    const Rect3& R = a.rects[o.src];
+    const int nr = R.ni, nc = R.nj, nf = R.nk;
+    const long long s13 = (long long)(nf - 2) * (nc - 2), s24 = (long long)(nf - 2) * (nr - 2), s56 = (long long)(nc - 2) * (nr - 2);
+    long long k = cell;
+    int ii, jj, kk;
+    if (k < s13) { ii = 1; kk = 2 + (int)(k / (nc - 2)); jj = 2 + (int)(k % (nc - 2)); }
+    else if ((k -= s13) < s24) { jj = nc; kk = 2 + (int)(k / (nr - 2)); ii = 2 + (int)(k % (nr - 2)); }
+    else if ((k -= s24) < s13) { ii = nr; kk = 2 + (int)(k / (nc - 2)); jj = 2 + (int)(k % (nc - 2)); }
+    else if ((k -= s13) < s24) { jj = 1; kk = 2 + (int)(k / (nr - 2)); ii = 2 + (int)(k % (nr - 2)); }
+    else if ((k -= s24) < s56) { kk = 1; jj = 2 + (int)(k / (nr - 2)); ii = 2 + (int)(k % (nr - 2)); }
+    else { k -= s56; kk = nf; jj = 2 + (int)(k / (nr - 2)); ii = 2 + (int)(k % (nr - 2)); }
+    const PatchDev& K = a.patches[o.dst_patch];
+    double* qc1d = a.regs + K.ffl + (long long)nvar * K.lenbc + (long long)nvar * cell;
+    const double* src = a.pool + R.off;
+    const long long pl = (long long)nr * nc * nf;
+    const long long idx = ((long long)(kk - 1) * nc + (jj - 1)) * nr + (ii - 1);
+    for (int m = 0; m < nvar; ++m) qc1d[m] = src[m * pl + idx];
+    return;
+  }
+  const int ia = (int)(cell % o.ni), jb = (int)((cell / o.ni) % o.nj), kc = (int)(cell / ((long long)o.ni * o.nj));
+  int dni, dnj; long long plane;
+  double* dst = fill3_dst(a, o, dni, dnj, plane);
+  const long long dk = ((long long)(o.dk0 + kc) * dnj + (o.dj0 + jb)) * dni + (o.di0 + ia);
+  if (o.kind == F3_COPY) {
+    const PatchDev& S = a.patches[o.src];
+    const long long sp = (long long)S.mitot * S.mjtot * S.mktot;
+    const long long sk = ((long long)(o.sk0 + kc) * S.mjtot + (o.sj0 + jb)) * S.mitot + (o.si0 + ia);
+    int mode = 0; double ai = 1.0, ac = 0.0;
+    if (o.level >= 0) { mode = a.modes.mode[o.level]; ai = a.modes.alphai[o.level]; ac = a.modes.alphac[o.level]; }
+    const double* qn = a.pool + S.q[S.cur];
+    const double* qo = a.pool + S.q[1 - S.cur];
+    for (int m = 0; m < nvar; ++m) {
+      double v;
+      if (mode == 0) v = qn[m * sp + sk];
+      else if (mode == 1) v = qo[m * sp + sk];
+      else v = qn[m * sp + sk] * ai + qo[m * sp + sk] * ac;
+      dst[m * plane + dk] = v;
+    }
+    return;
+  }
+  const Rect3& R = a.rects[o.src];
+  const double* vc = a.pool + R.off;
+  const long long cp = (long long)R.ni * R.nj * R.nk;
+  auto VC = [&](int m, int i, int j, int k) { return vc[m * cp + ((long long)(k - 1) * R.nj + (j - 1)) * R.ni + (i - 1)]; };
+  const int lev = o.level;
+  const int rx = a.lc.intratx[lev - 1], ry = a.lc.intraty[lev - 1], rz = a.lc.intratz[lev - 1];
+  const int ifg = o.si0 + ia, jfg = o.sj0 + jb, kfg = o.sk0 + kc;
+  const int icg = floordiv3(ifg, rx), jcg = floordiv3(jfg, ry), kcg = floordiv3(kfg, rz);
+  const int ic = icg - o.cilo + 1, jc = jcg - o.cjlo + 1, kcc = kcg - o.cklo + 1;
+  if (o.kind == F3_INTERP) {
+    // filpatch.f:182-269 limited trilinear-slope interpolation
+    const double hxf = a.lc.hx[lev], hyf = a.lc.hy[lev], hzf = a.lc.hz[lev];
+    const double hxc = a.lc.hx[lev - 1], hyc = a.lc.hy[lev - 1], hzc = a.lc.hz[lev - 1];
+    const double xlc = a.xlower + o.cilo * hxc, ybc = a.ylower + o.cjlo * hyc, zfc = a.zlower + o.cklo * hzc;
+    const double eta1 = ((a.xlower + (ifg + 0.5) * hxf) - (xlc + (ic - 0.5) * hxc)) / hxc;
+    const double eta2 = ((a.ylower + (jfg + 0.5) * hyf) - (ybc + (jc - 0.5) * hyc)) / hyc;
+    const double eta3 = ((a.zlower + (kfg + 0.5) * hzf) - (zfc + (kcc - 0.5) * hzc)) / hzc;
+    for (int m = 0; m < nvar; ++m) {
+      const double valp100 = VC(m, ic + 1, jc, kcc), valm100 = VC(m, ic - 1, jc, kcc), valc = VC(m, ic, jc, kcc);
+      const double valp010 = VC(m, ic, jc + 1, kcc), valm010 = VC(m, ic, jc - 1, kcc);
+      const double valp001 = VC(m, ic, jc, kcc + 1), valm001 = VC(m, ic, jc, kcc - 1);
+      const double dupc = valp100 - valc, dumc = valc - valm100, ducc = valp100 - valm100;
+      double du = dmin(fabs(dupc), fabs(dumc));
+      du = dmin(2.0 * du, 0.5 * fabs(ducc));
+      const double fu = dmax(0.0, dsign(1.0, dupc * dumc));
+      const double uslope = du * dsign(1.0, ducc) * fu;
+      const double dvpc = valp010 - valc, dvmc = valc - valm010, dvcc = valp010 - valm010;
+      double dv = dmin(fabs(dvpc), fabs(dvmc));
+      dv = dmin(2.0 * dv, 0.5 * fabs(dvcc));
+      const double fv = dmax(0.0, dsign(1.0, dvpc * dvmc));
+      const double vslope = dv * dsign(1.0, dvcc) * fv;
+      const double dwpc = valp001 - valc, dwmc = valc - valm001, dwcc = valp001 - valm001;
+      double dw = dmin(fabs(dwpc), fabs(dwmc));
+      dw = dmin(2.0 * dw, 0.5 * fabs(dwcc));
+      const double fw = dmax(0.0, dsign(1.0, dwpc * dwmc));
+      const double wslope = dw * dsign(1.0, dwcc) * fw;
+      dst[m * plane + dk] = valc + eta1 * uslope + eta2 * vslope + eta3 * wslope;
+    }
+    return;
+  }
+  // F3_FILVAL: filval.f:84-137 minmod-limited interpolation into a new patch
+  const int ico = ifg - icg * rx + 1, jco = jfg - jcg * ry + 1, kco = kfg - kcg * rz + 1;
+  const double xoff = ((double)ico - .5) / rx - .5, yoff = ((double)jco - .5) / ry - .5, zoff = ((double)kco - .5) / rz - .5;
+  for (int m = 0; m < nvar; ++m) {
+    double slp = VC(m, ic + 1, jc, kcc) - VC(m, ic, jc, kcc), slm = VC(m, ic, jc, kcc) - VC(m, ic - 1, jc, kcc);
+    double s = dmin(fabs(slp), fabs(slm)) * dsign(1.0, VC(m, ic + 1, jc, kcc) - VC(m, ic - 1, jc, kcc));
+    const double dudx = (slm * slp > 0.0) ? s : 0.0;
+    slp = VC(m, ic, jc + 1, kcc) - VC(m, ic, jc, kcc); slm = VC(m, ic, jc, kcc) - VC(m, ic, jc - 1, kcc);
+    s = dmin(fabs(slp), fabs(slm)) * dsign(1.0, VC(m, ic, jc + 1, kcc) - VC(m, ic, jc - 1, kcc));
+    const double dudy = (slm * slp > 0.0) ? s : 0.0;
+    slp = VC(m, ic, jc, kcc + 1) - VC(m, ic, jc, kcc); slm = VC(m, ic, jc, kcc) - VC(m, ic, jc, kcc - 1);
+    s = dmin(fabs(slp), fabs(slm)) * dsign(1.0, VC(m, ic, jc, kcc + 1) - VC(m, ic, jc, kcc - 1));
+    const double dudz = (slm * slp > 0.0) ? s : 0.0;
+    dst[m * plane + dk] = VC(m, ic, jc, kcc) + xoff * dudx + yoff * dudy + zoff * dudz;
+  }
+}
+
+// bc3amr.f90:70-380. phase 0: x sides per (j,k) row; 1: y sides per (i,k); 2: z sides per (i,j).
+__global__ void bc3_kernel(Bc3Args a, int phase) {
+  const int op = blockIdx.y;
+  if (op >= a.nops) return;
+  const Bc3Op o = a.ops[op];
+  double* v;
+  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = a.pool + P.q[P.cur]; }
+  else v = a.pool + a.rects[o.dst_rect].off;
+  const int nr = o.nrow, nc = o.ncol, nf = o.nfil;
+  const long long plane = (long long)nr * nc * nf;
+  auto V = [&](int m, int i, int j, int k) -> double& { return v[m * plane + ((long long)(k - 1) * nc + (j - 1)) * nr + (i - 1)]; };
+  const int nvar = a.nvar;
+  const int lines = phase == 0 ? nc * nf : phase == 1 ? nr * nf : nr * nc;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < lines; t += gridDim.x * blockDim.x) {
+    if (phase == 0) {
+      const int j = t % nc + 1, k = t / nc + 1;
+      if (o.nxl > 0 && (o.bxl == 1 || o.bxl == 3)) {
+        for (int i = 1; i <= o.nxl; ++i) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, o.bxl == 1 ? o.nxl + 1 : 2 * o.nxl + 1 - i, j, k);
+        if (o.bxl == 3) for (int i = 1; i <= o.nxl; ++i) V(1, i, j, k) = -V(1, i, j, k);
+      }
+      if (o.ibeg > 0 && (o.bxr == 1 || o.bxr == 3)) {
+        for (int i = o.ibeg; i <= nr; ++i) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, o.bxr == 1 ? o.ibeg - 1 : 2 * o.ibeg - 1 - i, j, k);
+        if (o.bxr == 3) for (int i = o.ibeg; i <= nr; ++i) V(1, i, j, k) = -V(1, i, j, k);
+      }
+    } else if (phase == 1) {
+      const int i = t % nr + 1, k = t / nr + 1;
+      if (o.nyl > 0 && (o.byl == 1 || o.byl == 3)) {
+        for (int j = 1; j <= o.nyl; ++j) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, o.byl == 1 ? o.nyl + 1 : 2 * o.nyl + 1 - j, k);
+        if (o.byl == 3) for (int j = 1; j <= o.nyl; ++j) V(2, i, j, k) = -V(2, i, j, k);
+      }
+      if (o.jbeg > 0 && (o.byr == 1 || o.byr == 3)) {
+        for (int j = o.jbeg; j <= nc; ++j) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, o.byr == 1 ? o.jbeg - 1 : 2 * o.jbeg - 1 - j, k);
+        if (o.byr == 3) for (int j = o.jbeg; j <= nc; ++j) V(2, i, j, k) = -V(2, i, j, k);
+      }
+    } else {
+      const int i = t % nr + 1, j = t / nr + 1;
+      if (o.nzl > 0 && (o.bzl == 1 || o.bzl == 3)) {
+        for (int k = 1; k <= o.nzl; ++k) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, j, o.bzl == 1 ? o.nzl + 1 : 2 * o.nzl + 1 - k);
+        if (o.bzl == 3) for (int k = 1; k <= o.nzl; ++k) V(3, i, j, k) = -V(3, i, j, k);
+      }
+      if (o.kbeg > 0 && (o.bzr == 1 || o.bzr == 3)) {
+        for (int k = o.kbeg; k <= nf; ++k) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, j, o.bzr == 1 ? o.kbeg - 1 : 2 * o.kbeg - 1 - k);
+        if (o.bzr == 3) for (int k = o.kbeg; k <= nf; ++k) V(3, i, j, k) = -V(3, i, j, k);
+      }
+    }
+  }
+}
+
+// upbnd.f:4-94: one coarse cell per thread, its terms in listbc order
+__global__ void upbnd3_kernel(double* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
+                              const Upbnd3Term* terms, double volume, int nvar) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const Upbnd3Cell c = cells[t];
+  const PatchDev& P = patches[c.patch];
+  const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
+  double* q = pool + P.q[P.cur];
+  const long long at = ((long long)c.ke * P.mjtot + c.je) * P.mitot + c.ie;
+  for (int m = 0; m < nvar; ++m) {
+    double v = q[m * plane + at];
+    for (int k = 0; k < c.count; ++k) {
+      const Upbnd3Term tm = terms[c.first + k];
+      v = v + tm.sgn * regs[tm.reg + m] / volume;
+    }
+    q[m * plane + at] = v;
+  }
+}
+
+// update.f:118-178: mean of the fine cells over each covered coarse cell
+__global__ void average3_kernel(double* pool, const PatchDev* patches, const Avg3* rects, int n, int rx, int ry, int rz, int nvar) {
+  const int r = blockIdx.y;
+  if (r >= n) return;
+  const Avg3 A = rects[r];
+  const PatchDev& C = patches[A.cpatch];
+  const PatchDev& F = patches[A.kpatch];
+  const long long cpl = (long long)C.mitot * C.mjtot * C.mktot, fpl = (long long)F.mitot * F.mjtot * F.mktot;
+  double* qc = pool + C.q[C.cur];
+  const double* qf = pool + F.q[F.cur];
+  const int totrat = rx * ry * rz;
+  const int cells = A.ni * A.nj * A.nk;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cells; t += gridDim.x * blockDim.x) {
+    const int a = t % A.ni, b = (t / A.ni) % A.nj, c = t / (A.ni * A.nj);
+    const long long cat = ((long long)(A.ck0 + c) * C.mjtot + (A.cj0 + b)) * C.mitot + (A.ci0 + a);
+    const int fi = A.fi0 + a * rx, fj = A.fj0 + b * ry, fk = A.fk0 + c * rz;
+    for (int m = 0; m < nvar; ++m) {
+      double v = 0.0;
+      for (int kco = 0; kco < rz; ++kco)
+        for (int jco = 0; jco < ry; ++jco)
+          for (int ico = 0; ico < rx; ++ico) v = v + qf[m * fpl + ((long long)(fk + kco) * F.mjtot + (fj + jco)) * F.mitot + (fi + ico)];
+      qc[m * cpl + cat] = v / totrat;
+    }
+  }
+}
+
+// spest.f + flag2refine.f: BADPT (2) where the undivided difference exceeds tolsp, else GOODPT (0)
+__global__ void flags3_kernel(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
+                              int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* out, long long ncells) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ncells; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(cell0, np, t);
+    const PatchDev& P = patches[plist[pi]];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+    const long long loc = t - cell0[pi];
+    const int i = (int)(loc % mx) + 1, j = (int)((loc / mx) % my) + 1, k = (int)(loc / ((long long)mx * my)) + 1;
+    const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
+    const double* q = pool + P.q[P.cur];
+    auto Q = [&](int m, int ii, int jj, int kk) { return q[(m - 1) * plane + ((long long)(kk - 1 + NG3) * P.mjtot + (jj - 1 + NG3)) * P.mitot + (ii - 1 + NG3)]; };
+    double dq = 0.0;
+    if (flag_pressure) {
+      auto pres = [&](int a, int b, int c) {
+        const double rho = Q(1, a, b, c), mu = Q(2, a, b, c), mv = Q(3, a, b, c), mw = Q(4, a, b, c);
+        return gamma1 * (Q(5, a, b, c) - 0.5 * (mu * mu + mv * mv + mw * mw) / rho);
+      };
+      const double dpi = fabs(pres(i + 1, j, k) - pres(i - 1, j, k));
+      const double dpj = fabs(pres(i, j + 1, k) - pres(i, j - 1, k));
+      const double dpk = fabs(pres(i, j, k + 1) - pres(i, j, k - 1));
+      dq = dmax(dmax(dmax(dq, dpi), dpj), dpk);
+    } else {
+      for (int m = 1; m <= nvar; ++m) {
+        const double dqi = fabs(Q(m, i + 1, j, k) - Q(m, i - 1, j, k));
+        const double dqj = fabs(Q(m, i, j + 1, k) - Q(m, i, j - 1, k));
+        const double dqk = fabs(Q(m, i, j, k + 1) - Q(m, i, j, k - 1));
+        dq = dmax(dmax(dmax(dq, dqi), dqj), dqk);
+      }
+    }
+    out[t] = (dq > tolsp) ? (int8_t)2 : (int8_t)0;
+  }
+}
+
+// gauges_module.f90:376-430 trilinear sample
+__global__ void gauges3_kernel(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const Gauge3Job J = jobs[t];
+  const PatchDev& P = patches[J.patch];
+  const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
+  const double* q = pool + P.q[P.cur];
+  auto Q = [&](int m, int ii, int jj, int kk) { return q[m * plane + ((long long)(kk - 1) * P.mjtot + (jj - 1)) * P.mitot + (ii - 1)]; };
+  const double xoff = J.xoff, yoff = J.yoff, zoff = J.zoff;
+  const int ii = J.ii, jj = J.jj, kk = J.kk;
+  for (int m = 0; m < nvar; ++m) {
+    double v = (1.0 - xoff) * (1.0 - yoff) * Q(m, ii, jj, kk) + xoff * (1.0 - yoff) * Q(m, ii + 1, jj, kk) +
+               (1.0 - xoff) * yoff * Q(m, ii, jj + 1, kk) + xoff * yoff * Q(m, ii + 1, jj + 1, kk);
+    v = v * (1.0 - zoff);
+    v = v + zoff * ((1.0 - xoff) * (1.0 - yoff) * Q(m, ii, jj, kk + 1) + xoff * (1.0 - yoff) * Q(m, ii + 1, jj, kk + 1) +
+                    (1.0 - xoff) * yoff * Q(m, ii, jj + 1, kk + 1) + xoff * yoff * Q(m, ii + 1, jj + 1, kk + 1));
+    out[(long long)J.slot * nvar + m] = v;
+  }
+}
+
+__global__ void mass3_kernel(const double* pool, const PatchDev* patches, const int* plist, int np, double* out) {
+  const int p = blockIdx.y;
+  if (p >= np) return;
+  const PatchDev& P = patches[plist[p]];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+  const double* q = pool + P.q[P.cur];
+  double s = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my * mz; t += gridDim.x * blockDim.x) {
+    const int i = t % mx, j = (t / mx) % my, k = t / (mx * my);
+    s += q[((long long)(k + NG3) * P.mjtot + (j + NG3)) * P.mitot + (i + NG3)];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+__global__ void gather3_kernel(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
+                               long long total, double* out) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(cell0, np, t);
+    const PatchDev& P = patches[plist[pi]];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+    const long long n = (long long)mx * my * mz;
+    const long long loc = t - cell0[pi];
+    const int i = (int)(loc % mx), j = (int)((loc / mx) % my), k = (int)(loc / ((long long)mx * my));
+    const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
+    const double* q = pool + P.q[P.cur];
+    const long long at = ((long long)(k + NG3) * P.mjtot + (j + NG3)) * P.mitot + (i + NG3);
+    for (int m = 0; m < nvar; ++m) out[cell0[pi] * nvar + m * n + loc] = q[m * plane + at];
+  }
+}
+
+int grid_for(long long n, int block) {
+  const long long g = (n + block - 1) / block;
+  return (int)std::max<long long>(1, std::min<long long>(g, 148LL * 64));
+}
+
+}  // namespace
+
+void launch_step3(const Step3Args& a, long long items[3], long long faces, long long cells, cudaStream_t s) {
+  if (items[0] > 0) sweep3_kernel<1><<<grid_for(items[0], 128), 128, 0, s>>>(a);
+  if (items[1] > 0) sweep3_kernel<2><<<grid_for(items[1], 128), 128, 0, s>>>(a);
+  if (items[2] > 0) sweep3_kernel<3><<<grid_for(items[2], 128), 128, 0, s>>>(a);
+  AMR_CUDA(cudaGetLastError());
+  if (faces > 0) face3_kernel<<<grid_for(faces, 128), 128, 0, s>>>(a);
+  if (cells > 0) update3_kernel<<<grid_for(cells, 256), 256, 0, s>>>(a);
+  AMR_CUDA(cudaGetLastError());
+}
+
+void launch_fsv3(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fsv3* e, int n,
+                 int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s) {
+  if (n <= 0) return;
+  fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(flux, fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz);
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_fad3(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fad3* e, int n,
+                 int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s) {
+  if (n <= 0) return;
+  fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(flux, fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz);
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_qad3(double* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp, int nvar,
+                 double hx, double hy, double hz, double delt, cudaStream_t s) {
+  if (njobs <= 0) return;
+  qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(pool, regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_fill3(const Fill3Args& a, cudaStream_t s) {
+  if (a.nchunks <= 0) return;
+  for (int base = 0; base < a.nchunks; base += 1 << 30) {
+    Fill3Args b = a;
+    b.chunks = a.chunks + base;
+    b.nchunks = std::min(1 << 30, a.nchunks - base);
+    fill3_kernel<<<b.nchunks, 128, 0, s>>>(b);
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s) {
+  if (a.nops <= 0) return;
+  for (int base = 0; base < a.nops; base += 65535) {
+    Bc3Args b = a;
+    b.ops = a.ops + base;
+    b.nops = std::min(65535, a.nops - base);
+    bc3_kernel<<<dim3(4, b.nops), 128, 0, s>>>(b, phase);
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_upbnd3(double* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n, const Upbnd3Term* terms,
+                   double volume, int nvar, cudaStream_t s) {
+  if (n <= 0) return;
+  upbnd3_kernel<<<(n + 127) / 128, 128, 0, s>>>(pool, regs, patches, cells, n, terms, volume, nvar);
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, int rx, int ry, int rz, int nvar, cudaStream_t s) {
+  if (n <= 0) return;
+  for (int base = 0; base < n; base += 65535) {
+    const int cnt = std::min(65535, n - base);
+    average3_kernel<<<dim3(4, cnt), 128, 0, s>>>(pool, patches, r + base, cnt, rx, ry, rz, nvar);
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_flags3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int flag_pressure,
+                   double gamma1, double tolsp, int nvar, int8_t* out, long long ncells, cudaStream_t s) {
+  if (ncells <= 0) return;
+  flags3_kernel<<<grid_for(ncells, 256), 256, 0, s>>>(pool, patches, plist, cell0, np, flag_pressure, gamma1, tolsp, nvar, out, ncells);
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_gauges3(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s) {
+  if (n <= 0) return;
+  gauges3_kernel<<<(n + 63) / 64, 64, 0, s>>>(pool, patches, jobs, n, nvar, out);
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_mass3(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s) {
+  if (np <= 0) return;
+  for (int base = 0; base < np; base += 65535) {
+    const int cnt = std::min(65535, np - base);
+    mass3_kernel<<<dim3(8, cnt), 128, 0, s>>>(pool, patches, plist + base, cnt, out);
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_gather3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
+                    long long total, double* out, cudaStream_t s) {
+  if (total <= 0) return;
+  gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(pool, patches, plist, cell0, np, nvar, total, out);
+  AMR_CUDA(cudaGetLastError());
+}
+
+}  // namespace amrb

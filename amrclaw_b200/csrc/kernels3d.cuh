@@ -1,0 +1,102 @@
+// Work items and launch wrappers of the 3D patch-advance kernels (kernels3d.cu).
+#pragma once
+#include "common.cuh"
+#include "riemann3d.cuh"
+
+namespace amrb {
+
+// Number of per-cell values a sweep leaves for the face kernel: faddm(5),
+// faddp(5), gadd(2 sides x 3 offsets x 5), hadd(2 x 3 x 5).
+constexpr int STASH3 = 70;
+
+struct Step3Params {
+  double gamma, gamma1;
+  int efix;
+  int mthlim[3];
+  int order;   // method(2)
+  int m3, m4;  // method(3) = 10*m3 + m4
+};
+
+// All patches of a level: prefix sums of the sweep items and face cells per patch.
+struct Step3Args {
+  const double* pool;
+  double* newq;              // nullptr: update in place is not used; q[1-cur] is written
+  const PatchDev* patches;
+  const int* plist;          // patch ids of the level, in level order
+  int np;
+  const long long* sweep0;   // [3][np+1]: first sweep item (= stash slot) of each patch, per direction
+  const long long* face0;    // [np+1]: first face cell of each patch ((mx+1)(my+1)(mz+1) each)
+  const long long* cell0;    // [np+1]: first interior cell of each patch (mx*my*mz each)
+  long long stash_stride;    // slots of one direction region x 3 (SoA stride)
+  double* stash;             // [STASH3][stash_stride]
+  double* flux;              // [6 comps][5][face cells]
+  long long flux_stride;     // face cells of the level
+  double dt, dx, dy, dz;
+  unsigned long long* cflmax;
+  Step3Params sp;
+};
+
+// fluxsv.f:4-94 entries (coarse patch faces next to a kid) and fluxad.f:4-155 registers.
+struct Fsv3 { int patch; int pidx; int i, j, k, side; long long dst; };  // i,j,k: 1-based interior cell
+struct Fad3 { int patch; int pidx; int side; int a0, b0; int na, nb; int seg; };  // one coarse face of a fine patch
+
+struct Qad3Job { int patch; int side; int slab; int row0; int nreg; int reg0; int ratio_a, ratio_b; };
+
+// ghost fill (filpatch.f / intfil.f / filval.f / cstore.f as programs)
+enum Fill3Kind { F3_COPY = 0, F3_INTERP = 1, F3_FILVAL = 2, F3_RING = 3 };
+struct Rect3 { long long off; int ni, nj, nk; };
+struct Fill3Op {
+  int kind;
+  int dst_patch, dst_rect;
+  int di0, dj0, dk0;     // origin (0-based) in the destination array
+  int ni, nj, nk;        // extent
+  int src;               // COPY: patch; INTERP/FILVAL/RING: rect
+  int si0, sj0, sk0;     // COPY: origin in the source enlarged array; INTERP/FILVAL: global fine index of the origin
+  int level;             // COPY: source level for time modes (-1: current); INTERP/FILVAL: fine level
+  int cilo, cjlo, cklo;  // global coarse index of the rect origin
+};
+struct Fill3Chunk { int op; long long start; int count; };
+struct Bc3Op {
+  int dst_patch, dst_rect;
+  int nrow, ncol, nfil;
+  int nxl, ibeg, nyl, jbeg, nzl, kbeg;   // ghost extents (0: side inside the domain)
+  int bxl, bxr, byl, byr, bzl, bzr;      // boundary codes (1 extrapolation, 3 wall)
+};
+struct Fill3Args {
+  double* pool; double* regs;
+  const PatchDev* patches;
+  const Rect3* rects;
+  const Fill3Op* ops;
+  const Fill3Chunk* chunks; int nchunks;
+  int nvar;
+  SrcMode modes;
+  LevelConst lc;
+  double xlower, ylower, zlower;
+};
+struct Bc3Args { double* pool; const PatchDev* patches; const Rect3* rects; const Bc3Op* ops; int nops; int nvar; };
+
+struct Avg3 { int cpatch, kpatch; int ci0, cj0, ck0, ni, nj, nk; int fi0, fj0, fk0; };
+struct Upbnd3Cell { int patch; int ie, je, ke; int first, count; };
+struct Upbnd3Term { long long reg; double sgn; };
+struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff; };
+
+void launch_step3(const Step3Args& a, long long items_per_dir[3], long long faces, long long cells, cudaStream_t s);
+void launch_fsv3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
+                 const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s);
+void launch_fad3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
+                 const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s);
+void launch_qad3(double* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
+                 int nvar, double hx, double hy, double hz, double delt, cudaStream_t s);
+void launch_fill3(const Fill3Args& a, cudaStream_t s);
+void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s);
+void launch_upbnd3(double* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
+                   const Upbnd3Term* terms, double volume, int nvar, cudaStream_t s);
+void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, int rx, int ry, int rz, int nvar, cudaStream_t s);
+void launch_flags3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
+                   int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* out, long long ncells, cudaStream_t s);
+void launch_gauges3(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s);
+void launch_mass3(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s);
+void launch_gather3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
+                    long long total, double* out, cudaStream_t s);
+
+}  // namespace amrb

@@ -1,0 +1,29 @@
+// The interface the C ABI drives: one AMR solve on one device (2D or 3D).
+#pragma once
+#include <string>
+#include <vector>
+
+namespace amrb {
+
+class AmrSolver {
+ public:
+  virtual ~AmrSolver() = default;
+  virtual int num_dim() const = 0;
+  virtual void set_batched(bool on) = 0;
+  virtual void set_profile(bool on) = 0;
+  virtual void run(int max_cycles) = 0;                    // tick.f
+  virtual double level_advance(int level, double* cfl) = 0;  // advanc.f; returns dtnew
+  virtual void update_level(int level) = 0;                 // update.f
+  virtual void regrid_from(int lbase) = 0;                  // regrid.f
+  virtual void valout(const char* dir) = 0;                 // valout.f90 (dir == nullptr: the run's output dir)
+  virtual double mass() = 0;                                // conck.f, level 1
+  virtual std::vector<double> info() = 0;
+  virtual std::vector<int> grid_rows() = 0;                 // 2 + 2*num_dim ints per grid
+  virtual std::vector<double> values() = 0;
+  virtual std::vector<double> gauge_rows() = 0;             // (3 + nvar) doubles per sample
+};
+
+// Builds and initialises the 3D solver (amr3d.cu) from the data files in rundir.
+AmrSolver* make_solver3(const std::string& rundir, const std::string& outdir, bool write_output);
+
+}  // namespace amrb

@@ -26,9 +26,11 @@ const char* amrgpu_last_error(void);
 
 /* Reads claw.data, amr.data, regions.data, gauges.data and setprob.data from
  * rundir (the files setrun.py writes), builds the initial hierarchy on the device
- * and writes frame 0 when output_t0 is set.
+ * and writes frame 0 when output_t0 is set. num_dim in claw.data selects the 2D
+ * path (amr2) or the 3D path (amr3, Euler equations).
  * Replaces the start-up of src/2d/amr2.f90:140-612 (input reading :148-394,
- * domain.f:4-110, setgrd.f:4-142, ginit.f:17-86, conck.f:6-73). */
+ * domain.f:4-110, setgrd.f:4-142, ginit.f:17-86, conck.f:6-73) and of
+ * src/3d/amr3.f90 (domain.f, setgrd.f, ginit.f of src/3d). */
 int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu_ctx** ctx);
 
 /* 1: advance every patch of a level in one launch (batched path, default);
@@ -74,7 +76,7 @@ int amrgpu_regrid(amrgpu_ctx* ctx, int lbase);
 /* Write fort.qNNNN / fort.tNNNN into dir (ASCII form of src/2d/valout.f90:8-397). */
 int amrgpu_valout(amrgpu_ctx* ctx, const char* dir);
 
-/* Total of q(1)*dx*dy over level 1 (src/2d/conck.f:6-73). */
+/* Total of q(1)*dx*dy (3D: *dz) over level 1 (src/2d/conck.f:6-73, src/3d/conck.f). */
 int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
 
 /* Run statistics: out[0..n) = time, cell updates, coarse steps, finest level,
@@ -87,16 +89,22 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
  * and list set-up, device-program compilation. */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 
-/* Hierarchy rows (grid_number, level, ilo, ihi, jlo, jhi) in output order
- * (src/2d/valout.f90 loop order); *n_out receives the row count. */
+/* Hierarchy rows in output order (valout.f90 loop order): (grid_number, level,
+ * ilo, ihi, jlo, jhi) in 2D, (..., klo, khi) appended in 3D, i.e. 2 + 2*num_dim
+ * ints per row; *n_out receives the row count. */
 int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out);
 
-/* Interior cell values of every grid in amrgpu_grids order, [m][j][i] per grid. */
+/* Interior cell values of every grid in amrgpu_grids order, [m][j][i] per grid
+ * in 2D and [m][k][j][i] in 3D. */
 int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out);
 
 /* Gauge samples as rows (gauge number, level, time, q1..qmeqn), grouped by gauge
  * (src/2d/gauges_module.f90:313-500). */
 int amrgpu_gauges(amrgpu_ctx* ctx, double* out, int cap_rows, int* n_out);
+
+/* 2 or 3: the dimension of the context's run (0 for a null context). No
+ * counterpart in the reference, whose 2D and 3D programs are separate builds. */
+int amrgpu_num_dim(amrgpu_ctx* ctx);
 
 /* Release the context and its device memory. */
 int amrgpu_destroy(amrgpu_ctx* ctx);

@@ -1,4 +1,4 @@
-"""ctypes wrapper of the CPU oracle (test infrastructure only; see oracle/amr2d.cpp)."""
+"""ctypes wrapper of the CPU oracle (test infrastructure only; see oracle/amr2d.cpp, oracle/amr3d.cpp)."""
 from __future__ import annotations
 
 import ctypes
@@ -40,6 +40,19 @@ def load() -> ctypes.CDLL:
         lib.oracle2d_values.restype = ctypes.c_long
         lib.oracle2d_values.argtypes = [vp, vp, ctypes.c_long]
         lib.oracle2d_gauges.argtypes = [vp, vp, ctypes.c_int]
+        lib.oracle3d_create.restype = vp
+        lib.oracle3d_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        lib.oracle3d_destroy.argtypes = [vp]
+        lib.oracle3d_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        for n in ("oracle3d_time", "oracle3d_cell_updates", "oracle3d_mass", "oracle3d_mass0"):
+            getattr(lib, n).restype = ctypes.c_double
+            getattr(lib, n).argtypes = [vp]
+        for n in ("oracle3d_lfine", "oracle3d_ncycle"):
+            getattr(lib, n).argtypes = [vp]
+        lib.oracle3d_grids.argtypes = [vp, vp, ctypes.c_int]
+        lib.oracle3d_values.restype = ctypes.c_long
+        lib.oracle3d_values.argtypes = [vp, vp, ctypes.c_long]
+        lib.oracle3d_gauges.argtypes = [vp, vp, ctypes.c_int]
         _lib = lib
     return _lib
 
@@ -94,3 +107,51 @@ class Oracle2D:
             self.close()
         except Exception:
             pass
+
+
+class Oracle3D(Oracle2D):
+    """The 3D restatement (oracle/amr3d.cpp) behind the same interface; grid rows have 8 columns."""
+
+    def __init__(self, rundir: str, outdir: str | None = None, write_output: bool = False, threads: int = 1):
+        self.lib = load()
+        self.h = self.lib.oracle3d_create(rundir.encode(), (outdir or rundir).encode(), int(write_output), threads)
+        if not self.h:
+            raise RuntimeError("oracle3d_create failed for %s" % rundir)
+
+    def run(self, max_cycles: int = 0) -> float:
+        sec = ctypes.c_double()
+        if self.lib.oracle3d_run(self.h, max_cycles, ctypes.byref(sec)) != 0:
+            raise RuntimeError("oracle run failed")
+        return sec.value
+
+    def time(self) -> float:
+        return self.lib.oracle3d_time(self.h)
+
+    def cell_updates(self) -> float:
+        return self.lib.oracle3d_cell_updates(self.h)
+
+    def mass(self) -> float:
+        return self.lib.oracle3d_mass(self.h)
+
+    def grids(self) -> np.ndarray:
+        n = self.lib.oracle3d_grids(self.h, None, 0)
+        a = np.zeros((n, 8), dtype=np.int32)
+        self.lib.oracle3d_grids(self.h, a.ctypes.data, n)
+        return a
+
+    def values(self) -> np.ndarray:
+        n = self.lib.oracle3d_values(self.h, None, 0)
+        a = np.zeros(n, dtype=np.float64)
+        self.lib.oracle3d_values(self.h, a.ctypes.data, n)
+        return a
+
+    def gauges(self, nvar: int) -> np.ndarray:
+        n = self.lib.oracle3d_gauges(self.h, None, 0)
+        a = np.zeros((n, 3 + nvar), dtype=np.float64)
+        self.lib.oracle3d_gauges(self.h, a.ctypes.data, n)
+        return a
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.oracle3d_destroy(self.h)
+            self.h = None

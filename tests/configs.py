@@ -97,3 +97,56 @@ def euler_quadrants(n: int = 100, levels: int = 4, tfinal: float = 0.8, ratio: i
     a.flag2refine = True; a.flag2refine_tol = 0.1; a.regrid_interval = 2; a.regrid_buffer_width = 2
     a.clustering_cutoff = 0.7
     return rd
+
+
+def advection_swirl_regression() -> ClawRunData:
+    """tests/advection_3d_swirl/setrun.py of the reference (gauges 1, 2 pinned)."""
+    rd = ClawRunData(num_dim=3)
+    rd.probdata.add_param("problem", "advection_swirl")
+    c = rd.clawdata
+    c.lower = [0.0, 0.0, 0.0]; c.upper = [1.0, 1.0, 1.0]; c.num_cells = [40, 40, 40]
+    c.num_eqn = 1; c.num_waves = 1; c.num_aux = 3; c.capa_index = 0
+    c.output_style = 1; c.num_output_times = 2; c.tfinal = 0.1; c.output_t0 = True
+    c.dt_variable = True; c.dt_initial = 0.01; c.dt_max = 1e99; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.steps_max = 5000; c.order = 2; c.transverse_waves = 22; c.limiter = ["mc"]
+    c.bc_lower = ["extrap"] * 3; c.bc_upper = ["extrap"] * 3
+    rd.gaugedata.gauges = [[1, 0.55, 0.4, 0.4, 0., 1e9], [2, 0.45, 0.6, 0.4, 0., 1e9]]
+    a = rd.amrdata
+    a.amr_levels_max = 2
+    a.refinement_ratios_x = [2, 2, 2, 2]; a.refinement_ratios_y = [2, 2, 2, 2]
+    a.refinement_ratios_z = [2, 2, 2, 2]; a.refinement_ratios_t = [2, 2, 2, 2]
+    a.aux_type = ["xleft", "yleft", "zleft"]
+    a.flag2refine = True; a.flag2refine_tol = 0.5; a.regrid_interval = 2; a.regrid_buffer_width = 3
+    a.clustering_cutoff = 0.7
+    a.max1d = 32
+    return rd
+
+
+def euler_blast(n: int = 64, levels: int = 3, tfinal: float = 0.5, seed: int = 0, max1d: int = 68) -> ClawRunData:
+    """3D Euler radial blast on [-1,1]^3: rho = 1, p = 5 within r < 0.2 of a centre drawn
+    uniformly from [-0.1,0.1]^3 (numpy default_rng(seed)), p = 1 outside, u = 0; Roe +
+    entropy fix, pressure-difference flagging at 0.2, extrapolation boundaries."""
+    import numpy as np
+    cx, cy, cz = np.random.default_rng(seed).uniform(-0.1, 0.1, 3)
+    rd = ClawRunData(num_dim=3)
+    p = rd.probdata
+    p.add_param("problem", "euler_blast")
+    p.add_param("gamma", 1.4)
+    p.add_param("x0", float(cx)); p.add_param("y0", float(cy)); p.add_param("z0", float(cz))
+    p.add_param("r0", 0.2); p.add_param("pin", 5.0); p.add_param("pout", 1.0)
+    p.add_param("flag_pressure", 1)
+    c = rd.clawdata
+    c.lower = [-1.0, -1.0, -1.0]; c.upper = [1.0, 1.0, 1.0]; c.num_cells = [n, n, n]
+    c.num_eqn = 5; c.num_waves = 3; c.num_aux = 0
+    c.output_style = 1; c.num_output_times = 1; c.tfinal = tfinal; c.output_t0 = False
+    c.dt_variable = True; c.dt_initial = 0.2 / n; c.dt_max = 1e99; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.steps_max = 100000; c.order = 2; c.transverse_waves = 22; c.limiter = ["mc", "mc", "mc"]
+    c.bc_lower = ["extrap"] * 3; c.bc_upper = ["extrap"] * 3
+    a = rd.amrdata
+    a.amr_levels_max = levels
+    r = [2] * max(1, levels - 1)
+    a.refinement_ratios_x = list(r); a.refinement_ratios_y = list(r); a.refinement_ratios_z = list(r); a.refinement_ratios_t = list(r)
+    a.flag2refine = True; a.flag2refine_tol = 0.2; a.regrid_interval = 2; a.regrid_buffer_width = 2
+    a.clustering_cutoff = 0.7
+    a.max1d = max1d
+    return rd

@@ -1,0 +1,91 @@
+"""GPU path versus the CPU oracle on the same inputs (3D Euler).
+
+FP64 results must be bit-identical: the same hierarchy (boxes, grid numbers,
+order), the same cell values, the same gauge samples and the same cell-update
+count. The oracle itself is pinned to the reference's 3D regression gauges in
+test_oracle3d.py.
+"""
+import tempfile
+
+import numpy as np
+import pytest
+
+import configs
+from oracle.pyoracle import Oracle3D
+
+pytestmark = pytest.mark.gpu
+
+
+def _both(rd, batched=True, max_cycles=0, split=None):
+    from amrclaw_b200 import Solver
+    with tempfile.TemporaryDirectory() as d:
+        rd.write(d)
+        o = Oracle3D(d, threads=8)
+        o.run(max_cycles)
+        ref = dict(grids=o.grids(), values=o.values(), gauges=o.gauges(5), time=o.time(), mass=o.mass(),
+                   cells=o.cell_updates())
+        o.close()
+        with Solver(d, batched=batched) as s:
+            assert s.num_dim == 3
+            if split:
+                for _ in range(max_cycles // split):
+                    s.run(split)
+            else:
+                s.run(max_cycles)
+            gpu = dict(grids=s.grids(), values=s.values(), gauges=s.gauges(5), info=s.info(), mass=s.mass())
+    return ref, gpu
+
+
+def _assert_identical(ref, gpu):
+    assert gpu["grids"].shape[1] == 8
+    np.testing.assert_array_equal(gpu["grids"], ref["grids"])
+    assert gpu["values"].shape == ref["values"].shape
+    diff = np.nonzero(gpu["values"] != ref["values"])[0]
+    assert diff.size == 0, "values differ at %d cells, first %s: gpu %r oracle %r" % (
+        diff.size, diff[:3], gpu["values"][diff[:3]], ref["values"][diff[:3]])
+    assert gpu["info"]["time"] == ref["time"]
+    assert gpu["info"]["cell_updates"] == ref["cells"]
+    assert gpu["info"]["num_dim"] == 3.0
+    np.testing.assert_allclose(gpu["mass"], ref["mass"], rtol=1e-13)
+    np.testing.assert_array_equal(gpu["gauges"], ref["gauges"])
+
+
+def _with_gauges(rd):
+    rd.gaugedata.gauges.append([1, 0.05, -0.02, 0.03, 0.0, 1e9])
+    rd.gaugedata.gauges.append([2, 0.31, 0.12, -0.27, 0.0, 1e9])
+    return rd
+
+
+def test_blast_two_levels_many_patches():
+    rd = _with_gauges(configs.euler_blast(n=16, levels=2, tfinal=0.05, max1d=12))
+    ref, gpu = _both(rd)
+    assert (ref["grids"][:, 1] == 2).sum() > 1
+    _assert_identical(ref, gpu)
+    assert len(gpu["gauges"]) > 0
+
+
+def test_blast_three_levels_regrids():
+    rd = _with_gauges(configs.euler_blast(n=16, levels=3, tfinal=0.1, max1d=16))
+    ref, gpu = _both(rd)
+    assert (ref["grids"][:, 1] == 3).any()
+    _assert_identical(ref, gpu)
+
+
+def test_blast_wall_boundaries_reach_the_wall():
+    rd = configs.euler_blast(n=12, levels=2, tfinal=0.6, max1d=16)
+    rd.clawdata.bc_lower = ["wall"] * 3
+    rd.clawdata.bc_upper = ["extrap", "wall", "extrap"]
+    ref, gpu = _both(rd)
+    _assert_identical(ref, gpu)
+
+
+def test_plain_per_patch_path_matches_batched():
+    rd = configs.euler_blast(n=16, levels=2, tfinal=0.05, max1d=12)
+    ref, gpu = _both(rd, batched=False)
+    _assert_identical(ref, gpu)
+
+
+def test_split_run_equals_one_run():
+    rd = configs.euler_blast(n=16, levels=3, tfinal=10.0, max1d=20)
+    ref, gpu = _both(rd, max_cycles=6, split=2)
+    _assert_identical(ref, gpu)
