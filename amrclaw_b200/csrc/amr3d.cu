@@ -887,9 +887,11 @@ class Amr3Gpu : public AmrSolver {
   // advanc.f:4-139 with par_advanc (:166-303) for all patches of the level at once
   double advanc(int lev) {
     HPROF("advanc3");
+    PhaseTimer tph(hprof);
     Plan3& L = plan[lev];
     const double t = node[lgrids[lev][0]].time;
     const double dt = possk[lev];
+    tph.next("adv_launch");
     bound_level(lev, t);
     if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
     if (lev > 1 && !L.qad.empty()) {
@@ -934,7 +936,9 @@ class Amr3Gpu : public AmrSolver {
     flip_level(lev);
     unsigned long long cbits = 0;
     AMR_CUDA(cudaMemcpyAsync(&cbits, d_cfl, sizeof(cbits), cudaMemcpyDeviceToHost, st));
+    tph.next("adv_sync");
     sync_stream();
+    tph.close();
     double cmax;
     std::memcpy(&cmax, &cbits, sizeof(double));
     if (profile) {
@@ -976,6 +980,7 @@ class Amr3Gpu : public AmrSolver {
 
   // update.f:4-192 (upbnd then averaging)
   void update(int lev) {
+    HPROF("update3");
     Plan3& L = plan[lev];
     const double vol = hxposs[lev] * hyposs[lev] * hzposs[lev];
     launch_upbnd3(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, vol, nvar, st);
@@ -1203,6 +1208,8 @@ class Amr3Gpu : public AmrSolver {
   void flglvl(int lcheck, int lbase, std::vector<double>& badpts, I1& i1flags) {
     int idim = iregsz[lbase], jdim = jregsz[lbase], kdim = kregsz[lbase];
     I1 dom1;
+    PhaseTimer tph(hprof);
+    tph.next("flg_domain");
     domprep(i1flags, lbase, idim, jdim, kdim);
     domshrink(i1flags, dom1, idim, jdim, kdim);
     for (int lev = lbase + 1; lev <= lcheck; ++lev) {
@@ -1212,8 +1219,11 @@ class Amr3Gpu : public AmrSolver {
     }
     i1flags = dom1;
     extend_borders(i1flags, iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]);
+    tph.next("flg_spest");
     spest(lcheck, dom1);
+    tph.next("flg_bufnst");
     const int numbad = bufnst(lcheck, dom1);
+    tph.next("flg_colate");
     badpts.clear();
     if (numbad == 0) return;
     const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
@@ -1458,13 +1468,19 @@ class Amr3Gpu : public AmrSolver {
       if (newstl[lcheck + 1] != 0) lfnew = std::max(lcheck + 1, lfnew);
       --lcheck;
     }
+    PhaseTimer tph(hprof);
+    tph.next("rg_newlevels");
     for (int lev = lbase; lev <= p.mxnest; ++lev) for (int m : lgrids[lev]) { node[m].has_cfl = false; node[m].listbc.clear(); }
     for (int l2 = lbase + 1; l2 <= p.mxnest; ++l2) {
       std::vector<int> nl;
+      tph.next("rg_alloc");
       for (int m = newstl[l2]; m != 0; m = node[m].levelptr) { alloc_patch(m); nl.push_back(m); }
       // descriptors: current levels (levels below l2 already replaced), the old grids of l2 and the new ones
+      tph.next("rg_desc");
       sync_descriptors(&nl, 0);
+      tph.next("rg_fill");
       if (newstl[l2] != 0) fill_new_level(l2);
+      tph.next("rg_free");
       int m = lstart[l2];
       while (m != 0) {
         const int mold = m;
@@ -1479,12 +1495,15 @@ class Amr3Gpu : public AmrSolver {
       for (int q = lstart[l2]; q != 0; q = node[q].levelptr) lgrids[l2].push_back(q);
     }
     lfine = lfnew;
+    tph.next("rg_prep_lists");
     for (int lev = lbase; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
     for (int lev = lbase + 1; lev <= p.mxnest; ++lev) arrange(lev);
     make_lists();
     for (int lev = lbase + 1; lev <= lfine; ++lev) make_bndry(lev);
+    tph.next("rg_compile");
     compile_all(lbase);
     sync_stream();
+    tph.close();
     t_regrid += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0c).count();
   }
 

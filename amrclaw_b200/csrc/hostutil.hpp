@@ -34,6 +34,21 @@ struct ScopedTimer {
     a.second += 1;
   }
 };
+// Consecutive phases of one scope: next() closes the running phase and opens another.
+struct PhaseTimer {
+  HostProf& P; const char* name = nullptr; std::chrono::steady_clock::time_point t0;
+  explicit PhaseTimer(HostProf& p) : P(p) {}
+  void close() {
+    if (name && P.on) {
+      auto& a = P.acc[name];
+      a.first += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      a.second += 1;
+    }
+    name = nullptr;
+  }
+  void next(const char* n) { close(); name = n; t0 = std::chrono::steady_clock::now(); }
+  ~PhaseTimer() { close(); }
+};
 #define HPROF(name) ScopedTimer _hp_##__LINE__(hprof, name)  // rinfinity of amr_module.f90 (a default-REAL literal)
 
 // ------------------------------------------------------------------ device pool
@@ -51,6 +66,8 @@ struct Arena {
     fr[0] = n;
   }
   void grow(long long need) {
+    // kernels on any stream may still use the pool: let them finish before it moves
+    AMR_CUDA(cudaDeviceSynchronize());
     long long ncap = std::max(cap * 2, cap + rnd(need) + (1 << 20));
     double* nd = nullptr;
     AMR_CUDA(cudaMalloc(&nd, sizeof(double) * ncap));
