@@ -12,6 +12,7 @@
 // projec.f, shiftset.f, colate.f, smartbis.f, findcut.f, moment.f, nestck.f,
 // grdfit.f, birect.f, gfixup.f, filval.f) with the gradient test on the device.
 #include "kernels3d.cuh"
+#include "flags3d.cuh"
 #include "params.hpp"
 #include "gridindex.hpp"
 #include "workpool.hpp"
@@ -92,16 +93,17 @@ void merge_prog(Prog3& D, const Prog3& S) {
 struct Plan3 {
   Prog3 bound, saveqc;
   std::vector<int> plist;
-  std::vector<long long> sweep0, face0, cell0;
-  long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;
+  std::vector<long long> sweep0, comp0, face0, cell0;
+  long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;  // items: interfaces per direction
   std::vector<Fsv3> fsv;
   std::vector<Fad3> fad;
   std::vector<Qad3Job> qad;
   std::vector<Upbnd3Cell> upc;
   std::vector<Upbnd3Term> upt;
   std::vector<Avg3> avg;
+  long long avg_max = 0;  // cells of the largest averaging rectangle
   DBuf<int> d_plist;
-  DBuf<long long> d_sweep0, d_face0, d_cell0;
+  DBuf<long long> d_sweep0, d_comp0, d_face0, d_cell0;
   DBuf<Fsv3> d_fsv;
   DBuf<Fad3> d_fad;
   DBuf<Qad3Job> d_qad;
@@ -110,16 +112,15 @@ struct Plan3 {
   DBuf<Avg3> d_avg;
   void free_dev() {
     bound.free_dev(); saveqc.free_dev();
-    d_plist.free(); d_sweep0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_fad.free(); d_qad.free();
+    d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_fad.free(); d_qad.free();
     d_upc.free(); d_upt.free(); d_avg.free();
   }
 };
 
-// integer*1 level array with indices (0:is+1, 0:js+1, 0:ks+1)
-struct I1 {
-  std::vector<int8_t> v; int is = 0, js = 0, ks = 0;
-  void init(int a, int b, int c) { is = a; js = b; ks = c; v.assign((size_t)(a + 2) * (b + 2) * (c + 2), 0); }
-  int8_t& operator()(int i, int j, int k) { return v[(size_t)i + (size_t)(is + 2) * ((size_t)j + (size_t)(js + 2) * k)]; }
+// read-only view of a level int8 array (the nesting domain read back for nestck.f)
+struct LvlView {
+  const int8_t* v; LvlDims d;
+  int8_t operator()(int i, int j, int k) const { return v[d.at(i, j, k)]; }
 };
 
 struct Tgt3 { int patch, rect, ni, nj, nk; };
@@ -151,7 +152,12 @@ class Amr3Gpu : public AmrSolver {
   Plan3 plan[12];
   Prog3 newfill;
   DBuf<double> d_stash, d_flux;
-  DBuf<int8_t> fl_out;
+  DBuf<int8_t> lv_a, lv_b, lv_n, lv_t1, lv_t2;   // level flag arrays (flglvl)
+  DBuf<LvlBox> lv_boxes, lv_proj;
+  DBuf<long long> lv_c0;
+  DBuf<int> lv_plist;
+  int8_t* lv_host = nullptr;                       // pinned read-back: flags, then the nesting domain
+  size_t lv_host_cap = 0;
   DBuf<double> d_gauge_out;
   unsigned long long* d_cfl = nullptr;
   double* d_mass = nullptr;
@@ -185,7 +191,10 @@ class Amr3Gpu : public AmrSolver {
     newfill.free_dev();
     pool.destroy(); regs.destroy();
     stg.destroy();
-    d_patches.free(); d_stash.free(); d_flux.free(); fl_out.free(); d_gauge_out.free();
+    d_patches.free(); d_stash.free(); d_flux.free(); d_gauge_out.free();
+    for (DBuf<int8_t>* b : {&lv_a, &lv_b, &lv_n, &lv_t1, &lv_t2}) b->free();
+    lv_boxes.free(); lv_proj.free(); lv_c0.free(); lv_plist.free();
+    if (lv_host) cudaFreeHost(lv_host);
     if (d_cfl) cudaFree(d_cfl);
     if (d_mass) cudaFree(d_mass);
     for (cudaEvent_t e : {ev_a, ev_b, ev_run0, ev_run1}) if (e) cudaEventDestroy(e);
@@ -645,17 +654,24 @@ class Amr3Gpu : public AmrSolver {
     L.plist = lgrids[lev];
     const int np = (int)L.plist.size();
     L.sweep0.assign((size_t)3 * (np + 1), 0);
+    L.comp0.assign((size_t)3 * (np + 1), 0);
     L.face0.assign(np + 1, 0); L.cell0.assign(np + 1, 0);
-    long long slot = 0;
+    long long slot = 0, comp = 0;
     for (int d = 0; d < 3; ++d) {
+      comp = 0;
       for (int k = 0; k < np; ++k) {
         const HPatch3& g = node[L.plist[k]];
         const long long mx = g.nx(), my = g.ny(), mz = g.nz();
+        const long long n1 = d == 0 ? mx : d == 1 ? my : mz;
+        const long long pencils = d == 0 ? (my + 2) * (mz + 2) : d == 1 ? (mx + 2) * (mz + 2) : (mx + 2) * (my + 2);
         L.sweep0[(size_t)d * (np + 1) + k] = slot;
-        slot += d == 0 ? (my + 2) * (mz + 2) * (mx + 1) : d == 1 ? (mx + 2) * (mz + 2) * (my + 1) : (mx + 2) * (my + 2) * (mz + 1);
+        L.comp0[(size_t)d * (np + 1) + k] = comp;
+        slot += pencils * (n1 + 1);
+        comp += pencils * (n1 + 3);
       }
       L.sweep0[(size_t)d * (np + 1) + np] = slot;
-      L.items[d] = L.sweep0[(size_t)d * (np + 1) + np] - L.sweep0[(size_t)d * (np + 1)];
+      L.comp0[(size_t)d * (np + 1) + np] = comp;
+      L.items[d] = comp;
     }
     L.slots = slot;
     for (int k = 0; k < np; ++k) {
@@ -700,14 +716,15 @@ class Amr3Gpu : public AmrSolver {
     }
     L.d_plist.upload(L.plist, st, stg);
     L.d_sweep0.upload(L.sweep0, st, stg);
+    L.d_comp0.upload(L.comp0, st, stg);
     L.d_face0.upload(L.face0, st, stg);
     L.d_cell0.upload(L.cell0, st, stg);
     L.d_fsv.upload(L.fsv, st, stg);
     L.d_fad.upload(L.fad, st, stg);
     L.d_qad.upload(L.qad, st, stg);
     // staging and face-flux buffers sized for the largest level
-    d_stash.ensure(std::max<size_t>(d_stash.n, (size_t)(L.slots * STASH3)));
-    d_flux.ensure(std::max<size_t>(d_flux.n, (size_t)(L.faces * 30)));
+    d_stash.reserve(std::max<size_t>(d_stash.n, (size_t)(L.slots * STASH3)));
+    d_flux.reserve(std::max<size_t>(d_flux.n, (size_t)(L.faces * 30)));
   }
 
   // update.f:4-192 + upbnd.f:4-94 for coarse level lev
@@ -761,6 +778,8 @@ class Amr3Gpu : public AmrSolver {
         }
       }
     }
+    L.avg_max = 0;
+    for (const Avg3& a : L.avg) L.avg_max = std::max<long long>(L.avg_max, (long long)a.ni * a.nj * a.nk);
     L.d_upc.upload(L.upc, st, stg); L.d_upt.upload(L.upt, st, stg); L.d_avg.upload(L.avg, st, stg);
   }
 
@@ -907,19 +926,20 @@ class Amr3Gpu : public AmrSolver {
     a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.dz = hzposs[lev]; a.cflmax = d_cfl;
     if (batched) {
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
-      a.sweep0 = L.d_sweep0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
+      a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
       launch_step3(a, L.items, L.faces, L.cells, st);
       nkernels += 5;
     } else {
       // one patch per launch sequence: per-patch prefix arrays are views of the level's
       const int np = (int)L.plist.size();
-      if ((int)pp_sweep.size() != np) build_plain_views(L);
+      build_plain_views(L);
       for (int k = 0; k < np; ++k) {
         Step3Args b = a;
         b.plist = L.d_plist.d + k; b.np = 1;
-        b.sweep0 = d_pp_sweep.d + (size_t)6 * k; b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
+        b.sweep0 = d_pp_sweep.d + (size_t)12 * k; b.comp0 = d_pp_sweep.d + (size_t)12 * k + 6;
+        b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
         long long it[3];
-        for (int d = 0; d < 3; ++d) it[d] = L.sweep0[(size_t)d * (np + 1) + k + 1] - L.sweep0[(size_t)d * (np + 1) + k];
+        for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
         launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st);
         nkernels += 5;
       }
@@ -957,25 +977,27 @@ class Amr3Gpu : public AmrSolver {
     ++nsteps_launched;
     return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
   }
-  // per-patch sweep prefix views for the plain path: [x0, x1, y0, y1, z0, z1] per patch
+  // one-patch views of the sweep prefixes for the plain path, 12 per patch:
+  // stash slots [x0, x1, y0, y1, z0, z1], then interfaces [x0, x1, y0, y1, z0, z1]
   std::vector<long long> pp_sweep;
   DBuf<long long> d_pp_sweep;
   void build_plain_views(Plan3& L) {
     const int np = (int)L.plist.size();
-    pp_sweep.assign((size_t)6 * np, 0);
+    pp_sweep.assign((size_t)12 * np, 0);
     for (int k = 0; k < np; ++k)
       for (int d = 0; d < 3; ++d) {
-        pp_sweep[(size_t)6 * k + 2 * d] = L.sweep0[(size_t)d * (np + 1) + k];
-        pp_sweep[(size_t)6 * k + 2 * d + 1] = L.sweep0[(size_t)d * (np + 1) + k + 1];
+        pp_sweep[(size_t)12 * k + 2 * d] = L.sweep0[(size_t)d * (np + 1) + k];
+        pp_sweep[(size_t)12 * k + 2 * d + 1] = L.sweep0[(size_t)d * (np + 1) + k + 1];
+        pp_sweep[(size_t)12 * k + 6 + 2 * d] = L.comp0[(size_t)d * (np + 1) + k];
+        pp_sweep[(size_t)12 * k + 6 + 2 * d + 1] = L.comp0[(size_t)d * (np + 1) + k + 1];
       }
     d_pp_sweep.upload(pp_sweep, st, stg);
   }
   // the new values were written to the other buffer: swap store1 / store2 of every patch of the level
   void flip_level(int lev) {
     for (int m : lgrids[lev]) { node[m].cur ^= 1; h_patches[m].cur = node[m].cur; }
-    // descriptors of this level only: a small upload
-    for (int m : lgrids[lev])
-      AMR_CUDA(cudaMemcpyAsync(d_patches.d + m, stg.put(&h_patches[m], sizeof(PatchDev), st), sizeof(PatchDev), cudaMemcpyHostToDevice, st));
+    launch_flip(d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), st);
+    ++nkernels;
   }
 
   // update.f:4-192 (upbnd then averaging)
@@ -984,7 +1006,7 @@ class Amr3Gpu : public AmrSolver {
     Plan3& L = plan[lev];
     const double vol = hxposs[lev] * hyposs[lev] * hzposs[lev];
     launch_upbnd3(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, vol, nvar, st);
-    launch_average3(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), intratx[lev], intraty[lev], intratz[lev], nvar, st);
+    launch_average3(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), L.avg_max, intratx[lev], intraty[lev], intratz[lev], nvar, st);
     nkernels += 2;
   }
 
@@ -1034,117 +1056,50 @@ class Amr3Gpu : public AmrSolver {
     dj.free();
   }
 
-  // ================================================================ regrid (host flag arrays)
-  void extend_borders(I1& f, int is, int js, int ks) {
-    for (int k = 1; k <= ks; ++k) for (int j = 1; j <= js; ++j) { if (f(1, j, k) == 1) f(0, j, k) = 1; if (f(is, j, k) == 1) f(is + 1, j, k) = 1; }
-    for (int k = 1; k <= ks; ++k) for (int i = 1; i <= is; ++i) { if (f(i, 1, k) == 1) f(i, 0, k) = 1; if (f(i, js, k) == 1) f(i, js + 1, k) = 1; }
-    for (int j = 1; j <= js; ++j) for (int i = 1; i <= is; ++i) { if (f(i, j, 1) == 1) f(i, j, 0) = 1; if (f(i, j, ks) == 1) f(i, j, ks + 1) = 1; }
-  }
-  void fill_edges_corners(I1& f, int is, int js, int ks) {
-    for (int k = 1; k <= ks; ++k) {
-      if (f(0, 1, k) + f(1, 0, k) == 2) f(0, 0, k) = 1;
-      if (f(0, js, k) + f(1, js + 1, k) == 2) f(0, js + 1, k) = 1;
-      if (f(is, 0, k) + f(is + 1, 1, k) == 2) f(is + 1, 0, k) = 1;
-      if (f(is, js + 1, k) + f(is + 1, js, k) == 2) f(is + 1, js + 1, k) = 1;
-    }
-    for (int i = 1; i <= is; ++i) {
-      if (f(i, 0, 1) + f(i, 1, 0) == 2) f(i, 0, 0) = 1;
-      if (f(i, js, 0) + f(i, js + 1, 1) == 2) f(i, js + 1, 0) = 1;
-      if (f(i, 0, ks) + f(i, 1, ks + 1) == 2) f(i, 0, ks + 1) = 1;
-      if (f(i, js + 1, ks) + f(i, js, ks + 1) == 2) f(i, js + 1, ks + 1) = 1;
-    }
-    for (int j = 1; j <= js; ++j) {
-      if (f(0, j, 1) + f(1, j, 0) == 2) f(0, j, 0) = 1;
-      if (f(is, j, 0) + f(is + 1, j, 1) == 2) f(is + 1, j, 0) = 1;
-      if (f(0, j, ks) + f(1, j, ks + 1) == 2) f(0, j, ks + 1) = 1;
-      if (f(is + 1, j, ks) + f(is, j, ks + 1) == 2) f(is + 1, j, ks + 1) = 1;
-    }
-    if (f(0, 0, 1) + f(0, 1, 0) + f(1, 0, 0) == 3) f(0, 0, 0) = 1;
-    if (f(is + 1, 0, 1) + f(is + 1, 1, 0) + f(is, 0, 0) == 3) f(is + 1, 0, 0) = 1;
-    if (f(0, js + 1, 1) + f(0, js, 0) + f(1, js + 1, 0) == 3) f(0, js + 1, 0) = 1;
-    if (f(is + 1, js + 1, 1) + f(is + 1, js, 0) + f(is, js + 1, 0) == 3) f(is + 1, js + 1, 0) = 1;
-    if (f(0, 0, ks) + f(0, 1, ks + 1) + f(1, 0, ks + 1) == 3) f(0, 0, ks + 1) = 1;
-    if (f(is + 1, 0, ks) + f(is + 1, 1, ks + 1) + f(is, 0, ks + 1) == 3) f(is + 1, 0, ks + 1) = 1;
-    if (f(0, js + 1, ks) + f(0, js, ks + 1) + f(1, js + 1, ks + 1) == 3) f(0, js + 1, ks + 1) = 1;
-    if (f(is + 1, js + 1, ks) + f(is + 1, js, ks + 1) + f(is, js + 1, ks + 1) == 3) f(is + 1, js + 1, ks + 1) = 1;
-  }
-  // domprep.f
-  void domprep(I1& f, int lbase, int ib, int jb, int kb) {
-    f.init(ib, jb, kb);
+  // ================================================================ regrid: level flag arrays on the device
+  // flglvl.f:4-85 with domprep.f, domshrink.f, domup.f, domcopy.f, spest.f (+ flag2refine.f,
+  // setflags.f), bufnst.f (+ projec.f, shiftset.f) and colate.f. The arrays live in device
+  // memory; one read-back returns the flags (for the ordered point list) and the nesting
+  // domain (for nestck.f). Returns the points (i-.5, j-.5, k-.5) in (k, j, i) order.
+  void flglvl(int lcheck, int lbase, std::vector<double>& badpts, LvlView& dom) {
+    PhaseTimer tph(hprof);
+    tph.next("flg_device");
+    const LvlDims d0{iregsz[lbase], jregsz[lbase], kregsz[lbase]};
+    const LvlDims dl{iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]};
+    const size_t need = (size_t)dl.size();
+    for (DBuf<int8_t>* b : {&lv_a, &lv_b, &lv_n, &lv_t1, &lv_t2}) b->reserve(need);
+    std::vector<LvlBox> boxes;
     for (int m = lstart[lbase]; m != 0; m = node[m].levelptr) {
       const HPatch3& g = node[m];
-      for (int k = g.klo + 1; k <= g.khi + 1; ++k) for (int j = g.jlo + 1; j <= g.jhi + 1; ++j)
-        std::memset(&f(g.ilo + 1, j, k), 1, (size_t)g.nx());
+      boxes.push_back(LvlBox{g.ilo + 1, g.ihi + 1, g.jlo + 1, g.jhi + 1, g.klo + 1, g.khi + 1});
     }
-    extend_borders(f, ib, jb, kb);
-    fill_edges_corners(f, ib, jb, kb);
-  }
-  // domshrink.f (27-cell erosion; planes processed on the host threads)
-  void domshrink(I1& in, I1& out, int id, int jd, int kd) {
-    if (out.is != id || out.js != jd || out.ks != kd) out.init(id, jd, kd);
-    pool_host.run(kd, [&](int kk) {
-      const int k = kk + 1;
-      for (int j = 1; j <= jd; ++j)
-        for (int i = 1; i <= id; ++i) {
-          bool ok = true;
-          for (int c = -1; c <= 1 && ok; ++c)
-            for (int b = -1; b <= 1 && ok; ++b) {
-              const int8_t* row = &in(i - 1, j + b, k + c);
-              if (row[0] <= 0 || row[1] <= 0 || row[2] <= 0) ok = false;
-            }
-          out(i, j, k) = ok ? in(i, j, k) : 0;
-        }
-    });
-    extend_borders(out, id, jd, kd);
-  }
-  // domup.f
-  void domup(I1& fine, I1& crse, int ib, int jb, int kb, int is, int js, int ks, int lev) {
-    fine.init(is, js, ks);
-    const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
-    for (int k = 1; k <= kb; ++k) for (int j = 1; j <= jb; ++j) for (int i = 1; i <= ib; ++i) {
-      const int8_t v = crse(i, j, k);
-      if (v == 0) continue;
-      for (int mk = 1; mk <= rz; ++mk) for (int mj = 1; mj <= ry; ++mj) for (int mi = 1; mi <= rx; ++mi)
-        fine((i - 1) * rx + mi, (j - 1) * ry + mj, (k - 1) * rz + mk) = v;
+    lv_boxes.upload(boxes, st, stg);
+    launch_domprep(lv_a.d, d0, lv_boxes.d, (int)boxes.size(), st);
+    launch_domshrink(lv_a.d, lv_b.d, d0, st);
+    LvlDims dc = d0;
+    for (int lev = lbase + 1; lev <= lcheck; ++lev) {
+      const LvlDims df{dc.is * intratx[lev - 1], dc.js * intraty[lev - 1], dc.ks * intratz[lev - 1]};
+      launch_domup(lv_b.d, dc, lv_a.d, df, intratx[lev - 1], intraty[lev - 1], intratz[lev - 1], st);
+      launch_domshrink(lv_a.d, lv_b.d, df, st);
+      dc = df;
     }
-    extend_borders(fine, is, js, ks);
-    fill_edges_corners(fine, is, js, ks);
-  }
-
-  // spest.f + flag2refine.f (device) + setflags.f (host add)
-  void spest(int lcheck, I1& flags) {
-    const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
-    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) std::memset(&flags(1, j, k), 0, (size_t)isize);
-    if (!p.flag_gradient) return;
-    const std::vector<int>& G = lgrids[lcheck];
-    const double t = node[G[0]].time;
-    bound_level(lcheck, t);
-    std::vector<long long> c0(G.size() + 1, 0);
-    for (size_t k = 0; k < G.size(); ++k) c0[k + 1] = c0[k] + (long long)node[G[k]].nx() * node[G[k]].ny() * node[G[k]].nz();
-    fl_out.ensure(std::max<long long>(c0.back(), 1));
-    DBuf<long long> dc; dc.upload(c0, st, stg);
-    DBuf<int> dp; dp.upload(G, st, stg);
-    launch_flags3(pool.d, d_patches.d, dp.d, dc.d, (int)G.size(), flag_pressure, sp.gamma1, p.tolsp, nvar, fl_out.d, c0.back(), st);
-    std::vector<int8_t> hf(c0.back());
-    if (c0.back()) AMR_CUDA(cudaMemcpyAsync(hf.data(), fl_out.d, c0.back(), cudaMemcpyDeviceToHost, st));
-    sync_stream();
-    dc.free(); dp.free();
-    for (size_t n = 0; n < G.size(); ++n) {
-      const HPatch3& g = node[G[n]];
-      const int8_t* src = hf.data() + c0[n];
-      for (int k = 0; k < g.nz(); ++k)
-        for (int j = 0; j < g.ny(); ++j) {
-          int8_t* row = &flags(g.ilo + 1, g.jlo + 1 + j, g.klo + 1 + k);
-          const int8_t* s = src + ((size_t)k * g.ny() + j) * g.nx();
-          for (int i = 0; i < g.nx(); ++i) row[i] = (int8_t)(row[i] + s[i]);
-        }
+    // domcopy.f: the nesting domain keeps the shrunk array (its ring already extended); the
+    // shrunk array itself becomes the flag array
+    AMR_CUDA(cudaMemcpyAsync(lv_n.d, lv_b.d, need, cudaMemcpyDeviceToDevice, st));
+    launch_zero_interior(lv_b.d, dl, st);
+    if (p.flag_gradient) {
+      const std::vector<int>& G = lgrids[lcheck];
+      bound_level(lcheck, node[G[0]].time);
+      std::vector<long long> c0(G.size() + 1, 0);
+      for (size_t k = 0; k < G.size(); ++k) c0[k + 1] = c0[k] + (long long)node[G[k]].nx() * node[G[k]].ny() * node[G[k]].nz();
+      lv_c0.upload(c0, st, stg);
+      lv_plist.upload(G, st, stg);
+      launch_flag_cells3(pool.d, d_patches.d, lv_plist.d, lv_c0.d, (int)G.size(), c0.back(), flag_pressure, sp.gamma1, p.tolsp, nvar,
+                         lv_b.d, dl, st);
     }
-  }
-
-  // bufnst.f + projec.f + shiftset.f; returns the number of flagged cells
-  int bufnst(int lcheck, I1& f) {
-    const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
+    std::vector<LvlBox> proj;
     if (lcheck + 2 <= p.mxnest) {
+      // projec.f: level lcheck+2's new grids, with one more cell on each side when ibuff = 0
       const int lrx = intratx[lcheck] * intratx[lcheck + 1], lry = intraty[lcheck] * intraty[lcheck + 1], lrz = intratz[lcheck] * intratz[lcheck + 1];
       for (int mk = newstl[lcheck + 2]; mk != 0; mk = node[mk].levelptr) {
         const HPatch3& c = node[mk];
@@ -1158,80 +1113,42 @@ class Amr3Gpu : public AmrSolver {
           if (jend * lry == c.jhi + 1) jend = jend + 1;
           if (kend * lrz == c.khi + 1) kend = kend + 1;
         }
-        for (int k = kst + 1; k <= kend + 1; ++k) for (int j = jst + 1; j <= jend + 1; ++j) for (int i = ist + 1; i <= iend + 1; ++i)
-          if (f(i, j, k) == 0) f(i, j, k) = 3;
+        // kept inside the array (0:is+1, ...); the ring is cleared right after
+        proj.push_back(LvlBox{std::max(ist + 1, 0), std::min(iend + 1, dl.is + 1), std::max(jst + 1, 0), std::min(jend + 1, dl.js + 1),
+                              std::max(kst + 1, 0), std::min(kend + 1, dl.ks + 1)});
       }
     }
-    for (int k = 0; k <= ksize + 1; ++k) for (int j = 0; j <= jsize + 1; ++j) { f(0, j, k) = 0; f(isize + 1, j, k) = 0; }
-    for (int k = 0; k <= ksize + 1; ++k) for (int i = 0; i <= isize + 1; ++i) { f(i, 0, k) = 0; f(i, jsize + 1, k) = 0; }
-    for (int j = 0; j <= jsize + 1; ++j) for (int i = 0; i <= isize + 1; ++i) { f(i, j, 0) = 0; f(i, j, ksize + 1) = 0; }
-    // shiftset.f: every positive flag, visited in (k, j, i) order, stamps its value on the
-    // (2*ibuff+1)^3 box around it, so a cell ends with the value of the lexicographically last
-    // (k, j, i) source within ibuff of it in every direction. Three separable passes find it:
-    // the last source along i, then the last j-row holding one, then the last k-plane.
-    const int b = p.ibuff;
-    I1 f2, t1, t2;
-    f2.init(isize, jsize, ksize); t1.init(isize, jsize, ksize); t2.init(isize, jsize, ksize);
-    pool_host.run(ksize, [&](int kk0) {
-      const int k = kk0 + 1;
-      for (int j = 1; j <= jsize; ++j)
-        for (int i = 0; i <= isize + 1; ++i) {
-          int8_t v = 0;
-          for (int s = std::min(i + b, isize); s >= std::max(i - b, 1); --s)
-            if (f(s, j, k) > 0) { v = f(s, j, k); break; }
-          t1(i, j, k) = v;
-        }
-      for (int jj = 0; jj <= jsize + 1; ++jj)
-        for (int i = 0; i <= isize + 1; ++i) {
-          int8_t v = 0;
-          for (int j = std::min(jj + b, jsize); j >= std::max(jj - b, 1); --j)
-            if (t1(i, j, k) > 0) { v = t1(i, j, k); break; }
-          t2(i, jj, k) = v;
-        }
-    });
-    pool_host.run(ksize + 2, [&](int kk) {
-      for (int jj = 0; jj <= jsize + 1; ++jj)
-        for (int ii = 0; ii <= isize + 1; ++ii) {
-          int8_t v = 0;
-          for (int k = std::min(kk + b, ksize); k >= std::max(kk - b, 1); --k)
-            if (t2(ii, jj, k) > 0) { v = t2(ii, jj, k); break; }
-          f2(ii, jj, kk) = v;
-        }
-    });
-    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) for (int i = 1; i <= isize; ++i) f(i, j, k) = (int8_t)(f(i, j, k) + f2(i, j, k));
-    int numbad = 0;
-    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) for (int i = 1; i <= isize; ++i) if (f(i, j, k) != 0) ++numbad;
-    return numbad;
-  }
-
-  // flglvl.f + colate.f: flagged points (i-.5, j-.5, k-.5) and the nesting domain of level lcheck
-  void flglvl(int lcheck, int lbase, std::vector<double>& badpts, I1& i1flags) {
-    int idim = iregsz[lbase], jdim = jregsz[lbase], kdim = kregsz[lbase];
-    I1 dom1;
-    PhaseTimer tph(hprof);
-    tph.next("flg_domain");
-    domprep(i1flags, lbase, idim, jdim, kdim);
-    domshrink(i1flags, dom1, idim, jdim, kdim);
-    for (int lev = lbase + 1; lev <= lcheck; ++lev) {
-      domup(i1flags, dom1, idim, jdim, kdim, intratx[lev - 1] * idim, intraty[lev - 1] * jdim, intratz[lev - 1] * kdim, lev - 1);
-      idim *= intratx[lev - 1]; jdim *= intraty[lev - 1]; kdim *= intratz[lev - 1];
-      domshrink(i1flags, dom1, idim, jdim, kdim);
+    lv_proj.upload(proj, st, stg);
+    launch_bufnst3(lv_b.d, dl, lv_proj.d, (int)proj.size(), p.ibuff, lv_t1.d, lv_t2.d, st);
+    launch_colate3(lv_b.d, lv_n.d, dl, st);
+    nkernels += 20;
+    if (lv_host_cap < 2 * need) {
+      if (lv_host) AMR_CUDA(cudaFreeHost(lv_host));
+      lv_host_cap = 2 * need;
+      AMR_CUDA(cudaMallocHost((void**)&lv_host, lv_host_cap));
     }
-    i1flags = dom1;
-    extend_borders(i1flags, iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]);
-    tph.next("flg_spest");
-    spest(lcheck, dom1);
-    tph.next("flg_bufnst");
-    const int numbad = bufnst(lcheck, dom1);
-    tph.next("flg_colate");
+    AMR_CUDA(cudaMemcpyAsync(lv_host, lv_b.d, need, cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaMemcpyAsync(lv_host + need, lv_n.d, need, cudaMemcpyDeviceToHost, st));
+    tph.next("flg_sync");
+    sync_stream();
+    tph.next("flg_points");
+    dom = LvlView{lv_host + need, dl};
     badpts.clear();
-    if (numbad == 0) return;
-    const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
-    for (int k = 1; k <= ksize; ++k) for (int j = 1; j <= jsize; ++j) for (int i = 1; i <= isize; ++i) {
-      const int8_t v = std::min(dom1(i, j, k), i1flags(i, j, k));
-      dom1(i, j, k) = v;
-      if (v != 0) { badpts.push_back((double)i - .5); badpts.push_back((double)j - .5); badpts.push_back((double)k - .5); }
-    }
+    const int8_t* F = lv_host;
+    for (int k = 1; k <= dl.ks; ++k)
+      for (int j = 1; j <= dl.js; ++j) {
+        const int8_t* row = F + dl.at(0, j, k);
+        int i = 1;
+        while (i <= dl.is) {
+          if (i + 8 <= dl.is + 1) {
+            uint64_t w;
+            std::memcpy(&w, row + i, 8);
+            if (w == 0) { i += 8; continue; }
+          }
+          if (row[i] != 0) { badpts.push_back((double)i - .5); badpts.push_back((double)j - .5); badpts.push_back((double)k - .5); }
+          ++i;
+        }
+      }
   }
 
   // moment.f
@@ -1346,7 +1263,7 @@ class Amr3Gpu : public AmrSolver {
     }
   }
   // nestck.f
-  bool nestck(int mnew, int lbase, std::vector<double>& bp, int ibase, int npts, std::vector<int>& numptc, int icl, int& nclust, I1& dom) {
+  bool nestck(int mnew, int lbase, std::vector<double>& bp, int ibase, int npts, std::vector<int>& numptc, int icl, int& nclust, const LvlView& dom) {
     if (lbase == 1) return true;
     const HPatch3& n = node[mnew];
     const int lev = n.level;
@@ -1381,7 +1298,7 @@ class Amr3Gpu : public AmrSolver {
   // grdfit.f
   void grdfit(int lbase, int lcheck, double t) {
     std::vector<double> bp;
-    I1 i1flags;
+    LvlView i1flags{nullptr, LvlDims{0, 0, 0}};
     {
       HPROF("flglvl3");
       flglvl(lcheck, lbase, bp, i1flags);

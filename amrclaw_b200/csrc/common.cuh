@@ -49,4 +49,7 @@ struct SrcMode {
   double alphai[MAXLV + 2], alphac[MAXLV + 2];
 };
 
+// cur ^= 1 for every patch in plist (the step wrote the other buffer); kernels2d.cu.
+void launch_flip(PatchDev* patches, const int* plist, int np, cudaStream_t s);
+
 }  // namespace amrb

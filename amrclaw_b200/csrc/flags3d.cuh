@@ -1,0 +1,38 @@
+// Level-wide int8 flag arrays of 3D regridding on the device (flglvl.f and the
+// routines it drives). An array of level L covers (0:is+1, 0:js+1, 0:ks+1) with is,
+// js, ks the level's cell counts (iregsz, jregsz, kregsz), i fastest, the ring of one
+// cell on every side as in the reference's integer*1 arrays.
+#pragma once
+#include "common.cuh"
+
+namespace amrb {
+
+struct LvlDims {
+  int is, js, ks;
+  __host__ __device__ long long size() const { return (long long)(is + 2) * (js + 2) * (ks + 2); }
+  __host__ __device__ long long at(int i, int j, int k) const { return i + (long long)(is + 2) * (j + (long long)(js + 2) * k); }
+};
+
+// One box (array coordinates, inclusive) of domprep.f (value 1) or projec.f (3 where 0).
+struct LvlBox { int i0, i1, j0, j1, k0, k1; };
+
+// domprep.f:4-169: zero, the boxes set to 1, then the border ring.
+void launch_domprep(int8_t* a, LvlDims d, const LvlBox* boxes, int nbox, cudaStream_t s);
+// domshrink.f:4-93: 27-cell erosion of `in` into a fresh `out`, then extend_borders.
+void launch_domshrink(const int8_t* in, int8_t* out, LvlDims d, cudaStream_t s);
+// domup.f:4-185: a fresh fine array from the coarse one, then the border ring.
+void launch_domup(const int8_t* crse, LvlDims cd, int8_t* fine, LvlDims fd, int rx, int ry, int rz, cudaStream_t s);
+// spest.f: the interior of `f` set to 0 (the ring keeps its values).
+void launch_zero_interior(int8_t* f, LvlDims d, cudaStream_t s);
+// spest.f + flag2refine.f + setflags.f: BADPT (2) or GOODPT (0) into the level array for
+// every interior cell of the patches in plist (patch cells at [cell0[p], cell0[p+1])).
+void launch_flag_cells3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
+                        long long ncells, int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* f, LvlDims d,
+                        cudaStream_t s);
+// bufnst.f + projec.f + shiftset.f: project the boxes (3 where 0), zero the ring, then
+// add the ibuff-dilated flags (t1, t2: scratch arrays of the same dims).
+void launch_bufnst3(int8_t* f, LvlDims d, const LvlBox* proj, int nproj, int ibuff, int8_t* t1, int8_t* t2, cudaStream_t s);
+// colate.f:4-78: f = min(f, dom) over the interior.
+void launch_colate3(int8_t* f, const int8_t* dom, LvlDims d, cudaStream_t s);
+
+}  // namespace amrb

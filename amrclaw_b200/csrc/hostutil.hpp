@@ -143,7 +143,7 @@ template <class T> struct DBuf {
     n = cnt;
     if (n > cap) {
       if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(n, 16) * 3 / 2;
+      cap = std::max<size_t>(n, 16) * 2;
       AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
     }
     if (n) AMR_CUDA(cudaMemcpyAsync(d, stg.put(h, sizeof(T) * n, s), sizeof(T) * n, cudaMemcpyHostToDevice, s));
@@ -152,6 +152,16 @@ template <class T> struct DBuf {
     if (m > cap) {
       if (d) AMR_CUDA(cudaFree(d));
       cap = std::max<size_t>(m, 16) * 3 / 2;
+      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
+    }
+    n = m;
+  }
+  // ensure() for large scratch that changes size with the hierarchy: grows to twice the
+  // request, so a slowly growing level does not reallocate (and synchronise) every regrid
+  void reserve(size_t m) {
+    if (m > cap) {
+      if (d) AMR_CUDA(cudaFree(d));
+      cap = std::max<size_t>(m, 16) * 2;
       AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
     }
     n = m;

@@ -131,7 +131,6 @@ void launch_flags2(const double* pool, const PatchDev* patches, const int* plist
                    int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s);
 void launch_gauges2(const double* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
                     double* out, cudaStream_t s);
-void launch_flip(PatchDev* patches, const int* plist, int np, cudaStream_t s);
 void launch_zero_tiny(double* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s);
 void launch_mass2(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s);
 void launch_gather_interior2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff,

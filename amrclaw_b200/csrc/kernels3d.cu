@@ -17,8 +17,8 @@
 //   fill3 / bc3         ghost-fill programs (intfil.f, filpatch.f, filval.f, cstore.f)
 //                       and bc3amr.f90 extrapolation / wall boundaries.
 //   upbnd3 / average3   level sync (upbnd.f, update.f).
-//   flags3, gauges3, mass3, gather3: flagging (spest.f + flag2refine.f), gauge
-//                       sampling (gauges_module.f90:302-460), conck.f, output gather.
+//   gauges3, mass3, gather3: gauge sampling (gauges_module.f90:302-460), conck.f,
+//                       output gather. (Flagging kernels: flags3d.cu.)
 #include "kernels3d.cuh"
 #include <algorithm>
 
@@ -55,279 +55,283 @@ __device__ __forceinline__ double philim3(int meth, double r) {
 }
 
 // ------------------------------------------------------------------- sweeps
+// One thread per interface of a pencil. A tile of SW_T consecutive interfaces (of the
+// level's pencils of one direction, pencils of n1+3 interfaces 0..n1+2 each) makes
+// its Riemann solves once and shares the waves in shared memory; tiles overlap by
+// three interfaces so that every cell's two interfaces (c and c+1) and their
+// neighbours (for the limiters) fall in the tile that owns the cell.
+//   phase A  rpn3 at the thread's interface (waves to shared memory)
+//   phase B1 limiter and second-order correction of interface e; faddm/faddp of e;
+//            transverse terms of the apdq side (flux3.f: to cell i = e), stored
+//   phase B2 transverse terms of the amdq side (to cell i-1 = e-1), added to what B1
+//            stored for that cell, term by term in flux3.f's statement order
+constexpr int SW_T = 128;
+constexpr int SW_OWN = SW_T - 3;
+
+// (a - 3*b) (m4 = 2) or a: the doubly transverse inputs of flux3.f:429-507
+__device__ __forceinline__ void dt_input(int m4, double sgn3, const double* a, const double* b, double* o) {
+#pragma unroll
+  for (int m = 0; m < 5; ++m) o[m] = (m4 == 2) ? a[m] + sgn3 * b[m] : a[m];
+}
+
 template <int DIR>
-__global__ void __launch_bounds__(128) sweep3_kernel(Step3Args A) {
+__global__ void __launch_bounds__(SW_T, 3) sweep3_kernel(Step3Args A) {
+  __shared__ double sW[15][SW_T];
+  const long long* c0 = A.comp0 + (long long)(DIR - 1) * (A.np + 1);
   const long long* s0 = A.sweep0 + (long long)(DIR - 1) * (A.np + 1);
-  const long long first = s0[0], last = s0[A.np];
+  const long long first = c0[0], last = c0[A.np];
+  const int l = threadIdx.x;
+  const long long g = first + (long long)blockIdx.x * SW_OWN - 1 + l;
+  const bool valid = g >= first && g < last;
   const Step3Params sp = A.sp;
-  double cfl = 0.0;
-  for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < last; t += (long long)gridDim.x * blockDim.x) {
-    const int pi = find_patch(s0, A.np, t);
+  const double dn = DIR == 1 ? A.dx : DIR == 2 ? A.dy : A.dz;
+  const double dtdx = A.dt / dn;
+  // transverse steps of flux3's dtdy / dtdz arguments for this sweep (step3.f:192, 300, 416)
+  const double dtdy = DIR == 1 ? A.dt / A.dy : DIR == 2 ? A.dt / A.dz : A.dt / A.dx;
+  const double dtdz = DIR == 1 ? A.dt / A.dz : DIR == 2 ? A.dt / A.dx : A.dt / A.dy;
+  int e = -1, n1 = 0;
+  long long slot = 0;  // stash slot of pencil cell e (meaningful for e in 1..n1+1)
+  Roe3D R;
+  double W[3][5], S[3], AM[5], AP[5];
+  if (valid) {
+    const int pi = find_patch(c0, A.np, g);
     const PatchDev& P = A.patches[A.plist[pi]];
     const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
-    const int n1 = DIR == 1 ? mx : DIR == 2 ? my : mz;
+    n1 = DIR == 1 ? mx : DIR == 2 ? my : mz;
     const int n2 = DIR == 1 ? my : mx;
-    const long long loc = t - s0[pi];
-    const int c = (int)(loc % (n1 + 1)) + 1;
-    const long long pen = loc / (n1 + 1);
+    const long long loc = g - c0[pi];
+    e = (int)(loc % (n1 + 3));
+    const long long pen = loc / (n1 + 3);
     const int a = (int)(pen % (n2 + 2)), b = (int)(pen / (n2 + 2));
+    slot = s0[pi] + pen * (n1 + 1) + (e - 1);
     const long long mi = P.mitot, mj = P.mjtot;
-    long long base, step;  // enlarged-array index of pencil cell e is base + e*step
+    long long base, step;  // enlarged-array index of pencil cell x is base + x*step (cell 0: enlarged index 1)
     if (DIR == 1) { base = ((long long)(b - 1 + NG3) * mj + (a - 1 + NG3)) * mi + (NG3 - 1); step = 1; }
     else if (DIR == 2) { base = ((long long)(b - 1 + NG3) * mj + (NG3 - 1)) * mi + (a - 1 + NG3); step = mi; }
     else { base = ((long long)(NG3 - 1) * mj + (b - 1 + NG3)) * mi + (a - 1 + NG3); step = mi * mj; }
     const long long plane = mi * mj * P.mktot;
     const double* q = A.pool + P.q[P.cur];
-    const double dn = DIR == 1 ? A.dx : DIR == 2 ? A.dy : A.dz;
-    const double dtdx = A.dt / dn;
-    // transverse steps of flux3's dtdy / dtdz arguments for this sweep (step3.f:192, 300, 416)
-    const double dtdy = DIR == 1 ? A.dt / A.dy : DIR == 2 ? A.dt / A.dz : A.dt / A.dx;
-    const double dtdz = DIR == 1 ? A.dt / A.dz : DIR == 2 ? A.dt / A.dx : A.dt / A.dy;
-    const bool hasB = (c + 1 <= n1 + 1);
-    // cells c-2 .. c+2 (index 0..4), 1-based components
-    double Q[5][6];
+    double QL[6], QR[6];
+    const long long atl = base + (long long)(e - 1) * step, atr = atl + step;
 #pragma unroll
-    for (int x = 0; x < 5; ++x) {
-      const int e = c - 2 + x;
-      if (e > n1 + 2) { for (int m = 0; m < 6; ++m) Q[x][m] = 1.0; continue; }
-      const long long at = base + (long long)e * step;
+    for (int m = 1; m <= 5; ++m) { QL[m] = q[(m - 1) * plane + atl]; QR[m] = q[(m - 1) * plane + atr]; }
+    QL[0] = QR[0] = 0.0;
+    R = roe3d(sp.gamma1, QL, QR);
+    euler3d_rpn_roe(sp.gamma, sp.gamma1, sp.efix != 0, DIR, QL, QR, R, W, S, AM, AP);
 #pragma unroll
-      for (int m = 1; m <= 5; ++m) Q[x][m] = q[(m - 1) * plane + at];
-      Q[x][0] = 0.0;
-    }
-    // Riemann solves at interfaces c-1 .. c+2 (interface e sits between cells e-1 and e)
-    double Wc[3][5], Sc[3], AMc[5], APc[5];
-    double Wn[3][5], Sn[3], AMn[5], APn[5];
-    double dl_c[3], dr_c[3], dr_n[3];  // dot(W_{c-1},W_c), dot(W_c,W_{c+1}), dot(W_{c+1},W_{c+2})
-    {
-      double Wp[3][5], Sp[3], t1[5], t2[5];
-      euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[0], Q[1], Wp, Sp, t1, t2);
-      euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[1], Q[2], Wc, Sc, AMc, APc);
+    for (int k = 0; k < 3; ++k)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        double d = 0.0;
+      for (int m = 0; m < 5; ++m) sW[k * 5 + m][l] = W[k][m];
+  }
+  __syncthreads();
+  // interfaces 1..n1+1 carry fluxes; the tile edges only serve their neighbours
+  const bool live = valid && e >= 1 && e <= n1 + 1 && l >= 1 && l <= SW_T - 2;
+  const bool owned = live && l <= SW_T - 3;
+  double cfl = 0.0;
+  double CQ[5];
 #pragma unroll
-        for (int m = 0; m < 5; ++m) d = d + Wp[k][m] * Wc[k][m];
-        dl_c[k] = d;
-      }
-    }
-    euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[2], Q[3], Wn, Sn, AMn, APn);
+  for (int m = 0; m < 5; ++m) CQ[m] = 0.0;
+  double* st = A.stash + slot;
+  const long long ss = A.stash_stride;
+  const double c6 = 1.0 / 6.0;
+  const int m3 = sp.m3, m4 = sp.m4;
+  if (live) {
+    // Courant number of interface e (flux3.f:237-246)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      double d = 0.0;
-#pragma unroll
-      for (int m = 0; m < 5; ++m) d = d + Wc[k][m] * Wn[k][m];
-      dr_c[k] = d;
-    }
-    if (hasB) {
-      double Wq[3][5], Sq[3], t1[5], t2[5];
-      euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, DIR, Q[3], Q[4], Wq, Sq, t1, t2);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        double d = 0.0;
-#pragma unroll
-        for (int m = 0; m < 5; ++m) d = d + Wn[k][m] * Wq[k][m];
-        dr_n[k] = d;
-      }
-    }
-    // Courant number of interface c (flux3.f:237-246)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cfl = dmax(cfl, dmax(dtdx * Sc[k], -dtdx * Sc[k]));
-    // limiter (limiter.f) and second-order corrections of interfaces c and c+1
-    double CQc[5], CQn[5];
-    const double dtdxave = 0.5 * (dtdx + dtdx);
-#pragma unroll
-    for (int m = 0; m < 5; ++m) { CQc[m] = 0.0; CQn[m] = 0.0; }
+    for (int k = 0; k < 3; ++k) cfl = dmax(cfl, dmax(dtdx * S[k], -dtdx * S[k]));
     if (sp.order != 1) {
+      // limiter.f: r from the unlimited neighbour waves, upwind side by the speed's sign
+      const double dtdxave = 0.5 * (dtdx + dtdx);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         if (sp.mthlim[k] == 0) continue;
-        double wn = 0.0;
+        double dl = 0.0, dr = 0.0, wn = 0.0;
 #pragma unroll
-        for (int m = 0; m < 5; ++m) wn = wn + Wc[k][m] * Wc[k][m];
+        for (int m = 0; m < 5; ++m) dl = dl + sW[k * 5 + m][l - 1] * W[k][m];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) dr = dr + W[k][m] * sW[k * 5 + m][l + 1];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) wn = wn + W[k][m] * W[k][m];
         if (wn != 0.0) {
-          const double r = (Sc[k] > 0.0) ? dl_c[k] / wn : dr_c[k] / wn;
+          const double r = (S[k] > 0.0) ? dl / wn : dr / wn;
           const double phi = philim3(sp.mthlim[k], r);
 #pragma unroll
-          for (int m = 0; m < 5; ++m) Wc[k][m] = phi * Wc[k][m];
+          for (int m = 0; m < 5; ++m) W[k][m] = phi * W[k][m];
         }
-        if (hasB) {
-          double wn2 = 0.0;
+      }
 #pragma unroll
-          for (int m = 0; m < 5; ++m) wn2 = wn2 + Wn[k][m] * Wn[k][m];
-          if (wn2 != 0.0) {
-            const double r = (Sn[k] > 0.0) ? dr_c[k] / wn2 : dr_n[k] / wn2;
-            const double phi = philim3(sp.mthlim[k], r);
+      for (int m = 0; m < 5; ++m) {
+        double x = 0.0;
 #pragma unroll
-            for (int m = 0; m < 5; ++m) Wn[k][m] = phi * Wn[k][m];
+        for (int k = 0; k < 3; ++k) x = x + 0.5 * fabs(S[k]) * (1.0 - fabs(S[k]) * dtdxave) * W[k][m];
+        CQ[m] = x;
+      }
+    }
+    if (owned) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        double fm = 0.0 + AM[m], fp = 0.0 - AP[m];
+        if (sp.order != 1) { fm = fm + CQ[m]; fp = fp + CQ[m]; }
+        st[(long long)m * ss] = fm;
+        st[(long long)(5 + m) * ss] = fp;
+      }
+      if (e <= n1) {
+        if (m3 <= 0) {
+          for (int x = 10; x < STASH3; ++x) st[(long long)x * ss] = 0.0;
+        } else {
+          // apdq side of interface e: the terms of cell e (flux3.f:429-505, 552-628 with i = e)
+          double bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
+          euler3d_trans(R, DIR, 2, AP, bm, bp);
+          euler3d_trans(R, DIR, 3, AP, cm, cp);
+          if (m3 == 2) { euler3d_trans(R, DIR, 2, CQ, bmq, bpq); euler3d_trans(R, DIR, 3, CQ, cmq, cpq); }
+          else {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = 0.0;
+          }
+          // gadd: (side, offset d) at element 10 + ((side-1)*3 + d+1)*5 + m
+          {
+            double P1[5], P2[5], M1[5], M2[5];
+            if (m4 > 0) {
+              double t[5];
+              dt_input(m4, -3.0, cp, cpq, t);
+              euler3d_trans(R, DIR, 2, t, P1, P2);
+              dt_input(m4, -3.0, cm, cmq, t);
+              euler3d_trans(R, DIR, 2, t, M1, M2);
+            }
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+              double g01 = 0.0 - 0.5 * dtdx * bm[m], g11 = 0.0 - 0.5 * dtdx * bp[m];
+              double g00 = 0.0, g02 = 0.0, g10 = 0.0, g12 = 0.0;
+              if (m4 > 0) {
+                g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
+                g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
+                g12 = g12 - c6 * dtdx * dtdz * P2[m];
+                g02 = g02 - c6 * dtdx * dtdz * P1[m];
+                g10 = g10 + c6 * dtdx * dtdz * M2[m];
+                g00 = g00 + c6 * dtdx * dtdz * M1[m];
+              }
+              if (m3 == 2) { g11 = g11 + dtdx * bpq[m]; g01 = g01 + dtdx * bmq[m]; }
+              st[(long long)(10 + 0 * 5 + m) * ss] = g00;
+              st[(long long)(10 + 1 * 5 + m) * ss] = g01;
+              st[(long long)(10 + 2 * 5 + m) * ss] = g02;
+              st[(long long)(10 + 3 * 5 + m) * ss] = g10;
+              st[(long long)(10 + 4 * 5 + m) * ss] = g11;
+              st[(long long)(10 + 5 * 5 + m) * ss] = g12;
+            }
+          }
+          // hadd at element 40 + ((side-1)*3 + d+1)*5 + m
+          {
+            double X1[5], X2[5], Y1[5], Y2[5];
+            if (m4 > 0) {
+              double t[5];
+              dt_input(m4, -3.0, bp, bpq, t);
+              euler3d_trans(R, DIR, 3, t, X1, X2);
+              dt_input(m4, -3.0, bm, bmq, t);
+              euler3d_trans(R, DIR, 3, t, Y1, Y2);
+            }
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+              double h01 = 0.0 - 0.5 * dtdx * cm[m], h11 = 0.0 - 0.5 * dtdx * cp[m];
+              double h00 = 0.0, h02 = 0.0, h10 = 0.0, h12 = 0.0;
+              if (m4 > 0) {
+                h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
+                h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
+                h12 = h12 - c6 * dtdx * dtdy * X2[m];
+                h02 = h02 - c6 * dtdx * dtdy * X1[m];
+                h10 = h10 + c6 * dtdx * dtdy * Y2[m];
+                h00 = h00 + c6 * dtdx * dtdy * Y1[m];
+              }
+              if (m3 == 2) { h11 = h11 + dtdx * cpq[m]; h01 = h01 + dtdx * cmq[m]; }
+              st[(long long)(40 + 0 * 5 + m) * ss] = h00;
+              st[(long long)(40 + 1 * 5 + m) * ss] = h01;
+              st[(long long)(40 + 2 * 5 + m) * ss] = h02;
+              st[(long long)(40 + 3 * 5 + m) * ss] = h10;
+              st[(long long)(40 + 4 * 5 + m) * ss] = h11;
+              st[(long long)(40 + 5 * 5 + m) * ss] = h12;
+            }
           }
         }
       }
-#pragma unroll
-      for (int m = 0; m < 5; ++m) {
-        double x = 0.0, y = 0.0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          x = x + 0.5 * fabs(Sc[k]) * (1.0 - fabs(Sc[k]) * dtdxave) * Wc[k][m];
-          y = y + 0.5 * fabs(Sn[k]) * (1.0 - fabs(Sn[k]) * dtdxave) * Wn[k][m];
-        }
-        CQc[m] = x; CQn[m] = y;
-      }
     }
-    double* st = A.stash + t;
-    const long long ss = A.stash_stride;
+  }
+  __syncthreads();
+  // amdq side of interface e: the terms of cell e-1, owned by thread l-1 of this tile
+  if (live && m3 > 0 && e >= 2 && l >= 2) {
+    double* sc = st - 1;
+    double bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
+    euler3d_trans(R, DIR, 2, AM, bm, bp);
+    euler3d_trans(R, DIR, 3, AM, cm, cp);
+    if (m3 == 2) { euler3d_trans(R, DIR, 2, CQ, bmq, bpq); euler3d_trans(R, DIR, 3, CQ, cmq, cpq); }
+    else {
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      double fm = 0.0 + AMc[m], fp = 0.0 - APc[m];
-      if (sp.order != 1) { fm = fm + CQc[m]; fp = fp + CQc[m]; }
-      st[(long long)m * ss] = fm;
-      st[(long long)(5 + m) * ss] = fp;
+      for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = 0.0;
     }
-    if (sp.m3 <= 0) {
-      for (int e = 10; e < STASH3; ++e) st[(long long)e * ss] = 0.0;
-      continue;
-    }
-    const double c6 = 1.0 / 6.0;
-    const int m3 = sp.m3, m4 = sp.m4;
-    double G[2][3][5], H[2][3][5];
-#pragma unroll
-    for (int s = 0; s < 2; ++s)
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int m = 0; m < 5; ++m) { G[s][d][m] = 0.0; H[s][d][m] = 0.0; }
-    // ---- terms of interface c (the apdq side; flux3.f:429-505 and 552-628 for cell i = c)
     {
-      const Roe3D R = roe3d(sp.gamma1, Q[1], Q[2]);
-      double bma[5], bpa[5], cma[5], cpa[5], bmq[5], bpq[5], cmq[5], cpq[5];
-      euler3d_trans(R, DIR, 2, APc, bma, bpa);
-      euler3d_trans(R, DIR, 3, APc, cma, cpa);
-      if (m3 == 2) { euler3d_trans(R, DIR, 2, CQc, bmq, bpq); euler3d_trans(R, DIR, 3, CQc, cmq, cpq); }
-#pragma unroll
-      for (int m = 0; m < 5; ++m) { G[0][1][m] = G[0][1][m] - 0.5 * dtdx * bma[m]; G[1][1][m] = G[1][1][m] - 0.5 * dtdx * bpa[m]; }
+      double P1[5], P2[5], M1[5], M2[5];
       if (m4 > 0) {
-        double c2p[5], c2m[5], P1[5], P2[5], M1[5], M2[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          c2p[m] = (m4 == 2) ? cpa[m] - 3.0 * cpq[m] : cpa[m];
-          c2m[m] = (m4 == 2) ? cma[m] - 3.0 * cmq[m] : cma[m];
-        }
-        euler3d_trans(R, DIR, 2, c2p, P1, P2);
-        euler3d_trans(R, DIR, 2, c2m, M1, M2);
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          G[1][1][m] = G[1][1][m] + c6 * dtdx * dtdz * (P2[m] - M2[m]);
-          G[0][1][m] = G[0][1][m] + c6 * dtdx * dtdz * (P1[m] - M1[m]);
-          G[1][2][m] = G[1][2][m] - c6 * dtdx * dtdz * P2[m];
-          G[0][2][m] = G[0][2][m] - c6 * dtdx * dtdz * P1[m];
-          G[1][0][m] = G[1][0][m] + c6 * dtdx * dtdz * M2[m];
-          G[0][0][m] = G[0][0][m] + c6 * dtdx * dtdz * M1[m];
-        }
-      }
-      if (m3 == 2) {
-#pragma unroll
-        for (int m = 0; m < 5; ++m) { G[1][1][m] = G[1][1][m] + dtdx * bpq[m]; G[0][1][m] = G[0][1][m] + dtdx * bmq[m]; }
-      }
-      // hadd
-      double X1[5], X2[5], Y1[5], Y2[5];
-      if (m4 > 0) {
-        double bp2[5], bm2[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          bp2[m] = (m4 == 2) ? bpa[m] - 3.0 * bpq[m] : bpa[m];
-          bm2[m] = (m4 == 2) ? bma[m] - 3.0 * bmq[m] : bma[m];
-        }
-        euler3d_trans(R, DIR, 3, bp2, X1, X2);
-        euler3d_trans(R, DIR, 3, bm2, Y1, Y2);
+        double t[5];
+        dt_input(m4, 3.0, cp, cpq, t);
+        euler3d_trans(R, DIR, 2, t, P1, P2);
+        dt_input(m4, 3.0, cm, cmq, t);
+        euler3d_trans(R, DIR, 2, t, M1, M2);
       }
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        H[0][1][m] = H[0][1][m] - 0.5 * dtdx * cma[m];
-        H[1][1][m] = H[1][1][m] - 0.5 * dtdx * cpa[m];
+        double g01 = sc[(long long)(10 + 1 * 5 + m) * ss], g11 = sc[(long long)(10 + 4 * 5 + m) * ss];
+        g01 = g01 - 0.5 * dtdx * bm[m];
+        g11 = g11 - 0.5 * dtdx * bp[m];
         if (m4 > 0) {
-          H[1][1][m] = H[1][1][m] + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
-          H[0][1][m] = H[0][1][m] + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
-          H[1][2][m] = H[1][2][m] - c6 * dtdx * dtdy * X2[m];
-          H[0][2][m] = H[0][2][m] - c6 * dtdx * dtdy * X1[m];
-          H[1][0][m] = H[1][0][m] + c6 * dtdx * dtdy * Y2[m];
-          H[0][0][m] = H[0][0][m] + c6 * dtdx * dtdy * Y1[m];
+          double g00 = sc[(long long)(10 + 0 * 5 + m) * ss], g02 = sc[(long long)(10 + 2 * 5 + m) * ss];
+          double g10 = sc[(long long)(10 + 3 * 5 + m) * ss], g12 = sc[(long long)(10 + 5 * 5 + m) * ss];
+          g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
+          g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
+          g12 = g12 - c6 * dtdx * dtdz * P2[m];
+          g02 = g02 - c6 * dtdx * dtdz * P1[m];
+          g10 = g10 + c6 * dtdx * dtdz * M2[m];
+          g00 = g00 + c6 * dtdx * dtdz * M1[m];
+          sc[(long long)(10 + 0 * 5 + m) * ss] = g00;
+          sc[(long long)(10 + 2 * 5 + m) * ss] = g02;
+          sc[(long long)(10 + 3 * 5 + m) * ss] = g10;
+          sc[(long long)(10 + 5 * 5 + m) * ss] = g12;
         }
-        if (m3 == 2) {
-          H[1][1][m] = H[1][1][m] + dtdx * cpq[m];
-          H[0][1][m] = H[0][1][m] + dtdx * cmq[m];
-        }
+        if (m3 == 2) { g11 = g11 - dtdx * bpq[m]; g01 = g01 - dtdx * bmq[m]; }
+        sc[(long long)(10 + 1 * 5 + m) * ss] = g01;
+        sc[(long long)(10 + 4 * 5 + m) * ss] = g11;
       }
     }
-    // ---- terms of interface c+1 (the amdq side, added to cell i-1 = c)
-    if (hasB) {
-      const Roe3D R = roe3d(sp.gamma1, Q[2], Q[3]);
-      double bmm[5], bpm[5], cmm[5], cpm[5], bmq[5], bpq[5], cmq[5], cpq[5];
-      euler3d_trans(R, DIR, 2, AMn, bmm, bpm);
-      euler3d_trans(R, DIR, 3, AMn, cmm, cpm);
-      if (m3 == 2) { euler3d_trans(R, DIR, 2, CQn, bmq, bpq); euler3d_trans(R, DIR, 3, CQn, cmq, cpq); }
-#pragma unroll
-      for (int m = 0; m < 5; ++m) { G[0][1][m] = G[0][1][m] - 0.5 * dtdx * bmm[m]; G[1][1][m] = G[1][1][m] - 0.5 * dtdx * bpm[m]; }
-      if (m4 > 0) {
-        double c2p[5], c2m[5], P1[5], P2[5], M1[5], M2[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          c2p[m] = (m4 == 2) ? cpm[m] + 3.0 * cpq[m] : cpm[m];
-          c2m[m] = (m4 == 2) ? cmm[m] + 3.0 * cmq[m] : cmm[m];
-        }
-        euler3d_trans(R, DIR, 2, c2p, P1, P2);
-        euler3d_trans(R, DIR, 2, c2m, M1, M2);
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          G[1][1][m] = G[1][1][m] + c6 * dtdx * dtdz * (P2[m] - M2[m]);
-          G[0][1][m] = G[0][1][m] + c6 * dtdx * dtdz * (P1[m] - M1[m]);
-          G[1][2][m] = G[1][2][m] - c6 * dtdx * dtdz * P2[m];
-          G[0][2][m] = G[0][2][m] - c6 * dtdx * dtdz * P1[m];
-          G[1][0][m] = G[1][0][m] + c6 * dtdx * dtdz * M2[m];
-          G[0][0][m] = G[0][0][m] + c6 * dtdx * dtdz * M1[m];
-        }
-      }
-      if (m3 == 2) {
-#pragma unroll
-        for (int m = 0; m < 5; ++m) { G[1][1][m] = G[1][1][m] - dtdx * bpq[m]; G[0][1][m] = G[0][1][m] - dtdx * bmq[m]; }
-      }
+    {
       double X1[5], X2[5], Y1[5], Y2[5];
       if (m4 > 0) {
-        double bp2[5], bm2[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          bp2[m] = (m4 == 2) ? bpm[m] + 3.0 * bpq[m] : bpm[m];
-          bm2[m] = (m4 == 2) ? bmm[m] + 3.0 * bmq[m] : bmm[m];
-        }
-        euler3d_trans(R, DIR, 3, bp2, X1, X2);
-        euler3d_trans(R, DIR, 3, bm2, Y1, Y2);
+        double t[5];
+        dt_input(m4, 3.0, bp, bpq, t);
+        euler3d_trans(R, DIR, 3, t, X1, X2);
+        dt_input(m4, 3.0, bm, bmq, t);
+        euler3d_trans(R, DIR, 3, t, Y1, Y2);
       }
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        H[0][1][m] = H[0][1][m] - 0.5 * dtdx * cmm[m];
-        H[1][1][m] = H[1][1][m] - 0.5 * dtdx * cpm[m];
+        double h01 = sc[(long long)(40 + 1 * 5 + m) * ss], h11 = sc[(long long)(40 + 4 * 5 + m) * ss];
+        h01 = h01 - 0.5 * dtdx * cm[m];
+        h11 = h11 - 0.5 * dtdx * cp[m];
         if (m4 > 0) {
-          H[1][1][m] = H[1][1][m] + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
-          H[0][1][m] = H[0][1][m] + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
-          H[1][2][m] = H[1][2][m] - c6 * dtdx * dtdy * X2[m];
-          H[0][2][m] = H[0][2][m] - c6 * dtdx * dtdy * X1[m];
-          H[1][0][m] = H[1][0][m] + c6 * dtdx * dtdy * Y2[m];
-          H[0][0][m] = H[0][0][m] + c6 * dtdx * dtdy * Y1[m];
+          double h00 = sc[(long long)(40 + 0 * 5 + m) * ss], h02 = sc[(long long)(40 + 2 * 5 + m) * ss];
+          double h10 = sc[(long long)(40 + 3 * 5 + m) * ss], h12 = sc[(long long)(40 + 5 * 5 + m) * ss];
+          h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
+          h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
+          h12 = h12 - c6 * dtdx * dtdy * X2[m];
+          h02 = h02 - c6 * dtdx * dtdy * X1[m];
+          h10 = h10 + c6 * dtdx * dtdy * Y2[m];
+          h00 = h00 + c6 * dtdx * dtdy * Y1[m];
+          sc[(long long)(40 + 0 * 5 + m) * ss] = h00;
+          sc[(long long)(40 + 2 * 5 + m) * ss] = h02;
+          sc[(long long)(40 + 3 * 5 + m) * ss] = h10;
+          sc[(long long)(40 + 5 * 5 + m) * ss] = h12;
         }
-        if (m3 == 2) {
-          H[1][1][m] = H[1][1][m] - dtdx * cpq[m];
-          H[0][1][m] = H[0][1][m] - dtdx * cmq[m];
-        }
+        if (m3 == 2) { h11 = h11 - dtdx * cpq[m]; h01 = h01 - dtdx * cmq[m]; }
+        sc[(long long)(40 + 1 * 5 + m) * ss] = h01;
+        sc[(long long)(40 + 4 * 5 + m) * ss] = h11;
       }
     }
-#pragma unroll
-    for (int s = 0; s < 2; ++s)
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          st[(long long)(10 + (s * 3 + d) * 5 + m) * ss] = G[s][d][m];
-          st[(long long)(40 + (s * 3 + d) * 5 + m) * ss] = H[s][d][m];
-        }
   }
   // block-wide max of the Courant number, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
@@ -816,40 +820,6 @@ __global__ void average3_kernel(double* pool, const PatchDev* patches, const Avg
   }
 }
 
-// spest.f + flag2refine.f: BADPT (2) where the undivided difference exceeds tolsp, else GOODPT (0)
-__global__ void flags3_kernel(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
-                              int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* out, long long ncells) {
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ncells; t += (long long)gridDim.x * blockDim.x) {
-    const int pi = find_patch(cell0, np, t);
-    const PatchDev& P = patches[plist[pi]];
-    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
-    const long long loc = t - cell0[pi];
-    const int i = (int)(loc % mx) + 1, j = (int)((loc / mx) % my) + 1, k = (int)(loc / ((long long)mx * my)) + 1;
-    const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
-    const double* q = pool + P.q[P.cur];
-    auto Q = [&](int m, int ii, int jj, int kk) { return q[(m - 1) * plane + ((long long)(kk - 1 + NG3) * P.mjtot + (jj - 1 + NG3)) * P.mitot + (ii - 1 + NG3)]; };
-    double dq = 0.0;
-    if (flag_pressure) {
-      auto pres = [&](int a, int b, int c) {
-        const double rho = Q(1, a, b, c), mu = Q(2, a, b, c), mv = Q(3, a, b, c), mw = Q(4, a, b, c);
-        return gamma1 * (Q(5, a, b, c) - 0.5 * (mu * mu + mv * mv + mw * mw) / rho);
-      };
-      const double dpi = fabs(pres(i + 1, j, k) - pres(i - 1, j, k));
-      const double dpj = fabs(pres(i, j + 1, k) - pres(i, j - 1, k));
-      const double dpk = fabs(pres(i, j, k + 1) - pres(i, j, k - 1));
-      dq = dmax(dmax(dmax(dq, dpi), dpj), dpk);
-    } else {
-      for (int m = 1; m <= nvar; ++m) {
-        const double dqi = fabs(Q(m, i + 1, j, k) - Q(m, i - 1, j, k));
-        const double dqj = fabs(Q(m, i, j + 1, k) - Q(m, i, j - 1, k));
-        const double dqk = fabs(Q(m, i, j, k + 1) - Q(m, i, j, k - 1));
-        dq = dmax(dmax(dmax(dq, dqi), dqj), dqk);
-      }
-    }
-    out[t] = (dq > tolsp) ? (int8_t)2 : (int8_t)0;
-  }
-}
-
 // gauges_module.f90:376-430 trilinear sample
 __global__ void gauges3_kernel(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -909,10 +879,11 @@ int grid_for(long long n, int block) {
 
 }  // namespace
 
-void launch_step3(const Step3Args& a, long long items[3], long long faces, long long cells, cudaStream_t s) {
-  if (items[0] > 0) sweep3_kernel<1><<<grid_for(items[0], 128), 128, 0, s>>>(a);
-  if (items[1] > 0) sweep3_kernel<2><<<grid_for(items[1], 128), 128, 0, s>>>(a);
-  if (items[2] > 0) sweep3_kernel<3><<<grid_for(items[2], 128), 128, 0, s>>>(a);
+void launch_step3(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s) {
+  auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
+  if (items[0] > 0) sweep3_kernel<1><<<tiles(items[0]), SW_T, 0, s>>>(a);
+  if (items[1] > 0) sweep3_kernel<2><<<tiles(items[1]), SW_T, 0, s>>>(a);
+  if (items[2] > 0) sweep3_kernel<3><<<tiles(items[2]), SW_T, 0, s>>>(a);
   AMR_CUDA(cudaGetLastError());
   if (faces > 0) face3_kernel<<<grid_for(faces, 128), 128, 0, s>>>(a);
   if (cells > 0) update3_kernel<<<grid_for(cells, 256), 256, 0, s>>>(a);
@@ -963,18 +934,14 @@ void launch_upbnd3(double* pool, const double* regs, const PatchDev* patches, co
   upbnd3_kernel<<<(n + 127) / 128, 128, 0, s>>>(pool, regs, patches, cells, n, terms, volume, nvar);
   AMR_CUDA(cudaGetLastError());
 }
-void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, int rx, int ry, int rz, int nvar, cudaStream_t s) {
+void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, long long max_cells, int rx, int ry, int rz, int nvar,
+                     cudaStream_t s) {
   if (n <= 0) return;
+  const int bx = (int)std::max<long long>(1, std::min<long long>((max_cells + 127) / 128, 1024));
   for (int base = 0; base < n; base += 65535) {
     const int cnt = std::min(65535, n - base);
-    average3_kernel<<<dim3(4, cnt), 128, 0, s>>>(pool, patches, r + base, cnt, rx, ry, rz, nvar);
+    average3_kernel<<<dim3(bx, cnt), 128, 0, s>>>(pool, patches, r + base, cnt, rx, ry, rz, nvar);
   }
-  AMR_CUDA(cudaGetLastError());
-}
-void launch_flags3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int flag_pressure,
-                   double gamma1, double tolsp, int nvar, int8_t* out, long long ncells, cudaStream_t s) {
-  if (ncells <= 0) return;
-  flags3_kernel<<<grid_for(ncells, 256), 256, 0, s>>>(pool, patches, plist, cell0, np, flag_pressure, gamma1, tolsp, nvar, out, ncells);
   AMR_CUDA(cudaGetLastError());
 }
 void launch_gauges3(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s) {

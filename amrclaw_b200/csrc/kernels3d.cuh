@@ -24,7 +24,8 @@ struct Step3Args {
   const PatchDev* patches;
   const int* plist;          // patch ids of the level, in level order
   int np;
-  const long long* sweep0;   // [3][np+1]: first sweep item (= stash slot) of each patch, per direction
+  const long long* sweep0;   // [3][np+1]: first stash slot of each patch, per direction ((n1+1) per pencil)
+  const long long* comp0;    // [3][np+1]: first interface of each patch, per direction ((n1+3) per pencil)
   const long long* face0;    // [np+1]: first face cell of each patch ((mx+1)(my+1)(mz+1) each)
   const long long* cell0;    // [np+1]: first interior cell of each patch (mx*my*mz each)
   long long stash_stride;    // slots of one direction region x 3 (SoA stride)
@@ -80,7 +81,8 @@ struct Upbnd3Cell { int patch; int ie, je, ke; int first, count; };
 struct Upbnd3Term { long long reg; double sgn; };
 struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff; };
 
-void launch_step3(const Step3Args& a, long long items_per_dir[3], long long faces, long long cells, cudaStream_t s);
+// interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction
+void launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s);
 void launch_fsv3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
                  const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s);
 void launch_fad3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
@@ -91,9 +93,8 @@ void launch_fill3(const Fill3Args& a, cudaStream_t s);
 void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s);
 void launch_upbnd3(double* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
                    const Upbnd3Term* terms, double volume, int nvar, cudaStream_t s);
-void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, int rx, int ry, int rz, int nvar, cudaStream_t s);
-void launch_flags3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
-                   int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* out, long long ncells, cudaStream_t s);
+void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, long long max_cells, int rx, int ry, int rz, int nvar,
+                     cudaStream_t s);
 void launch_gauges3(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s);
 void launch_mass3(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s);
 void launch_gather3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,

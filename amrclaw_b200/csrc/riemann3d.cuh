@@ -76,13 +76,13 @@ __device__ __forceinline__ void euler3d_trans(const Roe3D& R, int ixyz, int icoo
   euler3d_split(R, mn, mt1, mt2, d, bm, bp);
 }
 
-// rpn3 at one interface: L = q(i-1), R = q(i) (1-based arrays of 5). Returns the
-// waves (3 x 5, 0-based components), speeds, and the fluctuations.
-__device__ __forceinline__ void euler3d_rpn(double gam, double g1, bool efix, int ixyz, const double* L, const double* R,
-                                            double wave[3][5], double s[3], double* amdq, double* apdq) {
+// rpn3 at one interface: L = q(i-1), R = q(i) (1-based arrays of 5) with their Roe
+// average o = roe3d(g1, L, R). Returns the waves (3 x 5, 0-based components), speeds,
+// and the fluctuations.
+__device__ __forceinline__ void euler3d_rpn_roe(double gam, double g1, bool efix, int ixyz, const double* L, const double* R,
+                                                const Roe3D& o, double wave[3][5], double s[3], double* amdq, double* apdq) {
   int mu, mv, mw;
   frame3d(ixyz, mu, mv, mw);
-  const Roe3D o = roe3d(g1, L, R);
   const double u = o.u[mu], v = o.u[mv], w = o.u[mw], a = o.a;
   const double d1 = R[1] - L[1], du = R[mu] - L[mu], dv = R[mv] - L[mv], dw = R[mw] - L[mw], d5 = R[5] - L[5];
   const double a3 = o.g1a2 * (o.euv * d1 + u * du + v * dv + w * dw - d5);
@@ -159,6 +159,12 @@ __device__ __forceinline__ void euler3d_rpn(double gam, double g1, bool efix, in
       apdq[m] = df[m] - am;
     }
   }
+}
+
+__device__ __forceinline__ void euler3d_rpn(double gam, double g1, bool efix, int ixyz, const double* L, const double* R,
+                                            double wave[3][5], double s[3], double* amdq, double* apdq) {
+  const Roe3D o = roe3d(g1, L, R);
+  euler3d_rpn_roe(gam, g1, efix, ixyz, L, R, o, wave, s, amdq, apdq);
 }
 
 }  // namespace amrb
