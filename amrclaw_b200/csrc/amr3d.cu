@@ -561,6 +561,7 @@ class Amr3Gpu : public AmrSolver {
 
   // saveqc.f:3-111 for the kids at level lev+1
   void compile_saveqc(int lev) {
+    HPROF("compile_saveqc3");
     Prog3& P = plan[lev].saveqc;
     P.clear();
     if (lev + 1 > p.mxnest || lstart[lev + 1] == 0) { upload_prog(P); return; }
@@ -586,6 +587,7 @@ class Amr3Gpu : public AmrSolver {
   }
 
   void upload_prog(Prog3& P) {
+    HPROF("upload_prog3");
     if (P.scratch_off >= 0) pool.release(P.scratch_off, P.scratch_alloc);
     P.scratch_alloc = std::max<long long>(P.scratch_len, 1);
     P.scratch_off = pool.alloc(P.scratch_alloc);
@@ -714,6 +716,8 @@ class Amr3Gpu : public AmrSolver {
         add(6, nxc_, nyc_, rx, ry);
       }
     }
+    PhaseTimer tph(hprof);
+    tph.next("cs_upload");
     L.d_plist.upload(L.plist, st, stg);
     L.d_sweep0.upload(L.sweep0, st, stg);
     L.d_comp0.upload(L.comp0, st, stg);
@@ -723,6 +727,7 @@ class Amr3Gpu : public AmrSolver {
     L.d_fad.upload(L.fad, st, stg);
     L.d_qad.upload(L.qad, st, stg);
     // staging and face-flux buffers sized for the largest level
+    tph.next("cs_reserve");
     d_stash.reserve(std::max<size_t>(d_stash.n, (size_t)(L.slots * STASH3)));
     d_flux.reserve(std::max<size_t>(d_flux.n, (size_t)(L.faces * 30)));
   }
@@ -740,25 +745,36 @@ class Amr3Gpu : public AmrSolver {
       for (int m : lgrids[lev]) {
         const HPatch3& g = node[m];
         if (g.has_cfl) {
-          const int mi = mitot(m), mj = mjtot(m), mk = mktot(m);
-          std::vector<int> used((size_t)mi * mj * mk, 0), slot((size_t)mi * mj * mk, -1), order;
-          std::vector<std::vector<Upbnd3Term>> terms;
-          for (size_t e = 0; e + 5 < g.listbc.size(); e += 6) {
-            const int* b = &g.listbc[e];
-            const int side = b[3], norm = 1 << (side - 1);
-            const size_t key = ((size_t)(b[2] - 1) * mj + (b[1] - 1)) * mi + (b[0] - 1);
-            if ((used[key] / norm) % 2 == 1) continue;
-            if (slot[key] < 0) { slot[key] = (int)terms.size(); terms.emplace_back(); order.push_back((int)key); }
-            terms[slot[key]].push_back(Upbnd3Term{node[b[4]].ffl + (long long)nvar * (b[5] - 1), chsign[side]});
-            used[key] += norm;
+          // upbnd.f: the entries of one coarse cell in listbc order, each side at most once
+          // (the iused bit mask); cells are independent, so they are grouped by a sort
+          const int mi = mitot(m), mj = mjtot(m);
+          const size_t ne = g.listbc.size() / 6;
+          if (ne >= (1u << 24)) throw std::runtime_error("upbnd: too many register entries on one patch");
+          std::vector<unsigned long long> ord(ne);
+          for (size_t e = 0; e < ne; ++e) {
+            const int* b = &g.listbc[6 * e];
+            const unsigned long long key = ((unsigned long long)(b[2] - 1) * mj + (b[1] - 1)) * mi + (b[0] - 1);
+            ord[e] = (key << 24) | e;
           }
-          for (int key : order) {
+          std::sort(ord.begin(), ord.end());
+          for (size_t a0 = 0; a0 < ne;) {
+            const unsigned long long key = ord[a0] >> 24;
+            size_t a1 = a0;
+            while (a1 < ne && (ord[a1] >> 24) == key) ++a1;
             Upbnd3Cell c{};
-            c.patch = m; c.ie = key % mi; c.je = (key / mi) % mj; c.ke = key / (mi * mj);
-            const auto& T = terms[slot[key]];
-            c.first = (int)L.upt.size(); c.count = (int)T.size();
-            L.upt.insert(L.upt.end(), T.begin(), T.end());
+            c.patch = m; c.ie = (int)(key % mi); c.je = (int)((key / mi) % mj); c.ke = (int)(key / ((unsigned long long)mi * mj));
+            c.first = (int)L.upt.size();
+            int used = 0;
+            for (size_t q = a0; q < a1; ++q) {
+              const int* b = &g.listbc[6 * (ord[q] & 0xffffff)];
+              const int side = b[3], norm = 1 << (side - 1);
+              if ((used / norm) % 2 == 1) continue;
+              L.upt.push_back(Upbnd3Term{node[b[4]].ffl + (long long)nvar * (b[5] - 1), chsign[side]});
+              used += norm;
+            }
+            c.count = (int)L.upt.size() - c.first;
             L.upc.push_back(c);
+            a0 = a1;
           }
         }
         XF.query(g.ilo * rx, g.ihi * rx + rx - 1, g.jlo * ry, g.jhi * ry + ry - 1, g.klo * rz, g.khi * rz + rz - 1, hits);
@@ -871,7 +887,11 @@ class Amr3Gpu : public AmrSolver {
   }
 
   void compile_all(int lbase = 0) {
+    HPROF("compile_all3");
+    PhaseTimer tph(hprof);
+    tph.next("ca_desc");
     sync_descriptors();
+    tph.close();
     for (int lev = 1; lev <= p.mxnest; ++lev) {
       if (lev > lfine) { plan[lev].plist.clear(); continue; }
       if (lev > lbase) compile_bound(lev);
@@ -1472,10 +1492,19 @@ class Amr3Gpu : public AmrSolver {
     }
     AMR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (cudaEvent_t* e : {&ev_a, &ev_b, &ev_run0, &ev_run1}) AMR_CUDA(cudaEventCreate(e));
-    pool.init((long long)nvar * (nxc + 4) * (nyc + 4) * (nzc + 4) * 4 + (1 << 22));
+    // room for the finer levels from the start (16x the level-1 storage): growing the pool
+    // later moves it, which waits for the device
+    pool.init((long long)nvar * (nxc + 4) * (nyc + 4) * (nzc + 4) * 32 + (1 << 22));
     regs.init(1 << 20);
     AMR_CUDA(cudaMalloc(&d_cfl, sizeof(unsigned long long)));
     AMR_CUDA(cudaMalloc(&d_mass, sizeof(double)));
+    {
+      // sweep staging and face fluxes: reserved at once for twice a level-1 sweep
+      const long long n = (long long)nxc * nyc * nzc;
+      d_stash.reserve((size_t)(STASH3 * 3 * (n + 4LL * (nxc * nyc + nyc * nzc + nxc * nzc))));
+      d_flux.reserve((size_t)(30 * (n + 2LL * (nxc * nyc + nyc * nzc + nxc * nzc) + 8)));
+      d_stash.n = d_flux.n = 0;
+    }
     node.assign(10001, HPatch3());
     for (int k = 1; k <= 10000; ++k) node[k].nextfree = k + 1;
     node[10000].nextfree = 0;

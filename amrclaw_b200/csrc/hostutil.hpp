@@ -138,12 +138,14 @@ struct Staging {
 
 template <class T> struct DBuf {
   T* d = nullptr; size_t cap = 0, n = 0;
+  // smallest allocation (64 KiB): small per-level arrays then rarely reallocate
+  static constexpr size_t kMin = (64 << 10) / sizeof(T) > 16 ? (64 << 10) / sizeof(T) : 16;
   void upload(const std::vector<T>& h, cudaStream_t s, Staging& stg) { upload(h.data(), h.size(), s, stg); }
   void upload(const T* h, size_t cnt, cudaStream_t s, Staging& stg) {
     n = cnt;
     if (n > cap) {
       if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(n, 16) * 2;
+      cap = std::max<size_t>(n * 2, kMin);
       AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
     }
     if (n) AMR_CUDA(cudaMemcpyAsync(d, stg.put(h, sizeof(T) * n, s), sizeof(T) * n, cudaMemcpyHostToDevice, s));
@@ -161,7 +163,7 @@ template <class T> struct DBuf {
   void reserve(size_t m) {
     if (m > cap) {
       if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(m, 16) * 2;
+      cap = std::max<size_t>(m * 2, kMin);
       AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
     }
     n = m;
