@@ -22,6 +22,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <memory>
 #include <vector>
 
@@ -96,8 +97,8 @@ struct Plan3 {
   std::vector<long long> sweep0, comp0, face0, cell0;
   long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;  // items: interfaces per direction
   std::vector<Fsv3> fsv;
-  std::vector<Fad3> fad;
-  std::vector<Qad3Job> qad;
+  std::vector<long long> seg0;  // register segments (lenbc) prefix over plist; fad/qad lists are built from it on the device
+  long long nseg = 0;
   std::vector<Upbnd3Cell> upc;
   std::vector<Upbnd3Term> upt;
   std::vector<Avg3> avg;
@@ -105,6 +106,7 @@ struct Plan3 {
   DBuf<int> d_plist;
   DBuf<long long> d_sweep0, d_comp0, d_face0, d_cell0;
   DBuf<Fsv3> d_fsv;
+  DBuf<long long> d_seg0;
   DBuf<Fad3> d_fad;
   DBuf<Qad3Job> d_qad;
   DBuf<Upbnd3Cell> d_upc;
@@ -112,10 +114,13 @@ struct Plan3 {
   DBuf<Avg3> d_avg;
   void free_dev() {
     bound.free_dev(); saveqc.free_dev();
-    d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_fad.free(); d_qad.free();
+    d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_seg0.free(); d_fad.free(); d_qad.free();
     d_upc.free(); d_upt.free(); d_avg.free();
   }
 };
+
+// a flagged cell (1-based level indices); the reference stores its centre (i-.5, j-.5, k-.5)
+struct FlagPt { int c[3]; };
 
 // read-only view of a level int8 array (the nesting domain read back for nestck.f)
 struct LvlView {
@@ -682,40 +687,29 @@ class Amr3Gpu : public AmrSolver {
       L.cell0[k + 1] = L.cell0[k] + (long long)g.nx() * g.ny() * g.nz();
     }
     L.faces = L.face0[np]; L.cells = L.cell0[np];
-    L.fsv.clear(); L.fad.clear(); L.qad.clear();
+    L.seg0.assign(np + 1, 0);
+    std::vector<long long> fsv0(np + 1, 0);
     for (int k = 0; k < np; ++k) {
+      const HPatch3& g = node[L.plist[k]];
+      L.seg0[k + 1] = L.seg0[k] + ((lev > 1 && g.ffl >= 0) ? g.lenbc : 0);
+      fsv0[k + 1] = fsv0[k] + (g.has_cfl ? (long long)(g.listbc.size() / 6) : 0);
+    }
+    L.nseg = L.seg0[np];
+    // fluxsv.f entries: one per listbc entry of the coarse patches, written in place
+    L.fsv.resize(fsv0[np]);
+    pool_host.run(np, [&](int k) {
       const int m = L.plist[k];
       const HPatch3& g = node[m];
-      if (g.has_cfl)
-        for (size_t e = 0; e + 5 < g.listbc.size(); e += 6) {
-          const int* b = &g.listbc[e];
-          Fsv3 f{};
-          f.patch = m; f.pidx = k; f.i = b[0] - G3; f.j = b[1] - G3; f.k = b[2] - G3; f.side = b[3];
-          f.dst = node[b[4]].ffl + (long long)nvar * (b[5] - 1);
-          L.fsv.push_back(f);
-        }
-      if (lev > 1 && g.ffl >= 0) {
-        const int rx = intratx[lev - 1], ry = intraty[lev - 1], rz = intratz[lev - 1];
-        const int nxc_ = g.nx() / rx, nyc_ = g.ny() / ry, nzc_ = g.nz() / rz;
-        int seg = 0;
-        auto add = [&](int side, int na, int nb, int ra, int rb) {
-          for (int bc = 0; bc < nb; ++bc)
-            for (int ac = 0; ac < na; ++ac) {
-              L.fad.push_back(Fad3{m, k, side, ac * ra, bc * rb, ra, rb, seg});
-              Qad3Job q{};
-              q.patch = m; q.side = side; q.slab = bc; q.row0 = ac * ra; q.nreg = 1; q.reg0 = seg; q.ratio_a = ra; q.ratio_b = rb;
-              L.qad.push_back(q);
-              ++seg;
-            }
-        };
-        add(1, nyc_, nzc_, ry, rz);
-        add(2, nxc_, nzc_, rx, rz);
-        add(3, nyc_, nzc_, ry, rz);
-        add(4, nxc_, nzc_, rx, rz);
-        add(5, nxc_, nyc_, rx, ry);
-        add(6, nxc_, nyc_, rx, ry);
+      if (!g.has_cfl) return;
+      Fsv3* out = L.fsv.data() + fsv0[k];
+      for (size_t e = 0; e + 5 < g.listbc.size(); e += 6) {
+        const int* b = &g.listbc[e];
+        Fsv3 f{};
+        f.patch = m; f.pidx = k; f.i = b[0] - G3; f.j = b[1] - G3; f.k = b[2] - G3; f.side = b[3];
+        f.dst = node[b[4]].ffl + (long long)nvar * (b[5] - 1);
+        *out++ = f;
       }
-    }
+    });
     PhaseTimer tph(hprof);
     tph.next("cs_upload");
     L.d_plist.upload(L.plist, st, stg);
@@ -724,8 +718,15 @@ class Amr3Gpu : public AmrSolver {
     L.d_face0.upload(L.face0, st, stg);
     L.d_cell0.upload(L.cell0, st, stg);
     L.d_fsv.upload(L.fsv, st, stg);
-    L.d_fad.upload(L.fad, st, stg);
-    L.d_qad.upload(L.qad, st, stg);
+    L.d_seg0.upload(L.seg0, st, stg);
+    L.d_fad.reserve(L.nseg);
+    L.d_qad.reserve(L.nseg);
+    if (lev > 1 && L.nseg > 0) {
+      // the descriptors of this level must be on the device (compile_all uploads them first)
+      launch_expand_fadqad3(L.d_plist.d, L.d_seg0.d, np, d_patches.d, intratx[lev - 1], intraty[lev - 1], intratz[lev - 1], L.nseg,
+                            L.d_fad.d, L.d_qad.d, st);
+      ++nkernels;
+    }
     // staging and face-flux buffers sized for the largest level
     tph.next("cs_reserve");
     d_stash.reserve(std::max<size_t>(d_stash.n, (size_t)(L.slots * STASH3)));
@@ -739,64 +740,77 @@ class Amr3Gpu : public AmrSolver {
     L.upc.clear(); L.upt.clear(); L.avg.clear();
     if (lev < p.mxnest && lstart[lev + 1] != 0) {
       const GridIndex& XF = GI(lev + 1);
-      std::vector<int> hits;
       const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
-      const double chsign[7] = {0, 1., -1., -1., 1., 1., -1.};
-      for (int m : lgrids[lev]) {
-        const HPatch3& g = node[m];
-        if (g.has_cfl) {
-          // upbnd.f: the entries of one coarse cell in listbc order, each side at most once
-          // (the iused bit mask); cells are independent, so they are grouped by a sort
-          const int mi = mitot(m), mj = mjtot(m);
-          const size_t ne = g.listbc.size() / 6;
-          if (ne >= (1u << 24)) throw std::runtime_error("upbnd: too many register entries on one patch");
-          std::vector<unsigned long long> ord(ne);
-          for (size_t e = 0; e < ne; ++e) {
-            const int* b = &g.listbc[6 * e];
-            const unsigned long long key = ((unsigned long long)(b[2] - 1) * mj + (b[1] - 1)) * mi + (b[0] - 1);
-            ord[e] = (key << 24) | e;
-          }
-          std::sort(ord.begin(), ord.end());
-          for (size_t a0 = 0; a0 < ne;) {
-            const unsigned long long key = ord[a0] >> 24;
-            size_t a1 = a0;
-            while (a1 < ne && (ord[a1] >> 24) == key) ++a1;
-            Upbnd3Cell c{};
-            c.patch = m; c.ie = (int)(key % mi); c.je = (int)((key / mi) % mj); c.ke = (int)(key / ((unsigned long long)mi * mj));
-            c.first = (int)L.upt.size();
-            int used = 0;
-            for (size_t q = a0; q < a1; ++q) {
-              const int* b = &g.listbc[6 * (ord[q] & 0xffffff)];
-              const int side = b[3], norm = 1 << (side - 1);
-              if ((used / norm) % 2 == 1) continue;
-              L.upt.push_back(Upbnd3Term{node[b[4]].ffl + (long long)nvar * (b[5] - 1), chsign[side]});
-              used += norm;
-            }
-            c.count = (int)L.upt.size() - c.first;
-            L.upc.push_back(c);
-            a0 = a1;
-          }
-        }
-        XF.query(g.ilo * rx, g.ihi * rx + rx - 1, g.jlo * ry, g.jhi * ry + ry - 1, g.klo * rz, g.khi * rz + rz - 1, hits);
-        for (int r : hits) {
-          const int kk = XF.id(r);
-          const HPatch3& f = node[kk];
-          const int iclo = f.ilo / rx, jclo = f.jlo / ry, kclo = f.klo / rz, ichi = f.ihi / rx, jchi = f.jhi / ry, kchi = f.khi / rz;
-          const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), kplo = std::max(g.klo, kclo);
-          const int iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi), kphi = std::min(g.khi, kchi);
-          if (iplo > iphi || jplo > jphi || kplo > kphi) continue;
-          Avg3 a{};
-          a.cpatch = m; a.kpatch = kk;
-          a.ci0 = iplo - g.ilo + G3; a.cj0 = jplo - g.jlo + G3; a.ck0 = kplo - g.klo + G3;
-          a.ni = iphi - iplo + 1; a.nj = jphi - jplo + 1; a.nk = kphi - kplo + 1;
-          a.fi0 = iplo * rx - f.ilo + G3; a.fj0 = jplo * ry - f.jlo + G3; a.fk0 = kplo * rz - f.klo + G3;
-          L.avg.push_back(a);
-        }
+      const std::vector<int>& G = lgrids[lev];
+      struct Part { std::vector<Upbnd3Cell> upc; std::vector<Upbnd3Term> upt; std::vector<Avg3> avg; };
+      std::vector<Part> part(G.size());
+      pool_host.run((int)G.size(), [&](int n) { update_lists(G[n], XF, rx, ry, rz, part[n].upc, part[n].upt, part[n].avg); });
+      for (Part& q : part) {
+        const int base = (int)L.upt.size();
+        for (Upbnd3Cell c : q.upc) { c.first += base; L.upc.push_back(c); }
+        L.upt.insert(L.upt.end(), q.upt.begin(), q.upt.end());
+        L.avg.insert(L.avg.end(), q.avg.begin(), q.avg.end());
       }
     }
     L.avg_max = 0;
     for (const Avg3& a : L.avg) L.avg_max = std::max<long long>(L.avg_max, (long long)a.ni * a.nj * a.nk);
     L.d_upc.upload(L.upc, st, stg); L.d_upt.upload(L.upt, st, stg); L.d_avg.upload(L.avg, st, stg);
+  }
+  // update.f:4-192 and upbnd.f:4-94 for one coarse patch m: its register cells and the
+  // rectangles its kids average into
+  void update_lists(int m, const GridIndex& XF, int rx, int ry, int rz, std::vector<Upbnd3Cell>& upc, std::vector<Upbnd3Term>& upt,
+                    std::vector<Avg3>& avg) {
+    static const double chsign[7] = {0, 1., -1., -1., 1., 1., -1.};
+    const HPatch3& g = node[m];
+    if (g.has_cfl) {
+      // upbnd.f: the entries of one coarse cell in listbc order, each side at most once
+      // (the iused bit mask); cells are independent, so they are grouped by a sort
+      const int mi = mitot(m), mj = mjtot(m);
+      const size_t ne = g.listbc.size() / 6;
+      if (ne >= (1u << 24)) throw std::runtime_error("upbnd: too many register entries on one patch");
+      std::vector<unsigned long long> ord(ne);
+      for (size_t e = 0; e < ne; ++e) {
+        const int* b = &g.listbc[6 * e];
+        const unsigned long long key = ((unsigned long long)(b[2] - 1) * mj + (b[1] - 1)) * mi + (b[0] - 1);
+        ord[e] = (key << 24) | e;
+      }
+      std::sort(ord.begin(), ord.end());
+      for (size_t a0 = 0; a0 < ne;) {
+        const unsigned long long key = ord[a0] >> 24;
+        size_t a1 = a0;
+        while (a1 < ne && (ord[a1] >> 24) == key) ++a1;
+        Upbnd3Cell c{};
+        c.patch = m; c.ie = (int)(key % mi); c.je = (int)((key / mi) % mj); c.ke = (int)(key / ((unsigned long long)mi * mj));
+        c.first = (int)upt.size();
+        int used = 0;
+        for (size_t q = a0; q < a1; ++q) {
+          const int* b = &g.listbc[6 * (ord[q] & 0xffffff)];
+          const int side = b[3], norm = 1 << (side - 1);
+          if ((used / norm) % 2 == 1) continue;
+          upt.push_back(Upbnd3Term{node[b[4]].ffl + (long long)nvar * (b[5] - 1), chsign[side]});
+          used += norm;
+        }
+        c.count = (int)upt.size() - c.first;
+        upc.push_back(c);
+        a0 = a1;
+      }
+    }
+    std::vector<int> hits;
+    XF.query(g.ilo * rx, g.ihi * rx + rx - 1, g.jlo * ry, g.jhi * ry + ry - 1, g.klo * rz, g.khi * rz + rz - 1, hits);
+    for (int r : hits) {
+      const int kk = XF.id(r);
+      const HPatch3& f = node[kk];
+      const int iclo = f.ilo / rx, jclo = f.jlo / ry, kclo = f.klo / rz, ichi = f.ihi / rx, jchi = f.jhi / ry, kchi = f.khi / rz;
+      const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), kplo = std::max(g.klo, kclo);
+      const int iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi), kphi = std::min(g.khi, kchi);
+      if (iplo > iphi || jplo > jphi || kplo > kphi) continue;
+      Avg3 a{};
+      a.cpatch = m; a.kpatch = kk;
+      a.ci0 = iplo - g.ilo + G3; a.cj0 = jplo - g.jlo + G3; a.ck0 = kplo - g.klo + G3;
+      a.ni = iphi - iplo + 1; a.nj = jphi - jplo + 1; a.nk = kphi - kplo + 1;
+      a.fi0 = iplo * rx - f.ilo + G3; a.fj0 = jplo * ry - f.jlo + G3; a.fk0 = kplo * rz - f.klo + G3;
+      avg.push_back(a);
+    }
   }
 
   // prepf.f:4-41
@@ -868,12 +882,15 @@ class Amr3Gpu : public AmrSolver {
     listsp[lev] = maxsp;
     if (maxsp == 0) return;
     const GridIndex& XF = GI(lev + 1);
-    std::vector<int> hits;
     const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
-    for (int mp = lstart[lev]; mp != 0; mp = node[mp].levelptr) {
-      HPatch3& g = node[mp];
+    std::vector<int> parents;
+    for (int mp = lstart[lev]; mp != 0; mp = node[mp].levelptr) parents.push_back(mp);
+    // each parent's list depends only on its own box and the kids: built concurrently
+    pool_host.run((int)parents.size(), [&](int n) {
+      HPatch3& g = node[parents[n]];
       g.listbc.clear();
       g.has_cfl = true;
+      std::vector<int> hits;
       XF.query((g.ilo - 1) * rx, (g.ihi + 2) * rx - 1, (g.jlo - 1) * ry, (g.jhi + 2) * ry - 1, (g.klo - 1) * rz, (g.khi + 2) * rz - 1, hits);
       for (int r : hits) {
         const int k = XF.id(r);
@@ -883,7 +900,7 @@ class Amr3Gpu : public AmrSolver {
         const int iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi), kphi = std::min(g.khi, kchi);
         if ((iplo <= iphi + 1 && jplo <= jphi + 1) && kplo <= kphi + 1) setuse(g.listbc, k, g, iclo, ichi, jclo, jchi, kclo, kchi);
       }
-    }
+    });
   }
 
   void compile_all(int lbase = 0) {
@@ -933,8 +950,8 @@ class Amr3Gpu : public AmrSolver {
     tph.next("adv_launch");
     bound_level(lev, t);
     if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
-    if (lev > 1 && !L.qad.empty()) {
-      launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st);
+    if (lev > 1 && L.nseg > 0) {
+      launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.nseg, sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st);
       ++nkernels;
     }
     sample_gauges(lev);
@@ -969,8 +986,8 @@ class Amr3Gpu : public AmrSolver {
       launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
       ++nkernels;
     }
-    if (!L.fad.empty()) {
-      launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.fad.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
+    if (lev > 1 && L.nseg > 0) {
+      launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.nseg, nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
       ++nkernels;
     }
     flip_level(lev);
@@ -1080,8 +1097,8 @@ class Amr3Gpu : public AmrSolver {
   // flglvl.f:4-85 with domprep.f, domshrink.f, domup.f, domcopy.f, spest.f (+ flag2refine.f,
   // setflags.f), bufnst.f (+ projec.f, shiftset.f) and colate.f. The arrays live in device
   // memory; one read-back returns the flags (for the ordered point list) and the nesting
-  // domain (for nestck.f). Returns the points (i-.5, j-.5, k-.5) in (k, j, i) order.
-  void flglvl(int lcheck, int lbase, std::vector<double>& badpts, LvlView& dom) {
+  // domain (for nestck.f). Returns the flagged cells in (k, j, i) order.
+  void flglvl(int lcheck, int lbase, std::vector<FlagPt>& badpts, LvlView& dom) {
     PhaseTimer tph(hprof);
     tph.next("flg_device");
     const LvlDims d0{iregsz[lbase], jregsz[lbase], kregsz[lbase]};
@@ -1165,67 +1182,61 @@ class Amr3Gpu : public AmrSolver {
             std::memcpy(&w, row + i, 8);
             if (w == 0) { i += 8; continue; }
           }
-          if (row[i] != 0) { badpts.push_back((double)i - .5); badpts.push_back((double)j - .5); badpts.push_back((double)k - .5); }
+          if (row[i] != 0) badpts.push_back(FlagPt{{i, j, k}});
           ++i;
         }
       }
   }
 
-  // moment.f
-  static void moment(int rect[6], const double* bp, int npt, double& usage) {
-    double emx1 = bp[0], emn1 = emx1, emx2 = bp[1], emn2 = emx2, emx3 = bp[2], emn3 = emx3;
-    for (int q = 0; q < npt; ++q) {
-      const double* b = bp + 3 * q;
-      if (b[0] > emx1) emx1 = b[0];
-      if (b[0] < emn1) emn1 = b[0];
-      if (b[1] > emx2) emx2 = b[1];
-      if (b[1] < emn2) emn2 = b[1];
-      if (b[2] > emx3) emx3 = b[2];
-      if (b[2] < emn3) emn3 = b[2];
-    }
-    rect[0] = (int)std::lround(emn1 - .5); rect[1] = (int)std::lround(emx1 - .5);
-    rect[2] = (int)std::lround(emn2 - .5); rect[3] = (int)std::lround(emx2 - .5);
-    rect[4] = (int)std::lround(emn3 - .5); rect[5] = (int)std::lround(emx3 - .5);
+  // ---------------------------------------------------------------- clustering
+  // A flagged point of the reference is the cell centre (i-.5, j-.5, k-.5) in units of the
+  // level's cells (colate.f). The routines below keep the integer cell index instead; every
+  // comparison the reference makes on the centres is the same comparison on the indices
+  // (c - .5 < m - .5  <=>  c < m), and every decision depends only on the set of points in
+  // a cluster (histograms, minima, maxima, cut predicates), never on their order.
+
+  // moment.f:4-70: bounding box (rect: ilo, ihi, jlo, jhi, klo, khi, 0-based) and efficiency
+  static void moment(int rect[6], const FlagPt* p, int n, double& usage) {
+    int lo[3] = {p[0].c[0], p[0].c[1], p[0].c[2]}, hi[3] = {lo[0], lo[1], lo[2]};
+    for (int q = 1; q < n; ++q)
+      for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], p[q].c[d]); hi[d] = std::max(hi[d], p[q].c[d]); }
+    for (int d = 0; d < 3; ++d) { rect[2 * d] = lo[d] - 1; rect[2 * d + 1] = hi[d] - 1; }
     const int gpall = (rect[1] - rect[0] + 1) * (rect[3] - rect[2] + 1) * (rect[5] - rect[4] + 1);
-    usage = (double)npt / gpall;
+    usage = (double)n / gpall;
   }
-  // signs.f + findcut.f
-  static void findcut(const double* bp, int ist, int iend, int idim, int jdim, int kdim, int& index, int& iside) {
-    std::vector<int> iscr(idim + 2, 0), jscr(jdim + 2, 0), kscr(kdim + 2, 0);
-    int ilo = 1, ihi = idim, jlo = 1, jhi = jdim, klo = 1, khi = kdim;
-    for (int q = ist; q <= iend; ++q) {
-      const double* b = bp + 3 * (q - 1);
-      iscr[(int)(b[0] + 1.1)] += 1; jscr[(int)(b[1] + 1.1)] += 1; kscr[(int)(b[2] + 1.1)] += 1;
+  // signs.f + findcut.f: a hole in the signature, else the largest Laplacian sign change
+  static void findcut(const FlagPt* p, int n, const int dims[3], int& index, int& iside) {
+    std::vector<int> scr[3];
+    for (int d = 0; d < 3; ++d) scr[d].assign(dims[d] + 2, 0);
+    for (int q = 0; q < n; ++q)
+      for (int d = 0; d < 3; ++d) scr[d][p[q].c[d]] += 1;
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = 1; hi[d] = dims[d];
+      for (int t = 1; t <= dims[d]; ++t) if (scr[d][t] != 0) { lo[d] = t; break; }
+      for (int t = 1; t <= dims[d]; ++t) if (scr[d][dims[d] + 1 - t] != 0) { hi[d] = dims[d] + 1 - t; break; }
     }
-    for (int t = 1; t <= idim; ++t) if (iscr[t] != 0) { ilo = t; break; }
-    for (int t = 1; t <= idim; ++t) if (iscr[idim + 1 - t] != 0) { ihi = idim + 1 - t; break; }
-    for (int t = 1; t <= jdim; ++t) if (jscr[t] != 0) { jlo = t; break; }
-    for (int t = 1; t <= jdim; ++t) if (jscr[jdim + 1 - t] != 0) { jhi = jdim + 1 - t; break; }
-    for (int t = 1; t <= kdim; ++t) if (kscr[t] != 0) { klo = t; break; }
-    for (int t = 1; t <= kdim; ++t) if (kscr[kdim + 1 - t] != 0) { khi = kdim + 1 - t; break; }
-    for (int i = ilo; i <= ihi; ++i) if (iscr[i] == 0) { index = i; iside = 1; return; }
-    for (int j = jlo; j <= jhi; ++j) if (jscr[j] == 0) { index = j; iside = 2; return; }
-    for (int k = klo; k <= khi; ++k) if (kscr[k] == 0) { index = k; iside = 3; return; }
-    auto lap = [&](std::vector<int>& s, int lo, int hi, int& locmax, int& idx, int& mid) {
-      int pre = s[lo];
-      for (int i = lo + 1; i <= hi - 1; ++i) { const int cur = s[i]; s[i] = s[i + 1] - 2 * cur + pre; pre = cur; }
-      locmax = 0; idx = 0; mid = (lo + hi) / 2;
-      for (int i = lo + 2; i <= hi - 2 + 1; ++i) {
-        const int t1 = s[i - 1], t2 = s[i], d = std::abs(t1 - t2);
+    for (int d = 0; d < 3; ++d)
+      for (int t = lo[d]; t <= hi[d]; ++t)
+        if (scr[d][t] == 0) { index = t; iside = d + 1; return; }
+    auto lap = [&](std::vector<int>& sc, int l0, int h0, int& locmax, int& idx, int& mid) {
+      int pre = sc[l0];
+      for (int t = l0 + 1; t <= h0 - 1; ++t) { const int cur = sc[t]; sc[t] = sc[t + 1] - 2 * cur + pre; pre = cur; }
+      locmax = 0; idx = 0; mid = (l0 + h0) / 2;
+      for (int t = l0 + 2; t <= h0 - 2 + 1; ++t) {
+        const int t1 = sc[t - 1], t2 = sc[t], dd = std::abs(t1 - t2);
         if (t1 * t2 < 0) {
-          if (d > locmax) { locmax = d; idx = i; }
-          else if (d == locmax && std::abs(i - mid) < std::abs(idx - mid)) idx = i;
+          if (dd > locmax) { locmax = dd; idx = t; }
+          else if (dd == locmax && std::abs(t - mid) < std::abs(idx - mid)) idx = t;
         }
       }
     };
     int lv[3][4];
-    lap(iscr, ilo, ihi, lv[0][0], lv[0][2], lv[0][3]); lv[0][1] = 1;
-    lap(jscr, jlo, jhi, lv[1][0], lv[1][2], lv[1][3]); lv[1][1] = 2;
-    lap(kscr, klo, khi, lv[2][0], lv[2][2], lv[2][3]); lv[2][1] = 3;
+    for (int d = 0; d < 3; ++d) { lap(scr[d], lo[d], hi[d], lv[d][0], lv[d][2], lv[d][3]); lv[d][1] = d + 1; }
     for (int a = 0; a < 2; ++a)
       for (int b = a + 1; b < 3; ++b)
         if (lv[a][0] < lv[b][0]) for (int t = 0; t < 4; ++t) std::swap(lv[a][t], lv[b][t]);
-    int icount = (lv[0][0] > lv[1][0]) ? 1 : (lv[1][0] > lv[2][0]) ? 2 : 3;
+    const int icount = (lv[0][0] > lv[1][0]) ? 1 : (lv[1][0] > lv[2][0]) ? 2 : 3;
     if (icount != 1)
       for (int a = 0; a < icount - 1; ++a)
         for (int b = a + 1; b < icount; ++b)
@@ -1234,56 +1245,35 @@ class Amr3Gpu : public AmrSolver {
     iside = lv[0][1];
     if (lv[0][0] < 2) index = 0;
   }
-  // smartbis.f (numptc 1-based)
-  static void smartbis(std::vector<double>& bp, int npts, double cutoff, std::vector<int>& numptc, int& nclust, int idim, int jdim, int kdim) {
-    nclust = 1;
-    numptc.assign(2, 0);
-    numptc[1] = npts;
-    int icl = 1, ist = 1, iend = numptc[icl];
-    while (true) {
-      int rect[6]; double usenew;
-      moment(rect, bp.data() + 3 * (ist - 1), numptc[icl], usenew);
-      bool advance = (usenew >= cutoff);
-      int index = 0, iside = 0;
-      if (!advance) { findcut(bp.data(), ist, iend, idim, jdim, kdim, index, iside); if (index == 0) advance = true; }
-      if (advance) {
-        icl = icl + 1;
-        if (icl > nclust) break;
-        ist = iend + 1;
-        iend = ist + numptc[icl] - 1;
-        continue;
-      }
-      const double fmid = index - .5;
-      const int idir = iside;
-      auto c = [&](int q) { return bp[3 * (q - 1) + idir - 1]; };
-      auto swp = [&](int a, int b) { for (int d = 0; d < 3; ++d) std::swap(bp[3 * (a - 1) + d], bp[3 * (b - 1) + d]); };
-      int itop = ist - 1, ibot = iend + 1, i = ist;
-      while (true) {
-        if (c(i) < fmid) {
-          bool done = false;
-          while (true) {
-            ibot = ibot - 1;
-            if (c(ibot) < fmid) { if (ibot == i) { done = true; break; } continue; }
-            swp(ibot, i);
-            break;
-          }
-          if (done) break;
-          if (itop + 1 < ibot) continue;
-          break;
-        } else {
-          itop = itop + 1;
-          if (itop + 1 >= ibot) break;
-          i = i + 1;
-        }
-      }
-      numptc[icl] = itop - ist + 1;
-      numptc.insert(numptc.begin() + icl + 1, iend - ibot + 1);
-      nclust = nclust + 1;
-      iend = itop;
+  // smartbis.f: bisect until every cluster's efficiency reaches cutoff or it has no cut.
+  // The reference keeps the cluster at or above the cut first (smartbis.f swaps the
+  // points below it to the bottom), so clusters come out in depth-first order, upper part
+  // first. Large independent halves are clustered on other threads.
+  static void smartbis_rec(FlagPt* p, int n, double cutoff, const int dims[3], std::vector<int>& counts, int depth) {
+    int rect[6];
+    double usenew;
+    moment(rect, p, n, usenew);
+    int index = 0, iside = 0;
+    if (usenew < cutoff) findcut(p, n, dims, index, iside);
+    if (usenew >= cutoff || index == 0) { counts.push_back(n); return; }
+    const int d = iside - 1;
+    FlagPt* mid = std::partition(p, p + n, [&](const FlagPt& q) { return q.c[d] >= index; });
+    const int n1 = (int)(mid - p);
+    if (depth < 4 && n > 20000) {
+      std::vector<int> right;
+      auto fut = std::async(std::launch::async, [&] { smartbis_rec(mid, n - n1, cutoff, dims, right, depth + 1); });
+      smartbis_rec(p, n1, cutoff, dims, counts, depth + 1);
+      fut.get();
+      counts.insert(counts.end(), right.begin(), right.end());
+    } else {
+      smartbis_rec(p, n1, cutoff, dims, counts, depth + 1);
+      smartbis_rec(mid, n - n1, cutoff, dims, counts, depth + 1);
     }
   }
-  // nestck.f
-  bool nestck(int mnew, int lbase, std::vector<double>& bp, int ibase, int npts, std::vector<int>& numptc, int icl, int& nclust, const LvlView& dom) {
+  // nestck.f: a new grid must lie in the nesting domain of its base; otherwise split its
+  // points at the middle of its longest side (points below the middle first) and retry
+  bool nestck(int mnew, int lbase, std::vector<FlagPt>& bp, int ibase, int npts, std::vector<int>& numptc, int icl, int& nclust,
+              const LvlView& dom) {
     if (lbase == 1) return true;
     const HPatch3& n = node[mnew];
     const int lev = n.level;
@@ -1297,19 +1287,12 @@ class Amr3Gpu : public AmrSolver {
     if (npts <= 1) throw std::runtime_error("nestck: a single point cannot be properly nested");
     double sidemx = std::max(n.xhi - n.xlo, n.yhi - n.ylo);
     sidemx = std::max(sidemx, n.zhi - n.zlo);
-    double rmid; int idir;
-    if (n.xhi - n.xlo >= sidemx) { rmid = (double)(float)((n.ihi + n.ilo + 1) / 2.f); rmid = rmid / rx; idir = 1; }
-    else if (n.yhi - n.ylo >= sidemx) { rmid = (double)(float)((n.jhi + n.jlo + 1) / 2.f); rmid = rmid / ry; idir = 2; }
-    else { rmid = (double)(float)((n.khi + n.klo + 1) / 2.f); rmid = rmid / rz; idir = 3; }
-    auto c = [&](int q) { return bp[3 * (ibase + q - 1) + idir - 1]; };
-    int ipt = 1, ntop = npts;
-    while (true) {
-      if (c(ipt) < rmid) { ipt = ipt + 1; if (ipt <= ntop) continue; break; }
-      for (int d = 0; d < 3; ++d) std::swap(bp[3 * (ibase + ipt - 1) + d], bp[3 * (ibase + ntop - 1) + d]);
-      ntop = ntop - 1;
-      if (ipt <= ntop) continue;
-      break;
-    }
+    double rmid; int d;
+    if (n.xhi - n.xlo >= sidemx) { rmid = (double)(float)((n.ihi + n.ilo + 1) / 2.f); rmid = rmid / rx; d = 0; }
+    else if (n.yhi - n.ylo >= sidemx) { rmid = (double)(float)((n.jhi + n.jlo + 1) / 2.f); rmid = rmid / ry; d = 1; }
+    else { rmid = (double)(float)((n.khi + n.klo + 1) / 2.f); rmid = rmid / rz; d = 2; }
+    FlagPt* p = bp.data() + ibase;
+    const int ntop = (int)(std::partition(p, p + npts, [&](const FlagPt& q) { return (double)q.c[d] - .5 < rmid; }) - p);
     numptc[icl] = ntop;
     numptc.insert(numptc.begin() + icl + 1, npts - ntop);
     nclust = nclust + 1;
@@ -1317,26 +1300,29 @@ class Amr3Gpu : public AmrSolver {
   }
   // grdfit.f
   void grdfit(int lbase, int lcheck, double t) {
-    std::vector<double> bp;
+    std::vector<FlagPt> bp;
     LvlView i1flags{nullptr, LvlDims{0, 0, 0}};
     {
       HPROF("flglvl3");
       flglvl(lcheck, lbase, bp, i1flags);
     }
-    const int npts = (int)bp.size() / 3;
+    const int npts = (int)bp.size();
     if (npts == 0) return;
     HPROF("cluster3");
     const int levnew = lcheck + 1;
     const double hxf = hxposs[levnew], hyf = hyposs[levnew], hzf = hzposs[levnew];
-    std::vector<int> numptc;
-    int nclust = 0;
-    smartbis(bp, npts, p.cut, numptc, nclust, iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]);
+    std::vector<int> counts;
+    const int dims[3] = {iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]};
+    smartbis_rec(bp.data(), npts, p.cut, dims, counts, 0);
+    std::vector<int> numptc(1, 0);  // 1-based as in the reference
+    numptc.insert(numptc.end(), counts.begin(), counts.end());
+    int nclust = (int)counts.size();
     int ibase = 0, icl = 1, prv = 0;
     while (icl <= nclust) {
       const int mnew = nodget();
       while (true) {
         int rect[6]; double usage;
-        moment(rect, bp.data() + 3 * ibase, numptc[icl], usage);
+        moment(rect, bp.data() + ibase, numptc[icl], usage);
         HPatch3& n = node[mnew];
         n.ilo = rect[0] * intratx[lcheck]; n.jlo = rect[2] * intraty[lcheck]; n.klo = rect[4] * intratz[lcheck];
         n.ihi = (rect[1] + 1) * intratx[lcheck] - 1; n.jhi = (rect[3] + 1) * intraty[lcheck] - 1; n.khi = (rect[5] + 1) * intratz[lcheck] - 1;

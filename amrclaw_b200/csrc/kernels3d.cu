@@ -872,6 +872,30 @@ __global__ void gather3_kernel(const double* pool, const PatchDev* patches, cons
   }
 }
 
+// fluxad.f / qad.f work lists of a level, from the per-patch segment prefix: segment
+// seg of a fine patch is (side, ac, bc) in cstore.f's order (sides 1..6, ac fastest)
+__global__ void expand_fadqad3_kernel(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry,
+                                      int rz, long long total, Fad3* fad, Qad3Job* qad) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(pre, np, t);
+    const int m = plist[pi];
+    const PatchDev& P = patches[m];
+    const int nxc = (P.ihi - P.ilo + 1) / rx, nyc = (P.jhi - P.jlo + 1) / ry, nzc = (P.khi - P.klo + 1) / rz;
+    const int seg = (int)(t - pre[pi]);
+    const int cnt[6] = {nyc * nzc, nxc * nzc, nyc * nzc, nxc * nzc, nxc * nyc, nxc * nyc};
+    const int nas[6] = {nyc, nxc, nyc, nxc, nxc, nxc};
+    const int ras[6] = {ry, rx, ry, rx, rx, rx}, rbs[6] = {rz, rz, rz, rz, ry, ry};
+    int side = 0, r = seg;
+    while (side < 5 && r >= cnt[side]) { r -= cnt[side]; ++side; }
+    const int ac = r % nas[side], bc = r / nas[side];
+    const int ra = ras[side], rb = rbs[side];
+    fad[t] = Fad3{m, pi, side + 1, ac * ra, bc * rb, ra, rb, seg};
+    Qad3Job q;
+    q.patch = m; q.side = side + 1; q.slab = bc; q.row0 = ac * ra; q.nreg = 1; q.reg0 = seg; q.ratio_a = ra; q.ratio_b = rb;
+    qad[t] = q;
+  }
+}
+
 int grid_for(long long n, int block) {
   const long long g = (n + block - 1) / block;
   return (int)std::max<long long>(1, std::min<long long>(g, 148LL * 64));
@@ -887,6 +911,13 @@ void launch_step3(const Step3Args& a, const long long items[3], long long faces,
   AMR_CUDA(cudaGetLastError());
   if (faces > 0) face3_kernel<<<grid_for(faces, 128), 128, 0, s>>>(a);
   if (cells > 0) update3_kernel<<<grid_for(cells, 256), 256, 0, s>>>(a);
+  AMR_CUDA(cudaGetLastError());
+}
+
+void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,
+                           long long total, Fad3* fad, Qad3Job* qad, cudaStream_t s) {
+  if (total <= 0) return;
+  expand_fadqad3_kernel<<<grid_for(total, 256), 256, 0, s>>>(plist, pre, np, patches, rx, ry, rz, total, fad, qad);
   AMR_CUDA(cudaGetLastError());
 }
 

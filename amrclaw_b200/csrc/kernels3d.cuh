@@ -83,6 +83,10 @@ struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff;
 
 // interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction
 void launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s);
+// Builds the level's fluxad/qad work lists on the device: pre[np+1] is the prefix of the
+// register segments (lenbc) of the patches in plist (0 for patches without registers).
+void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,
+                           long long total, Fad3* fad, Qad3Job* qad, cudaStream_t s);
 void launch_fsv3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
                  const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s);
 void launch_fad3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
