@@ -336,11 +336,12 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
 template <class S>
 static void launch_step2_t(const StepArgs& a, int grid, cudaStream_t s) {
   const size_t sm = sizeof(double) * Step2Layout<S>::TOTAL;
-  static bool attr = false;
-  if (!attr) {
+  // once per process (thread-safe static initialisation; contexts may run on several host threads)
+  static const bool attr = [&] {
     AMR_CUDA(cudaFuncSetAttribute(step2_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    attr = true;
-  }
+    return true;
+  }();
+  (void)attr;
   if (grid <= 0) return;
   step2_kernel<S><<<grid, STEP2_THREADS, sm, s>>>(a);
   AMR_CUDA(cudaGetLastError());

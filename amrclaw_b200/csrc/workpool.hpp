@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <cstdlib>
 #include <exception>
 #include <functional>
 #include <mutex>
@@ -15,8 +16,15 @@ namespace amrb {
 
 class WorkPool {
  public:
+  // nthreads <= 0: AMRGPU_HOST_THREADS if set (a server running many contexts lowers it),
+  // else up to 16 hardware threads
   explicit WorkPool(int nthreads = 0) {
+    if (nthreads <= 0) {
+      const char* e = std::getenv("AMRGPU_HOST_THREADS");
+      nthreads = e ? std::atoi(e) : 0;
+    }
     if (nthreads <= 0) nthreads = (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+    nthreads = std::min(nthreads, 64);
     for (int t = 1; t < nthreads; ++t) workers_.emplace_back([this] { loop(); });
   }
   ~WorkPool() {

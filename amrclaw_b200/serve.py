@@ -1,0 +1,210 @@
+"""Serving loop: independent AMR solves admitted by HBM budget, run concurrently.
+
+Each admitted request gets its own context (device pool, CUDA stream) driven by its own
+host thread; the C library releases the interpreter while it works, so the level steps
+of all admitted solves are in flight on the device together and overlap there. A
+request waits in arrival order until both a slot and its estimated device memory are
+free; finished solves release both. Latency is completion time minus arrival time.
+
+    python -m amrclaw_b200.serve [--requests N] [--rate R] [--budget-gb G] [--slots S] [--scale small|full]
+
+prints one JSON line: p50/p99 latency, aggregate cell-updates/s, makespan, admissions.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional
+
+import numpy as np
+
+from . import problems
+from .replicas import percentiles
+
+KINDS = ("advection", "euler", "acoustics")
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float          # seconds after the start of the stream
+    kind: str               # advection | euler | acoustics
+    n: int                  # base grid n x n
+    levels: int
+    ratio: int
+    tfinal: float
+    precision: str          # "fp64" (the FP32 form is requested as "fp32")
+    params: dict = field(default_factory=dict)
+
+    def rundata(self):
+        if self.kind == "advection":
+            return problems.advection_square(self.n, self.levels, self.ratio, self.tfinal, **self.params)
+        if self.kind == "euler":
+            return problems.euler_quadrants(self.n, self.levels, self.ratio, self.tfinal, **self.params)
+        return problems.acoustics_pulse(self.n, self.levels, self.ratio, self.tfinal, **self.params)
+
+    def nvar(self) -> int:
+        return {"advection": 1, "euler": 4, "acoustics": 3}[self.kind]
+
+    def est_bytes(self) -> int:
+        """Device memory reserved for admission: the context's initial pool (two buffers of
+        every level's worth of base grid, as the library sizes it), registers and scratch."""
+        pool = 8 * (self.nvar() * (self.n + 4) ** 2 * 8 * self.levels + (1 << 22))
+        return int(pool + (24 << 20))
+
+
+def synthetic_requests(n: int = 512, rate: float = 200.0, seed: int = 1, scale: str = "small") -> List[Request]:
+    """A seeded Poisson stream of independent solves.
+
+    scale "full": base grids 32^2-256^2 (log-uniform), 2-4 levels, ratio 2 or 4, final
+    times 0.1-1.0 (the serving configuration as stated). scale "small": 32^2-96^2, 2-3
+    levels, ratio 2, final times 0.05-0.2, for runs that finish in seconds. Problems are
+    drawn uniformly from advection, Euler quadrants and acoustics, each with a seeded
+    perturbation of its parameters; precision is fp64/fp32 with equal odds."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for rid in range(n):
+        t += rng.exponential(1.0 / rate)
+        kind = KINDS[int(rng.integers(0, 3))]
+        if scale == "full":
+            nb = int(round(math.exp(rng.uniform(math.log(32), math.log(256))) / 2)) * 2
+            levels = int(rng.integers(2, 5)); ratio = int(rng.choice([2, 4])); tfinal = float(rng.uniform(0.1, 1.0))
+        else:
+            nb = int(round(math.exp(rng.uniform(math.log(32), math.log(96))) / 2)) * 2
+            levels = int(rng.integers(2, 4)); ratio = 2; tfinal = float(rng.uniform(0.05, 0.2))
+        prec = "fp32" if rng.uniform() < 0.5 else "fp64"
+        if kind == "advection":
+            x0 = float(rng.uniform(0.05, 0.3)); y0 = float(rng.uniform(0.05, 0.3))
+            params = dict(u=float(rng.uniform(0.3, 0.7)), v=float(rng.uniform(0.7, 1.2)), x0=x0, x1=x0 + 0.4, y0=y0, y1=y0 + 0.4)
+        elif kind == "euler":
+            params = dict(xs=float(rng.uniform(0.6, 0.85)), ys=float(rng.uniform(0.6, 0.85)))
+        else:
+            params = dict(r0=float(rng.uniform(0.2, 0.4)), width=float(rng.uniform(0.04, 0.08)))
+        out.append(Request(rid, t, kind, nb, levels, ratio, tfinal, prec, params))
+    return out
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    done: float
+    cell_updates: float
+    mass: float
+    values: Optional[np.ndarray]
+    device_ms: float
+    pool_peak_bytes: float
+    error: Optional[str] = None
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def run_one(req: Request, keep_values: bool = False):
+    """One solve from start to tfinal on the current device: (cell updates, mass, values, device ms, pool peak)."""
+    from . import Solver
+    with Solver(req.rundata(), batched=True) as s:
+        s.run(0)
+        inf = s.info()
+        vals = s.values() if keep_values else None
+        return inf["cell_updates"], s.mass(), vals, inf["last_run_ms"], inf["pool_peak_bytes"]
+
+
+def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: bool = False,
+          clock: Callable[[], float] = time.perf_counter, runner: Optional[Callable] = None) -> dict:
+    """Admit the requests as they arrive (arrival times relative to the call), run them
+    concurrently, return the per-request results and the summary. `runner(req, keep_values)`
+    performs one solve (default run_one: the FP64 device path for every request)."""
+    runner = runner or run_one
+    pending = sorted(requests, key=lambda r: r.arrival)
+    waiting: List[Request] = []
+    results: List[Result] = []
+    lock = threading.Condition()
+    state = {"used": 0, "active": 0, "peak_active": 0, "peak_used": 0}
+    t0 = clock()
+
+    def worker(req: Request, admitted: float, est: int):
+        err = None
+        cells = mass = dev_ms = peak = 0.0
+        vals = None
+        try:
+            cells, mass, vals, dev_ms, peak = runner(req, keep_values)
+        except Exception as e:  # reported per request; the server keeps going
+            err = str(e)
+        done = clock() - t0
+        with lock:
+            results.append(Result(req.rid, req.arrival, admitted, done, cells, mass, vals, dev_ms, peak, err))
+            state["used"] -= est
+            state["active"] -= 1
+            lock.notify_all()
+
+    threads = []
+    with lock:
+        while pending or waiting or state["active"]:
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(pending.pop(0))
+            # FIFO admission: the oldest waiting request first, while slot and memory allow
+            while waiting and state["active"] < slots:
+                est = waiting[0].est_bytes()
+                if state["used"] + est > budget_bytes and state["active"] > 0:
+                    break
+                req = waiting.pop(0)
+                state["used"] += est
+                state["active"] += 1
+                state["peak_active"] = max(state["peak_active"], state["active"])
+                state["peak_used"] = max(state["peak_used"], state["used"])
+                th = threading.Thread(target=worker, args=(req, now, est), daemon=True)
+                th.start()
+                threads.append(th)
+            wait = 0.05
+            if pending:
+                wait = max(0.0, min(wait, pending[0].arrival - (clock() - t0)))
+            lock.wait(timeout=wait)
+    for th in threads:
+        th.join()
+    makespan = clock() - t0
+    ok = [r for r in results if r.error is None]
+    lat = [r.latency for r in ok]
+    p50, p99 = percentiles(lat, (50, 99))
+    cells = sum(r.cell_updates for r in ok)
+    summary = {
+        "requests": len(requests), "completed": len(ok), "failed": len(results) - len(ok),
+        "p50_latency_ms": 1e3 * p50, "p99_latency_ms": 1e3 * p99, "makespan_s": makespan,
+        "cell_updates": cells, "throughput_cell_updates_per_s": cells / makespan if makespan > 0 else 0.0,
+        "peak_concurrent": state["peak_active"], "peak_reserved_bytes": state["peak_used"],
+        "budget_bytes": budget_bytes, "slots": slots,
+        "fp32_requests": sum(1 for r in requests if r.precision == "fp32"),
+        "fp32_form": "not built: fp32 requests run on the fp64 path",
+    }
+    return {"summary": summary, "results": sorted(results, key=lambda r: r.rid)}
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--scale", default="small", choices=["small", "full"])
+    ap.add_argument("--budget-gb", type=float, default=16.0)
+    ap.add_argument("--slots", type=int, default=16)
+    args = ap.parse_args(argv)
+    os.environ.setdefault("AMRGPU_HOST_THREADS", "2")
+    reqs = synthetic_requests(args.requests, args.rate, args.seed, args.scale)
+    out = serve(reqs, int(args.budget_gb * (1 << 30)), args.slots)
+    s = out["summary"]
+    s.update({"scale": args.scale, "rate_per_s": args.rate, "seed": args.seed,
+              "mix": {k: sum(1 for r in reqs if r.kind == k) for k in KINDS}})
+    print(json.dumps(s), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -168,7 +168,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    from amrclaw_b200 import Solver
+    from amrclaw_b200 import Solver, replicas
     rd, cfg, nvar, naux, ndim = workload(args.workload)
     bytes_per_update = (2 * nvar + naux) * 8
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
@@ -199,13 +199,7 @@ def main():
         clk = clocks.stop()
         i1 = s.info()
         s.close()
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-            c = torch.tensor([cells], device="cuda", dtype=torch.float64)
-            dist.all_reduce(c)
-            cells = float(c.item())
+        ms, cells = replicas.combine(ms, cells, dist, device="cuda")
         value = cells / (ms * 1e-3)
         kern_ms = i1["step_kernel_ms"] - i0["step_kernel_ms"]
         kern_cells = i1["step_kernel_cells"] - i0["step_kernel_cells"]
