@@ -32,7 +32,8 @@ def _check(lib, rc: int, what: str) -> None:
 class Solver:
     """One AMR run on the GPU (the reference's ``amr2`` program from init to tfinal)."""
 
-    def __init__(self, rundata_or_dir, outdir: str | None = None, write_output: bool = False, batched: bool = True):
+    def __init__(self, rundata_or_dir, outdir: str | None = None, write_output: bool = False, batched: bool = True,
+                 precision: str = "fp64"):
         self._lib = _lib.load()
         if isinstance(rundata_or_dir, ClawRunData):
             self._tmp = tempfile.TemporaryDirectory(prefix="amrgpu_")
@@ -44,8 +45,12 @@ class Solver:
         self.outdir = outdir or rundir
         if write_output:
             os.makedirs(self.outdir, exist_ok=True)
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.precision = precision
         h = ctypes.c_void_p()
-        _check(self._lib, self._lib.amrgpu_init(rundir.encode(), self.outdir.encode(), int(write_output), ctypes.byref(h)),
+        _check(self._lib, self._lib.amrgpu_init_precision(rundir.encode(), self.outdir.encode(), int(write_output),
+                                                          64 if precision == "fp64" else 32, ctypes.byref(h)),
                "amrgpu_init")
         self._h = h
         self.set_batched(batched)
@@ -92,7 +97,7 @@ class Solver:
                 "cflmax", "kernels", "pool_peak_bytes", "substeps", "step_kernel_ms", "step_kernel_cells",
                 "last_run_ms", "last_run_cells", "finished", "h2d_bytes",
                 "regrid_flags_s", "regrid_hostflags_s", "regrid_cluster_s", "regrid_fill_s", "regrid_prep_s", "regrid_compile_s",
-                "num_dim"]
+                "num_dim", "precision_bits"]
         out = (ctypes.c_double * len(keys))()
         _check(self._lib, self._lib.amrgpu_info(self._h, out, len(keys)), "amrgpu_info")
         return dict(zip(keys, list(out)))

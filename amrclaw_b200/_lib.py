@@ -15,6 +15,8 @@ c_ll_p = ctypes.POINTER(ctypes.c_longlong)
 SIGNATURES = {
     "amrgpu_last_error": (ctypes.c_char_p, []),
     "amrgpu_init": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "amrgpu_init_precision": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_void_p)]),
     "amrgpu_set_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "amrgpu_set_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "amrgpu_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -60,12 +60,15 @@ struct FillProg {
   std::vector<int> bc_stage;
   int nstages = 0;
   long long scratch_off = -1, scratch_len = 0, scratch_alloc = 0;
+  // the scratch starts at zero each run: programs whose rects come from icall copies
+  // (saveqc.f, filval.f90) leave uncovered cells at the reference's initial 0
+  bool zero_scratch = false;
   DBuf<ScratchRect> d_rects;
   DBuf<FillOp> d_ops;
   DBuf<FillChunk> d_chunks;
   DBuf<BcOp> d_bcs;
   std::vector<int> ch_lo, ch_hi, bc_lo, bc_hi;
-  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; }
+  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; zero_scratch = false; }
   int add_rect(int ni, int nj, int nvar) {
     ScratchRect r;
     r.off = scratch_len; r.ni = ni; r.nj = nj;
@@ -142,6 +145,10 @@ class Amr2Gpu {
   // run state
   double time = 0, start_time = 0;
   int ncycle = 0;
+#ifdef AMRB_DEBUG_HOOKS
+  struct DebugStop {};
+  int dbg_stop = 0, dbg_count = 0;
+#endif
   double rvol = 0, rvoll[12] = {0};
   double cfl_level = 0, cflmax_run = 0;
   double tmass0 = 0;
@@ -275,17 +282,27 @@ class Amr2Gpu {
   int mitot(int m) const { return node[m].nx() + 2 * ng; }
   int mjtot(int m) const { return node[m].ny() + 2 * ng; }
 
+  // Patch pool offsets count elements of the storage type: doubles, or floats in the FP32
+  // form (two per pool double; the pool's 32-double rounding keeps them 256-byte aligned).
+  bool f32 = false;
+  long long palloc(long long n) { return f32 ? pool.alloc((n + 1) / 2) * 2 : pool.alloc(n); }
+  void pfree(long long off, long long n) {
+    if (off < 0) return;
+    if (f32) pool.release(off / 2, (n + 1) / 2); else pool.release(off, n);
+  }
+  size_t elem() const { return f32 ? sizeof(float) : sizeof(double); }
+
   void alloc_patch(int m) {
     id_hwm = std::max(id_hwm, m + 1);
     HPatch& g = node[m];
     g.nq = (long long)nvar * mitot(m) * mjtot(m);
-    g.q0 = pool.alloc(g.nq);
-    g.q1 = pool.alloc(g.nq);
+    g.q0 = palloc(g.nq);
+    g.q1 = palloc(g.nq);
     g.cur = 0;
   }
   void free_patch(int m) {
     HPatch& g = node[m];
-    pool.release(g.q0, g.nq); pool.release(g.q1, g.nq);
+    pfree(g.q0, g.nq); pfree(g.q1, g.nq);
     g.q0 = g.q1 = -1;
     if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
     g.ffl = -1;
@@ -637,6 +654,7 @@ class Amr2Gpu {
     HPROF("compile_saveqc");
     FillProg& P = plan[lev].saveqc;
     P.clear();
+    P.zero_scratch = true;
     P.scratch_len = 0;
     if (lev + 1 > p.mxnest || lstart[lev + 1] == 0) { upload_prog(P); return; }
     const double hxc = hxposs[lev], hyc = hyposs[lev];
@@ -662,9 +680,9 @@ class Amr2Gpu {
 
   void upload_prog(FillProg& P) {
     HPROF("upload_prog");
-    if (P.scratch_off >= 0) pool.release(P.scratch_off, P.scratch_alloc);
+    if (P.scratch_off >= 0) pfree(P.scratch_off, P.scratch_alloc);
     P.scratch_alloc = std::max<long long>(P.scratch_len, 1);
-    P.scratch_off = pool.alloc(P.scratch_alloc);
+    P.scratch_off = palloc(P.scratch_alloc);
     std::vector<ScratchRect> rects = P.rects;
     for (auto& r : rects) r.off += P.scratch_off;
     P.d_rects.upload(rects, st, stg);
@@ -705,21 +723,23 @@ class Amr2Gpu {
   }
 
   void run_prog(FillProg& P, const SrcMode& modes) {
+    if (P.zero_scratch && P.scratch_len > 0 && P.nstages > 0)
+      AMR_CUDA(cudaMemsetAsync(reinterpret_cast<char*>(pool.d) + elem() * P.scratch_off, 0, elem() * P.scratch_len, st));
     for (int s = 0; s < P.nstages; ++s) {
       if (P.ch_hi[s] > P.ch_lo[s]) {
         FillArgs a{};
         a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
         a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
         a.lc = lc; a.xlower = xlower; a.ylower = ylower;
-        launch_fill(a, st);
+        launch_fill(a, st, f32);
         ++nkernels;
       }
       if (P.bc_hi[s] > P.bc_lo[s]) {
         BcArgs b{};
         b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.bc_lo[s];
         b.nops = P.bc_hi[s] - P.bc_lo[s]; b.nvar = nvar;
-        launch_bc(b, 0, st);
-        launch_bc(b, 1, st);
+        launch_bc(b, 0, st, f32);
+        launch_bc(b, 1, st, f32);
         nkernels += 2;
       }
     }
@@ -997,7 +1017,7 @@ class Amr2Gpu {
     bound_level(lev, t);
     if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
     if (lev > 1 && !L.qad.empty()) {
-      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st);
+      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st, f32);
       ++nkernels;
     }
     // gauges (gauges_module.f90:313-452): sampled before the step on the finest covering grid
@@ -1028,7 +1048,7 @@ class Amr2Gpu {
           d_gauge_out.free(); d_gauge_out = nb;
         }
         DBuf<GaugeJob> dj; dj.upload(jobs, st, stg);
-        launch_gauges2(pool.d, d_patches.d, dj.d, (int)jobs.size(), nvar, d_gauge_out.d, st);
+        launch_gauges2(pool.d, d_patches.d, dj.d, (int)jobs.size(), nvar, d_gauge_out.d, st, f32);
         sync_stream();
         dj.free();
       }
@@ -1041,14 +1061,14 @@ class Amr2Gpu {
     a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
     if (batched) {
       a.work = L.d_work.d; a.nwork = (int)L.work.size(); a.queue = nullptr;
-      launch_step2(prob.solver, a, (int)L.work.size(), st);
+      launch_step2(prob.solver, a, (int)L.work.size(), st, f32);
       ++nkernels;
     } else {
       for (size_t k = 0; k < L.plist.size(); ++k) {
         a.work = L.d_work.d + L.patch_work_lo[k];
         a.nwork = L.patch_work_hi[k] - L.patch_work_lo[k];
         a.queue = nullptr;
-        launch_step2(prob.solver, a, a.nwork, st);
+        launch_step2(prob.solver, a, a.nwork, st, f32);
         ++nkernels;
       }
     }
@@ -1085,6 +1105,8 @@ class Amr2Gpu {
   // scratch rects in the fixed device array (noalloc2d.cu); no gauge sampling, no
   // profiling events, no host timers. Returns dtnew like advanc.
   void run_prog_fixed(FillProg& P, const SrcMode& modes, const double* scratch) {
+    if (P.zero_scratch && P.scratch_len > 0 && P.nstages > 0)
+      AMR_CUDA(cudaMemsetAsync(const_cast<double*>(scratch), 0, sizeof(double) * P.scratch_len, st));
     for (int s = 0; s < P.nstages; ++s) {
       if (P.ch_hi[s] > P.ch_lo[s]) {
         FillArgs a{};
@@ -1117,7 +1139,7 @@ class Amr2Gpu {
     run_prog_fixed(L.bound, M, scratch);
     if (kids) { SrcMode Z{}; run_prog_fixed(L.saveqc, Z, scratch); }
     if (lev > 1 && !L.qad.empty()) {
-      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st);
+      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st, f32);
       ++nkernels;
     }
     AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
@@ -1125,7 +1147,7 @@ class Amr2Gpu {
     a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.fsv = L.d_fsv.d; a.fad = L.d_fad.d;
     a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
     a.work = L.d_work.d; a.nwork = (int)L.work.size(); a.queue = nullptr;
-    launch_step2(prob.solver, a, (int)L.work.size(), st);
+    launch_step2(prob.solver, a, (int)L.work.size(), st, f32);
     launch_flip(d_patches.d, L.d_plist.d, (int)L.plist.size(), st);
     nkernels += 2;
     unsigned long long cbits = 0;
@@ -1149,8 +1171,8 @@ class Amr2Gpu {
     HPROF("update");
     LevelPlan& L = plan[lev];
     const double area = hxposs[lev] * hyposs[lev];
-    launch_upbnd(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, area, nvar, st);
-    launch_average(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), intratx[lev], intraty[lev], nvar, st);
+    launch_upbnd(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, area, nvar, st, f32);
+    launch_average(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), intratx[lev], intraty[lev], nvar, st, f32);
     nkernels += 2;
   }
 
@@ -1319,7 +1341,7 @@ class Amr2Gpu {
     DBuf<int8_t>& dout = fl_out; dout.ensure(std::max<long long>(off.back(), 1));
     DBuf<long long>& doff = fl_off; doff.upload(off, st, stg);
     DBuf<int>& dpl = fl_pl; dpl.upload(G, st, stg);
-    launch_flags2(pool.d, d_patches.d, dpl.d, doff.d, (int)G.size(), use_old, p.flag_component, p.tolsp, nvar, dout.d, st);
+    launch_flags2(pool.d, d_patches.d, dpl.d, doff.d, (int)G.size(), use_old, p.flag_component, p.tolsp, nvar, dout.d, st, f32);
     std::vector<int8_t> hflag(off.back());
     if (off.back()) AMR_CUDA(cudaMemcpyAsync(hflag.data(), dout.d, off.back(), cudaMemcpyDeviceToHost, st));
     sync_stream();
@@ -1527,6 +1549,7 @@ class Amr2Gpu {
     HPROF("fill_new_level");
     FillProg& P = newfill;
     P.clear();
+    P.zero_scratch = true;
     P.rects.clear();
     P.scratch_len = 0;
     GI(lev - 1); GI(lev);
@@ -1539,7 +1562,7 @@ class Amr2Gpu {
     SrcMode M{};
     run_prog(P, M);
     sync_stream();
-    pool.release(P.scratch_off, P.scratch_alloc);
+    pfree(P.scratch_off, P.scratch_alloc);
     P.scratch_off = -1;
   }
   // filval.f90 for new patch m: coarse values around it, then copies from the old grids
@@ -1765,9 +1788,16 @@ class Amr2Gpu {
       g.time = t;
       std::vector<double> q;
       qinit(g.nx(), g.ny(), g.xlo, g.ylo, hxposs[g.level], hyposs[g.level], q);
-      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q0, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
-      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q1, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
-      h2d_bytes += 2.0 * sizeof(double) * q.size();
+      std::vector<float> qf;
+      const void* src = q.data();
+      if (f32) {  // the FP32 form stores the initial values rounded to float
+        qf.assign(q.begin(), q.end());
+        src = qf.data();
+      }
+      char* base = reinterpret_cast<char*>(pool.d);
+      AMR_CUDA(cudaMemcpyAsync(base + elem() * g.q0, src, elem() * q.size(), cudaMemcpyHostToDevice, st));
+      AMR_CUDA(cudaMemcpyAsync(base + elem() * g.q1, src, elem() * q.size(), cudaMemcpyHostToDevice, st));
+      h2d_bytes += 2.0 * elem() * q.size();
       sync_stream();
     }
   }
@@ -1785,7 +1815,7 @@ class Amr2Gpu {
 
   double mass() {
     AMR_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double), st));
-    launch_mass2(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st);
+    launch_mass2(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st, f32);
     double m = 0;
     AMR_CUDA(cudaMemcpyAsync(&m, d_mass, sizeof(double), cudaMemcpyDeviceToHost, st));
     sync_stream();
@@ -1839,6 +1869,9 @@ class Amr2Gpu {
           for (int i = lbase + 1; i <= lfine; ++i) tlevel[i] = tlevel[lbase];
         }
         const double dtl = advanc(level);
+#ifdef AMRB_DEBUG_HOOKS
+        if (dbg_stop > 0 && ++dbg_count >= dbg_stop) throw DebugStop();
+#endif
         ntogo[level] -= 1;
         dtnew[level] = std::min(dtnew[level], dtl);
         tlevel[level] = tlevel[level] + possk[level];
@@ -1903,7 +1936,7 @@ class Amr2Gpu {
     DBuf<double> d; d.ensure(tot);
     DBuf<int> dp; dp.upload(pl, st, stg);
     DBuf<long long> doff; doff.upload(off, st, stg);
-    launch_gather_interior2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, st);
+    launch_gather_interior2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, st, f32);
     AMR_CUDA(cudaMemcpyAsync(out.data(), d.d, sizeof(double) * tot, cudaMemcpyDeviceToHost, st));
     sync_stream();
     d.free(); dp.free(); doff.free();
@@ -1939,7 +1972,7 @@ static std::string fort_e(double v, int w, int d) {
 
 void Amr2Gpu::output(double t) {
   for (int lev = 1; lev <= lfine; ++lev) {
-    launch_zero_tiny(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st);
+    launch_zero_tiny(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
     ++nkernels;
   }
   if (write_output) {
@@ -2022,7 +2055,7 @@ class Solver2 : public AmrSolver {
     return {g.time, g.rvol, (double)g.ncycle, (double)g.lfine, g.t_step, g.t_regrid, g.tmass0,
             g.cflmax_run, (double)g.nkernels, (double)g.pool.peak * 8.0, (double)g.nsteps_launched,
             g.step_kernel_ms, g.step_kernel_cells, g.last_run_ms, g.run_cells, g.finished() ? 1.0 : 0.0, g.h2d_bytes,
-            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0};
+            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;
@@ -2075,8 +2108,13 @@ extern "C" {
 const char* amrgpu_last_error(void) { return g_err.c_str(); }
 
 int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu_ctx** out) {
+  return amrgpu_init_precision(rundir, outdir, write_output, 64, out);
+}
+
+int amrgpu_init_precision(const char* rundir, const char* outdir, int write_output, int precision_bits, amrgpu_ctx** out) {
   if (!rundir || !out) { g_err = "amrgpu_init: null argument"; return AMRGPU_EINVAL; }
   *out = nullptr;
+  if (precision_bits != 64 && precision_bits != 32) { g_err = "amrgpu_init: precision_bits must be 64 or 32"; return AMRGPU_EINVAL; }
   return guarded([&] {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw std::runtime_error("no CUDA device is visible");
@@ -2091,8 +2129,10 @@ int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu
       ctx->s2 = &s2->g;
       s2->g.outdir = outdir ? outdir : "";
       s2->g.write_output = write_output != 0;
+      s2->g.f32 = precision_bits == 32;
       s2->g.init(rundir);
     } else if (nd == 3) {
+      if (precision_bits != 64) throw std::runtime_error("the FP32 form is built for the 2D path only");
       ctx->s.reset(amrb::make_solver3(rundir, outdir ? outdir : "", write_output != 0));
     } else {
       throw std::runtime_error("num_dim must be 2 or 3");
@@ -2131,6 +2171,7 @@ int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* 
 int amrgpu_level_advance_noalloc(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out) {
   if (!ctx) return AMRGPU_EINVAL;
   if (!ctx->s2) { g_err = "amrgpu_level_advance_noalloc: 2D runs only"; return AMRGPU_EINVAL; }
+  if (ctx->s2->f32) { g_err = "amrgpu_level_advance_noalloc: FP64 contexts only"; return AMRGPU_EINVAL; }
   try {
     amrb::Amr2Gpu& s = *ctx->s2;
     if (level < 1 || level > s.lfine) { g_err = "level out of range"; return AMRGPU_EINVAL; }
@@ -2213,6 +2254,36 @@ int amrgpu_destroy(amrgpu_ctx* ctx) {
   delete ctx;
   return AMRGPU_OK;
 }
+
+#ifdef AMRB_DEBUG_HOOKS
+// Debug builds only (-DAMRB_DEBUG_HOOKS): stop after the n-th level substep; read a patch.
+int amrgpu_debug_run_substeps(amrgpu_ctx* ctx, int n) {
+  amrb::Amr2Gpu& g = *ctx->s2;
+  g.dbg_stop = n; g.dbg_count = 0; g.max_cycles = 0;
+  int stopped = 0;
+  try { g.tick(); } catch (amrb::Amr2Gpu::DebugStop&) { stopped = 1; }
+  g.dbg_stop = 0;
+  return stopped;
+}
+long amrgpu_debug_patch(amrgpu_ctx* ctx, int grid, int store, double* out, long cap) {
+  amrb::Amr2Gpu& g = *ctx->s2;
+  if (grid <= 0 || grid >= (int)g.node.size() || g.node[grid].q0 < 0) return 0;
+  const auto& h = g.node[grid];
+  const long n = (long)h.nq;
+  const long long off = (store == 1) == (h.cur == 0) ? h.q0 : h.q1;
+  if (out && cap >= n) {
+    cudaStreamSynchronize(g.st);
+    if (g.f32) {
+      std::vector<float> t(n);
+      cudaMemcpy(t.data(), reinterpret_cast<float*>(g.pool.d) + off, sizeof(float) * n, cudaMemcpyDeviceToHost);
+      for (long k = 0; k < n; ++k) out[k] = t[k];
+    } else {
+      cudaMemcpy(out, g.pool.d + off, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    }
+  }
+  return n;
+}
+#endif
 
 int amrgpu_num_dim(amrgpu_ctx* ctx) { return ctx ? ctx->s->num_dim() : 0; }
 

@@ -55,12 +55,15 @@ struct Prog3 {
   std::vector<int> bc_stage;
   int nstages = 0;
   long long scratch_off = -1, scratch_len = 0, scratch_alloc = 0;
+  // the scratch starts at zero each run: programs whose rects come from icall copies
+  // (saveqc.f, filval.f) leave uncovered cells at the reference's initial 0
+  bool zero_scratch = false;
   DBuf<Rect3> d_rects;
   DBuf<Fill3Op> d_ops;
   DBuf<Fill3Chunk> d_chunks;
   DBuf<Bc3Op> d_bcs;
   std::vector<int> ch_lo, ch_hi, bc_lo, bc_hi;
-  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; scratch_len = 0; }
+  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; scratch_len = 0; zero_scratch = false; }
   int add_rect(int ni, int nj, int nk, int nvar) {
     Rect3 r; r.off = scratch_len; r.ni = ni; r.nj = nj; r.nk = nk;
     scratch_len += Arena::rnd((long long)ni * nj * nk * nvar);
@@ -569,6 +572,7 @@ class Amr3Gpu : public AmrSolver {
     HPROF("compile_saveqc3");
     Prog3& P = plan[lev].saveqc;
     P.clear();
+    P.zero_scratch = true;
     if (lev + 1 > p.mxnest || lstart[lev + 1] == 0) { upload_prog(P); return; }
     GI(lev);
     const double hxc = hxposs[lev], hyc = hyposs[lev], hzc = hzposs[lev];
@@ -635,6 +639,8 @@ class Amr3Gpu : public AmrSolver {
   }
 
   void run_prog(Prog3& P, const SrcMode& modes) {
+    if (P.zero_scratch && P.scratch_len > 0 && P.nstages > 0)
+      AMR_CUDA(cudaMemsetAsync(pool.d + P.scratch_off, 0, sizeof(double) * P.scratch_len, st));
     for (int s = 0; s < P.nstages; ++s) {
       if (P.ch_hi[s] > P.ch_lo[s]) {
         Fill3Args a{};
@@ -1365,6 +1371,7 @@ class Amr3Gpu : public AmrSolver {
     HPROF("fill_new_level3");
     Prog3& P = newfill;
     P.clear();
+    P.zero_scratch = true;
     GI(lev - 1); GI(lev);
     std::vector<int> nl;
     for (int m = newstl[lev]; m != 0; m = node[m].levelptr) nl.push_back(m);
@@ -1747,7 +1754,7 @@ class Amr3Gpu : public AmrSolver {
   std::vector<double> info() override {
     return {time, rvol, (double)ncycle, (double)lfine, t_step, t_regrid, tmass0, cflmax_run, (double)nkernels, (double)pool.peak * 8.0,
             (double)nsteps_launched, step_kernel_ms, step_kernel_cells, last_run_ms, run_cells, finished() ? 1.0 : 0.0, h2d_bytes,
-            0, 0, 0, 0, 0, 0, 3.0};
+            0, 0, 0, 0, 0, 0, 3.0, 64.0};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;

@@ -37,9 +37,9 @@ struct Step2Layout {
 };
 
 // One sweep direction of flux2.f over the tile. IXY = 1: lines are rows, IXY = 2: columns.
-template <class S, int IXY>
-__device__ void step2_sweep(const StepParams& sp, const double* Qs, double* W, double* X, double* TR, double* F1,
-                            double* F2, int i0, int j0, int tw, int th, double dtdx, double& cfl) {
+template <class S, int IXY, class R>
+__device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR, R* F1,
+                            R* F2, int i0, int j0, int tw, int th, R dtdx, R& cfl) {
   using L = Step2Layout<S>;
   constexpr int ME = L::ME, MW = L::MW, T = L::T, QW = L::QW;
   const int tid = threadIdx.x;
@@ -50,12 +50,12 @@ __device__ void step2_sweep(const StepParams& sp, const double* Qs, double* W, d
   const int l0 = (IXY == 1) ? j0 - 1 : i0 - 1;  // first line
   const int nfr = na + 3;                     // faces for the normal solve: a0-1 .. a0+na+1
   const int nfl = na + 1;                     // limited faces: a0 .. a0+na
-  auto qptr = [&](int m, int line, int pos) -> const double* {
+  auto qptr = [&](int m, int line, int pos) -> const R* {
     // returns &Q(m, ...) ; Q layout [m][b][a] with a = i-(i0-2), b = j-(j0-2)
     if (IXY == 1) return &Qs[(m * QW + (line - (j0 - 2))) * QW + (pos - (i0 - 2))];
     return &Qs[(m * QW + (pos - (j0 - 2))) * QW + (line - (i0 - 2))];
   };
-  auto loadq = [&](double* q, int line, int pos) {
+  auto loadq = [&](R* q, int line, int pos) {
 #pragma unroll
     for (int m = 0; m < ME; ++m) q[m] = *qptr(m, line, pos);
   };
@@ -65,12 +65,12 @@ __device__ void step2_sweep(const StepParams& sp, const double* Qs, double* W, d
     for (int it = tid; it < nlc * nfr; it += STEP2_THREADS) {
       const int rr = it / nfr, ff = it % nfr;
       const int line = l0 + lc0 + rr, f = a0 - 1 + ff;
-      double qL[ME], qR[ME];
+      R qL[ME], qR[ME];
       loadq(qL, line, f - 1);
       loadq(qR, line, f);
-      double wave[MW][ME], s[MW], amdq[ME], apdq[ME];
-      S::template rpn<double>(sp.prob, IXY, qL, qR, wave, s, amdq, apdq);
-      double* rec = W + (rr * (T + 3) + ff) * L::WREC;
+      R wave[MW][ME], s[MW], amdq[ME], apdq[ME];
+      S::template rpn<R>(sp.prob, IXY, qL, qR, wave, s, amdq, apdq);
+      R* rec = W + (rr * (T + 3) + ff) * L::WREC;
 #pragma unroll
       for (int mw = 0; mw < MW; ++mw) {
 #pragma unroll
@@ -89,55 +89,55 @@ __device__ void step2_sweep(const StepParams& sp, const double* Qs, double* W, d
     for (int it = tid; it < nlc * nfl; it += STEP2_THREADS) {
       const int rr = it / nfl, fa = it % nfl;
       const int line = l0 + lc0 + rr, f = a0 + fa;
-      const double* rm = W + (rr * (T + 3) + fa) * L::WREC;       // face f-1
-      const double* rc = rm + L::WREC;                             // face f
-      const double* rp = rc + L::WREC;                             // face f+1
-      double amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
+      const R* rm = W + (rr * (T + 3) + fa) * L::WREC;       // face f-1
+      const R* rc = rm + L::WREC;                             // face f
+      const R* rp = rc + L::WREC;                             // face f+1
+      R amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
 #pragma unroll
       for (int m = 0; m < ME; ++m) { amdq[m] = rc[MW * ME + MW + m]; apdq[m] = rc[MW * ME + MW + ME + m]; }
 #pragma unroll
-      for (int m = 0; m < ME; ++m) { fm[m] = 0.0 + amdq[m]; fp[m] = 0.0 - apdq[m]; }
+      for (int m = 0; m < ME; ++m) { fm[m] = R(0) + amdq[m]; fp[m] = R(0) - apdq[m]; }
       if (sp.order != 1) {
-        double wl[MW][ME];
+        R wl[MW][ME];
 #pragma unroll
         for (int mw = 0; mw < MW; ++mw) {
-          const double smw = rc[MW * ME + mw];
+          const R smw = rc[MW * ME + mw];
 #pragma unroll
           for (int m = 0; m < ME; ++m) wl[mw][m] = rc[mw * ME + m];
           if (sp.mthlim[mw] == 0) continue;
-          double wn2 = 0.0, dotl = 0.0, dotr = 0.0;
+          R wn2 = R(0), dotl = R(0), dotr = R(0);
 #pragma unroll
           for (int m = 0; m < ME; ++m) {
             wn2 = wn2 + rc[mw * ME + m] * rc[mw * ME + m];
             dotl = dotl + rm[mw * ME + m] * rc[mw * ME + m];
             dotr = dotr + rc[mw * ME + m] * rp[mw * ME + m];
           }
-          if (wn2 == 0.0) continue;
-          const double r = (smw > 0.0) ? dotl / wn2 : dotr / wn2;
-          double wlim = 0.0;
+          if (wn2 == R(0)) continue;
+          const R r = (smw > R(0)) ? dotl / wn2 : dotr / wn2;
+          R wlim = R(0);
           switch (sp.mthlim[mw]) {
-            case 1: wlim = dmax(0.0, dmin(1.0, r)); break;
-            case 2: wlim = dmax(0.0, dmax(dmin(1.0, 2.0 * r), dmin(2.0, r))); break;
-            case 3: wlim = (r + fabs(r)) / (1.0 + fabs(r)); break;
-            case 4: { const double c = (1.0 + r) / 2.0; wlim = dmax(0.0, dmin(c, dmin(2.0, 2.0 * r))); } break;
+            case 1: wlim = dmax(R(0), dmin(R(1), r)); break;
+            case 2: wlim = dmax(R(0), dmax(dmin(R(1), R(2) * r), dmin(R(2), r))); break;
+            case 3: wlim = (r + fabs(r)) / (R(1) + fabs(r)); break;
+            case 4: { const R c = (R(1) + r) / R(2); wlim = dmax(R(0), dmin(c, dmin(R(2), R(2) * r))); } break;
             case 5: wlim = r; break;
           }
 #pragma unroll
           for (int m = 0; m < ME; ++m) wl[mw][m] = wlim * wl[mw][m];
         }
-        const double dtdxave = 0.5 * (dtdx + dtdx);
+        const R dtdxave = R(0.5) * (dtdx + dtdx);
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-          double c = 0.0;
+          R c = R(0);
 #pragma unroll
           for (int mw = 0; mw < MW; ++mw) {
-            const double smw = rc[MW * ME + mw];
-            const double abs_sign = sp.use_fwaves ? dsign(1.0, smw) : fabs(smw);
-            c = c + abs_sign * (1.0 - fabs(smw) * dtdxave) * wl[mw][m];
+            const R smw = rc[MW * ME + mw];
+            const R abs_sign = sp.use_fwaves ? dsign(R(1), smw) : fabs(smw);
+            c = c + abs_sign * (R(1) - fabs(smw) * dtdxave) * wl[mw][m];
           }
           cqxx[m] = c;
-          fm[m] = fm[m] + 0.5 * c;
-          fp[m] = fp[m] + 0.5 * c;
+          fm[m] = fm[m] + R(0.5) * c;
+          fp[m] = fp[m] + R(0.5) * c;
         }
       }
       // flux increments into the tile's face arrays (interior lines only)
@@ -157,26 +157,26 @@ __device__ void step2_sweep(const StepParams& sp, const double* Qs, double* W, d
           }
         }
       }
-      double* xr = X + (rr * (T + 1) + fa) * L::XREC;
+      R* xr = X + (rr * (T + 1) + fa) * L::XREC;
       if (sp.trans != 0) {
-        double am2[ME], ap2[ME];
+        R am2[ME], ap2[ME];
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
           am2[m] = amdq[m]; ap2[m] = apdq[m];
           if (sp.order > 1 && sp.trans == 2) { am2[m] = amdq[m] + cqxx[m]; ap2[m] = apdq[m] - cqxx[m]; }
         }
-        double qL[ME], qR[ME];
+        R qL[ME], qR[ME];
         loadq(qL, line, f - 1);
         loadq(qR, line, f);
-        double bm1[ME], bp1[ME], bm2[ME], bp2[ME];
-        S::template rpt<double>(sp.prob, IXY, 1, qL, qR, am2, bm1, bp1);
-        S::template rpt<double>(sp.prob, IXY, 2, qL, qR, ap2, bm2, bp2);
+        R bm1[ME], bp1[ME], bm2[ME], bp2[ME];
+        S::template rpt<R>(sp.prob, IXY, 1, qL, qR, am2, bm1, bp1);
+        S::template rpt<R>(sp.prob, IXY, 2, qL, qR, ap2, bm2, bp2);
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-          xr[0 * ME + m] = 0.5 * dtdx * bm1[m];
-          xr[1 * ME + m] = 0.5 * dtdx * bp1[m];
-          xr[2 * ME + m] = 0.5 * dtdx * bm2[m];
-          xr[3 * ME + m] = 0.5 * dtdx * bp2[m];
+          xr[0 * ME + m] = R(0.5) * dtdx * bm1[m];
+          xr[1 * ME + m] = R(0.5) * dtdx * bp1[m];
+          xr[2 * ME + m] = R(0.5) * dtdx * bm2[m];
+          xr[3 * ME + m] = R(0.5) * dtdx * bp2[m];
         }
       }
     }
@@ -185,45 +185,45 @@ __device__ void step2_sweep(const StepParams& sp, const double* Qs, double* W, d
     if (sp.trans != 0) {
       for (int it = tid; it < nlc * na; it += STEP2_THREADS) {
         const int rr = it / na, ca = it % na;
-        const double* xa = X + (rr * (T + 1) + ca + 1) * L::XREC;  // face c+1 (amdq part)
-        const double* xb = X + (rr * (T + 1) + ca) * L::XREC;      // face c   (apdq part)
-        double* tr = TR + (((lc0 + rr) * T + ca) * 2) * ME;
+        const R* xa = X + (rr * (T + 1) + ca + 1) * L::XREC;  // face c+1 (amdq part)
+        const R* xb = X + (rr * (T + 1) + ca) * L::XREC;      // face c   (apdq part)
+        R* tr = TR + (((lc0 + rr) * T + ca) * 2) * ME;
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-          tr[m] = (0.0 - xa[0 * ME + m]) - xb[2 * ME + m];
-          tr[ME + m] = (0.0 - xa[1 * ME + m]) - xb[3 * ME + m];
+          tr[m] = (R(0) - xa[0 * ME + m]) - xb[2 * ME + m];
+          tr[ME + m] = (R(0) - xa[1 * ME + m]) - xb[3 * ME + m];
         }
       }
     } else {
       for (int it = tid; it < nlc * na; it += STEP2_THREADS) {
         const int rr = it / na, ca = it % na;
-        double* tr = TR + (((lc0 + rr) * T + ca) * 2) * ME;
+        R* tr = TR + (((lc0 + rr) * T + ca) * 2) * ME;
 #pragma unroll
-        for (int m = 0; m < ME; ++m) { tr[m] = 0.0; tr[ME + m] = 0.0; }
+        for (int m = 0; m < ME; ++m) { tr[m] = R(0); tr[ME + m] = R(0); }
       }
     }
     __syncthreads();
   }
 }
 
-template <class S>
+template <class S, class R>
 __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
   using L = Step2Layout<S>;
   constexpr int ME = L::ME, T = L::T, QW = L::QW;
-  extern __shared__ double smem[];
-  double* Qs = smem;
-  double* FM = Qs + L::NQ;
-  double* FP = FM + L::NF;
-  double* GM = FP + L::NF;
-  double* GP = GM + L::NF;
-  double* TR = GP + L::NF;
-  double* W = TR + L::NTR;
-  double* X = W + L::NW;
-  double* red = X + L::NX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* Qs = reinterpret_cast<R*>(smem_raw);
+  R* FM = Qs + L::NQ;
+  R* FP = FM + L::NF;
+  R* GM = FP + L::NF;
+  R* GP = GM + L::NF;
+  R* TR = GP + L::NF;
+  R* W = TR + L::NTR;
+  R* X = W + L::NW;
+  R* red = X + L::NX;
   __shared__ int s_item;
   const int tid = threadIdx.x;
-  const double dtdx = a.dt / a.dx, dtdy = a.dt / a.dy;
-  double cfl = 0.0;
+  const R dtdx = (R)(a.dt / a.dx), dtdy = (R)(a.dt / a.dy);
+  R cfl = R(0);
   int iter = 0;
   while (true) {
     int w;
@@ -243,8 +243,8 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
     const int mitot = P.mitot, mjtot = P.mjtot;
     const int i0 = wk.ti0, j0 = wk.tj0;
     const int tw = min(T, mx - i0 + 1), th = min(T, my - j0 + 1);
-    const double* qin = a.pool + P.q[P.cur];
-    double* qout = a.pool + P.q[1 - P.cur];
+    const R* qin = static_cast<const R*>(a.pool) + P.q[P.cur];
+    R* qout = static_cast<R*>(a.pool) + P.q[1 - P.cur];
     const long long plane = (long long)mitot * mjtot;
     // load the tile with its two ghost layers: interior (i,j) -> enlarged 0-based (i+1, j+1)
     const int lw = tw + 4, lh = th + 4;
@@ -256,26 +256,26 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
     }
     __syncthreads();
     // x-sweeps: FM/FP initialised, per-cell transverse parts in TR
-    step2_sweep<S, 1>(a.sp, Qs, W, X, TR, FM, FP, i0, j0, tw, th, dtdx, cfl);
+    step2_sweep<S, 1, R>(a.sp, Qs, W, X, TR, FM, FP, i0, j0, tw, th, dtdx, cfl);
     // GX(c, f) = (0 + part2(row f-1)) + part1(row f) -> GM and GP
     for (int it = tid; it < ME * (th + 1) * tw; it += STEP2_THREADS) {
       const int m = it / ((th + 1) * tw), rem = it % ((th + 1) * tw);
       const int fb = rem / tw, ca = rem % tw;
-      const double up = TR[((fb * T + ca) * 2) * ME + ME + m];        // row f-1 = line index fb
-      const double dn = TR[(((fb + 1) * T + ca) * 2) * ME + m];       // row f   = line index fb+1
-      const double g = (0.0 + up) + dn;
+      const R up = TR[((fb * T + ca) * 2) * ME + ME + m];        // row f-1 = line index fb
+      const R dn = TR[(((fb + 1) * T + ca) * 2) * ME + m];       // row f   = line index fb+1
+      const R g = (R(0) + up) + dn;
       GM[(m * (T + 1) + fb) * T + ca] = g;
       GP[(m * (T + 1) + fb) * T + ca] = g;
     }
     __syncthreads();
     // y-sweeps: GM/GP += faddm/faddp, per-cell transverse parts in TR
-    step2_sweep<S, 2>(a.sp, Qs, W, X, TR, GM, GP, i0, j0, tw, th, dtdy, cfl);
+    step2_sweep<S, 2, R>(a.sp, Qs, W, X, TR, GM, GP, i0, j0, tw, th, dtdy, cfl);
     // FM(f, r) = (FM + part2(col f-1)) + part1(col f)
     for (int it = tid; it < ME * th * (tw + 1); it += STEP2_THREADS) {
       const int m = it / (th * (tw + 1)), rem = it % (th * (tw + 1));
       const int rb = rem / (tw + 1), fa = rem % (tw + 1);
-      const double up = TR[((fa * T + rb) * 2) * ME + ME + m];        // column f-1 = line index fa
-      const double dn = TR[(((fa + 1) * T + rb) * 2) * ME + m];       // column f   = line index fa+1
+      const R up = TR[((fa * T + rb) * 2) * ME + ME + m];        // column f-1 = line index fa
+      const R dn = TR[(((fa + 1) * T + rb) * 2) * ME + m];       // column f   = line index fa+1
       const int k = (m * T + rb) * (T + 1) + fa;
       FM[k] = (FM[k] + up) + dn;
       FP[k] = (FP[k] + up) + dn;
@@ -285,10 +285,10 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
     for (int it = tid; it < ME * th * tw; it += STEP2_THREADS) {
       const int m = it / (th * tw), rem = it % (th * tw);
       const int rb = rem / tw, ca = rem % tw;
-      const double q = Qs[(m * QW + rb + 2) * QW + ca + 2];
-      const double fmr = FM[(m * T + rb) * (T + 1) + ca + 1], fpl = FP[(m * T + rb) * (T + 1) + ca];
-      const double gmt = GM[(m * (T + 1) + rb + 1) * T + ca], gpb = GP[(m * (T + 1) + rb) * T + ca];
-      const double qn = q - dtdx * (fmr - fpl) - dtdy * (gmt - gpb);
+      const R q = Qs[(m * QW + rb + 2) * QW + ca + 2];
+      const R fmr = FM[(m * T + rb) * (T + 1) + ca + 1], fpl = FP[(m * T + rb) * (T + 1) + ca];
+      const R gmt = GM[(m * (T + 1) + rb + 1) * T + ca], gpb = GP[(m * (T + 1) + rb) * T + ca];
+      const R qn = q - dtdx * (fmr - fpl) - dtdy * (gmt - gpb);
       const int ie = i0 + ca + 1, je = j0 + rb + 1;
       qout[m * plane + (long long)je * mitot + ie] = qn;
     }
@@ -297,11 +297,12 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
       const FsvEntry e = a.fsv[wk.fsv_start + it / ME];
       const int m = it % ME;
       const int ca = e.ic - i0, rb = e.jc - j0;
+      // register values stay FP64 in both forms
       double v = 0.0;
-      if (e.side == 1) v = -FP[(m * T + rb) * (T + 1) + ca] * a.dt * a.dy;
-      else if (e.side == 2) v = -GM[(m * (T + 1) + rb + 1) * T + ca] * a.dt * a.dx;
-      else if (e.side == 3) v = -FM[(m * T + rb) * (T + 1) + ca + 1] * a.dt * a.dy;
-      else v = -GP[(m * (T + 1) + rb) * T + ca] * a.dt * a.dx;
+      if (e.side == 1) v = -(double)FP[(m * T + rb) * (T + 1) + ca] * a.dt * a.dy;
+      else if (e.side == 2) v = -(double)GM[(m * (T + 1) + rb + 1) * T + ca] * a.dt * a.dx;
+      else if (e.side == 3) v = -(double)FM[(m * T + rb) * (T + 1) + ca + 1] * a.dt * a.dy;
+      else v = -(double)GP[(m * (T + 1) + rb) * T + ca] * a.dt * a.dx;
       a.regs[e.dst + m] = v;
     }
     // fluxad epilogue: fine boundary fluxes accumulated into this patch's registers
@@ -313,10 +314,10 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
       double s = *svd;
       for (int l = 0; l < r; ++l) {
         const int f = e.f0 + l;
-        if (e.side == 1) s = s + FM[(m * T + (f - j0)) * (T + 1) + 0] * a.dt * a.dy;
-        else if (e.side == 2) s = s + GP[(m * (T + 1) + th) * T + (f - i0)] * a.dt * a.dx;
-        else if (e.side == 3) s = s + FP[(m * T + (f - j0)) * (T + 1) + tw] * a.dt * a.dy;
-        else s = s + GM[(m * (T + 1) + 0) * T + (f - i0)] * a.dt * a.dx;
+        if (e.side == 1) s = s + (double)FM[(m * T + (f - j0)) * (T + 1) + 0] * a.dt * a.dy;
+        else if (e.side == 2) s = s + (double)GP[(m * (T + 1) + th) * T + (f - i0)] * a.dt * a.dx;
+        else if (e.side == 3) s = s + (double)FP[(m * T + (f - j0)) * (T + 1) + tw] * a.dt * a.dy;
+        else s = s + (double)GM[(m * (T + 1) + 0) * T + (f - i0)] * a.dt * a.dx;
       }
       *svd = s;
     }
@@ -327,57 +328,68 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
   if ((tid & 31) == 0) red[tid >> 5] = cfl;
   __syncthreads();
   if (tid == 0) {
-    double c = 0.0;
+    R c = R(0);
     for (int k = 0; k < STEP2_THREADS / 32; ++k) c = dmax(c, red[k]);
-    atomicMax(a.cflmax, (unsigned long long)__double_as_longlong(c));
+    atomicMax(a.cflmax, (unsigned long long)__double_as_longlong((double)c));
   }
 }
 
-template <class S>
+template <class S, class R>
 static void launch_step2_t(const StepArgs& a, int grid, cudaStream_t s) {
-  const size_t sm = sizeof(double) * Step2Layout<S>::TOTAL;
+  const size_t sm = sizeof(R) * Step2Layout<S>::TOTAL;
   // once per process (thread-safe static initialisation; contexts may run on several host threads)
   static const bool attr = [&] {
-    AMR_CUDA(cudaFuncSetAttribute(step2_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    AMR_CUDA(cudaFuncSetAttribute(step2_kernel<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     return true;
   }();
   (void)attr;
   if (grid <= 0) return;
-  step2_kernel<S><<<grid, STEP2_THREADS, sm, s>>>(a);
+  step2_kernel<S, R><<<grid, STEP2_THREADS, sm, s>>>(a);
   AMR_CUDA(cudaGetLastError());
 }
 
-void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s) {
+template <class R>
+static void launch_step2_r(int solver, const StepArgs& a, int grid, cudaStream_t s) {
   switch (solver) {
-    case SOLVER_ADVECTION: launch_step2_t<Advection2>(a, grid, s); break;
-    case SOLVER_ACOUSTICS: launch_step2_t<Acoustics2>(a, grid, s); break;
-    case SOLVER_EULER: launch_step2_t<Euler2>(a, grid, s); break;
+    case SOLVER_ADVECTION: launch_step2_t<Advection2, R>(a, grid, s); break;
+    case SOLVER_ACOUSTICS: launch_step2_t<Acoustics2, R>(a, grid, s); break;
+    case SOLVER_EULER: launch_step2_t<Euler2, R>(a, grid, s); break;
     default: throw std::runtime_error("launch_step2: unsupported solver");
   }
 }
 
-size_t step2_smem_bytes(int solver) {
+void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s, bool f32) {
+  if (f32) launch_step2_r<float>(solver, a, grid, s);
+  else launch_step2_r<double>(solver, a, grid, s);
+}
+
+size_t step2_smem_bytes(int solver, bool f32) {
+  const size_t w = f32 ? sizeof(float) : sizeof(double);
   switch (solver) {
-    case SOLVER_ADVECTION: return sizeof(double) * Step2Layout<Advection2>::TOTAL;
-    case SOLVER_ACOUSTICS: return sizeof(double) * Step2Layout<Acoustics2>::TOTAL;
-    case SOLVER_EULER: return sizeof(double) * Step2Layout<Euler2>::TOTAL;
+    case SOLVER_ADVECTION: return w * Step2Layout<Advection2>::TOTAL;
+    case SOLVER_ACOUSTICS: return w * Step2Layout<Acoustics2>::TOTAL;
+    case SOLVER_EULER: return w * Step2Layout<Euler2>::TOTAL;
   }
   return 0;
 }
 
 // ======================================================================= ghost fill
-__device__ __forceinline__ double* fill_dst(const FillArgs& a, const FillOp& o, int& ldi, long long& plane) {
+// Storage type T (double, or float in the FP32 form); the fill arithmetic is FP64.
+template <class T>
+__device__ __forceinline__ T* fill_dst(const FillArgs& a, const FillOp& o, int& ldi, long long& plane) {
   if (o.dst_patch >= 0) {
     const PatchDev& P = a.patches[o.dst_patch];
     ldi = P.mitot; plane = (long long)P.mitot * P.mjtot;
-    return a.pool + P.q[P.cur];
+    return static_cast<T*>(a.pool) + P.q[P.cur];
   }
   const ScratchRect& R = a.rects[o.dst_rect];
   ldi = R.ni; plane = (long long)R.ni * R.nj;
-  return a.pool + R.off;
+  return static_cast<T*>(a.pool) + R.off;
 }
 
+template <class T>
 __global__ void fill_kernel(FillArgs a) {
+  const T* pool = static_cast<const T*>(a.pool);
   const int c = blockIdx.x;
   if (c >= a.nchunks) return;
   const FillChunk ch = a.chunks[c];
@@ -397,13 +409,13 @@ __global__ void fill_kernel(FillArgs a) {
     else { k -= ncol - 2; ii = 1 + k; jj = 0; }
     const PatchDev& K = a.patches[o.dst_patch];
     double* qc1d = a.regs + K.ffl + (long long)nvar * K.lenbc + (long long)nvar * cell;
-    const double* src = a.pool + R.off;
+    const T* src = pool + R.off;
     const long long pl = (long long)nrow * ncol;
-    for (int m = 0; m < nvar; ++m) qc1d[m] = src[m * pl + (long long)jj * nrow + ii];
+    for (int m = 0; m < nvar; ++m) qc1d[m] = (double)src[m * pl + (long long)jj * nrow + ii];
     return;
   }
   int ldi; long long plane;
-  double* dst = fill_dst(a, o, ldi, plane);
+  T* dst = fill_dst<T>(a, o, ldi, plane);
   const long long dk = (long long)(o.dj0 + jb) * ldi + (o.di0 + ia);
   if (o.kind == FILL_COPY) {
     const PatchDev& S = a.patches[o.src];
@@ -411,14 +423,14 @@ __global__ void fill_kernel(FillArgs a) {
     const long long sk = (long long)(o.sj0 + jb) * S.mitot + (o.si0 + ia);
     int mode = 0; double ai = 1.0, ac = 0.0;
     if (o.level >= 0) { mode = a.modes.mode[o.level]; ai = a.modes.alphai[o.level]; ac = a.modes.alphac[o.level]; }
-    const double* qn = a.pool + S.q[S.cur];
-    const double* qo = a.pool + S.q[1 - S.cur];
+    const T* qn = pool + S.q[S.cur];
+    const T* qo = pool + S.q[1 - S.cur];
     for (int m = 0; m < nvar; ++m) {
       double v;
-      if (mode == 0) v = qn[m * sp + sk];
-      else if (mode == 1) v = qo[m * sp + sk];
-      else v = qn[m * sp + sk] * ai + qo[m * sp + sk] * ac;
-      dst[m * plane + dk] = v;
+      if (mode == 0) v = (double)qn[m * sp + sk];
+      else if (mode == 1) v = (double)qo[m * sp + sk];
+      else v = (double)qn[m * sp + sk] * ai + (double)qo[m * sp + sk] * ac;
+      dst[m * plane + dk] = (T)v;
     }
     return;
   }
@@ -426,12 +438,12 @@ __global__ void fill_kernel(FillArgs a) {
     const ScratchRect& R = a.rects[o.src];
     const long long sp = (long long)R.ni * R.nj;
     const long long sk = (long long)(o.sj0 + jb) * R.ni + (o.si0 + ia);
-    const double* src = a.pool + R.off;
+    const T* src = pool + R.off;
     for (int m = 0; m < nvar; ++m) dst[m * plane + dk] = src[m * sp + sk];
     return;
   }
   const ScratchRect& R = a.rects[o.src];
-  const double* vc = a.pool + R.off;
+  const T* vc = pool + R.off;
   const long long cp = (long long)R.ni * R.nj;
   const int lev = o.level;
   const int rx = a.lc.intratx[lev - 1], ry = a.lc.intraty[lev - 1];
@@ -448,7 +460,7 @@ __global__ void fill_kernel(FillArgs a) {
     const double xcc = xlow_c + (ic - 0.5) * dxc;
     const double xcf = a.xlower + (ifg + 0.5) * dxf;
     const double eta1 = (xcf - xcc) / dxc;
-    auto CI = [&](int m, int i, int j) { return vc[m * cp + (long long)(j - 1) * R.ni + (i - 1)]; };
+    auto CI = [&](int m, int i, int j) { return (double)vc[m * cp + (long long)(j - 1) * R.ni + (i - 1)]; };
     for (int m = 0; m < nvar; ++m) {
       const double valp10 = CI(m, ic + 1, jc), valm10 = CI(m, ic - 1, jc), valc = CI(m, ic, jc);
       const double valp01 = CI(m, ic, jc + 1), valm01 = CI(m, ic, jc - 1);
@@ -462,7 +474,7 @@ __global__ void fill_kernel(FillArgs a) {
       dv = dmin(2.0 * dv, 0.5 * fabs(dvcc));
       const double fv = dmax(0.0, dsign(1.0, dvpc * dvmc));
       const double vslope = dv * dsign(1.0, dvcc) * fv;
-      dst[m * plane + dk] = valc + eta1 * uslope + eta2 * vslope;
+      dst[m * plane + dk] = (T)(valc + eta1 * uslope + eta2 * vslope);
     }
     return;
   }
@@ -471,7 +483,7 @@ __global__ void fill_kernel(FillArgs a) {
     const int icg = floordiv(ifg, rx), jcg = floordiv(jfg, ry);
     const int ico = ifg - icg * rx + 1, jco = jfg - jcg * ry + 1;
     const int i = icg - o.cilo + 1, j = jcg - o.cjlo + 1;  // 1-based in valc
-    auto VC = [&](int m, int ii, int jj) { return vc[m * cp + (long long)(jj - 1) * R.ni + (ii - 1)]; };
+    auto VC = [&](int m, int ii, int jj) { return (double)vc[m * cp + (long long)(jj - 1) * R.ni + (ii - 1)]; };
     const double yoff = ((double)jco - 0.5) / ry - 0.5;
     const double xoff = ((double)ico - 0.5) / rx - 0.5;
     for (int m = 0; m < nvar; ++m) {
@@ -481,28 +493,30 @@ __global__ void fill_kernel(FillArgs a) {
       s1p = VC(m, i, j + 1) - VC(m, i, j); s1m = VC(m, i, j) - VC(m, i, j - 1);
       double slopey = dmin(fabs(s1p), fabs(s1m)) * dsign(1.0, VC(m, i, j + 1) - VC(m, i, j - 1));
       if (s1m * s1p <= 0.0) slopey = 0.0;
-      dst[m * plane + dk] = VC(m, i, j) + xoff * slopex + yoff * slopey;
+      dst[m * plane + dk] = (T)(VC(m, i, j) + xoff * slopex + yoff * slopey);
     }
     return;
   }
 }
 
-void launch_fill(const FillArgs& a, cudaStream_t s) {
+void launch_fill(const FillArgs& a, cudaStream_t s, bool f32) {
   if (a.nchunks <= 0) return;
-  fill_kernel<<<a.nchunks, 128, 0, s>>>(a);
+  if (f32) fill_kernel<float><<<a.nchunks, 128, 0, s>>>(a);
+  else fill_kernel<double><<<a.nchunks, 128, 0, s>>>(a);
   AMR_CUDA(cudaGetLastError());
 }
 
 // phase 0: x-sides over all rows; phase 1: y-sides over all columns (after phase 0)
+template <class T>
 __global__ void bc_kernel(BcArgs a, int phase) {
   const int op = blockIdx.y;
   if (op >= a.nops) return;
   const BcOp o = a.ops[op];
-  double* v; int nrow = o.nrow, ncol = o.ncol;
-  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = a.pool + P.q[P.cur]; }
-  else v = a.pool + a.rects[o.dst_rect].off;
+  T* v; int nrow = o.nrow, ncol = o.ncol;
+  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = static_cast<T*>(a.pool) + P.q[P.cur]; }
+  else v = static_cast<T*>(a.pool) + a.rects[o.dst_rect].off;
   const long long plane = (long long)nrow * ncol;
-  auto V = [&](int m, int i, int j) -> double& { return v[m * plane + (long long)(j - 1) * nrow + (i - 1)]; };
+  auto V = [&](int m, int i, int j) -> T& { return v[m * plane + (long long)(j - 1) * nrow + (i - 1)]; };
   const int nvar = a.nvar;
   if (phase == 0) {
     const int nl = (o.nxl > 0 && (o.bxl == 1 || o.bxl == 3)) ? o.nxl : 0;
@@ -543,21 +557,22 @@ __global__ void bc_kernel(BcArgs a, int phase) {
   }
 }
 
-void launch_bc(const BcArgs& a, int phase, cudaStream_t s) {
+void launch_bc(const BcArgs& a, int phase, cudaStream_t s, bool f32) {
   if (a.nops <= 0) return;
   for (int base = 0; base < a.nops; base += 65535) {
     BcArgs b = a;
     b.ops = a.ops + base;
     b.nops = std::min(65535, a.nops - base);
     dim3 grid(2, b.nops);
-    bc_kernel<<<grid, 128, 0, s>>>(b, phase);
+    if (f32) bc_kernel<float><<<grid, 128, 0, s>>>(b, phase);
+    else bc_kernel<double><<<grid, 128, 0, s>>>(b, phase);
     AMR_CUDA(cudaGetLastError());
   }
 }
 
 // ======================================================================= qad
-template <class S>
-__global__ void qad2_kernel(double* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
+template <class S, class T>
+__global__ void qad2_kernel(T* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
                             ProbDev prob, LevelConst lc, double delt) {
   constexpr int ME = S::MEQN, MW = S::MWAVES;
   const int jb = blockIdx.x;
@@ -567,7 +582,7 @@ __global__ void qad2_kernel(double* pool, double* regs, const PatchDev* patches,
   const int lev = P.level;
   const int rx = lc.intratx[lev - 1], ry = lc.intraty[lev - 1];
   const double hx = lc.hx[lev], hy = lc.hy[lev];
-  const double* q = pool + P.q[P.cur];
+  const T* q = pool + P.q[P.cur];
   const long long plane = (long long)P.mitot * P.mjtot;
   for (int sgi = threadIdx.x; sgi < J.nseg; sgi += blockDim.x) {
     const int seg = J.seg0 + sgi;
@@ -579,25 +594,26 @@ __global__ void qad2_kernel(double* pool, double* regs, const PatchDev* patches,
     const int r = (J.side == 1 || J.side == 3) ? ry : rx;
     for (int l = 1; l <= r; ++l) {
       const int f = sgi * r + l;  // fine row (sides 1,3) or column (sides 2,4), 1-based interior
-      double qf[ME], qcr[ME];
+      T qf[ME], qcr[ME];
       long long k;
       if (J.side == 1) k = (long long)(f + 1) * P.mitot + 1;
       else if (J.side == 2) k = (long long)(P.mjtot - 2) * P.mitot + (f + 1);
       else if (J.side == 3) k = (long long)(f + 1) * P.mitot + (P.mitot - 2);
       else k = (long long)1 * P.mitot + (f + 1);
 #pragma unroll
-      for (int m = 0; m < ME; ++m) { qf[m] = q[m * plane + k]; qcr[m] = qc[m]; }
-      double wave[MW][ME], s[MW], amdq[ME], apdq[ME];
-      if (J.side == 1) S::template rpn<double>(prob, 1, qcr, qf, wave, s, amdq, apdq);
-      else if (J.side == 2) S::template rpn<double>(prob, 2, qf, qcr, wave, s, amdq, apdq);
-      else if (J.side == 3) S::template rpn<double>(prob, 1, qf, qcr, wave, s, amdq, apdq);
-      else S::template rpn<double>(prob, 2, qcr, qf, wave, s, amdq, apdq);
+      for (int m = 0; m < ME; ++m) { qf[m] = q[m * plane + k]; qcr[m] = (T)qc[m]; }
+      T wave[MW][ME], s[MW], amdq[ME], apdq[ME];
+      if (J.side == 1) S::template rpn<T>(prob, 1, qcr, qf, wave, s, amdq, apdq);
+      else if (J.side == 2) S::template rpn<T>(prob, 2, qf, qcr, wave, s, amdq, apdq);
+      else if (J.side == 3) S::template rpn<T>(prob, 1, qf, qcr, wave, s, amdq, apdq);
+      else S::template rpn<T>(prob, 2, qcr, qf, wave, s, amdq, apdq);
 #pragma unroll
       for (int m = 0; m < ME; ++m) {
-        if (J.side == 1) sv[m] = sv[m] + amdq[m] * hy * delt + apdq[m] * hy * delt;
-        else if (J.side == 2) sv[m] = sv[m] - amdq[m] * hx * delt - apdq[m] * hx * delt;
-        else if (J.side == 3) sv[m] = sv[m] - amdq[m] * hy * delt - apdq[m] * hy * delt;
-        else sv[m] = sv[m] + amdq[m] * hx * delt + apdq[m] * hx * delt;
+        const double am = amdq[m], ap = apdq[m];  // registers accumulate in FP64
+        if (J.side == 1) sv[m] = sv[m] + am * hy * delt + ap * hy * delt;
+        else if (J.side == 2) sv[m] = sv[m] - am * hx * delt - ap * hx * delt;
+        else if (J.side == 3) sv[m] = sv[m] - am * hy * delt - ap * hy * delt;
+        else sv[m] = sv[m] + am * hx * delt + ap * hx * delt;
       }
     }
 #pragma unroll
@@ -605,52 +621,62 @@ __global__ void qad2_kernel(double* pool, double* regs, const PatchDev* patches,
   }
 }
 
-void launch_qad2(int solver, double* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
-                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s) {
+template <class T>
+static void launch_qad2_t(int solver, T* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
+                          const ProbDev& prob, LevelConst lc, double delt, cudaStream_t s) {
+  switch (solver) {
+    case SOLVER_ADVECTION: qad2_kernel<Advection2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
+    case SOLVER_ACOUSTICS: qad2_kernel<Acoustics2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
+    case SOLVER_EULER: qad2_kernel<Euler2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
+  }
+}
+
+void launch_qad2(int solver, void* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
+                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s, bool f32) {
   if (njobs <= 0) return;
   (void)nvar;
-  switch (solver) {
-    case SOLVER_ADVECTION: qad2_kernel<Advection2><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
-    case SOLVER_ACOUSTICS: qad2_kernel<Acoustics2><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
-    case SOLVER_EULER: qad2_kernel<Euler2><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
-  }
+  if (f32) launch_qad2_t(solver, static_cast<float*>(pool), regs, patches, jobs, njobs, prob, lc, delt, s);
+  else launch_qad2_t(solver, static_cast<double*>(pool), regs, patches, jobs, njobs, prob, lc, delt, s);
   AMR_CUDA(cudaGetLastError());
 }
 
 // ======================================================================= update
-__global__ void upbnd_kernel(double* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells,
+template <class T>
+__global__ void upbnd_kernel(T* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells,
                              int ncells, const UpbndTerm* terms, double area, int nvar) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ncells * nvar) return;
   const int c = t / nvar, m = t % nvar;
   const UpbndCell C = cells[c];
   const PatchDev& P = patches[C.patch];
-  double* v = pool + P.q[P.cur] + (long long)m * P.mitot * P.mjtot + (long long)C.je * P.mitot + C.ie;
-  double val = *v;
+  T* v = pool + P.q[P.cur] + (long long)m * P.mitot * P.mjtot + (long long)C.je * P.mitot + C.ie;
+  double val = (double)*v;
   for (int k = 0; k < C.count; ++k) {
-    const UpbndTerm T = terms[C.first + k];
-    val = val + T.sgn * regs[T.reg + m] / area;
+    const UpbndTerm U = terms[C.first + k];
+    val = val + U.sgn * regs[U.reg + m] / area;
   }
-  *v = val;
+  *v = (T)val;
 }
 
-void launch_upbnd(double* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
-                  const UpbndTerm* terms, double area, int nvar, cudaStream_t s) {
+void launch_upbnd(void* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
+                  const UpbndTerm* terms, double area, int nvar, cudaStream_t s, bool f32) {
   if (ncells <= 0) return;
   const int n = ncells * nvar;
-  upbnd_kernel<<<(n + 127) / 128, 128, 0, s>>>(pool, regs, patches, cells, ncells, terms, area, nvar);
+  if (f32) upbnd_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, cells, ncells, terms, area, nvar);
+  else upbnd_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, cells, ncells, terms, area, nvar);
   AMR_CUDA(cudaGetLastError());
 }
 
-__global__ void average_kernel(double* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry,
+template <class T>
+__global__ void average_kernel(T* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry,
                                int nvar) {
   const int r = blockIdx.y;
   if (r >= nrects) return;
   const AvgRect A = rects[r];
   const PatchDev& C = patches[A.cpatch];
   const PatchDev& K = patches[A.kpatch];
-  double* qc = pool + C.q[C.cur];
-  const double* qf = pool + K.q[K.cur];
+  T* qc = pool + C.q[C.cur];
+  const T* qf = pool + K.q[K.cur];
   const long long cpl = (long long)C.mitot * C.mjtot, fpl = (long long)K.mitot * K.mjtot;
   const double totrat = (double)(rx * ry);
   const int n = A.ni * A.nj * nvar;
@@ -660,29 +686,31 @@ __global__ void average_kernel(double* pool, const PatchDev* patches, const AvgR
     const int fi = A.fi0 + aa * rx, fj = A.fj0 + b * ry;
     double s = 0.0;
     for (int jco = 0; jco < ry; ++jco)
-      for (int ico = 0; ico < rx; ++ico) s = s + qf[m * fpl + (long long)(fj + jco) * K.mitot + (fi + ico)];
+      for (int ico = 0; ico < rx; ++ico) s = s + (double)qf[m * fpl + (long long)(fj + jco) * K.mitot + (fi + ico)];
     s = s / totrat;
-    qc[m * cpl + (long long)(A.cj0 + b) * C.mitot + (A.ci0 + aa)] = s;
+    qc[m * cpl + (long long)(A.cj0 + b) * C.mitot + (A.ci0 + aa)] = (T)s;
   }
 }
 
-void launch_average(double* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
-                    cudaStream_t s) {
+void launch_average(void* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
+                    cudaStream_t s, bool f32) {
   for (int base = 0; base < nrects; base += 65535) {
     const int n = std::min(65535, nrects - base);
     dim3 grid(4, n);
-    average_kernel<<<grid, 128, 0, s>>>(pool, patches, rects + base, n, rx, ry, nvar);
+    if (f32) average_kernel<<<grid, 128, 0, s>>>(static_cast<float*>(pool), patches, rects + base, n, rx, ry, nvar);
+    else average_kernel<<<grid, 128, 0, s>>>(static_cast<double*>(pool), patches, rects + base, n, rx, ry, nvar);
     AMR_CUDA(cudaGetLastError());
   }
 }
 
 // ======================================================================= flags, gauges, misc
-__global__ void flags2_kernel(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff,
+template <class T>
+__global__ void flags2_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* outoff,
                               int use_old, int flag_component, double tolsp, int nvar, int8_t* out) {
   const int pi = blockIdx.y;
   const PatchDev P = patches[plist[pi]];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
-  const double* q = pool + P.q[use_old ? 1 - P.cur : P.cur];
+  const T* q = pool + P.q[use_old ? 1 - P.cur : P.cur];
   const long long plane = (long long)P.mitot * P.mjtot;
   const int m0 = flag_component > 0 ? flag_component - 1 : 0, m1 = flag_component > 0 ? flag_component - 1 : nvar - 1;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my; t += gridDim.x * blockDim.x) {
@@ -690,9 +718,9 @@ __global__ void flags2_kernel(const double* pool, const PatchDev* patches, const
     const int ie = i + 1, je = j + 1;
     int8_t f = 0;
     for (int m = m0; m <= m1; ++m) {
-      const double* qm = q + m * plane;
-      const double dqi = fabs(qm[(long long)je * P.mitot + ie + 1] - qm[(long long)je * P.mitot + ie - 1]);
-      const double dqj = fabs(qm[(long long)(je + 1) * P.mitot + ie] - qm[(long long)(je - 1) * P.mitot + ie]);
+      const T* qm = q + m * plane;
+      const double dqi = fabs((double)qm[(long long)je * P.mitot + ie + 1] - (double)qm[(long long)je * P.mitot + ie - 1]);
+      const double dqj = fabs((double)qm[(long long)(je + 1) * P.mitot + ie] - (double)qm[(long long)(je - 1) * P.mitot + ie]);
       const double dq = dmax(0.0, dmax(dqi, dqj));
       if (dq > tolsp) { f = 1; break; }
     }
@@ -700,27 +728,33 @@ __global__ void flags2_kernel(const double* pool, const PatchDev* patches, const
   }
 }
 
-void launch_flags2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
-                   int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s) {
+void launch_flags2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
+                   int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s, bool f32) {
   for (int base = 0; base < np; base += 65535) {
     const int n = std::min(65535, np - base);
     dim3 grid(8, n);
-    flags2_kernel<<<grid, 128, 0, s>>>(pool, patches, plist + base, outoff + base, use_old, flag_component, tolsp, nvar, out);
+    if (f32)
+      flags2_kernel<<<grid, 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, outoff + base, use_old, flag_component,
+                                         tolsp, nvar, out);
+    else
+      flags2_kernel<<<grid, 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, outoff + base, use_old, flag_component,
+                                         tolsp, nvar, out);
     AMR_CUDA(cudaGetLastError());
   }
 }
 
-__global__ void gauges2_kernel(const double* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
+template <class T>
+__global__ void gauges2_kernel(const T* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
                                double* out) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= njobs) return;
   const GaugeJob G = jobs[t];
   const PatchDev& P = patches[G.patch];
-  const double* q = pool + P.q[P.cur];
+  const T* q = pool + P.q[P.cur];
   const long long plane = (long long)P.mitot * P.mjtot;
   const double xo = G.xoff, yo = G.yoff;
   // Q(n, ii, jj) with ii, jj 1-based enlarged indices
-  auto Q = [&](int m, int i, int j) { return q[m * plane + (long long)(j - 1) * P.mitot + (i - 1)]; };
+  auto Q = [&](int m, int i, int j) { return (double)q[m * plane + (long long)(j - 1) * P.mitot + (i - 1)]; };
   for (int m = 0; m < nvar; ++m) {
     double v = (1.0 - xo) * (1.0 - yo) * Q(m, G.ii, G.jj) + xo * (1.0 - yo) * Q(m, G.ii + 1, G.jj) +
                (1.0 - xo) * yo * Q(m, G.ii, G.jj + 1) + xo * yo * Q(m, G.ii + 1, G.jj + 1);
@@ -729,10 +763,11 @@ __global__ void gauges2_kernel(const double* pool, const PatchDev* patches, cons
   }
 }
 
-void launch_gauges2(const double* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
-                    double* out, cudaStream_t s) {
+void launch_gauges2(const void* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
+                    double* out, cudaStream_t s, bool f32) {
   if (njobs <= 0) return;
-  gauges2_kernel<<<(njobs + 63) / 64, 64, 0, s>>>(pool, patches, jobs, njobs, nvar, out);
+  if (f32) gauges2_kernel<<<(njobs + 63) / 64, 64, 0, s>>>(static_cast<const float*>(pool), patches, jobs, njobs, nvar, out);
+  else gauges2_kernel<<<(njobs + 63) / 64, 64, 0, s>>>(static_cast<const double*>(pool), patches, jobs, njobs, nvar, out);
   AMR_CUDA(cudaGetLastError());
 }
 
@@ -746,61 +781,69 @@ void launch_flip(PatchDev* patches, const int* plist, int np, cudaStream_t s) {
   AMR_CUDA(cudaGetLastError());
 }
 
-__global__ void zero_tiny_kernel(double* pool, const PatchDev* patches, const int* plist, int nvar) {
+template <class T>
+__global__ void zero_tiny_kernel(T* pool, const PatchDev* patches, const int* plist, int nvar) {
   const PatchDev P = patches[plist[blockIdx.y]];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
-  double* q = pool + P.q[P.cur];
+  T* q = pool + P.q[P.cur];
   const long long plane = (long long)P.mitot * P.mjtot;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my * nvar; t += gridDim.x * blockDim.x) {
     const int m = t / (mx * my), rem = t % (mx * my);
     const int i = rem % mx + 2, j = rem / mx + 2;
-    double& v = q[m * plane + (long long)j * P.mitot + i];
-    if (fabs(v) < 1e-90) v = 0.0;
+    T& v = q[m * plane + (long long)j * P.mitot + i];
+    if (fabs((double)v) < 1e-90) v = (T)0;
   }
 }
-void launch_zero_tiny(double* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s) {
+void launch_zero_tiny(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32) {
   for (int base = 0; base < np; base += 65535) {
     const int n = std::min(65535, np - base);
-    zero_tiny_kernel<<<dim3(4, n), 128, 0, s>>>(pool, patches, plist + base, nvar);
+    if (f32) zero_tiny_kernel<<<dim3(4, n), 128, 0, s>>>(static_cast<float*>(pool), patches, plist + base, nvar);
+    else zero_tiny_kernel<<<dim3(4, n), 128, 0, s>>>(static_cast<double*>(pool), patches, plist + base, nvar);
     AMR_CUDA(cudaGetLastError());
   }
 }
 
-__global__ void mass2_kernel(const double* pool, const PatchDev* patches, const int* plist, int np, double* out) {
+template <class T>
+__global__ void mass2_kernel(const T* pool, const PatchDev* patches, const int* plist, int np, double* out) {
   double s = 0.0;
   for (int pi = blockIdx.y; pi < np; pi += gridDim.y) {
     const PatchDev P = patches[plist[pi]];
     const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
-    const double* q = pool + P.q[P.cur];
+    const T* q = pool + P.q[P.cur];
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my; t += gridDim.x * blockDim.x)
-      s += q[(long long)(t / mx + 2) * P.mitot + (t % mx + 2)];
+      s += (double)q[(long long)(t / mx + 2) * P.mitot + (t % mx + 2)];
   }
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
-void launch_mass2(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s) {
+void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32) {
   if (np <= 0) return;
-  mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(pool, patches, plist, np, out);
+  if (f32) mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist, np, out);
+  else mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist, np, out);
   AMR_CUDA(cudaGetLastError());
 }
 
-__global__ void gather_interior2_kernel(const double* pool, const PatchDev* patches, const int* plist,
+template <class T>
+__global__ void gather_interior2_kernel(const T* pool, const PatchDev* patches, const int* plist,
                                         const long long* outoff, int nvar, double* out) {
   const PatchDev P = patches[plist[blockIdx.y]];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
-  const double* q = pool + P.q[P.cur];
+  const T* q = pool + P.q[P.cur];
   const long long plane = (long long)P.mitot * P.mjtot;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my * nvar; t += gridDim.x * blockDim.x) {
     const int m = t / (mx * my), rem = t % (mx * my);
     const int i = rem % mx + 2, j = rem / mx + 2;
-    out[outoff[blockIdx.y] + t] = q[m * plane + (long long)j * P.mitot + i];
+    out[outoff[blockIdx.y] + t] = (double)q[m * plane + (long long)j * P.mitot + i];
   }
 }
-void launch_gather_interior2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff,
-                             int np, int nvar, double* out, cudaStream_t s) {
+void launch_gather_interior2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff,
+                             int np, int nvar, double* out, cudaStream_t s, bool f32) {
   for (int base = 0; base < np; base += 65535) {
     const int n = std::min(65535, np - base);
-    gather_interior2_kernel<<<dim3(8, n), 128, 0, s>>>(pool, patches, plist + base, outoff + base, nvar, out);
+    if (f32)
+      gather_interior2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, outoff + base, nvar, out);
+    else
+      gather_interior2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, outoff + base, nvar, out);
     AMR_CUDA(cudaGetLastError());
   }
 }

@@ -41,8 +41,9 @@ struct StepParams {
   int mcapa;
 };
 
+// pool: the patch pool, of double, or of float in the FP32 form (offsets count elements)
 struct StepArgs {
-  double* pool;
+  void* pool;
   double* regs;
   const PatchDev* patches;
   const StepWork* work;
@@ -86,7 +87,7 @@ struct BcOp {
 };
 
 struct FillArgs {
-  double* pool;
+  void* pool;
   double* regs;
   const PatchDev* patches;
   const ScratchRect* rects;
@@ -100,7 +101,7 @@ struct FillArgs {
 };
 
 struct BcArgs {
-  double* pool;
+  void* pool;
   const PatchDev* patches;
   const ScratchRect* rects;
   const BcOp* ops;
@@ -117,24 +118,26 @@ struct AvgRect { int cpatch, kpatch; int ci0, cj0, ni, nj; int fi0, fj0; };  // 
 
 struct GaugeJob { int patch; int ii, jj; int slot; double xoff, yoff; };
 
-// Launch wrappers (kernels2d.cu)
-void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s);
-void launch_fill(const FillArgs& a, cudaStream_t s);
-void launch_bc(const BcArgs& a, int phase, cudaStream_t s);
-void launch_qad2(int solver, double* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
-                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s);
-void launch_upbnd(double* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
-                  const UpbndTerm* terms, double area, int nvar, cudaStream_t s);
-void launch_average(double* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
-                    cudaStream_t s);
-void launch_flags2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
-                   int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s);
-void launch_gauges2(const double* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
-                    double* out, cudaStream_t s);
-void launch_zero_tiny(double* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s);
-void launch_mass2(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s);
-void launch_gather_interior2(const double* pool, const PatchDev* patches, const int* plist, const long long* outoff,
-                             int np, int nvar, double* out, cudaStream_t s);
-size_t step2_smem_bytes(int solver);
+// Launch wrappers (kernels2d.cu). f32: the pool holds float (the FP32 form): storage,
+// Riemann solves and flux differencing in FP32; flux registers, register corrections,
+// time interpolation weights, averages and totals in FP64.
+void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s, bool f32);
+void launch_fill(const FillArgs& a, cudaStream_t s, bool f32);
+void launch_bc(const BcArgs& a, int phase, cudaStream_t s, bool f32);
+void launch_qad2(int solver, void* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
+                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s, bool f32);
+void launch_upbnd(void* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
+                  const UpbndTerm* terms, double area, int nvar, cudaStream_t s, bool f32);
+void launch_average(void* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
+                    cudaStream_t s, bool f32);
+void launch_flags2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
+                   int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s, bool f32);
+void launch_gauges2(const void* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
+                    double* out, cudaStream_t s, bool f32);
+void launch_zero_tiny(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32);
+void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32);
+void launch_gather_interior2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff,
+                             int np, int nvar, double* out, cudaStream_t s, bool f32);
+size_t step2_smem_bytes(int solver, bool f32);
 
 }  // namespace amrb

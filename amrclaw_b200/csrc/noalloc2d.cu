@@ -54,7 +54,7 @@ __global__ void fill_kernel_fixed(FillArgs a, const double* scratch, long long o
   if (o.dst_patch >= 0) {
     const PatchDev& P = a.patches[o.dst_patch];
     ldi = P.mitot; plane = (long long)P.mitot * P.mjtot;
-    dst = a.pool + P.q[P.cur];
+    dst = static_cast<double*>(a.pool) + P.q[P.cur];
   } else {
     const ScratchRect& R = a.rects[o.dst_rect];
     ldi = R.ni; plane = (long long)R.ni * R.nj;
@@ -67,8 +67,8 @@ __global__ void fill_kernel_fixed(FillArgs a, const double* scratch, long long o
     const long long sk = (long long)(o.sj0 + jb) * S.mitot + (o.si0 + ia);
     int mode = 0; double ai = 1.0, ac = 0.0;
     if (o.level >= 0) { mode = a.modes.mode[o.level]; ai = a.modes.alphai[o.level]; ac = a.modes.alphac[o.level]; }
-    const double* qn = a.pool + S.q[S.cur];
-    const double* qo = a.pool + S.q[1 - S.cur];
+    const double* qn = static_cast<double*>(a.pool) + S.q[S.cur];
+    const double* qo = static_cast<double*>(a.pool) + S.q[1 - S.cur];
     for (int m = 0; m < nvar; ++m) {
       double v;
       if (mode == 0) v = qn[m * sp + sk];
@@ -146,7 +146,7 @@ __global__ void bc_kernel_fixed(BcArgs a, int phase, const double* scratch, long
   if (op >= a.nops) return;
   const BcOp o = a.ops[op];
   double* v; const int nrow = o.nrow, ncol = o.ncol;
-  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = a.pool + P.q[P.cur]; }
+  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = static_cast<double*>(a.pool) + P.q[P.cur]; }
   else v = const_cast<double*>(scratch) + (a.rects[o.dst_rect].off - off0);
   const long long plane = (long long)nrow * ncol;
   auto V = [&](int m, int i, int j) -> double& { return v[m * plane + (long long)(j - 1) * nrow + (i - 1)]; };

@@ -33,6 +33,13 @@ const char* amrgpu_last_error(void);
  * src/3d/amr3.f90 (domain.f, setgrd.f, ginit.f of src/3d). */
 int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu_ctx** ctx);
 
+/* amrgpu_init with a choice of precision. precision_bits = 64: the FP64 path, bit-
+ * identical to the reference's arithmetic. precision_bits = 32: the FP32 form (2D runs):
+ * patch storage, ghost values, Riemann solves and flux differencing in FP32; flux
+ * registers (fluxsv/fluxad/qad sums), register corrections, averaging sums, totals and
+ * time/dt bookkeeping in FP64. No counterpart in the reference (FP64 only). */
+int amrgpu_init_precision(const char* rundir, const char* outdir, int write_output, int precision_bits, amrgpu_ctx** ctx);
+
 /* 1: advance every patch of a level in one launch (batched path, default);
  * 0: one launch per patch (plain per-patch path). */
 int amrgpu_set_batched(amrgpu_ctx* ctx, int batched);
@@ -86,7 +93,8 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
  * amrgpu_run call, cell updates of that call, 1 when tfinal was reached,
  * bytes of initial data copied host to device, then regrid seconds spent in:
  * device flagging, host flag processing, clustering, new-grid fill, register
- * and list set-up, device-program compilation. */
+ * and list set-up, device-program compilation, then the number of space dimensions
+ * and the precision in bits (64 or 32). */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 
 /* Hierarchy rows in output order (valout.f90 loop order): (grid_number, level,

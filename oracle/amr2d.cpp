@@ -1043,7 +1043,7 @@ struct Amr2 {
     const double hx = hxposs[level], hy = hyposs[level], delt = possk[level];
     const int nxg = g.ihi - g.ilo + 1, nyg = g.jhi - g.jlo + 1;
     const int mitot = nxg + 2 * nghost, mjtot = nyg + 2 * nghost;
-    if (level < mxnest) g.q2 = g.q1;
+    if (level < mxnest || dbg_keep_input) g.q2 = g.q1;
     const double xlow = g.xlo - nghost * hx, ylow = g.ylo - nghost * hy;
     if (g.has_ffl) {
       const int lenbc = 2 * (nxg / intratx[level - 1] + nyg / intraty[level - 1]);
@@ -2209,15 +2209,29 @@ struct Amr2 {
 
   // ================================================================ tick.f
   double tick_seconds = 0, regrid_seconds = 0;
+  // tick.f runs once per program; here a run may be split by max_cycles, so the
+  // scheduler's state (cycle count, output index, level times) persists across calls
+  // test hook: stop the scheduler right after the n-th level substep of a call
+  struct DebugStop {};
+  int dbg_stop = 0, dbg_count = 0;
+  bool dbg_keep_input = false;  // test hook: keep store2 on the finest level too (the step's ghost-filled input)
+  bool tick_started = false;
+  int tk_nextout = 0;
+  double tk_tlevel[12] = {0};
   void tick(double start_time) {
-    double dtnew[12], tlevel[12];
+    double dtnew[12];
+    double* tlevel = tk_tlevel;
     int ntogo[12];
-    ncycle = 0;
+    int cycles = 0;
     setbestsrc();
     int nextout = 0;
     if (iout == 0) { iout = IINFINITY; nextout = 0; if (nout > 0) nextout = 1; }
-    tlevel[1] = time;
-    for (int i = 2; i <= mxnest; ++i) tlevel[i] = tlevel[1];
+    if (tick_started) nextout = tk_nextout;
+    if (!tick_started) {
+      tlevel[1] = time;
+      for (int i = 2; i <= mxnest; ++i) tlevel[i] = tlevel[1];
+    }
+    tick_started = true;
     while (!(ncycle >= nstop || time >= tfinal)) {
       double outtime;
       if (nout > 0) outtime = (nextout <= nout) ? tout[nextout - 1] : RINFINITY;
@@ -2253,6 +2267,7 @@ struct Amr2 {
         // 90
         double dtlevnew;
         advanc(level, dtlevnew);
+        if (dbg_stop > 0 && ++dbg_count >= dbg_stop) throw DebugStop();
         ntogo[level] = ntogo[level] - 1;
         dtnew[level] = std::min(dtnew[level], dtlevnew);
         tlevel[level] = tlevel[level] + possk[level];
@@ -2299,8 +2314,10 @@ struct Amr2 {
         for (int i = 2; i <= mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
       }
       if ((ncycle % iout == 0) || dumpout) valout(1, lfine, time);
-      if (max_cycles > 0 && ncycle >= max_cycles) break;
+      ++cycles;
+      if (max_cycles > 0 && cycles >= max_cycles) break;
     }
+    tk_nextout = nextout;
   }
   int max_cycles = 0;
   static double omp_wtime_safe() {
@@ -2384,6 +2401,36 @@ int oracle2d_lfine(void* h) { return ((Amr2*)h)->lfine; }
 int oracle2d_ncycle(void* h) { return ((Amr2*)h)->ncycle; }
 
 // Hierarchy as rows of (grid_number, level, ilo, ihi, jlo, jhi) in output order (level, list order).
+// Test hook: run until the n-th level substep from now (0: no stop), leaving the state
+// right after that substep. Returns 1 if it stopped there, 0 if the run ended first.
+int oracle2d_run_substeps(void* h, int n) {
+  Amr2* a = (Amr2*)h;
+  a->dbg_stop = n; a->dbg_count = 0; a->dbg_keep_input = true;
+  a->max_cycles = 0;
+  int stopped = 0;
+  try { a->tick(a->t0); } catch (Amr2::DebugStop&) { stopped = 1; }
+  a->dbg_stop = 0;
+  return stopped;
+}
+// Test hook: the enlarged array of grid `grid` (store 1 or 2) as [m][j][i]; returns the
+// number of doubles (nvar * mitot * mjtot), 0 if the grid does not exist.
+long oracle2d_patch(void* h, int grid, int store, double* out, long cap) {
+  Amr2* a = (Amr2*)h;
+  if (grid <= 0 || grid >= (int)a->node.size()) return 0;
+  const auto& g = a->node[grid];
+  const std::vector<double>& q = store == 2 ? g.q2 : g.q1;
+  const int mitot = g.ihi - g.ilo + 1 + 2 * a->nghost, mjtot = g.jhi - g.jlo + 1 + 2 * a->nghost;
+  const long n = (long)a->nvar * mitot * mjtot;
+  if ((long)q.size() < n) return 0;
+  if (out)
+    for (int m = 0; m < a->nvar && m * (long)mitot * mjtot < cap; ++m)
+      for (int j = 0; j < mjtot; ++j)
+        for (int i = 0; i < mitot; ++i) {
+          const long at = ((long)m * mjtot + j) * mitot + i;
+          if (at < cap) out[at] = q[(size_t)m + (size_t)a->nvar * ((size_t)i + (size_t)mitot * j)];
+        }
+  return n;
+}
 int oracle2d_grids(void* h, int* out, int cap) {
   Amr2* a = (Amr2*)h;
   int n = 0;

@@ -72,3 +72,27 @@ def test_advection_bench_config_short_run():
     rd = configs.advection_square_bench(n=50, tfinal=2.0, levels=3)
     ref, gpu = _both(rd, 1, max_cycles=12)
     _assert_identical(ref, gpu)
+
+
+def test_four_levels_wave_leaving_the_domain():
+    # a new fine grid whose coarse neighbourhood is not covered by the coarser level
+    # (filval/saveqc read the reference's initial zeros there), at an outflow boundary
+    from amrclaw_b200 import problems
+    ref, gpu = _both(problems.acoustics_pulse(64, levels=4, ratio=2, tfinal=0.4), 3)
+    _assert_identical(ref, gpu)
+
+
+def test_split_run_equals_one_run():
+    from amrclaw_b200 import Solver, problems
+    rd = problems.euler_quadrants(32, levels=3, ratio=2, tfinal=0.2)
+    with tempfile.TemporaryDirectory() as d:
+        rd.write(d)
+        o = Oracle2D(d)
+        o.run(0)
+        ref = dict(grids=o.grids(), values=o.values(), gauges=o.gauges(4), time=o.time(), mass=o.mass(), cells=o.cell_updates())
+        o.close()
+        with Solver(d) as s:
+            while not s.info()["finished"]:
+                s.run(3)
+            gpu = dict(grids=s.grids(), values=s.values(), info=s.info(), mass=s.mass())
+    _assert_identical(ref, gpu)
