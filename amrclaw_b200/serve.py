@@ -38,7 +38,7 @@ class Request:
     levels: int
     ratio: int
     tfinal: float
-    precision: str          # "fp64" (the FP32 form is requested as "fp32")
+    precision: str          # "fp64" or "fp32" (the FP32 form)
     params: dict = field(default_factory=dict)
 
     def rundata(self):
@@ -54,7 +54,8 @@ class Request:
     def est_bytes(self) -> int:
         """Device memory reserved for admission: the context's initial pool (two buffers of
         every level's worth of base grid, as the library sizes it), registers and scratch."""
-        pool = 8 * (self.nvar() * (self.n + 4) ** 2 * 8 * self.levels + (1 << 22))
+        word = 4 if self.precision == "fp32" else 8
+        pool = word * self.nvar() * (self.n + 4) ** 2 * 8 * self.levels + 8 * (1 << 22)
         return int(pool + (24 << 20))
 
 
@@ -109,9 +110,10 @@ class Result:
 
 
 def run_one(req: Request, keep_values: bool = False):
-    """One solve from start to tfinal on the current device: (cell updates, mass, values, device ms, pool peak)."""
+    """One solve from start to tfinal on the current device, in the request's precision:
+    (cell updates, mass, values, device ms, pool peak)."""
     from . import Solver
-    with Solver(req.rundata(), batched=True) as s:
+    with Solver(req.rundata(), batched=True, precision=req.precision) as s:
         s.run(0)
         inf = s.info()
         vals = s.values() if keep_values else None
@@ -122,7 +124,7 @@ def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: b
           clock: Callable[[], float] = time.perf_counter, runner: Optional[Callable] = None) -> dict:
     """Admit the requests as they arrive (arrival times relative to the call), run them
     concurrently, return the per-request results and the summary. `runner(req, keep_values)`
-    performs one solve (default run_one: the FP64 device path for every request)."""
+    performs one solve (default run_one: the device path in the request's precision)."""
     runner = runner or run_one
     pending = sorted(requests, key=lambda r: r.arrival)
     waiting: List[Request] = []
@@ -183,7 +185,6 @@ def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: b
         "peak_concurrent": state["peak_active"], "peak_reserved_bytes": state["peak_used"],
         "budget_bytes": budget_bytes, "slots": slots,
         "fp32_requests": sum(1 for r in requests if r.precision == "fp32"),
-        "fp32_form": "not built: fp32 requests run on the fp64 path",
     }
     return {"summary": summary, "results": sorted(results, key=lambda r: r.rid)}
 

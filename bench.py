@@ -113,6 +113,41 @@ def flush_l2(buf):
     torch.cuda.synchronize()
 
 
+def fp32_leg(cpu_threads: int) -> dict:
+    """The FP32 form on the 2D acoustic pulse (64^2 base grid, 4 levels, ratio 2, t = 0.4):
+    device throughput of the FP32 and FP64 runs, and the FP32 run's level-1 L1 error and
+    mass against the FP64 oracle (the reference's arithmetic)."""
+    from amrclaw_b200 import Solver, fields, problems
+    from oracle.pyoracle import Oracle2D
+    rd = problems.acoustics_pulse(64, levels=4, ratio=2, tfinal=0.4)
+    out = {"workload": "acoustics2d_pulse", "base_grid": "64x64", "levels": 4, "ratio": 2, "tfinal": 0.4}
+    with tempfile.TemporaryDirectory() as d:
+        rd.write(d)
+        o = Oracle2D(d, threads=cpu_threads)
+        o.run(0)
+        g64, v64, m64 = o.grids(), o.values(), o.mass()
+        o.close()
+        res = {}
+        for prec in ("fp64", "fp32"):
+            with Solver(d, precision=prec) as s:
+                s.run(0)
+                inf = s.info()
+                res[prec] = (s.grids(), s.values(), s.mass(), inf["cell_updates"] / (inf["last_run_ms"] * 1e-3))
+    ref = fields.level_array(g64, v64, 3, 1, (64, 64))
+    for prec, (g, v, m, cups) in res.items():
+        _, rel = fields.l1_error(fields.level_array(g, v, 3, 1, (64, 64)), ref, (2.0 / 64) ** 2)
+        out[prec] = {"value": cups, "unit": "cell-updates/s", "l1_rel_err_vs_fp64_oracle": [float(x) for x in rel],
+                     "mass_rel_diff_vs_fp64_oracle": abs(m - m64) / abs(m64)}
+    return out
+
+
+def serving_leg(n_requests: int = 64) -> dict:
+    """A seeded Poisson stream (200 requests/s) of small 2D solves, FP64/FP32 mixed."""
+    from amrclaw_b200 import serve
+    reqs = serve.synthetic_requests(n_requests, rate=200.0, seed=1, scale="small")
+    return serve.serve(reqs, budget_bytes=16 << 30, slots=16)["summary"]
+
+
 def run_reference(args, rank):
     """The reference's CPU path: the CPU restatement (the reference Fortran cannot be built here)."""
     if rank != 0:
@@ -243,6 +278,9 @@ def main():
             dist.destroy_process_group()
         return
     peak, peak_kind = peaks()
+    os.environ.setdefault("AMRGPU_HOST_THREADS", "2")
+    fp32 = fp32_leg(os.cpu_count() or 1) if not args.no_cpu_baseline else None
+    serving = serving_leg() if not args.no_cpu_baseline else None
     achieved = kern_cells * bytes_per_update / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
     cpu = None
     if not args.no_cpu_baseline:
@@ -266,6 +304,8 @@ def main():
         "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": pms / args.steps,
                   "speedup_batched_over_plain": value / plain_value if plain_value else None},
         "l1_err_vs_fp64": 0.0,
+        "fp32_form": fp32,
+        "serving": serving,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": None,
                      "kernel": "sweep3<1..3> + face3 + update3" if ndim == 3 else "step2 sweeps + update",
