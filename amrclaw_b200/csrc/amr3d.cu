@@ -50,10 +50,10 @@ struct HPatch3 {
 struct Prog3 {
   std::vector<Rect3> rects;
   std::vector<Fill3Op> ops;
-  std::vector<int> op_stage;
+  std::vector<int> op_stage, op_owner;  // owner: index of the patch (in the level list) the op serves
   std::vector<Bc3Op> bcs;
-  std::vector<int> bc_stage;
-  int nstages = 0;
+  std::vector<int> bc_stage, bc_owner;
+  int nstages = 0, nowners = 0;
   long long scratch_off = -1, scratch_len = 0, scratch_alloc = 0;
   // the scratch starts at zero each run: programs whose rects come from icall copies
   // (saveqc.f, filval.f) leave uncovered cells at the reference's initial 0
@@ -63,20 +63,29 @@ struct Prog3 {
   DBuf<Fill3Chunk> d_chunks;
   DBuf<Bc3Op> d_bcs;
   std::vector<int> ch_lo, ch_hi, bc_lo, bc_hi;
-  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; scratch_len = 0; zero_scratch = false; }
+  // [stage][owner] chunk and bc ranges, for replaying the program one patch at a time
+  std::vector<int> own_ch_lo, own_ch_hi, own_bc_lo, own_bc_hi;
+  void clear() {
+    rects.clear(); ops.clear(); op_stage.clear(); op_owner.clear(); bcs.clear(); bc_stage.clear(); bc_owner.clear();
+    nstages = 0; nowners = 0; scratch_len = 0; zero_scratch = false;
+  }
   int add_rect(int ni, int nj, int nk, int nvar) {
     Rect3 r; r.off = scratch_len; r.ni = ni; r.nj = nj; r.nk = nk;
     scratch_len += Arena::rnd((long long)ni * nj * nk * nvar);
     rects.push_back(r);
     return (int)rects.size() - 1;
   }
-  void add_op(const Fill3Op& o, int st) { ops.push_back(o); op_stage.push_back(st); nstages = std::max(nstages, st + 1); }
-  void add_bc(const Bc3Op& b, int st) { bcs.push_back(b); bc_stage.push_back(st); nstages = std::max(nstages, st + 1); }
+  void add_op(const Fill3Op& o, int st, int owner = 0) {
+    ops.push_back(o); op_stage.push_back(st); op_owner.push_back(owner); nstages = std::max(nstages, st + 1); nowners = std::max(nowners, owner + 1);
+  }
+  void add_bc(const Bc3Op& b, int st, int owner = 0) {
+    bcs.push_back(b); bc_stage.push_back(st); bc_owner.push_back(owner); nstages = std::max(nstages, st + 1); nowners = std::max(nowners, owner + 1);
+  }
   void free_dev() { d_rects.free(); d_ops.free(); d_chunks.free(); d_bcs.free(); }
 };
 
 // Appends program S after the ops already in D (rect indices and scratch offsets shifted).
-void merge_prog(Prog3& D, const Prog3& S) {
+void merge_prog(Prog3& D, const Prog3& S, int owner = 0) {
   const int r0 = (int)D.rects.size();
   const long long s0 = D.scratch_len;
   for (Rect3 r : S.rects) { r.off += s0; D.rects.push_back(r); }
@@ -85,12 +94,12 @@ void merge_prog(Prog3& D, const Prog3& S) {
     Fill3Op o = S.ops[k];
     if (o.dst_patch < 0) o.dst_rect += r0;
     if (o.kind != F3_COPY) o.src += r0;
-    D.add_op(o, S.op_stage[k]);
+    D.add_op(o, S.op_stage[k], owner);
   }
   for (size_t k = 0; k < S.bcs.size(); ++k) {
     Bc3Op b = S.bcs[k];
     if (b.dst_patch < 0) b.dst_rect += r0;
-    D.add_bc(b, S.bc_stage[k]);
+    D.add_bc(b, S.bc_stage[k], owner);
   }
 }
 
@@ -101,6 +110,7 @@ struct Plan3 {
   long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;  // items: interfaces per direction
   std::vector<Fsv3> fsv;
   std::vector<long long> seg0;  // register segments (lenbc) prefix over plist; fad/qad lists are built from it on the device
+  std::vector<long long> fsv0;  // fluxsv entries prefix over plist
   long long nseg = 0;
   std::vector<Upbnd3Cell> upc;
   std::vector<Upbnd3Term> upt;
@@ -168,6 +178,7 @@ class Amr3Gpu : public AmrSolver {
   size_t lv_host_cap = 0;
   DBuf<double> d_gauge_out;
   unsigned long long* d_cfl = nullptr;
+  unsigned long long* h_cfl = nullptr;  // pinned
   double* d_mass = nullptr;
   cudaStream_t st = nullptr;
   LevelConst lc{};
@@ -204,6 +215,7 @@ class Amr3Gpu : public AmrSolver {
     lv_boxes.free(); lv_proj.free(); lv_c0.free(); lv_plist.free();
     if (lv_host) cudaFreeHost(lv_host);
     if (d_cfl) cudaFree(d_cfl);
+    if (h_cfl) cudaFreeHost(h_cfl);
     if (d_mass) cudaFree(d_mass);
     for (cudaEvent_t e : {ev_a, ev_b, ev_run0, ev_run1}) if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
@@ -543,7 +555,7 @@ class Amr3Gpu : public AmrSolver {
     const std::vector<int>& G = lgrids[lev];
     std::vector<Prog3> part(G.size());
     pool_host.run((int)G.size(), [&](int k) { compile_bound_patch(part[k], lev, G[k]); });
-    for (auto& q : part) merge_prog(P, q);
+    for (size_t k = 0; k < part.size(); ++k) merge_prog(P, part[k], (int)k);
     upload_prog(P);
   }
 
@@ -605,37 +617,76 @@ class Amr3Gpu : public AmrSolver {
     P.d_rects.upload(rects, st, stg);
     std::vector<int> oidx(P.ops.size());
     for (size_t i = 0; i < oidx.size(); ++i) oidx[i] = (int)i;
-    std::stable_sort(oidx.begin(), oidx.end(), [&](int a, int b) { return P.op_stage[a] < P.op_stage[b]; });
+    // stage-major, then owner (patch) order: a stage's ops are one range, and so are one
+    // patch's ops within a stage (ops of one owner keep their compile order)
+    std::stable_sort(oidx.begin(), oidx.end(), [&](int a, int b) {
+      return P.op_stage[a] != P.op_stage[b] ? P.op_stage[a] < P.op_stage[b] : P.op_owner[a] < P.op_owner[b];
+    });
+    const int no = std::max(P.nowners, 1);
     std::vector<Fill3Op> ops;
     std::vector<Fill3Chunk> ch;
     P.ch_lo.assign(P.nstages, 0); P.ch_hi.assign(P.nstages, 0);
+    P.own_ch_lo.assign((size_t)P.nstages * no, 0); P.own_ch_hi.assign((size_t)P.nstages * no, 0);
     int s = -1;
     for (int k : oidx) {
       const int stg_ = P.op_stage[k];
       while (s < stg_) { ++s; P.ch_lo[s] = (int)ch.size(); P.ch_hi[s] = (int)ch.size(); }
       const int id = (int)ops.size();
       ops.push_back(P.ops[k]);
+      const size_t ow = (size_t)s * no + P.op_owner[k];
+      if (P.own_ch_hi[ow] == P.own_ch_lo[ow]) P.own_ch_lo[ow] = P.own_ch_hi[ow] = (int)ch.size();
       const long long cells = (long long)P.ops[k].ni * P.ops[k].nj * P.ops[k].nk;
       for (long long c0 = 0; c0 < cells; c0 += 128) ch.push_back(Fill3Chunk{id, c0, (int)std::min<long long>(128, cells - c0)});
       P.ch_hi[s] = (int)ch.size();
+      P.own_ch_hi[ow] = (int)ch.size();
     }
     while (s + 1 < P.nstages) { ++s; P.ch_lo[s] = P.ch_hi[s] = (int)ch.size(); }
     std::vector<int> bidx(P.bcs.size());
     for (size_t i = 0; i < bidx.size(); ++i) bidx[i] = (int)i;
-    std::stable_sort(bidx.begin(), bidx.end(), [&](int a, int b) { return P.bc_stage[a] < P.bc_stage[b]; });
+    std::stable_sort(bidx.begin(), bidx.end(), [&](int a, int b) {
+      return P.bc_stage[a] != P.bc_stage[b] ? P.bc_stage[a] < P.bc_stage[b] : P.bc_owner[a] < P.bc_owner[b];
+    });
     std::vector<Bc3Op> bcs;
     P.bc_lo.assign(P.nstages, 0); P.bc_hi.assign(P.nstages, 0);
+    P.own_bc_lo.assign((size_t)P.nstages * no, 0); P.own_bc_hi.assign((size_t)P.nstages * no, 0);
     s = -1;
     for (int k : bidx) {
       const int stg_ = P.bc_stage[k];
       while (s < stg_) { ++s; P.bc_lo[s] = (int)bcs.size(); P.bc_hi[s] = (int)bcs.size(); }
+      const size_t ow = (size_t)s * no + P.bc_owner[k];
+      if (P.own_bc_hi[ow] == P.own_bc_lo[ow]) P.own_bc_lo[ow] = P.own_bc_hi[ow] = (int)bcs.size();
       bcs.push_back(P.bcs[k]);
       P.bc_hi[s] = (int)bcs.size();
+      P.own_bc_hi[ow] = (int)bcs.size();
     }
     while (s + 1 < P.nstages) { ++s; P.bc_lo[s] = P.bc_hi[s] = (int)bcs.size(); }
     P.d_ops.upload(ops, st, stg);
     P.d_chunks.upload(ch, st, stg);
     P.d_bcs.upload(bcs, st, stg);
+  }
+
+  // one patch's part of a program (the per-patch bound.f call of the plain path)
+  void run_prog_owner(Prog3& P, const SrcMode& modes, int owner) {
+    const int no = std::max(P.nowners, 1);
+    if (owner >= no) return;
+    for (int s = 0; s < P.nstages; ++s) {
+      const size_t ow = (size_t)s * no + owner;
+      if (P.own_ch_hi[ow] > P.own_ch_lo[ow]) {
+        Fill3Args a{};
+        a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
+        a.chunks = P.d_chunks.d + P.own_ch_lo[ow]; a.nchunks = P.own_ch_hi[ow] - P.own_ch_lo[ow]; a.nvar = nvar; a.modes = modes;
+        a.lc = lc; a.xlower = xlower; a.ylower = ylower; a.zlower = zlower;
+        launch_fill3(a, st);
+        ++nkernels;
+      }
+      if (P.own_bc_hi[ow] > P.own_bc_lo[ow]) {
+        Bc3Args b{};
+        b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.own_bc_lo[ow];
+        b.nops = P.own_bc_hi[ow] - P.own_bc_lo[ow]; b.nvar = nvar;
+        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st);
+        nkernels += 3;
+      }
+    }
   }
 
   void run_prog(Prog3& P, const SrcMode& modes) {
@@ -694,7 +745,8 @@ class Amr3Gpu : public AmrSolver {
     }
     L.faces = L.face0[np]; L.cells = L.cell0[np];
     L.seg0.assign(np + 1, 0);
-    std::vector<long long> fsv0(np + 1, 0);
+    std::vector<long long>& fsv0 = L.fsv0;
+    fsv0.assign(np + 1, 0);
     for (int k = 0; k < np; ++k) {
       const HPatch3& g = node[L.plist[k]];
       L.seg0[k + 1] = L.seg0[k] + ((lev > 1 && g.ffl >= 0) ? g.lenbc : 0);
@@ -909,6 +961,10 @@ class Amr3Gpu : public AmrSolver {
     });
   }
 
+  // A regrid marks the plans of the levels it changed and compiles them all (ensure_all);
+  // every consumer also ensures its own plan, so a plan is never used stale.
+  enum { NEED_BOUND = 1, NEED_SAVEQC = 2, NEED_STEP = 4, NEED_UPDATE = 8 };
+  int dirty[12] = {0};
   void compile_all(int lbase = 0) {
     HPROF("compile_all3");
     PhaseTimer tph(hprof);
@@ -916,15 +972,24 @@ class Amr3Gpu : public AmrSolver {
     sync_descriptors();
     tph.close();
     for (int lev = 1; lev <= p.mxnest; ++lev) {
-      if (lev > lfine) { plan[lev].plist.clear(); continue; }
-      if (lev > lbase) compile_bound(lev);
-      if (lev >= lbase) {
-        compile_saveqc(lev);
-        compile_step(lev);
-        compile_update(lev);
-      }
+      if (lev > lfine) { plan[lev].plist.clear(); dirty[lev] = 0; continue; }
+      if (lev > lbase) dirty[lev] |= NEED_BOUND;
+      if (lev >= lbase) dirty[lev] |= NEED_SAVEQC | NEED_STEP | NEED_UPDATE;
     }
+    ensure_all();
   }
+  void ensure(int lev, int what) {
+    if (lev < 1 || lev > p.mxnest) return;
+    const int todo = dirty[lev] & what;
+    if (!todo) return;
+    dirty[lev] &= ~todo;
+    if (todo & NEED_BOUND) compile_bound(lev);
+    if (todo & NEED_SAVEQC) compile_saveqc(lev);
+    if (todo & NEED_STEP) compile_step(lev);
+    if (todo & NEED_UPDATE) compile_update(lev);
+  }
+  void ensure_all() { for (int lev = 1; lev <= p.mxnest; ++lev) ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP | NEED_UPDATE); }
+
 
   // ================================================================ level substep
   // intfil.f:115-154: which buffer of a source level serves time t (teps = possk/10)
@@ -944,39 +1009,68 @@ class Amr3Gpu : public AmrSolver {
     }
     return M;
   }
-  void bound_level(int lev, double t) { run_prog(plan[lev].bound, modes_for(lev, t)); }
+  void bound_level(int lev, double t) {
+    ensure(lev, NEED_BOUND);
+    run_prog(plan[lev].bound, modes_for(lev, t));
+  }
 
   // advanc.f:4-139 with par_advanc (:166-303) for all patches of the level at once
   double advanc(int lev) {
     HPROF("advanc3");
+    ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP);
     PhaseTimer tph(hprof);
     Plan3& L = plan[lev];
     const double t = node[lgrids[lev][0]].time;
     const double dt = possk[lev];
     tph.next("adv_launch");
-    bound_level(lev, t);
-    if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
-    if (lev > 1 && L.nseg > 0) {
-      launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.nseg, sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st);
-      ++nkernels;
-    }
-    sample_gauges(lev);
-    AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
-    if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
     Step3Args a{};
     a.pool = pool.d; a.patches = d_patches.d; a.sp = sp;
     a.stash = d_stash.d; a.stash_stride = L.slots; a.flux = d_flux.d; a.flux_stride = L.faces;
     a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.dz = hzposs[lev]; a.cflmax = d_cfl;
+    const bool kids = lev + 1 <= p.mxnest && lstart[lev + 1] != 0;
     if (batched) {
+      // every patch of the level in one launch per routine
+      bound_level(lev, t);
+      if (kids) { SrcMode M{}; run_prog(L.saveqc, M); }
+      if (lev > 1 && L.nseg > 0) {
+        launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.nseg, sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st);
+        ++nkernels;
+      }
+      sample_gauges(lev);
+      AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+      if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
       a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
       launch_step3(a, L.items, L.faces, L.cells, st);
       nkernels += 5;
+      if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
+      if (!L.fsv.empty()) {
+        launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
+        ++nkernels;
+      }
+      if (lev > 1 && L.nseg > 0) {
+        launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.nseg, nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
+        ++nkernels;
+      }
     } else {
-      // one patch per launch sequence: per-patch prefix arrays are views of the level's
+      // the reference's per-grid structure (advanc.f): bound for every grid, saveqc for the
+      // level, then par_advanc per grid (qad, stepgrid, fluxsv, fluxad), each grid its own
+      // launches; the per-grid arrays are views of the level's
       const int np = (int)L.plist.size();
+      const SrcMode M = modes_for(lev, t);
+      for (int k = 0; k < np; ++k) run_prog_owner(L.bound, M, k);
+      if (kids) { SrcMode Z{}; run_prog(L.saveqc, Z); }
+      sample_gauges(lev);
+      AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+      if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
       build_plain_views(L);
+      const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
       for (int k = 0; k < np; ++k) {
+        const long long q0 = L.seg0[k], nq = L.seg0[k + 1] - L.seg0[k];
+        if (lev > 1 && nq > 0) {
+          launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d + q0, (int)nq, sp, nvar, hx, hy, hz, dt, st);
+          ++nkernels;
+        }
         Step3Args b = a;
         b.plist = L.d_plist.d + k; b.np = 1;
         b.sweep0 = d_pp_sweep.d + (size_t)12 * k; b.comp0 = d_pp_sweep.d + (size_t)12 * k + 6;
@@ -985,22 +1079,24 @@ class Amr3Gpu : public AmrSolver {
         for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
         launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st);
         nkernels += 5;
+        const long long f0 = L.fsv0[k], nf = L.fsv0[k + 1] - L.fsv0[k];
+        if (nf > 0) {
+          launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d + f0, (int)nf, nvar, dt, hx, hy, hz, st);
+          ++nkernels;
+        }
+        if (lev > 1 && nq > 0) {
+          launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d + q0, (int)nq, nvar, dt, hx, hy, hz, st);
+          ++nkernels;
+        }
       }
-    }
-    if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
-    if (!L.fsv.empty()) {
-      launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
-      ++nkernels;
-    }
-    if (lev > 1 && L.nseg > 0) {
-      launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.nseg, nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
-      ++nkernels;
+      if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
     }
     flip_level(lev);
-    unsigned long long cbits = 0;
-    AMR_CUDA(cudaMemcpyAsync(&cbits, d_cfl, sizeof(cbits), cudaMemcpyDeviceToHost, st));
+    // into pinned memory, so the copy is queued and the host goes on compiling
+    AMR_CUDA(cudaMemcpyAsync(h_cfl, d_cfl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     tph.next("adv_sync");
     sync_stream();
+    const unsigned long long cbits = *h_cfl;
     tph.close();
     double cmax;
     std::memcpy(&cmax, &cbits, sizeof(double));
@@ -1046,6 +1142,7 @@ class Amr3Gpu : public AmrSolver {
   // update.f:4-192 (upbnd then averaging)
   void update(int lev) {
     HPROF("update3");
+    ensure(lev, NEED_UPDATE);
     Plan3& L = plan[lev];
     const double vol = hxposs[lev] * hyposs[lev] * hzposs[lev];
     launch_upbnd3(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, vol, nvar, st);
@@ -1490,7 +1587,9 @@ class Amr3Gpu : public AmrSolver {
     pool.init((long long)nvar * (nxc + 4) * (nyc + 4) * (nzc + 4) * 32 + (1 << 22));
     regs.init(1 << 20);
     AMR_CUDA(cudaMalloc(&d_cfl, sizeof(unsigned long long)));
+    AMR_CUDA(cudaMallocHost((void**)&h_cfl, sizeof(unsigned long long)));
     AMR_CUDA(cudaMalloc(&d_mass, sizeof(double)));
+    stg.reserve((size_t)256 << 20);
     {
       // sweep staging and face fluxes: reserved at once for twice a level-1 sweep
       const long long n = (long long)nxc * nyc * nzc;

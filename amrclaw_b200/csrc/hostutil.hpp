@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -55,16 +56,21 @@ struct PhaseTimer {
 struct Arena {
   double* d = nullptr;
   long long cap = 0;
-  std::map<long long, long long> fr;  // free blocks: offset -> length
+  // free blocks indexed both ways: by offset (for coalescing) and by size (best fit in
+  // O(log n); a level with thousands of patches would make a first-fit scan quadratic)
+  std::map<long long, long long> fr;              // offset -> length
+  std::set<std::pair<long long, long long>> bysz;  // (length, offset)
   long long inuse = 0, peak = 0;
   static long long rnd(long long n) { return (n + 31) / 32 * 32; }
   void init(long long n) {
     n = rnd(std::max<long long>(n, 1 << 20));
     AMR_CUDA(cudaMalloc(&d, sizeof(double) * n));
     cap = n;
-    fr.clear();
-    fr[0] = n;
+    fr.clear(); bysz.clear();
+    add_free(0, n);
   }
+  void add_free(long long off, long long n) { fr[off] = n; bysz.emplace(n, off); }
+  void del_free(std::map<long long, long long>::iterator it) { bysz.erase({it->second, it->first}); fr.erase(it); }
   void grow(long long need) {
     // kernels on any stream may still use the pool: let them finish before it moves
     AMR_CUDA(cudaDeviceSynchronize());
@@ -78,25 +84,26 @@ struct Arena {
     cap = ncap;
   }
   void release_raw(long long off, long long n) {
-    auto it = fr.emplace(off, n).first;
-    if (it != fr.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) { pv->second += it->second; fr.erase(it); it = pv; }
+    auto nx = fr.lower_bound(off);
+    if (nx != fr.begin()) {
+      auto pv = std::prev(nx);
+      if (pv->first + pv->second == off) { off = pv->first; n += pv->second; del_free(pv); }
     }
-    auto nx = std::next(it);
-    if (nx != fr.end() && it->first + it->second == nx->first) { it->second += nx->second; fr.erase(nx); }
+    nx = fr.lower_bound(off);
+    if (nx != fr.end() && off + n == nx->first) { n += nx->second; del_free(nx); }
+    add_free(off, n);
   }
   long long alloc(long long n) {
     n = rnd(std::max<long long>(n, 1));
     for (int pass = 0; pass < 2; ++pass) {
-      for (auto it = fr.begin(); it != fr.end(); ++it)
-        if (it->second >= n) {
-          const long long off = it->first, len = it->second;
-          fr.erase(it);
-          if (len > n) fr[off + n] = len - n;
-          inuse += n; peak = std::max(peak, inuse);
-          return off;
-        }
+      auto b = bysz.lower_bound({n, -1});  // smallest block that fits, lowest offset among equals
+      if (b != bysz.end()) {
+        const long long len = b->first, off = b->second;
+        del_free(fr.find(off));
+        if (len > n) add_free(off + n, len - n);
+        inuse += n; peak = std::max(peak, inuse);
+        return off;
+      }
       grow(n);
     }
     throw std::runtime_error("device pool exhausted");
@@ -133,6 +140,14 @@ struct Staging {
     return dst;
   }
   void reset() { used = 0; }
+  // pin the ring once at start-up: growing it later (cudaFreeHost + cudaMallocHost) costs
+  // milliseconds that vary with the host's memory state
+  void reserve(size_t bytes) {
+    if (bytes <= cap) return;
+    if (h) AMR_CUDA(cudaFreeHost(h));
+    cap = bytes; used = 0;
+    AMR_CUDA(cudaMallocHost((void**)&h, cap));
+  }
   void destroy() { if (h) cudaFreeHost(h); h = nullptr; cap = used = 0; }
 };
 

@@ -67,6 +67,9 @@ __device__ __forceinline__ double philim3(int meth, double r) {
 //            stored for that cell, term by term in flux3.f's statement order
 constexpr int SW_T = 128;
 constexpr int SW_OWN = SW_T - 3;
+#ifndef SW_MINB
+#define SW_MINB 3  // resident tiles per SM the register budget is sized for
+#endif
 
 // (a - 3*b) (m4 = 2) or a: the doubly transverse inputs of flux3.f:429-507
 __device__ __forceinline__ void dt_input(int m4, double sgn3, const double* a, const double* b, double* o) {
@@ -75,7 +78,7 @@ __device__ __forceinline__ void dt_input(int m4, double sgn3, const double* a, c
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(SW_T, 3) sweep3_kernel(Step3Args A) {
+__global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   __shared__ double sW[15][SW_T];
   const long long* c0 = A.comp0 + (long long)(DIR - 1) * (A.np + 1);
   const long long* s0 = A.sweep0 + (long long)(DIR - 1) * (A.np + 1);
