@@ -2132,8 +2132,7 @@ int amrgpu_init_precision(const char* rundir, const char* outdir, int write_outp
       s2->g.f32 = precision_bits == 32;
       s2->g.init(rundir);
     } else if (nd == 3) {
-      if (precision_bits != 64) throw std::runtime_error("the FP32 form is built for the 2D path only");
-      ctx->s.reset(amrb::make_solver3(rundir, outdir ? outdir : "", write_output != 0));
+      ctx->s.reset(amrb::make_solver3(rundir, outdir ? outdir : "", write_output != 0, precision_bits == 32));
     } else {
       throw std::runtime_error("num_dim must be 2 or 3");
     }

@@ -287,17 +287,28 @@ class Amr3Gpu : public AmrSolver {
     return m;
   }
   void putnod(int m) { node[m].nextfree = ndfree; ndfree = m; }
+  // Patch pool offsets count elements of the storage type: doubles, or floats in the FP32
+  // form (two per pool double; the pool's 32-double rounding keeps them 256-byte aligned).
+  bool f32 = false;
+  long long palloc(long long n) { return f32 ? pool.alloc((n + 1) / 2) * 2 : pool.alloc(n); }
+  void pfree(long long off, long long n) {
+    if (off < 0) return;
+    if (f32) pool.release(off / 2, (n + 1) / 2); else pool.release(off, n);
+  }
+  size_t elem() const { return f32 ? sizeof(float) : sizeof(double); }
+  char* pool_bytes() const { return reinterpret_cast<char*>(pool.d); }
+
   void alloc_patch(int m) {
     id_hwm = std::max(id_hwm, m + 1);
     HPatch3& g = node[m];
     g.nq = (long long)nvar * mitot(m) * mjtot(m) * mktot(m);
-    g.q0 = pool.alloc(g.nq);
-    g.q1 = pool.alloc(g.nq);
+    g.q0 = palloc(g.nq);
+    g.q1 = palloc(g.nq);
     g.cur = 0;
   }
   void free_patch(int m) {
     HPatch3& g = node[m];
-    pool.release(g.q0, g.nq); pool.release(g.q1, g.nq);
+    pfree(g.q0, g.nq); pfree(g.q1, g.nq);
     g.q0 = g.q1 = -1;
     if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
     g.ffl = -1; g.nffl = 0;
@@ -609,9 +620,9 @@ class Amr3Gpu : public AmrSolver {
 
   void upload_prog(Prog3& P) {
     HPROF("upload_prog3");
-    if (P.scratch_off >= 0) pool.release(P.scratch_off, P.scratch_alloc);
+    if (P.scratch_off >= 0) pfree(P.scratch_off, P.scratch_alloc);
     P.scratch_alloc = std::max<long long>(P.scratch_len, 1);
-    P.scratch_off = pool.alloc(P.scratch_alloc);
+    P.scratch_off = palloc(P.scratch_alloc);
     std::vector<Rect3> rects = P.rects;
     for (auto& r : rects) r.off += P.scratch_off;
     P.d_rects.upload(rects, st, stg);
@@ -676,14 +687,14 @@ class Amr3Gpu : public AmrSolver {
         a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
         a.chunks = P.d_chunks.d + P.own_ch_lo[ow]; a.nchunks = P.own_ch_hi[ow] - P.own_ch_lo[ow]; a.nvar = nvar; a.modes = modes;
         a.lc = lc; a.xlower = xlower; a.ylower = ylower; a.zlower = zlower;
-        launch_fill3(a, st);
+        launch_fill3(a, st, f32);
         ++nkernels;
       }
       if (P.own_bc_hi[ow] > P.own_bc_lo[ow]) {
         Bc3Args b{};
         b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.own_bc_lo[ow];
         b.nops = P.own_bc_hi[ow] - P.own_bc_lo[ow]; b.nvar = nvar;
-        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st);
+        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st, f32);
         nkernels += 3;
       }
     }
@@ -691,21 +702,21 @@ class Amr3Gpu : public AmrSolver {
 
   void run_prog(Prog3& P, const SrcMode& modes) {
     if (P.zero_scratch && P.scratch_len > 0 && P.nstages > 0)
-      AMR_CUDA(cudaMemsetAsync(pool.d + P.scratch_off, 0, sizeof(double) * P.scratch_len, st));
+      AMR_CUDA(cudaMemsetAsync(pool_bytes() + elem() * P.scratch_off, 0, elem() * P.scratch_len, st));
     for (int s = 0; s < P.nstages; ++s) {
       if (P.ch_hi[s] > P.ch_lo[s]) {
         Fill3Args a{};
         a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
         a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
         a.lc = lc; a.xlower = xlower; a.ylower = ylower; a.zlower = zlower;
-        launch_fill3(a, st);
+        launch_fill3(a, st, f32);
         ++nkernels;
       }
       if (P.bc_hi[s] > P.bc_lo[s]) {
         Bc3Args b{};
         b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.bc_lo[s];
         b.nops = P.bc_hi[s] - P.bc_lo[s]; b.nvar = nvar;
-        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st);
+        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st, f32);
         nkernels += 3;
       }
     }
@@ -1033,7 +1044,7 @@ class Amr3Gpu : public AmrSolver {
       bound_level(lev, t);
       if (kids) { SrcMode M{}; run_prog(L.saveqc, M); }
       if (lev > 1 && L.nseg > 0) {
-        launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.nseg, sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st);
+        launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.nseg, sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st, f32);
         ++nkernels;
       }
       sample_gauges(lev);
@@ -1041,15 +1052,15 @@ class Amr3Gpu : public AmrSolver {
       if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
       a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
-      launch_step3(a, L.items, L.faces, L.cells, st);
+      launch_step3(a, L.items, L.faces, L.cells, st, f32);
       nkernels += 5;
       if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
       if (!L.fsv.empty()) {
-        launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
+        launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st, f32);
         ++nkernels;
       }
       if (lev > 1 && L.nseg > 0) {
-        launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.nseg, nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st);
+        launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.nseg, nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st, f32);
         ++nkernels;
       }
     } else {
@@ -1068,7 +1079,7 @@ class Amr3Gpu : public AmrSolver {
       for (int k = 0; k < np; ++k) {
         const long long q0 = L.seg0[k], nq = L.seg0[k + 1] - L.seg0[k];
         if (lev > 1 && nq > 0) {
-          launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d + q0, (int)nq, sp, nvar, hx, hy, hz, dt, st);
+          launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d + q0, (int)nq, sp, nvar, hx, hy, hz, dt, st, f32);
           ++nkernels;
         }
         Step3Args b = a;
@@ -1077,15 +1088,15 @@ class Amr3Gpu : public AmrSolver {
         b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
         long long it[3];
         for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
-        launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st);
+        launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
         nkernels += 5;
         const long long f0 = L.fsv0[k], nf = L.fsv0[k + 1] - L.fsv0[k];
         if (nf > 0) {
-          launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d + f0, (int)nf, nvar, dt, hx, hy, hz, st);
+          launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d + f0, (int)nf, nvar, dt, hx, hy, hz, st, f32);
           ++nkernels;
         }
         if (lev > 1 && nq > 0) {
-          launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d + q0, (int)nq, nvar, dt, hx, hy, hz, st);
+          launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d + q0, (int)nq, nvar, dt, hx, hy, hz, st, f32);
           ++nkernels;
         }
       }
@@ -1145,8 +1156,8 @@ class Amr3Gpu : public AmrSolver {
     ensure(lev, NEED_UPDATE);
     Plan3& L = plan[lev];
     const double vol = hxposs[lev] * hyposs[lev] * hzposs[lev];
-    launch_upbnd3(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, vol, nvar, st);
-    launch_average3(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), L.avg_max, intratx[lev], intraty[lev], intratz[lev], nvar, st);
+    launch_upbnd3(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, vol, nvar, st, f32);
+    launch_average3(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), L.avg_max, intratx[lev], intraty[lev], intratz[lev], nvar, st, f32);
     nkernels += 2;
   }
 
@@ -1191,7 +1202,7 @@ class Amr3Gpu : public AmrSolver {
       d_gauge_out.free(); d_gauge_out = nb;
     }
     DBuf<Gauge3Job> dj; dj.upload(jobs, st, stg);
-    launch_gauges3(pool.d, d_patches.d, dj.d, (int)jobs.size(), nvar, d_gauge_out.d, st);
+    launch_gauges3(pool.d, d_patches.d, dj.d, (int)jobs.size(), nvar, d_gauge_out.d, st, f32);
     sync_stream();
     dj.free();
   }
@@ -1235,7 +1246,7 @@ class Amr3Gpu : public AmrSolver {
       lv_c0.upload(c0, st, stg);
       lv_plist.upload(G, st, stg);
       launch_flag_cells3(pool.d, d_patches.d, lv_plist.d, lv_c0.d, (int)G.size(), c0.back(), flag_pressure, sp.gamma1, p.tolsp, nvar,
-                         lv_b.d, dl, st);
+                         lv_b.d, dl, st, f32);
     }
     std::vector<LvlBox> proj;
     if (lcheck + 2 <= p.mxnest) {
@@ -1478,7 +1489,7 @@ class Amr3Gpu : public AmrSolver {
     upload_prog(P);
     run_prog(P, SrcMode{});
     sync_stream();
-    pool.release(P.scratch_off, P.scratch_alloc);
+    pfree(P.scratch_off, P.scratch_alloc);
     P.scratch_off = -1;
   }
 
@@ -1542,9 +1553,15 @@ class Amr3Gpu : public AmrSolver {
       g.time = t;
       std::vector<double> q;
       qinit(g, hxposs[g.level], hyposs[g.level], hzposs[g.level], q);
-      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q0, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
-      AMR_CUDA(cudaMemcpyAsync(pool.d + g.q1, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
-      h2d_bytes += 2.0 * sizeof(double) * q.size();
+      std::vector<float> qf;
+      const void* src = q.data();
+      if (f32) {  // the FP32 form stores the initial values rounded to float
+        qf.assign(q.begin(), q.end());
+        src = qf.data();
+      }
+      AMR_CUDA(cudaMemcpyAsync(pool_bytes() + elem() * g.q0, src, elem() * q.size(), cudaMemcpyHostToDevice, st));
+      AMR_CUDA(cudaMemcpyAsync(pool_bytes() + elem() * g.q1, src, elem() * q.size(), cudaMemcpyHostToDevice, st));
+      h2d_bytes += 2.0 * elem() * q.size();
       sync_stream();
     }
   }
@@ -1749,7 +1766,7 @@ class Amr3Gpu : public AmrSolver {
   double mass() {
     AMR_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double), st));
     DBuf<int> dp; dp.upload(lgrids[1], st, stg);
-    launch_mass3(pool.d, d_patches.d, dp.d, (int)lgrids[1].size(), d_mass, st);
+    launch_mass3(pool.d, d_patches.d, dp.d, (int)lgrids[1].size(), d_mass, st, f32);
     double m = 0;
     AMR_CUDA(cudaMemcpyAsync(&m, d_mass, sizeof(double), cudaMemcpyDeviceToHost, st));
     sync_stream();
@@ -1766,7 +1783,7 @@ class Amr3Gpu : public AmrSolver {
     DBuf<int> dp; dp.upload(pl, st, stg);
     DBuf<long long> dc; dc.upload(c0, st, stg);
     DBuf<double> dout; dout.ensure(out.size());
-    launch_gather3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nvar, c0.back(), dout.d, st);
+    launch_gather3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nvar, c0.back(), dout.d, st, f32);
     AMR_CUDA(cudaMemcpyAsync(out.data(), dout.d, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
     sync_stream();
     dp.free(); dc.free(); dout.free();
@@ -1853,7 +1870,7 @@ class Amr3Gpu : public AmrSolver {
   std::vector<double> info() override {
     return {time, rvol, (double)ncycle, (double)lfine, t_step, t_regrid, tmass0, cflmax_run, (double)nkernels, (double)pool.peak * 8.0,
             (double)nsteps_launched, step_kernel_ms, step_kernel_cells, last_run_ms, run_cells, finished() ? 1.0 : 0.0, h2d_bytes,
-            0, 0, 0, 0, 0, 0, 3.0, 64.0};
+            0, 0, 0, 0, 0, 0, 3.0, f32 ? 32.0 : 64.0};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;
@@ -1938,8 +1955,9 @@ L18:
   goto L18;
 }
 
-AmrSolver* make_solver3(const std::string& rundir, const std::string& outdir, bool write_output) {
+AmrSolver* make_solver3(const std::string& rundir, const std::string& outdir, bool write_output, bool f32) {
   std::unique_ptr<Amr3Gpu> s(new Amr3Gpu());
+  s->f32 = f32;
   s->outdir = outdir;
   s->write_output = write_output;
   s->init(rundir);

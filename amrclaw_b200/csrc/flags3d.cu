@@ -159,7 +159,8 @@ __device__ __forceinline__ int patch_of(const long long* pre, int np, long long 
 
 // flag2refine.f pattern of the 3D Euler example: undivided pressure difference (or of every
 // component) against tolsp; BADPT (2) / GOODPT (0) into the zeroed level array (setflags.f)
-__global__ void flag_cells_kernel(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
+template <class T>
+__global__ void flag_cells_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
                                   long long ncells, int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* f, LvlDims d) {
   GRID_STRIDE(t, ncells) {
     const int pi = patch_of(cell0, np, t);
@@ -168,7 +169,7 @@ __global__ void flag_cells_kernel(const double* pool, const PatchDev* patches, c
     const long long loc = t - cell0[pi];
     const int i = (int)(loc % mx) + 1, j = (int)((loc / mx) % my) + 1, k = (int)(loc / ((long long)mx * my)) + 1;
     const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
-    const double* q = pool + P.q[P.cur];
+    const T* q = pool + P.q[P.cur];
     auto Q = [&](int m, int ii, int jj, int kk) {
       return q[(m - 1) * plane + ((long long)(kk - 1 + NGF) * P.mjtot + (jj - 1 + NGF)) * P.mitot + (ii - 1 + NGF)];
     };
@@ -279,12 +280,16 @@ void launch_zero_interior(int8_t* f, LvlDims d, cudaStream_t s) {
   AMR_CUDA(cudaGetLastError());
 }
 
-void launch_flag_cells3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
+void launch_flag_cells3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
                         long long ncells, int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* f, LvlDims d,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool f32) {
   if (ncells <= 0) return;
-  flag_cells_kernel<<<blocks_for(ncells, 256), 256, 0, s>>>(pool, patches, plist, cell0, np, ncells, flag_pressure, gamma1, tolsp,
-                                                            nvar, f, d);
+  if (f32)
+    flag_cells_kernel<<<blocks_for(ncells, 256), 256, 0, s>>>(static_cast<const float*>(pool), patches, plist, cell0, np, ncells,
+                                                              flag_pressure, gamma1, tolsp, nvar, f, d);
+  else
+    flag_cells_kernel<<<blocks_for(ncells, 256), 256, 0, s>>>(static_cast<const double*>(pool), patches, plist, cell0, np, ncells,
+                                                              flag_pressure, gamma1, tolsp, nvar, f, d);
   AMR_CUDA(cudaGetLastError());
 }
 

@@ -26,9 +26,10 @@ void launch_domup(const int8_t* crse, LvlDims cd, int8_t* fine, LvlDims fd, int 
 void launch_zero_interior(int8_t* f, LvlDims d, cudaStream_t s);
 // spest.f + flag2refine.f + setflags.f: BADPT (2) or GOODPT (0) into the level array for
 // every interior cell of the patches in plist (patch cells at [cell0[p], cell0[p+1])).
-void launch_flag_cells3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
+// f32: the pool holds floats (the FP32 form); the differences are taken in FP64.
+void launch_flag_cells3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
                         long long ncells, int flag_pressure, double gamma1, double tolsp, int nvar, int8_t* f, LvlDims d,
-                        cudaStream_t s);
+                        cudaStream_t s, bool f32);
 // bufnst.f + projec.f + shiftset.f: project the boxes (3 where 0), zero the ring, then
 // add the ibuff-dilated flags (t1, t2: scratch arrays of the same dims).
 void launch_bufnst3(int8_t* f, LvlDims d, const LvlBox* proj, int nproj, int ibuff, int8_t* t1, int8_t* t2, cudaStream_t s);

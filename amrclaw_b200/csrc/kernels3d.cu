@@ -43,15 +43,16 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double 
   atomicMax(p, (unsigned long long)__double_as_longlong(v));
 }
 
-__device__ __forceinline__ double philim3(int meth, double r) {
+template <class T>
+__device__ __forceinline__ T philim3(int meth, T r) {
   switch (meth) {
-    case 1: return dmax(0.0, dmin(1.0, r));
-    case 2: return dmax(dmax(0.0, dmin(1.0, 2.0 * r)), dmin(2.0, r));
-    case 3: return (r + fabs(r)) / (1.0 + fabs(r));
-    case 4: { const double c = (1.0 + r) / 2.0; return dmax(0.0, dmin(dmin(c, 2.0), 2.0 * r)); }
+    case 1: return dmax(T(0), dmin(T(1), r));
+    case 2: return dmax(dmax(T(0), dmin(T(1), T(2) * r)), dmin(T(2), r));
+    case 3: return (r + fabs(r)) / (T(1) + fabs(r));
+    case 4: { const T c = (T(1) + r) / T(2); return dmax(T(0), dmin(dmin(c, T(2)), T(2) * r)); }
     case 5: return r;
   }
-  return 0.0;
+  return T(0);
 }
 
 // ------------------------------------------------------------------- sweeps
@@ -72,14 +73,15 @@ constexpr int SW_OWN = SW_T - 3;
 #endif
 
 // (a - 3*b) (m4 = 2) or a: the doubly transverse inputs of flux3.f:429-507
-__device__ __forceinline__ void dt_input(int m4, double sgn3, const double* a, const double* b, double* o) {
+template <class T>
+__device__ __forceinline__ void dt_input(int m4, T sgn3, const T* a, const T* b, T* o) {
 #pragma unroll
   for (int m = 0; m < 5; ++m) o[m] = (m4 == 2) ? a[m] + sgn3 * b[m] : a[m];
 }
 
-template <int DIR>
+template <int DIR, class T>
 __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
-  __shared__ double sW[15][SW_T];
+  __shared__ T sW[15][SW_T];
   const long long* c0 = A.comp0 + (long long)(DIR - 1) * (A.np + 1);
   const long long* s0 = A.sweep0 + (long long)(DIR - 1) * (A.np + 1);
   const long long first = c0[0], last = c0[A.np];
@@ -88,14 +90,14 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   const bool valid = g >= first && g < last;
   const Step3Params sp = A.sp;
   const double dn = DIR == 1 ? A.dx : DIR == 2 ? A.dy : A.dz;
-  const double dtdx = A.dt / dn;
+  const T dtdx = (T)(A.dt / dn);
   // transverse steps of flux3's dtdy / dtdz arguments for this sweep (step3.f:192, 300, 416)
-  const double dtdy = DIR == 1 ? A.dt / A.dy : DIR == 2 ? A.dt / A.dz : A.dt / A.dx;
-  const double dtdz = DIR == 1 ? A.dt / A.dz : DIR == 2 ? A.dt / A.dx : A.dt / A.dy;
+  const T dtdy = (T)(DIR == 1 ? A.dt / A.dy : DIR == 2 ? A.dt / A.dz : A.dt / A.dx);
+  const T dtdz = (T)(DIR == 1 ? A.dt / A.dz : DIR == 2 ? A.dt / A.dx : A.dt / A.dy);
   int e = -1, n1 = 0;
   long long slot = 0;  // stash slot of pencil cell e (meaningful for e in 1..n1+1)
-  Roe3D R;
-  double W[3][5], S[3], AM[5], AP[5];
+  Roe3T<T> R;
+  T W[3][5], S[3], AM[5], AP[5];
   if (valid) {
     const int pi = find_patch(c0, A.np, g);
     const PatchDev& P = A.patches[A.plist[pi]];
@@ -113,14 +115,14 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
     else if (DIR == 2) { base = ((long long)(b - 1 + NG3) * mj + (NG3 - 1)) * mi + (a - 1 + NG3); step = mi; }
     else { base = ((long long)(NG3 - 1) * mj + (b - 1 + NG3)) * mi + (a - 1 + NG3); step = mi * mj; }
     const long long plane = mi * mj * P.mktot;
-    const double* q = A.pool + P.q[P.cur];
-    double QL[6], QR[6];
+    const T* q = static_cast<const T*>(A.pool) + P.q[P.cur];
+    T QL[6], QR[6];
     const long long atl = base + (long long)(e - 1) * step, atr = atl + step;
 #pragma unroll
     for (int m = 1; m <= 5; ++m) { QL[m] = q[(m - 1) * plane + atl]; QR[m] = q[(m - 1) * plane + atr]; }
-    QL[0] = QR[0] = 0.0;
-    R = roe3d(sp.gamma1, QL, QR);
-    euler3d_rpn_roe(sp.gamma, sp.gamma1, sp.efix != 0, DIR, QL, QR, R, W, S, AM, AP);
+    QL[0] = QR[0] = T(0);
+    R = roe3d((T)sp.gamma1, QL, QR);
+    euler3d_rpn_roe((T)sp.gamma, (T)sp.gamma1, sp.efix != 0, DIR, QL, QR, R, W, S, AM, AP);
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -130,13 +132,13 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   // interfaces 1..n1+1 carry fluxes; the tile edges only serve their neighbours
   const bool live = valid && e >= 1 && e <= n1 + 1 && l >= 1 && l <= SW_T - 2;
   const bool owned = live && l <= SW_T - 3;
-  double cfl = 0.0;
-  double CQ[5];
+  T cfl = T(0);
+  T CQ[5];
 #pragma unroll
-  for (int m = 0; m < 5; ++m) CQ[m] = 0.0;
-  double* st = A.stash + slot;
+  for (int m = 0; m < 5; ++m) CQ[m] = T(0);
+  T* st = static_cast<T*>(A.stash) + slot;
   const long long ss = A.stash_stride;
-  const double c6 = 1.0 / 6.0;
+  const T c6 = (T)(1.0 / 6.0);
   const int m3 = sp.m3, m4 = sp.m4;
   if (live) {
     // Courant number of interface e (flux3.f:237-246)
@@ -144,67 +146,67 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
     for (int k = 0; k < 3; ++k) cfl = dmax(cfl, dmax(dtdx * S[k], -dtdx * S[k]));
     if (sp.order != 1) {
       // limiter.f: r from the unlimited neighbour waves, upwind side by the speed's sign
-      const double dtdxave = 0.5 * (dtdx + dtdx);
+      const T dtdxave = T(0.5) * (dtdx + dtdx);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         if (sp.mthlim[k] == 0) continue;
-        double dl = 0.0, dr = 0.0, wn = 0.0;
+        T dl = T(0), dr = T(0), wn = T(0);
 #pragma unroll
         for (int m = 0; m < 5; ++m) dl = dl + sW[k * 5 + m][l - 1] * W[k][m];
 #pragma unroll
         for (int m = 0; m < 5; ++m) dr = dr + W[k][m] * sW[k * 5 + m][l + 1];
 #pragma unroll
         for (int m = 0; m < 5; ++m) wn = wn + W[k][m] * W[k][m];
-        if (wn != 0.0) {
-          const double r = (S[k] > 0.0) ? dl / wn : dr / wn;
-          const double phi = philim3(sp.mthlim[k], r);
+        if (wn != T(0)) {
+          const T r = (S[k] > T(0)) ? dl / wn : dr / wn;
+          const T phi = philim3(sp.mthlim[k], r);
 #pragma unroll
           for (int m = 0; m < 5; ++m) W[k][m] = phi * W[k][m];
         }
       }
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        double x = 0.0;
+        T x = T(0);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) x = x + 0.5 * fabs(S[k]) * (1.0 - fabs(S[k]) * dtdxave) * W[k][m];
+        for (int k = 0; k < 3; ++k) x = x + T(0.5) * fabs(S[k]) * (T(1) - fabs(S[k]) * dtdxave) * W[k][m];
         CQ[m] = x;
       }
     }
     if (owned) {
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        double fm = 0.0 + AM[m], fp = 0.0 - AP[m];
+        T fm = T(0) + AM[m], fp = T(0) - AP[m];
         if (sp.order != 1) { fm = fm + CQ[m]; fp = fp + CQ[m]; }
         st[(long long)m * ss] = fm;
         st[(long long)(5 + m) * ss] = fp;
       }
       if (e <= n1) {
         if (m3 <= 0) {
-          for (int x = 10; x < STASH3; ++x) st[(long long)x * ss] = 0.0;
+          for (int x = 10; x < STASH3; ++x) st[(long long)x * ss] = T(0);
         } else {
           // apdq side of interface e: the terms of cell e (flux3.f:429-505, 552-628 with i = e)
-          double bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
+          T bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
           euler3d_trans(R, DIR, 2, AP, bm, bp);
           euler3d_trans(R, DIR, 3, AP, cm, cp);
           if (m3 == 2) { euler3d_trans(R, DIR, 2, CQ, bmq, bpq); euler3d_trans(R, DIR, 3, CQ, cmq, cpq); }
           else {
 #pragma unroll
-            for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = 0.0;
+            for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
           }
           // gadd: (side, offset d) at element 10 + ((side-1)*3 + d+1)*5 + m
           {
-            double P1[5], P2[5], M1[5], M2[5];
+            T P1[5], P2[5], M1[5], M2[5];
             if (m4 > 0) {
-              double t[5];
-              dt_input(m4, -3.0, cp, cpq, t);
+              T t[5];
+              dt_input(m4, T(-3), cp, cpq, t);
               euler3d_trans(R, DIR, 2, t, P1, P2);
-              dt_input(m4, -3.0, cm, cmq, t);
+              dt_input(m4, T(-3), cm, cmq, t);
               euler3d_trans(R, DIR, 2, t, M1, M2);
             }
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
-              double g01 = 0.0 - 0.5 * dtdx * bm[m], g11 = 0.0 - 0.5 * dtdx * bp[m];
-              double g00 = 0.0, g02 = 0.0, g10 = 0.0, g12 = 0.0;
+              T g01 = T(0) - T(0.5) * dtdx * bm[m], g11 = T(0) - T(0.5) * dtdx * bp[m];
+              T g00 = T(0), g02 = T(0), g10 = T(0), g12 = T(0);
               if (m4 > 0) {
                 g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
                 g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
@@ -224,18 +226,18 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
           }
           // hadd at element 40 + ((side-1)*3 + d+1)*5 + m
           {
-            double X1[5], X2[5], Y1[5], Y2[5];
+            T X1[5], X2[5], Y1[5], Y2[5];
             if (m4 > 0) {
-              double t[5];
-              dt_input(m4, -3.0, bp, bpq, t);
+              T t[5];
+              dt_input(m4, T(-3), bp, bpq, t);
               euler3d_trans(R, DIR, 3, t, X1, X2);
-              dt_input(m4, -3.0, bm, bmq, t);
+              dt_input(m4, T(-3), bm, bmq, t);
               euler3d_trans(R, DIR, 3, t, Y1, Y2);
             }
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
-              double h01 = 0.0 - 0.5 * dtdx * cm[m], h11 = 0.0 - 0.5 * dtdx * cp[m];
-              double h00 = 0.0, h02 = 0.0, h10 = 0.0, h12 = 0.0;
+              T h01 = T(0) - T(0.5) * dtdx * cm[m], h11 = T(0) - T(0.5) * dtdx * cp[m];
+              T h00 = T(0), h02 = T(0), h10 = T(0), h12 = T(0);
               if (m4 > 0) {
                 h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
                 h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
@@ -260,32 +262,32 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   __syncthreads();
   // amdq side of interface e: the terms of cell e-1, owned by thread l-1 of this tile
   if (live && m3 > 0 && e >= 2 && l >= 2) {
-    double* sc = st - 1;
-    double bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
+    T* sc = st - 1;
+    T bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
     euler3d_trans(R, DIR, 2, AM, bm, bp);
     euler3d_trans(R, DIR, 3, AM, cm, cp);
     if (m3 == 2) { euler3d_trans(R, DIR, 2, CQ, bmq, bpq); euler3d_trans(R, DIR, 3, CQ, cmq, cpq); }
     else {
 #pragma unroll
-      for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = 0.0;
+      for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
     }
     {
-      double P1[5], P2[5], M1[5], M2[5];
+      T P1[5], P2[5], M1[5], M2[5];
       if (m4 > 0) {
-        double t[5];
-        dt_input(m4, 3.0, cp, cpq, t);
+        T t[5];
+        dt_input(m4, T(3), cp, cpq, t);
         euler3d_trans(R, DIR, 2, t, P1, P2);
-        dt_input(m4, 3.0, cm, cmq, t);
+        dt_input(m4, T(3), cm, cmq, t);
         euler3d_trans(R, DIR, 2, t, M1, M2);
       }
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        double g01 = sc[(long long)(10 + 1 * 5 + m) * ss], g11 = sc[(long long)(10 + 4 * 5 + m) * ss];
-        g01 = g01 - 0.5 * dtdx * bm[m];
-        g11 = g11 - 0.5 * dtdx * bp[m];
+        T g01 = sc[(long long)(10 + 1 * 5 + m) * ss], g11 = sc[(long long)(10 + 4 * 5 + m) * ss];
+        g01 = g01 - T(0.5) * dtdx * bm[m];
+        g11 = g11 - T(0.5) * dtdx * bp[m];
         if (m4 > 0) {
-          double g00 = sc[(long long)(10 + 0 * 5 + m) * ss], g02 = sc[(long long)(10 + 2 * 5 + m) * ss];
-          double g10 = sc[(long long)(10 + 3 * 5 + m) * ss], g12 = sc[(long long)(10 + 5 * 5 + m) * ss];
+          T g00 = sc[(long long)(10 + 0 * 5 + m) * ss], g02 = sc[(long long)(10 + 2 * 5 + m) * ss];
+          T g10 = sc[(long long)(10 + 3 * 5 + m) * ss], g12 = sc[(long long)(10 + 5 * 5 + m) * ss];
           g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
           g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
           g12 = g12 - c6 * dtdx * dtdz * P2[m];
@@ -303,22 +305,22 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
       }
     }
     {
-      double X1[5], X2[5], Y1[5], Y2[5];
+      T X1[5], X2[5], Y1[5], Y2[5];
       if (m4 > 0) {
-        double t[5];
-        dt_input(m4, 3.0, bp, bpq, t);
+        T t[5];
+        dt_input(m4, T(3), bp, bpq, t);
         euler3d_trans(R, DIR, 3, t, X1, X2);
-        dt_input(m4, 3.0, bm, bmq, t);
+        dt_input(m4, T(3), bm, bmq, t);
         euler3d_trans(R, DIR, 3, t, Y1, Y2);
       }
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        double h01 = sc[(long long)(40 + 1 * 5 + m) * ss], h11 = sc[(long long)(40 + 4 * 5 + m) * ss];
-        h01 = h01 - 0.5 * dtdx * cm[m];
-        h11 = h11 - 0.5 * dtdx * cp[m];
+        T h01 = sc[(long long)(40 + 1 * 5 + m) * ss], h11 = sc[(long long)(40 + 4 * 5 + m) * ss];
+        h01 = h01 - T(0.5) * dtdx * cm[m];
+        h11 = h11 - T(0.5) * dtdx * cp[m];
         if (m4 > 0) {
-          double h00 = sc[(long long)(40 + 0 * 5 + m) * ss], h02 = sc[(long long)(40 + 2 * 5 + m) * ss];
-          double h10 = sc[(long long)(40 + 3 * 5 + m) * ss], h12 = sc[(long long)(40 + 5 * 5 + m) * ss];
+          T h00 = sc[(long long)(40 + 0 * 5 + m) * ss], h02 = sc[(long long)(40 + 2 * 5 + m) * ss];
+          T h10 = sc[(long long)(40 + 3 * 5 + m) * ss], h12 = sc[(long long)(40 + 5 * 5 + m) * ss];
           h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
           h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
           h12 = h12 - c6 * dtdx * dtdy * X2[m];
@@ -338,18 +340,19 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   }
   // block-wide max of the Courant number, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
-  if ((threadIdx.x & 31) == 0 && cfl > 0.0) atomic_max_nonneg(A.cflmax, cfl);
+  if ((threadIdx.x & 31) == 0 && cfl > T(0)) atomic_max_nonneg(A.cflmax, (double)cfl);
 }
 
 // stash element of gadd (kind 10) / hadd (kind 40) for side s (1,2), offset d (-1..1), component m (0..4)
 __device__ __forceinline__ int sidx(int kind, int s, int d, int m) { return kind + ((s - 1) * 3 + (d + 1)) * 5 + m; }
 
 // ------------------------------------------------------------------- faces
+template <class T>
 __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
   // face cells [face0[0], face0[np]): the level's, or one patch's through a one-patch view
   const long long first = A.face0[0], total = A.face0[A.np];
   const long long ss = A.stash_stride;
-  const double* S = A.stash;
+  const T* S = static_cast<const T*>(A.stash);
   for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int pi = find_patch(A.face0, A.np, t);
     const PatchDev& P = A.patches[A.plist[pi]];
@@ -362,22 +365,22 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
     auto xs = [&](int jj, int kk, int ii) { return bx + ((long long)(kk * (my + 2) + jj) * (mx + 1) + (ii - 1)); };
     auto ys = [&](int ii, int kk, int jj) { return by + ((long long)(kk * (mx + 2) + ii) * (my + 1) + (jj - 1)); };
     auto zs = [&](int ii, int jj, int kk) { return bz + ((long long)(jj * (mx + 2) + ii) * (mz + 1) + (kk - 1)); };
-    double* F = A.flux + t;
+    T* F = static_cast<T*>(A.flux) + t;
     const long long fs = A.flux_stride;
     if (j <= my && k <= mz) {  // x-face i
-      double fm[5], fp[5];
+      T fm[5], fp[5];
       const long long sx = xs(j, k, i);
 #pragma unroll
-      for (int m = 0; m < 5; ++m) { fm[m] = 0.0 + S[m * ss + sx]; fp[m] = 0.0 + S[(5 + m) * ss + sx]; }
+      for (int m = 0; m < 5; ++m) { fm[m] = T(0) + S[m * ss + sx]; fp[m] = T(0) + S[(5 + m) * ss + sx]; }
       // y-sweeps: k' = k-1, k, k+1 (d = +1, 0, -1); pencil i-1 (side 2) then i (side 1)
 #pragma unroll
       for (int d = 1; d >= -1; --d) {
         const long long s2 = ys(i - 1, k - d, j), s1 = ys(i, k - d, j);
 #pragma unroll
         for (int m = 0; m < 5; ++m) {
-          const double t2 = S[sidx(40, 2, d, m) * ss + s2];
+          const T t2 = S[sidx(40, 2, d, m) * ss + s2];
           fm[m] = fm[m] + t2; fp[m] = fp[m] + t2;
-          const double t1 = S[sidx(40, 1, d, m) * ss + s1];
+          const T t1 = S[sidx(40, 1, d, m) * ss + s1];
           fm[m] = fm[m] + t1; fp[m] = fp[m] + t1;
         }
       }
@@ -387,9 +390,9 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
         const long long s2 = zs(i - 1, j - d, k), s1 = zs(i, j - d, k);
 #pragma unroll
         for (int m = 0; m < 5; ++m) {
-          const double t2 = S[sidx(10, 2, d, m) * ss + s2];
+          const T t2 = S[sidx(10, 2, d, m) * ss + s2];
           fm[m] = fm[m] + t2; fp[m] = fp[m] + t2;
-          const double t1 = S[sidx(10, 1, d, m) * ss + s1];
+          const T t1 = S[sidx(10, 1, d, m) * ss + s1];
           fm[m] = fm[m] + t1; fp[m] = fp[m] + t1;
         }
       }
@@ -397,9 +400,9 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
       for (int m = 0; m < 5; ++m) { F[(0 * 5 + m) * fs] = fm[m]; F[(1 * 5 + m) * fs] = fp[m]; }
     }
     if (i <= mx && k <= mz) {  // y-face j
-      double gm[5], gp[5];
+      T gm[5], gp[5];
 #pragma unroll
-      for (int m = 0; m < 5; ++m) gm[m] = 0.0;
+      for (int m = 0; m < 5; ++m) gm[m] = T(0);
       // x-sweeps: k' = k-1, k, k+1 (d = +1, 0, -1); pencil j-1 (side 2) then j (side 1)
 #pragma unroll
       for (int d = 1; d >= -1; --d) {
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
           const long long sz = zs(i - d, jp, k);
 #pragma unroll
           for (int m = 0; m < 5; ++m) {
-            const double tv = S[sidx(40, side, d, m) * ss + sz];
+            const T tv = S[sidx(40, side, d, m) * ss + sz];
             gm[m] = gm[m] + tv; gp[m] = gp[m] + tv;
           }
         }
@@ -431,9 +434,9 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
       for (int m = 0; m < 5; ++m) { F[(2 * 5 + m) * fs] = gm[m]; F[(3 * 5 + m) * fs] = gp[m]; }
     }
     if (i <= mx && j <= my) {  // z-face k
-      double hm[5], hp[5];
+      T hm[5], hp[5];
 #pragma unroll
-      for (int m = 0; m < 5; ++m) hm[m] = 0.0;
+      for (int m = 0; m < 5; ++m) hm[m] = T(0);
       // x-sweeps: k' = k-1 (side 2) for j' = j-1, j, j+1 (d = +1, 0, -1), then k' = k (side 1)
 #pragma unroll
       for (int side = 2; side >= 1; --side) {
@@ -466,10 +469,11 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
 }
 
 // ------------------------------------------------------------------- update
+template <class T>
 __global__ void __launch_bounds__(256) update3_kernel(Step3Args A) {
   const long long first = A.cell0[0], total = A.cell0[A.np];
   const long long fs = A.flux_stride;
-  const double dtdx = A.dt / A.dx, dtdy = A.dt / A.dy, dtdz = A.dt / A.dz;
+  const T dtdx = (T)(A.dt / A.dx), dtdy = (T)(A.dt / A.dy), dtdz = (T)(A.dt / A.dz);
   for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int pi = find_patch(A.cell0, A.np, t);
     const PatchDev& P = A.patches[A.plist[pi]];
@@ -480,22 +484,23 @@ __global__ void __launch_bounds__(256) update3_kernel(Step3Args A) {
     auto fidx = [&](int ii, int jj, int kk) { return f0 + ((long long)(kk - 1) * (my + 1) + (jj - 1)) * (mx + 1) + (ii - 1); };
     const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
     const long long at = ((long long)(k - 1 + NG3) * P.mjtot + (j - 1 + NG3)) * P.mitot + (i - 1 + NG3);
-    const double* q = A.pool + P.q[P.cur];
-    double* qn = const_cast<double*>(A.pool) + P.q[1 - P.cur];
+    const T* q = static_cast<const T*>(A.pool) + P.q[P.cur];
+    T* qn = const_cast<T*>(static_cast<const T*>(A.pool)) + P.q[1 - P.cur];
     const long long c = fidx(i, j, k), cx = fidx(i + 1, j, k), cy = fidx(i, j + 1, k), cz = fidx(i, j, k + 1);
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
-      const double* F = A.flux + (long long)m * fs;
-      const double fmv = F[0 * 5 * fs + cx], fpv = F[1 * 5 * fs + c];
-      const double gmv = F[2 * 5 * fs + cy], gpv = F[3 * 5 * fs + c];
-      const double hmv = F[4 * 5 * fs + cz], hpv = F[5 * 5 * fs + c];
+      const T* F = static_cast<const T*>(A.flux) + (long long)m * fs;
+      const T fmv = F[0 * 5 * fs + cx], fpv = F[1 * 5 * fs + c];
+      const T gmv = F[2 * 5 * fs + cy], gpv = F[3 * 5 * fs + c];
+      const T hmv = F[4 * 5 * fs + cz], hpv = F[5 * 5 * fs + c];
       qn[m * plane + at] = q[m * plane + at] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv) - dtdz * (hmv - hpv);
     }
   }
 }
 
 // fluxsv.f:4-94: one register entry per thread
-__global__ void fsv3_kernel(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
+template <class T>
+__global__ void fsv3_kernel(const T* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
                             const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -512,11 +517,12 @@ __global__ void fsv3_kernel(const double* flux, long long fs, const long long* f
     case 5: comp = 5; c = fidx(E.i, E.j, E.k); h1 = hx; h2 = hy; break;
     default: comp = 4; c = fidx(E.i, E.j, E.k + 1); h1 = hx; h2 = hy; break;
   }
-  for (int m = 0; m < nvar; ++m) regs[E.dst + m] = -flux[((long long)comp * 5 + m) * fs + c] * dtc * h1 * h2;
+  for (int m = 0; m < nvar; ++m) regs[E.dst + m] = -(double)flux[((long long)comp * 5 + m) * fs + c] * dtc * h1 * h2;
 }
 
 // fluxad.f:4-155: one coarse face (register) of a fine patch per thread
-__global__ void fad3_kernel(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
+template <class T>
+__global__ void fad3_kernel(const T* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
                             const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -536,7 +542,7 @@ __global__ void fad3_kernel(const double* flux, long long fs, const long long* f
   }
   for (int m = 0; m < nvar; ++m) {
     double acc = sv[m];
-    const double* F = flux + ((long long)comp * 5 + m) * fs;
+    const T* F = flux + ((long long)comp * 5 + m) * fs;
     for (int ob = 1; ob <= E.nb; ++ob)
       for (int oa = 1; oa <= E.na; ++oa) {
         long long c;
@@ -548,14 +554,15 @@ __global__ void fad3_kernel(const double* flux, long long fs, const long long* f
           case 5: c = fidx(E.a0 + oa, E.b0 + ob, 1); break;
           default: c = fidx(E.a0 + oa, E.b0 + ob, mz + 1); break;
         }
-        acc = acc + F[c] * dtf * h1 * h2;
+        acc = acc + (double)F[c] * dtf * h1 * h2;
       }
     sv[m] = acc;
   }
 }
 
 // qad.f:4-534: one register of one side of a fine patch per thread
-__global__ void qad3_kernel(double* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
+template <class T>
+__global__ void qad3_kernel(T* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
                             int nvar, double hx, double hy, double hz, double delt) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= njobs) return;
@@ -563,13 +570,13 @@ __global__ void qad3_kernel(double* pool, double* regs, const PatchDev* patches,
   const PatchDev& P = patches[J.patch];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
   const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
-  const double* q = pool + P.q[P.cur];
+  const T* q = pool + P.q[P.cur];
   auto at = [&](int i, int j, int k) { return ((long long)(k - 1 + NG3) * P.mjtot + (j - 1 + NG3)) * P.mitot + (i - 1 + NG3); };
   double* sv = regs + P.ffl + (long long)nvar * J.reg0;
   const double* qc = regs + P.ffl + (long long)nvar * P.lenbc + (long long)nvar * J.reg0;
-  double C[6], Fv[6];
-  C[0] = 0.0; Fv[0] = 0.0;
-  for (int m = 1; m <= 5; ++m) C[m] = qc[m - 1];
+  T C[6], Fv[6];
+  C[0] = T(0); Fv[0] = T(0);
+  for (int m = 1; m <= 5; ++m) C[m] = (T)qc[m - 1];
   int dir; double sgn, h1, h2;
   switch (J.side) {
     case 1: dir = 1; sgn = 1.0; h1 = hy; h2 = hz; break;
@@ -596,13 +603,14 @@ __global__ void qad3_kernel(double* pool, double* regs, const PatchDev* patches,
       }
       const long long a = at(i, j, k);
       for (int m = 1; m <= 5; ++m) Fv[m] = q[(m - 1) * plane + a];
-      double W[3][5], S[3], am[5], ap[5];
+      T W[3][5], S[3], amT[5], apT[5];
       const bool low = (J.side == 1 || J.side == 4 || J.side == 5);
-      if (low) euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, dir, C, Fv, W, S, am, ap);
-      else euler3d_rpn(sp.gamma, sp.gamma1, sp.efix != 0, dir, Fv, C, W, S, am, ap);
+      if (low) euler3d_rpn((T)sp.gamma, (T)sp.gamma1, sp.efix != 0, dir, C, Fv, W, S, amT, apT);
+      else euler3d_rpn((T)sp.gamma, (T)sp.gamma1, sp.efix != 0, dir, Fv, C, W, S, amT, apT);
       for (int m = 0; m < 5; ++m) {
-        if (sgn > 0.0) acc[m] = acc[m] + am[m] * h1 * h2 * delt + ap[m] * h1 * h2 * delt;
-        else acc[m] = acc[m] - am[m] * h1 * h2 * delt - ap[m] * h1 * h2 * delt;
+        const double am = amT[m], ap = apT[m];  // the registers accumulate in FP64
+        if (sgn > 0.0) acc[m] = acc[m] + am * h1 * h2 * delt + ap * h1 * h2 * delt;
+        else acc[m] = acc[m] - am * h1 * h2 * delt - ap * h1 * h2 * delt;
       }
     }
   }
@@ -611,18 +619,22 @@ __global__ void qad3_kernel(double* pool, double* regs, const PatchDev* patches,
 }
 
 // ------------------------------------------------------------------- ghost fill
-__device__ __forceinline__ double* fill3_dst(const Fill3Args& a, const Fill3Op& o, int& ni, int& nj, long long& plane) {
+// storage type T (double, or float in the FP32 form); the fill arithmetic is FP64
+template <class T>
+__device__ __forceinline__ T* fill3_dst(const Fill3Args& a, const Fill3Op& o, int& ni, int& nj, long long& plane) {
   if (o.dst_patch >= 0) {
     const PatchDev& P = a.patches[o.dst_patch];
     ni = P.mitot; nj = P.mjtot; plane = (long long)P.mitot * P.mjtot * P.mktot;
-    return a.pool + P.q[P.cur];
+    return static_cast<T*>(a.pool) + P.q[P.cur];
   }
   const Rect3& R = a.rects[o.dst_rect];
   ni = R.ni; nj = R.nj; plane = (long long)R.ni * R.nj * R.nk;
-  return a.pool + R.off;
+  return static_cast<T*>(a.pool) + R.off;
 }
 
+template <class T>
 __global__ void fill3_kernel(Fill3Args a) {
+  const T* pool = static_cast<const T*>(a.pool);
   const int c = blockIdx.x;
   if (c >= a.nchunks) return;
   const Fill3Chunk ch = a.chunks[c];
@@ -645,15 +657,15 @@ __global__ void fill3_kernel(Fill3Args a) {
     else { k -= s56; kk = nf; jj = 2 + (int)(k / (nr - 2)); ii = 2 + (int)(k % (nr - 2)); }
     const PatchDev& K = a.patches[o.dst_patch];
     double* qc1d = a.regs + K.ffl + (long long)nvar * K.lenbc + (long long)nvar * cell;
-    const double* src = a.pool + R.off;
+    const T* src = pool + R.off;
     const long long pl = (long long)nr * nc * nf;
     const long long idx = ((long long)(kk - 1) * nc + (jj - 1)) * nr + (ii - 1);
-    for (int m = 0; m < nvar; ++m) qc1d[m] = src[m * pl + idx];
+    for (int m = 0; m < nvar; ++m) qc1d[m] = (double)src[m * pl + idx];
     return;
   }
   const int ia = (int)(cell % o.ni), jb = (int)((cell / o.ni) % o.nj), kc = (int)(cell / ((long long)o.ni * o.nj));
   int dni, dnj; long long plane;
-  double* dst = fill3_dst(a, o, dni, dnj, plane);
+  T* dst = fill3_dst<T>(a, o, dni, dnj, plane);
   const long long dk = ((long long)(o.dk0 + kc) * dnj + (o.dj0 + jb)) * dni + (o.di0 + ia);
   if (o.kind == F3_COPY) {
     const PatchDev& S = a.patches[o.src];
@@ -661,21 +673,21 @@ __global__ void fill3_kernel(Fill3Args a) {
     const long long sk = ((long long)(o.sk0 + kc) * S.mjtot + (o.sj0 + jb)) * S.mitot + (o.si0 + ia);
     int mode = 0; double ai = 1.0, ac = 0.0;
     if (o.level >= 0) { mode = a.modes.mode[o.level]; ai = a.modes.alphai[o.level]; ac = a.modes.alphac[o.level]; }
-    const double* qn = a.pool + S.q[S.cur];
-    const double* qo = a.pool + S.q[1 - S.cur];
+    const T* qn = pool + S.q[S.cur];
+    const T* qo = pool + S.q[1 - S.cur];
     for (int m = 0; m < nvar; ++m) {
       double v;
-      if (mode == 0) v = qn[m * sp + sk];
-      else if (mode == 1) v = qo[m * sp + sk];
-      else v = qn[m * sp + sk] * ai + qo[m * sp + sk] * ac;
-      dst[m * plane + dk] = v;
+      if (mode == 0) v = (double)qn[m * sp + sk];
+      else if (mode == 1) v = (double)qo[m * sp + sk];
+      else v = (double)qn[m * sp + sk] * ai + (double)qo[m * sp + sk] * ac;
+      dst[m * plane + dk] = (T)v;
     }
     return;
   }
   const Rect3& R = a.rects[o.src];
-  const double* vc = a.pool + R.off;
+  const T* vc = pool + R.off;
   const long long cp = (long long)R.ni * R.nj * R.nk;
-  auto VC = [&](int m, int i, int j, int k) { return vc[m * cp + ((long long)(k - 1) * R.nj + (j - 1)) * R.ni + (i - 1)]; };
+  auto VC = [&](int m, int i, int j, int k) { return (double)vc[m * cp + ((long long)(k - 1) * R.nj + (j - 1)) * R.ni + (i - 1)]; };
   const int lev = o.level;
   const int rx = a.lc.intratx[lev - 1], ry = a.lc.intraty[lev - 1], rz = a.lc.intratz[lev - 1];
   const int ifg = o.si0 + ia, jfg = o.sj0 + jb, kfg = o.sk0 + kc;
@@ -708,7 +720,7 @@ __global__ void fill3_kernel(Fill3Args a) {
       dw = dmin(2.0 * dw, 0.5 * fabs(dwcc));
       const double fw = dmax(0.0, dsign(1.0, dwpc * dwmc));
       const double wslope = dw * dsign(1.0, dwcc) * fw;
-      dst[m * plane + dk] = valc + eta1 * uslope + eta2 * vslope + eta3 * wslope;
+      dst[m * plane + dk] = (T)(valc + eta1 * uslope + eta2 * vslope + eta3 * wslope);
     }
     return;
   }
@@ -725,21 +737,22 @@ __global__ void fill3_kernel(Fill3Args a) {
     slp = VC(m, ic, jc, kcc + 1) - VC(m, ic, jc, kcc); slm = VC(m, ic, jc, kcc) - VC(m, ic, jc, kcc - 1);
     s = dmin(fabs(slp), fabs(slm)) * dsign(1.0, VC(m, ic, jc, kcc + 1) - VC(m, ic, jc, kcc - 1));
     const double dudz = (slm * slp > 0.0) ? s : 0.0;
-    dst[m * plane + dk] = VC(m, ic, jc, kcc) + xoff * dudx + yoff * dudy + zoff * dudz;
+    dst[m * plane + dk] = (T)(VC(m, ic, jc, kcc) + xoff * dudx + yoff * dudy + zoff * dudz);
   }
 }
 
 // bc3amr.f90:70-380. phase 0: x sides per (j,k) row; 1: y sides per (i,k); 2: z sides per (i,j).
+template <class T>
 __global__ void bc3_kernel(Bc3Args a, int phase) {
   const int op = blockIdx.y;
   if (op >= a.nops) return;
   const Bc3Op o = a.ops[op];
-  double* v;
-  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = a.pool + P.q[P.cur]; }
-  else v = a.pool + a.rects[o.dst_rect].off;
+  T* v;
+  if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = static_cast<T*>(a.pool) + P.q[P.cur]; }
+  else v = static_cast<T*>(a.pool) + a.rects[o.dst_rect].off;
   const int nr = o.nrow, nc = o.ncol, nf = o.nfil;
   const long long plane = (long long)nr * nc * nf;
-  auto V = [&](int m, int i, int j, int k) -> double& { return v[m * plane + ((long long)(k - 1) * nc + (j - 1)) * nr + (i - 1)]; };
+  auto V = [&](int m, int i, int j, int k) -> T& { return v[m * plane + ((long long)(k - 1) * nc + (j - 1)) * nr + (i - 1)]; };
   const int nvar = a.nvar;
   const int lines = phase == 0 ? nc * nf : phase == 1 ? nr * nf : nr * nc;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < lines; t += gridDim.x * blockDim.x) {
@@ -778,35 +791,37 @@ __global__ void bc3_kernel(Bc3Args a, int phase) {
 }
 
 // upbnd.f:4-94: one coarse cell per thread, its terms in listbc order
-__global__ void upbnd3_kernel(double* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
+template <class T>
+__global__ void upbnd3_kernel(T* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
                               const Upbnd3Term* terms, double volume, int nvar) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const Upbnd3Cell c = cells[t];
   const PatchDev& P = patches[c.patch];
   const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
-  double* q = pool + P.q[P.cur];
+  T* q = pool + P.q[P.cur];
   const long long at = ((long long)c.ke * P.mjtot + c.je) * P.mitot + c.ie;
   for (int m = 0; m < nvar; ++m) {
-    double v = q[m * plane + at];
+    double v = (double)q[m * plane + at];
     for (int k = 0; k < c.count; ++k) {
       const Upbnd3Term tm = terms[c.first + k];
       v = v + tm.sgn * regs[tm.reg + m] / volume;
     }
-    q[m * plane + at] = v;
+    q[m * plane + at] = (T)v;
   }
 }
 
 // update.f:118-178: mean of the fine cells over each covered coarse cell
-__global__ void average3_kernel(double* pool, const PatchDev* patches, const Avg3* rects, int n, int rx, int ry, int rz, int nvar) {
+template <class T>
+__global__ void average3_kernel(T* pool, const PatchDev* patches, const Avg3* rects, int n, int rx, int ry, int rz, int nvar) {
   const int r = blockIdx.y;
   if (r >= n) return;
   const Avg3 A = rects[r];
   const PatchDev& C = patches[A.cpatch];
   const PatchDev& F = patches[A.kpatch];
   const long long cpl = (long long)C.mitot * C.mjtot * C.mktot, fpl = (long long)F.mitot * F.mjtot * F.mktot;
-  double* qc = pool + C.q[C.cur];
-  const double* qf = pool + F.q[F.cur];
+  T* qc = pool + C.q[C.cur];
+  const T* qf = pool + F.q[F.cur];
   const int totrat = rx * ry * rz;
   const int cells = A.ni * A.nj * A.nk;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cells; t += gridDim.x * blockDim.x) {
@@ -817,21 +832,22 @@ __global__ void average3_kernel(double* pool, const PatchDev* patches, const Avg
       double v = 0.0;
       for (int kco = 0; kco < rz; ++kco)
         for (int jco = 0; jco < ry; ++jco)
-          for (int ico = 0; ico < rx; ++ico) v = v + qf[m * fpl + ((long long)(fk + kco) * F.mjtot + (fj + jco)) * F.mitot + (fi + ico)];
-      qc[m * cpl + cat] = v / totrat;
+          for (int ico = 0; ico < rx; ++ico) v = v + (double)qf[m * fpl + ((long long)(fk + kco) * F.mjtot + (fj + jco)) * F.mitot + (fi + ico)];
+      qc[m * cpl + cat] = (T)(v / totrat);
     }
   }
 }
 
 // gauges_module.f90:376-430 trilinear sample
-__global__ void gauges3_kernel(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out) {
+template <class T>
+__global__ void gauges3_kernel(const T* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const Gauge3Job J = jobs[t];
   const PatchDev& P = patches[J.patch];
   const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
-  const double* q = pool + P.q[P.cur];
-  auto Q = [&](int m, int ii, int jj, int kk) { return q[m * plane + ((long long)(kk - 1) * P.mjtot + (jj - 1)) * P.mitot + (ii - 1)]; };
+  const T* q = pool + P.q[P.cur];
+  auto Q = [&](int m, int ii, int jj, int kk) { return (double)q[m * plane + ((long long)(kk - 1) * P.mjtot + (jj - 1)) * P.mitot + (ii - 1)]; };
   const double xoff = J.xoff, yoff = J.yoff, zoff = J.zoff;
   const int ii = J.ii, jj = J.jj, kk = J.kk;
   for (int m = 0; m < nvar; ++m) {
@@ -844,22 +860,24 @@ __global__ void gauges3_kernel(const double* pool, const PatchDev* patches, cons
   }
 }
 
-__global__ void mass3_kernel(const double* pool, const PatchDev* patches, const int* plist, int np, double* out) {
+template <class T>
+__global__ void mass3_kernel(const T* pool, const PatchDev* patches, const int* plist, int np, double* out) {
   const int p = blockIdx.y;
   if (p >= np) return;
   const PatchDev& P = patches[plist[p]];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
-  const double* q = pool + P.q[P.cur];
+  const T* q = pool + P.q[P.cur];
   double s = 0.0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my * mz; t += gridDim.x * blockDim.x) {
     const int i = t % mx, j = (t / mx) % my, k = t / (mx * my);
-    s += q[((long long)(k + NG3) * P.mjtot + (j + NG3)) * P.mitot + (i + NG3)];
+    s += (double)q[((long long)(k + NG3) * P.mjtot + (j + NG3)) * P.mitot + (i + NG3)];
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
 
-__global__ void gather3_kernel(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
+template <class T>
+__global__ void gather3_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
                                long long total, double* out) {
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int pi = find_patch(cell0, np, t);
@@ -869,9 +887,9 @@ __global__ void gather3_kernel(const double* pool, const PatchDev* patches, cons
     const long long loc = t - cell0[pi];
     const int i = (int)(loc % mx), j = (int)((loc / mx) % my), k = (int)(loc / ((long long)mx * my));
     const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
-    const double* q = pool + P.q[P.cur];
+    const T* q = pool + P.q[P.cur];
     const long long at = ((long long)(k + NG3) * P.mjtot + (j + NG3)) * P.mitot + (i + NG3);
-    for (int m = 0; m < nvar; ++m) out[cell0[pi] * nvar + m * n + loc] = q[m * plane + at];
+    for (int m = 0; m < nvar; ++m) out[cell0[pi] * nvar + m * n + loc] = (double)q[m * plane + at];
   }
 }
 
@@ -906,15 +924,20 @@ int grid_for(long long n, int block) {
 
 }  // namespace
 
-void launch_step3(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s) {
+template <class T>
+static void launch_step3_t(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s) {
   auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
-  if (items[0] > 0) sweep3_kernel<1><<<tiles(items[0]), SW_T, 0, s>>>(a);
-  if (items[1] > 0) sweep3_kernel<2><<<tiles(items[1]), SW_T, 0, s>>>(a);
-  if (items[2] > 0) sweep3_kernel<3><<<tiles(items[2]), SW_T, 0, s>>>(a);
+  if (items[0] > 0) sweep3_kernel<1, T><<<tiles(items[0]), SW_T, 0, s>>>(a);
+  if (items[1] > 0) sweep3_kernel<2, T><<<tiles(items[1]), SW_T, 0, s>>>(a);
+  if (items[2] > 0) sweep3_kernel<3, T><<<tiles(items[2]), SW_T, 0, s>>>(a);
   AMR_CUDA(cudaGetLastError());
-  if (faces > 0) face3_kernel<<<grid_for(faces, 128), 128, 0, s>>>(a);
-  if (cells > 0) update3_kernel<<<grid_for(cells, 256), 256, 0, s>>>(a);
+  if (faces > 0) face3_kernel<T><<<grid_for(faces, 128), 128, 0, s>>>(a);
+  if (cells > 0) update3_kernel<T><<<grid_for(cells, 256), 256, 0, s>>>(a);
   AMR_CUDA(cudaGetLastError());
+}
+void launch_step3(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s, bool f32) {
+  if (f32) launch_step3_t<float>(a, items, faces, cells, s);
+  else launch_step3_t<double>(a, items, faces, cells, s);
 }
 
 void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,
@@ -924,77 +947,88 @@ void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const
   AMR_CUDA(cudaGetLastError());
 }
 
-void launch_fsv3(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fsv3* e, int n,
-                 int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s) {
+void launch_fsv3(const void* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fsv3* e, int n,
+                 int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s, bool f32) {
   if (n <= 0) return;
-  fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(flux, fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz);
+  if (f32) fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const float*>(flux), fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz);
+  else fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const double*>(flux), fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz);
   AMR_CUDA(cudaGetLastError());
 }
-void launch_fad3(const double* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fad3* e, int n,
-                 int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s) {
+void launch_fad3(const void* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fad3* e, int n,
+                 int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s, bool f32) {
   if (n <= 0) return;
-  fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(flux, fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz);
+  if (f32) fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const float*>(flux), fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz);
+  else fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const double*>(flux), fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz);
   AMR_CUDA(cudaGetLastError());
 }
-void launch_qad3(double* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp, int nvar,
-                 double hx, double hy, double hz, double delt, cudaStream_t s) {
+void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp, int nvar,
+                 double hx, double hy, double hz, double delt, cudaStream_t s, bool f32) {
   if (njobs <= 0) return;
-  qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(pool, regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
+  if (f32) qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
+  else qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
   AMR_CUDA(cudaGetLastError());
 }
-void launch_fill3(const Fill3Args& a, cudaStream_t s) {
+void launch_fill3(const Fill3Args& a, cudaStream_t s, bool f32) {
   if (a.nchunks <= 0) return;
   for (int base = 0; base < a.nchunks; base += 1 << 30) {
     Fill3Args b = a;
     b.chunks = a.chunks + base;
     b.nchunks = std::min(1 << 30, a.nchunks - base);
-    fill3_kernel<<<b.nchunks, 128, 0, s>>>(b);
+    if (f32) fill3_kernel<float><<<b.nchunks, 128, 0, s>>>(b);
+    else fill3_kernel<double><<<b.nchunks, 128, 0, s>>>(b);
   }
   AMR_CUDA(cudaGetLastError());
 }
-void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s) {
+void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s, bool f32) {
   if (a.nops <= 0) return;
   for (int base = 0; base < a.nops; base += 65535) {
     Bc3Args b = a;
     b.ops = a.ops + base;
     b.nops = std::min(65535, a.nops - base);
-    bc3_kernel<<<dim3(4, b.nops), 128, 0, s>>>(b, phase);
+    if (f32) bc3_kernel<float><<<dim3(4, b.nops), 128, 0, s>>>(b, phase);
+    else bc3_kernel<double><<<dim3(4, b.nops), 128, 0, s>>>(b, phase);
   }
   AMR_CUDA(cudaGetLastError());
 }
-void launch_upbnd3(double* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n, const Upbnd3Term* terms,
-                   double volume, int nvar, cudaStream_t s) {
+void launch_upbnd3(void* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n, const Upbnd3Term* terms,
+                   double volume, int nvar, cudaStream_t s, bool f32) {
   if (n <= 0) return;
-  upbnd3_kernel<<<(n + 127) / 128, 128, 0, s>>>(pool, regs, patches, cells, n, terms, volume, nvar);
+  if (f32) upbnd3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, cells, n, terms, volume, nvar);
+  else upbnd3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, cells, n, terms, volume, nvar);
   AMR_CUDA(cudaGetLastError());
 }
-void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, long long max_cells, int rx, int ry, int rz, int nvar,
-                     cudaStream_t s) {
+void launch_average3(void* pool, const PatchDev* patches, const Avg3* r, int n, long long max_cells, int rx, int ry, int rz, int nvar,
+                     cudaStream_t s, bool f32) {
   if (n <= 0) return;
   const int bx = (int)std::max<long long>(1, std::min<long long>((max_cells + 127) / 128, 1024));
   for (int base = 0; base < n; base += 65535) {
     const int cnt = std::min(65535, n - base);
-    average3_kernel<<<dim3(bx, cnt), 128, 0, s>>>(pool, patches, r + base, cnt, rx, ry, rz, nvar);
+    if (f32) average3_kernel<<<dim3(bx, cnt), 128, 0, s>>>(static_cast<float*>(pool), patches, r + base, cnt, rx, ry, rz, nvar);
+    else average3_kernel<<<dim3(bx, cnt), 128, 0, s>>>(static_cast<double*>(pool), patches, r + base, cnt, rx, ry, rz, nvar);
   }
   AMR_CUDA(cudaGetLastError());
 }
-void launch_gauges3(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s) {
+void launch_gauges3(const void* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s,
+                    bool f32) {
   if (n <= 0) return;
-  gauges3_kernel<<<(n + 63) / 64, 64, 0, s>>>(pool, patches, jobs, n, nvar, out);
+  if (f32) gauges3_kernel<<<(n + 63) / 64, 64, 0, s>>>(static_cast<const float*>(pool), patches, jobs, n, nvar, out);
+  else gauges3_kernel<<<(n + 63) / 64, 64, 0, s>>>(static_cast<const double*>(pool), patches, jobs, n, nvar, out);
   AMR_CUDA(cudaGetLastError());
 }
-void launch_mass3(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s) {
+void launch_mass3(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32) {
   if (np <= 0) return;
   for (int base = 0; base < np; base += 65535) {
     const int cnt = std::min(65535, np - base);
-    mass3_kernel<<<dim3(8, cnt), 128, 0, s>>>(pool, patches, plist + base, cnt, out);
+    if (f32) mass3_kernel<<<dim3(8, cnt), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, cnt, out);
+    else mass3_kernel<<<dim3(8, cnt), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, cnt, out);
   }
   AMR_CUDA(cudaGetLastError());
 }
-void launch_gather3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
-                    long long total, double* out, cudaStream_t s) {
+void launch_gather3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
+                    long long total, double* out, cudaStream_t s, bool f32) {
   if (total <= 0) return;
-  gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(pool, patches, plist, cell0, np, nvar, total, out);
+  if (f32) gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const float*>(pool), patches, plist, cell0, np, nvar, total, out);
+  else gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const double*>(pool), patches, plist, cell0, np, nvar, total, out);
   AMR_CUDA(cudaGetLastError());
 }
 

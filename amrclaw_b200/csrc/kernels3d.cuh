@@ -18,8 +18,9 @@ struct Step3Params {
 };
 
 // All patches of a level: prefix sums of the sweep items and face cells per patch.
+// pool, stash and flux hold double, or float in the FP32 form (offsets count elements)
 struct Step3Args {
-  const double* pool;
+  const void* pool;
   double* newq;              // nullptr: update in place is not used; q[1-cur] is written
   const PatchDev* patches;
   const int* plist;          // patch ids of the level, in level order
@@ -29,8 +30,8 @@ struct Step3Args {
   const long long* face0;    // [np+1]: first face cell of each patch ((mx+1)(my+1)(mz+1) each)
   const long long* cell0;    // [np+1]: first interior cell of each patch (mx*my*mz each)
   long long stash_stride;    // slots of one direction region x 3 (SoA stride)
-  double* stash;             // [STASH3][stash_stride]
-  double* flux;              // [6 comps][5][face cells]
+  void* stash;               // [STASH3][stash_stride]
+  void* flux;                // [6 comps][5][face cells]
   long long flux_stride;     // face cells of the level
   double dt, dx, dy, dz;
   unsigned long long* cflmax;
@@ -64,7 +65,7 @@ struct Bc3Op {
   int bxl, bxr, byl, byr, bzl, bzr;      // boundary codes (1 extrapolation, 3 wall)
 };
 struct Fill3Args {
-  double* pool; double* regs;
+  void* pool; double* regs;
   const PatchDev* patches;
   const Rect3* rects;
   const Fill3Op* ops;
@@ -74,34 +75,37 @@ struct Fill3Args {
   LevelConst lc;
   double xlower, ylower, zlower;
 };
-struct Bc3Args { double* pool; const PatchDev* patches; const Rect3* rects; const Bc3Op* ops; int nops; int nvar; };
+struct Bc3Args { void* pool; const PatchDev* patches; const Rect3* rects; const Bc3Op* ops; int nops; int nvar; };
 
 struct Avg3 { int cpatch, kpatch; int ci0, cj0, ck0, ni, nj, nk; int fi0, fj0, fk0; };
 struct Upbnd3Cell { int patch; int ie, je, ke; int first, count; };
 struct Upbnd3Term { long long reg; double sgn; };
 struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff; };
 
-// interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction
-void launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s);
+// Launch wrappers (kernels3d.cu). f32: the FP32 form (float storage, Riemann solves and
+// flux differencing; FP64 registers, register corrections, averages and totals).
+// interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction.
+void launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s, bool f32);
 // Builds the level's fluxad/qad work lists on the device: pre[np+1] is the prefix of the
 // register segments (lenbc) of the patches in plist (0 for patches without registers).
 void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,
                            long long total, Fad3* fad, Qad3Job* qad, cudaStream_t s);
-void launch_fsv3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
-                 const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s);
-void launch_fad3(const double* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
-                 const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s);
-void launch_qad3(double* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
-                 int nvar, double hx, double hy, double hz, double delt, cudaStream_t s);
-void launch_fill3(const Fill3Args& a, cudaStream_t s);
-void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s);
-void launch_upbnd3(double* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
-                   const Upbnd3Term* terms, double volume, int nvar, cudaStream_t s);
-void launch_average3(double* pool, const PatchDev* patches, const Avg3* r, int n, long long max_cells, int rx, int ry, int rz, int nvar,
-                     cudaStream_t s);
-void launch_gauges3(const double* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s);
-void launch_mass3(const double* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s);
-void launch_gather3(const double* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
-                    long long total, double* out, cudaStream_t s);
+void launch_fsv3(const void* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
+                 const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s, bool f32);
+void launch_fad3(const void* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
+                 const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s, bool f32);
+void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
+                 int nvar, double hx, double hy, double hz, double delt, cudaStream_t s, bool f32);
+void launch_fill3(const Fill3Args& a, cudaStream_t s, bool f32);
+void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s, bool f32);
+void launch_upbnd3(void* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
+                   const Upbnd3Term* terms, double volume, int nvar, cudaStream_t s, bool f32);
+void launch_average3(void* pool, const PatchDev* patches, const Avg3* r, int n, long long max_cells, int rx, int ry, int rz, int nvar,
+                     cudaStream_t s, bool f32);
+void launch_gauges3(const void* pool, const PatchDev* patches, const Gauge3Job* jobs, int n, int nvar, double* out, cudaStream_t s,
+                    bool f32);
+void launch_mass3(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32);
+void launch_gather3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
+                    long long total, double* out, cudaStream_t s, bool f32);
 
 }  // namespace amrb

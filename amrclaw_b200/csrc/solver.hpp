@@ -24,6 +24,7 @@ class AmrSolver {
 };
 
 // Builds and initialises the 3D solver (amr3d.cu) from the data files in rundir.
-AmrSolver* make_solver3(const std::string& rundir, const std::string& outdir, bool write_output);
+// f32: the FP32 form (float storage, Riemann solves and fluxes; FP64 registers and totals)
+AmrSolver* make_solver3(const std::string& rundir, const std::string& outdir, bool write_output, bool f32);
 
 }  // namespace amrb

@@ -113,10 +113,13 @@ def flush_l2(buf):
     torch.cuda.synchronize()
 
 
-def fp32_leg(cpu_threads: int) -> dict:
-    """The FP32 form on the 2D acoustic pulse (64^2 base grid, 4 levels, ratio 2, t = 0.4):
-    device throughput of the FP32 and FP64 runs, and the FP32 run's level-1 L1 error and
-    mass against the FP64 oracle (the reference's arithmetic)."""
+def fp32_leg(cpu_threads: int, rd3=None, cfg3=None) -> dict:
+    """The FP32 form. 2D acoustic pulse (64^2 base grid, 4 levels, ratio 2, t = 0.4): device
+    throughput of the FP32 and FP64 runs, and the FP32 run's level-1 L1 error and mass
+    against the FP64 oracle (the reference's arithmetic). 3D (rd3, the headline workload):
+    FP32 and FP64 device throughput over the whole solve and the FP32 level-1 L1 error
+    against the FP64 device run, which the parity tests hold bit-identical to the oracle
+    (the oracle itself would take minutes at this size)."""
     from amrclaw_b200 import Solver, fields, problems
     from oracle.pyoracle import Oracle2D
     rd = problems.acoustics_pulse(64, levels=4, ratio=2, tfinal=0.4)
@@ -138,6 +141,25 @@ def fp32_leg(cpu_threads: int) -> dict:
         _, rel = fields.l1_error(fields.level_array(g, v, 3, 1, (64, 64)), ref, (2.0 / 64) ** 2)
         out[prec] = {"value": cups, "unit": "cell-updates/s", "l1_rel_err_vs_fp64_oracle": [float(x) for x in rel],
                      "mass_rel_diff_vs_fp64_oracle": abs(m - m64) / abs(m64)}
+    if rd3 is not None:
+        n = cfg3["base_grid"]
+        n = int(str(n).split("x")[0]) if not isinstance(n, int) else n
+        o3 = {"workload": cfg3["workload"], "base_grid": cfg3["base_grid"], "levels": cfg3.get("levels")}
+        with tempfile.TemporaryDirectory() as d:
+            rd3.write(d)
+            res = {}
+            for prec in ("fp64", "fp32"):
+                with Solver(d, precision=prec) as s:
+                    s.run(0)
+                    inf = s.info()
+                    res[prec] = (s.grids(), s.values(), s.mass(), inf["cell_updates"], inf["last_run_ms"])
+        g, v, m, _, _ = res["fp64"]
+        ref = fields.level_array(g, v, 5, 1, (n, n, n))
+        for prec, (g, v, mm, cells, ms) in res.items():
+            _, rel = fields.l1_error(fields.level_array(g, v, 5, 1, (n, n, n)), ref, (2.0 / n) ** 3)
+            o3[prec] = {"value": cells / (ms * 1e-3), "unit": "cell-updates/s", "solve_ms": ms, "cell_updates": cells,
+                        "l1_rel_err_vs_fp64": [float(x) for x in rel], "mass_rel_diff_vs_fp64": abs(mm - m) / abs(m)}
+        out["blast3d"] = o3
     return out
 
 
@@ -278,8 +300,11 @@ def main():
             dist.destroy_process_group()
         return
     peak, peak_kind = peaks()
+    fp32 = None
+    if not args.no_cpu_baseline:
+        rd3, cfg3, _, _, nd3 = workload(args.workload)
+        fp32 = fp32_leg(os.cpu_count() or 1, rd3 if nd3 == 3 else None, cfg3)
     os.environ.setdefault("AMRGPU_HOST_THREADS", "2")
-    fp32 = fp32_leg(os.cpu_count() or 1) if not args.no_cpu_baseline else None
     serving = serving_leg() if not args.no_cpu_baseline else None
     achieved = kern_cells * bytes_per_update / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
     cpu = None
