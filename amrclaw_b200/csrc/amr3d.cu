@@ -37,6 +37,7 @@ struct HPatch3 {
   double xlo = 0, xhi = 0, ylo = 0, yhi = 0, zlo = 0, zhi = 0, time = 0;
   long long q0 = -1, q1 = -1, nq = 0;
   long long ffl = -1, nffl = 0;
+  long long aux = -1, na = 0;  // aux block: na values, then (time-modulated swirl) na setaux values
   int lenbc = 0;
   int cur = 0;
   bool has_cfl = false;
@@ -228,9 +229,26 @@ class Amr3Gpu : public AmrSolver {
 
   // ================================================================ setup
   void setup_problem() {
-    if (p.problem != "euler_blast") throw std::runtime_error("3D device path: unknown problem '" + p.problem + "' (the 3D device path solves the Euler equations)");
-    if (p.nvar != 5 || p.mwaves != 3) throw std::runtime_error("3D Euler needs num_eqn = 5 and num_waves = 3");
-    if (p.naux != 0) throw std::runtime_error("3D device path: aux arrays are not supported");
+    if (p.problem == "euler_blast") {
+      sp.solver = SOLVER3_EULER;
+      if (p.nvar != 5 || p.mwaves != 3) throw std::runtime_error("3D Euler needs num_eqn = 5 and num_waves = 3");
+      if (p.naux != 0) throw std::runtime_error("3D Euler: aux arrays are not used");
+    } else if (p.problem == "advection_swirl") {
+      sp.solver = SOLVER3_SWIRL;
+      if (p.nvar != 1 || p.mwaves != 1) throw std::runtime_error("the swirl needs num_eqn = 1 and num_waves = 1");
+      if (p.naux != 3 || p.auxtype.size() != 3 || p.auxtype[0] != "xleft" || p.auxtype[1] != "yleft" || p.auxtype[2] != "zleft")
+        throw std::runtime_error("the swirl needs 3 aux arrays of types xleft, yleft, zleft");
+      const std::string ic = p.ps("ic", "halfspace");
+      if (ic != "halfspace" && ic != "sphere") throw std::runtime_error("swirl: ic must be halfspace or sphere");
+      swirl_sphere = ic == "sphere";
+      sph_x = p.pn("x0", 0.5); sph_y = p.pn("y0", 0.25); sph_z = p.pn("z0", 0.5); sph_r = p.pn("r0", 0.15);
+      vel_period = p.pn("vel_period", 0.0);
+      // the wall condition negates the momentum components (2..4) of the Euler state
+      for (int d = 1; d <= 6; ++d)
+        if (p.mthbc[d] != 1) throw std::runtime_error("the swirl takes extrapolation boundaries only");
+    } else {
+      throw std::runtime_error("3D device path: unknown problem '" + p.problem + "' (euler_blast or advection_swirl)");
+    }
     if (p.nghost != G3) throw std::runtime_error("num_ghost must be 2");
     if (p.mcapa != 0 || p.dimsplit != 0) throw std::runtime_error("capacity functions and dimensional splitting are not supported");
     if (p.use_fwaves) throw std::runtime_error("f-waves are not supported in 3D");
@@ -248,12 +266,84 @@ class Amr3Gpu : public AmrSolver {
   }
   double blast_x = 0, blast_y = 0, blast_z = 0, blast_r = 0.2, blast_pin = 5, blast_pout = 1;
   int flag_pressure = 1;
+  // swirl: the initial condition is the half space x < 0.5 (tests/advection_3d_swirl/qinit.f)
+  // or the sphere of radius r0 about (x0, y0, z0); vel_period > 0 scales the velocity
+  // field by cos(pi t / vel_period) before each step (b4step3)
+  bool swirl_sphere = false;
+  double sph_x = 0.5, sph_y = 0.25, sph_z = 0.5, sph_r = 0.15, vel_period = 0.0;
+
+  // setaux of the swirl (tests/advection_3d_swirl/setaux.f:2-85): u, v, w at the left x-,
+  // y- and z-face of every cell of the enlarged patch, layout [ma][k][j][i]
+  void setaux(const HPatch3& g, double dx, double dy, double dz, std::vector<double>& a) const {
+    const int mi = g.nx() + 2 * G3, mj = g.ny() + 2 * G3, mk = g.nz() + 2 * G3;
+    const long long pl = (long long)mi * mj * mk;
+    a.assign((size_t)pl * 3, 0.0);
+    const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
+    const double dx2 = 0.5 * dx, dy2 = 0.5 * dy, dz2 = 0.5 * dz;
+    auto su = [&](double x, double y, double z) { double s = std::sin(pi * x); return 2.0 * (s * s) * std::sin(pi2 * y) * std::sin(pi2 * z); };
+    auto sv = [&](double x, double y, double z) { double s = std::sin(pi * y); return -std::sin(pi2 * x) * (s * s) * std::sin(pi2 * z); };
+    auto sw = [&](double x, double y, double z) { double s = std::sin(pi * z); return -std::sin(pi2 * x) * std::sin(pi2 * y) * (s * s); };
+    for (int k = 1 - G3; k <= g.nz() + G3; ++k) {
+      const double zc = g.zlo + (k - 0.5) * dz;
+      for (int j = 1 - G3; j <= g.ny() + G3; ++j) {
+        const double yc = g.ylo + (j - 0.5) * dy;
+        for (int i = 1 - G3; i <= g.nx() + G3; ++i) {
+          const double xc = g.xlo + (i - 0.5) * dx;
+          const long long at = ((long long)(k - 1 + G3) * mj + (j - 1 + G3)) * mi + (i - 1 + G3);
+          a[at] = su(xc - dx2, yc, zc);
+          a[pl + at] = sv(xc, yc - dy2, zc);
+          a[2 * pl + at] = sw(xc, yc, zc - dz2);
+        }
+      }
+    }
+  }
+  // setaux of new patches, computed on the host threads, into aux (and the setaux copy the
+  // time-modulated b4step3 scales)
+  void init_aux(const std::vector<int>& ms) {
+    if (p.naux == 0 || ms.empty()) return;
+    HPROF("init_aux3");
+    std::vector<std::vector<double>> A(ms.size());
+    pool_host.run((int)ms.size(), [&](int k) {
+      const HPatch3& g = node[ms[k]];
+      setaux(g, hxposs[g.level], hyposs[g.level], hzposs[g.level], A[k]);
+    });
+    std::vector<float> af;
+    for (size_t k = 0; k < ms.size(); ++k) {
+      const HPatch3& g = node[ms[k]];
+      const void* src = A[k].data();
+      if (f32) { af.assign(A[k].begin(), A[k].end()); src = af.data(); }
+      const size_t bytes = elem() * A[k].size();
+      for (int copy = 0; copy < (vel_period > 0.0 ? 2 : 1); ++copy)
+        AMR_CUDA(cudaMemcpyAsync(pool_bytes() + elem() * (g.aux + copy * g.na), stg.put(src, bytes, st), bytes, cudaMemcpyHostToDevice, st));
+      h2d_bytes += (vel_period > 0.0 ? 2.0 : 1.0) * bytes;
+    }
+  }
 
   // qinit (Euler blast): rho = 1, u = 0, p = pin within r0 of the centre, pout outside; layout [m][k][j][i]
   void qinit(const HPatch3& g, double dx, double dy, double dz, std::vector<double>& q) {
     const int mi = g.nx() + 2 * G3, mj = g.ny() + 2 * G3, mk = g.nz() + 2 * G3;
     const long long pl = (long long)mi * mj * mk;
     q.assign((size_t)pl * nvar, 0.0);
+    if (sp.solver == SOLVER3_SWIRL) {
+      // tests/advection_3d_swirl/qinit.f:5-42 (q = 1 for x < 0.5), or the sphere
+      for (int k = 1; k <= g.nz(); ++k) {
+        const double zc = g.zlo + (k - 0.5) * dz;
+        for (int j = 1; j <= g.ny(); ++j) {
+          const double yc = g.ylo + (j - 0.5) * dy;
+          for (int i = 1; i <= g.nx(); ++i) {
+            const double xc = g.xlo + (i - 0.5) * dx;
+            const long long at = ((long long)(k - 1 + G3) * mj + (j - 1 + G3)) * mi + (i - 1 + G3);
+            if (swirl_sphere) {
+              const double ddx = xc - sph_x, ddy = yc - sph_y, ddz = zc - sph_z;
+              q[at] = (ddx * ddx + ddy * ddy + ddz * ddz <= sph_r * sph_r) ? 1.0 : 0.0;
+            } else {
+              q[at] = (xc < 0.5) ? 1.0 : 0.0;
+            }
+          }
+        }
+      }
+      return;
+    }
     const double g1 = sp.gamma - 1.0;
     for (int k = 1; k <= g.nz(); ++k) {
       const double zc = g.zlo + (k - 0.5) * dz;
@@ -270,6 +360,17 @@ class Amr3Gpu : public AmrSolver {
         }
       }
     }
+  }
+
+  // cos(pi t / vel_period): the b4step3 scale of the swirl velocities at the step's start time
+  double b4step_factor(double t) const {
+    const double pi = 4.0 * std::atan(1.0);
+    return std::cos(pi * t / vel_period);
+  }
+  long long max_enlarged(int lev) const {
+    long long mx = 0;
+    for (int m : lgrids[lev]) mx = std::max(mx, (long long)mitot(m) * mjtot(m) * mktot(m));
+    return mx;
   }
 
   // ================================================================ node store
@@ -305,10 +406,16 @@ class Amr3Gpu : public AmrSolver {
     g.q0 = palloc(g.nq);
     g.q1 = palloc(g.nq);
     g.cur = 0;
+    if (p.naux > 0) {
+      g.na = (long long)p.naux * mitot(m) * mjtot(m) * mktot(m);
+      g.aux = palloc(g.na * (vel_period > 0.0 ? 2 : 1));
+    }
   }
   void free_patch(int m) {
     HPatch3& g = node[m];
     pfree(g.q0, g.nq); pfree(g.q1, g.nq);
+    if (g.aux >= 0) pfree(g.aux, g.na * (vel_period > 0.0 ? 2 : 1));
+    g.aux = -1; g.na = 0;
     g.q0 = g.q1 = -1;
     if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
     g.ffl = -1; g.nffl = 0;
@@ -319,6 +426,7 @@ class Amr3Gpu : public AmrSolver {
     d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl;
     d.ilo = g.ilo; d.ihi = g.ihi; d.jlo = g.jlo; d.jhi = g.jhi; d.klo = g.klo; d.khi = g.khi;
     d.mitot = mitot(m); d.mjtot = mjtot(m); d.mktot = mktot(m); d.level = g.level; d.lenbc = g.lenbc;
+    d.aux = g.aux;
   }
   void sync_descriptors(const std::vector<int>* extra = nullptr, int extra_levels_below = 0) {
     h_patches.assign(id_hwm, PatchDev{});
@@ -798,8 +906,8 @@ class Amr3Gpu : public AmrSolver {
     }
     // staging and face-flux buffers sized for the largest level
     tph.next("cs_reserve");
-    d_stash.reserve(std::max<size_t>(d_stash.n, (size_t)(L.slots * STASH3)));
-    d_flux.reserve(std::max<size_t>(d_flux.n, (size_t)(L.faces * 30)));
+    d_stash.reserve(std::max<size_t>(d_stash.n, (size_t)(L.slots * stash_values(nvar))));
+    d_flux.reserve(std::max<size_t>(d_flux.n, (size_t)(L.faces * 6 * nvar)));
   }
 
   // update.f:4-192 + upbnd.f:4-94 for coarse level lev
@@ -1049,6 +1157,10 @@ class Amr3Gpu : public AmrSolver {
       }
       sample_gauges(lev);
       AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+      if (vel_period > 0.0) {
+        launch_b4step3(pool.d, d_patches.d, L.d_plist.d, (int)L.plist.size(), p.naux, max_enlarged(lev), b4step_factor(t), st, f32);
+        ++nkernels;
+      }
       if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
       a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
@@ -1080,6 +1192,12 @@ class Amr3Gpu : public AmrSolver {
         const long long q0 = L.seg0[k], nq = L.seg0[k + 1] - L.seg0[k];
         if (lev > 1 && nq > 0) {
           launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d + q0, (int)nq, sp, nvar, hx, hy, hz, dt, st, f32);
+          ++nkernels;
+        }
+        if (vel_period > 0.0) {
+          const int m = L.plist[k];
+          launch_b4step3(pool.d, d_patches.d, L.d_plist.d + k, 1, p.naux, (long long)mitot(m) * mjtot(m) * mktot(m),
+                         b4step_factor(t), st, f32);
           ++nkernels;
         }
         Step3Args b = a;
@@ -1513,6 +1631,7 @@ class Amr3Gpu : public AmrSolver {
       std::vector<int> nl;
       tph.next("rg_alloc");
       for (int m = newstl[l2]; m != 0; m = node[m].levelptr) { alloc_patch(m); nl.push_back(m); }
+      init_aux(nl);
       // descriptors: current levels (levels below l2 already replaced), the old grids of l2 and the new ones
       tph.next("rg_desc");
       sync_descriptors(&nl, 0);
@@ -1562,6 +1681,7 @@ class Amr3Gpu : public AmrSolver {
       AMR_CUDA(cudaMemcpyAsync(pool_bytes() + elem() * g.q0, src, elem() * q.size(), cudaMemcpyHostToDevice, st));
       AMR_CUDA(cudaMemcpyAsync(pool_bytes() + elem() * g.q1, src, elem() * q.size(), cudaMemcpyHostToDevice, st));
       h2d_bytes += 2.0 * elem() * q.size();
+      init_aux({m});
       sync_stream();
     }
   }
@@ -1571,7 +1691,7 @@ class Amr3Gpu : public AmrSolver {
     nvar = p.nvar;
     blast_x = p.pn("x0", 0.0); blast_y = p.pn("y0", 0.0); blast_z = p.pn("z0", 0.0);
     blast_r = p.pn("r0", 0.2); blast_pin = p.pn("pin", 5.0); blast_pout = p.pn("pout", 1.0);
-    flag_pressure = (int)p.pn("flag_pressure", 1.0);
+    flag_pressure = p.problem == "euler_blast" ? (int)p.pn("flag_pressure", 1.0) : 0;
     setup_problem();
     xlower = p.lower[0]; ylower = p.lower[1]; zlower = p.lower[2];
     xupper = p.upper[0]; yupper = p.upper[1]; zupper = p.upper[2];
@@ -1610,8 +1730,8 @@ class Amr3Gpu : public AmrSolver {
     {
       // sweep staging and face fluxes: reserved at once for twice a level-1 sweep
       const long long n = (long long)nxc * nyc * nzc;
-      d_stash.reserve((size_t)(STASH3 * 3 * (n + 4LL * (nxc * nyc + nyc * nzc + nxc * nzc))));
-      d_flux.reserve((size_t)(30 * (n + 2LL * (nxc * nyc + nyc * nzc + nxc * nzc) + 8)));
+      d_stash.reserve((size_t)(stash_values(nvar) * 3 * (n + 4LL * (nxc * nyc + nyc * nzc + nxc * nzc))));
+      d_flux.reserve((size_t)(6 * nvar * (n + 2LL * (nxc * nyc + nyc * nzc + nxc * nzc) + 8)));
       d_stash.n = d_flux.n = 0;
     }
     node.assign(10001, HPatch3());
@@ -1666,7 +1786,7 @@ class Amr3Gpu : public AmrSolver {
     record_gauges = true;
     time = start_time;
     tmass0 = mass();
-    if (p.output_t0 && write_output) output(time);
+    if (p.output_t0) output(time);
   }
 
   // ================================================================ tick.f
@@ -1790,6 +1910,10 @@ class Amr3Gpu : public AmrSolver {
     return out;
   }
   void output(double t) {
+    for (int lev = 1; lev <= lfine; ++lev) {
+      launch_zero_tiny3(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
+      ++nkernels;
+    }
     if (!write_output) { ++frame; return; }
     const std::vector<double> v = gather_values();
     char fn[64];

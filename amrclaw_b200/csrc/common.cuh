@@ -34,6 +34,7 @@ struct PatchDev {
   int level;
   int lenbc;
   int pad;
+  long long aux;       // pool offset of the aux array [maux][k][j][i] of the enlarged patch (3D), -1 if none
 };
 
 // Per-level constants that device code needs (spacing, ratios, domain sizes).

@@ -73,15 +73,90 @@ constexpr int SW_OWN = SW_T - 3;
 #endif
 
 // (a - 3*b) (m4 = 2) or a: the doubly transverse inputs of flux3.f:429-507
-template <class T>
+template <int NV, class T>
 __device__ __forceinline__ void dt_input(int m4, T sgn3, const T* a, const T* b, T* o) {
 #pragma unroll
-  for (int m = 0; m < 5; ++m) o[m] = (m4 == 2) ? a[m] + sgn3 * b[m] : a[m];
+  for (int m = 0; m < NV; ++m) o[m] = (m4 == 2) ? a[m] + sgn3 * b[m] : a[m];
 }
 
-template <int DIR, class T>
+// ---- physics policies of the sweep: the problem's rpn3 / rpt3 / rptt3 at one interface.
+// imp: 1 splits the amdq side (cell e-1), 2 the apdq side (cell e); icoor: 2 the y-like,
+// 3 the z-like transverse direction; impt: the side (1 minus, 2 plus) of the first split.
+
+// Euler (Roe, entropy fix): every split uses the Roe average of the interface.
+template <class T>
+struct Euler3Phys {
+  static constexpr int NV = 5, NW = 3;
+  Roe3T<T> R;
+  template <int DIR>
+  __device__ __forceinline__ void load(const T*, const PatchDev&, long long, long long, long long, int) {}
+  template <int DIR>
+  __device__ __forceinline__ void rpn(const Step3Params& sp, const T* QL, const T* QR, T (&W)[NW][NV], T* S, T* AM, T* AP) {
+    R = roe3d((T)sp.gamma1, QL, QR);
+    euler3d_rpn_roe((T)sp.gamma, (T)sp.gamma1, sp.efix != 0, DIR, QL, QR, R, W, S, AM, AP);
+  }
+  template <int DIR>
+  __device__ __forceinline__ void rpt(int, int icoor, const T* in, T* m, T* p) const { euler3d_trans(R, DIR, icoor, in, m, p); }
+  template <int DIR>
+  __device__ __forceinline__ void rptt(int, int icoor, int, const T* in, T* m, T* p) const { euler3d_trans(R, DIR, icoor, in, m, p); }
+};
+
+// Advection in a face-centred velocity field (aux 1..3 = u, v, w at the left x-, y- and
+// z-face of each cell): the normal speed is the interface's own face velocity; a split
+// moves a fluctuation with the transverse face velocities of the cell it belongs to, on
+// its lower and upper face, in the pencil row it has already been moved to (impt).
+// The y-like / z-like axes of the sweeps are (j, k), (k, i), (i, j) (step3.f's aux1..3
+// and their third index).
+template <class T>
+struct Swirl3Phys {
+  static constexpr int NV = 1, NW = 1;
+  T un;
+  // [0]: cell e-1, [1]: cell e. vy: y-like face velocity at (dy, dz) = (0,0), (+1,0),
+  // (0,-1), (+1,-1), (0,+1), (+1,+1); vz: z-like one at (0,0), (0,+1), (-1,0), (-1,+1),
+  // (+1,0), (+1,+1)
+  T vy[2][6], vz[2][6];
+  template <int DIR>
+  __device__ __forceinline__ void load(const T* pool, const PatchDev& P, long long base, long long step, long long plane, int e) {
+    const T* a = pool + P.aux;
+    const long long mi = P.mitot, mij = (long long)P.mitot * P.mjtot;
+    const long long sy = DIR == 1 ? mi : DIR == 2 ? mij : 1;
+    const long long sz = DIR == 1 ? mij : DIR == 2 ? 1 : mi;
+    const int cy = DIR == 1 ? 1 : DIR == 2 ? 2 : 0, cz = DIR == 1 ? 2 : DIR == 2 ? 0 : 1;
+    un = a[(long long)(DIR - 1) * plane + base + (long long)e * step];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const long long at = base + (long long)(e - 1 + c) * step;
+      const T* ay = a + cy * plane + at;
+      const T* az = a + cz * plane + at;
+      vy[c][0] = ay[0]; vy[c][1] = ay[sy]; vy[c][2] = ay[-sz]; vy[c][3] = ay[sy - sz]; vy[c][4] = ay[sz]; vy[c][5] = ay[sy + sz];
+      vz[c][0] = az[0]; vz[c][1] = az[sz]; vz[c][2] = az[-sy]; vz[c][3] = az[sz - sy]; vz[c][4] = az[sy]; vz[c][5] = az[sy + sz];
+    }
+  }
+  template <int DIR>
+  __device__ __forceinline__ void rpn(const Step3Params&, const T* QL, const T* QR, T (&W)[NW][NV], T* S, T* AM, T* AP) {
+    W[0][0] = QR[1] - QL[1];
+    S[0] = un;
+    AM[0] = dmin(un, T(0)) * W[0][0];
+    AP[0] = dmax(un, T(0)) * W[0][0];
+  }
+  template <int DIR>
+  __device__ __forceinline__ void rpt(int imp, int icoor, const T* in, T* m, T* p) const {
+    const int c = imp - 1;
+    if (icoor == 2) { m[0] = dmin(vy[c][0], T(0)) * in[0]; p[0] = dmax(vy[c][1], T(0)) * in[0]; }
+    else { m[0] = dmin(vz[c][0], T(0)) * in[0]; p[0] = dmax(vz[c][1], T(0)) * in[0]; }
+  }
+  template <int DIR>
+  __device__ __forceinline__ void rptt(int imp, int icoor, int impt, const T* in, T* m, T* p) const {
+    const int c = imp - 1, o = impt == 1 ? 2 : 4;
+    if (icoor == 2) { m[0] = dmin(vy[c][o], T(0)) * in[0]; p[0] = dmax(vy[c][o + 1], T(0)) * in[0]; }
+    else { m[0] = dmin(vz[c][o], T(0)) * in[0]; p[0] = dmax(vz[c][o + 1], T(0)) * in[0]; }
+  }
+};
+
+template <int DIR, class T, class PH>
 __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
-  __shared__ T sW[15][SW_T];
+  constexpr int NV = PH::NV, NW = PH::NW, ST = stash_values(NV);
+  __shared__ T sW[NW * NV][SW_T];
   const long long* c0 = A.comp0 + (long long)(DIR - 1) * (A.np + 1);
   const long long* s0 = A.sweep0 + (long long)(DIR - 1) * (A.np + 1);
   const long long first = c0[0], last = c0[A.np];
@@ -96,8 +171,8 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   const T dtdz = (T)(DIR == 1 ? A.dt / A.dz : DIR == 2 ? A.dt / A.dx : A.dt / A.dy);
   int e = -1, n1 = 0;
   long long slot = 0;  // stash slot of pencil cell e (meaningful for e in 1..n1+1)
-  Roe3T<T> R;
-  T W[3][5], S[3], AM[5], AP[5];
+  PH ph;
+  T W[NW][NV], S[NW], AM[NV], AP[NV];
   if (valid) {
     const int pi = find_patch(c0, A.np, g);
     const PatchDev& P = A.patches[A.plist[pi]];
@@ -116,26 +191,26 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
     else { base = ((long long)(NG3 - 1) * mj + (b - 1 + NG3)) * mi + (a - 1 + NG3); step = mi * mj; }
     const long long plane = mi * mj * P.mktot;
     const T* q = static_cast<const T*>(A.pool) + P.q[P.cur];
-    T QL[6], QR[6];
+    T QL[NV + 1], QR[NV + 1];
     const long long atl = base + (long long)(e - 1) * step, atr = atl + step;
 #pragma unroll
-    for (int m = 1; m <= 5; ++m) { QL[m] = q[(m - 1) * plane + atl]; QR[m] = q[(m - 1) * plane + atr]; }
+    for (int m = 1; m <= NV; ++m) { QL[m] = q[(m - 1) * plane + atl]; QR[m] = q[(m - 1) * plane + atr]; }
     QL[0] = QR[0] = T(0);
-    R = roe3d((T)sp.gamma1, QL, QR);
-    euler3d_rpn_roe((T)sp.gamma, (T)sp.gamma1, sp.efix != 0, DIR, QL, QR, R, W, S, AM, AP);
+    ph.template load<DIR>(static_cast<const T*>(A.pool), P, base, step, plane, e);
+    ph.template rpn<DIR>(sp, QL, QR, W, S, AM, AP);
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < NW; ++k)
 #pragma unroll
-      for (int m = 0; m < 5; ++m) sW[k * 5 + m][l] = W[k][m];
+      for (int m = 0; m < NV; ++m) sW[k * NV + m][l] = W[k][m];
   }
   __syncthreads();
   // interfaces 1..n1+1 carry fluxes; the tile edges only serve their neighbours
   const bool live = valid && e >= 1 && e <= n1 + 1 && l >= 1 && l <= SW_T - 2;
   const bool owned = live && l <= SW_T - 3;
   T cfl = T(0);
-  T CQ[5];
+  T CQ[NV];
 #pragma unroll
-  for (int m = 0; m < 5; ++m) CQ[m] = T(0);
+  for (int m = 0; m < NV; ++m) CQ[m] = T(0);
   T* st = static_cast<T*>(A.stash) + slot;
   const long long ss = A.stash_stride;
   const T c6 = (T)(1.0 / 6.0);
@@ -143,68 +218,68 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   if (live) {
     // Courant number of interface e (flux3.f:237-246)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) cfl = dmax(cfl, dmax(dtdx * S[k], -dtdx * S[k]));
+    for (int k = 0; k < NW; ++k) cfl = dmax(cfl, dmax(dtdx * S[k], -dtdx * S[k]));
     if (sp.order != 1) {
       // limiter.f: r from the unlimited neighbour waves, upwind side by the speed's sign
       const T dtdxave = T(0.5) * (dtdx + dtdx);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < NW; ++k) {
         if (sp.mthlim[k] == 0) continue;
         T dl = T(0), dr = T(0), wn = T(0);
 #pragma unroll
-        for (int m = 0; m < 5; ++m) dl = dl + sW[k * 5 + m][l - 1] * W[k][m];
+        for (int m = 0; m < NV; ++m) dl = dl + sW[k * NV + m][l - 1] * W[k][m];
 #pragma unroll
-        for (int m = 0; m < 5; ++m) dr = dr + W[k][m] * sW[k * 5 + m][l + 1];
+        for (int m = 0; m < NV; ++m) dr = dr + W[k][m] * sW[k * NV + m][l + 1];
 #pragma unroll
-        for (int m = 0; m < 5; ++m) wn = wn + W[k][m] * W[k][m];
+        for (int m = 0; m < NV; ++m) wn = wn + W[k][m] * W[k][m];
         if (wn != T(0)) {
           const T r = (S[k] > T(0)) ? dl / wn : dr / wn;
           const T phi = philim3(sp.mthlim[k], r);
 #pragma unroll
-          for (int m = 0; m < 5; ++m) W[k][m] = phi * W[k][m];
+          for (int m = 0; m < NV; ++m) W[k][m] = phi * W[k][m];
         }
       }
 #pragma unroll
-      for (int m = 0; m < 5; ++m) {
+      for (int m = 0; m < NV; ++m) {
         T x = T(0);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) x = x + T(0.5) * fabs(S[k]) * (T(1) - fabs(S[k]) * dtdxave) * W[k][m];
+        for (int k = 0; k < NW; ++k) x = x + T(0.5) * fabs(S[k]) * (T(1) - fabs(S[k]) * dtdxave) * W[k][m];
         CQ[m] = x;
       }
     }
     if (owned) {
 #pragma unroll
-      for (int m = 0; m < 5; ++m) {
+      for (int m = 0; m < NV; ++m) {
         T fm = T(0) + AM[m], fp = T(0) - AP[m];
         if (sp.order != 1) { fm = fm + CQ[m]; fp = fp + CQ[m]; }
         st[(long long)m * ss] = fm;
-        st[(long long)(5 + m) * ss] = fp;
+        st[(long long)(NV + m) * ss] = fp;
       }
       if (e <= n1) {
         if (m3 <= 0) {
-          for (int x = 10; x < STASH3; ++x) st[(long long)x * ss] = T(0);
+          for (int x = 2 * NV; x < ST; ++x) st[(long long)x * ss] = T(0);
         } else {
           // apdq side of interface e: the terms of cell e (flux3.f:429-505, 552-628 with i = e)
-          T bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
-          euler3d_trans(R, DIR, 2, AP, bm, bp);
-          euler3d_trans(R, DIR, 3, AP, cm, cp);
-          if (m3 == 2) { euler3d_trans(R, DIR, 2, CQ, bmq, bpq); euler3d_trans(R, DIR, 3, CQ, cmq, cpq); }
+          T bm[NV], bp[NV], cm[NV], cp[NV], bmq[NV], bpq[NV], cmq[NV], cpq[NV];
+          ph.template rpt<DIR>(2, 2, AP, bm, bp);
+          ph.template rpt<DIR>(2, 3, AP, cm, cp);
+          if (m3 == 2) { ph.template rpt<DIR>(2, 2, CQ, bmq, bpq); ph.template rpt<DIR>(2, 3, CQ, cmq, cpq); }
           else {
 #pragma unroll
-            for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
+            for (int m = 0; m < NV; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
           }
           // gadd: (side, offset d) at element 10 + ((side-1)*3 + d+1)*5 + m
           {
-            T P1[5], P2[5], M1[5], M2[5];
+            T P1[NV], P2[NV], M1[NV], M2[NV];
             if (m4 > 0) {
-              T t[5];
-              dt_input(m4, T(-3), cp, cpq, t);
-              euler3d_trans(R, DIR, 2, t, P1, P2);
-              dt_input(m4, T(-3), cm, cmq, t);
-              euler3d_trans(R, DIR, 2, t, M1, M2);
+              T t[NV];
+              dt_input<NV>(m4, T(-3), cp, cpq, t);
+              ph.template rptt<DIR>(2, 2, 2, t, P1, P2);
+              dt_input<NV>(m4, T(-3), cm, cmq, t);
+              ph.template rptt<DIR>(2, 2, 1, t, M1, M2);
             }
 #pragma unroll
-            for (int m = 0; m < 5; ++m) {
+            for (int m = 0; m < NV; ++m) {
               T g01 = T(0) - T(0.5) * dtdx * bm[m], g11 = T(0) - T(0.5) * dtdx * bp[m];
               T g00 = T(0), g02 = T(0), g10 = T(0), g12 = T(0);
               if (m4 > 0) {
@@ -216,26 +291,26 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
                 g00 = g00 + c6 * dtdx * dtdz * M1[m];
               }
               if (m3 == 2) { g11 = g11 + dtdx * bpq[m]; g01 = g01 + dtdx * bmq[m]; }
-              st[(long long)(10 + 0 * 5 + m) * ss] = g00;
-              st[(long long)(10 + 1 * 5 + m) * ss] = g01;
-              st[(long long)(10 + 2 * 5 + m) * ss] = g02;
-              st[(long long)(10 + 3 * 5 + m) * ss] = g10;
-              st[(long long)(10 + 4 * 5 + m) * ss] = g11;
-              st[(long long)(10 + 5 * 5 + m) * ss] = g12;
+              st[(long long)(2 * NV + 0 * NV + m) * ss] = g00;
+              st[(long long)(2 * NV + 1 * NV + m) * ss] = g01;
+              st[(long long)(2 * NV + 2 * NV + m) * ss] = g02;
+              st[(long long)(2 * NV + 3 * NV + m) * ss] = g10;
+              st[(long long)(2 * NV + 4 * NV + m) * ss] = g11;
+              st[(long long)(2 * NV + 5 * NV + m) * ss] = g12;
             }
           }
           // hadd at element 40 + ((side-1)*3 + d+1)*5 + m
           {
-            T X1[5], X2[5], Y1[5], Y2[5];
+            T X1[NV], X2[NV], Y1[NV], Y2[NV];
             if (m4 > 0) {
-              T t[5];
-              dt_input(m4, T(-3), bp, bpq, t);
-              euler3d_trans(R, DIR, 3, t, X1, X2);
-              dt_input(m4, T(-3), bm, bmq, t);
-              euler3d_trans(R, DIR, 3, t, Y1, Y2);
+              T t[NV];
+              dt_input<NV>(m4, T(-3), bp, bpq, t);
+              ph.template rptt<DIR>(2, 3, 2, t, X1, X2);
+              dt_input<NV>(m4, T(-3), bm, bmq, t);
+              ph.template rptt<DIR>(2, 3, 1, t, Y1, Y2);
             }
 #pragma unroll
-            for (int m = 0; m < 5; ++m) {
+            for (int m = 0; m < NV; ++m) {
               T h01 = T(0) - T(0.5) * dtdx * cm[m], h11 = T(0) - T(0.5) * dtdx * cp[m];
               T h00 = T(0), h02 = T(0), h10 = T(0), h12 = T(0);
               if (m4 > 0) {
@@ -247,12 +322,12 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
                 h00 = h00 + c6 * dtdx * dtdy * Y1[m];
               }
               if (m3 == 2) { h11 = h11 + dtdx * cpq[m]; h01 = h01 + dtdx * cmq[m]; }
-              st[(long long)(40 + 0 * 5 + m) * ss] = h00;
-              st[(long long)(40 + 1 * 5 + m) * ss] = h01;
-              st[(long long)(40 + 2 * 5 + m) * ss] = h02;
-              st[(long long)(40 + 3 * 5 + m) * ss] = h10;
-              st[(long long)(40 + 4 * 5 + m) * ss] = h11;
-              st[(long long)(40 + 5 * 5 + m) * ss] = h12;
+              st[(long long)(8 * NV + 0 * NV + m) * ss] = h00;
+              st[(long long)(8 * NV + 1 * NV + m) * ss] = h01;
+              st[(long long)(8 * NV + 2 * NV + m) * ss] = h02;
+              st[(long long)(8 * NV + 3 * NV + m) * ss] = h10;
+              st[(long long)(8 * NV + 4 * NV + m) * ss] = h11;
+              st[(long long)(8 * NV + 5 * NV + m) * ss] = h12;
             }
           }
         }
@@ -263,78 +338,78 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   // amdq side of interface e: the terms of cell e-1, owned by thread l-1 of this tile
   if (live && m3 > 0 && e >= 2 && l >= 2) {
     T* sc = st - 1;
-    T bm[5], bp[5], cm[5], cp[5], bmq[5], bpq[5], cmq[5], cpq[5];
-    euler3d_trans(R, DIR, 2, AM, bm, bp);
-    euler3d_trans(R, DIR, 3, AM, cm, cp);
-    if (m3 == 2) { euler3d_trans(R, DIR, 2, CQ, bmq, bpq); euler3d_trans(R, DIR, 3, CQ, cmq, cpq); }
+    T bm[NV], bp[NV], cm[NV], cp[NV], bmq[NV], bpq[NV], cmq[NV], cpq[NV];
+    ph.template rpt<DIR>(1, 2, AM, bm, bp);
+    ph.template rpt<DIR>(1, 3, AM, cm, cp);
+    if (m3 == 2) { ph.template rpt<DIR>(1, 2, CQ, bmq, bpq); ph.template rpt<DIR>(1, 3, CQ, cmq, cpq); }
     else {
 #pragma unroll
-      for (int m = 0; m < 5; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
+      for (int m = 0; m < NV; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
     }
     {
-      T P1[5], P2[5], M1[5], M2[5];
+      T P1[NV], P2[NV], M1[NV], M2[NV];
       if (m4 > 0) {
-        T t[5];
-        dt_input(m4, T(3), cp, cpq, t);
-        euler3d_trans(R, DIR, 2, t, P1, P2);
-        dt_input(m4, T(3), cm, cmq, t);
-        euler3d_trans(R, DIR, 2, t, M1, M2);
+        T t[NV];
+        dt_input<NV>(m4, T(3), cp, cpq, t);
+        ph.template rptt<DIR>(1, 2, 2, t, P1, P2);
+        dt_input<NV>(m4, T(3), cm, cmq, t);
+        ph.template rptt<DIR>(1, 2, 1, t, M1, M2);
       }
 #pragma unroll
-      for (int m = 0; m < 5; ++m) {
-        T g01 = sc[(long long)(10 + 1 * 5 + m) * ss], g11 = sc[(long long)(10 + 4 * 5 + m) * ss];
+      for (int m = 0; m < NV; ++m) {
+        T g01 = sc[(long long)(2 * NV + 1 * NV + m) * ss], g11 = sc[(long long)(2 * NV + 4 * NV + m) * ss];
         g01 = g01 - T(0.5) * dtdx * bm[m];
         g11 = g11 - T(0.5) * dtdx * bp[m];
         if (m4 > 0) {
-          T g00 = sc[(long long)(10 + 0 * 5 + m) * ss], g02 = sc[(long long)(10 + 2 * 5 + m) * ss];
-          T g10 = sc[(long long)(10 + 3 * 5 + m) * ss], g12 = sc[(long long)(10 + 5 * 5 + m) * ss];
+          T g00 = sc[(long long)(2 * NV + 0 * NV + m) * ss], g02 = sc[(long long)(2 * NV + 2 * NV + m) * ss];
+          T g10 = sc[(long long)(2 * NV + 3 * NV + m) * ss], g12 = sc[(long long)(2 * NV + 5 * NV + m) * ss];
           g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
           g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
           g12 = g12 - c6 * dtdx * dtdz * P2[m];
           g02 = g02 - c6 * dtdx * dtdz * P1[m];
           g10 = g10 + c6 * dtdx * dtdz * M2[m];
           g00 = g00 + c6 * dtdx * dtdz * M1[m];
-          sc[(long long)(10 + 0 * 5 + m) * ss] = g00;
-          sc[(long long)(10 + 2 * 5 + m) * ss] = g02;
-          sc[(long long)(10 + 3 * 5 + m) * ss] = g10;
-          sc[(long long)(10 + 5 * 5 + m) * ss] = g12;
+          sc[(long long)(2 * NV + 0 * NV + m) * ss] = g00;
+          sc[(long long)(2 * NV + 2 * NV + m) * ss] = g02;
+          sc[(long long)(2 * NV + 3 * NV + m) * ss] = g10;
+          sc[(long long)(2 * NV + 5 * NV + m) * ss] = g12;
         }
         if (m3 == 2) { g11 = g11 - dtdx * bpq[m]; g01 = g01 - dtdx * bmq[m]; }
-        sc[(long long)(10 + 1 * 5 + m) * ss] = g01;
-        sc[(long long)(10 + 4 * 5 + m) * ss] = g11;
+        sc[(long long)(2 * NV + 1 * NV + m) * ss] = g01;
+        sc[(long long)(2 * NV + 4 * NV + m) * ss] = g11;
       }
     }
     {
-      T X1[5], X2[5], Y1[5], Y2[5];
+      T X1[NV], X2[NV], Y1[NV], Y2[NV];
       if (m4 > 0) {
-        T t[5];
-        dt_input(m4, T(3), bp, bpq, t);
-        euler3d_trans(R, DIR, 3, t, X1, X2);
-        dt_input(m4, T(3), bm, bmq, t);
-        euler3d_trans(R, DIR, 3, t, Y1, Y2);
+        T t[NV];
+        dt_input<NV>(m4, T(3), bp, bpq, t);
+        ph.template rptt<DIR>(1, 3, 2, t, X1, X2);
+        dt_input<NV>(m4, T(3), bm, bmq, t);
+        ph.template rptt<DIR>(1, 3, 1, t, Y1, Y2);
       }
 #pragma unroll
-      for (int m = 0; m < 5; ++m) {
-        T h01 = sc[(long long)(40 + 1 * 5 + m) * ss], h11 = sc[(long long)(40 + 4 * 5 + m) * ss];
+      for (int m = 0; m < NV; ++m) {
+        T h01 = sc[(long long)(8 * NV + 1 * NV + m) * ss], h11 = sc[(long long)(8 * NV + 4 * NV + m) * ss];
         h01 = h01 - T(0.5) * dtdx * cm[m];
         h11 = h11 - T(0.5) * dtdx * cp[m];
         if (m4 > 0) {
-          T h00 = sc[(long long)(40 + 0 * 5 + m) * ss], h02 = sc[(long long)(40 + 2 * 5 + m) * ss];
-          T h10 = sc[(long long)(40 + 3 * 5 + m) * ss], h12 = sc[(long long)(40 + 5 * 5 + m) * ss];
+          T h00 = sc[(long long)(8 * NV + 0 * NV + m) * ss], h02 = sc[(long long)(8 * NV + 2 * NV + m) * ss];
+          T h10 = sc[(long long)(8 * NV + 3 * NV + m) * ss], h12 = sc[(long long)(8 * NV + 5 * NV + m) * ss];
           h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
           h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
           h12 = h12 - c6 * dtdx * dtdy * X2[m];
           h02 = h02 - c6 * dtdx * dtdy * X1[m];
           h10 = h10 + c6 * dtdx * dtdy * Y2[m];
           h00 = h00 + c6 * dtdx * dtdy * Y1[m];
-          sc[(long long)(40 + 0 * 5 + m) * ss] = h00;
-          sc[(long long)(40 + 2 * 5 + m) * ss] = h02;
-          sc[(long long)(40 + 3 * 5 + m) * ss] = h10;
-          sc[(long long)(40 + 5 * 5 + m) * ss] = h12;
+          sc[(long long)(8 * NV + 0 * NV + m) * ss] = h00;
+          sc[(long long)(8 * NV + 2 * NV + m) * ss] = h02;
+          sc[(long long)(8 * NV + 3 * NV + m) * ss] = h10;
+          sc[(long long)(8 * NV + 5 * NV + m) * ss] = h12;
         }
         if (m3 == 2) { h11 = h11 - dtdx * cpq[m]; h01 = h01 - dtdx * cmq[m]; }
-        sc[(long long)(40 + 1 * 5 + m) * ss] = h01;
-        sc[(long long)(40 + 4 * 5 + m) * ss] = h11;
+        sc[(long long)(8 * NV + 1 * NV + m) * ss] = h01;
+        sc[(long long)(8 * NV + 4 * NV + m) * ss] = h11;
       }
     }
   }
@@ -343,11 +418,14 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   if ((threadIdx.x & 31) == 0 && cfl > T(0)) atomic_max_nonneg(A.cflmax, (double)cfl);
 }
 
-// stash element of gadd (kind 10) / hadd (kind 40) for side s (1,2), offset d (-1..1), component m (0..4)
-__device__ __forceinline__ int sidx(int kind, int s, int d, int m) { return kind + ((s - 1) * 3 + (d + 1)) * 5 + m; }
+// stash element of gadd / hadd for side s (1,2), offset d (-1..1), component m (0..NV-1)
+template <int NV>
+__device__ __forceinline__ int gidx(int s, int d, int m) { return 2 * NV + ((s - 1) * 3 + (d + 1)) * NV + m; }
+template <int NV>
+__device__ __forceinline__ int hidx(int s, int d, int m) { return 8 * NV + ((s - 1) * 3 + (d + 1)) * NV + m; }
 
 // ------------------------------------------------------------------- faces
-template <class T>
+template <class T, int NV>
 __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
   // face cells [face0[0], face0[np]): the level's, or one patch's through a one-patch view
   const long long first = A.face0[0], total = A.face0[A.np];
@@ -368,19 +446,19 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
     T* F = static_cast<T*>(A.flux) + t;
     const long long fs = A.flux_stride;
     if (j <= my && k <= mz) {  // x-face i
-      T fm[5], fp[5];
+      T fm[NV], fp[NV];
       const long long sx = xs(j, k, i);
 #pragma unroll
-      for (int m = 0; m < 5; ++m) { fm[m] = T(0) + S[m * ss + sx]; fp[m] = T(0) + S[(5 + m) * ss + sx]; }
+      for (int m = 0; m < NV; ++m) { fm[m] = T(0) + S[m * ss + sx]; fp[m] = T(0) + S[(NV + m) * ss + sx]; }
       // y-sweeps: k' = k-1, k, k+1 (d = +1, 0, -1); pencil i-1 (side 2) then i (side 1)
 #pragma unroll
       for (int d = 1; d >= -1; --d) {
         const long long s2 = ys(i - 1, k - d, j), s1 = ys(i, k - d, j);
 #pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          const T t2 = S[sidx(40, 2, d, m) * ss + s2];
+        for (int m = 0; m < NV; ++m) {
+          const T t2 = S[hidx<NV>(2, d, m) * ss + s2];
           fm[m] = fm[m] + t2; fp[m] = fp[m] + t2;
-          const T t1 = S[sidx(40, 1, d, m) * ss + s1];
+          const T t1 = S[hidx<NV>(1, d, m) * ss + s1];
           fm[m] = fm[m] + t1; fp[m] = fp[m] + t1;
         }
       }
@@ -389,33 +467,33 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
       for (int d = 1; d >= -1; --d) {
         const long long s2 = zs(i - 1, j - d, k), s1 = zs(i, j - d, k);
 #pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          const T t2 = S[sidx(10, 2, d, m) * ss + s2];
+        for (int m = 0; m < NV; ++m) {
+          const T t2 = S[gidx<NV>(2, d, m) * ss + s2];
           fm[m] = fm[m] + t2; fp[m] = fp[m] + t2;
-          const T t1 = S[sidx(10, 1, d, m) * ss + s1];
+          const T t1 = S[gidx<NV>(1, d, m) * ss + s1];
           fm[m] = fm[m] + t1; fp[m] = fp[m] + t1;
         }
       }
 #pragma unroll
-      for (int m = 0; m < 5; ++m) { F[(0 * 5 + m) * fs] = fm[m]; F[(1 * 5 + m) * fs] = fp[m]; }
+      for (int m = 0; m < NV; ++m) { F[(0 * NV + m) * fs] = fm[m]; F[(1 * NV + m) * fs] = fp[m]; }
     }
     if (i <= mx && k <= mz) {  // y-face j
-      T gm[5], gp[5];
+      T gm[NV], gp[NV];
 #pragma unroll
-      for (int m = 0; m < 5; ++m) gm[m] = T(0);
+      for (int m = 0; m < NV; ++m) gm[m] = T(0);
       // x-sweeps: k' = k-1, k, k+1 (d = +1, 0, -1); pencil j-1 (side 2) then j (side 1)
 #pragma unroll
       for (int d = 1; d >= -1; --d) {
         const long long s2 = xs(j - 1, k - d, i), s1 = xs(j, k - d, i);
 #pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          gm[m] = gm[m] + S[sidx(10, 2, d, m) * ss + s2];
-          gm[m] = gm[m] + S[sidx(10, 1, d, m) * ss + s1];
+        for (int m = 0; m < NV; ++m) {
+          gm[m] = gm[m] + S[gidx<NV>(2, d, m) * ss + s2];
+          gm[m] = gm[m] + S[gidx<NV>(1, d, m) * ss + s1];
         }
       }
       const long long sy = ys(i, k, j);
 #pragma unroll
-      for (int m = 0; m < 5; ++m) { gp[m] = gm[m] + S[(5 + m) * ss + sy]; gm[m] = gm[m] + S[m * ss + sy]; }
+      for (int m = 0; m < NV; ++m) { gp[m] = gm[m] + S[(NV + m) * ss + sy]; gm[m] = gm[m] + S[m * ss + sy]; }
       // z-sweeps: j' = j-1 (side 2) for i' = i-1, i, i+1 (d = +1, 0, -1), then j' = j (side 1)
 #pragma unroll
       for (int side = 2; side >= 1; --side) {
@@ -424,19 +502,19 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
         for (int d = 1; d >= -1; --d) {
           const long long sz = zs(i - d, jp, k);
 #pragma unroll
-          for (int m = 0; m < 5; ++m) {
-            const T tv = S[sidx(40, side, d, m) * ss + sz];
+          for (int m = 0; m < NV; ++m) {
+            const T tv = S[hidx<NV>(side, d, m) * ss + sz];
             gm[m] = gm[m] + tv; gp[m] = gp[m] + tv;
           }
         }
       }
 #pragma unroll
-      for (int m = 0; m < 5; ++m) { F[(2 * 5 + m) * fs] = gm[m]; F[(3 * 5 + m) * fs] = gp[m]; }
+      for (int m = 0; m < NV; ++m) { F[(2 * NV + m) * fs] = gm[m]; F[(3 * NV + m) * fs] = gp[m]; }
     }
     if (i <= mx && j <= my) {  // z-face k
-      T hm[5], hp[5];
+      T hm[NV], hp[NV];
 #pragma unroll
-      for (int m = 0; m < 5; ++m) hm[m] = T(0);
+      for (int m = 0; m < NV; ++m) hm[m] = T(0);
       // x-sweeps: k' = k-1 (side 2) for j' = j-1, j, j+1 (d = +1, 0, -1), then k' = k (side 1)
 #pragma unroll
       for (int side = 2; side >= 1; --side) {
@@ -445,7 +523,7 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
         for (int d = 1; d >= -1; --d) {
           const long long sx = xs(j - d, kp, i);
 #pragma unroll
-          for (int m = 0; m < 5; ++m) hm[m] = hm[m] + S[sidx(40, side, d, m) * ss + sx];
+          for (int m = 0; m < NV; ++m) hm[m] = hm[m] + S[hidx<NV>(side, d, m) * ss + sx];
         }
       }
       // y-sweeps: k' = k-1 (side 2) for i' = i-1, i, i+1, then k' = k (side 1)
@@ -456,20 +534,20 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
         for (int d = 1; d >= -1; --d) {
           const long long sy = ys(i - d, kp, j);
 #pragma unroll
-          for (int m = 0; m < 5; ++m) hm[m] = hm[m] + S[sidx(10, side, d, m) * ss + sy];
+          for (int m = 0; m < NV; ++m) hm[m] = hm[m] + S[gidx<NV>(side, d, m) * ss + sy];
         }
       }
       const long long sz = zs(i, j, k);
 #pragma unroll
-      for (int m = 0; m < 5; ++m) { hp[m] = hm[m] + S[(5 + m) * ss + sz]; hm[m] = hm[m] + S[m * ss + sz]; }
+      for (int m = 0; m < NV; ++m) { hp[m] = hm[m] + S[(NV + m) * ss + sz]; hm[m] = hm[m] + S[m * ss + sz]; }
 #pragma unroll
-      for (int m = 0; m < 5; ++m) { F[(4 * 5 + m) * fs] = hm[m]; F[(5 * 5 + m) * fs] = hp[m]; }
+      for (int m = 0; m < NV; ++m) { F[(4 * NV + m) * fs] = hm[m]; F[(5 * NV + m) * fs] = hp[m]; }
     }
   }
 }
 
 // ------------------------------------------------------------------- update
-template <class T>
+template <class T, int NV>
 __global__ void __launch_bounds__(256) update3_kernel(Step3Args A) {
   const long long first = A.cell0[0], total = A.cell0[A.np];
   const long long fs = A.flux_stride;
@@ -488,11 +566,11 @@ __global__ void __launch_bounds__(256) update3_kernel(Step3Args A) {
     T* qn = const_cast<T*>(static_cast<const T*>(A.pool)) + P.q[1 - P.cur];
     const long long c = fidx(i, j, k), cx = fidx(i + 1, j, k), cy = fidx(i, j + 1, k), cz = fidx(i, j, k + 1);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
+    for (int m = 0; m < NV; ++m) {
       const T* F = static_cast<const T*>(A.flux) + (long long)m * fs;
-      const T fmv = F[0 * 5 * fs + cx], fpv = F[1 * 5 * fs + c];
-      const T gmv = F[2 * 5 * fs + cy], gpv = F[3 * 5 * fs + c];
-      const T hmv = F[4 * 5 * fs + cz], hpv = F[5 * 5 * fs + c];
+      const T fmv = F[0 * NV * fs + cx], fpv = F[1 * NV * fs + c];
+      const T gmv = F[2 * NV * fs + cy], gpv = F[3 * NV * fs + c];
+      const T hmv = F[4 * NV * fs + cz], hpv = F[5 * NV * fs + c];
       qn[m * plane + at] = q[m * plane + at] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv) - dtdz * (hmv - hpv);
     }
   }
@@ -517,7 +595,7 @@ __global__ void fsv3_kernel(const T* flux, long long fs, const long long* face0,
     case 5: comp = 5; c = fidx(E.i, E.j, E.k); h1 = hx; h2 = hy; break;
     default: comp = 4; c = fidx(E.i, E.j, E.k + 1); h1 = hx; h2 = hy; break;
   }
-  for (int m = 0; m < nvar; ++m) regs[E.dst + m] = -(double)flux[((long long)comp * 5 + m) * fs + c] * dtc * h1 * h2;
+  for (int m = 0; m < nvar; ++m) regs[E.dst + m] = -(double)flux[((long long)comp * nvar + m) * fs + c] * dtc * h1 * h2;
 }
 
 // fluxad.f:4-155: one coarse face (register) of a fine patch per thread
@@ -542,7 +620,7 @@ __global__ void fad3_kernel(const T* flux, long long fs, const long long* face0,
   }
   for (int m = 0; m < nvar; ++m) {
     double acc = sv[m];
-    const T* F = flux + ((long long)comp * 5 + m) * fs;
+    const T* F = flux + ((long long)comp * nvar + m) * fs;
     for (int ob = 1; ob <= E.nb; ++ob)
       for (int oa = 1; oa <= E.na; ++oa) {
         long long c;
@@ -616,6 +694,72 @@ __global__ void qad3_kernel(T* pool, double* regs, const PatchDev* patches, cons
   }
   for (int m = 0; m < 5; ++m) sv[m] = acc[m];
   (void)nvar; (void)mz;
+}
+
+// qad.f:4-534 for the swirl: the coarse-fine Riemann problem moves the jump with the
+// normal face velocity of the fine patch (aux 1..3 are left-face velocities). On the
+// low sides that is the first interior fine cell's own face; on the high sides the ghost
+// cell beyond, at the cross-row index qad.f reads there (the coarse slab's first fine row
+// plus the position l along the coarse face, qad.f:186-193, 245-252, 506-513).
+template <class T>
+__global__ void qad3_swirl_kernel(T* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs,
+                                  double hx, double hy, double hz, double delt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= njobs) return;
+  const Qad3Job J = jobs[t];
+  const PatchDev& P = patches[J.patch];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+  const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
+  const T* q = pool + P.q[P.cur];
+  const T* aux = pool + P.aux;
+  auto at = [&](int i, int j, int k) { return ((long long)(k - 1 + NG3) * P.mjtot + (j - 1 + NG3)) * P.mitot + (i - 1 + NG3); };
+  double* sv = regs + P.ffl + J.reg0;
+  const T C = (T)regs[P.ffl + P.lenbc + J.reg0];
+  double sgn, h1, h2;
+  switch (J.side) {
+    case 1: case 3: h1 = hy; h2 = hz; break;
+    case 2: case 4: h1 = hx; h2 = hz; break;
+    default: h1 = hx; h2 = hy; break;
+  }
+  sgn = (J.side == 1 || J.side == 4 || J.side == 5) ? 1.0 : -1.0;
+  double acc = sv[0];
+  for (int ks = 1; ks <= J.ratio_b; ++ks) {
+    for (int l = 1; l <= J.ratio_a; ++l) {
+      const int r = J.row0 + l;
+      const int s = J.slab * J.ratio_b + ks;
+      const int x = J.slab * J.ratio_b + l;  // qad.f's cross-row index of the high sides
+      int i, j, k, ai, aj, ak, comp;
+      switch (J.side) {
+        case 1: i = 0; j = r; k = s; comp = 0; ai = 1; aj = r; ak = s; break;
+        case 2: i = r; j = my + 1; k = s; comp = 1; ai = r; aj = my + 1; ak = x; break;
+        case 3: i = mx + 1; j = r; k = s; comp = 0; ai = mx + 1; aj = r; ak = x; break;
+        case 4: i = r; j = 0; k = s; comp = 1; ai = r; aj = 1; ak = s; break;
+        case 5: i = r; j = s; k = 0; comp = 2; ai = r; aj = s; ak = 1; break;
+        default: i = r; j = s; k = mz + 1; comp = 2; ai = r; aj = x; ak = mz + 1; break;
+      }
+      const T fv = q[at(i, j, k)];
+      const T u = aux[comp * plane + at(ai, aj, ak)];
+      const T w = (sgn > 0.0) ? fv - C : C - fv;   // right state minus left state
+      const double am = dmin(u, T(0)) * w, ap = dmax(u, T(0)) * w;
+      if (sgn > 0.0) acc = acc + am * h1 * h2 * delt + ap * h1 * h2 * delt;
+      else acc = acc - am * h1 * h2 * delt - ap * h1 * h2 * delt;
+    }
+  }
+  sv[0] = acc;
+}
+
+// b4step3 of the time-modulated swirl: aux = aux0 * c over the enlarged patches of plist
+// (aux0, the setaux values, sits right after aux in the pool)
+template <class T>
+__global__ void b4step3_kernel(T* pool, const PatchDev* patches, const int* plist, int np, int naux, double c) {
+  const int pi = blockIdx.y;
+  if (pi >= np) return;
+  const PatchDev& P = patches[plist[pi]];
+  const long long n = (long long)naux * P.mitot * P.mjtot * P.mktot;
+  T* a = pool + P.aux;
+  const T* a0 = a + n;
+  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (long long)gridDim.x * blockDim.x)
+    a[x] = (T)((double)a0[x] * c);
 }
 
 // ------------------------------------------------------------------- ghost fill
@@ -924,20 +1068,25 @@ int grid_for(long long n, int block) {
 
 }  // namespace
 
-template <class T>
+template <class T, class PH>
 static void launch_step3_t(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s) {
   auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
-  if (items[0] > 0) sweep3_kernel<1, T><<<tiles(items[0]), SW_T, 0, s>>>(a);
-  if (items[1] > 0) sweep3_kernel<2, T><<<tiles(items[1]), SW_T, 0, s>>>(a);
-  if (items[2] > 0) sweep3_kernel<3, T><<<tiles(items[2]), SW_T, 0, s>>>(a);
+  if (items[0] > 0) sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, 0, s>>>(a);
+  if (items[1] > 0) sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, 0, s>>>(a);
+  if (items[2] > 0) sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, 0, s>>>(a);
   AMR_CUDA(cudaGetLastError());
-  if (faces > 0) face3_kernel<T><<<grid_for(faces, 128), 128, 0, s>>>(a);
-  if (cells > 0) update3_kernel<T><<<grid_for(cells, 256), 256, 0, s>>>(a);
+  if (faces > 0) face3_kernel<T, PH::NV><<<grid_for(faces, 128), 128, 0, s>>>(a);
+  if (cells > 0) update3_kernel<T, PH::NV><<<grid_for(cells, 256), 256, 0, s>>>(a);
   AMR_CUDA(cudaGetLastError());
 }
 void launch_step3(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s, bool f32) {
-  if (f32) launch_step3_t<float>(a, items, faces, cells, s);
-  else launch_step3_t<double>(a, items, faces, cells, s);
+  if (a.sp.solver == SOLVER3_SWIRL) {
+    if (f32) launch_step3_t<float, Swirl3Phys<float>>(a, items, faces, cells, s);
+    else launch_step3_t<double, Swirl3Phys<double>>(a, items, faces, cells, s);
+  } else {
+    if (f32) launch_step3_t<float, Euler3Phys<float>>(a, items, faces, cells, s);
+    else launch_step3_t<double, Euler3Phys<double>>(a, items, faces, cells, s);
+  }
 }
 
 void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,
@@ -964,8 +1113,50 @@ void launch_fad3(const void* flux, long long fs, const long long* face0, const P
 void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp, int nvar,
                  double hx, double hy, double hz, double delt, cudaStream_t s, bool f32) {
   if (njobs <= 0) return;
+  if (sp.solver == SOLVER3_SWIRL) {
+    if (f32) qad3_swirl_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, hx, hy, hz, delt);
+    else qad3_swirl_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, hx, hy, hz, delt);
+    AMR_CUDA(cudaGetLastError());
+    return;
+  }
   if (f32) qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
   else qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
+  AMR_CUDA(cudaGetLastError());
+}
+// valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
+template <class T>
+__global__ void zero_tiny3_kernel(T* pool, const PatchDev* patches, const int* plist, int np, int nvar) {
+  const int pi = blockIdx.y;
+  if (pi >= np) return;
+  const PatchDev& P = patches[plist[pi]];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+  const long long plane = (long long)P.mitot * P.mjtot * P.mktot, n = (long long)mx * my * mz;
+  T* q = pool + P.q[P.cur];
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n * nvar; t += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(t / n);
+    const long long c = t - (long long)m * n;
+    const int i = (int)(c % mx), j = (int)((c / mx) % my), k = (int)(c / ((long long)mx * my));
+    T& v = q[m * plane + ((long long)(k + NG3) * P.mjtot + (j + NG3)) * P.mitot + (i + NG3)];
+    if (fabs((double)v) < 1e-90) v = T(0);
+  }
+}
+void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32) {
+  for (int base = 0; base < np; base += 65535) {
+    const int cnt = std::min(65535, np - base);
+    if (f32) zero_tiny3_kernel<<<dim3(8, cnt), 256, 0, s>>>(static_cast<float*>(pool), patches, plist + base, cnt, nvar);
+    else zero_tiny3_kernel<<<dim3(8, cnt), 256, 0, s>>>(static_cast<double*>(pool), patches, plist + base, cnt, nvar);
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_b4step3(void* pool, const PatchDev* patches, const int* plist, int np, int naux, long long max_cells, double c,
+                    cudaStream_t s, bool f32) {
+  if (np <= 0) return;
+  const int bx = (int)std::max<long long>(1, std::min<long long>((naux * max_cells + 255) / 256, 1024));
+  for (int base = 0; base < np; base += 65535) {
+    const int cnt = std::min(65535, np - base);
+    if (f32) b4step3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<float*>(pool), patches, plist + base, cnt, naux, c);
+    else b4step3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<double*>(pool), patches, plist + base, cnt, naux, c);
+  }
   AMR_CUDA(cudaGetLastError());
 }
 void launch_fill3(const Fill3Args& a, cudaStream_t s, bool f32) {

@@ -5,11 +5,16 @@
 
 namespace amrb {
 
-// Number of per-cell values a sweep leaves for the face kernel: faddm(5),
-// faddp(5), gadd(2 sides x 3 offsets x 5), hadd(2 x 3 x 5).
-constexpr int STASH3 = 70;
+// Number of per-cell values a sweep leaves for the face kernel for nv equations:
+// faddm(nv), faddp(nv), gadd(2 sides x 3 offsets x nv), hadd(2 x 3 x nv).
+__host__ __device__ constexpr int stash_values(int nv) { return 14 * nv; }
+constexpr int STASH3 = stash_values(5);
+
+// Riemann plugins of the 3D device path (the problem's rpn3/rpt3/rptt3)
+enum Solver3 { SOLVER3_EULER = 0, SOLVER3_SWIRL = 1 };
 
 struct Step3Params {
+  int solver;  // Solver3
   double gamma, gamma1;
   int efix;
   int mthlim[3];
@@ -30,8 +35,8 @@ struct Step3Args {
   const long long* face0;    // [np+1]: first face cell of each patch ((mx+1)(my+1)(mz+1) each)
   const long long* cell0;    // [np+1]: first interior cell of each patch (mx*my*mz each)
   long long stash_stride;    // slots of one direction region x 3 (SoA stride)
-  void* stash;               // [STASH3][stash_stride]
-  void* flux;                // [6 comps][5][face cells]
+  void* stash;               // [stash_values(meqn)][stash_stride]
+  void* flux;                // [6 comps][meqn][face cells]
   long long flux_stride;     // face cells of the level
   double dt, dx, dy, dz;
   unsigned long long* cflmax;
@@ -96,6 +101,12 @@ void launch_fad3(const void* flux, long long flux_stride, const long long* face0
                  const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s, bool f32);
 void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
                  int nvar, double hx, double hy, double hz, double delt, cudaStream_t s, bool f32);
+// valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
+void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32);
+// b4step3 of the time-modulated swirl: aux = c * aux0 over the enlarged patches of plist
+// (max_cells: the largest enlarged patch)
+void launch_b4step3(void* pool, const PatchDev* patches, const int* plist, int np, int naux, long long max_cells, double c,
+                    cudaStream_t s, bool f32);
 void launch_fill3(const Fill3Args& a, cudaStream_t s, bool f32);
 void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s, bool f32);
 void launch_upbnd3(void* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,

@@ -98,6 +98,7 @@ struct RunParams {
   // problem plugin (setprob.data)
   std::string problem;
   std::map<std::string, double> probnum;
+  std::map<std::string, std::string> probstr;
   int flag_component = 0;
   std::string flag_mode;
 
@@ -177,12 +178,14 @@ struct RunParams {
     problem = s.str("problem");
     for (auto& kvp : s.kv) {
       if (kvp.first == "problem" || kvp.second.empty()) continue;
+      probstr[kvp.first] = s.str(kvp.first);
       try { probnum[kvp.first] = KeyFile::num(kvp.second[0]); } catch (...) {}
     }
     flag_component = s.n_or("flag_component", 0);
     flag_mode = s.has("flag_mode") ? s.str("flag_mode") : std::string("component");
   }
   double pn(const std::string& k, double d) const { auto it = probnum.find(k); return it == probnum.end() ? d : it->second; }
+  std::string ps(const std::string& k, const std::string& d) const { auto it = probstr.find(k); return it == probstr.end() ? d : it->second; }
 };
 
 }  // namespace amrb

@@ -64,3 +64,35 @@ def acoustics_pulse(n: int, levels: int = 3, ratio: int = 2, tfinal: float = 0.4
     _claw(rd, (-1.0, -1.0), (1.0, 1.0), n, 3, 2, tfinal, 0.5 / n, "mc", "extrap")
     _amr(rd, levels, ratio, 0.05)
     return rd
+
+
+def advection_swirl3d(n: int = 32, levels: int = 4, ratio: int = 2, tfinal: float = 1.5, sphere: bool = True,
+                      vel_period: float = 1.5, x0: float = 0.5, y0: float = 0.25, z0: float = 0.5, r0: float = 0.15,
+                      tol: float = 0.1, max1d: int = 32) -> ClawRunData:
+    """3D advection in the swirling field u = 2 sin^2(pi x) sin(2 pi y) sin(2 pi z), v and w
+    permuted likewise, on [0,1]^3 (examples/advection_3d_swirl), face-centred velocities in
+    aux 1..3. sphere: q = 1 within r0 of (x0, y0, z0), else the example's half space x < 0.5;
+    vel_period > 0 scales the field by cos(pi t / vel_period) before every step (b4step3)."""
+    rd = ClawRunData(num_dim=3)
+    p = rd.probdata
+    p.add_param("problem", "advection_swirl")
+    p.add_param("ic", "sphere" if sphere else "halfspace")
+    for k, val in (("x0", x0), ("y0", y0), ("z0", z0), ("r0", r0), ("vel_period", vel_period)):
+        p.add_param(k, val)
+    c = rd.clawdata
+    c.lower = [0.0, 0.0, 0.0]; c.upper = [1.0, 1.0, 1.0]; c.num_cells = [n, n, n]
+    c.num_eqn = 1; c.num_waves = 1; c.num_aux = 3; c.capa_index = 0
+    c.output_style = 1; c.num_output_times = 1; c.tfinal = tfinal; c.output_t0 = False
+    c.dt_variable = True; c.dt_initial = 0.4 / n; c.dt_max = 1e99; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.steps_max = 1000000; c.order = 2; c.transverse_waves = 22; c.limiter = ["mc"]
+    c.bc_lower = ["extrap"] * 3; c.bc_upper = ["extrap"] * 3
+    a = rd.amrdata
+    r = [ratio] * max(1, levels - 1)
+    a.amr_levels_max = levels
+    a.refinement_ratios_x = list(r); a.refinement_ratios_y = list(r); a.refinement_ratios_z = list(r)
+    a.refinement_ratios_t = list(r)
+    a.aux_type = ["xleft", "yleft", "zleft"]
+    a.flag2refine = True; a.flag2refine_tol = tol; a.regrid_interval = 2; a.regrid_buffer_width = 2
+    a.clustering_cutoff = 0.7
+    a.max1d = max1d
+    return rd

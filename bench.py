@@ -49,6 +49,31 @@ def workload(name: str):
     raise SystemExit("unknown workload %s" % name)
 
 
+# FP64 operations per cell-update of the 3D Euler CTU (transverse_waves 22) step kernels:
+# dadd + dmul + 2*dfma thread instructions of the three sweeps of a level-1 step, divided by
+# its cells (ncu instruction counts; the count does not depend on the patch sizes)
+FLOPS_PER_CELL_UPDATE_3D = 10.4e3
+
+
+def fp64_peak_tflops() -> float:
+    """Measured FP64 peak of this GPU: a 4096^3 DGEMM (2*N^3 flops), best of 5."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
 def oracle_cls(ndim):
     from oracle.pyoracle import Oracle2D, Oracle3D
     return Oracle3D if ndim == 3 else Oracle2D
@@ -307,6 +332,15 @@ def main():
     os.environ.setdefault("AMRGPU_HOST_THREADS", "2")
     serving = serving_leg() if not args.no_cpu_baseline else None
     achieved = kern_cells * bytes_per_update / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
+    fp64_roof = None
+    if ndim == 3 and kern_ms > 0:
+        # the roof that binds this step: FP64 arithmetic, against a DGEMM measured here
+        fpk = fp64_peak_tflops()
+        ach = kern_cells * FLOPS_PER_CELL_UPDATE_3D / (kern_ms * 1e-3) / 1e12
+        fp64_roof = {"achieved": ach, "peak": fpk, "unit": "TFLOP/s", "frac": ach / fpk,
+                     "flops_per_cell_update": FLOPS_PER_CELL_UPDATE_3D,
+                     "peak_kind": "measured here: FP64 DGEMM 4096^3, best of 5",
+                     "note": "built without FMA contraction for bit-exact FP64, so dadd/dmul issue at the dfma rate"}
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -335,7 +369,8 @@ def main():
                      "frac": achieved / peak if peak else None, "traffic": None,
                      "kernel": "sweep3<1..3> + face3 + update3" if ndim == 3 else "step2 sweeps + update",
                      "peak_kind": peak_kind,
-                     "bytes_per_cell_update": bytes_per_update},
+                     "bytes_per_cell_update": bytes_per_update,
+                     "fp64": fp64_roof},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d) // max(1, nstep),
                 "d2h_bytes_per_step": d2h // max(1, nstep), "seconds": t1 - t0, "coarse_steps": nstep,

@@ -105,6 +105,10 @@ struct Amr3 {
   std::string problem;
   double blast_x = 0, blast_y = 0, blast_z = 0, blast_r = 0.2, blast_pin = 5.0, blast_pout = 1.0;
   int flag_pressure = 0;  // 1: flag on the pressure difference (euler_3d_radial flag2refine pattern)
+  // swirl variants: the initial condition is the reference test's half space (x < 0.5) or a
+  // sphere; vel_period > 0 scales the velocities by cos(pi t / vel_period) in b4step3
+  bool swirl_sphere = false;
+  double sph_x = 0.5, sph_y = 0.25, sph_z = 0.5, sph_r = 0.15, vel_period = 0.0;
 
   // ---------------- state
   std::vector<Node3> node;
@@ -205,6 +209,9 @@ struct Amr3 {
     if (problem == "advection_swirl") {
       prob.solver = SOLVER_VC_ADVECTION;
       if (naux != 3) throw std::runtime_error("advection_swirl needs 3 aux components");
+      swirl_sphere = s.sget("ic", "halfspace") == "sphere";
+      sph_x = s.dget("x0", 0.5); sph_y = s.dget("y0", 0.25); sph_z = s.dget("z0", 0.5); sph_r = s.dget("r0", 0.15);
+      vel_period = s.dget("vel_period", 0.0);
     } else if (problem == "euler_blast") {
       prob.solver = SOLVER_EULER; prob.gamma = s.d("gamma"); prob.gamma1 = prob.gamma - 1.0;
       prob.efix = s.iget("efix", 1) != 0;
@@ -222,7 +229,20 @@ struct Amr3 {
   void qinit(int mbc, int mx, int my, int mz, double xl, double yl, double zl, double dx, double dy, double dz, double* q) {
     FArr3 Q{q, nvar, mx + 2 * mbc, my + 2 * mbc, mz + 2 * mbc};
     auto at = [&](int m, int i, int j, int k) -> double& { return Q(m, i + mbc, j + mbc, k + mbc); };
-    if (problem == "advection_swirl") {
+    if (problem == "advection_swirl" && swirl_sphere) {
+      // q = 1 inside the sphere of radius r0 about (x0, y0, z0), 0 outside
+      for (int k = 1; k <= mz; ++k) {
+        const double zc = zl + (k - 0.5) * dz;
+        for (int j = 1; j <= my; ++j) {
+          const double yc = yl + (j - 0.5) * dy;
+          for (int i = 1; i <= mx; ++i) {
+            const double xc = xl + (i - 0.5) * dx;
+            const double ddx = xc - sph_x, ddy = yc - sph_y, ddz = zc - sph_z;
+            at(1, i, j, k) = (ddx * ddx + ddy * ddy + ddz * ddz <= sph_r * sph_r) ? 1.0 : 0.0;
+          }
+        }
+      }
+    } else if (problem == "advection_swirl") {
       for (int i = 1; i <= mx; ++i) {
         const double x = xl + (i - 0.5) * dx;
         for (int j = 1; j <= my; ++j)
@@ -267,6 +287,18 @@ struct Amr3 {
         }
       }
     }
+  }
+
+  // b4step3 (src/3d/b4step3.f90:2-16 is the no-op default; stepgrid.f:113 calls it with the
+  // grid's time before step3): the time-modulated swirl sets the face velocities of the
+  // whole enlarged patch to setaux's values times cos(pi t / vel_period)
+  void b4step3(int mx, int my, int mz, double xl, double yl, double zl, double dx, double dy, double dz, double t, double* aux) {
+    if (problem != "advection_swirl" || vel_period <= 0.0) return;
+    setaux(nghost, mx, my, mz, xl, yl, zl, dx, dy, dz, aux);
+    const double pi = 4.0 * std::atan(1.0);
+    const double c = std::cos(pi * t / vel_period);
+    const size_t n = (size_t)naux * (mx + 2 * nghost) * (my + 2 * nghost) * (mz + 2 * nghost);
+    for (size_t i = 0; i < n; ++i) aux[i] = aux[i] * c;
   }
 
   // =================================================== node store (nodget.f)
@@ -1349,6 +1381,7 @@ struct Amr3 {
     if (!gauges.empty() && record_gauges) update_gauges(g.q1.data(), xlow, ylow, zlow, mitot, mjtot, mktot, mptr);
     const size_t n = qsize(mptr);
     std::vector<double> fm(n), fp(n), gm(n), gp(n), hm(n), hp(n);
+    if (naux > 0) b4step3(nx, ny, nz, g.xlo, g.ylo, g.zlo, hx, hy, hz, g.time, g.aux.data());
     stepgrid(g.q1.data(), fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mitot, mjtot, mktot, delt, dtnew, hx, hy, hz,
              g.aux.data(), cflgrid);
     if (g.has_cfl) fluxsv(mptr, fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mitot, mjtot, mktot, delt, hx, hy, hz);
@@ -2322,11 +2355,19 @@ struct Amr3 {
     return totmass * hx * hy * hz;
   }
 
-  // valout.f90 (3D ascii form)
+  // valout.f90 (3D ascii form); valout.f90:140-147 first zeroes |q| < 1e-90 of the interior cells in place
   void valout(int lbeg, int lend, double t) {
     for (int level = lbeg; level <= lend; ++level)
-      for (int m = lstart[level]; m != 0; m = node[m].levelptr)
-        for (double& v : node[m].q1) if (std::fabs(v) < 1e-90) v = 0.0;
+      for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+        const int mitot = mitot_of(m), mjtot = mjtot_of(m), mktot = mktot_of(m);
+        for (int k = nghost + 1; k <= mktot - nghost; ++k)
+          for (int j = nghost + 1; j <= mjtot - nghost; ++j)
+            for (int i = nghost + 1; i <= mitot - nghost; ++i)
+              for (int iv = 1; iv <= nvar; ++iv) {
+                double& v = node[m].q1[(size_t)(iv - 1) + (size_t)nvar * ((size_t)(i - 1) + (size_t)mitot * ((j - 1) + (size_t)mjtot * (k - 1)))];
+                if (std::fabs(v) < 1e-90) v = 0.0;
+              }
+      }
     if (write_output) {
       char fn[64];
       std::snprintf(fn, sizeof(fn), "/fort.q%04d", matlabu);
