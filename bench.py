@@ -185,6 +185,55 @@ def fp32_leg(cpu_threads: int, rd3=None, cfg3=None) -> dict:
             o3[prec] = {"value": cells / (ms * 1e-3), "unit": "cell-updates/s", "solve_ms": ms, "cell_updates": cells,
                         "l1_rel_err_vs_fp64": [float(x) for x in rel], "mass_rel_diff_vs_fp64": abs(mm - m) / abs(m)}
         out["blast3d"] = o3
+    out["swirl3d"] = swirl_fp32_leg(cpu_threads)
+    return out
+
+
+def swirl_fp32_leg(cpu_threads: int) -> dict:
+    """The FP32 form on the 3D swirl (sphere r = 0.15 at (0.5, 0.25, 0.5), velocity field
+    scaled by cos(pi t / 1.5), 32^3 base grid, 4 levels, ratio 2): level-1 L1 error and mass
+    against the FP64 oracle at t = 0.1 (an oracle run of seconds), and against the FP64
+    device path, which the parity tests hold bit-identical to the oracle, over the whole
+    period to t = 1.5; mass drift is the relative change of the level-1 mass over the run."""
+    from amrclaw_b200 import Solver, fields, problems
+    from oracle.pyoracle import Oracle3D
+    n = 32
+    out = {"workload": "swirl3d_sphere_modulated", "base_grid": "32x32x32", "levels": 4, "ratio": 2,
+           "velocity": "swirl x cos(pi t / 1.5)", "ic": "sphere r=0.15 at (0.5,0.25,0.5)"}
+
+    def run(tfinal, precisions, with_oracle):
+        rd = problems.advection_swirl3d(n=n, levels=4, tfinal=tfinal)
+        res = {}
+        with tempfile.TemporaryDirectory() as d:
+            rd.write(d)
+            if with_oracle:
+                o = Oracle3D(d, threads=cpu_threads)
+                o.run(0)
+                res["oracle"] = (o.grids(), o.values(), o.mass(), None, None, None)
+                o.close()
+            for prec in precisions:
+                with Solver(d, precision=prec) as s:
+                    m0 = s.mass()
+                    s.run(0)
+                    inf = s.info()
+                    res[prec] = (s.grids(), s.values(), s.mass(), m0, inf["cell_updates"], inf["last_run_ms"])
+        return res
+
+    def compare(res, ref_key, key):
+        g, v, m, _, _, _ = res[ref_key]
+        ref = fields.level_array(g, v, 1, 1, (n, n, n))
+        g2, v2, m2, m0, cells, ms = res[key]
+        _, rel = fields.l1_error(fields.level_array(g2, v2, 1, 1, (n, n, n)), ref, (1.0 / n) ** 3)
+        return float(rel[0]), abs(m2 - m) / abs(m), (m2 - m0) / m0, cells / (ms * 1e-3)
+
+    short = run(0.1, ("fp64", "fp32"), True)
+    full = run(1.5, ("fp64", "fp32"), False)
+    for prec in ("fp64", "fp32"):
+        l1o, mo, drift_s, _ = compare(short, "oracle", prec)
+        l1f, mf, drift, cups = compare(full, "fp64", prec)
+        out[prec] = {"value": cups, "unit": "cell-updates/s", "tfinal": 1.5,
+                     "l1_rel_err_vs_fp64_oracle_t0.1": l1o, "mass_rel_diff_vs_fp64_oracle_t0.1": mo,
+                     "l1_rel_err_vs_fp64_t1.5": l1f, "mass_rel_diff_vs_fp64_t1.5": mf, "mass_drift_t1.5": drift}
     return out
 
 

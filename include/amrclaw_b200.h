@@ -27,15 +27,16 @@ const char* amrgpu_last_error(void);
 /* Reads claw.data, amr.data, regions.data, gauges.data and setprob.data from
  * rundir (the files setrun.py writes), builds the initial hierarchy on the device
  * and writes frame 0 when output_t0 is set. num_dim in claw.data selects the 2D
- * path (amr2) or the 3D path (amr3, Euler equations).
+ * path (amr2) or the 3D path (amr3: Euler equations, or advection in the swirl's
+ * face-centred velocity field with aux arrays set by the problem's setaux).
  * Replaces the start-up of src/2d/amr2.f90:140-612 (input reading :148-394,
  * domain.f:4-110, setgrd.f:4-142, ginit.f:17-86, conck.f:6-73) and of
  * src/3d/amr3.f90 (domain.f, setgrd.f, ginit.f of src/3d). */
 int amrgpu_init(const char* rundir, const char* outdir, int write_output, amrgpu_ctx** ctx);
 
 /* amrgpu_init with a choice of precision. precision_bits = 64: the FP64 path, bit-
- * identical to the reference's arithmetic. precision_bits = 32: the FP32 form (2D runs):
- * patch storage, ghost values, Riemann solves and flux differencing in FP32; flux
+ * identical to the reference's arithmetic. precision_bits = 32: the FP32 form (2D and 3D):
+ * patch storage, ghost values, aux arrays, Riemann solves and flux differencing in FP32; flux
  * registers (fluxsv/fluxad/qad sums), register corrections, averaging sums, totals and
  * time/dt bookkeeping in FP64. No counterpart in the reference (FP64 only). */
 int amrgpu_init_precision(const char* rundir, const char* outdir, int write_output, int precision_bits, amrgpu_ctx** ctx);
