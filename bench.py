@@ -53,6 +53,10 @@ def workload(name: str):
 # dadd + dmul + 2*dfma thread instructions of the three sweeps of a level-1 step, divided by
 # its cells (ncu instruction counts; the count does not depend on the patch sizes)
 FLOPS_PER_CELL_UPDATE_3D = 10.4e3
+# DRAM bytes per cell-update of the same kernels (sweeps, face gather, update): ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of a level-1 substep of the 64^3 blast,
+# 1,108 MB over 262,144 cell-updates
+DRAM_BYTES_PER_CELL_UPDATE_3D = 1108.3e6 / 262144
 
 
 def fp64_peak_tflops() -> float:
@@ -415,10 +419,16 @@ def main():
         "fp32_form": fp32,
         "serving": serving,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None,
+                     "traffic": (DRAM_BYTES_PER_CELL_UPDATE_3D * kern_cells / step_launches
+                                 if ndim == 3 and step_launches else None),
+                     "traffic_note": "DRAM bytes per level substep of the step kernels: ncu bytes per cell-update "
+                                     "of a level-1 substep times the average cells of a timed substep",
                      "kernel": "sweep3<1..3> + face3 + update3" if ndim == 3 else "step2 sweeps + update",
                      "peak_kind": peak_kind,
                      "bytes_per_cell_update": bytes_per_update,
+                     "algorithmic_bytes_per_launch": (bytes_per_update * kern_cells / step_launches
+                                                      if step_launches else None),
                      "fp64": fp64_roof},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d) // max(1, nstep),
