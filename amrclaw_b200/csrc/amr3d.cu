@@ -673,8 +673,12 @@ class Amr3Gpu : public AmrSolver {
     for (int l = 1; l <= lev; ++l) GI(l);
     const std::vector<int>& G = lgrids[lev];
     std::vector<Prog3> part(G.size());
+    PhaseTimer tph(hprof);
+    tph.next("cb_patches");
     pool_host.run((int)G.size(), [&](int k) { compile_bound_patch(part[k], lev, G[k]); });
+    tph.next("cb_merge");
     for (size_t k = 0; k < part.size(); ++k) merge_prog(P, part[k], (int)k);
+    tph.next("cb_upload");
     upload_prog(P);
   }
 
@@ -726,6 +730,24 @@ class Amr3Gpu : public AmrSolver {
     upload_prog(P);
   }
 
+  // the stable order by (stage, owner): a counting sort by stage, then (only where the
+  // owners of a stage are not already ascending, which merge_prog's appends make them)
+  // a stable sort by owner inside the stage
+  static std::vector<int> stage_owner_order(const std::vector<int>& stage, const std::vector<int>& owner, int nstages) {
+    const size_t n = stage.size();
+    std::vector<int> start((size_t)std::max(nstages, 1) + 1, 0), idx(n);
+    for (size_t i = 0; i < n; ++i) ++start[stage[i] + 1];
+    for (int k = 0; k < nstages; ++k) start[k + 1] += start[k];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (size_t i = 0; i < n; ++i) idx[fill[stage[i]]++] = (int)i;
+    for (int k = 0; k < nstages; ++k) {
+      auto b = idx.begin() + start[k], e = idx.begin() + start[k + 1];
+      bool asc = true;
+      for (auto it = b; it != e && asc; ++it) if (it != b && owner[*(it - 1)] > owner[*it]) asc = false;
+      if (!asc) std::stable_sort(b, e, [&](int x, int y) { return owner[x] < owner[y]; });
+    }
+    return idx;
+  }
   void upload_prog(Prog3& P) {
     HPROF("upload_prog3");
     if (P.scratch_off >= 0) pfree(P.scratch_off, P.scratch_alloc);
@@ -734,13 +756,9 @@ class Amr3Gpu : public AmrSolver {
     std::vector<Rect3> rects = P.rects;
     for (auto& r : rects) r.off += P.scratch_off;
     P.d_rects.upload(rects, st, stg);
-    std::vector<int> oidx(P.ops.size());
-    for (size_t i = 0; i < oidx.size(); ++i) oidx[i] = (int)i;
     // stage-major, then owner (patch) order: a stage's ops are one range, and so are one
     // patch's ops within a stage (ops of one owner keep their compile order)
-    std::stable_sort(oidx.begin(), oidx.end(), [&](int a, int b) {
-      return P.op_stage[a] != P.op_stage[b] ? P.op_stage[a] < P.op_stage[b] : P.op_owner[a] < P.op_owner[b];
-    });
+    const std::vector<int> oidx = stage_owner_order(P.op_stage, P.op_owner, P.nstages);
     const int no = std::max(P.nowners, 1);
     std::vector<Fill3Op> ops;
     std::vector<Fill3Chunk> ch;
@@ -760,11 +778,7 @@ class Amr3Gpu : public AmrSolver {
       P.own_ch_hi[ow] = (int)ch.size();
     }
     while (s + 1 < P.nstages) { ++s; P.ch_lo[s] = P.ch_hi[s] = (int)ch.size(); }
-    std::vector<int> bidx(P.bcs.size());
-    for (size_t i = 0; i < bidx.size(); ++i) bidx[i] = (int)i;
-    std::stable_sort(bidx.begin(), bidx.end(), [&](int a, int b) {
-      return P.bc_stage[a] != P.bc_stage[b] ? P.bc_stage[a] < P.bc_stage[b] : P.bc_owner[a] < P.bc_owner[b];
-    });
+    const std::vector<int> bidx = stage_owner_order(P.bc_stage, P.bc_owner, P.nstages);
     std::vector<Bc3Op> bcs;
     P.bc_lo.assign(P.nstages, 0); P.bc_hi.assign(P.nstages, 0);
     P.own_bc_lo.assign((size_t)P.nstages * no, 0); P.own_bc_hi.assign((size_t)P.nstages * no, 0);
@@ -916,12 +930,15 @@ class Amr3Gpu : public AmrSolver {
     Plan3& L = plan[lev];
     L.upc.clear(); L.upt.clear(); L.avg.clear();
     if (lev < p.mxnest && lstart[lev + 1] != 0) {
+      PhaseTimer tph(hprof);
+      tph.next("cu_lists");
       const GridIndex& XF = GI(lev + 1);
       const int rx = intratx[lev], ry = intraty[lev], rz = intratz[lev];
       const std::vector<int>& G = lgrids[lev];
       struct Part { std::vector<Upbnd3Cell> upc; std::vector<Upbnd3Term> upt; std::vector<Avg3> avg; };
       std::vector<Part> part(G.size());
       pool_host.run((int)G.size(), [&](int n) { update_lists(G[n], XF, rx, ry, rz, part[n].upc, part[n].upt, part[n].avg); });
+      tph.next("cu_merge");
       for (Part& q : part) {
         const int base = (int)L.upt.size();
         for (Upbnd3Cell c : q.upc) { c.first += base; L.upc.push_back(c); }
@@ -942,26 +959,31 @@ class Amr3Gpu : public AmrSolver {
     if (g.has_cfl) {
       // upbnd.f: the entries of one coarse cell in listbc order, each side at most once
       // (the iused bit mask); cells are independent, so they are grouped by a sort
-      const int mi = mitot(m), mj = mjtot(m);
+      // (a counting sort by cell over the enlarged patch: stable, so a cell's entries keep
+      // their listbc order)
+      const int mi = mitot(m), mj = mjtot(m), mk = mktot(m);
       const size_t ne = g.listbc.size() / 6;
-      if (ne >= (1u << 24)) throw std::runtime_error("upbnd: too many register entries on one patch");
-      std::vector<unsigned long long> ord(ne);
-      for (size_t e = 0; e < ne; ++e) {
+      const long long ncell = (long long)mi * mj * mk;
+      std::vector<int> start((size_t)ncell + 1, 0), ord(ne);
+      auto cell_of = [&](size_t e) {
         const int* b = &g.listbc[6 * e];
-        const unsigned long long key = ((unsigned long long)(b[2] - 1) * mj + (b[1] - 1)) * mi + (b[0] - 1);
-        ord[e] = (key << 24) | e;
+        return ((long long)(b[2] - 1) * mj + (b[1] - 1)) * mi + (b[0] - 1);
+      };
+      for (size_t e = 0; e < ne; ++e) ++start[cell_of(e) + 1];
+      for (long long c = 0; c < ncell; ++c) start[c + 1] += start[c];
+      {
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (size_t e = 0; e < ne; ++e) ord[fill[cell_of(e)]++] = (int)e;
       }
-      std::sort(ord.begin(), ord.end());
       for (size_t a0 = 0; a0 < ne;) {
-        const unsigned long long key = ord[a0] >> 24;
-        size_t a1 = a0;
-        while (a1 < ne && (ord[a1] >> 24) == key) ++a1;
+        const long long key = cell_of(ord[a0]);
+        const size_t a1 = (size_t)start[key + 1];
         Upbnd3Cell c{};
-        c.patch = m; c.ie = (int)(key % mi); c.je = (int)((key / mi) % mj); c.ke = (int)(key / ((unsigned long long)mi * mj));
+        c.patch = m; c.ie = (int)(key % mi); c.je = (int)((key / mi) % mj); c.ke = (int)(key / ((long long)mi * mj));
         c.first = (int)upt.size();
         int used = 0;
         for (size_t q = a0; q < a1; ++q) {
-          const int* b = &g.listbc[6 * (ord[q] & 0xffffff)];
+          const int* b = &g.listbc[6 * ord[q]];
           const int side = b[3], norm = 1 << (side - 1);
           if ((used / norm) % 2 == 1) continue;
           upt.push_back(Upbnd3Term{node[b[4]].ffl + (long long)nvar * (b[5] - 1), chsign[side]});
@@ -1652,10 +1674,12 @@ class Amr3Gpu : public AmrSolver {
       for (int q = lstart[l2]; q != 0; q = node[q].levelptr) lgrids[l2].push_back(q);
     }
     lfine = lfnew;
-    tph.next("rg_prep_lists");
+    tph.next("rg_prepf_prepc");
     for (int lev = lbase; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
+    tph.next("rg_arrange_lists");
     for (int lev = lbase + 1; lev <= p.mxnest; ++lev) arrange(lev);
     make_lists();
+    tph.next("rg_bndry");
     for (int lev = lbase + 1; lev <= lfine; ++lev) make_bndry(lev);
     tph.next("rg_compile");
     compile_all(lbase);
