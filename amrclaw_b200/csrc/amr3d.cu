@@ -126,10 +126,13 @@ struct Plan3 {
   DBuf<Upbnd3Cell> d_upc;
   DBuf<Upbnd3Term> d_upt;
   DBuf<Avg3> d_avg;
+  // one-patch views of the sweep prefixes for the per-patch launches of the plain path:
+  // per patch, (first, last) slot and (first, last) interface of each direction
+  DBuf<long long> d_pp;
   void free_dev() {
     bound.free_dev(); saveqc.free_dev();
     d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_seg0.free(); d_fad.free(); d_qad.free();
-    d_upc.free(); d_upt.free(); d_avg.free();
+    d_upc.free(); d_upt.free(); d_avg.free(); d_pp.free();
   }
 };
 
@@ -207,6 +210,9 @@ class Amr3Gpu : public AmrSolver {
 
   ~Amr3Gpu() override {
     if (st) cudaStreamSynchronize(st);
+    for (auto& G : lgraph) G.reset();
+    if (d_sub) cudaFree(d_sub);
+    if (h_sub) cudaFreeHost(h_sub);
     for (auto& L : plan) L.free_dev();
     newfill.free_dev();
     pool.destroy(); regs.destroy();
@@ -799,7 +805,7 @@ class Amr3Gpu : public AmrSolver {
   }
 
   // one patch's part of a program (the per-patch bound.f call of the plain path)
-  void run_prog_owner(Prog3& P, const SrcMode& modes, int owner) {
+  void run_prog_owner(Prog3& P, const SrcMode& modes, int owner, const SrcMode* modes_dev = nullptr) {
     const int no = std::max(P.nowners, 1);
     if (owner >= no) return;
     for (int s = 0; s < P.nstages; ++s) {
@@ -808,6 +814,7 @@ class Amr3Gpu : public AmrSolver {
         Fill3Args a{};
         a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
         a.chunks = P.d_chunks.d + P.own_ch_lo[ow]; a.nchunks = P.own_ch_hi[ow] - P.own_ch_lo[ow]; a.nvar = nvar; a.modes = modes;
+        a.modes_dev = modes_dev;
         a.lc = lc; a.xlower = xlower; a.ylower = ylower; a.zlower = zlower;
         launch_fill3(a, st, f32);
         ++nkernels;
@@ -822,7 +829,7 @@ class Amr3Gpu : public AmrSolver {
     }
   }
 
-  void run_prog(Prog3& P, const SrcMode& modes) {
+  void run_prog(Prog3& P, const SrcMode& modes, const SrcMode* modes_dev = nullptr) {
     if (P.zero_scratch && P.scratch_len > 0 && P.nstages > 0)
       AMR_CUDA(cudaMemsetAsync(pool_bytes() + elem() * P.scratch_off, 0, elem() * P.scratch_len, st));
     for (int s = 0; s < P.nstages; ++s) {
@@ -830,6 +837,7 @@ class Amr3Gpu : public AmrSolver {
         Fill3Args a{};
         a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
         a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
+        a.modes_dev = modes_dev;
         a.lc = lc; a.xlower = xlower; a.ylower = ylower; a.zlower = zlower;
         launch_fill3(a, st, f32);
         ++nkernels;
@@ -908,6 +916,17 @@ class Amr3Gpu : public AmrSolver {
     L.d_comp0.upload(L.comp0, st, stg);
     L.d_face0.upload(L.face0, st, stg);
     L.d_cell0.upload(L.cell0, st, stg);
+    {
+      std::vector<long long> pp((size_t)12 * np, 0);
+      for (int k = 0; k < np; ++k)
+        for (int d = 0; d < 3; ++d) {
+          pp[(size_t)12 * k + 2 * d] = L.sweep0[(size_t)d * (np + 1) + k];
+          pp[(size_t)12 * k + 2 * d + 1] = L.sweep0[(size_t)d * (np + 1) + k + 1];
+          pp[(size_t)12 * k + 6 + 2 * d] = L.comp0[(size_t)d * (np + 1) + k];
+          pp[(size_t)12 * k + 6 + 2 * d + 1] = L.comp0[(size_t)d * (np + 1) + k + 1];
+        }
+      L.d_pp.upload(pp, st, stg);
+    }
     L.d_fsv.upload(L.fsv, st, stg);
     L.d_seg0.upload(L.seg0, st, stg);
     L.d_fad.reserve(L.nseg);
@@ -1124,6 +1143,7 @@ class Amr3Gpu : public AmrSolver {
     const int todo = dirty[lev] & what;
     if (!todo) return;
     dirty[lev] &= ~todo;
+    ++plan_gen[lev];
     if (todo & NEED_BOUND) compile_bound(lev);
     if (todo & NEED_SAVEQC) compile_saveqc(lev);
     if (todo & NEED_STEP) compile_step(lev);
@@ -1155,7 +1175,157 @@ class Amr3Gpu : public AmrSolver {
     run_prog(plan[lev].bound, modes_for(lev, t));
   }
 
-  // advanc.f:4-139 with par_advanc (:166-303) for all patches of the level at once
+  // ---- scalars of a level substep that change from substep to substep; a captured graph
+  // reads them from device memory, refreshed by one copy before each replay
+  struct Substep3 { SrcMode modes; double dt; double b4c; };
+  Substep3* d_sub = nullptr;  // [12] on the device
+  Substep3* h_sub = nullptr;  // [12] pinned
+  // a level's substep as two CUDA graphs around the gauge sampling: pre (ghost fill,
+  // saveqc, and the batched path's qad) and post (CFL reset, b4step3, step kernels,
+  // fluxsv/fluxad, flip, CFL read-back). Valid while the level's plans and the buffers
+  // they point into stay the same.
+  struct LevelGraph {
+    cudaGraphExec_t pre = nullptr, post = nullptr;
+    long long gen = -1;
+    int batched = -1;
+    const void* ptrs[6] = {};
+    long long kpre = 0, kpost = 0;
+    void reset() {
+      if (pre) cudaGraphExecDestroy(pre);
+      if (post) cudaGraphExecDestroy(post);
+      pre = post = nullptr; gen = -1;
+    }
+  };
+  LevelGraph lgraph[12];
+  bool use_graphs = false;
+  long long plan_gen[12] = {0};
+  long long graph_captures = 0, graph_replays = 0;
+
+  // the launches before the gauge sampling (ds: read dt and the fill modes from there)
+  void launch_pre(int lev, double t, double dt, const Substep3* ds) {
+    Plan3& L = plan[lev];
+    const bool kids = lev + 1 <= p.mxnest && lstart[lev + 1] != 0;
+    const SrcMode M = modes_for(lev, t);
+    const SrcMode* Md = ds ? &ds->modes : nullptr;
+    if (batched) {
+      // every patch of the level in one launch per routine
+      run_prog(L.bound, M, Md);
+      if (kids) { SrcMode Z{}; run_prog(L.saveqc, Z); }
+      if (lev > 1 && L.nseg > 0) {
+        launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.nseg, sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st, f32,
+                    ds ? &ds->dt : nullptr);
+        ++nkernels;
+      }
+    } else {
+      // the reference's per-grid structure (advanc.f): bound for every grid, saveqc for the level
+      const int np = (int)L.plist.size();
+      for (int k = 0; k < np; ++k) run_prog_owner(L.bound, M, k, Md);
+      if (kids) { SrcMode Z{}; run_prog(L.saveqc, Z); }
+    }
+  }
+  // the launches after the gauge sampling; timed: bracket the step kernels with ev_a/ev_b
+  void launch_post(int lev, double t, double dt, const Substep3* ds, bool timed) {
+    Plan3& L = plan[lev];
+    const double* dtd = ds ? &ds->dt : nullptr;
+    const double* cd = ds ? &ds->b4c : nullptr;
+    const double c = vel_period > 0.0 ? b4step_factor(t) : 1.0;
+    Step3Args a{};
+    a.pool = pool.d; a.patches = d_patches.d; a.sp = sp;
+    a.stash = d_stash.d; a.stash_stride = L.slots; a.flux = d_flux.d; a.flux_stride = L.faces;
+    a.dt = dt; a.dt_dev = dtd; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.dz = hzposs[lev]; a.cflmax = d_cfl;
+    AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+    const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
+    if (batched) {
+      if (vel_period > 0.0) {
+        launch_b4step3(pool.d, d_patches.d, L.d_plist.d, (int)L.plist.size(), p.naux, max_enlarged(lev), c, st, f32, cd);
+        ++nkernels;
+      }
+      if (timed) AMR_CUDA(cudaEventRecord(ev_a, st));
+      a.plist = L.d_plist.d; a.np = (int)L.plist.size();
+      a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
+      launch_step3(a, L.items, L.faces, L.cells, st, f32);
+      nkernels += 5;
+      if (timed) AMR_CUDA(cudaEventRecord(ev_b, st));
+      if (!L.fsv.empty()) {
+        launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hx, hy, hz, st, f32, dtd);
+        ++nkernels;
+      }
+      if (lev > 1 && L.nseg > 0) {
+        launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.nseg, nvar, dt, hx, hy, hz, st, f32, dtd);
+        ++nkernels;
+      }
+    } else {
+      // par_advanc per grid (qad, b4step3, stepgrid, fluxsv, fluxad), each grid its own
+      // launches; the per-grid arrays are views of the level's
+      const int np = (int)L.plist.size();
+      if (timed) AMR_CUDA(cudaEventRecord(ev_a, st));
+      for (int k = 0; k < np; ++k) {
+        const long long q0 = L.seg0[k], nq = L.seg0[k + 1] - L.seg0[k];
+        if (lev > 1 && nq > 0) {
+          launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d + q0, (int)nq, sp, nvar, hx, hy, hz, dt, st, f32, dtd);
+          ++nkernels;
+        }
+        if (vel_period > 0.0) {
+          const int m = L.plist[k];
+          launch_b4step3(pool.d, d_patches.d, L.d_plist.d + k, 1, p.naux, (long long)mitot(m) * mjtot(m) * mktot(m), c, st, f32, cd);
+          ++nkernels;
+        }
+        Step3Args b = a;
+        b.plist = L.d_plist.d + k; b.np = 1;
+        b.sweep0 = L.d_pp.d + (size_t)12 * k; b.comp0 = L.d_pp.d + (size_t)12 * k + 6;
+        b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
+        long long it[3];
+        for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
+        launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
+        nkernels += 5;
+        const long long f0 = L.fsv0[k], nf = L.fsv0[k + 1] - L.fsv0[k];
+        if (nf > 0) {
+          launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d + f0, (int)nf, nvar, dt, hx, hy, hz, st, f32, dtd);
+          ++nkernels;
+        }
+        if (lev > 1 && nq > 0) {
+          launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d + q0, (int)nq, nvar, dt, hx, hy, hz, st, f32, dtd);
+          ++nkernels;
+        }
+      }
+      if (timed) AMR_CUDA(cudaEventRecord(ev_b, st));
+    }
+    launch_flip(d_patches.d, L.d_plist.d, (int)L.plist.size(), st);
+    ++nkernels;
+    // into pinned memory, so the copy is queued and the host goes on compiling
+    AMR_CUDA(cudaMemcpyAsync(h_cfl, d_cfl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  }
+  // captures the level's two graphs if the current ones do not fit the plans and buffers
+  void ensure_graphs(int lev) {
+    LevelGraph& G = lgraph[lev];
+    const void* ptrs[6] = {pool.d, regs.d, d_patches.d, d_stash.d, d_flux.d, d_cfl};
+    bool ok = G.pre && G.gen == plan_gen[lev] && G.batched == (int)batched;
+    for (int k = 0; k < 6 && ok; ++k) ok = G.ptrs[k] == ptrs[k];
+    if (ok) return;
+    HPROF("graph_capture3");
+    G.reset();
+    const Substep3* ds = d_sub + lev;
+    const double t = node[lgrids[lev][0]].time, dt = possk[lev];
+    for (int part = 0; part < 2; ++part) {
+      cudaGraph_t g = nullptr;
+      const long long k0 = nkernels;
+      AMR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      if (part == 0) launch_pre(lev, t, dt, ds);
+      else launch_post(lev, t, dt, ds, false);
+      AMR_CUDA(cudaStreamEndCapture(st, &g));
+      AMR_CUDA(cudaGraphInstantiate(part == 0 ? &G.pre : &G.post, g, 0));
+      AMR_CUDA(cudaGraphDestroy(g));
+      (part == 0 ? G.kpre : G.kpost) = nkernels - k0;
+      nkernels = k0;
+    }
+    G.gen = plan_gen[lev]; G.batched = (int)batched;
+    for (int k = 0; k < 6; ++k) G.ptrs[k] = ptrs[k];
+    ++graph_captures;
+  }
+
+  // advanc.f:4-139 with par_advanc (:166-303): the level substep, batched (every patch of
+  // the level in one launch per routine) or plain (the reference's per-grid launches),
+  // launched directly or replayed from captured graphs
   double advanc(int lev) {
     HPROF("advanc3");
     ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP);
@@ -1164,87 +1334,24 @@ class Amr3Gpu : public AmrSolver {
     const double t = node[lgrids[lev][0]].time;
     const double dt = possk[lev];
     tph.next("adv_launch");
-    Step3Args a{};
-    a.pool = pool.d; a.patches = d_patches.d; a.sp = sp;
-    a.stash = d_stash.d; a.stash_stride = L.slots; a.flux = d_flux.d; a.flux_stride = L.faces;
-    a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.dz = hzposs[lev]; a.cflmax = d_cfl;
-    const bool kids = lev + 1 <= p.mxnest && lstart[lev + 1] != 0;
-    if (batched) {
-      // every patch of the level in one launch per routine
-      bound_level(lev, t);
-      if (kids) { SrcMode M{}; run_prog(L.saveqc, M); }
-      if (lev > 1 && L.nseg > 0) {
-        launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.nseg, sp, nvar, hxposs[lev], hyposs[lev], hzposs[lev], dt, st, f32);
-        ++nkernels;
-      }
+    if (use_graphs) {
+      ensure_graphs(lev);
+      Substep3& h = h_sub[lev];
+      h.modes = modes_for(lev, t); h.dt = dt; h.b4c = vel_period > 0.0 ? b4step_factor(t) : 1.0;
+      AMR_CUDA(cudaMemcpyAsync(d_sub + lev, &h, sizeof(Substep3), cudaMemcpyHostToDevice, st));
+      AMR_CUDA(cudaGraphLaunch(lgraph[lev].pre, st));
       sample_gauges(lev);
-      AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
-      if (vel_period > 0.0) {
-        launch_b4step3(pool.d, d_patches.d, L.d_plist.d, (int)L.plist.size(), p.naux, max_enlarged(lev), b4step_factor(t), st, f32);
-        ++nkernels;
-      }
       if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
-      a.plist = L.d_plist.d; a.np = (int)L.plist.size();
-      a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
-      launch_step3(a, L.items, L.faces, L.cells, st, f32);
-      nkernels += 5;
+      AMR_CUDA(cudaGraphLaunch(lgraph[lev].post, st));
       if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
-      if (!L.fsv.empty()) {
-        launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st, f32);
-        ++nkernels;
-      }
-      if (lev > 1 && L.nseg > 0) {
-        launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d, (int)L.nseg, nvar, dt, hxposs[lev], hyposs[lev], hzposs[lev], st, f32);
-        ++nkernels;
-      }
+      nkernels += lgraph[lev].kpre + lgraph[lev].kpost;
+      graph_replays += 2;
     } else {
-      // the reference's per-grid structure (advanc.f): bound for every grid, saveqc for the
-      // level, then par_advanc per grid (qad, stepgrid, fluxsv, fluxad), each grid its own
-      // launches; the per-grid arrays are views of the level's
-      const int np = (int)L.plist.size();
-      const SrcMode M = modes_for(lev, t);
-      for (int k = 0; k < np; ++k) run_prog_owner(L.bound, M, k);
-      if (kids) { SrcMode Z{}; run_prog(L.saveqc, Z); }
+      launch_pre(lev, t, dt, nullptr);
       sample_gauges(lev);
-      AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
-      if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
-      build_plain_views(L);
-      const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
-      for (int k = 0; k < np; ++k) {
-        const long long q0 = L.seg0[k], nq = L.seg0[k + 1] - L.seg0[k];
-        if (lev > 1 && nq > 0) {
-          launch_qad3(pool.d, regs.d, d_patches.d, L.d_qad.d + q0, (int)nq, sp, nvar, hx, hy, hz, dt, st, f32);
-          ++nkernels;
-        }
-        if (vel_period > 0.0) {
-          const int m = L.plist[k];
-          launch_b4step3(pool.d, d_patches.d, L.d_plist.d + k, 1, p.naux, (long long)mitot(m) * mjtot(m) * mktot(m),
-                         b4step_factor(t), st, f32);
-          ++nkernels;
-        }
-        Step3Args b = a;
-        b.plist = L.d_plist.d + k; b.np = 1;
-        b.sweep0 = d_pp_sweep.d + (size_t)12 * k; b.comp0 = d_pp_sweep.d + (size_t)12 * k + 6;
-        b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
-        long long it[3];
-        for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
-        launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
-        nkernels += 5;
-        const long long f0 = L.fsv0[k], nf = L.fsv0[k + 1] - L.fsv0[k];
-        if (nf > 0) {
-          launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d + f0, (int)nf, nvar, dt, hx, hy, hz, st, f32);
-          ++nkernels;
-        }
-        if (lev > 1 && nq > 0) {
-          launch_fad3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fad.d + q0, (int)nq, nvar, dt, hx, hy, hz, st, f32);
-          ++nkernels;
-        }
-      }
-      if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
+      launch_post(lev, t, dt, nullptr, profile);
     }
-    flip_level(lev);
-    // into pinned memory, so the copy is queued and the host goes on compiling
-    AMR_CUDA(cudaMemcpyAsync(h_cfl, d_cfl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    for (int m : lgrids[lev]) { node[m].cur ^= 1; h_patches[m].cur = node[m].cur; }
     tph.next("adv_sync");
     sync_stream();
     const unsigned long long cbits = *h_cfl;
@@ -1269,26 +1376,6 @@ class Amr3Gpu : public AmrSolver {
   }
   // one-patch views of the sweep prefixes for the plain path, 12 per patch:
   // stash slots [x0, x1, y0, y1, z0, z1], then interfaces [x0, x1, y0, y1, z0, z1]
-  std::vector<long long> pp_sweep;
-  DBuf<long long> d_pp_sweep;
-  void build_plain_views(Plan3& L) {
-    const int np = (int)L.plist.size();
-    pp_sweep.assign((size_t)12 * np, 0);
-    for (int k = 0; k < np; ++k)
-      for (int d = 0; d < 3; ++d) {
-        pp_sweep[(size_t)12 * k + 2 * d] = L.sweep0[(size_t)d * (np + 1) + k];
-        pp_sweep[(size_t)12 * k + 2 * d + 1] = L.sweep0[(size_t)d * (np + 1) + k + 1];
-        pp_sweep[(size_t)12 * k + 6 + 2 * d] = L.comp0[(size_t)d * (np + 1) + k];
-        pp_sweep[(size_t)12 * k + 6 + 2 * d + 1] = L.comp0[(size_t)d * (np + 1) + k + 1];
-      }
-    d_pp_sweep.upload(pp_sweep, st, stg);
-  }
-  // the new values were written to the other buffer: swap store1 / store2 of every patch of the level
-  void flip_level(int lev) {
-    for (int m : lgrids[lev]) { node[m].cur ^= 1; h_patches[m].cur = node[m].cur; }
-    launch_flip(d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), st);
-    ++nkernels;
-  }
 
   // update.f:4-192 (upbnd then averaging)
   void update(int lev) {
@@ -1750,6 +1837,8 @@ class Amr3Gpu : public AmrSolver {
     AMR_CUDA(cudaMalloc(&d_cfl, sizeof(unsigned long long)));
     AMR_CUDA(cudaMallocHost((void**)&h_cfl, sizeof(unsigned long long)));
     AMR_CUDA(cudaMalloc(&d_mass, sizeof(double)));
+    AMR_CUDA(cudaMalloc(&d_sub, sizeof(Substep3) * 12));
+    AMR_CUDA(cudaMallocHost((void**)&h_sub, sizeof(Substep3) * 12));
     stg.reserve((size_t)256 << 20);
     {
       // sweep staging and face fluxes: reserved at once for twice a level-1 sweep
@@ -1990,6 +2079,10 @@ class Amr3Gpu : public AmrSolver {
   int num_dim() const override { return 3; }
   void set_batched(bool on) override { batched = on; }
   void set_profile(bool on) override { profile = on; }
+  void set_graphs(bool on) override {
+    use_graphs = on;
+    if (!on) for (auto& G : lgraph) G.reset();
+  }
   void run(int mc) override { max_cycles = mc; tick(); }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > lfine) throw std::runtime_error("level out of range");
@@ -2018,7 +2111,7 @@ class Amr3Gpu : public AmrSolver {
   std::vector<double> info() override {
     return {time, rvol, (double)ncycle, (double)lfine, t_step, t_regrid, tmass0, cflmax_run, (double)nkernels, (double)pool.peak * 8.0,
             (double)nsteps_launched, step_kernel_ms, step_kernel_cells, last_run_ms, run_cells, finished() ? 1.0 : 0.0, h2d_bytes,
-            0, 0, 0, 0, 0, 0, 3.0, f32 ? 32.0 : 64.0};
+            0, 0, 0, 0, 0, 0, 3.0, f32 ? 32.0 : 64.0, (double)graph_captures, (double)graph_replays};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;

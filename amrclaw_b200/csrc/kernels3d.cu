@@ -165,10 +165,11 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   const bool valid = g >= first && g < last;
   const Step3Params sp = A.sp;
   const double dn = DIR == 1 ? A.dx : DIR == 2 ? A.dy : A.dz;
-  const T dtdx = (T)(A.dt / dn);
+  const double dt = A.dt_dev ? *A.dt_dev : A.dt;
+  const T dtdx = (T)(dt / dn);
   // transverse steps of flux3's dtdy / dtdz arguments for this sweep (step3.f:192, 300, 416)
-  const T dtdy = (T)(DIR == 1 ? A.dt / A.dy : DIR == 2 ? A.dt / A.dz : A.dt / A.dx);
-  const T dtdz = (T)(DIR == 1 ? A.dt / A.dz : DIR == 2 ? A.dt / A.dx : A.dt / A.dy);
+  const T dtdy = (T)(DIR == 1 ? dt / A.dy : DIR == 2 ? dt / A.dz : dt / A.dx);
+  const T dtdz = (T)(DIR == 1 ? dt / A.dz : DIR == 2 ? dt / A.dx : dt / A.dy);
   int e = -1, n1 = 0;
   long long slot = 0;  // stash slot of pencil cell e (meaningful for e in 1..n1+1)
   PH ph;
@@ -551,7 +552,8 @@ template <class T, int NV>
 __global__ void __launch_bounds__(256) update3_kernel(Step3Args A) {
   const long long first = A.cell0[0], total = A.cell0[A.np];
   const long long fs = A.flux_stride;
-  const T dtdx = (T)(A.dt / A.dx), dtdy = (T)(A.dt / A.dy), dtdz = (T)(A.dt / A.dz);
+  const double dt = A.dt_dev ? *A.dt_dev : A.dt;
+  const T dtdx = (T)(dt / A.dx), dtdy = (T)(dt / A.dy), dtdz = (T)(dt / A.dz);
   for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int pi = find_patch(A.cell0, A.np, t);
     const PatchDev& P = A.patches[A.plist[pi]];
@@ -579,9 +581,10 @@ __global__ void __launch_bounds__(256) update3_kernel(Step3Args A) {
 // fluxsv.f:4-94: one register entry per thread
 template <class T>
 __global__ void fsv3_kernel(const T* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
-                            const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz) {
+                            const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, const double* dt_dev) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
+  if (dt_dev) dtc = *dt_dev;
   const Fsv3 E = e[t];
   const PatchDev& P = patches[E.patch];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
@@ -601,9 +604,10 @@ __global__ void fsv3_kernel(const T* flux, long long fs, const long long* face0,
 // fluxad.f:4-155: one coarse face (register) of a fine patch per thread
 template <class T>
 __global__ void fad3_kernel(const T* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs,
-                            const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz) {
+                            const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz, const double* dt_dev) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
+  if (dt_dev) dtf = *dt_dev;
   const Fad3 E = e[t];
   const PatchDev& P = patches[E.patch];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
@@ -641,9 +645,10 @@ __global__ void fad3_kernel(const T* flux, long long fs, const long long* face0,
 // qad.f:4-534: one register of one side of a fine patch per thread
 template <class T>
 __global__ void qad3_kernel(T* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
-                            int nvar, double hx, double hy, double hz, double delt) {
+                            int nvar, double hx, double hy, double hz, double delt, const double* dt_dev) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= njobs) return;
+  if (dt_dev) delt = *dt_dev;
   const Qad3Job J = jobs[t];
   const PatchDev& P = patches[J.patch];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
@@ -703,9 +708,10 @@ __global__ void qad3_kernel(T* pool, double* regs, const PatchDev* patches, cons
 // plus the position l along the coarse face, qad.f:186-193, 245-252, 506-513).
 template <class T>
 __global__ void qad3_swirl_kernel(T* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs,
-                                  double hx, double hy, double hz, double delt) {
+                                  double hx, double hy, double hz, double delt, const double* dt_dev) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= njobs) return;
+  if (dt_dev) delt = *dt_dev;
   const Qad3Job J = jobs[t];
   const PatchDev& P = patches[J.patch];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
@@ -751,9 +757,10 @@ __global__ void qad3_swirl_kernel(T* pool, double* regs, const PatchDev* patches
 // b4step3 of the time-modulated swirl: aux = aux0 * c over the enlarged patches of plist
 // (aux0, the setaux values, sits right after aux in the pool)
 template <class T>
-__global__ void b4step3_kernel(T* pool, const PatchDev* patches, const int* plist, int np, int naux, double c) {
+__global__ void b4step3_kernel(T* pool, const PatchDev* patches, const int* plist, int np, int naux, double c, const double* c_dev) {
   const int pi = blockIdx.y;
   if (pi >= np) return;
+  if (c_dev) c = *c_dev;
   const PatchDev& P = patches[plist[pi]];
   const long long n = (long long)naux * P.mitot * P.mjtot * P.mktot;
   T* a = pool + P.aux;
@@ -816,7 +823,10 @@ __global__ void fill3_kernel(Fill3Args a) {
     const long long sp = (long long)S.mitot * S.mjtot * S.mktot;
     const long long sk = ((long long)(o.sk0 + kc) * S.mjtot + (o.sj0 + jb)) * S.mitot + (o.si0 + ia);
     int mode = 0; double ai = 1.0, ac = 0.0;
-    if (o.level >= 0) { mode = a.modes.mode[o.level]; ai = a.modes.alphai[o.level]; ac = a.modes.alphac[o.level]; }
+    if (o.level >= 0) {
+      const SrcMode& M = a.modes_dev ? *a.modes_dev : a.modes;
+      mode = M.mode[o.level]; ai = M.alphai[o.level]; ac = M.alphac[o.level];
+    }
     const T* qn = pool + S.q[S.cur];
     const T* qo = pool + S.q[1 - S.cur];
     for (int m = 0; m < nvar; ++m) {
@@ -1097,30 +1107,30 @@ void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const
 }
 
 void launch_fsv3(const void* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fsv3* e, int n,
-                 int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s, bool f32) {
+                 int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s, bool f32, const double* dt_dev) {
   if (n <= 0) return;
-  if (f32) fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const float*>(flux), fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz);
-  else fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const double*>(flux), fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz);
+  if (f32) fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const float*>(flux), fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz, dt_dev);
+  else fsv3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const double*>(flux), fs, face0, patches, regs, e, n, nvar, dtc, hx, hy, hz, dt_dev);
   AMR_CUDA(cudaGetLastError());
 }
 void launch_fad3(const void* flux, long long fs, const long long* face0, const PatchDev* patches, double* regs, const Fad3* e, int n,
-                 int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s, bool f32) {
+                 int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s, bool f32, const double* dt_dev) {
   if (n <= 0) return;
-  if (f32) fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const float*>(flux), fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz);
-  else fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const double*>(flux), fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz);
+  if (f32) fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const float*>(flux), fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz, dt_dev);
+  else fad3_kernel<<<(n + 127) / 128, 128, 0, s>>>(static_cast<const double*>(flux), fs, face0, patches, regs, e, n, nvar, dtf, hx, hy, hz, dt_dev);
   AMR_CUDA(cudaGetLastError());
 }
 void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp, int nvar,
-                 double hx, double hy, double hz, double delt, cudaStream_t s, bool f32) {
+                 double hx, double hy, double hz, double delt, cudaStream_t s, bool f32, const double* dt_dev) {
   if (njobs <= 0) return;
   if (sp.solver == SOLVER3_SWIRL) {
-    if (f32) qad3_swirl_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, hx, hy, hz, delt);
-    else qad3_swirl_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, hx, hy, hz, delt);
+    if (f32) qad3_swirl_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, hx, hy, hz, delt, dt_dev);
+    else qad3_swirl_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, hx, hy, hz, delt, dt_dev);
     AMR_CUDA(cudaGetLastError());
     return;
   }
-  if (f32) qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
-  else qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt);
+  if (f32) qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt, dt_dev);
+  else qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt, dt_dev);
   AMR_CUDA(cudaGetLastError());
 }
 // valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
@@ -1149,13 +1159,13 @@ void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, in
   AMR_CUDA(cudaGetLastError());
 }
 void launch_b4step3(void* pool, const PatchDev* patches, const int* plist, int np, int naux, long long max_cells, double c,
-                    cudaStream_t s, bool f32) {
+                    cudaStream_t s, bool f32, const double* c_dev) {
   if (np <= 0) return;
   const int bx = (int)std::max<long long>(1, std::min<long long>((naux * max_cells + 255) / 256, 1024));
   for (int base = 0; base < np; base += 65535) {
     const int cnt = std::min(65535, np - base);
-    if (f32) b4step3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<float*>(pool), patches, plist + base, cnt, naux, c);
-    else b4step3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<double*>(pool), patches, plist + base, cnt, naux, c);
+    if (f32) b4step3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<float*>(pool), patches, plist + base, cnt, naux, c, c_dev);
+    else b4step3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<double*>(pool), patches, plist + base, cnt, naux, c, c_dev);
   }
   AMR_CUDA(cudaGetLastError());
 }

@@ -39,6 +39,7 @@ struct Step3Args {
   void* flux;                // [6 comps][meqn][face cells]
   long long flux_stride;     // face cells of the level
   double dt, dx, dy, dz;
+  const double* dt_dev;      // if set, the time step is read here (a captured graph replays the launch)
   unsigned long long* cflmax;
   Step3Params sp;
 };
@@ -77,6 +78,7 @@ struct Fill3Args {
   const Fill3Chunk* chunks; int nchunks;
   int nvar;
   SrcMode modes;
+  const SrcMode* modes_dev;  // if set, the time-interpolation modes are read here (captured graphs)
   LevelConst lc;
   double xlower, ylower, zlower;
 };
@@ -95,18 +97,21 @@ void launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], lon
 // register segments (lenbc) of the patches in plist (0 for patches without registers).
 void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,
                            long long total, Fad3* fad, Qad3Job* qad, cudaStream_t s);
+// dt_dev / c_dev: if set, the scalar is read from device memory instead (captured graphs)
 void launch_fsv3(const void* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
-                 const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s, bool f32);
+                 const Fsv3* e, int n, int nvar, double dtc, double hx, double hy, double hz, cudaStream_t s, bool f32,
+                 const double* dt_dev = nullptr);
 void launch_fad3(const void* flux, long long flux_stride, const long long* face0, const PatchDev* patches, double* regs,
-                 const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s, bool f32);
+                 const Fad3* e, int n, int nvar, double dtf, double hx, double hy, double hz, cudaStream_t s, bool f32,
+                 const double* dt_dev = nullptr);
 void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
-                 int nvar, double hx, double hy, double hz, double delt, cudaStream_t s, bool f32);
+                 int nvar, double hx, double hy, double hz, double delt, cudaStream_t s, bool f32, const double* dt_dev = nullptr);
 // valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
 void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32);
 // b4step3 of the time-modulated swirl: aux = c * aux0 over the enlarged patches of plist
 // (max_cells: the largest enlarged patch)
 void launch_b4step3(void* pool, const PatchDev* patches, const int* plist, int np, int naux, long long max_cells, double c,
-                    cudaStream_t s, bool f32);
+                    cudaStream_t s, bool f32, const double* c_dev = nullptr);
 void launch_fill3(const Fill3Args& a, cudaStream_t s, bool f32);
 void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s, bool f32);
 void launch_upbnd3(void* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,

@@ -341,19 +341,30 @@ def main():
         launches = int(i1["kernels"] - i0["kernels"])
         step_launches = int(i1["substeps"] - i0["substeps"])
 
-        # ---------------- plain per-patch path on the same steps
-        p = Solver(d, batched=False)
-        p.run(args.warmup)
-        pms = 0.0
-        pcells = 0.0
-        for _ in range(args.steps):
-            flush_l2(flush)
-            p.run(1)
+        # ---------------- plain per-patch path on the same steps, and both paths replayed
+        # from captured CUDA graphs (3D)
+        def leg(batched, graphs):
+            p = Solver(d, batched=batched, graphs=graphs)
+            p.run(args.warmup)
+            pms = 0.0
+            pcells = 0.0
+            for _ in range(args.steps):
+                flush_l2(flush)
+                p.run(1)
+                inf = p.info()
+                pms += inf["last_run_ms"]
+                pcells += inf["last_run_cells"]
             inf = p.info()
-            pms += inf["last_run_ms"]
-            pcells += inf["last_run_cells"]
-        p.close()
-        plain_value = pcells / (pms * 1e-3)
+            p.close()
+            return pcells / (pms * 1e-3), pms / args.steps, inf
+
+        plain_value, plain_ms, _ = leg(False, False)
+        graph_legs = {}
+        if ndim == 3:
+            for name, b in (("plain_graphs", False), ("batched_graphs", True)):
+                v, m, inf = leg(b, True)
+                graph_legs[name] = {"value": v, "unit": "cell-updates/s", "ms_per_step": m,
+                                    "graph_captures": inf["graph_captures"], "graph_replays": inf["graph_replays"]}
 
         # ---------------- end to end through the C ABI: data files in, the whole solve to tfinal,
         # level-1 mass read back after every coarse step, final cell values read back
@@ -413,8 +424,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded initial conditions of the workload",
         "config": dict(cfg, l2="flushed between steps (256 MB write)", parallelism="replicas" if world > 1 else "single"),
-        "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": pms / args.steps,
+        "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": plain_ms,
                   "speedup_batched_over_plain": value / plain_value if plain_value else None},
+        "graphs": graph_legs or None,
         "l1_err_vs_fp64": 0.0,
         "fp32_form": fp32,
         "serving": serving,

@@ -45,6 +45,15 @@ int amrgpu_init_precision(const char* rundir, const char* outdir, int write_outp
  * 0: one launch per patch (plain per-patch path). */
 int amrgpu_set_batched(amrgpu_ctx* ctx, int batched);
 
+/* 1: capture each level substep of the 3D path as two CUDA graphs (ghost fill, saveqc,
+ * qad; then CFL reset, b4step3, the step kernels, fluxsv/fluxad, the store swap and the
+ * CFL read-back) and replay them, re-capturing when a regrid changes the level's plans;
+ * the per-substep scalars (dt, time-interpolation weights, the b4step3 factor) are
+ * copied to the device before each replay. Results are identical to direct launches.
+ * 0: launch directly (default). 2D contexts reject 1 (AMRGPU_EINVAL). No counterpart in
+ * the reference. */
+int amrgpu_set_graphs(amrgpu_ctx* ctx, int on);
+
 /* 1: record CUDA events around every patch-step launch (kernel time is then
  * reported by amrgpu_info); 0: no per-launch events. */
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on);
@@ -94,8 +103,8 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
  * amrgpu_run call, cell updates of that call, 1 when tfinal was reached,
  * bytes of initial data copied host to device, then regrid seconds spent in:
  * device flagging, host flag processing, clustering, new-grid fill, register
- * and list set-up, device-program compilation, then the number of space dimensions
- * and the precision in bits (64 or 32). */
+ * and list set-up, device-program compilation, then the number of space dimensions,
+ * the precision in bits (64 or 32), and (3D) the CUDA graphs captured and replayed. */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 
 /* Hierarchy rows in output order (valout.f90 loop order): (grid_number, level,

@@ -16,7 +16,7 @@ from oracle.pyoracle import Oracle3D
 pytestmark = pytest.mark.gpu
 
 
-def _both(rd, batched=True, max_cycles=0, split=None):
+def _both(rd, batched=True, max_cycles=0, split=None, graphs=False):
     from amrclaw_b200 import Solver
     with tempfile.TemporaryDirectory() as d:
         rd.write(d)
@@ -25,7 +25,7 @@ def _both(rd, batched=True, max_cycles=0, split=None):
         ref = dict(grids=o.grids(), values=o.values(), gauges=o.gauges(5), time=o.time(), mass=o.mass(),
                    cells=o.cell_updates())
         o.close()
-        with Solver(d, batched=batched) as s:
+        with Solver(d, batched=batched, graphs=graphs) as s:
             assert s.num_dim == 3
             if split:
                 for _ in range(max_cycles // split):
@@ -89,3 +89,15 @@ def test_split_run_equals_one_run():
     rd = configs.euler_blast(n=16, levels=3, tfinal=10.0, max1d=20)
     ref, gpu = _both(rd, max_cycles=6, split=2)
     _assert_identical(ref, gpu)
+
+
+@pytest.mark.parametrize("batched", [True, False])
+def test_cuda_graph_replay_is_identical(batched):
+    """Level substeps replayed from captured CUDA graphs (scalars read from device memory)
+    give the same results as direct launches; graphs are re-captured after regrids and
+    reused in between."""
+    rd = _with_gauges(configs.euler_blast(n=16, levels=3, tfinal=0.1, max1d=16))
+    ref, gpu = _both(rd, batched=batched, graphs=True)
+    _assert_identical(ref, gpu)
+    assert gpu["info"]["graph_captures"] > 0
+    assert gpu["info"]["graph_replays"] > 2 * gpu["info"]["graph_captures"]

@@ -25,7 +25,7 @@ L1_REL_TOL = 1e-5
 MASS_REL_TOL = 1e-6
 
 
-def _run(rd, batched=True, precision="fp64", gauge_rows_of=0):
+def _run(rd, batched=True, precision="fp64", gauge_rows_of=0, graphs=False):
     from amrclaw_b200 import Solver
     with tempfile.TemporaryDirectory() as d:
         rd.write(d)
@@ -34,7 +34,7 @@ def _run(rd, batched=True, precision="fp64", gauge_rows_of=0):
         ref = dict(grids=o.grids(), values=o.values(), gauges=o.gauges(gauge_rows_of or 1), time=o.time(), mass=o.mass(),
                    cells=o.cell_updates())
         o.close()
-        with Solver(d, batched=batched, precision=precision) as s:
+        with Solver(d, batched=batched, precision=precision, graphs=graphs) as s:
             s.run(0)
             gpu = dict(grids=s.grids(), values=s.values(), gauges=s.gauges(gauge_rows_of or 1), info=s.info(), mass=s.mass())
     return ref, gpu
@@ -65,6 +65,14 @@ def test_sphere_in_the_modulated_field_three_levels():
     ref, gpu = _run(rd, gauge_rows_of=1)
     _assert_identical(ref, gpu)
     assert (gpu["grids"][:, 1] == 3).any()
+
+
+def test_modulated_field_replayed_from_cuda_graphs():
+    """The b4step3 factor, dt and the fill weights reach the replayed graphs from device memory."""
+    rd = problems.advection_swirl3d(n=16, levels=3, tfinal=0.3, max1d=16)
+    ref, gpu = _run(rd, graphs=True)
+    _assert_identical(ref, gpu)
+    assert gpu["info"]["graph_replays"] > 0
 
 
 def test_plain_per_patch_path_matches_batched():
