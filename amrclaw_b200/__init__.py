@@ -33,7 +33,7 @@ class Solver:
     """One AMR run on the GPU (the reference's ``amr2`` program from init to tfinal)."""
 
     def __init__(self, rundata_or_dir, outdir: str | None = None, write_output: bool = False, batched: bool = True,
-                 precision: str = "fp64", graphs: bool = False):
+                 precision: str = "fp64", graphs: bool = False, schedule: int = 0):
         self._lib = _lib.load()
         if isinstance(rundata_or_dir, ClawRunData):
             self._tmp = tempfile.TemporaryDirectory(prefix="amrgpu_")
@@ -54,6 +54,8 @@ class Solver:
                "amrgpu_init")
         self._h = h
         self.set_batched(batched)
+        if schedule:
+            self.set_schedule(schedule)
         if graphs:
             self.set_graphs(True)
 
@@ -63,6 +65,10 @@ class Solver:
     def set_graphs(self, on: bool) -> None:
         """Replay each level substep from captured CUDA graphs (3D path)."""
         _check(self._lib, self._lib.amrgpu_set_graphs(self._h, int(on)), "amrgpu_set_graphs")
+
+    def set_schedule(self, schedule: int) -> None:
+        """Sweep schedule of the batched 3D path: 0 autotune, 1 per direction, 2 work queue."""
+        _check(self._lib, self._lib.amrgpu_set_schedule(self._h, int(schedule)), "amrgpu_set_schedule")
 
     def set_profile(self, on: bool) -> None:
         _check(self._lib, self._lib.amrgpu_set_profile(self._h, int(on)), "amrgpu_set_profile")
@@ -103,7 +109,8 @@ class Solver:
                 "cflmax", "kernels", "pool_peak_bytes", "substeps", "step_kernel_ms", "step_kernel_cells",
                 "last_run_ms", "last_run_cells", "finished", "h2d_bytes",
                 "regrid_flags_s", "regrid_hostflags_s", "regrid_cluster_s", "regrid_fill_s", "regrid_prep_s", "regrid_compile_s",
-                "num_dim", "precision_bits", "graph_captures", "graph_replays"]
+                "num_dim", "precision_bits", "graph_captures", "graph_replays", "levels_tuned_queue",
+                "levels_tuned_per_direction"]
         out = (ctypes.c_double * len(keys))()
         _check(self._lib, self._lib.amrgpu_info(self._h, out, len(keys)), "amrgpu_info")
         return dict(zip(keys, list(out)))

@@ -2029,6 +2029,9 @@ class Solver2 : public AmrSolver {
   void set_graphs(bool on) override {
     if (on) throw std::runtime_error("amrgpu_set_graphs: CUDA-graph replay is built for the 3D path");
   }
+  void set_schedule(int s) override {
+    if (s != 0) throw std::runtime_error("amrgpu_set_schedule: sweep schedules are built for the 3D path");
+  }
   void run(int max_cycles) override { g.max_cycles = max_cycles; g.tick(); }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > g.lfine) throw std::runtime_error("level out of range");
@@ -2058,7 +2061,7 @@ class Solver2 : public AmrSolver {
     return {g.time, g.rvol, (double)g.ncycle, (double)g.lfine, g.t_step, g.t_regrid, g.tmass0,
             g.cflmax_run, (double)g.nkernels, (double)g.pool.peak * 8.0, (double)g.nsteps_launched,
             g.step_kernel_ms, g.step_kernel_cells, g.last_run_ms, g.run_cells, g.finished() ? 1.0 : 0.0, g.h2d_bytes,
-            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0, 0.0, 0.0};
+            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0, 0.0, 0.0, 0.0, 0.0};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;
@@ -2152,6 +2155,11 @@ int amrgpu_set_batched(amrgpu_ctx* ctx, int batched) {
 int amrgpu_set_graphs(amrgpu_ctx* ctx, int on) {
   if (!ctx) return AMRGPU_EINVAL;
   return guarded([&] { ctx->s->set_graphs(on != 0); });
+}
+
+int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule) {
+  if (!ctx) return AMRGPU_EINVAL;
+  return guarded([&] { ctx->s->set_schedule(schedule); });
 }
 
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on) {

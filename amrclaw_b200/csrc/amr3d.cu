@@ -212,6 +212,8 @@ class Amr3Gpu : public AmrSolver {
     if (st) cudaStreamSynchronize(st);
     for (auto& G : lgraph) G.reset();
     if (d_sub) cudaFree(d_sub);
+    if (d_queue) cudaFree(d_queue);
+    for (cudaEvent_t e : {ev_t0, ev_t1}) if (e) cudaEventDestroy(e);
     if (h_sub) cudaFreeHost(h_sub);
     for (auto& L : plan) L.free_dev();
     newfill.free_dev();
@@ -1198,8 +1200,44 @@ class Amr3Gpu : public AmrSolver {
   };
   LevelGraph lgraph[12];
   bool use_graphs = false;
+  int tune_pending = -1;  // the schedule timed in the substep in flight
+  // Sweep schedule of the batched path: per-direction launches (one block per tile) or
+  // one persistent work-queue launch over the tiles of all three directions. schedule 0
+  // autotunes per level: the level's first substeps alternate the two (step kernels timed
+  // with events, per cell-update) until each has TUNE_RUNS samples, then the faster one is
+  // kept. 1 and 2 force one schedule. Results are identical under either.
+  static constexpr int TUNE_RUNS = 2;
+  int schedule = 0;
+  struct Tune { int runs[2] = {0, 0}; double ns_per_cell[2] = {0, 0}; int choice = -1; };
+  Tune tune[12];
+  unsigned int* d_queue = nullptr;
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+  // the schedule of level lev's next substep (0: per direction, 1: queue), and whether to time it
+  int pick_schedule(int lev, bool& timed) {
+    timed = false;
+    if (schedule == 1) return 0;
+    if (schedule == 2) return 1;
+    Tune& T = tune[lev];
+    if (T.choice >= 0) return T.choice;
+    if (use_graphs) return 0;  // captured untuned: per direction, the faster on the Euler blast
+    timed = true;
+    return T.runs[1] <= T.runs[0] ? 1 : 0;
+  }
+  void tune_record(int lev, int sched, double cells) {
+    float ms = 0;
+    AMR_CUDA(cudaEventElapsedTime(&ms, ev_t0, ev_t1));
+    Tune& T = tune[lev];
+    T.ns_per_cell[sched] += 1e6 * ms / std::max(cells, 1.0);
+    if (++T.runs[sched] >= TUNE_RUNS && T.runs[1 - sched] >= TUNE_RUNS)
+      T.choice = T.ns_per_cell[1] <= T.ns_per_cell[0] ? 1 : 0;
+  }
   long long plan_gen[12] = {0};
   long long graph_captures = 0, graph_replays = 0;
+  int tune_choices(int which) const {
+    int n = 0;
+    for (const Tune& T : tune) n += T.choice == which;
+    return n;
+  }
 
   // the launches before the gauge sampling (ds: read dt and the fill modes from there)
   void launch_pre(int lev, double t, double dt, const Substep3* ds) {
@@ -1243,8 +1281,13 @@ class Amr3Gpu : public AmrSolver {
       if (timed) AMR_CUDA(cudaEventRecord(ev_a, st));
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
       a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
-      launch_step3(a, L.items, L.faces, L.cells, st, f32);
-      nkernels += 5;
+      bool tt = false;
+      const int sched = pick_schedule(lev, tt);
+      if (ds) tt = false;  // captured into a graph: replayed untimed
+      a.queue = sched == 1 ? d_queue : nullptr;
+      if (tt) AMR_CUDA(cudaEventRecord(ev_t0, st));
+      nkernels += launch_step3(a, L.items, L.faces, L.cells, st, f32);
+      if (tt) { AMR_CUDA(cudaEventRecord(ev_t1, st)); tune_pending = sched; }
       if (timed) AMR_CUDA(cudaEventRecord(ev_b, st));
       if (!L.fsv.empty()) {
         launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hx, hy, hz, st, f32, dtd);
@@ -1276,8 +1319,7 @@ class Amr3Gpu : public AmrSolver {
         b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
         long long it[3];
         for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
-        launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
-        nkernels += 5;
+        nkernels += launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
         const long long f0 = L.fsv0[k], nf = L.fsv0[k + 1] - L.fsv0[k];
         if (nf > 0) {
           launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d + f0, (int)nf, nvar, dt, hx, hy, hz, st, f32, dtd);
@@ -1364,6 +1406,7 @@ class Amr3Gpu : public AmrSolver {
       step_kernel_ms += ms;
       step_kernel_cells += (double)L.cells;
     }
+    if (tune_pending >= 0) { tune_record(lev, tune_pending, (double)L.cells); tune_pending = -1; }
     for (int m : lgrids[lev]) {
       node[m].time = node[m].time + dt;
       const double cells = (double)node[m].nx() * node[m].ny() * node[m].nz();
@@ -1838,6 +1881,8 @@ class Amr3Gpu : public AmrSolver {
     AMR_CUDA(cudaMallocHost((void**)&h_cfl, sizeof(unsigned long long)));
     AMR_CUDA(cudaMalloc(&d_mass, sizeof(double)));
     AMR_CUDA(cudaMalloc(&d_sub, sizeof(Substep3) * 12));
+    AMR_CUDA(cudaMalloc(&d_queue, sizeof(unsigned int)));
+    AMR_CUDA(cudaEventCreate(&ev_t0)); AMR_CUDA(cudaEventCreate(&ev_t1));
     AMR_CUDA(cudaMallocHost((void**)&h_sub, sizeof(Substep3) * 12));
     stg.reserve((size_t)256 << 20);
     {
@@ -2083,6 +2128,12 @@ class Amr3Gpu : public AmrSolver {
     use_graphs = on;
     if (!on) for (auto& G : lgraph) G.reset();
   }
+  void set_schedule(int s) override {
+    if (s < 0 || s > 2) throw std::runtime_error("amrgpu_set_schedule: 0 (autotune), 1 (per direction) or 2 (work queue)");
+    schedule = s;
+    for (auto& T : tune) T = Tune();
+    for (auto& G : lgraph) G.reset();
+  }
   void run(int mc) override { max_cycles = mc; tick(); }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > lfine) throw std::runtime_error("level out of range");
@@ -2111,7 +2162,8 @@ class Amr3Gpu : public AmrSolver {
   std::vector<double> info() override {
     return {time, rvol, (double)ncycle, (double)lfine, t_step, t_regrid, tmass0, cflmax_run, (double)nkernels, (double)pool.peak * 8.0,
             (double)nsteps_launched, step_kernel_ms, step_kernel_cells, last_run_ms, run_cells, finished() ? 1.0 : 0.0, h2d_bytes,
-            0, 0, 0, 0, 0, 0, 3.0, f32 ? 32.0 : 64.0, (double)graph_captures, (double)graph_replays};
+            0, 0, 0, 0, 0, 0, 3.0, f32 ? 32.0 : 64.0, (double)graph_captures, (double)graph_replays,
+            (double)tune_choices(1), (double)tune_choices(0)};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;

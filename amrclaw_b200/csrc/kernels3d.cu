@@ -153,15 +153,15 @@ struct Swirl3Phys {
   }
 };
 
+// one tile of sweep direction DIR; sW: the block's wave buffer [NW*NV][SW_T]
 template <int DIR, class T, class PH>
-__global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
+__device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, T (*sW)[SW_T]) {
   constexpr int NV = PH::NV, NW = PH::NW, ST = stash_values(NV);
-  __shared__ T sW[NW * NV][SW_T];
   const long long* c0 = A.comp0 + (long long)(DIR - 1) * (A.np + 1);
   const long long* s0 = A.sweep0 + (long long)(DIR - 1) * (A.np + 1);
   const long long first = c0[0], last = c0[A.np];
   const int l = threadIdx.x;
-  const long long g = first + (long long)blockIdx.x * SW_OWN - 1 + l;
+  const long long g = first + tile * SW_OWN - 1 + l;
   const bool valid = g >= first && g < last;
   const Step3Params sp = A.sp;
   const double dn = DIR == 1 ? A.dx : DIR == 2 ? A.dy : A.dz;
@@ -417,6 +417,33 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
   // block-wide max of the Courant number, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
   if ((threadIdx.x & 31) == 0 && cfl > T(0)) atomic_max_nonneg(A.cflmax, (double)cfl);
+}
+
+// one launch per direction: a block per tile
+template <int DIR, class T, class PH>
+__global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
+  __shared__ T sW[PH::NW * PH::NV][SW_T];
+  sweep3_tile<DIR, T, PH>(A, blockIdx.x, sW);
+}
+
+// persistent work queue over the tiles of all three directions of the level (x tiles,
+// then y, then z): resident blocks take the next tile from an atomic counter until none
+// is left. The tiles are independent (each writes its own stash slots), so no block
+// waits on another.
+template <class T, class PH>
+__global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_queue_kernel(Step3Args A, unsigned int nx, unsigned int nxy, unsigned int ntot) {
+  __shared__ T sW[PH::NW * PH::NV][SW_T];
+  __shared__ unsigned int item;
+  for (;;) {
+    __syncthreads();  // the previous tile is done with sW and item
+    if (threadIdx.x == 0) item = atomicAdd(A.queue, 1u);
+    __syncthreads();
+    const unsigned int it = item;
+    if (it >= ntot) return;
+    if (it < nx) sweep3_tile<1, T, PH>(A, it, sW);
+    else if (it < nxy) sweep3_tile<2, T, PH>(A, it - nx, sW);
+    else sweep3_tile<3, T, PH>(A, it - nxy, sW);
+  }
 }
 
 // stash element of gadd / hadd for side s (1,2), offset d (-1..1), component m (0..NV-1)
@@ -1079,24 +1106,42 @@ int grid_for(long long n, int block) {
 }  // namespace
 
 template <class T, class PH>
-static void launch_step3_t(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s) {
+static int launch_step3_t(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s) {
   auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
-  if (items[0] > 0) sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, 0, s>>>(a);
-  if (items[1] > 0) sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, 0, s>>>(a);
-  if (items[2] > 0) sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, 0, s>>>(a);
-  AMR_CUDA(cudaGetLastError());
-  if (faces > 0) face3_kernel<T, PH::NV><<<grid_for(faces, 128), 128, 0, s>>>(a);
-  if (cells > 0) update3_kernel<T, PH::NV><<<grid_for(cells, 256), 256, 0, s>>>(a);
-  AMR_CUDA(cudaGetLastError());
-}
-void launch_step3(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s, bool f32) {
-  if (a.sp.solver == SOLVER3_SWIRL) {
-    if (f32) launch_step3_t<float, Swirl3Phys<float>>(a, items, faces, cells, s);
-    else launch_step3_t<double, Swirl3Phys<double>>(a, items, faces, cells, s);
+  int n = 0;
+  if (a.queue) {
+    const unsigned nx = tiles(items[0]), nxy = nx + tiles(items[1]), ntot = nxy + tiles(items[2]);
+    if (ntot > 0) {
+      // as many blocks as are resident at once (the queue hands out the tiles)
+      static const int resident = [] {
+        int dev = 0, sms = 0, per_sm = 0;
+        AMR_CUDA(cudaGetDevice(&dev));
+        AMR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        AMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep3_queue_kernel<T, PH>, SW_T, 0));
+        return std::max(1, sms * per_sm);
+      }();
+      AMR_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned int), s));
+      sweep3_queue_kernel<T, PH><<<std::min<unsigned>(ntot, (unsigned)resident), SW_T, 0, s>>>(a, nx, nxy, ntot);
+      ++n;
+    }
   } else {
-    if (f32) launch_step3_t<float, Euler3Phys<float>>(a, items, faces, cells, s);
-    else launch_step3_t<double, Euler3Phys<double>>(a, items, faces, cells, s);
+    if (items[0] > 0) { sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, 0, s>>>(a); ++n; }
+    if (items[1] > 0) { sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, 0, s>>>(a); ++n; }
+    if (items[2] > 0) { sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, 0, s>>>(a); ++n; }
   }
+  AMR_CUDA(cudaGetLastError());
+  if (faces > 0) { face3_kernel<T, PH::NV><<<grid_for(faces, 128), 128, 0, s>>>(a); ++n; }
+  if (cells > 0) { update3_kernel<T, PH::NV><<<grid_for(cells, 256), 256, 0, s>>>(a); ++n; }
+  AMR_CUDA(cudaGetLastError());
+  return n;
+}
+int launch_step3(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s, bool f32) {
+  if (a.sp.solver == SOLVER3_SWIRL) {
+    if (f32) return launch_step3_t<float, Swirl3Phys<float>>(a, items, faces, cells, s);
+    return launch_step3_t<double, Swirl3Phys<double>>(a, items, faces, cells, s);
+  }
+  if (f32) return launch_step3_t<float, Euler3Phys<float>>(a, items, faces, cells, s);
+  return launch_step3_t<double, Euler3Phys<double>>(a, items, faces, cells, s);
 }
 
 void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,

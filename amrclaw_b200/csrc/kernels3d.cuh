@@ -41,6 +41,7 @@ struct Step3Args {
   double dt, dx, dy, dz;
   const double* dt_dev;      // if set, the time step is read here (a captured graph replays the launch)
   unsigned long long* cflmax;
+  unsigned int* queue;       // if set: the sweeps of all three directions run as one persistent work-queue launch
   Step3Params sp;
 };
 
@@ -92,7 +93,8 @@ struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff;
 // Launch wrappers (kernels3d.cu). f32: the FP32 form (float storage, Riemann solves and
 // flux differencing; FP64 registers, register corrections, averages and totals).
 // interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction.
-void launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s, bool f32);
+// returns the number of kernels launched
+int launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s, bool f32);
 // Builds the level's fluxad/qad work lists on the device: pre[np+1] is the prefix of the
 // register segments (lenbc) of the patches in plist (0 for patches without registers).
 void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,

@@ -13,6 +13,8 @@ class AmrSolver {
   virtual void set_profile(bool on) = 0;
   // replay each level substep from captured CUDA graphs (3D path)
   virtual void set_graphs(bool on) = 0;
+  // sweep schedule of the batched 3D path: 0 autotune, 1 per direction, 2 work queue
+  virtual void set_schedule(int s) = 0;
   virtual void run(int max_cycles) = 0;                    // tick.f
   virtual double level_advance(int level, double* cfl) = 0;  // advanc.f; returns dtnew
   virtual void update_level(int level) = 0;                 // update.f

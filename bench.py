@@ -343,8 +343,8 @@ def main():
 
         # ---------------- plain per-patch path on the same steps, and both paths replayed
         # from captured CUDA graphs (3D)
-        def leg(batched, graphs):
-            p = Solver(d, batched=batched, graphs=graphs)
+        def leg(batched, graphs, schedule=0):
+            p = Solver(d, batched=batched, graphs=graphs, schedule=schedule)
             p.run(args.warmup)
             pms = 0.0
             pcells = 0.0
@@ -365,6 +365,12 @@ def main():
                 v, m, inf = leg(b, True)
                 graph_legs[name] = {"value": v, "unit": "cell-updates/s", "ms_per_step": m,
                                     "graph_captures": inf["graph_captures"], "graph_replays": inf["graph_replays"]}
+            # the batched path's two sweep schedules forced (the value leg autotunes per level)
+            for name, sch in (("batched_per_direction", 1), ("batched_work_queue", 2)):
+                v, m, _ = leg(True, False, sch)
+                graph_legs[name] = {"value": v, "unit": "cell-updates/s", "ms_per_step": m}
+            graph_legs["value_leg_levels_tuned"] = {"work_queue": i1["levels_tuned_queue"],
+                                                    "per_direction": i1["levels_tuned_per_direction"]}
 
         # ---------------- end to end through the C ABI: data files in, the whole solve to tfinal,
         # level-1 mass read back after every coarse step, final cell values read back
@@ -426,7 +432,7 @@ def main():
         "config": dict(cfg, l2="flushed between steps (256 MB write)", parallelism="replicas" if world > 1 else "single"),
         "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": plain_ms,
                   "speedup_batched_over_plain": value / plain_value if plain_value else None},
-        "graphs": graph_legs or None,
+        "schedules": graph_legs or None,
         "l1_err_vs_fp64": 0.0,
         "fp32_form": fp32,
         "serving": serving,

@@ -54,6 +54,14 @@ int amrgpu_set_batched(amrgpu_ctx* ctx, int batched);
  * the reference. */
 int amrgpu_set_graphs(amrgpu_ctx* ctx, int on);
 
+/* Sweep schedule of the batched 3D path. 1: one launch per sweep direction (a block per
+ * tile of 128 interfaces); 2: one persistent work-queue launch in which resident blocks
+ * take the tiles of all three directions from an atomic counter; 0 (default): autotune
+ * per level (the level's first substeps alternate the two, timed with CUDA events per
+ * cell-update, and the faster is kept). Results are identical under every schedule.
+ * 2D contexts accept only 0. No counterpart in the reference. */
+int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule);
+
 /* 1: record CUDA events around every patch-step launch (kernel time is then
  * reported by amrgpu_info); 0: no per-launch events. */
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on);
@@ -104,7 +112,9 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
  * bytes of initial data copied host to device, then regrid seconds spent in:
  * device flagging, host flag processing, clustering, new-grid fill, register
  * and list set-up, device-program compilation, then the number of space dimensions,
- * the precision in bits (64 or 32), and (3D) the CUDA graphs captured and replayed. */
+ * the precision in bits (64 or 32), and (3D) the CUDA graphs captured and replayed and
+ * the number of levels whose autotuned sweep schedule is the work queue, and the number
+ * whose is per direction. */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 
 /* Hierarchy rows in output order (valout.f90 loop order): (grid_number, level,

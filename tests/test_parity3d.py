@@ -16,7 +16,7 @@ from oracle.pyoracle import Oracle3D
 pytestmark = pytest.mark.gpu
 
 
-def _both(rd, batched=True, max_cycles=0, split=None, graphs=False):
+def _both(rd, batched=True, max_cycles=0, split=None, graphs=False, schedule=0):
     from amrclaw_b200 import Solver
     with tempfile.TemporaryDirectory() as d:
         rd.write(d)
@@ -25,7 +25,7 @@ def _both(rd, batched=True, max_cycles=0, split=None, graphs=False):
         ref = dict(grids=o.grids(), values=o.values(), gauges=o.gauges(5), time=o.time(), mass=o.mass(),
                    cells=o.cell_updates())
         o.close()
-        with Solver(d, batched=batched, graphs=graphs) as s:
+        with Solver(d, batched=batched, graphs=graphs, schedule=schedule) as s:
             assert s.num_dim == 3
             if split:
                 for _ in range(max_cycles // split):
@@ -101,3 +101,12 @@ def test_cuda_graph_replay_is_identical(batched):
     _assert_identical(ref, gpu)
     assert gpu["info"]["graph_captures"] > 0
     assert gpu["info"]["graph_replays"] > 2 * gpu["info"]["graph_captures"]
+
+
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_sweep_schedules_are_identical(schedule):
+    """Per-direction sweep launches (1) and the persistent work-queue launch (2) give the
+    oracle's results; the default (0) autotunes between them per level."""
+    rd = _with_gauges(configs.euler_blast(n=16, levels=3, tfinal=0.1, max1d=16))
+    ref, gpu = _both(rd, schedule=schedule)
+    _assert_identical(ref, gpu)
