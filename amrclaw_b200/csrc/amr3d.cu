@@ -1213,16 +1213,18 @@ class Amr3Gpu : public AmrSolver {
   unsigned int* d_queue = nullptr;
   cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
   // the schedule of level lev's next substep (0: per direction, 1: queue), and whether to time it
-  int pick_schedule(int lev, bool& timed) {
+  // (capturing: for a graph, never timed; a level is captured once it is tuned)
+  int pick_schedule(int lev, bool& timed, bool capturing) {
     timed = false;
     if (schedule == 1) return 0;
     if (schedule == 2) return 1;
     Tune& T = tune[lev];
     if (T.choice >= 0) return T.choice;
-    if (use_graphs) return 0;  // captured untuned: per direction, the faster on the Euler blast
+    if (capturing) return 0;
     timed = true;
     return T.runs[1] <= T.runs[0] ? 1 : 0;
   }
+  bool tuned(int lev) const { return schedule != 0 || tune[lev].choice >= 0; }
   void tune_record(int lev, int sched, double cells) {
     float ms = 0;
     AMR_CUDA(cudaEventElapsedTime(&ms, ev_t0, ev_t1));
@@ -1282,8 +1284,7 @@ class Amr3Gpu : public AmrSolver {
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
       a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
       bool tt = false;
-      const int sched = pick_schedule(lev, tt);
-      if (ds) tt = false;  // captured into a graph: replayed untimed
+      const int sched = pick_schedule(lev, tt, ds != nullptr);
       a.queue = sched == 1 ? d_queue : nullptr;
       if (tt) AMR_CUDA(cudaEventRecord(ev_t0, st));
       nkernels += launch_step3(a, L.items, L.faces, L.cells, st, f32);
@@ -1376,7 +1377,8 @@ class Amr3Gpu : public AmrSolver {
     const double t = node[lgrids[lev][0]].time;
     const double dt = possk[lev];
     tph.next("adv_launch");
-    if (use_graphs) {
+    // with graphs, a level's substeps launch directly until its sweep schedule is tuned
+    if (use_graphs && (!batched || tuned(lev))) {
       ensure_graphs(lev);
       Substep3& h = h_sub[lev];
       h.modes = modes_for(lev, t); h.dt = dt; h.b4c = vel_period > 0.0 ? b4step_factor(t) : 1.0;

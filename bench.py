@@ -334,6 +334,8 @@ def main():
         clk = clocks.stop()
         i1 = s.info()
         s.close()
+        batched_regrid_ms = 1e3 * (i1["regrid_seconds"] - i0["regrid_seconds"]) / args.steps
+        batched_advance_ms = 1e3 * (i1["step_seconds"] - i0["step_seconds"]) / args.steps - batched_regrid_ms
         ms, cells = replicas.combine(ms, cells, dist, device="cuda")
         value = cells / (ms * 1e-3)
         kern_ms = i1["step_kernel_ms"] - i0["step_kernel_ms"]
@@ -346,6 +348,7 @@ def main():
         def leg(batched, graphs, schedule=0):
             p = Solver(d, batched=batched, graphs=graphs, schedule=schedule)
             p.run(args.warmup)
+            j0 = p.info()
             pms = 0.0
             pcells = 0.0
             for _ in range(args.steps):
@@ -356,9 +359,13 @@ def main():
                 pcells += inf["last_run_cells"]
             inf = p.info()
             p.close()
+            # host wall time of the steps, split into regrid and the rest (the level substeps)
+            inf["regrid_ms_per_step"] = 1e3 * (inf["regrid_seconds"] - j0["regrid_seconds"]) / args.steps
+            inf["advance_ms_per_step"] = (1e3 * (inf["step_seconds"] - j0["step_seconds"]) / args.steps
+                                          - inf["regrid_ms_per_step"])
             return pcells / (pms * 1e-3), pms / args.steps, inf
 
-        plain_value, plain_ms, _ = leg(False, False)
+        plain_value, plain_ms, plain_inf = leg(False, False)
         graph_legs = {}
         if ndim == 3:
             for name, b in (("plain_graphs", False), ("batched_graphs", True)):
@@ -431,8 +438,13 @@ def main():
         "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded initial conditions of the workload",
         "config": dict(cfg, l2="flushed between steps (256 MB write)", parallelism="replicas" if world > 1 else "single"),
         "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": plain_ms,
-                  "speedup_batched_over_plain": value / plain_value if plain_value else None},
+                  "speedup_batched_over_plain": value / plain_value if plain_value else None,
+                  "advance_ms_per_step": plain_inf["advance_ms_per_step"],
+                  "regrid_ms_per_step": plain_inf["regrid_ms_per_step"],
+                  "advance_speedup_batched_over_plain": (plain_inf["advance_ms_per_step"] / batched_advance_ms
+                                                         if batched_advance_ms > 0 else None)},
         "schedules": graph_legs or None,
+        "advance_ms_per_step": batched_advance_ms, "regrid_ms_per_step": batched_regrid_ms,
         "l1_err_vs_fp64": 0.0,
         "fp32_form": fp32,
         "serving": serving,

@@ -97,10 +97,19 @@ def test_cuda_graph_replay_is_identical(batched):
     give the same results as direct launches; graphs are re-captured after regrids and
     reused in between."""
     rd = _with_gauges(configs.euler_blast(n=16, levels=3, tfinal=0.1, max1d=16))
-    ref, gpu = _both(rd, batched=batched, graphs=True)
+    ref, gpu = _both(rd, batched=batched, graphs=True, schedule=1)
     _assert_identical(ref, gpu)
     assert gpu["info"]["graph_captures"] > 0
     assert gpu["info"]["graph_replays"] > 2 * gpu["info"]["graph_captures"]
+
+
+def test_autotuned_schedule_then_graphs_is_identical():
+    """Levels launch directly while the sweep schedule is tuned, then replay graphs."""
+    rd = configs.euler_blast(n=16, levels=3, tfinal=0.1, max1d=16)
+    ref, gpu = _both(rd, graphs=True)
+    _assert_identical(ref, gpu)
+    assert gpu["info"]["levels_tuned_queue"] + gpu["info"]["levels_tuned_per_direction"] >= 2
+    assert gpu["info"]["graph_replays"] > 0
 
 
 @pytest.mark.parametrize("schedule", [1, 2])
