@@ -1717,6 +1717,8 @@ class Amr2Gpu {
       lc.iregsz[l] = iregsz[l]; lc.jregsz[l] = jregsz[l]; lc.intratx[l] = intratx[l]; lc.intraty[l] = intraty[l];
     }
     AMR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    retain_pool_memory();
+    AllocStreamScope alloc_scope(st);
     for (cudaEvent_t* e : {&ev_a, &ev_b, &ev_run0, &ev_run1}) AMR_CUDA(cudaEventCreate(e));
     long long est = (long long)nvar * (nxc + 4) * (nyc + 4) * 8 * std::max(1, p.mxnest) + (1 << 22);
     pool.init(est);
@@ -2024,6 +2026,7 @@ class Solver2 : public AmrSolver {
  public:
   Amr2Gpu g;
   int num_dim() const override { return 2; }
+  cudaStream_t stream() const override { return g.st; }
   void set_batched(bool on) override { g.batched = on; }
   void set_profile(bool on) override { g.profile = on; }
   void set_graphs(bool on) override {
@@ -2108,6 +2111,12 @@ static int guarded(F&& f) {
     return AMRGPU_ERROR;
   }
 }
+// the same, with the context's stream ordering its buffer reallocations
+template <class F>
+static int guarded(amrgpu_ctx* ctx, F&& f) {
+  amrb::AllocStreamScope scope(ctx->s->stream());
+  return guarded(std::forward<F>(f));
+}
 
 extern "C" {
 
@@ -2154,12 +2163,12 @@ int amrgpu_set_batched(amrgpu_ctx* ctx, int batched) {
 
 int amrgpu_set_graphs(amrgpu_ctx* ctx, int on) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] { ctx->s->set_graphs(on != 0); });
+  return guarded(ctx, [&] { ctx->s->set_graphs(on != 0); });
 }
 
 int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] { ctx->s->set_schedule(schedule); });
+  return guarded(ctx, [&] { ctx->s->set_schedule(schedule); });
 }
 
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on) {
@@ -2170,12 +2179,12 @@ int amrgpu_set_profile(amrgpu_ctx* ctx, int on) {
 
 int amrgpu_run(amrgpu_ctx* ctx, int max_cycles) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] { ctx->s->run(max_cycles); });
+  return guarded(ctx, [&] { ctx->s->run(max_cycles); });
 }
 
 int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* cfl_out) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] {
+  return guarded(ctx, [&] {
     double cfl = 0;
     const double d = ctx->s->level_advance(level, &cfl);
     if (dtnew_out) *dtnew_out = d;
@@ -2208,27 +2217,27 @@ int amrgpu_level_advance_noalloc(amrgpu_ctx* ctx, int level, double* dtnew_out, 
 
 int amrgpu_update(amrgpu_ctx* ctx, int level) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] { ctx->s->update_level(level); });
+  return guarded(ctx, [&] { ctx->s->update_level(level); });
 }
 
 int amrgpu_regrid(amrgpu_ctx* ctx, int lbase) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] { ctx->s->regrid_from(lbase); });
+  return guarded(ctx, [&] { ctx->s->regrid_from(lbase); });
 }
 
 int amrgpu_valout(amrgpu_ctx* ctx, const char* dir) {
   if (!ctx) return AMRGPU_EINVAL;
-  return guarded([&] { ctx->s->valout(dir); });
+  return guarded(ctx, [&] { ctx->s->valout(dir); });
 }
 
 int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out) {
   if (!ctx || !mass_out) return AMRGPU_EINVAL;
-  return guarded([&] { *mass_out = ctx->s->mass(); });
+  return guarded(ctx, [&] { *mass_out = ctx->s->mass(); });
 }
 
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n) {
   if (!ctx || !out) return AMRGPU_EINVAL;
-  return guarded([&] {
+  return guarded(ctx, [&] {
     const std::vector<double> v = ctx->s->info();
     for (int k = 0; k < n && k < (int)v.size(); ++k) out[k] = v[k];
   });
@@ -2236,7 +2245,7 @@ int amrgpu_info(amrgpu_ctx* ctx, double* out, int n) {
 
 int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out) {
   if (!ctx || !n_out) return AMRGPU_EINVAL;
-  return guarded([&] {
+  return guarded(ctx, [&] {
     const std::vector<int> r = ctx->s->grid_rows();
     const int w = 2 + 2 * ctx->s->num_dim();
     const int n = (int)(r.size() / w);
@@ -2247,7 +2256,7 @@ int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out) {
 
 int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out) {
   if (!ctx || !n_out) return AMRGPU_EINVAL;
-  return guarded([&] {
+  return guarded(ctx, [&] {
     const std::vector<double> v = ctx->s->values();
     if (out) std::memcpy(out, v.data(), sizeof(double) * std::min<long long>(cap, (long long)v.size()));
     *n_out = (long long)v.size();
@@ -2256,7 +2265,7 @@ int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out)
 
 int amrgpu_gauges(amrgpu_ctx* ctx, double* out, int cap_rows, int* n_out) {
   if (!ctx || !n_out) return AMRGPU_EINVAL;
-  return guarded([&] {
+  return guarded(ctx, [&] {
     const std::vector<double> v = ctx->s->gauge_rows();
     const int w = 3 + ctx->nvar;
     const int n = (int)(v.size() / w);

@@ -1874,6 +1874,8 @@ class Amr3Gpu : public AmrSolver {
       lc.intratx[l] = intratx[l]; lc.intraty[l] = intraty[l]; lc.intratz[l] = intratz[l];
     }
     AMR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    retain_pool_memory();
+    AllocStreamScope alloc_scope(st);
     for (cudaEvent_t* e : {&ev_a, &ev_b, &ev_run0, &ev_run1}) AMR_CUDA(cudaEventCreate(e));
     // room for the finer levels from the start (16x the level-1 storage): growing the pool
     // later moves it, which waits for the device
@@ -2124,6 +2126,7 @@ class Amr3Gpu : public AmrSolver {
 
   // ================================================================ AmrSolver
   int num_dim() const override { return 3; }
+  cudaStream_t stream() const override { return st; }
   void set_batched(bool on) override { batched = on; }
   void set_profile(bool on) override { profile = on; }
   void set_graphs(bool on) override {

@@ -16,6 +16,35 @@ namespace amrb {
 
 static const double RINF = (double)10.e32f;
 
+// Device-buffer reallocations of this process (cudaFree + cudaMalloc: both wait for the
+// device): count and host seconds, reported with the section timers.
+inline long long g_dbuf_reallocs = 0;
+inline double g_dbuf_realloc_s = 0;
+// uploads through the pinned staging ring: bytes, ring wraps (each waits for the stream)
+// and host seconds in the copy into the ring
+inline double g_stage_bytes = 0, g_stage_copy_s = 0;
+inline long long g_stage_wraps = 0;
+
+// Stream-ordered reallocation. While a context works on the calling thread its stream is
+// set here, and device buffers that grow are freed and allocated in that stream's order
+// (cudaFreeAsync / cudaMallocAsync) instead of cudaFree / cudaMalloc, which wait for the
+// whole device. The device's default memory pool keeps freed memory for reuse
+// (retain_pool_memory), so a grown buffer seldom maps new pages.
+inline thread_local cudaStream_t t_alloc_stream = nullptr;
+struct AllocStreamScope {
+  cudaStream_t prev;
+  explicit AllocStreamScope(cudaStream_t s) : prev(t_alloc_stream) { t_alloc_stream = s; }
+  ~AllocStreamScope() { t_alloc_stream = prev; }
+};
+inline void retain_pool_memory() {
+  int dev = 0;
+  AMR_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t mp;
+  AMR_CUDA(cudaDeviceGetDefaultMemPool(&mp, dev));
+  unsigned long long thr = ~0ull;
+  AMR_CUDA(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr));
+}
+
 // Host-side section timers, printed at context destruction when AMRB_PROF is set.
 struct HostProf {
   std::map<std::string, std::pair<double, long long>> acc;
@@ -23,6 +52,8 @@ struct HostProf {
   ~HostProf() {
     if (!on) return;
     for (auto& kv : acc) std::fprintf(stderr, "PROF %-22s %9.4f s %8lld calls\n", kv.first.c_str(), kv.second.first, kv.second.second);
+    std::fprintf(stderr, "PROF %-22s %9.4f s %8lld calls\n", "dbuf_realloc", g_dbuf_realloc_s, g_dbuf_reallocs);
+    std::fprintf(stderr, "PROF %-22s %9.4f s %8lld wraps %.1f MB\n", "staging_copy", g_stage_copy_s, g_stage_wraps, g_stage_bytes / 1e6);
   }
 };
 struct ScopedTimer {
@@ -126,6 +157,7 @@ struct Staging {
   const void* put(const void* src, size_t n, cudaStream_t s) {
     const size_t n2 = (n + 255) & ~(size_t)255;
     if (used + n2 > cap) {
+      ++g_stage_wraps;
       AMR_CUDA(cudaStreamSynchronize(s));
       used = 0;
       if (n2 > cap) {
@@ -135,7 +167,10 @@ struct Staging {
       }
     }
     char* dst = h + used;
+    const auto t0 = std::chrono::steady_clock::now();
     std::memcpy(dst, src, n);
+    g_stage_copy_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    g_stage_bytes += (double)n;
     used += n2;
     return dst;
   }
@@ -153,34 +188,35 @@ struct Staging {
 
 template <class T> struct DBuf {
   T* d = nullptr; size_t cap = 0, n = 0;
+  void realloc_to(size_t c) {
+    const auto t0 = std::chrono::steady_clock::now();
+    cap = c;
+    if (t_alloc_stream) {
+      if (d) AMR_CUDA(cudaFreeAsync(d, t_alloc_stream));
+      AMR_CUDA(cudaMallocAsync((void**)&d, sizeof(T) * cap, t_alloc_stream));
+    } else {
+      if (d) AMR_CUDA(cudaFree(d));
+      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
+    }
+    ++g_dbuf_reallocs;
+    g_dbuf_realloc_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
   // smallest allocation (64 KiB): small per-level arrays then rarely reallocate
   static constexpr size_t kMin = (64 << 10) / sizeof(T) > 16 ? (64 << 10) / sizeof(T) : 16;
   void upload(const std::vector<T>& h, cudaStream_t s, Staging& stg) { upload(h.data(), h.size(), s, stg); }
   void upload(const T* h, size_t cnt, cudaStream_t s, Staging& stg) {
     n = cnt;
-    if (n > cap) {
-      if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(n * 2, kMin);
-      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
-    }
+    if (n > cap) realloc_to(std::max<size_t>(n * 2, kMin));
     if (n) AMR_CUDA(cudaMemcpyAsync(d, stg.put(h, sizeof(T) * n, s), sizeof(T) * n, cudaMemcpyHostToDevice, s));
   }
   void ensure(size_t m) {
-    if (m > cap) {
-      if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(m, 16) * 3 / 2;
-      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
-    }
+    if (m > cap) realloc_to(std::max<size_t>(m, 16) * 3 / 2);
     n = m;
   }
   // ensure() for large scratch that changes size with the hierarchy: grows to twice the
   // request, so a slowly growing level does not reallocate (and synchronise) every regrid
   void reserve(size_t m) {
-    if (m > cap) {
-      if (d) AMR_CUDA(cudaFree(d));
-      cap = std::max<size_t>(m * 2, kMin);
-      AMR_CUDA(cudaMalloc(&d, sizeof(T) * cap));
-    }
+    if (m > cap) realloc_to(std::max<size_t>(m * 2, kMin));
     n = m;
   }
   void free() { if (d) cudaFree(d); d = nullptr; cap = n = 0; }

@@ -1,5 +1,6 @@
 // The interface the C ABI drives: one AMR solve on one device (2D or 3D).
 #pragma once
+#include <cuda_runtime.h>
 #include <string>
 #include <vector>
 
@@ -9,6 +10,7 @@ class AmrSolver {
  public:
   virtual ~AmrSolver() = default;
   virtual int num_dim() const = 0;
+  virtual cudaStream_t stream() const = 0;  // the stream the solve's work is ordered on
   virtual void set_batched(bool on) = 0;
   virtual void set_profile(bool on) = 0;
   // replay each level substep from captured CUDA graphs (3D path)
