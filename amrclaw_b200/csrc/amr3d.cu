@@ -42,7 +42,6 @@ struct HPatch3 {
   int cur = 0;
   bool has_cfl = false;
   std::vector<int> listbc;  // 6 ints per entry (setuse.f): i, j, k (enlarged, 1-based), side, kid, register
-  std::vector<int> bnd;
   int nx() const { return ihi - ilo + 1; }
   int ny() const { return jhi - jlo + 1; }
   int nz() const { return khi - klo + 1; }
@@ -462,18 +461,6 @@ class Amr3Gpu : public AmrSolver {
       for (int m = lstart[lev]; m != 0; m = node[m].levelptr) lgrids[lev].push_back(m);
     }
   }
-  // init_bndryList.f:50-107 (neighbours by their i,j extents, most recent first)
-  void make_bndry(int lev) {
-    const GridIndex& X = GI(lev);
-    std::vector<int> hits;
-    for (int m : lgrids[lev]) {
-      HPatch3& g = node[m];
-      g.bnd.clear();
-      X.query(g.ilo - G3, g.ihi + G3, g.jlo - G3, g.jhi + G3, -(1 << 29), 1 << 29, hits);
-      for (size_t k = hits.size(); k-- > 0;)
-        if (X.id(hits[k]) != m) g.bnd.push_back(X.id(hits[k]));
-    }
-  }
   // regrid.f:122-159: cost nx*ny, most expensive first, quick_sort1.f tie breaking
   static void qsorti(std::vector<int>& ord, int n, const std::vector<long long>& a);
   void arrange(int lev) {
@@ -508,7 +495,7 @@ class Amr3Gpu : public AmrSolver {
         const int mn = nodget();
         HPatch3& a = node[m]; HPatch3& b = node[mn];
         b = a;
-        b.bnd.clear(); b.listbc.clear(); b.q0 = b.q1 = -1; b.ffl = -1;
+        b.listbc.clear(); b.q0 = b.q1 = -1; b.ffl = -1;
         b.levelptr = a.levelptr; a.levelptr = mn;
         if (dir == 0) { b.ihi = a.ihi; a.ihi = a.ilo + nl - 1; b.ilo = a.ihi + 1; b.xlo = mid; a.xhi = mid; }
         else if (dir == 1) { b.jhi = a.jhi; a.jhi = a.jlo + nl - 1; b.jlo = a.jhi + 1; b.ylo = mid; a.yhi = mid; }
@@ -586,13 +573,17 @@ class Amr3Gpu : public AmrSolver {
     std::vector<int8_t> used((size_t)ni * nj * nk, 0);
     auto U = [&](int i, int j, int k) -> int8_t& { return used[((size_t)(k - klo) * nj + (j - jlo)) * ni + (i - ilo)]; };
     std::vector<Fill3Op> copies;
+    // the same-level grids that meet the region (intfil.f walks bndList of msrc, the grids
+    // next to it; a level's grids are disjoint, so every cell has at most one source and
+    // the order of the copies does not matter)
     std::vector<int> src;
-    if (msrc == -1) {
+    {
       const GridIndex& X = GI(level);
       std::vector<int> hits;
       X.query(ilo, ihi, jlo, jhi, klo, khi, hits);
-      for (int r : hits) src.push_back(X.id(r));
-    } else src = node[msrc].bnd;
+      for (int r : hits)
+        if (X.id(r) != msrc) src.push_back(X.id(r));
+    }
     for (int m : src) {
       const HPatch3& g = node[m];
       const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi);
@@ -960,12 +951,21 @@ class Amr3Gpu : public AmrSolver {
       std::vector<Part> part(G.size());
       pool_host.run((int)G.size(), [&](int n) { update_lists(G[n], XF, rx, ry, rz, part[n].upc, part[n].upt, part[n].avg); });
       tph.next("cu_merge");
-      for (Part& q : part) {
-        const int base = (int)L.upt.size();
-        for (Upbnd3Cell c : q.upc) { c.first += base; L.upc.push_back(c); }
-        L.upt.insert(L.upt.end(), q.upt.begin(), q.upt.end());
-        L.avg.insert(L.avg.end(), q.avg.begin(), q.avg.end());
+      // the parts in coarse-grid order: offsets by prefix sums, copies in parallel
+      const size_t np = part.size();
+      std::vector<size_t> oc(np + 1, 0), ot(np + 1, 0), oa(np + 1, 0);
+      for (size_t n = 0; n < np; ++n) {
+        oc[n + 1] = oc[n] + part[n].upc.size();
+        ot[n + 1] = ot[n] + part[n].upt.size();
+        oa[n + 1] = oa[n] + part[n].avg.size();
       }
+      L.upc.resize(oc[np]); L.upt.resize(ot[np]); L.avg.resize(oa[np]);
+      pool_host.run((int)np, [&](int n) {
+        const Part& q = part[n];
+        for (size_t k = 0; k < q.upc.size(); ++k) { Upbnd3Cell c = q.upc[k]; c.first += (int)ot[n]; L.upc[oc[n] + k] = c; }
+        std::copy(q.upt.begin(), q.upt.end(), L.upt.begin() + ot[n]);
+        std::copy(q.avg.begin(), q.avg.end(), L.avg.begin() + oa[n]);
+      });
     }
     L.avg_max = 0;
     for (const Avg3& a : L.avg) L.avg_max = std::max<long long>(L.avg_max, (long long)a.ni * a.nj * a.nk);
@@ -1797,7 +1797,7 @@ class Amr3Gpu : public AmrSolver {
         const int mold = m;
         m = node[m].levelptr;
         free_patch(mold);
-        node[mold].bnd.clear(); node[mold].listbc.clear();
+        node[mold].listbc.clear();
         putnod(mold);
       }
       lstart[l2] = newstl[l2];
@@ -1811,8 +1811,6 @@ class Amr3Gpu : public AmrSolver {
     tph.next("rg_arrange_lists");
     for (int lev = lbase + 1; lev <= p.mxnest; ++lev) arrange(lev);
     make_lists();
-    tph.next("rg_bndry");
-    for (int lev = lbase + 1; lev <= lfine; ++lev) make_bndry(lev);
     tph.next("rg_compile");
     compile_all(lbase);
     sync_stream();
@@ -1916,7 +1914,6 @@ class Amr3Gpu : public AmrSolver {
     ginit(lstart[1], start_time);
     arrange(1);
     make_lists();
-    make_bndry(1);
     compile_all(0);
     // setgrd.f
     record_gauges = false;
@@ -1933,7 +1930,6 @@ class Amr3Gpu : public AmrSolver {
       lfine = levnew;
       arrange(levnew);
       make_lists();
-      make_bndry(levnew);
       compile_all(levold);
       ++levnew;
     }
