@@ -66,6 +66,11 @@ class Solver:
         """Replay each level substep from captured CUDA graphs (3D path)."""
         _check(self._lib, self._lib.amrgpu_set_graphs(self._h, int(on)), "amrgpu_set_graphs")
 
+    def checkpoint(self, path: str | None = None) -> None:
+        """Write a checkpoint of the run at its current coarse-step boundary (3D); a run
+        whose claw.data sets restart / restart_file continues from it."""
+        _check(self._lib, self._lib.amrgpu_checkpoint(self._h, path.encode() if path else None), "amrgpu_checkpoint")
+
     def set_schedule(self, schedule: int) -> None:
         """Sweep schedule of the batched 3D path: 0 autotune, 1 per direction, 2 work queue."""
         _check(self._lib, self._lib.amrgpu_set_schedule(self._h, int(schedule)), "amrgpu_set_schedule")

@@ -1693,6 +1693,7 @@ class Amr2Gpu {
     if (p.ndim != 2) throw std::runtime_error("this solver handles 2D runs");
     if (p.nghost != 2) throw std::runtime_error("num_ghost must be 2");
     if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
+    if (p.restart || p.checkpt_style != 0) throw std::runtime_error("checkpoint/restart is built for the 3D device path");
     if (p.dimsplit != 0) throw std::runtime_error("only the unsplit method is supported");
     if (p.src_split != 0) throw std::runtime_error("source terms are not supported");
     nvar = p.nvar; ng = p.nghost;
@@ -2035,6 +2036,9 @@ class Solver2 : public AmrSolver {
   void set_schedule(int s) override {
     if (s != 0) throw std::runtime_error("amrgpu_set_schedule: sweep schedules are built for the 3D path");
   }
+  void write_checkpoint(const char*) override {
+    throw std::runtime_error("amrgpu_checkpoint: checkpoint/restart is built for the 3D path");
+  }
   void run(int max_cycles) override { g.max_cycles = max_cycles; g.tick(); }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > g.lfine) throw std::runtime_error("level out of range");
@@ -2169,6 +2173,11 @@ int amrgpu_set_graphs(amrgpu_ctx* ctx, int on) {
 int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule) {
   if (!ctx) return AMRGPU_EINVAL;
   return guarded(ctx, [&] { ctx->s->set_schedule(schedule); });
+}
+
+int amrgpu_checkpoint(amrgpu_ctx* ctx, const char* path) {
+  if (!ctx) return AMRGPU_EINVAL;
+  return guarded(ctx, [&] { ctx->s->write_checkpoint(path); });
 }
 
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on) {

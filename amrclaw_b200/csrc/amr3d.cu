@@ -1901,6 +1901,12 @@ class Amr3Gpu : public AmrSolver {
     start_time = p.t0;
     glast.assign(p.gauges.size(), 0.0);
     for (size_t i = 0; i < p.gauges.size(); ++i) glast[i] = p.gauges[i].t1;
+    if (p.restart) {
+      // amr3.f90:466-480: the run continues from the checkpoint named in claw.data
+      const std::string f = p.restart_file;
+      restart_from(!f.empty() && f[0] == '/' ? f : dir + "/" + f);
+      return;
+    }
     // domain.f
     const int ms = nodget();
     HPatch3& g = node[ms];
@@ -1947,6 +1953,162 @@ class Amr3Gpu : public AmrSolver {
     if (p.output_t0) output(time);
   }
 
+  // ================================================================ check.f / restrt.f
+  // A checkpoint, taken at a coarse-step boundary, holds what the continued run reads:
+  // the scheduler state (time, cycle, step sizes, regrid counters, level times, output and
+  // gauge cursors), the grid table with its free list (grid numbers continue as they
+  // would have), both solution buffers and the aux block of every grid, and the gauge
+  // samples so far. The fill programs, step plans and register lists are compiled again
+  // from the grids. The flux registers and saved coarse rings are not kept: at a
+  // coarse-step boundary each entry upbnd will read is rewritten (fluxsv, saveqc, prepf)
+  // before it is read. The layout is this library's own (little-endian, versioned); the
+  // reference dumps its raw alloc array instead.
+  static constexpr char CHK_MAGIC[8] = {'A', 'M', 'R', 'B', '3', 'C', 'K', '1'};
+  struct ChkHead {
+    int nvar, naux, f32, mxnest, lfine, ncycle, frame, nextout, nnodes, ndfree, id_hwm, gslots, ngrows, ngauges;
+    int icheck[12], lstart[12];
+    double time, start_time, tmass0, cflmax_run, rvol, rvoll[12], possk[12], tlevel[12];
+  };
+  struct ChkNode {
+    int ilo, ihi, jlo, jhi, klo, khi, level, levelptr, nextfree;
+    double xlo, xhi, ylo, yhi, zlo, zhi, time;
+  };
+  void checkpoint(const std::string& path) {
+    HPROF("checkpoint3");
+    sync_stream();
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write checkpoint " + path);
+    auto put = [&](const void* d, size_t n) {
+      if (n && std::fwrite(d, 1, n, f) != n) { std::fclose(f); throw std::runtime_error("short write to " + path); }
+    };
+    ChkHead h{};
+    h.nvar = nvar; h.naux = p.naux; h.f32 = f32 ? 1 : 0; h.mxnest = p.mxnest; h.lfine = lfine; h.ncycle = ncycle;
+    h.frame = frame; h.nextout = tk_nextout; h.nnodes = (int)node.size(); h.ndfree = ndfree; h.id_hwm = id_hwm;
+    h.gslots = gslots; h.ngrows = (int)grows.size(); h.ngauges = (int)glast.size();
+    for (int l = 0; l < 12; ++l) {
+      h.icheck[l] = icheck[l]; h.lstart[l] = lstart[l]; h.rvoll[l] = rvoll[l]; h.possk[l] = possk[l];
+      h.tlevel[l] = tk_tlevel[l];
+    }
+    h.time = time; h.start_time = start_time; h.tmass0 = tmass0; h.cflmax_run = cflmax_run; h.rvol = rvol;
+    if (!tick_started) for (int l = 1; l <= p.mxnest; ++l) h.tlevel[l] = time;
+    put(CHK_MAGIC, 8);
+    put(&h, sizeof h);
+    std::vector<ChkNode> nodes(node.size());
+    for (size_t m = 0; m < node.size(); ++m) {
+      const HPatch3& g = node[m];
+      nodes[m] = ChkNode{g.ilo, g.ihi, g.jlo, g.jhi, g.klo, g.khi, g.level, g.levelptr, g.nextfree,
+                         g.xlo, g.xhi, g.ylo, g.yhi, g.zlo, g.zhi, g.time};
+    }
+    put(nodes.data(), sizeof(ChkNode) * nodes.size());
+    // per grid, level by level in list order: store1, store2, aux block (storage precision)
+    std::vector<char> buf;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) {
+        const HPatch3& g = node[m];
+        const long long offs[2] = {g.cur == 0 ? g.q0 : g.q1, g.cur == 0 ? g.q1 : g.q0};
+        for (long long off : offs) {
+          buf.resize(elem() * g.nq);
+          AMR_CUDA(cudaMemcpy(buf.data(), pool_bytes() + elem() * off, buf.size(), cudaMemcpyDeviceToHost));
+          put(buf.data(), buf.size());
+        }
+        if (g.aux >= 0) {
+          buf.resize(elem() * g.na * (vel_period > 0.0 ? 2 : 1));
+          AMR_CUDA(cudaMemcpy(buf.data(), pool_bytes() + elem() * g.aux, buf.size(), cudaMemcpyDeviceToHost));
+          put(buf.data(), buf.size());
+        }
+      }
+    put(glast.data(), sizeof(double) * glast.size());
+    put(grows.data(), sizeof(GRow) * grows.size());
+    if (gslots) {
+      std::vector<double> gv((size_t)gslots * nvar);
+      AMR_CUDA(cudaMemcpy(gv.data(), d_gauge_out.d, sizeof(double) * gv.size(), cudaMemcpyDeviceToHost));
+      put(gv.data(), sizeof(double) * gv.size());
+    }
+    if (std::fclose(f) != 0) throw std::runtime_error("cannot close " + path);
+  }
+  // restrt.f: the grids and scheduler state of a checkpoint, in place of domain.f/setgrd.f
+  void restart_from(const std::string& path) {
+    HPROF("restart3");
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot read checkpoint " + path);
+    auto get = [&](void* d, size_t n) {
+      if (n && std::fread(d, 1, n, f) != n) { std::fclose(f); throw std::runtime_error("checkpoint " + path + " is truncated"); }
+    };
+    char magic[8];
+    get(magic, 8);
+    if (std::memcmp(magic, CHK_MAGIC, 8) != 0) { std::fclose(f); throw std::runtime_error(path + " is not a 3D checkpoint of this library"); }
+    ChkHead h{};
+    get(&h, sizeof h);
+    if (h.nvar != nvar || h.naux != p.naux || h.f32 != (f32 ? 1 : 0) || h.mxnest != p.mxnest || h.ngauges != (int)glast.size() ||
+        h.nnodes < 2 || h.lfine < 1 || h.lfine > p.mxnest) {
+      std::fclose(f);
+      throw std::runtime_error("checkpoint " + path + " does not match this run (equations, aux, precision, levels or gauges)");
+    }
+    std::vector<ChkNode> nodes((size_t)h.nnodes);
+    get(nodes.data(), sizeof(ChkNode) * nodes.size());
+    node.assign(nodes.size(), HPatch3());
+    for (size_t m = 0; m < nodes.size(); ++m) {
+      const ChkNode& c = nodes[m];
+      HPatch3& g = node[m];
+      g.ilo = c.ilo; g.ihi = c.ihi; g.jlo = c.jlo; g.jhi = c.jhi; g.klo = c.klo; g.khi = c.khi;
+      g.level = c.level; g.levelptr = c.levelptr; g.nextfree = c.nextfree;
+      g.xlo = c.xlo; g.xhi = c.xhi; g.ylo = c.ylo; g.yhi = c.yhi; g.zlo = c.zlo; g.zhi = c.zhi; g.time = c.time;
+    }
+    ndfree = h.ndfree; id_hwm = 0; lfine = h.lfine;
+    for (int l = 0; l < 12; ++l) {
+      icheck[l] = h.icheck[l]; lstart[l] = h.lstart[l]; rvoll[l] = h.rvoll[l]; possk[l] = h.possk[l]; tk_tlevel[l] = h.tlevel[l];
+    }
+    ncycle = h.ncycle; frame = h.frame; tk_nextout = h.nextout; tick_started = true;
+    time = h.time; start_time = h.start_time; tmass0 = h.tmass0; cflmax_run = h.cflmax_run; rvol = h.rvol;
+    std::vector<char> buf;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) {
+        alloc_patch(m);  // cur = 0: q0 takes store1, q1 store2
+        HPatch3& g = node[m];
+        for (long long off : {g.q0, g.q1}) {
+          buf.resize(elem() * g.nq);
+          get(buf.data(), buf.size());
+          AMR_CUDA(cudaMemcpy(pool_bytes() + elem() * off, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+        }
+        if (g.aux >= 0) {
+          buf.resize(elem() * g.na * (vel_period > 0.0 ? 2 : 1));
+          get(buf.data(), buf.size());
+          AMR_CUDA(cudaMemcpy(pool_bytes() + elem() * g.aux, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+        }
+        h2d_bytes += 2.0 * elem() * g.nq;
+      }
+    get(glast.data(), sizeof(double) * glast.size());
+    grows.resize((size_t)h.ngrows);
+    get(grows.data(), sizeof(GRow) * grows.size());
+    gslots = h.gslots;
+    if (gslots) {
+      std::vector<double> gv((size_t)gslots * nvar);
+      get(gv.data(), sizeof(double) * gv.size());
+      d_gauge_out.ensure(std::max<size_t>(gv.size() * 2, 4096));
+      AMR_CUDA(cudaMemcpy(d_gauge_out.d, gv.data(), sizeof(double) * gv.size(), cudaMemcpyHostToDevice));
+    }
+    std::fclose(f);
+    for (int lev = 1; lev <= p.mxnest; ++lev) touch(lev);
+    make_lists();
+    for (int level = 1; level <= lfine - 1; ++level) { prepf(level + 1); prepc(level); }
+    compile_all(0);
+    sync_stream();
+    record_gauges = true;
+  }
+  void checkpoint_file(const char* path) {
+    if (path && *path) { checkpoint(path); return; }
+    char fn[64];
+    if (p.checkpt_style < 0) {
+      std::snprintf(fn, sizeof(fn), "/fort.chk%s", chk_a ? "aaaaa" : "bbbbb");  // check_twofiles.f
+      chk_a = !chk_a;
+    } else std::snprintf(fn, sizeof(fn), "/fort.chk%05d", ncycle);
+    checkpoint(outdir + fn);
+  }
+  bool chk_a = true;
+  int tk_nextchk = 0;
+  bool tk_dumpchk = false, final_chk_done = false;
+  void write_checkpoint(const char* path) override { checkpoint_file(path); }
+
   // ================================================================ tick.f
   bool finished() const { return ncycle >= p.nstop || time >= p.tfinal; }
   void tick() {
@@ -1963,17 +2125,30 @@ class Amr3Gpu : public AmrSolver {
     if (tick_started) nextout = tk_nextout;
     double* tlevel = tk_tlevel;
     if (!tick_started) { tlevel[1] = time; for (int i = 2; i <= p.mxnest; ++i) tlevel[i] = tlevel[1]; }
+    if (!tick_started || tk_nextchk == 0) {
+      // tick.f:73-81: checkpoint times still to come
+      tk_nextchk = 1;
+      while (tk_nextchk <= (int)p.tchk.size() && p.tchk[tk_nextchk - 1] <= time) ++tk_nextchk;
+    }
     tick_started = true;
     while (!finished()) {
       double outtime;
       if (p.nout > 0) outtime = (nextout <= p.nout) ? p.tout[nextout - 1] : RINF;
       else outtime = p.tfinal;
+      const double chktime = (tk_nextchk <= (int)p.tchk.size()) ? p.tchk[tk_nextchk - 1] : RINF;
       bool dumpout = false;
       if (time < outtime && time + (double)1.001f * possk[1] >= outtime) {
         possk[1] = outtime - time;
         for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
         if (p.nout > 0) { ++nextout; dumpout = true; }
       }
+      // tick.f:146-157: shorten the step to land on a checkpoint time
+      if (time < chktime && time + possk[1] >= chktime) {
+        possk[1] = chktime - time;
+        for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
+        ++tk_nextchk;
+        tk_dumpchk = true;
+      } else tk_dumpchk = false;
       int level = 1;
       ntogo[level] = 1;
       for (int i = 1; i <= 10; ++i) dtnew[i] = RINF;
@@ -2026,11 +2201,21 @@ class Amr3Gpu : public AmrSolver {
         possk[1] = dtnew[1];
         for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
       }
+      // tick.f:322-326
+      if (((p.checkpt_style == 3 || p.checkpt_style == -3) && ncycle % p.checkpt_interval == 0) || tk_dumpchk) {
+        checkpoint_file(nullptr);
+        tk_dumpchk = true;
+      }
       if ((ncycle % iout == 0) || dumpout) output(time);
       ++cycles;
       if (max_cycles > 0 && cycles >= max_cycles) break;
     }
     tk_nextout = nextout;
+    // tick.f:365-368: a final checkpoint unless the last step just wrote one
+    if (finished() && p.checkpt_style != 0 && !tk_dumpchk && !final_chk_done) {
+      checkpoint_file(nullptr);
+      final_chk_done = true;
+    }
     AMR_CUDA(cudaEventRecord(ev_run1, st));
     sync_stream();
     float ms = 0;

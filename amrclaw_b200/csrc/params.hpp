@@ -101,6 +101,11 @@ struct RunParams {
   std::map<std::string, std::string> probstr;
   int flag_component = 0;
   std::string flag_mode;
+  // restart and checkpointing (amr3.f90:308-325)
+  bool restart = false;
+  std::string restart_file;
+  int checkpt_style = 0, checkpt_interval = 0;
+  std::vector<double> tchk;
 
   void load(const std::string& dir) {
     KeyFile c, a, r, g, s;
@@ -133,6 +138,15 @@ struct RunParams {
     use_fwaves = c.b("use_fwaves");
     for (int k = 0; k < mwaves; ++k) mthlim.push_back(c.n("limiter", k));
     nghost = c.n("num_ghost");
+    restart = c.has("restart") && c.b("restart");
+    restart_file = c.has("restart_file") ? c.str("restart_file") : std::string();
+    checkpt_style = c.n_or("checkpt_style", 0);
+    if (checkpt_style == 2 || checkpt_style == -2) {
+      if (c.has("checkpt_times")) for (auto& v : c.at("checkpt_times")) tchk.push_back(KeyFile::num(v));
+    } else if (checkpt_style == 3 || checkpt_style == -3) {
+      checkpt_interval = c.n("checkpt_interval");
+      if (checkpt_interval < 1) throw std::runtime_error("checkpt_interval must be positive");
+    }
     for (int d = 0; d < ndim; ++d) { mthbc[2 * d + 1] = c.n("bc_lower", d); mthbc[2 * d + 2] = c.n("bc_upper", d); }
     for (int d = 0; d < ndim; ++d)
       if ((mthbc[2 * d + 1] == 2) != (mthbc[2 * d + 2] == 2))

@@ -22,6 +22,7 @@ class AmrSolver {
   virtual void update_level(int level) = 0;                 // update.f
   virtual void regrid_from(int lbase) = 0;                  // regrid.f
   virtual void valout(const char* dir) = 0;                 // valout.f90 (dir == nullptr: the run's output dir)
+  virtual void write_checkpoint(const char* path) = 0;      // check.f (path == nullptr: fort.chkNNNNN in the output dir)
   virtual double mass() = 0;                                // conck.f, level 1
   virtual std::vector<double> info() = 0;
   virtual std::vector<int> grid_rows() = 0;                 // 2 + 2*num_dim ints per grid

@@ -115,6 +115,8 @@ class ClawData:
     restart: bool = False
     restart_file: str = "fort.chk00000"
     checkpt_style: int = 0
+    checkpt_times: List[float] = field(default_factory=list)
+    checkpt_interval: int = 1
 
     def write(self, path: str) -> None:
         # order follows src/2d/amr2.f90:148-335 (3D: src/3d/amr3.f90)
@@ -181,6 +183,11 @@ class ClawData:
         w.put("restart", bool(self.restart))
         w.put("restart_file", str(self.restart_file))
         w.put("checkpt_style", int(self.checkpt_style))
+        if abs(int(self.checkpt_style)) == 2:
+            w.put("num_checkpt_times", len(self.checkpt_times))
+            w.put("checkpt_times", [float(t) for t in self.checkpt_times])
+        elif abs(int(self.checkpt_style)) == 3:
+            w.put("checkpt_interval", int(self.checkpt_interval))
         w.close()
 
 

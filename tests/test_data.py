@@ -41,3 +41,17 @@ def test_codes(tmp_path):
     assert vals["transverse_waves"] == ["2"]
     regions = [l for l in open(tmp_path / "regions.data") if l.strip() and not l.startswith("#") and "=:" not in l]
     assert len(regions) == 2
+
+
+def test_checkpoint_fields_follow_the_style(tmp_path):
+    """amr3.f90:311-325: style 2 is followed by the checkpoint times, style 3 by the interval."""
+    rd = configs.euler_blast(n=8, levels=2, tfinal=0.1)
+    rd.clawdata.checkpt_style = 2
+    rd.clawdata.checkpt_times = [0.05, 0.08]
+    rd.write(str(tmp_path))
+    names = _names(tmp_path / "claw.data")
+    assert names[-3:] == ["checkpt_style", "num_checkpt_times", "checkpt_times"]
+    rd.clawdata.checkpt_style = 3
+    rd.clawdata.checkpt_interval = 4
+    rd.write(str(tmp_path))
+    assert _names(tmp_path / "claw.data")[-2:] == ["checkpt_style", "checkpt_interval"]
