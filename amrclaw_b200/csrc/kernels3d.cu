@@ -153,10 +153,15 @@ struct Swirl3Phys {
   }
 };
 
-// one tile of sweep direction DIR; sW: the block's wave buffer [NW*NV][SW_T]
+// one tile of sweep direction DIR. sW: the block's shared buffer, first the waves
+// [NW*NV][SW_T], then (after they are read) the transverse terms [12*NV][SW_T] of the
+// tile's cells: the apdq side writes them, the amdq side of the next interface adds to
+// them there, and each cell's terms then go to the stash in one coalesced write
 template <int DIR, class T, class PH>
 __device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, T (*sW)[SW_T]) {
-  constexpr int NV = PH::NV, NW = PH::NW, ST = stash_values(NV);
+  constexpr int NV = PH::NV, NW = PH::NW;
+  T* const sG = &sW[0][0];
+  auto G = [&](int x, int col) -> T& { return sG[x * SW_T + col]; };
   const long long* c0 = A.comp0 + (long long)(DIR - 1) * (A.np + 1);
   const long long* s0 = A.sweep0 + (long long)(DIR - 1) * (A.np + 1);
   const long long first = c0[0], last = c0[A.np];
@@ -256,89 +261,87 @@ __device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, 
         st[(long long)m * ss] = fm;
         st[(long long)(NV + m) * ss] = fp;
       }
-      if (e <= n1) {
-        if (m3 <= 0) {
-          for (int x = 2 * NV; x < ST; ++x) st[(long long)x * ss] = T(0);
-        } else {
-          // apdq side of interface e: the terms of cell e (flux3.f:429-505, 552-628 with i = e)
-          T bm[NV], bp[NV], cm[NV], cp[NV], bmq[NV], bpq[NV], cmq[NV], cpq[NV];
-          ph.template rpt<DIR>(2, 2, AP, bm, bp);
-          ph.template rpt<DIR>(2, 3, AP, cm, cp);
-          if (m3 == 2) { ph.template rpt<DIR>(2, 2, CQ, bmq, bpq); ph.template rpt<DIR>(2, 3, CQ, cmq, cpq); }
-          else {
+      if (e <= n1 && m3 <= 0)
+        for (int x = 2 * NV; x < stash_values(NV); ++x) st[(long long)x * ss] = T(0);
+    }
+  }
+  __syncthreads();  // the waves in sW are read: the buffer takes the transverse terms now
+  if (owned && e <= n1 && m3 > 0) {
+    // apdq side of interface e: the terms of cell e (flux3.f:429-505, 552-628 with i = e)
+    T bm[NV], bp[NV], cm[NV], cp[NV], bmq[NV], bpq[NV], cmq[NV], cpq[NV];
+    ph.template rpt<DIR>(2, 2, AP, bm, bp);
+    ph.template rpt<DIR>(2, 3, AP, cm, cp);
+    if (m3 == 2) { ph.template rpt<DIR>(2, 2, CQ, bmq, bpq); ph.template rpt<DIR>(2, 3, CQ, cmq, cpq); }
+    else {
 #pragma unroll
-            for (int m = 0; m < NV; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
-          }
-          // gadd: (side, offset d) at element 10 + ((side-1)*3 + d+1)*5 + m
-          {
-            T P1[NV], P2[NV], M1[NV], M2[NV];
-            if (m4 > 0) {
-              T t[NV];
-              dt_input<NV>(m4, T(-3), cp, cpq, t);
-              ph.template rptt<DIR>(2, 2, 2, t, P1, P2);
-              dt_input<NV>(m4, T(-3), cm, cmq, t);
-              ph.template rptt<DIR>(2, 2, 1, t, M1, M2);
-            }
+      for (int m = 0; m < NV; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
+    }
+    // gadd (side, offset d): row ((side-1)*3 + d+1)*NV + m of the shared terms
+    {
+      T P1[NV], P2[NV], M1[NV], M2[NV];
+      if (m4 > 0) {
+        T t[NV];
+        dt_input<NV>(m4, T(-3), cp, cpq, t);
+        ph.template rptt<DIR>(2, 2, 2, t, P1, P2);
+        dt_input<NV>(m4, T(-3), cm, cmq, t);
+        ph.template rptt<DIR>(2, 2, 1, t, M1, M2);
+      }
 #pragma unroll
-            for (int m = 0; m < NV; ++m) {
-              T g01 = T(0) - T(0.5) * dtdx * bm[m], g11 = T(0) - T(0.5) * dtdx * bp[m];
-              T g00 = T(0), g02 = T(0), g10 = T(0), g12 = T(0);
-              if (m4 > 0) {
-                g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
-                g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
-                g12 = g12 - c6 * dtdx * dtdz * P2[m];
-                g02 = g02 - c6 * dtdx * dtdz * P1[m];
-                g10 = g10 + c6 * dtdx * dtdz * M2[m];
-                g00 = g00 + c6 * dtdx * dtdz * M1[m];
-              }
-              if (m3 == 2) { g11 = g11 + dtdx * bpq[m]; g01 = g01 + dtdx * bmq[m]; }
-              st[(long long)(2 * NV + 0 * NV + m) * ss] = g00;
-              st[(long long)(2 * NV + 1 * NV + m) * ss] = g01;
-              st[(long long)(2 * NV + 2 * NV + m) * ss] = g02;
-              st[(long long)(2 * NV + 3 * NV + m) * ss] = g10;
-              st[(long long)(2 * NV + 4 * NV + m) * ss] = g11;
-              st[(long long)(2 * NV + 5 * NV + m) * ss] = g12;
-            }
-          }
-          // hadd at element 40 + ((side-1)*3 + d+1)*5 + m
-          {
-            T X1[NV], X2[NV], Y1[NV], Y2[NV];
-            if (m4 > 0) {
-              T t[NV];
-              dt_input<NV>(m4, T(-3), bp, bpq, t);
-              ph.template rptt<DIR>(2, 3, 2, t, X1, X2);
-              dt_input<NV>(m4, T(-3), bm, bmq, t);
-              ph.template rptt<DIR>(2, 3, 1, t, Y1, Y2);
-            }
-#pragma unroll
-            for (int m = 0; m < NV; ++m) {
-              T h01 = T(0) - T(0.5) * dtdx * cm[m], h11 = T(0) - T(0.5) * dtdx * cp[m];
-              T h00 = T(0), h02 = T(0), h10 = T(0), h12 = T(0);
-              if (m4 > 0) {
-                h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
-                h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
-                h12 = h12 - c6 * dtdx * dtdy * X2[m];
-                h02 = h02 - c6 * dtdx * dtdy * X1[m];
-                h10 = h10 + c6 * dtdx * dtdy * Y2[m];
-                h00 = h00 + c6 * dtdx * dtdy * Y1[m];
-              }
-              if (m3 == 2) { h11 = h11 + dtdx * cpq[m]; h01 = h01 + dtdx * cmq[m]; }
-              st[(long long)(8 * NV + 0 * NV + m) * ss] = h00;
-              st[(long long)(8 * NV + 1 * NV + m) * ss] = h01;
-              st[(long long)(8 * NV + 2 * NV + m) * ss] = h02;
-              st[(long long)(8 * NV + 3 * NV + m) * ss] = h10;
-              st[(long long)(8 * NV + 4 * NV + m) * ss] = h11;
-              st[(long long)(8 * NV + 5 * NV + m) * ss] = h12;
-            }
-          }
+      for (int m = 0; m < NV; ++m) {
+        T g01 = T(0) - T(0.5) * dtdx * bm[m], g11 = T(0) - T(0.5) * dtdx * bp[m];
+        T g00 = T(0), g02 = T(0), g10 = T(0), g12 = T(0);
+        if (m4 > 0) {
+          g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
+          g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
+          g12 = g12 - c6 * dtdx * dtdz * P2[m];
+          g02 = g02 - c6 * dtdx * dtdz * P1[m];
+          g10 = g10 + c6 * dtdx * dtdz * M2[m];
+          g00 = g00 + c6 * dtdx * dtdz * M1[m];
         }
+        if (m3 == 2) { g11 = g11 + dtdx * bpq[m]; g01 = g01 + dtdx * bmq[m]; }
+        G(0 * NV + m, l) = g00;
+        G(1 * NV + m, l) = g01;
+        G(2 * NV + m, l) = g02;
+        G(3 * NV + m, l) = g10;
+        G(4 * NV + m, l) = g11;
+        G(5 * NV + m, l) = g12;
+      }
+    }
+    // hadd: row (6 + (side-1)*3 + d+1)*NV + m
+    {
+      T X1[NV], X2[NV], Y1[NV], Y2[NV];
+      if (m4 > 0) {
+        T t[NV];
+        dt_input<NV>(m4, T(-3), bp, bpq, t);
+        ph.template rptt<DIR>(2, 3, 2, t, X1, X2);
+        dt_input<NV>(m4, T(-3), bm, bmq, t);
+        ph.template rptt<DIR>(2, 3, 1, t, Y1, Y2);
+      }
+#pragma unroll
+      for (int m = 0; m < NV; ++m) {
+        T h01 = T(0) - T(0.5) * dtdx * cm[m], h11 = T(0) - T(0.5) * dtdx * cp[m];
+        T h00 = T(0), h02 = T(0), h10 = T(0), h12 = T(0);
+        if (m4 > 0) {
+          h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
+          h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
+          h12 = h12 - c6 * dtdx * dtdy * X2[m];
+          h02 = h02 - c6 * dtdx * dtdy * X1[m];
+          h10 = h10 + c6 * dtdx * dtdy * Y2[m];
+          h00 = h00 + c6 * dtdx * dtdy * Y1[m];
+        }
+        if (m3 == 2) { h11 = h11 + dtdx * cpq[m]; h01 = h01 + dtdx * cmq[m]; }
+        G(6 * NV + m, l) = h00;
+        G(7 * NV + m, l) = h01;
+        G(8 * NV + m, l) = h02;
+        G(9 * NV + m, l) = h10;
+        G(10 * NV + m, l) = h11;
+        G(11 * NV + m, l) = h12;
       }
     }
   }
   __syncthreads();
   // amdq side of interface e: the terms of cell e-1, owned by thread l-1 of this tile
   if (live && m3 > 0 && e >= 2 && l >= 2) {
-    T* sc = st - 1;
     T bm[NV], bp[NV], cm[NV], cp[NV], bmq[NV], bpq[NV], cmq[NV], cpq[NV];
     ph.template rpt<DIR>(1, 2, AM, bm, bp);
     ph.template rpt<DIR>(1, 3, AM, cm, cp);
@@ -358,26 +361,26 @@ __device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, 
       }
 #pragma unroll
       for (int m = 0; m < NV; ++m) {
-        T g01 = sc[(long long)(2 * NV + 1 * NV + m) * ss], g11 = sc[(long long)(2 * NV + 4 * NV + m) * ss];
+        T g01 = G(1 * NV + m, l - 1), g11 = G(4 * NV + m, l - 1);
         g01 = g01 - T(0.5) * dtdx * bm[m];
         g11 = g11 - T(0.5) * dtdx * bp[m];
         if (m4 > 0) {
-          T g00 = sc[(long long)(2 * NV + 0 * NV + m) * ss], g02 = sc[(long long)(2 * NV + 2 * NV + m) * ss];
-          T g10 = sc[(long long)(2 * NV + 3 * NV + m) * ss], g12 = sc[(long long)(2 * NV + 5 * NV + m) * ss];
+          T g00 = G(0 * NV + m, l - 1), g02 = G(2 * NV + m, l - 1);
+          T g10 = G(3 * NV + m, l - 1), g12 = G(5 * NV + m, l - 1);
           g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
           g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
           g12 = g12 - c6 * dtdx * dtdz * P2[m];
           g02 = g02 - c6 * dtdx * dtdz * P1[m];
           g10 = g10 + c6 * dtdx * dtdz * M2[m];
           g00 = g00 + c6 * dtdx * dtdz * M1[m];
-          sc[(long long)(2 * NV + 0 * NV + m) * ss] = g00;
-          sc[(long long)(2 * NV + 2 * NV + m) * ss] = g02;
-          sc[(long long)(2 * NV + 3 * NV + m) * ss] = g10;
-          sc[(long long)(2 * NV + 5 * NV + m) * ss] = g12;
+          G(0 * NV + m, l - 1) = g00;
+          G(2 * NV + m, l - 1) = g02;
+          G(3 * NV + m, l - 1) = g10;
+          G(5 * NV + m, l - 1) = g12;
         }
         if (m3 == 2) { g11 = g11 - dtdx * bpq[m]; g01 = g01 - dtdx * bmq[m]; }
-        sc[(long long)(2 * NV + 1 * NV + m) * ss] = g01;
-        sc[(long long)(2 * NV + 4 * NV + m) * ss] = g11;
+        G(1 * NV + m, l - 1) = g01;
+        G(4 * NV + m, l - 1) = g11;
       }
     }
     {
@@ -391,39 +394,48 @@ __device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, 
       }
 #pragma unroll
       for (int m = 0; m < NV; ++m) {
-        T h01 = sc[(long long)(8 * NV + 1 * NV + m) * ss], h11 = sc[(long long)(8 * NV + 4 * NV + m) * ss];
+        T h01 = G(7 * NV + m, l - 1), h11 = G(10 * NV + m, l - 1);
         h01 = h01 - T(0.5) * dtdx * cm[m];
         h11 = h11 - T(0.5) * dtdx * cp[m];
         if (m4 > 0) {
-          T h00 = sc[(long long)(8 * NV + 0 * NV + m) * ss], h02 = sc[(long long)(8 * NV + 2 * NV + m) * ss];
-          T h10 = sc[(long long)(8 * NV + 3 * NV + m) * ss], h12 = sc[(long long)(8 * NV + 5 * NV + m) * ss];
+          T h00 = G(6 * NV + m, l - 1), h02 = G(8 * NV + m, l - 1);
+          T h10 = G(9 * NV + m, l - 1), h12 = G(11 * NV + m, l - 1);
           h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
           h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
           h12 = h12 - c6 * dtdx * dtdy * X2[m];
           h02 = h02 - c6 * dtdx * dtdy * X1[m];
           h10 = h10 + c6 * dtdx * dtdy * Y2[m];
           h00 = h00 + c6 * dtdx * dtdy * Y1[m];
-          sc[(long long)(8 * NV + 0 * NV + m) * ss] = h00;
-          sc[(long long)(8 * NV + 2 * NV + m) * ss] = h02;
-          sc[(long long)(8 * NV + 3 * NV + m) * ss] = h10;
-          sc[(long long)(8 * NV + 5 * NV + m) * ss] = h12;
+          G(6 * NV + m, l - 1) = h00;
+          G(8 * NV + m, l - 1) = h02;
+          G(9 * NV + m, l - 1) = h10;
+          G(11 * NV + m, l - 1) = h12;
         }
         if (m3 == 2) { h11 = h11 - dtdx * cpq[m]; h01 = h01 - dtdx * cmq[m]; }
-        sc[(long long)(8 * NV + 1 * NV + m) * ss] = h01;
-        sc[(long long)(8 * NV + 4 * NV + m) * ss] = h11;
+        G(7 * NV + m, l - 1) = h01;
+        G(10 * NV + m, l - 1) = h11;
       }
     }
   }
+  __syncthreads();
+  // the cell's transverse terms to the stash
+  if (owned && e <= n1 && m3 > 0)
+    for (int x = 0; x < 12 * NV; ++x) st[(long long)(2 * NV + x) * ss] = G(x, l);
   // block-wide max of the Courant number, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
   if ((threadIdx.x & 31) == 0 && cfl > T(0)) atomic_max_nonneg(A.cflmax, (double)cfl);
 }
 
 // one launch per direction: a block per tile
+// shared memory of a sweep block: the larger of the wave buffer and the transverse terms
+template <class T, class PH>
+constexpr int sweep3_smem_bytes() {
+  return (PH::NW > 12 ? PH::NW : 12) * PH::NV * SW_T * (int)sizeof(T);
+}
 template <int DIR, class T, class PH>
 __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
-  __shared__ T sW[PH::NW * PH::NV][SW_T];
-  sweep3_tile<DIR, T, PH>(A, blockIdx.x, sW);
+  extern __shared__ __align__(16) unsigned char sweep_smem[];
+  sweep3_tile<DIR, T, PH>(A, blockIdx.x, reinterpret_cast<T (*)[SW_T]>(sweep_smem));
 }
 
 // persistent work queue over the tiles of all three directions of the level (x tiles,
@@ -432,7 +444,8 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
 // waits on another.
 template <class T, class PH>
 __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_queue_kernel(Step3Args A, unsigned int nx, unsigned int nxy, unsigned int ntot) {
-  __shared__ T sW[PH::NW * PH::NV][SW_T];
+  extern __shared__ __align__(16) unsigned char sweep_smem[];
+  T (*sW)[SW_T] = reinterpret_cast<T (*)[SW_T]>(sweep_smem);
   __shared__ unsigned int item;
   for (;;) {
     __syncthreads();  // the previous tile is done with sW and item
@@ -1108,6 +1121,15 @@ int grid_for(long long n, int block) {
 template <class T, class PH>
 static int launch_step3_t(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s) {
   auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
+  constexpr int smem = sweep3_smem_bytes<T, PH>();
+  static const bool smem_set = [] {
+    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<1, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<2, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<3, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    AMR_CUDA(cudaFuncSetAttribute(sweep3_queue_kernel<T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return true;
+  }();
+  (void)smem_set;
   int n = 0;
   if (a.queue) {
     const unsigned nx = tiles(items[0]), nxy = nx + tiles(items[1]), ntot = nxy + tiles(items[2]);
@@ -1117,17 +1139,17 @@ static int launch_step3_t(const Step3Args& a, const long long items[3], long lon
         int dev = 0, sms = 0, per_sm = 0;
         AMR_CUDA(cudaGetDevice(&dev));
         AMR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        AMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep3_queue_kernel<T, PH>, SW_T, 0));
+        AMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep3_queue_kernel<T, PH>, SW_T, smem));
         return std::max(1, sms * per_sm);
       }();
       AMR_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned int), s));
-      sweep3_queue_kernel<T, PH><<<std::min<unsigned>(ntot, (unsigned)resident), SW_T, 0, s>>>(a, nx, nxy, ntot);
+      sweep3_queue_kernel<T, PH><<<std::min<unsigned>(ntot, (unsigned)resident), SW_T, smem, s>>>(a, nx, nxy, ntot);
       ++n;
     }
   } else {
-    if (items[0] > 0) { sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, 0, s>>>(a); ++n; }
-    if (items[1] > 0) { sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, 0, s>>>(a); ++n; }
-    if (items[2] > 0) { sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, 0, s>>>(a); ++n; }
+    if (items[0] > 0) { sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, smem, s>>>(a); ++n; }
+    if (items[1] > 0) { sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, smem, s>>>(a); ++n; }
+    if (items[2] > 0) { sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, smem, s>>>(a); ++n; }
   }
   AMR_CUDA(cudaGetLastError());
   if (faces > 0) { face3_kernel<T, PH::NV><<<grid_for(faces, 128), 128, 0, s>>>(a); ++n; }
