@@ -55,8 +55,8 @@ def workload(name: str):
 FLOPS_PER_CELL_UPDATE_3D = 10.4e3
 # DRAM bytes per cell-update of the same kernels (sweeps, face gather, update): ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of a level-1 substep of the 64^3 blast,
-# 1,108 MB over 262,144 cell-updates
-DRAM_BYTES_PER_CELL_UPDATE_3D = 1108.3e6 / 262144
+# 1,070 MB over 262,144 cell-updates
+DRAM_BYTES_PER_CELL_UPDATE_3D = 1070.2e6 / 262144
 
 
 def fp64_peak_tflops() -> float:
