@@ -218,7 +218,7 @@ class Amr3Gpu : public AmrSolver {
     newfill.free_dev();
     pool.destroy(); regs.destroy();
     stg.destroy();
-    d_patches.free(); d_stash.free(); d_flux.free(); d_gauge_out.free();
+    d_patches.free(); d_stash.free(); d_flux.free(); d_gauge_out.free(); d_aux_jobs.free(); d_aux_fac.free();
     for (DBuf<int8_t>* b : {&lv_a, &lv_b, &lv_n, &lv_t1, &lv_t2}) b->free();
     lv_boxes.free(); lv_proj.free(); lv_c0.free(); lv_plist.free();
     if (lv_host) cudaFreeHost(lv_host);
@@ -280,50 +280,64 @@ class Amr3Gpu : public AmrSolver {
   double sph_x = 0.5, sph_y = 0.25, sph_z = 0.5, sph_r = 0.15, vel_period = 0.0;
 
   // setaux of the swirl (tests/advection_3d_swirl/setaux.f:2-85): u, v, w at the left x-,
-  // y- and z-face of every cell of the enlarged patch, layout [ma][k][j][i]
-  void setaux(const HPatch3& g, double dx, double dy, double dz, std::vector<double>& a) const {
+  // y- and z-face of every cell of the enlarged patch, as one-dimensional factors
+  void aux_factors(const HPatch3& g, double dx, double dy, double dz, double* f) const {
     const int mi = g.nx() + 2 * G3, mj = g.ny() + 2 * G3, mk = g.nz() + 2 * G3;
-    const long long pl = (long long)mi * mj * mk;
-    a.assign((size_t)pl * 3, 0.0);
     const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
     const double dx2 = 0.5 * dx, dy2 = 0.5 * dy, dz2 = 0.5 * dz;
-    auto su = [&](double x, double y, double z) { double s = std::sin(pi * x); return 2.0 * (s * s) * std::sin(pi2 * y) * std::sin(pi2 * z); };
-    auto sv = [&](double x, double y, double z) { double s = std::sin(pi * y); return -std::sin(pi2 * x) * (s * s) * std::sin(pi2 * z); };
-    auto sw = [&](double x, double y, double z) { double s = std::sin(pi * z); return -std::sin(pi2 * x) * std::sin(pi2 * y) * (s * s); };
+    // Each velocity is a product of one-dimensional factors, evaluated left to right:
+    //   u(x,y,z) = ((2 sin^2(pi x)) sin(2 pi y)) sin(2 pi z)   at (xc - dx/2, yc, zc)
+    //   v(x,y,z) = ((-sin(2 pi x)) sin^2(pi y)) sin(2 pi z)    at (xc, yc - dy/2, zc)
+    //   w(x,y,z) = ((-sin(2 pi x)) sin(2 pi y)) sin^2(pi z)    at (xc, yc, zc - dz/2)
+    // so the factors are computed once per index along each axis (here, with the host's
+    // sin) and multiplied on the device in the same order: the products round as the
+    // expressions of setaux.f do. Layout: ua, va, wa [mi], ub, vb, wb [mj], uc, vc, wc [mk].
+    double *ua = f, *va = ua + mi, *wa = va + mi, *ub = wa + mi, *vb = ub + mj, *wb = vb + mj;
+    double *uc = wb + mj, *vc = uc + mk, *wc = vc + mk;
+    for (int i = 1 - G3; i <= g.nx() + G3; ++i) {
+      const double xc = g.xlo + (i - 0.5) * dx;
+      const double s = std::sin(pi * (xc - dx2));
+      ua[i - 1 + G3] = 2.0 * (s * s);
+      va[i - 1 + G3] = wa[i - 1 + G3] = -std::sin(pi2 * xc);
+    }
+    for (int j = 1 - G3; j <= g.ny() + G3; ++j) {
+      const double yc = g.ylo + (j - 0.5) * dy;
+      const double s = std::sin(pi * (yc - dy2));
+      ub[j - 1 + G3] = wb[j - 1 + G3] = std::sin(pi2 * yc);
+      vb[j - 1 + G3] = s * s;
+    }
     for (int k = 1 - G3; k <= g.nz() + G3; ++k) {
       const double zc = g.zlo + (k - 0.5) * dz;
-      for (int j = 1 - G3; j <= g.ny() + G3; ++j) {
-        const double yc = g.ylo + (j - 0.5) * dy;
-        for (int i = 1 - G3; i <= g.nx() + G3; ++i) {
-          const double xc = g.xlo + (i - 0.5) * dx;
-          const long long at = ((long long)(k - 1 + G3) * mj + (j - 1 + G3)) * mi + (i - 1 + G3);
-          a[at] = su(xc - dx2, yc, zc);
-          a[pl + at] = sv(xc, yc - dy2, zc);
-          a[2 * pl + at] = sw(xc, yc, zc - dz2);
-        }
-      }
+      const double s = std::sin(pi * (zc - dz2));
+      uc[k - 1 + G3] = vc[k - 1 + G3] = std::sin(pi2 * zc);
+      wc[k - 1 + G3] = s * s;
     }
   }
-  // setaux of new patches, computed on the host threads, into aux (and the setaux copy the
-  // time-modulated b4step3 scales)
+  // setaux of new patches (tests/advection_3d_swirl/setaux.f:2-85) into their aux blocks,
+  // and into the unscaled copy the time-modulated b4step3 reads
+  DBuf<Setaux3Job> d_aux_jobs;
+  DBuf<double> d_aux_fac;
   void init_aux(const std::vector<int>& ms) {
     if (p.naux == 0 || ms.empty()) return;
     HPROF("init_aux3");
-    std::vector<std::vector<double>> A(ms.size());
+    std::vector<Setaux3Job> jobs(ms.size());
+    long long nf = 0, maxc = 0;
+    for (size_t k = 0; k < ms.size(); ++k) {
+      const int m = ms[k];
+      Setaux3Job& J = jobs[k];
+      J.aux = node[m].aux; J.mi = mitot(m); J.mj = mjtot(m); J.mk = mktot(m); J.f0 = nf;
+      nf += 3LL * (J.mi + J.mj + J.mk);
+      maxc = std::max(maxc, (long long)J.mi * J.mj * J.mk);
+    }
+    std::vector<double> fac((size_t)nf);
     pool_host.run((int)ms.size(), [&](int k) {
       const HPatch3& g = node[ms[k]];
-      setaux(g, hxposs[g.level], hyposs[g.level], hzposs[g.level], A[k]);
+      aux_factors(g, hxposs[g.level], hyposs[g.level], hzposs[g.level], fac.data() + jobs[k].f0);
     });
-    std::vector<float> af;
-    for (size_t k = 0; k < ms.size(); ++k) {
-      const HPatch3& g = node[ms[k]];
-      const void* src = A[k].data();
-      if (f32) { af.assign(A[k].begin(), A[k].end()); src = af.data(); }
-      const size_t bytes = elem() * A[k].size();
-      for (int copy = 0; copy < (vel_period > 0.0 ? 2 : 1); ++copy)
-        AMR_CUDA(cudaMemcpyAsync(pool_bytes() + elem() * (g.aux + copy * g.na), stg.put(src, bytes, st), bytes, cudaMemcpyHostToDevice, st));
-      h2d_bytes += (vel_period > 0.0 ? 2.0 : 1.0) * bytes;
-    }
+    d_aux_jobs.upload(jobs, st, stg);
+    d_aux_fac.upload(fac, st, stg);
+    launch_setaux3(pool.d, d_aux_jobs.d, (int)jobs.size(), maxc, d_aux_fac.d, vel_period > 0.0 ? 2 : 1, st, f32);
+    ++nkernels;
   }
 
   // qinit (Euler blast): rho = 1, u = 0, p = pin within r0 of the centre, pout outside; layout [m][k][j][i]

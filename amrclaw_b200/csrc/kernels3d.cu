@@ -1200,6 +1200,37 @@ void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Jo
   else qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt, dt_dev);
   AMR_CUDA(cudaGetLastError());
 }
+template <class T>
+__global__ void setaux3_kernel(T* pool, const Setaux3Job* jobs, int njobs, const double* fac, int copies) {
+  const int jb = blockIdx.y;
+  if (jb >= njobs) return;
+  const Setaux3Job J = jobs[jb];
+  const long long pl = (long long)J.mi * J.mj * J.mk;
+  const double* ua = fac + J.f0;
+  const double *va = ua + J.mi, *wa = va + J.mi, *ub = wa + J.mi, *vb = ub + J.mj, *wb = vb + J.mj;
+  const double *uc = wb + J.mj, *vc = uc + J.mk, *wc = vc + J.mk;
+  T* a = pool + J.aux;
+  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < pl; x += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(x % J.mi), j = (int)((x / J.mi) % J.mj), k = (int)(x / ((long long)J.mi * J.mj));
+    const double u = ua[i] * ub[j] * uc[k], v = va[i] * vb[j] * vc[k], w = wa[i] * wb[j] * wc[k];
+    for (int c = 0; c < copies; ++c) {
+      T* o = a + (long long)c * 3 * pl;
+      o[x] = (T)u; o[pl + x] = (T)v; o[2 * pl + x] = (T)w;
+    }
+  }
+}
+void launch_setaux3(void* pool, const Setaux3Job* jobs, int njobs, long long max_cells, const double* fac, int copies,
+                    cudaStream_t s, bool f32) {
+  if (njobs <= 0) return;
+  const int bx = (int)std::max<long long>(1, std::min<long long>((max_cells + 255) / 256, 1024));
+  for (int base = 0; base < njobs; base += 65535) {
+    const int cnt = std::min(65535, njobs - base);
+    if (f32) setaux3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<float*>(pool), jobs + base, cnt, fac, copies);
+    else setaux3_kernel<<<dim3(bx, cnt), 256, 0, s>>>(static_cast<double*>(pool), jobs + base, cnt, fac, copies);
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+
 // valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
 template <class T>
 __global__ void zero_tiny3_kernel(T* pool, const PatchDev* patches, const int* plist, int np, int nvar) {

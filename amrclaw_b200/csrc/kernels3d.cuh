@@ -108,6 +108,14 @@ void launch_fad3(const void* flux, long long flux_stride, const long long* face0
                  const double* dt_dev = nullptr);
 void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
                  int nvar, double hx, double hy, double hz, double delt, cudaStream_t s, bool f32, const double* dt_dev = nullptr);
+// setaux of the swirl from its one-dimensional factors: for a patch whose enlarged array
+// has mi x mj x mk cells and whose aux block starts at pool offset `aux`, fac + f0 holds
+// ua, va, wa [mi], ub, vb, wb [mj], uc, vc, wc [mk]; the kernel writes
+// aux = (ua*ub)*uc, (va*vb)*vc, (wa*wb)*wc in [3][k][j][i], `copies` times (the
+// time-modulated field keeps a second, unscaled copy)
+struct Setaux3Job { long long aux, f0; int mi, mj, mk, pad; };
+void launch_setaux3(void* pool, const Setaux3Job* jobs, int njobs, long long max_cells, const double* fac, int copies,
+                    cudaStream_t s, bool f32);
 // valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
 void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32);
 // b4step3 of the time-modulated swirl: aux = c * aux0 over the enlarged patches of plist

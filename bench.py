@@ -26,6 +26,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -46,6 +48,21 @@ def workload(name: str):
         rd = configs.euler_quadrants(n=100, levels=4, tfinal=0.8)
         return rd, dict(workload=name, base_grid="100x100", levels=4, ratio=2, solver="Roe+entropy fix", meqn=4,
                         naux=0, tfinal=0.8, precision="fp64"), 4, 0, 2
+    if name == "advection2d_square":
+        rd = configs.advection_square_bench(n=50, tfinal=2.0, levels=3)
+        return rd, dict(workload=name, base_grid="50x50", levels=3, ratio=2, solver="constant advection (0.5, 1.0)",
+                        meqn=1, naux=0, tfinal=2.0, bc="periodic", limiter="MC", precision="fp64"), 1, 0, 2
+    if name == "acoustics2d_pulse_fp32":
+        from amrclaw_b200 import problems
+        rd = problems.acoustics_pulse(64, levels=4, ratio=2, tfinal=0.4)
+        return rd, dict(workload=name, base_grid="64x64", levels=4, ratio=2, solver="acoustics rho=1 K=4", meqn=3,
+                        naux=0, tfinal=0.4, precision="fp32"), 3, 0, 2
+    if name == "swirl3d_fp32":
+        from amrclaw_b200 import problems
+        rd = problems.advection_swirl3d(n=32, levels=4, tfinal=1.5)
+        return rd, dict(workload=name, base_grid="32x32x32", levels=4, ratio=2,
+                        solver="advection in the swirl field x cos(pi t / 1.5), sphere r=0.15", meqn=1, naux=3,
+                        tfinal=1.5, precision="fp32"), 1, 3, 3
     raise SystemExit("unknown workload %s" % name)
 
 
@@ -314,13 +331,15 @@ def main():
 
     from amrclaw_b200 import Solver, replicas
     rd, cfg, nvar, naux, ndim = workload(args.workload)
-    bytes_per_update = (2 * nvar + naux) * 8
+    prec = cfg["precision"]
+    headline = args.workload == "euler3d_blast"  # the workload the FP64 roof and traffic figures were measured on
+    bytes_per_update = (2 * nvar + naux) * (4 if prec == "fp32" else 8)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 
     with tempfile.TemporaryDirectory() as d:
         rd.write(d)
         # ---------------- batched path (the value)
-        s = Solver(d, batched=True)
+        s = Solver(d, batched=True, precision=prec)
         s.run(args.warmup)
         s.set_profile(True)
         i0 = s.info()
@@ -355,7 +374,7 @@ def main():
         # ---------------- plain per-patch path on the same steps, and both paths replayed
         # from captured CUDA graphs (3D)
         def leg(batched, graphs, schedule=0):
-            p = Solver(d, batched=batched, graphs=graphs, schedule=schedule)
+            p = Solver(d, batched=batched, graphs=graphs, schedule=schedule, precision=prec)
             p.run(args.warmup)
             j0 = p.info()
             pms = 0.0
@@ -392,7 +411,7 @@ def main():
         # level-1 mass read back after every coarse step, final cell values read back
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        e = Solver(d, batched=True)
+        e = Solver(d, batched=True, precision=prec)
         nstep = 0
         while not e.info()["finished"]:
             e.run(1)
@@ -401,25 +420,41 @@ def main():
         vals = e.values()
         t1 = time.perf_counter()
         einf = e.info()
+        egrids = e.grids()
         e.close()
         e2e_value = einf["cell_updates"] / (t1 - t0)
         h2d = einf["h2d_bytes"]
         d2h = vals.nbytes + 8 * nstep
+        # the FP32 form's level-1 L1 error against the FP64 path (bit-identical to the oracle
+        # in the parity tests) over the same whole solve
+        l1_err = 0.0
+        if prec == "fp32":
+            from amrclaw_b200 import fields
+            dims = tuple(int(x) for x in cfg["base_grid"].split("x"))
+            with Solver(d, batched=True) as f64:
+                f64.run(0)
+                ref = fields.level_array(f64.grids(), f64.values(), nvar, 1, dims)
+            got = fields.level_array(egrids, vals, nvar, 1, dims)
+            width = [rd.clawdata.upper[k] - rd.clawdata.lower[k] for k in range(ndim)]
+            vol = float(np.prod([width[k] / dims[k] for k in range(ndim)]))
+            _, rel = fields.l1_error(got, ref, vol)
+            l1_err = float(rel.max())
 
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
     peak, peak_kind = peaks()
+    # the FP32-form and serving legs run with the headline workload (they solve fixed problems of their own)
     fp32 = None
-    if not args.no_cpu_baseline:
+    if headline and not args.no_cpu_baseline:
         rd3, cfg3, _, _, nd3 = workload(args.workload)
         fp32 = fp32_leg(os.cpu_count() or 1, rd3 if nd3 == 3 else None, cfg3)
     os.environ.setdefault("AMRGPU_HOST_THREADS", "2")
-    serving = serving_leg() if not args.no_cpu_baseline else None
+    serving = serving_leg() if headline and not args.no_cpu_baseline else None
     achieved = kern_cells * bytes_per_update / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
     fp64_roof = None
-    if ndim == 3 and kern_ms > 0:
+    if headline and kern_ms > 0:
         # the roof that binds this step: FP64 arithmetic, against a DGEMM measured here
         fpk = fp64_peak_tflops()
         ach = kern_cells * FLOPS_PER_CELL_UPDATE_3D / (kern_ms * 1e-3) / 1e12
@@ -444,7 +479,8 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded initial conditions of the workload",
+        "vs_baseline": None, "dtype": "f32" if prec == "fp32" else "f64",
+        "data": "synthetic: seeded initial conditions of the workload",
         "config": dict(cfg, l2="flushed between steps (256 MB write)", parallelism="replicas" if world > 1 else "single"),
         "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": plain_ms,
                   "speedup_batched_over_plain": value / plain_value if plain_value else None,
@@ -454,13 +490,13 @@ def main():
                                                          if batched_advance_ms > 0 else None)},
         "schedules": graph_legs or None,
         "advance_ms_per_step": batched_advance_ms, "regrid_ms_per_step": batched_regrid_ms,
-        "l1_err_vs_fp64": 0.0,
+        "l1_err_vs_fp64": l1_err,
         "fp32_form": fp32,
         "serving": serving,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": (DRAM_BYTES_PER_CELL_UPDATE_3D * kern_cells / step_launches
-                                 if ndim == 3 and step_launches else None),
+                                 if headline and step_launches else None),
                      "traffic_note": "DRAM bytes per level substep of the step kernels: ncu bytes per cell-update "
                                      "of a level-1 substep times the average cells of a timed substep",
                      "kernel": "sweep3<1..3> + face3 + update3" if ndim == 3 else "step2 sweeps + update",
