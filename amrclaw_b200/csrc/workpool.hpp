@@ -4,6 +4,7 @@
 #pragma once
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdlib>
 #include <exception>
@@ -30,30 +31,60 @@ class WorkPool {
   ~WorkPool() {
     {
       std::lock_guard<std::mutex> g(mu_);
-      stop_ = true;
+      stop_.store(true);
     }
     cv_.notify_all();
     for (auto& w : workers_) w.join();
   }
   int size() const { return (int)workers_.size() + 1; }
 
-  // Calls f(i) for i in [0, n) on all threads; rethrows the first exception.
+  // Calls f(i) for i in [0, n) on the caller and up to n-1 helpers; rethrows the first
+  // exception. A regrid makes many such calls in a row: idle workers poll for kSpinUs
+  // microseconds before they sleep, so a call that follows soon finds them awake, and only
+  // as many workers as there are items beyond the first join a call.
   void run(int n, const std::function<void(int)>& f) {
     if (n <= 0) return;
-    if (workers_.empty() || n == 1) { for (int i = 0; i < n; ++i) f(i); return; }
+    const int helpers = std::min<int>((int)workers_.size(), n - 1);
+    if (helpers == 0) { for (int i = 0; i < n; ++i) f(i); return; }
     {
       std::lock_guard<std::mutex> g(mu_);
-      job_ = &f; n_ = n; next_.store(0); err_ = nullptr; active_ = (int)workers_.size(); ++gen_;
+      job_ = &f; n_ = n; next_.store(0); err_ = nullptr;
+      active_.store(helpers);
+      const unsigned long long gen = (state_.load() >> 32) + 1;
+      state_.store((gen << 32) | (unsigned)helpers, std::memory_order_release);
     }
     cv_.notify_all();
     work();
-    std::unique_lock<std::mutex> lk(mu_);
-    done_cv_.wait(lk, [this] { return active_ == 0; });
-    job_ = nullptr;
+    spin_while([this] { return active_.load(std::memory_order_acquire) != 0; });
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      done_cv_.wait(lk, [this] { return active_.load() == 0; });
+      job_ = nullptr;
+    }
     if (err_) std::rethrow_exception(err_);
   }
 
  private:
+  static constexpr int kSpinUs = 100;
+  static void relax() {
+#if defined(__x86_64__) || defined(__i386__)
+    __builtin_ia32_pause();
+#else
+    std::this_thread::yield();
+#endif
+  }
+  // polls cond() for at most kSpinUs microseconds and returns as soon as it is false;
+  // after the first polls it yields between polls, so that with more threads than cores
+  // the threads it waits for get to run
+  template <class C>
+  static void spin_while(C cond) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int s = 0; cond(); ++s) {
+      if (s < 256) relax();
+      else std::this_thread::yield();
+      if ((s & 31) == 31 && std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(kSpinUs)) return;
+    }
+  }
   void work() {
     while (true) {
       const int i = next_.fetch_add(1);
@@ -66,19 +97,32 @@ class WorkPool {
       }
     }
   }
+  // state_ = (generation << 32) | free helper slots of that generation's call: a worker
+  // takes at most one slot of each generation it sees, so every helper counted in
+  // active_ belongs to the call that set it
   void loop() {
-    unsigned seen = 0;
+    // generation 0 is "no call yet": a worker that starts after the first call was posted
+    // still joins it
+    unsigned long long seen = 0;
     while (true) {
-      {
+      spin_while([&] { return (state_.load(std::memory_order_acquire) >> 32) == seen && !stop_.load(); });
+      if ((state_.load(std::memory_order_acquire) >> 32) == seen) {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
-        if (stop_) return;
-        seen = gen_;
+        cv_.wait(lk, [&] { return stop_.load() || (state_.load() >> 32) != seen; });
       }
+      if (stop_.load()) return;
+      unsigned long long v = state_.load(std::memory_order_acquire);
+      bool took = false;
+      while (true) {
+        seen = v >> 32;
+        if ((v & 0xffffffffull) == 0) break;
+        if (state_.compare_exchange_weak(v, v - 1, std::memory_order_acq_rel)) { took = true; break; }
+      }
+      if (!took) continue;  // this call has its helpers
       work();
-      {
+      if (active_.fetch_sub(1) == 1) {
         std::lock_guard<std::mutex> g(mu_);
-        if (--active_ == 0) done_cv_.notify_all();
+        done_cv_.notify_all();
       }
     }
   }
@@ -86,10 +130,10 @@ class WorkPool {
   std::mutex mu_;
   std::condition_variable cv_, done_cv_;
   const std::function<void(int)>* job_ = nullptr;
-  int n_ = 0, active_ = 0;
-  std::atomic<int> next_{0};
-  unsigned gen_ = 0;
-  bool stop_ = false;
+  int n_ = 0;
+  std::atomic<int> next_{0}, active_{0};
+  std::atomic<unsigned long long> state_{0};
+  std::atomic<bool> stop_{false};
   std::exception_ptr err_;
 };
 
