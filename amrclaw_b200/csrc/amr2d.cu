@@ -1693,7 +1693,6 @@ class Amr2Gpu {
     if (p.ndim != 2) throw std::runtime_error("this solver handles 2D runs");
     if (p.nghost != 2) throw std::runtime_error("num_ghost must be 2");
     if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
-    if (p.restart || p.checkpt_style != 0) throw std::runtime_error("checkpoint/restart is built for the 3D device path");
     if (p.dimsplit != 0) throw std::runtime_error("only the unsplit method is supported");
     if (p.src_split != 0) throw std::runtime_error("source terms are not supported");
     nvar = p.nvar; ng = p.nghost;
@@ -1731,6 +1730,12 @@ class Amr2Gpu {
     node[10000].nextfree = 0;
     ndfree = 1;
     start_time = p.t0;
+    if (p.restart) {
+      // amr2.f90: the run continues from the checkpoint named in claw.data (restrt.f)
+      const std::string f = p.restart_file;
+      restart_from(!f.empty() && f[0] == '/' ? f : dir + "/" + f);
+      return;
+    }
     // domain.f
     const int ms = nodget();
     node[ms].xlo = xlower; node[ms].ylo = ylower; node[ms].yhi = yupper; node[ms].xhi = xupper;
@@ -1828,6 +1833,151 @@ class Amr2Gpu {
   // valout.f90: zero |q| < 1e-90 in place (the reference does) and optionally write fort.q / fort.t
   void output(double t);
 
+  // ================================================================ check.f / restrt.f
+  // A checkpoint, taken at a coarse-step boundary, holds what the continued run reads:
+  // the scheduler state (time, cycle, step sizes, regrid counters, level times, output
+  // cursor), the grid table with its free list (grid numbers continue as they would have),
+  // both solution buffers of every grid, and the gauge samples so far. Neighbour lists,
+  // register lists, fill programs and step plans are compiled again from the grids; the
+  // flux registers and saved coarse rings are not kept, because each entry that upbnd
+  // will read is rewritten (fluxsv, saveqc, prepf) before it is read. The layout is this
+  // library's own (little-endian, versioned).
+  static constexpr char CHK_MAGIC[8] = {'A', 'M', 'R', 'B', '2', 'C', 'K', '1'};
+  struct ChkHead {
+    int nvar, f32, mxnest, lfine, ncycle, frame, nextout, iout, nnodes, ndfree, gslots, ngrows, ngauges, pad;
+    int icheck[12], lstart[12];
+    double time, start_time, tmass0, cflmax_run, rvol, rvoll[12], possk[12], tlevel[12];
+  };
+  struct ChkNode { int ilo, ihi, jlo, jhi, level, levelptr, nextfree, pad; double xlo, xhi, ylo, yhi, time; };
+  void checkpoint(const std::string& path) {
+    sync_stream();
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write checkpoint " + path);
+    auto put = [&](const void* d, size_t n) {
+      if (n && std::fwrite(d, 1, n, f) != n) { std::fclose(f); throw std::runtime_error("short write to " + path); }
+    };
+    ChkHead h{};
+    h.nvar = nvar; h.f32 = f32 ? 1 : 0; h.mxnest = p.mxnest; h.lfine = lfine; h.ncycle = ncycle; h.frame = frame;
+    h.nextout = tk_nextout; h.iout = tk_iout; h.nnodes = (int)node.size(); h.ndfree = ndfree; h.gslots = gslots;
+    h.ngrows = (int)grows.size(); h.ngauges = (int)glast.size();
+    for (int l = 0; l < 12; ++l) {
+      h.icheck[l] = icheck[l]; h.lstart[l] = lstart[l]; h.rvoll[l] = rvoll[l]; h.possk[l] = possk[l];
+      h.tlevel[l] = tick_started ? tk_tlevel[l] : time;
+    }
+    if (!tick_started) {
+      h.iout = p.iout; h.nextout = 0;
+      if (h.iout == 0) { h.iout = 999999999; h.nextout = p.nout > 0 ? 1 : 0; }
+    }
+    h.time = time; h.start_time = start_time; h.tmass0 = tmass0; h.cflmax_run = cflmax_run; h.rvol = rvol;
+    put(CHK_MAGIC, 8);
+    put(&h, sizeof h);
+    std::vector<ChkNode> nodes(node.size());
+    for (size_t m = 0; m < node.size(); ++m) {
+      const HPatch& g = node[m];
+      nodes[m] = ChkNode{g.ilo, g.ihi, g.jlo, g.jhi, g.level, g.levelptr, g.nextfree, 0, g.xlo, g.xhi, g.ylo, g.yhi, g.time};
+    }
+    put(nodes.data(), sizeof(ChkNode) * nodes.size());
+    std::vector<char> buf;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) {
+        const HPatch& g = node[m];
+        const long long offs[2] = {g.cur == 0 ? g.q0 : g.q1, g.cur == 0 ? g.q1 : g.q0};
+        for (long long off : offs) {
+          buf.resize(elem() * g.nq);
+          AMR_CUDA(cudaMemcpy(buf.data(), reinterpret_cast<char*>(pool.d) + elem() * off, buf.size(), cudaMemcpyDeviceToHost));
+          put(buf.data(), buf.size());
+        }
+      }
+    put(glast.data(), sizeof(double) * glast.size());
+    put(grows.data(), sizeof(GaugeRow) * grows.size());
+    if (gslots) {
+      std::vector<double> gv((size_t)gslots * nvar);
+      AMR_CUDA(cudaMemcpy(gv.data(), d_gauge_out.d, sizeof(double) * gv.size(), cudaMemcpyDeviceToHost));
+      put(gv.data(), sizeof(double) * gv.size());
+    }
+    if (std::fclose(f) != 0) throw std::runtime_error("cannot close " + path);
+  }
+  // restrt.f: the grids and scheduler state of a checkpoint, in place of domain.f/setgrd.f
+  void restart_from(const std::string& path) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot read checkpoint " + path);
+    auto get = [&](void* d, size_t n) {
+      if (n && std::fread(d, 1, n, f) != n) { std::fclose(f); throw std::runtime_error("checkpoint " + path + " is truncated"); }
+    };
+    char magic[8];
+    get(magic, 8);
+    if (std::memcmp(magic, CHK_MAGIC, 8) != 0) { std::fclose(f); throw std::runtime_error(path + " is not a 2D checkpoint of this library"); }
+    ChkHead h{};
+    get(&h, sizeof h);
+    if (h.nvar != nvar || h.f32 != (f32 ? 1 : 0) || h.mxnest != p.mxnest || h.ngauges != (int)p.gauges.size() || h.nnodes < 2 ||
+        h.lfine < 1 || h.lfine > p.mxnest) {
+      std::fclose(f);
+      throw std::runtime_error("checkpoint " + path + " does not match this run (equations, precision, levels or gauges)");
+    }
+    std::vector<ChkNode> nodes((size_t)h.nnodes);
+    get(nodes.data(), sizeof(ChkNode) * nodes.size());
+    node.assign(nodes.size(), HPatch());
+    for (size_t m = 0; m < nodes.size(); ++m) {
+      const ChkNode& c = nodes[m];
+      HPatch& g = node[m];
+      g.ilo = c.ilo; g.ihi = c.ihi; g.jlo = c.jlo; g.jhi = c.jhi; g.level = c.level; g.levelptr = c.levelptr;
+      g.nextfree = c.nextfree; g.xlo = c.xlo; g.xhi = c.xhi; g.ylo = c.ylo; g.yhi = c.yhi; g.time = c.time;
+    }
+    ndfree = h.ndfree; lfine = h.lfine;
+    for (int l = 0; l < 12; ++l) {
+      icheck[l] = h.icheck[l]; lstart[l] = h.lstart[l]; rvoll[l] = h.rvoll[l]; possk[l] = h.possk[l]; tk_tlevel[l] = h.tlevel[l];
+    }
+    ncycle = h.ncycle; frame = h.frame; tk_nextout = h.nextout; tk_iout = h.iout; tick_started = true;
+    time = h.time; start_time = h.start_time; tmass0 = h.tmass0; cflmax_run = h.cflmax_run; rvol = h.rvol;
+    std::vector<char> buf;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m = lstart[lev]; m != 0; m = node[m].levelptr) {
+        alloc_patch(m);
+        HPatch& g = node[m];
+        g.cur = 0;  // q0 takes store1, q1 store2
+        for (long long off : {g.q0, g.q1}) {
+          buf.resize(elem() * g.nq);
+          get(buf.data(), buf.size());
+          AMR_CUDA(cudaMemcpy(reinterpret_cast<char*>(pool.d) + elem() * off, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+        }
+        h2d_bytes += 2.0 * elem() * g.nq;
+      }
+    glast.resize((size_t)h.ngauges);
+    get(glast.data(), sizeof(double) * glast.size());
+    grows.resize((size_t)h.ngrows);
+    get(grows.data(), sizeof(GaugeRow) * grows.size());
+    gslots = h.gslots;
+    if (gslots) {
+      std::vector<double> gv((size_t)gslots * nvar);
+      get(gv.data(), sizeof(double) * gv.size());
+      d_gauge_out.ensure(std::max<size_t>(gv.size() * 2, 4096));
+      AMR_CUDA(cudaMemcpy(d_gauge_out.d, gv.data(), sizeof(double) * gv.size(), cudaMemcpyHostToDevice));
+    }
+    std::fclose(f);
+    for (int lev = 1; lev <= p.mxnest; ++lev) touch(lev);
+    make_lists();
+    for (int lev = 1; lev <= lfine; ++lev) make_bndry(lev);
+    sync_descriptors();
+    for (int lev = 1; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
+    compile_all();
+    record_gauges = true;
+    mbestsrc.assign(p.gauges.size(), 0);
+    setbestsrc();
+    sync_stream();
+  }
+  void checkpoint_file(const char* path) {
+    if (path && *path) { checkpoint(path); return; }
+    char fn[64];
+    if (p.checkpt_style < 0) {
+      std::snprintf(fn, sizeof(fn), "/fort.chk%s", chk_a ? "aaaaa" : "bbbbb");  // check_twofiles.f
+      chk_a = !chk_a;
+    } else std::snprintf(fn, sizeof(fn), "/fort.chk%05d", ncycle);
+    checkpoint(outdir + fn);
+  }
+  bool chk_a = true;
+  int tk_nextchk = 0;
+  bool tk_dumpchk = false, final_chk_done = false;
+
   // ================================================================ tick.f
   void tick() {
     double dtnew[12];
@@ -1842,6 +1992,11 @@ class Amr2Gpu {
       for (int i = 2; i <= p.mxnest; ++i) tlevel[i] = tlevel[1];
       tick_started = true;
     }
+    if (tk_nextchk == 0) {
+      // tick.f:73-81: checkpoint times still to come
+      tk_nextchk = 1;
+      while (tk_nextchk <= (int)p.tchk.size() && p.tchk[tk_nextchk - 1] <= time) ++tk_nextchk;
+    }
     int& iout = tk_iout;
     int& nextout = tk_nextout;
     int cycles_this_call = 0;
@@ -1850,12 +2005,20 @@ class Amr2Gpu {
     const auto tstart = std::chrono::steady_clock::now();
     while (!(ncycle >= p.nstop || time >= p.tfinal)) {
       double outtime = (p.nout > 0) ? (nextout <= p.nout ? p.tout[nextout - 1] : RINF) : p.tfinal;
+      const double chktime = (tk_nextchk <= (int)p.tchk.size()) ? p.tchk[tk_nextchk - 1] : RINF;
       bool dumpout = false;
       if (time < outtime && time + (double)1.001f * possk[1] >= outtime) {
         possk[1] = outtime - time;
         for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
         if (p.nout > 0) { ++nextout; dumpout = true; }
       }
+      // tick.f:146-157: shorten the step to land on a checkpoint time
+      if (time < chktime && time + possk[1] >= chktime) {
+        possk[1] = chktime - time;
+        for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
+        ++tk_nextchk;
+        tk_dumpchk = true;
+      } else tk_dumpchk = false;
       int level = 1;
       ntogo[level] = 1;
       for (int i = 1; i <= 10; ++i) dtnew[i] = RINF;
@@ -1911,9 +2074,19 @@ class Amr2Gpu {
         possk[1] = dtnew[1];
         for (int i = 2; i <= p.mxnest; ++i) possk[i] = possk[i - 1] / kratio[i - 1];
       }
+      // tick.f:322-326
+      if (((p.checkpt_style == 3 || p.checkpt_style == -3) && ncycle % p.checkpt_interval == 0) || tk_dumpchk) {
+        checkpoint_file(nullptr);
+        tk_dumpchk = true;
+      }
       if ((ncycle % iout == 0) || dumpout) output(time);
       ++cycles_this_call;
       if (max_cycles > 0 && cycles_this_call >= max_cycles) break;
+    }
+    // tick.f:365-368: a final checkpoint unless the last step just wrote one
+    if (finished() && p.checkpt_style != 0 && !tk_dumpchk && !final_chk_done) {
+      checkpoint_file(nullptr);
+      final_chk_done = true;
     }
     AMR_CUDA(cudaEventRecord(ev_run1, st));
     sync_stream();
@@ -2036,9 +2209,7 @@ class Solver2 : public AmrSolver {
   void set_schedule(int s) override {
     if (s != 0) throw std::runtime_error("amrgpu_set_schedule: sweep schedules are built for the 3D path");
   }
-  void write_checkpoint(const char*) override {
-    throw std::runtime_error("amrgpu_checkpoint: checkpoint/restart is built for the 3D path");
-  }
+  void write_checkpoint(const char* path) override { g.checkpoint_file(path); }
   void run(int max_cycles) override { g.max_cycles = max_cycles; g.tick(); }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > g.lfine) throw std::runtime_error("level out of range");

@@ -54,17 +54,17 @@ int amrgpu_set_batched(amrgpu_ctx* ctx, int batched);
  * the reference. */
 int amrgpu_set_graphs(amrgpu_ctx* ctx, int on);
 
-/* Writes a checkpoint of a 3D run at the current coarse-step boundary (check.f:4-104):
- * the scheduler state, the grid table with its free list, both solution buffers and the
- * aux block of every grid, and the gauge samples so far. path == NULL: fort.chkNNNNN
+/* Writes a checkpoint of the run at the current coarse-step boundary (check.f:4-104):
+ * the scheduler state, the grid table with its free list, both solution buffers (and, in
+ * 3D, the aux block) of every grid, and the gauge samples so far. path == NULL: fort.chkNNNNN
  * (NNNNN = coarse steps taken) in the output directory, or fort.chkaaaaa / fort.chkbbbbb
  * alternately when checkpt_style < 0. A run continues from it when claw.data sets
  * restart = T and restart_file (restrt.f: amrgpu_init reads it in place of the initial
  * grids); continuing gives the same results as the run that was not interrupted.
  * checkpt_style 2 (at checkpt_times) and 3 (every checkpt_interval coarse steps) write
  * them during amrgpu_run, and any style but 0 writes one at the end (tick.f:322-368).
- * The layout is this library's own, not the reference's fort.chk. 2D contexts return
- * AMRGPU_ERROR. */
+ * The layout is this library's own, not the reference's fort.chk (one layout for 2D
+ * runs, one for 3D). */
 int amrgpu_checkpoint(amrgpu_ctx* ctx, const char* path);
 
 /* Sweep schedule of the batched 3D path. 1: one launch per sweep direction (a block per
