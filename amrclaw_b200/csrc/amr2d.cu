@@ -177,6 +177,11 @@ class Amr2Gpu {
   int status = 0;
 
   ~Amr2Gpu() {
+    if (st) cudaStreamSynchronize(st);
+    for (auto& G : lgraph) G.reset();
+    if (d_sub) cudaFree(d_sub);
+    if (h_sub) cudaFreeHost(h_sub);
+    if (h_cfl) cudaFreeHost(h_cfl);
     for (int l = 0; l < 12; ++l) free_plan(l);
     newfill.d_rects.free(); newfill.d_ops.free(); newfill.d_chunks.free(); newfill.d_bcs.free();
     pool.destroy(); regs.destroy();
@@ -576,6 +581,7 @@ class Amr2Gpu {
   // bound.f90:51-158 for every patch of the level: compiled per patch on the host
   // threads, then joined in level order.
   void compile_bound(int lev) {
+    ++plan_gen[lev];
     HPROF("compile_bound");
     FillProg& P = plan[lev].bound;
     P.clear();
@@ -651,6 +657,7 @@ class Amr2Gpu {
 
   // saveqc.f:13-109 for the kids at level lev+1
   void compile_saveqc(int lev) {
+    ++plan_gen[lev];
     HPROF("compile_saveqc");
     FillProg& P = plan[lev].saveqc;
     P.clear();
@@ -722,7 +729,7 @@ class Amr2Gpu {
     P.d_bcs.upload(bcs, st, stg);
   }
 
-  void run_prog(FillProg& P, const SrcMode& modes) {
+  void run_prog(FillProg& P, const SrcMode& modes, const SrcMode* modes_dev = nullptr) {
     if (P.zero_scratch && P.scratch_len > 0 && P.nstages > 0)
       AMR_CUDA(cudaMemsetAsync(reinterpret_cast<char*>(pool.d) + elem() * P.scratch_off, 0, elem() * P.scratch_len, st));
     for (int s = 0; s < P.nstages; ++s) {
@@ -730,6 +737,7 @@ class Amr2Gpu {
         FillArgs a{};
         a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.rects = P.d_rects.d; a.ops = P.d_ops.d;
         a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
+        a.modes_dev = modes_dev;
         a.lc = lc; a.xlower = xlower; a.ylower = ylower;
         launch_fill(a, st, f32);
         ++nkernels;
@@ -747,6 +755,7 @@ class Amr2Gpu {
 
   // ================================================================ step work, registers, update plans
   void compile_step(int lev) {
+    ++plan_gen[lev];
     HPROF("compile_step");
     LevelPlan& L = plan[lev];
     L.work.clear(); L.fsv.clear(); L.fad.clear(); L.patch_work_lo.clear(); L.patch_work_hi.clear(); L.qad.clear();
@@ -805,6 +814,7 @@ class Amr2Gpu {
 
   // update.f:16-189 + upbnd.f:18-127 for coarse level lev
   void compile_update(int lev) {
+    ++plan_gen[lev];
     HPROF("compile_update");
     LevelPlan& L = plan[lev];
     L.upc.clear(); L.upt.clear(); L.avg.clear();
@@ -998,29 +1008,110 @@ class Amr2Gpu {
     return M;
   }
 
-  void bound_level(int lev, double t) {
+  SrcMode bound_modes(int lev, double t) {
     SrcMode M = modes_for(lev, t);
     for (int l = 1; l <= lev; ++l)
       if (M.mode[l] < 0 && !lgrids[l].empty() && l != lev + 100) {
         // a level whose time cannot serve this fill; only an error if the program reads it
         M.mode[l] = 0;
       }
-    run_prog(plan[lev].bound, M);
+    return M;
   }
+  void bound_level(int lev, double t) { run_prog(plan[lev].bound, bound_modes(lev, t)); }
 
-  // ================================================================ level substep (advanc.f:10-142)
-  double advanc(int lev) {
-    HPROF("advanc");
+  // ---- scalars of a level substep that change from substep to substep; a captured graph
+  // reads them from device memory, refreshed by one copy before each replay
+  struct Substep2 { SrcMode modes; double dt; };
+  Substep2* d_sub = nullptr;  // [12] on the device
+  Substep2* h_sub = nullptr;  // [12] pinned
+  unsigned long long* h_cfl = nullptr;  // pinned: the CFL read-back of a substep
+  // a level's substep as two CUDA graphs around the gauge sampling: pre (ghost fill,
+  // saveqc, qad) and post (CFL reset, step, store swap, CFL read-back). Valid while the
+  // level's plans and the buffers they point into stay the same.
+  struct LevelGraph {
+    cudaGraphExec_t pre = nullptr, post = nullptr;
+    long long gen = -1;
+    int batched = -1;
+    const void* ptrs[4] = {};
+    long long kpre = 0, kpost = 0;
+    void reset() {
+      if (pre) cudaGraphExecDestroy(pre);
+      if (post) cudaGraphExecDestroy(post);
+      pre = post = nullptr; gen = -1;
+    }
+  };
+  LevelGraph lgraph[12];
+  bool use_graphs = false;
+  long long plan_gen[12] = {0};
+  long long graph_captures = 0, graph_replays = 0;
+
+  // the launches before the gauge sampling (ds: read dt and the fill modes from there)
+  void launch_pre(int lev, double t, double dt, const Substep2* ds) {
     LevelPlan& L = plan[lev];
-    const double t = node[lgrids[lev][0]].time;
-    const double dt = possk[lev];
-    bound_level(lev, t);
+    run_prog(L.bound, bound_modes(lev, t), ds ? &ds->modes : nullptr);
     if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
     if (lev > 1 && !L.qad.empty()) {
-      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st, f32);
+      launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st, f32,
+                  ds ? &ds->dt : nullptr);
       ++nkernels;
     }
-    // gauges (gauges_module.f90:313-452): sampled before the step on the finest covering grid
+  }
+  // the patch step (plain = one launch per patch, batched = one launch per level), the
+  // store swap and the CFL read-back; timed: bracket the step with ev_a / ev_b
+  void launch_post(int lev, double dt, const Substep2* ds, bool timed) {
+    LevelPlan& L = plan[lev];
+    AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
+    if (timed) AMR_CUDA(cudaEventRecord(ev_a, st));
+    StepArgs a{};
+    a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.fsv = L.d_fsv.d; a.fad = L.d_fad.d;
+    a.dt = dt; a.dt_dev = ds ? &ds->dt : nullptr; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
+    if (batched) {
+      a.work = L.d_work.d; a.nwork = (int)L.work.size(); a.queue = nullptr;
+      launch_step2(prob.solver, a, (int)L.work.size(), st, f32);
+      ++nkernels;
+    } else {
+      for (size_t k = 0; k < L.plist.size(); ++k) {
+        a.work = L.d_work.d + L.patch_work_lo[k];
+        a.nwork = L.patch_work_hi[k] - L.patch_work_lo[k];
+        a.queue = nullptr;
+        launch_step2(prob.solver, a, a.nwork, st, f32);
+        ++nkernels;
+      }
+    }
+    if (timed) AMR_CUDA(cudaEventRecord(ev_b, st));
+    launch_flip(d_patches.d, L.d_plist.d, (int)L.plist.size(), st);
+    ++nkernels;
+    AMR_CUDA(cudaMemcpyAsync(h_cfl, d_cfl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  }
+  // captures the level's two graphs if the current ones do not fit the plans and buffers
+  void ensure_graphs(int lev) {
+    LevelGraph& G = lgraph[lev];
+    const void* ptrs[4] = {pool.d, regs.d, d_patches.d, d_cfl};
+    bool ok = G.pre && G.gen == plan_gen[lev] && G.batched == (int)batched;
+    for (int k = 0; k < 4 && ok; ++k) ok = G.ptrs[k] == ptrs[k];
+    if (ok) return;
+    HPROF("graph_capture");
+    G.reset();
+    const Substep2* ds = d_sub + lev;
+    const double t = node[lgrids[lev][0]].time, dt = possk[lev];
+    for (int part = 0; part < 2; ++part) {
+      cudaGraph_t g = nullptr;
+      const long long k0 = nkernels;
+      AMR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      if (part == 0) launch_pre(lev, t, dt, ds);
+      else launch_post(lev, dt, ds, false);
+      AMR_CUDA(cudaStreamEndCapture(st, &g));
+      AMR_CUDA(cudaGraphInstantiate(part == 0 ? &G.pre : &G.post, g, 0));
+      AMR_CUDA(cudaGraphDestroy(g));
+      (part == 0 ? G.kpre : G.kpost) = nkernels - k0;
+      nkernels = k0;
+    }
+    G.gen = plan_gen[lev]; G.batched = (int)batched;
+    for (int k = 0; k < 4; ++k) G.ptrs[k] = ptrs[k];
+    ++graph_captures;
+  }
+  // gauges (gauges_module.f90:313-452): sampled before the step on the finest covering grid
+  void sample_gauges(int lev) {
     if (record_gauges && !p.gauges.empty()) {
       std::vector<GaugeJob> jobs;
       const double hx = hxposs[lev], hy = hyposs[lev];
@@ -1053,34 +1144,37 @@ class Amr2Gpu {
         dj.free();
       }
     }
-    // the patch step: plain = one launch per patch, batched = one launch per level
-    AMR_CUDA(cudaMemsetAsync(d_cfl, 0, sizeof(unsigned long long), st));
-    if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
-    StepArgs a{};
-    a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.fsv = L.d_fsv.d; a.fad = L.d_fad.d;
-    a.dt = dt; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
-    if (batched) {
-      a.work = L.d_work.d; a.nwork = (int)L.work.size(); a.queue = nullptr;
-      launch_step2(prob.solver, a, (int)L.work.size(), st, f32);
-      ++nkernels;
+  }
+
+  // ================================================================ level substep (advanc.f:10-142)
+  // launched directly, or replayed from captured graphs
+  double advanc(int lev) {
+    HPROF("advanc");
+    LevelPlan& L = plan[lev];
+    const double t = node[lgrids[lev][0]].time;
+    const double dt = possk[lev];
+    if (use_graphs) {
+      ensure_graphs(lev);
+      Substep2& h = h_sub[lev];
+      h.modes = bound_modes(lev, t); h.dt = dt;
+      AMR_CUDA(cudaMemcpyAsync(d_sub + lev, &h, sizeof(Substep2), cudaMemcpyHostToDevice, st));
+      AMR_CUDA(cudaGraphLaunch(lgraph[lev].pre, st));
+      sample_gauges(lev);
+      if (profile) AMR_CUDA(cudaEventRecord(ev_a, st));
+      AMR_CUDA(cudaGraphLaunch(lgraph[lev].post, st));
+      if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
+      nkernels += lgraph[lev].kpre + lgraph[lev].kpost;
+      graph_replays += 2;
     } else {
-      for (size_t k = 0; k < L.plist.size(); ++k) {
-        a.work = L.d_work.d + L.patch_work_lo[k];
-        a.nwork = L.patch_work_hi[k] - L.patch_work_lo[k];
-        a.queue = nullptr;
-        launch_step2(prob.solver, a, a.nwork, st, f32);
-        ++nkernels;
-      }
+      launch_pre(lev, t, dt, nullptr);
+      sample_gauges(lev);
+      launch_post(lev, dt, nullptr, profile);
     }
-    if (profile) AMR_CUDA(cudaEventRecord(ev_b, st));
-    launch_flip(d_patches.d, L.d_plist.d, (int)L.plist.size(), st);
-    ++nkernels;
-    unsigned long long cbits = 0;
-    AMR_CUDA(cudaMemcpyAsync(&cbits, d_cfl, sizeof(cbits), cudaMemcpyDeviceToHost, st));
     {
       HPROF("advanc_sync");
       sync_stream();
     }
+    const unsigned long long cbits = *h_cfl;
     double cmax;
     std::memcpy(&cmax, &cbits, sizeof(double));
     if (profile) {
@@ -1098,6 +1192,7 @@ class Amr2Gpu {
     cfl_level = cmax;
     cflmax_run = std::max(cflmax_run, cmax);
     ++nsteps_launched;
+    (void)L;
     return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
   }
 
@@ -1724,7 +1819,10 @@ class Amr2Gpu {
     pool.init(est);
     regs.init(1 << 20);
     AMR_CUDA(cudaMalloc(&d_cfl, sizeof(unsigned long long)));
+    AMR_CUDA(cudaMallocHost((void**)&h_cfl, sizeof(unsigned long long)));
     AMR_CUDA(cudaMalloc(&d_mass, sizeof(double)));
+    AMR_CUDA(cudaMalloc(&d_sub, sizeof(Substep2) * 12));
+    AMR_CUDA(cudaMallocHost((void**)&h_sub, sizeof(Substep2) * 12));
     node.assign(10001, HPatch());
     for (int k = 1; k <= 10000; ++k) node[k].nextfree = k + 1;
     node[10000].nextfree = 0;
@@ -2204,7 +2302,8 @@ class Solver2 : public AmrSolver {
   void set_batched(bool on) override { g.batched = on; }
   void set_profile(bool on) override { g.profile = on; }
   void set_graphs(bool on) override {
-    if (on) throw std::runtime_error("amrgpu_set_graphs: CUDA-graph replay is built for the 3D path");
+    g.use_graphs = on;
+    if (!on) for (auto& G : g.lgraph) G.reset();
   }
   void set_schedule(int s) override {
     if (s != 0) throw std::runtime_error("amrgpu_set_schedule: sweep schedules are built for the 3D path");
@@ -2239,7 +2338,7 @@ class Solver2 : public AmrSolver {
     return {g.time, g.rvol, (double)g.ncycle, (double)g.lfine, g.t_step, g.t_regrid, g.tmass0,
             g.cflmax_run, (double)g.nkernels, (double)g.pool.peak * 8.0, (double)g.nsteps_launched,
             g.step_kernel_ms, g.step_kernel_cells, g.last_run_ms, g.run_cells, g.finished() ? 1.0 : 0.0, g.h2d_bytes,
-            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0, 0.0, 0.0, 0.0, 0.0};
+            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0, (double)g.graph_captures, (double)g.graph_replays, 0.0, 0.0};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;

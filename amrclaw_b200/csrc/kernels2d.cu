@@ -222,7 +222,8 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
   R* red = X + L::NX;
   __shared__ int s_item;
   const int tid = threadIdx.x;
-  const R dtdx = (R)(a.dt / a.dx), dtdy = (R)(a.dt / a.dy);
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+  const R dtdx = (R)(dt / a.dx), dtdy = (R)(dt / a.dy);
   R cfl = R(0);
   int iter = 0;
   while (true) {
@@ -299,10 +300,10 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
       const int ca = e.ic - i0, rb = e.jc - j0;
       // register values stay FP64 in both forms
       double v = 0.0;
-      if (e.side == 1) v = -(double)FP[(m * T + rb) * (T + 1) + ca] * a.dt * a.dy;
-      else if (e.side == 2) v = -(double)GM[(m * (T + 1) + rb + 1) * T + ca] * a.dt * a.dx;
-      else if (e.side == 3) v = -(double)FM[(m * T + rb) * (T + 1) + ca + 1] * a.dt * a.dy;
-      else v = -(double)GP[(m * (T + 1) + rb) * T + ca] * a.dt * a.dx;
+      if (e.side == 1) v = -(double)FP[(m * T + rb) * (T + 1) + ca] * dt * a.dy;
+      else if (e.side == 2) v = -(double)GM[(m * (T + 1) + rb + 1) * T + ca] * dt * a.dx;
+      else if (e.side == 3) v = -(double)FM[(m * T + rb) * (T + 1) + ca + 1] * dt * a.dy;
+      else v = -(double)GP[(m * (T + 1) + rb) * T + ca] * dt * a.dx;
       a.regs[e.dst + m] = v;
     }
     // fluxad epilogue: fine boundary fluxes accumulated into this patch's registers
@@ -314,10 +315,10 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
       double s = *svd;
       for (int l = 0; l < r; ++l) {
         const int f = e.f0 + l;
-        if (e.side == 1) s = s + (double)FM[(m * T + (f - j0)) * (T + 1) + 0] * a.dt * a.dy;
-        else if (e.side == 2) s = s + (double)GP[(m * (T + 1) + th) * T + (f - i0)] * a.dt * a.dx;
-        else if (e.side == 3) s = s + (double)FP[(m * T + (f - j0)) * (T + 1) + tw] * a.dt * a.dy;
-        else s = s + (double)GM[(m * (T + 1) + 0) * T + (f - i0)] * a.dt * a.dx;
+        if (e.side == 1) s = s + (double)FM[(m * T + (f - j0)) * (T + 1) + 0] * dt * a.dy;
+        else if (e.side == 2) s = s + (double)GP[(m * (T + 1) + th) * T + (f - i0)] * dt * a.dx;
+        else if (e.side == 3) s = s + (double)FP[(m * T + (f - j0)) * (T + 1) + tw] * dt * a.dy;
+        else s = s + (double)GM[(m * (T + 1) + 0) * T + (f - i0)] * dt * a.dx;
       }
       *svd = s;
     }
@@ -422,7 +423,10 @@ __global__ void fill_kernel(FillArgs a) {
     const long long sp = (long long)S.mitot * S.mjtot;
     const long long sk = (long long)(o.sj0 + jb) * S.mitot + (o.si0 + ia);
     int mode = 0; double ai = 1.0, ac = 0.0;
-    if (o.level >= 0) { mode = a.modes.mode[o.level]; ai = a.modes.alphai[o.level]; ac = a.modes.alphac[o.level]; }
+    if (o.level >= 0) {
+      const SrcMode& M = a.modes_dev ? *a.modes_dev : a.modes;
+      mode = M.mode[o.level]; ai = M.alphai[o.level]; ac = M.alphac[o.level];
+    }
     const T* qn = pool + S.q[S.cur];
     const T* qo = pool + S.q[1 - S.cur];
     for (int m = 0; m < nvar; ++m) {
@@ -573,10 +577,11 @@ void launch_bc(const BcArgs& a, int phase, cudaStream_t s, bool f32) {
 // ======================================================================= qad
 template <class S, class T>
 __global__ void qad2_kernel(T* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
-                            ProbDev prob, LevelConst lc, double delt) {
+                            ProbDev prob, LevelConst lc, double delt, const double* dt_dev) {
   constexpr int ME = S::MEQN, MW = S::MWAVES;
   const int jb = blockIdx.x;
   if (jb >= njobs) return;
+  if (dt_dev) delt = *dt_dev;
   const QadJob J = jobs[jb];
   const PatchDev P = patches[J.patch];
   const int lev = P.level;
@@ -623,20 +628,20 @@ __global__ void qad2_kernel(T* pool, double* regs, const PatchDev* patches, cons
 
 template <class T>
 static void launch_qad2_t(int solver, T* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
-                          const ProbDev& prob, LevelConst lc, double delt, cudaStream_t s) {
+                          const ProbDev& prob, LevelConst lc, double delt, cudaStream_t s, const double* dt_dev) {
   switch (solver) {
-    case SOLVER_ADVECTION: qad2_kernel<Advection2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
-    case SOLVER_ACOUSTICS: qad2_kernel<Acoustics2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
-    case SOLVER_EULER: qad2_kernel<Euler2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt); break;
+    case SOLVER_ADVECTION: qad2_kernel<Advection2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt, dt_dev); break;
+    case SOLVER_ACOUSTICS: qad2_kernel<Acoustics2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt, dt_dev); break;
+    case SOLVER_EULER: qad2_kernel<Euler2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt, dt_dev); break;
   }
 }
 
 void launch_qad2(int solver, void* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
-                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s, bool f32) {
+                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s, bool f32, const double* dt_dev) {
   if (njobs <= 0) return;
   (void)nvar;
-  if (f32) launch_qad2_t(solver, static_cast<float*>(pool), regs, patches, jobs, njobs, prob, lc, delt, s);
-  else launch_qad2_t(solver, static_cast<double*>(pool), regs, patches, jobs, njobs, prob, lc, delt, s);
+  if (f32) launch_qad2_t(solver, static_cast<float*>(pool), regs, patches, jobs, njobs, prob, lc, delt, s, dt_dev);
+  else launch_qad2_t(solver, static_cast<double*>(pool), regs, patches, jobs, njobs, prob, lc, delt, s, dt_dev);
   AMR_CUDA(cudaGetLastError());
 }
 

@@ -52,6 +52,7 @@ struct StepArgs {
   const FsvEntry* fsv;
   const FadEntry* fad;
   double dt, dx, dy;
+  const double* dt_dev;  // if set, the time step is read here (a captured graph replays the launch)
   unsigned long long* cflmax;  // max Courant number of the level (bit pattern of a non-negative double)
   StepParams sp;
 };
@@ -96,6 +97,7 @@ struct FillArgs {
   int nchunks;
   int nvar;
   SrcMode modes;
+  const SrcMode* modes_dev;  // if set, the time-interpolation modes are read here (captured graphs)
   LevelConst lc;
   double xlower, ylower;
 };
@@ -124,8 +126,10 @@ struct GaugeJob { int patch; int ii, jj; int slot; double xoff, yoff; };
 void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s, bool f32);
 void launch_fill(const FillArgs& a, cudaStream_t s, bool f32);
 void launch_bc(const BcArgs& a, int phase, cudaStream_t s, bool f32);
+// dt_dev: if set, delt is read there (captured graphs)
 void launch_qad2(int solver, void* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
-                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s, bool f32);
+                 const ProbDev& prob, int nvar, LevelConst lc, double delt, cudaStream_t s, bool f32,
+                 const double* dt_dev = nullptr);
 void launch_upbnd(void* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
                   const UpbndTerm* terms, double area, int nvar, cudaStream_t s, bool f32);
 void launch_average(void* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,

@@ -395,11 +395,12 @@ def main():
 
         plain_value, plain_ms, plain_inf = leg(False, False)
         graph_legs = {}
+        for name, b in (("plain_graphs", False), ("batched_graphs", True)):
+            v, m, inf = leg(b, True)
+            graph_legs[name] = {"value": v, "unit": "cell-updates/s", "ms_per_step": m,
+                                "advance_ms_per_step": inf["advance_ms_per_step"],
+                                "graph_captures": inf["graph_captures"], "graph_replays": inf["graph_replays"]}
         if ndim == 3:
-            for name, b in (("plain_graphs", False), ("batched_graphs", True)):
-                v, m, inf = leg(b, True)
-                graph_legs[name] = {"value": v, "unit": "cell-updates/s", "ms_per_step": m,
-                                    "graph_captures": inf["graph_captures"], "graph_replays": inf["graph_replays"]}
             # the batched path's two sweep schedules forced (the value leg autotunes per level)
             for name, sch in (("batched_per_direction", 1), ("batched_work_queue", 2)):
                 v, m, _ = leg(True, False, sch)

@@ -45,13 +45,12 @@ int amrgpu_init_precision(const char* rundir, const char* outdir, int write_outp
  * 0: one launch per patch (plain per-patch path). */
 int amrgpu_set_batched(amrgpu_ctx* ctx, int batched);
 
-/* 1: capture each level substep of the 3D path as two CUDA graphs (ghost fill, saveqc,
- * qad; then CFL reset, b4step3, the step kernels, fluxsv/fluxad, the store swap and the
- * CFL read-back) and replay them, re-capturing when a regrid changes the level's plans;
- * the per-substep scalars (dt, time-interpolation weights, the b4step3 factor) are
- * copied to the device before each replay. Results are identical to direct launches.
- * 0: launch directly (default). 2D contexts reject 1 (AMRGPU_EINVAL). No counterpart in
- * the reference. */
+/* 1: capture each level substep as two CUDA graphs (ghost fill, saveqc, qad; then CFL
+ * reset, (3D) b4step3, the step kernels, fluxsv/fluxad, the store swap and the CFL
+ * read-back) and replay them, re-capturing when a regrid changes the level's plans; the
+ * per-substep scalars (dt, time-interpolation weights, the b4step3 factor) are copied to
+ * the device before each replay. Results are identical to direct launches. 0: launch
+ * directly (default). No counterpart in the reference. */
 int amrgpu_set_graphs(amrgpu_ctx* ctx, int on);
 
 /* Writes a checkpoint of the run at the current coarse-step boundary (check.f:4-104):
@@ -125,7 +124,7 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
  * bytes of initial data copied host to device, then regrid seconds spent in:
  * device flagging, host flag processing, clustering, new-grid fill, register
  * and list set-up, device-program compilation, then the number of space dimensions,
- * the precision in bits (64 or 32), and (3D) the CUDA graphs captured and replayed and
+ * the precision in bits (64 or 32), the CUDA graphs captured and replayed, and (3D)
  * the number of levels whose autotuned sweep schedule is the work queue, and the number
  * whose is per direction. */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);

@@ -17,7 +17,7 @@ from oracle.pyoracle import Oracle2D
 pytestmark = pytest.mark.gpu
 
 
-def _both(rd, nvar, batched=True, max_cycles=0):
+def _both(rd, nvar, batched=True, max_cycles=0, graphs=False):
     from amrclaw_b200 import Solver
     with tempfile.TemporaryDirectory() as d:
         rd.write(d)
@@ -26,7 +26,7 @@ def _both(rd, nvar, batched=True, max_cycles=0):
         ref = dict(grids=o.grids(), values=o.values(), gauges=o.gauges(nvar), time=o.time(), mass=o.mass(),
                    cells=o.cell_updates())
         o.close()
-        with Solver(d, batched=batched) as s:
+        with Solver(d, batched=batched, graphs=graphs) as s:
             s.run(max_cycles)
             gpu = dict(grids=s.grids(), values=s.values(), gauges=s.gauges(nvar), info=s.info(), mass=s.mass())
     return ref, gpu
@@ -96,3 +96,30 @@ def test_split_run_equals_one_run():
                 s.run(3)
             gpu = dict(grids=s.grids(), values=s.values(), info=s.info(), mass=s.mass())
     _assert_identical(ref, gpu)
+
+
+@pytest.mark.parametrize("batched", [True, False])
+def test_cuda_graph_replay_is_identical(batched):
+    """Level substeps replayed from captured CUDA graphs (dt and the fill weights read from
+    device memory) give the oracle's results; graphs are re-captured after regrids and
+    reused in between."""
+    ref, gpu = _both(configs.acoustics_radial_regression(), 3, batched=batched, graphs=True)
+    _assert_identical(ref, gpu)
+    assert_gauges_match(gpu["gauges"], gauge_rows("acoustics_2d_radial"))
+    assert gpu["info"]["graph_captures"] > 0
+    assert gpu["info"]["graph_replays"] > 2 * gpu["info"]["graph_captures"]
+
+
+def test_cuda_graph_replay_fp32_periodic():
+    """The FP32 form and periodic boundaries under graph replay match direct launches."""
+    from amrclaw_b200 import Solver
+    rd = configs.advection_square_bench(n=32, tfinal=0.3, levels=3)
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        rd.write(d)
+        for graphs in (False, True):
+            with Solver(d, precision="fp32", graphs=graphs) as s:
+                s.run(0)
+                out.append((s.grids(), s.values()))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
