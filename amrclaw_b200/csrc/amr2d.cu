@@ -753,6 +753,36 @@ class Amr2Gpu {
     }
   }
 
+  // Two independent programs stage by stage (the bound and saveqc programs of a level:
+  // saveqc reads the level's interiors and its own scratch, bound writes the ghost cells
+  // and its own scratch): stage s of both in one fill launch, then their boundary ops,
+  // both phases, in one launch. Q may be null; P's fills read their time-interpolation
+  // modes from modes (or modes_dev), Q's from zero modes.
+  void run_prog_pair(FillProg& P, const SrcMode& modes, const SrcMode* modes_dev, FillProg* Q) {
+    for (FillProg* X : {&P, Q})
+      if (X && X->zero_scratch && X->scratch_len > 0 && X->nstages > 0)
+        AMR_CUDA(cudaMemsetAsync(reinterpret_cast<char*>(pool.d) + elem() * X->scratch_off, 0, elem() * X->scratch_len, st));
+    const int ns = std::max(P.nstages, Q ? Q->nstages : 0);
+    for (int s = 0; s < ns; ++s) {
+      FillArgs fa[2]{};
+      BcArgs ba[2]{};
+      FillProg* X2[2] = {&P, Q};
+      for (int k = 0; k < 2; ++k) {
+        FillArgs& a = fa[k];
+        BcArgs& b = ba[k];
+        a.pool = pool.d; a.regs = regs.d; a.patches = d_patches.d; a.nvar = nvar; a.lc = lc; a.xlower = xlower; a.ylower = ylower;
+        b.pool = pool.d; b.patches = d_patches.d; b.nvar = nvar;
+        FillProg* X = X2[k];
+        if (!X || s >= X->nstages) continue;
+        a.rects = X->d_rects.d; a.ops = X->d_ops.d; a.chunks = X->d_chunks.d + X->ch_lo[s]; a.nchunks = X->ch_hi[s] - X->ch_lo[s];
+        if (k == 0) { a.modes = modes; a.modes_dev = modes_dev; }
+        b.rects = X->d_rects.d; b.ops = X->d_bcs.d + X->bc_lo[s]; b.nops = X->bc_hi[s] - X->bc_lo[s];
+      }
+      if (fa[0].nchunks + fa[1].nchunks > 0) { launch_fill_pair(fa[0], fa[1], st, f32); ++nkernels; }
+      if (ba[0].nops + ba[1].nops > 0) { launch_bc_pair(ba[0], ba[1], st, f32); ++nkernels; }
+    }
+  }
+
   // ================================================================ step work, registers, update plans
   void compile_step(int lev) {
     ++plan_gen[lev];
@@ -1048,8 +1078,14 @@ class Amr2Gpu {
   // the launches before the gauge sampling (ds: read dt and the fill modes from there)
   void launch_pre(int lev, double t, double dt, const Substep2* ds) {
     LevelPlan& L = plan[lev];
-    run_prog(L.bound, bound_modes(lev, t), ds ? &ds->modes : nullptr);
-    if (lev + 1 <= p.mxnest && lstart[lev + 1] != 0) { SrcMode M{}; run_prog(L.saveqc, M); }
+    const bool kids = lev + 1 <= p.mxnest && lstart[lev + 1] != 0;
+    if (batched) {
+      // bound and saveqc of the whole level, their stages sharing launches
+      run_prog_pair(L.bound, bound_modes(lev, t), ds ? &ds->modes : nullptr, kids ? &L.saveqc : nullptr);
+    } else {
+      run_prog(L.bound, bound_modes(lev, t), ds ? &ds->modes : nullptr);
+      if (kids) { SrcMode M{}; run_prog(L.saveqc, M); }
+    }
     if (lev > 1 && !L.qad.empty()) {
       launch_qad2(prob.solver, pool.d, regs.d, d_patches.d, L.d_qad.d, (int)L.qad.size(), prob, nvar, lc, dt, st, f32,
                   ds ? &ds->dt : nullptr);
@@ -1166,8 +1202,12 @@ class Amr2Gpu {
       nkernels += lgraph[lev].kpre + lgraph[lev].kpost;
       graph_replays += 2;
     } else {
+      PhaseTimer tph(hprof);
+      tph.next("adv_pre");
       launch_pre(lev, t, dt, nullptr);
+      tph.next("adv_gauges");
       sample_gauges(lev);
+      tph.next("adv_post");
       launch_post(lev, dt, nullptr, profile);
     }
     {

@@ -388,11 +388,10 @@ __device__ __forceinline__ T* fill_dst(const FillArgs& a, const FillOp& o, int& 
   return static_cast<T*>(a.pool) + R.off;
 }
 
+// one 128-cell chunk c of a fill program (one block)
 template <class T>
-__global__ void fill_kernel(FillArgs a) {
+__device__ __forceinline__ void fill_chunk(const FillArgs& a, int c) {
   const T* pool = static_cast<const T*>(a.pool);
-  const int c = blockIdx.x;
-  if (c >= a.nchunks) return;
   const FillChunk ch = a.chunks[c];
   if ((int)threadIdx.x >= ch.count) return;
   const FillOp o = a.ops[ch.op];
@@ -503,18 +502,38 @@ __global__ void fill_kernel(FillArgs a) {
   }
 }
 
+template <class T>
+__global__ void fill_kernel(FillArgs a) {
+  const int c = blockIdx.x;
+  if (c >= a.nchunks) return;
+  fill_chunk<T>(a, c);
+}
+// the chunks of two independent programs in one launch: a's, then b's
+template <class T>
+__global__ void fill_pair_kernel(FillArgs a, FillArgs b) {
+  const int c = blockIdx.x;
+  if (c < a.nchunks) fill_chunk<T>(a, c);
+  else if (c - a.nchunks < b.nchunks) fill_chunk<T>(b, c - a.nchunks);
+}
+
 void launch_fill(const FillArgs& a, cudaStream_t s, bool f32) {
   if (a.nchunks <= 0) return;
   if (f32) fill_kernel<float><<<a.nchunks, 128, 0, s>>>(a);
   else fill_kernel<double><<<a.nchunks, 128, 0, s>>>(a);
   AMR_CUDA(cudaGetLastError());
 }
+void launch_fill_pair(const FillArgs& a, const FillArgs& b, cudaStream_t s, bool f32) {
+  const long long n = (long long)a.nchunks + b.nchunks;
+  if (n <= 0) return;
+  if (n >= (1LL << 31)) throw std::runtime_error("fill program too large for one launch");
+  if (f32) fill_pair_kernel<float><<<(unsigned)n, 128, 0, s>>>(a, b);
+  else fill_pair_kernel<double><<<(unsigned)n, 128, 0, s>>>(a, b);
+  AMR_CUDA(cudaGetLastError());
+}
 
 // phase 0: x-sides over all rows; phase 1: y-sides over all columns (after phase 0)
 template <class T>
-__global__ void bc_kernel(BcArgs a, int phase) {
-  const int op = blockIdx.y;
-  if (op >= a.nops) return;
+__device__ __forceinline__ void bc_op(const BcArgs& a, int op, int phase) {
   const BcOp o = a.ops[op];
   T* v; int nrow = o.nrow, ncol = o.ncol;
   if (o.dst_patch >= 0) { const PatchDev& P = a.patches[o.dst_patch]; v = static_cast<T*>(a.pool) + P.q[P.cur]; }
@@ -561,6 +580,40 @@ __global__ void bc_kernel(BcArgs a, int phase) {
   }
 }
 
+template <class T>
+__global__ void bc_kernel(BcArgs a, int phase) {
+  const int op = blockIdx.y;
+  if (op >= a.nops) return;
+  bc_op<T>(a, op, phase);
+}
+// the ops of two independent programs, one block per op doing phase 0 then phase 1 (the
+// y-sides read the corners the x-sides wrote; each op has its own destination array)
+template <class T>
+__global__ void bc_pair_kernel(BcArgs a, BcArgs b) {
+  const int op = blockIdx.y;
+  const bool first = op < a.nops;
+  const BcArgs& A = first ? a : b;
+  const int o = first ? op : op - a.nops;
+  if (o >= A.nops) return;
+  bc_op<T>(A, o, 0);
+  __syncthreads();
+  bc_op<T>(A, o, 1);
+}
+void launch_bc_pair(const BcArgs& a, const BcArgs& b, cudaStream_t s, bool f32) {
+  const int n = a.nops + b.nops;
+  if (n <= 0) return;
+  if (n > 65535) {  // more ops than one grid column: one program at a time, both phases
+    for (const BcArgs* x : {&a, &b}) {
+      if (x->nops <= 0) continue;
+      launch_bc(*x, 0, s, f32);
+      launch_bc(*x, 1, s, f32);
+    }
+    return;
+  }
+  if (f32) bc_pair_kernel<float><<<dim3(1, n), 128, 0, s>>>(a, b);
+  else bc_pair_kernel<double><<<dim3(1, n), 128, 0, s>>>(a, b);
+  AMR_CUDA(cudaGetLastError());
+}
 void launch_bc(const BcArgs& a, int phase, cudaStream_t s, bool f32) {
   if (a.nops <= 0) return;
   for (int base = 0; base < a.nops; base += 65535) {

@@ -125,6 +125,10 @@ struct GaugeJob { int patch; int ii, jj; int slot; double xoff, yoff; };
 // time interpolation weights, averages and totals in FP64.
 void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s, bool f32);
 void launch_fill(const FillArgs& a, cudaStream_t s, bool f32);
+// one launch over the chunks of two independent programs (b may have no chunks)
+void launch_fill_pair(const FillArgs& a, const FillArgs& b, cudaStream_t s, bool f32);
+// both boundary phases of the ops of two independent programs in one launch
+void launch_bc_pair(const BcArgs& a, const BcArgs& b, cudaStream_t s, bool f32);
 void launch_bc(const BcArgs& a, int phase, cudaStream_t s, bool f32);
 // dt_dev: if set, delt is read there (captured graphs)
 void launch_qad2(int solver, void* pool, double* regs, const PatchDev* patches, const QadJob* jobs, int njobs,
