@@ -1049,6 +1049,7 @@ class Amr3Gpu : public AmrSolver {
 
   // prepf.f:4-41
   void prepf(int lev) {
+    HPROF("prepf3");
     std::vector<std::pair<long long, long long>> zr;
     for (int k = lstart[lev]; k != 0; k = node[k].levelptr) {
       HPatch3& g = node[k];
@@ -1107,6 +1108,7 @@ class Amr3Gpu : public AmrSolver {
   }
   // prepc.f:4-138
   void prepc(int lev) {
+    HPROF("prepc3");
     int maxsp = 0;
     for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) {
       const HPatch3& f = node[k];
@@ -1137,8 +1139,9 @@ class Amr3Gpu : public AmrSolver {
     });
   }
 
-  // A regrid marks the plans of the levels it changed and compiles them all (ensure_all);
-  // every consumer also ensures its own plan, so a plan is never used stale.
+  // A regrid marks the plans of the levels it changed; every consumer ensures its own plan
+  // before use, so a plan is never used stale. The marked plans are compiled while the GPU
+  // runs the level substeps that follow (compile_while_busy), the rest on first use.
   enum { NEED_BOUND = 1, NEED_SAVEQC = 2, NEED_STEP = 4, NEED_UPDATE = 8 };
   int dirty[12] = {0};
   void compile_all(int lbase = 0) {
@@ -1152,7 +1155,6 @@ class Amr3Gpu : public AmrSolver {
       if (lev > lbase) dirty[lev] |= NEED_BOUND;
       if (lev >= lbase) dirty[lev] |= NEED_SAVEQC | NEED_STEP | NEED_UPDATE;
     }
-    ensure_all();
   }
   void ensure(int lev, int what) {
     if (lev < 1 || lev > p.mxnest) return;
@@ -1165,7 +1167,38 @@ class Amr3Gpu : public AmrSolver {
     if (todo & NEED_STEP) compile_step(lev);
     if (todo & NEED_UPDATE) compile_update(lev);
   }
-  void ensure_all() { for (int lev = 1; lev <= p.mxnest; ++lev) ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP | NEED_UPDATE); }
+  // While the substep of level lev runs on the GPU the host compiles marked plans, in the
+  // order the next consumers want them: the finer levels' substeps, then the updates from
+  // the finest down, then the rest. It stops once the stream has drained (what is left is
+  // compiled on first use). No plan compiled here is one the substep in flight reads: that
+  // substep's own plans were ensured before its launch, and compiling a plan touches only
+  // that plan's buffers and scratch (uploads and stream-ordered reallocations queue behind
+  // the substep; a pool growth waits for the device first).
+  void compile_while_busy(int lev) {
+    auto busy = [&]() {
+      const cudaError_t e = cudaStreamQuery(st);
+      if (e == cudaErrorNotReady) return true;
+      AMR_CUDA(e);
+      return false;
+    };
+    for (int l = lev + 1; l <= lfine; ++l)
+      for (int what : {NEED_BOUND, NEED_SAVEQC, NEED_STEP}) {
+        if (!(dirty[l] & what)) continue;
+        if (!busy()) return;
+        ensure(l, what);
+      }
+    for (int l = lfine; l >= 1; --l)
+      if (dirty[l] & NEED_UPDATE) {
+        if (!busy()) return;
+        ensure(l, NEED_UPDATE);
+      }
+    for (int l = 1; l <= lfine; ++l)
+      for (int what : {NEED_BOUND, NEED_SAVEQC, NEED_STEP}) {
+        if (!(dirty[l] & what)) continue;
+        if (!busy()) return;
+        ensure(l, what);
+      }
+  }
 
 
   // ================================================================ level substep
@@ -1410,6 +1443,8 @@ class Amr3Gpu : public AmrSolver {
       launch_post(lev, t, dt, nullptr, profile);
     }
     for (int m : lgrids[lev]) { node[m].cur ^= 1; h_patches[m].cur = node[m].cur; }
+    tph.next("adv_compile");
+    compile_while_busy(lev);
     tph.next("adv_sync");
     sync_stream();
     const unsigned long long cbits = *h_cfl;
@@ -2268,6 +2303,7 @@ class Amr3Gpu : public AmrSolver {
   }
   void output(double t) {
     for (int lev = 1; lev <= lfine; ++lev) {
+      ensure(lev, NEED_STEP);
       launch_zero_tiny3(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
       ++nkernels;
     }

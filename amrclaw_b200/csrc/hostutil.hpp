@@ -24,6 +24,9 @@ inline double g_dbuf_realloc_s = 0;
 // and host seconds in the copy into the ring
 inline double g_stage_bytes = 0, g_stage_copy_s = 0;
 inline long long g_stage_wraps = 0;
+// pool (Arena) growths: count, host seconds and bytes added
+inline long long g_arena_grows = 0;
+inline double g_arena_grow_s = 0, g_arena_grow_bytes = 0;
 
 // Stream-ordered reallocation. While a context works on the calling thread its stream is
 // set here, and device buffers that grow are freed and allocated in that stream's order
@@ -54,6 +57,7 @@ struct HostProf {
     for (auto& kv : acc) std::fprintf(stderr, "PROF %-22s %9.4f s %8lld calls\n", kv.first.c_str(), kv.second.first, kv.second.second);
     std::fprintf(stderr, "PROF %-22s %9.4f s %8lld calls\n", "dbuf_realloc", g_dbuf_realloc_s, g_dbuf_reallocs);
     std::fprintf(stderr, "PROF %-22s %9.4f s %8lld wraps %.1f MB\n", "staging_copy", g_stage_copy_s, g_stage_wraps, g_stage_bytes / 1e6);
+    std::fprintf(stderr, "PROF %-22s %9.4f s %8lld grows %.1f MB\n", "arena_grow", g_arena_grow_s, g_arena_grows, g_arena_grow_bytes / 1e6);
   }
 };
 struct ScopedTimer {
@@ -103,6 +107,7 @@ struct Arena {
   void add_free(long long off, long long n) { fr[off] = n; bysz.emplace(n, off); }
   void del_free(std::map<long long, long long>::iterator it) { bysz.erase({it->second, it->first}); fr.erase(it); }
   void grow(long long need) {
+    const auto t0 = std::chrono::steady_clock::now();
     // kernels on any stream may still use the pool: let them finish before it moves
     AMR_CUDA(cudaDeviceSynchronize());
     long long ncap = std::max(cap * 2, cap + rnd(need) + (1 << 20));
@@ -112,7 +117,10 @@ struct Arena {
     AMR_CUDA(cudaFree(d));
     d = nd;
     release_raw(cap, ncap - cap);
+    g_arena_grow_bytes += (double)sizeof(double) * (ncap - cap);
     cap = ncap;
+    ++g_arena_grows;
+    g_arena_grow_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
   void release_raw(long long off, long long n) {
     auto nx = fr.lower_bound(off);
