@@ -1002,21 +1002,69 @@ class Amr2Gpu {
   }
 
   // Programs of levels finer than lbase change with a regrid of lbase+1..; the
-  // saveqc, step and update plans of lbase itself change with its kids.
+  // saveqc, step and update plans of lbase itself change with its kids. A regrid marks
+  // them; every consumer ensures its own plan before use, so a plan is never used stale.
+  // The marked plans are compiled while the GPU runs the level substeps that follow
+  // (compile_while_busy), the rest on first use. Compiling reads only the hierarchy
+  // (rectangles, lists, register offsets), which changes only in a regrid.
+  enum { NEED_BOUND = 1, NEED_SAVEQC = 2, NEED_STEP = 4, NEED_UPDATE = 8 };
+  int dirty[12] = {0};
   void compile_all(int lbase = 0) {
     sync_descriptors();
     for (int lev = 1; lev <= p.mxnest; ++lev) {
       if (lev > lfine) {
         plan[lev].work.clear(); plan[lev].plist.clear();
+        dirty[lev] = 0;
         continue;
       }
-      if (lev > lbase) compile_bound(lev);
-      if (lev >= lbase) {
-        compile_saveqc(lev);
-        compile_step(lev);
-        compile_update(lev);
-      }
+      if (lev > lbase) dirty[lev] |= NEED_BOUND;
+      if (lev >= lbase) dirty[lev] |= NEED_SAVEQC | NEED_STEP | NEED_UPDATE;
     }
+  }
+  void ensure(int lev, int what) {
+    if (lev < 1 || lev > p.mxnest) return;
+    const int todo = dirty[lev] & what;
+    if (!todo) return;
+    dirty[lev] &= ~todo;
+    if (todo & NEED_BOUND) compile_bound(lev);
+    if (todo & NEED_SAVEQC) compile_saveqc(lev);
+    if (todo & NEED_STEP) compile_step(lev);
+    if (todo & NEED_UPDATE) compile_update(lev);
+  }
+  // every marked plan, before control returns to a caller of the C ABI: the fixed-scratch
+  // substep (amrgpu_level_advance_noalloc) then finds its level compiled and allocates nothing
+  void ensure_all() { for (int lev = 1; lev <= p.mxnest; ++lev) ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP | NEED_UPDATE); }
+  // While the substep of level lev runs on the GPU the host compiles marked plans, in the
+  // order the next consumers want them: the finer levels' substeps, then the updates from
+  // the finest down, then the rest. It stops once the stream has drained. No plan compiled
+  // here is one the substep in flight reads: that substep's own plans were ensured before
+  // its launch, and compiling a plan touches only that plan's buffers and scratch (uploads
+  // and stream-ordered reallocations queue behind the substep; a pool growth waits for the
+  // device first).
+  void compile_while_busy(int lev) {
+    auto busy = [&]() {
+      const cudaError_t e = cudaStreamQuery(st);
+      if (e == cudaErrorNotReady) return true;
+      AMR_CUDA(e);
+      return false;
+    };
+    for (int l = lev + 1; l <= lfine; ++l)
+      for (int what : {NEED_BOUND, NEED_SAVEQC, NEED_STEP}) {
+        if (!(dirty[l] & what)) continue;
+        if (!busy()) return;
+        ensure(l, what);
+      }
+    for (int l = lfine; l >= 1; --l)
+      if (dirty[l] & NEED_UPDATE) {
+        if (!busy()) return;
+        ensure(l, NEED_UPDATE);
+      }
+    for (int l = 1; l <= lfine; ++l)
+      for (int what : {NEED_BOUND, NEED_SAVEQC, NEED_STEP}) {
+        if (!(dirty[l] & what)) continue;
+        if (!busy()) return;
+        ensure(l, what);
+      }
   }
 
   // ================================================================ time interpolation modes (intfil.f90:183-232)
@@ -1047,7 +1095,10 @@ class Amr2Gpu {
       }
     return M;
   }
-  void bound_level(int lev, double t) { run_prog(plan[lev].bound, bound_modes(lev, t)); }
+  void bound_level(int lev, double t) {
+    ensure(lev, NEED_BOUND);
+    run_prog(plan[lev].bound, bound_modes(lev, t));
+  }
 
   // ---- scalars of a level substep that change from substep to substep; a captured graph
   // reads them from device memory, refreshed by one copy before each replay
@@ -1186,6 +1237,7 @@ class Amr2Gpu {
   // launched directly, or replayed from captured graphs
   double advanc(int lev) {
     HPROF("advanc");
+    ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP);
     LevelPlan& L = plan[lev];
     const double t = node[lgrids[lev][0]].time;
     const double dt = possk[lev];
@@ -1209,6 +1261,10 @@ class Amr2Gpu {
       sample_gauges(lev);
       tph.next("adv_post");
       launch_post(lev, dt, nullptr, profile);
+    }
+    {
+      HPROF("advanc_compile");
+      compile_while_busy(lev);
     }
     {
       HPROF("advanc_sync");
@@ -1262,6 +1318,7 @@ class Amr2Gpu {
     }
   }
   double advanc_fixed(int lev, const double* scratch) {
+    ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP);
     LevelPlan& L = plan[lev];
     const bool kids = lev + 1 <= p.mxnest && lstart[lev + 1] != 0;
     if (L.bound.scratch_len > NOALLOC_SCRATCH_DOUBLES || (kids && L.saveqc.scratch_len > NOALLOC_SCRATCH_DOUBLES))
@@ -1304,6 +1361,7 @@ class Amr2Gpu {
 
   void update(int lev) {
     HPROF("update");
+    ensure(lev, NEED_UPDATE);
     LevelPlan& L = plan[lev];
     const double area = hxposs[lev] * hyposs[lev];
     launch_upbnd(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, area, nvar, st, f32);
@@ -1923,6 +1981,7 @@ class Amr2Gpu {
     frame = p.output_t0 ? 0 : 1;
     tmass0 = mass();
     if (p.output_t0) output(time);
+    ensure_all();
     sync_stream();
   }
 
@@ -1960,6 +2019,7 @@ class Amr2Gpu {
   }
 
   double mass() {
+    ensure(1, NEED_STEP);
     AMR_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double), st));
     launch_mass2(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st, f32);
     double m = 0;
@@ -2098,6 +2158,7 @@ class Amr2Gpu {
     sync_descriptors();
     for (int lev = 1; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }
     compile_all();
+    ensure_all();
     record_gauges = true;
     mbestsrc.assign(p.gauges.size(), 0);
     setbestsrc();
@@ -2286,6 +2347,7 @@ static std::string fort_e(double v, int w, int d) {
 
 void Amr2Gpu::output(double t) {
   for (int lev = 1; lev <= lfine; ++lev) {
+    ensure(lev, NEED_STEP);
     launch_zero_tiny(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
     ++nkernels;
   }
@@ -2349,7 +2411,11 @@ class Solver2 : public AmrSolver {
     if (s != 0) throw std::runtime_error("amrgpu_set_schedule: sweep schedules are built for the 3D path");
   }
   void write_checkpoint(const char* path) override { g.checkpoint_file(path); }
-  void run(int max_cycles) override { g.max_cycles = max_cycles; g.tick(); }
+  void run(int max_cycles) override {
+    g.max_cycles = max_cycles;
+    g.tick();
+    g.ensure_all();
+  }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > g.lfine) throw std::runtime_error("level out of range");
     const double d = g.advanc(level);
@@ -2365,6 +2431,7 @@ class Solver2 : public AmrSolver {
     if (lbase < 1 || lbase > g.lfine || lbase >= g.p.mxnest) throw std::runtime_error("lbase out of range");
     g.regrid(lbase);
     g.setbestsrc();
+    g.ensure_all();
   }
   void valout(const char* dir) override {
     const std::string keep = g.outdir;
