@@ -134,6 +134,16 @@ class Amr2Gpu {
   int id_hwm = 1;  // 1 + largest patch id that ever held storage (descriptor table size)
   LevelPlan plan[12];
   FillProg newfill;  // gfixup/filval program of the level being regridded
+  // Richardson estimation (errest.f) of the level being flagged: the ghost fill of the
+  // big step, the virtual patches of both steps, one byte per 2x2 block
+  FillProg rich_prog;
+  DBuf<PatchDev> rich_vp;
+  DBuf<StepWork> rich_work;
+  DBuf<int> rich_rect;
+  DBuf<long long> rich_off;
+  DBuf<int8_t> rich_out;
+  DBuf<unsigned long long> rich_cfl;
+  long long rich_buf = -1, rich_len = 0;
   unsigned long long* d_cfl = nullptr;
   double* d_mass = nullptr;
   DBuf<double> d_gauge_out;
@@ -184,6 +194,8 @@ class Amr2Gpu {
     if (h_cfl) cudaFreeHost(h_cfl);
     for (int l = 0; l < 12; ++l) free_plan(l);
     newfill.d_rects.free(); newfill.d_ops.free(); newfill.d_chunks.free(); newfill.d_bcs.free();
+    rich_prog.d_rects.free(); rich_prog.d_ops.free(); rich_prog.d_chunks.free(); rich_prog.d_bcs.free();
+    rich_vp.free(); rich_work.free(); rich_rect.free(); rich_off.free(); rich_out.free(); rich_cfl.free();
     pool.destroy(); regs.destroy();
     if (st) cudaStreamSynchronize(st);
     stg.destroy();
@@ -595,30 +607,48 @@ class Amr2Gpu {
   }
   void compile_bound_patch(FillProg& P, int lev, int m) {
     P.scratch_len = 0;
-    {
-      const HPatch& g = node[m];
-      const double hx = hxposs[lev], hy = hyposs[lev];
-      Tgt T{m, -1, mitot(m), mjtot(m)};
-      const int mi = T.ni, mj = T.nj;
-      int s = 0;
-      double xl = g.xlo - ng * hx, xr, yb;
-      if (xl < xlower && xperdom) s = std::max(s, c_prefil(P, lev, T, g.ilo - ng, g.ilo - 1, g.jlo, g.jhi, g.ilo - ng, g.jlo - ng));
-      else s = std::max(s, c_filrecur(P, lev, T, 1, ng + 1, g.ilo - ng, g.ilo - 1, g.jlo, g.jhi, false, m));
-      xr = g.xhi + ng * hx;
-      if (xr > xupper && xperdom) s = std::max(s, c_prefil(P, lev, T, g.ihi + 1, g.ihi + ng, g.jlo, g.jhi, g.ilo - ng, g.jlo - ng));
-      else s = std::max(s, c_filrecur(P, lev, T, mi - ng + 1, ng + 1, g.ihi + 1, g.ihi + ng, g.jlo, g.jhi, false, m));
-      xl = g.xlo - ng * hx; xr = g.xhi + ng * hx; yb = g.ylo - ng * hy;
-      if ((yb < ylower && yperdom) || ((xl < xlower || xr > xupper) && xperdom))
-        s = std::max(s, c_prefil(P, lev, T, g.ilo - ng, g.ihi + ng, g.jlo - ng, g.jlo - 1, g.ilo - ng, g.jlo - ng));
-      else s = std::max(s, c_filrecur(P, lev, T, 1, 1, g.ilo - ng, g.ihi + ng, g.jlo - ng, g.jlo - 1, false, m));
-      const double yt = g.yhi + ng * hy;
-      if ((yt > yupper && yperdom) || ((xl < xlower || xr > xupper) && xperdom))
-        s = std::max(s, c_prefil(P, lev, T, g.ilo - ng, g.ihi + ng, g.jhi + 1, g.jhi + ng, g.ilo - ng, g.jlo - ng));
-      else s = std::max(s, c_filrecur(P, lev, T, 1, mj - ng + 1, g.ilo - ng, g.ihi + ng, g.jhi + 1, g.jhi + ng, false, m));
-      bool any;
-      BcOp b = make_bc(T, hx, hy, g.xlo - ng * hx, g.xhi + ng * hx, g.ylo - ng * hy, g.yhi + ng * hy, any);
-      if (any) P.add_bc(b, s);
-    }
+    bound_strips(P, lev, m, Tgt{m, -1, mitot(m), mjtot(m)}, ng);
+  }
+  // bound.f90:51-158 with ghost width gw into target T (the enlarged array of patch m, or
+  // a scratch rect of the same shape): the four strips, then the physical boundaries
+  void bound_strips(FillProg& P, int lev, int m, Tgt T, int gw) {
+    const HPatch& g = node[m];
+    const double hx = hxposs[lev], hy = hyposs[lev];
+    const int mi = T.ni, mj = T.nj;
+    int s = 0;
+    double xl = g.xlo - gw * hx, xr, yb;
+    if (xl < xlower && xperdom) s = std::max(s, c_prefil(P, lev, T, g.ilo - gw, g.ilo - 1, g.jlo, g.jhi, g.ilo - gw, g.jlo - gw));
+    else s = std::max(s, c_filrecur(P, lev, T, 1, gw + 1, g.ilo - gw, g.ilo - 1, g.jlo, g.jhi, false, m));
+    xr = g.xhi + gw * hx;
+    if (xr > xupper && xperdom) s = std::max(s, c_prefil(P, lev, T, g.ihi + 1, g.ihi + gw, g.jlo, g.jhi, g.ilo - gw, g.jlo - gw));
+    else s = std::max(s, c_filrecur(P, lev, T, mi - gw + 1, gw + 1, g.ihi + 1, g.ihi + gw, g.jlo, g.jhi, false, m));
+    xl = g.xlo - gw * hx; xr = g.xhi + gw * hx; yb = g.ylo - gw * hy;
+    if ((yb < ylower && yperdom) || ((xl < xlower || xr > xupper) && xperdom))
+      s = std::max(s, c_prefil(P, lev, T, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jlo - 1, g.ilo - gw, g.jlo - gw));
+    else s = std::max(s, c_filrecur(P, lev, T, 1, 1, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jlo - 1, false, m));
+    const double yt = g.yhi + gw * hy;
+    if ((yt > yupper && yperdom) || ((xl < xlower || xr > xupper) && xperdom))
+      s = std::max(s, c_prefil(P, lev, T, g.ilo - gw, g.ihi + gw, g.jhi + 1, g.jhi + gw, g.ilo - gw, g.jlo - gw));
+    else s = std::max(s, c_filrecur(P, lev, T, 1, mj - gw + 1, g.ilo - gw, g.ihi + gw, g.jhi + 1, g.jhi + gw, false, m));
+    bool any;
+    BcOp b = make_bc(T, hx, hy, g.xlo - gw * hx, g.xhi + gw * hx, g.ylo - gw * hy, g.yhi + gw * hy, any);
+    if (any) P.add_bc(b, s);
+  }
+
+  // prepbigstep.f:28-58 for patch m: copysol.f puts the old interior in the middle of a
+  // scratch rect with twice the ghost width, bound.f90 fills that ring at the previous time
+  // (same-level sources from the patch's neighbour list, as intfil does with msrc = m)
+  void compile_bigstep_patch(FillProg& P, int lev, int m) {
+    P.scratch_len = 0;
+    const HPatch& g = node[m];
+    const int gw = 2 * ng, ni = g.nx() + 2 * gw, nj = g.ny() + 2 * gw;
+    const int R = P.add_rect(ni, nj, nvar);
+    FillOp o{};
+    o.kind = FILL_COPY; o.dst_patch = -1; o.dst_rect = R;
+    o.di0 = gw; o.dj0 = gw; o.ni = g.nx(); o.nj = g.ny();
+    o.src = m; o.si0 = ng; o.sj0 = ng; o.level = lev;  // the time mode of level lev picks the old values
+    P.add_op(o, 0);
+    bound_strips(P, lev, m, Tgt{-1, R, ni, nj}, gw);
   }
 
   // icall.f / preicall.f: copies of store1 of every grid at `level` into a rect
@@ -1516,6 +1546,105 @@ class Amr2Gpu {
     return true;
   }
 
+  // errest.f:4-63 for the grids G of level lcheck, launched on the stream: the big step
+  // (prepbigstep.f: 2*dt, 2*h on the old values coarsened by 2), the regular step
+  // (prepregstep.f: dt, h on the values just flagged, ghost cells included) and errf1.f's
+  // estimate of component 1, one byte est >= tol per 2x2 block of interior cells (patch k's
+  // blocks from boff[k], i fastest). Both steps run the level step kernel on "virtual
+  // patches": pool arrays with descriptors of their own and no flux registers. The step
+  // results only feed the estimate (stepgrid's Courant number and dtnew are dropped: the
+  // next advanc.f resets cfl_level). Freed by richardson_release after the stream syncs.
+  void richardson_launch(int lcheck, const std::vector<int>& G, int use_old, std::vector<long long>& boff) {
+    HPROF("richardson");
+    if (p.naux > 0) throw std::runtime_error("Richardson estimation needs num_aux = 0 (no auxcoarsen)");
+    const int np = (int)G.size();
+    const double hx = hxposs[lcheck], hy = hyposs[lcheck], dt = possk[lcheck];
+    const double tpre = node[G[0]].time - dt;
+    FillProg& P = rich_prog;
+    P.clear();
+    P.zero_scratch = true;
+    P.scratch_len = 0;
+    for (int l = 1; l <= lcheck; ++l) GI(l);
+    std::vector<FillProg> part(np);
+    pool_host.run(np, [&](int k) { compile_bigstep_patch(part[k], lcheck, G[k]); });
+    std::vector<int> rect_of(np);
+    for (int k = 0; k < np; ++k) { rect_of[k] = (int)P.rects.size(); merge_prog(P, part[k]); }
+    upload_prog(P);
+    // virtual patches: k the coarsened values, np+k the regular step; buffers in one block
+    std::vector<PatchDev> vp(2 * (size_t)np);
+    std::vector<long long> vo(2 * (size_t)np + 1, 0);
+    boff.assign(np + 1, 0);
+    for (int k = 0; k < np; ++k) {
+      const HPatch& g = node[G[k]];
+      const long long mi2 = g.nx() / 2 + 2 * ng, mj2 = g.ny() / 2 + 2 * ng;
+      vo[k + 1] = vo[k] + 2 * Arena::rnd(nvar * mi2 * mj2);
+      boff[k + 1] = boff[k] + (long long)(g.nx() / 2) * (g.ny() / 2);
+    }
+    for (int k = 0; k < np; ++k) vo[np + k + 1] = vo[np + k] + Arena::rnd((long long)nvar * mitot(G[k]) * mjtot(G[k]));
+    rich_len = std::max<long long>(vo[2 * np], 1);
+    rich_buf = palloc(rich_len);
+    std::vector<StepWork> work;
+    auto tiles = [&](int v, int mx, int my) {
+      for (int tj = 1; tj <= my; tj += TILE2)
+        for (int ti = 1; ti <= mx; ti += TILE2) work.push_back(StepWork{v, ti, tj, 0, 0, 0, 0});
+    };
+    for (int k = 0; k < np; ++k) {
+      const HPatch& g = node[G[k]];
+      PatchDev B{};
+      const int nx2 = g.nx() / 2, ny2 = g.ny() / 2;
+      B.mitot = nx2 + 2 * ng; B.mjtot = ny2 + 2 * ng; B.mktot = 1;
+      B.q[0] = rich_buf + vo[k]; B.q[1] = B.q[0] + Arena::rnd((long long)nvar * B.mitot * B.mjtot);
+      B.cur = 0; B.ilo = 0; B.ihi = nx2 - 1; B.jlo = 0; B.jhi = ny2 - 1;
+      B.ffl = -1; B.level = lcheck; B.aux = -1;
+      vp[k] = B;
+      tiles(k, nx2, ny2);
+    }
+    const int nbig = (int)work.size();
+    for (int k = 0; k < np; ++k) {
+      const HPatch& g = node[G[k]];
+      PatchDev R{};
+      const int in_cur = use_old ? 1 - g.cur : g.cur;
+      R.q[0] = in_cur == 0 ? g.q0 : g.q1; R.q[1] = rich_buf + vo[np + k];
+      R.cur = 0; R.ilo = g.ilo; R.ihi = g.ihi; R.jlo = g.jlo; R.jhi = g.jhi;
+      R.mitot = mitot(G[k]); R.mjtot = mjtot(G[k]); R.mktot = 1;
+      R.ffl = -1; R.level = lcheck; R.aux = -1;
+      vp[np + k] = R;
+      tiles(np + k, g.nx(), g.ny());
+    }
+    const int nreg = (int)work.size() - nbig;
+    rich_vp.upload(vp, st, stg);
+    rich_work.upload(work, st, stg);
+    rich_rect.upload(rect_of, st, stg);
+    rich_off.upload(boff, st, stg);
+    rich_out.ensure(std::max<long long>(boff[np], 1));
+    rich_cfl.ensure(1);
+    // the ghost ring at tpre, then coarsen.f
+    run_prog(P, bound_modes(lcheck, tpre));
+    launch_coarsen2(pool.d, P.d_rects.d, rich_rect.d, rich_vp.d, np, nvar, st, f32);
+    StepArgs a{};
+    a.pool = pool.d; a.regs = regs.d; a.patches = rich_vp.d; a.fsv = nullptr; a.fad = nullptr;
+    a.cflmax = rich_cfl.d; a.sp = sp; a.queue = nullptr; a.dt_dev = nullptr;
+    if (nbig > 0) {
+      a.work = rich_work.d; a.nwork = nbig;
+      a.dt = 2.0 * dt; a.dx = 2.0 * hx; a.dy = 2.0 * hy;
+      launch_step2(prob.solver, a, nbig, st, f32);
+    }
+    if (nreg > 0) {
+      a.work = rich_work.d + nbig; a.nwork = nreg;
+      a.dt = dt; a.dx = hx; a.dy = hy;
+      launch_step2(prob.solver, a, nreg, st, f32);
+    }
+    const double order = (double)((1 << (sp.order + 1)) - 2);
+    launch_errf2(pool.d, rich_vp.d, np, ng, order, p.tol, rich_off.d, rich_out.d, st, f32);
+    nkernels += 3 + (nbig > 0) + (nreg > 0);
+  }
+  void richardson_release() {
+    pfree(rich_prog.scratch_off, rich_prog.scratch_alloc);
+    rich_prog.scratch_off = -1;
+    pfree(rich_buf, rich_len);
+    rich_buf = -1;
+  }
+
   // flagger.f + bufnst2.f + colate2.f: the sorted, unique flagged points of level lcheck
   std::vector<Pt> flag_points(int lcheck, int lbase) {
     const int mbuff = std::max(ng, p.ibuff + 1);
@@ -1537,7 +1666,15 @@ class Amr2Gpu {
     launch_flags2(pool.d, d_patches.d, dpl.d, doff.d, (int)G.size(), use_old, p.flag_component, p.tolsp, nvar, dout.d, st, f32);
     std::vector<int8_t> hflag(off.back());
     if (off.back()) AMR_CUDA(cudaMemcpyAsync(hflag.data(), dout.d, off.back(), cudaMemcpyDeviceToHost, st));
+    std::vector<long long> roff;
+    std::vector<int8_t> rbits;
+    if (p.flag_richardson) {
+      richardson_launch(lcheck, G, use_old, roff);
+      rbits.resize(roff.back());
+      if (roff.back()) AMR_CUDA(cudaMemcpyAsync(rbits.data(), rich_out.d, roff.back(), cudaMemcpyDeviceToHost, st));
+    }
     sync_stream();
+    if (p.flag_richardson) richardson_release();
     const auto tf1 = std::chrono::steady_clock::now();
     tr_flags += std::chrono::duration<double>(tf1 - tf0).count();
     const double dx = hxposs[lcheck], dy = hyposs[lcheck];
@@ -1594,6 +1731,23 @@ class Amr2Gpu {
           if (v == FLAG_UNSET && p.flag_gradient && gf[(size_t)(j - 1) * mx + (i - 1)]) v = FLAG_DO;
           f[B.idx(g.ilo + i - 1, g.jlo + j - 1)] = v;
         }
+      // errf1.f:55-95: a block with a flag still unset gets DOFLAG on all four cells when
+      // est >= tol. The reference indexes the flag array (nx + 2*mbuff wide) with the fine
+      // grid's ghost width, so a block's flags sit mbuff - nghost cells below and left of
+      // the cells whose values it compares; they are placed the same way here (cells that
+      // land in the buffer zone are dropped by shiftset2.f, as there)
+      if (p.flag_richardson) {
+        const int8_t* rb = rbits.data() + roff[k];
+        const int nxc = mx / 2, nyc = my / 2, sh = ng - mbuff;
+        for (int jc = 0; jc < nyc; ++jc)
+          for (int ic = 0; ic < nxc; ++ic) {
+            if (!rb[(size_t)jc * nxc + ic]) continue;
+            const int i0 = g.ilo + sh + 2 * ic, j0 = g.jlo + sh + 2 * jc;
+            int8_t* c[4] = {&f[B.idx(i0, j0)], &f[B.idx(i0 + 1, j0)], &f[B.idx(i0, j0 + 1)], &f[B.idx(i0 + 1, j0 + 1)]};
+            if (*c[0] == FLAG_UNSET || *c[1] == FLAG_UNSET || *c[2] == FLAG_UNSET || *c[3] == FLAG_UNSET)
+              for (int8_t* q : c) *q = FLAG_DO;
+          }
+      }
       // projec2.f: cells under level lcheck+2 grids just created
       if (lcheck + 2 <= p.mxnest) {
         std::vector<int> cand;
@@ -1954,6 +2108,13 @@ class Amr2Gpu {
         const int levold = levnew - 1;
         if (lstart[levold] == 0) break;
         compile_all();
+        // setgrd.f:41-53: Richardson estimation needs the level one step ahead before it
+        // is flagged; that step is not counted as integration work
+        if (p.flag_richardson) {
+          advanc(levold);
+          rvol = 0;
+          for (double& r : rvoll) r = 0;
+        }
         for (int i = 1; i <= p.mxnest; ++i) newstl[i] = 0;
         grdfit(levold, levold, start_time);
         int lfnew = levold;
@@ -1967,7 +2128,12 @@ class Amr2Gpu {
         make_bndry(levnew);
         ++levnew;
       }
-      // store1 and store2 of the initial levels hold the same qinit data; both buffers were filled
+      // store1 and store2 of the initial levels hold the same qinit data (both buffers were
+      // filled), unless the Richardson steps above advanced them: setgrd.f:106-121 swaps the
+      // stores, putting the initial values back in store1, and resets the times
+      if (p.flag_richardson)
+        for (int lev = 1; !(lev == p.mxnest || lev > lfine); ++lev)
+          for (int m : lgrids[lev]) { node[m].cur ^= 1; node[m].time = start_time; }
       compile_all();
       for (int lev = lfine - 1; lev >= 1; --lev) update(lev);
       for (int lev = 1; lev <= lfine - 1; ++lev) { prepf(lev + 1); prepc(lev); }

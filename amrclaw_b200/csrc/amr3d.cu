@@ -2276,13 +2276,12 @@ class Amr3Gpu : public AmrSolver {
 
   // ================================================================ results
   double mass() {
+    ensure(1, NEED_STEP);  // the level's patch list on the device
     AMR_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double), st));
-    DBuf<int> dp; dp.upload(lgrids[1], st, stg);
-    launch_mass3(pool.d, d_patches.d, dp.d, (int)lgrids[1].size(), d_mass, st, f32);
+    launch_mass3(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st, f32);
     double m = 0;
     AMR_CUDA(cudaMemcpyAsync(&m, d_mass, sizeof(double), cudaMemcpyDeviceToHost, st));
     sync_stream();
-    dp.free();
     return m * hxposs[1] * hyposs[1] * hzposs[1];
   }
   std::vector<double> gather_values() {

@@ -906,4 +906,69 @@ void launch_gather_interior2(const void* pool, const PatchDev* patches, const in
   }
 }
 
+// ======================================================================= Richardson estimation
+// coarsen.f:4-33: 2x2 means of scratch rect rect_of[k] (twice the ghost width) into the
+// first buffer of virtual patch k (its enlarged array, ghost cells included); FP64 sums
+template <class T>
+__global__ void coarsen2_kernel(T* pool, const ScratchRect* rects, const int* rect_of, const PatchDev* vp, int nvar) {
+  const int k = blockIdx.y;
+  const PatchDev P = vp[k];
+  const ScratchRect R = rects[rect_of[k]];
+  const T* src = pool + R.off;
+  T* dst = pool + P.q[0];
+  const long long splane = (long long)R.ni * R.nj, dplane = (long long)P.mitot * P.mjtot;
+  const int n = P.mitot * P.mjtot;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * nvar; t += gridDim.x * blockDim.x) {
+    const int m = t / n, rem = t % n;
+    const int i = rem % P.mitot, j = rem / P.mitot;
+    const T* s0 = src + m * splane + (long long)(2 * j) * R.ni + 2 * i;
+    const double v = ((((double)s0[0] + (double)s0[1]) + (double)s0[R.ni]) + (double)s0[R.ni + 1]) / 4.0;
+    dst[m * dplane + (long long)j * P.mitot + i] = (T)v;
+  }
+}
+void launch_coarsen2(void* pool, const ScratchRect* rects, const int* rect_of, const PatchDev* vp, int np, int nvar,
+                     cudaStream_t s, bool f32) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    if (f32) coarsen2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<float*>(pool), rects, rect_of + base, vp + base, nvar);
+    else coarsen2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<double*>(pool), rects, rect_of + base, vp + base, nvar);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
+// errf1.f:40-71: for each 2x2 block of interior cells of patch k, the mean of component 1
+// after the regular step (second buffer of virtual patch np+k) against the coarse cell
+// after the big step (second buffer of virtual patch k); one byte est >= tol per block,
+// blocks i fastest from outoff[k]
+template <class T>
+__global__ void errf2_kernel(const T* pool, const PatchDev* vp, int np, int ng, double order, double tol,
+                             const long long* outoff, int8_t* out) {
+  const int k = blockIdx.y;
+  const PatchDev C = vp[k], F = vp[np + k];
+  const int nxc = (F.ihi - F.ilo + 1) / 2, nyc = (F.jhi - F.jlo + 1) / 2;
+  const T* fine = pool + F.q[1];
+  const T* crse = pool + C.q[1];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nxc * nyc; t += gridDim.x * blockDim.x) {
+    const int ic = t % nxc, jc = t / nxc;
+    const T* f0 = fine + (long long)(2 * jc + ng) * F.mitot + (2 * ic + ng);
+    const double t1 = (double)f0[0], t2 = (double)f0[1], t3 = (double)f0[F.mitot + 1], t4 = (double)f0[F.mitot];
+    const double aval = (((t1 + t2) + t3) + t4) / 4.0;
+    const double est = fabs((aval - (double)crse[(long long)(jc + ng) * C.mitot + (ic + ng)]) / order);
+    out[outoff[k] + t] = est >= tol ? 1 : 0;
+  }
+}
+void launch_errf2(const void* pool, const PatchDev* vp, int np, int ng, double order, double tol, const long long* outoff,
+                  int8_t* out, cudaStream_t s, bool f32) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    // virtual patches base..base+n-1 and their regular-step partners np+base..: pass the
+    // array from base with the partner distance np unchanged
+    if (f32)
+      errf2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const float*>(pool), vp + base, np, ng, order, tol, outoff + base, out);
+    else
+      errf2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const double*>(pool), vp + base, np, ng, order, tol, outoff + base, out);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
 }  // namespace amrb

@@ -147,5 +147,11 @@ void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, i
 void launch_gather_interior2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff,
                              int np, int nvar, double* out, cudaStream_t s, bool f32);
 size_t step2_smem_bytes(int solver, bool f32);
+// Richardson estimation (errest.f): rect_of[k] is the scratch rect of virtual patch k
+void launch_coarsen2(void* pool, const ScratchRect* rects, const int* rect_of, const PatchDev* vp, int np, int nvar,
+                     cudaStream_t s, bool f32);
+// vp[0..np): the big-step patches, vp[np..2np): the regular-step patches
+void launch_errf2(const void* pool, const PatchDev* vp, int np, int ng, double order, double tol, const long long* outoff,
+                  int8_t* out, cudaStream_t s, bool f32);
 
 }  // namespace amrb

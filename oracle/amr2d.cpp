@@ -1454,7 +1454,75 @@ struct Amr2 {
       bool keep = false;
       for (double f : g.flags) if (f == UNSET) { keep = true; break; }
       if (flag_gradient && keep) flag2refine2(nxg, nyg, nghost, mbuff, use, tolsp, g.flags.data());
+      keep = false;
+      for (double f : g.flags) if (f == UNSET) { keep = true; break; }
+      // flagger.f:93-105: locbig is a copy of the values just flagged, ghost cells included
+      if (flag_richardson && keep) errest(mptr, lcheck, std::vector<double>(use, use + (size_t)nvar * mitot * mjtot), mbuff);
     }
+  }
+
+  // errest.f:4-63 for grid mptr of level lcheck: a step of 2*dt on the old values
+  // coarsened by 2 (prepbigstep.f:5-64 with copysol.f and coarsen.f:4-33), a regular step
+  // on `big` (prepregstep.f:5-36), then errf1.f:40-95 on component 1
+  void errest(int mptr, int lcheck, std::vector<double> big, int mbuff) {
+    if (naux > 0) throw std::runtime_error("Richardson estimation needs num_aux = 0 (no auxcoarsen)");
+    const Node2& g = node[mptr];
+    const int nx = g.ihi - g.ilo + 1, ny = g.jhi - g.jlo + 1;
+    const int mitot = nx + 2 * nghost, mjtot = ny + 2 * nghost;
+    const int mi2tot = nx / 2 + 2 * nghost, mj2tot = ny / 2 + 2 * nghost;
+    const int ng2 = 2 * nghost, midub = nx + 4 * nghost, mjdub = ny + 4 * nghost;
+    const double hx = hxposs[lcheck], hy = hyposs[lcheck];
+    const double hx2 = 2.0 * hx, hy2 = 2.0 * hy;
+    const double dt = possk[lcheck], dt2 = 2.0 * dt;  // `2. * dt`: the REAL literal 2. is exact
+    const double tpre = g.time - dt;
+    // copysol.f: the interior of the old values into an array with twice the ghost width
+    std::vector<double> valdub((size_t)nvar * midub * mjdub, 0.0);
+    FArr V{valdub.data(), nvar, midub, mjdub};
+    const FArr Q2{const_cast<double*>(g.q2.data()), nvar, mitot, mjtot};
+    for (int j = nghost + 1; j <= mjtot - nghost; ++j)
+      for (int i = nghost + 1; i <= mitot - nghost; ++i)
+        for (int m = 1; m <= nvar; ++m) V(m, i - nghost + ng2, j - nghost + ng2) = Q2(m, i, j);
+    bound(tpre, ng2, valdub.data(), midub, mjdub, mptr);
+    // coarsen.f
+    std::vector<double> valbgc((size_t)nvar * mi2tot * mj2tot);
+    FArr C{valbgc.data(), nvar, mi2tot, mj2tot};
+    for (int j = 1; j <= mj2tot; ++j) {
+      const int jf = 2 * (j - 1) + 1;
+      for (int i = 1; i <= mi2tot; ++i) {
+        const int iff = 2 * (i - 1) + 1;
+        for (int m = 1; m <= nvar; ++m) C(m, i, j) = (((V(m, iff, jf) + V(m, iff + 1, jf)) + V(m, iff, jf + 1)) + V(m, iff + 1, jf + 1)) / 4.0;
+      }
+    }
+    double dtnew, cflg;
+    {
+      const size_t nf = (size_t)nvar * mi2tot * mj2tot;
+      std::vector<double> fm(nf), fp(nf), gm(nf), gp(nf);
+      stepgrid(valbgc.data(), fm.data(), fp.data(), gm.data(), gp.data(), mi2tot, mj2tot, nghost, dt2, dtnew, hx2, hy2, nullptr, cflg);
+    }
+    {
+      const size_t nf = (size_t)nvar * mitot * mjtot;
+      std::vector<double> fm(nf), fp(nf), gm(nf), gp(nf);
+      stepgrid(big.data(), fm.data(), fp.data(), gm.data(), gp.data(), mitot, mjtot, nghost, dt, dtnew, hx, hy, nullptr, cflg);
+    }
+    // errf1.f: the flag array (nx+2*mbuff wide) is indexed with the fine grid's ghost
+    // width, as in the reference
+    const FArr F{big.data(), nvar, mitot, mjtot};
+    const int mib = nx + 2 * mbuff;
+    auto RF = [&](int i, int j) -> double& { return node[mptr].flags[(size_t)(i - 1) + (size_t)mib * (j - 1)]; };
+    const double order = (double)((1 << (method[2] + 1)) - 2);
+    std::vector<double> rflag((size_t)mi2tot * mj2tot, UNSET);
+    for (int j = nghost + 1, jf = nghost + 1; j <= mj2tot - nghost; ++j, jf += 2)
+      for (int i = nghost + 1, iff = nghost + 1; i <= mi2tot - nghost; ++i, iff += 2) {
+        if (RF(iff, jf) == UNSET || RF(iff + 1, jf) == UNSET || RF(iff, jf + 1) == UNSET || RF(iff + 1, jf + 1) == UNSET) {
+          const double aval = (((F(1, iff, jf) + F(1, iff + 1, jf)) + F(1, iff + 1, jf + 1)) + F(1, iff, jf + 1)) / 4.0;
+          const double est = std::fabs((aval - C(1, i, j)) / order);
+          if (est >= tol) rflag[(size_t)(i - 1) + (size_t)mi2tot * (j - 1)] = DOFLAG;
+        }
+      }
+    for (int j = nghost + 1, jf = nghost + 1; j <= mj2tot - nghost; ++j, jf += 2)
+      for (int i = nghost + 1, iff = nghost + 1; i <= mi2tot - nghost; ++i, iff += 2)
+        if (rflag[(size_t)(i - 1) + (size_t)mi2tot * (j - 1)] == DOFLAG)
+          RF(iff, jf) = RF(iff + 1, jf) = RF(iff, jf + 1) = RF(iff + 1, jf + 1) = DOFLAG;
   }
 
   void setIndices(int ist[3], int iend[3], int jst[3], int jend[3], int ilo, int ihi, int jlo, int jhi, int ishift[3], int jshift[3], int level) {
@@ -2111,6 +2179,14 @@ struct Amr2 {
       if (lstart[levold] == 0) break;
       const int lbase = levold;
       int lfnew = lbase;
+      // setgrd.f:41-53: Richardson estimation needs the level one step ahead before it is
+      // flagged; that step is not counted as integration work
+      if (flag_richardson) {
+        double dtlev;
+        advanc(levold, dtlev);
+        rvol = 0;
+        for (double& r : rvoll) r = 0;
+      }
       for (int i = 1; i <= mxnest; ++i) newstl[i] = 0;
       grdfit(lbase, levold, t, start_time);
       if (newstl[levnew] != 0) lfnew = levnew;
