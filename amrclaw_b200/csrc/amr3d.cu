@@ -172,6 +172,14 @@ class Amr3Gpu : public AmrSolver {
   std::vector<PatchDev> h_patches;
   Plan3 plan[12];
   Prog3 newfill;
+  // Richardson estimation (errest.f) of the level being flagged: the ghost fill of the big
+  // step, the virtual patches of both steps and their step prefixes
+  Prog3 rich_prog;
+  DBuf<PatchDev> rich_vp;
+  DBuf<int> rich_rect, rich_plist;
+  DBuf<long long> rich_pre;
+  DBuf<unsigned long long> rich_cfl;
+  long long rich_buf = -1, rich_len = 0;
   DBuf<double> d_stash, d_flux;
   DBuf<int8_t> lv_a, lv_b, lv_n, lv_t1, lv_t2;   // level flag arrays (flglvl)
   DBuf<LvlBox> lv_boxes, lv_proj;
@@ -216,6 +224,8 @@ class Amr3Gpu : public AmrSolver {
     if (h_sub) cudaFreeHost(h_sub);
     for (auto& L : plan) L.free_dev();
     newfill.free_dev();
+    rich_prog.free_dev();
+    rich_vp.free(); rich_rect.free(); rich_plist.free(); rich_pre.free(); rich_cfl.free();
     pool.destroy(); regs.destroy();
     stg.destroy();
     d_patches.free(); d_stash.free(); d_flux.free(); d_gauge_out.free(); d_aux_jobs.free(); d_aux_fac.free();
@@ -259,7 +269,10 @@ class Amr3Gpu : public AmrSolver {
     if (p.nghost != G3) throw std::runtime_error("num_ghost must be 2");
     if (p.mcapa != 0 || p.dimsplit != 0) throw std::runtime_error("capacity functions and dimensional splitting are not supported");
     if (p.use_fwaves) throw std::runtime_error("f-waves are not supported in 3D");
-    if (p.flag_richardson || p.tol > 0) throw std::runtime_error("Richardson estimation (flag_richardson_tol > 0) is not supported");
+    if (p.flag_richardson && p.naux > 0) throw std::runtime_error("Richardson estimation needs num_aux = 0 (no auxcoarsen)");
+    // bufnst.f:21-24 adds store2's first component to the flags whenever tol > 0: without
+    // errest.f having written flags there, that would be the old solution
+    if (!p.flag_richardson && p.tol > 0) throw std::runtime_error("flag_richardson_tol > 0 needs flag_richardson");
     for (int d = 1; d <= 6; ++d)
       if (p.mthbc[d] != 1 && p.mthbc[d] != 3) throw std::runtime_error("3D device path: boundaries must be extrapolation or wall");
     sp.gamma = p.pn("gamma", 1.4); sp.gamma1 = sp.gamma - 1.0;
@@ -595,8 +608,18 @@ class Amr3Gpu : public AmrSolver {
       const GridIndex& X = GI(level);
       std::vector<int> hits;
       X.query(ilo, ihi, jlo, jhi, klo, khi, hits);
-      for (int r : hits)
-        if (X.id(r) != msrc) src.push_back(X.id(r));
+      // init_bndryList.f keeps the grids that meet msrc grown by nghost in i and j (not k):
+      // every source of a ghost strip of width nghost, but not all of a wider ring's
+      const HPatch3* gm = msrc > 0 ? &node[msrc] : nullptr;
+      for (int r : hits) {
+        const int m = X.id(r);
+        if (m == msrc) continue;
+        if (gm) {
+          const HPatch3& q = node[m];
+          if (std::max(q.ilo, gm->ilo - G3) > std::min(q.ihi, gm->ihi + G3) || std::max(q.jlo, gm->jlo - G3) > std::min(q.jhi, gm->jhi + G3)) continue;
+        }
+        src.push_back(m);
+      }
     }
     for (int m : src) {
       const HPatch3& g = node[m];
@@ -663,21 +686,36 @@ class Amr3Gpu : public AmrSolver {
   }
 
   // bound.f:4-211 for one patch
-  void compile_bound_patch(Prog3& P, int lev, int m) {
+  void compile_bound_patch(Prog3& P, int lev, int m) { bound_strips(P, lev, m, Tgt3{m, -1, mitot(m), mjtot(m), mktot(m)}, G3); }
+  // bound.f with ghost width gw into target T (the enlarged array of patch m, or a scratch
+  // rect of the same shape): the six strips, then the physical boundaries
+  void bound_strips(Prog3& P, int lev, int m, Tgt3 T, int gw) {
     const HPatch3& g = node[m];
-    const int mi = mitot(m), mj = mjtot(m), mk = mktot(m);
-    Tgt3 T{m, -1, mi, mj, mk};
+    const int mi = T.ni, mj = T.nj, mk = T.nk;
     int s = 0;
-    s = std::max(s, c_filrecur(P, lev, T, 1, 1, G3 + 1, g.ilo - G3, g.ilo - 1, g.jlo - G3, g.jhi + G3, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, mi - G3 + 1, 1, G3 + 1, g.ihi + 1, g.ihi + G3, g.jlo - G3, g.jhi + G3, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, G3 + 1, 1, G3 + 1, g.ilo, g.ihi, g.jlo - G3, g.jlo - 1, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, G3 + 1, mj - G3 + 1, G3 + 1, g.ilo, g.ihi, g.jhi + 1, g.jhi + G3, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, 1, 1, 1, g.ilo - G3, g.ihi + G3, g.jlo - G3, g.jhi + G3, g.klo - G3, g.klo - 1, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, 1, 1, mk - G3 + 1, g.ilo - G3, g.ihi + G3, g.jlo - G3, g.jhi + G3, g.khi + 1, g.khi + G3, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, 1, 1, gw + 1, g.ilo - gw, g.ilo - 1, g.jlo - gw, g.jhi + gw, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, mi - gw + 1, 1, gw + 1, g.ihi + 1, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, gw + 1, 1, gw + 1, g.ilo, g.ihi, g.jlo - gw, g.jlo - 1, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, gw + 1, mj - gw + 1, gw + 1, g.ilo, g.ihi, g.jhi + 1, g.jhi + gw, g.klo, g.khi, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, 1, 1, 1, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.klo - gw, g.klo - 1, false, m));
+    s = std::max(s, c_filrecur(P, lev, T, 1, 1, mk - gw + 1, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.khi + 1, g.khi + gw, false, m));
     const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
     bool any;
-    Bc3Op b = make_bc(T, hx, hy, hz, g.xlo - G3 * hx, g.xhi + G3 * hx, g.ylo - G3 * hy, g.yhi + G3 * hy, g.zlo - G3 * hz, g.zhi + G3 * hz, any);
+    Bc3Op b = make_bc(T, hx, hy, hz, g.xlo - gw * hx, g.xhi + gw * hx, g.ylo - gw * hy, g.yhi + gw * hy, g.zlo - gw * hz, g.zhi + gw * hz, any);
     if (any) P.add_bc(b, s);
+  }
+  // errest.f:35-76 for patch m: copysol.f puts the old interior in the middle of a scratch
+  // rect with twice the ghost width, bound.f fills that ring at the previous time
+  void compile_bigstep_patch(Prog3& P, int lev, int m) {
+    const HPatch3& g = node[m];
+    const int gw = 2 * G3, ni = g.nx() + 2 * gw, nj = g.ny() + 2 * gw, nk = g.nz() + 2 * gw;
+    const int R = P.add_rect(ni, nj, nk, nvar);
+    Fill3Op o{};
+    o.kind = F3_COPY; o.dst_patch = -1; o.dst_rect = R;
+    o.di0 = gw; o.dj0 = gw; o.dk0 = gw; o.ni = g.nx(); o.nj = g.ny(); o.nk = g.nz();
+    o.src = m; o.si0 = G3; o.sj0 = G3; o.sk0 = G3; o.level = lev;  // the time mode of level lev picks the old values
+    P.add_op(o, 0);
+    bound_strips(P, lev, m, Tgt3{-1, R, ni, nj, nk}, gw);
   }
   void compile_bound(int lev) {
     HPROF("compile_bound3");
@@ -1529,6 +1567,129 @@ class Amr3Gpu : public AmrSolver {
   }
 
   // ================================================================ regrid: level flag arrays on the device
+  // errest.f:4-141 for the grids G of level lcheck, launched on the stream: the big step
+  // (2*dt, 2*h on the old values coarsened by 2, ghost ring of twice the width filled at
+  // t-dt), the regular step (dt, h on the values spest.f flags: store1 with its ghost
+  // cells just filled) and errf1.f's estimate of component 1; when tol > 0 the flagged
+  // blocks add BADPT to the level array f (bufnst.f:21-24 with setflags.f). Both steps run
+  // the level step kernels on "virtual patches": pool arrays with descriptors of their own
+  // and no flux registers; their Courant numbers and dtnew are dropped (the next advanc.f
+  // resets cfl_level). richardson_release frees the buffers after the stream syncs.
+  void richardson_launch(int lcheck, const std::vector<int>& G, int8_t* f, LvlDims dl) {
+    HPROF("richardson3");
+    const int np = (int)G.size();
+    const double hx = hxposs[lcheck], hy = hyposs[lcheck], hz = hzposs[lcheck], dt = possk[lcheck];
+    const double tpre = node[G[0]].time - dt;
+    Prog3& P = rich_prog;
+    P.clear();
+    P.zero_scratch = true;
+    for (int l = 1; l <= lcheck; ++l) GI(l);
+    std::vector<Prog3> part(np);
+    pool_host.run(np, [&](int k) { compile_bigstep_patch(part[k], lcheck, G[k]); });
+    std::vector<int> rect_of(np);
+    for (int k = 0; k < np; ++k) { rect_of[k] = (int)P.rects.size(); merge_prog(P, part[k], k); }
+    upload_prog(P);
+    // virtual patches: k the coarsened values, np+k the regular step; buffers in one block
+    std::vector<PatchDev> vp(2 * (size_t)np);
+    std::vector<long long> vo(2 * (size_t)np + 1, 0);
+    for (int k = 0; k < np; ++k) {
+      const HPatch3& g = node[G[k]];
+      const long long n2 = (long long)(g.nx() / 2 + 2 * G3) * (g.ny() / 2 + 2 * G3) * (g.nz() / 2 + 2 * G3);
+      vo[k + 1] = vo[k] + 2 * Arena::rnd(nvar * n2);
+    }
+    for (int k = 0; k < np; ++k) vo[np + k + 1] = vo[np + k] + Arena::rnd((long long)nvar * mitot(G[k]) * mjtot(G[k]) * mktot(G[k]));
+    rich_len = std::max<long long>(vo[2 * np], 1);
+    rich_buf = palloc(rich_len);
+    for (int k = 0; k < np; ++k) {
+      const HPatch3& g = node[G[k]];
+      PatchDev B{};
+      const int nx2 = g.nx() / 2, ny2 = g.ny() / 2, nz2 = g.nz() / 2;
+      B.mitot = nx2 + 2 * G3; B.mjtot = ny2 + 2 * G3; B.mktot = nz2 + 2 * G3;
+      B.q[0] = rich_buf + vo[k]; B.q[1] = B.q[0] + Arena::rnd((long long)nvar * B.mitot * B.mjtot * B.mktot);
+      B.cur = 0; B.ilo = 0; B.ihi = nx2 - 1; B.jlo = 0; B.jhi = ny2 - 1; B.klo = 0; B.khi = nz2 - 1;
+      B.ffl = -1; B.level = lcheck; B.aux = -1;
+      vp[k] = B;
+      PatchDev R{};
+      R.q[0] = g.cur == 0 ? g.q0 : g.q1; R.q[1] = rich_buf + vo[np + k];
+      R.cur = 0; R.ilo = g.ilo; R.ihi = g.ihi; R.jlo = g.jlo; R.jhi = g.jhi; R.klo = g.klo; R.khi = g.khi;
+      R.mitot = mitot(G[k]); R.mjtot = mjtot(G[k]); R.mktot = mktot(G[k]);
+      R.ffl = -1; R.level = lcheck; R.aux = -1;
+      vp[np + k] = R;
+    }
+    // step prefixes of both lists, as compile_step builds them for a level:
+    // [sweep0 3*(n+1) | comp0 3*(n+1) | face0 n+1 | cell0 n+1] per list
+    std::vector<long long> pre;
+    long long items[2][3], slots[2], faces[2], cells[2], base[2];
+    for (int li = 0; li < 2; ++li) {
+      base[li] = (long long)pre.size();
+      const int n = np, first = li * np;
+      std::vector<long long> sw(3 * (size_t)(n + 1), 0), cp(3 * (size_t)(n + 1), 0), fc(n + 1, 0), ce(n + 1, 0);
+      long long slot = 0;
+      for (int d = 0; d < 3; ++d) {
+        long long comp = 0;
+        for (int k = 0; k < n; ++k) {
+          const PatchDev& V = vp[first + k];
+          const long long mx = V.ihi - V.ilo + 1, my = V.jhi - V.jlo + 1, mz = V.khi - V.klo + 1;
+          const long long n1 = d == 0 ? mx : d == 1 ? my : mz;
+          const long long pencils = d == 0 ? (my + 2) * (mz + 2) : d == 1 ? (mx + 2) * (mz + 2) : (mx + 2) * (my + 2);
+          sw[(size_t)d * (n + 1) + k] = slot; cp[(size_t)d * (n + 1) + k] = comp;
+          slot += pencils * (n1 + 1);
+          comp += pencils * (n1 + 3);
+        }
+        sw[(size_t)d * (n + 1) + n] = slot; cp[(size_t)d * (n + 1) + n] = comp;
+        items[li][d] = comp;
+      }
+      for (int k = 0; k < n; ++k) {
+        const PatchDev& V = vp[first + k];
+        const long long mx = V.ihi - V.ilo + 1, my = V.jhi - V.jlo + 1, mz = V.khi - V.klo + 1;
+        fc[k + 1] = fc[k] + (mx + 1) * (my + 1) * (mz + 1);
+        ce[k + 1] = ce[k] + mx * my * mz;
+      }
+      slots[li] = slot; faces[li] = fc[n]; cells[li] = ce[n];
+      pre.insert(pre.end(), sw.begin(), sw.end());
+      pre.insert(pre.end(), cp.begin(), cp.end());
+      pre.insert(pre.end(), fc.begin(), fc.end());
+      pre.insert(pre.end(), ce.begin(), ce.end());
+    }
+    std::vector<int> pl(2 * (size_t)np);
+    for (int k = 0; k < 2 * np; ++k) pl[k] = k;
+    rich_vp.upload(vp, st, stg);
+    rich_rect.upload(rect_of, st, stg);
+    rich_plist.upload(pl, st, stg);
+    rich_pre.upload(pre, st, stg);
+    rich_cfl.ensure(1);
+    d_stash.reserve(std::max<size_t>(d_stash.n, (size_t)(std::max(slots[0], slots[1]) * stash_values(nvar))));
+    d_flux.reserve(std::max<size_t>(d_flux.n, (size_t)(std::max(faces[0], faces[1]) * 6 * nvar)));
+    // the ghost ring at tpre, coarsen.f, then the two steps
+    run_prog(P, modes_for(lcheck, tpre));
+    launch_coarsen3(pool.d, P.d_rects.d, rich_rect.d, rich_vp.d, np, nvar, st, f32);
+    nkernels += 1;
+    for (int li = 0; li < 2; ++li) {
+      if (cells[li] == 0) continue;
+      Step3Args a{};
+      a.pool = pool.d; a.patches = rich_vp.d; a.sp = sp;
+      a.plist = rich_plist.d + li * np; a.np = np;
+      const long long* b = rich_pre.d + base[li];
+      a.sweep0 = b; a.comp0 = b + 3 * (np + 1); a.face0 = b + 6 * (np + 1); a.cell0 = b + 7 * (np + 1);
+      a.stash = d_stash.d; a.stash_stride = slots[li]; a.flux = d_flux.d; a.flux_stride = faces[li];
+      a.dt = li == 0 ? 2.0 * dt : dt;
+      a.dx = li == 0 ? 2.0 * hx : hx; a.dy = li == 0 ? 2.0 * hy : hy; a.dz = li == 0 ? 2.0 * hz : hz;
+      a.cflmax = rich_cfl.d; a.queue = nullptr; a.dt_dev = nullptr;
+      nkernels += launch_step3(a, items[li], faces[li], cells[li], st, f32);
+    }
+    if (p.tol > 0) {
+      const double order = (double)((1 << (sp.order + 1)) - 2);
+      launch_errf3(pool.d, rich_vp.d, np, order, p.tol, f, dl, st, f32);
+      nkernels += 1;
+    }
+  }
+  void richardson_release() {
+    pfree(rich_prog.scratch_off, rich_prog.scratch_alloc);
+    rich_prog.scratch_off = -1;
+    pfree(rich_buf, rich_len);
+    rich_buf = -1;
+  }
+
   // flglvl.f:4-85 with domprep.f, domshrink.f, domup.f, domcopy.f, spest.f (+ flag2refine.f,
   // setflags.f), bufnst.f (+ projec.f, shiftset.f) and colate.f. The arrays live in device
   // memory; one read-back returns the flags (for the ordered point list) and the nesting
@@ -1559,9 +1720,11 @@ class Amr3Gpu : public AmrSolver {
     // shrunk array itself becomes the flag array
     AMR_CUDA(cudaMemcpyAsync(lv_n.d, lv_b.d, need, cudaMemcpyDeviceToDevice, st));
     launch_zero_interior(lv_b.d, dl, st);
+    // spest.f fills the ghost cells of every grid whether or not it flags by gradient:
+    // errest.f steps those values
+    if (p.flag_gradient || p.flag_richardson) bound_level(lcheck, node[lgrids[lcheck][0]].time);
     if (p.flag_gradient) {
       const std::vector<int>& G = lgrids[lcheck];
-      bound_level(lcheck, node[G[0]].time);
       std::vector<long long> c0(G.size() + 1, 0);
       for (size_t k = 0; k < G.size(); ++k) c0[k + 1] = c0[k] + (long long)node[G[k]].nx() * node[G[k]].ny() * node[G[k]].nz();
       lv_c0.upload(c0, st, stg);
@@ -1569,6 +1732,7 @@ class Amr3Gpu : public AmrSolver {
       launch_flag_cells3(pool.d, d_patches.d, lv_plist.d, lv_c0.d, (int)G.size(), c0.back(), flag_pressure, sp.gamma1, p.tolsp, nvar,
                          lv_b.d, dl, st, f32);
     }
+    if (p.flag_richardson) richardson_launch(lcheck, lgrids[lcheck], lv_b.d, dl);
     std::vector<LvlBox> proj;
     if (lcheck + 2 <= p.mxnest) {
       // projec.f: level lcheck+2's new grids, with one more cell on each side when ibuff = 0
@@ -1603,6 +1767,7 @@ class Amr3Gpu : public AmrSolver {
     AMR_CUDA(cudaMemcpyAsync(lv_host + need, lv_n.d, need, cudaMemcpyDeviceToHost, st));
     tph.next("flg_sync");
     sync_stream();
+    if (p.flag_richardson) richardson_release();
     tph.next("flg_points");
     dom = LvlView{lv_host + need, dl};
     badpts.clear();
@@ -1976,6 +2141,13 @@ class Amr3Gpu : public AmrSolver {
     while (levnew <= p.mxnest) {
       const int levold = levnew - 1;
       if (lstart[levold] == 0) break;
+      // setgrd.f:41-53: Richardson estimation needs the level one step ahead before it is
+      // flagged; that step is not counted as integration work
+      if (p.flag_richardson) {
+        advanc(levold);
+        rvol = 0;
+        for (double& r : rvoll) r = 0;
+      }
       for (int i = 1; i <= p.mxnest; ++i) newstl[i] = 0;
       grdfit(levold, levold, start_time);
       if (newstl[levnew] == 0) break;
@@ -1988,7 +2160,12 @@ class Amr3Gpu : public AmrSolver {
       compile_all(levold);
       ++levnew;
     }
-    // setgrd.f:110-121 swaps store1/store2 after re-initialising store2: both hold qinit, nothing to do.
+    // setgrd.f:110-121 swaps store1/store2 after re-initialising store2. Both hold qinit
+    // (both buffers were filled), unless the Richardson steps above advanced the levels:
+    // then the swap puts the initial values back in store1, and the times are reset.
+    if (p.flag_richardson)
+      for (int lev = 1; !(lev == p.mxnest || lev > lfine); ++lev)
+        for (int m : lgrids[lev]) { node[m].cur ^= 1; node[m].time = start_time; }
     // update.f runs before prepf/prepc, so no coarse patch has a register list yet (averaging only).
     make_lists();
     compile_all(0);

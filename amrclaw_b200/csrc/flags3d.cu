@@ -308,4 +308,74 @@ void launch_colate3(int8_t* f, const int8_t* dom, LvlDims d, cudaStream_t s) {
   AMR_CUDA(cudaGetLastError());
 }
 
+// ======================================================================= Richardson estimation
+namespace {
+template <class T>
+__global__ void coarsen3_kernel(T* pool, const Rect3* rects, const int* rect_of, const PatchDev* vp, int nvar) {
+  const int k = blockIdx.y;
+  const PatchDev P = vp[k];
+  const Rect3 R = rects[rect_of[k]];
+  const T* src = pool + R.off;
+  T* dst = pool + P.q[0];
+  const long long sj = R.ni, sk = (long long)R.ni * R.nj, splane = sk * R.nk;
+  const long long n = (long long)P.mitot * P.mjtot * P.mktot;
+  GRID_STRIDE(t, n * nvar) {
+    const int m = (int)(t / n);
+    const long long rem = t % n;
+    const int i = (int)(rem % P.mitot), j = (int)((rem / P.mitot) % P.mjtot), kk = (int)(rem / ((long long)P.mitot * P.mjtot));
+    const T* s0 = src + m * splane + (2 * kk) * sk + (2 * j) * sj + 2 * i;
+    const double v = (((((((double)s0[0] + (double)s0[1]) + (double)s0[sj]) + (double)s0[sj + 1]) + (double)s0[sk]) + (double)s0[sk + 1]) +
+                      (double)s0[sk + sj]) + (double)s0[sk + sj + 1];
+    dst[m * n + rem] = (T)(v / 8.0);
+  }
+}
+template <class T>
+__global__ void errf3_kernel(const T* pool, const PatchDev* vp, int np, double order, double tol, int8_t* f, LvlDims d) {
+  const int k = blockIdx.y;
+  const PatchDev C = vp[k], F = vp[np + k];
+  const int nxc = (F.ihi - F.ilo + 1) / 2, nyc = (F.jhi - F.jlo + 1) / 2, nzc = (F.khi - F.klo + 1) / 2;
+  const T* fine = pool + F.q[1];
+  const T* crse = pool + C.q[1];
+  const long long fj = F.mitot, fk = (long long)F.mitot * F.mjtot;
+  GRID_STRIDE(t, (long long)nxc * nyc * nzc) {
+    const int ic = (int)(t % nxc), jc = (int)((t / nxc) % nyc), kc = (int)(t / ((long long)nxc * nyc));
+    const T* f0 = fine + (2 * kc + NGF) * fk + (2 * jc + NGF) * fj + (2 * ic + NGF);
+    // errf1.f: term1..term8 in the reference's order
+    const double aval = ((((((((double)f0[0] + (double)f0[1]) + (double)f0[fj + 1]) + (double)f0[fj]) + (double)f0[fk]) + (double)f0[fk + 1]) +
+                         (double)f0[fk + fj + 1]) + (double)f0[fk + fj]) / 8.0;
+    const double c = (double)crse[((long long)(kc + NGF) * C.mjtot + (jc + NGF)) * C.mitot + (ic + NGF)];
+    const double est = fabs((aval - c) / order);
+    if (est >= tol) {
+      const int gi = F.ilo + 2 * ic + 1, gj = F.jlo + 2 * jc + 1, gk = F.klo + 2 * kc + 1;  // array index = global + 1
+      for (int dk = 0; dk <= 1; ++dk)
+        for (int dj = 0; dj <= 1; ++dj)
+          for (int di = 0; di <= 1; ++di) {
+            int8_t& a = f[d.at(gi + di, gj + dj, gk + dk)];
+            a = (int8_t)(a + 2);
+          }
+    }
+  }
+}
+}  // namespace
+
+void launch_coarsen3(void* pool, const Rect3* rects, const int* rect_of, const PatchDev* vp, int np, int nvar, cudaStream_t s,
+                     bool f32) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    if (f32) coarsen3_kernel<<<dim3(16, n), 256, 0, s>>>(static_cast<float*>(pool), rects, rect_of + base, vp + base, nvar);
+    else coarsen3_kernel<<<dim3(16, n), 256, 0, s>>>(static_cast<double*>(pool), rects, rect_of + base, vp + base, nvar);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+void launch_errf3(const void* pool, const PatchDev* vp, int np, double order, double tol, int8_t* f, LvlDims d, cudaStream_t s,
+                  bool f32) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    // the partners of vp[base..] are np entries further on, from the shifted pointer too
+    if (f32) errf3_kernel<<<dim3(8, n), 256, 0, s>>>(static_cast<const float*>(pool), vp + base, np, order, tol, f, d);
+    else errf3_kernel<<<dim3(8, n), 256, 0, s>>>(static_cast<const double*>(pool), vp + base, np, order, tol, f, d);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
 }  // namespace amrb

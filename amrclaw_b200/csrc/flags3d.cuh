@@ -4,6 +4,7 @@
 // cell on every side as in the reference's integer*1 arrays.
 #pragma once
 #include "common.cuh"
+#include "kernels3d.cuh"
 
 namespace amrb {
 
@@ -35,5 +36,18 @@ void launch_flag_cells3(const void* pool, const PatchDev* patches, const int* pl
 void launch_bufnst3(int8_t* f, LvlDims d, const LvlBox* proj, int nproj, int ibuff, int8_t* t1, int8_t* t2, cudaStream_t s);
 // colate.f:4-78: f = min(f, dom) over the interior.
 void launch_colate3(int8_t* f, const int8_t* dom, LvlDims d, cudaStream_t s);
+
+// Richardson estimation (errest.f, coarsen.f, errf1.f). vp[0..np): virtual patches of the
+// coarsened grids, vp[np..2np): those of the regular step (same index boxes as the grids).
+// coarsen.f:1-25: the 2x2x2 means of scratch rect rect_of[k] (twice the ghost width) into
+// the first buffer of vp[k], ghost cells included; FP64 sums.
+void launch_coarsen3(void* pool, const Rect3* rects, const int* rect_of, const PatchDev* vp, int np, int nvar, cudaStream_t s,
+                     bool f32);
+// errf1.f:55-116 + setflags.f: for every 2x2x2 block of interior cells of grid k, the mean
+// of component 1 after the regular step (second buffer of vp[np+k]) against the coarse
+// cell after the big step (second buffer of vp[k]); where |difference / order| >= tol,
+// BADPT is added to the block's eight cells of the level array f.
+void launch_errf3(const void* pool, const PatchDev* vp, int np, double order, double tol, int8_t* f, LvlDims d, cudaStream_t s,
+                  bool f32);
 
 }  // namespace amrb

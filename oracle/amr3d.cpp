@@ -188,7 +188,10 @@ struct Amr3 {
     }
     if (naux > 0) for (int k = 0; k < naux; ++k) auxtype.push_back(a.s("aux_type", k));
     flag_richardson = a.b("flag_richardson"); tol = a.d("flag_richardson_tol");
-    if (flag_richardson) throw std::runtime_error("Richardson error estimation is not supported");
+    if (flag_richardson && naux > 0) throw std::runtime_error("Richardson estimation needs num_aux = 0 (no auxcoarsen)");
+    // bufnst.f:21-24 adds store2's first component to the flags whenever tol > 0: without
+    // errest.f having written flags there, that would be the old solution
+    if (!flag_richardson && tol > 0) throw std::runtime_error("flag_richardson_tol > 0 needs flag_richardson");
     flag_gradient = a.b("flag2refine"); tolsp = a.d("flag2refine_tol");
     kcheck = a.i("regrid_interval"); ibuff = a.i("regrid_buffer_width");
     cut = a.d("clustering_cutoff");
@@ -928,9 +931,9 @@ struct Amr3 {
   }
 
   // bound.f:4-211
-  void bound(double t, double* valbig, int mitot, int mjtot, int mktot, int mptr) {
+  void bound(double t, double* valbig, int mitot, int mjtot, int mktot, int mptr, int ng = -1) {
     const Node3& g = node[mptr];
-    const int ng = nghost;
+    if (ng < 0) ng = nghost;
     const int lev = g.level;
     const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
     filrecur(lev, valbig, mitot, mjtot, mktot, t, 1, 1, ng + 1, g.ilo - ng, g.ilo - 1, g.jlo - ng, g.jhi + ng, g.klo, g.khi, false, mptr);
@@ -1869,18 +1872,9 @@ struct Amr3 {
     const int isize = iregsz[lcheck], jsize = jregsz[lcheck], ksize = kregsz[lcheck];
     for (int mptr = lstart[lcheck]; mptr != 0; mptr = node[mptr].levelptr) {
       Node3& g = node[mptr];
-      if (tol > 0) {
-        // setflags(iflags, ..., store2, nvar, ...): adds q(1) of store2 over the interior
-        const int mitot = mitot_of(mptr), mjtot = mjtot_of(mptr), mktot = mktot_of(mptr);
-        const int ibeg = g.ilo - nghost, jbeg = g.jlo - nghost, kbeg = g.klo - nghost;
-        for (int k = nghost + 1; k <= mktot - nghost; ++k)
-          for (int j = nghost + 1; j <= mjtot - nghost; ++j)
-            for (int i = nghost + 1; i <= mitot - nghost; ++i) {
-              signed char& c = f(ibeg + i, jbeg + j, kbeg + k);
-              const double q2v = g.q2.empty() ? 0.0 : g.q2[(size_t)nvar * ((size_t)(i - 1) + (size_t)mitot * ((j - 1) + (size_t)mjtot * (k - 1)))];
-              c = (signed char)(int)((double)c + q2v);
-            }
-      }
+      // bufnst.f:21-24 (tol > 0): setflags adds component 1 of store2, where errf1.f left
+      // goodpt/badpt; errest() above adds those flags itself (a tolerance without
+      // flag_richardson is refused at input)
       g.tmp.clear();
       g.tmp.shrink_to_fit();
     }
@@ -1938,6 +1932,92 @@ struct Amr3 {
   }
 
   // flglvl.f:4-85: returns the flagged points and the nesting domain (i1flags) of level lcheck
+  // errest.f:4-141 for the grids of level lcheck: per grid, the old interior (copysol.f) in
+  // an array with twice the ghost width, filled by bound at t-dt and coarsened by 2
+  // (coarsen.f), stepped by 2*dt at 2*h; the spest copy (tmp) stepped by dt; errf1.f:1-120
+  // flags the 2x2x2 blocks whose estimate of component 1 reaches tol (allowflag.f: true),
+  // and bufnst.f:21-24 (setflags.f) adds them to the level flags when tol > 0
+  void errest(int lcheck, I1& flags) {
+    const std::vector<int> G(levelgrids[lcheck]);
+    const double hx = hxposs[lcheck], hy = hyposs[lcheck], hz = hzposs[lcheck];
+    const double hx2 = 2.0 * hx, hy2 = 2.0 * hy, hz2 = 2.0 * hz;
+    const double dt = possk[lcheck], dt2 = 2.0 * dt;  // `2. * dt`: the REAL literal 2. is exact
+    const int ng2 = 2 * nghost;
+    std::vector<std::vector<double>> bgc(G.size());
+    // first loop of errest.f: every grid's coarsened big-step input before any step
+    for (size_t n = 0; n < G.size(); ++n) {
+      const int mptr = G[n];
+      const Node3& g = node[mptr];
+      const int nx = g.ihi - g.ilo + 1, ny = g.jhi - g.jlo + 1, nz = g.khi - g.klo + 1;
+      const int mitot = nx + 2 * nghost, mjtot = ny + 2 * nghost, mktot = nz + 2 * nghost;
+      const int mi2 = nx / 2 + 2 * nghost, mj2 = ny / 2 + 2 * nghost, mk2 = nz / 2 + 2 * nghost;
+      const int midub = nx + 4 * nghost, mjdub = ny + 4 * nghost, mkdub = nz + 4 * nghost;
+      const double tpre = g.time - dt;
+      std::vector<double> dub((size_t)nvar * midub * mjdub * mkdub, 0.0);
+      FArr3 V{dub.data(), nvar, midub, mjdub, mkdub};
+      const FArr3 Q2{const_cast<double*>(g.q2.data()), nvar, mitot, mjtot, mktot};
+      for (int k = nghost + 1; k <= mktot - nghost; ++k)
+        for (int j = nghost + 1; j <= mjtot - nghost; ++j)
+          for (int i = nghost + 1; i <= mitot - nghost; ++i)
+            for (int m = 1; m <= nvar; ++m) V(m, i - nghost + ng2, j - nghost + ng2, k - nghost + ng2) = Q2(m, i, j, k);
+      bound(tpre, dub.data(), midub, mjdub, mkdub, mptr, ng2);
+      bgc[n].assign((size_t)nvar * mi2 * mj2 * mk2, 0.0);
+      FArr3 C{bgc[n].data(), nvar, mi2, mj2, mk2};
+      for (int m = 1; m <= nvar; ++m)
+        for (int k = 1; k <= mk2; ++k) {
+          const int kf = 2 * (k - 1) + 1;
+          for (int j = 1; j <= mj2; ++j) {
+            const int jf = 2 * (j - 1) + 1;
+            for (int i = 1; i <= mi2; ++i) {
+              const int iff = 2 * (i - 1) + 1;
+              C(m, i, j, k) = (((((((V(m, iff, jf, kf) + V(m, iff + 1, jf, kf)) + V(m, iff, jf + 1, kf)) + V(m, iff + 1, jf + 1, kf)) +
+                                  V(m, iff, jf, kf + 1)) + V(m, iff + 1, jf, kf + 1)) + V(m, iff, jf + 1, kf + 1)) + V(m, iff + 1, jf + 1, kf + 1)) / 8.0;
+            }
+          }
+        }
+    }
+    const double order = (double)((1 << (method[2] + 1)) - 2);
+    for (size_t n = 0; n < G.size(); ++n) {
+      const int mptr = G[n];
+      Node3& g = node[mptr];
+      const int nx = g.ihi - g.ilo + 1, ny = g.jhi - g.jlo + 1, nz = g.khi - g.klo + 1;
+      const int mitot = nx + 2 * nghost, mjtot = ny + 2 * nghost, mktot = nz + 2 * nghost;
+      const int mi2 = nx / 2 + 2 * nghost, mj2 = ny / 2 + 2 * nghost, mk2 = nz / 2 + 2 * nghost;
+      double dtnew, cflg;
+      {
+        const size_t nf = (size_t)nvar * mi2 * mj2 * mk2;
+        std::vector<double> fm(nf), fp(nf), gm(nf), gp(nf), hm(nf), hp(nf);
+        stepgrid(bgc[n].data(), fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mi2, mj2, mk2, dt2, dtnew, hx2, hy2, hz2,
+                 nullptr, cflg);
+      }
+      std::vector<double> big = g.tmp;
+      {
+        const size_t nf = (size_t)nvar * mitot * mjtot * mktot;
+        std::vector<double> fm(nf), fp(nf), gm(nf), gp(nf), hm(nf), hp(nf);
+        stepgrid(big.data(), fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mitot, mjtot, mktot, dt, dtnew, hx, hy, hz,
+                 nullptr, cflg);
+      }
+      if (!(tol > 0)) continue;
+      const FArr3 F{big.data(), nvar, mitot, mjtot, mktot};
+      const FArr3 C{bgc[n].data(), nvar, mi2, mj2, mk2};
+      for (int k = nghost + 1, kf = nghost + 1; k <= mk2 - nghost; ++k, kf += 2)
+        for (int j = nghost + 1, jf = nghost + 1; j <= mj2 - nghost; ++j, jf += 2)
+          for (int i = nghost + 1, iff = nghost + 1; i <= mi2 - nghost; ++i, iff += 2) {
+            const double aval = (((((((F(1, iff, jf, kf) + F(1, iff + 1, jf, kf)) + F(1, iff + 1, jf + 1, kf)) + F(1, iff, jf + 1, kf)) +
+                                    F(1, iff, jf, kf + 1)) + F(1, iff + 1, jf, kf + 1)) + F(1, iff + 1, jf + 1, kf + 1)) + F(1, iff, jf + 1, kf + 1)) / 8.0;
+            const double est = std::fabs((aval - C(1, i, j, k)) / order);
+            if (!(est >= tol)) continue;
+            // setflags.f: iflags(ibeg+i, ...) with ibeg = ilo - nghost
+            for (int dk = 0; dk <= 1; ++dk)
+              for (int dj = 0; dj <= 1; ++dj)
+                for (int di = 0; di <= 1; ++di) {
+                  signed char& f = flags(g.ilo - nghost + iff + di, g.jlo - nghost + jf + dj, g.klo - nghost + kf + dk);
+                  f = (signed char)(f + (signed char)BADPT);
+                }
+          }
+    }
+  }
+
   void flglvl(int lcheck, int lbase, std::vector<double>& badpts, I1& i1flags) {
     int idim = iregsz[lbase], jdim = jregsz[lbase], kdim = kregsz[lbase];
     I1 dom1;
@@ -1950,6 +2030,7 @@ struct Amr3 {
     }
     domcopy(i1flags, dom1, iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]);
     spest(lcheck, dom1);
+    if (flag_richardson) errest(lcheck, dom1);
     const int numbad = bufnst(lcheck, dom1);
     badpts.clear();
     if (numbad > 0) colate(badpts, lcheck, dom1, i1flags);
@@ -2309,6 +2390,14 @@ struct Amr3 {
       if (lstart[levold] == 0) break;
       const int lbase = levold;
       int lfnew = lbase;
+      // setgrd.f:41-53: Richardson estimation needs the level one step ahead before it is
+      // flagged; that step is not counted as integration work
+      if (flag_richardson) {
+        double dtlev;
+        advanc(levold, dtlev);
+        rvol = 0;
+        for (double& r : rvoll) r = 0;
+      }
       for (int i = 1; i <= mxnest; ++i) newstl[i] = 0;
       grdfit(lbase, levold, start_time);
       if (newstl[levnew] != 0) lfnew = levnew;
