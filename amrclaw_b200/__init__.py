@@ -33,7 +33,7 @@ class Solver:
     """One AMR run on the GPU (the reference's ``amr2`` program from init to tfinal)."""
 
     def __init__(self, rundata_or_dir, outdir: str | None = None, write_output: bool = False, batched: bool = True,
-                 precision: str = "fp64", graphs: bool = False, schedule: int = 0):
+                 precision: str = "fp64", graphs: bool = False, schedule: int | None = None):
         self._lib = _lib.load()
         if isinstance(rundata_or_dir, ClawRunData):
             self._tmp = tempfile.TemporaryDirectory(prefix="amrgpu_")
@@ -54,7 +54,7 @@ class Solver:
                "amrgpu_init")
         self._h = h
         self.set_batched(batched)
-        if schedule:
+        if schedule is not None:
             self.set_schedule(schedule)
         if graphs:
             self.set_graphs(True)
@@ -72,7 +72,8 @@ class Solver:
         _check(self._lib, self._lib.amrgpu_checkpoint(self._h, path.encode() if path else None), "amrgpu_checkpoint")
 
     def set_schedule(self, schedule: int) -> None:
-        """Sweep schedule of the batched 3D path: 0 autotune, 1 per direction, 2 work queue."""
+        """Sweep schedule of the batched 3D path: 1 per direction (the default), 2 work queue,
+        0 autotune per level. 2D runs accept only 0 (they have a single schedule)."""
         _check(self._lib, self._lib.amrgpu_set_schedule(self._h, int(schedule)), "amrgpu_set_schedule")
 
     def set_profile(self, on: bool) -> None:

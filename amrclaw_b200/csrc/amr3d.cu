@@ -1287,12 +1287,14 @@ class Amr3Gpu : public AmrSolver {
   bool use_graphs = false;
   int tune_pending = -1;  // the schedule timed in the substep in flight
   // Sweep schedule of the batched path: per-direction launches (one block per tile) or
-  // one persistent work-queue launch over the tiles of all three directions. schedule 0
-  // autotunes per level: the level's first substeps alternate the two (step kernels timed
-  // with events, per cell-update) until each has TUNE_RUNS samples, then the faster one is
-  // kept. 1 and 2 force one schedule. Results are identical under either.
+  // one persistent work-queue launch over the tiles of all three directions. 1 (the
+  // default) and 2 force one schedule. 0 autotunes per level: the level's first substeps
+  // alternate the two (step kernels timed with events, per cell-update) until each has
+  // TUNE_RUNS samples, then the faster one is kept. On the 3D workloads measured the tuner
+  // always kept per-direction launches, and its trial substeps of the queue cost time, so
+  // it is not the default. Results are identical under every schedule.
   static constexpr int TUNE_RUNS = 2;
-  int schedule = 0;
+  int schedule = 1;
   struct Tune { int runs[2] = {0, 0}; double ns_per_cell[2] = {0, 0}; int choice = -1; };
   Tune tune[12];
   unsigned int* d_queue = nullptr;

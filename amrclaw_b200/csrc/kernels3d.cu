@@ -466,6 +466,7 @@ template <int NV>
 __device__ __forceinline__ int hidx(int s, int d, int m) { return 8 * NV + ((s - 1) * 3 + (d + 1)) * NV + m; }
 
 // ------------------------------------------------------------------- faces
+constexpr int FB_I = 8, FB_J = 4, FB_K = 4;  // face bricks: one warp per k-plane, a block per brick
 template <class T, int NV>
 __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
   // face cells [face0[0], face0[np]): the level's, or one patch's through a one-patch view
@@ -476,15 +477,34 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
     const int pi = find_patch(A.face0, A.np, t);
     const PatchDev& P = A.patches[A.plist[pi]];
     const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+    // Thread t takes the face cells of its patch in brick order: slabs of FB_K k-planes,
+    // rows of FB_J j-lines in a slab, bricks of FB_I faces in a row (the last of each
+    // smaller), i fastest inside a brick. A warp then reads the j- and k-contiguous
+    // stashes of the y and z sweeps in whole sectors, and the warps of a block share
+    // them through L1. The sums of every face are the same; only which thread makes
+    // them changes.
+    const int NI = mx + 1, NJ = my + 1, NK = mz + 1;
     const long long loc = t - A.face0[pi];
-    const int i = (int)(loc % (mx + 1)) + 1;
-    const int j = (int)((loc / (mx + 1)) % (my + 1)) + 1;
-    const int k = (int)(loc / ((long long)(mx + 1) * (my + 1))) + 1;
+    const long long slab = (long long)NI * NJ * FB_K;
+    const int kb = (int)(loc / slab);
+    const int kcnt = min(FB_K, NK - kb * FB_K);
+    const long long r1 = loc - kb * slab;
+    const long long row = (long long)NI * FB_J * kcnt;
+    const int jb = (int)(r1 / row);
+    const int jcnt = min(FB_J, NJ - jb * FB_J);
+    const int r2 = (int)(r1 - jb * row);
+    const int bsz = FB_I * jcnt * kcnt;
+    const int ib = r2 / bsz;
+    const int icnt = min(FB_I, NI - ib * FB_I);
+    const int r3 = r2 - ib * bsz;
+    const int i = ib * FB_I + r3 % icnt + 1;
+    const int j = jb * FB_J + (r3 / icnt) % jcnt + 1;
+    const int k = kb * FB_K + r3 / (icnt * jcnt) + 1;
     const long long bx = A.sweep0[pi], by = A.sweep0[(A.np + 1) + pi], bz = A.sweep0[2 * (A.np + 1) + pi];
     auto xs = [&](int jj, int kk, int ii) { return bx + ((long long)(kk * (my + 2) + jj) * (mx + 1) + (ii - 1)); };
     auto ys = [&](int ii, int kk, int jj) { return by + ((long long)(kk * (mx + 2) + ii) * (my + 1) + (jj - 1)); };
     auto zs = [&](int ii, int jj, int kk) { return bz + ((long long)(jj * (mx + 2) + ii) * (mz + 1) + (kk - 1)); };
-    T* F = static_cast<T*>(A.flux) + t;
+    T* F = static_cast<T*>(A.flux) + A.face0[pi] + ((long long)(k - 1) * NJ + (j - 1)) * NI + (i - 1);
     const long long fs = A.flux_stride;
     if (j <= my && k <= mz) {  // x-face i
       T fm[NV], fp[NV];

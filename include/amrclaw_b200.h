@@ -66,10 +66,10 @@ int amrgpu_set_graphs(amrgpu_ctx* ctx, int on);
  * runs, one for 3D). */
 int amrgpu_checkpoint(amrgpu_ctx* ctx, const char* path);
 
-/* Sweep schedule of the batched 3D path. 1: one launch per sweep direction (a block per
- * tile of 128 interfaces); 2: one persistent work-queue launch in which resident blocks
- * take the tiles of all three directions from an atomic counter; 0 (default): autotune
- * per level (the level's first substeps alternate the two, timed with CUDA events per
+/* Sweep schedule of the batched 3D path. 1 (default): one launch per sweep direction (a
+ * block per tile of 128 interfaces); 2: one persistent work-queue launch in which resident
+ * blocks take the tiles of all three directions from an atomic counter; 0: autotune per
+ * level (the level's first substeps alternate the two, timed with CUDA events per
  * cell-update, and the faster is kept). Results are identical under every schedule.
  * 2D contexts accept only 0. No counterpart in the reference. */
 int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule);
