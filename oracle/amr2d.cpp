@@ -168,6 +168,8 @@ struct Amr2 {
     method[1] = vtime ? 2 : 1;
     method[2] = c.i("order"); method[3] = c.i("transverse_waves");
     dimensional_split = c.i("dimensional_split");
+    // stepgrid_dimSplit.f is not restated: refuse rather than take unsplit steps
+    if (dimensional_split != 0) throw std::runtime_error("dimensional splitting is not supported");
     method[4] = c.i("verbosity"); method[5] = c.i("source_split");
     mcapa = c.i("capa_index"); use_fwaves = c.b("use_fwaves");
     for (int k = 0; k < mwaves; ++k) mthlim.push_back(c.i("limiter", k));
