@@ -91,6 +91,10 @@ struct PhaseTimer {
 struct Arena {
   double* d = nullptr;
   long long cap = 0;
+  // the context stream when one was set at init: the arena then lives in the device's
+  // stream-ordered memory pool, and a new context reuses what an earlier one gave back
+  // instead of mapping fresh pages
+  cudaStream_t s = nullptr;
   // free blocks indexed both ways: by offset (for coalescing) and by size (best fit in
   // O(log n); a level with thousands of patches would make a first-fit scan quadratic)
   std::map<long long, long long> fr;              // offset -> length
@@ -99,7 +103,9 @@ struct Arena {
   static long long rnd(long long n) { return (n + 31) / 32 * 32; }
   void init(long long n) {
     n = rnd(std::max<long long>(n, 1 << 20));
-    AMR_CUDA(cudaMalloc(&d, sizeof(double) * n));
+    s = t_alloc_stream;
+    if (s) AMR_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * n, s));
+    else AMR_CUDA(cudaMalloc(&d, sizeof(double) * n));
     cap = n;
     fr.clear(); bysz.clear();
     add_free(0, n);
@@ -112,9 +118,16 @@ struct Arena {
     AMR_CUDA(cudaDeviceSynchronize());
     long long ncap = std::max(cap * 2, cap + rnd(need) + (1 << 20));
     double* nd = nullptr;
-    AMR_CUDA(cudaMalloc(&nd, sizeof(double) * ncap));
-    AMR_CUDA(cudaMemcpy(nd, d, sizeof(double) * cap, cudaMemcpyDeviceToDevice));
-    AMR_CUDA(cudaFree(d));
+    if (s) {
+      // in the context stream's order: later work on that stream sees the moved pool
+      AMR_CUDA(cudaMallocAsync((void**)&nd, sizeof(double) * ncap, s));
+      AMR_CUDA(cudaMemcpyAsync(nd, d, sizeof(double) * cap, cudaMemcpyDeviceToDevice, s));
+      AMR_CUDA(cudaFreeAsync(d, s));
+    } else {
+      AMR_CUDA(cudaMalloc(&nd, sizeof(double) * ncap));
+      AMR_CUDA(cudaMemcpy(nd, d, sizeof(double) * cap, cudaMemcpyDeviceToDevice));
+      AMR_CUDA(cudaFree(d));
+    }
     d = nd;
     release_raw(cap, ncap - cap);
     g_arena_grow_bytes += (double)sizeof(double) * (ncap - cap);
@@ -153,7 +166,13 @@ struct Arena {
     inuse -= n;
     release_raw(off, n);
   }
-  void destroy() { if (d) cudaFree(d); d = nullptr; }
+  void destroy() {
+    if (d) {
+      if (s) { cudaFreeAsync(d, s); cudaStreamSynchronize(s); }
+      else cudaFree(d);
+    }
+    d = nullptr;
+  }
 };
 
 // Pinned host staging for host-to-device uploads: a copy from pinned memory is
