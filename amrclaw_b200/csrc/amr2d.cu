@@ -2038,6 +2038,8 @@ class Amr2Gpu {
   void init(const std::string& dir) {
     p.load(dir);
     if (p.ndim != 2) throw std::runtime_error("this solver handles 2D runs");
+    if (write_output && p.output_format != 1)
+      throw std::runtime_error("only ASCII output (output_format 1) is written: binary and NetCDF output are not supported");
     if (p.nghost != 2) throw std::runtime_error("num_ghost must be 2");
     if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
     if (p.dimsplit != 0) throw std::runtime_error("only the unsplit method is supported");

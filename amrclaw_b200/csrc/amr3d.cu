@@ -2058,6 +2058,8 @@ class Amr3Gpu : public AmrSolver {
   void init(const std::string& dir) {
     p.load(dir);
     if (p.ndim != 3) throw std::runtime_error("num_dim must be 3");
+    if (write_output && p.output_format != 1)
+      throw std::runtime_error("only ASCII output (output_format 1) is written: binary and NetCDF output are not supported");
     nvar = p.nvar;
     blast_x = p.pn("x0", 0.0); blast_y = p.pn("y0", 0.0); blast_z = p.pn("z0", 0.0);
     blast_r = p.pn("r0", 0.2); blast_pin = p.pn("pin", 5.0); blast_pout = p.pn("pout", 1.0);

@@ -76,6 +76,7 @@ struct RunParams {
   int nvar = 1, mwaves = 1, naux = 0;
   double t0 = 0;
   int output_style = 1, nout = 0, iout = 0, nstop = 999999999;
+  int output_format = 1;  // 1 ascii, 2 netcdf, 3 binary (valout.f90:108-113)
   double tfinal = 0;
   bool output_t0 = true;
   std::vector<double> tout;
@@ -116,6 +117,7 @@ struct RunParams {
     nvar = c.n("num_eqn"); mwaves = c.n("num_waves"); naux = c.n("num_aux");
     t0 = c.f("t0");
     output_style = c.n("output_style");
+    if (c.has("output_format")) output_format = c.n("output_format");
     if (output_style == 1) {
       nout = c.n("num_output_times"); tfinal = c.f("tfinal"); output_t0 = c.b("output_t0");
       for (int k = 1; k <= nout; ++k) tout.push_back(t0 + k * (tfinal - t0) / (double)nout);
