@@ -20,13 +20,17 @@ __all__ = ["ClawRunData", "Solver", "AmrError"]
 
 
 class AmrError(RuntimeError):
-    pass
+    """A failed C-ABI call; ``code`` is its status (1 AMRGPU_ERROR, 2 AMRGPU_EINVAL)."""
+
+    def __init__(self, msg: str, code: int = 1):
+        super().__init__(msg)
+        self.code = code
 
 
 def _check(lib, rc: int, what: str) -> None:
     if rc != 0:
         msg = lib.amrgpu_last_error()
-        raise AmrError("%s failed: %s" % (what, msg.decode() if msg else "error %d" % rc))
+        raise AmrError("%s failed: %s" % (what, msg.decode() if msg else "error %d" % rc), rc)
 
 
 class Solver:
@@ -75,6 +79,11 @@ class Solver:
         """Sweep schedule of the batched 3D path: 1 per direction (the default), 2 work queue,
         0 autotune per level. 2D runs accept only 0 (they have a single schedule)."""
         _check(self._lib, self._lib.amrgpu_set_schedule(self._h, int(schedule)), "amrgpu_set_schedule")
+
+    def set_solver(self, name: str, params=()) -> None:
+        """The Riemann solver plugin by name, with its problem constants (amrgpu_set_solver)."""
+        vals = (ctypes.c_double * max(1, len(params)))(*[float(x) for x in params])
+        _check(self._lib, self._lib.amrgpu_set_solver(self._h, name.encode(), vals, len(params)), "amrgpu_set_solver")
 
     def set_profile(self, on: bool) -> None:
         _check(self._lib, self._lib.amrgpu_set_profile(self._h, int(on)), "amrgpu_set_profile")

@@ -21,6 +21,7 @@
 #include "workpool.hpp"
 #include "noalloc2d.cuh"
 #include "hostutil.hpp"
+#include "valout.hpp"
 #include "solver.hpp"
 #include <algorithm>
 #include <chrono>
@@ -226,6 +227,50 @@ class Amr2Gpu {
     sp.prob = prob;
     for (int k = 0; k < MAXVAR; ++k) sp.mthlim[k] = k < (int)p.mthlim.size() ? p.mthlim[k] : 0;
     sp.order = p.order; sp.trans = p.trans; sp.use_fwaves = p.use_fwaves ? 1 : 0; sp.mcapa = p.mcapa;
+  }
+
+  // amrgpu_set_solver: rpn2/rpt2 plugin by name with its /cparam/ constants.
+  //   advection       [u, v]         (examples/advection_2d_square/setprob.f:4, /cparam/ ubar,vbar)
+  //   acoustics       [rho, bulk]    (/cparam/ rho,bulk,cc,zz of the acoustics solvers)
+  //   euler_roe_efix  [gamma] or [gamma, efix]  (examples/euler_2d_quadrants/setprob.f:7)
+  // No constants keep the current ones. The equations and waves of the run must match.
+  void set_solver(const std::string& name, const std::vector<double>& v) {
+    ProbDev q = prob;
+    auto need = [&](int me, int mw, size_t n0, size_t n1) {
+      if (p.nvar != me || p.mwaves != mw)
+        throw std::invalid_argument("Riemann solver '" + name + "' needs num_eqn = " + std::to_string(me) +
+                                    " and num_waves = " + std::to_string(mw));
+      if (!v.empty() && v.size() != n0 && v.size() != n1)
+        throw std::invalid_argument("Riemann solver '" + name + "': wrong number of constants");
+    };
+    if (name == "advection") {
+      need(1, 1, 2, 2);
+      q.solver = SOLVER_ADVECTION;
+      if (!v.empty()) { q.ubar = v[0]; q.vbar = v[1]; }
+    } else if (name == "acoustics") {
+      need(3, 2, 2, 2);
+      q.solver = SOLVER_ACOUSTICS;
+      if (!v.empty()) {
+        if (!(v[0] > 0.0) || !(v[1] > 0.0)) throw std::invalid_argument("acoustics: rho and bulk must be positive");
+        q.rho = v[0]; q.bulk = v[1];
+        q.cc = std::sqrt(q.bulk / q.rho); q.zz = q.rho * q.cc;
+      }
+    } else if (name == "euler_roe_efix") {
+      need(4, 4, 1, 2);
+      q.solver = SOLVER_EULER;
+      if (!v.empty()) {
+        if (!(v[0] > 1.0)) throw std::invalid_argument("euler_roe_efix: gamma must exceed 1");
+        q.gamma = v[0]; q.gamma1 = q.gamma - 1.0;
+        if (v.size() == 2) q.efix = v[1] != 0.0 ? 1 : 0;
+      }
+    } else {
+      throw std::invalid_argument("unknown 2D Riemann solver '" + name + "' (advection, acoustics, euler_roe_efix)");
+    }
+    if (q.solver != prob.solver)
+      throw std::invalid_argument("Riemann solver '" + name + "' does not solve this run's equations");
+    prob = q;
+    sp.prob = q;
+    for (auto& G : lgraph) G.reset();  // captured launches hold the old constants
   }
 
   // qinit of the supported problems (per-application qinit.f of the reference)
@@ -1348,7 +1393,10 @@ class Amr2Gpu {
     }
   }
   double advanc_fixed(int lev, const double* scratch) {
-    ensure(lev, NEED_BOUND | NEED_SAVEQC | NEED_STEP);
+    // compiling a plan would allocate (pool rectangles, device lists): every C-ABI exit
+    // compiles all of them (ensure_all), so a marked plan here is a broken promise
+    if (dirty[lev] & (NEED_BOUND | NEED_SAVEQC | NEED_STEP))
+      throw std::invalid_argument("amrgpu_level_advance_noalloc: the level's device programs are not compiled");
     LevelPlan& L = plan[lev];
     const bool kids = lev + 1 <= p.mxnest && lstart[lev + 1] != 0;
     if (L.bound.scratch_len > NOALLOC_SCRATCH_DOUBLES || (kids && L.saveqc.scratch_len > NOALLOC_SCRATCH_DOUBLES))
@@ -2491,28 +2539,9 @@ class Amr2Gpu {
 
 namespace amrb {
 
-// Fortran Ew.d text of a double (the e26.16 / e18.8 fields of valout.f90).
-static std::string fort_e(double v, int w, int d) {
-  std::string out;
-  if (v == 0.0) {
-    out = std::string(std::signbit(v) ? "-" : "") + "0." + std::string(d, '0') + "E+00";
-  } else {
-    char buf[64];
-    std::snprintf(buf, sizeof(buf), "%.*e", d - 1, std::fabs(v));
-    const std::string s(buf);
-    const size_t e = s.find('e');
-    std::string digits;
-    for (size_t k = 0; k < e; ++k) if (s[k] != '.') digits.push_back(s[k]);
-    const int ex = std::atoi(s.c_str() + e + 1) + 1;
-    char eb[16];
-    if (std::abs(ex) <= 99) std::snprintf(eb, sizeof(eb), "E%c%02d", ex < 0 ? '-' : '+', std::abs(ex));
-    else std::snprintf(eb, sizeof(eb), "%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
-    out = std::string(std::signbit(v) ? "-" : "") + "0." + digits + eb;
-  }
-  if ((int)out.size() < w) out = std::string(w - out.size(), ' ') + out;
-  return out;
-}
-
+// valout.f90:8-397 (ASCII): |q| < 1e-90 becomes 0 in place on the interior cells, with or
+// without files; fort.qNNNN holds per grid (output order) its header and then j-rows of
+// i-cells, one line of meqn e26.16 values per cell and a blank line after every row.
 void Amr2Gpu::output(double t) {
   for (int lev = 1; lev <= lfine; ++lev) {
     ensure(lev, NEED_STEP);
@@ -2521,20 +2550,16 @@ void Amr2Gpu::output(double t) {
   }
   if (write_output) {
     const std::vector<double> v = gather_values();
-    char fn[64];
-    std::snprintf(fn, sizeof(fn), "/fort.q%04d", frame);
-    FILE* f = std::fopen((outdir + fn).c_str(), "w");
-    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+    FILE* f = open_output(outdir, "fort.q", frame);
     size_t pos = 0;
     int ngrids = 0;
     for (int lev = 1; lev <= lfine; ++lev)
       for (int m : lgrids[lev]) {
         const HPatch& g = node[m];
         ++ngrids;
-        std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n",
-                     m, lev, g.nx(), g.ny());
-        std::fprintf(f, "%s    xlow\n%s    ylow\n%s    dx\n%s    dy\n\n", fort_e(g.xlo, 26, 16).c_str(), fort_e(g.ylo, 26, 16).c_str(),
-                     fort_e(hxposs[lev], 26, 16).c_str(), fort_e(hyposs[lev], 26, 16).c_str());
+        const int n2[2] = {g.nx(), g.ny()};
+        const double lo[2] = {g.xlo, g.ylo}, h[2] = {hxposs[lev], hyposs[lev]};
+        write_grid_header(f, 2, m, lev, n2, lo, h);
         const size_t cells = (size_t)g.nx() * g.ny();
         for (int j = 0; j < g.ny(); ++j) {
           for (int i = 0; i < g.nx(); ++i) {
@@ -2545,13 +2570,8 @@ void Amr2Gpu::output(double t) {
         }
         pos += cells * nvar;
       }
-    std::fclose(f);
-    std::snprintf(fn, sizeof(fn), "/fort.t%04d", frame);
-    f = std::fopen((outdir + fn).c_str(), "w");
-    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
-    std::fprintf(f, "%s    time\n%6d                 meqn\n%6d                 ngrids\n%6d                 naux\n%6d                 ndim\n%6d                 nghost\n\n",
-                 fort_e(t, 18, 8).c_str(), nvar, ngrids, 0, 2, ng);
-    std::fclose(f);
+    if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.q in " + outdir);
+    write_fort_t(outdir, frame, t, nvar, ngrids, p.naux, 2, ng);
   }
   ++frame;
 }
@@ -2579,6 +2599,7 @@ class Solver2 : public AmrSolver {
     if (s != 0) throw std::runtime_error("amrgpu_set_schedule: sweep schedules are built for the 3D path");
   }
   void write_checkpoint(const char* path) override { g.checkpoint_file(path); }
+  void set_solver(const std::string& name, const std::vector<double>& v) override { g.set_solver(name, v); }
   void run(int max_cycles) override {
     g.max_cycles = max_cycles;
     g.tick();
@@ -2646,6 +2667,7 @@ struct amrgpu_ctx {
   std::unique_ptr<amrb::AmrSolver> s;
   amrb::Amr2Gpu* s2 = nullptr;  // the 2D solver, for the 2D-only entry points
   int nvar = 0;
+  int device = -1;  // the CUDA device current when the context was created
 };
 
 static thread_local std::string g_err;
@@ -2687,6 +2709,7 @@ int amrgpu_init_precision(const char* rundir, const char* outdir, int write_outp
     const int nd = c.n("num_dim");
     std::unique_ptr<amrgpu_ctx> ctx(new amrgpu_ctx());
     ctx->nvar = c.n("num_eqn");
+    AMR_CUDA(cudaGetDevice(&ctx->device));
     if (nd == 2) {
       auto* s2 = new amrb::Solver2();
       ctx->s.reset(s2);
@@ -2731,6 +2754,20 @@ int amrgpu_set_profile(amrgpu_ctx* ctx, int on) {
   return AMRGPU_OK;
 }
 
+int amrgpu_set_solver(amrgpu_ctx* ctx, const char* name, const double* params, int n) {
+  if (!ctx || !name || n < 0 || (n > 0 && !params)) { g_err = "amrgpu_set_solver: bad argument"; return AMRGPU_EINVAL; }
+  try {
+    ctx->s->set_solver(name, std::vector<double>(params, params + n));
+    return AMRGPU_OK;
+  } catch (std::invalid_argument& e) {
+    g_err = e.what();
+    return AMRGPU_EINVAL;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return AMRGPU_ERROR;
+  }
+}
+
 int amrgpu_run(amrgpu_ctx* ctx, int max_cycles) {
   if (!ctx) return AMRGPU_EINVAL;
   return guarded(ctx, [&] { ctx->s->run(max_cycles); });
@@ -2753,6 +2790,12 @@ int amrgpu_level_advance_noalloc(amrgpu_ctx* ctx, int level, double* dtnew_out, 
   try {
     amrb::Amr2Gpu& s = *ctx->s2;
     if (level < 1 || level > s.lfine) { g_err = "level out of range"; return AMRGPU_EINVAL; }
+    // the fixed array is looked up per device: the context's device must be the current one
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != ctx->device) {
+      g_err = "amrgpu_level_advance_noalloc: call with the context's device current";
+      return AMRGPU_EINVAL;
+    }
     double* scratch = nullptr;
     std::string err;
     if (amrb::fixed_scratch_address(&scratch, err) != 0) { g_err = err; return AMRGPU_ERROR; }

@@ -13,6 +13,7 @@
 // grdfit.f, birect.f, gfixup.f, filval.f) with the gradient test on the device.
 #include "kernels3d.cuh"
 #include "flags3d.cuh"
+#include "valout.hpp"
 #include "params.hpp"
 #include "gridindex.hpp"
 #include "workpool.hpp"
@@ -2465,74 +2466,99 @@ class Amr3Gpu : public AmrSolver {
     sync_stream();
     return m * hxposs[1] * hyposs[1] * hzposs[1];
   }
-  std::vector<double> gather_values() {
+  // interior values of every grid in output order, [m][k][j][i] per grid: the solution, or
+  // with aux set the aux arrays (naux components)
+  std::vector<double> gather_values(bool aux = false) {
+    const int nc = aux ? p.naux : nvar;
     std::vector<int> pl;
     std::vector<long long> c0(1, 0);
     for (int lev = 1; lev <= lfine; ++lev)
       for (int m : lgrids[lev]) { pl.push_back(m); c0.push_back(c0.back() + (long long)node[m].nx() * node[m].ny() * node[m].nz()); }
-    std::vector<double> out((size_t)c0.back() * nvar);
+    std::vector<double> out((size_t)c0.back() * nc);
     if (out.empty()) return out;
     DBuf<int> dp; dp.upload(pl, st, stg);
     DBuf<long long> dc; dc.upload(c0, st, stg);
     DBuf<double> dout; dout.ensure(out.size());
-    launch_gather3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nvar, c0.back(), dout.d, st, f32);
+    launch_gather3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nc, c0.back(), dout.d, st, f32, aux);
     AMR_CUDA(cudaMemcpyAsync(out.data(), dout.d, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
     sync_stream();
     dp.free(); dc.free(); dout.free();
     return out;
   }
-  void output(double t) {
-    for (int lev = 1; lev <= lfine; ++lev) {
-      ensure(lev, NEED_STEP);
-      launch_zero_tiny3(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
-      ++nkernels;
-    }
-    if (!write_output) { ++frame; return; }
-    const std::vector<double> v = gather_values();
-    char fn[64];
-    std::snprintf(fn, sizeof(fn), "/fort.q%04d", frame);
-    FILE* f = std::fopen((outdir + fn).c_str(), "w");
-    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+  // the rows of fort.q / fort.a (src/3d/valout.f90:140-160): per grid in output order, its
+  // header, then k-planes of j-rows of i-cells, one line of nc e26.16 values per cell, a
+  // blank line after every j-row, every k-plane and every grid
+  void write_frame_file(FILE* f, const std::vector<double>& v, int nc) {
     size_t off = 0;
-    int ngrids = 0;
-    auto E = [](double x, int w, int d) {
-      char b[64];
-      std::snprintf(b, sizeof(b), "%*.*E", w, d - 1, x);  // e.g. 1.0000000000000000E+00 (width w)
-      return std::string(b);
-    };
     for (int lev = 1; lev <= lfine; ++lev)
       for (int m : lgrids[lev]) {
-        ++ngrids;
         const HPatch3& g = node[m];
-        std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n%6d                 mz\n",
-                     m, lev, g.nx(), g.ny(), g.nz());
-        std::fprintf(f, "%s    xlow\n%s    ylow\n%s    zlow\n%s    dx\n%s    dy\n%s    dz\n\n", E(g.xlo, 26, 17).c_str(), E(g.ylo, 26, 17).c_str(),
-                     E(g.zlo, 26, 17).c_str(), E(hxposs[lev], 26, 17).c_str(), E(hyposs[lev], 26, 17).c_str(), E(hzposs[lev], 26, 17).c_str());
+        const int n3[3] = {g.nx(), g.ny(), g.nz()};
+        const double lo[3] = {g.xlo, g.ylo, g.zlo}, h[3] = {hxposs[lev], hyposs[lev], hzposs[lev]};
+        write_grid_header(f, 3, m, lev, n3, lo, h);
         const size_t n = (size_t)g.nx() * g.ny() * g.nz();
         for (int k = 0; k < g.nz(); ++k) {
           for (int j = 0; j < g.ny(); ++j) {
             for (int i = 0; i < g.nx(); ++i) {
-              for (int iv = 0; iv < nvar; ++iv) {
-                double x = v[off + iv * n + ((size_t)k * g.ny() + j) * g.nx() + i];
-                if (std::fabs(x) < 1e-90) x = 0.0;
-                std::fputs(E(x, 26, 17).c_str(), f);
-              }
+              for (int iv = 0; iv < nc; ++iv) std::fputs(fort_e(v[off + iv * n + ((size_t)k * g.ny() + j) * g.nx() + i], 26, 16).c_str(), f);
               std::fputc('\n', f);
             }
             std::fputs("  \n", f);
           }
           std::fputs("  \n", f);
         }
-        off += n * nvar;
+        std::fputs("  \n", f);
+        off += n * nc;
       }
-    std::fclose(f);
-    std::snprintf(fn, sizeof(fn), "/fort.t%04d", frame);
-    f = std::fopen((outdir + fn).c_str(), "w");
-    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
-    std::fprintf(f, "%s    time\n%6d                 meqn\n%6d                 ngrids\n%6d                 naux\n%6d                 ndim\n%6d                 nghost\n\n",
-                 E(t, 18, 9).c_str(), nvar, ngrids, 0, 3, G3);
-    std::fclose(f);
+  }
+  // valout.f90: |q| < 1e-90 (and |aux| < 1e-90 when aux is written) become 0 in place on the
+  // interior cells, with or without files
+  void output(double t) {
+    const bool aux = p.out_aux(t);
+    for (int lev = 1; lev <= lfine; ++lev) {
+      ensure(lev, NEED_STEP);
+      launch_zero_tiny3(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
+      ++nkernels;
+      if (aux) {
+        launch_zero_tiny3(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), p.naux, st, f32, true);
+        ++nkernels;
+      }
+    }
+    if (!write_output) { ++frame; return; }
+    int ngrids = 0;
+    for (int lev = 1; lev <= lfine; ++lev) ngrids += (int)lgrids[lev].size();
+    FILE* f = open_output(outdir, "fort.q", frame);
+    write_frame_file(f, gather_values(), nvar);
+    if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.q in " + outdir);
+    if (aux) {
+      f = open_output(outdir, "fort.a", frame);
+      write_frame_file(f, gather_values(true), p.naux);
+      if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.a in " + outdir);
+    }
+    write_fort_t(outdir, frame, t, nvar, ngrids, p.naux, 3, G3);
     ++frame;
+  }
+
+  // amrgpu_set_solver: rpn3/rpt3/rptt3 plugin by name with its /cparam/ constants.
+  //   euler_roe_efix  [gamma] or [gamma, efix]  (/cparam/ gamma,gamma1 of the 3D Euler examples)
+  //   vc_advection    []  (face velocities come from aux 1..3; examples/advection_3d_swirl)
+  // No constants keep the current ones. The run's equations and aux must match.
+  void set_solver(const std::string& name, const std::vector<double>& v) override {
+    if (name == "euler_roe_efix") {
+      if (sp.solver != SOLVER3_EULER) throw std::invalid_argument("euler_roe_efix does not solve this run's equations");
+      if (!v.empty() && v.size() != 1 && v.size() != 2) throw std::invalid_argument("euler_roe_efix: wrong number of constants");
+      if (!v.empty()) {
+        if (!(v[0] > 1.0)) throw std::invalid_argument("euler_roe_efix: gamma must exceed 1");
+        sp.gamma = v[0]; sp.gamma1 = sp.gamma - 1.0;
+        if (v.size() == 2) sp.efix = v[1] != 0.0 ? 1 : 0;
+      }
+    } else if (name == "vc_advection") {
+      if (sp.solver != SOLVER3_SWIRL) throw std::invalid_argument("vc_advection does not solve this run's equations");
+      if (!v.empty()) throw std::invalid_argument("vc_advection takes no constants (velocities are aux arrays)");
+    } else {
+      throw std::invalid_argument("unknown 3D Riemann solver '" + name + "' (euler_roe_efix, vc_advection)");
+    }
+    for (auto& G : lgraph) G.reset();  // captured launches hold the old constants
   }
 
   // ================================================================ AmrSolver

@@ -153,6 +153,11 @@ struct Swirl3Phys {
   }
 };
 
+// the registered 3D plugins satisfy the device plugin contract (include/amrgpu_riemann.cuh)
+static_assert(amrgpu_plugin::Check3D<Euler3Phys<double>, Step3Params, double>::value, "euler_roe_efix: rpn3/rpt3/rptt3 contract");
+static_assert(amrgpu_plugin::Check3D<Swirl3Phys<double>, Step3Params, double>::value, "vc_advection: rpn3/rpt3/rptt3 contract");
+static_assert(amrgpu_plugin::Check3D<Euler3Phys<float>, Step3Params, float>::value, "euler_roe_efix (FP32): contract");
+
 // one tile of sweep direction DIR. sW: the block's shared buffer, first the waves
 // [NW*NV][SW_T], then (after they are read) the transverse terms [12*NV][SW_T] of the
 // tile's cells: the apdq side writes them, the amdq side of the next interface adds to
@@ -1090,9 +1095,11 @@ __global__ void mass3_kernel(const T* pool, const PatchDev* patches, const int* 
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
 
+// interior values of the listed patches, [m][k][j][i] per patch: the solution (store1),
+// or with aux set the patch's aux array (nvar = naux components)
 template <class T>
 __global__ void gather3_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
-                               long long total, double* out) {
+                               long long total, double* out, bool aux) {
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int pi = find_patch(cell0, np, t);
     const PatchDev& P = patches[plist[pi]];
@@ -1101,7 +1108,7 @@ __global__ void gather3_kernel(const T* pool, const PatchDev* patches, const int
     const long long loc = t - cell0[pi];
     const int i = (int)(loc % mx), j = (int)((loc / mx) % my), k = (int)(loc / ((long long)mx * my));
     const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
-    const T* q = pool + P.q[P.cur];
+    const T* q = pool + (aux ? P.aux : P.q[P.cur]);
     const long long at = ((long long)(k + NG3) * P.mjtot + (j + NG3)) * P.mitot + (i + NG3);
     for (int m = 0; m < nvar; ++m) out[cell0[pi] * nvar + m * n + loc] = (double)q[m * plane + at];
   }
@@ -1253,13 +1260,13 @@ void launch_setaux3(void* pool, const Setaux3Job* jobs, int njobs, long long max
 
 // valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
 template <class T>
-__global__ void zero_tiny3_kernel(T* pool, const PatchDev* patches, const int* plist, int np, int nvar) {
+__global__ void zero_tiny3_kernel(T* pool, const PatchDev* patches, const int* plist, int np, int nvar, bool aux) {
   const int pi = blockIdx.y;
   if (pi >= np) return;
   const PatchDev& P = patches[plist[pi]];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
   const long long plane = (long long)P.mitot * P.mjtot * P.mktot, n = (long long)mx * my * mz;
-  T* q = pool + P.q[P.cur];
+  T* q = pool + (aux ? P.aux : P.q[P.cur]);
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n * nvar; t += (long long)gridDim.x * blockDim.x) {
     const int m = (int)(t / n);
     const long long c = t - (long long)m * n;
@@ -1268,11 +1275,12 @@ __global__ void zero_tiny3_kernel(T* pool, const PatchDev* patches, const int* p
     if (fabs((double)v) < 1e-90) v = T(0);
   }
 }
-void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32) {
+void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32,
+                       bool aux) {
   for (int base = 0; base < np; base += 65535) {
     const int cnt = std::min(65535, np - base);
-    if (f32) zero_tiny3_kernel<<<dim3(8, cnt), 256, 0, s>>>(static_cast<float*>(pool), patches, plist + base, cnt, nvar);
-    else zero_tiny3_kernel<<<dim3(8, cnt), 256, 0, s>>>(static_cast<double*>(pool), patches, plist + base, cnt, nvar);
+    if (f32) zero_tiny3_kernel<<<dim3(8, cnt), 256, 0, s>>>(static_cast<float*>(pool), patches, plist + base, cnt, nvar, aux);
+    else zero_tiny3_kernel<<<dim3(8, cnt), 256, 0, s>>>(static_cast<double*>(pool), patches, plist + base, cnt, nvar, aux);
   }
   AMR_CUDA(cudaGetLastError());
 }
@@ -1344,10 +1352,10 @@ void launch_mass3(const void* pool, const PatchDev* patches, const int* plist, i
   AMR_CUDA(cudaGetLastError());
 }
 void launch_gather3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
-                    long long total, double* out, cudaStream_t s, bool f32) {
+                    long long total, double* out, cudaStream_t s, bool f32, bool aux) {
   if (total <= 0) return;
-  if (f32) gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const float*>(pool), patches, plist, cell0, np, nvar, total, out);
-  else gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const double*>(pool), patches, plist, cell0, np, nvar, total, out);
+  if (f32) gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const float*>(pool), patches, plist, cell0, np, nvar, total, out, aux);
+  else gather3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const double*>(pool), patches, plist, cell0, np, nvar, total, out, aux);
   AMR_CUDA(cudaGetLastError());
 }
 

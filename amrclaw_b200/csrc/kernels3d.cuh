@@ -117,7 +117,8 @@ struct Setaux3Job { long long aux, f0; int mi, mj, mk, pad; };
 void launch_setaux3(void* pool, const Setaux3Job* jobs, int njobs, long long max_cells, const double* fac, int copies,
                     cudaStream_t s, bool f32);
 // valout.f90:140-147: |q| < 1e-90 of the interior cells of plist set to 0 in place
-void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32);
+void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32,
+                       bool aux = false);
 // b4step3 of the time-modulated swirl: aux = c * aux0 over the enlarged patches of plist
 // (max_cells: the largest enlarged patch)
 void launch_b4step3(void* pool, const PatchDev* patches, const int* plist, int np, int naux, long long max_cells, double c,
@@ -132,6 +133,6 @@ void launch_gauges3(const void* pool, const PatchDev* patches, const Gauge3Job* 
                     bool f32);
 void launch_mass3(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32);
 void launch_gather3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
-                    long long total, double* out, cudaStream_t s, bool f32);
+                    long long total, double* out, cudaStream_t s, bool f32, bool aux = false);
 
 }  // namespace amrb

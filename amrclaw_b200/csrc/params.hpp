@@ -77,6 +77,8 @@ struct RunParams {
   double t0 = 0;
   int output_style = 1, nout = 0, iout = 0, nstop = 999999999;
   int output_format = 1;  // 1 ascii, 2 netcdf, 3 binary (valout.f90:108-113)
+  std::vector<int> output_aux_components;  // per aux component, 1: written to fort.aNNNN (amr2.f90:212-218)
+  bool output_aux_onlyonce = true;
   double tfinal = 0;
   bool output_t0 = true;
   std::vector<double> tout;
@@ -118,6 +120,10 @@ struct RunParams {
     t0 = c.f("t0");
     output_style = c.n("output_style");
     if (c.has("output_format")) output_format = c.n("output_format");
+    if (naux > 0 && c.has("output_aux_components")) {
+      for (int k = 0; k < naux; ++k) output_aux_components.push_back(c.n("output_aux_components", k));
+      if (c.has("output_aux_onlyonce")) output_aux_onlyonce = c.b("output_aux_onlyonce");
+    }
     if (output_style == 1) {
       nout = c.n("num_output_times"); tfinal = c.f("tfinal"); output_t0 = c.b("output_t0");
       for (int k = 1; k <= nout; ++k) tout.push_back(t0 + k * (tfinal - t0) / (double)nout);
@@ -199,6 +205,13 @@ struct RunParams {
     }
     flag_component = s.n_or("flag_component", 0);
     flag_mode = s.has("flag_mode") ? s.str("flag_mode") : std::string("component");
+  }
+  // valout.f90: aux arrays go to fort.aNNNN when any component is requested, every frame or
+  // (output_aux_onlyonce) only at the initial time
+  bool out_aux(double time) const {
+    int n = 0;
+    for (int x : output_aux_components) n += x;
+    return n > 0 && (!output_aux_onlyonce || std::fabs(time - t0) < 1e-90);
   }
   double pn(const std::string& k, double d) const { auto it = probnum.find(k); return it == probnum.end() ? d : it->second; }
   std::string ps(const std::string& k, const std::string& d) const { auto it = probstr.find(k); return it == probstr.end() ? d : it->second; }

@@ -15,6 +15,7 @@
 // FMA contraction, results are bit-identical to the CPU oracle.
 #pragma once
 #include "common.cuh"
+#include "../../include/amrgpu_riemann.cuh"
 
 namespace amrb {
 
@@ -222,5 +223,11 @@ struct Euler2 {
     }
   }
 };
+
+// the registered 2D plugins satisfy the device plugin contract (include/amrgpu_riemann.cuh)
+static_assert(amrgpu_plugin::Check2D<Advection2, ProbDev, double>::value, "advection: rpn2/rpt2 contract");
+static_assert(amrgpu_plugin::Check2D<Acoustics2, ProbDev, double>::value, "acoustics: rpn2/rpt2 contract");
+static_assert(amrgpu_plugin::Check2D<Euler2, ProbDev, double>::value, "euler_roe_efix: rpn2/rpt2 contract");
+static_assert(amrgpu_plugin::Check2D<Euler2, ProbDev, float>::value, "euler_roe_efix (FP32): rpn2/rpt2 contract");
 
 }  // namespace amrb

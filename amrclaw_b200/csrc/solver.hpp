@@ -17,6 +17,11 @@ class AmrSolver {
   virtual void set_graphs(bool on) = 0;
   // sweep schedule of the batched 3D path: 0 autotune, 1 per direction, 2 work queue
   virtual void set_schedule(int s) = 0;
+  // the Riemann solver plugin by registry name and its problem constants (the reference's
+  // link-time choice of rpn2/rpt2 (rpn3/rpt3/rptt3) and setprob's /cparam/ common block);
+  // std::invalid_argument for an unknown name, a wrong number of constants or a solver
+  // whose equations and waves do not match the run
+  virtual void set_solver(const std::string& name, const std::vector<double>& params) = 0;
   virtual void run(int max_cycles) = 0;                    // tick.f
   virtual double level_advance(int level, double* cfl) = 0;  // advanc.f; returns dtnew
   virtual void update_level(int level) = 0;                 // update.f

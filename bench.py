@@ -265,6 +265,24 @@ def serving_leg(n_requests: int = 64) -> dict:
     return serve.serve(reqs, budget_bytes=16 << 30, slots=16)["summary"]
 
 
+def parity_record(state: dict, o, prec: str) -> dict:
+    """The value leg's final state against the oracle after the same coarse steps."""
+    g, v = o.grids(), o.values()
+    same_grids = g.shape == state["grids"].shape and bool(np.array_equal(g, state["grids"]))
+    rec = {"against": "oracle (FP64 CPU restatement), same workload, same coarse steps",
+           "grids": int(len(state["grids"])), "cells": int(state["values"].size),
+           "hierarchy_identical": same_grids, "time_identical": state["time"] == o.time(),
+           "cell_updates_identical": state["cells"] == o.cell_updates()}
+    if same_grids and v.shape == state["values"].shape:
+        diff = int(np.count_nonzero(v != state["values"]))
+        rec["values_differing"] = diff
+        if prec == "fp32":
+            rec["max_rel_err"] = float(np.max(np.abs(v - state["values"]) / np.maximum(np.abs(v), 1e-300)))
+    ok = same_grids and rec.get("values_differing") == 0 and rec["time_identical"] and rec["cell_updates_identical"]
+    rec["result"] = "bit-identical" if ok else ("hierarchy differs" if not same_grids else "values differ")
+    return rec
+
+
 REFERENCE_BUDGET_S = 120
 
 
@@ -307,7 +325,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="euler3d_blast")
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=0, help="oracle coarse steps timed (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -367,6 +385,8 @@ def main():
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
         i1 = s.info()
+        # the state after the timed steps, compared with the oracle over the same steps
+        value_state = dict(grids=s.grids(), values=s.values(), time=i1["time"], cells=i1["cell_updates"])
         s.close()
         batched_regrid_ms = 1e3 * (i1["regrid_seconds"] - i0["regrid_seconds"]) / args.steps
         batched_advance_ms = 1e3 * (i1["step_seconds"] - i0["step_seconds"]) / args.steps - batched_regrid_ms
@@ -477,19 +497,26 @@ def main():
                      "peak_kind": "measured here: FP64 DGEMM 4096^3, best of 5",
                      "note": "built without FMA contraction for bit-exact FP64, so dadd/dmul issue at the dfma rate"}
     cpu = None
+    parity = None
     if not args.no_cpu_baseline:
+        # the oracle over the value leg's coarse steps: untimed up to the first timed step,
+        # then timed over the same steps; its state afterwards is the parity check of the
+        # value leg (FP64: bit-identical hierarchy and cell values required)
         threads = os.cpu_count() or 1
+        cpu_steps = args.cpu_steps if args.cpu_steps > 0 else args.steps
         with tempfile.TemporaryDirectory() as d:
             rd.write(d)
             o = oracle_cls(ndim)(d, threads=threads)
             o.run(args.warmup)
             c0 = o.cell_updates()
-            sec = o.run(args.cpu_steps)
+            sec = o.run(cpu_steps)
             cpu_v = (o.cell_updates() - c0) / sec
+            if cpu_steps == args.steps:
+                parity = parity_record(value_state, o, prec)
             o.close()
         cpu = {"value": cpu_v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": "coarse steps %d..%d of the same workload on the CPU restatement (OpenMP over patches)" % (
-                   args.warmup, args.warmup + args.cpu_steps)}
+               "sample": "coarse steps %d..%d of the same workload (the value leg's timed steps) on the CPU "
+                         "restatement (OpenMP over patches)" % (args.warmup, args.warmup + cpu_steps)}
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -497,13 +524,6 @@ def main():
         "data": "synthetic: seeded initial conditions of the workload",
         "config": dict(cfg, l2="flushed between steps (256 MB write)", parallelism="replicas" if world > 1 else "single",
                        process_warmup="one untimed solve of the same %d coarse steps before the timed legs" % (args.warmup + args.steps)),
-        "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": plain_ms,
-                  "speedup_batched_over_plain": value / plain_value if plain_value else None,
-                  "advance_ms_per_step": plain_inf["advance_ms_per_step"],
-                  "regrid_ms_per_step": plain_inf["regrid_ms_per_step"],
-                  "advance_speedup_batched_over_plain": (plain_inf["advance_ms_per_step"] / batched_advance_ms
-                                                         if batched_advance_ms > 0 else None)},
-        "schedules": graph_legs or None,
         "advance_ms_per_step": batched_advance_ms, "regrid_ms_per_step": batched_regrid_ms,
         "l1_err_vs_fp64": l1_err,
         "fp32_form": fp32,
@@ -529,6 +549,15 @@ def main():
         "gpu_launches": launches,
         "level_substeps": step_launches,
         "clocks": clk,
+        "parity": parity,
+        # last, so that a reader that keeps only the tail of the line still sees them
+        "schedules": graph_legs or None,
+        "plain": {"value": plain_value, "unit": "cell-updates/s", "ms_per_step": plain_ms,
+                  "speedup_batched_over_plain": value / plain_value if plain_value else None,
+                  "advance_ms_per_step": plain_inf["advance_ms_per_step"],
+                  "regrid_ms_per_step": plain_inf["regrid_ms_per_step"],
+                  "advance_speedup_batched_over_plain": (plain_inf["advance_ms_per_step"] / batched_advance_ms
+                                                         if batched_advance_ms > 0 else None)},
     }
     print(json.dumps(line), flush=True)
     if dist:

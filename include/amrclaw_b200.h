@@ -74,6 +74,25 @@ int amrgpu_checkpoint(amrgpu_ctx* ctx, const char* path);
  * 2D contexts accept only 0. No counterpart in the reference. */
 int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule);
 
+/* Selects the Riemann solver plugin of the run by registry name and sets its problem
+ * constants (params[0..n), n = 0 keeps the current ones). Replaces the reference's
+ * plugin binding: the rpn2/rpt2 (2D) or rpn3/rpt3/rptt3 (3D) routines linked into the
+ * program and called at src/2d/flux2.f:125,202,219, src/2d/qad.f:129 and
+ * src/3d/flux3.f:220-226,302-365,411-422, with their constants in setprob's /cparam/
+ * common block (examples/advection_2d_square/setprob.f:4, examples/euler_2d_quadrants/
+ * setprob.f:7). Registered device plugins (their per-interface contract is declared in
+ * include/amrgpu_riemann.cuh):
+ *   2D  "advection"       params u, v            (num_eqn 1, num_waves 1)
+ *       "acoustics"       params rho, bulk       (num_eqn 3, num_waves 2)
+ *       "euler_roe_efix"  params gamma[, efix]   (num_eqn 4, num_waves 4)
+ *   3D  "euler_roe_efix"  params gamma[, efix]   (num_eqn 5, num_waves 3)
+ *       "vc_advection"    no params; face velocities in aux 1..3 (num_eqn 1, num_aux 3)
+ * Unknown names, a wrong count or invalid constants, and solvers whose equations do not
+ * match the run return AMRGPU_EINVAL and leave the run unchanged. The choice applies to
+ * every later substep (and, in 3D Euler, to the pressure of the flagging). The problem
+ * named in setprob.data still sets the initial data and the default solver. */
+int amrgpu_set_solver(amrgpu_ctx* ctx, const char* name, const double* params, int n);
+
 /* 1: record CUDA events around every patch-step launch (kernel time is then
  * reported by amrgpu_info); 0: no per-launch events. */
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on);
@@ -91,6 +110,8 @@ int amrgpu_level_advance(amrgpu_ctx* ctx, int level, double* dtnew_out, double* 
 
 /* amrgpu_level_advance without any device allocation. No counterpart in the
  * reference (its level advance allocates per call from the alloc heap).
+ * 2D, FP64 contexts only: 3D and FP32 contexts return AMRGPU_EINVAL, and so does a
+ * call made while another device than the context's is current.
  * The ghost-fill and saved-coarse-value programs stage their coarse scratch
  * rectangles in one file-scope device array of 4194304 doubles (32 MiB)
  * instead of the context's device pool; a level whose programs need more

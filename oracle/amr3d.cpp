@@ -83,6 +83,8 @@ struct Amr3 {
   double t0;
   int output_style = 1, nout = 0, iout = 0, nstop = IINFINITY3;
   double tfinal = 0; bool output_t0 = true;
+  std::vector<int> output_aux_components;
+  bool output_aux_onlyonce = true;
   std::vector<double> tout;
   double dt_initial, dt_max, cflv1, cfl;
   int nv1; bool vtime;
@@ -168,6 +170,11 @@ struct Amr3 {
     dimensional_split = c.i("dimensional_split");
     method[4] = c.i("verbosity"); method[5] = c.i("source_split");
     mcapa = c.i("capa_index"); use_fwaves = c.b("use_fwaves");
+    // amr2.f90:212-218 (amr3.f90 alike): aux components written to fort.aNNNN
+    if (naux > 0 && c.has("output_aux_components")) {
+      for (int k = 0; k < naux; ++k) output_aux_components.push_back(c.i("output_aux_components", k));
+      output_aux_onlyonce = c.has("output_aux_onlyonce") ? c.b("output_aux_onlyonce") : true;
+    }
     for (int k = 0; k < mwaves; ++k) mthlim.push_back(c.i("limiter", k));
     nghost = c.i("num_ghost");
     for (int d = 0; d < 3; ++d) { mthbc[2 * d + 1] = c.i("bc_lower", d); mthbc[2 * d + 2] = c.i("bc_upper", d); }
@@ -2445,7 +2452,57 @@ struct Amr3 {
   }
 
   // valout.f90 (3D ascii form); valout.f90:140-147 first zeroes |q| < 1e-90 of the interior cells in place
+  // src/3d/valout.f90:190-260: fort.aNNNN, the aux arrays in fort.q's layout (headers, then
+  // naux values per interior cell), after zeroing |aux| < 1e-90 of the interior cells in place
+  void zero_tiny_aux(int lbeg, int lend) {
+    for (int level = lbeg; level <= lend; ++level)
+      for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+        const int mitot = mitot_of(m), mjtot = mjtot_of(m), mktot = mktot_of(m);
+        for (int k = nghost + 1; k <= mktot - nghost; ++k)
+          for (int j = nghost + 1; j <= mjtot - nghost; ++j)
+            for (int i = nghost + 1; i <= mitot - nghost; ++i)
+              for (int ia = 1; ia <= naux; ++ia) {
+                double& v = node[m].aux[(size_t)(ia - 1) + (size_t)naux * ((size_t)(i - 1) + (size_t)mitot * ((j - 1) + (size_t)mjtot * (k - 1)))];
+                if (std::fabs(v) < 1e-90) v = 0.0;
+              }
+      }
+  }
+  void write_aux(int lbeg, int lend) {
+    char fn[64];
+    std::snprintf(fn, sizeof(fn), "/fort.a%04d", matlabu);
+    FILE* f = std::fopen((outdir + fn).c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+    for (int level = lbeg; level <= lend; ++level)
+      for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+        Node3& g = node[m];
+        const int mitot = mitot_of(m), mjtot = mjtot_of(m), mktot = mktot_of(m);
+        std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n%6d                 mz\n",
+                     m, level, g.ihi - g.ilo + 1, g.jhi - g.jlo + 1, g.khi - g.klo + 1);
+        std::fprintf(f, "%s    xlow\n%s    ylow\n%s    zlow\n%s    dx\n%s    dy\n%s    dz\n\n", fmtE(g.xlo, 26, 16).c_str(),
+                     fmtE(g.ylo, 26, 16).c_str(), fmtE(g.zlo, 26, 16).c_str(), fmtE(hxposs[level], 26, 16).c_str(),
+                     fmtE(hyposs[level], 26, 16).c_str(), fmtE(hzposs[level], 26, 16).c_str());
+        for (int k = nghost + 1; k <= mktot - nghost; ++k) {
+          for (int j = nghost + 1; j <= mjtot - nghost; ++j) {
+            for (int i = nghost + 1; i <= mitot - nghost; ++i) {
+              for (int ia = 1; ia <= naux; ++ia)
+                std::fputs(fmtE(g.aux[(size_t)(ia - 1) + (size_t)naux * ((size_t)(i - 1) + (size_t)mitot * ((j - 1) + (size_t)mjtot * (k - 1)))], 26, 16).c_str(), f);
+              std::fputc('\n', f);
+            }
+            std::fputs("  \n", f);
+          }
+          std::fputs("  \n", f);
+        }
+        std::fputs("  \n", f);
+      }
+    std::fclose(f);
+  }
+
   void valout(int lbeg, int lend, double t) {
+    // valout.f90: aux output when any component is requested, every frame or only at t0
+    int naux_out = 0;
+    for (int x : output_aux_components) naux_out += x;
+    const bool out_aux = naux_out > 0 && (!output_aux_onlyonce || std::fabs(t - t0) < 1e-90);
+    if (out_aux) zero_tiny_aux(lbeg, lend);
     for (int level = lbeg; level <= lend; ++level)
       for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
         const int mitot = mitot_of(m), mjtot = mjtot_of(m), mktot = mktot_of(m);
@@ -2483,8 +2540,10 @@ struct Amr3 {
             }
             std::fputs("  \n", f);
           }
+          std::fputs("  \n", f);  // src/3d/valout.f90:159
         }
       std::fclose(f);
+      if (out_aux) write_aux(lbeg, lend);
       std::snprintf(fn, sizeof(fn), "/fort.t%04d", matlabu);
       f = std::fopen((outdir + fn).c_str(), "w");
       std::fprintf(f, "%s    time\n%6d                 meqn\n%6d                 ngrids\n%6d                 naux\n%6d                 ndim\n%6d                 nghost\n\n",

@@ -2,15 +2,19 @@
 
 Reads tests/<case>/regression_data/gauge*.txt of the reference checkout
 (gauge rows "level time q(1..meqn)", printed e15.7) and writes one compact
-fixture per case here: rows "gauge_id level time q...". Run from the repository
-root with the reference mounted at /root/reference; the fixtures are committed so
-the tests never read the reference at run time.
+fixture per case here: rows "gauge_id level time q...". Usage:
+
+    python tests/golden/make_golden.py <path of the reference checkout>
+
+The fixtures are committed so the tests never read the reference at run time.
 """
 import glob
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <path of the reference checkout>")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = {"advection_2d_square": [1, 2], "acoustics_2d_radial": [0, 1, 2], "advection_3d_swirl": [1, 2]}
 
