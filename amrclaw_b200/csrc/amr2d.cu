@@ -227,6 +227,7 @@ class Amr2Gpu {
     sp.prob = prob;
     for (int k = 0; k < MAXVAR; ++k) sp.mthlim[k] = k < (int)p.mthlim.size() ? p.mthlim[k] : 0;
     sp.order = p.order; sp.trans = p.trans; sp.use_fwaves = p.use_fwaves ? 1 : 0; sp.mcapa = p.mcapa;
+    sp.split = p.dimsplit;
   }
 
   // amrgpu_set_solver: rpn2/rpt2 plugin by name with its /cparam/ constants.
@@ -1672,6 +1673,7 @@ class Amr2Gpu {
     StepArgs a{};
     a.pool = pool.d; a.regs = regs.d; a.patches = rich_vp.d; a.fsv = nullptr; a.fad = nullptr;
     a.cflmax = rich_cfl.d; a.sp = sp; a.queue = nullptr; a.dt_dev = nullptr;
+    a.sp.split = 0;  // errest's big and regular steps call the unsplit stepgrid (prepbigstep.f:60, prepregstep.f:23)
     if (nbig > 0) {
       a.work = rich_work.d; a.nwork = nbig;
       a.dt = 2.0 * dt; a.dx = 2.0 * hx; a.dy = 2.0 * hy;
@@ -2090,7 +2092,8 @@ class Amr2Gpu {
       throw std::runtime_error("only ASCII output (output_format 1) is written: binary and NetCDF output are not supported");
     if (p.nghost != 2) throw std::runtime_error("num_ghost must be 2");
     if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
-    if (p.dimsplit != 0) throw std::runtime_error("only the unsplit method is supported");
+    // amr2.f90:258-263: Godunov splitting (stepgrid_dimSplit.f) or unsplit; Strang stops the reference
+    if (p.dimsplit > 1) throw std::runtime_error("Strang splitting is not supported (dimensional_split must be 0 or 1)");
     if (p.src_split != 0) throw std::runtime_error("source terms are not supported");
     nvar = p.nvar; ng = p.nghost;
     setup_problem();

@@ -109,6 +109,11 @@ struct Plan3 {
   std::vector<int> plist;
   std::vector<long long> sweep0, comp0, face0, cell0;
   long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;  // items: interfaces per direction
+  // dimensionally split step: interfaces of the split pencils per direction and patch, the
+  // enlarged cells of each patch in the split scratch, and per-patch views of both
+  std::vector<long long> scomp0, ecell0;
+  long long sitems[3] = {0, 0, 0}, ecells = 0;
+  DBuf<long long> d_scomp0, d_ecell0, d_spp;
   std::vector<Fsv3> fsv;
   std::vector<long long> seg0;  // register segments (lenbc) prefix over plist; fad/qad lists are built from it on the device
   std::vector<long long> fsv0;  // fluxsv entries prefix over plist
@@ -133,6 +138,7 @@ struct Plan3 {
     bound.free_dev(); saveqc.free_dev();
     d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_seg0.free(); d_fad.free(); d_qad.free();
     d_upc.free(); d_upt.free(); d_avg.free(); d_pp.free();
+    d_scomp0.free(); d_ecell0.free(); d_spp.free();
   }
 };
 
@@ -182,6 +188,7 @@ class Amr3Gpu : public AmrSolver {
   DBuf<unsigned long long> rich_cfl;
   long long rich_buf = -1, rich_len = 0;
   DBuf<double> d_stash, d_flux;
+  DBuf<double> d_split;  // the split step's y-updated values (nvar x enlarged cells of the largest level)
   DBuf<int8_t> lv_a, lv_b, lv_n, lv_t1, lv_t2;   // level flag arrays (flglvl)
   DBuf<LvlBox> lv_boxes, lv_proj;
   DBuf<long long> lv_c0;
@@ -229,7 +236,7 @@ class Amr3Gpu : public AmrSolver {
     rich_vp.free(); rich_rect.free(); rich_plist.free(); rich_pre.free(); rich_cfl.free();
     pool.destroy(); regs.destroy();
     stg.destroy();
-    d_patches.free(); d_stash.free(); d_flux.free(); d_gauge_out.free(); d_aux_jobs.free(); d_aux_fac.free();
+    d_patches.free(); d_stash.free(); d_flux.free(); d_split.free(); d_gauge_out.free(); d_aux_jobs.free(); d_aux_fac.free();
     for (DBuf<int8_t>* b : {&lv_a, &lv_b, &lv_n, &lv_t1, &lv_t2}) b->free();
     lv_boxes.free(); lv_proj.free(); lv_c0.free(); lv_plist.free();
     if (lv_host) cudaFreeHost(lv_host);
@@ -268,7 +275,9 @@ class Amr3Gpu : public AmrSolver {
       throw std::runtime_error("3D device path: unknown problem '" + p.problem + "' (euler_blast or advection_swirl)");
     }
     if (p.nghost != G3) throw std::runtime_error("num_ghost must be 2");
-    if (p.mcapa != 0 || p.dimsplit != 0) throw std::runtime_error("capacity functions and dimensional splitting are not supported");
+    if (p.mcapa != 0) throw std::runtime_error("capacity functions are not supported in 3D");
+    // amr3.f90:241-246: Godunov splitting (stepgrid_dimSplit.f) or unsplit; Strang stops the reference
+    if (p.dimsplit > 1) throw std::runtime_error("Strang splitting is not supported (dimensional_split must be 0 or 1)");
     if (p.use_fwaves) throw std::runtime_error("f-waves are not supported in 3D");
     if (p.flag_richardson && p.naux > 0) throw std::runtime_error("Richardson estimation needs num_aux = 0 (no auxcoarsen)");
     // bufnst.f:21-24 adds store2's first component to the flags whenever tol > 0: without
@@ -931,6 +940,23 @@ class Amr3Gpu : public AmrSolver {
       L.cell0[k + 1] = L.cell0[k] + (long long)g.nx() * g.ny() * g.nz();
     }
     L.faces = L.face0[np]; L.cells = L.cell0[np];
+    if (p.dimsplit) {
+      L.scomp0.assign((size_t)3 * (np + 1), 0);
+      L.ecell0.assign(np + 1, 0);
+      for (int d = 0; d < 3; ++d) {
+        long long c = 0;
+        for (int k = 0; k < np; ++k) {
+          const HPatch3& g = node[L.plist[k]];
+          const long long n1 = d == 0 ? g.nx() : d == 1 ? g.ny() : g.nz();
+          L.scomp0[(size_t)d * (np + 1) + k] = c;
+          c += split_pencils(d, g.nx(), g.ny(), g.nz()) * (n1 + 3);
+        }
+        L.scomp0[(size_t)d * (np + 1) + np] = c;
+        L.sitems[d] = c;
+      }
+      for (int k = 0; k < np; ++k) L.ecell0[k + 1] = L.ecell0[k] + (long long)mitot(L.plist[k]) * mjtot(L.plist[k]) * mktot(L.plist[k]);
+      L.ecells = L.ecell0[np];
+    }
     L.seg0.assign(np + 1, 0);
     std::vector<long long>& fsv0 = L.fsv0;
     fsv0.assign(np + 1, 0);
@@ -973,6 +999,21 @@ class Amr3Gpu : public AmrSolver {
         }
       L.d_pp.upload(pp, st, stg);
     }
+    if (p.dimsplit) {
+      L.d_scomp0.upload(L.scomp0, st, stg);
+      L.d_ecell0.upload(L.ecell0, st, stg);
+      // per patch: (first, last) split interface of each direction, then (first, last) scratch cell
+      std::vector<long long> spp((size_t)8 * np, 0);
+      for (int k = 0; k < np; ++k) {
+        for (int d = 0; d < 3; ++d) {
+          spp[(size_t)8 * k + 2 * d] = L.scomp0[(size_t)d * (np + 1) + k];
+          spp[(size_t)8 * k + 2 * d + 1] = L.scomp0[(size_t)d * (np + 1) + k + 1];
+        }
+        spp[(size_t)8 * k + 6] = L.ecell0[k];
+        spp[(size_t)8 * k + 7] = L.ecell0[k + 1];
+      }
+      L.d_spp.upload(spp, st, stg);
+    }
     L.d_fsv.upload(L.fsv, st, stg);
     L.d_seg0.upload(L.seg0, st, stg);
     L.d_fad.reserve(L.nseg);
@@ -987,6 +1028,7 @@ class Amr3Gpu : public AmrSolver {
     tph.next("cs_reserve");
     d_stash.reserve(std::max<size_t>(d_stash.n, (size_t)(L.slots * stash_values(nvar))));
     d_flux.reserve(std::max<size_t>(d_flux.n, (size_t)(L.faces * 6 * nvar)));
+    if (p.dimsplit) d_split.reserve(std::max<size_t>(d_split.n, (size_t)(L.ecells * nvar)));
   }
 
   // update.f:4-192 + upbnd.f:4-94 for coarse level lev
@@ -1276,7 +1318,7 @@ class Amr3Gpu : public AmrSolver {
     cudaGraphExec_t pre = nullptr, post = nullptr;
     long long gen = -1;
     int batched = -1;
-    const void* ptrs[6] = {};
+    const void* ptrs[7] = {};
     long long kpre = 0, kpost = 0;
     void reset() {
       if (pre) cudaGraphExecDestroy(pre);
@@ -1371,12 +1413,18 @@ class Amr3Gpu : public AmrSolver {
       if (timed) AMR_CUDA(cudaEventRecord(ev_a, st));
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
       a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
-      bool tt = false;
-      const int sched = pick_schedule(lev, tt, ds != nullptr);
-      a.queue = sched == 1 ? d_queue : nullptr;
-      if (tt) AMR_CUDA(cudaEventRecord(ev_t0, st));
-      nkernels += launch_step3(a, L.items, L.faces, L.cells, st, f32);
-      if (tt) { AMR_CUDA(cudaEventRecord(ev_t1, st)); tune_pending = sched; }
+      if (p.dimsplit) {
+        // stepgrid_dimSplit.f: x, y, z sweeps with their updates, one launch each
+        a.scomp0 = L.d_scomp0.d; a.ecell0 = L.d_ecell0.d; a.split = d_split.d;
+        nkernels += launch_split3(a, L.sitems, st, f32);
+      } else {
+        bool tt = false;
+        const int sched = pick_schedule(lev, tt, ds != nullptr);
+        a.queue = sched == 1 ? d_queue : nullptr;
+        if (tt) AMR_CUDA(cudaEventRecord(ev_t0, st));
+        nkernels += launch_step3(a, L.items, L.faces, L.cells, st, f32);
+        if (tt) { AMR_CUDA(cudaEventRecord(ev_t1, st)); tune_pending = sched; }
+      }
       if (timed) AMR_CUDA(cudaEventRecord(ev_b, st));
       if (!L.fsv.empty()) {
         launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d, (int)L.fsv.size(), nvar, dt, hx, hy, hz, st, f32, dtd);
@@ -1407,8 +1455,14 @@ class Amr3Gpu : public AmrSolver {
         b.sweep0 = L.d_pp.d + (size_t)12 * k; b.comp0 = L.d_pp.d + (size_t)12 * k + 6;
         b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
         long long it[3];
-        for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
-        nkernels += launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
+        if (p.dimsplit) {
+          b.scomp0 = L.d_spp.d + (size_t)8 * k; b.ecell0 = L.d_spp.d + (size_t)8 * k + 6; b.split = d_split.d;
+          for (int d = 0; d < 3; ++d) it[d] = L.scomp0[(size_t)d * (np + 1) + k + 1] - L.scomp0[(size_t)d * (np + 1) + k];
+          nkernels += launch_split3(b, it, st, f32);
+        } else {
+          for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
+          nkernels += launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
+        }
         const long long f0 = L.fsv0[k], nf = L.fsv0[k + 1] - L.fsv0[k];
         if (nf > 0) {
           launch_fsv3(d_flux.d, L.faces, L.d_face0.d, d_patches.d, regs.d, L.d_fsv.d + f0, (int)nf, nvar, dt, hx, hy, hz, st, f32, dtd);
@@ -1429,9 +1483,9 @@ class Amr3Gpu : public AmrSolver {
   // captures the level's two graphs if the current ones do not fit the plans and buffers
   void ensure_graphs(int lev) {
     LevelGraph& G = lgraph[lev];
-    const void* ptrs[6] = {pool.d, regs.d, d_patches.d, d_stash.d, d_flux.d, d_cfl};
+    const void* ptrs[7] = {pool.d, regs.d, d_patches.d, d_stash.d, d_flux.d, d_cfl, d_split.d};
     bool ok = G.pre && G.gen == plan_gen[lev] && G.batched == (int)batched;
-    for (int k = 0; k < 6 && ok; ++k) ok = G.ptrs[k] == ptrs[k];
+    for (int k = 0; k < 7 && ok; ++k) ok = G.ptrs[k] == ptrs[k];
     if (ok) return;
     HPROF("graph_capture3");
     G.reset();
@@ -1450,7 +1504,7 @@ class Amr3Gpu : public AmrSolver {
       nkernels = k0;
     }
     G.gen = plan_gen[lev]; G.batched = (int)batched;
-    for (int k = 0; k < 6; ++k) G.ptrs[k] = ptrs[k];
+    for (int k = 0; k < 7; ++k) G.ptrs[k] = ptrs[k];
     ++graph_captures;
   }
 

@@ -36,12 +36,89 @@ struct Step2Layout {
   static constexpr int TOTAL = NQ + 4 * NF + NTR + NW + NX + 32;
 };
 
+// flux2.f:136-194 at one face from the wave records (waves, speeds, amdq, apdq) of the face
+// (rc) and of its neighbours (rm: face f-1, rp: face f+1): limiter.f's limited waves, the
+// second-order correction cqxx, fm = (0 + amdq) + cqxx/2 and fp = (0 - apdq) + cqxx/2
+template <class S, class R>
+__device__ __forceinline__ void face_fluxes(const StepParams& sp, const R* rm, const R* rc, const R* rp, R dtdx,
+                                            R (&amdq)[S::MEQN], R (&apdq)[S::MEQN], R (&cqxx)[S::MEQN],
+                                            R (&fm)[S::MEQN], R (&fp)[S::MEQN]) {
+  constexpr int ME = S::MEQN, MW = S::MWAVES;
+#pragma unroll
+  for (int m = 0; m < ME; ++m) { amdq[m] = rc[MW * ME + MW + m]; apdq[m] = rc[MW * ME + MW + ME + m]; }
+#pragma unroll
+  for (int m = 0; m < ME; ++m) { fm[m] = R(0) + amdq[m]; fp[m] = R(0) - apdq[m]; cqxx[m] = R(0); }
+  if (sp.order == 1) return;
+  R wl[MW][ME];
+#pragma unroll
+  for (int mw = 0; mw < MW; ++mw) {
+    const R smw = rc[MW * ME + mw];
+#pragma unroll
+    for (int m = 0; m < ME; ++m) wl[mw][m] = rc[mw * ME + m];
+    if (sp.mthlim[mw] == 0) continue;
+    R wn2 = R(0), dotl = R(0), dotr = R(0);
+#pragma unroll
+    for (int m = 0; m < ME; ++m) {
+      wn2 = wn2 + rc[mw * ME + m] * rc[mw * ME + m];
+      dotl = dotl + rm[mw * ME + m] * rc[mw * ME + m];
+      dotr = dotr + rc[mw * ME + m] * rp[mw * ME + m];
+    }
+    if (wn2 == R(0)) continue;
+    const R r = (smw > R(0)) ? dotl / wn2 : dotr / wn2;
+    R wlim = R(0);
+    switch (sp.mthlim[mw]) {
+      case 1: wlim = dmax(R(0), dmin(R(1), r)); break;
+      case 2: wlim = dmax(R(0), dmax(dmin(R(1), R(2) * r), dmin(R(2), r))); break;
+      case 3: wlim = (r + fabs(r)) / (R(1) + fabs(r)); break;
+      case 4: { const R c = (R(1) + r) / R(2); wlim = dmax(R(0), dmin(c, dmin(R(2), R(2) * r))); } break;
+      case 5: wlim = r; break;
+    }
+#pragma unroll
+    for (int m = 0; m < ME; ++m) wl[mw][m] = wlim * wl[mw][m];
+  }
+  const R dtdxave = R(0.5) * (dtdx + dtdx);
+#pragma unroll
+  for (int m = 0; m < ME; ++m) {
+    R c = R(0);
+#pragma unroll
+    for (int mw = 0; mw < MW; ++mw) {
+      const R smw = rc[MW * ME + mw];
+      const R abs_sign = sp.use_fwaves ? dsign(R(1), smw) : fabs(smw);
+      c = c + abs_sign * (R(1) - fabs(smw) * dtdxave) * wl[mw][m];
+    }
+    cqxx[m] = c;
+    fm[m] = fm[m] + R(0.5) * c;
+    fp[m] = fp[m] + R(0.5) * c;
+  }
+}
+
+// rpn2 at one face into its wave record: waves [MW][ME], speeds [MW], amdq [ME], apdq [ME]
+template <class S, class R>
+__device__ __forceinline__ void face_record(const StepParams& sp, int ixy, const R* qL, const R* qR, R* rec, R dtdx,
+                                            bool count_cfl, R& cfl) {
+  constexpr int ME = S::MEQN, MW = S::MWAVES;
+  R wave[MW][ME], s[MW], amdq[ME], apdq[ME];
+  S::template rpn<R>(sp.prob, ixy, qL, qR, wave, s, amdq, apdq);
+#pragma unroll
+  for (int mw = 0; mw < MW; ++mw) {
+#pragma unroll
+    for (int m = 0; m < ME; ++m) rec[mw * ME + m] = wave[mw][m];
+    rec[MW * ME + mw] = s[mw];
+  }
+#pragma unroll
+  for (int m = 0; m < ME; ++m) { rec[MW * ME + MW + m] = amdq[m]; rec[MW * ME + MW + ME + m] = apdq[m]; }
+  if (count_cfl) {
+#pragma unroll
+    for (int mw = 0; mw < MW; ++mw) cfl = dmax(cfl, dmax(dtdx * s[mw], -dtdx * s[mw]));
+  }
+}
+
 // One sweep direction of flux2.f over the tile. IXY = 1: lines are rows, IXY = 2: columns.
 template <class S, int IXY, class R>
 __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR, R* F1,
                             R* F2, int i0, int j0, int tw, int th, R dtdx, R& cfl) {
   using L = Step2Layout<S>;
-  constexpr int ME = L::ME, MW = L::MW, T = L::T, QW = L::QW;
+  constexpr int ME = L::ME, T = L::T, QW = L::QW;
   const int tid = threadIdx.x;
   // along-line extents
   const int na = (IXY == 1) ? tw : th;       // cells along the line inside the tile
@@ -68,21 +145,7 @@ __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR
       R qL[ME], qR[ME];
       loadq(qL, line, f - 1);
       loadq(qR, line, f);
-      R wave[MW][ME], s[MW], amdq[ME], apdq[ME];
-      S::template rpn<R>(sp.prob, IXY, qL, qR, wave, s, amdq, apdq);
-      R* rec = W + (rr * (T + 3) + ff) * L::WREC;
-#pragma unroll
-      for (int mw = 0; mw < MW; ++mw) {
-#pragma unroll
-        for (int m = 0; m < ME; ++m) rec[mw * ME + m] = wave[mw][m];
-        rec[MW * ME + mw] = s[mw];
-      }
-#pragma unroll
-      for (int m = 0; m < ME; ++m) { rec[MW * ME + MW + m] = amdq[m]; rec[MW * ME + MW + ME + m] = apdq[m]; }
-      if (ff >= 1 && ff <= nfl) {
-#pragma unroll
-        for (int mw = 0; mw < MW; ++mw) cfl = dmax(cfl, dmax(dtdx * s[mw], -dtdx * s[mw]));
-      }
+      face_record<S, R>(sp, IXY, qL, qR, W + (rr * (T + 3) + ff) * L::WREC, dtdx, ff >= 1 && ff <= nfl, cfl);
     }
     __syncthreads();
     // phase 2: limiter, second-order correction, transverse splitting
@@ -93,53 +156,7 @@ __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR
       const R* rc = rm + L::WREC;                             // face f
       const R* rp = rc + L::WREC;                             // face f+1
       R amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
-#pragma unroll
-      for (int m = 0; m < ME; ++m) { amdq[m] = rc[MW * ME + MW + m]; apdq[m] = rc[MW * ME + MW + ME + m]; }
-#pragma unroll
-      for (int m = 0; m < ME; ++m) { fm[m] = R(0) + amdq[m]; fp[m] = R(0) - apdq[m]; }
-      if (sp.order != 1) {
-        R wl[MW][ME];
-#pragma unroll
-        for (int mw = 0; mw < MW; ++mw) {
-          const R smw = rc[MW * ME + mw];
-#pragma unroll
-          for (int m = 0; m < ME; ++m) wl[mw][m] = rc[mw * ME + m];
-          if (sp.mthlim[mw] == 0) continue;
-          R wn2 = R(0), dotl = R(0), dotr = R(0);
-#pragma unroll
-          for (int m = 0; m < ME; ++m) {
-            wn2 = wn2 + rc[mw * ME + m] * rc[mw * ME + m];
-            dotl = dotl + rm[mw * ME + m] * rc[mw * ME + m];
-            dotr = dotr + rc[mw * ME + m] * rp[mw * ME + m];
-          }
-          if (wn2 == R(0)) continue;
-          const R r = (smw > R(0)) ? dotl / wn2 : dotr / wn2;
-          R wlim = R(0);
-          switch (sp.mthlim[mw]) {
-            case 1: wlim = dmax(R(0), dmin(R(1), r)); break;
-            case 2: wlim = dmax(R(0), dmax(dmin(R(1), R(2) * r), dmin(R(2), r))); break;
-            case 3: wlim = (r + fabs(r)) / (R(1) + fabs(r)); break;
-            case 4: { const R c = (R(1) + r) / R(2); wlim = dmax(R(0), dmin(c, dmin(R(2), R(2) * r))); } break;
-            case 5: wlim = r; break;
-          }
-#pragma unroll
-          for (int m = 0; m < ME; ++m) wl[mw][m] = wlim * wl[mw][m];
-        }
-        const R dtdxave = R(0.5) * (dtdx + dtdx);
-#pragma unroll
-        for (int m = 0; m < ME; ++m) {
-          R c = R(0);
-#pragma unroll
-          for (int mw = 0; mw < MW; ++mw) {
-            const R smw = rc[MW * ME + mw];
-            const R abs_sign = sp.use_fwaves ? dsign(R(1), smw) : fabs(smw);
-            c = c + abs_sign * (R(1) - fabs(smw) * dtdxave) * wl[mw][m];
-          }
-          cqxx[m] = c;
-          fm[m] = fm[m] + R(0.5) * c;
-          fp[m] = fp[m] + R(0.5) * c;
-        }
-      }
+      face_fluxes<S, R>(sp, rm, rc, rp, dtdx, amdq, apdq, cqxx, fm, fp);
       // flux increments into the tile's face arrays (interior lines only)
       const int lin = (IXY == 1) ? line - j0 : line - i0;
       if (lin >= 0 && lin < ((IXY == 1) ? th : tw)) {
@@ -203,6 +220,58 @@ __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR
       }
     }
     __syncthreads();
+  }
+}
+
+// The flux-register epilogue of a tile (fluxsv.f:10-109 on coarse faces next to finer grids,
+// fluxad.f:7-96 on this patch's fine boundary faces). FM, FP: [ME][xrows][T+1] x-faces of
+// the tile's rows starting at row 0 of FM / FP; GM, GP: [ME][T+1][T] y-faces. Register
+// values stay FP64 in both forms.
+template <int ME, class R>
+__device__ __forceinline__ void register_epilogue(const StepArgs& a, const StepWork& wk, const PatchDev& P, int i0, int j0,
+                                                  int tw, int th, double dt, const R* FM, const R* FP, const R* GM,
+                                                  const R* GP, int xrows) {
+  constexpr int T = TILE2;
+  const int tid = threadIdx.x;
+  for (int it = tid; it < wk.fsv_count * ME; it += STEP2_THREADS) {
+    const FsvEntry e = a.fsv[wk.fsv_start + it / ME];
+    const int m = it % ME;
+    const int ca = e.ic - i0, rb = e.jc - j0;
+    double v = 0.0;
+    if (e.side == 1) v = -(double)FP[(m * xrows + rb) * (T + 1) + ca] * dt * a.dy;
+    else if (e.side == 2) v = -(double)GM[(m * (T + 1) + rb + 1) * T + ca] * dt * a.dx;
+    else if (e.side == 3) v = -(double)FM[(m * xrows + rb) * (T + 1) + ca + 1] * dt * a.dy;
+    else v = -(double)GP[(m * (T + 1) + rb) * T + ca] * dt * a.dx;
+    a.regs[e.dst + m] = v;
+  }
+  for (int it = tid; it < wk.fad_count * ME; it += STEP2_THREADS) {
+    const FadEntry e = a.fad[wk.fad_start + it / ME];
+    const int m = it % ME;
+    const int r = e.pad;
+    double* svd = a.regs + P.ffl + (long long)ME * e.seg + m;
+    double s = *svd;
+    for (int l = 0; l < r; ++l) {
+      const int f = e.f0 + l;
+      if (e.side == 1) s = s + (double)FM[(m * xrows + (f - j0)) * (T + 1) + 0] * dt * a.dy;
+      else if (e.side == 2) s = s + (double)GP[(m * (T + 1) + th) * T + (f - i0)] * dt * a.dx;
+      else if (e.side == 3) s = s + (double)FP[(m * xrows + (f - j0)) * (T + 1) + tw] * dt * a.dy;
+      else s = s + (double)GM[(m * (T + 1) + 0) * T + (f - i0)] * dt * a.dx;
+    }
+    *svd = s;
+  }
+}
+
+// Block maximum of the Courant number into the level maximum (bit pattern of a non-negative double).
+template <class R>
+__device__ __forceinline__ void cfl_to_level(R cfl, R* red, unsigned long long* cflmax) {
+  const int tid = threadIdx.x;
+  for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+  if ((tid & 31) == 0) red[tid >> 5] = cfl;
+  __syncthreads();
+  if (tid == 0) {
+    R c = R(0);
+    for (int k = 0; k < STEP2_THREADS / 32; ++k) c = dmax(c, red[k]);
+    atomicMax(cflmax, (unsigned long long)__double_as_longlong((double)c));
   }
 }
 
@@ -293,50 +362,171 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
       const int ie = i0 + ca + 1, je = j0 + rb + 1;
       qout[m * plane + (long long)je * mitot + ie] = qn;
     }
-    // fluxsv epilogue: coarse fluxes next to finer grids into the kids' registers
-    for (int it = tid; it < wk.fsv_count * ME; it += STEP2_THREADS) {
-      const FsvEntry e = a.fsv[wk.fsv_start + it / ME];
-      const int m = it % ME;
-      const int ca = e.ic - i0, rb = e.jc - j0;
-      // register values stay FP64 in both forms
-      double v = 0.0;
-      if (e.side == 1) v = -(double)FP[(m * T + rb) * (T + 1) + ca] * dt * a.dy;
-      else if (e.side == 2) v = -(double)GM[(m * (T + 1) + rb + 1) * T + ca] * dt * a.dx;
-      else if (e.side == 3) v = -(double)FM[(m * T + rb) * (T + 1) + ca + 1] * dt * a.dy;
-      else v = -(double)GP[(m * (T + 1) + rb) * T + ca] * dt * a.dx;
-      a.regs[e.dst + m] = v;
-    }
-    // fluxad epilogue: fine boundary fluxes accumulated into this patch's registers
-    for (int it = tid; it < wk.fad_count * ME; it += STEP2_THREADS) {
-      const FadEntry e = a.fad[wk.fad_start + it / ME];
-      const int m = it % ME;
-      const int r = e.pad;
-      double* svd = a.regs + P.ffl + (long long)ME * e.seg + m;
-      double s = *svd;
-      for (int l = 0; l < r; ++l) {
-        const int f = e.f0 + l;
-        if (e.side == 1) s = s + (double)FM[(m * T + (f - j0)) * (T + 1) + 0] * dt * a.dy;
-        else if (e.side == 2) s = s + (double)GP[(m * (T + 1) + th) * T + (f - i0)] * dt * a.dx;
-        else if (e.side == 3) s = s + (double)FP[(m * T + (f - j0)) * (T + 1) + tw] * dt * a.dy;
-        else s = s + (double)GM[(m * (T + 1) + 0) * T + (f - i0)] * dt * a.dx;
-      }
-      *svd = s;
-    }
+    register_epilogue<ME, R>(a, wk, P, i0, j0, tw, th, dt, FM, FP, GM, GP, T);
     __syncthreads();
   }
-  // block max of the Courant number -> level maximum
-  for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
-  if ((tid & 31) == 0) red[tid >> 5] = cfl;
-  __syncthreads();
-  if (tid == 0) {
-    R c = R(0);
-    for (int k = 0; k < STEP2_THREADS / 32; ++k) c = dmax(c, red[k]);
-    atomicMax(a.cflmax, (unsigned long long)__double_as_longlong((double)c));
+  cfl_to_level(cfl, red, a.cflmax);
+}
+
+// ======================================================================= Godunov-split patch step
+// stepgrid_dimSplit.f:4-201 with step2x.f90, step2y.f90 and flux2_dimSplit.f over one tile.
+// The reference sweeps x along every row of the enlarged patch (ghost rows included) and
+// x-updates every row's interior cells before the y-sweeps read them, so the tile sweeps
+// its own rows and two rows on each side (all staged with the tile), x-updates them, then
+// sweeps y along its columns over the x-updated values and y-updates. The Courant number
+// takes every face each tile computes (the maximum is unchanged by faces counted twice).
+// Face fluxes are fm = (0 + amdq) + cqxx/2, fp = (0 - apdq) + cqxx/2: flux2_dimSplit's
+// faddm = amdq, faddp = -apdq (+ cqxx/2) added to zeroed arrays give the same values.
+template <class S>
+struct Split2Layout {
+  static constexpr int ME = S::MEQN, MW = S::MWAVES, T = TILE2, QW = T + 4;
+  static constexpr int NQ = ME * QW * QW;           // staged q of the tile and two ghost layers
+  static constexpr int NFX = ME * QW * (T + 1);      // fm / fp of every staged row
+  static constexpr int NQX = ME * QW * T;            // x-updated q of the tile's columns
+  static constexpr int NG = ME * (T + 1) * T;        // gm / gp
+  static constexpr int WREC = MW * ME + MW + 2 * ME;
+  static constexpr int NW = STEP2_RC * (T + 3) * WREC;
+  static constexpr int TOTAL = NQ + 2 * NFX + NQX + 2 * NG + NW + 32;
+};
+
+template <class S, class R>
+__global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
+  using L = Split2Layout<S>;
+  constexpr int ME = L::ME, T = L::T, QW = L::QW, WREC = L::WREC;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* Qs = reinterpret_cast<R*>(smem_raw);
+  R* FXm = Qs + L::NQ;
+  R* FXp = FXm + L::NFX;
+  R* Qx = FXp + L::NFX;
+  R* GM = Qx + L::NQX;
+  R* GP = GM + L::NG;
+  R* W = GP + L::NG;
+  R* red = W + L::NW;
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+  const R dtdx = (R)(dt / a.dx), dtdy = (R)(dt / a.dy);
+  R cfl = R(0);
+  int iter = 0;
+  while (true) {
+    int w;
+    if (a.queue) {
+      if (tid == 0) s_item = atomicAdd(a.queue, 1);
+      __syncthreads();
+      w = s_item;
+      __syncthreads();
+    } else {
+      w = blockIdx.x + iter * gridDim.x;
+    }
+    ++iter;
+    if (w >= a.nwork) break;
+    const StepWork wk = a.work[w];
+    const PatchDev P = a.patches[wk.patch];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+    const int mitot = P.mitot, mjtot = P.mjtot;
+    const int i0 = wk.ti0, j0 = wk.tj0;
+    const int tw = min(T, mx - i0 + 1), th = min(T, my - j0 + 1);
+    const R* qin = static_cast<const R*>(a.pool) + P.q[P.cur];
+    R* qout = static_cast<R*>(a.pool) + P.q[1 - P.cur];
+    const long long plane = (long long)mitot * mjtot;
+    const int lw = tw + 4, lh = th + 4;
+    for (int it = tid; it < ME * lw * lh; it += STEP2_THREADS) {
+      const int m = it / (lw * lh), rem = it % (lw * lh);
+      const int b = rem / lw, aa = rem % lw;
+      const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
+      Qs[(m * QW + b) * QW + aa] = qin[m * plane + (long long)je * mitot + ie];
+    }
+    __syncthreads();
+    // step2x.f90: rows b (j = j0-2+b), faces ff (i = i0-1+ff, between staged columns ff, ff+1)
+    {
+      const int nfr = tw + 3, nfl = tw + 1;
+      for (int b0 = 0; b0 < lh; b0 += STEP2_RC) {
+        const int nb = min(STEP2_RC, lh - b0);
+        for (int it = tid; it < nb * nfr; it += STEP2_THREADS) {
+          const int rr = it / nfr, ff = it % nfr, b = b0 + rr;
+          R qL[ME], qR[ME];
+#pragma unroll
+          for (int m = 0; m < ME; ++m) { qL[m] = Qs[(m * QW + b) * QW + ff]; qR[m] = Qs[(m * QW + b) * QW + ff + 1]; }
+          face_record<S, R>(a.sp, 1, qL, qR, W + (rr * (T + 3) + ff) * WREC, dtdx, ff >= 1 && ff <= nfl, cfl);
+        }
+        __syncthreads();
+        for (int it = tid; it < nb * nfl; it += STEP2_THREADS) {
+          const int rr = it / nfl, fa = it % nfl, b = b0 + rr;
+          const R* rm = W + (rr * (T + 3) + fa) * WREC;
+          R amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
+          face_fluxes<S, R>(a.sp, rm, rm + WREC, rm + 2 * WREC, dtdx, amdq, apdq, cqxx, fm, fp);
+#pragma unroll
+          for (int m = 0; m < ME; ++m) {
+            FXm[(m * QW + b) * (T + 1) + fa] = fm[m];
+            FXp[(m * QW + b) * (T + 1) + fa] = fp[m];
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // stepgrid_dimSplit.f:88-103: x-update of every staged row's tile cells
+    for (int it = tid; it < ME * lh * tw; it += STEP2_THREADS) {
+      const int m = it / (lh * tw), rem = it % (lh * tw);
+      const int b = rem / tw, c = rem % tw;
+      Qx[(m * QW + b) * T + c] =
+          Qs[(m * QW + b) * QW + c + 2] - dtdx * (FXm[(m * QW + b) * (T + 1) + c + 1] - FXp[(m * QW + b) * (T + 1) + c]);
+    }
+    __syncthreads();
+    // step2y.f90: columns c (i = i0+c), faces ff (j = j0-1+ff, between x-updated rows ff, ff+1)
+    {
+      const int nfr = th + 3, nfl = th + 1;
+      for (int c0 = 0; c0 < tw; c0 += STEP2_RC) {
+        const int nc = min(STEP2_RC, tw - c0);
+        for (int it = tid; it < nc * nfr; it += STEP2_THREADS) {
+          const int rr = it / nfr, ff = it % nfr, c = c0 + rr;
+          R qL[ME], qR[ME];
+#pragma unroll
+          for (int m = 0; m < ME; ++m) { qL[m] = Qx[(m * QW + ff) * T + c]; qR[m] = Qx[(m * QW + ff + 1) * T + c]; }
+          face_record<S, R>(a.sp, 2, qL, qR, W + (rr * (T + 3) + ff) * WREC, dtdy, ff >= 1 && ff <= nfl, cfl);
+        }
+        __syncthreads();
+        for (int it = tid; it < nc * nfl; it += STEP2_THREADS) {
+          const int rr = it / nfl, fb = it % nfl, c = c0 + rr;
+          const R* rm = W + (rr * (T + 3) + fb) * WREC;
+          R amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
+          face_fluxes<S, R>(a.sp, rm, rm + WREC, rm + 2 * WREC, dtdy, amdq, apdq, cqxx, fm, fp);
+#pragma unroll
+          for (int m = 0; m < ME; ++m) {
+            GM[(m * (T + 1) + fb) * T + c] = fm[m];
+            GP[(m * (T + 1) + fb) * T + c] = fp[m];
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // stepgrid_dimSplit.f:118-133: y-update of the tile's cells into the other buffer
+    for (int it = tid; it < ME * th * tw; it += STEP2_THREADS) {
+      const int m = it / (th * tw), rem = it % (th * tw);
+      const int rb = rem / tw, ca = rem % tw;
+      const R qn = Qx[(m * QW + rb + 2) * T + ca] - dtdy * (GM[(m * (T + 1) + rb + 1) * T + ca] - GP[(m * (T + 1) + rb) * T + ca]);
+      qout[m * plane + (long long)(j0 + rb + 1) * mitot + (i0 + ca + 1)] = qn;
+    }
+    // the tile's own rows start at staged row 2 of FXm / FXp
+    register_epilogue<ME, R>(a, wk, P, i0, j0, tw, th, dt, FXm + 2 * (T + 1), FXp + 2 * (T + 1), GM, GP, QW);
+    __syncthreads();
   }
+  cfl_to_level(cfl, red, a.cflmax);
 }
 
 template <class S, class R>
 static void launch_step2_t(const StepArgs& a, int grid, cudaStream_t s) {
+  if (a.sp.split) {
+    const size_t sm = sizeof(R) * Split2Layout<S>::TOTAL;
+    static const bool attr = [&] {
+      AMR_CUDA(cudaFuncSetAttribute(step2s_kernel<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      return true;
+    }();
+    (void)attr;
+    if (grid <= 0) return;
+    step2s_kernel<S, R><<<grid, STEP2_THREADS, sm, s>>>(a);
+    AMR_CUDA(cudaGetLastError());
+    return;
+  }
   const size_t sm = sizeof(R) * Step2Layout<S>::TOTAL;
   // once per process (thread-safe static initialisation; contexts may run on several host threads)
   static const bool attr = [&] {

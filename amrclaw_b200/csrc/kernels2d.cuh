@@ -39,6 +39,7 @@ struct StepParams {
   int trans;             // method(3)
   int use_fwaves;
   int mcapa;
+  int split;             // dimensional_split: 0 unsplit (stepgrid.f), 1 Godunov (stepgrid_dimSplit.f)
 };
 
 // pool: the patch pool, of double, or of float in the FP32 form (offsets count elements)

@@ -91,6 +91,8 @@ struct Euler3Phys {
   template <int DIR>
   __device__ __forceinline__ void load(const T*, const PatchDev&, long long, long long, long long, int) {}
   template <int DIR>
+  __device__ __forceinline__ void load_normal(const T*, const PatchDev&, long long, long long, long long, int) {}
+  template <int DIR>
   __device__ __forceinline__ void rpn(const Step3Params& sp, const T* QL, const T* QR, T (&W)[NW][NV], T* S, T* AM, T* AP) {
     R = roe3d((T)sp.gamma1, QL, QR);
     euler3d_rpn_roe((T)sp.gamma, (T)sp.gamma1, sp.efix != 0, DIR, QL, QR, R, W, S, AM, AP);
@@ -131,6 +133,11 @@ struct Swirl3Phys {
       vy[c][0] = ay[0]; vy[c][1] = ay[sy]; vy[c][2] = ay[-sz]; vy[c][3] = ay[sy - sz]; vy[c][4] = ay[sz]; vy[c][5] = ay[sy + sz];
       vz[c][0] = az[0]; vz[c][1] = az[sz]; vz[c][2] = az[-sy]; vz[c][3] = az[sz - sy]; vz[c][4] = az[sy]; vz[c][5] = az[sy + sz];
     }
+  }
+  // the split step's rpn3 needs only the interface's own face velocity (no transverse rows)
+  template <int DIR>
+  __device__ __forceinline__ void load_normal(const T* pool, const PatchDev& P, long long base, long long step, long long plane, int e) {
+    un = pool[P.aux + (long long)(DIR - 1) * plane + base + (long long)e * step];
   }
   template <int DIR>
   __device__ __forceinline__ void rpn(const Step3Params&, const T* QL, const T* QR, T (&W)[NW][NV], T* S, T* AM, T* AP) {
@@ -462,6 +469,144 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_queue_kernel(Step3Args A
     else if (it < nxy) sweep3_tile<2, T, PH>(A, it - nx, sW);
     else sweep3_tile<3, T, PH>(A, it - nxy, sW);
   }
+}
+
+// ------------------------------------------------------------------- dimensional splitting
+// stepgrid_dimSplit.f:4-264 (step3x.f, step3y.f, step3z.f, flux3_dimSplit.f) as one launch
+// per direction. Pencils (split_pencils): x along every (j, k) row of the enlarged patch,
+// y along the interior i and every k, z along the interior (i, j); each of n1+3 interfaces
+// 0..n1+2 (cells e-1 | e), in tiles of SW_T consecutive interfaces overlapping by three like
+// the unsplit sweeps. A thread solves its interface (waves shared for the limiter), forms
+// fm = 0 + (amdq + cqxx) and fp = 0 + (-apdq + cqxx) (flux3_dimSplit.f's faddm = amdq,
+// faddp = -apdq, + cqxx, added to zeroed arrays), and updates the cell it owns:
+//   x: q[cur] -> q[1-cur] (every row; only interior i are written or read later)
+//   y: q[1-cur] -> the level's split scratch (interior i and j, every k)
+//   z: split scratch -> q[1-cur] (interior cells)
+// Faces of interior pencils go to the flux array for fluxsv / fluxad.
+template <int DIR, class T, class PH>
+__global__ void __launch_bounds__(SW_T) split3_kernel(Step3Args A) {
+  constexpr int NV = PH::NV, NW = PH::NW;
+  __shared__ T sW[NW * NV][SW_T];
+  __shared__ T sF[2 * NV][SW_T];
+  const long long* c0 = A.scomp0 + (long long)(DIR - 1) * (A.np + 1);
+  const long long first = c0[0], last = c0[A.np];
+  const int l = threadIdx.x;
+  const long long g = first + (long long)blockIdx.x * SW_OWN - 1 + l;
+  const bool valid = g >= first && g < last;
+  const Step3Params sp = A.sp;
+  const double dn = DIR == 1 ? A.dx : DIR == 2 ? A.dy : A.dz;
+  const double dt = A.dt_dev ? *A.dt_dev : A.dt;
+  const T dtdx = (T)(dt / dn);
+  int e = -1, n1 = 0, pi = 0;
+  bool interior_pencil = false;
+  long long base = 0, step = 0, plane = 0, fidx0 = 0, fstep = 0;
+  const T* qi = nullptr;
+  T* qo = nullptr;
+  PH ph;
+  T W[NW][NV], S[NW], AM[NV], AP[NV];
+  if (valid) {
+    pi = find_patch(c0, A.np, g);
+    const PatchDev& P = A.patches[A.plist[pi]];
+    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+    n1 = DIR == 1 ? mx : DIR == 2 ? my : mz;
+    const int na = DIR == 1 ? my + 4 : mx;  // pencils: a fastest, then b
+    const long long loc = g - c0[pi];
+    e = (int)(loc % (n1 + 3));
+    const long long pen = loc / (n1 + 3);
+    const int a = (int)(pen % na), b = (int)(pen / na);
+    const long long mi = P.mitot, mj = P.mjtot;
+    // enlarged 0-based index of pencil cell x (1-based along the pencil) is base + (x + 1) * step
+    long long ie = 0, je = 0, ke = 0;
+    if (DIR == 1) { je = a; ke = b; step = 1; interior_pencil = a >= 2 && a < my + 2 && b >= 2 && b < mz + 2; }
+    else if (DIR == 2) { ie = a + 2; ke = b; step = mi; interior_pencil = b >= 2 && b < mz + 2; }
+    else { ie = a + 2; je = b + 2; step = mi * mj; interior_pencil = true; }
+    base = (ke * mj + je) * mi + ie;
+    plane = mi * mj * P.mktot;
+    const T* pool = static_cast<const T*>(A.pool);
+    T* scratch = static_cast<T*>(A.split) + (long long)NV * A.ecell0[pi];
+    qi = DIR == 1 ? pool + P.q[P.cur] : DIR == 2 ? pool + P.q[1 - P.cur] : scratch;
+    qo = DIR == 1 ? const_cast<T*>(pool) + P.q[1 - P.cur] : DIR == 2 ? scratch : const_cast<T*>(pool) + P.q[1 - P.cur];
+    // face (e) of this pencil in the patch's face block: x-faces i = e, y-faces j = e, z-faces k = e
+    // (face cell (i, j, k) is ((k-1)*NJ + (j-1))*NI + (i-1) of the block, as face3_kernel)
+    const long long NI = mx + 1, NJ = my + 1;
+    if (DIR == 1) { fidx0 = ((long long)(b - 2) * NJ + (a - 2)) * NI - 1; fstep = 1; }              // j = a-1, k = b-1
+    else if (DIR == 2) { fidx0 = ((long long)(b - 2) * NJ - 1) * NI + a; fstep = NI; }              // i = a+1, k = b-1
+    else { fidx0 = (long long)b * NI + a - NJ * NI; fstep = NJ * NI; }                              // i = a+1, j = b+1
+    fidx0 += A.face0[pi];
+    T QL[NV + 1], QR[NV + 1];
+    const long long atl = base + (long long)e * step, atr = atl + step;  // cells e-1 and e
+#pragma unroll
+    for (int m = 1; m <= NV; ++m) { QL[m] = qi[(m - 1) * plane + atl]; QR[m] = qi[(m - 1) * plane + atr]; }
+    QL[0] = QR[0] = T(0);
+    ph.template load_normal<DIR>(pool, P, base, step, plane, e + 1);
+    ph.template rpn<DIR>(sp, QL, QR, W, S, AM, AP);
+#pragma unroll
+    for (int k = 0; k < NW; ++k)
+#pragma unroll
+      for (int m = 0; m < NV; ++m) sW[k * NV + m][l] = W[k][m];
+  }
+  __syncthreads();
+  const bool live = valid && e >= 1 && e <= n1 + 1 && l >= 1 && l <= SW_T - 2;
+  const bool owned = live && l <= SW_T - 3;
+  T cfl = T(0);
+  if (live) {
+#pragma unroll
+    for (int k = 0; k < NW; ++k) cfl = dmax(cfl, dmax(dtdx * S[k], -dtdx * S[k]));
+    T CQ[NV];
+#pragma unroll
+    for (int m = 0; m < NV; ++m) CQ[m] = T(0);
+    if (sp.order != 1) {
+      const T dtdxave = T(0.5) * (dtdx + dtdx);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        if (sp.mthlim[k] == 0) continue;
+        T dl = T(0), dr = T(0), wn = T(0);
+#pragma unroll
+        for (int m = 0; m < NV; ++m) dl = dl + sW[k * NV + m][l - 1] * W[k][m];
+#pragma unroll
+        for (int m = 0; m < NV; ++m) dr = dr + W[k][m] * sW[k * NV + m][l + 1];
+#pragma unroll
+        for (int m = 0; m < NV; ++m) wn = wn + W[k][m] * W[k][m];
+        if (wn != T(0)) {
+          const T r = (S[k] > T(0)) ? dl / wn : dr / wn;
+          const T phi = philim3(sp.mthlim[k], r);
+#pragma unroll
+          for (int m = 0; m < NV; ++m) W[k][m] = phi * W[k][m];
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < NV; ++m) {
+        T x = T(0);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) x = x + T(0.5) * fabs(S[k]) * (T(1) - fabs(S[k]) * dtdxave) * W[k][m];
+        CQ[m] = x;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      const T fm = sp.order != 1 ? T(0) + (AM[m] + CQ[m]) : T(0) + AM[m];
+      const T fp = sp.order != 1 ? T(0) + (-AP[m] + CQ[m]) : T(0) + (-AP[m]);
+      sF[m][l] = fm;
+      sF[NV + m][l] = fp;
+      if (owned && interior_pencil) {
+        T* F = static_cast<T*>(A.flux) + fidx0 + (long long)e * fstep;
+        const long long fs = A.flux_stride;
+        const int c = 2 * (DIR - 1) * NV;
+        F[(c + m) * fs] = fm;
+        F[(c + NV + m) * fs] = fp;
+      }
+    }
+  }
+  __syncthreads();
+  // the cell e (1..n1) of the pencil: its right face is interface e+1 (thread l+1)
+  if (owned && e <= n1) {
+    const long long at = base + (long long)(e + 1) * step;
+#pragma unroll
+    for (int m = 0; m < NV; ++m)
+      qo[m * plane + at] = qi[m * plane + at] - dtdx * (sF[m][l + 1] - sF[NV + m][l]);
+  }
+  for (int o = 16; o > 0; o >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
+  if ((threadIdx.x & 31) == 0 && cfl > T(0)) atomic_max_nonneg(A.cflmax, (double)cfl);
 }
 
 // stash element of gadd / hadd for side s (1,2), offset d (-1..1), component m (0..NV-1)
@@ -1184,6 +1329,25 @@ static int launch_step3_t(const Step3Args& a, const long long items[3], long lon
   AMR_CUDA(cudaGetLastError());
   return n;
 }
+template <class T, class PH>
+static int launch_split3_t(const Step3Args& a, const long long items[3], cudaStream_t s) {
+  auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
+  int n = 0;
+  if (items[0] > 0) { split3_kernel<1, T, PH><<<tiles(items[0]), SW_T, 0, s>>>(a); ++n; }
+  if (items[1] > 0) { split3_kernel<2, T, PH><<<tiles(items[1]), SW_T, 0, s>>>(a); ++n; }
+  if (items[2] > 0) { split3_kernel<3, T, PH><<<tiles(items[2]), SW_T, 0, s>>>(a); ++n; }
+  AMR_CUDA(cudaGetLastError());
+  return n;
+}
+int launch_split3(const Step3Args& a, const long long items[3], cudaStream_t s, bool f32) {
+  if (a.sp.solver == SOLVER3_SWIRL) {
+    if (f32) return launch_split3_t<float, Swirl3Phys<float>>(a, items, s);
+    return launch_split3_t<double, Swirl3Phys<double>>(a, items, s);
+  }
+  if (f32) return launch_split3_t<float, Euler3Phys<float>>(a, items, s);
+  return launch_split3_t<double, Euler3Phys<double>>(a, items, s);
+}
+
 int launch_step3(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s, bool f32) {
   if (a.sp.solver == SOLVER3_SWIRL) {
     if (f32) return launch_step3_t<float, Swirl3Phys<float>>(a, items, faces, cells, s);

@@ -43,6 +43,12 @@ struct Step3Args {
   unsigned long long* cflmax;
   unsigned int* queue;       // if set: the sweeps of all three directions run as one persistent work-queue launch
   Step3Params sp;
+  // dimensionally split step (stepgrid_dimSplit.f): [3][np+1] first interface of each patch
+  // per direction over the split pencils, [np+1] first enlarged cell of each patch in the
+  // level's split scratch (the y-updated values), and that scratch
+  const long long* scomp0 = nullptr;
+  const long long* ecell0 = nullptr;
+  void* split = nullptr;
 };
 
 // fluxsv.f:4-94 entries (coarse patch faces next to a kid) and fluxad.f:4-155 registers.
@@ -95,6 +101,15 @@ struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff;
 // interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction.
 // returns the number of kernels launched
 int launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s, bool f32);
+// the Godunov-split step of the level (stepgrid_dimSplit.f): x, y and z sweeps with their
+// updates, interfaces_per_dir counting the split pencils (scomp0); returns launches made
+int launch_split3(const Step3Args& a, const long long interfaces_per_dir[3], cudaStream_t s, bool f32);
+// pencils of a patch of mx x my x mz cells in the split sweep of direction d (0, 1, 2):
+// x along every (j, k) row of the enlarged patch, y along the interior i and every k,
+// z along the interior (i, j)
+__host__ __device__ inline long long split_pencils(int d, long long mx, long long my, long long mz) {
+  return d == 0 ? (my + 4) * (mz + 4) : d == 1 ? mx * (mz + 4) : mx * my;
+}
 // Builds the level's fluxad/qad work lists on the device: pre[np+1] is the prefix of the
 // register segments (lenbc) of the patches in plist (0 for patches without registers).
 void launch_expand_fadqad3(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry, int rz,

@@ -168,8 +168,8 @@ struct Amr2 {
     method[1] = vtime ? 2 : 1;
     method[2] = c.i("order"); method[3] = c.i("transverse_waves");
     dimensional_split = c.i("dimensional_split");
-    // stepgrid_dimSplit.f is not restated: refuse rather than take unsplit steps
-    if (dimensional_split != 0) throw std::runtime_error("dimensional splitting is not supported");
+    // amr2.f90:258-263: Godunov splitting (1) only; Strang splitting stops the reference
+    if (dimensional_split > 1) throw std::runtime_error("Strang splitting is not supported (amrclaw stops)");
     method[4] = c.i("verbosity"); method[5] = c.i("source_split");
     mcapa = c.i("capa_index"); use_fwaves = c.b("use_fwaves");
     for (int k = 0; k < mwaves; ++k) mthlim.push_back(c.i("limiter", k));
@@ -524,6 +524,124 @@ struct Amr2 {
           }
         }
     if (cflgrid > 0.0) dtnew = dt * cfl / cflgrid;
+    else dtnew = RINFINITY;
+  }
+
+  // flux2_dimSplit.f: the normal fluctuations, limiter and second-order correction of one
+  // slice, without transverse terms (faddm = amdq, faddp = -apdq, then + cqxx/2)
+  void flux2_dimSplit(int ixy, int maxm, int meqn, int maux, int mbc, int mx, Work1d& W, double& cfl1d) {
+    const int base = 1 - mbc;
+    Slice q1d{W.q1d.data(), meqn, base};
+    Slice aux2{W.aux2.data(), std::max(maux, 1), base};
+    Slice faddm{W.faddm.data(), meqn, base}, faddp{W.faddp.data(), meqn, base};
+    auto dtdx1d = [&](int i) -> double& { return W.dtdx1d[i - base]; };
+    Waves wave{W.wave.data(), meqn, mwaves, base};
+    Slice s{W.s.data(), mwaves, base};
+    Slice cqxx{W.cqxx.data(), meqn, base};
+    bool limit = false;
+    for (int mw = 1; mw <= mwaves; ++mw) if (mthlim[mw - 1] > 0) limit = true;
+    for (int i = 1 - mbc; i <= mx + mbc; ++i)
+      for (int m = 1; m <= meqn; ++m) { faddm(m, i) = 0.0; faddp(m, i) = 0.0; }
+    // rpn2 writes amdq into faddm and apdq into faddp directly (flux2_dimSplit.f:55-57)
+    rpn2(prob, ixy, meqn, mwaves, mbc, mx, q1d, q1d, aux2, aux2, wave, s, faddm, faddp);
+    for (int i = 1 - mbc; i <= mx + mbc; ++i)
+      for (int m = 1; m <= meqn; ++m) faddp(m, i) = -faddp(m, i);
+    cfl1d = 0.0;
+    for (int mw = 1; mw <= mwaves; ++mw)
+      for (int i = 1; i <= mx + 1; ++i)
+        cfl1d = std::max(cfl1d, std::max(dtdx1d(i) * s(mw, i), -dtdx1d(i - 1) * s(mw, i)));
+    if (method[2] == 1) return;
+    if (limit) limiter(maxm, meqn, mbc, mx, wave, s);
+    for (int i = 1; i <= mx + 1; ++i) {
+      const double dtdxave = 0.5 * (dtdx1d(i - 1) + dtdx1d(i));
+      for (int m = 1; m <= meqn; ++m) {
+        cqxx(m, i) = 0.0;
+        for (int mw = 1; mw <= mwaves; ++mw) {
+          const double abs_sign = use_fwaves ? dsign(1.0, s(mw, i)) : std::fabs(s(mw, i));
+          cqxx(m, i) = cqxx(m, i) + abs_sign * (1.0 - std::fabs(s(mw, i)) * dtdxave) * wave(m, mw, i);
+        }
+        faddm(m, i) = faddm(m, i) + 0.5 * cqxx(m, i);
+        faddp(m, i) = faddp(m, i) + 0.5 * cqxx(m, i);
+      }
+    }
+  }
+
+  // stepgrid_dimSplit.f:4-201 with step2x.f90 / step2y.f90: Godunov splitting. x-sweeps over
+  // every row (ghost rows included), the x-update of every row's interior cells, then
+  // y-sweeps over the interior columns of the x-updated values and the y-update.
+  void stepgrid_dimSplit(double* q, double* fm, double* fp, double* gm, double* gp, int mitot, int mjtot, int mbc,
+                         double dt, double& dtnew, double dx, double dy, const double* aux, double& cflgrid_out) {
+    const int mx = mitot - 2 * mbc, my = mjtot - 2 * mbc, meqn = nvar, maux = naux;
+    const int maxm = std::max(mx, my);
+    const size_t nf = (size_t)meqn * mitot * mjtot;
+    auto at = [&](int i, int j) { return (size_t)(i + mbc - 1) + (size_t)mitot * (j + mbc - 1); };
+    auto Q = [&](int m, int i, int j) -> double& { return q[(m - 1) + meqn * at(i, j)]; };
+    auto F = [&](double* f, int m, int i, int j) -> double& { return f[(m - 1) + meqn * at(i, j)]; };
+    auto A = [&](int m, int i, int j) { return aux[(m - 1) + maux * at(i, j)]; };
+    Work1d W;
+    W.ensure(maxm, mbc, meqn, mwaves, maux);
+    const int base = 1 - mbc;
+    auto fa = [&](std::vector<double>& v, int m, int i) { return v[(m - 1) + meqn * (i - base)]; };
+    double cfl_grid = 0.0;
+    // step2x.f90
+    double cflx = 0.0;
+    const double dtdx = dt / dx, dtdy = dt / dy;
+    std::fill(fm, fm + nf, 0.0);
+    std::fill(fp, fp + nf, 0.0);
+    for (int j = 1 - mbc; j <= my + mbc; ++j) {
+      for (int i = 1 - mbc; i <= mx + mbc; ++i) for (int m = 1; m <= meqn; ++m) W.q1d[(m - 1) + meqn * (i - base)] = Q(m, i, j);
+      if (mcapa > 0) { for (int i = 1 - mbc; i <= mx + mbc; ++i) W.dtdx1d[i - base] = dtdx / A(mcapa, i, j); }
+      else std::fill(W.dtdx1d.begin(), W.dtdx1d.end(), dtdx);
+      if (maux > 0)
+        for (int i = 1 - mbc; i <= mx + mbc; ++i)
+          for (int m = 1; m <= maux; ++m) W.aux2[(m - 1) + maux * (i - base)] = A(m, i, j);
+      double cfl1d;
+      flux2_dimSplit(1, maxm, meqn, maux, mbc, mx, W, cfl1d);
+      cflx = std::max(cflx, cfl1d);
+      for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 1; m <= meqn; ++m) {
+          F(fm, m, i, j) = F(fm, m, i, j) + fa(W.faddm, m, i);
+          F(fp, m, i, j) = F(fp, m, i, j) + fa(W.faddp, m, i);
+        }
+    }
+    cfl_grid = std::max(cfl_grid, cflx);
+    for (int j = 1 - mbc; j <= my + mbc; ++j)
+      for (int i = 1; i <= mx; ++i)
+        for (int m = 1; m <= meqn; ++m) {
+          if (mcapa == 0) Q(m, i, j) = Q(m, i, j) - dtdx * (F(fm, m, i + 1, j) - F(fp, m, i, j));
+          else Q(m, i, j) = Q(m, i, j) - dtdx * (F(fm, m, i + 1, j) - F(fp, m, i, j)) / A(mcapa, i, j);
+        }
+    // step2y.f90
+    double cfly = 0.0;
+    std::fill(gm, gm + nf, 0.0);
+    std::fill(gp, gp + nf, 0.0);
+    for (int i = 1; i <= mx; ++i) {
+      for (int j = 1 - mbc; j <= my + mbc; ++j) for (int m = 1; m <= meqn; ++m) W.q1d[(m - 1) + meqn * (j - base)] = Q(m, i, j);
+      if (mcapa > 0) { for (int j = 1 - mbc; j <= my + mbc; ++j) W.dtdx1d[j - base] = dtdy / A(mcapa, i, j); }
+      else std::fill(W.dtdx1d.begin(), W.dtdx1d.end(), dtdy);
+      if (maux > 0)
+        for (int j = 1 - mbc; j <= my + mbc; ++j)
+          for (int m = 1; m <= maux; ++m) W.aux2[(m - 1) + maux * (j - base)] = A(m, i, j);
+      double cfl1d;
+      flux2_dimSplit(2, maxm, meqn, maux, mbc, my, W, cfl1d);
+      cfly = std::max(cfly, cfl1d);
+      for (int j = 1; j <= my + 1; ++j)
+        for (int m = 1; m <= meqn; ++m) {
+          F(gm, m, i, j) = F(gm, m, i, j) + fa(W.faddm, m, j);
+          F(gp, m, i, j) = F(gp, m, i, j) + fa(W.faddp, m, j);
+        }
+    }
+    cfl_grid = std::max(cfl_grid, cfly);
+    for (int j = 1; j <= my; ++j)
+      for (int i = 1; i <= mx; ++i)
+        for (int m = 1; m <= meqn; ++m) {
+          if (mcapa == 0) Q(m, i, j) = Q(m, i, j) - dtdy * (F(gm, m, i, j + 1) - F(gp, m, i, j));
+          else Q(m, i, j) = Q(m, i, j) - dtdy * (F(gm, m, i, j + 1) - F(gp, m, i, j)) / A(mcapa, i, j);
+        }
+    // the level's Courant number decides dtnew (stepgrid_dimSplit.f:171-179); per grid, its
+    // own maximum gives the same level minimum
+    cflgrid_out = cfl_grid;
+    if (cfl_grid > 0.0) dtnew = dt * cfl / cfl_grid;
     else dtnew = RINFINITY;
   }
 
@@ -1054,8 +1172,13 @@ struct Amr2 {
     if (!gauges.empty()) update_gauges(g.q1.data(), xlow, ylow, mitot, mjtot, mptr);
     const size_t nf = (size_t)nvar * mitot * mjtot;
     std::vector<double> fm(nf), fp(nf), gm(nf), gp(nf);
-    stepgrid(g.q1.data(), fm.data(), fp.data(), gm.data(), gp.data(), mitot, mjtot, nghost, delt, dtnew, hx, hy,
-             g.aux.data(), cflgrid);
+    // advanc.f:256-270: unsplit or Godunov-split step
+    if (dimensional_split == 0)
+      stepgrid(g.q1.data(), fm.data(), fp.data(), gm.data(), gp.data(), mitot, mjtot, nghost, delt, dtnew, hx, hy,
+               g.aux.data(), cflgrid);
+    else
+      stepgrid_dimSplit(g.q1.data(), fm.data(), fp.data(), gm.data(), gp.data(), mitot, mjtot, nghost, delt, dtnew, hx,
+                        hy, g.aux.data(), cflgrid);
     if (g.has_cfl) fluxsv(mptr, fm.data(), fp.data(), gm.data(), gp.data(), mitot, mjtot, delt, hx, hy);
     if (g.has_ffl) {
       const int lenbc = 2 * (nxg / intratx[level - 1] + nyg / intraty[level - 1]);

@@ -182,7 +182,8 @@ struct Amr3 {
     yperdom = (mthbc[3] == 2 && mthbc[4] == 2);
     zperdom = (mthbc[5] == 2 && mthbc[6] == 2);
     if (xperdom || yperdom || zperdom) throw std::runtime_error("periodic boundaries are not supported in 3D");
-    if (dimensional_split != 0) throw std::runtime_error("dimensional splitting is not supported");
+    // amr3.f90:241-246: Godunov splitting (1) only; Strang splitting stops the reference
+    if (dimensional_split > 1) throw std::runtime_error("Strang splitting is not supported (amrclaw stops)");
     if (method[3] < 0) throw std::runtime_error("transverse_waves < 0 (dimensional splitting) is not supported");
     if (mcapa != 0) throw std::runtime_error("capacity functions are not supported in 3D");
     mxnest = a.i("amr_levels_max");
@@ -683,6 +684,138 @@ struct Amr3 {
             }
           }
       }
+  }
+
+  // flux3_dimSplit.f:4-260: the normal fluctuations, limiter and second-order correction of
+  // one pencil, without transverse terms: faddm = amdq, faddp = -apdq, both + cqxx
+  void flux3_dimSplit(int ixyz, int meqn, int mbc, int mx, Pencil& W, double& cfl1d) {
+    const int base = W.base;
+    Slice q1d = W.sl(W.q1d);
+    auto dtdx1d = [&](int i) -> double { return W.dtdx1d[i - base]; };
+    Slice aux2c{W.aux2.data() + (size_t)W.maux * W.L, W.maux, base};  // aux2(:, :, 2): the pencil's own aux
+    Slice faddm = W.sl(W.faddm), faddp = W.sl(W.faddp);
+    Waves wave{W.wave.data(), meqn, mwaves, base};
+    Slice s{W.s.data(), mwaves, base};
+    bool limit = false;
+    for (int mw = 1; mw <= mwaves; ++mw) if (mthlim[mw - 1] > 0) limit = true;
+    for (int m = 1; m <= meqn; ++m)
+      for (int i = 1 - mbc; i <= mx + mbc; ++i) { faddm(m, i) = 0.0; faddp(m, i) = 0.0; }
+    // rpn3 writes amdq into faddm and apdq into faddp (flux3_dimSplit.f:150-160)
+    rpn3(prob, ixyz, meqn, mwaves, mbc, mx, q1d, q1d, aux2c, aux2c, wave, s, faddm, faddp);
+    for (int i = 1; i <= mx + 1; ++i)
+      for (int m = 1; m <= meqn; ++m) faddp(m, i) = -faddp(m, i);
+    cfl1d = 0.0;
+    for (int mw = 1; mw <= mwaves; ++mw)
+      for (int i = 1; i <= mx + 1; ++i)
+        cfl1d = std::max(cfl1d, std::max(dtdx1d(i) * s(mw, i), -dtdx1d(i - 1) * s(mw, i)));
+    if (method[2] == 1) return;
+    if (limit) limiter(meqn, mx, wave, s);
+    for (int i = 1; i <= mx + 1; ++i) {
+      const double dtdxave = 0.5 * (dtdx1d(i - 1) + dtdx1d(i));
+      for (int m = 1; m <= meqn; ++m) {
+        double cqxx = 0.0;
+        for (int mw = 1; mw <= mwaves; ++mw) {
+          const double sg = use_fwaves ? dsign(1.0, s(mw, i)) : std::fabs(s(mw, i));
+          cqxx = cqxx + 0.5 * sg * (1.0 - std::fabs(s(mw, i)) * dtdxave) * wave(m, mw, i);
+        }
+        faddm(m, i) = faddm(m, i) + cqxx;
+        faddp(m, i) = faddp(m, i) + cqxx;
+      }
+    }
+  }
+
+  // stepgrid_dimSplit.f:4-264 with step3x.f / step3y.f / step3z.f: Godunov splitting. x-sweeps
+  // over every (j, k) pencil of the enlarged patch and the x-update of their interior cells;
+  // y-sweeps over the interior i, every k, of the x-updated values and the y-update of the
+  // interior j; z-sweeps over the interior (i, j) and the z-update of the interior cells.
+  void stepgrid_dimSplit(double* q, double* fm, double* fp, double* gm, double* gp, double* hm, double* hp, int mitot,
+                         int mjtot, int mktot, double dt, double& dtnew, double dx, double dy, double dz, const double* aux,
+                         double& cflgrid_out) {
+    const int mbc = nghost, meqn = nvar, maux = naux;
+    const int mx = mitot - 2 * mbc, my = mjtot - 2 * mbc, mz = mktot - 2 * mbc;
+    const int maxm = std::max(mx, std::max(my, mz));
+    auto at = [&](int i, int j, int k) { return (size_t)(i + mbc - 1) + (size_t)mitot * ((size_t)(j + mbc - 1) + (size_t)mjtot * (k + mbc - 1)); };
+    auto Q = [&](int m, int i, int j, int k) -> double& { return q[(m - 1) + (size_t)meqn * at(i, j, k)]; };
+    auto A = [&](int m, int i, int j, int k) { return aux[(m - 1) + (size_t)maux * at(i, j, k)]; };
+    auto F = [&](double* f, int m, int i, int j, int k) -> double& { return f[(m - 1) + (size_t)meqn * at(i, j, k)]; };
+    Pencil W;
+    W.init(maxm, mbc, meqn, mwaves, maux);
+    const int base = W.base;
+    auto fa = [&](std::vector<double>& v, int m, int i) { return v[(m - 1) + (size_t)meqn * (i - base)]; };
+    auto pencil_in = [&](int n, double dtdn, auto qat, auto aat) {
+      for (int x = 1 - mbc; x <= n + mbc; ++x)
+        for (int m = 1; m <= meqn; ++m) W.q1d[(m - 1) + (size_t)meqn * (x - base)] = qat(m, x);
+      std::fill(W.dtdx1d.begin(), W.dtdx1d.end(), dtdn);
+      if (maux > 0)
+        for (int x = 1 - mbc; x <= n + mbc; ++x)
+          for (int ma = 1; ma <= maux; ++ma) W.aux2[(ma - 1) + (size_t)W.maux * ((x - base) + (size_t)W.L)] = aat(ma, x);
+    };
+    const size_t nf = (size_t)meqn * mitot * mjtot * mktot;
+    double cfl_grid = 0.0;
+    const double dtdx = dt / dx, dtdy = dt / dy, dtdz = dt / dz;
+    // step3x.f
+    std::fill(fm, fm + nf, 0.0); std::fill(fp, fp + nf, 0.0);
+    double cflx = 0.0;
+    for (int k = 1 - mbc; k <= mz + mbc; ++k)
+      for (int j = 1 - mbc; j <= my + mbc; ++j) {
+        pencil_in(mx, dtdx, [&](int m, int x) { return Q(m, x, j, k); }, [&](int ma, int x) { return A(ma, x, j, k); });
+        double cfl1d;
+        flux3_dimSplit(1, meqn, mbc, mx, W, cfl1d);
+        cflx = std::max(cflx, cfl1d);
+        for (int i = 1; i <= mx + 1; ++i)
+          for (int m = 1; m <= meqn; ++m) {
+            F(fm, m, i, j, k) = F(fm, m, i, j, k) + fa(W.faddm, m, i);
+            F(fp, m, i, j, k) = F(fp, m, i, j, k) + fa(W.faddp, m, i);
+          }
+      }
+    cfl_grid = std::max(cfl_grid, cflx);
+    for (int k = 1 - mbc; k <= mz + mbc; ++k)
+      for (int j = 1 - mbc; j <= my + mbc; ++j)
+        for (int i = 1; i <= mx; ++i)
+          for (int m = 1; m <= meqn; ++m) Q(m, i, j, k) = Q(m, i, j, k) - dtdx * (F(fm, m, i + 1, j, k) - F(fp, m, i, j, k));
+    // step3y.f
+    std::fill(gm, gm + nf, 0.0); std::fill(gp, gp + nf, 0.0);
+    double cfly = 0.0;
+    for (int k = 1 - mbc; k <= mz + mbc; ++k)
+      for (int i = 1; i <= mx; ++i) {
+        pencil_in(my, dtdy, [&](int m, int x) { return Q(m, i, x, k); }, [&](int ma, int x) { return A(ma, i, x, k); });
+        double cfl1d;
+        flux3_dimSplit(2, meqn, mbc, my, W, cfl1d);
+        cfly = std::max(cfly, cfl1d);
+        for (int j = 1; j <= my + 1; ++j)
+          for (int m = 1; m <= meqn; ++m) {
+            F(gm, m, i, j, k) = F(gm, m, i, j, k) + fa(W.faddm, m, j);
+            F(gp, m, i, j, k) = F(gp, m, i, j, k) + fa(W.faddp, m, j);
+          }
+      }
+    cfl_grid = std::max(cfl_grid, cfly);
+    for (int k = 1 - mbc; k <= mz + mbc; ++k)
+      for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i)
+          for (int m = 1; m <= meqn; ++m) Q(m, i, j, k) = Q(m, i, j, k) - dtdy * (F(gm, m, i, j + 1, k) - F(gp, m, i, j, k));
+    // step3z.f
+    std::fill(hm, hm + nf, 0.0); std::fill(hp, hp + nf, 0.0);
+    double cflz = 0.0;
+    for (int j = 1; j <= my; ++j)
+      for (int i = 1; i <= mx; ++i) {
+        pencil_in(mz, dtdz, [&](int m, int x) { return Q(m, i, j, x); }, [&](int ma, int x) { return A(ma, i, j, x); });
+        double cfl1d;
+        flux3_dimSplit(3, meqn, mbc, mz, W, cfl1d);
+        cflz = std::max(cflz, cfl1d);
+        for (int k = 1; k <= mz + 1; ++k)
+          for (int m = 1; m <= meqn; ++m) {
+            F(hm, m, i, j, k) = F(hm, m, i, j, k) + fa(W.faddm, m, k);
+            F(hp, m, i, j, k) = F(hp, m, i, j, k) + fa(W.faddp, m, k);
+          }
+      }
+    cfl_grid = std::max(cfl_grid, cflz);
+    for (int k = 1; k <= mz; ++k)
+      for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i)
+          for (int m = 1; m <= meqn; ++m) Q(m, i, j, k) = Q(m, i, j, k) - dtdz * (F(hm, m, i, j, k + 1) - F(hp, m, i, j, k));
+    cflgrid_out = cfl_grid;
+    if (cfl_grid > 0.0) dtnew = dt * cfl / cfl_grid;
+    else dtnew = RINFINITY3;
   }
 
   // stepgrid.f:4-236 ; returns dtnew through the argument and the grid's Courant number
@@ -1392,8 +1525,13 @@ struct Amr3 {
     const size_t n = qsize(mptr);
     std::vector<double> fm(n), fp(n), gm(n), gp(n), hm(n), hp(n);
     if (naux > 0) b4step3(nx, ny, nz, g.xlo, g.ylo, g.zlo, hx, hy, hz, g.time, g.aux.data());
-    stepgrid(g.q1.data(), fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mitot, mjtot, mktot, delt, dtnew, hx, hy, hz,
-             g.aux.data(), cflgrid);
+    // src/3d/advanc.f:261-280: unsplit or Godunov-split step
+    if (dimensional_split == 0)
+      stepgrid(g.q1.data(), fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mitot, mjtot, mktot, delt, dtnew, hx,
+               hy, hz, g.aux.data(), cflgrid);
+    else
+      stepgrid_dimSplit(g.q1.data(), fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mitot, mjtot, mktot, delt,
+                        dtnew, hx, hy, hz, g.aux.data(), cflgrid);
     if (g.has_cfl) fluxsv(mptr, fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), mitot, mjtot, mktot, delt, hx, hy, hz);
     if (g.has_ffl)
       fluxad(fm.data(), fp.data(), gm.data(), gp.data(), hm.data(), hp.data(), g.ffl.data(), mitot, mjtot, mktot, intratx[level - 1],

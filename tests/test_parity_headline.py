@@ -56,7 +56,7 @@ def test_euler3d_blast_full_size_twelve_coarse_steps():
     gpu, ref = _compare(rd, 3, cycles=12)
     assert gpu["info"]["coarse_steps"] == 12
     levels = ref["grids"][:, 1]
-    assert (levels == 3).any() and (levels == 2).sum() > 1
+    assert (levels == 2).any() and (levels == 3).sum() > 1
 
 
 def test_euler2d_quadrants_full_size_whole_run():
