@@ -143,7 +143,6 @@ struct Plan3 {
 };
 
 // a flagged cell (1-based level indices); the reference stores its centre (i-.5, j-.5, k-.5)
-struct FlagPt { int c[3]; };
 
 // read-only view of a level int8 array (the nesting domain read back for nestck.f)
 struct LvlView {
@@ -1751,7 +1750,10 @@ class Amr3Gpu : public AmrSolver {
   // setflags.f), bufnst.f (+ projec.f, shiftset.f) and colate.f. The arrays live in device
   // memory; one read-back returns the flags (for the ordered point list) and the nesting
   // domain (for nestck.f). Returns the flagged cells in (k, j, i) order.
-  void flglvl(int lcheck, int lbase, std::vector<FlagPt>& badpts, LvlView& dom) {
+  // flglvl.f on the device: the level's flag array (lv_b) with buffering and nesting
+  // applied (colate.f); only the nesting-domain array comes back to the host (nestck.f
+  // reads it). The clusters are then found from device signatures (cluster_on_device).
+  void flglvl(int lcheck, int lbase, LvlView& dom) {
     PhaseTimer tph(hprof);
     tph.next("flg_device");
     const LvlDims d0{iregsz[lbase], jregsz[lbase], kregsz[lbase]};
@@ -1815,58 +1817,94 @@ class Amr3Gpu : public AmrSolver {
     launch_bufnst3(lv_b.d, dl, lv_proj.d, (int)proj.size(), p.ibuff, lv_t1.d, lv_t2.d, st);
     launch_colate3(lv_b.d, lv_n.d, dl, st);
     nkernels += 20;
-    if (lv_host_cap < 2 * need) {
+    if (lv_host_cap < need) {
       if (lv_host) AMR_CUDA(cudaFreeHost(lv_host));
-      lv_host_cap = 2 * need;
+      lv_host_cap = need;
       AMR_CUDA(cudaMallocHost((void**)&lv_host, lv_host_cap));
     }
-    AMR_CUDA(cudaMemcpyAsync(lv_host, lv_b.d, need, cudaMemcpyDeviceToHost, st));
-    AMR_CUDA(cudaMemcpyAsync(lv_host + need, lv_n.d, need, cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaMemcpyAsync(lv_host, lv_n.d, need, cudaMemcpyDeviceToHost, st));
+    lv_dims = dl;
     tph.next("flg_sync");
     sync_stream();
     if (p.flag_richardson) richardson_release();
-    tph.next("flg_points");
-    dom = LvlView{lv_host + need, dl};
-    badpts.clear();
-    const int8_t* F = lv_host;
-    for (int k = 1; k <= dl.ks; ++k)
-      for (int j = 1; j <= dl.js; ++j) {
-        const int8_t* row = F + dl.at(0, j, k);
-        int i = 1;
-        while (i <= dl.is) {
-          if (i + 8 <= dl.is + 1) {
-            uint64_t w;
-            std::memcpy(&w, row + i, 8);
-            if (w == 0) { i += 8; continue; }
-          }
-          if (row[i] != 0) badpts.push_back(FlagPt{{i, j, k}});
-          ++i;
-        }
-      }
+    dom = LvlView{lv_host, dl};
   }
 
   // ---------------------------------------------------------------- clustering
-  // A flagged point of the reference is the cell centre (i-.5, j-.5, k-.5) in units of the
-  // level's cells (colate.f). The routines below keep the integer cell index instead; every
-  // comparison the reference makes on the centres is the same comparison on the indices
-  // (c - .5 < m - .5  <=>  c < m), and every decision depends only on the set of points in
-  // a cluster (histograms, minima, maxima, cut predicates), never on their order.
-
-  // moment.f:4-70: bounding box (rect: ilo, ihi, jlo, jhi, klo, khi, 0-based) and efficiency
-  static void moment(int rect[6], const FlagPt* p, int n, double& usage) {
-    int lo[3] = {p[0].c[0], p[0].c[1], p[0].c[2]}, hi[3] = {lo[0], lo[1], lo[2]};
-    for (int q = 1; q < n; ++q)
-      for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], p[q].c[d]); hi[d] = std::max(hi[d], p[q].c[d]); }
-    for (int d = 0; d < 3; ++d) { rect[2 * d] = lo[d] - 1; rect[2 * d + 1] = hi[d] - 1; }
-    const int gpall = (rect[1] - rect[0] + 1) * (rect[3] - rect[2] + 1) * (rect[5] - rect[4] + 1);
-    usage = (double)n / gpall;
+  // Berger-Rigoutsos bisection (smartbis.f:25-177, signs.f:4-86, findcut.f:4-198,
+  // moment.f:4-70) driven by signatures made on the device: a cluster is a box of the
+  // level's flag array, its points the flagged cells inside. Each wave of the bisection
+  // sends the boxes of all undecided clusters to the device, which counts the flagged
+  // cells per i, per j and per k of every box (launch_signatures3); only those counts come
+  // back. From them the host takes the cluster's point count and bounding box (moment.f:
+  // the first and last non-zero count per axis), its efficiency, and the cut (findcut.f).
+  // A point of the reference is the cell centre (i-.5, j-.5, k-.5); every comparison it
+  // makes on centres is the same comparison on the integer indices, and every decision
+  // depends only on the counts, so the clusters are the reference's.
+  struct Clu3 {
+    SigBox box;   // where its points lie (a sub-box of its parent's bounding box)
+    int n = 0;    // points
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // bounding box of the points (moment.f)
+  };
+  DBuf<SigBox> sig_boxes;
+  DBuf<int> sig_off, sig_hist;
+  LvlDims lv_dims{0, 0, 0};
+  // signs.f on the device for the boxes of clus; fills n, lo, hi of each; scr (optional)
+  // receives each cluster's counts per axis at their level indices (0..dims+1)
+  void signatures(std::vector<Clu3>& clus, std::vector<std::array<std::vector<int>, 3>>* scr) {
+    const int nb = (int)clus.size();
+    if (nb == 0) return;
+    std::vector<SigBox> bx(nb);
+    std::vector<int> off(nb + 1, 0);
+    int maxlen = 0;
+    long long maxvol = 0;
+    for (int b = 0; b < nb; ++b) {
+      bx[b] = clus[b].box;
+      const int len = (bx[b].hi[0] - bx[b].lo[0] + 1) + (bx[b].hi[1] - bx[b].lo[1] + 1) + (bx[b].hi[2] - bx[b].lo[2] + 1);
+      off[b + 1] = off[b] + len;
+      maxlen = std::max(maxlen, len);
+      maxvol = std::max(maxvol, (long long)(bx[b].hi[0] - bx[b].lo[0] + 1) * (bx[b].hi[1] - bx[b].lo[1] + 1) * (bx[b].hi[2] - bx[b].lo[2] + 1));
+    }
+    sig_boxes.upload(bx, st, stg);
+    sig_off.upload(off, st, stg);
+    sig_hist.reserve((size_t)off[nb]);
+    launch_signatures3(lv_b.d, lv_dims, sig_boxes.d, nb, sig_off.d, off[nb], maxlen, maxvol, sig_hist.d, st);
+    ++nkernels;
+    std::vector<int> h((size_t)off[nb]);
+    AMR_CUDA(cudaMemcpyAsync(h.data(), sig_hist.d, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    const int dims[3] = {lv_dims.is, lv_dims.js, lv_dims.ks};
+    if (scr) scr->assign(nb, {});
+    for (int b = 0; b < nb; ++b) {
+      Clu3& c = clus[b];
+      const int* hh = h.data() + off[b];
+      c.n = 0;
+      for (int d = 0; d < 3; ++d) {
+        const int len = c.box.hi[d] - c.box.lo[d] + 1;
+        int first = -1, last = -1, sum = 0;
+        for (int t = 0; t < len; ++t)
+          if (hh[t]) { if (first < 0) first = t; last = t; sum += hh[t]; }
+        if (d == 0) c.n = sum;
+        c.lo[d] = first < 0 ? c.box.lo[d] : c.box.lo[d] + first;
+        c.hi[d] = last < 0 ? c.box.hi[d] : c.box.lo[d] + last;
+        if (scr) {
+          std::vector<int>& v = (*scr)[b][d];
+          v.assign(dims[d] + 2, 0);
+          for (int t = 0; t < len; ++t) v[c.box.lo[d] + t] = hh[t];
+        }
+        hh += len;
+      }
+    }
   }
-  // signs.f + findcut.f: a hole in the signature, else the largest Laplacian sign change
-  static void findcut(const FlagPt* p, int n, const int dims[3], int& index, int& iside) {
-    std::vector<int> scr[3];
-    for (int d = 0; d < 3; ++d) scr[d].assign(dims[d] + 2, 0);
-    for (int q = 0; q < n; ++q)
-      for (int d = 0; d < 3; ++d) scr[d][p[q].c[d]] += 1;
+  // moment.f:4-70: bounding box (rect: ilo, ihi, jlo, jhi, klo, khi, 0-based) and efficiency
+  static void moment(int rect[6], const Clu3& c, double& usage) {
+    for (int d = 0; d < 3; ++d) { rect[2 * d] = c.lo[d] - 1; rect[2 * d + 1] = c.hi[d] - 1; }
+    const int gpall = (rect[1] - rect[0] + 1) * (rect[3] - rect[2] + 1) * (rect[5] - rect[4] + 1);
+    usage = (double)c.n / gpall;
+  }
+  // findcut.f on a cluster's signatures scr (counts at level indices 0..dims+1): a hole in
+  // a signature, else the largest Laplacian sign change (ties to the middle)
+  static void findcut(std::array<std::vector<int>, 3>& scr, const int dims[3], int& index, int& iside) {
     int lo[3], hi[3];
     for (int d = 0; d < 3; ++d) {
       lo[d] = 1; hi[d] = dims[d];
@@ -1902,35 +1940,61 @@ class Amr3Gpu : public AmrSolver {
     iside = lv[0][1];
     if (lv[0][0] < 2) index = 0;
   }
-  // smartbis.f: bisect until every cluster's efficiency reaches cutoff or it has no cut.
-  // The reference keeps the cluster at or above the cut first (smartbis.f swaps the
-  // points below it to the bottom), so clusters come out in depth-first order, upper part
-  // first. Large independent halves are clustered on other threads.
-  static void smartbis_rec(FlagPt* p, int n, double cutoff, const int dims[3], std::vector<int>& counts, int depth) {
-    int rect[6];
-    double usenew;
-    moment(rect, p, n, usenew);
-    int index = 0, iside = 0;
-    if (usenew < cutoff) findcut(p, n, dims, index, iside);
-    if (usenew >= cutoff || index == 0) { counts.push_back(n); return; }
-    const int d = iside - 1;
-    FlagPt* mid = std::partition(p, p + n, [&](const FlagPt& q) { return q.c[d] >= index; });
-    const int n1 = (int)(mid - p);
-    if (depth < 4 && n > 20000) {
-      std::vector<int> right;
-      auto fut = std::async(std::launch::async, [&] { smartbis_rec(mid, n - n1, cutoff, dims, right, depth + 1); });
-      smartbis_rec(p, n1, cutoff, dims, counts, depth + 1);
-      fut.get();
-      counts.insert(counts.end(), right.begin(), right.end());
-    } else {
-      smartbis_rec(p, n1, cutoff, dims, counts, depth + 1);
-      smartbis_rec(mid, n - n1, cutoff, dims, counts, depth + 1);
+  // smartbis.f: bisect until every cluster's efficiency reaches cutoff or it has no cut;
+  // breadth first (one signature wave per depth), then the leaves in the reference's
+  // depth-first order: the part at or above the cut before the part below it
+  std::vector<Clu3> cluster_on_device(double cutoff) {
+    const int dims[3] = {lv_dims.is, lv_dims.js, lv_dims.ks};
+    struct Node { Clu3 c; int child = -1; };  // child: the upper part; child+1 the lower part
+    std::vector<Node> T(1);
+    T[0].c.box = SigBox{{1, 1, 1}, {dims[0], dims[1], dims[2]}};
+    std::vector<int> wave{0};
+    std::vector<std::array<std::vector<int>, 3>> scr;
+    while (!wave.empty()) {
+      std::vector<Clu3> cl(wave.size());
+      for (size_t w = 0; w < wave.size(); ++w) cl[w] = T[wave[w]].c;
+      signatures(cl, &scr);
+      std::vector<int> next;
+      for (size_t w = 0; w < wave.size(); ++w) {
+        T[wave[w]].c = cl[w];
+        const Clu3& c = cl[w];
+        if (c.n == 0) continue;  // only the whole array of a level without flags
+        int rect[6];
+        double usenew;
+        moment(rect, c, usenew);
+        int index = 0, iside = 0;
+        if (usenew < cutoff) findcut(scr[w], dims, index, iside);
+        if (usenew >= cutoff || index == 0) continue;
+        const int d = iside - 1;
+        Clu3 up, dn;
+        up.box = dn.box = SigBox{{c.lo[0], c.lo[1], c.lo[2]}, {c.hi[0], c.hi[1], c.hi[2]}};
+        up.box.lo[d] = index;
+        dn.box.hi[d] = index - 1;
+        const int id = (int)T.size();
+        T[wave[w]].child = id;
+        T.push_back(Node{up, -1});
+        T.push_back(Node{dn, -1});
+        next.push_back(id);
+        next.push_back(id + 1);
+      }
+      wave.swap(next);
     }
+    std::vector<Clu3> leaves;
+    if (T[0].c.n == 0) return leaves;
+    std::vector<int> stack{0};
+    while (!stack.empty()) {
+      const int id = stack.back();
+      stack.pop_back();
+      if (T[id].child < 0) { leaves.push_back(T[id].c); continue; }
+      stack.push_back(T[id].child + 1);  // lower part after
+      stack.push_back(T[id].child);      // upper part first
+    }
+    return leaves;
   }
   // nestck.f: a new grid must lie in the nesting domain of its base; otherwise split its
-  // points at the middle of its longest side (points below the middle first) and retry
-  bool nestck(int mnew, int lbase, std::vector<FlagPt>& bp, int ibase, int npts, std::vector<int>& numptc, int icl, int& nclust,
-              const LvlView& dom) {
+  // points at the middle of its longest side (points with centre below the middle first)
+  // and retry: clus[icl] becomes the lower part and the upper part follows it
+  bool nestck(int mnew, int lbase, std::vector<Clu3>& clus, int icl, const LvlView& dom) {
     if (lbase == 1) return true;
     const HPatch3& n = node[mnew];
     const int lev = n.level;
@@ -1941,58 +2005,55 @@ class Amr3Gpu : public AmrSolver {
         for (int i = n.ilo / rx + 1; i <= n.ihi / rx + 1; ++i)
           if (dom(i, j, k) == 0) { nested = false; break; }
     if (nested) return true;
-    if (npts <= 1) throw std::runtime_error("nestck: a single point cannot be properly nested");
+    if (clus[icl].n <= 1) throw std::runtime_error("nestck: a single point cannot be properly nested");
     double sidemx = std::max(n.xhi - n.xlo, n.yhi - n.ylo);
     sidemx = std::max(sidemx, n.zhi - n.zlo);
     double rmid; int d;
     if (n.xhi - n.xlo >= sidemx) { rmid = (double)(float)((n.ihi + n.ilo + 1) / 2.f); rmid = rmid / rx; d = 0; }
     else if (n.yhi - n.ylo >= sidemx) { rmid = (double)(float)((n.jhi + n.jlo + 1) / 2.f); rmid = rmid / ry; d = 1; }
     else { rmid = (double)(float)((n.khi + n.klo + 1) / 2.f); rmid = rmid / rz; d = 2; }
-    FlagPt* p = bp.data() + ibase;
-    const int ntop = (int)(std::partition(p, p + npts, [&](const FlagPt& q) { return (double)q.c[d] - .5 < rmid; }) - p);
-    numptc[icl] = ntop;
-    numptc.insert(numptc.begin() + icl + 1, npts - ntop);
-    nclust = nclust + 1;
+    // the largest index whose centre lies below rmid
+    const Clu3 c = clus[icl];
+    int cut = c.lo[d] - 1;
+    for (int t = c.lo[d]; t <= c.hi[d]; ++t) if ((double)t - .5 < rmid) cut = t;
+    std::vector<Clu3> parts(2);
+    parts[0].box = parts[1].box = SigBox{{c.lo[0], c.lo[1], c.lo[2]}, {c.hi[0], c.hi[1], c.hi[2]}};
+    parts[0].box.hi[d] = cut;
+    parts[1].box.lo[d] = cut + 1;
+    signatures(parts, nullptr);
+    clus[icl] = parts[0];
+    clus.insert(clus.begin() + icl + 1, parts[1]);
     return false;
   }
   // grdfit.f
   void grdfit(int lbase, int lcheck, double t) {
-    std::vector<FlagPt> bp;
     LvlView i1flags{nullptr, LvlDims{0, 0, 0}};
     {
       HPROF("flglvl3");
-      flglvl(lcheck, lbase, bp, i1flags);
+      flglvl(lcheck, lbase, i1flags);
     }
-    const int npts = (int)bp.size();
-    if (npts == 0) return;
     HPROF("cluster3");
+    std::vector<Clu3> clus = cluster_on_device(p.cut);
+    if (clus.empty()) return;
     const int levnew = lcheck + 1;
     const double hxf = hxposs[levnew], hyf = hyposs[levnew], hzf = hzposs[levnew];
-    std::vector<int> counts;
-    const int dims[3] = {iregsz[lcheck], jregsz[lcheck], kregsz[lcheck]};
-    smartbis_rec(bp.data(), npts, p.cut, dims, counts, 0);
-    std::vector<int> numptc(1, 0);  // 1-based as in the reference
-    numptc.insert(numptc.end(), counts.begin(), counts.end());
-    int nclust = (int)counts.size();
-    int ibase = 0, icl = 1, prv = 0;
-    while (icl <= nclust) {
+    int prv = 0;
+    for (size_t icl = 0; icl < clus.size(); ++icl) {
       const int mnew = nodget();
       while (true) {
         int rect[6]; double usage;
-        moment(rect, bp.data() + ibase, numptc[icl], usage);
+        moment(rect, clus[icl], usage);
         HPatch3& n = node[mnew];
         n.ilo = rect[0] * intratx[lcheck]; n.jlo = rect[2] * intraty[lcheck]; n.klo = rect[4] * intratz[lcheck];
         n.ihi = (rect[1] + 1) * intratx[lcheck] - 1; n.jhi = (rect[3] + 1) * intraty[lcheck] - 1; n.khi = (rect[5] + 1) * intratz[lcheck] - 1;
         n.xlo = n.ilo * hxf + xlower; n.ylo = n.jlo * hyf + ylower; n.zlo = n.klo * hzf + zlower;
         n.xhi = (n.ihi + 1) * hxf + xlower; n.yhi = (n.jhi + 1) * hyf + ylower; n.zhi = (n.khi + 1) * hzf + zlower;
         n.level = levnew; n.time = t;
-        if (nestck(mnew, lbase, bp, ibase, numptc[icl], numptc, icl, nclust, i1flags)) break;
+        if (nestck(mnew, lbase, clus, (int)icl, i1flags)) break;
       }
       if (newstl[levnew] == 0) newstl[levnew] = mnew;
       else node[prv].levelptr = mnew;
       prv = mnew;
-      ibase += numptc[icl];
-      ++icl;
     }
     birect(newstl[levnew]);
   }

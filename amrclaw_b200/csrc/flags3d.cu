@@ -308,6 +308,46 @@ void launch_colate3(int8_t* f, const int8_t* dom, LvlDims d, cudaStream_t s) {
   AMR_CUDA(cudaGetLastError());
 }
 
+// ======================================================================= signatures (signs.f)
+namespace {
+// The row / column / plane counts of the flagged cells (f != 0) of each box: blockIdx.y is
+// the box, blockIdx.x a slab of its cells; counts are made in shared memory and added to
+// the box's histograms (integer sums, so the order of the adds does not matter).
+__global__ void signatures3_kernel(const int8_t* f, LvlDims d, const SigBox* boxes, const int* off, int* hist) {
+  extern __shared__ int sh[];
+  const SigBox B = boxes[blockIdx.y];
+  const int ni = B.hi[0] - B.lo[0] + 1, nj = B.hi[1] - B.lo[1] + 1, nk = B.hi[2] - B.lo[2] + 1;
+  const int nh = ni + nj + nk;
+  for (int t = threadIdx.x; t < nh; t += blockDim.x) sh[t] = 0;
+  __syncthreads();
+  const long long vol = (long long)ni * nj * nk;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < vol; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % ni), j = (int)((t / ni) % nj), k = (int)(t / ((long long)ni * nj));
+    if (f[d.at(B.lo[0] + i, B.lo[1] + j, B.lo[2] + k)] != 0) {
+      atomicAdd(&sh[i], 1);
+      atomicAdd(&sh[ni + j], 1);
+      atomicAdd(&sh[ni + nj + k], 1);
+    }
+  }
+  __syncthreads();
+  int* h = hist + off[blockIdx.y];
+  for (int t = threadIdx.x; t < nh; t += blockDim.x)
+    if (sh[t]) atomicAdd(&h[t], sh[t]);
+}
+}  // namespace
+
+void launch_signatures3(const int8_t* f, LvlDims d, const SigBox* boxes, int nbox, const int* off, int total, int maxlen,
+                        long long maxvol, int* hist, cudaStream_t s) {
+  if (nbox <= 0) return;
+  AMR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t)total, s));
+  const int slabs = (int)std::max<long long>(1, std::min<long long>(64, (maxvol + 8191) / 8192));
+  for (int base = 0; base < nbox; base += 65535) {
+    const int cnt = std::min(65535, nbox - base);
+    signatures3_kernel<<<dim3(slabs, cnt), 256, sizeof(int) * (size_t)maxlen, s>>>(f, d, boxes + base, off + base, hist);
+  }
+  AMR_CUDA(cudaGetLastError());
+}
+
 // ======================================================================= Richardson estimation
 namespace {
 template <class T>

@@ -37,6 +37,14 @@ void launch_bufnst3(int8_t* f, LvlDims d, const LvlBox* proj, int nproj, int ibu
 // colate.f:4-78: f = min(f, dom) over the interior.
 void launch_colate3(int8_t* f, const int8_t* dom, LvlDims d, cudaStream_t s);
 
+// A cluster's box in the level array (1-based interior indices, inclusive).
+struct SigBox { int lo[3], hi[3]; };
+// signs.f:4-86: for every box, the counts of flagged cells (f != 0) per i, per j and per k
+// of the box: hist[off[b] .. +ni) per i, then nj per j, then nk per k. total: ints of
+// hist; maxlen: the largest ni+nj+nk; maxvol: the largest box volume.
+void launch_signatures3(const int8_t* f, LvlDims d, const SigBox* boxes, int nbox, const int* off, int total, int maxlen,
+                        long long maxvol, int* hist, cudaStream_t s);
+
 // Richardson estimation (errest.f, coarsen.f, errf1.f). vp[0..np): virtual patches of the
 // coarsened grids, vp[np..2np): those of the regular step (same index boxes as the grids).
 // coarsen.f:1-25: the 2x2x2 means of scratch rect rect_of[k] (twice the ghost width) into

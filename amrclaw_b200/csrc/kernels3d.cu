@@ -66,7 +66,10 @@ __device__ __forceinline__ T philim3(int meth, T r) {
 //            transverse terms of the apdq side (flux3.f: to cell i = e), stored
 //   phase B2 transverse terms of the amdq side (to cell i-1 = e-1), added to what B1
 //            stored for that cell, term by term in flux3.f's statement order
-constexpr int SW_T = 128;
+#ifndef SW_TILE
+#define SW_TILE 128  // interfaces per sweep tile (threads per block)
+#endif
+constexpr int SW_T = SW_TILE;
 constexpr int SW_OWN = SW_T - 3;
 #ifndef SW_MINB
 #define SW_MINB 3  // resident tiles per SM the register budget is sized for

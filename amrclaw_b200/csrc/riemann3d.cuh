@@ -57,23 +57,13 @@ __device__ __forceinline__ void euler3d_split(const Roe3T<T>& R, int mn, int mt1
   w[1][4] = a3 * T(0.5) * R.u2 + a2 * R.u[mt1] + a4 * R.u[mt2]; sp[1] = un;
   w[2][0] = a5; w[2][mn - 1] = a5 * (un + a); w[2][mt1 - 1] = a5 * R.u[mt1]; w[2][mt2 - 1] = a5 * R.u[mt2];
   w[2][4] = a5 * (R.enth + un * a); sp[2] = un + a;
-  // bm = sum_k min(s_k, 0) w_k and bp = sum_k max(s_k, 0) w_k, in k order (the CPU
-  // restatement's arithmetic). For finite waves a term whose factor is min(s_k,0) = +-0 or
-  // max(s_k,0) = +-0 is a signed zero, and adding a signed zero leaves these sums unchanged
-  // (they start at +0 and a round-to-nearest sum is never -0 after it), so such terms are
-  // skipped and s_k * w_k is formed once: the same bits with one product per term instead of
-  // two. A NaN speed still reaches both sums.
-  bool neg[3], pos[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) { neg[k] = !(sp[k] >= T(0)); pos[k] = !(sp[k] <= T(0)); }
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
     T am = T(0), ap = T(0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const T t = sp[k] * w[k][m];
-      if (neg[k]) am = am + t;
-      if (pos[k]) ap = ap + t;
+      am = am + dmin(sp[k], T(0)) * w[k][m];
+      ap = ap + dmax(sp[k], T(0)) * w[k][m];
     }
     bm[m] = am; bp[m] = ap;
   }
