@@ -17,6 +17,7 @@
 #include "kernels2d.cuh"
 #include "params.hpp"
 #include "cluster2d.hpp"
+#include "flags3d.cuh"
 #include "gridindex.hpp"
 #include "workpool.hpp"
 #include "noalloc2d.cuh"
@@ -1199,6 +1200,7 @@ class Amr2Gpu {
   };
   LevelGraph lgraph[12];
   bool use_graphs = false;
+  bool stepped = false;  // a level substep has run (store2 then holds the last step's input)
   long long plan_gen[12] = {0};
   long long graph_captures = 0, graph_replays = 0;
 
@@ -1364,6 +1366,7 @@ class Amr2Gpu {
     cfl_level = cmax;
     cflmax_run = std::max(cflmax_run, cmax);
     ++nsteps_launched;
+    stepped = true;
     (void)L;
     return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
   }
@@ -1435,6 +1438,7 @@ class Amr2Gpu {
     cfl_level = cmax;
     cflmax_run = std::max(cflmax_run, cmax);
     ++nsteps_launched;
+    stepped = true;
     return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
   }
 
@@ -1881,24 +1885,144 @@ class Amr2Gpu {
     return pts;
   }
 
+  // ---------------------------------------------------------------- clustering
+  // Berger-Rigoutsos bisection (smartbis.f:25-177, signs.f:16-71, findcut.f:7-130,
+  // moment.f:16-75) driven by signatures made on the device. The level's points (the
+  // buffered, nested, wrapped and deduplicated flags of flag_points) are scattered into a
+  // one-plane device array; a cluster is a box of it and its points the flagged cells
+  // inside. Each wave of the bisection sends the boxes of all undecided clusters to the
+  // device, which counts the points per i and per j of every box; only those counts come
+  // back, and the host takes from them the count, the bounding box, the efficiency and the
+  // cut. Every decision depends only on these counts, as the reference's do on its points.
+  struct Clu2 { SigBox box; int n = 0; int lo[2] = {0, 0}, hi[2] = {0, 0}; };
+  DBuf<int8_t> sig_mask;
+  DBuf<int> sig_pts, sig_off, sig_hist;
+  DBuf<SigBox> sig_boxes;
+  LvlDims sig_dims{0, 0, 1};
+  // signs.f on the device for the boxes of clus (1-based array indices = level index + 1);
+  // fills n, lo, hi; si / sj (optional): each cluster's counts at 1-based level positions
+  void signatures(std::vector<Clu2>& clus, std::vector<std::vector<int>>* si, std::vector<std::vector<int>>* sj) {
+    const int nb = (int)clus.size();
+    if (nb == 0) return;
+    std::vector<SigBox> bx(nb);
+    std::vector<int> off(nb + 1, 0);
+    int maxlen = 0;
+    long long maxvol = 0;
+    for (int b = 0; b < nb; ++b) {
+      bx[b] = clus[b].box;
+      const int ni = bx[b].hi[0] - bx[b].lo[0] + 1, nj = bx[b].hi[1] - bx[b].lo[1] + 1;
+      off[b + 1] = off[b] + ni + nj + 1;
+      maxlen = std::max(maxlen, ni + nj + 1);
+      maxvol = std::max(maxvol, (long long)ni * nj);
+    }
+    sig_boxes.upload(bx, st, stg);
+    sig_off.upload(off, st, stg);
+    sig_hist.ensure((size_t)off[nb]);
+    launch_signatures3(sig_mask.d, sig_dims, sig_boxes.d, nb, sig_off.d, off[nb], maxlen, maxvol, sig_hist.d, st);
+    ++nkernels;
+    std::vector<int> h((size_t)off[nb]);
+    AMR_CUDA(cudaMemcpyAsync(h.data(), sig_hist.d, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    if (si) { si->assign(nb, {}); sj->assign(nb, {}); }
+    for (int b = 0; b < nb; ++b) {
+      Clu2& c = clus[b];
+      const int* hh = h.data() + off[b];
+      for (int d = 0; d < 2; ++d) {
+        const int len = c.box.hi[d] - c.box.lo[d] + 1;
+        int first = -1, last = -1, sum = 0;
+        for (int t = 0; t < len; ++t)
+          if (hh[t]) { if (first < 0) first = t; last = t; sum += hh[t]; }
+        if (d == 0) c.n = sum;
+        c.lo[d] = first < 0 ? c.box.lo[d] : c.box.lo[d] + first;
+        c.hi[d] = last < 0 ? c.box.hi[d] : c.box.lo[d] + last;
+        if (si) {
+          std::vector<int>& v = d == 0 ? (*si)[b] : (*sj)[b];
+          v.assign((d == 0 ? sig_dims.is : sig_dims.js) + 2, 0);
+          for (int t = 0; t < len; ++t) v[c.box.lo[d] + t] = hh[t];
+        }
+        hh += len;
+      }
+    }
+  }
+  // moment.f: rect (0-based level indices ilo, ihi, jlo, jhi) and efficiency of a cluster
+  static double moment2(const Clu2& c, int rect[4]) {
+    rect[0] = c.lo[0] - 1; rect[1] = c.hi[0] - 1; rect[2] = c.lo[1] - 1; rect[3] = c.hi[1] - 1;
+    return (double)c.n / (double)((rect[1] - rect[0] + 1) * (rect[3] - rect[2] + 1));
+  }
+  // smartbis.f, breadth first over the device signatures; leaves in the reference's order
+  // (the part at or above the cut first)
+  std::vector<Clu2> bisect_on_device(const std::vector<Pt>& pts, int lcheck, double cutoff) {
+    sig_dims = LvlDims{iregsz[lcheck], jregsz[lcheck], 1};
+    sig_mask.ensure((size_t)sig_dims.size());
+    std::vector<int> flat(2 * pts.size());
+    for (size_t k = 0; k < pts.size(); ++k) { flat[2 * k] = pts[k].i; flat[2 * k + 1] = pts[k].j; }
+    sig_pts.upload(flat, st, stg);
+    launch_scatter_points2(sig_pts.d, (int)pts.size(), sig_mask.d, sig_dims, st);
+    ++nkernels;
+    struct Node { Clu2 c; int child = -1; };
+    std::vector<Node> T(1);
+    T[0].c.box = SigBox{{1, 1, 1}, {sig_dims.is, sig_dims.js, 1}};
+    std::vector<int> wave{0};
+    std::vector<std::vector<int>> si, sj;
+    while (!wave.empty()) {
+      std::vector<Clu2> cl(wave.size());
+      for (size_t w = 0; w < wave.size(); ++w) cl[w] = T[wave[w]].c;
+      signatures(cl, &si, &sj);
+      std::vector<int> next;
+      for (size_t w = 0; w < wave.size(); ++w) {
+        T[wave[w]].c = cl[w];
+        const Clu2& c = cl[w];
+        if (c.n == 0) continue;
+        int rect[4];
+        if (moment2(c, rect) >= cutoff) continue;
+        int dir = 0;
+        const int cut = find_cut_sig(si[w], sj[w], sig_dims.is, sig_dims.js, dir);
+        if (cut == 0) continue;
+        const int d = dir - 1;
+        Clu2 up, dn;
+        up.box = dn.box = SigBox{{c.lo[0], c.lo[1], 1}, {c.hi[0], c.hi[1], 1}};
+        up.box.lo[d] = cut;
+        dn.box.hi[d] = cut - 1;
+        const int id = (int)T.size();
+        T[wave[w]].child = id;
+        T.push_back(Node{up, -1});
+        T.push_back(Node{dn, -1});
+        next.push_back(id);
+        next.push_back(id + 1);
+      }
+      wave.swap(next);
+    }
+    std::vector<Clu2> leaves;
+    if (T[0].c.n == 0) return leaves;
+    std::vector<int> stack{0};
+    while (!stack.empty()) {
+      const int id = stack.back();
+      stack.pop_back();
+      if (T[id].child < 0) { leaves.push_back(T[id].c); continue; }
+      stack.push_back(T[id].child + 1);
+      stack.push_back(T[id].child);
+    }
+    return leaves;
+  }
+
   // grdfit2.f:20-150
   void grdfit(int lbase, int lcheck, double t) {
     std::vector<Pt> pts = flag_points(lcheck, lbase);
     if (pts.empty()) return;
     const int levnew = lcheck + 1;
     const double hxf = hxposs[levnew], hyf = hyposs[levnew];
-    std::vector<int> cnt;
     const auto tc0 = std::chrono::steady_clock::now();
+    std::vector<Clu2> cl;
     {
       HPROF("bisect");
-      bisect(pts, p.cut, iregsz[lcheck], jregsz[lcheck], cnt);
+      cl = bisect_on_device(pts, lcheck, p.cut);
     }
-    int base = 0, icl = 0, prv = 0;
-    while (icl < (int)cnt.size()) {
+    int icl = 0, prv = 0;
+    while (icl < (int)cl.size()) {
       const int mnew = nodget();
       while (true) {
         int rect[4];
-        bbox_usage(&pts[base], cnt[icl], rect);
+        moment2(cl[icl], rect);
         HPatch& n = node[mnew];
         n.ilo = rect[0] * intratx[lcheck]; n.jlo = rect[2] * intraty[lcheck];
         n.ihi = (rect[1] + 1) * intratx[lcheck] - 1; n.jhi = (rect[3] + 1) * intraty[lcheck] - 1;
@@ -1913,28 +2037,26 @@ class Amr2Gpu {
         else if (l2 <= lbase) n2 = n1;
         else n2 = base_check(n, l2, std::max(ng, p.ibuff + 1));
         if (n1 && n2) break;
-        const int npts = cnt[icl];
-        if (npts <= 1) throw std::runtime_error("a single flagged point cannot be properly nested");
+        if (cl[icl].n <= 1) throw std::runtime_error("a single flagged point cannot be properly nested");
         double rmid; int dir;
         if (n.xhi - n.xlo > n.yhi - n.ylo) { rmid = (n.ihi + n.ilo + 1) / 2.; rmid = rmid / intratx[levnew - 1]; dir = 1; }
         else { rmid = (n.jhi + n.jlo + 1) / 2.; rmid = rmid / intraty[levnew - 1]; dir = 2; }
-        int ipt = base, ntop = base + npts - 1;
-        auto coord = [&](int k) { return (dir == 1 ? pts[k].i : pts[k].j) + 0.5; };
-        while (true) {
-          if (coord(ipt) < rmid) { ++ipt; if (ipt <= ntop) continue; break; }
-          std::swap(pts[ipt], pts[ntop]);
-          --ntop;
-          if (ipt <= ntop) continue;
-          break;
-        }
-        const int front = ntop - base + 1;
-        cnt[icl] = front;
-        cnt.insert(cnt.begin() + icl + 1, npts - front);
+        // points with centre (index + .5) below rmid first, then the rest (nestck2.f:130-160)
+        const Clu2 c = cl[icl];
+        const int d = dir - 1;
+        int cut = c.lo[d] - 1;  // the largest 1-based array index whose point centre lies below rmid
+        for (int a = c.lo[d]; a <= c.hi[d]; ++a) if ((a - 1) + 0.5 < rmid) cut = a;
+        std::vector<Clu2> parts(2);
+        parts[0].box = parts[1].box = SigBox{{c.lo[0], c.lo[1], 1}, {c.hi[0], c.hi[1], 1}};
+        parts[0].box.hi[d] = cut;
+        parts[1].box.lo[d] = cut + 1;
+        signatures(parts, nullptr, nullptr);
+        cl[icl] = parts[0];
+        cl.insert(cl.begin() + icl + 1, parts[1]);
       }
       if (newstl[levnew] == 0) newstl[levnew] = mnew;
       else node[prv].levelptr = mnew;
       prv = mnew;
-      base += cnt[icl];
       ++icl;
     }
     birect(newstl[levnew]);
@@ -2088,8 +2210,8 @@ class Amr2Gpu {
   void init(const std::string& dir) {
     p.load(dir);
     if (p.ndim != 2) throw std::runtime_error("this solver handles 2D runs");
-    if (write_output && p.output_format != 1)
-      throw std::runtime_error("only ASCII output (output_format 1) is written: binary and NetCDF output are not supported");
+    if (write_output && p.output_format != 1 && p.output_format != 3)
+      throw std::runtime_error("output_format must be 1 (ASCII) or 3 (binary): NetCDF and HDF5 output are not supported");
     if (p.nghost != 2) throw std::runtime_error("num_ghost must be 2");
     if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
     // amr2.f90:258-263: Godunov splitting (stepgrid_dimSplit.f) or unsplit; Strang stops the reference
@@ -2379,6 +2501,7 @@ class Amr2Gpu {
     compile_all();
     ensure_all();
     record_gauges = true;
+    stepped = true;
     mbestsrc.assign(p.gauges.size(), 0);
     setbestsrc();
     sync_stream();
@@ -2546,12 +2669,44 @@ namespace amrb {
 // without files; fort.qNNNN holds per grid (output order) its header and then j-rows of
 // i-cells, one line of meqn e26.16 values per cell and a blank line after every row.
 void Amr2Gpu::output(double t) {
+  const bool binary = p.output_format == 3;  // valout.f90:172-176: nothing zeroed
   for (int lev = 1; lev <= lfine; ++lev) {
     ensure(lev, NEED_STEP);
+    if (binary) continue;
     launch_zero_tiny(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
     ++nkernels;
   }
-  if (write_output) {
+  if (write_output && binary) {
+    // fort.q: the grid headers only; fort.b: every grid's whole array, q(m,i,j) with m fastest
+    std::vector<int> pl;
+    std::vector<long long> off(1, 0);
+    FILE* f = open_output(outdir, "fort.q", frame);
+    int ngrids = 0;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) {
+        const HPatch& g = node[m];
+        ++ngrids;
+        const int n2[2] = {g.nx(), g.ny()};
+        const double lo[2] = {g.xlo, g.ylo}, h[2] = {hxposs[lev], hyposs[lev]};
+        write_grid_header(f, 2, m, lev, n2, lo, h);
+        pl.push_back(m);
+        off.push_back(off.back() + (long long)nvar * (g.nx() + 2 * ng) * (g.ny() + 2 * ng));
+      }
+    if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.q in " + outdir);
+    std::vector<double> v((size_t)off.back());
+    off.pop_back();
+    if (!v.empty()) {
+      DBuf<double> d; d.ensure(v.size());
+      DBuf<int> dp; dp.upload(pl, st, stg);
+      DBuf<long long> doff; doff.upload(off, st, stg);
+      launch_gather_enlarged2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, p.dimsplit, stepped, st, f32);
+      AMR_CUDA(cudaMemcpyAsync(v.data(), d.d, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, st));
+      sync_stream();
+      d.free(); dp.free(); doff.free();
+    }
+    write_raw(open_output(outdir, "fort.b", frame, "wb"), v, outdir);
+    write_fort_t(outdir, frame, t, nvar, ngrids, p.naux, 2, ng);
+  } else if (write_output) {
     const std::vector<double> v = gather_values();
     FILE* f = open_output(outdir, "fort.q", frame);
     size_t pos = 0;

@@ -1560,6 +1560,7 @@ class Amr3Gpu : public AmrSolver {
     cfl_level = cmax;
     cflmax_run = std::max(cflmax_run, cmax);
     ++nsteps_launched;
+    stepped = true;
     return cmax > 0.0 ? dt * p.cfl_desired / cmax : RINF;
   }
   // one-patch views of the sweep prefixes for the plain path, 12 per patch:
@@ -2174,8 +2175,8 @@ class Amr3Gpu : public AmrSolver {
   void init(const std::string& dir) {
     p.load(dir);
     if (p.ndim != 3) throw std::runtime_error("num_dim must be 3");
-    if (write_output && p.output_format != 1)
-      throw std::runtime_error("only ASCII output (output_format 1) is written: binary and NetCDF output are not supported");
+    if (write_output && p.output_format != 1 && p.output_format != 3)
+      throw std::runtime_error("output_format must be 1 (ASCII) or 3 (binary): NetCDF and HDF5 output are not supported");
     nvar = p.nvar;
     blast_x = p.pn("x0", 0.0); blast_y = p.pn("y0", 0.0); blast_z = p.pn("z0", 0.0);
     blast_r = p.pn("r0", 0.2); blast_pin = p.pn("pin", 5.0); blast_pout = p.pn("pout", 1.0);
@@ -2440,6 +2441,7 @@ class Amr3Gpu : public AmrSolver {
     compile_all(0);
     sync_stream();
     record_gauges = true;
+    stepped = true;
   }
   void checkpoint_file(const char* path) {
     if (path && *path) { checkpoint(path); return; }
@@ -2628,10 +2630,32 @@ class Amr3Gpu : public AmrSolver {
   }
   // valout.f90: |q| < 1e-90 (and |aux| < 1e-90 when aux is written) become 0 in place on the
   // interior cells, with or without files
+  // whole arrays (ghost cells included) of every grid in output order, q(m,i,j,k) with m
+  // fastest as raw doubles: binary output (valout.f90:161-172)
+  std::vector<double> gather_enlarged(bool aux) {
+    const int nc = aux ? p.naux : nvar;
+    std::vector<int> pl;
+    std::vector<long long> c0(1, 0);
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) { pl.push_back(m); c0.push_back(c0.back() + (long long)mitot(m) * mjtot(m) * mktot(m)); }
+    std::vector<double> out((size_t)c0.back() * nc);
+    if (out.empty()) return out;
+    DBuf<int> dp; dp.upload(pl, st, stg);
+    DBuf<long long> dc; dc.upload(c0, st, stg);
+    DBuf<double> dout; dout.ensure(out.size());
+    launch_gather_enlarged3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nc, c0.back(), dout.d, aux, p.dimsplit, stepped, st, f32);
+    AMR_CUDA(cudaMemcpyAsync(out.data(), dout.d, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
+    sync_stream();
+    dp.free(); dc.free(); dout.free();
+    return out;
+  }
+  bool stepped = false;  // a level substep has run (store2 then holds the last step's input)
   void output(double t) {
     const bool aux = p.out_aux(t);
+    const bool binary = p.output_format == 3;
     for (int lev = 1; lev <= lfine; ++lev) {
       ensure(lev, NEED_STEP);
+      if (binary) continue;  // the binary form zeroes nothing
       launch_zero_tiny3(pool.d, d_patches.d, plan[lev].d_plist.d, (int)plan[lev].plist.size(), nvar, st, f32);
       ++nkernels;
       if (aux) {
@@ -2642,6 +2666,22 @@ class Amr3Gpu : public AmrSolver {
     if (!write_output) { ++frame; return; }
     int ngrids = 0;
     for (int lev = 1; lev <= lfine; ++lev) ngrids += (int)lgrids[lev].size();
+    if (binary) {
+      FILE* f = open_output(outdir, "fort.q", frame);
+      for (int lev = 1; lev <= lfine; ++lev)
+        for (int m : lgrids[lev]) {
+          const HPatch3& g = node[m];
+          const int n3[3] = {g.nx(), g.ny(), g.nz()};
+          const double lo[3] = {g.xlo, g.ylo, g.zlo}, h[3] = {hxposs[lev], hyposs[lev], hzposs[lev]};
+          write_grid_header(f, 3, m, lev, n3, lo, h);
+        }
+      if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.q in " + outdir);
+      write_raw(open_output(outdir, "fort.b", frame, "wb"), gather_enlarged(false), outdir);
+      if (aux) write_raw(open_output(outdir, "fort.a", frame, "wb"), gather_enlarged(true), outdir);
+      write_fort_t(outdir, frame, t, nvar, ngrids, p.naux, 3, G3);
+      ++frame;
+      return;
+    }
     FILE* f = open_output(outdir, "fort.q", frame);
     write_frame_file(f, gather_values(), nvar);
     if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.q in " + outdir);

@@ -155,6 +155,40 @@ inline int find_cut(const Pt* p, int n, int idim, int jdim, int& dir) {
   return index;
 }
 
+// find_cut on signatures already counted (is, js: counts at 1-based positions 1..idim, 1..jdim).
+inline int find_cut_sig(std::vector<int> is, std::vector<int> js, int idim, int jdim, int& dir) {
+  int ilo = 1, ihi = idim, jlo = 1, jhi = jdim;
+  for (int t = 1; t <= idim; ++t) if (is[t] != 0) { ilo = t; break; }
+  for (int t = 1; t <= idim; ++t) if (is[idim + 1 - t] != 0) { ihi = idim + 1 - t; break; }
+  for (int t = 1; t <= jdim; ++t) if (js[t] != 0) { jlo = t; break; }
+  for (int t = 1; t <= jdim; ++t) if (js[jdim + 1 - t] != 0) { jhi = jdim + 1 - t; break; }
+  for (int i = ilo; i <= ihi; ++i) if (is[i] == 0) { dir = 1; return i; }
+  for (int j = jlo; j <= jhi; ++j) if (js[j] == 0) { dir = 2; return j; }
+  auto lap = [](std::vector<int>& s, int lo, int hi, int& best, int& idx) {
+    int pre = s[lo];
+    for (int i = lo + 1; i <= hi - 1; ++i) { const int cur = s[i]; s[i] = s[i + 1] - 2 * cur + pre; pre = cur; }
+    best = 0; idx = 0;
+    const int mid = (lo + hi) / 2;
+    for (int i = lo + 2; i <= hi - 2 + 1; ++i) {
+      const int a = s[i - 1], b = s[i], d = std::abs(a - b);
+      if (a * b < 0) {
+        if (d > best) { best = d; idx = i; }
+        else if (d == best && std::abs(i - mid) < std::abs(idx - mid)) idx = i;
+      }
+    }
+  };
+  int bi, ii, bj, ij;
+  lap(is, ilo, ihi, bi, ii);
+  lap(js, jlo, jhi, bj, ij);
+  int index, best;
+  if (bi > bj) { index = ii; dir = 1; best = bi; }
+  else if (bi < bj) { index = ij; dir = 2; best = bj; }
+  else if (std::abs(ii - (ilo + ihi) / 2) < std::abs(ij - (jlo + jhi) / 2)) { index = ii; dir = 1; best = bi; }
+  else { index = ij; dir = 2; best = bj; }
+  if (best < 2) index = 0;
+  return index;
+}
+
 // Partition pts[a..b] (inclusive) so that points with coordinate >= cut stay at the
 // front, in the in-place swap order of smartbis.f:128-154. Returns the count at the front.
 inline int split_front(std::vector<Pt>& pts, int a, int b, int dir, int cut) {

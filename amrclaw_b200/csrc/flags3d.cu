@@ -336,6 +336,19 @@ __global__ void signatures3_kernel(const int8_t* f, LvlDims d, const SigBox* box
 }
 }  // namespace
 
+namespace {
+__global__ void scatter_points_kernel(const int* pts, int n, int8_t* f, LvlDims d) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    f[d.at(pts[2 * t] + 1, pts[2 * t + 1] + 1, 1)] = 1;
+}
+}  // namespace
+
+void launch_scatter_points2(const int* pts, int n, int8_t* f, LvlDims d, cudaStream_t s) {
+  AMR_CUDA(cudaMemsetAsync(f, 0, (size_t)d.size(), s));
+  if (n > 0) scatter_points_kernel<<<blocks_for(n, 256), 256, 0, s>>>(pts, n, f, d);
+  AMR_CUDA(cudaGetLastError());
+}
+
 void launch_signatures3(const int8_t* f, LvlDims d, const SigBox* boxes, int nbox, const int* off, int total, int maxlen,
                         long long maxvol, int* hist, cudaStream_t s) {
   if (nbox <= 0) return;

@@ -44,6 +44,9 @@ struct SigBox { int lo[3], hi[3]; };
 // hist; maxlen: the largest ni+nj+nk; maxvol: the largest box volume.
 void launch_signatures3(const int8_t* f, LvlDims d, const SigBox* boxes, int nbox, const int* off, int total, int maxlen,
                         long long maxvol, int* hist, cudaStream_t s);
+// 2D: the level's flag array as a one-plane array (d.ks = 1): zeroed, then 1 at every point
+// (pts: n pairs of 0-based level indices i, j) at array position (i+1, j+1, 1)
+void launch_scatter_points2(const int* pts, int n, int8_t* f, LvlDims d, cudaStream_t s);
 
 // Richardson estimation (errest.f, coarsen.f, errf1.f). vp[0..np): virtual patches of the
 // coarsened grids, vp[np..2np): those of the regular step (same index boxes as the grids).

@@ -464,12 +464,16 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
         __syncthreads();
       }
     }
-    // stepgrid_dimSplit.f:88-103: x-update of every staged row's tile cells
+    // stepgrid_dimSplit.f:88-103: x-update of every staged row's tile cells. The rows that
+    // are the patch's ghost rows (below row 1 or above row my) keep their x-updated values
+    // in the new store1, as the reference's array does (binary output writes them).
     for (int it = tid; it < ME * lh * tw; it += STEP2_THREADS) {
       const int m = it / (lh * tw), rem = it % (lh * tw);
       const int b = rem / tw, c = rem % tw;
-      Qx[(m * QW + b) * T + c] =
-          Qs[(m * QW + b) * QW + c + 2] - dtdx * (FXm[(m * QW + b) * (T + 1) + c + 1] - FXp[(m * QW + b) * (T + 1) + c]);
+      const R v = Qs[(m * QW + b) * QW + c + 2] - dtdx * (FXm[(m * QW + b) * (T + 1) + c + 1] - FXp[(m * QW + b) * (T + 1) + c]);
+      Qx[(m * QW + b) * T + c] = v;
+      const int jrow = j0 - 2 + b;
+      if (jrow < 1 || jrow > my) qout[m * plane + (long long)(jrow + 1) * mitot + (i0 + c + 1)] = v;
     }
     __syncthreads();
     // step2y.f90: columns c (i = i0+c), faces ff (j = j0-1+ff, between x-updated rows ff, ff+1)
@@ -1092,6 +1096,35 @@ void launch_gather_interior2(const void* pool, const PatchDev* patches, const in
       gather_interior2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, outoff + base, nvar, out);
     else
       gather_interior2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, outoff + base, nvar, out);
+    AMR_CUDA(cudaGetLastError());
+  }
+}
+
+// The whole arrays (ghost cells included) of the listed patches, q(m,i,j) with m fastest,
+// for binary output: a cell comes from store1 when the last step wrote it there (the
+// interior, or with split the cells of interior i; every cell before any step) and else
+// from the step's input buffer, whose ghost cells that step's fill set.
+template <class T>
+__global__ void gather_enlarged2_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* outoff,
+                                        int nvar, double* out, int split, bool stepped) {
+  const PatchDev P = patches[plist[blockIdx.y]];
+  const long long plane = (long long)P.mitot * P.mjtot;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % P.mitot), j = (int)(c / P.mitot);
+    const bool in_i = i >= 2 && i < P.mitot - 2, in_j = j >= 2 && j < P.mjtot - 2;
+    const bool written = !stepped || (split ? in_i : (in_i && in_j));
+    const T* q = pool + (written ? P.q[P.cur] : P.q[1 - P.cur]);
+    for (int m = 0; m < nvar; ++m) out[outoff[blockIdx.y] + c * nvar + m] = (double)q[m * plane + c];
+  }
+}
+void launch_gather_enlarged2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
+                             int nvar, double* out, int split, bool stepped, cudaStream_t s, bool f32) {
+  for (int base = 0; base < np; base += 65535) {
+    const int n = std::min(65535, np - base);
+    if (f32)
+      gather_enlarged2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, outoff + base, nvar, out, split, stepped);
+    else
+      gather_enlarged2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, outoff + base, nvar, out, split, stepped);
     AMR_CUDA(cudaGetLastError());
   }
 }

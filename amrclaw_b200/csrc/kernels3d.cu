@@ -605,8 +605,18 @@ __global__ void __launch_bounds__(SW_T) split3_kernel(Step3Args A) {
   if (owned && e <= n1) {
     const long long at = base + (long long)(e + 1) * step;
 #pragma unroll
-    for (int m = 0; m < NV; ++m)
-      qo[m * plane + at] = qi[m * plane + at] - dtdx * (sF[m][l + 1] - sF[NV + m][l]);
+    for (int m = 0; m < NV; ++m) qo[m * plane + at] = qi[m * plane + at] - dtdx * (sF[m][l + 1] - sF[NV + m][l]);
+  }
+  // z: the two ghost layers at each end of the pencil keep their y-updated values in
+  // store1 as well (the reference's array holds them; binary output writes them). The end
+  // interfaces hold both cells of their layer pair; z reads the scratch, so no race.
+  if (DIR == 3 && valid && (e == 0 || e == n1 + 2)) {
+    const long long atl = base + (long long)e * step;
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      qo[m * plane + atl] = qi[m * plane + atl];
+      qo[m * plane + atl + step] = qi[m * plane + atl + step];
+    }
   }
   for (int o = 16; o > 0; o >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
   if ((threadIdx.x & 31) == 0 && cfl > T(0)) atomic_max_nonneg(A.cflmax, (double)cfl);
@@ -1262,6 +1272,28 @@ __global__ void gather3_kernel(const T* pool, const PatchDev* patches, const int
   }
 }
 
+// The whole arrays (ghost cells included) of the listed patches, q(m,i,j,k) with m fastest
+// (the reference's layout), for binary output: enlarged cells [cell0[p], cell0[p+1]) of
+// patch p. aux: the aux arrays. Otherwise a cell comes from store1 when the last step wrote
+// it there (written: the interior, or with split the cells of interior i; all cells when
+// nothing has been stepped yet) and from the step's input buffer, whose ghost cells that
+// step's fill set, when it did not.
+template <class T>
+__global__ void gather_enlarged3_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
+                                        int nvar, long long total, double* out, bool aux, int split, bool stepped) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(cell0, np, t);
+    const PatchDev& P = patches[plist[pi]];
+    const long long loc = t - cell0[pi];
+    const long long mi = P.mitot, mj = P.mjtot, mk = P.mktot, plane = mi * mj * mk;
+    const int ie = (int)(loc % mi), je = (int)((loc / mi) % mj), ke = (int)(loc / (mi * mj));
+    const bool in_i = ie >= NG3 && ie < mi - NG3, in_j = je >= NG3 && je < mj - NG3, in_k = ke >= NG3 && ke < mk - NG3;
+    const bool written = !stepped || (split ? in_i : (in_i && in_j && in_k));
+    const T* q = pool + (aux ? P.aux : written ? P.q[P.cur] : P.q[1 - P.cur]);
+    for (int m = 0; m < nvar; ++m) out[(cell0[pi] + loc) * nvar + m] = (double)q[m * plane + loc];
+  }
+}
+
 // fluxad.f / qad.f work lists of a level, from the per-patch segment prefix: segment
 // seg of a fine patch is (side, ac, bc) in cstore.f's order (sides 1..6, ac fastest)
 __global__ void expand_fadqad3_kernel(const int* plist, const long long* pre, int np, const PatchDev* patches, int rx, int ry,
@@ -1516,6 +1548,13 @@ void launch_mass3(const void* pool, const PatchDev* patches, const int* plist, i
     if (f32) mass3_kernel<<<dim3(8, cnt), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, cnt, out);
     else mass3_kernel<<<dim3(8, cnt), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, cnt, out);
   }
+  AMR_CUDA(cudaGetLastError());
+}
+void launch_gather_enlarged3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
+                             long long total, double* out, bool aux, int split, bool stepped, cudaStream_t s, bool f32) {
+  if (total <= 0) return;
+  if (f32) gather_enlarged3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const float*>(pool), patches, plist, cell0, np, nvar, total, out, aux, split, stepped);
+  else gather_enlarged3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const double*>(pool), patches, plist, cell0, np, nvar, total, out, aux, split, stepped);
   AMR_CUDA(cudaGetLastError());
 }
 void launch_gather3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,

@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace amrb {
 
@@ -52,6 +53,13 @@ inline void write_grid_header(FILE* f, int ndim, int grid, int level, const int*
   for (int d = 0; d < ndim; ++d) std::fprintf(f, "%s    %s\n", fort_e(lower[d], 26, 16).c_str(), ll[d]);
   for (int d = 0; d < ndim; ++d) std::fprintf(f, "%s    %s\n", fort_e(delta[d], 26, 16).c_str(), dd[d]);
   std::fputc('\n', f);
+}
+
+// raw doubles of a binary output file (stream access, no record markers); closes f
+inline void write_raw(FILE* f, const std::vector<double>& v, const std::string& dir) {
+  const size_t n = v.empty() ? 0 : std::fwrite(v.data(), sizeof(double), v.size(), f);
+  const bool ok = n == v.size();
+  if (std::fclose(f) != 0 || !ok) throw std::runtime_error("cannot write binary output in " + dir);
 }
 
 // fort.tNNNN (t_file_format of valout.f90)

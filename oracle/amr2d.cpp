@@ -161,6 +161,7 @@ struct Amr2 {
       for (int k = 1; k <= nout; ++k) tout[k - 1] = t0 + k * (tfinal - t0) / (double)nout;
     }
     output_format = c.iget("output_format", 1);
+    if (output_format != 1 && output_format != 3) throw std::runtime_error("output_format must be 1 (ASCII) or 3 (binary)");
     dt_initial = c.d("dt_initial"); dt_max = c.d("dt_max");
     cflv1 = c.d("cfl_max"); cfl = c.d("cfl_desired"); nv1 = c.i("steps_max");
     if (output_style != 3) nstop = IINFINITY;
@@ -2365,9 +2366,13 @@ struct Amr2 {
     return totmass;
   }
 
-  // valout.f90:8-397 (ascii form) ; zeroes |q| < 1e-90 in place like the reference
+  // valout.f90:8-397. ASCII (output_format 1): zeroes |q| < 1e-90 in place like the
+  // reference and writes the values into fort.q. Binary (3, valout.f90:172-176): fort.q
+  // holds the grid headers only and fort.b every grid's whole array (ghost cells
+  // included, q(m,i,j) with m fastest) as raw doubles, nothing zeroed.
   void valout(int lbeg, int lend, double t) {
-    for (int level = lbeg; level <= lend; ++level)
+    const bool binary = output_format == 3;
+    for (int level = lbeg; level <= lend && !binary; ++level)
       for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
         Node2& g = node[m];
         const int mitot = mitot_of(m), mjtot = mjtot_of(m);
@@ -2375,7 +2380,31 @@ struct Amr2 {
         for (int j = nghost + 1; j <= mjtot - nghost; ++j) for (int i = nghost + 1; i <= mitot - nghost; ++i)
           for (int iv = 1; iv <= nvar; ++iv) if (std::fabs(Q(iv, i, j)) < 1e-90) Q(iv, i, j) = 0.0;
       }
-    if (write_output) {
+    if (write_output && binary) {
+      char fn[64], fb[64];
+      std::snprintf(fn, sizeof(fn), "/fort.q%04d", matlabu);
+      std::snprintf(fb, sizeof(fb), "/fort.b%04d", matlabu);
+      FILE* f = std::fopen((outdir + fn).c_str(), "w");
+      FILE* b = std::fopen((outdir + fb).c_str(), "wb");
+      int ngrids = 0;
+      for (int level = lbeg; level <= lend; ++level)
+        for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+          ++ngrids;
+          Node2& g = node[m];
+          std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n",
+                       m, level, g.ihi - g.ilo + 1, g.jhi - g.jlo + 1);
+          std::fprintf(f, "%s    xlow\n%s    ylow\n%s    dx\n%s    dy\n\n", fmtE(g.xlo, 26, 16).c_str(), fmtE(g.ylo, 26, 16).c_str(),
+                       fmtE(hxposs[level], 26, 16).c_str(), fmtE(hyposs[level], 26, 16).c_str());
+          std::fwrite(g.q1.data(), sizeof(double), g.q1.size(), b);
+        }
+      std::fclose(f);
+      std::fclose(b);
+      std::snprintf(fn, sizeof(fn), "/fort.t%04d", matlabu);
+      f = std::fopen((outdir + fn).c_str(), "w");
+      std::fprintf(f, "%s    time\n%6d                 meqn\n%6d                 ngrids\n%6d                 naux\n%6d                 ndim\n%6d                 nghost\n\n",
+                   fmtE(t, 18, 8).c_str(), nvar, ngrids, naux, 2, nghost);
+      std::fclose(f);
+    } else if (write_output) {
       char fn[64];
       std::snprintf(fn, sizeof(fn), "/fort.q%04d", matlabu);
       FILE* f = std::fopen((outdir + fn).c_str(), "w");

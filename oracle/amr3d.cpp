@@ -85,6 +85,7 @@ struct Amr3 {
   double tfinal = 0; bool output_t0 = true;
   std::vector<int> output_aux_components;
   bool output_aux_onlyonce = true;
+  int output_format = 1;
   std::vector<double> tout;
   double dt_initial, dt_max, cflv1, cfl;
   int nv1; bool vtime;
@@ -170,6 +171,8 @@ struct Amr3 {
     dimensional_split = c.i("dimensional_split");
     method[4] = c.i("verbosity"); method[5] = c.i("source_split");
     mcapa = c.i("capa_index"); use_fwaves = c.b("use_fwaves");
+    output_format = c.iget("output_format", 1);
+    if (output_format != 1 && output_format != 3) throw std::runtime_error("output_format must be 1 (ASCII) or 3 (binary)");
     // amr2.f90:212-218 (amr3.f90 alike): aux components written to fort.aNNNN
     if (naux > 0 && c.has("output_aux_components")) {
       for (int k = 0; k < naux; ++k) output_aux_components.push_back(c.i("output_aux_components", k));
@@ -2635,11 +2638,52 @@ struct Amr3 {
     std::fclose(f);
   }
 
+  // Binary form (output_format 3, src/3d/valout.f90:161-172): fort.q holds the grid headers
+  // only, fort.b every grid's whole array (ghost cells included, q(m,i,j,k) with m fastest)
+  // as raw doubles and, when aux output is due, fort.a the aux arrays likewise; nothing is
+  // zeroed.
+  void valout_binary(int lbeg, int lend, double t, bool out_aux) {
+    char fn[64], fb[64], fa[64];
+    std::snprintf(fn, sizeof(fn), "/fort.q%04d", matlabu);
+    std::snprintf(fb, sizeof(fb), "/fort.b%04d", matlabu);
+    std::snprintf(fa, sizeof(fa), "/fort.a%04d", matlabu);
+    FILE* f = std::fopen((outdir + fn).c_str(), "w");
+    FILE* b = std::fopen((outdir + fb).c_str(), "wb");
+    FILE* a = out_aux ? std::fopen((outdir + fa).c_str(), "wb") : nullptr;
+    if (!f || !b || (out_aux && !a)) throw std::runtime_error("cannot write output files in " + outdir);
+    int ngrids = 0;
+    for (int level = lbeg; level <= lend; ++level)
+      for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+        ++ngrids;
+        Node3& g = node[m];
+        std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n%6d                 mz\n",
+                     m, level, g.ihi - g.ilo + 1, g.jhi - g.jlo + 1, g.khi - g.klo + 1);
+        std::fprintf(f, "%s    xlow\n%s    ylow\n%s    zlow\n%s    dx\n%s    dy\n%s    dz\n\n", fmtE(g.xlo, 26, 16).c_str(),
+                     fmtE(g.ylo, 26, 16).c_str(), fmtE(g.zlo, 26, 16).c_str(), fmtE(hxposs[level], 26, 16).c_str(),
+                     fmtE(hyposs[level], 26, 16).c_str(), fmtE(hzposs[level], 26, 16).c_str());
+        std::fwrite(g.q1.data(), sizeof(double), g.q1.size(), b);
+        if (a) std::fwrite(g.aux.data(), sizeof(double), g.aux.size(), a);
+      }
+    std::fclose(f);
+    std::fclose(b);
+    if (a) std::fclose(a);
+    std::snprintf(fn, sizeof(fn), "/fort.t%04d", matlabu);
+    f = std::fopen((outdir + fn).c_str(), "w");
+    std::fprintf(f, "%s    time\n%6d                 meqn\n%6d                 ngrids\n%6d                 naux\n%6d                 ndim\n%6d                 nghost\n\n",
+                 fmtE(t, 18, 8).c_str(), nvar, ngrids, naux, 3, nghost);
+    std::fclose(f);
+  }
+
   void valout(int lbeg, int lend, double t) {
     // valout.f90: aux output when any component is requested, every frame or only at t0
     int naux_out = 0;
     for (int x : output_aux_components) naux_out += x;
     const bool out_aux = naux_out > 0 && (!output_aux_onlyonce || std::fabs(t - t0) < 1e-90);
+    if (output_format == 3) {
+      if (write_output) valout_binary(lbeg, lend, t, out_aux);
+      matlabu = matlabu + 1;
+      return;
+    }
     if (out_aux) zero_tiny_aux(lbeg, lend);
     for (int level = lbeg; level <= lend; ++level)
       for (int m = lstart[level]; m != 0; m = node[m].levelptr) {

@@ -22,7 +22,7 @@ E26 = r"[ -]*-?0\.\d{16}(E[+-]\d\d|[+-]\d{3})"
 
 
 def _files(d):
-    return sorted(f for f in os.listdir(d) if re.fullmatch(r"fort\.[qta]\d{4}", f))
+    return sorted(f for f in os.listdir(d) if re.fullmatch(r"fort\.[qtab]\d{4}", f))
 
 
 def _run_both(rd, ndim, tmp):
@@ -188,3 +188,71 @@ def test_fort_q_layout_follows_header_format_and_rows():
                 pos += 1
             vpos += cells * meqn
         assert lines[pos:] == [""]
+
+
+# ----------------------------------------------------------------- binary form (output_format 3)
+def _binary(rd):
+    rd.clawdata.output_format = "binary"
+    return rd
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("split", [False, True])
+def test_2d_binary_frames_byte_identical_to_the_oracle(split):
+    """fort.b holds every grid's whole array (ghost cells as the last step left them)."""
+    rd = _binary(configs.euler_quadrants(n=32, levels=3, tfinal=0.15))
+    rd.clawdata.num_output_times = 2
+    rd.clawdata.output_t0 = True
+    if split:
+        rd.clawdata.dimensional_split = "godunov"
+    with tempfile.TemporaryDirectory() as tmp:
+        og, dg, _ = _run_both(rd, 2, tmp)
+        _assert_same_files(og, dg)
+        assert sum(n.startswith("fort.b") for n in _files(dg)) == 3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("split", [False, True])
+def test_3d_binary_frames_byte_identical_to_the_oracle(split):
+    rd = _binary(configs.euler_blast(n=16, levels=2, tfinal=0.08, max1d=12))
+    rd.clawdata.num_output_times = 2
+    rd.clawdata.output_t0 = True
+    if split:
+        rd.clawdata.dimensional_split = "godunov"
+    with tempfile.TemporaryDirectory() as tmp:
+        og, dg, _ = _run_both(rd, 3, tmp)
+        _assert_same_files(og, dg)
+
+
+@pytest.mark.gpu
+def test_3d_binary_aux_frames_byte_identical_to_the_oracle():
+    rd = _binary(problems.advection_swirl3d(n=16, levels=2, tfinal=0.1))
+    c = rd.clawdata
+    c.num_output_times = 2; c.output_t0 = True
+    c.output_aux_components = "all"; c.output_aux_onlyonce = False
+    with tempfile.TemporaryDirectory() as tmp:
+        og, dg, _ = _run_both(rd, 3, tmp)
+        _assert_same_files(og, dg)
+        assert sum(n.startswith("fort.a") for n in _files(dg)) == 3
+
+
+def test_binary_layout_whole_arrays_with_ghost_cells():
+    """The oracle's fort.b: per grid nvar * (mx+4) * (my+4) doubles, q(m,i,j) with m fastest;
+    the interior matches the run's values and fort.q holds the headers only."""
+    rd = _binary(configs.acoustics_radial_regression())
+    rd.clawdata.output_t0 = True
+    rd.clawdata.tfinal = 0.02
+    with tempfile.TemporaryDirectory() as tmp:
+        out, g, v = _oracle_frames(rd, 2, tmp)
+        raw = np.fromfile(os.path.join(out, "fort.b0001"), dtype="<f8")
+        lines = open(os.path.join(out, "fort.q0001")).read().split("\n")
+    assert len(lines) == 9 * len(g) + 1
+    pos, vpos = 0, 0
+    for row in g:
+        mx, my = row[3] - row[2] + 1, row[5] - row[4] + 1
+        a = raw[pos:pos + 3 * (mx + 4) * (my + 4)].reshape(my + 4, mx + 4, 3)
+        inner = np.transpose(a[2:-2, 2:-2, :], (2, 0, 1)).ravel()
+        np.testing.assert_array_equal(inner, v[vpos:vpos + 3 * mx * my])
+        pos += a.size
+        vpos += 3 * mx * my
+    assert pos == raw.size
