@@ -2216,7 +2216,9 @@ class Amr2Gpu {
     if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
     // amr2.f90:258-263: Godunov splitting (stepgrid_dimSplit.f) or unsplit; Strang stops the reference
     if (p.dimsplit > 1) throw std::runtime_error("Strang splitting is not supported (dimensional_split must be 0 or 1)");
-    if (p.src_split != 0) throw std::runtime_error("source terms are not supported");
+    // stepgrid.f:176-180 calls src2 after the step when method(5) = 1; the library's default
+    // src2 (src/2d/src2.f90) does nothing, and no registered problem has a source term
+    if (p.src_split > 1) throw std::runtime_error("source_split must be 0 or 1 (stepgrid.f calls src2 only for 1)");
     nvar = p.nvar; ng = p.nghost;
     setup_problem();
     xlower = p.lower[0]; ylower = p.lower[1]; xupper = p.upper[0]; yupper = p.upper[1];
@@ -2699,7 +2701,7 @@ void Amr2Gpu::output(double t) {
       DBuf<double> d; d.ensure(v.size());
       DBuf<int> dp; dp.upload(pl, st, stg);
       DBuf<long long> doff; doff.upload(off, st, stg);
-      launch_gather_enlarged2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, p.dimsplit, stepped, st, f32);
+      launch_gather_enlarged2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, stepped ? p.dimsplit : 0, st, f32);
       AMR_CUDA(cudaMemcpyAsync(v.data(), d.d, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, st));
       sync_stream();
       d.free(); dp.free(); doff.free();

@@ -2643,7 +2643,7 @@ class Amr3Gpu : public AmrSolver {
     DBuf<int> dp; dp.upload(pl, st, stg);
     DBuf<long long> dc; dc.upload(c0, st, stg);
     DBuf<double> dout; dout.ensure(out.size());
-    launch_gather_enlarged3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nc, c0.back(), dout.d, aux, p.dimsplit, stepped, st, f32);
+    launch_gather_enlarged3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nc, c0.back(), dout.d, aux, stepped ? p.dimsplit : 0, st, f32);
     AMR_CUDA(cudaMemcpyAsync(out.data(), dout.d, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
     sync_stream();
     dp.free(); dc.free(); dout.free();

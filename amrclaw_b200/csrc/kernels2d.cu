@@ -1102,29 +1102,31 @@ void launch_gather_interior2(const void* pool, const PatchDev* patches, const in
 
 // The whole arrays (ghost cells included) of the listed patches, q(m,i,j) with m fastest,
 // for binary output: a cell comes from store1 when the last step wrote it there (the
-// interior, or with split the cells of interior i; every cell before any step) and else
-// from the step's input buffer, whose ghost cells that step's fill set.
+// interior, or after split steps the cells of interior i) and else from the other buffer:
+// the step's input, whose ghost cells that step's fill set (or, before any step, the second
+// copy of the initial values, whose ghost cells are zero as the reference's are after
+// setgrd.f swaps its stores).
 template <class T>
 __global__ void gather_enlarged2_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* outoff,
-                                        int nvar, double* out, int split, bool stepped) {
+                                        int nvar, double* out, int split) {
   const PatchDev P = patches[plist[blockIdx.y]];
   const long long plane = (long long)P.mitot * P.mjtot;
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(c % P.mitot), j = (int)(c / P.mitot);
     const bool in_i = i >= 2 && i < P.mitot - 2, in_j = j >= 2 && j < P.mjtot - 2;
-    const bool written = !stepped || (split ? in_i : (in_i && in_j));
+    const bool written = split ? in_i : (in_i && in_j);
     const T* q = pool + (written ? P.q[P.cur] : P.q[1 - P.cur]);
     for (int m = 0; m < nvar; ++m) out[outoff[blockIdx.y] + c * nvar + m] = (double)q[m * plane + c];
   }
 }
 void launch_gather_enlarged2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
-                             int nvar, double* out, int split, bool stepped, cudaStream_t s, bool f32) {
+                             int nvar, double* out, int split, cudaStream_t s, bool f32) {
   for (int base = 0; base < np; base += 65535) {
     const int n = std::min(65535, np - base);
     if (f32)
-      gather_enlarged2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, outoff + base, nvar, out, split, stepped);
+      gather_enlarged2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist + base, outoff + base, nvar, out, split);
     else
-      gather_enlarged2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, outoff + base, nvar, out, split, stepped);
+      gather_enlarged2_kernel<<<dim3(8, n), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist + base, outoff + base, nvar, out, split);
     AMR_CUDA(cudaGetLastError());
   }
 }

@@ -147,7 +147,7 @@ void launch_zero_tiny(void* pool, const PatchDev* patches, const int* plist, int
 void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32);
 // whole arrays (ghost cells included) in the reference's q(m,i,j) order, for binary output
 void launch_gather_enlarged2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
-                             int nvar, double* out, int split, bool stepped, cudaStream_t s, bool f32);
+                             int nvar, double* out, int split, cudaStream_t s, bool f32);
 void launch_gather_interior2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff,
                              int np, int nvar, double* out, cudaStream_t s, bool f32);
 size_t step2_smem_bytes(int solver, bool f32);

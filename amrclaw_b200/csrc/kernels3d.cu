@@ -1275,12 +1275,13 @@ __global__ void gather3_kernel(const T* pool, const PatchDev* patches, const int
 // The whole arrays (ghost cells included) of the listed patches, q(m,i,j,k) with m fastest
 // (the reference's layout), for binary output: enlarged cells [cell0[p], cell0[p+1]) of
 // patch p. aux: the aux arrays. Otherwise a cell comes from store1 when the last step wrote
-// it there (written: the interior, or with split the cells of interior i; all cells when
-// nothing has been stepped yet) and from the step's input buffer, whose ghost cells that
-// step's fill set, when it did not.
+// it there (the interior, or after split steps the cells of interior i) and from the other
+// buffer when it did not: that is the step's input, whose ghost cells its fill set (or,
+// before any step, the second copy of the initial values, whose ghost cells are zero as
+// the reference's are after setgrd.f swaps its stores).
 template <class T>
 __global__ void gather_enlarged3_kernel(const T* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np,
-                                        int nvar, long long total, double* out, bool aux, int split, bool stepped) {
+                                        int nvar, long long total, double* out, bool aux, int split) {
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
     const int pi = find_patch(cell0, np, t);
     const PatchDev& P = patches[plist[pi]];
@@ -1288,7 +1289,7 @@ __global__ void gather_enlarged3_kernel(const T* pool, const PatchDev* patches, 
     const long long mi = P.mitot, mj = P.mjtot, mk = P.mktot, plane = mi * mj * mk;
     const int ie = (int)(loc % mi), je = (int)((loc / mi) % mj), ke = (int)(loc / (mi * mj));
     const bool in_i = ie >= NG3 && ie < mi - NG3, in_j = je >= NG3 && je < mj - NG3, in_k = ke >= NG3 && ke < mk - NG3;
-    const bool written = !stepped || (split ? in_i : (in_i && in_j && in_k));
+    const bool written = split ? in_i : (in_i && in_j && in_k);
     const T* q = pool + (aux ? P.aux : written ? P.q[P.cur] : P.q[1 - P.cur]);
     for (int m = 0; m < nvar; ++m) out[(cell0[pi] + loc) * nvar + m] = (double)q[m * plane + loc];
   }
@@ -1551,10 +1552,10 @@ void launch_mass3(const void* pool, const PatchDev* patches, const int* plist, i
   AMR_CUDA(cudaGetLastError());
 }
 void launch_gather_enlarged3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
-                             long long total, double* out, bool aux, int split, bool stepped, cudaStream_t s, bool f32) {
+                             long long total, double* out, bool aux, int split, cudaStream_t s, bool f32) {
   if (total <= 0) return;
-  if (f32) gather_enlarged3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const float*>(pool), patches, plist, cell0, np, nvar, total, out, aux, split, stepped);
-  else gather_enlarged3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const double*>(pool), patches, plist, cell0, np, nvar, total, out, aux, split, stepped);
+  if (f32) gather_enlarged3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const float*>(pool), patches, plist, cell0, np, nvar, total, out, aux, split);
+  else gather_enlarged3_kernel<<<grid_for(total, 256), 256, 0, s>>>(static_cast<const double*>(pool), patches, plist, cell0, np, nvar, total, out, aux, split);
   AMR_CUDA(cudaGetLastError());
 }
 void launch_gather3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,

@@ -149,7 +149,7 @@ void launch_gauges3(const void* pool, const PatchDev* patches, const Gauge3Job* 
 void launch_mass3(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32);
 // whole arrays (ghost cells included) in the reference's q(m,i,j,k) order, for binary output
 void launch_gather_enlarged3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
-                             long long total, double* out, bool aux, int split, bool stepped, cudaStream_t s, bool f32);
+                             long long total, double* out, bool aux, int split, cudaStream_t s, bool f32);
 void launch_gather3(const void* pool, const PatchDev* patches, const int* plist, const long long* cell0, int np, int nvar,
                     long long total, double* out, cudaStream_t s, bool f32, bool aux = false);
 
