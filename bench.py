@@ -44,6 +44,13 @@ def workload(name: str):
         return rd, dict(workload=name, base_grid="64x64x64", levels=3, ratio=2, solver="Roe+entropy fix, CTU 3D (22)",
                         meqn=5, naux=0, tfinal=0.5, seed=0, max1d=68, flag="pressure difference > 0.2",
                         bc="extrapolation", precision="fp64"), 5, 0, 3
+    if name == "euler3d_blast_48":
+        # the same blast on a 48^3 base grid with 2 levels: the profiling case (its level-1 step
+        # staging is larger than L2, its device memory a few hundred MB)
+        rd = configs.euler_blast(n=48, levels=2, tfinal=0.5, seed=0, max1d=68)
+        return rd, dict(workload=name, base_grid="48x48x48", levels=2, ratio=2, solver="Roe+entropy fix, CTU 3D (22)",
+                        meqn=5, naux=0, tfinal=0.5, seed=0, max1d=68, flag="pressure difference > 0.2",
+                        bc="extrapolation", precision="fp64"), 5, 0, 3
     if name == "euler2d_quadrants":
         rd = configs.euler_quadrants(n=100, levels=4, tfinal=0.8)
         return rd, dict(workload=name, base_grid="100x100", levels=4, ratio=2, solver="Roe+entropy fix", meqn=4,
