@@ -1913,7 +1913,7 @@ class Amr2Gpu {
       const int ni = bx[b].hi[0] - bx[b].lo[0] + 1, nj = bx[b].hi[1] - bx[b].lo[1] + 1;
       off[b + 1] = off[b] + ni + nj + 1;
       maxlen = std::max(maxlen, ni + nj + 1);
-      maxvol = std::max(maxvol, (long long)ni * nj);
+      maxvol = std::max(maxvol, (long long)nj);  // i-rows of the box
     }
     sig_boxes.upload(bx, st, stg);
     sig_off.upload(off, st, stg);

@@ -54,6 +54,7 @@ struct Prog3 {
   std::vector<int> op_stage, op_owner;  // owner: index of the patch (in the level list) the op serves
   std::vector<Bc3Op> bcs;
   std::vector<int> bc_stage, bc_owner;
+  std::vector<long long> bc_lines;  // per stage: the most boundary lines of one op (bc3 grid size)
   int nstages = 0, nowners = 0;
   long long scratch_off = -1, scratch_len = 0, scratch_alloc = 0;
   // the scratch starts at zero each run: programs whose rects come from icall copies
@@ -107,7 +108,7 @@ void merge_prog(Prog3& D, const Prog3& S, int owner = 0) {
 struct Plan3 {
   Prog3 bound, saveqc;
   std::vector<int> plist;
-  std::vector<long long> sweep0, comp0, face0, cell0;
+  std::vector<long long> sweep0, comp0, face0, cell0, brick0;
   long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;  // items: interfaces per direction
   // dimensionally split step: interfaces of the split pencils per direction and patch, the
   // enlarged cells of each patch in the split scratch, and per-patch views of both
@@ -123,7 +124,7 @@ struct Plan3 {
   std::vector<Avg3> avg;
   long long avg_max = 0;  // cells of the largest averaging rectangle
   DBuf<int> d_plist;
-  DBuf<long long> d_sweep0, d_comp0, d_face0, d_cell0;
+  DBuf<long long> d_sweep0, d_comp0, d_face0, d_cell0, d_brick0;
   DBuf<Fsv3> d_fsv;
   DBuf<long long> d_seg0;
   DBuf<Fad3> d_fad;
@@ -136,7 +137,7 @@ struct Plan3 {
   DBuf<long long> d_pp;
   void free_dev() {
     bound.free_dev(); saveqc.free_dev();
-    d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_seg0.free(); d_fad.free(); d_qad.free();
+    d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_brick0.free(); d_fsv.free(); d_seg0.free(); d_fad.free(); d_qad.free();
     d_upc.free(); d_upt.free(); d_avg.free(); d_pp.free();
     d_scomp0.free(); d_ecell0.free(); d_spp.free();
   }
@@ -243,8 +244,11 @@ class Amr3Gpu : public AmrSolver {
     if (h_cfl) cudaFreeHost(h_cfl);
     if (d_mass) cudaFree(d_mass);
     for (cudaEvent_t e : {ev_a, ev_b, ev_run0, ev_run1}) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {sweep_ss.fork, sweep_ss.join[0], sweep_ss.join[1]}) if (e) cudaEventDestroy(e);
+    for (cudaStream_t x : sweep_ss.side) if (x) { cudaStreamSynchronize(x); cudaStreamDestroy(x); }
     if (st) cudaStreamDestroy(st);
   }
+  SweepStreams sweep_ss{};  // the side streams of the sweep directions
   void sync_stream() { AMR_CUDA(cudaStreamSynchronize(st)); stg.reset(); }
 
   int mitot(int m) const { return node[m].nx() + 2 * G3; }
@@ -840,7 +844,7 @@ class Amr3Gpu : public AmrSolver {
     while (s + 1 < P.nstages) { ++s; P.ch_lo[s] = P.ch_hi[s] = (int)ch.size(); }
     const std::vector<int> bidx = stage_owner_order(P.bc_stage, P.bc_owner, P.nstages);
     std::vector<Bc3Op> bcs;
-    P.bc_lo.assign(P.nstages, 0); P.bc_hi.assign(P.nstages, 0);
+    P.bc_lo.assign(P.nstages, 0); P.bc_hi.assign(P.nstages, 0); P.bc_lines.assign(P.nstages, 0);
     P.own_bc_lo.assign((size_t)P.nstages * no, 0); P.own_bc_hi.assign((size_t)P.nstages * no, 0);
     s = -1;
     for (int k : bidx) {
@@ -851,6 +855,8 @@ class Amr3Gpu : public AmrSolver {
       bcs.push_back(P.bcs[k]);
       P.bc_hi[s] = (int)bcs.size();
       P.own_bc_hi[ow] = (int)bcs.size();
+      const Bc3Op& o = P.bcs[k];
+      P.bc_lines[s] = std::max(P.bc_lines[s], std::max((long long)o.ncol * o.nfil, std::max((long long)o.nrow * o.nfil, (long long)o.nrow * o.ncol)));
     }
     while (s + 1 < P.nstages) { ++s; P.bc_lo[s] = P.bc_hi[s] = (int)bcs.size(); }
     P.d_ops.upload(ops, st, stg);
@@ -877,7 +883,7 @@ class Amr3Gpu : public AmrSolver {
         Bc3Args b{};
         b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.own_bc_lo[ow];
         b.nops = P.own_bc_hi[ow] - P.own_bc_lo[ow]; b.nvar = nvar;
-        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st, f32);
+        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st, f32, P.bc_lines[s]);
         nkernels += 3;
       }
     }
@@ -900,7 +906,7 @@ class Amr3Gpu : public AmrSolver {
         Bc3Args b{};
         b.pool = pool.d; b.patches = d_patches.d; b.rects = P.d_rects.d; b.ops = P.d_bcs.d + P.bc_lo[s];
         b.nops = P.bc_hi[s] - P.bc_lo[s]; b.nvar = nvar;
-        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st, f32);
+        for (int ph = 0; ph < 3; ++ph) launch_bc3(b, ph, st, f32, P.bc_lines[s]);
         nkernels += 3;
       }
     }
@@ -914,7 +920,7 @@ class Amr3Gpu : public AmrSolver {
     const int np = (int)L.plist.size();
     L.sweep0.assign((size_t)3 * (np + 1), 0);
     L.comp0.assign((size_t)3 * (np + 1), 0);
-    L.face0.assign(np + 1, 0); L.cell0.assign(np + 1, 0);
+    L.face0.assign(np + 1, 0); L.cell0.assign(np + 1, 0); L.brick0.assign(np + 1, 0);
     long long slot = 0, comp = 0;
     for (int d = 0; d < 3; ++d) {
       comp = 0;
@@ -937,6 +943,7 @@ class Amr3Gpu : public AmrSolver {
       const HPatch3& g = node[L.plist[k]];
       L.face0[k + 1] = L.face0[k] + (long long)(g.nx() + 1) * (g.ny() + 1) * (g.nz() + 1);
       L.cell0[k + 1] = L.cell0[k] + (long long)g.nx() * g.ny() * g.nz();
+      L.brick0[k + 1] = L.brick0[k] + face3_bricks(g.nx(), g.ny(), g.nz());
     }
     L.faces = L.face0[np]; L.cells = L.cell0[np];
     if (p.dimsplit) {
@@ -987,6 +994,7 @@ class Amr3Gpu : public AmrSolver {
     L.d_comp0.upload(L.comp0, st, stg);
     L.d_face0.upload(L.face0, st, stg);
     L.d_cell0.upload(L.cell0, st, stg);
+    L.d_brick0.upload(L.brick0, st, stg);
     {
       std::vector<long long> pp((size_t)12 * np, 0);
       for (int k = 0; k < np; ++k)
@@ -1411,7 +1419,7 @@ class Amr3Gpu : public AmrSolver {
       }
       if (timed) AMR_CUDA(cudaEventRecord(ev_a, st));
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
-      a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
+      a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d; a.brick0 = L.d_brick0.d;
       if (p.dimsplit) {
         // stepgrid_dimSplit.f: x, y, z sweeps with their updates, one launch each
         a.scomp0 = L.d_scomp0.d; a.ecell0 = L.d_ecell0.d; a.split = d_split.d;
@@ -1421,7 +1429,7 @@ class Amr3Gpu : public AmrSolver {
         const int sched = pick_schedule(lev, tt, ds != nullptr);
         a.queue = sched == 1 ? d_queue : nullptr;
         if (tt) AMR_CUDA(cudaEventRecord(ev_t0, st));
-        nkernels += launch_step3(a, L.items, L.faces, L.cells, st, f32);
+        nkernels += launch_step3(a, L.items, L.faces, L.cells, st, f32, &sweep_ss);
         if (tt) { AMR_CUDA(cudaEventRecord(ev_t1, st)); tune_pending = sched; }
       }
       if (timed) AMR_CUDA(cudaEventRecord(ev_b, st));
@@ -1452,7 +1460,7 @@ class Amr3Gpu : public AmrSolver {
         Step3Args b = a;
         b.plist = L.d_plist.d + k; b.np = 1;
         b.sweep0 = L.d_pp.d + (size_t)12 * k; b.comp0 = L.d_pp.d + (size_t)12 * k + 6;
-        b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
+        b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k; b.brick0 = L.d_brick0.d + k;
         long long it[3];
         if (p.dimsplit) {
           b.scomp0 = L.d_spp.d + (size_t)8 * k; b.ecell0 = L.d_spp.d + (size_t)8 * k + 6; b.split = d_split.d;
@@ -1460,7 +1468,7 @@ class Amr3Gpu : public AmrSolver {
           nkernels += launch_split3(b, it, st, f32);
         } else {
           for (int d = 0; d < 3; ++d) it[d] = L.comp0[(size_t)d * (np + 1) + k + 1] - L.comp0[(size_t)d * (np + 1) + k];
-          nkernels += launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32);
+          nkernels += launch_step3(b, it, L.face0[k + 1] - L.face0[k], L.cell0[k + 1] - L.cell0[k], st, f32, &sweep_ss);
         }
         const long long f0 = L.fsv0[k], nf = L.fsv0[k + 1] - L.fsv0[k];
         if (nf > 0) {
@@ -1674,13 +1682,13 @@ class Amr3Gpu : public AmrSolver {
       vp[np + k] = R;
     }
     // step prefixes of both lists, as compile_step builds them for a level:
-    // [sweep0 3*(n+1) | comp0 3*(n+1) | face0 n+1 | cell0 n+1] per list
+    // [sweep0 3*(n+1) | comp0 3*(n+1) | face0 n+1 | cell0 n+1 | brick0 n+1] per list
     std::vector<long long> pre;
     long long items[2][3], slots[2], faces[2], cells[2], base[2];
     for (int li = 0; li < 2; ++li) {
       base[li] = (long long)pre.size();
       const int n = np, first = li * np;
-      std::vector<long long> sw(3 * (size_t)(n + 1), 0), cp(3 * (size_t)(n + 1), 0), fc(n + 1, 0), ce(n + 1, 0);
+      std::vector<long long> sw(3 * (size_t)(n + 1), 0), cp(3 * (size_t)(n + 1), 0), fc(n + 1, 0), ce(n + 1, 0), bk(n + 1, 0);
       long long slot = 0;
       for (int d = 0; d < 3; ++d) {
         long long comp = 0;
@@ -1701,12 +1709,14 @@ class Amr3Gpu : public AmrSolver {
         const long long mx = V.ihi - V.ilo + 1, my = V.jhi - V.jlo + 1, mz = V.khi - V.klo + 1;
         fc[k + 1] = fc[k] + (mx + 1) * (my + 1) * (mz + 1);
         ce[k + 1] = ce[k] + mx * my * mz;
+        bk[k + 1] = bk[k] + face3_bricks(mx, my, mz);
       }
       slots[li] = slot; faces[li] = fc[n]; cells[li] = ce[n];
       pre.insert(pre.end(), sw.begin(), sw.end());
       pre.insert(pre.end(), cp.begin(), cp.end());
       pre.insert(pre.end(), fc.begin(), fc.end());
       pre.insert(pre.end(), ce.begin(), ce.end());
+      pre.insert(pre.end(), bk.begin(), bk.end());
     }
     std::vector<int> pl(2 * (size_t)np);
     for (int k = 0; k < 2 * np; ++k) pl[k] = k;
@@ -1727,7 +1737,7 @@ class Amr3Gpu : public AmrSolver {
       a.pool = pool.d; a.patches = rich_vp.d; a.sp = sp;
       a.plist = rich_plist.d + li * np; a.np = np;
       const long long* b = rich_pre.d + base[li];
-      a.sweep0 = b; a.comp0 = b + 3 * (np + 1); a.face0 = b + 6 * (np + 1); a.cell0 = b + 7 * (np + 1);
+      a.sweep0 = b; a.comp0 = b + 3 * (np + 1); a.face0 = b + 6 * (np + 1); a.cell0 = b + 7 * (np + 1); a.brick0 = b + 8 * (np + 1);
       a.stash = d_stash.d; a.stash_stride = slots[li]; a.flux = d_flux.d; a.flux_stride = faces[li];
       a.dt = li == 0 ? 2.0 * dt : dt;
       a.dx = li == 0 ? 2.0 * hx : hx; a.dy = li == 0 ? 2.0 * hy : hy; a.dz = li == 0 ? 2.0 * hz : hz;
@@ -1864,7 +1874,7 @@ class Amr3Gpu : public AmrSolver {
       const int len = (bx[b].hi[0] - bx[b].lo[0] + 1) + (bx[b].hi[1] - bx[b].lo[1] + 1) + (bx[b].hi[2] - bx[b].lo[2] + 1);
       off[b + 1] = off[b] + len;
       maxlen = std::max(maxlen, len);
-      maxvol = std::max(maxvol, (long long)(bx[b].hi[0] - bx[b].lo[0] + 1) * (bx[b].hi[1] - bx[b].lo[1] + 1) * (bx[b].hi[2] - bx[b].lo[2] + 1));
+      maxvol = std::max(maxvol, (long long)(bx[b].hi[1] - bx[b].lo[1] + 1) * (bx[b].hi[2] - bx[b].lo[2] + 1));  // i-rows
     }
     sig_boxes.upload(bx, st, stg);
     sig_off.upload(off, st, stg);
@@ -2207,6 +2217,9 @@ class Amr3Gpu : public AmrSolver {
       lc.intratx[l] = intratx[l]; lc.intraty[l] = intraty[l]; lc.intratz[l] = intratz[l];
     }
     AMR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (cudaStream_t& x : sweep_ss.side) AMR_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    AMR_CUDA(cudaEventCreateWithFlags(&sweep_ss.fork, cudaEventDisableTiming));
+    for (cudaEvent_t& e : sweep_ss.join) AMR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     retain_pool_memory();
     AllocStreamScope alloc_scope(st);
     for (cudaEvent_t* e : {&ev_a, &ev_b, &ev_run0, &ev_run1}) AMR_CUDA(cudaEventCreate(e));

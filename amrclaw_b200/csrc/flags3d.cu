@@ -311,8 +311,10 @@ void launch_colate3(int8_t* f, const int8_t* dom, LvlDims d, cudaStream_t s) {
 // ======================================================================= signatures (signs.f)
 namespace {
 // The row / column / plane counts of the flagged cells (f != 0) of each box: blockIdx.y is
-// the box, blockIdx.x a slab of its cells; counts are made in shared memory and added to
-// the box's histograms (integer sums, so the order of the adds does not matter).
+// the box, each warp takes i-rows (fixed j, k) of it in turn, 32 cells of a row at a time
+// (lane = i, coalesced reads). The i-counts go to shared memory one lane per bin; the j-
+// and k-counts of a chunk are summed across the warp first and added once. Counts are
+// integers, so the order of the adds does not matter.
 __global__ void signatures3_kernel(const int8_t* f, LvlDims d, const SigBox* boxes, const int* off, int* hist) {
   extern __shared__ int sh[];
   const SigBox B = boxes[blockIdx.y];
@@ -320,13 +322,21 @@ __global__ void signatures3_kernel(const int8_t* f, LvlDims d, const SigBox* box
   const int nh = ni + nj + nk;
   for (int t = threadIdx.x; t < nh; t += blockDim.x) sh[t] = 0;
   __syncthreads();
-  const long long vol = (long long)ni * nj * nk;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < vol; t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % ni), j = (int)((t / ni) % nj), k = (int)(t / ((long long)ni * nj));
-    if (f[d.at(B.lo[0] + i, B.lo[1] + j, B.lo[2] + k)] != 0) {
-      atomicAdd(&sh[i], 1);
-      atomicAdd(&sh[ni + j], 1);
-      atomicAdd(&sh[ni + nj + k], 1);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const long long rows = (long long)nj * nk;
+  for (long long r = (long long)blockIdx.x * nwarps + warp; r < rows; r += (long long)gridDim.x * nwarps) {
+    const int j = (int)(r % nj), k = (int)(r / nj);
+    const int8_t* row = f + d.at(B.lo[0], B.lo[1] + j, B.lo[2] + k);
+    int cnt = 0;
+    for (int i0 = 0; i0 < ni; i0 += 32) {
+      const int i = i0 + lane;
+      const int flag = (i < ni && row[i] != 0) ? 1 : 0;
+      if (flag) atomicAdd(&sh[i], 1);
+      cnt += __popc(__ballot_sync(0xffffffffu, flag));
+    }
+    if (lane == 0 && cnt) {
+      atomicAdd(&sh[ni + j], cnt);
+      atomicAdd(&sh[ni + nj + k], cnt);
     }
   }
   __syncthreads();
@@ -334,9 +344,6 @@ __global__ void signatures3_kernel(const int8_t* f, LvlDims d, const SigBox* box
   for (int t = threadIdx.x; t < nh; t += blockDim.x)
     if (sh[t]) atomicAdd(&h[t], sh[t]);
 }
-}  // namespace
-
-namespace {
 __global__ void scatter_points_kernel(const int* pts, int n, int8_t* f, LvlDims d) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
     f[d.at(pts[2 * t] + 1, pts[2 * t + 1] + 1, 1)] = 1;
@@ -350,10 +357,11 @@ void launch_scatter_points2(const int* pts, int n, int8_t* f, LvlDims d, cudaStr
 }
 
 void launch_signatures3(const int8_t* f, LvlDims d, const SigBox* boxes, int nbox, const int* off, int total, int maxlen,
-                        long long maxvol, int* hist, cudaStream_t s) {
+                        long long maxrows, int* hist, cudaStream_t s) {
   if (nbox <= 0) return;
   AMR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t)total, s));
-  const int slabs = (int)std::max<long long>(1, std::min<long long>(64, (maxvol + 8191) / 8192));
+  // blocks of 8 warps, a warp per i-row: enough blocks per box for its rows
+  const int slabs = (int)std::max<long long>(1, std::min<long long>(64, (maxrows + 7) / 8));
   for (int base = 0; base < nbox; base += 65535) {
     const int cnt = std::min(65535, nbox - base);
     signatures3_kernel<<<dim3(slabs, cnt), 256, sizeof(int) * (size_t)maxlen, s>>>(f, d, boxes + base, off + base, hist);

@@ -41,9 +41,9 @@ void launch_colate3(int8_t* f, const int8_t* dom, LvlDims d, cudaStream_t s);
 struct SigBox { int lo[3], hi[3]; };
 // signs.f:4-86: for every box, the counts of flagged cells (f != 0) per i, per j and per k
 // of the box: hist[off[b] .. +ni) per i, then nj per j, then nk per k. total: ints of
-// hist; maxlen: the largest ni+nj+nk; maxvol: the largest box volume.
+// hist; maxlen: the largest ni+nj+nk; maxrows: the largest nj*nk (i-rows of a box).
 void launch_signatures3(const int8_t* f, LvlDims d, const SigBox* boxes, int nbox, const int* off, int total, int maxlen,
-                        long long maxvol, int* hist, cudaStream_t s);
+                        long long maxrows, int* hist, cudaStream_t s);
 // 2D: the level's flag array as a one-plane array (d.ks = 1): zeroed, then 1 at every point
 // (pts: n pairs of 0-based level indices i, j) at array position (i+1, j+1, 1)
 void launch_scatter_points2(const int* pts, int n, int8_t* f, LvlDims d, cudaStream_t s);

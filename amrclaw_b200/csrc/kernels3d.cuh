@@ -34,6 +34,7 @@ struct Step3Args {
   const long long* comp0;    // [3][np+1]: first interface of each patch, per direction ((n1+3) per pencil)
   const long long* face0;    // [np+1]: first face cell of each patch ((mx+1)(my+1)(mz+1) each)
   const long long* cell0;    // [np+1]: first interior cell of each patch (mx*my*mz each)
+  const long long* brick0;   // [np+1]: first face brick of each patch (face3_bricks each)
   long long stash_stride;    // slots of one direction region x 3 (SoA stride)
   void* stash;               // [stash_values(meqn)][stash_stride]
   void* flux;                // [6 comps][meqn][face cells]
@@ -100,7 +101,22 @@ struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff;
 // flux differencing; FP64 registers, register corrections, averages and totals).
 // interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction.
 // returns the number of kernels launched
-int launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s, bool f32);
+// The face gather takes the face cells of a patch in bricks of FB_I x FB_J x FB_K, one
+// block per brick.
+constexpr int FB_I = 8, FB_J = 4, FB_K = 4;
+__host__ __device__ inline long long face3_bricks(long long mx, long long my, long long mz) {
+  return ((mx + 1 + FB_I - 1) / FB_I) * ((my + 1 + FB_J - 1) / FB_J) * ((mz + 1 + FB_K - 1) / FB_K);
+}
+
+// Two side streams and the events that fork them off the solve's stream and join them back:
+// the three sweep directions of a level (independent of one another) then run at once, and
+// the tail blocks of one direction overlap the others instead of leaving SMs idle.
+struct SweepStreams {
+  cudaStream_t side[2];
+  cudaEvent_t fork, join[2];
+};
+int launch_step3(const Step3Args& a, const long long interfaces_per_dir[3], long long faces, long long cells, cudaStream_t s, bool f32,
+                 const SweepStreams* ss = nullptr);
 // the Godunov-split step of the level (stepgrid_dimSplit.f): x, y and z sweeps with their
 // updates, interfaces_per_dir counting the split pencils (scomp0); returns launches made
 int launch_split3(const Step3Args& a, const long long interfaces_per_dir[3], cudaStream_t s, bool f32);
@@ -139,7 +155,7 @@ void launch_zero_tiny3(void* pool, const PatchDev* patches, const int* plist, in
 void launch_b4step3(void* pool, const PatchDev* patches, const int* plist, int np, int naux, long long max_cells, double c,
                     cudaStream_t s, bool f32, const double* c_dev = nullptr);
 void launch_fill3(const Fill3Args& a, cudaStream_t s, bool f32);
-void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s, bool f32);
+void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s, bool f32, long long max_lines);
 void launch_upbnd3(void* pool, const double* regs, const PatchDev* patches, const Upbnd3Cell* cells, int n,
                    const Upbnd3Term* terms, double volume, int nvar, cudaStream_t s, bool f32);
 void launch_average3(void* pool, const PatchDev* patches, const Avg3* r, int n, long long max_cells, int rx, int ry, int rz, int nvar,
