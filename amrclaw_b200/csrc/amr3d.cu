@@ -108,7 +108,7 @@ void merge_prog(Prog3& D, const Prog3& S, int owner = 0) {
 struct Plan3 {
   Prog3 bound, saveqc;
   std::vector<int> plist;
-  std::vector<long long> sweep0, comp0, face0, cell0, brick0;
+  std::vector<long long> sweep0, comp0, face0, cell0;
   long long items[3] = {0, 0, 0}, faces = 0, cells = 0, slots = 0;  // items: interfaces per direction
   // dimensionally split step: interfaces of the split pencils per direction and patch, the
   // enlarged cells of each patch in the split scratch, and per-patch views of both
@@ -124,7 +124,7 @@ struct Plan3 {
   std::vector<Avg3> avg;
   long long avg_max = 0;  // cells of the largest averaging rectangle
   DBuf<int> d_plist;
-  DBuf<long long> d_sweep0, d_comp0, d_face0, d_cell0, d_brick0;
+  DBuf<long long> d_sweep0, d_comp0, d_face0, d_cell0;
   DBuf<Fsv3> d_fsv;
   DBuf<long long> d_seg0;
   DBuf<Fad3> d_fad;
@@ -137,7 +137,7 @@ struct Plan3 {
   DBuf<long long> d_pp;
   void free_dev() {
     bound.free_dev(); saveqc.free_dev();
-    d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_brick0.free(); d_fsv.free(); d_seg0.free(); d_fad.free(); d_qad.free();
+    d_plist.free(); d_sweep0.free(); d_comp0.free(); d_face0.free(); d_cell0.free(); d_fsv.free(); d_seg0.free(); d_fad.free(); d_qad.free();
     d_upc.free(); d_upt.free(); d_avg.free(); d_pp.free();
     d_scomp0.free(); d_ecell0.free(); d_spp.free();
   }
@@ -920,7 +920,7 @@ class Amr3Gpu : public AmrSolver {
     const int np = (int)L.plist.size();
     L.sweep0.assign((size_t)3 * (np + 1), 0);
     L.comp0.assign((size_t)3 * (np + 1), 0);
-    L.face0.assign(np + 1, 0); L.cell0.assign(np + 1, 0); L.brick0.assign(np + 1, 0);
+    L.face0.assign(np + 1, 0); L.cell0.assign(np + 1, 0);
     long long slot = 0, comp = 0;
     for (int d = 0; d < 3; ++d) {
       comp = 0;
@@ -943,7 +943,6 @@ class Amr3Gpu : public AmrSolver {
       const HPatch3& g = node[L.plist[k]];
       L.face0[k + 1] = L.face0[k] + (long long)(g.nx() + 1) * (g.ny() + 1) * (g.nz() + 1);
       L.cell0[k + 1] = L.cell0[k] + (long long)g.nx() * g.ny() * g.nz();
-      L.brick0[k + 1] = L.brick0[k] + face3_bricks(g.nx(), g.ny(), g.nz());
     }
     L.faces = L.face0[np]; L.cells = L.cell0[np];
     if (p.dimsplit) {
@@ -994,7 +993,6 @@ class Amr3Gpu : public AmrSolver {
     L.d_comp0.upload(L.comp0, st, stg);
     L.d_face0.upload(L.face0, st, stg);
     L.d_cell0.upload(L.cell0, st, stg);
-    L.d_brick0.upload(L.brick0, st, stg);
     {
       std::vector<long long> pp((size_t)12 * np, 0);
       for (int k = 0; k < np; ++k)
@@ -1419,7 +1417,7 @@ class Amr3Gpu : public AmrSolver {
       }
       if (timed) AMR_CUDA(cudaEventRecord(ev_a, st));
       a.plist = L.d_plist.d; a.np = (int)L.plist.size();
-      a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d; a.brick0 = L.d_brick0.d;
+      a.sweep0 = L.d_sweep0.d; a.comp0 = L.d_comp0.d; a.face0 = L.d_face0.d; a.cell0 = L.d_cell0.d;
       if (p.dimsplit) {
         // stepgrid_dimSplit.f: x, y, z sweeps with their updates, one launch each
         a.scomp0 = L.d_scomp0.d; a.ecell0 = L.d_ecell0.d; a.split = d_split.d;
@@ -1460,7 +1458,7 @@ class Amr3Gpu : public AmrSolver {
         Step3Args b = a;
         b.plist = L.d_plist.d + k; b.np = 1;
         b.sweep0 = L.d_pp.d + (size_t)12 * k; b.comp0 = L.d_pp.d + (size_t)12 * k + 6;
-        b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k; b.brick0 = L.d_brick0.d + k;
+        b.face0 = L.d_face0.d + k; b.cell0 = L.d_cell0.d + k;
         long long it[3];
         if (p.dimsplit) {
           b.scomp0 = L.d_spp.d + (size_t)8 * k; b.ecell0 = L.d_spp.d + (size_t)8 * k + 6; b.split = d_split.d;
@@ -1682,13 +1680,13 @@ class Amr3Gpu : public AmrSolver {
       vp[np + k] = R;
     }
     // step prefixes of both lists, as compile_step builds them for a level:
-    // [sweep0 3*(n+1) | comp0 3*(n+1) | face0 n+1 | cell0 n+1 | brick0 n+1] per list
+    // [sweep0 3*(n+1) | comp0 3*(n+1) | face0 n+1 | cell0 n+1] per list
     std::vector<long long> pre;
     long long items[2][3], slots[2], faces[2], cells[2], base[2];
     for (int li = 0; li < 2; ++li) {
       base[li] = (long long)pre.size();
       const int n = np, first = li * np;
-      std::vector<long long> sw(3 * (size_t)(n + 1), 0), cp(3 * (size_t)(n + 1), 0), fc(n + 1, 0), ce(n + 1, 0), bk(n + 1, 0);
+      std::vector<long long> sw(3 * (size_t)(n + 1), 0), cp(3 * (size_t)(n + 1), 0), fc(n + 1, 0), ce(n + 1, 0);
       long long slot = 0;
       for (int d = 0; d < 3; ++d) {
         long long comp = 0;
@@ -1709,14 +1707,12 @@ class Amr3Gpu : public AmrSolver {
         const long long mx = V.ihi - V.ilo + 1, my = V.jhi - V.jlo + 1, mz = V.khi - V.klo + 1;
         fc[k + 1] = fc[k] + (mx + 1) * (my + 1) * (mz + 1);
         ce[k + 1] = ce[k] + mx * my * mz;
-        bk[k + 1] = bk[k] + face3_bricks(mx, my, mz);
       }
       slots[li] = slot; faces[li] = fc[n]; cells[li] = ce[n];
       pre.insert(pre.end(), sw.begin(), sw.end());
       pre.insert(pre.end(), cp.begin(), cp.end());
       pre.insert(pre.end(), fc.begin(), fc.end());
       pre.insert(pre.end(), ce.begin(), ce.end());
-      pre.insert(pre.end(), bk.begin(), bk.end());
     }
     std::vector<int> pl(2 * (size_t)np);
     for (int k = 0; k < 2 * np; ++k) pl[k] = k;
@@ -1737,7 +1733,7 @@ class Amr3Gpu : public AmrSolver {
       a.pool = pool.d; a.patches = rich_vp.d; a.sp = sp;
       a.plist = rich_plist.d + li * np; a.np = np;
       const long long* b = rich_pre.d + base[li];
-      a.sweep0 = b; a.comp0 = b + 3 * (np + 1); a.face0 = b + 6 * (np + 1); a.cell0 = b + 7 * (np + 1); a.brick0 = b + 8 * (np + 1);
+      a.sweep0 = b; a.comp0 = b + 3 * (np + 1); a.face0 = b + 6 * (np + 1); a.cell0 = b + 7 * (np + 1);
       a.stash = d_stash.d; a.stash_stride = slots[li]; a.flux = d_flux.d; a.flux_stride = faces[li];
       a.dt = li == 0 ? 2.0 * dt : dt;
       a.dx = li == 0 ? 2.0 * hx : hx; a.dy = li == 0 ? 2.0 * hy : hy; a.dz = li == 0 ? 2.0 * hz : hz;

@@ -629,41 +629,47 @@ template <int NV>
 __device__ __forceinline__ int hidx(int s, int d, int m) { return 8 * NV + ((s - 1) * 3 + (d + 1)) * NV + m; }
 
 // ------------------------------------------------------------------- faces
+constexpr int FB_I = 8, FB_J = 4, FB_K = 4;  // face bricks: one warp per k-plane, a block per brick
 template <class T, int NV>
 __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
-  // bricks [brick0[0], brick0[np]): the level's, or one patch's through a one-patch view.
-  // blockIdx.y is the face direction; a block takes one brick of face cells of that
-  // direction, 8 x 4 x 4 (i, j, k), with its 128 threads laid out so that each warp's
-  // loads of the three sweeps' staged increments touch few sectors: the x, y and z
-  // stashes are contiguous along i, j and k, and a warp covers 2x4x4 (x-faces), 4x2x4
-  // (y-faces) or 4x4x2 (z-faces) cells. The sums of every face are the same; only which
-  // thread makes them changes.
-  const long long firstb = A.brick0[0], totalb = A.brick0[A.np];
+  // face cells [face0[0], face0[np]): the level's, or one patch's through a one-patch view
+  const long long first = A.face0[0], total = A.face0[A.np];
   const long long ss = A.stash_stride;
   const T* S = static_cast<const T*>(A.stash);
-  const int fdir = blockIdx.y;
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  int di, dj, dk;
-  if (fdir == 0) { di = (l & 1) + 2 * w; dj = (l >> 1) & 3; dk = l >> 3; }
-  else if (fdir == 1) { di = (l & 3) + 4 * (w & 1); dj = ((l >> 2) & 1) + 2 * (w >> 1); dk = l >> 3; }
-  else { di = (l & 3) + 4 * (w & 1); dj = (l >> 2) & 3; dk = (l >> 4) + 2 * (w >> 1); }
-  for (long long bidx = firstb + blockIdx.x; bidx < totalb; bidx += gridDim.x) {
-    const int pi = find_patch(A.brick0, A.np, bidx);
+  for (long long t = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int pi = find_patch(A.face0, A.np, t);
     const PatchDev& P = A.patches[A.plist[pi]];
     const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
+    // Thread t takes the face cells of its patch in brick order: slabs of FB_K k-planes,
+    // rows of FB_J j-lines in a slab, bricks of FB_I faces in a row (the last of each
+    // smaller), i fastest inside a brick. A warp then reads the j- and k-contiguous
+    // stashes of the y and z sweeps in whole sectors, and the warps of a block share
+    // them through L1. The sums of every face are the same; only which thread makes
+    // them changes.
     const int NI = mx + 1, NJ = my + 1, NK = mz + 1;
-    const int nbi = (NI + FB_I - 1) / FB_I, nbj = (NJ + FB_J - 1) / FB_J;
-    const long long loc = bidx - A.brick0[pi];
-    const int ib = (int)(loc % nbi), jb = (int)((loc / nbi) % nbj), kb = (int)(loc / ((long long)nbi * nbj));
-    const int i = ib * FB_I + di + 1, j = jb * FB_J + dj + 1, k = kb * FB_K + dk + 1;
-    if (i > NI || j > NJ || k > NK) continue;
+    const long long loc = t - A.face0[pi];
+    const long long slab = (long long)NI * NJ * FB_K;
+    const int kb = (int)(loc / slab);
+    const int kcnt = min(FB_K, NK - kb * FB_K);
+    const long long r1 = loc - kb * slab;
+    const long long row = (long long)NI * FB_J * kcnt;
+    const int jb = (int)(r1 / row);
+    const int jcnt = min(FB_J, NJ - jb * FB_J);
+    const int r2 = (int)(r1 - jb * row);
+    const int bsz = FB_I * jcnt * kcnt;
+    const int ib = r2 / bsz;
+    const int icnt = min(FB_I, NI - ib * FB_I);
+    const int r3 = r2 - ib * bsz;
+    const int i = ib * FB_I + r3 % icnt + 1;
+    const int j = jb * FB_J + (r3 / icnt) % jcnt + 1;
+    const int k = kb * FB_K + r3 / (icnt * jcnt) + 1;
     const long long bx = A.sweep0[pi], by = A.sweep0[(A.np + 1) + pi], bz = A.sweep0[2 * (A.np + 1) + pi];
     auto xs = [&](int jj, int kk, int ii) { return bx + ((long long)(kk * (my + 2) + jj) * (mx + 1) + (ii - 1)); };
     auto ys = [&](int ii, int kk, int jj) { return by + ((long long)(kk * (mx + 2) + ii) * (my + 1) + (jj - 1)); };
     auto zs = [&](int ii, int jj, int kk) { return bz + ((long long)(jj * (mx + 2) + ii) * (mz + 1) + (kk - 1)); };
     T* F = static_cast<T*>(A.flux) + A.face0[pi] + ((long long)(k - 1) * NJ + (j - 1)) * NI + (i - 1);
     const long long fs = A.flux_stride;
-    if (fdir == 0 && j <= my && k <= mz) {  // x-face i
+    if (j <= my && k <= mz) {  // x-face i
       T fm[NV], fp[NV];
       const long long sx = xs(j, k, i);
 #pragma unroll
@@ -695,7 +701,7 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
 #pragma unroll
       for (int m = 0; m < NV; ++m) { F[(0 * NV + m) * fs] = fm[m]; F[(1 * NV + m) * fs] = fp[m]; }
     }
-    if (fdir == 1 && i <= mx && k <= mz) {  // y-face j
+    if (i <= mx && k <= mz) {  // y-face j
       T gm[NV], gp[NV];
 #pragma unroll
       for (int m = 0; m < NV; ++m) gm[m] = T(0);
@@ -729,7 +735,7 @@ __global__ void __launch_bounds__(128) face3_kernel(Step3Args A) {
 #pragma unroll
       for (int m = 0; m < NV; ++m) { F[(2 * NV + m) * fs] = gm[m]; F[(3 * NV + m) * fs] = gp[m]; }
     }
-    if (fdir == 2 && i <= mx && j <= my) {  // z-face k
+    if (i <= mx && j <= my) {  // z-face k
       T hm[NV], hp[NV];
 #pragma unroll
       for (int m = 0; m < NV; ++m) hm[m] = T(0);
@@ -1367,8 +1373,7 @@ static int launch_step3_t(const Step3Args& a, const long long items[3], long lon
     if (items[2] > 0) { sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, smem, s>>>(a); ++n; }
   }
   AMR_CUDA(cudaGetLastError());
-  // a block per brick (about faces / 128 of them; the kernel strides over the rest)
-  if (faces > 0) { face3_kernel<T, PH::NV><<<dim3(grid_for(faces, 128), 3), 128, 0, s>>>(a); ++n; }
+  if (faces > 0) { face3_kernel<T, PH::NV><<<grid_for(faces, 128), 128, 0, s>>>(a); ++n; }
   if (cells > 0) { update3_kernel<T, PH::NV><<<grid_for(cells, 256), 256, 0, s>>>(a); ++n; }
   AMR_CUDA(cudaGetLastError());
   return n;

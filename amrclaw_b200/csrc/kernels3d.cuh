@@ -34,7 +34,6 @@ struct Step3Args {
   const long long* comp0;    // [3][np+1]: first interface of each patch, per direction ((n1+3) per pencil)
   const long long* face0;    // [np+1]: first face cell of each patch ((mx+1)(my+1)(mz+1) each)
   const long long* cell0;    // [np+1]: first interior cell of each patch (mx*my*mz each)
-  const long long* brick0;   // [np+1]: first face brick of each patch (face3_bricks each)
   long long stash_stride;    // slots of one direction region x 3 (SoA stride)
   void* stash;               // [stash_values(meqn)][stash_stride]
   void* flux;                // [6 comps][meqn][face cells]
@@ -101,13 +100,6 @@ struct Gauge3Job { int patch; int ii, jj, kk; int slot; double xoff, yoff, zoff;
 // flux differencing; FP64 registers, register corrections, averages and totals).
 // interfaces_per_dir: the interfaces (comp0 ranges) of each sweep direction.
 // returns the number of kernels launched
-// The face gather takes the face cells of a patch in bricks of FB_I x FB_J x FB_K, one
-// block per brick.
-constexpr int FB_I = 8, FB_J = 4, FB_K = 4;
-__host__ __device__ inline long long face3_bricks(long long mx, long long my, long long mz) {
-  return ((mx + 1 + FB_I - 1) / FB_I) * ((my + 1 + FB_J - 1) / FB_J) * ((mz + 1 + FB_K - 1) / FB_K);
-}
-
 // Two side streams and the events that fork them off the solve's stream and join them back:
 // the three sweep directions of a level (independent of one another) then run at once, and
 // the tail blocks of one direction overlap the others instead of leaving SMs idle.

@@ -30,7 +30,7 @@ def _rank(rank, world, port, out):
 
 def test_two_gloo_ranks_take_max_time_and_sum_cells():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
