@@ -262,11 +262,15 @@ class GaugeData:
     min_time_increment: float = 0.0
 
     def write(self, path: str) -> None:
-        # gauges_module.f90:92: gauge_num x y [z] t_start t_end (+ min_time_increment)
+        # gauges_module.f90:92: gauge_num x y [z] t_start t_end (+ min_time_increment). The
+        # location and times carry the digits the reference's writer gives them
+        # (src/python/amrclaw/data.py:246: %17.10e and %13.6e): a gauge on a cell edge lands
+        # in the same grid as it does there.
         w = _Writer(path)
         w.put("num_gauges", len(self.gauges))
         for g in self.gauges:
-            w.row("%i " % int(g[0]) + "".join("%20.14e  " % float(x) for x in g[1:]) + "%20.14e" % float(self.min_time_increment))
+            w.row("%4i" % int(g[0]) + "".join("  %17.10e" % float(x) for x in g[1:-2]) +
+                  "".join("  %13.6e" % float(x) for x in g[-2:]) + "  %20.14e" % float(self.min_time_increment))
         w.close()
 
 

@@ -109,6 +109,7 @@ struct Amr2 {
   ProbParams prob;
   std::string problem;
   double prob_x0 = 0.1, prob_x1 = 0.6, prob_y0 = 0.1, prob_y1 = 0.6, prob_width = 0.2;
+  double ann[8] = {0};  // advection_annulus: A1, beta1, x1, y1, A2, beta2, x2, y2 (setprob.f)
   int flag_component = 0;  // 0 = all components (flag2refine2.f90 default), else one component
 
   // ---------------- state (amr_module)
@@ -225,6 +226,11 @@ struct Amr2 {
       prob.cc = std::sqrt(prob.bulk / prob.rho); prob.zz = prob.rho * prob.cc;
       prob_width = s.dget("width", problem == "acoustics_cosine" ? 0.2 : 0.05);
       prob_x0 = s.dget("r0", problem == "acoustics_cosine" ? 0.5 : 0.3);
+    } else if (problem == "advection_annulus") {
+      // tests/advection_2d_annulus/setprob.f: the two Gaussians of qinit.f
+      prob.solver = SOLVER_VC_ADVECTION;
+      const char* names[8] = {"A1", "beta1", "x1", "y1", "A2", "beta2", "x2", "y2"};
+      for (int k = 0; k < 8; ++k) ann[k] = s.d(names[k]);
     } else if (problem == "euler_quadrants") {
       prob.solver = SOLVER_EULER; prob.gamma = s.d("gamma"); prob.gamma1 = prob.gamma - 1.0;
       prob.efix = s.iget("efix", 1) != 0;
@@ -269,6 +275,19 @@ struct Amr2 {
           at(1, i, j) = std::exp(-(z * z)); at(2, i, j) = 0.0; at(3, i, j) = 0.0;
         }
       }
+    } else if (problem == "advection_annulus") {
+      // tests/advection_2d_annulus/qinit.f: two Gaussians at the physical point of the
+      // cell centre (mapc2p.f)
+      for (int i = 1; i <= mx; ++i) {
+        const double xc = xl + (i - 0.5) * dx;
+        for (int j = 1; j <= my; ++j) {
+          const double yc = yl + (j - 0.5) * dy;
+          double xp, yp;
+          mapc2p_annulus(xc, yc, xp, yp);
+          at(1, i, j) = ann[0] * std::exp(-ann[1] * ((xp - ann[2]) * (xp - ann[2]) + (yp - ann[3]) * (yp - ann[3]))) +
+                        ann[4] * std::exp(-ann[5] * ((xp - ann[6]) * (xp - ann[6]) + (yp - ann[7]) * (yp - ann[7])));
+        }
+      }
     } else if (problem == "euler_quadrants") {
       // examples/euler_2d_quadrants/qinit.f:33-72
       const double rpp[5] = {0, 1.5, 0.3, 0.029032258064516, 0.3};
@@ -292,6 +311,38 @@ struct Amr2 {
         }
       }
     }
+  }
+
+  // tests/advection_2d_annulus/mapc2p.f: polar coordinates, xc = r, yc = theta
+  static void mapc2p_annulus(double xc, double yc, double& xp, double& yp) {
+    xp = xc * std::cos(yc);
+    yp = xc * std::sin(yc);
+  }
+  // tests/advection_2d_annulus/stream.f
+  static double stream_annulus(double x, double y) { return 3.1415926535897931 * (x * x + y * y); }
+
+  // setaux: aux(naux, 1-mbc:mx+mbc, 1-mbc:my+mbc) of a patch with lower corner (xlow, ylow).
+  // tests/advection_2d_annulus/setaux.f: the edge velocities by differencing the stream
+  // function between mapped corners, and the capacity kappa = (mapped area) / (dxc*dyc).
+  // It sets every cell, so values copied in before (icall) are overwritten.
+  void setaux(int mbc, int mx, int my, double xlow, double ylow, double dxc, double dyc, double* aux) const {
+    if (problem != "advection_annulus") throw std::runtime_error("setaux: no aux arrays for problem " + problem);
+    FArr A{aux, naux, mx + 2 * mbc, my + 2 * mbc};
+    for (int j = 1 - mbc; j <= my + mbc; ++j)
+      for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+        double xc[5], yc[5], xp[5], yp[5];
+        xc[0] = xlow + (i - 1) * dxc; yc[0] = ylow + (j - 1) * dyc;
+        xc[1] = xc[0]; yc[1] = yc[0] + dyc;
+        xc[2] = xc[0] + dxc; yc[2] = yc[0] + dyc;
+        xc[3] = xc[0] + dxc; yc[3] = yc[0];
+        for (int c = 0; c < 4; ++c) mapc2p_annulus(xc[c], yc[c], xp[c], yp[c]);
+        A(1, i + mbc, j + mbc) = (stream_annulus(xp[1], yp[1]) - stream_annulus(xp[0], yp[0])) / dyc;
+        A(2, i + mbc, j + mbc) = -(stream_annulus(xp[3], yp[3]) - stream_annulus(xp[0], yp[0])) / dxc;
+        xp[4] = xp[0]; yp[4] = yp[0];
+        double area = 0.0;
+        for (int c = 0; c < 4; ++c) area = area + 0.5 * (yp[c] + yp[c + 1]) * (xp[c + 1] - xp[c]);
+        A(3, i + mbc, j + mbc) = area / (dxc * dyc);
+      }
   }
 
   // =================================================== node store (nodget.f)
@@ -916,22 +967,29 @@ struct Amr2 {
   }
 
   // =================================================== same-level copies (icall / intcopy)
-  void icall(double* valp, int nrow, int ncol, int ilo, int ihi, int jlo, int jhi, int level, int iputst, int jputst) {
-    FArr val{valp, nvar, nrow, ncol};
+  // icall.f: q and (auxp != nullptr) aux of the intersecting grids' interiors
+  void icall(double* valp, int nrow, int ncol, int ilo, int ihi, int jlo, int jhi, int level, int iputst, int jputst,
+             double* auxp = nullptr) {
+    FArr val{valp, nvar, nrow, ncol}, aux{auxp, naux, nrow, ncol};
     for (int mptr = lstart[level]; mptr != 0; mptr = node[mptr].levelptr) {
       const Node2& g = node[mptr];
       const int ixlo = std::max(g.ilo, ilo), ixhi = std::min(g.ihi, ihi), jxlo = std::max(g.jlo, jlo), jxhi = std::min(g.jhi, jhi);
       if (!(ixlo <= ixhi && jxlo <= jxhi)) continue;
       const int mitot = mitot_of(mptr);
-      for (int j = jxlo; j <= jxhi; ++j) for (int i = ixlo; i <= ixhi; ++i) for (int ivar = 1; ivar <= nvar; ++ivar)
-        val(ivar, i - ilo + iputst, j - jlo + jputst) = g.q1[(ivar - 1) + (size_t)nvar * ((j - g.jlo + nghost) * (size_t)mitot + (i - g.ilo + nghost))];
+      for (int j = jxlo; j <= jxhi; ++j)
+        for (int i = ixlo; i <= ixhi; ++i) {
+          const size_t at = (j - g.jlo + nghost) * (size_t)mitot + (i - g.ilo + nghost);
+          for (int ivar = 1; ivar <= nvar; ++ivar) val(ivar, i - ilo + iputst, j - jlo + jputst) = g.q1[(ivar - 1) + (size_t)nvar * at];
+          if (auxp)
+            for (int ia = 1; ia <= naux; ++ia) aux(ia, i - ilo + iputst, j - jlo + jputst) = g.aux[(ia - 1) + (size_t)naux * at];
+        }
     }
   }
   void intcopy(double* valp, int nrow, int ncol, int ilo, int ihi, int jlo, int jhi, int level, int iputst, int jputst) {
     icall(valp, nrow, ncol, ilo, ihi, jlo, jhi, level, iputst, jputst);  // identical for naux = 0
   }
-  // preintcopy.f / preicall.f (non-spherical branch)
-  void preintcopy(double* valp, int nrow, int ncol, int ilo, int ihi, int jlo, int jhi, int level) {
+  // preintcopy.f / preicall.f (non-spherical branch; aux with auxp)
+  void preintcopy(double* valp, int nrow, int ncol, int ilo, int ihi, int jlo, int jhi, int level, double* auxp = nullptr) {
     int ist[3], iend[3], jst[3], jend[3], ishift[3], jshift[3];
     if (xperdom) {
       ist[0] = ilo; ist[1] = 0; ist[2] = iregsz[level]; iend[0] = -1; iend[1] = iregsz[level] - 1; iend[2] = ihi;
@@ -953,7 +1011,8 @@ struct Amr2 {
       for (int j = 0; j < 3; ++j) {
         const int j1 = std::max(jlo, jst[j]), j2 = std::min(jhi, jend[j]);
         if (j1 > j2) continue;
-        icall(valp, nrow, ncol, i1 + ishift[i], i2 + ishift[i], j1 + jshift[j], j2 + jshift[j], level, (i1 - ilo) + 1, (j1 - jlo) + 1);
+        icall(valp, nrow, ncol, i1 + ishift[i], i2 + ishift[i], j1 + jshift[j], j2 + jshift[j], level, (i1 - ilo) + 1, (j1 - jlo) + 1,
+              auxp);
       }
     }
   }
@@ -972,26 +1031,40 @@ struct Amr2 {
       const int ichi = (k.ihi + 1) / intratx[level - 1], jchi = (k.jhi + 1) / intraty[level - 1];
       const int nrow = ichi - iclo + 1, ncol = jchi - jclo + 1;
       const double xl = k.xlo - hxc, yb = k.ylo - hyc, xr = k.xhi + hxc, yt = k.yhi + hyc;
-      std::vector<double> tmp((size_t)nrow * ncol * nvar, 0.0);
+      std::vector<double> tmp((size_t)nrow * ncol * nvar, 0.0), tx((size_t)nrow * ncol * naux, NEEDS_TO_BE_SET);
+      double* txp = naux > 0 ? tx.data() : nullptr;
       const bool sticks = (iclo < 0 || ichi == iregsz[levc] || jclo < 0 || jchi == jregsz[levc]);
-      if (sticks && (xperdom || yperdom || spheredom)) preintcopy(tmp.data(), nrow, ncol, iclo, ichi, jclo, jchi, level - 1);
-      else icall(tmp.data(), nrow, ncol, iclo, ichi, jclo, jchi, level - 1, 1, 1);
+      if (sticks && (xperdom || yperdom || spheredom)) preintcopy(tmp.data(), nrow, ncol, iclo, ichi, jclo, jchi, level - 1, txp);
+      else icall(tmp.data(), nrow, ncol, iclo, ichi, jclo, jchi, level - 1, 1, 1, txp);
+      // saveqc.f:86-90: the ring's aux where it leaves the domain
+      if (naux > 0 && sticks) setaux(0, nrow, ncol, xl, yb, hxc, hyc, txp);
       bc2amr(tmp.data(), nrow, ncol, hxc, hyc, xl, xr, yb, yt);
       // cstore.f:4-63
       FArr qc{tmp.data(), nvar, nrow, ncol};
       double* qc1d = k.ffl.data() + (size_t)nvar * lenbc;
       int index = 0;
-      for (int j = 2; j <= ncol - 1; ++j) { ++index; for (int iv = 1; iv <= nvar; ++iv) qc1d[(iv - 1) + nvar * (index - 1)] = qc(iv, 1, j); }
-      for (int i = 2; i <= nrow - 1; ++i) { ++index; for (int iv = 1; iv <= nvar; ++iv) qc1d[(iv - 1) + nvar * (index - 1)] = qc(iv, i, ncol); }
-      for (int j = 2; j <= ncol - 1; ++j) { ++index; for (int iv = 1; iv <= nvar; ++iv) qc1d[(iv - 1) + nvar * (index - 1)] = qc(iv, nrow, j); }
-      for (int i = 2; i <= nrow - 1; ++i) { ++index; for (int iv = 1; iv <= nvar; ++iv) qc1d[(iv - 1) + nvar * (index - 1)] = qc(iv, i, 1); }
+      FArr ac{txp, naux, nrow, ncol};
+      double* auxc1d = k.ffl.data() + (size_t)2 * nvar * lenbc;
+      auto put = [&](int ii, int jj) {
+        ++index;
+        for (int iv = 1; iv <= nvar; ++iv) qc1d[(iv - 1) + nvar * (index - 1)] = qc(iv, ii, jj);
+        for (int ia = 1; ia <= naux; ++ia) auxc1d[(ia - 1) + naux * (index - 1)] = ac(ia, ii, jj);
+      };
+      for (int j = 2; j <= ncol - 1; ++j) put(1, j);
+      for (int i = 2; i <= nrow - 1; ++i) put(i, ncol);
+      for (int j = 2; j <= ncol - 1; ++j) put(nrow, j);
+      for (int i = 2; i <= nrow - 1; ++i) put(i, 1);
       (void)time_k;
     }
   }
 
   // ================================================================== qad
+  // qad.f:4-370. aux: the fine grid's aux (naux, mitot, mjtot), auxc1d: the coarse ring's
+  // (naux, lenbc); the aux of each Riemann problem comes from the cell of its q, except that
+  // a face-type component (xleft / yleft) on the fine grid's lower face takes the fine
+  // cell's own face value (qad.f:79-89, 175-185, 246-256, 298-308)
   void qad(double* valbigp, int mitot, int mjtot, double* svdflx, const double* qc1d, int lenbc, int lratiox, int lratioy,
-           double hx, double hy, double delt) {
+           double hx, double hy, double delt, const double* aux, const double* auxc1d) {
     (void)lenbc;
     FArr valbig{valbigp, nvar, mitot, mjtot};
     const int max1dp1 = std::max(mitot, mjtot) + 2;
@@ -1010,17 +1083,32 @@ struct Amr2 {
     Slice AM{amdq.data(), nvar, 1 - mbc}, AP{apdq.data(), nvar, 1 - mbc};
     Waves WV{wave.data(), nvar, mwaves, 1 - mbc};
     Slice S{s.data(), mwaves, 1 - mbc};
-    Slice AUX{auxd.data(), 1, 0};
+    (void)auxd;
+    const int la = std::max(naux, 1);
+    std::vector<double> auxl((size_t)la * max1dp1, 0.0), auxr = auxl;
+    Slice AXL{auxl.data(), la, 1 - mbc}, AXR{auxr.data(), la, 1 - mbc};
+    auto al = [&](int ma, int p) -> double& { return auxl[(ma - 1) + la * (p - 1)]; };
+    auto ar = [&](int ma, int p) -> double& { return auxr[(ma - 1) + la * (p - 1)]; };
+    FArr AF{(double*)aux, naux, mitot, mjtot};
+    auto AC = [&](int ma, int k) { return auxc1d[(ma - 1) + naux * (k - 1)]; };
+    auto is_type = [&](int ma, const char* t) { return auxtype[ma - 1] == t; };
     const int nc = mjtot - 2 * nghost, nr = mitot - 2 * nghost;
     int index = 0;
     // side 1
-    for (int j = nghost + 1; j <= mjtot - nghost; ++j) for (int iv = 1; iv <= nvar; ++iv) pl(iv, j - nghost + 1) = valbig(iv, nghost, j);
+    for (int j = nghost + 1; j <= mjtot - nghost; ++j) {
+      for (int ma = 1; ma <= naux; ++ma) al(ma, j - nghost + 1) = is_type(ma, "xleft") ? AF(ma, nghost + 1, j) : AF(ma, nghost, j);
+      for (int iv = 1; iv <= nvar; ++iv) pl(iv, j - nghost + 1) = valbig(iv, nghost, j);
+    }
     int lind = 0;
     for (int jc = 1; jc <= (mjtot - 2 * nghost) / lratioy; ++jc) {
       ++index;
-      for (int l = 1; l <= lratioy; ++l) { ++lind; for (int iv = 1; iv <= nvar; ++iv) pr(iv, lind) = QC(iv, index); }
+      for (int l = 1; l <= lratioy; ++l) {
+        ++lind;
+        for (int ma = 1; ma <= naux; ++ma) ar(ma, lind) = AC(ma, index);
+        for (int iv = 1; iv <= nvar; ++iv) pr(iv, lind) = QC(iv, index);
+      }
     }
-    rpn2(prob, 1, nvar, mwaves, mbc, nc + 1 - 2 * nghost, QL, QR, AUX, AUX, WV, S, AM, AP);
+    rpn2(prob, 1, nvar, mwaves, mbc, nc + 1 - 2 * nghost, QL, QR, AXL, AXR, WV, S, AM, AP);
     int influx = 0;
     for (int j = 1; j <= nc / lratioy; ++j) {
       ++influx;
@@ -1031,13 +1119,21 @@ struct Amr2 {
     }
     // side 2
     if (mjtot != 2 * nghost + 1) {
-      for (int i = nghost + 1; i <= mitot - nghost; ++i) for (int iv = 1; iv <= nvar; ++iv) pr(iv, i - nghost) = valbig(iv, i, mjtot - nghost + 1);
+      for (int i = nghost + 1; i <= mitot - nghost; ++i) {
+        for (int ma = 1; ma <= naux; ++ma) ar(ma, i - nghost) = AF(ma, i, mjtot - nghost + 1);
+        for (int iv = 1; iv <= nvar; ++iv) pr(iv, i - nghost) = valbig(iv, i, mjtot - nghost + 1);
+      }
       lind = 0;
       for (int ic = 1; ic <= (mitot - 2 * nghost) / lratiox; ++ic) {
         ++index;
-        for (int l = 1; l <= lratiox; ++l) { ++lind; for (int iv = 1; iv <= nvar; ++iv) pl(iv, lind + 1) = QC(iv, index); }
+        for (int l = 1; l <= lratiox; ++l) {
+          ++lind;
+          for (int ma = 1; ma <= naux; ++ma)
+            al(ma, lind + 1) = is_type(ma, "yleft") ? AF(ma, (ic - 1) * lratiox + nghost + l, mjtot - nghost + 1) : AC(ma, index);
+          for (int iv = 1; iv <= nvar; ++iv) pl(iv, lind + 1) = QC(iv, index);
+        }
       }
-      rpn2(prob, 2, nvar, mwaves, mbc, nr + 1 - 2 * nghost, QL, QR, AUX, AUX, WV, S, AM, AP);
+      rpn2(prob, 2, nvar, mwaves, mbc, nr + 1 - 2 * nghost, QL, QR, AXL, AXR, WV, S, AM, AP);
       for (int i = 1; i <= nr / lratiox; ++i) {
         ++influx;
         const int ifine = (i - 1) * lratiox;
@@ -1047,13 +1143,21 @@ struct Amr2 {
       }
     }
     // side 3
-    for (int j = nghost + 1; j <= mjtot - nghost; ++j) for (int iv = 1; iv <= nvar; ++iv) pr(iv, j - nghost) = valbig(iv, mitot - nghost + 1, j);
+    for (int j = nghost + 1; j <= mjtot - nghost; ++j) {
+      for (int ma = 1; ma <= naux; ++ma) ar(ma, j - nghost) = AF(ma, mitot - nghost + 1, j);
+      for (int iv = 1; iv <= nvar; ++iv) pr(iv, j - nghost) = valbig(iv, mitot - nghost + 1, j);
+    }
     lind = 0;
     for (int jc = 1; jc <= (mjtot - 2 * nghost) / lratioy; ++jc) {
       ++index;
-      for (int l = 1; l <= lratioy; ++l) { ++lind; for (int iv = 1; iv <= nvar; ++iv) pl(iv, lind + 1) = QC(iv, index); }
+      for (int l = 1; l <= lratioy; ++l) {
+        ++lind;
+        for (int ma = 1; ma <= naux; ++ma)
+          al(ma, lind + 1) = is_type(ma, "xleft") ? AF(ma, mitot - nghost + 1, (jc - 1) * lratioy + nghost + l) : AC(ma, index);
+        for (int iv = 1; iv <= nvar; ++iv) pl(iv, lind + 1) = QC(iv, index);
+      }
     }
-    rpn2(prob, 1, nvar, mwaves, mbc, nc + 1 - 2 * nghost, QL, QR, AUX, AUX, WV, S, AM, AP);
+    rpn2(prob, 1, nvar, mwaves, mbc, nc + 1 - 2 * nghost, QL, QR, AXL, AXR, WV, S, AM, AP);
     for (int j = 1; j <= nc / lratioy; ++j) {
       ++influx;
       const int jfine = (j - 1) * lratioy;
@@ -1063,13 +1167,20 @@ struct Amr2 {
     }
     // side 4
     if (mjtot != 2 * nghost + 1) {
-      for (int i = nghost + 1; i <= mitot - nghost; ++i) for (int iv = 1; iv <= nvar; ++iv) pl(iv, i - nghost + 1) = valbig(iv, i, nghost);
+      for (int i = nghost + 1; i <= mitot - nghost; ++i) {
+        for (int ma = 1; ma <= naux; ++ma) al(ma, i - nghost + 1) = is_type(ma, "yleft") ? AF(ma, i, nghost + 1) : AF(ma, i, nghost);
+        for (int iv = 1; iv <= nvar; ++iv) pl(iv, i - nghost + 1) = valbig(iv, i, nghost);
+      }
       lind = 0;
       for (int ic = 1; ic <= (mitot - 2 * nghost) / lratiox; ++ic) {
         ++index;
-        for (int l = 1; l <= lratiox; ++l) { ++lind; for (int iv = 1; iv <= nvar; ++iv) pr(iv, lind) = QC(iv, index); }
+        for (int l = 1; l <= lratiox; ++l) {
+          ++lind;
+          for (int ma = 1; ma <= naux; ++ma) ar(ma, lind) = AC(ma, index);
+          for (int iv = 1; iv <= nvar; ++iv) pr(iv, lind) = QC(iv, index);
+        }
       }
-      rpn2(prob, 2, nvar, mwaves, mbc, nr + 1 - 2 * nghost, QL, QR, AUX, AUX, WV, S, AM, AP);
+      rpn2(prob, 2, nvar, mwaves, mbc, nr + 1 - 2 * nghost, QL, QR, AXL, AXR, WV, S, AM, AP);
       for (int i = 1; i <= nr / lratiox; ++i) {
         ++influx;
         const int ifine = (i - 1) * lratiox;
@@ -1168,7 +1279,8 @@ struct Amr2 {
     const double xlow = g.xlo - nghost * hx, ylow = g.ylo - nghost * hy;
     if (g.has_ffl) {
       const int lenbc = 2 * (nxg / intratx[level - 1] + nyg / intraty[level - 1]);
-      qad(g.q1.data(), mitot, mjtot, g.ffl.data(), g.ffl.data() + (size_t)nvar * lenbc, lenbc, intratx[level - 1], intraty[level - 1], hx, hy, delt);
+      qad(g.q1.data(), mitot, mjtot, g.ffl.data(), g.ffl.data() + (size_t)nvar * lenbc, lenbc, intratx[level - 1], intraty[level - 1], hx, hy, delt,
+          g.aux.data(), g.ffl.data() + (size_t)2 * nvar * lenbc);
     }
     if (!gauges.empty()) update_gauges(g.q1.data(), xlow, ylow, mitot, mjtot, mptr);
     const size_t nf = (size_t)nvar * mitot * mjtot;
@@ -1232,6 +1344,8 @@ struct Amr2 {
       if (iflag % 2 == 1) continue;
       const int mkid = LB(4), lkid = LB(5);
       double sgnm = (iside == 2 || iside == 3 || iside == 6) ? -1.0 : 1.0;
+      // upbnd.f:104-108: with a capacity array the correction is divided by kappa
+      if (mcapa > 0) sgnm = sgnm / node[mptr].aux[(mcapa - 1) + (size_t)naux * ((icrse - 1) + (size_t)mitot * (jcrse - 1))];
       const double* svd = node[mkid].ffl.data();
       for (int iv = 1; iv <= nvar; ++iv)
         val(iv, icrse, jcrse) = val(iv, icrse, jcrse) + sgnm * svd[(size_t)nvar * (lkid - 1) + iv - 1] / area;
@@ -1258,13 +1372,25 @@ struct Amr2 {
         int jff = jplo * intraty[lget] - k.jlo + nghost + 1;
         const double totrat = intratx[lget] * intraty[lget];
         auto F = [&](int iv, int i, int j) { return k.q1[(iv - 1) + (size_t)nvar * ((j - 1) * (size_t)mi + i - 1)]; };
+        auto FA = [&](int i, int j) { return k.aux[(mcapa - 1) + (size_t)naux * ((j - 1) * (size_t)mi + i - 1)]; };
+        auto CA = [&](int i, int j) { return g.aux[(mcapa - 1) + (size_t)naux * ((j - 1) * (size_t)mitot + i - 1)]; };
         for (int i = iplo - g.ilo + nghost + 1; i <= iphi - g.ilo + nghost + 1; ++i) {
           for (int j = jplo - g.jlo + nghost + 1; j <= jphi - g.jlo + nghost + 1; ++j) {
             for (int iv = 1; iv <= nvar; ++iv) Q(iv, i, j) = 0.0;
-            for (int jco = 1; jco <= intraty[lget]; ++jco)
-              for (int ico = 1; ico <= intratx[lget]; ++ico)
-                for (int iv = 1; iv <= nvar; ++iv) Q(iv, i, j) = Q(iv, i, j) + F(iv, iff + ico - 1, jff + jco - 1);
-            for (int iv = 1; iv <= nvar; ++iv) Q(iv, i, j) = Q(iv, i, j) / totrat;
+            if (mcapa == 0) {
+              for (int jco = 1; jco <= intraty[lget]; ++jco)
+                for (int ico = 1; ico <= intratx[lget]; ++ico)
+                  for (int iv = 1; iv <= nvar; ++iv) Q(iv, i, j) = Q(iv, i, j) + F(iv, iff + ico - 1, jff + jco - 1);
+              for (int iv = 1; iv <= nvar; ++iv) Q(iv, i, j) = Q(iv, i, j) / totrat;
+            } else {
+              // update.f:150-160: kappa-weighted average of the fine cells
+              for (int jco = 1; jco <= intraty[lget]; ++jco)
+                for (int ico = 1; ico <= intratx[lget]; ++ico) {
+                  const double capa = FA(iff + ico - 1, jff + jco - 1);
+                  for (int iv = 1; iv <= nvar; ++iv) Q(iv, i, j) = Q(iv, i, j) + F(iv, iff + ico - 1, jff + jco - 1) * capa;
+                }
+              for (int iv = 1; iv <= nvar; ++iv) Q(iv, i, j) = Q(iv, i, j) / (totrat * CA(i, j));
+            }
             jff += intraty[lget];
           }
           iff += intratx[lget];
@@ -2151,7 +2277,7 @@ struct Amr2 {
 
   // filval.f90:3-214 (naux = 0 branch)
   void filval(double* valp, int mitot, int mjtot, double dx, double dy, int level, double t, int mic, int mjc, double xleft,
-              double xright, double ybot, double ytop, int ilo, int ihi, int jlo, int jhi) {
+              double xright, double ybot, double ytop, int ilo, int ihi, int jlo, int jhi, double* auxp) {
     (void)t;
     const int rx = intratx[level - 1], ry = intraty[level - 1];
     const double dxc = dx * rx, dyc = dy * ry;
@@ -2159,16 +2285,35 @@ struct Amr2 {
     const int iclo = ilo / rx - 1, jclo = jlo / ry - 1, ichi = (ihi + 1) / rx - 1 + 1, jchi = (jhi + 1) / ry - 1 + 1;
     const bool sxf = (ilo < 0) || (ihi >= iregsz[level]), syf = (jlo < 0) || (jhi >= jregsz[level]);
     const bool sxc = (iclo < 0) || (ichi >= iregsz[level - 1]), syc = (jclo < 0) || (jchi >= jregsz[level - 1]);
-    std::vector<double> valc((size_t)nvar * mic * mjc, 0.0);
-    if ((xperdom && sxc) || (yperdom && syc) || spheredom) preintcopy(valc.data(), mic, mjc, iclo, ichi, jclo, jchi, level - 1);
-    else intcopy(valc.data(), mic, mjc, iclo, ichi, jclo, jchi, level - 1, 1, 1);
+    std::vector<double> valc((size_t)nvar * mic * mjc, 0.0), auxc((size_t)naux * mic * mjc, 0.0);
+    FArr val{valp, nvar, mitot, mjtot}, VC{valc.data(), nvar, mic, mjc}, AUX{auxp, naux, mitot, mjtot}, AUXC{auxc.data(), naux, mic, mjc};
+    if (naux == 0) {
+      if ((xperdom && sxc) || (yperdom && syc) || spheredom) preintcopy(valc.data(), mic, mjc, iclo, ichi, jclo, jchi, level - 1);
+      else intcopy(valc.data(), mic, mjc, iclo, ichi, jclo, jchi, level - 1, 1, 1);
+    } else {
+      // filval.f90:75-96: q and aux of the coarse cells, then setaux on the coarse patch
+      for (int j = 1; j <= mjc; ++j) for (int i = 1; i <= mic; ++i) AUXC(1, i, j) = NEEDS_TO_BE_SET;
+      if ((xperdom && sxc) || (yperdom && syc) || spheredom) preintcopy(valc.data(), mic, mjc, iclo, ichi, jclo, jchi, level - 1, auxc.data());
+      else icall(valc.data(), mic, mjc, iclo, ichi, jclo, jchi, level - 1, 1, 1, auxc.data());
+      setaux(0, mic, mjc, xl, yb, dxc, dyc, auxc.data());
+    }
     bc2amr(valc.data(), mic, mjc, dxc, dyc, xl, xr, yb, yt);
-    FArr val{valp, nvar, mitot, mjtot}, VC{valc.data(), nvar, mic, mjc};
-    for (int j = 1; j <= mjtot; ++j) for (int i = 1; i <= mitot; ++i) val(1, i, j) = NEEDS_TO_BE_SET;
-    if ((xperdom && sxf) || (yperdom && syf) || spheredom) preintcopy(valp, mitot, mjtot, ilo - nghost, ihi + nghost, jlo - nghost, jhi + nghost, level);
-    else intcopy(valp, mitot, mjtot, ilo - nghost, ihi + nghost, jlo - nghost, jhi + nghost, level, 1, 1);
     std::vector<double> setflags((size_t)mitot * mjtot);
-    for (int j = 1; j <= mjtot; ++j) for (int i = 1; i <= mitot; ++i) setflags[(i - 1) + (size_t)mitot * (j - 1)] = val(1, i, j);
+    if (naux > 0) {
+      // filval.f90:112-130: copy q and aux from the old grids of the level; the first aux
+      // component marks the cells still to interpolate; then setaux on the new grid
+      for (int j = 1; j <= mjtot; ++j) for (int i = 1; i <= mitot; ++i) AUX(1, i, j) = NEEDS_TO_BE_SET;
+      if ((xperdom && sxf) || (yperdom && syf) || spheredom)
+        preintcopy(valp, mitot, mjtot, ilo - nghost, ihi + nghost, jlo - nghost, jhi + nghost, level, auxp);
+      else icall(valp, mitot, mjtot, ilo - nghost, ihi + nghost, jlo - nghost, jhi + nghost, level, 1, 1, auxp);
+      for (int j = 1; j <= mjtot; ++j) for (int i = 1; i <= mitot; ++i) setflags[(i - 1) + (size_t)mitot * (j - 1)] = AUX(1, i, j);
+      setaux(nghost, mitot - 2 * nghost, mjtot - 2 * nghost, xleft, ybot, dx, dy, auxp);
+    } else {
+      for (int j = 1; j <= mjtot; ++j) for (int i = 1; i <= mitot; ++i) val(1, i, j) = NEEDS_TO_BE_SET;
+      if ((xperdom && sxf) || (yperdom && syf) || spheredom) preintcopy(valp, mitot, mjtot, ilo - nghost, ihi + nghost, jlo - nghost, jhi + nghost, level);
+      else intcopy(valp, mitot, mjtot, ilo - nghost, ihi + nghost, jlo - nghost, jhi + nghost, level, 1, 1);
+      for (int j = 1; j <= mjtot; ++j) for (int i = 1; i <= mitot; ++i) setflags[(i - 1) + (size_t)mitot * (j - 1)] = val(1, i, j);
+    }
     for (int j = 2; j <= mjc - 1; ++j)
       for (int i = 2; i <= mic - 1; ++i)
         for (int iv = 1; iv <= nvar; ++iv) {
@@ -2189,6 +2334,30 @@ struct Amr2 {
             }
           }
         }
+    // fixcapaq.f:4-62: conserve kappa*q, not q, over each coarse cell, adjusting only the
+    // interpolated fine cells
+    if (mcapa != 0)
+      for (int ic = 2; ic <= mic - 1; ++ic)
+        for (int jc = 2; jc <= mjc - 1; ++jc)
+          for (int iv = 1; iv <= nvar; ++iv) {
+            double capaqfine = 0.0;
+            for (int ico = 1; ico <= rx; ++ico) {
+              const int ifine = (ic - 2) * rx + nghost + ico;
+              for (int jco = 1; jco <= ry; ++jco) {
+                const int jfine = (jc - 2) * ry + nghost + jco;
+                capaqfine = capaqfine + AUX(mcapa, ifine, jfine) * val(iv, ifine, jfine);
+              }
+            }
+            const double dcapaq = AUXC(mcapa, ic, jc) * VC(iv, ic, jc) - capaqfine / (double)(rx * ry);
+            for (int ico = 1; ico <= rx; ++ico) {
+              const int ifine = (ic - 2) * rx + nghost + ico;
+              for (int jco = 1; jco <= ry; ++jco) {
+                const int jfine = (jc - 2) * ry + nghost + jco;
+                if (setflags[(ifine - 1) + (size_t)mitot * (jfine - 1)] == NEEDS_TO_BE_SET)
+                  val(iv, ifine, jfine) = val(iv, ifine, jfine) + dcapaq / AUX(mcapa, ifine, jfine);
+              }
+            }
+          }
   }
 
   void gfixup(int lbase, int lfnew) {
@@ -2201,14 +2370,18 @@ struct Amr2 {
       const double hx = hxposs[lcheck], hy = hyposs[lcheck];
       std::vector<int> lnew;
       for (int m = newstl[lcheck]; m != 0; m = node[m].levelptr) lnew.push_back(m);
-      for (int m : lnew) node[m].q1.assign((size_t)nvar * mitot_of(m) * mjtot_of(m), 0.0);
+      for (int m : lnew) {
+        node[m].q1.assign((size_t)nvar * mitot_of(m) * mjtot_of(m), 0.0);
+        node[m].aux.assign((size_t)naux * mitot_of(m) * mjtot_of(m), 0.0);
+      }
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
       for (int k = 0; k < (int)lnew.size(); ++k) {
         const int m = lnew[k];
         Node2& g = node[m];
         const int nxg = g.ihi - g.ilo + 1, nyg = g.jhi - g.jlo + 1;
         const int mic = nxg / intratx[lcheck - 1] + 2, mjc = nyg / intraty[lcheck - 1] + 2;
-        filval(g.q1.data(), mitot_of(m), mjtot_of(m), hx, hy, lcheck, g.time, mic, mjc, g.xlo, g.xhi, g.ylo, g.yhi, g.ilo, g.ihi, g.jlo, g.jhi);
+        filval(g.q1.data(), mitot_of(m), mjtot_of(m), hx, hy, lcheck, g.time, mic, mjc, g.xlo, g.xhi, g.ylo, g.yhi, g.ilo, g.ihi, g.jlo, g.jhi,
+               g.aux.data());
       }
       int mptr = lstart[lcheck];
       while (mptr != 0) {
@@ -2262,6 +2435,10 @@ struct Amr2 {
       double* loc;
       if (first) {
         g.q1.assign(n, 0.0);
+        if (naux > 0) {  // ginit.f:48-58
+          g.aux.assign((size_t)naux * (nxg + 2 * nghost) * (nyg + 2 * nghost), 0.0);
+          setaux(nghost, nxg, nyg, g.xlo, g.ylo, hx, hy, g.aux.data());
+        }
         if (level < mxnest) { g.q2.assign(n, 0.0); g.has_q2 = true; }
         g.time = start_time;
         loc = g.q1.data();
@@ -2360,7 +2537,11 @@ struct Amr2 {
       const Node2& g = node[m];
       const int mitot = mitot_of(m), mjtot = mjtot_of(m);
       for (int j = nghost + 1; j <= mjtot - nghost; ++j)
-        for (int i = nghost + 1; i <= mitot - nghost; ++i) totmass = totmass + g.q1[(size_t)nvar * ((j - 1) * (size_t)mitot + i - 1)];
+        for (int i = nghost + 1; i <= mitot - nghost; ++i) {
+          const size_t at = (j - 1) * (size_t)mitot + i - 1;
+          if (mcapa == 0) totmass = totmass + g.q1[(size_t)nvar * at];
+          else totmass = totmass + g.q1[(size_t)nvar * at] * g.aux[(mcapa - 1) + (size_t)naux * at];  // conck.f:55-59
+        }
     }
     totmass = totmass * hx * hy;
     return totmass;
@@ -2561,7 +2742,21 @@ struct Amr2 {
   // ================================================================ amr2.f90 driver
   void init(const std::string& dir) {
     read_input(dir);
-    if (naux != 0 || mcapa != 0) throw std::runtime_error("2D oracle: aux arrays are not supported for these problems");
+    // amr2.f90:398-425: the capacity component is the aux component typed "capacity"
+    int mc = 0;
+    for (int k = 0; k < naux; ++k) {
+      if (auxtype[k] == "leftface") auxtype[k] = "xleft";
+      if (auxtype[k] == "bottomface") auxtype[k] = "yleft";
+      if (auxtype[k] == "capacity") {
+        if (mc != 0) throw std::runtime_error("only 1 capacity allowed");
+        mc = k + 1;
+      }
+      if (auxtype[k] != "xleft" && auxtype[k] != "yleft" && auxtype[k] != "capacity" && auxtype[k] != "center")
+        throw std::runtime_error("unknown type for auxiliary variables");
+    }
+    if (mc != mcapa) throw std::runtime_error("mcapa does not agree with auxtype");
+    if (naux > 0 && problem != "advection_annulus")
+      throw std::runtime_error("2D oracle: problem " + problem + " has no aux arrays (setaux)");
     hxposs[1] = (xupper - xlower) / nx;
     hyposs[1] = (yupper - ylower) / ny;
     matlabu = output_t0 ? 0 : 1;

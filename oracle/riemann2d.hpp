@@ -17,6 +17,11 @@
 //  * euler: Roe solver, 4 waves (two acoustic, entropy, shear), Harten-Hyman
 //    entropy fix for transonic rarefactions; Roe-linearised transverse solver
 //    (FVMHP 2002, sections 15.3.3-15.3.5, 19.3.3 and 21.6).
+//  * vc_advection: advection in a face-centred velocity field, aux(1) = u at the
+//    left face and aux(2) = v at the bottom face of each cell (the rpn2/rpt2 pair
+//    tests/advection_2d_annulus/Makefile names); the normal speed is the interface's
+//    own face velocity, a transverse split moves asdq with the transverse face
+//    velocities of the cell it came from (FVMHP 2002, sections 9.5 and 20.8).
 #pragma once
 #include <cmath>
 #include <algorithm>
@@ -51,7 +56,16 @@ inline double dsign(double a, double b) { return b >= 0.0 ? std::fabs(a) : -std:
 inline void rpn2(const ProbParams& P, int ixy, int meqn, int mwaves, int mbc, int mx,
                  Slice ql, Slice qr, Slice auxl, Slice auxr, Waves wave, Slice s,
                  Slice amdq, Slice apdq) {
-  (void)auxl; (void)auxr;
+  (void)auxr;
+  if (P.solver == SOLVER_VC_ADVECTION) {
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+      wave(1, 1, i) = ql(1, i) - qr(1, i - 1);
+      s(1, i) = auxl(ixy, i);
+      amdq(1, i) = std::min(auxl(ixy, i), 0.0) * wave(1, 1, i);
+      apdq(1, i) = std::max(auxl(ixy, i), 0.0) * wave(1, 1, i);
+    }
+    return;
+  }
   if (P.solver == SOLVER_ADVECTION) {
     for (int i = 2 - mbc; i <= mx + mbc; ++i) {
       wave(1, 1, i) = ql(1, i) - qr(1, i - 1);
@@ -195,7 +209,18 @@ inline void rpn2(const ProbParams& P, int ixy, int meqn, int mwaves, int mbc, in
 inline void rpt2(const ProbParams& P, int ixy, int imp, int meqn, int mbc, int mx,
                  Slice ql, Slice qr, Slice aux1, Slice aux2, Slice aux3,
                  Slice asdq, Slice bmasdq, Slice bpasdq) {
-  (void)imp; (void)aux1; (void)aux2; (void)aux3;
+  (void)aux1;
+  if (P.solver == SOLVER_VC_ADVECTION) {
+    // kv: the transverse velocity component; i1: the cell asdq belongs to (i-1 for the
+    // amdq side, i for apdq); aux2 holds its row, aux3 the row above
+    const int kv = 3 - ixy;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+      const int i1 = i - 2 + imp;
+      bmasdq(1, i) = std::min(aux2(kv, i1), 0.0) * asdq(1, i);
+      bpasdq(1, i) = std::max(aux3(kv, i1), 0.0) * asdq(1, i);
+    }
+    return;
+  }
   if (P.solver == SOLVER_ADVECTION) {
     const double st = (ixy == 1) ? P.vbar : P.ubar;
     const double stm = std::min(st, 0.0), stp = std::max(st, 0.0);

@@ -99,6 +99,33 @@ def euler_quadrants(n: int = 100, levels: int = 4, tfinal: float = 0.8, ratio: i
     return rd
 
 
+def advection_annulus_regression() -> ClawRunData:
+    """tests/advection_2d_annulus/setrun.py of the reference (gauges 1, 2 pinned): advection
+    on the mapped annulus 0.2 <= r <= 1, with face velocities and the capacity kappa in aux."""
+    rd = ClawRunData(num_dim=2)
+    p = rd.probdata
+    p.add_param("problem", "advection_annulus")
+    for name, val in (("A1", 1.0), ("beta1", 40.0), ("x1", -0.5), ("y1", 0.0),
+                      ("A2", -1.0), ("beta2", 40.0), ("x2", 0.5), ("y2", 0.0)):
+        p.add_param(name, val)
+    c = rd.clawdata
+    c.lower = [0.2, 0.0]; c.upper = [1.0, 2.0 * math.pi]; c.num_cells = [20, 120]
+    c.num_eqn = 1; c.num_waves = 1; c.num_aux = 3; c.capa_index = 3
+    c.output_style = 1; c.num_output_times = 1; c.tfinal = 0.5; c.output_t0 = True
+    c.output_aux_components = "none"; c.output_aux_onlyonce = True
+    c.dt_variable = True; c.dt_initial = 0.005; c.dt_max = 1e99; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.steps_max = 1000; c.order = 2; c.transverse_waves = 2; c.limiter = ["vanleer"]
+    c.bc_lower = ["extrap", "periodic"]; c.bc_upper = ["extrap", "periodic"]
+    rd.gaugedata.gauges = [[1, 0.5, 0.5 * math.pi, 0., 10.], [2, 0.5, 1.5 * math.pi, 0., 10.]]
+    a = rd.amrdata
+    a.amr_levels_max = 3; a.refinement_ratios_x = [2, 2]; a.refinement_ratios_y = [2, 2]; a.refinement_ratios_t = [2, 2]
+    a.aux_type = ["xleft", "yleft", "capacity"]
+    a.flag2refine = True; a.flag2refine_tol = 0.02; a.regrid_interval = 2; a.regrid_buffer_width = 3
+    a.clustering_cutoff = 0.7
+    rd.regiondata.regions = [[1, 2, 0., 10., 0.2, 1., 0., 2. * math.pi], [3, 3, 0., 10., 0.5, 1., 0., 0.5 * math.pi]]
+    return rd
+
+
 def advection_swirl_regression() -> ClawRunData:
     """tests/advection_3d_swirl/setrun.py of the reference (gauges 1, 2 pinned)."""
     rd = ClawRunData(num_dim=3)

@@ -16,7 +16,8 @@ if len(sys.argv) != 2:
     sys.exit("usage: make_golden.py <path of the reference checkout>")
 REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = {"advection_2d_square": [1, 2], "acoustics_2d_radial": [0, 1, 2], "advection_3d_swirl": [1, 2]}
+CASES = {"advection_2d_square": [1, 2], "acoustics_2d_radial": [0, 1, 2], "advection_3d_swirl": [1, 2],
+         "advection_2d_annulus": [1, 2]}
 
 for case, ids in CASES.items():
     rows = []

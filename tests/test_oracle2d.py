@@ -28,6 +28,13 @@ def test_acoustics_radial_gauges_match_reference():
     assert_gauges_match(g, gauge_rows("acoustics_2d_radial"))
 
 
+def test_advection_annulus_gauges_match_reference():
+    # tests/advection_2d_annulus/regression_data/gauge0000{1,2}.txt of the reference: a mapped
+    # grid with face velocities and the capacity kappa in aux (capa_index 3), periodic in theta
+    g = _run(configs.advection_annulus_regression(), 1)
+    assert_gauges_match(g, gauge_rows("advection_2d_annulus"))
+
+
 def test_oracle_detects_a_planted_mistake():
     # A planted change of the limiter must break the pin (the comparison has teeth).
     rd = configs.advection_square_regression()
