@@ -36,11 +36,16 @@
 
 namespace amrb {
 
+// the "not set" marker of aux values (amr_module.f90:170, a default-real literal)
+static const double NEEDS_TO_BE_SET = (double)10.e33f;
+
 // ------------------------------------------------------------------ host patch metadata
 struct HPatch {
   int ilo = 0, ihi = 0, jlo = 0, jhi = 0, level = 0, levelptr = 0, nextfree = 0;
   double xlo = 0, xhi = 0, ylo = 0, yhi = 0, time = 0;
   long long q0 = -1, q1 = -1, nq = 0;
+  long long aux = -1;                // pool offset of the aux array [m][j][i] (enlarged), -1 without aux
+  std::vector<double> haux;          // its host copy (setaux values; icall copies read them)
   long long ffl = -1, nffl = 0;
   int lenbc = 0;
   int cur = 0;
@@ -65,12 +70,17 @@ struct FillProg {
   // the scratch starts at zero each run: programs whose rects come from icall copies
   // (saveqc.f, filval.f90) leave uncovered cells at the reference's initial 0
   bool zero_scratch = false;
+  std::vector<double> capa;  // coarse kappa of the FIXCAPA ops' source rects (filval.f90's auxc)
   DBuf<ScratchRect> d_rects;
   DBuf<FillOp> d_ops;
   DBuf<FillChunk> d_chunks;
   DBuf<BcOp> d_bcs;
+  DBuf<double> d_capa;
   std::vector<int> ch_lo, ch_hi, bc_lo, bc_hi;
-  void clear() { rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); nstages = 0; zero_scratch = false; }
+  void clear() {
+    rects.clear(); ops.clear(); op_stage.clear(); bcs.clear(); bc_stage.clear(); capa.clear();
+    nstages = 0; zero_scratch = false;
+  }
   int add_rect(int ni, int nj, int nvar) {
     ScratchRect r;
     r.off = scratch_len; r.ni = ni; r.nj = nj;
@@ -221,10 +231,43 @@ class Amr2Gpu {
     } else if (pr == "euler_quadrants") {
       prob.solver = SOLVER_EULER; prob.gamma = p.pn("gamma", 1.4); prob.gamma1 = prob.gamma - 1.0;
       prob.efix = (int)p.pn("efix", 1.0);
+    } else if (pr == "advection_annulus") {
+      // tests/advection_2d_annulus: vc advection on the mapped annulus (setprob.f: the two
+      // Gaussians of qinit.f)
+      prob.solver = SOLVER_VC_ADVECTION;
+      const char* names[8] = {"A1", "beta1", "x1", "y1", "A2", "beta2", "x2", "y2"};
+      for (int k = 0; k < 8; ++k) ann[k] = p.pn(names[k], 0.0);
     } else throw std::runtime_error("unknown problem '" + pr + "'");
-    const int me = prob.solver == SOLVER_ADVECTION ? 1 : prob.solver == SOLVER_ACOUSTICS ? 3 : 4;
-    const int mw = prob.solver == SOLVER_ADVECTION ? 1 : prob.solver == SOLVER_ACOUSTICS ? 2 : 4;
+    const bool adv = prob.solver == SOLVER_ADVECTION || prob.solver == SOLVER_VC_ADVECTION;
+    const int me = adv ? 1 : prob.solver == SOLVER_ACOUSTICS ? 3 : 4;
+    const int mw = adv ? 1 : prob.solver == SOLVER_ACOUSTICS ? 2 : 4;
     if (p.nvar != me || p.mwaves != mw) throw std::runtime_error("num_eqn/num_waves do not match the Riemann solver");
+    // aux arrays: amr2.f90:398-425 (one capacity component, typed "capacity"; the types
+    // qad.f reads); only problems with a setaux carry them
+    prob.naux = p.naux;
+    int mc = 0;
+    for (int k = 0; k < p.naux; ++k) {
+      std::string t = k < (int)p.auxtype.size() ? p.auxtype[k] : "";
+      if (t == "leftface") t = "xleft";
+      if (t == "bottomface") t = "yleft";
+      int code;
+      if (t == "xleft") code = AUX_XLEFT;
+      else if (t == "yleft") code = AUX_YLEFT;
+      else if (t == "capacity") code = AUX_CAPACITY;
+      else if (t == "center") code = AUX_CENTER;
+      else throw std::runtime_error("unknown type for auxiliary variables: " + t);
+      if (code == AUX_CAPACITY) {
+        if (mc != 0) throw std::runtime_error("only 1 capacity allowed");
+        mc = k + 1;
+      }
+      if (k < MAXAUX2) prob.auxtype[k] = code;
+    }
+    if (mc != p.mcapa) throw std::runtime_error("capa_index does not agree with aux_type");
+    if (p.naux > 0 && pr != "advection_annulus")
+      throw std::runtime_error("problem '" + pr + "' has no aux arrays (setaux)");
+    if (p.naux > MAXAUX2) throw std::runtime_error("at most " + std::to_string(MAXAUX2) + " aux components in 2D");
+    if (prob.solver == SOLVER_VC_ADVECTION && p.naux < VcAdvection2::NAUX)
+      throw std::runtime_error("vc_advection reads aux(1) and aux(2): num_aux must be at least 2");
     sp.prob = prob;
     for (int k = 0; k < MAXVAR; ++k) sp.mthlim[k] = k < (int)p.mthlim.size() ? p.mthlim[k] : 0;
     sp.order = p.order; sp.trans = p.trans; sp.use_fwaves = p.use_fwaves ? 1 : 0; sp.mcapa = p.mcapa;
@@ -235,6 +278,7 @@ class Amr2Gpu {
   //   advection       [u, v]         (examples/advection_2d_square/setprob.f:4, /cparam/ ubar,vbar)
   //   acoustics       [rho, bulk]    (/cparam/ rho,bulk,cc,zz of the acoustics solvers)
   //   euler_roe_efix  [gamma] or [gamma, efix]  (examples/euler_2d_quadrants/setprob.f:7)
+  //   vc_advection    []             (velocities are aux(1), aux(2); tests/advection_2d_annulus)
   // No constants keep the current ones. The equations and waves of the run must match.
   void set_solver(const std::string& name, const std::vector<double>& v) {
     ProbDev q = prob;
@@ -265,8 +309,12 @@ class Amr2Gpu {
         q.gamma = v[0]; q.gamma1 = q.gamma - 1.0;
         if (v.size() == 2) q.efix = v[1] != 0.0 ? 1 : 0;
       }
+    } else if (name == "vc_advection") {
+      need(1, 1, 0, 0);
+      if (p.naux < VcAdvection2::NAUX) throw std::invalid_argument("vc_advection reads aux(1) and aux(2): the run has no aux arrays");
+      q.solver = SOLVER_VC_ADVECTION;
     } else {
-      throw std::invalid_argument("unknown 2D Riemann solver '" + name + "' (advection, acoustics, euler_roe_efix)");
+      throw std::invalid_argument("unknown 2D Riemann solver '" + name + "' (advection, acoustics, euler_roe_efix, vc_advection)");
     }
     if (q.solver != prob.solver)
       throw std::invalid_argument("Riemann solver '" + name + "' does not solve this run's equations");
@@ -305,6 +353,18 @@ class Amr2Gpu {
           Q(0, i, j) = pv; Q(1, i, j) = 0.0; Q(2, i, j) = 0.0;
         }
       }
+    } else if (pr == "advection_annulus") {
+      // tests/advection_2d_annulus/qinit.f: two Gaussians at the mapped cell centre
+      for (int i = 1; i <= mx; ++i) {
+        const double xc = xl + (i - 0.5) * dx;
+        for (int j = 1; j <= my; ++j) {
+          const double yc = yl + (j - 0.5) * dy;
+          double xp, yp;
+          mapc2p_annulus(xc, yc, xp, yp);
+          Q(0, i, j) = ann[0] * std::exp(-ann[1] * ((xp - ann[2]) * (xp - ann[2]) + (yp - ann[3]) * (yp - ann[3]))) +
+                       ann[4] * std::exp(-ann[5] * ((xp - ann[6]) * (xp - ann[6]) + (yp - ann[7]) * (yp - ann[7])));
+        }
+      }
     } else if (pr == "euler_quadrants") {
       const double rpp[5] = {0, 1.5, 0.3, 0.029032258064516, 0.3};
       const double rpr[5] = {0, 1.5, 0.532258064516129, 0.137992831541219, 0.532258064516129};
@@ -326,6 +386,39 @@ class Amr2Gpu {
       }
     }
   }
+
+  // tests/advection_2d_annulus/mapc2p.f and stream.f
+  static void mapc2p_annulus(double xc, double yc, double& xp, double& yp) {
+    xp = xc * std::cos(yc);
+    yp = xc * std::sin(yc);
+  }
+  static double stream_annulus(double x, double y) { return 3.1415926535897931 * (x * x + y * y); }
+  // setaux of the problem for an array of (mx + 2 mbc) x (my + 2 mbc) cells whose interior
+  // starts at (xlow, ylow): tests/advection_2d_annulus/setaux.f, the edge velocities by
+  // differencing the stream function between mapped corners and kappa = mapped area /
+  // (dxc dyc). It sets every cell. Layout [m][j][i].
+  void setaux(int mbc, int mx, int my, double xlow, double ylow, double dxc, double dyc, std::vector<double>& aux) const {
+    const int mi = mx + 2 * mbc, mj = my + 2 * mbc;
+    const size_t plane = (size_t)mi * mj;
+    aux.assign((size_t)p.naux * plane, 0.0);
+    for (int j = 1 - mbc; j <= my + mbc; ++j)
+      for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+        double xc[5], yc[5], xp[5], yp[5];
+        xc[0] = xlow + (i - 1) * dxc; yc[0] = ylow + (j - 1) * dyc;
+        xc[1] = xc[0]; yc[1] = yc[0] + dyc;
+        xc[2] = xc[0] + dxc; yc[2] = yc[0] + dyc;
+        xc[3] = xc[0] + dxc; yc[3] = yc[0];
+        for (int c = 0; c < 4; ++c) mapc2p_annulus(xc[c], yc[c], xp[c], yp[c]);
+        const size_t k = (size_t)(j + mbc - 1) * mi + (i + mbc - 1);
+        aux[k] = (stream_annulus(xp[1], yp[1]) - stream_annulus(xp[0], yp[0])) / dyc;
+        aux[plane + k] = -(stream_annulus(xp[3], yp[3]) - stream_annulus(xp[0], yp[0])) / dxc;
+        xp[4] = xp[0]; yp[4] = yp[0];
+        double area = 0.0;
+        for (int c = 0; c < 4; ++c) area = area + 0.5 * (yp[c] + yp[c + 1]) * (xp[c + 1] - xp[c]);
+        if (p.naux > 2) aux[2 * plane + k] = area / (dxc * dyc);
+      }
+  }
+  double ann[8] = {0};  // advection_annulus: A1, beta1, x1, y1, A2, beta2, x2, y2
 
   // ================================================================ node numbers (nodget.f / putnod.f)
   int nodget() {
@@ -356,6 +449,9 @@ class Amr2Gpu {
   }
   size_t elem() const { return f32 ? sizeof(float) : sizeof(double); }
 
+  // storage of a new patch; with aux arrays its aux is set by setaux on the patch
+  // (ginit.f:48-58; filval.f90:112-130, whose copies from the old grids the problem's
+  // setaux overwrites) and uploaded
   void alloc_patch(int m) {
     id_hwm = std::max(id_hwm, m + 1);
     HPatch& g = node[m];
@@ -363,10 +459,25 @@ class Amr2Gpu {
     g.q0 = palloc(g.nq);
     g.q1 = palloc(g.nq);
     g.cur = 0;
+    g.aux = -1;
+    g.haux.clear();
+    if (p.naux > 0) {
+      setaux(ng, g.nx(), g.ny(), g.xlo, g.ylo, hxposs[g.level], hyposs[g.level], g.haux);
+      g.aux = palloc((long long)g.haux.size());
+      upload_to(reinterpret_cast<char*>(pool.d) + sizeof(double) * g.aux, g.haux.data(), sizeof(double) * g.haux.size());
+    }
+  }
+  void upload_to(void* dst, const void* src, size_t bytes) {
+    if (!bytes) return;
+    AMR_CUDA(cudaMemcpyAsync(dst, stg.put(src, bytes, st), bytes, cudaMemcpyHostToDevice, st));
+    h2d_bytes += (double)bytes;
   }
   void free_patch(int m) {
     HPatch& g = node[m];
     pfree(g.q0, g.nq); pfree(g.q1, g.nq);
+    if (g.aux >= 0) pfree(g.aux, (long long)g.haux.size());
+    g.aux = -1;
+    g.haux.clear();
     g.q0 = g.q1 = -1;
     if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
     g.ffl = -1;
@@ -380,7 +491,7 @@ class Amr2Gpu {
       for (int m : lgrids[lev]) {
         const HPatch& g = node[m];
         PatchDev& d = h_patches[m];
-        d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl;
+        d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl; d.aux = g.aux;
         d.ilo = g.ilo; d.ihi = g.ihi; d.jlo = g.jlo; d.jhi = g.jhi; d.klo = d.khi = 0;
         d.mitot = mitot(m); d.mjtot = mjtot(m); d.mktot = 1;
         d.level = g.level; d.lenbc = g.lenbc;
@@ -624,10 +735,13 @@ class Amr2Gpu {
     const long long s0 = D.scratch_len;
     for (ScratchRect r : S.rects) { r.off += s0; D.rects.push_back(r); }
     D.scratch_len += S.scratch_len;
+    const int c0 = (int)D.capa.size();
+    D.capa.insert(D.capa.end(), S.capa.begin(), S.capa.end());
     for (size_t k = 0; k < S.ops.size(); ++k) {
       FillOp o = S.ops[k];
       if (o.dst_patch < 0) o.dst_rect += r0;
       if (o.kind != FILL_COPY) o.src += r0;
+      if (o.kind == FILL_FIXCAPA) o.capa0 += c0;
       D.add_op(o, S.op_stage[k]);
     }
     for (size_t k = 0; k < S.bcs.size(); ++k) {
@@ -758,8 +872,46 @@ class Amr2Gpu {
       FillOp o{};
       o.kind = FILL_RING; o.dst_patch = k; o.dst_rect = -1; o.ni = g.lenbc; o.nj = 1; o.src = R;
       P.add_op(o, 1);
+      if (p.naux > 0) ring_aux(k, lev, iclo, jclo, nrow, ncol, sticks);
     }
     upload_prog(P);
+  }
+  // saveqc.f:58-90 and cstore.f for the aux: the coarse ring's aux, copied from the coarse
+  // grids' aux (icall), or set by setaux on the whole ring where it leaves the domain (the
+  // problem's setaux sets every cell); stored after svdflx and qc1d of kid k, in cstore's
+  // order. The aux does not change between regrids, so it is written when saveqc is compiled.
+  void ring_aux(int k, int lev, int iclo, int jclo, int nrow, int ncol, bool sticks) {
+    const HPatch& g = node[k];
+    const int na = p.naux;
+    const double hxc = hxposs[lev], hyc = hyposs[lev];
+    std::vector<double> tx;
+    if (sticks) setaux(0, nrow, ncol, g.xlo - hxc, g.ylo - hyc, hxc, hyc, tx);
+    const size_t rpl = (size_t)nrow * ncol;
+    const GridIndex& XC = GI(lev);
+    std::vector<int> hits;
+    std::vector<double> ac((size_t)na * g.lenbc, NEEDS_TO_BE_SET);
+    int index = 0;
+    auto put = [&](int ii, int jj) {  // 0-based cell of the ring rect
+      double* dst = &ac[(size_t)na * index++];
+      if (sticks) {
+        for (int m = 0; m < na; ++m) dst[m] = tx[m * rpl + (size_t)jj * nrow + ii];
+        return;
+      }
+      const int I = iclo + ii, J = jclo + jj;
+      XC.query2(I, I, J, J, hits);
+      for (int r : hits) {
+        const HPatch& c = node[XC.id(r)];
+        if (I < c.ilo || I > c.ihi || J < c.jlo || J > c.jhi) continue;
+        const int mi = c.nx() + 2 * ng, mj = c.ny() + 2 * ng;
+        const size_t at = (size_t)(J - c.jlo + ng) * mi + (I - c.ilo + ng);
+        for (int m = 0; m < na; ++m) dst[m] = c.haux[(size_t)m * mi * mj + at];
+      }
+    };
+    for (int j = 1; j <= ncol - 2; ++j) put(0, j);
+    for (int i = 1; i <= nrow - 2; ++i) put(i, ncol - 1);
+    for (int j = 1; j <= ncol - 2; ++j) put(nrow - 1, j);
+    for (int i = 1; i <= nrow - 2; ++i) put(i, 0);
+    upload_to(regs.d + g.ffl + (long long)2 * nvar * g.lenbc, ac.data(), sizeof(double) * ac.size());
   }
 
   void upload_prog(FillProg& P) {
@@ -804,6 +956,7 @@ class Amr2Gpu {
     P.d_ops.upload(ops, st, stg);
     P.d_chunks.upload(ch, st, stg);
     P.d_bcs.upload(bcs, st, stg);
+    if (!P.capa.empty()) P.d_capa.upload(P.capa, st, stg);
   }
 
   void run_prog(FillProg& P, const SrcMode& modes, const SrcMode* modes_dev = nullptr) {
@@ -816,6 +969,7 @@ class Amr2Gpu {
         a.chunks = P.d_chunks.d + P.ch_lo[s]; a.nchunks = P.ch_hi[s] - P.ch_lo[s]; a.nvar = nvar; a.modes = modes;
         a.modes_dev = modes_dev;
         a.lc = lc; a.xlower = xlower; a.ylower = ylower;
+        a.mcapa = p.mcapa; a.capa = P.d_capa.d;
         launch_fill(a, st, f32);
         ++nkernels;
       }
@@ -957,7 +1111,9 @@ class Amr2Gpu {
         const int norm = 1 << (side1 - 1);
         const size_t key = (size_t)(e[1] - 1) * mi + (e[0] - 1);
         if ((used[key] / norm) % 2 == 1) continue;
-        const double sgn = (side == 2 || side == 3 || side == 6) ? -1.0 : 1.0;
+        double sgn = (side == 2 || side == 3 || side == 6) ? -1.0 : 1.0;
+        // upbnd.f:104-108: with a capacity array the correction is divided by kappa
+        if (p.mcapa > 0) sgn = sgn / g.haux[(size_t)(p.mcapa - 1) * mi * mj + key];
         if (slot[key] < 0) { slot[key] = (int)terms.size(); terms.emplace_back(); order.push_back((int)key); }
         terms[slot[key]].push_back(UpbndTerm{node[e[3]].ffl + (long long)nvar * (e[4] - 1), sgn});
         used[key] += norm;
@@ -995,7 +1151,7 @@ class Amr2Gpu {
       HPatch& g = node[k];
       g.lenbc = 2 * (g.nx() / intratx[lev - 1] + g.ny() / intraty[lev - 1]);
       if (g.ffl >= 0) regs.release(g.ffl, g.nffl);
-      g.nffl = (long long)2 * nvar * g.lenbc;
+      g.nffl = (long long)(2 * nvar + p.naux) * g.lenbc;  // svdflx, qc1d, auxc1d (saveqc.f's ffluxptr)
       g.ffl = regs.alloc(g.nffl);
       zr.emplace_back(g.ffl, Arena::rnd(g.nffl));
     }
@@ -1448,7 +1604,7 @@ class Amr2Gpu {
     LevelPlan& L = plan[lev];
     const double area = hxposs[lev] * hyposs[lev];
     launch_upbnd(pool.d, regs.d, d_patches.d, L.d_upc.d, (int)L.upc.size(), L.d_upt.d, area, nvar, st, f32);
-    launch_average(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), intratx[lev], intraty[lev], nvar, st, f32);
+    launch_average(pool.d, d_patches.d, L.d_avg.d, (int)L.avg.size(), intratx[lev], intraty[lev], nvar, st, f32, p.mcapa);
     nkernels += 2;
   }
 
@@ -2121,12 +2277,31 @@ class Amr2Gpu {
       }
       std::vector<int> rr;
       runs(cov, nx, ny, rr);
+      int capa0 = -1;
+      if (p.mcapa > 0 && !rr.empty()) {
+        // filval.f90:90-96: setaux on the coarse patch (no ghost cells, lower corner one
+        // coarse cell out); fixcapaq reads its kappa
+        std::vector<double> ac;
+        setaux(0, mic, mjc, g.xlo - dxc, g.ylo - dyc, dxc, dyc, ac);
+        capa0 = (int)P.capa.size();
+        P.capa.insert(P.capa.end(), ac.begin() + (size_t)(p.mcapa - 1) * mic * mjc, ac.begin() + (size_t)p.mcapa * mic * mjc);
+      }
       for (size_t k = 0; k < rr.size(); k += 4) {
         FillOp o2{};
         o2.kind = FILL_FILVAL; o2.dst_patch = m; o2.dst_rect = -1;
         o2.di0 = rr[k] + ng; o2.dj0 = rr[k + 1] + ng; o2.ni = rr[k + 2]; o2.nj = rr[k + 3];
         o2.src = R; o2.si0 = g.ilo + rr[k]; o2.sj0 = g.jlo + rr[k + 1]; o2.level = lev; o2.cilo = iclo; o2.cjlo = jclo;
         P.add_op(o2, 1);
+        if (capa0 >= 0) {
+          // fixcapaq.f over the coarse cells of the interpolated region (old and new grids are
+          // unions of coarse cells, so each coarse cell's fine block is all copied or all
+          // interpolated and only the latter change)
+          if (rr[k] % rx || rr[k + 1] % ry || rr[k + 2] % rx || rr[k + 3] % ry)
+            throw std::runtime_error("filval: interpolated region not aligned with the coarse cells");
+          FillOp o3 = o2;
+          o3.kind = FILL_FIXCAPA; o3.ni = rr[k + 2] / rx; o3.nj = rr[k + 3] / ry; o3.capa0 = capa0;
+          P.add_op(o3, 2);
+        }
       }
     }
   }
@@ -2195,7 +2370,7 @@ class Amr2Gpu {
     auto put = [&](int m) {
       const HPatch& g = node[m];
       PatchDev& d = h_patches[m];
-      d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl;
+      d.q[0] = g.q0; d.q[1] = g.q1; d.cur = g.cur; d.ffl = g.ffl; d.aux = g.aux;
       d.ilo = g.ilo; d.ihi = g.ihi; d.jlo = g.jlo; d.jhi = g.jhi;
       d.mitot = mitot(m); d.mjtot = mjtot(m); d.mktot = 1; d.level = g.level; d.lenbc = g.lenbc;
     };
@@ -2213,7 +2388,7 @@ class Amr2Gpu {
     if (write_output && p.output_format != 1 && p.output_format != 3)
       throw std::runtime_error("output_format must be 1 (ASCII) or 3 (binary): NetCDF and HDF5 output are not supported");
     if (p.nghost != 2) throw std::runtime_error("num_ghost must be 2");
-    if (p.mcapa != 0 || p.naux != 0) throw std::runtime_error("capacity / aux arrays are not supported by the 2D device path");
+    if (f32 && p.naux != 0) throw std::runtime_error("the FP32 form has no 2D aux arrays (capacity, face velocities)");
     // amr2.f90:258-263: Godunov splitting (stepgrid_dimSplit.f) or unsplit; Strang stops the reference
     if (p.dimsplit > 1) throw std::runtime_error("Strang splitting is not supported (dimensional_split must be 0 or 1)");
     // stepgrid.f:176-180 calls src2 after the step when method(5) = 1; the library's default
@@ -2364,7 +2539,7 @@ class Amr2Gpu {
   double mass() {
     ensure(1, NEED_STEP);
     AMR_CUDA(cudaMemsetAsync(d_mass, 0, sizeof(double), st));
-    launch_mass2(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st, f32);
+    launch_mass2(pool.d, d_patches.d, plan[1].d_plist.d, (int)plan[1].plist.size(), d_mass, st, f32, p.mcapa);
     double m = 0;
     AMR_CUDA(cudaMemcpyAsync(&m, d_mass, sizeof(double), cudaMemcpyDeviceToHost, st));
     sync_stream();

@@ -33,14 +33,29 @@ struct Step2Layout {
   static constexpr int NW = STEP2_RC * (T + 3) * WREC;
   static constexpr int XREC = 4 * ME;
   static constexpr int NX = STEP2_RC * (T + 1) * XREC;
-  static constexpr int TOTAL = NQ + 4 * NF + NTR + NW + NX + 32;
+  // aux of the tile and its two ghost layers, [m][b][a] like the staged q (solvers that read aux)
+  static constexpr int NA = S::NAUX > 0 ? MAXAUX2 : 0;
+  static constexpr int NAQ = NA * QW * QW;
+  static constexpr int TOTAL = NQ + 4 * NF + NTR + NW + NX + NAQ + 32;
+};
+
+// aux values a plugin reads at one cell of a staged aux tile ([m][b][a], QW x QW)
+template <class S, class R>
+struct AuxCell {
+  R v[S::NAUX > 0 ? S::NAUX : 1];
+  __device__ __forceinline__ void load(const R* As, int QW, int b, int a) {
+#pragma unroll
+    for (int m = 0; m < S::NAUX; ++m) v[m] = As[(m * QW + b) * QW + a];
+  }
 };
 
 // flux2.f:136-194 at one face from the wave records (waves, speeds, amdq, apdq) of the face
 // (rc) and of its neighbours (rm: face f-1, rp: face f+1): limiter.f's limited waves, the
 // second-order correction cqxx, fm = (0 + amdq) + cqxx/2 and fp = (0 - apdq) + cqxx/2
+// dl, dr: dtdx1d of the cells left and right of the face (dt/dx, divided by the capacity of
+// the cell when there is one: step2.f90:83-88)
 template <class S, class R>
-__device__ __forceinline__ void face_fluxes(const StepParams& sp, const R* rm, const R* rc, const R* rp, R dtdx,
+__device__ __forceinline__ void face_fluxes(const StepParams& sp, const R* rm, const R* rc, const R* rp, R dl, R dr,
                                             R (&amdq)[S::MEQN], R (&apdq)[S::MEQN], R (&cqxx)[S::MEQN],
                                             R (&fm)[S::MEQN], R (&fp)[S::MEQN]) {
   constexpr int ME = S::MEQN, MW = S::MWAVES;
@@ -76,7 +91,7 @@ __device__ __forceinline__ void face_fluxes(const StepParams& sp, const R* rm, c
 #pragma unroll
     for (int m = 0; m < ME; ++m) wl[mw][m] = wlim * wl[mw][m];
   }
-  const R dtdxave = R(0.5) * (dtdx + dtdx);
+  const R dtdxave = R(0.5) * (dl + dr);
 #pragma unroll
   for (int m = 0; m < ME; ++m) {
     R c = R(0);
@@ -92,13 +107,15 @@ __device__ __forceinline__ void face_fluxes(const StepParams& sp, const R* rm, c
   }
 }
 
-// rpn2 at one face into its wave record: waves [MW][ME], speeds [MW], amdq [ME], apdq [ME]
+// rpn2 at one face into its wave record: waves [MW][ME], speeds [MW], amdq [ME], apdq [ME].
+// auxL, auxR: aux of the cells left and right of the face; dl, dr: their dtdx1d (flux2.f's
+// Courant number takes dtdx1d(i)*s and -dtdx1d(i-1)*s)
 template <class S, class R>
-__device__ __forceinline__ void face_record(const StepParams& sp, int ixy, const R* qL, const R* qR, R* rec, R dtdx,
-                                            bool count_cfl, R& cfl) {
+__device__ __forceinline__ void face_record(const StepParams& sp, int ixy, const R* qL, const R* qR, const R* auxL,
+                                            const R* auxR, R* rec, R dl, R dr, bool count_cfl, R& cfl) {
   constexpr int ME = S::MEQN, MW = S::MWAVES;
   R wave[MW][ME], s[MW], amdq[ME], apdq[ME];
-  S::template rpn<R>(sp.prob, ixy, qL, qR, wave, s, amdq, apdq);
+  S::template rpn<R>(sp.prob, ixy, qL, qR, auxL, auxR, wave, s, amdq, apdq);
 #pragma unroll
   for (int mw = 0; mw < MW; ++mw) {
 #pragma unroll
@@ -109,16 +126,18 @@ __device__ __forceinline__ void face_record(const StepParams& sp, int ixy, const
   for (int m = 0; m < ME; ++m) { rec[MW * ME + MW + m] = amdq[m]; rec[MW * ME + MW + ME + m] = apdq[m]; }
   if (count_cfl) {
 #pragma unroll
-    for (int mw = 0; mw < MW; ++mw) cfl = dmax(cfl, dmax(dtdx * s[mw], -dtdx * s[mw]));
+    for (int mw = 0; mw < MW; ++mw) cfl = dmax(cfl, dmax(dr * s[mw], -dl * s[mw]));
   }
 }
 
 // One sweep direction of flux2.f over the tile. IXY = 1: lines are rows, IXY = 2: columns.
+// As: the staged aux tile (Step2Layout::NA components, null without aux)
 template <class S, int IXY, class R>
-__device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR, R* F1,
+__device__ void step2_sweep(const StepParams& sp, const R* Qs, const R* As, R* W, R* X, R* TR, R* F1,
                             R* F2, int i0, int j0, int tw, int th, R dtdx, R& cfl) {
   using L = Step2Layout<S>;
   constexpr int ME = L::ME, T = L::T, QW = L::QW;
+  const bool capa = L::NA > 0 && sp.mcapa > 0;
   const int tid = threadIdx.x;
   // along-line extents
   const int na = (IXY == 1) ? tw : th;       // cells along the line inside the tile
@@ -136,6 +155,15 @@ __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR
 #pragma unroll
     for (int m = 0; m < ME; ++m) q[m] = *qptr(m, line, pos);
   };
+  // staged aux coordinates (b, a) of a cell of the sweep, as qptr
+  auto abt = [&](int line, int pos) { return (IXY == 1) ? line - (j0 - 2) : pos - (j0 - 2); };
+  auto aat = [&](int line, int pos) { return (IXY == 1) ? pos - (i0 - 2) : line - (i0 - 2); };
+  auto auxc = [&](AuxCell<S, R>& c, int line, int pos) { if (S::NAUX > 0) c.load(As, QW, abt(line, pos), aat(line, pos)); };
+  // dtdx1d of a cell (step2.f90:83-88)
+  auto d1d = [&](int line, int pos) -> R {
+    if (!capa) return dtdx;
+    return dtdx / As[((sp.mcapa - 1) * QW + abt(line, pos)) * QW + aat(line, pos)];
+  };
   for (int lc0 = 0; lc0 < nl; lc0 += STEP2_RC) {
     const int nlc = min(STEP2_RC, nl - lc0);
     // phase 1: normal Riemann problems
@@ -145,7 +173,11 @@ __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR
       R qL[ME], qR[ME];
       loadq(qL, line, f - 1);
       loadq(qR, line, f);
-      face_record<S, R>(sp, IXY, qL, qR, W + (rr * (T + 3) + ff) * L::WREC, dtdx, ff >= 1 && ff <= nfl, cfl);
+      AuxCell<S, R> aL, aR;
+      auxc(aL, line, f - 1);
+      auxc(aR, line, f);
+      face_record<S, R>(sp, IXY, qL, qR, aL.v, aR.v, W + (rr * (T + 3) + ff) * L::WREC, d1d(line, f - 1), d1d(line, f),
+                        ff >= 1 && ff <= nfl, cfl);
     }
     __syncthreads();
     // phase 2: limiter, second-order correction, transverse splitting
@@ -156,7 +188,8 @@ __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR
       const R* rc = rm + L::WREC;                             // face f
       const R* rp = rc + L::WREC;                             // face f+1
       R amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
-      face_fluxes<S, R>(sp, rm, rc, rp, dtdx, amdq, apdq, cqxx, fm, fp);
+      const R dl = d1d(line, f - 1), dr = d1d(line, f);
+      face_fluxes<S, R>(sp, rm, rc, rp, dl, dr, amdq, apdq, cqxx, fm, fp);
       // flux increments into the tile's face arrays (interior lines only)
       const int lin = (IXY == 1) ? line - j0 : line - i0;
       if (lin >= 0 && lin < ((IXY == 1) ? th : tw)) {
@@ -185,15 +218,19 @@ __device__ void step2_sweep(const StepParams& sp, const R* Qs, R* W, R* X, R* TR
         R qL[ME], qR[ME];
         loadq(qL, line, f - 1);
         loadq(qR, line, f);
+        // the aux of the split's cell (f-1 for amdq, f for apdq) in the rows below, at and above
+        AuxCell<S, R> b1, b2, b3, c1, c2, c3;
+        auxc(b1, line - 1, f - 1); auxc(b2, line, f - 1); auxc(b3, line + 1, f - 1);
+        auxc(c1, line - 1, f); auxc(c2, line, f); auxc(c3, line + 1, f);
         R bm1[ME], bp1[ME], bm2[ME], bp2[ME];
-        S::template rpt<R>(sp.prob, IXY, 1, qL, qR, am2, bm1, bp1);
-        S::template rpt<R>(sp.prob, IXY, 2, qL, qR, ap2, bm2, bp2);
+        S::template rpt<R>(sp.prob, IXY, 1, qL, qR, b1.v, b2.v, b3.v, am2, bm1, bp1);
+        S::template rpt<R>(sp.prob, IXY, 2, qL, qR, c1.v, c2.v, c3.v, ap2, bm2, bp2);
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-          xr[0 * ME + m] = R(0.5) * dtdx * bm1[m];
-          xr[1 * ME + m] = R(0.5) * dtdx * bp1[m];
-          xr[2 * ME + m] = R(0.5) * dtdx * bm2[m];
-          xr[3 * ME + m] = R(0.5) * dtdx * bp2[m];
+          xr[0 * ME + m] = R(0.5) * dl * bm1[m];
+          xr[1 * ME + m] = R(0.5) * dl * bp1[m];
+          xr[2 * ME + m] = R(0.5) * dr * bm2[m];
+          xr[3 * ME + m] = R(0.5) * dr * bp2[m];
         }
       }
     }
@@ -288,11 +325,13 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
   R* TR = GP + L::NF;
   R* W = TR + L::NTR;
   R* X = W + L::NW;
-  R* red = X + L::NX;
+  R* As = X + L::NX;
+  R* red = As + L::NAQ;
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;
   const R dtdx = (R)(dt / a.dx), dtdy = (R)(dt / a.dy);
+  const bool capa = L::NA > 0 && a.sp.mcapa > 0;
   R cfl = R(0);
   int iter = 0;
   while (true) {
@@ -324,9 +363,19 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
       const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
       Qs[(m * QW + b) * QW + aa] = qin[m * plane + (long long)je * mitot + ie];
     }
+    if (L::NA > 0) {
+      const R* aux = static_cast<const R*>(a.pool) + P.aux;
+      const int na = min(L::NA, a.sp.prob.naux);
+      for (int it = tid; it < na * lw * lh; it += STEP2_THREADS) {
+        const int m = it / (lw * lh), rem = it % (lw * lh);
+        const int b = rem / lw, aa = rem % lw;
+        const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
+        As[(m * QW + b) * QW + aa] = aux[m * plane + (long long)je * mitot + ie];
+      }
+    }
     __syncthreads();
     // x-sweeps: FM/FP initialised, per-cell transverse parts in TR
-    step2_sweep<S, 1, R>(a.sp, Qs, W, X, TR, FM, FP, i0, j0, tw, th, dtdx, cfl);
+    step2_sweep<S, 1, R>(a.sp, Qs, As, W, X, TR, FM, FP, i0, j0, tw, th, dtdx, cfl);
     // GX(c, f) = (0 + part2(row f-1)) + part1(row f) -> GM and GP
     for (int it = tid; it < ME * (th + 1) * tw; it += STEP2_THREADS) {
       const int m = it / ((th + 1) * tw), rem = it % ((th + 1) * tw);
@@ -339,7 +388,7 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
     }
     __syncthreads();
     // y-sweeps: GM/GP += faddm/faddp, per-cell transverse parts in TR
-    step2_sweep<S, 2, R>(a.sp, Qs, W, X, TR, GM, GP, i0, j0, tw, th, dtdy, cfl);
+    step2_sweep<S, 2, R>(a.sp, Qs, As, W, X, TR, GM, GP, i0, j0, tw, th, dtdy, cfl);
     // FM(f, r) = (FM + part2(col f-1)) + part1(col f)
     for (int it = tid; it < ME * th * (tw + 1); it += STEP2_THREADS) {
       const int m = it / (th * (tw + 1)), rem = it % (th * (tw + 1));
@@ -351,14 +400,16 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
       FP[k] = (FP[k] + up) + dn;
     }
     __syncthreads();
-    // conservative update (stepgrid.f:154-173, mcapa = 0)
+    // conservative update (stepgrid.f:154-173; with a capacity array the flux difference is
+    // divided by kappa)
     for (int it = tid; it < ME * th * tw; it += STEP2_THREADS) {
       const int m = it / (th * tw), rem = it % (th * tw);
       const int rb = rem / tw, ca = rem % tw;
       const R q = Qs[(m * QW + rb + 2) * QW + ca + 2];
       const R fmr = FM[(m * T + rb) * (T + 1) + ca + 1], fpl = FP[(m * T + rb) * (T + 1) + ca];
       const R gmt = GM[(m * (T + 1) + rb + 1) * T + ca], gpb = GP[(m * (T + 1) + rb) * T + ca];
-      const R qn = q - dtdx * (fmr - fpl) - dtdy * (gmt - gpb);
+      const R qn = capa ? q - (dtdx * (fmr - fpl) + dtdy * (gmt - gpb)) / As[((a.sp.mcapa - 1) * QW + rb + 2) * QW + ca + 2]
+                        : q - dtdx * (fmr - fpl) - dtdy * (gmt - gpb);
       const int ie = i0 + ca + 1, je = j0 + rb + 1;
       qout[m * plane + (long long)je * mitot + ie] = qn;
     }
@@ -386,7 +437,9 @@ struct Split2Layout {
   static constexpr int NG = ME * (T + 1) * T;        // gm / gp
   static constexpr int WREC = MW * ME + MW + 2 * ME;
   static constexpr int NW = STEP2_RC * (T + 3) * WREC;
-  static constexpr int TOTAL = NQ + 2 * NFX + NQX + 2 * NG + NW + 32;
+  static constexpr int NA = S::NAUX > 0 ? MAXAUX2 : 0;
+  static constexpr int NAQ = NA * QW * QW;           // staged aux, [m][b][a] like Qs
+  static constexpr int TOTAL = NQ + 2 * NFX + NQX + 2 * NG + NW + NAQ + 32;
 };
 
 template <class S, class R>
@@ -401,11 +454,16 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
   R* GM = Qx + L::NQX;
   R* GP = GM + L::NG;
   R* W = GP + L::NG;
-  R* red = W + L::NW;
+  R* As = W + L::NW;
+  R* red = As + L::NAQ;
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;
   const R dtdx = (R)(dt / a.dx), dtdy = (R)(dt / a.dy);
+  const bool capa = L::NA > 0 && a.sp.mcapa > 0;
+  // kappa of staged cell (b, c); dtdx1d of it for the step d (flux2_dimSplit.f with capa)
+  auto kap = [&](int b, int c) -> R { return As[((a.sp.mcapa - 1) * QW + b) * QW + c]; };
+  auto d1d = [&](R d, int b, int c) -> R { return capa ? d / kap(b, c) : d; };
   R cfl = R(0);
   int iter = 0;
   while (true) {
@@ -436,6 +494,16 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
       const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
       Qs[(m * QW + b) * QW + aa] = qin[m * plane + (long long)je * mitot + ie];
     }
+    if (L::NA > 0) {
+      const R* aux = static_cast<const R*>(a.pool) + P.aux;
+      const int na = min(L::NA, a.sp.prob.naux);
+      for (int it = tid; it < na * lw * lh; it += STEP2_THREADS) {
+        const int m = it / (lw * lh), rem = it % (lw * lh);
+        const int b = rem / lw, aa = rem % lw;
+        const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
+        As[(m * QW + b) * QW + aa] = aux[m * plane + (long long)je * mitot + ie];
+      }
+    }
     __syncthreads();
     // step2x.f90: rows b (j = j0-2+b), faces ff (i = i0-1+ff, between staged columns ff, ff+1)
     {
@@ -447,14 +515,18 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
           R qL[ME], qR[ME];
 #pragma unroll
           for (int m = 0; m < ME; ++m) { qL[m] = Qs[(m * QW + b) * QW + ff]; qR[m] = Qs[(m * QW + b) * QW + ff + 1]; }
-          face_record<S, R>(a.sp, 1, qL, qR, W + (rr * (T + 3) + ff) * WREC, dtdx, ff >= 1 && ff <= nfl, cfl);
+          AuxCell<S, R> aL, aR;
+          if (S::NAUX > 0) { aL.load(As, QW, b, ff); aR.load(As, QW, b, ff + 1); }
+          face_record<S, R>(a.sp, 1, qL, qR, aL.v, aR.v, W + (rr * (T + 3) + ff) * WREC, d1d(dtdx, b, ff),
+                            d1d(dtdx, b, ff + 1), ff >= 1 && ff <= nfl, cfl);
         }
         __syncthreads();
         for (int it = tid; it < nb * nfl; it += STEP2_THREADS) {
           const int rr = it / nfl, fa = it % nfl, b = b0 + rr;
           const R* rm = W + (rr * (T + 3) + fa) * WREC;
           R amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
-          face_fluxes<S, R>(a.sp, rm, rm + WREC, rm + 2 * WREC, dtdx, amdq, apdq, cqxx, fm, fp);
+          face_fluxes<S, R>(a.sp, rm, rm + WREC, rm + 2 * WREC, d1d(dtdx, b, fa + 1), d1d(dtdx, b, fa + 2), amdq, apdq,
+                            cqxx, fm, fp);
 #pragma unroll
           for (int m = 0; m < ME; ++m) {
             FXm[(m * QW + b) * (T + 1) + fa] = fm[m];
@@ -470,7 +542,8 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
     for (int it = tid; it < ME * lh * tw; it += STEP2_THREADS) {
       const int m = it / (lh * tw), rem = it % (lh * tw);
       const int b = rem / tw, c = rem % tw;
-      const R v = Qs[(m * QW + b) * QW + c + 2] - dtdx * (FXm[(m * QW + b) * (T + 1) + c + 1] - FXp[(m * QW + b) * (T + 1) + c]);
+      const R df = dtdx * (FXm[(m * QW + b) * (T + 1) + c + 1] - FXp[(m * QW + b) * (T + 1) + c]);
+      const R v = Qs[(m * QW + b) * QW + c + 2] - (capa ? df / kap(b, c + 2) : df);
       Qx[(m * QW + b) * T + c] = v;
       const int jrow = j0 - 2 + b;
       if (jrow < 1 || jrow > my) qout[m * plane + (long long)(jrow + 1) * mitot + (i0 + c + 1)] = v;
@@ -486,14 +559,18 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
           R qL[ME], qR[ME];
 #pragma unroll
           for (int m = 0; m < ME; ++m) { qL[m] = Qx[(m * QW + ff) * T + c]; qR[m] = Qx[(m * QW + ff + 1) * T + c]; }
-          face_record<S, R>(a.sp, 2, qL, qR, W + (rr * (T + 3) + ff) * WREC, dtdy, ff >= 1 && ff <= nfl, cfl);
+          AuxCell<S, R> aL, aR;
+          if (S::NAUX > 0) { aL.load(As, QW, ff, c + 2); aR.load(As, QW, ff + 1, c + 2); }
+          face_record<S, R>(a.sp, 2, qL, qR, aL.v, aR.v, W + (rr * (T + 3) + ff) * WREC, d1d(dtdy, ff, c + 2),
+                            d1d(dtdy, ff + 1, c + 2), ff >= 1 && ff <= nfl, cfl);
         }
         __syncthreads();
         for (int it = tid; it < nc * nfl; it += STEP2_THREADS) {
           const int rr = it / nfl, fb = it % nfl, c = c0 + rr;
           const R* rm = W + (rr * (T + 3) + fb) * WREC;
           R amdq[ME], apdq[ME], cqxx[ME], fm[ME], fp[ME];
-          face_fluxes<S, R>(a.sp, rm, rm + WREC, rm + 2 * WREC, dtdy, amdq, apdq, cqxx, fm, fp);
+          face_fluxes<S, R>(a.sp, rm, rm + WREC, rm + 2 * WREC, d1d(dtdy, fb + 1, c + 2), d1d(dtdy, fb + 2, c + 2), amdq,
+                            apdq, cqxx, fm, fp);
 #pragma unroll
           for (int m = 0; m < ME; ++m) {
             GM[(m * (T + 1) + fb) * T + c] = fm[m];
@@ -507,7 +584,8 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2s_kernel(StepArgs a) {
     for (int it = tid; it < ME * th * tw; it += STEP2_THREADS) {
       const int m = it / (th * tw), rem = it % (th * tw);
       const int rb = rem / tw, ca = rem % tw;
-      const R qn = Qx[(m * QW + rb + 2) * T + ca] - dtdy * (GM[(m * (T + 1) + rb + 1) * T + ca] - GP[(m * (T + 1) + rb) * T + ca]);
+      const R dg = dtdy * (GM[(m * (T + 1) + rb + 1) * T + ca] - GP[(m * (T + 1) + rb) * T + ca]);
+      const R qn = Qx[(m * QW + rb + 2) * T + ca] - (capa ? dg / kap(rb + 2, ca + 2) : dg);
       qout[m * plane + (long long)(j0 + rb + 1) * mitot + (i0 + ca + 1)] = qn;
     }
     // the tile's own rows start at staged row 2 of FXm / FXp
@@ -549,6 +627,7 @@ static void launch_step2_r(int solver, const StepArgs& a, int grid, cudaStream_t
     case SOLVER_ADVECTION: launch_step2_t<Advection2, R>(a, grid, s); break;
     case SOLVER_ACOUSTICS: launch_step2_t<Acoustics2, R>(a, grid, s); break;
     case SOLVER_EULER: launch_step2_t<Euler2, R>(a, grid, s); break;
+    case SOLVER_VC_ADVECTION: launch_step2_t<VcAdvection2, R>(a, grid, s); break;
     default: throw std::runtime_error("launch_step2: unsupported solver");
   }
 }
@@ -564,6 +643,7 @@ size_t step2_smem_bytes(int solver, bool f32) {
     case SOLVER_ADVECTION: return w * Step2Layout<Advection2>::TOTAL;
     case SOLVER_ACOUSTICS: return w * Step2Layout<Acoustics2>::TOTAL;
     case SOLVER_EULER: return w * Step2Layout<Euler2>::TOTAL;
+    case SOLVER_VC_ADVECTION: return w * Step2Layout<VcAdvection2>::TOTAL;
   }
   return 0;
 }
@@ -672,6 +752,31 @@ __device__ __forceinline__ void fill_chunk(const FillArgs& a, int c) {
       const double fv = dmax(0.0, dsign(1.0, dvpc * dvmc));
       const double vslope = dv * dsign(1.0, dvcc) * fv;
       dst[m * plane + dk] = (T)(valc + eta1 * uslope + eta2 * vslope);
+    }
+    return;
+  }
+  if (o.kind == FILL_FIXCAPA) {
+    // fixcapaq.f:4-62 for one coarse cell of an interpolated region: conserve kappa*q over
+    // the coarse cell, adding the difference over kappa to each of its fine cells
+    const PatchDev& F = a.patches[o.dst_patch];
+    const T* kap = pool + F.aux + (long long)(a.mcapa - 1) * plane;
+    const int bi = o.si0 + ia * rx, bj = o.sj0 + jb * ry;  // global fine index of the block origin
+    const int i = floordiv(bi, rx) - o.cilo + 1, j = floordiv(bj, ry) - o.cjlo + 1;  // 1-based in valc
+    const long long k0 = (long long)(o.dj0 + jb * ry) * ldi + (o.di0 + ia * rx);
+    const double kc = a.capa[o.capa0 + (long long)(j - 1) * R.ni + (i - 1)];
+    for (int m = 0; m < nvar; ++m) {
+      double capaqfine = 0.0;
+      for (int ico = 0; ico < rx; ++ico)
+        for (int jco = 0; jco < ry; ++jco) {
+          const long long k = k0 + (long long)jco * ldi + ico;
+          capaqfine = capaqfine + (double)kap[k] * (double)dst[m * plane + k];
+        }
+      const double dcapaq = kc * (double)vc[m * cp + (long long)(j - 1) * R.ni + (i - 1)] - capaqfine / (double)(rx * ry);
+      for (int ico = 0; ico < rx; ++ico)
+        for (int jco = 0; jco < ry; ++jco) {
+          const long long k = k0 + (long long)jco * ldi + ico;
+          dst[m * plane + k] = (T)((double)dst[m * plane + k] + dcapaq / (double)kap[k]);
+        }
     }
     return;
   }
@@ -835,11 +940,15 @@ __global__ void qad2_kernel(T* pool, double* regs, const PatchDev* patches, cons
   const int rx = lc.intratx[lev - 1], ry = lc.intraty[lev - 1];
   const double hx = lc.hx[lev], hy = lc.hy[lev];
   const T* q = pool + P.q[P.cur];
+  const T* aux = pool + P.aux;
   const long long plane = (long long)P.mitot * P.mjtot;
+  constexpr int NA = S::NAUX > 0 ? S::NAUX : 1;
   for (int sgi = threadIdx.x; sgi < J.nseg; sgi += blockDim.x) {
     const int seg = J.seg0 + sgi;
     double* svd = regs + P.ffl + (long long)ME * seg;
     const double* qc = regs + P.ffl + (long long)ME * P.lenbc + (long long)ME * seg;
+    // auxc1d(:, seg) of the saved coarse ring (cstore.f), after svdflx and qc1d
+    const double* ac = regs + P.ffl + (long long)2 * ME * P.lenbc + (long long)prob.naux * seg;
     double sv[ME];
 #pragma unroll
     for (int m = 0; m < ME; ++m) sv[m] = svd[m];
@@ -854,11 +963,27 @@ __global__ void qad2_kernel(T* pool, double* regs, const PatchDev* patches, cons
       else k = (long long)1 * P.mitot + (f + 1);
 #pragma unroll
       for (int m = 0; m < ME; ++m) { qf[m] = q[m * plane + k]; qcr[m] = (T)qc[m]; }
+      // qad.f:79-89, 160-185, 231-256, 298-308: the fine cell's aux, except that the aux of
+      // the state across the interface is the coarse ring's, or the fine cell's own face
+      // value for a face-type component on that face (xleft on sides 1 and 3, yleft on 2, 4)
+      T af[NA], ax[NA];
+      if (S::NAUX > 0) {
+        const int face_type = (J.side == 1 || J.side == 3) ? AUX_XLEFT : AUX_YLEFT;
+        // sides 1 and 4: the fine state's aux is the ghost cell's, or the first interior
+        // cell's (its lower face is the interface) for the face-type component
+        const long long kin = (J.side == 1) ? k + 1 : (J.side == 4) ? k + P.mitot : k;
+#pragma unroll
+        for (int m = 0; m < S::NAUX; ++m) {
+          const bool ft = prob.auxtype[m] == face_type;
+          if (J.side == 1 || J.side == 4) { af[m] = ft ? aux[m * plane + kin] : aux[m * plane + k]; ax[m] = (T)ac[m]; }
+          else { af[m] = aux[m * plane + k]; ax[m] = ft ? aux[m * plane + k] : (T)ac[m]; }
+        }
+      }
       T wave[MW][ME], s[MW], amdq[ME], apdq[ME];
-      if (J.side == 1) S::template rpn<T>(prob, 1, qcr, qf, wave, s, amdq, apdq);
-      else if (J.side == 2) S::template rpn<T>(prob, 2, qf, qcr, wave, s, amdq, apdq);
-      else if (J.side == 3) S::template rpn<T>(prob, 1, qf, qcr, wave, s, amdq, apdq);
-      else S::template rpn<T>(prob, 2, qcr, qf, wave, s, amdq, apdq);
+      if (J.side == 1) S::template rpn<T>(prob, 1, qcr, qf, ax, af, wave, s, amdq, apdq);
+      else if (J.side == 2) S::template rpn<T>(prob, 2, qf, qcr, af, ax, wave, s, amdq, apdq);
+      else if (J.side == 3) S::template rpn<T>(prob, 1, qf, qcr, af, ax, wave, s, amdq, apdq);
+      else S::template rpn<T>(prob, 2, qcr, qf, ax, af, wave, s, amdq, apdq);
 #pragma unroll
       for (int m = 0; m < ME; ++m) {
         const double am = amdq[m], ap = apdq[m];  // registers accumulate in FP64
@@ -880,6 +1005,7 @@ static void launch_qad2_t(int solver, T* pool, double* regs, const PatchDev* pat
     case SOLVER_ADVECTION: qad2_kernel<Advection2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt, dt_dev); break;
     case SOLVER_ACOUSTICS: qad2_kernel<Acoustics2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt, dt_dev); break;
     case SOLVER_EULER: qad2_kernel<Euler2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt, dt_dev); break;
+    case SOLVER_VC_ADVECTION: qad2_kernel<VcAdvection2, T><<<njobs, 64, 0, s>>>(pool, regs, patches, jobs, njobs, prob, lc, delt, dt_dev); break;
   }
 }
 
@@ -919,9 +1045,11 @@ void launch_upbnd(void* pool, const double* regs, const PatchDev* patches, const
   AMR_CUDA(cudaGetLastError());
 }
 
+// update.f:133-163: the average of the fine cells over a coarse cell, kappa-weighted and
+// divided by totrat * kappa of the coarse cell when there is a capacity (mcapa > 0)
 template <class T>
 __global__ void average_kernel(T* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry,
-                               int nvar) {
+                               int nvar, int mcapa) {
   const int r = blockIdx.y;
   if (r >= nrects) return;
   const AvgRect A = rects[r];
@@ -937,20 +1065,32 @@ __global__ void average_kernel(T* pool, const PatchDev* patches, const AvgRect* 
     const int b = rem / A.ni, aa = rem % A.ni;
     const int fi = A.fi0 + aa * rx, fj = A.fj0 + b * ry;
     double s = 0.0;
-    for (int jco = 0; jco < ry; ++jco)
-      for (int ico = 0; ico < rx; ++ico) s = s + (double)qf[m * fpl + (long long)(fj + jco) * K.mitot + (fi + ico)];
-    s = s / totrat;
-    qc[m * cpl + (long long)(A.cj0 + b) * C.mitot + (A.ci0 + aa)] = (T)s;
+    const long long kc = (long long)(A.cj0 + b) * C.mitot + (A.ci0 + aa);
+    if (mcapa == 0) {
+      for (int jco = 0; jco < ry; ++jco)
+        for (int ico = 0; ico < rx; ++ico) s = s + (double)qf[m * fpl + (long long)(fj + jco) * K.mitot + (fi + ico)];
+      s = s / totrat;
+    } else {
+      const T* kf = pool + K.aux + (long long)(mcapa - 1) * fpl;
+      const T* kcap = pool + C.aux + (long long)(mcapa - 1) * cpl;
+      for (int jco = 0; jco < ry; ++jco)
+        for (int ico = 0; ico < rx; ++ico) {
+          const long long kk = (long long)(fj + jco) * K.mitot + (fi + ico);
+          s = s + (double)qf[m * fpl + kk] * (double)kf[kk];
+        }
+      s = s / (totrat * (double)kcap[kc]);
+    }
+    qc[m * cpl + kc] = (T)s;
   }
 }
 
 void launch_average(void* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
-                    cudaStream_t s, bool f32) {
+                    cudaStream_t s, bool f32, int mcapa) {
   for (int base = 0; base < nrects; base += 65535) {
     const int n = std::min(65535, nrects - base);
     dim3 grid(4, n);
-    if (f32) average_kernel<<<grid, 128, 0, s>>>(static_cast<float*>(pool), patches, rects + base, n, rx, ry, nvar);
-    else average_kernel<<<grid, 128, 0, s>>>(static_cast<double*>(pool), patches, rects + base, n, rx, ry, nvar);
+    if (f32) average_kernel<<<grid, 128, 0, s>>>(static_cast<float*>(pool), patches, rects + base, n, rx, ry, nvar, mcapa);
+    else average_kernel<<<grid, 128, 0, s>>>(static_cast<double*>(pool), patches, rects + base, n, rx, ry, nvar, mcapa);
     AMR_CUDA(cudaGetLastError());
   }
 }
@@ -1055,23 +1195,28 @@ void launch_zero_tiny(void* pool, const PatchDev* patches, const int* plist, int
   }
 }
 
+// conck.f:44-60: the first component over the interior, times kappa with a capacity
 template <class T>
-__global__ void mass2_kernel(const T* pool, const PatchDev* patches, const int* plist, int np, double* out) {
+__global__ void mass2_kernel(const T* pool, const PatchDev* patches, const int* plist, int np, double* out, int mcapa) {
   double s = 0.0;
   for (int pi = blockIdx.y; pi < np; pi += gridDim.y) {
     const PatchDev P = patches[plist[pi]];
     const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
     const T* q = pool + P.q[P.cur];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my; t += gridDim.x * blockDim.x)
-      s += (double)q[(long long)(t / mx + 2) * P.mitot + (t % mx + 2)];
+    const T* kap = mcapa > 0 ? pool + P.aux + (long long)(mcapa - 1) * P.mitot * P.mjtot : nullptr;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mx * my; t += gridDim.x * blockDim.x) {
+      const long long k = (long long)(t / mx + 2) * P.mitot + (t % mx + 2);
+      s += kap ? (double)q[k] * (double)kap[k] : (double)q[k];
+    }
   }
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
-void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32) {
+void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32,
+                  int mcapa) {
   if (np <= 0) return;
-  if (f32) mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist, np, out);
-  else mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist, np, out);
+  if (f32) mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(static_cast<const float*>(pool), patches, plist, np, out, mcapa);
+  else mass2_kernel<<<dim3(4, std::min(np, 4096)), 128, 0, s>>>(static_cast<const double*>(pool), patches, plist, np, out, mcapa);
   AMR_CUDA(cudaGetLastError());
 }
 

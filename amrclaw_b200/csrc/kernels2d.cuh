@@ -59,7 +59,7 @@ struct StepArgs {
 };
 
 // ---------------------------------------------------------------- ghost-fill programs
-enum FillKind { FILL_COPY = 0, FILL_INTERP = 1, FILL_PIECE = 2, FILL_FILVAL = 3, FILL_RING = 4 };
+enum FillKind { FILL_COPY = 0, FILL_INTERP = 1, FILL_PIECE = 2, FILL_FILVAL = 3, FILL_RING = 4, FILL_FIXCAPA = 5 };
 
 struct ScratchRect {
   long long off;         // pool offset (doubles), layout [m][j][i]
@@ -76,7 +76,10 @@ struct FillOp {
   int si0, sj0;          // COPY/PIECE: origin in the source array (0-based); INTERP/FILVAL: global fine index of the region origin
   int level;             // COPY: source level for the time mode (-1: always store1); INTERP/FILVAL: fine level
   int cilo, cjlo;        // INTERP/FILVAL: global coarse index of the source rect origin
+  int capa0;             // FIXCAPA: first of the source rect's coarse kappa values in FillArgs::capa
 };
+// FIXCAPA (fixcapaq.f): di0/dj0 and si0/sj0 as FILVAL (the fine region's origin), ni x nj the
+// coarse cells the region covers; each unit is one coarse cell and its fine block.
 
 struct FillChunk { int op, start, count; };
 
@@ -101,6 +104,8 @@ struct FillArgs {
   const SrcMode* modes_dev;  // if set, the time-interpolation modes are read here (captured graphs)
   LevelConst lc;
   double xlower, ylower;
+  int mcapa;                 // capacity component of the patches' aux (FIXCAPA)
+  const double* capa;        // coarse kappa of the FIXCAPA ops' source rects
 };
 
 struct BcArgs {
@@ -137,14 +142,16 @@ void launch_qad2(int solver, void* pool, double* regs, const PatchDev* patches, 
                  const double* dt_dev = nullptr);
 void launch_upbnd(void* pool, const double* regs, const PatchDev* patches, const UpbndCell* cells, int ncells,
                   const UpbndTerm* terms, double area, int nvar, cudaStream_t s, bool f32);
+// mcapa > 0: kappa-weighted averages (update.f:150-160)
 void launch_average(void* pool, const PatchDev* patches, const AvgRect* rects, int nrects, int rx, int ry, int nvar,
-                    cudaStream_t s, bool f32);
+                    cudaStream_t s, bool f32, int mcapa = 0);
 void launch_flags2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
                    int use_old, int flag_component, double tolsp, int nvar, int8_t* out, cudaStream_t s, bool f32);
 void launch_gauges2(const void* pool, const PatchDev* patches, const GaugeJob* jobs, int njobs, int nvar,
                     double* out, cudaStream_t s, bool f32);
 void launch_zero_tiny(void* pool, const PatchDev* patches, const int* plist, int np, int nvar, cudaStream_t s, bool f32);
-void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32);
+void launch_mass2(const void* pool, const PatchDev* patches, const int* plist, int np, double* out, cudaStream_t s, bool f32,
+                  int mcapa = 0);
 // whole arrays (ghost cells included) in the reference's q(m,i,j) order, for binary output
 void launch_gather_enlarged2(const void* pool, const PatchDev* patches, const int* plist, const long long* outoff, int np,
                              int nvar, double* out, int split, cudaStream_t s, bool f32);

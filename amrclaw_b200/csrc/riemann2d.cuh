@@ -11,6 +11,8 @@
 //   acoustics   constant-coefficient characteristic decomposition (FVMHP 3.8, 21.5)
 //   euler       Roe solver, 4 waves, Harten-Hyman entropy fix (FVMHP 15.3);
 //               transverse Roe splitting (FVMHP 21.6)
+//   vc_advection  advection in a face-centred velocity field: aux(1) = u at the left
+//               face, aux(2) = v at the bottom face of each cell (FVMHP 9.5, 20.8)
 // Arithmetic is written in a fixed evaluation order so that, built without
 // FMA contraction, results are bit-identical to the CPU oracle.
 #pragma once
@@ -21,12 +23,17 @@ namespace amrb {
 
 enum SolverKind { SOLVER_ADVECTION = 1, SOLVER_ACOUSTICS = 2, SOLVER_EULER = 3, SOLVER_VC_ADVECTION = 4 };
 
+constexpr int MAXAUX2 = 3;  // aux components a 2D run may carry (the staged aux tile)
+enum AuxType { AUX_CENTER = 0, AUX_XLEFT = 1, AUX_YLEFT = 2, AUX_CAPACITY = 3 };
+
 struct ProbDev {
   int solver;
   int efix;
   double ubar, vbar, wbar;
   double rho, bulk, cc, zz;
   double gamma, gamma1;
+  int naux;                 // aux components of the run (0..MAXAUX2)
+  int auxtype[MAXAUX2];     // amr.data aux_type codes (qad.f picks face values by them)
 };
 
 // std::min / std::max semantics (first argument on ties), including signed zeros.
@@ -36,18 +43,18 @@ template <class R> __host__ __device__ __forceinline__ R dsign(R a, R b) { retur
 
 // ---------------------------------------------------------------- advection
 struct Advection2 {
-  static constexpr int MEQN = 1, MWAVES = 1;
+  static constexpr int MEQN = 1, MWAVES = 1, NAUX = 0;
   template <class R>
-  __device__ static void rpn(const ProbDev& P, int ixy, const R* qL, const R* qR, R (&wave)[MWAVES][MEQN],
-                             R (&s)[MWAVES], R (&amdq)[MEQN], R (&apdq)[MEQN]) {
+  __device__ static void rpn(const ProbDev& P, int ixy, const R* qL, const R* qR, const R*, const R*,
+                             R (&wave)[MWAVES][MEQN], R (&s)[MWAVES], R (&amdq)[MEQN], R (&apdq)[MEQN]) {
     wave[0][0] = qR[0] - qL[0];
     s[0] = (ixy == 1) ? R(P.ubar) : R(P.vbar);
     amdq[0] = dmin(s[0], R(0)) * wave[0][0];
     apdq[0] = dmax(s[0], R(0)) * wave[0][0];
   }
   template <class R>
-  __device__ static void rpt(const ProbDev& P, int ixy, int imp, const R* qL, const R* qR, const R* asdq,
-                             R (&bm)[MEQN], R (&bp)[MEQN]) {
+  __device__ static void rpt(const ProbDev& P, int ixy, int imp, const R* qL, const R* qR, const R*, const R*,
+                             const R*, const R* asdq, R (&bm)[MEQN], R (&bp)[MEQN]) {
     const R st = (ixy == 1) ? R(P.vbar) : R(P.ubar);
     bm[0] = dmin(st, R(0)) * asdq[0];
     bp[0] = dmax(st, R(0)) * asdq[0];
@@ -56,10 +63,10 @@ struct Advection2 {
 
 // ---------------------------------------------------------------- acoustics
 struct Acoustics2 {
-  static constexpr int MEQN = 3, MWAVES = 2;
+  static constexpr int MEQN = 3, MWAVES = 2, NAUX = 0;
   template <class R>
-  __device__ static void rpn(const ProbDev& P, int ixy, const R* qL, const R* qR, R (&wave)[MWAVES][MEQN],
-                             R (&s)[MWAVES], R (&amdq)[MEQN], R (&apdq)[MEQN]) {
+  __device__ static void rpn(const ProbDev& P, int ixy, const R* qL, const R* qR, const R*, const R*,
+                             R (&wave)[MWAVES][MEQN], R (&s)[MWAVES], R (&amdq)[MEQN], R (&apdq)[MEQN]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
     const R zz = R(P.zz), cc = R(P.cc);
     const R d1 = qR[0] - qL[0];
@@ -80,8 +87,8 @@ struct Acoustics2 {
     }
   }
   template <class R>
-  __device__ static void rpt(const ProbDev& P, int ixy, int imp, const R* qL, const R* qR, const R* asdq,
-                             R (&bm)[MEQN], R (&bp)[MEQN]) {
+  __device__ static void rpt(const ProbDev& P, int ixy, int imp, const R* qL, const R* qR, const R*, const R*,
+                             const R*, const R* asdq, R (&bm)[MEQN], R (&bp)[MEQN]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
     const R zz = R(P.zz), cc = R(P.cc);
     const R a1 = (-asdq[0] + zz * asdq[mv]) / (R(2) * zz);
@@ -93,10 +100,10 @@ struct Acoustics2 {
 
 // ---------------------------------------------------------------- euler (Roe)
 struct Euler2 {
-  static constexpr int MEQN = 4, MWAVES = 4;
+  static constexpr int MEQN = 4, MWAVES = 4, NAUX = 0;
   template <class R>
-  __device__ static void rpn(const ProbDev& P, int ixy, const R* qL, const R* qR, R (&wave)[MWAVES][MEQN],
-                             R (&s)[MWAVES], R (&amdq)[MEQN], R (&apdq)[MEQN]) {
+  __device__ static void rpn(const ProbDev& P, int ixy, const R* qL, const R* qR, const R*, const R*,
+                             R (&wave)[MWAVES][MEQN], R (&s)[MWAVES], R (&amdq)[MEQN], R (&apdq)[MEQN]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
     const R g1 = R(P.gamma1), gam = R(P.gamma);
     const R rl = qL[0], rr = qR[0];
@@ -184,8 +191,8 @@ struct Euler2 {
     }
   }
   template <class R>
-  __device__ static void rpt(const ProbDev& P, int ixy, int imp, const R* qL, const R* qR, const R* asdq,
-                             R (&bm)[MEQN], R (&bp)[MEQN]) {
+  __device__ static void rpt(const ProbDev& P, int ixy, int imp, const R* qL, const R* qR, const R*, const R*,
+                             const R*, const R* asdq, R (&bm)[MEQN], R (&bp)[MEQN]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
     const R g1 = R(P.gamma1);
     const R rl = qL[0], rr = qR[0];
@@ -224,10 +231,37 @@ struct Euler2 {
   }
 };
 
+// ---------------------------------------------------------------- vc_advection
+// auxL / auxR: aux of the cells left and right of the interface (the reference's auxr(:,i-1)
+// and auxl(:,i)); the normal speed is the right cell's own face velocity. rpt: aux1/aux2/aux3
+// are the aux of the cell asdq belongs to in the rows below, at and above the sweep's row;
+// the split moves asdq with that cell's transverse face velocities on its lower face
+// (aux2) and on its upper face (aux3, the lower face of the cell above).
+struct VcAdvection2 {
+  static constexpr int MEQN = 1, MWAVES = 1, NAUX = 2;
+  template <class R>
+  __device__ static void rpn(const ProbDev&, int ixy, const R* qL, const R* qR, const R*, const R* auxR,
+                             R (&wave)[MWAVES][MEQN], R (&s)[MWAVES], R (&amdq)[MEQN], R (&apdq)[MEQN]) {
+    const R u = auxR[ixy - 1];
+    wave[0][0] = qR[0] - qL[0];
+    s[0] = u;
+    amdq[0] = dmin(u, R(0)) * wave[0][0];
+    apdq[0] = dmax(u, R(0)) * wave[0][0];
+  }
+  template <class R>
+  __device__ static void rpt(const ProbDev&, int ixy, int, const R*, const R*, const R*, const R* aux2,
+                             const R* aux3, const R* asdq, R (&bm)[MEQN], R (&bp)[MEQN]) {
+    const int kv = 3 - ixy;
+    bm[0] = dmin(aux2[kv - 1], R(0)) * asdq[0];
+    bp[0] = dmax(aux3[kv - 1], R(0)) * asdq[0];
+  }
+};
+
 // the registered 2D plugins satisfy the device plugin contract (include/amrgpu_riemann.cuh)
 static_assert(amrgpu_plugin::Check2D<Advection2, ProbDev, double>::value, "advection: rpn2/rpt2 contract");
 static_assert(amrgpu_plugin::Check2D<Acoustics2, ProbDev, double>::value, "acoustics: rpn2/rpt2 contract");
 static_assert(amrgpu_plugin::Check2D<Euler2, ProbDev, double>::value, "euler_roe_efix: rpn2/rpt2 contract");
 static_assert(amrgpu_plugin::Check2D<Euler2, ProbDev, float>::value, "euler_roe_efix (FP32): rpn2/rpt2 contract");
+static_assert(amrgpu_plugin::Check2D<VcAdvection2, ProbDev, double>::value, "vc_advection: rpn2/rpt2 contract");
 
 }  // namespace amrb

@@ -13,14 +13,21 @@
  * name and sets its constants (the reference's /cparam/ common block).
  *
  * 2D plugin (a struct S; R is float or double; P is the constants struct):
- *   static constexpr int MEQN, MWAVES;
+ *   static constexpr int MEQN, MWAVES, NAUX;
  *   __device__ static void rpn(const P&, int ixy, const R* qL, const R* qR,
+ *                              const R* auxL, const R* auxR,
  *                              R (&wave)[MWAVES][MEQN], R (&s)[MWAVES],
  *                              R (&amdq)[MEQN], R (&apdq)[MEQN]);
  *       qL: the state left of the interface (cell i-1), qR: right of it (cell i);
+ *       auxL, auxR: their aux values (the reference's auxr(:,i-1), auxl(:,i));
  *   __device__ static void rpt(const P&, int ixy, int imp, const R* qL, const R* qR,
+ *                              const R* aux1, const R* aux2, const R* aux3,
  *                              const R* asdq, R (&bmasdq)[MEQN], R (&bpasdq)[MEQN]);
- *       imp = 1 splits amdq (cell i-1), imp = 2 splits apdq (cell i).
+ *       imp = 1 splits amdq (cell i-1), imp = 2 splits apdq (cell i); aux1/aux2/aux3 are
+ *       the aux values of that cell in the rows below, at and above the sweep's row (the
+ *       reference's aux1/aux2/aux3 slices at index i-2+imp).
+ *   NAUX: the leading aux components the plugin reads (0: none; the aux pointers may then
+ *   be null).
  *
  * 3D plugin (a struct S<R> holding the interface's per-call state):
  *   static constexpr int NV (meqn), NW (mwaves);
@@ -50,11 +57,12 @@ template <class S, class P, class R>
 struct Check2D {
   static constexpr int ME = S::MEQN, MW = S::MWAVES;
   using Rpn = decltype(S::template rpn<R>(std::declval<const P&>(), 1, (const R*)nullptr, (const R*)nullptr,
-                                         std::declval<R (&)[MW][ME]>(), std::declval<R (&)[MW]>(),
-                                         std::declval<R (&)[ME]>(), std::declval<R (&)[ME]>()));
+                                         (const R*)nullptr, (const R*)nullptr, std::declval<R (&)[MW][ME]>(),
+                                         std::declval<R (&)[MW]>(), std::declval<R (&)[ME]>(), std::declval<R (&)[ME]>()));
   using Rpt = decltype(S::template rpt<R>(std::declval<const P&>(), 1, 1, (const R*)nullptr, (const R*)nullptr,
-                                         (const R*)nullptr, std::declval<R (&)[ME]>(), std::declval<R (&)[ME]>()));
-  static constexpr bool value = ME >= 1 && MW >= 1 && std::is_void<Rpn>::value && std::is_void<Rpt>::value;
+                                         (const R*)nullptr, (const R*)nullptr, (const R*)nullptr, (const R*)nullptr,
+                                         std::declval<R (&)[ME]>(), std::declval<R (&)[ME]>()));
+  static constexpr bool value = ME >= 1 && MW >= 1 && S::NAUX >= 0 && std::is_void<Rpn>::value && std::is_void<Rpt>::value;
 };
 
 /* Compile-time check of the 3D contract: instantiated on every registered 3D plugin. */
