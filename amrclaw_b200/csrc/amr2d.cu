@@ -2548,6 +2548,7 @@ class Amr2Gpu {
 
   // valout.f90: zero |q| < 1e-90 in place (the reference does) and optionally write fort.q / fort.t
   void output(double t);
+  void write_aux(bool binary);
 
   // ================================================================ check.f / restrt.f
   // A checkpoint, taken at a coarse-step boundary, holds what the continued run reads:
@@ -2908,7 +2909,69 @@ void Amr2Gpu::output(double t) {
     if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.q in " + outdir);
     write_fort_t(outdir, frame, t, nvar, ngrids, p.naux, 2, ng);
   }
+  if (p.out_aux(t)) write_aux(binary);
   ++frame;
+}
+
+// src/2d/valout.f90:216-286: fort.aNNNN when aux output is due. The aux arrays do not change
+// during a run, so they come from the host copies. ASCII: fort.q's headers and layout, after
+// zeroing |aux| < 1e-90 of the interior cells in place (on the device too); binary: every
+// grid's whole aux array, aux(m,i,j) with m fastest, nothing zeroed.
+void Amr2Gpu::write_aux(bool binary) {
+  const int na = p.naux;
+  if (!binary)
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) {
+        HPatch& g = node[m];
+        const int mi = mitot(m), mj = mjtot(m);
+        const size_t pl = (size_t)mi * mj;
+        bool changed = false;
+        for (int a = 0; a < na; ++a)
+          for (int j = ng; j < mj - ng; ++j)
+            for (int i = ng; i < mi - ng; ++i) {
+              double& v = g.haux[a * pl + (size_t)j * mi + i];
+              if (std::fabs(v) < 1e-90) {
+                if (v != 0.0 || std::signbit(v)) changed = true;
+                v = 0.0;
+              }
+            }
+        if (changed) {
+          upload_to(reinterpret_cast<char*>(pool.d) + sizeof(double) * g.aux, g.haux.data(), sizeof(double) * g.haux.size());
+          // the saved coarse rings copy these values (saveqc.f reads them every step)
+          for (int l = 1; l <= p.mxnest; ++l) dirty[l] |= NEED_SAVEQC;
+        }
+      }
+  if (!write_output) return;
+  if (binary) {
+    std::vector<double> v;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) {
+        const HPatch& g = node[m];
+        const size_t pl = (size_t)mitot(m) * mjtot(m);
+        for (size_t k = 0; k < pl; ++k)
+          for (int a = 0; a < na; ++a) v.push_back(g.haux[a * pl + k]);
+      }
+    write_raw(open_output(outdir, "fort.a", frame, "wb"), v, outdir);
+    return;
+  }
+  FILE* f = open_output(outdir, "fort.a", frame);
+  for (int lev = 1; lev <= lfine; ++lev)
+    for (int m : lgrids[lev]) {
+      const HPatch& g = node[m];
+      const int n2[2] = {g.nx(), g.ny()};
+      const double lo[2] = {g.xlo, g.ylo}, h[2] = {hxposs[lev], hyposs[lev]};
+      write_grid_header(f, 2, m, lev, n2, lo, h);
+      const int mi = mitot(m), mj = mjtot(m);
+      const size_t pl = (size_t)mi * mj;
+      for (int j = ng; j < mj - ng; ++j) {
+        for (int i = ng; i < mi - ng; ++i) {
+          for (int a = 0; a < na; ++a) std::fputs(fort_e(g.haux[a * pl + (size_t)j * mi + i], 26, 16).c_str(), f);
+          std::fputc('\n', f);
+        }
+        std::fputs("  \n", f);
+      }
+    }
+  if (std::fclose(f) != 0) throw std::runtime_error("cannot close fort.a in " + outdir);
 }
 
 }  // namespace amrb

@@ -88,6 +88,8 @@ struct Amr2 {
   double tfinal = 0; bool output_t0 = true;
   std::vector<double> tout;
   int output_format = 1;
+  std::vector<int> output_aux_components;
+  bool output_aux_onlyonce = true;
   double dt_initial, dt_max, cflv1, cfl;
   int nv1; bool vtime;
   int method[8] = {0};
@@ -163,6 +165,10 @@ struct Amr2 {
     }
     output_format = c.iget("output_format", 1);
     if (output_format != 1 && output_format != 3) throw std::runtime_error("output_format must be 1 (ASCII) or 3 (binary)");
+    if (naux > 0 && c.has("output_aux_components")) {
+      for (int k = 0; k < naux; ++k) output_aux_components.push_back(c.i("output_aux_components", k));
+      output_aux_onlyonce = c.has("output_aux_onlyonce") ? c.b("output_aux_onlyonce") : true;
+    }
     dt_initial = c.d("dt_initial"); dt_max = c.d("dt_max");
     cflv1 = c.d("cfl_max"); cfl = c.d("cfl_desired"); nv1 = c.i("steps_max");
     if (output_style != 3) nstop = IINFINITY;
@@ -2551,8 +2557,53 @@ struct Amr2 {
   // reference and writes the values into fort.q. Binary (3, valout.f90:172-176): fort.q
   // holds the grid headers only and fort.b every grid's whole array (ghost cells
   // included, q(m,i,j) with m fastest) as raw doubles, nothing zeroed.
+  // src/2d/valout.f90:216-286: fort.aNNNN, the aux arrays, when any component is requested
+  // (every frame, or only at t0 with output_aux_onlyonce). ASCII: fort.q's headers and
+  // layout, after zeroing |aux| < 1e-90 of the interior cells in place; binary: each grid's
+  // whole aux array (ghost cells included, aux(m,i,j) with m fastest), nothing zeroed.
+  void write_aux(int lbeg, int lend, bool binary) {
+    char fn[64];
+    std::snprintf(fn, sizeof(fn), "/fort.a%04d", matlabu);
+    FILE* f = std::fopen((outdir + fn).c_str(), binary ? "wb" : "w");
+    if (!f) throw std::runtime_error("cannot write " + outdir + fn);
+    for (int level = lbeg; level <= lend; ++level)
+      for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+        Node2& g = node[m];
+        if (binary) { std::fwrite(g.aux.data(), sizeof(double), g.aux.size(), f); continue; }
+        const int mitot = mitot_of(m), mjtot = mjtot_of(m);
+        std::fprintf(f, "%6d                 grid_number\n%6d                 AMR_level\n%6d                 mx\n%6d                 my\n",
+                     m, level, g.ihi - g.ilo + 1, g.jhi - g.jlo + 1);
+        std::fprintf(f, "%s    xlow\n%s    ylow\n%s    dx\n%s    dy\n\n", fmtE(g.xlo, 26, 16).c_str(), fmtE(g.ylo, 26, 16).c_str(),
+                     fmtE(hxposs[level], 26, 16).c_str(), fmtE(hyposs[level], 26, 16).c_str());
+        FArr A{g.aux.data(), naux, mitot, mjtot};
+        for (int j = nghost + 1; j <= mjtot - nghost; ++j) {
+          for (int i = nghost + 1; i <= mitot - nghost; ++i) {
+            for (int ia = 1; ia <= naux; ++ia) std::fputs(fmtE(A(ia, i, j), 26, 16).c_str(), f);
+            std::fputc('\n', f);
+          }
+          std::fputs("  \n", f);
+        }
+      }
+    std::fclose(f);
+  }
+  void zero_tiny_aux(int lbeg, int lend) {
+    for (int level = lbeg; level <= lend; ++level)
+      for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
+        const int mitot = mitot_of(m), mjtot = mjtot_of(m);
+        FArr A{node[m].aux.data(), naux, mitot, mjtot};
+        for (int j = nghost + 1; j <= mjtot - nghost; ++j)
+          for (int i = nghost + 1; i <= mitot - nghost; ++i)
+            for (int ia = 1; ia <= naux; ++ia) if (std::fabs(A(ia, i, j)) < 1e-90) A(ia, i, j) = 0.0;
+      }
+  }
+
   void valout(int lbeg, int lend, double t) {
     const bool binary = output_format == 3;
+    int naux_out = 0;
+    for (int x : output_aux_components) naux_out += x;
+    const bool out_aux = naux_out > 0 && (!output_aux_onlyonce || std::fabs(t - t0) < 1e-90);
+    if (out_aux && !binary) zero_tiny_aux(lbeg, lend);
+    if (out_aux && write_output) write_aux(lbeg, lend, binary);
     for (int level = lbeg; level <= lend && !binary; ++level)
       for (int m = lstart[level]; m != 0; m = node[m].levelptr) {
         Node2& g = node[m];

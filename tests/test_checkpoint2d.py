@@ -77,6 +77,15 @@ def test_periodic_advection_restart_is_identical():
     _assert_same(full, cont)
 
 
+def test_annulus_restart_is_identical():
+    """aux arrays (face velocities, capacity) are set again by setaux on the restored grids."""
+    mk = configs.advection_annulus_regression
+    with tempfile.TemporaryDirectory() as d1, tempfile.TemporaryDirectory() as d2:
+        full = _solve(mk(), d1)
+        cont = _interrupted(mk(), d2, 7)
+    _assert_same(full, cont)
+
+
 def test_checkpoint_cadence_and_final_checkpoint():
     from amrclaw_b200 import Solver
     rd = problems.advection_square(32, levels=2, tfinal=0.1)

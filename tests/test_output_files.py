@@ -21,6 +21,11 @@ from oracle.pyoracle import Oracle2D, Oracle3D
 E26 = r"[ -]*-?0\.\d{16}(E[+-]\d\d|[+-]\d{3})"
 
 
+def _binary(rd):
+    rd.clawdata.output_format = "binary"
+    return rd
+
+
 def _files(d):
     return sorted(f for f in os.listdir(d) if re.fullmatch(r"fort\.[qtab]\d{4}", f))
 
@@ -118,6 +123,24 @@ def test_3d_aux_frames_byte_identical_to_the_oracle():
         assert re.search(r"^\s+3\s+naux$", open(os.path.join(dg, "fort.t0001")).read(), re.M)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("binary", [False, True], ids=["ascii", "binary"])
+def test_2d_aux_frames_byte_identical_to_the_oracle(binary):
+    """The annulus (aux: u, v, kappa): fort.a at t0 only (output_aux_onlyonce), naux = 3."""
+    rd = configs.advection_annulus_regression()
+    c = rd.clawdata
+    c.num_output_times = 2; c.output_t0 = True
+    c.output_aux_components = "all"; c.output_aux_onlyonce = True
+    if binary:
+        _binary(rd)
+    with tempfile.TemporaryDirectory() as tmp:
+        og, dg, _ = _run_both(rd, 2, tmp)
+        _assert_same_files(og, dg)
+        names = _files(dg)
+        assert [n for n in names if n.startswith("fort.a")] == ["fort.a0000"]
+        assert re.search(r"^\s+3\s+naux$", open(os.path.join(dg, "fort.t0001")).read(), re.M)
+
+
 # ----------------------------------------------------------------- CPU: the oracle's layout
 def _fortran_float(field):
     """Value of an Ew.d field: 0.ddddE+xx, or 0.dddd+xxx when the exponent has 3 digits."""
@@ -198,11 +221,6 @@ def test_fort_q_layout_follows_header_format_and_rows():
 
 
 # ----------------------------------------------------------------- binary form (output_format 3)
-def _binary(rd):
-    rd.clawdata.output_format = "binary"
-    return rd
-
-
 @pytest.mark.gpu
 @pytest.mark.parametrize("split", [False, True])
 def test_2d_binary_frames_byte_identical_to_the_oracle(split):

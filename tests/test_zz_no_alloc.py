@@ -41,6 +41,20 @@ def test_noalloc_level_advance_matches_level_advance(level):
     assert o1 == o0
 
 
+@pytest.mark.parametrize("level", [1, 2])
+def test_noalloc_level_advance_with_aux_and_capacity(level):
+    """The annulus: the step reads the patches' aux and the saved coarse rings' aux."""
+    rd = configs.advection_annulus_regression()
+    with tempfile.TemporaryDirectory() as d:
+        rd.write(d)
+        g0, v0, o0 = _advance_twice(d, level, noalloc=False)
+        g1, v1, o1 = _advance_twice(d, level, noalloc=True)
+    np.testing.assert_array_equal(g1, g0)
+    assert (g0[:, 1] == level).any()
+    np.testing.assert_array_equal(v1, v0)
+    assert o1 == o0
+
+
 def test_noalloc_substeps_allocate_nothing():
     """After the first call (which looks up the array's address and may load the kernels),
     further substeps change neither the context's peak pool bytes nor the device's free memory."""
