@@ -20,7 +20,8 @@ __all__ = ["ClawRunData", "Solver", "AmrError"]
 
 
 class AmrError(RuntimeError):
-    """A failed C-ABI call; ``code`` is its status (1 AMRGPU_ERROR, 2 AMRGPU_EINVAL)."""
+    """A failed C-ABI call; ``code`` is its status (1 AMRGPU_ERROR, 2 AMRGPU_EINVAL,
+    3 AMRGPU_ENOMEM: a capped device pool would have grown past its cap)."""
 
     def __init__(self, msg: str, code: int = 1):
         super().__init__(msg)
@@ -37,7 +38,8 @@ class Solver:
     """One AMR run on the GPU (the reference's ``amr2`` program from init to tfinal)."""
 
     def __init__(self, rundata_or_dir, outdir: str | None = None, write_output: bool = False, batched: bool = True,
-                 precision: str = "fp64", graphs: bool = False, schedule: int | None = None):
+                 precision: str = "fp64", graphs: bool = False, schedule: int | None = None,
+                 pool_limit: int = 0):
         self._lib = _lib.load()
         if isinstance(rundata_or_dir, ClawRunData):
             self._tmp = tempfile.TemporaryDirectory(prefix="amrgpu_")
@@ -62,6 +64,8 @@ class Solver:
             self.set_schedule(schedule)
         if graphs:
             self.set_graphs(True)
+        if pool_limit:
+            self.set_pool_limit(pool_limit)
 
     def set_batched(self, batched: bool) -> None:
         _check(self._lib, self._lib.amrgpu_set_batched(self._h, int(batched)), "amrgpu_set_batched")
@@ -84,6 +88,11 @@ class Solver:
         """The Riemann solver plugin by name, with its problem constants (amrgpu_set_solver)."""
         vals = (ctypes.c_double * max(1, len(params)))(*[float(x) for x in params])
         _check(self._lib, self._lib.amrgpu_set_solver(self._h, name.encode(), vals, len(params)), "amrgpu_set_solver")
+
+    def set_pool_limit(self, nbytes: int) -> None:
+        """Cap the context's device pools at nbytes (0: no cap); growth past it raises
+        AmrError with code 3 (amrgpu_set_pool_limit)."""
+        _check(self._lib, self._lib.amrgpu_set_pool_limit(self._h, int(nbytes)), "amrgpu_set_pool_limit")
 
     def set_profile(self, on: bool) -> None:
         _check(self._lib, self._lib.amrgpu_set_profile(self._h, int(on)), "amrgpu_set_profile")
@@ -125,7 +134,7 @@ class Solver:
                 "last_run_ms", "last_run_cells", "finished", "h2d_bytes",
                 "regrid_flags_s", "regrid_hostflags_s", "regrid_cluster_s", "regrid_fill_s", "regrid_prep_s", "regrid_compile_s",
                 "num_dim", "precision_bits", "graph_captures", "graph_replays", "levels_tuned_queue",
-                "levels_tuned_per_direction"]
+                "levels_tuned_per_direction", "pool_bytes"]
         out = (ctypes.c_double * len(keys))()
         _check(self._lib, self._lib.amrgpu_info(self._h, out, len(keys)), "amrgpu_info")
         return dict(zip(keys, list(out)))

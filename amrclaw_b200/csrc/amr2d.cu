@@ -2998,6 +2998,7 @@ class Solver2 : public AmrSolver {
   }
   void write_checkpoint(const char* path) override { g.checkpoint_file(path); }
   void set_solver(const std::string& name, const std::vector<double>& v) override { g.set_solver(name, v); }
+  void set_pool_limit(long long bytes) override { set_arena_limits(g.pool, g.regs, bytes); }
   void run(int max_cycles) override {
     g.max_cycles = max_cycles;
     g.tick();
@@ -3032,7 +3033,8 @@ class Solver2 : public AmrSolver {
     return {g.time, g.rvol, (double)g.ncycle, (double)g.lfine, g.t_step, g.t_regrid, g.tmass0,
             g.cflmax_run, (double)g.nkernels, (double)g.pool.peak * 8.0, (double)g.nsteps_launched,
             g.step_kernel_ms, g.step_kernel_cells, g.last_run_ms, g.run_cells, g.finished() ? 1.0 : 0.0, g.h2d_bytes,
-            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0, (double)g.graph_captures, (double)g.graph_replays, 0.0, 0.0};
+            g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0, (double)g.graph_captures, (double)g.graph_replays, 0.0, 0.0,
+            8.0 * (double)(g.pool.cap + g.regs.cap)};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;
@@ -3075,6 +3077,9 @@ static int guarded(F&& f) {
   try {
     f();
     return AMRGPU_OK;
+  } catch (amrb::PoolLimitError& e) {
+    g_err = e.what();
+    return AMRGPU_ENOMEM;
   } catch (std::exception& e) {
     g_err = e.what();
     return AMRGPU_ERROR;
@@ -3156,6 +3161,20 @@ int amrgpu_set_solver(amrgpu_ctx* ctx, const char* name, const double* params, i
   if (!ctx || !name || n < 0 || (n > 0 && !params)) { g_err = "amrgpu_set_solver: bad argument"; return AMRGPU_EINVAL; }
   try {
     ctx->s->set_solver(name, std::vector<double>(params, params + n));
+    return AMRGPU_OK;
+  } catch (std::invalid_argument& e) {
+    g_err = e.what();
+    return AMRGPU_EINVAL;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return AMRGPU_ERROR;
+  }
+}
+
+int amrgpu_set_pool_limit(amrgpu_ctx* ctx, long long bytes) {
+  if (!ctx) { g_err = "amrgpu_set_pool_limit: null context"; return AMRGPU_EINVAL; }
+  try {
+    ctx->s->set_pool_limit(bytes);
     return AMRGPU_OK;
   } catch (std::invalid_argument& e) {
     g_err = e.what();

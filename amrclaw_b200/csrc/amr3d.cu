@@ -2740,6 +2740,7 @@ class Amr3Gpu : public AmrSolver {
     for (auto& T : tune) T = Tune();
     for (auto& G : lgraph) G.reset();
   }
+  void set_pool_limit(long long bytes) override { set_arena_limits(pool, regs, bytes); }
   void run(int mc) override { max_cycles = mc; tick(); }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > lfine) throw std::runtime_error("level out of range");
@@ -2769,7 +2770,7 @@ class Amr3Gpu : public AmrSolver {
     return {time, rvol, (double)ncycle, (double)lfine, t_step, t_regrid, tmass0, cflmax_run, (double)nkernels, (double)pool.peak * 8.0,
             (double)nsteps_launched, step_kernel_ms, step_kernel_cells, last_run_ms, run_cells, finished() ? 1.0 : 0.0, h2d_bytes,
             0, 0, 0, 0, 0, 0, 3.0, f32 ? 32.0 : 64.0, (double)graph_captures, (double)graph_replays,
-            (double)tune_choices(1), (double)tune_choices(0)};
+            (double)tune_choices(1), (double)tune_choices(0), 8.0 * (double)(pool.cap + regs.cap)};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;

@@ -88,9 +88,15 @@ struct PhaseTimer {
 #define HPROF(name) ScopedTimer _hp_##__LINE__(hprof, name)  // rinfinity of amr_module.f90 (a default-REAL literal)
 
 // ------------------------------------------------------------------ device pool
+// An allocation that would grow a capped pool past its limit (amrgpu_set_pool_limit).
+struct PoolLimitError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 struct Arena {
   double* d = nullptr;
   long long cap = 0;
+  long long limit = 0;  // most doubles the pool may hold (0: no limit)
   // the context stream when one was set at init: the arena then lives in the device's
   // stream-ordered memory pool, and a new context reuses what an earlier one gave back
   // instead of mapping fresh pages
@@ -115,8 +121,12 @@ struct Arena {
   void grow(long long need) {
     const auto t0 = std::chrono::steady_clock::now();
     // kernels on any stream may still use the pool: let them finish before it moves
+    if (limit > 0 && cap + rnd(need) > limit)
+      throw PoolLimitError("device pool limit reached: " + std::to_string(sizeof(double) * (cap + rnd(need))) +
+                           " bytes needed, limit " + std::to_string(sizeof(double) * limit));
     AMR_CUDA(cudaDeviceSynchronize());
     long long ncap = std::max(cap * 2, cap + rnd(need) + (1 << 20));
+    if (limit > 0) ncap = std::min(ncap, limit);
     double* nd = nullptr;
     if (s) {
       // in the context stream's order: later work on that stream sees the moved pool
@@ -174,6 +184,19 @@ struct Arena {
     d = nullptr;
   }
 };
+
+// amrgpu_set_pool_limit: the patch pool and the register pool of a context share the cap,
+// each limited to what it holds now plus the rest of the cap (0 removes it)
+inline void set_arena_limits(Arena& pool, Arena& regs, long long bytes) {
+  if (bytes < 0) throw std::invalid_argument("amrgpu_set_pool_limit: negative size");
+  if (bytes == 0) { pool.limit = regs.limit = 0; return; }
+  const long long held = (long long)sizeof(double) * (pool.cap + regs.cap);
+  if (bytes < held)
+    throw std::invalid_argument("amrgpu_set_pool_limit: the pools already hold " + std::to_string(held) + " bytes");
+  const long long spare = (bytes - held) / (long long)sizeof(double);
+  pool.limit = pool.cap + spare;
+  regs.limit = regs.cap + spare;
+}
 
 // Pinned host staging for host-to-device uploads: a copy from pinned memory is
 // queued without the driver's pageable bounce. Space is reused only after the

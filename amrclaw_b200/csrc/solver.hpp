@@ -22,6 +22,10 @@ class AmrSolver {
   // std::invalid_argument for an unknown name, a wrong number of constants or a solver
   // whose equations and waves do not match the run
   virtual void set_solver(const std::string& name, const std::vector<double>& params) = 0;
+  // cap the device pools (patch storage and scratch, flux registers) at `bytes` in all;
+  // growth past it throws PoolLimitError. 0 removes the cap. The pools already hold
+  // pool_bytes(); a cap below that is refused (std::invalid_argument).
+  virtual void set_pool_limit(long long bytes) = 0;
   virtual void run(int max_cycles) = 0;                    // tick.f
   virtual double level_advance(int level, double* cfl) = 0;  // advanc.f; returns dtnew
   virtual void update_level(int level) = 0;                 // update.f

@@ -3,8 +3,12 @@
 Each admitted request gets its own context (device pool, CUDA stream) driven by its own
 host thread; the C library releases the interpreter while it works, so the level steps
 of all admitted solves are in flight on the device together and overlap there. A
-request waits in arrival order until both a slot and its estimated device memory are
-free; finished solves release both. Latency is completion time minus arrival time.
+request waits in arrival order until both a slot and its reserved device memory are
+free; finished solves release both. Each context's pools are capped at the request's
+reservation (amrgpu_set_pool_limit), so the budget holds: a solve that would outgrow
+its reservation stops with AMRGPU_ENOMEM, gives its reservation back and waits again,
+first in line, with twice the reservation (at most the whole budget). Latency is
+completion time minus arrival time.
 
     python -m amrclaw_b200.serve [--requests N] [--rate R] [--budget-gb G] [--slots S] [--scale small|full]
 
@@ -27,6 +31,7 @@ from . import problems
 from .replicas import percentiles
 
 KINDS = ("advection", "euler", "acoustics")
+ENOMEM = 3  # AMRGPU_ENOMEM
 
 
 @dataclass
@@ -40,6 +45,8 @@ class Request:
     tfinal: float
     precision: str          # "fp64" or "fp32" (the FP32 form)
     params: dict = field(default_factory=dict)
+    reserve: int = 0        # device bytes reserved at admission (0: est_bytes())
+    retries: int = 0        # admissions after a pool-cap stop
 
     def rundata(self):
         if self.kind == "advection":
@@ -52,11 +59,14 @@ class Request:
         return {"advection": 1, "euler": 4, "acoustics": 3}[self.kind]
 
     def est_bytes(self) -> int:
-        """Device memory reserved for admission: the context's initial pool (two buffers of
-        every level's worth of base grid, as the library sizes it), registers and scratch."""
-        word = 4 if self.precision == "fp32" else 8
-        pool = word * self.nvar() * (self.n + 4) ** 2 * 8 * self.levels + 8 * (1 << 22)
-        return int(pool + (24 << 20))
+        """Device memory reserved for admission: the context's initial patch pool (sized in
+        doubles in both precisions: eight arrays of the enlarged base grid per level, and
+        4 Mi doubles), its register pool (1 Mi doubles) and room for growth."""
+        pool = 8 * (self.nvar() * (self.n + 4) ** 2 * 8 * self.levels + (1 << 22))
+        return int(pool + 8 * (1 << 20) + (24 << 20))
+
+    def reservation(self) -> int:
+        return self.reserve or self.est_bytes()
 
 
 def synthetic_requests(n: int = 512, rate: float = 200.0, seed: int = 1, scale: str = "small") -> List[Request]:
@@ -110,10 +120,10 @@ class Result:
 
 
 def run_one(req: Request, keep_values: bool = False):
-    """One solve from start to tfinal on the current device, in the request's precision:
-    (cell updates, mass, values, device ms, pool peak)."""
+    """One solve from start to tfinal on the current device, in the request's precision, its
+    pools capped at the request's reservation: (cell updates, mass, values, device ms, pool peak)."""
     from . import Solver
-    with Solver(req.rundata(), batched=True, precision=req.precision) as s:
+    with Solver(req.rundata(), batched=True, precision=req.precision, pool_limit=req.reservation()) as s:
         s.run(0)
         inf = s.info()
         vals = s.values() if keep_values else None
@@ -130,22 +140,31 @@ def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: b
     waiting: List[Request] = []
     results: List[Result] = []
     lock = threading.Condition()
-    state = {"used": 0, "active": 0, "peak_active": 0, "peak_used": 0}
+    state = {"used": 0, "active": 0, "peak_active": 0, "peak_used": 0, "pool_retries": 0}
     t0 = clock()
 
     def worker(req: Request, admitted: float, est: int):
         err = None
         cells = mass = dev_ms = peak = 0.0
         vals = None
+        retry = False
         try:
             cells, mass, vals, dev_ms, peak = runner(req, keep_values)
         except Exception as e:  # reported per request; the server keeps going
             err = str(e)
+            # AMRGPU_ENOMEM: the solve outgrew its reservation; readmit with twice as much
+            retry = getattr(e, "code", None) == ENOMEM and est < budget_bytes
         done = clock() - t0
         with lock:
-            results.append(Result(req.rid, req.arrival, admitted, done, cells, mass, vals, dev_ms, peak, err))
             state["used"] -= est
             state["active"] -= 1
+            if retry:
+                req.reserve = min(2 * est, budget_bytes)
+                req.retries += 1
+                state["pool_retries"] += 1
+                waiting.insert(0, req)
+            else:
+                results.append(Result(req.rid, req.arrival, admitted, done, cells, mass, vals, dev_ms, peak, err))
             lock.notify_all()
 
     threads = []
@@ -156,7 +175,7 @@ def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: b
                 waiting.append(pending.pop(0))
             # FIFO admission: the oldest waiting request first, while slot and memory allow
             while waiting and state["active"] < slots:
-                est = waiting[0].est_bytes()
+                est = waiting[0].reservation()
                 if state["used"] + est > budget_bytes and state["active"] > 0:
                     break
                 req = waiting.pop(0)
@@ -183,7 +202,7 @@ def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: b
         "p50_latency_ms": 1e3 * p50, "p99_latency_ms": 1e3 * p99, "makespan_s": makespan,
         "cell_updates": cells, "throughput_cell_updates_per_s": cells / makespan if makespan > 0 else 0.0,
         "peak_concurrent": state["peak_active"], "peak_reserved_bytes": state["peak_used"],
-        "budget_bytes": budget_bytes, "slots": slots,
+        "budget_bytes": budget_bytes, "slots": slots, "pool_retries": state["pool_retries"],
         "fp32_requests": sum(1 for r in requests if r.precision == "fp32"),
     }
     return {"summary": summary, "results": sorted(results, key=lambda r: r.rid)}

@@ -18,6 +18,7 @@ extern "C" {
 #define AMRGPU_OK 0
 #define AMRGPU_ERROR 1
 #define AMRGPU_EINVAL 2
+#define AMRGPU_ENOMEM 3  /* a capped device pool would have to grow past its cap */
 
 typedef struct amrgpu_ctx amrgpu_ctx;
 
@@ -85,6 +86,7 @@ int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule);
  *   2D  "advection"       params u, v            (num_eqn 1, num_waves 1)
  *       "acoustics"       params rho, bulk       (num_eqn 3, num_waves 2)
  *       "euler_roe_efix"  params gamma[, efix]   (num_eqn 4, num_waves 4)
+ *       "vc_advection"    no params; face velocities in aux 1..2 (num_eqn 1)
  *   3D  "euler_roe_efix"  params gamma[, efix]   (num_eqn 5, num_waves 3)
  *       "vc_advection"    no params; face velocities in aux 1..3 (num_eqn 1, num_aux 3)
  * Unknown names, a wrong count or invalid constants, and solvers whose equations do not
@@ -92,6 +94,15 @@ int amrgpu_set_schedule(amrgpu_ctx* ctx, int schedule);
  * every later substep (and, in 3D Euler, to the pressure of the flagging). The problem
  * named in setprob.data still sets the initial data and the default solver. */
 int amrgpu_set_solver(amrgpu_ctx* ctx, const char* name, const double* params, int n);
+
+/* Caps the context's device pools (patch storage and fill scratch, flux registers) at
+ * `bytes` in all; 0 removes the cap. No counterpart in the reference, whose storage is one
+ * growable array (igetsp.f calls resize_storage, src/2d/resize_alloc.f90, when it runs
+ * out): a serving loop that admits solves by an HBM budget caps each at its share.
+ * A later call that would grow a pool past the cap returns AMRGPU_ENOMEM and the solve
+ * stops there (destroy the context). A cap below what the pools already hold returns
+ * AMRGPU_EINVAL and changes nothing. */
+int amrgpu_set_pool_limit(amrgpu_ctx* ctx, long long bytes);
 
 /* 1: record CUDA events around every patch-step launch (kernel time is then
  * reported by amrgpu_info); 0: no per-launch events. */
@@ -147,7 +158,8 @@ int amrgpu_mass(amrgpu_ctx* ctx, double* mass_out);
  * and list set-up, device-program compilation, then the number of space dimensions,
  * the precision in bits (64 or 32), the CUDA graphs captured and replayed, and (3D)
  * the number of levels whose autotuned sweep schedule is the work queue, and the number
- * whose is per direction. */
+ * whose is per direction, then the bytes the device pools hold now (what
+ * amrgpu_set_pool_limit counts). */
 int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 
 /* Hierarchy rows in output order (valout.f90 loop order): (grid_number, level,

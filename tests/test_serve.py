@@ -45,6 +45,54 @@ def test_admission_respects_slots_and_budget():
     assert [r.rid for r in out["results"]] == list(range(24))
 
 
+def test_pool_cap_stop_readmits_with_twice_the_reservation():
+    """A solve that outgrows its reservation (the library's AMRGPU_ENOMEM under the pool
+    cap) gives the reservation back and is admitted again, first in line, with twice as
+    much; the reserved total never passes the budget and the accounting returns to zero."""
+    from amrclaw_b200 import AmrError
+    reqs = serve.synthetic_requests(12, rate=2000.0, seed=9, scale="small")
+    need = {r.rid: (2 if r.rid % 3 == 0 else 1) * r.est_bytes() for r in reqs}
+    seen = {}
+    live = {"bytes": 0, "max": 0}
+    mu = threading.Lock()
+
+    def fake(req, keep):
+        with mu:
+            seen.setdefault(req.rid, []).append(req.reservation())
+            live["bytes"] += req.reservation(); live["max"] = max(live["max"], live["bytes"])
+        try:
+            time.sleep(0.01)
+            if req.reservation() < need[req.rid]:
+                raise AmrError("amrgpu_run failed: device pool limit reached", serve.ENOMEM)
+            return float(req.n * req.n), 1.0, None, 1.0, float(need[req.rid])
+        finally:
+            with mu:
+                live["bytes"] -= req.reservation()
+
+    budget = 6 * max(r.est_bytes() for r in reqs)
+    out = serve.serve(reqs, budget_bytes=budget, slots=4, runner=fake)
+    s = out["summary"]
+    assert s["completed"] == 12 and s["failed"] == 0
+    assert s["pool_retries"] == sum(1 for r in reqs if r.rid % 3 == 0)
+    for r in reqs:
+        e = r.est_bytes()
+        assert seen[r.rid] == ([e, 2 * e] if r.rid % 3 == 0 else [e])
+    assert live["max"] <= budget and live["bytes"] == 0
+
+
+def test_pool_cap_stop_is_final_at_the_whole_budget():
+    from amrclaw_b200 import AmrError
+    reqs = serve.synthetic_requests(2, rate=2000.0, seed=2, scale="small")
+
+    def fake(req, keep):
+        raise AmrError("amrgpu_run failed: device pool limit reached", serve.ENOMEM)
+
+    out = serve.serve(reqs, budget_bytes=4 * max(r.est_bytes() for r in reqs), slots=2, runner=fake)
+    s = out["summary"]
+    assert s["failed"] == 2 and s["completed"] == 0
+    assert all(r.error and "pool limit" in r.error for r in out["results"])
+
+
 @pytest.mark.gpu
 def test_results_identical_alone_and_in_the_mix():
     reqs = serve.synthetic_requests(6, rate=1000.0, seed=7, scale="small")
@@ -58,3 +106,26 @@ def test_results_identical_alone_and_in_the_mix():
         cells, mass, vals, _, _ = alone[res.rid]
         assert res.cell_updates == cells
         np.testing.assert_array_equal(res.values, vals)
+
+
+@pytest.mark.gpu
+def test_pool_cap_stops_a_solve_with_enomem():
+    """amrgpu_set_pool_limit: a cap below what the pools hold is refused (EINVAL); a cap at
+    what they hold makes the first growth of a refining run stop with AMRGPU_ENOMEM."""
+    from amrclaw_b200 import AmrError, Solver, problems
+    rd = problems.euler_quadrants(64, levels=3, ratio=4, tfinal=0.02)
+    # level 3 everywhere from t = 0.005: the first regrid after that outgrows the pools
+    rd.regiondata.regions = [[3, 3, 0.005, 1e9, 0.0, 1.0, 0.0, 1.0]]
+    with Solver(rd) as s:
+        held = int(s.info()["pool_bytes"])
+        assert held > 0
+        with pytest.raises(AmrError) as e:
+            s.set_pool_limit(held - 8)
+        assert e.value.code == 2
+        s.set_pool_limit(held)
+        with pytest.raises(AmrError) as e:
+            s.run(0)
+        assert e.value.code == serve.ENOMEM and "pool limit" in str(e.value)
+    with Solver(rd, pool_limit=1 << 34) as s:  # a roomy cap changes nothing
+        s.run(0)
+        assert s.info()["finished"] == 1.0
