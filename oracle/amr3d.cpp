@@ -23,9 +23,10 @@
 //                   tick.f (same cycle as src/2d/tick.f:4-391), conck.f:4-87
 //   output          valout.f90 (3D header), gauges_module.f90:302-460
 //
-// Periodic boundaries (prefilp.f, preicall.f, preintcopy.f) are not restated:
-// the 3D configurations use extrapolation or wall boundaries; a periodic run is
-// rejected at start-up.
+//   periodic        prefilp.f:1-266 (prefilrecur over 27 regions), preicall.f:1-141,
+//                   preintcopy.f, bound.f:60-199, filpatch.f:168-179, saveqc.f:72-91,
+//                   filval.f:52-68, prepc.f:84-122, domprep.f, domshrink.f, domup.f,
+//                   domcopy.f, shiftset.f (the periodic branches)
 #include "common.hpp"
 #include "riemann3d.hpp"
 #include <algorithm>
@@ -184,7 +185,6 @@ struct Amr3 {
     xperdom = (mthbc[1] == 2 && mthbc[2] == 2);
     yperdom = (mthbc[3] == 2 && mthbc[4] == 2);
     zperdom = (mthbc[5] == 2 && mthbc[6] == 2);
-    if (xperdom || yperdom || zperdom) throw std::runtime_error("periodic boundaries are not supported in 3D");
     // amr3.f90:241-246: Godunov splitting (1) only; Strang splitting stops the reference
     if (dimensional_split > 1) throw std::runtime_error("Strang splitting is not supported (amrclaw stops)");
     if (method[3] < 0) throw std::runtime_error("transverse_waves < 0 (dimensional splitting) is not supported");
@@ -1024,7 +1024,12 @@ struct Amr3 {
       const int nrowc = iphi - iplo + 1, ncolc = jphi - jplo + 1, nfilc = kphi - kplo + 1;
       if (nrowc > ihi - ilo + 3 || ncolc > jhi - jlo + 3 || nfilc > khi - klo + 3) throw std::runtime_error("filrecur: coarse box too large");
       std::vector<double> valcrse((size_t)nrowc * ncolc * nfilc * nvar, 0.0);
-      filrecur(levc, valcrse.data(), nrowc, ncolc, nfilc, t, 1, 1, 1, iplo, iphi, jplo, jphi, kplo, kphi, true, -1);
+      // filpatch.f:168-179: a coarse box that leaves a periodic domain is filled by prefilrecur
+      const bool sticks = iplo < 0 || jplo < 0 || kplo < 0 || iphi >= iregsz[levc] || jphi >= jregsz[levc] || kphi >= kregsz[levc];
+      if ((xperdom || yperdom || zperdom) && sticks)
+        prefilrecur(levc, valcrse.data(), nrowc, ncolc, nfilc, t, 1, 1, 1, iplo, iphi, jplo, jphi, kplo, kphi, iplo, jplo, kplo);
+      else
+        filrecur(levc, valcrse.data(), nrowc, ncolc, nfilc, t, 1, 1, 1, iplo, iphi, jplo, jphi, kplo, kphi, true, -1);
       FArr3 VC{valcrse.data(), nvar, nrowc, ncolc, nfilc};
       FArr3 VB{valbig, nvar, mitot, mjtot, mktot};
       const double ratiox = (double)(float)rx, ratioy = (double)(float)ry, ratioz = (double)(float)rz;
@@ -1073,18 +1078,101 @@ struct Amr3 {
     if (patchOnly) bc3amr(valbig, mitot, mjtot, mktot, hxf, hyf, hzf, xlp, xrp, ybp, ytp, zfp, zrp);
   }
 
-  // bound.f:4-211
+  // prefilp.f / preicall.f / preintcopy.f: the three index ranges of one direction (below
+  // the domain, inside, above) and the shift that maps each into the domain when periodic
+  void per_ranges(bool per, int lo, int hi, int n, int st[3], int en[3], int sh[3]) const {
+    if (per) {
+      st[0] = lo; st[1] = 0; st[2] = n; en[0] = -1; en[1] = n - 1; en[2] = hi; sh[0] = n; sh[1] = 0; sh[2] = -n;
+    } else {
+      st[0] = n; st[1] = lo; st[2] = n; en[0] = -1; en[1] = hi; en[2] = -1; sh[0] = sh[1] = sh[2] = 0;
+    }
+  }
+
+  // prefilp.f:1-141 (prefilrecur): the patch [ilo,ihi]x[jlo,jhi]x[klo,khi] of level, split
+  // into the 27 regions; each non-empty region is filled by filrecur on a scratch patch of
+  // its own size at its periodically shifted place, then copied to valbig, whose array
+  // starts at index (iglo, jglo, kglo) (patchCopyOut)
+  void prefilrecur(int level, double* valbig, int mitot, int mjtot, int mktot, double t, int nrowst, int ncolst, int nfilst,
+                   int ilo, int ihi, int jlo, int jhi, int klo, int khi, int iglo, int jglo, int kglo) {
+    (void)nrowst; (void)ncolst; (void)nfilst;
+    int ist[3], iend[3], ishift[3], jst[3], jend[3], jshift[3], kst[3], kend[3], kshift[3];
+    per_ranges(xperdom, ilo, ihi, iregsz[level], ist, iend, ishift);
+    per_ranges(yperdom, jlo, jhi, jregsz[level], jst, jend, jshift);
+    per_ranges(zperdom, klo, khi, kregsz[level], kst, kend, kshift);
+    FArr3 VB{valbig, nvar, mitot, mjtot, mktot};
+    for (int i = 0; i < 3; ++i) {
+      const int i1 = std::max(ilo, ist[i]), i2 = std::min(ihi, iend[i]);
+      if (i1 > i2) continue;
+      for (int j = 0; j < 3; ++j) {
+        const int j1 = std::max(jlo, jst[j]), j2 = std::min(jhi, jend[j]);
+        if (j1 > j2) continue;
+        for (int k = 0; k < 3; ++k) {
+          const int k1 = std::max(klo, kst[k]), k2 = std::min(khi, kend[k]);
+          if (k1 > k2) continue;
+          const int mi = i2 - i1 + 1, mj = j2 - j1 + 1, mk = k2 - k1 + 1;
+          std::vector<double> vp((size_t)nvar * mi * mj * mk, 0.0);
+          filrecur(level, vp.data(), mi, mj, mk, t, 1, 1, 1, i1 + ishift[i], i2 + ishift[i], j1 + jshift[j], j2 + jshift[j],
+                   k1 + kshift[k], k2 + kshift[k], true, -1);
+          FArr3 VP{vp.data(), nvar, mi, mj, mk};
+          const int is = i1 - iglo, js = j1 - jglo, ks = k1 - kglo;
+          for (int kk = 1; kk <= mk; ++kk)
+            for (int jj = 1; jj <= mj; ++jj)
+              for (int ii = 1; ii <= mi; ++ii)
+                for (int m = 1; m <= nvar; ++m) VB(m, is + ii, js + jj, ks + kk) = VP(m, ii, jj, kk);
+        }
+      }
+    }
+  }
+
+  // preicall.f:1-141 / preintcopy.f: icall over the 27 regions with periodic shifts, each
+  // put at its place in val (iputst = i1 - ilo + 1)
+  void preicall(double* val, double* aux, int nrow, int ncol, int nfil, int ilo, int ihi, int jlo, int jhi, int klo, int khi,
+                int level) {
+    int ist[3], iend[3], ishift[3], jst[3], jend[3], jshift[3], kst[3], kend[3], kshift[3];
+    per_ranges(xperdom, ilo, ihi, iregsz[level], ist, iend, ishift);
+    per_ranges(yperdom, jlo, jhi, jregsz[level], jst, jend, jshift);
+    per_ranges(zperdom, klo, khi, kregsz[level], kst, kend, kshift);
+    for (int i = 0; i < 3; ++i) {
+      const int i1 = std::max(ilo, ist[i]), i2 = std::min(ihi, iend[i]);
+      if (i1 > i2) continue;
+      for (int j = 0; j < 3; ++j) {
+        const int j1 = std::max(jlo, jst[j]), j2 = std::min(jhi, jend[j]);
+        if (j1 > j2) continue;
+        for (int k = 0; k < 3; ++k) {
+          const int k1 = std::max(klo, kst[k]), k2 = std::min(khi, kend[k]);
+          if (k1 > k2) continue;
+          icall(val, aux, nrow, ncol, nfil, i1 + ishift[i], i2 + ishift[i], j1 + jshift[j], j2 + jshift[j], k1 + kshift[k],
+                k2 + kshift[k], level, i1 - ilo + 1, j1 - jlo + 1, k1 - klo + 1);
+        }
+      }
+    }
+  }
+
+  // bound.f:4-211: the six ghost slabs, each by prefilrecur where it leaves a periodic
+  // domain (the tests of bound.f:60-199), else by filrecur; then bc3amr on the whole array
   void bound(double t, double* valbig, int mitot, int mjtot, int mktot, int mptr, int ng = -1) {
     const Node3& g = node[mptr];
     if (ng < 0) ng = nghost;
     const int lev = g.level;
     const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
-    filrecur(lev, valbig, mitot, mjtot, mktot, t, 1, 1, ng + 1, g.ilo - ng, g.ilo - 1, g.jlo - ng, g.jhi + ng, g.klo, g.khi, false, mptr);
-    filrecur(lev, valbig, mitot, mjtot, mktot, t, mitot - ng + 1, 1, ng + 1, g.ihi + 1, g.ihi + ng, g.jlo - ng, g.jhi + ng, g.klo, g.khi, false, mptr);
-    filrecur(lev, valbig, mitot, mjtot, mktot, t, ng + 1, 1, ng + 1, g.ilo, g.ihi, g.jlo - ng, g.jlo - 1, g.klo, g.khi, false, mptr);
-    filrecur(lev, valbig, mitot, mjtot, mktot, t, ng + 1, mjtot - ng + 1, ng + 1, g.ilo, g.ihi, g.jhi + 1, g.jhi + ng, g.klo, g.khi, false, mptr);
-    filrecur(lev, valbig, mitot, mjtot, mktot, t, 1, 1, 1, g.ilo - ng, g.ihi + ng, g.jlo - ng, g.jhi + ng, g.klo - ng, g.klo - 1, false, mptr);
-    filrecur(lev, valbig, mitot, mjtot, mktot, t, 1, 1, mktot - ng + 1, g.ilo - ng, g.ihi + ng, g.jlo - ng, g.jhi + ng, g.khi + 1, g.khi + ng, false, mptr);
+    const int iglo = g.ilo - ng, jglo = g.jlo - ng, kglo = g.klo - ng;
+    auto slab = [&](bool per, int nrs, int ncs, int nfs, int i0, int i1, int j0, int j1, int k0, int k1) {
+      if (per) prefilrecur(lev, valbig, mitot, mjtot, mktot, t, nrs, ncs, nfs, i0, i1, j0, j1, k0, k1, iglo, jglo, kglo);
+      else filrecur(lev, valbig, mitot, mjtot, mktot, t, nrs, ncs, nfs, i0, i1, j0, j1, k0, k1, false, mptr);
+    };
+    const bool ystick = (g.ylo - ng * hy < ylower) || (g.yhi + ng * hy > yupper);
+    const bool xstick = (g.xlo - ng * hx < xlower) || (g.xhi + ng * hx > xupper);
+    // left, right (x), front, rear (y), bottom, top (z)
+    slab((xperdom && g.xlo - ng * hx < xlower) || (yperdom && ystick), 1, 1, ng + 1, g.ilo - ng, g.ilo - 1, g.jlo - ng, g.jhi + ng,
+         g.klo, g.khi);
+    slab((xperdom && g.xhi + ng * hx > xupper) || (yperdom && ystick), mitot - ng + 1, 1, ng + 1, g.ihi + 1, g.ihi + ng, g.jlo - ng,
+         g.jhi + ng, g.klo, g.khi);
+    slab(yperdom && g.ylo - ng * hy < ylower, ng + 1, 1, ng + 1, g.ilo, g.ihi, g.jlo - ng, g.jlo - 1, g.klo, g.khi);
+    slab(yperdom && g.yhi + ng * hy > yupper, ng + 1, mjtot - ng + 1, ng + 1, g.ilo, g.ihi, g.jhi + 1, g.jhi + ng, g.klo, g.khi);
+    slab((zperdom && g.zlo - ng * hz < zlower) || (xperdom && xstick) || (yperdom && ystick), 1, 1, 1, g.ilo - ng, g.ihi + ng,
+         g.jlo - ng, g.jhi + ng, g.klo - ng, g.klo - 1);
+    slab((zperdom && g.zhi + ng * hz > zupper) || (xperdom && xstick) || (yperdom && ystick), 1, 1, mktot - ng + 1, g.ilo - ng,
+         g.ihi + ng, g.jlo - ng, g.jhi + ng, g.khi + 1, g.khi + ng);
     bc3amr(valbig, mitot, mjtot, mktot, hx, hy, hz, g.xlo - ng * hx, g.xhi + ng * hx, g.ylo - ng * hy, g.yhi + ng * hy,
            g.zlo - ng * hz, g.zhi + ng * hz);
   }
@@ -1132,8 +1220,16 @@ struct Amr3 {
       const double xr = K.xhi + hxc, yr = K.yhi + hyc, zt = K.zhi + hzc;
       std::vector<double> tq((size_t)nrow * ncol * nfil * nvar, 0.0), ta((size_t)nrow * ncol * nfil * std::max(naux, 1), 0.0);
       const bool sticksout = (iclo < 0 || ichi == iregsz[levc] || jclo < 0 || jchi == jregsz[levc] || kclo < 0 || kchi == kregsz[levc]);
-      icall(tq.data(), ta.data(), nrow, ncol, nfil, iclo, ichi, jclo, jchi, kclo, kchi, levc, 1, 1, 1);
-      if (naux > 0 && sticksout) setaux(0, nrow, ncol, nfil, xl, yf, zb, hxc, hyc, hzc, ta.data());
+      // saveqc.f:78-91 takes the periodic copy only when all three directions are periodic;
+      // with fewer it leaves the ring's cells beyond a periodic face unset (uninitialised
+      // memory there, zero density here, and qad's Roe solve breaks). The copy is taken
+      // whenever a direction is periodic: the same as the reference with all three
+      // periodic or none, and defined with one or two. The aux keeps the reference's rule.
+      const bool perdom3 = xperdom && yperdom && zperdom;
+      if (sticksout && (xperdom || yperdom || zperdom))
+        preicall(tq.data(), ta.data(), nrow, ncol, nfil, iclo, ichi, jclo, jchi, kclo, kchi, levc);
+      else icall(tq.data(), ta.data(), nrow, ncol, nfil, iclo, ichi, jclo, jchi, kclo, kchi, levc, 1, 1, 1);
+      if (naux > 0 && sticksout && !perdom3) setaux(0, nrow, ncol, nfil, xl, yf, zb, hxc, hyc, hzc, ta.data());
       bc3amr(tq.data(), nrow, ncol, nfil, hxc, hyc, hzc, xl, xr, yf, yr, zb, zt);
       // cstore: sides 1 (x left), 2 (y top), 3 (x right), 4 (y bottom), 5 (z bottom), 6 (z top)
       FArr3 QC{tq.data(), nvar, nrow, ncol, nfil};
@@ -1701,6 +1797,18 @@ struct Amr3 {
         const int iphi = std::min(p.ihi, ichi), jphi = std::min(p.jhi, jchi), kphi = std::min(p.khi, kchi);
         if ((iplo <= iphi + 1 && jplo <= jphi + 1) && kplo <= kphi + 1)
           setuse(p.listbc, ispot, mkid, p.ilo, p.ihi, p.jlo, p.jhi, p.klo, p.khi, iclo, ichi, jclo, jchi, kclo, kchi);
+        // prepc.f:84-122: fine grids touching a periodic boundary, through their images
+        const int imax = iregsz[level] - 1, jmax = jregsz[level] - 1, kmax = kregsz[level] - 1;
+        const int ni = iregsz[level], nj = jregsz[level], nk = kregsz[level];
+        auto use = [&](int a0, int a1, int b0, int b1, int c0, int c1) {
+          setuse(p.listbc, ispot, mkid, p.ilo, p.ihi, p.jlo, p.jhi, p.klo, p.khi, a0, a1, b0, b1, c0, c1);
+        };
+        if (xperdom && p.ilo == 0 && ichi == imax) use(iclo - ni, ichi - ni, jclo, jchi, kclo, kchi);
+        if (xperdom && iclo == 0 && p.ihi == imax) use(iclo + ni, ichi + ni, jclo, jchi, kclo, kchi);
+        if (yperdom && p.jlo == 0 && jchi == jmax) use(iclo, ichi, jclo - nj, jchi - nj, kclo, kchi);
+        if (yperdom && jclo == 0 && p.jhi == jmax) use(iclo, ichi, jclo + nj, jchi + nj, kclo, kchi);
+        if (zperdom && p.klo == 0 && kchi == kmax) use(iclo, ichi, jclo, jchi, kclo - nk, kchi - nk);
+        if (zperdom && kclo == 0 && p.khi == kmax) use(iclo, ichi, jclo, jchi, kclo + nk, kchi + nk);
       }
     }
   }
@@ -1871,19 +1979,37 @@ struct Amr3 {
   }
 
   // ================================================================ regrid: domain flags
-  // Boundary extension shared by domprep/domshrink/domup/domcopy (non-periodic branches).
-  void extend_borders(I1& f, int is, int js, int ks) {
-    for (int k = 1; k <= ks; ++k) for (int j = 1; j <= js; ++j) {
-      if (f(1, j, k) == 1) f(0, j, k) = 1;
-      if (f(is, j, k) == 1) f(is + 1, j, k) = 1;
+  // The border ring of domprep/domshrink/domup/domcopy, direction by direction (x, y, z):
+  // a periodic direction copies the far interior layer over the whole ring of the other two
+  // indices (0..n+1); otherwise the interior edge is extended over the interior (skipped in
+  // domshrink's periodic directions, which keep their ring: skip_periodic).
+  void extend_borders(I1& f, int is, int js, int ks, bool skip_periodic = false) {
+    if (xperdom) {
+      if (!skip_periodic)
+        for (int k = 0; k <= ks + 1; ++k) for (int j = 0; j <= js + 1; ++j) { f(0, j, k) = f(is, j, k); f(is + 1, j, k) = f(1, j, k); }
+    } else {
+      for (int k = 1; k <= ks; ++k) for (int j = 1; j <= js; ++j) {
+        if (f(1, j, k) == 1) f(0, j, k) = 1;
+        if (f(is, j, k) == 1) f(is + 1, j, k) = 1;
+      }
     }
-    for (int k = 1; k <= ks; ++k) for (int i = 1; i <= is; ++i) {
-      if (f(i, 1, k) == 1) f(i, 0, k) = 1;
-      if (f(i, js, k) == 1) f(i, js + 1, k) = 1;
+    if (yperdom) {
+      if (!skip_periodic)
+        for (int k = 0; k <= ks + 1; ++k) for (int i = 0; i <= is + 1; ++i) { f(i, 0, k) = f(i, js, k); f(i, js + 1, k) = f(i, 1, k); }
+    } else {
+      for (int k = 1; k <= ks; ++k) for (int i = 1; i <= is; ++i) {
+        if (f(i, 1, k) == 1) f(i, 0, k) = 1;
+        if (f(i, js, k) == 1) f(i, js + 1, k) = 1;
+      }
     }
-    for (int j = 1; j <= js; ++j) for (int i = 1; i <= is; ++i) {
-      if (f(i, j, 1) == 1) f(i, j, 0) = 1;
-      if (f(i, j, ks) == 1) f(i, j, ks + 1) = 1;
+    if (zperdom) {
+      if (!skip_periodic)
+        for (int j = 0; j <= js + 1; ++j) for (int i = 0; i <= is + 1; ++i) { f(i, j, 0) = f(i, j, ks); f(i, j, ks + 1) = f(i, j, 1); }
+    } else {
+      for (int j = 1; j <= js; ++j) for (int i = 1; i <= is; ++i) {
+        if (f(i, j, 1) == 1) f(i, j, 0) = 1;
+        if (f(i, j, ks) == 1) f(i, j, ks + 1) = 1;
+      }
     }
   }
   // domprep.f:82-154 / domup.f:96-169: edge and corner cells of the border ring
@@ -1937,7 +2063,7 @@ struct Amr3 {
             if (in(i + a, j + b, k + c) <= 0) { ok = false; break; }
           out(i, j, k) = ok ? in(i, j, k) : 0;
         }
-    extend_borders(out, id, jd, kd);
+    extend_borders(out, id, jd, kd, true);
   }
   // domup.f:4-185
   void domup(I1& fine, I1& crse, int ib, int jb, int kb, int is, int js, int ks, int lev) {
@@ -2045,10 +2171,21 @@ struct Amr3 {
           if (f(i, j, k) == (signed char)GOODPT) f(i, j, k) = (signed char)BADPRO;
       }
     }
-    // shiftset.f (non-periodic: zero ring, buffer by ibuff from interior flags, add)
-    for (int k = 0; k <= ksize + 1; ++k) for (int j = 0; j <= jsize + 1; ++j) { f(0, j, k) = 0; f(isize + 1, j, k) = 0; }
-    for (int k = 0; k <= ksize + 1; ++k) for (int i = 0; i <= isize + 1; ++i) { f(i, 0, k) = 0; f(i, jsize + 1, k) = 0; }
-    for (int j = 0; j <= jsize + 1; ++j) for (int i = 0; i <= isize + 1; ++i) { f(i, j, 0) = 0; f(i, j, ksize + 1) = 0; }
+    // shiftset.f: the ring is the periodic image (or zero), then every interior flag is
+    // buffered by ibuff into a second array whose interior is added back (the ring of the
+    // second array is not: buffering does not wrap)
+    for (int k = 0; k <= ksize + 1; ++k) for (int j = 0; j <= jsize + 1; ++j) {
+      f(0, j, k) = xperdom ? f(isize, j, k) : 0;
+      f(isize + 1, j, k) = xperdom ? f(1, j, k) : 0;
+    }
+    for (int k = 0; k <= ksize + 1; ++k) for (int i = 0; i <= isize + 1; ++i) {
+      f(i, 0, k) = yperdom ? f(i, jsize, k) : 0;
+      f(i, jsize + 1, k) = yperdom ? f(i, 1, k) : 0;
+    }
+    for (int j = 0; j <= jsize + 1; ++j) for (int i = 0; i <= isize + 1; ++i) {
+      f(i, j, 0) = zperdom ? f(i, j, ksize) : 0;
+      f(i, j, ksize + 1) = zperdom ? f(i, j, 1) : 0;
+    }
     I1 f2;
     f2.init(isize, jsize, ksize);
     for (int k = 1; k <= ksize; ++k)
@@ -2389,7 +2526,9 @@ struct Amr3 {
     const int iclo = g.ilo / rx - 1, jclo = g.jlo / ry - 1, kclo = g.klo / rz - 1;
     const int ichi = (g.ihi + 1) / rx - 1 + 1, jchi = (g.jhi + 1) / ry - 1 + 1, kchi = (g.khi + 1) / rz - 1 + 1;
     std::vector<double> valc((size_t)nvar * mic * mjc * mkc, 0.0);
-    icall(valc.data(), nullptr, mic, mjc, mkc, iclo, ichi, jclo, jchi, kclo, kchi, levc, 1, 1, 1);
+    // filval.f:52-58: preintcopy with any periodic direction (the fine copy below is intcopy)
+    if (xperdom || yperdom || zperdom) preicall(valc.data(), nullptr, mic, mjc, mkc, iclo, ichi, jclo, jchi, kclo, kchi, levc);
+    else icall(valc.data(), nullptr, mic, mjc, mkc, iclo, ichi, jclo, jchi, kclo, kchi, levc, 1, 1, 1);
     bc3amr(valc.data(), mic, mjc, mkc, hxc, hyc, hzc, xl, xr, yf, yr, zb, zt);
     FArr3 V{g.q1.data(), nvar, mitot, mjtot, mktot}, VC{valc.data(), nvar, mic, mjc, mkc};
     std::vector<double> dudx(mic + 1), dudy(mic + 1), dudz(mic + 1);
