@@ -161,6 +161,9 @@ class Amr3Gpu : public AmrSolver {
   Step3Params sp{};
   int nvar = 5;
   double xlower, ylower, zlower, xupper, yupper, zupper;
+  // periodic directions (both sides of the direction have mthbc 2)
+  bool xperdom = false, yperdom = false, zperdom = false;
+  bool anyper() const { return xperdom || yperdom || zperdom; }
   int nxc, nyc, nzc;
   std::vector<HPatch3> node;
   int ndfree = 0, lfine = 1, id_hwm = 1;
@@ -287,7 +290,12 @@ class Amr3Gpu : public AmrSolver {
     // errest.f having written flags there, that would be the old solution
     if (!p.flag_richardson && p.tol > 0) throw std::runtime_error("flag_richardson_tol > 0 needs flag_richardson");
     for (int d = 1; d <= 6; ++d)
-      if (p.mthbc[d] != 1 && p.mthbc[d] != 3) throw std::runtime_error("3D device path: boundaries must be extrapolation or wall");
+      if (p.mthbc[d] != 1 && p.mthbc[d] != 2 && p.mthbc[d] != 3)
+        throw std::runtime_error("3D device path: boundaries must be extrapolation, periodic or wall");
+    for (int d = 0; d < 3; ++d)
+      if ((p.mthbc[2 * d + 1] == 2) != (p.mthbc[2 * d + 2] == 2))
+        throw std::runtime_error("3D device path: a periodic direction needs mthbc 2 on both of its sides");
+    xperdom = p.mthbc[1] == 2; yperdom = p.mthbc[3] == 2; zperdom = p.mthbc[5] == 2;
     sp.gamma = p.pn("gamma", 1.4); sp.gamma1 = sp.gamma - 1.0;
     sp.efix = (int)p.pn("efix", 1.0);
     for (int k = 0; k < 3; ++k) sp.mthlim[k] = k < (int)p.mthlim.size() ? p.mthlim[k] : 0;
@@ -673,7 +681,12 @@ class Amr3Gpu : public AmrSolver {
       const int nrowc = iphi - iplo + 1, ncolc = jphi - jplo + 1, nfilc = kphi - kplo + 1;
       if (nrowc > ni + 2 || ncolc > nj + 2 || nfilc > nk + 2) throw std::runtime_error("ghost fill: coarse box too large");
       const int R = P.add_rect(nrowc, ncolc, nfilc, nvar);
-      const int cst = c_filrecur(P, level - 1, Tgt3{-1, R, nrowc, ncolc, nfilc}, 1, 1, 1, iplo, iphi, jplo, jphi, kplo, kphi, true, -1);
+      // filpatch.f:168-179: a coarse box that leaves a periodic domain is filled by prefilrecur
+      const bool sticks = iplo < 0 || jplo < 0 || kplo < 0 || iphi >= iregsz[level - 1] || jphi >= jregsz[level - 1] ||
+                          kphi >= kregsz[level - 1];
+      const Tgt3 C{-1, R, nrowc, ncolc, nfilc};
+      const int cst = (anyper() && sticks) ? c_prefil3(P, level - 1, C, iplo, iphi, jplo, jphi, kplo, kphi, iplo, jplo, kplo)
+                                           : c_filrecur(P, level - 1, C, 1, 1, 1, iplo, iphi, jplo, jphi, kplo, kphi, true, -1);
       stage = cst + 1;
       std::vector<std::array<int, 6>> boxes;
       runs3(used, ni, nj, nk, boxes);
@@ -698,6 +711,72 @@ class Amr3Gpu : public AmrSolver {
     return stage;
   }
 
+  // prefilp.f / preicall.f: the three index ranges of one direction (below the domain,
+  // inside, above) and the shift that maps each into the domain when it is periodic
+  void per_ranges(bool per, int lo, int hi, int n, int st[3], int en[3], int sh[3]) const {
+    if (per) {
+      st[0] = lo; st[1] = 0; st[2] = n; en[0] = -1; en[1] = n - 1; en[2] = hi; sh[0] = n; sh[1] = 0; sh[2] = -n;
+    } else {
+      st[0] = n; st[1] = lo; st[2] = n; en[0] = -1; en[1] = hi; en[2] = -1; sh[0] = sh[1] = sh[2] = 0;
+    }
+  }
+  // prefilp.f:1-141 (prefilrecur): region [ilo,ihi]x[jlo,jhi]x[klo,khi] of `level` split into
+  // its 27 pieces; each non-empty piece is filled (filrecur, patch-only) into a scratch rect
+  // of its own size at its periodically shifted place, then copied into T, whose array
+  // starts at index (iglo, jglo, kglo). Returns the stage completing the region.
+  int c_prefil3(Prog3& P, int level, Tgt3 T, int ilo, int ihi, int jlo, int jhi, int klo, int khi, int iglo, int jglo, int kglo) {
+    int ist[3], iend[3], ish[3], jst[3], jend[3], jsh[3], kst[3], kend[3], ksh[3];
+    per_ranges(xperdom, ilo, ihi, iregsz[level], ist, iend, ish);
+    per_ranges(yperdom, jlo, jhi, jregsz[level], jst, jend, jsh);
+    per_ranges(zperdom, klo, khi, kregsz[level], kst, kend, ksh);
+    int done = 0;
+    for (int a = 0; a < 3; ++a) {
+      const int i1 = std::max(ilo, ist[a]), i2 = std::min(ihi, iend[a]);
+      if (i1 > i2) continue;
+      for (int b = 0; b < 3; ++b) {
+        const int j1 = std::max(jlo, jst[b]), j2 = std::min(jhi, jend[b]);
+        if (j1 > j2) continue;
+        for (int c = 0; c < 3; ++c) {
+          const int k1 = std::max(klo, kst[c]), k2 = std::min(khi, kend[c]);
+          if (k1 > k2) continue;
+          const int mi = i2 - i1 + 1, mj = j2 - j1 + 1, mk = k2 - k1 + 1;
+          const int R = P.add_rect(mi, mj, mk, nvar);
+          const int st_ = c_filrecur(P, level, Tgt3{-1, R, mi, mj, mk}, 1, 1, 1, i1 + ish[a], i2 + ish[a], j1 + jsh[b], j2 + jsh[b],
+                                     k1 + ksh[c], k2 + ksh[c], true, -1);
+          Fill3Op o{};
+          o.kind = F3_PIECE; o.dst_patch = T.patch; o.dst_rect = T.rect;
+          o.di0 = i1 - iglo; o.dj0 = j1 - jglo; o.dk0 = k1 - kglo; o.ni = mi; o.nj = mj; o.nk = mk;
+          o.src = R; o.si0 = 0; o.sj0 = 0; o.sk0 = 0;
+          P.add_op(o, st_ + 1);
+          done = std::max(done, st_ + 1);
+        }
+      }
+    }
+    return done;
+  }
+  // preicall.f:1-141 / preintcopy.f: icall over the 27 pieces with periodic shifts, each
+  // put at its place in T (iput = i1 - ilo + 1)
+  void c_preicall3(Prog3& P, Tgt3 T, int ilo, int ihi, int jlo, int jhi, int klo, int khi, int level, int st_) {
+    int ist[3], iend[3], ish[3], jst[3], jend[3], jsh[3], kst[3], kend[3], ksh[3];
+    per_ranges(xperdom, ilo, ihi, iregsz[level], ist, iend, ish);
+    per_ranges(yperdom, jlo, jhi, jregsz[level], jst, jend, jsh);
+    per_ranges(zperdom, klo, khi, kregsz[level], kst, kend, ksh);
+    for (int a = 0; a < 3; ++a) {
+      const int i1 = std::max(ilo, ist[a]), i2 = std::min(ihi, iend[a]);
+      if (i1 > i2) continue;
+      for (int b = 0; b < 3; ++b) {
+        const int j1 = std::max(jlo, jst[b]), j2 = std::min(jhi, jend[b]);
+        if (j1 > j2) continue;
+        for (int c = 0; c < 3; ++c) {
+          const int k1 = std::max(klo, kst[c]), k2 = std::min(khi, kend[c]);
+          if (k1 > k2) continue;
+          c_icall(P, T, i1 + ish[a], i2 + ish[a], j1 + jsh[b], j2 + jsh[b], k1 + ksh[c], k2 + ksh[c], level, i1 - ilo + 1, j1 - jlo + 1,
+                  k1 - klo + 1, st_);
+        }
+      }
+    }
+  }
+
   // bound.f:4-211 for one patch
   void compile_bound_patch(Prog3& P, int lev, int m) { bound_strips(P, lev, m, Tgt3{m, -1, mitot(m), mjtot(m), mktot(m)}, G3); }
   // bound.f with ghost width gw into target T (the enlarged array of patch m, or a scratch
@@ -705,14 +784,28 @@ class Amr3Gpu : public AmrSolver {
   void bound_strips(Prog3& P, int lev, int m, Tgt3 T, int gw) {
     const HPatch3& g = node[m];
     const int mi = T.ni, mj = T.nj, mk = T.nk;
-    int s = 0;
-    s = std::max(s, c_filrecur(P, lev, T, 1, 1, gw + 1, g.ilo - gw, g.ilo - 1, g.jlo - gw, g.jhi + gw, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, mi - gw + 1, 1, gw + 1, g.ihi + 1, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, gw + 1, 1, gw + 1, g.ilo, g.ihi, g.jlo - gw, g.jlo - 1, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, gw + 1, mj - gw + 1, gw + 1, g.ilo, g.ihi, g.jhi + 1, g.jhi + gw, g.klo, g.khi, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, 1, 1, 1, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.klo - gw, g.klo - 1, false, m));
-    s = std::max(s, c_filrecur(P, lev, T, 1, 1, mk - gw + 1, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.khi + 1, g.khi + gw, false, m));
     const double hx = hxposs[lev], hy = hyposs[lev], hz = hzposs[lev];
+    // bound.f:60-199: a strip that leaves a periodic domain is filled by prefilrecur (the
+    // x strips also when the patch leaves a periodic y range, the z strips when it leaves
+    // a periodic x or y range: their corners lie there)
+    const bool xl = g.xlo - gw * hx < xlower, xr = g.xhi + gw * hx > xupper;
+    const bool yl = g.ylo - gw * hy < ylower, yr = g.yhi + gw * hy > yupper;
+    const bool zl = g.zlo - gw * hz < zlower, zr = g.zhi + gw * hz > zupper;
+    const bool ystick = yperdom && (yl || yr), xstick = xperdom && (xl || xr);
+    const int iglo = g.ilo - gw, jglo = g.jlo - gw, kglo = g.klo - gw;
+    auto strip = [&](bool per, int nrs, int ncs, int nfs, int i0, int i1, int j0, int j1, int k0, int k1) {
+      return per ? c_prefil3(P, lev, T, i0, i1, j0, j1, k0, k1, iglo, jglo, kglo)
+                 : c_filrecur(P, lev, T, nrs, ncs, nfs, i0, i1, j0, j1, k0, k1, false, m);
+    };
+    int s = 0;
+    s = std::max(s, strip((xperdom && xl) || ystick, 1, 1, gw + 1, g.ilo - gw, g.ilo - 1, g.jlo - gw, g.jhi + gw, g.klo, g.khi));
+    s = std::max(s, strip((xperdom && xr) || ystick, mi - gw + 1, 1, gw + 1, g.ihi + 1, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.klo, g.khi));
+    s = std::max(s, strip(yperdom && yl, gw + 1, 1, gw + 1, g.ilo, g.ihi, g.jlo - gw, g.jlo - 1, g.klo, g.khi));
+    s = std::max(s, strip(yperdom && yr, gw + 1, mj - gw + 1, gw + 1, g.ilo, g.ihi, g.jhi + 1, g.jhi + gw, g.klo, g.khi));
+    s = std::max(s, strip((zperdom && zl) || xstick || ystick, 1, 1, 1, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jhi + gw, g.klo - gw,
+                          g.klo - 1));
+    s = std::max(s, strip((zperdom && zr) || xstick || ystick, 1, 1, mk - gw + 1, g.ilo - gw, g.ihi + gw, g.jlo - gw, g.jhi + gw,
+                          g.khi + 1, g.khi + gw));
     bool any;
     Bc3Op b = make_bc(T, hx, hy, hz, g.xlo - gw * hx, g.xhi + gw * hx, g.ylo - gw * hy, g.yhi + gw * hy, g.zlo - gw * hz, g.zhi + gw * hz, any);
     if (any) P.add_bc(b, s);
@@ -783,7 +876,13 @@ class Amr3Gpu : public AmrSolver {
       const int nrow = ichi - iclo + 1, ncol = jchi - jclo + 1, nfil = kchi - kclo + 1;
       const int R = P.add_rect(nrow, ncol, nfil, nvar);
       Tgt3 T{-1, R, nrow, ncol, nfil};
-      c_icall(P, T, iclo, ichi, jclo, jchi, kclo, kchi, lev, 1, 1, 1, 0);
+      // saveqc.f:72-91: the periodic copy where the ring leaves the domain. The reference
+      // takes it only with all three directions periodic and leaves the ring's cells beyond
+      // a periodic face unset otherwise; here (as in the CPU restatement) it is taken
+      // whenever a direction is periodic, which is the reference with three or none
+      const bool sticksout = iclo < 0 || ichi == iregsz[lev] || jclo < 0 || jchi == jregsz[lev] || kclo < 0 || kchi == kregsz[lev];
+      if (sticksout && anyper()) c_preicall3(P, T, iclo, ichi, jclo, jchi, kclo, kchi, lev, 0);
+      else c_icall(P, T, iclo, ichi, jclo, jchi, kclo, kchi, lev, 1, 1, 1, 0);
       bool any;
       Bc3Op b = make_bc(T, hxc, hyc, hzc, g.xlo - hxc, g.xhi + hxc, g.ylo - hyc, g.yhi + hyc, g.zlo - hzc, g.zhi + hzc, any);
       if (any) P.add_bc(b, 0);
@@ -1212,15 +1311,34 @@ class Amr3Gpu : public AmrSolver {
       HPatch3& g = node[parents[n]];
       g.listbc.clear();
       g.has_cfl = true;
-      std::vector<int> hits;
-      XF.query((g.ilo - 1) * rx, (g.ihi + 2) * rx - 1, (g.jlo - 1) * ry, (g.jhi + 2) * ry - 1, (g.klo - 1) * rz, (g.khi + 2) * rz - 1, hits);
-      for (int r : hits) {
-        const int k = XF.id(r);
+      // the kids within one coarse cell of the patch, in level order; a patch on a periodic
+      // face also meets kids through their periodic images, which can lie anywhere
+      const int imax = iregsz[lev] - 1, jmax = jregsz[lev] - 1, kmax = kregsz[lev] - 1;
+      const bool wrap = (xperdom && (g.ilo == 0 || g.ihi == imax)) || (yperdom && (g.jlo == 0 || g.jhi == jmax)) ||
+                        (zperdom && (g.klo == 0 || g.khi == kmax));
+      std::vector<int> kids;
+      if (wrap) {
+        for (int k = lstart[lev + 1]; k != 0; k = node[k].levelptr) kids.push_back(k);
+      } else {
+        std::vector<int> hits;
+        XF.query((g.ilo - 1) * rx, (g.ihi + 2) * rx - 1, (g.jlo - 1) * ry, (g.jhi + 2) * ry - 1, (g.klo - 1) * rz, (g.khi + 2) * rz - 1, hits);
+        for (int r : hits) kids.push_back(XF.id(r));
+      }
+      const int ni = iregsz[lev], nj = jregsz[lev], nk = kregsz[lev];
+      for (int k : kids) {
         const HPatch3& f = node[k];
         const int iclo = f.ilo / rx, jclo = f.jlo / ry, kclo = f.klo / rz, ichi = f.ihi / rx, jchi = f.jhi / ry, kchi = f.khi / rz;
         const int iplo = std::max(g.ilo, iclo), jplo = std::max(g.jlo, jclo), kplo = std::max(g.klo, kclo);
         const int iphi = std::min(g.ihi, ichi), jphi = std::min(g.jhi, jchi), kphi = std::min(g.khi, kchi);
         if ((iplo <= iphi + 1 && jplo <= jphi + 1) && kplo <= kphi + 1) setuse(g.listbc, k, g, iclo, ichi, jclo, jchi, kclo, kchi);
+        if (!wrap) continue;
+        // prepc.f:84-122: fine grids touching a periodic boundary, through their images
+        if (xperdom && g.ilo == 0 && ichi == imax) setuse(g.listbc, k, g, iclo - ni, ichi - ni, jclo, jchi, kclo, kchi);
+        if (xperdom && iclo == 0 && g.ihi == imax) setuse(g.listbc, k, g, iclo + ni, ichi + ni, jclo, jchi, kclo, kchi);
+        if (yperdom && g.jlo == 0 && jchi == jmax) setuse(g.listbc, k, g, iclo, ichi, jclo - nj, jchi - nj, kclo, kchi);
+        if (yperdom && jclo == 0 && g.jhi == jmax) setuse(g.listbc, k, g, iclo, ichi, jclo + nj, jchi + nj, kclo, kchi);
+        if (zperdom && g.klo == 0 && kchi == kmax) setuse(g.listbc, k, g, iclo, ichi, jclo, jchi, kclo - nk, kchi - nk);
+        if (zperdom && kclo == 0 && g.khi == kmax) setuse(g.listbc, k, g, iclo, ichi, jclo, jchi, kclo + nk, kchi + nk);
       }
     });
   }
@@ -1773,18 +1891,20 @@ class Amr3Gpu : public AmrSolver {
       boxes.push_back(LvlBox{g.ilo + 1, g.ihi + 1, g.jlo + 1, g.jhi + 1, g.klo + 1, g.khi + 1});
     }
     lv_boxes.upload(boxes, st, stg);
-    launch_domprep(lv_a.d, d0, lv_boxes.d, (int)boxes.size(), st);
-    launch_domshrink(lv_a.d, lv_b.d, d0, st);
+    const int per = (xperdom ? 1 : 0) | (yperdom ? 2 : 0) | (zperdom ? 4 : 0);
+    launch_domprep(lv_a.d, d0, lv_boxes.d, (int)boxes.size(), st, per);
+    launch_domshrink(lv_a.d, lv_b.d, d0, st, per);
     LvlDims dc = d0;
     for (int lev = lbase + 1; lev <= lcheck; ++lev) {
       const LvlDims df{dc.is * intratx[lev - 1], dc.js * intraty[lev - 1], dc.ks * intratz[lev - 1]};
-      launch_domup(lv_b.d, dc, lv_a.d, df, intratx[lev - 1], intraty[lev - 1], intratz[lev - 1], st);
-      launch_domshrink(lv_a.d, lv_b.d, df, st);
+      launch_domup(lv_b.d, dc, lv_a.d, df, intratx[lev - 1], intraty[lev - 1], intratz[lev - 1], st, per);
+      launch_domshrink(lv_a.d, lv_b.d, df, st, per);
       dc = df;
     }
-    // domcopy.f: the nesting domain keeps the shrunk array (its ring already extended); the
-    // shrunk array itself becomes the flag array
+    // domcopy.f: the nesting domain keeps the shrunk array (its ring extended again: without
+    // periodic directions that changes nothing); the shrunk array itself becomes the flag array
     AMR_CUDA(cudaMemcpyAsync(lv_n.d, lv_b.d, need, cudaMemcpyDeviceToDevice, st));
+    if (per) launch_domcopy_borders(lv_n.d, dl, st, per);
     launch_zero_interior(lv_b.d, dl, st);
     // spest.f fills the ghost cells of every grid whether or not it flags by gradient:
     // errest.f steps those values
@@ -2075,7 +2195,9 @@ class Amr3Gpu : public AmrSolver {
     const int mic = g.nx() / rx + 2, mjc = g.ny() / ry + 2, mkc = g.nz() / rz + 2;
     const int R = P.add_rect(mic, mjc, mkc, nvar);
     Tgt3 C{-1, R, mic, mjc, mkc};
-    c_icall(P, C, iclo, ichi, jclo, jchi, kclo, kchi, lev - 1, 1, 1, 1, 0);
+    // filval.f:52-58: preintcopy with any periodic direction (the fine copy below is intcopy)
+    if (anyper()) c_preicall3(P, C, iclo, ichi, jclo, jchi, kclo, kchi, lev - 1, 0);
+    else c_icall(P, C, iclo, ichi, jclo, jchi, kclo, kchi, lev - 1, 1, 1, 1, 0);
     bool any;
     Bc3Op b = make_bc(C, hxc, hyc, hzc, g.xlo - hxc, g.xhi + hxc, g.ylo - hyc, g.yhi + hyc, g.zlo - hzc, g.zhi + hzc, any);
     if (any) P.add_bc(b, 0);

@@ -244,9 +244,42 @@ __global__ void colate_kernel(int8_t* f, const int8_t* dom, LvlDims d) {
   }
 }
 
-void borders(int8_t* a, LvlDims d, bool edges, cudaStream_t s) {
-  const long long n = 2LL * ((long long)d.js * d.ks + (long long)d.is * d.ks + (long long)d.is * d.js);
-  extend_kernel<<<blocks_for(n, 256), 256, 0, s>>>(a, d);
+// extend_borders with periodic directions, one direction per launch in the order x, y, z
+// (a later direction reads ring cells an earlier one wrote): a periodic direction copies
+// the far interior layer over its whole ring face (0..n+1 in the other two indices); a
+// non-periodic one extends a 1 of the adjacent interior cell (other indices interior only)
+__global__ void border_dir_kernel(int8_t* a, LvlDims d, int dir, int periodic) {
+  const int e = periodic ? 2 : 0, o = periodic ? 0 : 1;
+  const long long na = (dir == 0 ? d.js : d.is) + e, nb = (dir == 2 ? d.js : d.ks) + e;
+  GRID_STRIDE(t, 2 * na * nb) {
+    const bool hi = t >= na * nb;
+    const long long r = hi ? t - na * nb : t;
+    const int u = (int)(r % na) + o, v = (int)(r / na) + o;
+    const int n = dir == 0 ? d.is : dir == 1 ? d.js : d.ks;
+    const int ring = hi ? n + 1 : 0;
+    const int src = periodic ? (hi ? 1 : n) : (hi ? n : 1);
+    long long at, from;
+    if (dir == 0) { at = d.at(ring, u, v); from = d.at(src, u, v); }
+    else if (dir == 1) { at = d.at(u, ring, v); from = d.at(u, src, v); }
+    else { at = d.at(u, v, ring); from = d.at(u, v, src); }
+    if (periodic) a[at] = a[from];
+    else if (a[from] == 1) a[at] = 1;
+  }
+}
+
+// per: bit 0, 1, 2 set for periodic x, y, z; skip: leave the ring of periodic directions as it is
+void borders(int8_t* a, LvlDims d, bool edges, cudaStream_t s, int per = 0, bool skip = false) {
+  if (per == 0) {
+    const long long n = 2LL * ((long long)d.js * d.ks + (long long)d.is * d.ks + (long long)d.is * d.js);
+    extend_kernel<<<blocks_for(n, 256), 256, 0, s>>>(a, d);
+  } else {
+    for (int dir = 0; dir < 3; ++dir) {
+      const bool p = (per >> dir) & 1;
+      if (p && skip) continue;
+      const long long na = (dir == 0 ? d.js : d.is) + (p ? 2 : 0), nb = (dir == 2 ? d.js : d.ks) + (p ? 2 : 0);
+      border_dir_kernel<<<blocks_for(2 * na * nb, 256), 256, 0, s>>>(a, d, dir, p ? 1 : 0);
+    }
+  }
   if (edges) {
     edges_kernel<<<blocks_for(4LL * (d.is + d.js + d.ks), 256), 256, 0, s>>>(a, d);
     corners_kernel<<<1, 32, 0, s>>>(a, d);
@@ -255,23 +288,28 @@ void borders(int8_t* a, LvlDims d, bool edges, cudaStream_t s) {
 
 }  // namespace
 
-void launch_domprep(int8_t* a, LvlDims d, const LvlBox* boxes, int nbox, cudaStream_t s) {
+void launch_domprep(int8_t* a, LvlDims d, const LvlBox* boxes, int nbox, cudaStream_t s, int per) {
   AMR_CUDA(cudaMemsetAsync(a, 0, d.size(), s));
   for (int b0 = 0; b0 < nbox; b0 += 65535)
     boxes_kernel<<<dim3(8, std::min(65535, nbox - b0)), 256, 0, s>>>(a, d, boxes + b0, std::min(65535, nbox - b0), 0);
-  borders(a, d, true, s);
+  borders(a, d, true, s, per);
   AMR_CUDA(cudaGetLastError());
 }
 
-void launch_domshrink(const int8_t* in, int8_t* out, LvlDims d, cudaStream_t s) {
+void launch_domshrink(const int8_t* in, int8_t* out, LvlDims d, cudaStream_t s, int per) {
   shrink_kernel<<<blocks_for(d.size(), 256), 256, 0, s>>>(in, out, d);
-  borders(out, d, false, s);
+  borders(out, d, false, s, per, true);
   AMR_CUDA(cudaGetLastError());
 }
 
-void launch_domup(const int8_t* crse, LvlDims cd, int8_t* fine, LvlDims fd, int rx, int ry, int rz, cudaStream_t s) {
+void launch_domup(const int8_t* crse, LvlDims cd, int8_t* fine, LvlDims fd, int rx, int ry, int rz, cudaStream_t s, int per) {
   up_kernel<<<blocks_for(fd.size(), 256), 256, 0, s>>>(crse, cd, fine, fd, rx, ry, rz);
-  borders(fine, fd, true, s);
+  borders(fine, fd, true, s, per);
+  AMR_CUDA(cudaGetLastError());
+}
+
+void launch_domcopy_borders(int8_t* a, LvlDims d, cudaStream_t s, int per) {
+  borders(a, d, false, s, per);
   AMR_CUDA(cudaGetLastError());
 }
 

@@ -17,12 +17,17 @@ struct LvlDims {
 // One box (array coordinates, inclusive) of domprep.f (value 1) or projec.f (3 where 0).
 struct LvlBox { int i0, i1, j0, j1, k0, k1; };
 
+// per: periodic directions (bit 0 x, bit 1 y, bit 2 z). The border ring of a periodic
+// direction is the periodic image of the far interior layer, over the whole ring face.
 // domprep.f:4-169: zero, the boxes set to 1, then the border ring.
-void launch_domprep(int8_t* a, LvlDims d, const LvlBox* boxes, int nbox, cudaStream_t s);
-// domshrink.f:4-93: 27-cell erosion of `in` into a fresh `out`, then extend_borders.
-void launch_domshrink(const int8_t* in, int8_t* out, LvlDims d, cudaStream_t s);
+void launch_domprep(int8_t* a, LvlDims d, const LvlBox* boxes, int nbox, cudaStream_t s, int per = 0);
+// domshrink.f:4-93: 27-cell erosion of `in` into a fresh `out` (zero ring), then
+// extend_borders in the non-periodic directions (the periodic ones keep the zero ring).
+void launch_domshrink(const int8_t* in, int8_t* out, LvlDims d, cudaStream_t s, int per = 0);
 // domup.f:4-185: a fresh fine array from the coarse one, then the border ring.
-void launch_domup(const int8_t* crse, LvlDims cd, int8_t* fine, LvlDims fd, int rx, int ry, int rz, cudaStream_t s);
+void launch_domup(const int8_t* crse, LvlDims cd, int8_t* fine, LvlDims fd, int rx, int ry, int rz, cudaStream_t s, int per = 0);
+// domcopy.f:4-82: the border ring of the copied array (extend_borders, all directions).
+void launch_domcopy_borders(int8_t* a, LvlDims d, cudaStream_t s, int per);
 // spest.f: the interior of `f` set to 0 (the ring keeps its values).
 void launch_zero_interior(int8_t* f, LvlDims d, cudaStream_t s);
 // spest.f + flag2refine.f + setflags.f: BADPT (2) or GOODPT (0) into the level array for

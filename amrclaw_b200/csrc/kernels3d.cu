@@ -168,6 +168,130 @@ static_assert(amrgpu_plugin::Check3D<Euler3Phys<double>, Step3Params, double>::v
 static_assert(amrgpu_plugin::Check3D<Swirl3Phys<double>, Step3Params, double>::value, "vc_advection: rpn3/rpt3/rptt3 contract");
 static_assert(amrgpu_plugin::Check3D<Euler3Phys<float>, Step3Params, float>::value, "euler_roe_efix (FP32): contract");
 
+// The transverse and doubly transverse terms of one side of interface e (flux3.f:429-507
+// for gadd, 552-630 for hadd): imp 2 splits apdq into the terms of cell e, imp 1 splits
+// amdq into the terms of cell e-1. g points at the cell's column of the shared terms
+// (row x at g[x * SW_T]): gadd (side, offset d) in rows ((side-1)*3 + d+1)*NV + m, hadd in
+// rows (6 + (side-1)*3 + d+1)*NV + m. imp 2 starts every term from zero, imp 1 adds to what
+// imp 2 left. Each term gets its summands in flux3.f's statement order: the transverse
+// split, the doubly transverse parts, then the second-order part (m3 = 2). The splits are
+// made in an order that keeps few of them live at once: the z-like ones first (their
+// doubly transverse parts feed gadd), then the y-like ones; the hadd terms wait in shared
+// memory between their first summand and the rest.
+template <int DIR, class T, class PH>
+__device__ __forceinline__ void trans_side(const PH& ph, int imp, const T* F, const T* CQ, int m3, int m4, T dtdx, T dtdy,
+                                           T dtdz, T* g) {
+  constexpr int NV = PH::NV;
+  auto G = [&](int x) -> T& { return g[x * SW_T]; };
+  const T c6 = (T)(1.0 / 6.0);
+  const T sgn3 = imp == 2 ? T(-3) : T(3);
+  const bool first = imp == 2;
+  // z-like split of the fluctuation and of the second-order part
+  T cm[NV], cp[NV], cmq[NV], cpq[NV];
+  ph.template rpt<DIR>(imp, 3, F, cm, cp);
+  if (m3 == 2) ph.template rpt<DIR>(imp, 3, CQ, cmq, cpq);
+  else {
+#pragma unroll
+    for (int m = 0; m < NV; ++m) cmq[m] = cpq[m] = T(0);
+  }
+  // hadd: the first summand of the (0, 1, 1) and (1, 1, 1) terms
+#pragma unroll
+  for (int m = 0; m < NV; ++m) {
+    const T b01 = first ? T(0) : G(7 * NV + m), b11 = first ? T(0) : G(10 * NV + m);
+    G(7 * NV + m) = b01 - T(0.5) * dtdx * cm[m];
+    G(10 * NV + m) = b11 - T(0.5) * dtdx * cp[m];
+  }
+  // gadd: the y-like split, the doubly transverse parts of the z-like split, the second order
+  {
+    T P1[NV], P2[NV], M1[NV], M2[NV];
+    if (m4 > 0) {
+      T t[NV];
+      dt_input<NV>(m4, sgn3, cp, cpq, t);
+      ph.template rptt<DIR>(imp, 2, 2, t, P1, P2);
+      dt_input<NV>(m4, sgn3, cm, cmq, t);
+      ph.template rptt<DIR>(imp, 2, 1, t, M1, M2);
+    }
+    T bm[NV], bp[NV];
+    ph.template rpt<DIR>(imp, 2, F, bm, bp);
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      T g01 = (first ? T(0) : G(1 * NV + m)) - T(0.5) * dtdx * bm[m];
+      T g11 = (first ? T(0) : G(4 * NV + m)) - T(0.5) * dtdx * bp[m];
+      if (m4 > 0) {
+        T g00 = first ? T(0) : G(0 * NV + m), g02 = first ? T(0) : G(2 * NV + m);
+        T g10 = first ? T(0) : G(3 * NV + m), g12 = first ? T(0) : G(5 * NV + m);
+        g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
+        g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
+        g12 = g12 - c6 * dtdx * dtdz * P2[m];
+        g02 = g02 - c6 * dtdx * dtdz * P1[m];
+        g10 = g10 + c6 * dtdx * dtdz * M2[m];
+        g00 = g00 + c6 * dtdx * dtdz * M1[m];
+        G(0 * NV + m) = g00;
+        G(2 * NV + m) = g02;
+        G(3 * NV + m) = g10;
+        G(5 * NV + m) = g12;
+      } else if (first) {
+        G(0 * NV + m) = T(0);
+        G(2 * NV + m) = T(0);
+        G(3 * NV + m) = T(0);
+        G(5 * NV + m) = T(0);
+      }
+      G(1 * NV + m) = g01;
+      G(4 * NV + m) = g11;
+    }
+    T bmq[NV], bpq[NV];
+    if (m3 == 2) {
+      ph.template rpt<DIR>(imp, 2, CQ, bmq, bpq);
+#pragma unroll
+      for (int m = 0; m < NV; ++m) {
+        G(4 * NV + m) = first ? G(4 * NV + m) + dtdx * bpq[m] : G(4 * NV + m) - dtdx * bpq[m];
+        G(1 * NV + m) = first ? G(1 * NV + m) + dtdx * bmq[m] : G(1 * NV + m) - dtdx * bmq[m];
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) bmq[m] = bpq[m] = T(0);
+    }
+    // hadd: the doubly transverse parts of the y-like split, then the second order
+    T X1[NV], X2[NV], Y1[NV], Y2[NV];
+    if (m4 > 0) {
+      T t[NV];
+      dt_input<NV>(m4, sgn3, bp, bpq, t);
+      ph.template rptt<DIR>(imp, 3, 2, t, X1, X2);
+      dt_input<NV>(m4, sgn3, bm, bmq, t);
+      ph.template rptt<DIR>(imp, 3, 1, t, Y1, Y2);
+    }
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      T h01 = G(7 * NV + m), h11 = G(10 * NV + m);
+      if (m4 > 0) {
+        T h00 = first ? T(0) : G(6 * NV + m), h02 = first ? T(0) : G(8 * NV + m);
+        T h10 = first ? T(0) : G(9 * NV + m), h12 = first ? T(0) : G(11 * NV + m);
+        h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
+        h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
+        h12 = h12 - c6 * dtdx * dtdy * X2[m];
+        h02 = h02 - c6 * dtdx * dtdy * X1[m];
+        h10 = h10 + c6 * dtdx * dtdy * Y2[m];
+        h00 = h00 + c6 * dtdx * dtdy * Y1[m];
+        G(6 * NV + m) = h00;
+        G(8 * NV + m) = h02;
+        G(9 * NV + m) = h10;
+        G(11 * NV + m) = h12;
+      } else if (first) {
+        G(6 * NV + m) = T(0);
+        G(8 * NV + m) = T(0);
+        G(9 * NV + m) = T(0);
+        G(11 * NV + m) = T(0);
+      }
+      if (m3 == 2) {
+        h11 = first ? h11 + dtdx * cpq[m] : h11 - dtdx * cpq[m];
+        h01 = first ? h01 + dtdx * cmq[m] : h01 - dtdx * cmq[m];
+      }
+      G(7 * NV + m) = h01;
+      G(10 * NV + m) = h11;
+    }
+  }
+}
+
 // one tile of sweep direction DIR. sW: the block's shared buffer, first the waves
 // [NW*NV][SW_T], then (after they are read) the transverse terms [12*NV][SW_T] of the
 // tile's cells: the apdq side writes them, the amdq side of the next interface adds to
@@ -235,12 +359,12 @@ __device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, 
   T* st = static_cast<T*>(A.stash) + slot;
   const long long ss = A.stash_stride;
   const T c6 = (T)(1.0 / 6.0);
-  const int m3 = sp.m3, m4 = sp.m4;
+  const int m3 = sp.m3, m4 = sp.m4, order = sp.order;
   if (live) {
     // Courant number of interface e (flux3.f:237-246)
 #pragma unroll
     for (int k = 0; k < NW; ++k) cfl = dmax(cfl, dmax(dtdx * S[k], -dtdx * S[k]));
-    if (sp.order != 1) {
+    if (order != 1) {
       // limiter.f: r from the unlimited neighbour waves, upwind side by the speed's sign
       const T dtdxave = T(0.5) * (dtdx + dtdx);
 #pragma unroll
@@ -272,7 +396,7 @@ __device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, 
 #pragma unroll
       for (int m = 0; m < NV; ++m) {
         T fm = T(0) + AM[m], fp = T(0) - AP[m];
-        if (sp.order != 1) { fm = fm + CQ[m]; fp = fp + CQ[m]; }
+        if (order != 1) { fm = fm + CQ[m]; fp = fp + CQ[m]; }
         st[(long long)m * ss] = fm;
         st[(long long)(NV + m) * ss] = fp;
       }
@@ -281,157 +405,11 @@ __device__ __forceinline__ void sweep3_tile(const Step3Args& A, long long tile, 
     }
   }
   __syncthreads();  // the waves in sW are read: the buffer takes the transverse terms now
-  if (owned && e <= n1 && m3 > 0) {
-    // apdq side of interface e: the terms of cell e (flux3.f:429-505, 552-628 with i = e)
-    T bm[NV], bp[NV], cm[NV], cp[NV], bmq[NV], bpq[NV], cmq[NV], cpq[NV];
-    ph.template rpt<DIR>(2, 2, AP, bm, bp);
-    ph.template rpt<DIR>(2, 3, AP, cm, cp);
-    if (m3 == 2) { ph.template rpt<DIR>(2, 2, CQ, bmq, bpq); ph.template rpt<DIR>(2, 3, CQ, cmq, cpq); }
-    else {
-#pragma unroll
-      for (int m = 0; m < NV; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
-    }
-    // gadd (side, offset d): row ((side-1)*3 + d+1)*NV + m of the shared terms
-    {
-      T P1[NV], P2[NV], M1[NV], M2[NV];
-      if (m4 > 0) {
-        T t[NV];
-        dt_input<NV>(m4, T(-3), cp, cpq, t);
-        ph.template rptt<DIR>(2, 2, 2, t, P1, P2);
-        dt_input<NV>(m4, T(-3), cm, cmq, t);
-        ph.template rptt<DIR>(2, 2, 1, t, M1, M2);
-      }
-#pragma unroll
-      for (int m = 0; m < NV; ++m) {
-        T g01 = T(0) - T(0.5) * dtdx * bm[m], g11 = T(0) - T(0.5) * dtdx * bp[m];
-        T g00 = T(0), g02 = T(0), g10 = T(0), g12 = T(0);
-        if (m4 > 0) {
-          g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
-          g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
-          g12 = g12 - c6 * dtdx * dtdz * P2[m];
-          g02 = g02 - c6 * dtdx * dtdz * P1[m];
-          g10 = g10 + c6 * dtdx * dtdz * M2[m];
-          g00 = g00 + c6 * dtdx * dtdz * M1[m];
-        }
-        if (m3 == 2) { g11 = g11 + dtdx * bpq[m]; g01 = g01 + dtdx * bmq[m]; }
-        G(0 * NV + m, l) = g00;
-        G(1 * NV + m, l) = g01;
-        G(2 * NV + m, l) = g02;
-        G(3 * NV + m, l) = g10;
-        G(4 * NV + m, l) = g11;
-        G(5 * NV + m, l) = g12;
-      }
-    }
-    // hadd: row (6 + (side-1)*3 + d+1)*NV + m
-    {
-      T X1[NV], X2[NV], Y1[NV], Y2[NV];
-      if (m4 > 0) {
-        T t[NV];
-        dt_input<NV>(m4, T(-3), bp, bpq, t);
-        ph.template rptt<DIR>(2, 3, 2, t, X1, X2);
-        dt_input<NV>(m4, T(-3), bm, bmq, t);
-        ph.template rptt<DIR>(2, 3, 1, t, Y1, Y2);
-      }
-#pragma unroll
-      for (int m = 0; m < NV; ++m) {
-        T h01 = T(0) - T(0.5) * dtdx * cm[m], h11 = T(0) - T(0.5) * dtdx * cp[m];
-        T h00 = T(0), h02 = T(0), h10 = T(0), h12 = T(0);
-        if (m4 > 0) {
-          h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
-          h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
-          h12 = h12 - c6 * dtdx * dtdy * X2[m];
-          h02 = h02 - c6 * dtdx * dtdy * X1[m];
-          h10 = h10 + c6 * dtdx * dtdy * Y2[m];
-          h00 = h00 + c6 * dtdx * dtdy * Y1[m];
-        }
-        if (m3 == 2) { h11 = h11 + dtdx * cpq[m]; h01 = h01 + dtdx * cmq[m]; }
-        G(6 * NV + m, l) = h00;
-        G(7 * NV + m, l) = h01;
-        G(8 * NV + m, l) = h02;
-        G(9 * NV + m, l) = h10;
-        G(10 * NV + m, l) = h11;
-        G(11 * NV + m, l) = h12;
-      }
-    }
-  }
+  // apdq side of interface e: the terms of cell e (flux3.f:429-505, 552-628 with i = e)
+  if (owned && e <= n1 && m3 > 0) trans_side<DIR, T, PH>(ph, 2, AP, CQ, m3, m4, dtdx, dtdy, dtdz, sG + l);
   __syncthreads();
   // amdq side of interface e: the terms of cell e-1, owned by thread l-1 of this tile
-  if (live && m3 > 0 && e >= 2 && l >= 2) {
-    T bm[NV], bp[NV], cm[NV], cp[NV], bmq[NV], bpq[NV], cmq[NV], cpq[NV];
-    ph.template rpt<DIR>(1, 2, AM, bm, bp);
-    ph.template rpt<DIR>(1, 3, AM, cm, cp);
-    if (m3 == 2) { ph.template rpt<DIR>(1, 2, CQ, bmq, bpq); ph.template rpt<DIR>(1, 3, CQ, cmq, cpq); }
-    else {
-#pragma unroll
-      for (int m = 0; m < NV; ++m) bmq[m] = bpq[m] = cmq[m] = cpq[m] = T(0);
-    }
-    {
-      T P1[NV], P2[NV], M1[NV], M2[NV];
-      if (m4 > 0) {
-        T t[NV];
-        dt_input<NV>(m4, T(3), cp, cpq, t);
-        ph.template rptt<DIR>(1, 2, 2, t, P1, P2);
-        dt_input<NV>(m4, T(3), cm, cmq, t);
-        ph.template rptt<DIR>(1, 2, 1, t, M1, M2);
-      }
-#pragma unroll
-      for (int m = 0; m < NV; ++m) {
-        T g01 = G(1 * NV + m, l - 1), g11 = G(4 * NV + m, l - 1);
-        g01 = g01 - T(0.5) * dtdx * bm[m];
-        g11 = g11 - T(0.5) * dtdx * bp[m];
-        if (m4 > 0) {
-          T g00 = G(0 * NV + m, l - 1), g02 = G(2 * NV + m, l - 1);
-          T g10 = G(3 * NV + m, l - 1), g12 = G(5 * NV + m, l - 1);
-          g11 = g11 + c6 * dtdx * dtdz * (P2[m] - M2[m]);
-          g01 = g01 + c6 * dtdx * dtdz * (P1[m] - M1[m]);
-          g12 = g12 - c6 * dtdx * dtdz * P2[m];
-          g02 = g02 - c6 * dtdx * dtdz * P1[m];
-          g10 = g10 + c6 * dtdx * dtdz * M2[m];
-          g00 = g00 + c6 * dtdx * dtdz * M1[m];
-          G(0 * NV + m, l - 1) = g00;
-          G(2 * NV + m, l - 1) = g02;
-          G(3 * NV + m, l - 1) = g10;
-          G(5 * NV + m, l - 1) = g12;
-        }
-        if (m3 == 2) { g11 = g11 - dtdx * bpq[m]; g01 = g01 - dtdx * bmq[m]; }
-        G(1 * NV + m, l - 1) = g01;
-        G(4 * NV + m, l - 1) = g11;
-      }
-    }
-    {
-      T X1[NV], X2[NV], Y1[NV], Y2[NV];
-      if (m4 > 0) {
-        T t[NV];
-        dt_input<NV>(m4, T(3), bp, bpq, t);
-        ph.template rptt<DIR>(1, 3, 2, t, X1, X2);
-        dt_input<NV>(m4, T(3), bm, bmq, t);
-        ph.template rptt<DIR>(1, 3, 1, t, Y1, Y2);
-      }
-#pragma unroll
-      for (int m = 0; m < NV; ++m) {
-        T h01 = G(7 * NV + m, l - 1), h11 = G(10 * NV + m, l - 1);
-        h01 = h01 - T(0.5) * dtdx * cm[m];
-        h11 = h11 - T(0.5) * dtdx * cp[m];
-        if (m4 > 0) {
-          T h00 = G(6 * NV + m, l - 1), h02 = G(8 * NV + m, l - 1);
-          T h10 = G(9 * NV + m, l - 1), h12 = G(11 * NV + m, l - 1);
-          h11 = h11 + c6 * dtdx * dtdy * (X2[m] - Y2[m]);
-          h01 = h01 + c6 * dtdx * dtdy * (X1[m] - Y1[m]);
-          h12 = h12 - c6 * dtdx * dtdy * X2[m];
-          h02 = h02 - c6 * dtdx * dtdy * X1[m];
-          h10 = h10 + c6 * dtdx * dtdy * Y2[m];
-          h00 = h00 + c6 * dtdx * dtdy * Y1[m];
-          G(6 * NV + m, l - 1) = h00;
-          G(8 * NV + m, l - 1) = h02;
-          G(9 * NV + m, l - 1) = h10;
-          G(11 * NV + m, l - 1) = h12;
-        }
-        if (m3 == 2) { h11 = h11 - dtdx * cpq[m]; h01 = h01 - dtdx * cmq[m]; }
-        G(7 * NV + m, l - 1) = h01;
-        G(10 * NV + m, l - 1) = h11;
-      }
-    }
-  }
+  if (live && m3 > 0 && e >= 2 && l >= 2) trans_side<DIR, T, PH>(ph, 1, AM, CQ, m3, m4, dtdx, dtdy, dtdz, sG + (l - 1));
   __syncthreads();
   // the cell's transverse terms to the stash
   if (owned && e <= n1 && m3 > 0)
@@ -1064,6 +1042,11 @@ __global__ void fill3_kernel(Fill3Args a) {
   const Rect3& R = a.rects[o.src];
   const T* vc = pool + R.off;
   const long long cp = (long long)R.ni * R.nj * R.nk;
+  if (o.kind == F3_PIECE) {
+    const long long sk = ((long long)(o.sk0 + kc) * R.nj + (o.sj0 + jb)) * R.ni + (o.si0 + ia);
+    for (int m = 0; m < nvar; ++m) dst[m * plane + dk] = vc[m * cp + sk];
+    return;
+  }
   auto VC = [&](int m, int i, int j, int k) { return (double)vc[m * cp + ((long long)(k - 1) * R.nj + (j - 1)) * R.ni + (i - 1)]; };
   const int lev = o.level;
   const int rx = a.lc.intratx[lev - 1], ry = a.lc.intraty[lev - 1], rz = a.lc.intratz[lev - 1];
@@ -1327,20 +1310,55 @@ int grid_for(long long n, int block) {
 }  // namespace
 
 template <class T, class PH>
+static void set_sweep_smem() {
+  static const bool done = [] {
+    constexpr int smem = sweep3_smem_bytes<T, PH>();
+    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<1, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<2, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<3, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return true;
+  }();
+  (void)done;
+}
+// the three sweep directions of a level, one launch each: x on s, y and z on the side
+// streams (if given) joined back before the face gather
+template <class T, class PH>
+static int launch_sweeps(const Step3Args& a, const long long items[3], cudaStream_t s, const SweepStreams* ss) {
+  auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
+  constexpr int smem = sweep3_smem_bytes<T, PH>();
+  set_sweep_smem<T, PH>();
+  int n = 0;
+  cudaStream_t sy = s, sz = s;
+  if (ss) {
+    AMR_CUDA(cudaEventRecord(ss->fork, s));
+    AMR_CUDA(cudaStreamWaitEvent(ss->side[0], ss->fork, 0));
+    AMR_CUDA(cudaStreamWaitEvent(ss->side[1], ss->fork, 0));
+    sy = ss->side[0]; sz = ss->side[1];
+  }
+  if (items[0] > 0) { sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, smem, s>>>(a); ++n; }
+  if (items[1] > 0) { sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, smem, sy>>>(a); ++n; }
+  if (items[2] > 0) { sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, smem, sz>>>(a); ++n; }
+  if (ss) {
+    AMR_CUDA(cudaEventRecord(ss->join[0], ss->side[0]));
+    AMR_CUDA(cudaEventRecord(ss->join[1], ss->side[1]));
+    AMR_CUDA(cudaStreamWaitEvent(s, ss->join[0], 0));
+    AMR_CUDA(cudaStreamWaitEvent(s, ss->join[1], 0));
+  }
+  return n;
+}
+
+template <class T, class PH>
 static int launch_step3_t(const Step3Args& a, const long long items[3], long long faces, long long cells, cudaStream_t s,
                           const SweepStreams* ss) {
   auto tiles = [](long long n) { return (unsigned)((n + SW_OWN - 1) / SW_OWN); };
   constexpr int smem = sweep3_smem_bytes<T, PH>();
-  static const bool smem_set = [] {
-    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<1, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<2, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    AMR_CUDA(cudaFuncSetAttribute(sweep3_kernel<3, T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    AMR_CUDA(cudaFuncSetAttribute(sweep3_queue_kernel<T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    return true;
-  }();
-  (void)smem_set;
   int n = 0;
   if (a.queue) {
+    static const bool smem_set = [] {
+      AMR_CUDA(cudaFuncSetAttribute(sweep3_queue_kernel<T, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      return true;
+    }();
+    (void)smem_set;
     const unsigned nx = tiles(items[0]), nxy = nx + tiles(items[1]), ntot = nxy + tiles(items[2]);
     if (ntot > 0) {
       // as many blocks as are resident at once (the queue hands out the tiles)
@@ -1355,22 +1373,8 @@ static int launch_step3_t(const Step3Args& a, const long long items[3], long lon
       sweep3_queue_kernel<T, PH><<<std::min<unsigned>(ntot, (unsigned)resident), SW_T, smem, s>>>(a, nx, nxy, ntot);
       ++n;
     }
-  } else if (ss) {
-    // x on the solve's stream, y and z on the side streams, joined before the face gather
-    AMR_CUDA(cudaEventRecord(ss->fork, s));
-    AMR_CUDA(cudaStreamWaitEvent(ss->side[0], ss->fork, 0));
-    AMR_CUDA(cudaStreamWaitEvent(ss->side[1], ss->fork, 0));
-    if (items[0] > 0) { sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, smem, s>>>(a); ++n; }
-    if (items[1] > 0) { sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, smem, ss->side[0]>>>(a); ++n; }
-    if (items[2] > 0) { sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, smem, ss->side[1]>>>(a); ++n; }
-    AMR_CUDA(cudaEventRecord(ss->join[0], ss->side[0]));
-    AMR_CUDA(cudaEventRecord(ss->join[1], ss->side[1]));
-    AMR_CUDA(cudaStreamWaitEvent(s, ss->join[0], 0));
-    AMR_CUDA(cudaStreamWaitEvent(s, ss->join[1], 0));
   } else {
-    if (items[0] > 0) { sweep3_kernel<1, T, PH><<<tiles(items[0]), SW_T, smem, s>>>(a); ++n; }
-    if (items[1] > 0) { sweep3_kernel<2, T, PH><<<tiles(items[1]), SW_T, smem, s>>>(a); ++n; }
-    if (items[2] > 0) { sweep3_kernel<3, T, PH><<<tiles(items[2]), SW_T, smem, s>>>(a); ++n; }
+    n += launch_sweeps<T, PH>(a, items, s, ss);
   }
   AMR_CUDA(cudaGetLastError());
   if (faces > 0) { face3_kernel<T, PH::NV><<<grid_for(faces, 128), 128, 0, s>>>(a); ++n; }

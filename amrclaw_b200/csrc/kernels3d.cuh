@@ -58,7 +58,9 @@ struct Fad3 { int patch; int pidx; int side; int a0, b0; int na, nb; int seg; };
 struct Qad3Job { int patch; int side; int slab; int row0; int nreg; int reg0; int ratio_a, ratio_b; };
 
 // ghost fill (filpatch.f / intfil.f / filval.f / cstore.f as programs)
-enum Fill3Kind { F3_COPY = 0, F3_INTERP = 1, F3_FILVAL = 2, F3_RING = 3 };
+// F3_PIECE: a scratch rect's cells (src, from si0, sj0, sk0) copied into place: the pieces
+// prefilp.f fills at periodically shifted indices
+enum Fill3Kind { F3_COPY = 0, F3_INTERP = 1, F3_FILVAL = 2, F3_RING = 3, F3_PIECE = 4 };
 struct Rect3 { long long off; int ni, nj, nk; };
 struct Fill3Op {
   int kind;
@@ -66,7 +68,7 @@ struct Fill3Op {
   int di0, dj0, dk0;     // origin (0-based) in the destination array
   int ni, nj, nk;        // extent
   int src;               // COPY: patch; INTERP/FILVAL/RING: rect
-  int si0, sj0, sk0;     // COPY: origin in the source enlarged array; INTERP/FILVAL: global fine index of the origin
+  int si0, sj0, sk0;     // COPY/PIECE: origin in the source array; INTERP/FILVAL: global fine index of the origin
   int level;             // COPY: source level for time modes (-1: current); INTERP/FILVAL: fine level
   int cilo, cjlo, cklo;  // global coarse index of the rect origin
 };

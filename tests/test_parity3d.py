@@ -119,3 +119,38 @@ def test_sweep_schedules_are_identical(schedule):
     rd = _with_gauges(configs.euler_blast(n=16, levels=3, tfinal=0.1, max1d=16))
     ref, gpu = _both(rd, schedule=schedule)
     _assert_identical(ref, gpu)
+
+
+def _periodic_blast(n, levels, tfinal, max1d, bc, centre=(0.8, -0.85, 0.9)):
+    """The blast centred near a corner, so that it crosses the periodic faces early."""
+    rd = configs.euler_blast(n=n, levels=levels, tfinal=tfinal, max1d=max1d)
+    for k, name in enumerate(("x0", "y0", "z0")):
+        rd.probdata.add_param(name, centre[k])
+    rd.clawdata.bc_lower = list(bc)
+    rd.clawdata.bc_upper = list(bc)
+    return rd
+
+
+@pytest.mark.parametrize("bc", [("periodic", "periodic", "periodic"), ("periodic", "wall", "extrap"),
+                                ("extrap", "periodic", "periodic")])
+def test_blast_periodic_boundaries(bc):
+    """Periodic faces (prefilp.f pieces in bound and filpatch, preicall.f in saveqc and
+    filval, prepc.f register images, periodic domain-flag rings), alone and mixed with wall
+    and extrapolation faces, on three levels with regrids."""
+    rd = _with_gauges(_periodic_blast(n=12, levels=3, tfinal=0.15, max1d=16, bc=bc))
+    ref, gpu = _both(rd)
+    lev2 = ref["grids"][ref["grids"][:, 1] == 2]
+    per = [k for k in range(3) if bc[k] == "periodic"]
+    # refined grids touch both faces of a periodic direction: the blast wrapped around
+    assert any((lev2[:, 2 + 2 * k] == 0).any() and (lev2[:, 3 + 2 * k] == 2 * 12 - 1).any() for k in per)
+    _assert_identical(ref, gpu)
+
+
+def test_blast_periodic_plain_path_and_richardson():
+    """The per-patch path with Richardson estimation on a periodic domain (the big step's
+    wide ghost ring is filled through the periodic pieces too)."""
+    rd = _periodic_blast(n=12, levels=2, tfinal=0.1, max1d=16, bc=("periodic",) * 3)
+    rd.amrdata.flag_richardson = True
+    rd.amrdata.flag_richardson_tol = 2e-3
+    ref, gpu = _both(rd, batched=False)
+    _assert_identical(ref, gpu)
