@@ -39,7 +39,7 @@ class Solver:
 
     def __init__(self, rundata_or_dir, outdir: str | None = None, write_output: bool = False, batched: bool = True,
                  precision: str = "fp64", graphs: bool = False, schedule: int | None = None,
-                 pool_limit: int = 0):
+                 pool_limit: int = 0, step_batching_us: int = 0):
         self._lib = _lib.load()
         if isinstance(rundata_or_dir, ClawRunData):
             self._tmp = tempfile.TemporaryDirectory(prefix="amrgpu_")
@@ -66,6 +66,8 @@ class Solver:
             self.set_graphs(True)
         if pool_limit:
             self.set_pool_limit(pool_limit)
+        if step_batching_us:
+            self.set_step_batching(step_batching_us)
 
     def set_batched(self, batched: bool) -> None:
         _check(self._lib, self._lib.amrgpu_set_batched(self._h, int(batched)), "amrgpu_set_batched")
@@ -93,6 +95,12 @@ class Solver:
         """Cap the context's device pools at nbytes (0: no cap); growth past it raises
         AmrError with code 3 (amrgpu_set_pool_limit)."""
         _check(self._lib, self._lib.amrgpu_set_pool_limit(self._h, int(nbytes)), "amrgpu_set_pool_limit")
+
+    def set_step_batching(self, window_us: int) -> None:
+        """Launch this (2D) solve's level steps together with those of other solves of the same
+        plugin and precision running at the same time in this process, waiting at most
+        window_us microseconds for them (amrgpu_set_step_batching); 0 launches them alone."""
+        _check(self._lib, self._lib.amrgpu_set_step_batching(self._h, int(window_us)), "amrgpu_set_step_batching")
 
     def set_profile(self, on: bool) -> None:
         _check(self._lib, self._lib.amrgpu_set_profile(self._h, int(on)), "amrgpu_set_profile")
@@ -134,7 +142,8 @@ class Solver:
                 "last_run_ms", "last_run_cells", "finished", "h2d_bytes",
                 "regrid_flags_s", "regrid_hostflags_s", "regrid_cluster_s", "regrid_fill_s", "regrid_prep_s", "regrid_compile_s",
                 "num_dim", "precision_bits", "graph_captures", "graph_replays", "levels_tuned_queue",
-                "levels_tuned_per_direction", "pool_bytes"]
+                "levels_tuned_per_direction", "pool_bytes", "step_batch_submits", "step_batch_shared",
+                "step_batch_members"]
         out = (ctypes.c_double * len(keys))()
         _check(self._lib, self._lib.amrgpu_info(self._h, out, len(keys)), "amrgpu_info")
         return dict(zip(keys, list(out)))

@@ -23,6 +23,7 @@ SIGNATURES = {
     "amrgpu_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "amrgpu_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, c_double_p, ctypes.c_int]),
     "amrgpu_set_pool_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "amrgpu_set_step_batching": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "amrgpu_checkpoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "amrgpu_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "amrgpu_level_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p, c_double_p]),

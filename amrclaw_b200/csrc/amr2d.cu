@@ -21,6 +21,7 @@
 #include "gridindex.hpp"
 #include "workpool.hpp"
 #include "noalloc2d.cuh"
+#include "stepbatch.hpp"
 #include "hostutil.hpp"
 #include "valout.hpp"
 #include "solver.hpp"
@@ -200,6 +201,7 @@ class Amr2Gpu {
 
   ~Amr2Gpu() {
     if (st) cudaStreamSynchronize(st);
+    if (batch_window_us > 0) StepBatcher::get().leave(batch_member);
     for (auto& G : lgraph) G.reset();
     if (d_sub) cudaFree(d_sub);
     if (h_sub) cudaFreeHost(h_sub);
@@ -1356,6 +1358,12 @@ class Amr2Gpu {
   };
   LevelGraph lgraph[12];
   bool use_graphs = false;
+  // cross-request batching of the level step (amrgpu_set_step_batching): membership in the
+  // process's step batcher, the window a leader waits for the other members, and counts of
+  // the submissions made and of those that shared their launch with another solve
+  StepBatcher::Member batch_member;
+  int batch_window_us = 0;
+  long long batch_submits = 0, batch_shared = 0, batch_members_seen = 0;
   bool stepped = false;  // a level substep has run (store2 then holds the last step's input)
   long long plan_gen[12] = {0};
   long long graph_captures = 0, graph_replays = 0;
@@ -1388,7 +1396,15 @@ class Amr2Gpu {
     a.dt = dt; a.dt_dev = ds ? &ds->dt : nullptr; a.dx = hxposs[lev]; a.dy = hyposs[lev]; a.cflmax = d_cfl; a.sp = sp;
     if (batched) {
       a.work = L.d_work.d; a.nwork = (int)L.work.size(); a.queue = nullptr;
-      launch_step2(prob.solver, a, (int)L.work.size(), st, f32);
+      if (batch_window_us > 0 && !use_graphs && !sp.split) {
+        // the level step goes out in one launch with the steps other solves submit meanwhile
+        StepBatcher::get().submit(batch_member, a, (int)L.work.size(), st, batch_window_us);
+        ++batch_submits;
+        batch_members_seen += batch_member.batch_size;
+        if (batch_member.batch_size > 1) ++batch_shared;
+      } else {
+        launch_step2(prob.solver, a, (int)L.work.size(), st, f32);
+      }
       ++nkernels;
     } else {
       for (size_t k = 0; k < L.plist.size(); ++k) {
@@ -2997,8 +3013,21 @@ class Solver2 : public AmrSolver {
     if (s != 0) throw std::runtime_error("amrgpu_set_schedule: sweep schedules are built for the 3D path");
   }
   void write_checkpoint(const char* path) override { g.checkpoint_file(path); }
-  void set_solver(const std::string& name, const std::vector<double>& v) override { g.set_solver(name, v); }
+  void set_solver(const std::string& name, const std::vector<double>& v) override {
+    g.set_solver(name, v);
+    if (g.batch_window_us > 0) {  // the plugin picks the batch this solve's steps join
+      StepBatcher::get().leave(g.batch_member);
+      StepBatcher::get().join(g.batch_member, StepBatcher::make_key(g.prob.solver, g.f32));
+    }
+  }
   void set_pool_limit(long long bytes) override { set_arena_limits(g.pool, g.regs, bytes); }
+  void set_step_batching(int window_us) override {
+    if (window_us < 0) throw std::invalid_argument("amrgpu_set_step_batching: negative window");
+    if ((window_us > 0) == (g.batch_window_us > 0)) { g.batch_window_us = window_us; return; }
+    if (window_us > 0) StepBatcher::get().join(g.batch_member, StepBatcher::make_key(g.prob.solver, g.f32));
+    else StepBatcher::get().leave(g.batch_member);
+    g.batch_window_us = window_us;
+  }
   void run(int max_cycles) override {
     g.max_cycles = max_cycles;
     g.tick();
@@ -3034,7 +3063,8 @@ class Solver2 : public AmrSolver {
             g.cflmax_run, (double)g.nkernels, (double)g.pool.peak * 8.0, (double)g.nsteps_launched,
             g.step_kernel_ms, g.step_kernel_cells, g.last_run_ms, g.run_cells, g.finished() ? 1.0 : 0.0, g.h2d_bytes,
             g.tr_flags, g.tr_host, g.tr_cluster, g.tr_fill, g.tr_prep, g.tr_compile, 2.0, g.f32 ? 32.0 : 64.0, (double)g.graph_captures, (double)g.graph_replays, 0.0, 0.0,
-            8.0 * (double)(g.pool.cap + g.regs.cap)};
+            8.0 * (double)(g.pool.cap + g.regs.cap), (double)g.batch_submits, (double)g.batch_shared,
+            (double)g.batch_members_seen};
   }
   std::vector<int> grid_rows() override {
     std::vector<int> r;
@@ -3175,6 +3205,20 @@ int amrgpu_set_pool_limit(amrgpu_ctx* ctx, long long bytes) {
   if (!ctx) { g_err = "amrgpu_set_pool_limit: null context"; return AMRGPU_EINVAL; }
   try {
     ctx->s->set_pool_limit(bytes);
+    return AMRGPU_OK;
+  } catch (std::invalid_argument& e) {
+    g_err = e.what();
+    return AMRGPU_EINVAL;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return AMRGPU_ERROR;
+  }
+}
+
+int amrgpu_set_step_batching(amrgpu_ctx* ctx, int window_us) {
+  if (!ctx) { g_err = "amrgpu_set_step_batching: null context"; return AMRGPU_EINVAL; }
+  try {
+    ctx->s->set_step_batching(window_us);
     return AMRGPU_OK;
   } catch (std::invalid_argument& e) {
     g_err = e.what();

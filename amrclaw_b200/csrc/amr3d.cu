@@ -2863,6 +2863,9 @@ class Amr3Gpu : public AmrSolver {
     for (auto& G : lgraph) G.reset();
   }
   void set_pool_limit(long long bytes) override { set_arena_limits(pool, regs, bytes); }
+  void set_step_batching(int window_us) override {
+    if (window_us != 0) throw std::invalid_argument("amrgpu_set_step_batching: cross-request batching is built for the 2D path");
+  }
   void run(int mc) override { max_cycles = mc; tick(); }
   double level_advance(int level, double* cfl) override {
     if (level < 1 || level > lfine) throw std::runtime_error("level out of range");

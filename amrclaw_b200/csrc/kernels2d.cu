@@ -20,6 +20,52 @@ namespace amrb {
 
 __device__ __forceinline__ int floordiv(int a, int b) { int q = a / b; if ((a % b != 0) && ((a < 0) != (b < 0))) --q; return q; }
 
+// ------------------------------------------------------------------ bulk-copy staging
+// The tile rows reach shared memory through the TMA engine's untiled bulk copy
+// (cp.async.bulk global -> shared, completion counted in bytes on an mbarrier). A bulk copy
+// wants 16-byte aligned source and destination and a multiple of 16 bytes: each row is
+// copied from its start rounded down to 16 bytes to its end rounded up, into a staging row
+// of RW elements, and read from the element offset the rounding left. The pool's blocks are
+// 256-byte aligned and sized in whole 256-byte granules, so the widened rows stay inside
+// the row's own block.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// waits for the phase with the given parity, at most about a second of SM clock
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > 2000000000LL) return false;
+  return true;
+}
+// elements of a staging row: the widest row (QW) plus the rounding on both ends
+template <class R, int QW>
+__host__ __device__ constexpr int stage_row() {
+  constexpr int E = 16 / (int)sizeof(R);
+  return (QW + 2 * (E - 1) + E - 1) / E * E;
+}
+
 // ======================================================================= patch step
 template <class S>
 struct Step2Layout {
@@ -312,26 +358,158 @@ __device__ __forceinline__ void cfl_to_level(R cfl, R* red, unsigned long long* 
   }
 }
 
+// The shared-memory layout of a step block.
 template <class S, class R>
-__global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
+struct Step2Smem {
+  using L = Step2Layout<S>;
+  R *Qs, *FM, *FP, *GM, *GP, *TR, *W, *X, *As, *red;
+  __device__ explicit Step2Smem(unsigned char* raw) {
+    Qs = reinterpret_cast<R*>(raw);
+    FM = Qs + L::NQ; FP = FM + L::NF; GM = FP + L::NF; GP = GM + L::NF; TR = GP + L::NF;
+    W = TR + L::NTR; X = W + L::NW; As = X + L::NX; red = As + L::NAQ;
+  }
+};
+
+// One tile of one patch: stepgrid.f / step2.f90 / flux2.f over the tile, its update and its
+// flux-register epilogue, with the Courant number of its faces folded into cfl. s_bar is the
+// block's bulk-copy barrier and phase the parity of its next phase. Returns false (after
+// flagging a.cflmax as infinite) if the tile's bulk copies did not complete in time.
+template <class S, class R>
+__device__ __forceinline__ bool step2_tile(const StepArgs& a, const StepWork& wk, const Step2Smem<S, R>& sm,
+                                           unsigned long long& s_bar, int& s_ok, unsigned& phase, R& cfl) {
   using L = Step2Layout<S>;
   constexpr int ME = L::ME, T = L::T, QW = L::QW;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* Qs = reinterpret_cast<R*>(smem_raw);
-  R* FM = Qs + L::NQ;
-  R* FP = FM + L::NF;
-  R* GM = FP + L::NF;
-  R* GP = GM + L::NF;
-  R* TR = GP + L::NF;
-  R* W = TR + L::NTR;
-  R* X = W + L::NW;
-  R* As = X + L::NX;
-  R* red = As + L::NAQ;
-  __shared__ int s_item;
+  constexpr int SE = 16 / (int)sizeof(R), RW = stage_row<R, QW>();
+  static_assert(ME * QW * RW <= L::NW + L::NX, "bulk-copy staging must fit in W and X");
+  static_assert(((L::NQ + 4 * L::NF + L::NTR) * sizeof(R)) % 16 == 0 && (RW * sizeof(R)) % 16 == 0,
+                "staging rows must be 16-byte aligned");
+  R *Qs = sm.Qs, *FM = sm.FM, *FP = sm.FP, *GM = sm.GM, *GP = sm.GP, *TR = sm.TR, *W = sm.W, *X = sm.X, *As = sm.As;
+  (void)X;
   const int tid = threadIdx.x;
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;
   const R dtdx = (R)(dt / a.dx), dtdy = (R)(dt / a.dy);
   const bool capa = L::NA > 0 && a.sp.mcapa > 0;
+  const PatchDev P = a.patches[wk.patch];
+  const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
+  const int mitot = P.mitot, mjtot = P.mjtot;
+  const int i0 = wk.ti0, j0 = wk.tj0;
+  const int tw = min(T, mx - i0 + 1), th = min(T, my - j0 + 1);
+  R* qout = static_cast<R*>(a.pool) + P.q[1 - P.cur];
+  const long long plane = (long long)mitot * mjtot;
+  // load the tile with its two ghost layers: interior (i,j) -> enlarged 0-based (i+1, j+1).
+  // Each row (m, b) of lw values starts at pool element rowg(m, b); thread r < ME*lh
+  // announces its row's bytes on the barrier and issues the bulk copy into staging row r
+  // (W and X, free between tiles); thread 0 arrives once every row is announced.
+  const int lw = tw + 4, lh = th + 4;
+  const long long q0 = P.q[P.cur] + (long long)(j0 - 1) * mitot + (i0 - 1);
+  auto rowg = [&](int m, int b) { return q0 + m * plane + (long long)b * mitot; };
+  if (tid < ME * lh) {
+    const int m = tid / lh, b = tid % lh;
+    const long long g = rowg(m, b), g0 = g & ~(long long)(SE - 1), g1 = (g + lw + SE - 1) & ~(long long)(SE - 1);
+    const unsigned bytes = (unsigned)((g1 - g0) * (long long)sizeof(R));
+    mbar_expect_tx(&s_bar, bytes);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    bulk_g2s(W + tid * RW, static_cast<const R*>(a.pool) + g0, bytes, &s_bar);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive(&s_bar);
+    s_ok = mbar_wait_bounded(&s_bar, phase) ? 1 : 0;
+  }
+  __syncthreads();
+  // every thread observes the completed phase itself (it completed: no wait)
+  if (s_ok && tid != 0) mbar_wait_bounded(&s_bar, phase);
+  phase ^= 1u;
+  if (!s_ok) {
+    // the copies did not complete: flag the level's Courant number as infinite (the host
+    // stops on it) and leave once this block's copies have landed or their wait ran out
+    if (tid == 0) {
+      atomicMax(a.cflmax, 0x7FF0000000000000ull);
+      mbar_wait_bounded(&s_bar, phase ^ 1u);
+    }
+    return false;
+  }
+  for (int it = tid; it < ME * lw * lh; it += STEP2_THREADS) {
+    const int m = it / (lw * lh), rem = it % (lw * lh);
+    const int b = rem / lw, aa = rem % lw;
+    const int off = (int)(rowg(m, b) & (SE - 1));
+    Qs[(m * QW + b) * QW + aa] = W[(m * lh + b) * RW + off + aa];
+  }
+  if (L::NA > 0) {
+    const R* aux = static_cast<const R*>(a.pool) + P.aux;
+    const int na = min(L::NA, a.sp.prob.naux);
+    for (int it = tid; it < na * lw * lh; it += STEP2_THREADS) {
+      const int m = it / (lw * lh), rem = it % (lw * lh);
+      const int b = rem / lw, aa = rem % lw;
+      const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
+      As[(m * QW + b) * QW + aa] = aux[m * plane + (long long)je * mitot + ie];
+    }
+  }
+  __syncthreads();
+  // x-sweeps: FM/FP initialised, per-cell transverse parts in TR
+  step2_sweep<S, 1, R>(a.sp, Qs, As, W, X, TR, FM, FP, i0, j0, tw, th, dtdx, cfl);
+  // GX(c, f) = (0 + part2(row f-1)) + part1(row f) -> GM and GP
+  for (int it = tid; it < ME * (th + 1) * tw; it += STEP2_THREADS) {
+    const int m = it / ((th + 1) * tw), rem = it % ((th + 1) * tw);
+    const int fb = rem / tw, ca = rem % tw;
+    const R up = TR[((fb * T + ca) * 2) * ME + ME + m];        // row f-1 = line index fb
+    const R dn = TR[(((fb + 1) * T + ca) * 2) * ME + m];       // row f   = line index fb+1
+    const R g = (R(0) + up) + dn;
+    GM[(m * (T + 1) + fb) * T + ca] = g;
+    GP[(m * (T + 1) + fb) * T + ca] = g;
+  }
+  __syncthreads();
+  // y-sweeps: GM/GP += faddm/faddp, per-cell transverse parts in TR
+  step2_sweep<S, 2, R>(a.sp, Qs, As, W, X, TR, GM, GP, i0, j0, tw, th, dtdy, cfl);
+  // FM(f, r) = (FM + part2(col f-1)) + part1(col f)
+  for (int it = tid; it < ME * th * (tw + 1); it += STEP2_THREADS) {
+    const int m = it / (th * (tw + 1)), rem = it % (th * (tw + 1));
+    const int rb = rem / (tw + 1), fa = rem % (tw + 1);
+    const R up = TR[((fa * T + rb) * 2) * ME + ME + m];        // column f-1 = line index fa
+    const R dn = TR[(((fa + 1) * T + rb) * 2) * ME + m];       // column f   = line index fa+1
+    const int k = (m * T + rb) * (T + 1) + fa;
+    FM[k] = (FM[k] + up) + dn;
+    FP[k] = (FP[k] + up) + dn;
+  }
+  __syncthreads();
+  // conservative update (stepgrid.f:154-173; with a capacity array the flux difference is
+  // divided by kappa)
+  for (int it = tid; it < ME * th * tw; it += STEP2_THREADS) {
+    const int m = it / (th * tw), rem = it % (th * tw);
+    const int rb = rem / tw, ca = rem % tw;
+    const R q = Qs[(m * QW + rb + 2) * QW + ca + 2];
+    const R fmr = FM[(m * T + rb) * (T + 1) + ca + 1], fpl = FP[(m * T + rb) * (T + 1) + ca];
+    const R gmt = GM[(m * (T + 1) + rb + 1) * T + ca], gpb = GP[(m * (T + 1) + rb) * T + ca];
+    const R qn = capa ? q - (dtdx * (fmr - fpl) + dtdy * (gmt - gpb)) / As[((a.sp.mcapa - 1) * QW + rb + 2) * QW + ca + 2]
+                      : q - dtdx * (fmr - fpl) - dtdy * (gmt - gpb);
+    const int ie = i0 + ca + 1, je = j0 + rb + 1;
+    qout[m * plane + (long long)je * mitot + ie] = qn;
+  }
+  register_epilogue<ME, R>(a, wk, P, i0, j0, tw, th, dt, FM, FP, GM, GP, T);
+  __syncthreads();
+  return true;
+}
+
+// the bulk-copy barrier of a step block: one arrival per phase (thread 0), the rows' bytes
+// as its transactions
+__device__ __forceinline__ void step2_barrier_init(unsigned long long& s_bar) {
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+template <class S, class R>
+__global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Step2Smem<S, R> sm(smem_raw);
+  __shared__ int s_item;
+  __shared__ __align__(8) unsigned long long s_bar;
+  __shared__ int s_ok;
+  step2_barrier_init(s_bar);
+  unsigned phase = 0;
+  const int tid = threadIdx.x;
   R cfl = R(0);
   int iter = 0;
   while (true) {
@@ -346,77 +524,37 @@ __global__ void __launch_bounds__(STEP2_THREADS) step2_kernel(StepArgs a) {
     }
     ++iter;
     if (w >= a.nwork) break;
-    const StepWork wk = a.work[w];
-    const PatchDev P = a.patches[wk.patch];
-    const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1;
-    const int mitot = P.mitot, mjtot = P.mjtot;
-    const int i0 = wk.ti0, j0 = wk.tj0;
-    const int tw = min(T, mx - i0 + 1), th = min(T, my - j0 + 1);
-    const R* qin = static_cast<const R*>(a.pool) + P.q[P.cur];
-    R* qout = static_cast<R*>(a.pool) + P.q[1 - P.cur];
-    const long long plane = (long long)mitot * mjtot;
-    // load the tile with its two ghost layers: interior (i,j) -> enlarged 0-based (i+1, j+1)
-    const int lw = tw + 4, lh = th + 4;
-    for (int it = tid; it < ME * lw * lh; it += STEP2_THREADS) {
-      const int m = it / (lw * lh), rem = it % (lw * lh);
-      const int b = rem / lw, aa = rem % lw;
-      const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
-      Qs[(m * QW + b) * QW + aa] = qin[m * plane + (long long)je * mitot + ie];
-    }
-    if (L::NA > 0) {
-      const R* aux = static_cast<const R*>(a.pool) + P.aux;
-      const int na = min(L::NA, a.sp.prob.naux);
-      for (int it = tid; it < na * lw * lh; it += STEP2_THREADS) {
-        const int m = it / (lw * lh), rem = it % (lw * lh);
-        const int b = rem / lw, aa = rem % lw;
-        const int ie = (i0 - 2 + aa) + 1, je = (j0 - 2 + b) + 1;
-        As[(m * QW + b) * QW + aa] = aux[m * plane + (long long)je * mitot + ie];
-      }
-    }
-    __syncthreads();
-    // x-sweeps: FM/FP initialised, per-cell transverse parts in TR
-    step2_sweep<S, 1, R>(a.sp, Qs, As, W, X, TR, FM, FP, i0, j0, tw, th, dtdx, cfl);
-    // GX(c, f) = (0 + part2(row f-1)) + part1(row f) -> GM and GP
-    for (int it = tid; it < ME * (th + 1) * tw; it += STEP2_THREADS) {
-      const int m = it / ((th + 1) * tw), rem = it % ((th + 1) * tw);
-      const int fb = rem / tw, ca = rem % tw;
-      const R up = TR[((fb * T + ca) * 2) * ME + ME + m];        // row f-1 = line index fb
-      const R dn = TR[(((fb + 1) * T + ca) * 2) * ME + m];       // row f   = line index fb+1
-      const R g = (R(0) + up) + dn;
-      GM[(m * (T + 1) + fb) * T + ca] = g;
-      GP[(m * (T + 1) + fb) * T + ca] = g;
-    }
-    __syncthreads();
-    // y-sweeps: GM/GP += faddm/faddp, per-cell transverse parts in TR
-    step2_sweep<S, 2, R>(a.sp, Qs, As, W, X, TR, GM, GP, i0, j0, tw, th, dtdy, cfl);
-    // FM(f, r) = (FM + part2(col f-1)) + part1(col f)
-    for (int it = tid; it < ME * th * (tw + 1); it += STEP2_THREADS) {
-      const int m = it / (th * (tw + 1)), rem = it % (th * (tw + 1));
-      const int rb = rem / (tw + 1), fa = rem % (tw + 1);
-      const R up = TR[((fa * T + rb) * 2) * ME + ME + m];        // column f-1 = line index fa
-      const R dn = TR[(((fa + 1) * T + rb) * 2) * ME + m];       // column f   = line index fa+1
-      const int k = (m * T + rb) * (T + 1) + fa;
-      FM[k] = (FM[k] + up) + dn;
-      FP[k] = (FP[k] + up) + dn;
-    }
-    __syncthreads();
-    // conservative update (stepgrid.f:154-173; with a capacity array the flux difference is
-    // divided by kappa)
-    for (int it = tid; it < ME * th * tw; it += STEP2_THREADS) {
-      const int m = it / (th * tw), rem = it % (th * tw);
-      const int rb = rem / tw, ca = rem % tw;
-      const R q = Qs[(m * QW + rb + 2) * QW + ca + 2];
-      const R fmr = FM[(m * T + rb) * (T + 1) + ca + 1], fpl = FP[(m * T + rb) * (T + 1) + ca];
-      const R gmt = GM[(m * (T + 1) + rb + 1) * T + ca], gpb = GP[(m * (T + 1) + rb) * T + ca];
-      const R qn = capa ? q - (dtdx * (fmr - fpl) + dtdy * (gmt - gpb)) / As[((a.sp.mcapa - 1) * QW + rb + 2) * QW + ca + 2]
-                        : q - dtdx * (fmr - fpl) - dtdy * (gmt - gpb);
-      const int ie = i0 + ca + 1, je = j0 + rb + 1;
-      qout[m * plane + (long long)je * mitot + ie] = qn;
-    }
-    register_epilogue<ME, R>(a, wk, P, i0, j0, tw, th, dt, FM, FP, GM, GP, T);
-    __syncthreads();
+    if (!step2_tile<S, R>(a, a.work[w], sm, s_bar, s_ok, phase, cfl)) return;
   }
-  cfl_to_level(cfl, red, a.cflmax);
+  cfl_to_level(cfl, sm.red, a.cflmax);
+}
+
+// The level substeps of several solves in one launch (cross-request batching): the tiles of
+// member k are items [work0[k], work0[k+1]) of the combined list, each stepped with member
+// k's arguments exactly as step2_kernel steps it. A block's Courant number goes to a
+// member's level maximum whenever the block moves on to the next member.
+template <class S, class R>
+__global__ void __launch_bounds__(STEP2_THREADS) step2_batch_kernel(const __grid_constant__ StepBatch B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Step2Smem<S, R> sm(smem_raw);
+  __shared__ __align__(8) unsigned long long s_bar;
+  __shared__ int s_ok;
+  step2_barrier_init(s_bar);
+  unsigned phase = 0;
+  R cfl = R(0);
+  int cur = -1;
+  for (int w = blockIdx.x; w < B.work0[B.n]; w += gridDim.x) {
+    int k = 0;
+    while (w >= B.work0[k + 1]) ++k;
+    if (k != cur) {
+      if (cur >= 0) cfl_to_level(cfl, sm.red, B.m[cur].cflmax);
+      cfl = R(0);
+      cur = k;
+    }
+    const StepArgs& a = B.m[k];
+    if (!step2_tile<S, R>(a, a.work[w - B.work0[k]], sm, s_bar, s_ok, phase, cfl)) return;
+  }
+  if (cur >= 0) cfl_to_level(cfl, sm.red, B.m[cur].cflmax);
 }
 
 // ======================================================================= Godunov-split patch step
@@ -635,6 +773,33 @@ static void launch_step2_r(int solver, const StepArgs& a, int grid, cudaStream_t
 void launch_step2(int solver, const StepArgs& a, int grid, cudaStream_t s, bool f32) {
   if (f32) launch_step2_r<float>(solver, a, grid, s);
   else launch_step2_r<double>(solver, a, grid, s);
+}
+
+template <class S, class R>
+static void launch_step2_batch_t(const StepBatch& b, int grid, cudaStream_t s) {
+  const size_t sm = sizeof(R) * Step2Layout<S>::TOTAL;
+  static const bool attr = [&] {
+    AMR_CUDA(cudaFuncSetAttribute(step2_batch_kernel<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    return true;
+  }();
+  (void)attr;
+  if (grid <= 0) return;
+  step2_batch_kernel<S, R><<<grid, STEP2_THREADS, sm, s>>>(b);
+  AMR_CUDA(cudaGetLastError());
+}
+template <class R>
+static void launch_step2_batch_r(int solver, const StepBatch& b, int grid, cudaStream_t s) {
+  switch (solver) {
+    case SOLVER_ADVECTION: launch_step2_batch_t<Advection2, R>(b, grid, s); break;
+    case SOLVER_ACOUSTICS: launch_step2_batch_t<Acoustics2, R>(b, grid, s); break;
+    case SOLVER_EULER: launch_step2_batch_t<Euler2, R>(b, grid, s); break;
+    case SOLVER_VC_ADVECTION: launch_step2_batch_t<VcAdvection2, R>(b, grid, s); break;
+    default: throw std::runtime_error("launch_step2_batch: unsupported solver");
+  }
+}
+void launch_step2_batch(int solver, const StepBatch& b, int grid, cudaStream_t s, bool f32) {
+  if (f32) launch_step2_batch_r<float>(solver, b, grid, s);
+  else launch_step2_batch_r<double>(solver, b, grid, s);
 }
 
 size_t step2_smem_bytes(int solver, bool f32) {

@@ -58,6 +58,19 @@ struct StepArgs {
   StepParams sp;
 };
 
+// The level substeps of up to STEP2_BATCH_MAX solves (of one Riemann plugin and one
+// precision) in one launch: member k's tiles are items [work0[k], work0[k+1]) of the
+// combined work list, stepped with m[k]. Passed to the kernel by value.
+constexpr int STEP2_BATCH_MAX = 16;
+struct StepBatch {
+  int n;
+  int work0[STEP2_BATCH_MAX + 1];
+  StepArgs m[STEP2_BATCH_MAX];
+};
+static_assert(sizeof(StepBatch) < 32000, "a StepBatch must fit in the kernel parameter space");
+// one launch of the batched step over b's members (grid: blocks; 0 launches nothing)
+void launch_step2_batch(int solver, const StepBatch& b, int grid, cudaStream_t s, bool f32);
+
 // ---------------------------------------------------------------- ghost-fill programs
 enum FillKind { FILL_COPY = 0, FILL_INTERP = 1, FILL_PIECE = 2, FILL_FILVAL = 3, FILL_RING = 4, FILL_FIXCAPA = 5 };
 

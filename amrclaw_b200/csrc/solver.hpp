@@ -26,6 +26,10 @@ class AmrSolver {
   // growth past it throws PoolLimitError. 0 removes the cap. The pools already hold
   // pool_bytes(); a cap below that is refused (std::invalid_argument).
   virtual void set_pool_limit(long long bytes) = 0;
+  // hand each batched level step to the process's step batcher, which launches the steps
+  // that solves of the same plugin and precision submit within window_us together (2D);
+  // 0 launches them alone. std::invalid_argument for a negative window or a 3D solve.
+  virtual void set_step_batching(int window_us) = 0;
   virtual void run(int max_cycles) = 0;                    // tick.f
   virtual double level_advance(int level, double* cfl) = 0;  // advanc.f; returns dtnew
   virtual void update_level(int level) = 0;                 // update.f

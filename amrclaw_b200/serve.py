@@ -10,7 +10,7 @@ its reservation stops with AMRGPU_ENOMEM, gives its reservation back and waits a
 first in line, with twice the reservation (at most the whole budget). Latency is
 completion time minus arrival time.
 
-    python -m amrclaw_b200.serve [--requests N] [--rate R] [--budget-gb G] [--slots S] [--scale small|full]
+    python -m amrclaw_b200.serve [--requests N] [--rate R] [--budget-gb G] [--slots S] [--scale small|full] [--batch-us W]
 
 prints one JSON line: p50/p99 latency, aggregate cell-updates/s, makespan, admissions.
 """
@@ -119,23 +119,57 @@ class Result:
         return self.done - self.arrival
 
 
-def run_one(req: Request, keep_values: bool = False):
+def run_one(req: Request, keep_values: bool = False, batch_us: int = 0):
     """One solve from start to tfinal on the current device, in the request's precision, its
-    pools capped at the request's reservation: (cell updates, mass, values, device ms, pool peak)."""
+    pools capped at the request's reservation: (cell updates, mass, values, device ms, pool
+    peak). batch_us > 0: its level steps go out in shared launches with those of the other
+    solves of the same plugin and precision running meanwhile (amrgpu_set_step_batching)."""
     from . import Solver
-    with Solver(req.rundata(), batched=True, precision=req.precision, pool_limit=req.reservation()) as s:
+    with Solver(req.rundata(), batched=True, precision=req.precision, pool_limit=req.reservation(),
+                step_batching_us=batch_us) as s:
         s.run(0)
         inf = s.info()
         vals = s.values() if keep_values else None
+        STEP_BATCH_STATS.add(inf)
         return inf["cell_updates"], s.mass(), vals, inf["last_run_ms"], inf["pool_peak_bytes"]
 
 
+class _BatchStats:
+    """Level steps the solves of this process submitted to the step batcher, how many of
+    them shared their launch with another solve, and the members those launches carried."""
+
+    def __init__(self):
+        self.mu = threading.Lock()
+        self.reset()
+
+    def reset(self):
+        self.submits = self.shared = self.members = 0.0
+
+    def add(self, inf: dict):
+        with self.mu:
+            self.submits += inf.get("step_batch_submits", 0.0)
+            self.shared += inf.get("step_batch_shared", 0.0)
+            self.members += inf.get("step_batch_members", 0.0)
+
+    def summary(self) -> dict:
+        with self.mu:
+            return {"level_steps_submitted": int(self.submits), "level_steps_in_shared_launches": int(self.shared),
+                    "mean_solves_per_launch": self.members / self.submits if self.submits else 0.0}
+
+
+STEP_BATCH_STATS = _BatchStats()
+
+
 def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: bool = False,
-          clock: Callable[[], float] = time.perf_counter, runner: Optional[Callable] = None) -> dict:
+          clock: Callable[[], float] = time.perf_counter, runner: Optional[Callable] = None,
+          batch_us: int = 0) -> dict:
     """Admit the requests as they arrive (arrival times relative to the call), run them
     concurrently, return the per-request results and the summary. `runner(req, keep_values)`
-    performs one solve (default run_one: the device path in the request's precision)."""
-    runner = runner or run_one
+    performs one solve (default run_one: the device path in the request's precision, with
+    cross-request step batching when batch_us > 0)."""
+    if runner is None:
+        STEP_BATCH_STATS.reset()
+        runner = lambda req, keep: run_one(req, keep, batch_us)  # noqa: E731
     pending = sorted(requests, key=lambda r: r.arrival)
     waiting: List[Request] = []
     results: List[Result] = []
@@ -204,7 +238,10 @@ def serve(requests: List[Request], budget_bytes: int, slots: int, keep_values: b
         "peak_concurrent": state["peak_active"], "peak_reserved_bytes": state["peak_used"],
         "budget_bytes": budget_bytes, "slots": slots, "pool_retries": state["pool_retries"],
         "fp32_requests": sum(1 for r in requests if r.precision == "fp32"),
+        "step_batching_window_us": batch_us,
     }
+    if batch_us:
+        summary["step_batching"] = STEP_BATCH_STATS.summary()
     return {"summary": summary, "results": sorted(results, key=lambda r: r.rid)}
 
 
@@ -216,10 +253,12 @@ def main(argv=None) -> None:
     ap.add_argument("--scale", default="small", choices=["small", "full"])
     ap.add_argument("--budget-gb", type=float, default=16.0)
     ap.add_argument("--slots", type=int, default=16)
+    ap.add_argument("--batch-us", type=int, default=0,
+                    help="cross-request step batching window in microseconds (0: each solve launches alone)")
     args = ap.parse_args(argv)
     os.environ.setdefault("AMRGPU_HOST_THREADS", "2")
     reqs = synthetic_requests(args.requests, args.rate, args.seed, args.scale)
-    out = serve(reqs, int(args.budget_gb * (1 << 30)), args.slots)
+    out = serve(reqs, int(args.budget_gb * (1 << 30)), args.slots, batch_us=args.batch_us)
     s = out["summary"]
     s.update({"scale": args.scale, "rate_per_s": args.rate, "seed": args.seed,
               "mix": {k: sum(1 for r in reqs if r.kind == k) for k in KINDS}})

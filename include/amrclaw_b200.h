@@ -104,6 +104,16 @@ int amrgpu_set_solver(amrgpu_ctx* ctx, const char* name, const double* params, i
  * AMRGPU_EINVAL and changes nothing. */
 int amrgpu_set_pool_limit(amrgpu_ctx* ctx, long long bytes);
 
+/* Cross-request batching of the level step, for serving loops that run several solves
+ * at once in one process (each on its own host thread). window_us > 0: each batched level
+ * step of this (2D) context is handed to the process's step batcher, which launches the
+ * steps that contexts of the same Riemann plugin and precision submit within window_us
+ * microseconds as one kernel over all their tiles; window_us = 0: the context launches
+ * its steps alone (the default). Results do not depend on the batching. No counterpart in
+ * the reference (one solve per program). AMRGPU_EINVAL for a negative window or a 3D
+ * context. Captured-graph replay and dimensionally split steps launch alone. */
+int amrgpu_set_step_batching(amrgpu_ctx* ctx, int window_us);
+
 /* 1: record CUDA events around every patch-step launch (kernel time is then
  * reported by amrgpu_info); 0: no per-launch events. */
 int amrgpu_set_profile(amrgpu_ctx* ctx, int on);

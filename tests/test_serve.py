@@ -129,3 +129,43 @@ def test_pool_cap_stops_a_solve_with_enomem():
     with Solver(rd, pool_limit=1 << 34) as s:  # a roomy cap changes nothing
         s.run(0)
         assert s.info()["finished"] == 1.0
+
+
+@pytest.mark.gpu
+def test_cross_request_step_batching_identical_alone_and_in_the_mix():
+    """Level steps of concurrent solves of the same plugin and precision go out in shared
+    launches (step2_batch_kernel); every result is bit-identical to the solve run alone."""
+    reqs = serve.synthetic_requests(8, rate=100000.0, seed=11, scale="small")
+    for k, r in enumerate(reqs):
+        r.kind = "euler" if k % 2 == 0 else "acoustics"
+        r.params = {}
+        r.precision = "fp64" if k % 2 == 0 else "fp32"
+        r.n = 32 + 4 * (k // 2); r.levels = 2; r.ratio = 2; r.tfinal = 0.06
+    alone = {r.rid: serve.run_one(r, keep_values=True) for r in reqs}
+    out = serve.serve(reqs, budget_bytes=1 << 34, slots=8, keep_values=True, batch_us=3000)
+    s = out["summary"]
+    assert s["completed"] == len(reqs)
+    st = s["step_batching"]
+    assert st["level_steps_submitted"] > 0
+    assert st["level_steps_in_shared_launches"] > 0 and st["mean_solves_per_launch"] > 1.0
+    for res in out["results"]:
+        cells, mass, vals, _, _ = alone[res.rid]
+        assert res.cell_updates == cells
+        np.testing.assert_array_equal(res.values, vals)
+
+
+@pytest.mark.gpu
+def test_step_batching_refuses_bad_windows_and_3d():
+    import configs
+    from amrclaw_b200 import AmrError, Solver, problems
+    with Solver(problems.acoustics_pulse(32, levels=2, ratio=2, tfinal=0.02)) as s:
+        with pytest.raises(AmrError) as e:
+            s.set_step_batching(-1)
+        assert e.value.code == 2
+        s.set_step_batching(100)
+        s.set_step_batching(0)
+        s.run(0)
+    with Solver(configs.euler_blast(n=8, levels=1, tfinal=0.01, max1d=8)) as s3:
+        with pytest.raises(AmrError) as e:
+            s3.set_step_batching(100)
+        assert e.value.code == 2
