@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libamrgpu.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["kernels2d.cu", "noalloc2d.cu", "amr2d.cu", "kernels3d.cu", "flags3d.cu", "amr3d.cu"]
+SOURCES = ["kernels2d.cu", "noalloc2d.cu", "amr2d.cu", "kernels3d.cu", "flags3d.cu", "amr3d.cu", "amr1d.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

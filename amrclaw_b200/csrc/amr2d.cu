@@ -1523,6 +1523,9 @@ class Amr2Gpu {
     const unsigned long long cbits = *h_cfl;
     double cmax;
     std::memcpy(&cmax, &cbits, sizeof(double));
+    // a step block whose bulk copies of its tile did not complete flags the level's
+    // Courant number as infinite (no wave speed makes it so)
+    if (std::isinf(cmax)) throw std::runtime_error("level step: a tile's staging copies did not complete");
     if (profile) {
       float ms = 0;
       AMR_CUDA(cudaEventElapsedTime(&ms, ev_a, ev_b));
@@ -3153,8 +3156,11 @@ int amrgpu_init_precision(const char* rundir, const char* outdir, int write_outp
       s2->g.init(rundir);
     } else if (nd == 3) {
       ctx->s.reset(amrb::make_solver3(rundir, outdir ? outdir : "", write_output != 0, precision_bits == 32));
+    } else if (nd == 1) {
+      if (precision_bits != 64) throw std::invalid_argument("amrgpu_init: the 1D path is FP64 only");
+      ctx->s.reset(amrb::make_solver1(rundir, outdir ? outdir : "", write_output != 0));
     } else {
-      throw std::runtime_error("num_dim must be 2 or 3");
+      throw std::runtime_error("num_dim must be 1, 2 or 3");
     }
     *out = ctx.release();
   });

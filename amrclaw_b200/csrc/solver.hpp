@@ -46,5 +46,7 @@ class AmrSolver {
 // Builds and initialises the 3D solver (amr3d.cu) from the data files in rundir.
 // f32: the FP32 form (float storage, Riemann solves and fluxes; FP64 registers and totals)
 AmrSolver* make_solver3(const std::string& rundir, const std::string& outdir, bool write_output, bool f32);
+// Builds and initialises the 1D solver (amr1d.cu); FP64 only
+AmrSolver* make_solver1(const std::string& rundir, const std::string& outdir, bool write_output);
 
 }  // namespace amrb

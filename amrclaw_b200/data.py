@@ -168,8 +168,9 @@ class ClawData:
         w.blank()
         w.put("dt_variable", bool(self.dt_variable))
         w.put("order", int(self.order))
-        w.put("transverse_waves", _code(_TRANSVERSE, self.transverse_waves))
-        w.put("dimensional_split", _code(_SPLIT, self.dimensional_split))
+        if nd > 1:  # src/1d/amr1.f90 reads order, verbosity, source_split, capa_index, use_fwaves
+            w.put("transverse_waves", _code(_TRANSVERSE, self.transverse_waves))
+            w.put("dimensional_split", _code(_SPLIT, self.dimensional_split))
         w.put("verbosity", int(self.verbosity))
         w.put("source_split", _code(_SOURCE, self.source_split))
         w.put("capa_index", int(self.capa_index))
@@ -216,7 +217,9 @@ class AmrData:
         w = _Writer(path)
         w.put("amr_levels_max", int(self.amr_levels_max))
         n = max(abs(self.amr_levels_max) - 1, 1)
-        for name in ("refinement_ratios_x", "refinement_ratios_y") + (("refinement_ratios_z",) if num_dim == 3 else ()) + ("refinement_ratios_t",):
+        names = ("refinement_ratios_x",) + (("refinement_ratios_y",) if num_dim > 1 else ()) + \
+            (("refinement_ratios_z",) if num_dim == 3 else ()) + ("refinement_ratios_t",)
+        for name in names:
             v = list(getattr(self, name))
             if len(v) < n:
                 raise ValueError("require len(%s) >= %d" % (name, n))
@@ -239,7 +242,7 @@ class AmrData:
         for name in ("dprint", "eprint", "edebug", "gprint", "nprint", "pprint", "rprint", "sprint", "tprint", "uprint"):
             w.put(name, False)
         w.blank()
-        w.put("max1d", int(self.max1d if self.max1d else (60 if num_dim == 2 else 32)))
+        w.put("max1d", int(self.max1d if self.max1d else {1: 500, 2: 60}.get(num_dim, 32)))
         w.close()
 
 
@@ -294,6 +297,12 @@ class ClawRunData:
 
     def __init__(self, num_dim: int = 2):
         self.clawdata = ClawData(num_dim=num_dim)
+        if num_dim == 1:
+            self.clawdata.lower = [0.0]
+            self.clawdata.upper = [1.0]
+            self.clawdata.num_cells = [100]
+            self.clawdata.bc_lower = ["extrap"]
+            self.clawdata.bc_upper = ["extrap"]
         if num_dim == 3:
             self.clawdata.lower = [0.0, 0.0, 0.0]
             self.clawdata.upper = [1.0, 1.0, 1.0]

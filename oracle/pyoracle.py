@@ -53,6 +53,17 @@ def load() -> ctypes.CDLL:
         lib.oracle3d_values.restype = ctypes.c_long
         lib.oracle3d_values.argtypes = [vp, vp, ctypes.c_long]
         lib.oracle3d_gauges.argtypes = [vp, vp, ctypes.c_int]
+        lib.oracle1d_create.restype = vp
+        lib.oracle1d_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+        lib.oracle1d_destroy.argtypes = [vp]
+        lib.oracle1d_run.argtypes = [vp, ctypes.c_int]
+        for n in ("oracle1d_time", "oracle1d_cell_updates", "oracle1d_mass"):
+            getattr(lib, n).restype = ctypes.c_double
+            getattr(lib, n).argtypes = [vp]
+        lib.oracle1d_grids.argtypes = [vp, vp, ctypes.c_int]
+        lib.oracle1d_values.restype = ctypes.c_long
+        lib.oracle1d_values.argtypes = [vp, vp, ctypes.c_long]
+        lib.oracle1d_gauges.argtypes = [vp, vp, ctypes.c_int]
         _lib = lib
     return _lib
 
@@ -154,4 +165,51 @@ class Oracle3D(Oracle2D):
     def close(self) -> None:
         if self.h:
             self.lib.oracle3d_destroy(self.h)
+            self.h = None
+
+
+class Oracle1D:
+    """The 1D restatement (oracle/amr1d.cpp)."""
+
+    def __init__(self, rundir: str, outdir: str | None = None, write_output: bool = False):
+        self.lib = load()
+        self.h = self.lib.oracle1d_create(rundir.encode(), (outdir or rundir).encode(), int(write_output))
+        if not self.h:
+            raise RuntimeError("oracle1d_create failed for %s" % rundir)
+        self.nvar = None
+
+    def run(self, max_cycles: int = 0) -> None:
+        if self.lib.oracle1d_run(self.h, max_cycles) != 0:
+            raise RuntimeError("oracle run failed")
+
+    def time(self) -> float:
+        return self.lib.oracle1d_time(self.h)
+
+    def cell_updates(self) -> float:
+        return self.lib.oracle1d_cell_updates(self.h)
+
+    def mass(self) -> float:
+        return self.lib.oracle1d_mass(self.h)
+
+    def grids(self) -> np.ndarray:
+        n = self.lib.oracle1d_grids(self.h, None, 0)
+        a = np.zeros((n, 4), dtype=np.int32)
+        self.lib.oracle1d_grids(self.h, a.ctypes.data, n)
+        return a
+
+    def values(self) -> np.ndarray:
+        n = self.lib.oracle1d_values(self.h, None, 0)
+        a = np.zeros(n, dtype=np.float64)
+        self.lib.oracle1d_values(self.h, a.ctypes.data, n)
+        return a
+
+    def gauges(self, nvar: int) -> np.ndarray:
+        n = self.lib.oracle1d_gauges(self.h, None, 0)
+        a = np.zeros((n, 3 + nvar), dtype=np.float64)
+        self.lib.oracle1d_gauges(self.h, a.ctypes.data, n)
+        return a
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.oracle1d_destroy(self.h)
             self.h = None

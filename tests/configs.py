@@ -177,3 +177,44 @@ def euler_blast(n: int = 64, levels: int = 3, tfinal: float = 0.5, seed: int = 0
     a.clustering_cutoff = 0.7
     a.max1d = max1d
     return rd
+
+
+def _regression_1d(problem: str, params: dict, lower: float, upper: float, n: int, meqn: int, mwaves: int, tfinal: float,
+                   nout: int, dt_initial: float, steps_max: int, limiter: list, bc: str, gauges: list, levels: int,
+                   ratios: list, tol: float, ibuff: int) -> ClawRunData:
+    rd = ClawRunData(num_dim=1)
+    rd.probdata.add_param("problem", problem)
+    for k, v in params.items():
+        rd.probdata.add_param(k, v)
+    c = rd.clawdata
+    c.lower = [lower]; c.upper = [upper]; c.num_cells = [n]
+    c.num_eqn = meqn; c.num_waves = mwaves; c.num_aux = 0
+    c.output_style = 1; c.num_output_times = nout; c.tfinal = tfinal; c.output_t0 = True
+    c.dt_variable = True; c.dt_initial = dt_initial; c.dt_max = 1e99; c.cfl_desired = 0.9; c.cfl_max = 1.0
+    c.steps_max = steps_max; c.order = 2; c.limiter = limiter
+    c.bc_lower = [bc]; c.bc_upper = [bc]
+    rd.gaugedata.gauges = gauges
+    a = rd.amrdata
+    a.amr_levels_max = levels; a.refinement_ratios_x = ratios; a.refinement_ratios_t = ratios
+    a.flag2refine = True; a.flag2refine_tol = tol; a.regrid_interval = 2; a.regrid_buffer_width = ibuff
+    a.clustering_cutoff = 0.7
+    return rd
+
+
+def acoustics_1d_regression() -> ClawRunData:
+    """tests/acoustics_1d_homogeneous/setrun.py of the reference (gauges 0, 1 pinned)."""
+    return _regression_1d("acoustics_1d", {"rho": 1.0, "bulk": 4.0, "beta": 200.0}, -1.0, 1.0, 40, 2, 2, 0.2, 1, 1e-2, 500,
+                          ["vanleer", "vanleer"], "extrap", [[0, 0.0, 0.0, 0.8], [1, 0.6, 0.0, 0.8]], 3, [2, 2], 0.1, 2)
+
+
+def advection_1d_regression() -> ClawRunData:
+    """tests/advection_1d_example1/setrun.py of the reference (gauges 0, 1 pinned)."""
+    return _regression_1d("advection_1d", {"u": 1.0, "beta": 400.0}, 0.0, 1.0, 40, 1, 1, 0.2, 1, 0.01, 500, ["mc"],
+                          "periodic", [[0, 0.2, 0.0, 1e9], [1, 0.9, 0.0, 1e9]], 3, [2, 2], 0.1, 2)
+
+
+def euler_1d_regression() -> ClawRunData:
+    """tests/euler_1d_wcblast/setrun.py of the reference (gauges 1, 2 pinned): the Woodward-Colella
+    blast waves between walls, 4 levels with ratios 2, 6, 10."""
+    return _regression_1d("euler_1d_wcblast", {"gamma": 1.4}, 0.0, 1.0, 50, 3, 3, 0.015, 2, 1e-6, 5000,
+                          ["minmod"] * 3, "wall", [[1, 0.3, 0.0, 1e9], [2, 0.85, 0.0, 1e9]], 4, [2, 6, 10], 0.1, 3)

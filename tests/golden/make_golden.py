@@ -17,7 +17,8 @@ if len(sys.argv) != 2:
 REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = {"advection_2d_square": [1, 2], "acoustics_2d_radial": [0, 1, 2], "advection_3d_swirl": [1, 2],
-         "advection_2d_annulus": [1, 2]}
+         "advection_2d_annulus": [1, 2], "acoustics_1d_homogeneous": [0, 1], "advection_1d_example1": [0, 1],
+         "euler_1d_wcblast": [1, 2]}
 
 for case, ids in CASES.items():
     rows = []
