@@ -124,9 +124,15 @@ def run_one(req: Request, keep_values: bool = False, batch_us: int = 0):
     pools capped at the request's reservation: (cell updates, mass, values, device ms, pool
     peak). batch_us > 0: its level steps go out in shared launches with those of the other
     solves of the same plugin and precision running meanwhile (amrgpu_set_step_batching)."""
-    from . import Solver
-    with Solver(req.rundata(), batched=True, precision=req.precision, pool_limit=req.reservation(),
-                step_batching_us=batch_us) as s:
+    from . import AmrError, Solver
+    with Solver(req.rundata(), batched=True, precision=req.precision, step_batching_us=batch_us) as s:
+        # the pools a new context starts with can already exceed a small reservation: that
+        # is the same outcome as outgrowing it (readmission with twice the reservation)
+        held = int(s.info()["pool_bytes"])
+        if req.reservation() < held:
+            raise AmrError("reservation of %d bytes is below the %d bytes the new context's pools hold"
+                           % (req.reservation(), held), ENOMEM)
+        s.set_pool_limit(req.reservation())
         s.run(0)
         inf = s.info()
         vals = s.values() if keep_values else None

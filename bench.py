@@ -265,11 +265,22 @@ def swirl_fp32_leg(cpu_threads: int) -> dict:
     return out
 
 
-def serving_leg(n_requests: int = 64) -> dict:
-    """A seeded Poisson stream (200 requests/s) of small 2D solves, FP64/FP32 mixed."""
+def serving_leg(scale: str = "small", n_requests: int = 64, batch_us: int = 0) -> dict:
+    """A seeded Poisson stream (200 requests/s) of 2D solves, FP64/FP32 mixed.
+
+    "small" is 64 shrunken requests under a 16 GiB budget and 16 slots; "full" is the
+    serving configuration itself: requests at the full 2D problem sizes under a 160 GiB
+    budget and 32 slots, with level steps of concurrent solves batched across requests
+    when batch_us > 0."""
     from amrclaw_b200 import serve
-    reqs = serve.synthetic_requests(n_requests, rate=200.0, seed=1, scale="small")
-    return serve.serve(reqs, budget_bytes=16 << 30, slots=16)["summary"]
+    if scale == "full":
+        reqs = serve.synthetic_requests(n_requests, rate=200.0, seed=1, scale="full")
+        out = serve.serve(reqs, budget_bytes=160 << 30, slots=32, batch_us=batch_us)["summary"]
+    else:
+        reqs = serve.synthetic_requests(n_requests, rate=200.0, seed=1, scale="small")
+        out = serve.serve(reqs, budget_bytes=16 << 30, slots=16, batch_us=batch_us)["summary"]
+    out["scale"] = scale
+    return out
 
 
 def parity_record(state: dict, o, prec: str) -> dict:
@@ -334,6 +345,10 @@ def main():
     ap.add_argument("--workload", default="euler3d_blast")
     ap.add_argument("--cpu-steps", type=int, default=0, help="oracle coarse steps timed (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving", default="small", choices=["small", "full", "none"],
+                    help="serving leg: 64 shrunken requests (small) or the full-size stream (full)")
+    ap.add_argument("--serving-requests", type=int, default=0, help="requests in the serving leg (default 64 small, 512 full)")
+    ap.add_argument("--serving-batch-us", type=int, default=0, help="cross-request step batching window of the serving leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -492,7 +507,10 @@ def main():
         rd3, cfg3, _, _, nd3 = workload(args.workload)
         fp32 = fp32_leg(os.cpu_count() or 1, rd3 if nd3 == 3 else None, cfg3)
     os.environ.setdefault("AMRGPU_HOST_THREADS", "2")
-    serving = serving_leg() if headline and not args.no_cpu_baseline else None
+    serving = None
+    if headline and not args.no_cpu_baseline and args.serving != "none":
+        nreq = args.serving_requests or (512 if args.serving == "full" else 64)
+        serving = serving_leg(args.serving, nreq, args.serving_batch_us)
     achieved = kern_cells * bytes_per_update / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
     fp64_roof = None
     if headline and kern_ms > 0:
