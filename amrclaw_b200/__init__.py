@@ -168,7 +168,7 @@ class Solver:
     def values(self) -> np.ndarray:
         n = ctypes.c_longlong()
         _check(self._lib, self._lib.amrgpu_values(self._h, None, 0, ctypes.byref(n)), "amrgpu_values")
-        a = np.zeros(n.value, dtype=np.float64)
+        a = np.empty(n.value, dtype=np.float64)
         _check(self._lib, self._lib.amrgpu_values(self._h, a.ctypes.data_as(_lib.c_double_p), n.value, ctypes.byref(n)),
                "amrgpu_values")
         return a

@@ -1665,6 +1665,12 @@ class Solver1 : public AmrSolver {
       for (int m = g.lstart[lev]; m != 0; m = g.node[m].levelptr) r.insert(r.end(), {m, lev, g.node[m].ilo, g.node[m].ihi});
     return r;
   }
+  long long value_count() override {
+    long long n = 0;
+    for (int lev = 1; lev <= g.lfine; ++lev)
+      for (int m = g.lstart[lev]; m != 0; m = g.node[m].levelptr) n += (long long)g.nvar * (g.mitot_of(m) - 2 * g.nghost);
+    return n;
+  }
   std::vector<double> values() override {
     std::vector<double> out;
     for (int lev = 1; lev <= g.lfine; ++lev)

@@ -2837,23 +2837,32 @@ class Amr2Gpu {
   bool finished() const { return ncycle >= p.nstop || time >= p.tfinal; }
 
   // interior values of all grids (levels 1..lfine, list order), layout [m][j][i] per grid
-  std::vector<double> gather_values() {
+  long long count_values() const {
+    long long tot = 0;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) tot += (long long)nvar * node[m].nx() * node[m].ny();
+    return tot;
+  }
+  // gather_values into out (room for count_values() doubles), copied there from the device
+  void gather_into(double* out) {
     std::vector<int> pl;
     std::vector<long long> off(1, 0);
     for (int lev = 1; lev <= lfine; ++lev)
       for (int m : lgrids[lev]) { pl.push_back(m); off.push_back(off.back() + (long long)nvar * node[m].nx() * node[m].ny()); }
+    const long long tot = off.back();
     off.pop_back();
-    long long tot = 0;
-    for (int m : pl) tot += (long long)nvar * node[m].nx() * node[m].ny();
-    std::vector<double> out(tot);
-    if (tot == 0) return out;
+    if (tot == 0) return;
     DBuf<double> d; d.ensure(tot);
     DBuf<int> dp; dp.upload(pl, st, stg);
     DBuf<long long> doff; doff.upload(off, st, stg);
     launch_gather_interior2(pool.d, d_patches.d, dp.d, doff.d, (int)pl.size(), nvar, d.d, st, f32);
-    AMR_CUDA(cudaMemcpyAsync(out.data(), d.d, sizeof(double) * tot, cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaMemcpyAsync(out, d.d, sizeof(double) * tot, cudaMemcpyDeviceToHost, st));
     sync_stream();
     d.free(); dp.free(); doff.free();
+  }
+  std::vector<double> gather_values() {
+    std::vector<double> out((size_t)count_values());
+    if (!out.empty()) gather_into(out.data());
     return out;
   }
 };
@@ -3079,6 +3088,8 @@ class Solver2 : public AmrSolver {
     return r;
   }
   std::vector<double> values() override { return g.gather_values(); }
+  long long value_count() override { return g.count_values(); }
+  void values_into(double* out) override { g.gather_into(out); }
   std::vector<double> gauge_rows() override {
     const int nv = g.nvar;
     std::vector<double> vals((size_t)g.gslots * nv), out;
@@ -3321,9 +3332,15 @@ int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out) {
 int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out) {
   if (!ctx || !n_out) return AMRGPU_EINVAL;
   return guarded(ctx, [&] {
-    const std::vector<double> v = ctx->s->values();
-    if (out) std::memcpy(out, v.data(), sizeof(double) * std::min<long long>(cap, (long long)v.size()));
-    *n_out = (long long)v.size();
+    // a size query gathers nothing; a buffer with room for every value receives the device
+    // copy directly
+    const long long n = ctx->s->value_count();
+    if (out && cap >= n) ctx->s->values_into(out);
+    else if (out) {
+      const std::vector<double> v = ctx->s->values();
+      std::memcpy(out, v.data(), sizeof(double) * std::min<long long>(cap, (long long)v.size()));
+    }
+    *n_out = n;
   });
 }
 

@@ -2716,21 +2716,32 @@ class Amr3Gpu : public AmrSolver {
   }
   // interior values of every grid in output order, [m][k][j][i] per grid: the solution, or
   // with aux set the aux arrays (naux components)
-  std::vector<double> gather_values(bool aux = false) {
+  long long count_values(bool aux = false) const {
+    long long n = 0;
+    for (int lev = 1; lev <= lfine; ++lev)
+      for (int m : lgrids[lev]) n += (long long)node[m].nx() * node[m].ny() * node[m].nz();
+    return n * (aux ? p.naux : nvar);
+  }
+  // gather_values into out (room for count_values(aux) doubles), copied there from the device
+  void gather_into(double* out, bool aux = false) {
     const int nc = aux ? p.naux : nvar;
     std::vector<int> pl;
     std::vector<long long> c0(1, 0);
     for (int lev = 1; lev <= lfine; ++lev)
       for (int m : lgrids[lev]) { pl.push_back(m); c0.push_back(c0.back() + (long long)node[m].nx() * node[m].ny() * node[m].nz()); }
-    std::vector<double> out((size_t)c0.back() * nc);
-    if (out.empty()) return out;
+    const long long total = c0.back() * nc;
+    if (total == 0) return;
     DBuf<int> dp; dp.upload(pl, st, stg);
     DBuf<long long> dc; dc.upload(c0, st, stg);
-    DBuf<double> dout; dout.ensure(out.size());
+    DBuf<double> dout; dout.ensure(total);
     launch_gather3(pool.d, d_patches.d, dp.d, dc.d, (int)pl.size(), nc, c0.back(), dout.d, st, f32, aux);
-    AMR_CUDA(cudaMemcpyAsync(out.data(), dout.d, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(cudaMemcpyAsync(out, dout.d, sizeof(double) * total, cudaMemcpyDeviceToHost, st));
     sync_stream();
     dp.free(); dc.free(); dout.free();
+  }
+  std::vector<double> gather_values(bool aux = false) {
+    std::vector<double> out((size_t)count_values(aux));
+    if (!out.empty()) gather_into(out.data(), aux);
     return out;
   }
   // the rows of fort.q / fort.a (src/3d/valout.f90:140-160): per grid in output order, its
@@ -2907,6 +2918,8 @@ class Amr3Gpu : public AmrSolver {
     return r;
   }
   std::vector<double> values() override { return gather_values(); }
+  long long value_count() override { return count_values(); }
+  void values_into(double* out) override { gather_into(out); }
   std::vector<double> gauge_rows() override {
     std::vector<double> vals((size_t)gslots * nvar), out;
     if (gslots) AMR_CUDA(cudaMemcpy(vals.data(), d_gauge_out.d, sizeof(double) * vals.size(), cudaMemcpyDeviceToHost));

@@ -72,8 +72,13 @@ __device__ __forceinline__ T philim3(int meth, T r) {
 constexpr int SW_T = SW_TILE;
 constexpr int SW_OWN = SW_T - 3;
 #ifndef SW_MINB
-#define SW_MINB 3  // resident tiles per SM the register budget is sized for
+#define SW_MINB 3  // resident tiles per SM the register budget is sized for (FP64)
 #endif
+#ifndef SW_MINB_F32
+#define SW_MINB_F32 5  // the same for the FP32 form: half the shared buffer, 96 registers, no spills
+#endif
+template <class T>
+constexpr int sweep_min_blocks() { return sizeof(T) == 4 ? SW_MINB_F32 : SW_MINB; }
 
 // (a - 3*b) (m4 = 2) or a: the doubly transverse inputs of flux3.f:429-507
 template <int NV, class T>
@@ -426,7 +431,7 @@ constexpr int sweep3_smem_bytes() {
   return (PH::NW > 12 ? PH::NW : 12) * PH::NV * SW_T * (int)sizeof(T);
 }
 template <int DIR, class T, class PH>
-__global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
+__global__ void __launch_bounds__(SW_T, sweep_min_blocks<T>()) sweep3_kernel(Step3Args A) {
   extern __shared__ __align__(16) unsigned char sweep_smem[];
   sweep3_tile<DIR, T, PH>(A, blockIdx.x, reinterpret_cast<T (*)[SW_T]>(sweep_smem));
 }
@@ -436,7 +441,7 @@ __global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_kernel(Step3Args A) {
 // is left. The tiles are independent (each writes its own stash slots), so no block
 // waits on another.
 template <class T, class PH>
-__global__ void __launch_bounds__(SW_T, SW_MINB) sweep3_queue_kernel(Step3Args A, unsigned int nx, unsigned int nxy, unsigned int ntot) {
+__global__ void __launch_bounds__(SW_T, sweep_min_blocks<T>()) sweep3_queue_kernel(Step3Args A, unsigned int nx, unsigned int nxy, unsigned int ntot) {
   extern __shared__ __align__(16) unsigned char sweep_smem[];
   T (*sW)[SW_T] = reinterpret_cast<T (*)[SW_T]>(sweep_smem);
   __shared__ unsigned int item;
@@ -823,44 +828,73 @@ __global__ void fad3_kernel(const T* flux, long long fs, const long long* face0,
     case 5: comp = 4; h1 = hx; h2 = hy; break;
     default: comp = 5; h1 = hx; h2 = hy; break;
   }
+  // the fine faces in fluxad.f's order (ob outer, oa inner), loaded FAD_B at a time so
+  // the loads are in flight together; the sum keeps that order
+  constexpr int FAD_B = 4;
+  const int nf = E.na * E.nb;
   for (int m = 0; m < nvar; ++m) {
     double acc = sv[m];
     const T* F = flux + ((long long)comp * nvar + m) * fs;
-    for (int ob = 1; ob <= E.nb; ++ob)
-      for (int oa = 1; oa <= E.na; ++oa) {
-        long long c;
-        switch (E.side) {
-          case 1: c = fidx(1, E.a0 + oa, E.b0 + ob); break;
-          case 2: c = fidx(E.a0 + oa, my + 1, E.b0 + ob); break;
-          case 3: c = fidx(mx + 1, E.a0 + oa, E.b0 + ob); break;
-          case 4: c = fidx(E.a0 + oa, 1, E.b0 + ob); break;
-          case 5: c = fidx(E.a0 + oa, E.b0 + ob, 1); break;
-          default: c = fidx(E.a0 + oa, E.b0 + ob, mz + 1); break;
+    for (int u0 = 0; u0 < nf; u0 += FAD_B) {
+      T v[FAD_B];
+#pragma unroll
+      for (int w = 0; w < FAD_B; ++w) {
+        v[w] = T(0);
+        const int u = u0 + w;
+        if (u < nf) {
+          const int oa = u % E.na + 1, ob = u / E.na + 1;
+          long long c;
+          switch (E.side) {
+            case 1: c = fidx(1, E.a0 + oa, E.b0 + ob); break;
+            case 2: c = fidx(E.a0 + oa, my + 1, E.b0 + ob); break;
+            case 3: c = fidx(mx + 1, E.a0 + oa, E.b0 + ob); break;
+            case 4: c = fidx(E.a0 + oa, 1, E.b0 + ob); break;
+            case 5: c = fidx(E.a0 + oa, E.b0 + ob, 1); break;
+            default: c = fidx(E.a0 + oa, E.b0 + ob, mz + 1); break;
+          }
+          v[w] = __ldg(F + c);  // the fluxes are read-only in this kernel
         }
-        acc = acc + (double)F[c] * dtf * h1 * h2;
       }
+#pragma unroll
+      for (int w = 0; w < FAD_B; ++w)
+        if (u0 + w < nf) acc = acc + (double)v[w] * dtf * h1 * h2;
+    }
     sv[m] = acc;
   }
 }
 
-// qad.f:4-534: one register of one side of a fine patch per thread
+// qad.f:4-534: one register of one side of a fine patch per group of QAD_G lanes. The
+// register sums ratio_a x ratio_b coarse-fine Riemann problems in a fixed order (fine rows
+// of the slab outer, cells of the coarse face inner). The group's lanes solve QAD_G of
+// them at a time, and the group's first lane adds their two terms per component into the
+// register in that order, so the sum is the one a single thread would make.
+constexpr int QAD_G = 4;
 template <class T>
-__global__ void qad3_kernel(T* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs, Step3Params sp,
-                            int nvar, double hx, double hy, double hz, double delt, const double* dt_dev) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= njobs) return;
+__global__ void __launch_bounds__(128) qad3_kernel(T* pool, double* regs, const PatchDev* patches, const Qad3Job* jobs, int njobs,
+                                                   Step3Params sp, int nvar, double hx, double hy, double hz, double delt,
+                                                   const double* dt_dev) {
+  const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = (int)(gt % QAD_G), lead = (threadIdx.x & 31) & ~(QAD_G - 1);
+  const long long t = gt / QAD_G;
+  const bool live = t < njobs;
   if (dt_dev) delt = *dt_dev;
-  const Qad3Job J = jobs[t];
+  // lanes past the last job stand in for it with no problems to solve (they still take
+  // part in the group shuffles)
+  const Qad3Job J = jobs[live ? t : njobs - 1];
+  const int n = live ? J.ratio_a * J.ratio_b : 0;
+  const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)((n + QAD_G - 1) / QAD_G));
   const PatchDev& P = patches[J.patch];
   const int mx = P.ihi - P.ilo + 1, my = P.jhi - P.jlo + 1, mz = P.khi - P.klo + 1;
   const long long plane = (long long)P.mitot * P.mjtot * P.mktot;
   const T* q = pool + P.q[P.cur];
   auto at = [&](int i, int j, int k) { return ((long long)(k - 1 + NG3) * P.mjtot + (j - 1 + NG3)) * P.mitot + (i - 1 + NG3); };
   double* sv = regs + P.ffl + (long long)nvar * J.reg0;
-  const double* qc = regs + P.ffl + (long long)nvar * P.lenbc + (long long)nvar * J.reg0;
   T C[6], Fv[6];
   C[0] = T(0); Fv[0] = T(0);
-  for (int m = 1; m <= 5; ++m) C[m] = (T)qc[m - 1];
+  if (live) {
+    const double* qc = regs + P.ffl + (long long)nvar * P.lenbc + (long long)nvar * J.reg0;
+    for (int m = 1; m <= 5; ++m) C[m] = (T)qc[m - 1];
+  }
   int dir; double sgn, h1, h2;
   switch (J.side) {
     case 1: dir = 1; sgn = 1.0; h1 = hy; h2 = hz; break;
@@ -871,9 +905,12 @@ __global__ void qad3_kernel(T* pool, double* regs, const PatchDev* patches, cons
     default: dir = 3; sgn = -1.0; h1 = hx; h2 = hy; break;
   }
   double acc[5];
-  for (int m = 0; m < 5; ++m) acc[m] = sv[m];
-  for (int ks = 1; ks <= J.ratio_b; ++ks) {       // fine rows of the slab (outer loop of qad.f)
-    for (int l = 1; l <= J.ratio_a; ++l) {         // fine cells of the coarse face
+  for (int m = 0; m < 5; ++m) acc[m] = (live && lane == 0) ? sv[m] : 0.0;
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int u = rd * QAD_G + lane;
+    double ta[5], tb[5];
+    if (u < n) {
+      const int ks = u / J.ratio_a + 1, l = u % J.ratio_a + 1;
       const int r = J.row0 + l;                    // fine index along the row, 1-based interior
       const int s = J.slab * J.ratio_b + ks;       // fine index across the rows
       int i, j, k;
@@ -893,13 +930,27 @@ __global__ void qad3_kernel(T* pool, double* regs, const PatchDev* patches, cons
       else euler3d_rpn((T)sp.gamma, (T)sp.gamma1, sp.efix != 0, dir, Fv, C, W, S, amT, apT);
       for (int m = 0; m < 5; ++m) {
         const double am = amT[m], ap = apT[m];  // the registers accumulate in FP64
-        if (sgn > 0.0) acc[m] = acc[m] + am * h1 * h2 * delt + ap * h1 * h2 * delt;
-        else acc[m] = acc[m] - am * h1 * h2 * delt - ap * h1 * h2 * delt;
+        ta[m] = am * h1 * h2 * delt;
+        tb[m] = ap * h1 * h2 * delt;
+      }
+    } else {
+      for (int m = 0; m < 5; ++m) { ta[m] = 0.0; tb[m] = 0.0; }
+    }
+#pragma unroll
+    for (int g = 0; g < QAD_G; ++g) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        const double a = __shfl_sync(0xffffffffu, ta[m], lead + g);
+        const double b = __shfl_sync(0xffffffffu, tb[m], lead + g);
+        if (lane == 0 && rd * QAD_G + g < n) {
+          if (sgn > 0.0) acc[m] = acc[m] + a + b;
+          else acc[m] = acc[m] - a - b;
+        }
       }
     }
   }
-  for (int m = 0; m < 5; ++m) sv[m] = acc[m];
-  (void)nvar; (void)mz;
+  if (live && lane == 0)
+    for (int m = 0; m < 5; ++m) sv[m] = acc[m];
 }
 
 // qad.f:4-534 for the swirl: the coarse-fine Riemann problem moves the jump with the
@@ -1101,9 +1152,42 @@ __global__ void fill3_kernel(Fill3Args a) {
   }
 }
 
-// bc3amr.f90:70-380. phase 0: x sides per (j,k) row; 1: y sides per (i,k); 2: z sides per (i,j).
+// One side of a boundary line: ghost cells lo..hi (1-based along the line, element g at
+// line[(g-1)*st]) set from the interior. code 1 copies cell s_ext into each; code 3 (wall)
+// mirrors cell refl-g into cell g and negates the normal momentum (neg). The sources of a
+// side never overlap its ghost cells, so every source is loaded before the first store.
 template <class T>
-__global__ void bc3_kernel(Bc3Args a, int phase) {
+__device__ __forceinline__ void bc3_side(T* line, long long st, int lo, int hi, int code, int s_ext, int refl, bool neg) {
+  if (code == 1) {
+    const T x = line[(long long)(s_ext - 1) * st];
+    for (int g = lo; g <= hi; ++g) line[(long long)(g - 1) * st] = x;
+    return;
+  }
+  constexpr int MAXG = 4;
+  const int n = hi - lo + 1;
+  if (n <= MAXG) {
+    T buf[MAXG];
+#pragma unroll
+    for (int u = 0; u < MAXG; ++u)
+      if (u < n) buf[u] = line[(long long)(refl - (lo + u) - 1) * st];
+#pragma unroll
+    for (int u = 0; u < MAXG; ++u)
+      if (u < n) line[(long long)(lo + u - 1) * st] = neg ? -buf[u] : buf[u];
+    return;
+  }
+  for (int g = lo; g <= hi; ++g) {
+    const T x = line[(long long)(refl - g - 1) * st];
+    line[(long long)(g - 1) * st] = neg ? -x : x;
+  }
+}
+
+// bc3amr.f90:70-380. phase 0: x sides per (j,k) row; 1: y sides per (i,k); 2: z sides per
+// (i,j). A thread owns one (component, line) pair, lines fastest so that neighbouring
+// threads touch neighbouring cells in phases 1 and 2. Within a line the low side is set
+// before the high side, as in the reference: the two differ only on a patch narrower than
+// its ghost regions, where the high side's mirror reads the low side's ghosts.
+template <class T, int phase>
+__global__ void __launch_bounds__(128, 8) bc3_kernel(Bc3Args a) {
   const int op = blockIdx.y;
   if (op >= a.nops) return;
   const Bc3Op o = a.ops[op];
@@ -1112,40 +1196,25 @@ __global__ void bc3_kernel(Bc3Args a, int phase) {
   else v = static_cast<T*>(a.pool) + a.rects[o.dst_rect].off;
   const int nr = o.nrow, nc = o.ncol, nf = o.nfil;
   const long long plane = (long long)nr * nc * nf;
-  auto V = [&](int m, int i, int j, int k) -> T& { return v[m * plane + ((long long)(k - 1) * nc + (j - 1)) * nr + (i - 1)]; };
-  const int nvar = a.nvar;
   const int lines = phase == 0 ? nc * nf : phase == 1 ? nr * nf : nr * nc;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < lines; t += gridDim.x * blockDim.x) {
-    if (phase == 0) {
-      const int j = t % nc + 1, k = t / nc + 1;
-      if (o.nxl > 0 && (o.bxl == 1 || o.bxl == 3)) {
-        for (int i = 1; i <= o.nxl; ++i) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, o.bxl == 1 ? o.nxl + 1 : 2 * o.nxl + 1 - i, j, k);
-        if (o.bxl == 3) for (int i = 1; i <= o.nxl; ++i) V(1, i, j, k) = -V(1, i, j, k);
-      }
-      if (o.ibeg > 0 && (o.bxr == 1 || o.bxr == 3)) {
-        for (int i = o.ibeg; i <= nr; ++i) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, o.bxr == 1 ? o.ibeg - 1 : 2 * o.ibeg - 1 - i, j, k);
-        if (o.bxr == 3) for (int i = o.ibeg; i <= nr; ++i) V(1, i, j, k) = -V(1, i, j, k);
-      }
-    } else if (phase == 1) {
-      const int i = t % nr + 1, k = t / nr + 1;
-      if (o.nyl > 0 && (o.byl == 1 || o.byl == 3)) {
-        for (int j = 1; j <= o.nyl; ++j) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, o.byl == 1 ? o.nyl + 1 : 2 * o.nyl + 1 - j, k);
-        if (o.byl == 3) for (int j = 1; j <= o.nyl; ++j) V(2, i, j, k) = -V(2, i, j, k);
-      }
-      if (o.jbeg > 0 && (o.byr == 1 || o.byr == 3)) {
-        for (int j = o.jbeg; j <= nc; ++j) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, o.byr == 1 ? o.jbeg - 1 : 2 * o.jbeg - 1 - j, k);
-        if (o.byr == 3) for (int j = o.jbeg; j <= nc; ++j) V(2, i, j, k) = -V(2, i, j, k);
-      }
+  const long long items = (long long)lines * a.nvar;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < items; t += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(t / lines), l = (int)(t % lines);
+    T* base = v + m * plane;
+    if constexpr (phase == 0) {
+      T* line = base + (long long)l * nr;  // row (j,k) = (l % nc + 1, l / nc + 1)
+      if (o.nxl > 0 && (o.bxl == 1 || o.bxl == 3)) bc3_side(line, 1, 1, o.nxl, o.bxl, o.nxl + 1, 2 * o.nxl + 1, o.bxl == 3 && m == 1);
+      if (o.ibeg > 0 && (o.bxr == 1 || o.bxr == 3)) bc3_side(line, 1, o.ibeg, nr, o.bxr, o.ibeg - 1, 2 * o.ibeg - 1, o.bxr == 3 && m == 1);
+    } else if constexpr (phase == 1) {
+      const int i = l % nr, k = l / nr;
+      T* line = base + (long long)k * nc * nr + i;
+      if (o.nyl > 0 && (o.byl == 1 || o.byl == 3)) bc3_side(line, nr, 1, o.nyl, o.byl, o.nyl + 1, 2 * o.nyl + 1, o.byl == 3 && m == 2);
+      if (o.jbeg > 0 && (o.byr == 1 || o.byr == 3)) bc3_side(line, nr, o.jbeg, nc, o.byr, o.jbeg - 1, 2 * o.jbeg - 1, o.byr == 3 && m == 2);
     } else {
-      const int i = t % nr + 1, j = t / nr + 1;
-      if (o.nzl > 0 && (o.bzl == 1 || o.bzl == 3)) {
-        for (int k = 1; k <= o.nzl; ++k) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, j, o.bzl == 1 ? o.nzl + 1 : 2 * o.nzl + 1 - k);
-        if (o.bzl == 3) for (int k = 1; k <= o.nzl; ++k) V(3, i, j, k) = -V(3, i, j, k);
-      }
-      if (o.kbeg > 0 && (o.bzr == 1 || o.bzr == 3)) {
-        for (int k = o.kbeg; k <= nf; ++k) for (int m = 0; m < nvar; ++m) V(m, i, j, k) = V(m, i, j, o.bzr == 1 ? o.kbeg - 1 : 2 * o.kbeg - 1 - k);
-        if (o.bzr == 3) for (int k = o.kbeg; k <= nf; ++k) V(3, i, j, k) = -V(3, i, j, k);
-      }
+      T* line = base + l;  // column (i,j) = (l % nr + 1, l / nr + 1)
+      const long long st = (long long)nr * nc;
+      if (o.nzl > 0 && (o.bzl == 1 || o.bzl == 3)) bc3_side(line, st, 1, o.nzl, o.bzl, o.nzl + 1, 2 * o.nzl + 1, o.bzl == 3 && m == 3);
+      if (o.kbeg > 0 && (o.bzr == 1 || o.bzr == 3)) bc3_side(line, st, o.kbeg, nf, o.bzr, o.kbeg - 1, 2 * o.kbeg - 1, o.bzr == 3 && m == 3);
     }
   }
 }
@@ -1441,8 +1510,10 @@ void launch_qad3(void* pool, double* regs, const PatchDev* patches, const Qad3Jo
     AMR_CUDA(cudaGetLastError());
     return;
   }
-  if (f32) qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt, dt_dev);
-  else qad3_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt, dt_dev);
+  const long long nthr = (long long)njobs * QAD_G;
+  const unsigned nb = (unsigned)((nthr + 127) / 128);
+  if (f32) qad3_kernel<<<nb, 128, 0, s>>>(static_cast<float*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt, dt_dev);
+  else qad3_kernel<<<nb, 128, 0, s>>>(static_cast<double*>(pool), regs, patches, jobs, njobs, sp, nvar, hx, hy, hz, delt, dt_dev);
   AMR_CUDA(cudaGetLastError());
 }
 template <class T>
@@ -1525,16 +1596,18 @@ void launch_fill3(const Fill3Args& a, cudaStream_t s, bool f32) {
   AMR_CUDA(cudaGetLastError());
 }
 // max_lines: the largest number of boundary lines an op of this phase has (nc*nf, nr*nf or
-// nr*nc); a row of blocks per op covers them one line per thread
+// nr*nc); a row of blocks per op covers them, one (component, line) pair per thread
 void launch_bc3(const Bc3Args& a, int phase, cudaStream_t s, bool f32, long long max_lines) {
   if (a.nops <= 0) return;
-  const int bx = (int)std::max<long long>(1, std::min<long long>((max_lines + 127) / 128, 64));
+  const int bx = (int)std::max<long long>(1, std::min<long long>((max_lines * a.nvar + 127) / 128, 1024));
   for (int base = 0; base < a.nops; base += 65535) {
     Bc3Args b = a;
     b.ops = a.ops + base;
     b.nops = std::min(65535, a.nops - base);
-    if (f32) bc3_kernel<float><<<dim3(bx, b.nops), 128, 0, s>>>(b, phase);
-    else bc3_kernel<double><<<dim3(bx, b.nops), 128, 0, s>>>(b, phase);
+    const dim3 g(bx, b.nops);
+    if (phase == 0) f32 ? bc3_kernel<float, 0><<<g, 128, 0, s>>>(b) : bc3_kernel<double, 0><<<g, 128, 0, s>>>(b);
+    else if (phase == 1) f32 ? bc3_kernel<float, 1><<<g, 128, 0, s>>>(b) : bc3_kernel<double, 1><<<g, 128, 0, s>>>(b);
+    else f32 ? bc3_kernel<float, 2><<<g, 128, 0, s>>>(b) : bc3_kernel<double, 2><<<g, 128, 0, s>>>(b);
   }
   AMR_CUDA(cudaGetLastError());
 }

@@ -1,5 +1,6 @@
 // The interface the C ABI drives: one AMR solve on one device (2D or 3D).
 #pragma once
+#include <algorithm>
 #include <cuda_runtime.h>
 #include <string>
 #include <vector>
@@ -40,6 +41,13 @@ class AmrSolver {
   virtual std::vector<double> info() = 0;
   virtual std::vector<int> grid_rows() = 0;                 // 2 + 2*num_dim ints per grid
   virtual std::vector<double> values() = 0;
+  // the number of doubles values() returns, without gathering them
+  virtual long long value_count() = 0;
+  // values() written straight into out (room for value_count() doubles)
+  virtual void values_into(double* out) {
+    const std::vector<double> v = values();
+    std::copy(v.begin(), v.end(), out);
+  }
   virtual std::vector<double> gauge_rows() = 0;             // (3 + nvar) doubles per sample
 };
 
