@@ -178,7 +178,10 @@ int amrgpu_info(amrgpu_ctx* ctx, double* out, int n);
 int amrgpu_grids(amrgpu_ctx* ctx, int* out, int cap, int* n_out);
 
 /* Interior cell values of every grid in amrgpu_grids order, [m][j][i] per grid
- * in 2D and [m][k][j][i] in 3D. */
+ * in 2D and [m][k][j][i] in 3D (one [m][i] row per grid in 1D). *n_out receives
+ * the number of values. out == NULL is a size query and gathers nothing; a buffer
+ * with room for all of them (cap >= *n_out) receives them straight from the
+ * device, a smaller one the first cap. */
 int amrgpu_values(amrgpu_ctx* ctx, double* out, long long cap, long long* n_out);
 
 /* Gauge samples as rows (gauge number, level, time, q1..qmeqn), grouped by gauge
