@@ -40,3 +40,31 @@ def test_init_reports_errors_without_crashing(tmp_path):
     assert rc != 0
     assert lib.amrgpu_last_error()
     assert lib.amrgpu_init(None, None, 0, ctypes.byref(h)) != 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_values_size_query_full_and_partial_buffers(tmp_path, dim):
+    """amrgpu_values: a NULL buffer returns the count, a full buffer receives every value
+    straight from the device, and a short one the first cap values, in both dimensions."""
+    import numpy as np
+    import configs
+    from amrclaw_b200 import Solver, _lib
+    rd = configs.euler_quadrants(n=32, levels=3, tfinal=0.05) if dim == 2 else \
+        configs.euler_blast(n=16, levels=2, tfinal=0.05, seed=0)
+    rd.write(str(tmp_path))
+    with Solver(str(tmp_path)) as s:
+        s.run(3)
+        lib = _lib.load()
+        n = ctypes.c_longlong()
+        assert lib.amrgpu_values(s._h, None, 0, ctypes.byref(n)) == 0
+        full = s.values()
+        assert n.value == full.size > 0
+        cap = n.value // 3
+        part = np.full(cap, np.nan)
+        m = ctypes.c_longlong()
+        assert lib.amrgpu_values(s._h, part.ctypes.data_as(_lib.c_double_p), cap, ctypes.byref(m)) == 0
+        assert m.value == n.value
+        assert np.array_equal(part, full[:cap])
+        again = s.values()
+        assert np.array_equal(again, full)
