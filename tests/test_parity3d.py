@@ -154,3 +154,20 @@ def test_blast_periodic_plain_path_and_richardson():
     rd.amrdata.flag_richardson_tol = 2e-3
     ref, gpu = _both(rd, batched=False)
     _assert_identical(ref, gpu)
+
+
+@pytest.mark.parametrize("ratios", [((3,), (3,), (3,)), ((4,), (2,), (3,)), ((2, 4), (2, 4), (2, 4))])
+@pytest.mark.parametrize("batched", [True, False])
+def test_blast_other_refinement_ratios(ratios, batched):
+    """Refinement ratios other than 2, isotropic and anisotropic: a coarse face of a fine
+    patch then holds 9 to 16 coarse-fine Riemann problems (qad.f), so the device's register
+    groups sum them over several rounds, and the last round of a 3 x 3 face is partial."""
+    levels = len(ratios[0]) + 1
+    rd = configs.euler_blast(n=12, levels=levels, tfinal=0.1, seed=3, max1d=40)
+    a = rd.amrdata
+    rx, ry, rz = (list(r) for r in ratios)
+    a.refinement_ratios_x = rx; a.refinement_ratios_y = ry; a.refinement_ratios_z = rz
+    a.refinement_ratios_t = [max(x, y, z) for x, y, z in zip(rx, ry, rz)]
+    ref, gpu = _both(rd, batched=batched)
+    _assert_identical(ref, gpu)
+    assert ref["grids"][:, 1].max() == levels  # the finest level exists
